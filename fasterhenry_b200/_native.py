@@ -1,0 +1,150 @@
+"""ctypes binding of ``libfhb200.so`` (the C ABI in include/fasterhenry_b200.h).
+
+The library is loaded from this package directory only (built in-tree by
+``fasterhenry_b200/build.py``).  There is no CPU fallback: if the library is
+missing or no B200 is present, the compute entry points raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfhb200.so")
+
+c_double_p = ctypes.POINTER(ctypes.c_double)
+c_int64_p = ctypes.POINTER(ctypes.c_int64)
+
+
+class Node(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_double), ("y", ctypes.c_double), ("z", ctypes.c_double)]
+
+
+class SegmentDef(ctypes.Structure):
+    _fields_ = [("a", ctypes.c_int64), ("b", ctypes.c_int64), ("width", ctypes.c_double),
+                ("height", ctypes.c_double), ("sigma", ctypes.c_double), ("has_width_dir", ctypes.c_int64),
+                ("width_dir", ctypes.c_double * 3)]
+
+
+class Port(ctypes.Structure):
+    _fields_ = [("positive", ctypes.c_int64), ("negative", ctypes.c_int64)]
+
+
+class Filament(ctypes.Structure):
+    _fields_ = [("start", ctypes.c_double * 3), ("end", ctypes.c_double * 3), ("length", ctypes.c_double),
+                ("dir_length", ctypes.c_double * 3), ("dir_width", ctypes.c_double * 3),
+                ("dir_height", ctypes.c_double * 3), ("width", ctypes.c_double), ("height", ctypes.c_double),
+                ("sigma", ctypes.c_double)]
+
+
+class AxisGrading(ctypes.Structure):
+    _fields_ = [("nw", ctypes.c_int64), ("nh", ctypes.c_int64), ("width_ratio", ctypes.c_double),
+                ("height_ratio", ctypes.c_double)]
+
+
+class Discretization(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int64), ("nw", ctypes.c_int64), ("nh", ctypes.c_int64), ("ratio", ctypes.c_double),
+                ("frequency_hz", ctypes.c_double), ("target_skin_depths", ctypes.c_double),
+                ("max_per_axis", ctypes.c_int64), ("per_segment", ctypes.POINTER(AxisGrading)),
+                ("per_segment_len", ctypes.c_int64)]
+
+
+class ErrorInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("detail", ctypes.c_int32), ("index_a", ctypes.c_int64),
+                ("index_b", ctypes.c_int64), ("frequency", ctypes.c_double), ("iterations", ctypes.c_int64),
+                ("residual", ctypes.c_double)]
+
+
+class Counts(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in ("nodes", "segments", "filaments", "meshes", "internal_meshes", "ports")]
+
+
+class Timing(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("inductance_s", "assembly_s", "solve_s", "total_s")]
+
+
+class SweepReport(ctypes.Structure):
+    _fields_ = [("refinement_iterations", ctypes.POINTER(ctypes.c_int32)), ("residual", c_double_p),
+                ("solve_s", ctypes.c_double), ("factor_s", ctypes.c_double), ("refine_s", ctypes.c_double)]
+
+
+# Status codes (fh_status)
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_NO_DEVICE = 2
+ERR_CUDA = 3
+ERR_OUT_OF_MEMORY = 4
+ERR_DEVICE_TIMEOUT = 5
+ERR_GEOMETRY = 10
+ERR_DISCRETIZE = 11
+ERR_KERNEL_COINCIDENT = 12
+ERR_KERNEL_NOT_FINITE = 13
+ERR_MESH = 14
+ERR_INVALID_GRADING = 15
+ERR_INVALID_FREQUENCY = 16
+ERR_SINGULAR = 17
+ERR_NOT_CONVERGED = 18
+ERR_PFFT = 19
+ERR_INVALID_EXCITATION = 20
+ERR_UNSUPPORTED = 30
+
+EXPORTS = [
+    "fh_abi_version", "fh_build_info", "fh_last_error", "fh_device_count", "fh_discretize", "fh_mesh_build",
+    "fh_solver_resolve", "fh_partial_inductance_matrix", "fh_lu_solve_c64", "fh_system_create", "fh_system_destroy",
+    "fh_system_counts", "fh_system_timing", "fh_system_filaments", "fh_system_resistances",
+    "fh_system_mesh_matrices", "fh_system_device_l_mesh", "fh_sweep", "fh_impedance", "fh_sweep_json",
+    "fh_write_zc_mat", "fh_spice_subckt",
+]
+
+_lib = None
+
+
+def load():
+    """Loads the in-tree library (raises OSError when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError("fasterhenry_b200 native library not built: %s (run python -m fasterhenry_b200.build)"
+                      % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    ei = P(ErrorInfo)
+    sz = ctypes.c_size_t
+    L.fh_abi_version.restype = ctypes.c_int32
+    L.fh_build_info.restype = ctypes.c_char_p
+    L.fh_last_error.restype = ctypes.c_char_p
+    L.fh_device_count.restype = ctypes.c_int32
+    L.fh_discretize.argtypes = [P(Node), sz, P(SegmentDef), sz, P(Discretization), P(Filament), sz, P(sz), c_int64_p, ei]
+    L.fh_mesh_build.argtypes = [P(SegmentDef), sz, sz, c_int64_p, P(Port), sz, c_int64_p, c_int64_p, c_double_p, sz, sz,
+                                P(sz), P(sz), P(sz), ei]
+    L.fh_solver_resolve.argtypes = [ctypes.c_int, sz]
+    L.fh_solver_resolve.restype = ctypes.c_int32
+    L.fh_partial_inductance_matrix.argtypes = [P(Filament), sz, c_double_p, P(ctypes.c_int8), ei]
+    L.fh_lu_solve_c64.argtypes = [c_double_p, sz, c_double_p, sz, c_double_p, ei]
+    L.fh_system_create.argtypes = [P(Node), sz, P(SegmentDef), sz, P(Port), sz, P(Discretization), ctypes.c_int,
+                                   P(ctypes.c_void_p), ei]
+    L.fh_system_destroy.argtypes = [ctypes.c_void_p]
+    L.fh_system_destroy.restype = None
+    L.fh_system_counts.argtypes = [ctypes.c_void_p, P(Counts)]
+    L.fh_system_timing.argtypes = [ctypes.c_void_p, P(Timing)]
+    L.fh_system_filaments.argtypes = [ctypes.c_void_p, P(Filament), sz]
+    L.fh_system_resistances.argtypes = [ctypes.c_void_p, c_double_p, sz]
+    L.fh_system_mesh_matrices.argtypes = [ctypes.c_void_p, c_double_p, c_double_p]
+    L.fh_system_device_l_mesh.argtypes = [ctypes.c_void_p, P(c_double_p), P(c_double_p)]
+    L.fh_sweep.argtypes = [ctypes.c_void_p, c_double_p, sz, ctypes.c_int, c_double_p, P(SweepReport), ei]
+    L.fh_impedance.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, c_double_p, ei]
+    L.fh_sweep_json.argtypes = [P(Port), P(ctypes.c_char_p), sz, c_double_p, sz, c_double_p, P(Counts), P(Timing),
+                                ctypes.c_char_p, sz, P(sz)]
+    L.fh_write_zc_mat.argtypes = [ctypes.c_char_p, sz, c_double_p, sz, c_double_p]
+    L.fh_spice_subckt.argtypes = [sz, c_double_p, sz, c_double_p, sz, ctypes.c_char_p, ctypes.c_char_p, sz, P(sz)]
+    for name in EXPORTS:
+        fn = getattr(L, name)
+        if fn.restype is ctypes.c_int:  # default
+            fn.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return load().fh_last_error().decode("utf-8", "replace")

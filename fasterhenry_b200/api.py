@@ -1,0 +1,585 @@
+"""Python host interface mirroring the reference library surface.
+
+Names, argument meanings and error behaviour follow the reference's public
+API (fasterhenry/src/lib.rs:77-118): ``Geometry`` / ``Node`` / ``SegmentDef``
+(geometry.rs), ``Port`` (mesh.rs), ``Discretization`` (solve.rs:409-510),
+``SolverChoice`` (solve.rs:169-193), ``MeshSystem.assemble`` / ``.sweep`` /
+``.impedance`` (solve.rs:680-893), ``solve`` (solve.rs:931),
+``partial_inductance_matrix`` (inductance/batch.rs:246), ``lu_solve``
+(dense.rs:43) and ``SweepResult`` (result.rs:47) with its JSON, MAT v4 and
+SPICE writers (fasterhenry-cli/src/{main,mat,spice}.rs).  Everything that
+computes runs through the C ABI on the GPU; nothing here falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import enum
+import json
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _native as N
+
+MU0 = 4.0e-7 * np.pi
+DENSE_PATH_MAX_FILAMENTS = 10_000
+
+
+# ---------------------------------------------------------------------------
+# Errors (SolveError, KernelError, MeshError, GeometryError, DiscretizeError)
+# ---------------------------------------------------------------------------
+class FasterHenryError(RuntimeError):
+    status = -1
+
+    def __init__(self, message: str, info: Optional[N.ErrorInfo] = None):
+        super().__init__(message)
+        self.info = info
+
+
+class NoDevice(FasterHenryError):
+    status = N.ERR_NO_DEVICE
+
+
+class CudaError(FasterHenryError):
+    status = N.ERR_CUDA
+
+
+class OutOfMemory(FasterHenryError):
+    status = N.ERR_OUT_OF_MEMORY
+
+
+class GeometryError(FasterHenryError):
+    status = N.ERR_GEOMETRY
+
+
+class DiscretizeError(FasterHenryError):
+    status = N.ERR_DISCRETIZE
+
+
+class KernelError(FasterHenryError):
+    @property
+    def first(self) -> int:
+        return int(self.info.index_a) if self.info else 0
+
+    @property
+    def second(self) -> int:
+        return int(self.info.index_b) if self.info else 0
+
+
+class CoincidentSamples(KernelError):
+    status = N.ERR_KERNEL_COINCIDENT
+
+
+class NotFinite(KernelError):
+    status = N.ERR_KERNEL_NOT_FINITE
+
+
+class MeshError(FasterHenryError):
+    status = N.ERR_MESH
+
+
+class InvalidGrading(FasterHenryError):
+    status = N.ERR_INVALID_GRADING
+
+
+class InvalidFrequency(FasterHenryError):
+    status = N.ERR_INVALID_FREQUENCY
+
+    @property
+    def index(self) -> int:
+        return int(self.info.index_a)
+
+    @property
+    def value(self) -> float:
+        return float(self.info.frequency)
+
+
+class Singular(FasterHenryError):
+    status = N.ERR_SINGULAR
+
+    @property
+    def frequency(self) -> float:
+        return float(self.info.frequency)
+
+
+class NotConverged(FasterHenryError):
+    status = N.ERR_NOT_CONVERGED
+
+
+class Unsupported(FasterHenryError):
+    status = N.ERR_UNSUPPORTED
+
+
+class InvalidArgument(FasterHenryError, ValueError):
+    status = N.ERR_INVALID_ARGUMENT
+
+
+_ERRORS = {c.status: c for c in (NoDevice, CudaError, OutOfMemory, GeometryError, DiscretizeError, CoincidentSamples,
+                                 NotFinite, MeshError, InvalidGrading, InvalidFrequency, Singular, NotConverged,
+                                 Unsupported, InvalidArgument)}
+
+
+def _check(status: int, info: Optional[N.ErrorInfo] = None) -> None:
+    if status == N.OK:
+        return
+    cls = _ERRORS.get(status, FasterHenryError)
+    raise cls(N.last_error() or ("status %d" % status), info)
+
+
+# ---------------------------------------------------------------------------
+# Geometry model (geometry.rs, mesh.rs)
+# ---------------------------------------------------------------------------
+@dataclasses.dataclass(frozen=True)
+class Node:
+    x: float
+    y: float
+    z: float
+
+
+@dataclasses.dataclass(frozen=True)
+class SegmentDef:
+    a: int
+    b: int
+    width: float
+    height: float
+    sigma: float
+    width_dir: Optional[Tuple[float, float, float]] = None
+
+
+@dataclasses.dataclass(frozen=True)
+class Port:
+    positive: int
+    negative: int
+    name: Optional[str] = None
+
+
+class Geometry:
+    """Nodes and the segments joining them (geometry.rs:338-467).  Validation
+    of nodes and segments happens in ``add_node`` / ``add_segment``, with the
+    reference's error conditions."""
+
+    def __init__(self):
+        self.nodes: List[Node] = []
+        self.segments: List[SegmentDef] = []
+
+    @classmethod
+    def from_parts(cls, nodes: Sequence, segments: Sequence) -> "Geometry":
+        g = cls()
+        for n in nodes:
+            g.add_node(n if isinstance(n, Node) else Node(*n))
+        for s in segments:
+            g.add_segment(s)
+        return g
+
+    def add_node(self, node) -> int:
+        node = node if isinstance(node, Node) else Node(*node)
+        if not all(np.isfinite([node.x, node.y, node.z])):
+            raise GeometryError("node %d has a non-finite coordinate" % len(self.nodes))
+        self.nodes.append(node)
+        return len(self.nodes) - 1
+
+    def add_segment(self, seg) -> int:
+        if isinstance(seg, dict):
+            seg = SegmentDef(seg["a"], seg["b"], seg["width"], seg["height"], seg["sigma"], seg.get("width_dir"))
+        idx = len(self.segments)
+        # Validate through the library's own rule (Segment::validate).
+        nodes, segs = _nodes(self.nodes), _segments([seg])
+        disc = _disc({"kind": "uniform", "nw": 1, "nh": 1})[0]
+        cnt = ctypes.c_size_t()
+        info = N.ErrorInfo()
+        st = N.load().fh_discretize(nodes, len(self.nodes), segs, 1, ctypes.byref(disc), None, 0, ctypes.byref(cnt),
+                                    None, ctypes.byref(info))
+        if st == N.ERR_GEOMETRY:
+            msg = N.last_error().replace("segment 0", "segment %d" % idx)
+            raise GeometryError(msg, info)
+        _check(st, info)
+        self.segments.append(seg)
+        return idx
+
+    def segment_count(self) -> int:
+        return len(self.segments)
+
+    @classmethod
+    def from_deck(cls, deck) -> "Geometry":
+        return cls.from_parts(deck.nodes, deck.segments)
+
+
+def _nodes(nodes: Sequence) -> ctypes.Array:
+    arr = (N.Node * max(1, len(nodes)))()
+    for i, n in enumerate(nodes):
+        if isinstance(n, Node):
+            arr[i].x, arr[i].y, arr[i].z = n.x, n.y, n.z
+        else:
+            arr[i].x, arr[i].y, arr[i].z = n
+    return arr
+
+
+def _segments(segs: Sequence) -> ctypes.Array:
+    arr = (N.SegmentDef * max(1, len(segs)))()
+    for i, s in enumerate(segs):
+        if isinstance(s, dict):
+            s = SegmentDef(s["a"], s["b"], s["width"], s["height"], s["sigma"], s.get("width_dir"))
+        arr[i].a, arr[i].b = s.a, s.b
+        arr[i].width, arr[i].height, arr[i].sigma = s.width, s.height, s.sigma
+        arr[i].has_width_dir = 0 if s.width_dir is None else 1
+        if s.width_dir is not None:
+            for k in range(3):
+                arr[i].width_dir[k] = s.width_dir[k]
+    return arr
+
+
+def _ports(ports: Sequence) -> ctypes.Array:
+    arr = (N.Port * max(1, len(ports)))()
+    for i, p in enumerate(ports):
+        if isinstance(p, Port):
+            arr[i].positive, arr[i].negative = p.positive, p.negative
+        else:
+            arr[i].positive, arr[i].negative = p[0], p[1]
+    return arr
+
+
+# ---------------------------------------------------------------------------
+# Discretization and SolverChoice (solve.rs:169-510)
+# ---------------------------------------------------------------------------
+class Discretization:
+    """Constructors mirror the reference's variants; the value is a dict
+    (the form the synthetic decks in ``fixtures`` use)."""
+
+    @staticmethod
+    def uniform(nw: int, nh: int) -> dict:
+        return {"kind": "uniform", "nw": nw, "nh": nh}
+
+    @staticmethod
+    def per_segment(grids: Sequence[Tuple[int, int]]) -> dict:
+        return {"kind": "per_segment", "grids": [tuple(g) for g in grids]}
+
+    @staticmethod
+    def graded(nw: int, nh: int, ratio: float) -> dict:
+        return {"kind": "graded", "nw": nw, "nh": nh, "ratio": ratio}
+
+    @staticmethod
+    def skin_depth(frequency_hz: float, target_skin_depths: float, ratio: float, max_per_axis: int = 32) -> dict:
+        return {"kind": "skin_depth", "frequency_hz": frequency_hz, "target_skin_depths": target_skin_depths,
+                "ratio": ratio, "max_per_axis": max_per_axis}
+
+    @staticmethod
+    def per_segment_graded(grids: Sequence[Tuple[int, int, float, float]]) -> dict:
+        return {"kind": "per_segment_graded", "grids": [tuple(g) for g in grids]}
+
+
+_KIND = {"uniform": 0, "per_segment": 1, "graded": 2, "skin_depth": 3, "per_segment_graded": 4}
+
+
+def _disc(d: dict):
+    c = N.Discretization()
+    c.kind = _KIND[d["kind"]]
+    c.nw, c.nh = d.get("nw", 0), d.get("nh", 0)
+    c.ratio = d.get("ratio", 1.0)
+    c.frequency_hz = d.get("frequency_hz", 0.0)
+    c.target_skin_depths = d.get("target_skin_depths", 0.0)
+    c.max_per_axis = d.get("max_per_axis", 32)
+    grids = d.get("grids", [])
+    arr = (N.AxisGrading * max(1, len(grids)))()
+    for i, g in enumerate(grids):
+        arr[i].nw, arr[i].nh = g[0], g[1]
+        arr[i].width_ratio = g[2] if len(g) > 2 else 1.0
+        arr[i].height_ratio = g[3] if len(g) > 3 else 1.0
+    c.per_segment = ctypes.cast(arr, ctypes.POINTER(N.AxisGrading))
+    c.per_segment_len = len(grids)
+    return c, arr
+
+
+class SolverChoice(enum.IntEnum):
+    AUTO = 0
+    DENSE = 1
+    ITERATIVE = 2
+
+    def resolve(self, filaments: int) -> str:
+        return "dense" if N.load().fh_solver_resolve(int(self), filaments) == 0 else "iterative"
+
+
+class Precision(enum.IntEnum):
+    """FP64: the reference's FP64 LU.  MIXED_BF16X3: FP32 factors with
+    split-BF16 x3 tensor-core trailing updates and FP64-residual refinement."""
+    FP64 = 0
+    MIXED_BF16X3 = 1
+
+
+# ---------------------------------------------------------------------------
+# Filaments and the fill
+# ---------------------------------------------------------------------------
+FILAMENT_FIELDS = 19
+
+
+def _fil_array(filaments: np.ndarray) -> ctypes.Array:
+    f = np.ascontiguousarray(filaments, dtype=np.float64).reshape(-1, FILAMENT_FIELDS)
+    arr = (N.Filament * max(1, len(f)))()
+    ctypes.memmove(arr, f.ctypes.data, f.nbytes)
+    return arr
+
+
+def discretize(geometry, discretization: dict) -> Tuple[np.ndarray, np.ndarray]:
+    """Filaments (n x 19: start, end, length, length/width/height unit
+    vectors, width, height, sigma) and the per-segment bundle sizes."""
+    nodes, segs = _geom_arrays(geometry)
+    disc, keep = _disc(discretization)
+    cnt = ctypes.c_size_t()
+    info = N.ErrorInfo()
+    nseg = len(geometry.segments)
+    per = np.zeros(max(1, nseg), dtype=np.int64)
+    L = N.load()
+    _check(L.fh_discretize(nodes, len(geometry.nodes), segs, nseg, ctypes.byref(disc), None, 0, ctypes.byref(cnt),
+                           None, ctypes.byref(info)), info)
+    out = (N.Filament * max(1, cnt.value))()
+    _check(L.fh_discretize(nodes, len(geometry.nodes), segs, nseg, ctypes.byref(disc), out, cnt.value,
+                           ctypes.byref(cnt), per.ctypes.data_as(N.c_int64_p), ctypes.byref(info)), info)
+    arr = np.frombuffer(out, dtype=np.float64, count=cnt.value * FILAMENT_FIELDS).reshape(-1, FILAMENT_FIELDS).copy()
+    return arr, per[:nseg].copy()
+
+
+def _geom_arrays(geometry):
+    return _nodes(geometry.nodes), _segments(geometry.segments)
+
+
+def partial_inductance_matrix(filaments: np.ndarray, methods: bool = False):
+    """Symmetric partial-inductance matrix of the filaments (batch.rs:246),
+    evaluated on the GPU.  With ``methods=True`` also returns the per-entry
+    inductance::Method ids."""
+    f = np.ascontiguousarray(filaments, dtype=np.float64).reshape(-1, FILAMENT_FIELDS)
+    n = len(f)
+    Lm = np.zeros((n, n), order="F")
+    meth = np.zeros((n, n), dtype=np.int8, order="F") if methods else None
+    info = N.ErrorInfo()
+    _check(N.load().fh_partial_inductance_matrix(_fil_array(f), n, Lm.ctypes.data_as(N.c_double_p),
+                                                 meth.ctypes.data_as(ctypes.POINTER(ctypes.c_int8)) if methods else None,
+                                                 ctypes.byref(info)), info)
+    return (Lm, meth) if methods else Lm
+
+
+def mutual_inductance(a: np.ndarray, b: np.ndarray) -> float:
+    """Partial mutual inductance of two filaments (inductance/mod.rs:215)."""
+    return float(partial_inductance_matrix(np.stack([a, b]))[0, 1])
+
+
+def self_inductance(f: np.ndarray) -> float:
+    """Partial self inductance (inductance/mod.rs:196)."""
+    return float(partial_inductance_matrix(np.asarray(f).reshape(1, -1))[0, 0])
+
+
+def lu_solve(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Solve a x = b (complex) with the device FP64 blocked LU (dense.rs:43).
+    Raises Singular on an exactly zero pivot."""
+    a = np.asarray(a, dtype=np.complex128)
+    if a.ndim != 2 or a.shape[0] != a.shape[1]:
+        raise InvalidArgument("lu_solve: the matrix must be square")
+    bb = np.asarray(b, dtype=np.complex128)
+    vec = bb.ndim == 1
+    bb = bb.reshape(a.shape[0], -1)
+    if bb.shape[0] != a.shape[0]:
+        raise InvalidArgument("lu_solve: right-hand side has the wrong number of rows")
+    af = np.asfortranarray(a)
+    bf = np.asfortranarray(bb)
+    x = np.zeros_like(bf, order="F")
+    info = N.ErrorInfo()
+    _check(N.load().fh_lu_solve_c64(af.ctypes.data_as(N.c_double_p), a.shape[0], bf.ctypes.data_as(N.c_double_p),
+                                    bf.shape[1], x.ctypes.data_as(N.c_double_p), ctypes.byref(info)), info)
+    return x.reshape(-1) if vec else x
+
+
+def mesh_matrix(geometry, per_segment: Sequence[int], ports: Sequence):
+    """Loop basis M as CSR (row_ptr, branch, sign, internal_count)
+    (mesh.rs:170)."""
+    segs = _segments(geometry.segments)
+    per = np.ascontiguousarray(per_segment, dtype=np.int64)
+    pts = _ports(ports)
+    nrows, nnz, nint = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_size_t()
+    info = N.ErrorInfo()
+    L = N.load()
+    _check(L.fh_mesh_build(segs, len(geometry.segments), len(geometry.nodes), per.ctypes.data_as(N.c_int64_p), pts,
+                           len(ports), None, None, None, 0, 0, ctypes.byref(nrows), ctypes.byref(nnz),
+                           ctypes.byref(nint), ctypes.byref(info)), info)
+    rp = np.zeros(nrows.value + 1, dtype=np.int64)
+    br = np.zeros(nnz.value, dtype=np.int64)
+    sg = np.zeros(nnz.value)
+    _check(L.fh_mesh_build(segs, len(geometry.segments), len(geometry.nodes), per.ctypes.data_as(N.c_int64_p), pts,
+                           len(ports), rp.ctypes.data_as(N.c_int64_p), br.ctypes.data_as(N.c_int64_p),
+                           sg.ctypes.data_as(N.c_double_p), len(rp), len(br), ctypes.byref(nrows), ctypes.byref(nnz),
+                           ctypes.byref(nint), ctypes.byref(info)), info)
+    return rp, br, sg, nint.value
+
+
+# ---------------------------------------------------------------------------
+# The dense system (MeshSystem) and the sweep result
+# ---------------------------------------------------------------------------
+@dataclasses.dataclass
+class SweepResult:
+    """result.rs:47-104: impedance_ohm[k][i][j] is Z at frequencies_hz[k]."""
+    ports: List[Port]
+    frequencies_hz: List[float]
+    impedance_ohm: np.ndarray          # (nf, p, p) complex
+    counts: Dict[str, int]
+    timing: Optional[Dict[str, float]] = None
+    refinement_iterations: Optional[List[int]] = None
+    residuals: Optional[List[float]] = None
+    precision: Precision = Precision.FP64
+
+    SCHEMA_VERSION = 1
+
+    def resistance(self, index: int) -> np.ndarray:
+        return self.impedance_ohm[index].real.copy()
+
+    def inductance(self, index: int) -> Optional[np.ndarray]:
+        omega = 2.0 * np.pi * self.frequencies_hz[index]
+        return None if omega == 0.0 else self.impedance_ohm[index].imag / omega
+
+    def without_timing(self) -> "SweepResult":
+        return dataclasses.replace(self, timing=None)
+
+    def _z_interleaved(self) -> np.ndarray:
+        z = np.ascontiguousarray(self.impedance_ohm, dtype=np.complex128)
+        return z.view(np.float64).reshape(-1)
+
+    def to_json(self) -> str:
+        """The reference's JSON document (schema_version 1), formatted by the
+        library (serde_json float formatting)."""
+        ports = _ports(self.ports)
+        names = (ctypes.c_char_p * max(1, len(self.ports)))()
+        for i, p in enumerate(self.ports):
+            names[i] = (p.name.encode() if isinstance(p, Port) and p.name else None)
+        f = np.ascontiguousarray(self.frequencies_hz, dtype=np.float64)
+        z = self._z_interleaved()
+        c = N.Counts(*[self.counts[k] for k in ("nodes", "segments", "filaments", "meshes", "internal_meshes", "ports")])
+        t = None
+        if self.timing is not None:
+            t = N.Timing(*[self.timing[k] for k in ("inductance_s", "assembly_s", "solve_s", "total_s")])
+        L = N.load()
+        length = ctypes.c_size_t()
+        args = [ports, names, len(self.ports), f.ctypes.data_as(N.c_double_p), len(f), z.ctypes.data_as(N.c_double_p),
+                ctypes.byref(c), ctypes.byref(t) if t is not None else None]
+        _check(L.fh_sweep_json(*args, None, 0, ctypes.byref(length)))
+        buf = ctypes.create_string_buffer(length.value + 1)
+        _check(L.fh_sweep_json(*args, buf, length.value + 1, ctypes.byref(length)))
+        return buf.value.decode()
+
+    def write_zc_mat(self, path: str) -> None:
+        f = np.ascontiguousarray(self.frequencies_hz, dtype=np.float64)
+        z = self._z_interleaved()
+        _check(N.load().fh_write_zc_mat(path.encode(), len(self.ports), f.ctypes.data_as(N.c_double_p), len(f),
+                                        z.ctypes.data_as(N.c_double_p)))
+
+    def spice_subckt(self, frequency_index: int, name: str) -> str:
+        f = np.ascontiguousarray(self.frequencies_hz, dtype=np.float64)
+        z = self._z_interleaved()
+        L = N.load()
+        length = ctypes.c_size_t()
+        args = [len(self.ports), f.ctypes.data_as(N.c_double_p), len(f), z.ctypes.data_as(N.c_double_p),
+                frequency_index, name.encode()]
+        _check(L.fh_spice_subckt(*args, None, 0, ctypes.byref(length)))
+        buf = ctypes.create_string_buffer(length.value + 1)
+        _check(L.fh_spice_subckt(*args, buf, length.value + 1, ctypes.byref(length)))
+        return buf.value.decode()
+
+
+class MeshSystem:
+    """Assembled dense system resident on the GPU (solve.rs:643-893)."""
+
+    def __init__(self, handle, geometry, ports):
+        self._h = handle
+        self.ports = [p if isinstance(p, Port) else Port(p[0], p[1]) for p in ports]
+        c = N.Counts()
+        _check(N.load().fh_system_counts(handle, ctypes.byref(c)))
+        self._counts = {k: int(getattr(c, k)) for k, _ in N.Counts._fields_}
+
+    @classmethod
+    def assemble(cls, geometry, ports: Sequence, discretization: dict,
+                 solver: SolverChoice = SolverChoice.DENSE) -> "MeshSystem":
+        nodes, segs = _geom_arrays(geometry)
+        pts = _ports(ports)
+        disc, keep = _disc(discretization)
+        h = ctypes.c_void_p()
+        info = N.ErrorInfo()
+        _check(N.load().fh_system_create(nodes, len(geometry.nodes), segs, len(geometry.segments), pts, len(ports),
+                                         ctypes.byref(disc), int(solver), ctypes.byref(h), ctypes.byref(info)), info)
+        return cls(h, geometry, ports)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            N.load().fh_system_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def counts(self) -> Dict[str, int]:
+        return dict(self._counts)
+
+    def timing(self) -> Dict[str, float]:
+        t = N.Timing()
+        _check(N.load().fh_system_timing(self._h, ctypes.byref(t)))
+        return {k: float(getattr(t, k)) for k, _ in N.Timing._fields_}
+
+    def filaments(self) -> np.ndarray:
+        n = self._counts["filaments"]
+        out = (N.Filament * max(1, n))()
+        _check(N.load().fh_system_filaments(self._h, out, n))
+        return np.frombuffer(out, dtype=np.float64, count=n * FILAMENT_FIELDS).reshape(-1, FILAMENT_FIELDS).copy()
+
+    def filament_resistances(self) -> np.ndarray:
+        n = self._counts["filaments"]
+        out = np.zeros(max(1, n))
+        _check(N.load().fh_system_resistances(self._h, out.ctypes.data_as(N.c_double_p), n))
+        return out[:n]
+
+    def mesh_matrices(self) -> Tuple[np.ndarray, np.ndarray]:
+        loops = self._counts["meshes"]
+        r = np.zeros((loops, loops), order="F")
+        l = np.zeros((loops, loops), order="F")
+        _check(N.load().fh_system_mesh_matrices(self._h, r.ctypes.data_as(N.c_double_p), l.ctypes.data_as(N.c_double_p)))
+        return r, l
+
+    def sweep(self, frequencies: Sequence[float], precision: Precision = Precision.FP64) -> SweepResult:
+        f = np.ascontiguousarray(frequencies, dtype=np.float64)
+        p = self._counts["ports"]
+        z = np.zeros((len(f), p, p), dtype=np.complex128)
+        iters = np.zeros(max(1, len(f)), dtype=np.int32)
+        resid = np.zeros(max(1, len(f)))
+        rep = N.SweepReport(iters.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), resid.ctypes.data_as(N.c_double_p))
+        info = N.ErrorInfo()
+        _check(N.load().fh_sweep(self._h, f.ctypes.data_as(N.c_double_p), len(f), int(precision),
+                                 z.ctypes.data_as(N.c_double_p), ctypes.byref(rep), ctypes.byref(info)), info)
+        timing = self.timing()
+        return SweepResult(self.ports, [float(x) for x in f], z, self.counts(), timing,
+                           [int(x) for x in iters[:len(f)]] if precision != Precision.FP64 else None,
+                           [float(x) for x in resid[:len(f)]] if precision != Precision.FP64 else None, precision)
+
+    def impedance(self, frequency: float, precision: Precision = Precision.FP64) -> np.ndarray:
+        return self.sweep([frequency], precision).impedance_ohm[0]
+
+
+def solve(geometry, ports: Sequence, discretization: dict, frequencies: Sequence[float],
+          precision: Precision = Precision.FP64) -> SweepResult:
+    """MeshSystem.assemble followed by MeshSystem.sweep (solve.rs:931-938)."""
+    with MeshSystem.assemble(geometry, ports, discretization) as system:
+        return system.sweep(frequencies, precision)
+
+
+def skin_depth(frequency_hz: float, sigma: float) -> float:
+    return 1.0 / np.sqrt(np.pi * frequency_hz * MU0 * sigma)
+
+
+def device_count() -> int:
+    return int(N.load().fh_device_count())
+
+
+def build_info() -> str:
+    return N.load().fh_build_info().decode()

@@ -1,0 +1,612 @@
+// C ABI of the device path: the dense system (MeshSystem), sweeps, and the
+// library-level kernels (fill, LU).  See include/fasterhenry_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "fh_device.cuh"
+#include "fh_lu.cuh"
+
+using namespace fhb;
+
+struct fh_system {
+    std::vector<fh_node> nodes;
+    std::vector<fh_segment_def> segments;
+    std::vector<fh_port> ports;
+    Discretized disc;
+    LoopBasis loops;
+    std::vector<double> resistances;
+    int64_t n = 0, nloops = 0, m = 0, p = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    double *d_Lm = nullptr, *d_Rm = nullptr;
+    fh_counts counts{};
+    fh_timing timing{};
+    FillStats fill{};
+    float ms_congruence = 0;
+    ~fh_system() {
+        if (d_Lm) cudaFree(d_Lm);
+        if (d_Rm) cudaFree(d_Rm);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace fhb {
+
+fh_status ensure_device(fh_error_info *err) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+        return fail(err, FH_ERR_NO_DEVICE, "no CUDA device is available (this library has no CPU fallback)");
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess)
+        return fail(err, FH_ERR_NO_DEVICE, "cannot query the CUDA device");
+    if (prop.major != 10)
+        return fail(err, FH_ERR_NO_DEVICE,
+                    std::string("this build targets sm_100a (B200); found ") + prop.name + " sm_" +
+                        std::to_string(prop.major) + std::to_string(prop.minor));
+    return FH_OK;
+}
+
+namespace {
+
+// RAII device buffer.
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    ~DBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t count) {
+        n = count;
+        return cudaMalloc((void **)&p, std::max<size_t>(1, count) * sizeof(T));
+    }
+};
+
+#define FHB_ALLOC(buf, count)                                                                   \
+    do {                                                                                        \
+        if ((buf).alloc(count) != cudaSuccess) {                                                \
+            cudaGetLastError();                                                                 \
+            return fail(err, FH_ERR_OUT_OF_MEMORY,                                              \
+                        "device allocation of " + std::to_string((size_t)(count) * sizeof(*(buf).p)) + \
+                            " bytes failed");                                                   \
+        }                                                                                       \
+    } while (0)
+
+double wall() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+std::string fstr(double v) {
+    char b[64];
+    snprintf(b, sizeof b, "%g", v);
+    return b;
+}
+
+constexpr double kTau = 6.283185307179586;
+
+// Factor + solve + Schur for `count` frequencies in FP64.  x_out (count x m x
+// p complex) receives the FP64 solutions; z (count x p x p) the impedances.
+fh_status sweep_chunk_fp64(fh_system *s, const double *d_omega, int count, double *d_x, double *d_z, int *h_singular,
+                           float *ms_factor, fh_error_info *err) {
+    const int64_t m = s->m, p = s->p, ld = s->nloops;
+    cudaStream_t st = s->stream;
+    if (m > 0) {
+        DBuf<double> a;
+        DBuf<int> piv, sing;
+        FHB_ALLOC(a, (size_t)count * m * m * 2);
+        FHB_ALLOC(piv, (size_t)count * m);
+        FHB_ALLOC(sing, (size_t)count);
+        FHB_CUDA(cudaMemsetAsync(sing.p, 0, sizeof(int) * count, st));
+        fh_status e = form_system<double>(s->d_Rm, s->d_Lm, ld, m, d_omega, count, a.p, st, err);
+        if (e) return e;
+        e = form_rhs<double>(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, st, err);
+        if (e) return e;
+        LuWork w;
+        DBuf<double> pv;
+        DBuf<int> pi;
+        DBuf<unsigned> tk;
+        w.max_chunks = 16;
+        FHB_ALLOC(pv, (size_t)count * w.max_chunks);
+        FHB_ALLOC(pi, (size_t)count * w.max_chunks);
+        FHB_ALLOC(tk, (size_t)count);
+        FHB_CUDA(cudaMemsetAsync(tk.p, 0, sizeof(unsigned) * count, st));
+        w.partial_val = pv.p;
+        w.partial_idx = pi.p;
+        w.tickets = tk.p;
+        LuBatch<double> b;
+        b.a = a.p;
+        b.pivots = piv.p;
+        b.singular = sing.p;
+        b.m = m;
+        b.count = count;
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, st);
+        e = lu_factor<double>(b, w, 64, TrailingUpdate::Simt, st, err);
+        cudaEventRecord(e1, st);
+        if (!e) e = lu_solve<double>(b, d_x, (int)p, 64, st, err);
+        if (e) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return e;
+        }
+        FHB_CUDA(cudaMemcpyAsync(h_singular, sing.p, sizeof(int) * count, cudaMemcpyDeviceToHost, st));
+        FHB_CUDA(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms_factor) *ms_factor += ms;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    } else {
+        std::fill(h_singular, h_singular + count, 0);
+    }
+    return schur(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, d_z, st, err);
+}
+
+// Mixed form: FP32 factors (trailing updates on the tensor cores when
+// available), FP64 residuals, iterative refinement of x.  Frequencies that do
+// not converge are flagged in h_failed.
+fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, double *d_x, double *d_z, int *h_singular,
+                            int *h_failed, int32_t *iters_out, double *resid_out, float *ms_factor, float *ms_refine,
+                            TrailingUpdate mode, fh_error_info *err) {
+    const int64_t m = s->m, p = s->p, ld = s->nloops;
+    cudaStream_t st = s->stream;
+    std::fill(h_failed, h_failed + count, 0);
+    if (m == 0) {
+        std::fill(h_singular, h_singular + count, 0);
+        return schur(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, d_z, st, err);
+    }
+    DBuf<float> a, d32;
+    DBuf<double> r, rnorm, bnorm, dnorm, xnorm;
+    DBuf<int> piv, sing;
+    const int64_t vec = m * p;  // complex entries per frequency
+    FHB_ALLOC(a, (size_t)count * m * m * 2);
+    FHB_ALLOC(d32, (size_t)count * vec * 2);
+    FHB_ALLOC(r, (size_t)count * vec * 2);
+    FHB_ALLOC(rnorm, (size_t)count);
+    FHB_ALLOC(bnorm, (size_t)count);
+    FHB_ALLOC(dnorm, (size_t)count);
+    FHB_ALLOC(xnorm, (size_t)count);
+    FHB_ALLOC(piv, (size_t)count * m);
+    FHB_ALLOC(sing, (size_t)count);
+    FHB_CUDA(cudaMemsetAsync(sing.p, 0, sizeof(int) * count, st));
+    fh_status e = form_system<float>(s->d_Rm, s->d_Lm, ld, m, d_omega, count, a.p, st, err);
+    if (e) return e;
+    e = form_rhs<double>(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, r.p, st, err);  // r0 = b
+    if (e) return e;
+    e = max_abs_per_matrix(r.p, 2 * vec, count, bnorm.p, st, err);
+    if (e) return e;
+    FHB_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * 2 * count * vec, st));
+    LuWork w;
+    DBuf<double> pv;
+    DBuf<int> pi;
+    DBuf<unsigned> tk;
+    w.max_chunks = 16;
+    FHB_ALLOC(pv, (size_t)count * w.max_chunks);
+    FHB_ALLOC(pi, (size_t)count * w.max_chunks);
+    FHB_ALLOC(tk, (size_t)count);
+    FHB_CUDA(cudaMemsetAsync(tk.p, 0, sizeof(unsigned) * count, st));
+    w.partial_val = pv.p;
+    w.partial_idx = pi.p;
+    w.tickets = tk.p;
+    LuBatch<float> b;
+    b.a = a.p;
+    b.pivots = piv.p;
+    b.singular = sing.p;
+    b.m = m;
+    b.count = count;
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    cudaEventRecord(e0, st);
+    e = lu_factor<float>(b, w, 64, mode, st, err);
+    cudaEventRecord(e1, st);
+    if (e) return e;
+    std::vector<double> hb(count), hd(count), hx(count), hr(count), prev(count, INFINITY);
+    std::vector<int> done(count, 0), grow(count, 0);
+    FHB_CUDA(cudaMemcpyAsync(hb.data(), bnorm.p, 8 * count, cudaMemcpyDeviceToHost, st));
+    const int kMaxIter = 40;
+    int it = 0;
+    for (; it < kMaxIter; ++it) {
+        e = convert_c64_to_c32(r.p, d32.p, count * vec, st, err);
+        if (!e) e = lu_solve<float>(b, d32.p, (int)p, 64, st, err);
+        if (!e) e = add_c32_to_c64(d_x, d32.p, count * vec, st, err);
+        if (!e) e = residual_fp64(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, r.p, rnorm.p, st, err);
+        if (e) return e;
+        // correction and solution norms (max-abs) for the stopping rule
+        e = max_abs_per_matrix_f32(d32.p, 2 * vec, count, dnorm.p, st, err);
+        if (!e) e = max_abs_per_matrix(d_x, 2 * vec, count, xnorm.p, st, err);
+        if (e) return e;
+        FHB_CUDA(cudaMemcpyAsync(hd.data(), dnorm.p, 8 * count, cudaMemcpyDeviceToHost, st));
+        FHB_CUDA(cudaMemcpyAsync(hx.data(), xnorm.p, 8 * count, cudaMemcpyDeviceToHost, st));
+        FHB_CUDA(cudaMemcpyAsync(hr.data(), rnorm.p, 8 * count, cudaMemcpyDeviceToHost, st));
+        FHB_CUDA(cudaStreamSynchronize(st));
+        bool all = true;
+        for (int f = 0; f < count; ++f) {
+            if (done[f]) continue;
+            double rel = hx[f] > 0 ? hd[f] / hx[f] : 0.0;
+            if (rel <= 1e-14 || hd[f] == 0.0) {
+                done[f] = 1;
+                if (iters_out) iters_out[f] = it + 1;
+                continue;
+            }
+            if (!(hd[f] < prev[f])) ++grow[f];
+            if (grow[f] >= 3 || !std::isfinite(hd[f])) {
+                done[f] = 1;
+                h_failed[f] = 1;
+                if (iters_out) iters_out[f] = it + 1;
+                continue;
+            }
+            prev[f] = hd[f];
+            all = false;
+        }
+        if (all) break;
+    }
+    for (int f = 0; f < count; ++f) {
+        if (!done[f]) {
+            h_failed[f] = 1;
+            if (iters_out) iters_out[f] = it;
+        }
+        if (resid_out) resid_out[f] = hb[f] > 0 ? hr[f] / hb[f] : 0.0;
+    }
+    cudaEventRecord(e2, st);
+    FHB_CUDA(cudaMemcpyAsync(h_singular, sing.p, sizeof(int) * count, cudaMemcpyDeviceToHost, st));
+    e = schur(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, d_z, st, err);
+    if (e) return e;
+    FHB_CUDA(cudaStreamSynchronize(st));
+    float ms1 = 0, ms2 = 0;
+    cudaEventElapsedTime(&ms1, e0, e1);
+    cudaEventElapsedTime(&ms2, e1, e2);
+    if (ms_factor) *ms_factor += ms1;
+    if (ms_refine) *ms_refine += ms2;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    return FH_OK;
+}
+
+}  // namespace
+}  // namespace fhb
+
+extern "C" {
+
+const char *fh_build_info(void) {
+    return "fasterhenry_b200 0.1.0 (sm_100a; FP64 fill; batched complex LU FP64 / FP32+bf16x3 tensor trailing "
+           "updates with FP64 iterative refinement)";
+}
+
+int32_t fh_device_count(void) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int usable = 0;
+    for (int d = 0; d < count; ++d) {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, d) == cudaSuccess && prop.major == 10) ++usable;
+    }
+    return usable;
+}
+
+fh_status fh_partial_inductance_matrix(const fh_filament *filaments, size_t n, double *L, int8_t *methods,
+                                       fh_error_info *err) {
+    clear_error(err);
+    if ((n && (!filaments || !L))) return fail(err, FH_ERR_INVALID_ARGUMENT, "null argument");
+    fh_status st = ensure_device(err);
+    if (st) return st;
+    if (n == 0) return FH_OK;
+    std::vector<DevFil> h(n);
+    for (size_t i = 0; i < n; ++i) h[i] = make_devfil(filaments[i]);
+    DBuf<DevFil> d_fil;
+    DBuf<double> d_L;
+    DBuf<int8_t> d_m;
+    FHB_ALLOC(d_fil, n);
+    FHB_ALLOC(d_L, n * n);
+    if (methods) FHB_ALLOC(d_m, n * n);
+    cudaStream_t s;
+    FHB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    std::unique_ptr<CUstream_st, decltype(&cudaStreamDestroy)> guard(s, &cudaStreamDestroy);
+    FHB_CUDA(cudaMemcpyAsync(d_fil.p, h.data(), n * sizeof(DevFil), cudaMemcpyHostToDevice, s));
+    FHB_CUDA(cudaMemsetAsync(d_L.p, 0, n * n * sizeof(double), s));
+    if (methods) FHB_CUDA(cudaMemsetAsync(d_m.p, 0, n * n, s));
+    st = device_fill(d_fil.p, (int64_t)n, d_L.p, methods ? d_m.p : nullptr, s, nullptr, err);
+    if (st) return st;
+    FHB_CUDA(cudaMemcpyAsync(L, d_L.p, n * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (methods) FHB_CUDA(cudaMemcpyAsync(methods, d_m.p, n * n, cudaMemcpyDeviceToHost, s));
+    FHB_CUDA(cudaStreamSynchronize(s));
+    return FH_OK;
+}
+
+fh_status fh_lu_solve_c64(const double *a, size_t n, const double *b, size_t nrhs, double *x, fh_error_info *err) {
+    clear_error(err);
+    if (n && (!a || !b || !x)) return fail(err, FH_ERR_INVALID_ARGUMENT, "null argument");
+    fh_status st = ensure_device(err);
+    if (st) return st;
+    if (n == 0) return FH_OK;
+    if (n > (size_t)INT32_MAX / 2) return fail(err, FH_ERR_INVALID_ARGUMENT, "order too large");
+    DBuf<double> d_a, d_x, pv;
+    DBuf<int> piv, sing, pi;
+    DBuf<unsigned> tk;
+    FHB_ALLOC(d_a, 2 * n * n);
+    FHB_ALLOC(d_x, 2 * n * nrhs);
+    FHB_ALLOC(piv, n);
+    FHB_ALLOC(sing, 1);
+    FHB_ALLOC(pv, 16);
+    FHB_ALLOC(pi, 16);
+    FHB_ALLOC(tk, 1);
+    cudaStream_t s;
+    FHB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    std::unique_ptr<CUstream_st, decltype(&cudaStreamDestroy)> guard(s, &cudaStreamDestroy);
+    FHB_CUDA(cudaMemcpyAsync(d_a.p, a, 16 * n * n, cudaMemcpyHostToDevice, s));
+    FHB_CUDA(cudaMemcpyAsync(d_x.p, b, 16 * n * nrhs, cudaMemcpyHostToDevice, s));
+    FHB_CUDA(cudaMemsetAsync(sing.p, 0, sizeof(int), s));
+    FHB_CUDA(cudaMemsetAsync(tk.p, 0, sizeof(unsigned), s));
+    LuWork w;
+    w.partial_val = pv.p;
+    w.partial_idx = pi.p;
+    w.tickets = tk.p;
+    w.max_chunks = 16;
+    LuBatch<double> lb;
+    lb.a = d_a.p;
+    lb.pivots = piv.p;
+    lb.singular = sing.p;
+    lb.m = (int64_t)n;
+    lb.count = 1;
+    st = lu_factor<double>(lb, w, 64, TrailingUpdate::Simt, s, err);
+    if (!st) st = lu_solve<double>(lb, d_x.p, (int)nrhs, 64, s, err);
+    if (st) return st;
+    int singular = 0;
+    FHB_CUDA(cudaMemcpyAsync(&singular, sing.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FHB_CUDA(cudaMemcpyAsync(x, d_x.p, 16 * n * nrhs, cudaMemcpyDeviceToHost, s));
+    FHB_CUDA(cudaStreamSynchronize(s));
+    if (singular) return fail(err, FH_ERR_SINGULAR, "the matrix is singular (zero pivot)");
+    return FH_OK;
+}
+
+fh_status fh_system_create(const fh_node *nodes, size_t n_nodes, const fh_segment_def *segments, size_t n_segments,
+                           const fh_port *ports, size_t n_ports, const fh_discretization *disc,
+                           fh_solver_choice choice, fh_system **out, fh_error_info *err) {
+    clear_error(err);
+    if (!out) return fail(err, FH_ERR_INVALID_ARGUMENT, "null output handle");
+    *out = nullptr;
+    const double t0 = wall();
+    std::unique_ptr<fh_system> s(new fh_system);
+    s->nodes.assign(nodes, nodes + n_nodes);
+    s->segments.assign(segments, segments + n_segments);
+    if (n_ports && !ports) return fail(err, FH_ERR_INVALID_ARGUMENT, "null ports");
+    s->ports.assign(ports, ports + n_ports);
+    fh_status st = discretize_geometry(nodes, n_nodes, segments, n_segments, disc, s->disc, err);
+    if (st) return st;
+    st = build_loops(segments, n_segments, n_nodes, s->disc.per_segment.data(), ports, n_ports, s->loops, err);
+    if (st) return st;
+    s->n = (int64_t)s->disc.filaments.size();
+    if (fh_solver_resolve(choice, (size_t)s->n) != 0)
+        return fail(err, FH_ERR_UNSUPPORTED,
+                    "the matrix-free (pFFT + GMRES) path is not provided by this build; choose FH_SOLVER_DENSE");
+    st = ensure_device(err);
+    if (st) return st;
+    FHB_CUDA(cudaGetDevice(&s->device));
+    FHB_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    cudaStream_t cs = s->stream;
+    s->nloops = s->loops.rows();
+    s->m = s->loops.internal;
+    s->p = s->nloops - s->m;
+    for (const fh_filament &f : s->disc.filaments)
+        s->resistances.push_back(f.length / (f.sigma * (f.width * f.height)));  // solve.rs:941-943
+    const int64_t n = s->n, loops = s->nloops;
+    std::vector<DevFil> h(n);
+    for (int64_t i = 0; i < n; ++i) h[i] = make_devfil(s->disc.filaments[i]);
+    DBuf<DevFil> d_fil;
+    DBuf<double> d_L, d_R, d_sign;
+    DBuf<int64_t> d_rp;
+    DBuf<int32_t> d_br;
+    FHB_ALLOC(d_fil, (size_t)n);
+    FHB_ALLOC(d_L, (size_t)n * n);
+    FHB_ALLOC(d_R, (size_t)n);
+    FHB_ALLOC(d_rp, s->loops.row_ptr.size());
+    FHB_ALLOC(d_br, s->loops.branch.size());
+    FHB_ALLOC(d_sign, s->loops.sign.size());
+    if (cudaMalloc(&s->d_Lm, std::max<size_t>(1, (size_t)loops * loops) * 8) != cudaSuccess ||
+        cudaMalloc(&s->d_Rm, std::max<size_t>(1, (size_t)loops * loops) * 8) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(err, FH_ERR_OUT_OF_MEMORY, "device allocation of the mesh matrices failed");
+    }
+    FHB_CUDA(cudaMemcpyAsync(d_fil.p, h.data(), n * sizeof(DevFil), cudaMemcpyHostToDevice, cs));
+    FHB_CUDA(cudaMemcpyAsync(d_R.p, s->resistances.data(), n * 8, cudaMemcpyHostToDevice, cs));
+    FHB_CUDA(cudaMemcpyAsync(d_rp.p, s->loops.row_ptr.data(), s->loops.row_ptr.size() * 8, cudaMemcpyHostToDevice, cs));
+    FHB_CUDA(cudaMemcpyAsync(d_br.p, s->loops.branch.data(), s->loops.branch.size() * 4, cudaMemcpyHostToDevice, cs));
+    FHB_CUDA(cudaMemcpyAsync(d_sign.p, s->loops.sign.data(), s->loops.sign.size() * 8, cudaMemcpyHostToDevice, cs));
+    FHB_CUDA(cudaMemsetAsync(d_L.p, 0, (size_t)n * n * 8, cs));
+    const double t1 = wall();
+    st = device_fill(d_fil.p, n, d_L.p, nullptr, cs, &s->fill, err);
+    if (st) return st;
+    FHB_CUDA(cudaStreamSynchronize(cs));
+    const double t2 = wall();
+    cudaEvent_t c0, c1;
+    cudaEventCreate(&c0);
+    cudaEventCreate(&c1);
+    cudaEventRecord(c0, cs);
+    st = device_congruence(d_L.p, d_R.p, n, d_rp.p, d_br.p, d_sign.p, loops, s->d_Lm, s->d_Rm, cs, err);
+    cudaEventRecord(c1, cs);
+    if (st) return st;
+    FHB_CUDA(cudaStreamSynchronize(cs));
+    cudaEventElapsedTime(&s->ms_congruence, c0, c1);
+    cudaEventDestroy(c0);
+    cudaEventDestroy(c1);
+    const double t3 = wall();
+    s->counts = fh_counts{(int64_t)n_nodes, (int64_t)n_segments, n, loops, s->m, s->p};
+    s->timing.inductance_s = t2 - t1;
+    s->timing.assembly_s = t3 - t0;
+    s->timing.solve_s = 0.0;
+    s->timing.total_s = s->timing.assembly_s;
+    *out = s.release();
+    return FH_OK;
+}
+
+void fh_system_destroy(fh_system *sys) { delete sys; }
+
+fh_status fh_system_counts(const fh_system *sys, fh_counts *counts) {
+    if (!sys || !counts) return fail(nullptr, FH_ERR_INVALID_ARGUMENT, "null argument");
+    *counts = sys->counts;
+    return FH_OK;
+}
+
+fh_status fh_system_timing(const fh_system *sys, fh_timing *timing) {
+    if (!sys || !timing) return fail(nullptr, FH_ERR_INVALID_ARGUMENT, "null argument");
+    *timing = sys->timing;
+    return FH_OK;
+}
+
+fh_status fh_system_filaments(const fh_system *sys, fh_filament *out, size_t capacity) {
+    if (!sys || !out) return fail(nullptr, FH_ERR_INVALID_ARGUMENT, "null argument");
+    if (capacity < sys->disc.filaments.size()) return fail(nullptr, FH_ERR_INVALID_ARGUMENT, "buffer too small");
+    std::copy(sys->disc.filaments.begin(), sys->disc.filaments.end(), out);
+    return FH_OK;
+}
+
+fh_status fh_system_resistances(const fh_system *sys, double *out, size_t capacity) {
+    if (!sys || !out) return fail(nullptr, FH_ERR_INVALID_ARGUMENT, "null argument");
+    if (capacity < sys->resistances.size()) return fail(nullptr, FH_ERR_INVALID_ARGUMENT, "buffer too small");
+    std::copy(sys->resistances.begin(), sys->resistances.end(), out);
+    return FH_OK;
+}
+
+fh_status fh_system_mesh_matrices(const fh_system *sys, double *r_mesh, double *l_mesh) {
+    if (!sys) return fail(nullptr, FH_ERR_INVALID_ARGUMENT, "null argument");
+    fh_error_info *err = nullptr;
+    size_t bytes = (size_t)sys->nloops * sys->nloops * 8;
+    if (r_mesh) FHB_CUDA(cudaMemcpy(r_mesh, sys->d_Rm, bytes, cudaMemcpyDeviceToHost));
+    if (l_mesh) FHB_CUDA(cudaMemcpy(l_mesh, sys->d_Lm, bytes, cudaMemcpyDeviceToHost));
+    return FH_OK;
+}
+
+fh_status fh_system_device_l_mesh(const fh_system *sys, const double **l_mesh, const double **r_mesh) {
+    if (!sys) return fail(nullptr, FH_ERR_INVALID_ARGUMENT, "null argument");
+    if (l_mesh) *l_mesh = sys->d_Lm;
+    if (r_mesh) *r_mesh = sys->d_Rm;
+    return FH_OK;
+}
+
+fh_status fh_sweep(fh_system *sys, const double *freqs, size_t nf, fh_precision precision, double *z_out,
+                   fh_sweep_report *report, fh_error_info *err) {
+    clear_error(err);
+    if (!sys || (nf && (!freqs || !z_out))) return fail(err, FH_ERR_INVALID_ARGUMENT, "null argument");
+    for (size_t k = 0; k < nf; ++k)
+        if (!(std::isfinite(freqs[k]) && freqs[k] >= 0.0))
+            return fail(err, FH_ERR_INVALID_FREQUENCY,
+                        "frequency " + std::to_string(k) + " is " + fstr(freqs[k]) +
+                            " Hz; frequencies must be finite and non-negative",
+                        (int64_t)k, -1, freqs[k]);
+    if (nf == 0) return FH_OK;
+    FHB_CUDA(cudaSetDevice(sys->device));
+    const double t0 = wall();
+    const int64_t m = sys->m, p = sys->p;
+    cudaStream_t st = sys->stream;
+    // Frequencies per batch from free device memory (the analogue of the
+    // reference's 2 GiB sweep budget, solve.rs:91 and 884).
+    size_t free_b = 0, total_b = 0;
+    FHB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const bool mixed = precision == FH_PRECISION_MIXED_BF16X3;
+    const double per = (mixed ? 8.0 : 16.0) * (double)m * (double)m + 64.0 * (double)(m * p + 64);
+    int chunk = (int)std::max(1.0, std::min<double>((double)nf, 0.8 * (double)free_b / std::max(per, 1.0)));
+    DBuf<double> d_omega, d_x, d_z;
+    FHB_ALLOC(d_omega, (size_t)chunk);
+    FHB_ALLOC(d_x, (size_t)chunk * m * p * 2);
+    FHB_ALLOC(d_z, (size_t)chunk * p * p * 2);
+    float ms_factor = 0, ms_refine = 0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    std::vector<int> singular((size_t)nf, 0), failed((size_t)nf, 0);
+    for (size_t c0 = 0; c0 < nf; c0 += (size_t)chunk) {
+        const int count = (int)std::min<size_t>((size_t)chunk, nf - c0);
+        std::vector<double> omega(count);
+        for (int f = 0; f < count; ++f) omega[f] = kTau * freqs[c0 + f];
+        FHB_CUDA(cudaMemcpyAsync(d_omega.p, omega.data(), 8 * count, cudaMemcpyHostToDevice, st));
+        fh_status e;
+        if (mixed) {
+            e = sweep_chunk_mixed(sys, d_omega.p, count, d_x.p, d_z.p, singular.data() + c0, failed.data() + c0,
+                                  report && report->refinement_iterations ? report->refinement_iterations + c0 : nullptr,
+                                  report && report->residual ? report->residual + c0 : nullptr, &ms_factor, &ms_refine,
+                                  TrailingUpdate::Simt, err);
+        } else {
+            e = sweep_chunk_fp64(sys, d_omega.p, count, d_x.p, d_z.p, singular.data() + c0, &ms_factor, err);
+        }
+        if (e) return e;
+        FHB_CUDA(cudaMemcpyAsync(z_out + 2 * c0 * p * p, d_z.p, 16 * (size_t)count * p * p, cudaMemcpyDeviceToHost, st));
+        FHB_CUDA(cudaStreamSynchronize(st));
+        // Refinement that did not converge: redo those frequencies in FP64.
+        std::vector<int> redo;
+        for (int f = 0; f < count; ++f)
+            if (failed[c0 + f]) redo.push_back(f);
+        if (!redo.empty()) {
+            std::vector<double> om2;
+            for (int f : redo) om2.push_back(omega[f]);
+            DBuf<double> d_om2, d_x2, d_z2;
+            FHB_ALLOC(d_om2, om2.size());
+            FHB_ALLOC(d_x2, om2.size() * m * p * 2);
+            FHB_ALLOC(d_z2, om2.size() * p * p * 2);
+            FHB_CUDA(cudaMemcpyAsync(d_om2.p, om2.data(), 8 * om2.size(), cudaMemcpyHostToDevice, st));
+            std::vector<int> sing2(om2.size(), 0);
+            e = sweep_chunk_fp64(sys, d_om2.p, (int)om2.size(), d_x2.p, d_z2.p, sing2.data(), &ms_factor, err);
+            if (e) return e;
+            std::vector<double> z2(om2.size() * p * p * 2);
+            FHB_CUDA(cudaMemcpyAsync(z2.data(), d_z2.p, 8 * z2.size(), cudaMemcpyDeviceToHost, st));
+            FHB_CUDA(cudaStreamSynchronize(st));
+            for (size_t k = 0; k < redo.size(); ++k) {
+                int f = redo[k];
+                singular[c0 + f] = sing2[k];
+                std::memcpy(z_out + 2 * (c0 + f) * p * p, z2.data() + 2 * k * p * p, 16 * (size_t)p * p);
+                if (report && report->refinement_iterations) report->refinement_iterations[c0 + f] = -1;
+            }
+        }
+    }
+    cudaEventRecord(e1, st);
+    FHB_CUDA(cudaStreamSynchronize(st));
+    float ms_total = 0;
+    cudaEventElapsedTime(&ms_total, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // First failing frequency in list order (solve.rs:877-879).
+    for (size_t k = 0; k < nf; ++k) {
+        bool bad = singular[k] != 0;
+        for (int64_t q = 0; q < p * p && !bad; ++q)
+            bad = !(std::isfinite(z_out[2 * (k * p * p + q)]) && std::isfinite(z_out[2 * (k * p * p + q) + 1]));
+        if (bad)
+            return fail(err, FH_ERR_SINGULAR,
+                        "the mesh system is singular or ill-conditioned at " + fstr(freqs[k]) + " Hz", (int64_t)k, -1,
+                        freqs[k]);
+    }
+    const double t1 = wall();
+    sys->timing.solve_s = t1 - t0;
+    sys->timing.total_s = sys->timing.assembly_s + sys->timing.solve_s;
+    if (report) {
+        report->solve_s = ms_total * 1e-3;
+        report->factor_s = ms_factor * 1e-3;
+        report->refine_s = ms_refine * 1e-3;
+    }
+    return FH_OK;
+}
+
+fh_status fh_impedance(fh_system *sys, double frequency_hz, fh_precision precision, double *z_out,
+                       fh_error_info *err) {
+    return fh_sweep(sys, &frequency_hz, 1, precision, z_out, nullptr, err);
+}
+
+}  // extern "C"

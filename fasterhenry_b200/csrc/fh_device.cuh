@@ -1,0 +1,68 @@
+// Device-side shared definitions: filament records in HBM, CUDA error
+// plumbing, non-contracted FP64 helpers for dispatch-critical arithmetic.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "fh_internal.h"
+
+namespace fhb {
+
+// A filament as the fill kernels read it: 32 doubles (256 B), all derived
+// quantities computed once on the host in the reference's operation order.
+struct __align__(16) DevFil {
+    double centre[3];   // (start + end) * 0.5
+    double axes[9];     // length, width, height unit vectors
+    double half[3];     // 0.5 * length, 0.5 * width, 0.5 * height
+    double area;        // width * height
+    double start[3];
+    double end[3];
+    double width, height;
+    double length;
+    double pad[7];
+};
+static_assert(sizeof(DevFil) == 256, "DevFil is 256 bytes");
+
+DevFil make_devfil(const fh_filament &f);
+
+// Gauss-Legendre rules 1..kMaxRule and the order thresholds, uploaded once.
+constexpr int kMaxRule = 17;
+struct QuadTables {
+    double nodes[kMaxRule + 1][kMaxRule];
+    double weights[kMaxRule + 1][kMaxRule];
+    double point_thresholds[16];   // tolerance 1e-8, orders 1..16
+    double sample_thresholds[8];   // tolerance 1e-6, orders 1..8
+};
+void host_quad_tables(QuadTables &t);
+
+#define FHB_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return ::fhb::fail(err, FH_ERR_CUDA,                                         \
+                               std::string(#call " failed: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+fh_status ensure_device(fh_error_info *err);
+
+// Fill the n x n column-major L on the device (d_L must be zero-filled by the
+// caller).  `d_methods` optional (n*n int8).  `stream` orders the work.
+struct FillStats {
+    int64_t pairs = 0, orthogonal = 0, point = 0, closed_form = 0, aligned_quadrature = 0, sampled = 0;
+    int64_t unique_aligned = 0;
+    double point_evaluations = 0.0;
+    float ms_classify = 0, ms_point = 0, ms_aligned = 0, ms_quadrature = 0, ms_sampled = 0;
+};
+fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_methods, cudaStream_t stream,
+                      FillStats *stats, fh_error_info *err);
+
+// R_m = M diag(R) M^T and L_m = M L M^T (loops x loops, column-major), upper
+// triangle evaluated in the reference's order and mirrored.
+fh_status device_congruence(const double *d_L, const double *d_R, int64_t n, const int64_t *d_row_ptr,
+                            const int32_t *d_branch, const double *d_sign, int64_t loops, double *d_Lm,
+                            double *d_Rm, cudaStream_t stream, fh_error_info *err);
+
+}  // namespace fhb

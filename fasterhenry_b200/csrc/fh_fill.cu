@@ -1,0 +1,1119 @@
+// Partial-inductance fill on the device (FP64 throughout).
+//
+// Replaces the reference's rayon row loop over `evaluate`
+// (fasterhenry/src/inductance/batch.rs:355-372, inductance/mod.rs:303-369).
+// The upper triangle is classified first — orthogonal pairs stay zero, every
+// other pair is appended to a work list for its method — and each method
+// then runs as its own kernel so that warps never diverge across methods:
+//
+//   point quadrature   thread per pair, lists bucketed by log2(#point pairs)
+//   bar closed form    thread per pair, 64 Hoer-Love terms summed in order
+//   aligned quadrature one CTA per distinct aligned-bar key: the panel tree
+//                      is walked by one thread, its Gauss points evaluated
+//                      by the whole CTA (the GPU analogue of memo.rs: equal
+//                      keys give bit-equal values, so one evaluation serves
+//                      every pair that shares the key)
+//   sampled filaments  warp per pair, lanes over cross-section samples
+//
+// Dispatch-critical arithmetic (direction cosines, alignment, the separating-
+// axis gap, Gauss orders) uses non-contracted __d*_rn operations in the
+// reference's order, so method choices match the reference's bit for bit on
+// identical inputs.  The value arithmetic is free to use FMA.
+#include <cub/cub.cuh>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "fh_device.cuh"
+
+namespace fhb {
+
+__constant__ QuadTables c_quad;
+
+namespace {
+
+// Method ids (inductance/mod.rs:130-152).
+enum : int8_t { kOrthogonal = 0, kClosedForm = 1, kAlignedQuadrature = 2, kPoint = 3, kSampled = 4 };
+
+constexpr int kPointBuckets = 17;                     // log2(cost) in 0..16
+constexpr int kCatAligned = kPointBuckets;            // aligned-bar pairs
+constexpr int kCatSampled = kPointBuckets + 1;        // sampled filaments
+constexpr int kCats = kPointBuckets + 2;
+constexpr double kMu0Over4Pi = 1.0e-7;
+constexpr double kClosedFormMaxError = 1e-10;
+constexpr double kEps = 2.220446049250313e-16;
+
+// ---- non-contracted helpers (reference evaluation order) ----
+__device__ __forceinline__ double ndot(const double *a, const double *b) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(a[0], b[0]), __dmul_rn(a[1], b[1])), __dmul_rn(a[2], b[2]));
+}
+__device__ __forceinline__ void ncross(const double *a, const double *b, double *o) {
+    o[0] = __dsub_rn(__dmul_rn(a[1], b[2]), __dmul_rn(a[2], b[1]));
+    o[1] = __dsub_rn(__dmul_rn(a[2], b[0]), __dmul_rn(a[0], b[2]));
+    o[2] = __dsub_rn(__dmul_rn(a[0], b[1]), __dmul_rn(a[1], b[0]));
+}
+__device__ __forceinline__ double nnorm(const double *a) { return __dsqrt_rn(ndot(a, a)); }
+__device__ __forceinline__ double rmax(double a, double b) {
+    return isnan(a) ? b : (isnan(b) ? a : (a > b ? a : b));
+}
+__device__ __forceinline__ double rmin(double a, double b) {
+    return isnan(a) ? b : (isnan(b) ? a : (a < b ? a : b));
+}
+__device__ __forceinline__ double signum(double x) { return isnan(x) ? x : (signbit(x) ? -1.0 : 1.0); }
+
+__device__ __forceinline__ int total_cmp(double x, double y) {
+    long long a = __double_as_longlong(x), b = __double_as_longlong(y);
+    a ^= (long long)(((unsigned long long)(a >> 63)) >> 1);
+    b ^= (long long)(((unsigned long long)(b >> 63)) >> 1);
+    return a < b ? -1 : (a > b ? 1 : 0);
+}
+
+// canonical, inductance/mod.rs:231-254.
+__device__ bool canonical_greater(const DevFil &a, const DevFil &b) {
+    const double ka[11] = {a.start[0], a.start[1], a.start[2], a.end[0], a.end[1], a.end[2],
+                           a.width,    a.height,   a.axes[3],  a.axes[4], a.axes[5]};
+    const double kb[11] = {b.start[0], b.start[1], b.start[2], b.end[0], b.end[1], b.end[2],
+                           b.width,    b.height,   b.axes[3],  b.axes[4], b.axes[5]};
+    for (int i = 0; i < 11; ++i) {
+        int c = total_cmp(ka[i], kb[i]);
+        if (c) return c > 0;
+    }
+    return false;
+}
+
+__device__ __forceinline__ double circumradius(const DevFil &f) {
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(f.half[0], f.half[0]), __dmul_rn(f.half[1], f.half[1])),
+                                __dmul_rn(f.half[2], f.half[2])));
+}
+__device__ __forceinline__ double projected_half_extent(const DevFil &f, const double *n) {
+    double s = 0.0;
+    for (int k = 0; k < 3; ++k) s = __dadd_rn(s, __dmul_rn(f.half[k], fabs(ndot(n, f.axes + 3 * k))));
+    return s;
+}
+
+// neumann::separation, neumann.rs:97-122.
+__device__ double separation(const DevFil &a, const DevFil &b) {
+    double delta[3] = {__dsub_rn(b.centre[0], a.centre[0]), __dsub_rn(b.centre[1], a.centre[1]),
+                       __dsub_rn(b.centre[2], a.centre[2])};
+    double distance = nnorm(delta);
+    double reach = __dadd_rn(circumradius(a), circumradius(b));
+    if (distance > __dmul_rn(8.0, reach)) return __dsub_rn(distance, reach);
+    double best = -INFINITY;
+    auto consider = [&](const double *n) {
+        double gap = __dsub_rn(__dsub_rn(fabs(ndot(n, delta)), projected_half_extent(a, n)),
+                               projected_half_extent(b, n));
+        best = rmax(best, gap);
+    };
+    for (int k = 0; k < 3; ++k) {
+        consider(a.axes + 3 * k);
+        consider(b.axes + 3 * k);
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double c[3];
+            ncross(a.axes + 3 * i, b.axes + 3 * j, c);
+            double nn = nnorm(c);
+            if (nn > 1e-9) {
+                double u[3] = {__ddiv_rn(c[0], nn), __ddiv_rn(c[1], nn), __ddiv_rn(c[2], nn)};
+                consider(u);
+            }
+        }
+    return best;
+}
+
+// OrderTable::order_for, gauss.rs:123-136; 0 = None.
+__device__ __forceinline__ int order_for(const double *thresholds, int count, double half, double distance) {
+    if (half <= 0.0) return 1;
+    if (isnan(distance) || distance <= 0.0) return 0;
+    double delta = __ddiv_rn(distance, half);
+    for (int i = 0; i < count; ++i)
+        if (delta >= thresholds[i]) return i + 1;
+    return 0;
+}
+
+__device__ __forceinline__ bool point_orders(const DevFil &f, double gap, int o[3]) {
+    for (int k = 0; k < 3; ++k) {
+        o[k] = order_for(c_quad.point_thresholds, 16, f.half[k], gap);
+        if (!o[k]) return false;
+    }
+    return o[0] * o[1] * o[2] <= 256;
+}
+
+// aligned_bars, inductance/mod.rs:280-300.  Returns false when not aligned.
+struct Aligned {
+    double length[2], width[2], height[2], offset[3];
+};
+__device__ bool aligned_bars(const DevFil &a, const DevFil &b, Aligned *o) {
+    const double kAligned = 1.0 - 1e-12;
+    double wb, hb;
+    if (fabs(ndot(a.axes + 3, b.axes + 3)) > kAligned) {
+        wb = b.half[1];
+        hb = b.half[2];
+    } else if (fabs(ndot(a.axes + 3, b.axes + 6)) > kAligned) {
+        wb = b.half[2];
+        hb = b.half[1];
+    } else {
+        return false;
+    }
+    if (o) {
+        double delta[3] = {__dsub_rn(b.centre[0], a.centre[0]), __dsub_rn(b.centre[1], a.centre[1]),
+                           __dsub_rn(b.centre[2], a.centre[2])};
+        o->length[0] = 2.0 * a.half[0];
+        o->length[1] = 2.0 * b.half[0];
+        o->width[0] = 2.0 * a.half[1];
+        o->width[1] = 2.0 * wb;
+        o->height[0] = 2.0 * a.half[2];
+        o->height[1] = 2.0 * hb;
+        o->offset[0] = ndot(delta, a.axes);
+        o->offset[1] = ndot(delta, a.axes + 3);
+        o->offset[2] = ndot(delta, a.axes + 6);
+    }
+    return true;
+}
+
+struct Classified {
+    int cat;          // -1 orthogonal
+    int orders;       // packed 5-bit orders (point), 6 fields
+    int cost;
+    bool swap;        // canonical order is (j, i)
+};
+
+// The dispatch of inductance/mod.rs:303-356 up to (not including) the
+// evaluation itself.
+__device__ Classified classify(const DevFil &fi, const DevFil &fj) {
+    Classified c{-1, 0, 0, false};
+    c.swap = canonical_greater(fi, fj);
+    const DevFil &a = c.swap ? fj : fi;
+    const DevFil &b = c.swap ? fi : fj;
+    double cosv = ndot(a.axes, b.axes);
+    if (fabs(cosv) < 1e-14) return c;
+    double cr[3];
+    ncross(a.axes, b.axes, cr);
+    bool parallel = nnorm(cr) < 1e-6;
+    bool aligned = parallel && aligned_bars(a, b, nullptr);
+    double gap = separation(a, b);
+    int oa[3], ob[3];
+    bool point = point_orders(a, gap, oa) && point_orders(b, gap, ob);
+    int cost = 0;
+    if (point) {
+        cost = oa[0] * oa[1] * oa[2] * ob[0] * ob[1] * ob[2];
+        if (aligned && cost > 4096) point = false;
+    }
+    if (point) {
+        int bucket = 31 - __clz(cost);
+        c.cat = bucket;
+        c.cost = cost;
+        c.orders = oa[0] | (oa[1] << 5) | (oa[2] << 10) | (ob[0] << 15) | (ob[1] << 20) | (ob[2] << 25);
+    } else if (aligned) {
+        c.cat = kCatAligned;
+    } else {
+        c.cat = kCatSampled;
+    }
+    return c;
+}
+
+// Error record: smallest (row, column) of the upper triangle that failed.
+struct DevError {
+    unsigned long long key;  // (row << 32) | col, ~0 when none
+    int code;                // FH_ERR_KERNEL_*
+};
+
+__device__ void record_error(DevError *e, int i, int j, int code) {
+    int lo = min(i, j), hi = max(i, j);
+    unsigned long long key = ((unsigned long long)lo << 32) | (unsigned)hi;
+    unsigned long long old = atomicMin(&e->key, key);
+    if (key < old) atomicExch(&e->code, code);
+}
+
+// Writes L[i][j] = L[j][i] and the method, or records a non-finite value.
+__device__ __forceinline__ void store_pair(double *L, int8_t *methods, int64_t n, int i, int j, double v, int8_t m,
+                                           DevError *e) {
+    if (!isfinite(v)) {
+        record_error(e, i, j, FH_ERR_KERNEL_NOT_FINITE);
+        return;
+    }
+    L[(int64_t)i + (int64_t)j * n] = v;
+    L[(int64_t)j + (int64_t)i * n] = v;
+    if (methods) {
+        methods[(int64_t)i + (int64_t)j * n] = m;
+        methods[(int64_t)j + (int64_t)i * n] = m;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Classification: pass 0 counts per category, pass 1 writes the work lists.
+// Block (32, 8) covers a 32 x 32 tile of the upper triangle.
+// ---------------------------------------------------------------------------
+template <bool kWrite>
+__global__ void __launch_bounds__(256) classify_kernel(const DevFil *__restrict__ fil, int n,
+                                                       unsigned long long *__restrict__ counts,
+                                                       unsigned long long *__restrict__ cursor,
+                                                       int4 *__restrict__ items) {
+    const int ti = blockIdx.y, tj = blockIdx.x;
+    if (ti > tj) return;
+    __shared__ DevFil s_i[32], s_j[32];
+    __shared__ unsigned s_count[kCats];
+    __shared__ unsigned long long s_base[kCats];
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    {
+        const double *gi = reinterpret_cast<const double *>(fil + (int64_t)ti * 32);
+        const double *gj = reinterpret_cast<const double *>(fil + (int64_t)tj * 32);
+        double *si = reinterpret_cast<double *>(s_i), *sj = reinterpret_cast<double *>(s_j);
+        int rows_i = min(32, n - ti * 32), rows_j = min(32, n - tj * 32);
+        for (int k = tid; k < 32 * 32; k += 256) {
+            if (k < rows_i * 32) si[k] = gi[k];
+            if (k < rows_j * 32) sj[k] = gj[k];
+        }
+    }
+    if (tid < kCats) s_count[tid] = 0;
+    __syncthreads();
+    const int j = tj * 32 + threadIdx.x;
+    Classified cls[4];
+    unsigned slot[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int i = ti * 32 + threadIdx.y + 8 * r;
+        cls[r].cat = -1;
+        if (i < n && j < n && i <= j) {
+            cls[r] = classify(s_i[threadIdx.y + 8 * r], s_j[threadIdx.x]);
+            if (cls[r].cat >= 0) slot[r] = atomicAdd(&s_count[cls[r].cat], 1u);
+        }
+    }
+    __syncthreads();
+    if (!kWrite) {
+        if (tid < kCats && s_count[tid]) atomicAdd(&counts[tid], (unsigned long long)s_count[tid]);
+        return;
+    }
+    if (tid < kCats) s_base[tid] = s_count[tid] ? atomicAdd(&cursor[tid], (unsigned long long)s_count[tid]) : 0ull;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        if (cls[r].cat < 0) continue;
+        const int i = ti * 32 + threadIdx.y + 8 * r;
+        int a = cls[r].swap ? j : i, b = cls[r].swap ? i : j;
+        items[s_base[cls[r].cat] + slot[r]] = make_int4(a, b, cls[r].orders, cls[r].cost);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Point quadrature (neumann.rs:196-266), thread per pair.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) point_kernel(const DevFil *__restrict__ fil, const int4 *__restrict__ items,
+                                                    int64_t count, double *__restrict__ L, int8_t *methods,
+                                                    int64_t n, DevError *err) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int4 it = items[t];
+        const DevFil &A = fil[it.x];
+        const DevFil &B = fil[it.y];
+        const int oa0 = it.z & 31, oa1 = (it.z >> 5) & 31, oa2 = (it.z >> 10) & 31;
+        const int ob0 = (it.z >> 15) & 31, ob1 = (it.z >> 20) & 31, ob2 = (it.z >> 25) & 31;
+        double ac[3] = {A.centre[0], A.centre[1], A.centre[2]};
+        double bc[3] = {B.centre[0], B.centre[1], B.centre[2]};
+        double aa[9], ba[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            aa[k] = A.axes[k];
+            ba[k] = B.axes[k];
+        }
+        const double ah0 = A.half[0], ah1 = 2.0 * A.half[1], ah2 = 2.0 * A.half[2];
+        const double bh0 = B.half[0], bh1 = 2.0 * B.half[1], bh2 = 2.0 * B.half[2];
+        double total = 0.0;
+        for (int la = 0; la < oa0; ++la) {
+            const double xl = ah0 * c_quad.nodes[oa0][la], wl = ah0 * c_quad.weights[oa0][la];
+            for (int wa = 0; wa < oa1; ++wa) {
+                const double xw = ah1 * (0.5 * c_quad.nodes[oa1][wa]), ww = 0.5 * c_quad.weights[oa1][wa];
+                for (int ha = 0; ha < oa2; ++ha) {
+                    const double xh = ah2 * (0.5 * c_quad.nodes[oa2][ha]), wh = 0.5 * c_quad.weights[oa2][ha];
+                    double p[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) p[d] = ac[d] + aa[d] * xl + aa[3 + d] * xw + aa[6 + d] * xh;
+                    const double wpa = wl * ww * wh;
+                    double inner = 0.0;
+                    for (int lb = 0; lb < ob0; ++lb) {
+                        const double yl = bh0 * c_quad.nodes[ob0][lb], vl = bh0 * c_quad.weights[ob0][lb];
+                        for (int wb = 0; wb < ob1; ++wb) {
+                            const double yw = bh1 * (0.5 * c_quad.nodes[ob1][wb]);
+                            const double vlw = vl * (0.5 * c_quad.weights[ob1][wb]);
+                            double q[3];
+#pragma unroll
+                            for (int d = 0; d < 3; ++d) q[d] = p[d] - (bc[d] + ba[d] * yl + ba[3 + d] * yw);
+                            for (int hb = 0; hb < ob2; ++hb) {
+                                const double yh = bh2 * (0.5 * c_quad.nodes[ob2][hb]);
+                                const double vh = 0.5 * c_quad.weights[ob2][hb];
+                                const double dx = q[0] - ba[6] * yh, dy = q[1] - ba[7] * yh, dz = q[2] - ba[8] * yh;
+                                inner += (vlw * vh) * rsqrt(dx * dx + dy * dy + dz * dz);
+                            }
+                        }
+                    }
+                    total += wpa * inner;
+                }
+            }
+        }
+        const double cosv = ndot(A.axes, B.axes);
+        store_pair(L, methods, n, it.x, it.y, kMu0Over4Pi * (total * cosv), kPoint, err);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Hoer-Love closed form (bar.rs:30-106), thread per pair, terms in order.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double log_term(double coefficient, double x, double r, double rest_sq) {
+    if (coefficient == 0.0 || x == 0.0) return 0.0;
+    double argument = x >= 0.0 ? x + r : rest_sq / (r - x);
+    return coefficient * x * log(argument);
+}
+__device__ __forceinline__ double atan_term(double x, double y, double z, double r) {
+    double product = x * y * z;
+    if (product == 0.0) return 0.0;
+    return -(product * z * z / 6.0) * atan(x * y / (z * r));
+}
+__device__ double primitive(double x, double y, double z) {
+    const double x2 = x * x, y2 = y * y, z2 = z * z;
+    const double x4 = x2 * x2, y4 = y2 * y2, z4 = z2 * z2;
+    const double r = sqrt(x2 + y2 + z2);
+    double s = log_term(y2 * z2 / 4.0 - y4 / 24.0 - z4 / 24.0, x, r, y2 + z2);
+    s += log_term(x2 * z2 / 4.0 - x4 / 24.0 - z4 / 24.0, y, r, x2 + z2);
+    s += log_term(x2 * y2 / 4.0 - x4 / 24.0 - y4 / 24.0, z, r, x2 + y2);
+    s += (x4 + y4 + z4 - 3.0 * (x2 * y2 + y2 * z2 + z2 * x2)) * r / 60.0;
+    s += atan_term(x, y, z, r);
+    s += atan_term(x, z, y, r);
+    s += atan_term(y, z, x, r);
+    return s;
+}
+__device__ __forceinline__ void corner_differences(double e1, double e2, double offset, double q[4]) {
+    double sum = 0.5 * (e1 + e2), diff = 0.5 * (e1 - e2);
+    q[0] = offset + sum;
+    q[1] = offset + diff;
+    q[2] = offset - diff;
+    q[3] = offset - sum;
+}
+__device__ void bar_integral(const Aligned &b, double *value, double *rel) {
+    double qx[4], qy[4], qz[4];
+    corner_differences(b.length[0], b.length[1], b.offset[0], qx);
+    corner_differences(b.width[0], b.width[1], b.offset[1], qy);
+    corner_differences(b.height[0], b.height[1], b.offset[2], qz);
+    const double signs[4] = {1.0, -1.0, -1.0, 1.0};
+    double v = 0.0, mag = 0.0;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
+            for (int k = 0; k < 4; ++k) {
+                double term = signs[i] * signs[j] * signs[k] * primitive(qx[i], qy[j], qz[k]);
+                v += term;
+                mag += fabs(term);
+            }
+    *value = v;
+    *rel = v > 0.0 ? 8.0 * kEps * mag / v : INFINITY;
+}
+
+// Aligned pairs: closed form when its error estimate allows, else queue the
+// pair for the quadrature kernel.
+__global__ void __launch_bounds__(128) closed_form_kernel(const DevFil *__restrict__ fil,
+                                                          const int4 *__restrict__ items, int64_t count,
+                                                          double *__restrict__ L, int8_t *methods, int64_t n,
+                                                          int4 *__restrict__ quad_items,
+                                                          unsigned long long *__restrict__ quad_count,
+                                                          DevError *err) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int4 it = items[t];
+        const DevFil &A = fil[it.x];
+        const DevFil &B = fil[it.y];
+        Aligned ab;
+        aligned_bars(A, B, &ab);
+        double v, rel;
+        bar_integral(ab, &v, &rel);
+        if (rel <= kClosedFormMaxError) {
+            const double cosv = ndot(A.axes, B.axes);
+            const double scale = signum(cosv) / (A.area * B.area);
+            store_pair(L, methods, n, it.x, it.y, kMu0Over4Pi * (v * scale), kClosedForm, err);
+        } else {
+            unsigned long long k = atomicAdd(quad_count, 1ull);
+            quad_items[k] = it;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Aligned quadrature (aligned.rs:206-402): CTA per distinct key.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double overlap_weight(double e1, double e2, double offset, double u) {
+    double hi = rmin(0.5 * e1, offset + 0.5 * e2 - u);
+    double lo = rmax(-0.5 * e1, offset - 0.5 * e2 - u);
+    return rmax(hi - lo, 0.0);
+}
+__device__ __forceinline__ double parallel_primitive(double q, double rho_sq) {
+    q = fabs(q);
+    double root = sqrt(q * q + rho_sq);
+    if (q == 0.0) return -root;
+    return q * log(q + root) - root;
+}
+// lines::parallel (lines.rs:54-70); false for coaxial overlap.
+__device__ __forceinline__ bool lines_parallel(double l1, double l2, double offset, double rho, double *out) {
+    double rho_sq = rho * rho;
+    double smooth = parallel_primitive(offset + l2, rho_sq) - parallel_primitive(offset, rho_sq) -
+                    parallel_primitive(offset + l2 - l1, rho_sq) + parallel_primitive(offset - l1, rho_sq);
+    double overlap = rmax(rmin(l1, offset + l2) - rmax(offset, 0.0), 0.0);
+    if (overlap == 0.0) {
+        *out = smooth;
+        return true;
+    }
+    if (rho > 0.0) {
+        *out = smooth - 2.0 * overlap * log(rho);
+        return true;
+    }
+    return false;
+}
+
+struct QuadCtx {
+    Aligned b;
+    double axial_start;
+};
+__device__ __forceinline__ double integrand(const QuadCtx &c, double u, double v) {
+    double weight = overlap_weight(c.b.width[0], c.b.width[1], c.b.offset[1], u) *
+                    overlap_weight(c.b.height[0], c.b.height[1], c.b.offset[2], v);
+    if (weight == 0.0) return 0.0;
+    double k;
+    if (!lines_parallel(c.b.length[0], c.b.length[1], c.axial_start, hypot(u, v), &k)) k = 0.0;
+    return weight * k;
+}
+
+struct Panel {
+    double u0, u1, v0, v1;
+    int depth;
+    int pad;
+};
+struct Leaf {
+    double a0, a1, b0, b1;  // direct: [a0,a1] x [b0,b1]; corner: a0 = a, b0 = b
+    int corner;
+    int pad;
+};
+
+constexpr int kQuadThreads = 128;
+constexpr int kStack = 320;
+constexpr int kLeaves = 32;
+constexpr long long kMaxPanels = 1 << 22;
+
+__device__ int break_points(double e1, double e2, double offset, double *out) {
+    double sum = 0.5 * (e1 + e2), diff = 0.5 * fabs(e1 - e2);
+    auto snap = [&](double x) { return fabs(x) <= 1e-12 * sum ? 0.0 : x; };
+    double p[5] = {snap(offset - sum), snap(offset - diff), snap(offset + diff), snap(offset + sum), 0.0};
+    int cnt = 4;
+    if (p[0] < 0.0 && p[3] > 0.0) cnt = 5;
+    // insertion sort (total order; values are finite, zeros are +0.0)
+    for (int i = 1; i < cnt; ++i) {
+        double x = p[i];
+        int k = i - 1;
+        while (k >= 0 && total_cmp(p[k], x) > 0) {
+            p[k + 1] = p[k];
+            --k;
+        }
+        p[k + 1] = x;
+    }
+    int m = 0;
+    for (int i = 0; i < cnt; ++i)
+        if (m == 0 || !(out[m - 1] == p[i])) out[m++] = p[i];
+    return m;
+}
+
+__global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
+    const DevFil *__restrict__ fil, const int4 *__restrict__ items, const int64_t *__restrict__ heads,
+    int64_t n_heads, double *__restrict__ values) {
+    __shared__ Panel stack[kStack];
+    __shared__ Leaf leaves[kLeaves];
+    __shared__ int s_nleaves, s_done;
+    __shared__ QuadCtx ctx;
+    __shared__ double s_red[kQuadThreads / 32];
+    __shared__ double r10n[10], r10w[10], r16n[16], r16w[16];
+    if (threadIdx.x < 10) {
+        r10n[threadIdx.x] = c_quad.nodes[10][threadIdx.x];
+        r10w[threadIdx.x] = c_quad.weights[10][threadIdx.x];
+    }
+    if (threadIdx.x < 16) {
+        r16n[threadIdx.x] = c_quad.nodes[16][threadIdx.x];
+        r16w[threadIdx.x] = c_quad.weights[16][threadIdx.x];
+    }
+    for (int64_t h = blockIdx.x; h < n_heads; h += gridDim.x) {
+        const int4 it = items[heads[h]];
+        int sp = 0;
+        double axial_scale = 0.0;
+        if (threadIdx.x == 0) {
+            const DevFil &A = fil[it.x];
+            const DevFil &B = fil[it.y];
+            aligned_bars(A, B, &ctx.b);
+            const Aligned &b = ctx.b;
+            ctx.axial_start = b.offset[0] + 0.5 * (b.length[0] - b.length[1]);
+            double l1 = b.length[0], l2 = b.length[1], as = ctx.axial_start;
+            double sep[4] = {as + l2, as, as + l2 - l1, as - l1};
+            double largest = 0.0;
+            for (int k = 0; k < 4; ++k) largest = rmax(largest, fabs(sep[k]));
+            axial_scale = INFINITY;
+            for (int k = 0; k < 4; ++k)
+                if (fabs(sep[k]) > 1e-9 * largest) axial_scale = rmin(axial_scale, fabs(sep[k]));
+            double us[5], vs[5];
+            int nu = break_points(b.width[0], b.width[1], b.offset[1], us);
+            int nv = break_points(b.height[0], b.height[1], b.offset[2], vs);
+            // Push panels in reverse so that they pop in the reference's order.
+            for (int a = nu - 2; a >= 0; --a)
+                for (int c = nv - 2; c >= 0; --c) stack[sp++] = Panel{us[a], us[a + 1], vs[c], vs[c + 1], 0, 0};
+        }
+        double acc = 0.0;
+        long long visited = 0;  // panels popped; bounded so that no input can loop without end
+        bool overflow = false;
+        for (;;) {
+            if (threadIdx.x == 0) {
+                // Walk the panel tree until the leaf buffer is full or the tree is done.
+                int nl = 0;
+                while (sp > 0 && nl < kLeaves) {
+                    if (++visited > kMaxPanels) {
+                        overflow = true;
+                        sp = 0;
+                        break;
+                    }
+                    Panel p = stack[--sp];
+                    double su = p.u1 - p.u0, sv = p.v1 - p.v0;
+                    if (su <= 0.0 || sv <= 0.0) continue;
+                    auto gap = [](double r0, double r1) { return r0 > 0.0 ? r0 : (r1 < 0.0 ? -r1 : 0.0); };
+                    double distance = hypot(gap(p.u0, p.u1), gap(p.v0, p.v1));
+                    double size = rmax(su, sv);
+                    bool split_u = false, split_v = false;
+                    double at = 0.0;
+                    if (p.depth >= 200 || sp + 2 > kStack) {
+                        leaves[nl++] = Leaf{p.u0, p.u1, p.v0, p.v1, 0, 0};
+                        continue;
+                    }
+                    if (distance > 0.0) {
+                        if (size <= distance) {
+                            leaves[nl++] = Leaf{p.u0, p.u1, p.v0, p.v1, 0, 0};
+                            continue;
+                        }
+                        if (su >= sv) {
+                            split_u = true;
+                            at = 0.5 * (p.u0 + p.u1);
+                        } else {
+                            split_v = true;
+                            at = 0.5 * (p.v0 + p.v1);
+                        }
+                    } else {
+                        double target = rmin(rmin(su, sv), axial_scale);
+                        if (su > 2.0 * target) {
+                            split_u = true;
+                            at = p.u0 == 0.0 ? target : -target;
+                        } else if (sv > 2.0 * target) {
+                            split_v = true;
+                            at = p.v0 == 0.0 ? target : -target;
+                        } else {
+                            double fa = p.u0 == 0.0 ? p.u1 : p.u0;
+                            double fb = p.v0 == 0.0 ? p.v1 : p.v0;
+                            leaves[nl++] = Leaf{fa, 0.0, fb, 0.0, 1, 0};
+                            continue;
+                        }
+                    }
+                    // push second half first so the first half is processed next
+                    if (split_u) {
+                        stack[sp++] = Panel{at, p.u1, p.v0, p.v1, p.depth + 1, 0};
+                        stack[sp++] = Panel{p.u0, at, p.v0, p.v1, p.depth + 1, 0};
+                    } else if (split_v) {
+                        stack[sp++] = Panel{p.u0, p.u1, at, p.v1, p.depth + 1, 0};
+                        stack[sp++] = Panel{p.u0, p.u1, p.v0, at, p.depth + 1, 0};
+                    }
+                }
+                s_nleaves = nl;
+                s_done = sp == 0;
+            }
+            __syncthreads();
+            const int nl = s_nleaves;
+            // Evaluate the leaves: direct leaves have 100 points, corner leaves 256 (each two terms).
+            for (int l = 0; l < nl; ++l) {
+                const Leaf lf = leaves[l];
+                if (!lf.corner) {
+                    double mu = 0.5 * (lf.a0 + lf.a1), hu = 0.5 * (lf.a1 - lf.a0);
+                    double mv = 0.5 * (lf.b0 + lf.b1), hv = 0.5 * (lf.b1 - lf.b0);
+                    for (int k = threadIdx.x; k < 100; k += kQuadThreads) {
+                        int a = k / 10, c = k % 10;
+                        double uu = mu + hu * r10n[a], wu = hu * r10w[a];
+                        double vv = mv + hv * r10n[c], wv = hv * r10w[c];
+                        acc += wu * wv * integrand(ctx, uu, vv);
+                    }
+                } else {
+                    const double A = lf.a0, B = lf.b0, ab = fabs(A * B);
+                    for (int k = threadIdx.x; k < 256; k += kQuadThreads) {
+                        int a = k / 16, c = k % 16;
+                        double tau = 0.5 + 0.5 * r16n[a], w_tau = 0.5 * r16w[a];
+                        double s = tau * tau * tau;
+                        double radial = w_tau * 3.0 * tau * tau * s;
+                        double t = 0.5 + 0.5 * r16n[c], w_t = 0.5 * r16w[c];
+                        double value = integrand(ctx, A * s, B * s * t) + integrand(ctx, A * s * t, B * s);
+                        acc += radial * w_t * value * ab;
+                    }
+                }
+            }
+            __syncthreads();
+            if (s_done) break;
+        }
+        // block reduction
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            for (int w = 0; w < kQuadThreads / 32; ++w) s += s_red[w];
+            values[h] = overflow ? NAN : s;  // reported as NotFinite by the scatter
+        }
+        __syncthreads();
+    }
+}
+
+// Writes every aligned-quadrature pair from its key's value.
+__global__ void aligned_scatter_kernel(const DevFil *__restrict__ fil, const int4 *__restrict__ items,
+                                       const int64_t *__restrict__ head_of, const double *__restrict__ head_value,
+                                       int64_t count, double *__restrict__ L, int8_t *methods, int64_t n,
+                                       DevError *err) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int4 it = items[t];
+        const DevFil &A = fil[it.x];
+        const DevFil &B = fil[it.y];
+        const double cosv = ndot(A.axes, B.axes);
+        const double scale = signum(cosv) / (A.area * B.area);
+        store_pair(L, methods, n, it.x, it.y, kMu0Over4Pi * (head_value[head_of[t]] * scale), kAlignedQuadrature,
+                   err);
+    }
+}
+
+// Key of an aligned pair: the nine numbers of AlignedBars (memo.rs:61-76).
+__device__ __forceinline__ void aligned_key(const DevFil *fil, int4 it, unsigned long long k[9]) {
+    Aligned b;
+    aligned_bars(fil[it.x], fil[it.y], &b);
+    const double v[9] = {b.length[0], b.length[1], b.width[0], b.width[1], b.height[0],
+                         b.height[1], b.offset[0], b.offset[1], b.offset[2]};
+    for (int i = 0; i < 9; ++i) k[i] = (unsigned long long)__double_as_longlong(v[i]);
+}
+
+__global__ void key_hash_kernel(const DevFil *__restrict__ fil, const int4 *__restrict__ items, int64_t count,
+                                unsigned long long *__restrict__ hash, int64_t *__restrict__ index) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        unsigned long long k[9];
+        aligned_key(fil, items[t], k);
+        unsigned long long h = 0x9e3779b97f4a7c15ull;
+        for (int i = 0; i < 9; ++i) {
+            h = (h ^ k[i]) * 0x9e3779b97f4a7c15ull;
+            h = (h << 29) | (h >> 35);
+        }
+        h ^= h >> 30;
+        h *= 0xbf58476d1ce4e5b9ull;
+        h ^= h >> 27;
+        h *= 0x94d049bb133111ebull;
+        h ^= h >> 31;
+        hash[t] = h;
+        index[t] = t;
+    }
+}
+
+// After sorting by hash: flag[t] = 1 when item t starts a new key run.
+__global__ void key_heads_kernel(const DevFil *__restrict__ fil, const int4 *__restrict__ items,
+                                 const unsigned long long *__restrict__ hash_sorted,
+                                 const int64_t *__restrict__ order, int64_t count, int64_t *__restrict__ head_pos) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        bool head = t == 0 || hash_sorted[t] != hash_sorted[t - 1];
+        if (!head) {
+            unsigned long long a[9], b[9];
+            aligned_key(fil, items[order[t]], a);
+            aligned_key(fil, items[order[t - 1]], b);
+            for (int i = 0; i < 9; ++i)
+                if (a[i] != b[i]) head = true;
+        }
+        head_pos[t] = head ? t : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Sampled filaments (neumann.rs:280-325 with lines.rs:72-170), warp per pair.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double skew_log_term(double x, double big_r, double a, double residual_sq) {
+    if (x == 0.0) return 0.0;
+    double argument = a >= 0.0 ? big_r + a : residual_sq / (big_r - a);
+    return argument > 0.0 ? x * log(argument) : 0.0;
+}
+__device__ double skew_primitive(double s, double t, double d, double cosv, double sinv) {
+    double sin_sq = sinv * sinv;
+    double versine = sin_sq / (1.0 + fabs(cosv));
+    double planar_sq, a_s, a_t;
+    if (cosv >= 0.0) {
+        double diff = s - t;
+        planar_sq = diff * diff + 2.0 * s * t * versine;
+        a_s = s * versine - diff;
+        a_t = t * versine + diff;
+    } else {
+        double sum = s + t;
+        planar_sq = sum * sum - 2.0 * s * t * versine;
+        a_s = sum - s * versine;
+        a_t = sum - t * versine;
+    }
+    double big_r = sqrt(rmax(planar_sq + d * d, 0.0));
+    double logs = skew_log_term(s, big_r, a_s, s * s * sin_sq + d * d) + skew_log_term(t, big_r, a_t, t * t * sin_sq + d * d);
+    if (d == 0.0 || big_r == 0.0) return logs;
+    return logs - (d / sinv) * atan((d * d * cosv + s * t * sin_sq) / (d * big_r * sinv));
+}
+__device__ bool lines_skew(const double *a0, const double *a1, const double *b0, const double *b1, double *out) {
+    double da[3] = {a1[0] - a0[0], a1[1] - a0[1], a1[2] - a0[2]};
+    double db[3] = {b1[0] - b0[0], b1[1] - b0[1], b1[2] - b0[2]};
+    double la = sqrt(da[0] * da[0] + da[1] * da[1] + da[2] * da[2]);
+    double lb = sqrt(db[0] * db[0] + db[1] * db[1] + db[2] * db[2]);
+    double u[3] = {da[0] / la, da[1] / la, da[2] / la}, v[3] = {db[0] / lb, db[1] / lb, db[2] / lb};
+    double cosv = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+    double c[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+    double sinv = sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    if (isnan(sinv) || sinv < 0.0) return false;
+    double w0[3] = {a0[0] - b0[0], a0[1] - b0[1], a0[2] - b0[2]};
+    double du = u[0] * w0[0] + u[1] * w0[1] + u[2] * w0[2];
+    double dv = v[0] * w0[0] + v[1] * w0[1] + v[2] * w0[2];
+    double sin_sq = sinv * sinv;
+    double s0 = (cosv * dv - du) / sin_sq, t0 = (dv - cosv * du) / sin_sq;
+    double r[3] = {w0[0] + u[0] * s0 - v[0] * t0, w0[1] + u[1] * s0 - v[1] * t0, w0[2] + u[2] * s0 - v[2] * t0};
+    double d = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    double w0n = sqrt(w0[0] * w0[0] + w0[1] * w0[1] + w0[2] * w0[2]);
+    if (d <= 1e-14 * (la + lb + w0n)) d = 0.0;
+    double s_lo = -s0, s_hi = la - s0, t_lo = -t0, t_hi = lb - t0;
+    *out = skew_primitive(s_hi, t_hi, d, cosv, sinv) - skew_primitive(s_hi, t_lo, d, cosv, sinv) -
+           skew_primitive(s_lo, t_hi, d, cosv, sinv) + skew_primitive(s_lo, t_lo, d, cosv, sinv);
+    return true;
+}
+
+__global__ void __launch_bounds__(128) sampled_kernel(const DevFil *__restrict__ fil, const int4 *__restrict__ items,
+                                                      int64_t count, double *__restrict__ L, int8_t *methods,
+                                                      int64_t n, DevError *err) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t t = warp; t < count; t += warps) {
+        const int4 it = items[t];
+        const DevFil &A = fil[it.x];
+        const DevFil &B = fil[it.y];
+        const double cosv = ndot(A.axes, B.axes);
+        double cr[3];
+        ncross(A.axes, B.axes, cr);
+        const bool parallel = nnorm(cr) < 1e-6;
+        const double gap = separation(A, B);
+        auto order = [&](double half, int bump) {
+            int o = order_for(c_quad.sample_thresholds, 8, half, gap);
+            return o ? o : 8 + bump;
+        };
+        const int oa0 = order(A.half[1], 0), oa1 = order(A.half[2], 0);
+        const int ob0 = order(B.half[1], 1), ob1 = order(B.half[2], 1);
+        const int na = oa0 * oa1, nb = ob0 * ob1;
+        const double la = 2.0 * A.half[0], lb = 2.0 * B.half[0];
+        double acc = 0.0;
+        int bad = 0;
+        for (int k = lane; k < na * nb; k += 32) {
+            const int ia = k / nb, ib = k % nb;
+            const int iaw = ia / oa1, iah = ia % oa1, ibw = ib / ob1, ibh = ib % ob1;
+            double pa[3], pb[3];
+            const double xaw = 0.5 * c_quad.nodes[oa0][iaw], xah = 0.5 * c_quad.nodes[oa1][iah];
+            const double xbw = 0.5 * c_quad.nodes[ob0][ibw], xbh = 0.5 * c_quad.nodes[ob1][ibh];
+            const double wa = (0.5 * c_quad.weights[oa0][iaw]) * (0.5 * c_quad.weights[oa1][iah]);
+            const double wb = (0.5 * c_quad.weights[ob0][ibw]) * (0.5 * c_quad.weights[ob1][ibh]);
+            for (int d = 0; d < 3; ++d) {
+                pa[d] = A.centre[d] + (A.axes[3 + d] * (2.0 * A.half[1] * xaw) + A.axes[6 + d] * (2.0 * A.half[2] * xah));
+                pb[d] = B.centre[d] + (B.axes[3 + d] * (2.0 * B.half[1] * xbw) + B.axes[6 + d] * (2.0 * B.half[2] * xbh));
+            }
+            double kernel = 0.0;
+            bool ok;
+            if (parallel) {
+                double delta[3] = {pb[0] - pa[0], pb[1] - pa[1], pb[2] - pa[2]};
+                double along = delta[0] * A.axes[0] + delta[1] * A.axes[1] + delta[2] * A.axes[2];
+                double rr[3] = {delta[0] - A.axes[0] * along, delta[1] - A.axes[1] * along, delta[2] - A.axes[2] * along};
+                double rho = sqrt(rr[0] * rr[0] + rr[1] * rr[1] + rr[2] * rr[2]);
+                ok = lines_parallel(la, lb, along + 0.5 * (la - lb), rho, &kernel);
+            } else {
+                double a0[3], a1[3], b0[3], b1[3];
+                for (int d = 0; d < 3; ++d) {
+                    a0[d] = pa[d] - A.axes[d] * A.half[0];
+                    a1[d] = pa[d] + A.axes[d] * A.half[0];
+                    b0[d] = pb[d] - B.axes[d] * B.half[0];
+                    b1[d] = pb[d] + B.axes[d] * B.half[0];
+                }
+                ok = lines_skew(a0, a1, b0, b1, &kernel);
+            }
+            if (!ok) bad = 1;
+            acc += wa * wb * kernel;
+        }
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        bad = __any_sync(0xffffffffu, bad);
+        if (lane == 0) {
+            if (bad) {
+                record_error(err, it.x, it.y, FH_ERR_KERNEL_COINCIDENT);
+            } else {
+                const double direction = parallel ? signum(cosv) : cosv;
+                store_pair(L, methods, n, it.x, it.y, kMu0Over4Pi * (acc * direction), kSampled, err);
+            }
+        }
+    }
+}
+
+// Upper-triangle congruence tile with mirrored store (solve.rs:1172-1200).
+// Entry (i, j), i <= j:  sum over (b, s_b) in row j of s_b * sum over (a, s_a)
+// in row i of s_a * B[b, a].  B is symmetric so B[b, a] is read as B[a + b n]
+// (bit-identical), which keeps the loads coalesced across i.
+template <bool kDiag>
+__global__ void __launch_bounds__(256) congruence_kernel(const double *__restrict__ B, const double *__restrict__ Rdiag,
+                                                         int64_t n, const int64_t *__restrict__ row_ptr,
+                                                         const int32_t *__restrict__ branch,
+                                                         const double *__restrict__ sign, int64_t loops,
+                                                         double *__restrict__ out) {
+    const int64_t I = blockIdx.y, J = blockIdx.x;
+    if (I > J) return;
+    __shared__ double tile[32][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;  // (32, 8)
+    for (int r = ty; r < 32; r += 8) {
+        const int64_t i = I * 32 + tx, j = J * 32 + r;
+        double v = 0.0;
+        if (i < loops && j < loops && i <= j) {
+            const int64_t pi0 = row_ptr[i], pi1 = row_ptr[i + 1], pj0 = row_ptr[j], pj1 = row_ptr[j + 1];
+            for (int64_t q = pj0; q < pj1; ++q) {
+                const int64_t b = branch[q];
+                double inner = 0.0;
+                for (int64_t p = pi0; p < pi1; ++p) {
+                    const int64_t a = branch[p];
+                    double bab;
+                    if (kDiag) bab = a == b ? Rdiag[a] : 0.0;
+                    else bab = B[a + b * n];
+                    inner = __dadd_rn(inner, __dmul_rn(sign[p], bab));
+                }
+                v = __dadd_rn(v, __dmul_rn(sign[q], inner));
+            }
+            out[i + j * loops] = v;
+        }
+        tile[r][tx] = v;
+    }
+    __syncthreads();
+    // Mirror: out[row + col*loops] = value(i = col, j = row) for row > col,
+    // with row = 32J + tx (coalesced) and col = 32I + r.
+    for (int r = ty; r < 32; r += 8) {
+        const int64_t row = J * 32 + tx, col = I * 32 + r;
+        if (row < loops && col < loops && row > col) out[row + col * loops] = tile[tx][r];
+    }
+}
+
+}  // namespace
+
+DevFil make_devfil(const fh_filament &f) {
+    DevFil d{};
+    for (int k = 0; k < 3; ++k) {
+        d.centre[k] = (f.start[k] + f.end[k]) * 0.5;
+        d.axes[k] = f.dir_length[k];
+        d.axes[3 + k] = f.dir_width[k];
+        d.axes[6 + k] = f.dir_height[k];
+        d.start[k] = f.start[k];
+        d.end[k] = f.end[k];
+    }
+    d.half[0] = 0.5 * f.length;
+    d.half[1] = 0.5 * f.width;
+    d.half[2] = 0.5 * f.height;
+    d.area = f.width * f.height;
+    d.width = f.width;
+    d.height = f.height;
+    d.length = f.length;
+    return d;
+}
+
+namespace {
+bool g_tables_uploaded[64] = {false};
+}
+
+fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_methods, cudaStream_t stream,
+                      FillStats *stats, fh_error_info *err) {
+    if (n == 0) return FH_OK;
+    if (n > 2000000000LL / 32) return fail(err, FH_ERR_INVALID_ARGUMENT, "too many filaments for the fill");
+    int dev = 0;
+    FHB_CUDA(cudaGetDevice(&dev));
+    if (dev < 64 && !g_tables_uploaded[dev]) {
+        QuadTables t;
+        host_quad_tables(t);
+        FHB_CUDA(cudaMemcpyToSymbol(c_quad, &t, sizeof t));
+        g_tables_uploaded[dev] = true;
+    }
+    FillStats local;
+    FillStats &st = stats ? *stats : local;
+    st = FillStats();
+    st.pairs = n * (n + 1) / 2;
+    cudaEvent_t ev[6];
+    for (auto &e : ev) FHB_CUDA(cudaEventCreate(&e));
+    struct Guard {
+        std::vector<void *> ptrs;
+        cudaEvent_t *ev;
+        ~Guard() {
+            for (void *p : ptrs) cudaFree(p);
+            for (int k = 0; k < 6; ++k) cudaEventDestroy(ev[k]);
+        }
+    } guard{{}, ev};
+    auto alloc = [&](void **p, size_t bytes) -> cudaError_t {
+        cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+        if (e == cudaSuccess) guard.ptrs.push_back(*p);
+        return e;
+    };
+    unsigned long long *d_counts = nullptr, *d_cursor = nullptr;
+    DevError *d_err = nullptr;
+    FHB_CUDA(alloc((void **)&d_counts, sizeof(unsigned long long) * kCats * 2 + sizeof(DevError) + 64));
+    d_cursor = d_counts + kCats;
+    d_err = reinterpret_cast<DevError *>(d_counts + 2 * kCats);
+    FHB_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * kCats * 2, stream));
+    FHB_CUDA(cudaMemsetAsync(d_err, 0xff, sizeof(unsigned long long), stream));
+    FHB_CUDA(cudaMemsetAsync(&d_err->code, 0, sizeof(int), stream));
+    const int T = (int)((n + 31) / 32);
+    dim3 grid(T, T), block(32, 8);
+    FHB_CUDA(cudaEventRecord(ev[0], stream));
+    classify_kernel<false><<<grid, block, 0, stream>>>(d_fil, (int)n, d_counts, nullptr, nullptr);
+    FHB_CUDA(cudaGetLastError());
+    unsigned long long counts[kCats];
+    FHB_CUDA(cudaMemcpyAsync(counts, d_counts, sizeof counts, cudaMemcpyDeviceToHost, stream));
+    FHB_CUDA(cudaStreamSynchronize(stream));
+    unsigned long long offsets[kCats + 1];
+    offsets[0] = 0;
+    for (int c = 0; c < kCats; ++c) offsets[c + 1] = offsets[c] + counts[c];
+    const unsigned long long total_items = offsets[kCats];
+    int4 *d_items = nullptr;
+    FHB_CUDA(alloc((void **)&d_items, sizeof(int4) * total_items));
+    FHB_CUDA(cudaMemcpyAsync(d_cursor, offsets, sizeof(unsigned long long) * kCats, cudaMemcpyHostToDevice, stream));
+    classify_kernel<true><<<grid, block, 0, stream>>>(d_fil, (int)n, nullptr, d_cursor, d_items);
+    FHB_CUDA(cudaGetLastError());
+    FHB_CUDA(cudaEventRecord(ev[1], stream));
+    const int sms = 148;
+    // Point quadrature over all buckets (contiguous, cost ascending).
+    const int64_t n_point = (int64_t)offsets[kPointBuckets];
+    st.point = n_point;
+    for (int c = 0; c < kPointBuckets; ++c) st.point_evaluations += (double)counts[c] * (1.5 * (double)(1ull << c));
+    if (n_point) {
+        int blocks = (int)std::min<int64_t>((n_point + 127) / 128, (int64_t)sms * 64);
+        point_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_items, n_point, d_L, d_methods, n, d_err);
+        FHB_CUDA(cudaGetLastError());
+    }
+    FHB_CUDA(cudaEventRecord(ev[2], stream));
+    // Aligned pairs: closed form, then the quadrature for the rest.
+    const int64_t n_aligned = (int64_t)counts[kCatAligned];
+    const int4 *d_aligned = d_items + offsets[kCatAligned];
+    int4 *d_quad = nullptr;
+    unsigned long long *d_qcount = d_cursor + kCatAligned;  // reuse the slot as a counter
+    FHB_CUDA(cudaMemsetAsync(d_qcount, 0, sizeof(unsigned long long), stream));
+    int64_t n_quad = 0;
+    if (n_aligned) {
+        FHB_CUDA(alloc((void **)&d_quad, sizeof(int4) * n_aligned));
+        int blocks = (int)std::min<int64_t>((n_aligned + 127) / 128, (int64_t)sms * 32);
+        closed_form_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_aligned, n_aligned, d_L, d_methods, n, d_quad,
+                                                       d_qcount, d_err);
+        FHB_CUDA(cudaGetLastError());
+        unsigned long long q = 0;
+        FHB_CUDA(cudaMemcpyAsync(&q, d_qcount, sizeof q, cudaMemcpyDeviceToHost, stream));
+        FHB_CUDA(cudaStreamSynchronize(stream));
+        n_quad = (int64_t)q;
+    }
+    FHB_CUDA(cudaEventRecord(ev[3], stream));
+    st.closed_form = n_aligned - n_quad;
+    st.aligned_quadrature = n_quad;
+    if (n_quad) {
+        // Distinct keys: hash, sort, flag run heads, max-scan to map every
+        // pair to its run head, evaluate heads only.
+        unsigned long long *d_hash, *d_hash_sorted;
+        int64_t *d_idx, *d_order, *d_headpos, *d_headof;
+        FHB_CUDA(alloc((void **)&d_hash, 8 * n_quad));
+        FHB_CUDA(alloc((void **)&d_hash_sorted, 8 * n_quad));
+        FHB_CUDA(alloc((void **)&d_idx, 8 * n_quad));
+        FHB_CUDA(alloc((void **)&d_order, 8 * n_quad));
+        FHB_CUDA(alloc((void **)&d_headpos, 8 * n_quad));
+        FHB_CUDA(alloc((void **)&d_headof, 8 * n_quad));
+        int blocks = (int)std::min<int64_t>((n_quad + 255) / 256, (int64_t)sms * 16);
+        key_hash_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_quad, n_quad, d_hash, d_idx);
+        FHB_CUDA(cudaGetLastError());
+        size_t tmp_bytes = 0, tmp2 = 0;
+        FHB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_hash, d_hash_sorted, d_idx, d_order,
+                                                 (int)n_quad, 0, 64, stream));
+        FHB_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tmp2, d_headpos, d_headof, cub::Max(), (int)n_quad, stream));
+        void *d_tmp = nullptr;
+        FHB_CUDA(alloc(&d_tmp, std::max(tmp_bytes, tmp2)));
+        tmp_bytes = std::max(tmp_bytes, tmp2);
+        FHB_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_hash, d_hash_sorted, d_idx, d_order, (int)n_quad,
+                                                 0, 64, stream));
+        key_heads_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_quad, d_hash_sorted, d_order, n_quad, d_headpos);
+        FHB_CUDA(cudaGetLastError());
+        FHB_CUDA(cub::DeviceScan::InclusiveScan(d_tmp, tmp_bytes, d_headpos, d_headof, cub::Max(), (int)n_quad, stream));
+        // Compact the heads: head positions are where headof[t] == t.
+        std::vector<int64_t> h_headof((size_t)n_quad), h_order((size_t)n_quad);
+        FHB_CUDA(cudaMemcpyAsync(h_headof.data(), d_headof, 8 * n_quad, cudaMemcpyDeviceToHost, stream));
+        FHB_CUDA(cudaMemcpyAsync(h_order.data(), d_order, 8 * n_quad, cudaMemcpyDeviceToHost, stream));
+        FHB_CUDA(cudaStreamSynchronize(stream));
+        // Build, per original item, the index of its head among the distinct keys.
+        std::vector<int64_t> head_item, item_head((size_t)n_quad);
+        std::vector<int64_t> head_rank((size_t)n_quad, -1);
+        for (int64_t t = 0; t < n_quad; ++t) {
+            if (h_headof[t] == t) {
+                head_rank[t] = (int64_t)head_item.size();
+                head_item.push_back(h_order[t]);
+            }
+            item_head[h_order[t]] = head_rank[h_headof[t]];
+        }
+        const int64_t n_heads = (int64_t)head_item.size();
+        st.unique_aligned = n_heads;
+        int64_t *d_heads, *d_item_head;
+        double *d_values;
+        FHB_CUDA(alloc((void **)&d_heads, 8 * n_heads));
+        FHB_CUDA(alloc((void **)&d_item_head, 8 * n_quad));
+        FHB_CUDA(alloc((void **)&d_values, 8 * n_heads));
+        FHB_CUDA(cudaMemcpyAsync(d_heads, head_item.data(), 8 * n_heads, cudaMemcpyHostToDevice, stream));
+        FHB_CUDA(cudaMemcpyAsync(d_item_head, item_head.data(), 8 * n_quad, cudaMemcpyHostToDevice, stream));
+        int qblocks = (int)std::min<int64_t>(n_heads, (int64_t)sms * 16);
+        aligned_quadrature_kernel<<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads, d_values);
+        FHB_CUDA(cudaGetLastError());
+        aligned_scatter_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_quad, d_item_head, d_values, n_quad, d_L,
+                                                           d_methods, n, d_err);
+        FHB_CUDA(cudaGetLastError());
+    }
+    FHB_CUDA(cudaEventRecord(ev[4], stream));
+    const int64_t n_sampled = (int64_t)counts[kCatSampled];
+    st.sampled = n_sampled;
+    if (n_sampled) {
+        int blocks = (int)std::min<int64_t>((n_sampled * 32 + 127) / 128, (int64_t)sms * 32);
+        sampled_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_items + offsets[kCatSampled], n_sampled, d_L, d_methods, n,
+                                                   d_err);
+        FHB_CUDA(cudaGetLastError());
+    }
+    FHB_CUDA(cudaEventRecord(ev[5], stream));
+    DevError h_err;
+    FHB_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof h_err, cudaMemcpyDeviceToHost, stream));
+    FHB_CUDA(cudaStreamSynchronize(stream));
+    st.orthogonal = st.pairs - (int64_t)total_items;
+    cudaEventElapsedTime(&st.ms_classify, ev[0], ev[1]);
+    cudaEventElapsedTime(&st.ms_point, ev[1], ev[2]);
+    cudaEventElapsedTime(&st.ms_aligned, ev[2], ev[3]);
+    cudaEventElapsedTime(&st.ms_quadrature, ev[3], ev[4]);
+    cudaEventElapsedTime(&st.ms_sampled, ev[4], ev[5]);
+    if (h_err.key != ~0ull) {
+        int64_t i = (int64_t)(h_err.key >> 32), j = (int64_t)(h_err.key & 0xffffffffull);
+        if (h_err.code == FH_ERR_KERNEL_COINCIDENT)
+            return fail(err, FH_ERR_KERNEL_COINCIDENT,
+                        "overlapping parallel filaments " + std::to_string(i) + " and " + std::to_string(j) +
+                            " have misaligned cross-sections and coincident sample lines",
+                        i, j);
+        return fail(err, FH_ERR_KERNEL_NOT_FINITE,
+                    "partial inductance of filaments " + std::to_string(i) + " and " + std::to_string(j) +
+                        " is not finite",
+                    i, j);
+    }
+    return FH_OK;
+}
+
+fh_status device_congruence(const double *d_L, const double *d_R, int64_t n, const int64_t *d_row_ptr,
+                            const int32_t *d_branch, const double *d_sign, int64_t loops, double *d_Lm, double *d_Rm,
+                            cudaStream_t stream, fh_error_info *err) {
+    if (loops == 0) return FH_OK;
+    const int T = (int)((loops + 31) / 32);
+    dim3 grid(T, T), block(32, 8);
+    congruence_kernel<false><<<grid, block, 0, stream>>>(d_L, nullptr, n, d_row_ptr, d_branch, d_sign, loops, d_Lm);
+    FHB_CUDA(cudaGetLastError());
+    congruence_kernel<true><<<grid, block, 0, stream>>>(nullptr, d_R, n, d_row_ptr, d_branch, d_sign, loops, d_Rm);
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+}  // namespace fhb

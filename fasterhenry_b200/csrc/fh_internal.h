@@ -1,0 +1,46 @@
+// Internal declarations shared by the host model (fh_host.cpp) and the
+// device side (fh_*.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/fasterhenry_b200.h"
+
+namespace fhb {
+
+// Records `msg` as this thread's fh_last_error() and fills `err`.
+fh_status fail(fh_error_info *err, fh_status status, const std::string &msg, int64_t a = -1,
+               int64_t b = -1, double frequency = 0.0, int32_t detail = 0);
+void clear_error(fh_error_info *err);
+
+struct Vec3 {
+    double x, y, z;
+};
+
+// Filament bundles of every segment, in segment order.
+struct Discretized {
+    std::vector<fh_filament> filaments;
+    std::vector<int64_t> per_segment;
+};
+
+fh_status validate_geometry(const fh_node *nodes, size_t n_nodes, const fh_segment_def *segs,
+                            size_t n_segs, fh_error_info *err);
+fh_status discretize_geometry(const fh_node *nodes, size_t n_nodes, const fh_segment_def *segs,
+                              size_t n_segs, const fh_discretization *disc, Discretized &out,
+                              fh_error_info *err);
+
+// Loop basis, CSR.
+struct LoopBasis {
+    std::vector<int64_t> row_ptr;
+    std::vector<int32_t> branch;
+    std::vector<double> sign;
+    int64_t internal = 0;
+    int64_t rows() const { return (int64_t)row_ptr.size() - 1; }
+};
+fh_status build_loops(const fh_segment_def *segs, size_t n_segs, size_t n_nodes,
+                      const int64_t *per_segment, const fh_port *ports, size_t n_ports,
+                      LoopBasis &out, fh_error_info *err);
+
+}  // namespace fhb

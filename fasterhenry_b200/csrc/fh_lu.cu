@@ -1,0 +1,663 @@
+// Batched blocked right-looking complex LU with partial pivoting.
+//
+// The algorithm is the reference's (fasterhenry/src/dense.rs:43-190: PA = LU,
+// pivot = first row of largest |re| + |im|, multipliers scaled by the
+// reciprocal of the pivot, zero pivot -> Singular), re-arranged for the GPU:
+//
+//   * every launch works on all frequencies of a sweep at once (grid.y /
+//     grid.z = matrix index), so one panel step is a handful of launches for
+//     the whole batch instead of one factorization per thread;
+//   * per panel column: a pivot search (one block per row chunk, the last
+//     block to finish reduces the partials and swaps the rows inside the
+//     panel) and a fused scale + rank-1 update of the panel;
+//   * after the panel: row interchanges of the trailing columns, a TRSM for
+//     U12 and the GEMM A22 -= L21 U12.  The GEMM is FP64 SIMT here (the FP64
+//     form) or split-BF16 x3 on the tensor cores (fh_gemm_tc.cu, FP32 form).
+//   * interchanges are never applied to the columns left of the panel: the
+//     forward substitution applies each panel's interchanges to the
+//     right-hand side just before that panel's L columns are used, which is
+//     the same elimination order.
+#include <cfloat>
+#include <climits>
+#include <cstdio>
+
+#include "fh_lu.cuh"
+
+namespace fhb {
+
+fh_status gemm_tc_update(float *a, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err);
+
+namespace {
+
+template <class T>
+struct __align__(2 * sizeof(T)) Cx {
+    T re, im;
+};
+
+template <class T>
+__device__ __forceinline__ Cx<T> cmul(Cx<T> a, Cx<T> b) {
+    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <class T>
+__device__ __forceinline__ Cx<T> csub(Cx<T> a, Cx<T> b) {
+    return {a.re - b.re, a.im - b.im};
+}
+template <class T>
+__device__ __forceinline__ Cx<T> cdiv(Cx<T> a, Cx<T> b) {
+    T ns = b.re * b.re + b.im * b.im;
+    T re = a.re * b.re + a.im * b.im;
+    T im = a.im * b.re - a.re * b.im;
+    return {re / ns, im / ns};
+}
+// y -= f * x
+template <class T>
+__device__ __forceinline__ void csubmul(Cx<T> &y, Cx<T> f, Cx<T> x) {
+    y.re -= f.re * x.re - f.im * x.im;
+    y.im -= f.re * x.im + f.im * x.re;
+}
+
+// ---------------------------------------------------------------------------
+// Pivot search for column j (rows j..m-1) of every matrix.  The last block of
+// a matrix to finish reduces the partials, records the pivot, flags a zero
+// pivot and swaps rows j and pivot across the panel's columns.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) pivot_kernel(Cx<T> *__restrict__ a, int64_t m, int j, int k0, int ncols,
+                                                    int *__restrict__ pivots, int *__restrict__ singular,
+                                                    double *__restrict__ pval, int *__restrict__ pidx,
+                                                    unsigned *__restrict__ tickets, int chunks) {
+    const int f = blockIdx.y;
+    Cx<T> *A = a + (int64_t)f * m * m;
+    double best = -1.0;
+    int bi = INT_MAX;
+    for (int64_t r = j + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
+        Cx<T> v = A[r + (int64_t)j * m];
+        const double n1 = (double)(fabs(v.re) + fabs(v.im));  // |re| + |im| in T
+        if (n1 > best || (n1 == best && r < bi)) {
+            best = n1;
+            bi = (int)r;
+        }
+    }
+    auto better = [](double v2, int i2, double v1, int i1) { return v2 > v1 || (v2 == v1 && i2 < i1); };
+    for (int o = 16; o > 0; o >>= 1) {
+        double v2 = __shfl_down_sync(0xffffffffu, best, o);
+        int i2 = __shfl_down_sync(0xffffffffu, bi, o);
+        if (better(v2, i2, best, bi)) {
+            best = v2;
+            bi = i2;
+        }
+    }
+    __shared__ double sv[8];
+    __shared__ int si[8];
+    __shared__ bool s_last;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        sv[warp] = best;
+        si[warp] = bi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+            if (better(sv[w], si[w], best, bi)) {
+                best = sv[w];
+                bi = si[w];
+            }
+        pval[f * chunks + blockIdx.x] = best;
+        pidx[f * chunks + blockIdx.x] = bi;
+        __threadfence();
+        unsigned ticket = atomicAdd(&tickets[f], 1u);
+        s_last = ticket == (unsigned)(chunks - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __shared__ int s_piv;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        double b = -1.0;
+        int i = INT_MAX;
+        for (int c = 0; c < chunks; ++c) {
+            double v2 = ((volatile double *)pval)[f * chunks + c];
+            int i2 = ((volatile int *)pidx)[f * chunks + c];
+            if (better(v2, i2, b, i)) {
+                b = v2;
+                i = i2;
+            }
+        }
+        int p = j;
+        if (b == 0.0) singular[f] = 1;  // exactly zero pivot (dense.rs:166-168)
+        else if (b > 0.0) p = i;       // all-NaN column: keep the diagonal
+        pivots[(int64_t)f * m + j] = p;
+        tickets[f] = 0;
+        s_piv = p;
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (p != j)
+        for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+            Cx<T> *col = A + (int64_t)(k0 + c) * m;
+            Cx<T> t = col[j];
+            col[j] = col[p];
+            col[p] = t;
+        }
+}
+
+// Scale column j below the pivot by 1/pivot and apply the rank-1 update to
+// the panel columns j+1 .. k0+ncols-1 (dense.rs:176-186).
+template <class T>
+__global__ void __launch_bounds__(256) panel_update_kernel(Cx<T> *__restrict__ a, int64_t m, int j, int k0, int ncols) {
+    const int f = blockIdx.y;
+    Cx<T> *A = a + (int64_t)f * m * m;
+    __shared__ Cx<T> prow[128];
+    const int rest = k0 + ncols - j;  // columns j .. k0+ncols-1
+    for (int c = threadIdx.x; c < rest; c += blockDim.x) prow[c] = A[j + (int64_t)(j + c) * m];
+    __syncthreads();
+    const Cx<T> one{(T)1, (T)0};
+    const Cx<T> inv = cdiv(one, prow[0]);
+    for (int64_t i = j + 1 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        Cx<T> l = cmul(A[i + (int64_t)j * m], inv);
+        A[i + (int64_t)j * m] = l;
+        for (int c = 1; c < rest; ++c) {
+            Cx<T> y = A[i + (int64_t)(j + c) * m];
+            csubmul(y, prow[c], l);
+            A[i + (int64_t)(j + c) * m] = y;
+        }
+    }
+}
+
+// Row interchanges of the panel applied to columns [c0, m).
+template <class T>
+__global__ void __launch_bounds__(256) swap_kernel(Cx<T> *__restrict__ a, int64_t m, int k0, int nb, int64_t c0,
+                                                   const int *__restrict__ pivots) {
+    const int f = blockIdx.y;
+    Cx<T> *A = a + (int64_t)f * m * m;
+    const int *piv = pivots + (int64_t)f * m;
+    for (int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m; c += (int64_t)gridDim.x * blockDim.x) {
+        Cx<T> *col = A + c * m;
+        for (int jj = 0; jj < nb; ++jj) {
+            int p = piv[k0 + jj];
+            if (p != k0 + jj) {
+                Cx<T> t = col[k0 + jj];
+                col[k0 + jj] = col[p];
+                col[p] = t;
+            }
+        }
+    }
+}
+
+// U12 = L11^{-1} A12 for columns [k0+nb, m): 64 columns per block, L11 and
+// the block's columns staged in shared memory.
+template <class T>
+__global__ void __launch_bounds__(64) trsm_kernel(Cx<T> *__restrict__ a, int64_t m, int k0, int nb) {
+    extern __shared__ unsigned char smem_raw[];
+    Cx<T> *Ls = reinterpret_cast<Cx<T> *>(smem_raw);  // [nb][nb] (row r, col k) at r*nb + k
+    Cx<T> *Bs = Ls + nb * nb;                          // [nb][64]
+    const int f = blockIdx.y;
+    Cx<T> *A = a + (int64_t)f * m * m;
+    const int64_t c0 = (int64_t)k0 + nb + (int64_t)blockIdx.x * 64;
+    for (int idx = threadIdx.x; idx < nb * nb; idx += 64) {
+        int r = idx % nb, k = idx / nb;
+        Ls[r * nb + k] = A[(k0 + r) + (int64_t)(k0 + k) * m];
+    }
+    const int64_t col = c0 + threadIdx.x;
+    for (int idx = threadIdx.x; idx < nb * 64; idx += 64) {
+        int r = idx % nb, cc = idx / nb;
+        int64_t c = c0 + cc;
+        Bs[r * 64 + cc] = c < m ? A[(k0 + r) + c * m] : Cx<T>{0, 0};
+    }
+    __syncthreads();
+    if (col < m) {
+        for (int k = 0; k < nb; ++k) {
+            Cx<T> xk = Bs[k * 64 + threadIdx.x];
+            for (int r = k + 1; r < nb; ++r) {
+                Cx<T> y = Bs[r * 64 + threadIdx.x];
+                csubmul(y, xk, Ls[r * nb + k]);
+                Bs[r * 64 + threadIdx.x] = y;
+            }
+        }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nb * 64; idx += 64) {
+        int r = idx % nb, cc = idx / nb;
+        int64_t c = c0 + cc;
+        if (c < m) A[(k0 + r) + c * m] = Bs[r * 64 + cc];
+    }
+}
+
+// A22 -= L21 U12 (SIMT).  Tile 64 x 64, K = nb <= 64; 256 threads, each a
+// 4 x 4 block of outputs interleaved with stride 16.
+template <class T>
+__global__ void __launch_bounds__(256) gemm_update_kernel(Cx<T> *__restrict__ a, int64_t m, int k0, int nb) {
+    extern __shared__ unsigned char smem_raw[];
+    Cx<T> *Ls = reinterpret_cast<Cx<T> *>(smem_raw);  // [nb][64]  Ls[k*64 + i]
+    Cx<T> *Us = Ls + nb * 64;                          // [nb][64]  Us[k*64 + j]
+    const int f = blockIdx.z;
+    Cx<T> *A = a + (int64_t)f * m * m;
+    const int64_t base = (int64_t)k0 + nb;
+    const int64_t i0 = base + (int64_t)blockIdx.y * 64, j0 = base + (int64_t)blockIdx.x * 64;
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < nb * 64; idx += 256) {
+        int ii = idx % 64, k = idx / 64;
+        int64_t row = i0 + ii;
+        Ls[k * 64 + ii] = row < m ? A[row + (int64_t)(k0 + k) * m] : Cx<T>{0, 0};
+        int kk = idx % nb, jj = idx / nb;
+        int64_t col = j0 + jj;
+        Us[kk * 64 + jj] = col < m ? A[(k0 + kk) + col * m] : Cx<T>{0, 0};
+    }
+    __syncthreads();
+    const int tx = tid & 15, ty = tid >> 4;
+    T accr[4][4], acci[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) accr[r][c] = acci[r][c] = (T)0;
+    for (int k = 0; k < nb; ++k) {
+        Cx<T> l[4], u[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) l[r] = Ls[k * 64 + tx + 16 * r];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) u[c] = Us[k * 64 + ty + 16 * c];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                accr[r][c] += l[r].re * u[c].re - l[r].im * u[c].im;
+                acci[r][c] += l[r].re * u[c].im + l[r].im * u[c].re;
+            }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        int64_t col = j0 + ty + 16 * c;
+        if (col >= m) continue;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            int64_t row = i0 + tx + 16 * r;
+            if (row >= m) continue;
+            Cx<T> y = A[row + col * m];
+            y.re -= accr[r][c];
+            y.im -= acci[r][c];
+            A[row + col * m] = y;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Solves.  x: count x nrhs columns of length m (matrix f, rhs q at
+// x + (f*nrhs + q)*m).
+// ---------------------------------------------------------------------------
+// Forward, one panel: apply the panel's interchanges, then L11 (unit).
+template <class T>
+__global__ void fwd_panel_kernel(const Cx<T> *__restrict__ a, int64_t m, int nrhs, int k0, int nb,
+                                 const int *__restrict__ pivots, Cx<T> *__restrict__ x) {
+    const int f = blockIdx.x / nrhs;
+    const Cx<T> *A = a + (int64_t)f * m * m;
+    Cx<T> *X = x + (int64_t)blockIdx.x * m;
+    __shared__ Cx<T> xs[128];
+    if (threadIdx.x == 0) {
+        const int *piv = pivots + (int64_t)f * m;
+        for (int jj = 0; jj < nb; ++jj) {
+            int p = piv[k0 + jj];
+            if (p != k0 + jj) {
+                Cx<T> t = X[k0 + jj];
+                X[k0 + jj] = X[p];
+                X[p] = t;
+            }
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < nb; r += blockDim.x) xs[r] = X[k0 + r];
+    __syncthreads();
+    for (int k = 0; k < nb; ++k) {
+        Cx<T> xk = xs[k];
+        for (int r = k + 1 + threadIdx.x; r < nb; r += blockDim.x) {
+            Cx<T> y = xs[r];
+            csubmul(y, xk, A[(k0 + r) + (int64_t)(k0 + k) * m]);
+            xs[r] = y;
+        }
+        __syncthreads();
+    }
+    for (int r = threadIdx.x; r < nb; r += blockDim.x) X[k0 + r] = xs[r];
+}
+
+// Backward, one panel: U11 (non-unit upper).
+template <class T>
+__global__ void bwd_panel_kernel2(const Cx<T> *__restrict__ a, int64_t m, int nrhs, int k0, int nb,
+                                  Cx<T> *__restrict__ x) {
+    const int f = blockIdx.x / nrhs;
+    const Cx<T> *A = a + (int64_t)f * m * m;
+    Cx<T> *X = x + (int64_t)blockIdx.x * m;
+    __shared__ Cx<T> xs[128];
+    for (int r = threadIdx.x; r < nb; r += blockDim.x) xs[r] = X[k0 + r];
+    __syncthreads();
+    for (int k = nb - 1; k >= 0; --k) {
+        if (threadIdx.x == 0) xs[k] = cdiv(xs[k], A[(k0 + k) + (int64_t)(k0 + k) * m]);
+        __syncthreads();
+        Cx<T> xk = xs[k];
+        for (int r = threadIdx.x; r < k; r += blockDim.x) {
+            Cx<T> y = xs[r];
+            csubmul(y, xk, A[(k0 + r) + (int64_t)(k0 + k) * m]);
+            xs[r] = y;
+        }
+        __syncthreads();
+    }
+    for (int r = threadIdx.x; r < nb; r += blockDim.x) X[k0 + r] = xs[r];
+}
+
+// x[r] -= sum_c A[r, k0 + c] x[k0 + c] for r in [r0, r1).
+template <class T>
+__global__ void __launch_bounds__(256) gemv_update_kernel(const Cx<T> *__restrict__ a, int64_t m, int nrhs, int k0,
+                                                          int nb, int64_t r0, int64_t r1, Cx<T> *__restrict__ x) {
+    const int g = blockIdx.y;  // (f, q)
+    const int f = g / nrhs;
+    const Cx<T> *A = a + (int64_t)f * m * m;
+    Cx<T> *X = x + (int64_t)g * m;
+    __shared__ Cx<T> xs[128];
+    for (int c = threadIdx.x; c < nb; c += blockDim.x) xs[c] = X[k0 + c];
+    __syncthreads();
+    for (int64_t r = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < r1; r += (int64_t)gridDim.x * blockDim.x) {
+        Cx<T> y = X[r];
+        for (int c = 0; c < nb; ++c) csubmul(y, xs[c], A[r + (int64_t)(k0 + c) * m]);
+        X[r] = y;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// System formation and FP64 residual.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) form_kernel(const double *__restrict__ R, const double *__restrict__ L, int64_t ld,
+                                                   int64_t m, const double *__restrict__ omega, int count,
+                                                   Cx<T> *__restrict__ a) {
+    const int64_t total = m * m;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t % m, j = t / m;
+        const double r = R[i + j * ld], l = L[i + j * ld];
+        for (int f = 0; f < count; ++f) a[(int64_t)f * total + t] = Cx<T>{(T)r, (T)(omega[f] * l)};
+    }
+}
+
+template <class T>
+__global__ void rhs_kernel(const double *__restrict__ R, const double *__restrict__ L, int64_t ld, int64_t m, int64_t p,
+                           const double *__restrict__ omega, int count, Cx<T> *__restrict__ b) {
+    const int64_t total = m * p;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total * count;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int f = (int)(t / total);
+        const int64_t e = t % total, i = e % m, q = e / m;
+        const double r = R[i + (m + q) * ld], l = L[i + (m + q) * ld];
+        b[t] = Cx<T>{(T)r, (T)(omega[f] * l)};
+    }
+}
+
+// r = b - (R + j w L) x for 8 frequencies per block row; b = Z_ep column q.
+constexpr int kResF = 8;
+__global__ void __launch_bounds__(128) residual_kernel(const double *__restrict__ R, const double *__restrict__ L,
+                                                       int64_t ld, int64_t m, int64_t p, const double *__restrict__ omega,
+                                                       int count, const Cx<double> *__restrict__ x,
+                                                       Cx<double> *__restrict__ r) {
+    __shared__ Cx<double> xs[64][kResF];
+    const int fg = blockIdx.y / (int)p, q = blockIdx.y % (int)p;
+    const int f0 = fg * kResF;
+    const int nf = min(kResF, count - f0);
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double sr_re[kResF], sr_im[kResF], sl_re[kResF], sl_im[kResF];
+#pragma unroll
+    for (int f = 0; f < kResF; ++f) sr_re[f] = sr_im[f] = sl_re[f] = sl_im[f] = 0.0;
+    for (int64_t c0 = 0; c0 < m; c0 += 64) {
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < 64 * kResF; idx += blockDim.x) {
+            int cc = idx % 64, f = idx / 64;
+            int64_t c = c0 + cc;
+            xs[cc][f] = (c < m && f < nf) ? x[((int64_t)(f0 + f) * p + q) * m + c] : Cx<double>{0.0, 0.0};
+        }
+        __syncthreads();
+        if (i < m) {
+            const int cmax = (int)min((int64_t)64, m - c0);
+            for (int cc = 0; cc < cmax; ++cc) {
+                const double rv = R[i + (c0 + cc) * ld], lv = L[i + (c0 + cc) * ld];
+#pragma unroll
+                for (int f = 0; f < kResF; ++f) {
+                    const Cx<double> xv = xs[cc][f];
+                    sr_re[f] += rv * xv.re;
+                    sr_im[f] += rv * xv.im;
+                    sl_re[f] += lv * xv.re;
+                    sl_im[f] += lv * xv.im;
+                }
+            }
+        }
+    }
+    if (i < m) {
+        const double br = R[i + (m + q) * ld], bl = L[i + (m + q) * ld];
+        for (int f = 0; f < nf; ++f) {
+            const double w = omega[f0 + f];
+            // (R + jwL) x = R x + j w (L x)
+            const double ax_re = sr_re[f] - w * sl_im[f];
+            const double ax_im = sr_im[f] + w * sl_re[f];
+            r[((int64_t)(f0 + f) * p + q) * m + i] = Cx<double>{br - ax_re, w * bl - ax_im};
+        }
+    }
+}
+
+// Z_f[i][j] = pp[i][j] - sum_k ep[k][i] x_f[k][j]; one block per (f, i, j).
+__global__ void __launch_bounds__(256) schur_kernel(const double *__restrict__ R, const double *__restrict__ L,
+                                                    int64_t ld, int64_t m, int64_t p, const double *__restrict__ omega,
+                                                    const Cx<double> *__restrict__ x, Cx<double> *__restrict__ z) {
+    const int64_t g = blockIdx.x;
+    const int f = (int)(g / (p * p));
+    const int64_t ij = g % (p * p), i = ij / p, j = ij % p;
+    const double w = omega[f];
+    double sre = 0.0, sim = 0.0;
+    const Cx<double> *X = x + ((int64_t)f * p + j) * m;
+    for (int64_t k = threadIdx.x; k < m; k += blockDim.x) {
+        const double er = R[k + (m + i) * ld], el = w * L[k + (m + i) * ld];
+        const Cx<double> xv = X[k];
+        sre += er * xv.re - el * xv.im;
+        sim += er * xv.im + el * xv.re;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sre += __shfl_down_sync(0xffffffffu, sre, o);
+        sim += __shfl_down_sync(0xffffffffu, sim, o);
+    }
+    __shared__ double s1[8], s2[8];
+    if ((threadIdx.x & 31) == 0) {
+        s1[threadIdx.x >> 5] = sre;
+        s2[threadIdx.x >> 5] = sim;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            a += s1[k];
+            b += s2[k];
+        }
+        const double pr = R[(m + i) + (m + j) * ld], pl = w * L[(m + i) + (m + j) * ld];
+        Cx<double> out{pr - a, pl - b};
+        if (w == 0.0) out.im = 0.0;  // DC: the real resistive network (solve.rs:811-815)
+        z[((int64_t)f * p + i) * p + j] = out;
+    }
+}
+
+__global__ void c64_to_c32_kernel(const double *__restrict__ s, float *__restrict__ d, int64_t n) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * n; t += (int64_t)gridDim.x * blockDim.x)
+        d[t] = (float)s[t];
+}
+__global__ void add_c32_kernel(double *__restrict__ x, const float *__restrict__ d, int64_t n) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * n; t += (int64_t)gridDim.x * blockDim.x)
+        x[t] += (double)d[t];
+}
+template <class T>
+__global__ void max_abs_kernel(const T *__restrict__ v, int64_t per, double *__restrict__ out) {
+    const T *V = v + (int64_t)blockIdx.x * per;
+    double mx = 0.0;
+    for (int64_t t = threadIdx.x; t < per; t += blockDim.x) mx = fmax(mx, (double)fabs(V[t]));
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    __shared__ double s[32];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) mx = fmax(mx, s[k]);
+        out[blockIdx.x] = mx;
+    }
+}
+
+inline int grid_for(int64_t work, int threads, int cap = 148 * 32) {
+    int64_t g = (work + threads - 1) / threads;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(g, cap));
+}
+
+}  // namespace
+
+template <class T>
+fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaStream_t s, fh_error_info *err) {
+    using C = Cx<T>;
+    C *a = reinterpret_cast<C *>(b.a);
+    const int64_t m = b.m;
+    if (m == 0 || b.count == 0) return FH_OK;
+    if (nb > 64 || nb < 1) return fail(err, FH_ERR_INVALID_ARGUMENT, "panel width must be in 1..64");
+    const size_t trsm_smem = sizeof(C) * (size_t)nb * (nb + 64);
+    const size_t gemm_smem = sizeof(C) * (size_t)nb * 128;
+    FHB_CUDA(cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
+    FHB_CUDA(cudaFuncSetAttribute(gemm_update_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem));
+    for (int64_t k0 = 0; k0 < m; k0 += nb) {
+        const int w_nb = (int)std::min<int64_t>(nb, m - k0);
+        for (int c = 0; c < w_nb; ++c) {
+            const int j = (int)(k0 + c);
+            const int chunks = std::min(w.max_chunks, (int)((m - j + 1023) / 1024));
+            pivot_kernel<T><<<dim3(chunks, b.count), 256, 0, s>>>(a, m, j, (int)k0, w_nb, b.pivots, b.singular,
+                                                                  w.partial_val, w.partial_idx, w.tickets, chunks);
+            if (j + 1 < m) {
+                const int ublocks = (int)std::max<int64_t>(1, std::min<int64_t>((m - j - 1 + 255) / 256, 64));
+                panel_update_kernel<T><<<dim3(ublocks, b.count), 256, 0, s>>>(a, m, j, (int)k0, w_nb);
+            }
+        }
+        const int64_t c0 = k0 + w_nb;
+        if (c0 >= m) break;
+        const int64_t ncols = m - c0;
+        swap_kernel<T><<<dim3(grid_for(ncols, 256, 1024), b.count), 256, 0, s>>>(a, m, (int)k0, w_nb, c0, b.pivots);
+        trsm_kernel<T><<<dim3((unsigned)((ncols + 63) / 64), b.count), 64, trsm_smem, s>>>(a, m, (int)k0, w_nb);
+        if (mode == TrailingUpdate::TensorBf16x3 && sizeof(T) == 4 && w_nb == nb) {
+            fh_status st = gemm_tc_update(reinterpret_cast<float *>(b.a), m, b.count, k0, nb, s, err);
+            if (st) return st;
+        } else {
+            const unsigned tiles = (unsigned)((ncols + 63) / 64);
+            gemm_update_kernel<T><<<dim3(tiles, tiles, b.count), 256, gemm_smem, s>>>(a, m, (int)k0, w_nb);
+        }
+        FHB_CUDA(cudaGetLastError());
+    }
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+template <class T>
+fh_status lu_solve(const LuBatch<T> &b, T *xv, int nrhs, int nb, cudaStream_t s, fh_error_info *err) {
+    using C = Cx<T>;
+    const C *a = reinterpret_cast<const C *>(b.a);
+    C *x = reinterpret_cast<C *>(xv);
+    const int64_t m = b.m;
+    if (m == 0) return FH_OK;
+    const int groups = b.count * nrhs;
+    for (int64_t k0 = 0; k0 < m; k0 += nb) {
+        const int w_nb = (int)std::min<int64_t>(nb, m - k0);
+        fwd_panel_kernel<T><<<groups, 64, 0, s>>>(a, m, nrhs, (int)k0, w_nb, b.pivots, x);
+        if (k0 + w_nb < m)
+            gemv_update_kernel<T><<<dim3(grid_for(m - k0 - w_nb, 256, 64), groups), 256, 0, s>>>(
+                a, m, nrhs, (int)k0, w_nb, k0 + w_nb, m, x);
+    }
+    const int64_t last = ((m - 1) / nb) * nb;
+    for (int64_t k0 = last; k0 >= 0; k0 -= nb) {
+        const int w_nb = (int)std::min<int64_t>(nb, m - k0);
+        bwd_panel_kernel2<T><<<groups, 64, 0, s>>>(a, m, nrhs, (int)k0, w_nb, x);
+        if (k0 > 0)
+            gemv_update_kernel<T><<<dim3(grid_for(k0, 256, 64), groups), 256, 0, s>>>(a, m, nrhs, (int)k0, w_nb, 0,
+                                                                                      k0, x);
+    }
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+template <class T>
+fh_status form_system(const double *Rm, const double *Lm, int64_t ld, int64_t m, const double *omega, int count, T *a,
+                      cudaStream_t s, fh_error_info *err) {
+    if (m == 0) return FH_OK;
+    form_kernel<T><<<grid_for(m * m, 256, 148 * 16), 256, 0, s>>>(Rm, Lm, ld, m, omega, count,
+                                                                   reinterpret_cast<Cx<T> *>(a));
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+template <class T>
+fh_status form_rhs(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega, int count,
+                   T *b, cudaStream_t s, fh_error_info *err) {
+    if (m == 0 || p == 0) return FH_OK;
+    rhs_kernel<T><<<grid_for(m * p * count, 256), 256, 0, s>>>(Rm, Lm, ld, m, p, omega, count,
+                                                               reinterpret_cast<Cx<T> *>(b));
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+fh_status residual_fp64(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega,
+                        int count, const double *x, double *r, double *rnorm, cudaStream_t s, fh_error_info *err) {
+    if (m == 0) return FH_OK;
+    const int fgroups = (count + kResF - 1) / kResF;
+    residual_kernel<<<dim3((unsigned)((m + 127) / 128), (unsigned)(fgroups * p)), 128, 0, s>>>(
+        Rm, Lm, ld, m, p, omega, count, reinterpret_cast<const Cx<double> *>(x), reinterpret_cast<Cx<double> *>(r));
+    FHB_CUDA(cudaGetLastError());
+    if (rnorm) {
+        max_abs_kernel<double><<<count, 256, 0, s>>>(r, 2 * m * p, rnorm);
+        FHB_CUDA(cudaGetLastError());
+    }
+    return FH_OK;
+}
+
+fh_status schur(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega, int count,
+                const double *x, double *z, cudaStream_t s, fh_error_info *err) {
+    if (p == 0 || count == 0) return FH_OK;
+    schur_kernel<<<(unsigned)(count * p * p), 256, 0, s>>>(Rm, Lm, ld, m, p, omega,
+                                                           reinterpret_cast<const Cx<double> *>(x),
+                                                           reinterpret_cast<Cx<double> *>(z));
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+fh_status convert_c64_to_c32(const double *src, float *dst, int64_t n, cudaStream_t s, fh_error_info *err) {
+    if (!n) return FH_OK;
+    c64_to_c32_kernel<<<grid_for(2 * n, 256), 256, 0, s>>>(src, dst, n);
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+fh_status add_c32_to_c64(double *x, const float *d, int64_t n, cudaStream_t s, fh_error_info *err) {
+    if (!n) return FH_OK;
+    add_c32_kernel<<<grid_for(2 * n, 256), 256, 0, s>>>(x, d, n);
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+fh_status max_abs_per_matrix(const double *v, int64_t per, int count, double *out, cudaStream_t s, fh_error_info *err) {
+    if (!count) return FH_OK;
+    max_abs_kernel<double><<<count, 256, 0, s>>>(v, per, out);
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+fh_status max_abs_per_matrix_f32(const float *v, int64_t per, int count, double *out, cudaStream_t s,
+                                 fh_error_info *err) {
+    if (!count) return FH_OK;
+    max_abs_kernel<float><<<count, 256, 0, s>>>(v, per, out);
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+template fh_status lu_factor<double>(LuBatch<double> &, LuWork &, int, TrailingUpdate, cudaStream_t, fh_error_info *);
+template fh_status lu_factor<float>(LuBatch<float> &, LuWork &, int, TrailingUpdate, cudaStream_t, fh_error_info *);
+template fh_status lu_solve<double>(const LuBatch<double> &, double *, int, int, cudaStream_t, fh_error_info *);
+template fh_status lu_solve<float>(const LuBatch<float> &, float *, int, int, cudaStream_t, fh_error_info *);
+template fh_status form_system<double>(const double *, const double *, int64_t, int64_t, const double *, int, double *,
+                                       cudaStream_t, fh_error_info *);
+template fh_status form_system<float>(const double *, const double *, int64_t, int64_t, const double *, int, float *,
+                                      cudaStream_t, fh_error_info *);
+template fh_status form_rhs<double>(const double *, const double *, int64_t, int64_t, int64_t, const double *, int,
+                                    double *, cudaStream_t, fh_error_info *);
+template fh_status form_rhs<float>(const double *, const double *, int64_t, int64_t, int64_t, const double *, int,
+                                   float *, cudaStream_t, fh_error_info *);
+
+}  // namespace fhb

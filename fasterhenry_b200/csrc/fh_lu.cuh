@@ -1,0 +1,71 @@
+// Batched blocked complex LU with partial pivoting (device), its solves, the
+// FP64 residual of R + jwL, and the Schur complement.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fh_device.cuh"
+
+namespace fhb {
+
+// A batch of `count` column-major complex matrices of order m (leading
+// dimension m), stored back to back with stride m*m complex entries.
+// T is double (FP64 form) or float (mixed form).
+template <class T>
+struct LuBatch {
+    T *a = nullptr;          // interleaved complex, count * m * m
+    int *pivots = nullptr;   // count * m: row interchanged with row k
+    int *singular = nullptr; // count flags (zero pivot met)
+    int64_t m = 0;
+    int count = 0;
+};
+
+// Workspace for the factorization (pivot search partials).
+struct LuWork {
+    double *partial_val = nullptr;
+    int *partial_idx = nullptr;
+    unsigned *tickets = nullptr;
+    int max_chunks = 0;
+};
+
+// How the trailing update A22 -= L21 U12 is computed for the FP32 form.
+enum class TrailingUpdate { Simt, TensorBf16x3 };
+
+template <class T>
+fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaStream_t s, fh_error_info *err);
+
+// Solve with the factors in place: x (count x m x nrhs, column-major per
+// matrix, stride m*nrhs) is overwritten.
+template <class T>
+fh_status lu_solve(const LuBatch<T> &b, T *x, int nrhs, int nb, cudaStream_t s, fh_error_info *err);
+
+// A_f = R + j w_f L for the top-left m x m block of R_m, L_m (ld = loops),
+// written as T complex into a (count x m x m).
+template <class T>
+fh_status form_system(const double *Rm, const double *Lm, int64_t ld, int64_t m, const double *omega, int count,
+                      T *a, cudaStream_t s, fh_error_info *err);
+
+// Right-hand sides b_f = Z_ep (m x p) at each frequency, as T complex.
+template <class T>
+fh_status form_rhs(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega,
+                   int count, T *b, cudaStream_t s, fh_error_info *err);
+
+// r_f = b_f - (R_ee + j w_f L_ee) x_f in FP64 for all f at once (one pass
+// over R_ee and L_ee).  x, b, r: count x m x p complex double.  Also returns
+// per-frequency max-norms of r and b through rnorm/bnorm (device, count each).
+fh_status residual_fp64(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega,
+                        int count, const double *x, double *r, double *rnorm, cudaStream_t s, fh_error_info *err);
+
+// Z_f = Z_pp - Z_ep^T X_f (p x p complex, row-major per frequency).
+fh_status schur(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega, int count,
+                const double *x, double *z, cudaStream_t s, fh_error_info *err);
+
+// Elementwise helpers.
+fh_status convert_c64_to_c32(const double *src, float *dst, int64_t n_complex, cudaStream_t s, fh_error_info *err);
+fh_status add_c32_to_c64(double *x, const float *d, int64_t n_complex, cudaStream_t s, fh_error_info *err);
+fh_status max_abs_per_matrix(const double *v, int64_t per_matrix, int count, double *out, cudaStream_t s,
+                             fh_error_info *err);
+fh_status max_abs_per_matrix_f32(const float *v, int64_t per_matrix, int count, double *out, cudaStream_t s,
+                                 fh_error_info *err);
+
+}  // namespace fhb

@@ -1,0 +1,287 @@
+/*
+ * fasterhenry_b200 — C ABI of the B200 (sm_100a) PEEC extraction path.
+ *
+ * The reference (2AMLogic/fasterhenry) is a Rust library; its hot path is the
+ * dense extraction
+ *     geometry -> filaments -> loop basis M -> partial inductance L (fill)
+ *     -> R_m = M R M^T, L_m = M L M^T (congruence)
+ *     -> per frequency: Z(w) = Z_pp - Z_ep^T (R_ee + jwL_ee)^-1 Z_ep  (LU + Schur)
+ * plus the matrix-free pFFT + GMRES alternative.  Each entry point below
+ * names the reference interface it replaces (paths relative to the reference
+ * project root).  A Rust crate binds these with `extern "C"` declarations
+ * (see INTEGRATION.md); the Python package binds them with ctypes.
+ *
+ * Conventions
+ *   - Plain pointers and sizes; all buffers are caller-owned HOST memory
+ *     unless a function says otherwise.  Opaque handles own device memory.
+ *   - SI units: metres, S/m, hertz, ohms, henries.
+ *   - Complex numbers are interleaved (re, im) doubles.
+ *   - Every function returns an fh_status; on failure the optional
+ *     fh_error_info out-struct carries the payload the reference's
+ *     SolveError / KernelError variant would carry, and fh_last_error()
+ *     returns a thread-local message.
+ *   - There is no CPU fallback: without a usable CUDA device every compute
+ *     entry point returns FH_ERR_NO_DEVICE.
+ */
+#ifndef FASTERHENRY_B200_H
+#define FASTERHENRY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FH_ABI_VERSION 1
+
+/* Status codes.  The FH_ERR_* values between 10 and 29 map 1:1 onto the
+ * reference's error variants: SolveError (fasterhenry/src/solve.rs:567-637),
+ * KernelError (fasterhenry/src/inductance/mod.rs:93-115), MeshError
+ * (fasterhenry/src/mesh.rs:94-144), DiscretizeError
+ * (fasterhenry/src/filament.rs:141-190), GeometryError
+ * (fasterhenry/src/geometry.rs:296-324). */
+typedef enum fh_status {
+    FH_OK = 0,
+    FH_ERR_INVALID_ARGUMENT = 1,   /* null pointer, size mismatch (reference: panic) */
+    FH_ERR_NO_DEVICE = 2,          /* no CUDA device / extension unusable */
+    FH_ERR_CUDA = 3,               /* a CUDA runtime call failed */
+    FH_ERR_OUT_OF_MEMORY = 4,      /* device allocation failed */
+    FH_ERR_DEVICE_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+    FH_ERR_GEOMETRY = 10,          /* GeometryError::{NonFiniteNode, DanglingNode, InvalidSegment} */
+    FH_ERR_DISCRETIZE = 11,        /* SolveError::Discretize{segment, source} */
+    FH_ERR_KERNEL_COINCIDENT = 12, /* KernelError::CoincidentSamples{first, second} */
+    FH_ERR_KERNEL_NOT_FINITE = 13, /* KernelError::NotFinite{first, second} */
+    FH_ERR_MESH = 14,              /* SolveError::Mesh(MeshError) */
+    FH_ERR_INVALID_GRADING = 15,   /* SolveError::InvalidGrading */
+    FH_ERR_INVALID_FREQUENCY = 16, /* SolveError::InvalidFrequency{index, value} */
+    FH_ERR_SINGULAR = 17,          /* SolveError::Singular{frequency} */
+    FH_ERR_NOT_CONVERGED = 18,     /* SolveError::NotConverged{frequency, port, iterations, residual};
+                                      also: mixed-precision refinement that did not reach its target */
+    FH_ERR_PFFT = 19,              /* SolveError::Pfft(PfftError) */
+    FH_ERR_INVALID_EXCITATION = 20,/* SolveError::InvalidExcitation */
+    FH_ERR_UNSUPPORTED = 30        /* a path this build does not provide */
+} fh_status;
+
+/* MeshError sub-codes carried in fh_error_info.detail for FH_ERR_MESH. */
+enum {
+    FH_MESH_NO_PORTS = 1,
+    FH_MESH_UNKNOWN_PORT_NODE = 2,
+    FH_MESH_DEGENERATE_PORT = 3,
+    FH_MESH_PORT_NOT_CONNECTED = 4,
+    FH_MESH_SEGMENT_COUNT_MISMATCH = 5,
+    FH_MESH_EMPTY_SEGMENT = 6
+};
+
+/* Payload of a failure (all fields optional / -1 when not applicable). */
+typedef struct fh_error_info {
+    int32_t status;       /* the fh_status returned */
+    int32_t detail;       /* sub-code (MeshError kind, ...) */
+    int64_t index_a;      /* segment / node / first filament / frequency index / port */
+    int64_t index_b;      /* second filament / node */
+    double frequency;     /* Singular / NotConverged / InvalidFrequency value */
+    int64_t iterations;   /* NotConverged */
+    double residual;      /* NotConverged relative residual */
+} fh_error_info;
+
+/* Node, geometry.rs:20-60. */
+typedef struct fh_node {
+    double x, y, z;
+} fh_node;
+
+/* SegmentDef, geometry.rs:226-270: node indices, cross-section, conductivity,
+ * optional width direction (has_width_dir != 0). */
+typedef struct fh_segment_def {
+    int64_t a, b;
+    double width, height, sigma;
+    int64_t has_width_dir;
+    double width_dir[3];
+} fh_segment_def;
+
+/* Port, mesh.rs:67-92: current enters at `positive`, leaves at `negative`. */
+typedef struct fh_port {
+    int64_t positive, negative;
+} fh_port;
+
+/* Filament record, filament.rs:33-139: 19 doubles. */
+typedef struct fh_filament {
+    double start[3], end[3];
+    double length;
+    double dir_length[3], dir_width[3], dir_height[3];
+    double width, height, sigma;
+} fh_filament;
+
+/* Discretization, solve.rs:409-510. */
+typedef enum fh_discretization_kind {
+    FH_DISC_UNIFORM = 0,
+    FH_DISC_PER_SEGMENT = 1,
+    FH_DISC_GRADED = 2,
+    FH_DISC_SKIN_DEPTH = 3,
+    FH_DISC_PER_SEGMENT_GRADED = 4
+} fh_discretization_kind;
+
+typedef struct fh_axis_grading {
+    int64_t nw, nh;
+    double width_ratio, height_ratio;
+} fh_axis_grading;
+
+typedef struct fh_discretization {
+    int64_t kind;                  /* fh_discretization_kind */
+    int64_t nw, nh;                /* UNIFORM / GRADED */
+    double ratio;                  /* GRADED / SKIN_DEPTH */
+    double frequency_hz;           /* SKIN_DEPTH */
+    double target_skin_depths;     /* SKIN_DEPTH */
+    int64_t max_per_axis;          /* SKIN_DEPTH (reference default 32) */
+    const fh_axis_grading *per_segment; /* PER_SEGMENT(_GRADED): one per segment */
+    int64_t per_segment_len;
+} fh_discretization;
+
+/* SolverChoice, solve.rs:169-193; DENSE_PATH_MAX_FILAMENTS = 10000 (solve.rs:133). */
+typedef enum fh_solver_choice {
+    FH_SOLVER_AUTO = 0,
+    FH_SOLVER_DENSE = 1,
+    FH_SOLVER_ITERATIVE = 2
+} fh_solver_choice;
+#define FH_DENSE_PATH_MAX_FILAMENTS 10000
+
+/* How the per-frequency complex LU is computed (no reference counterpart:
+ * the reference always runs the FP64 form). */
+typedef enum fh_precision {
+    FH_PRECISION_FP64 = 0,          /* FP64 blocked LU, partial pivoting (dense.rs) */
+    FH_PRECISION_MIXED_BF16X3 = 1   /* FP32 panels, split-BF16 x3 tensor-core trailing
+                                       updates, FP64-residual iterative refinement */
+} fh_precision;
+
+/* Counts, result.rs:110-126. */
+typedef struct fh_counts {
+    int64_t nodes, segments, filaments, meshes, internal_meshes, ports;
+} fh_counts;
+
+/* Timing, result.rs:129-141, plus device-event phase times. */
+typedef struct fh_timing {
+    double inductance_s;   /* fill */
+    double assembly_s;     /* discretize + mesh + fill + congruence */
+    double solve_s;        /* sweep */
+    double total_s;
+} fh_timing;
+
+/* Per-sweep report; arrays are optional (NULL) and have nf entries. */
+typedef struct fh_sweep_report {
+    int32_t *refinement_iterations;  /* mixed form: iterations per frequency */
+    double *residual;                /* final relative residual ||b - Ax|| / ||b|| per frequency */
+    double solve_s;                  /* device time of the sweep */
+    double factor_s;                 /* device time of the factorizations */
+    double refine_s;                 /* device time of the refinement */
+} fh_sweep_report;
+
+typedef struct fh_system fh_system;
+
+/* ---- library ---------------------------------------------------------- */
+
+/* ABI version and build string. */
+int32_t fh_abi_version(void);
+const char *fh_build_info(void);
+/* Thread-local message for the last failing call on this thread. */
+const char *fh_last_error(void);
+/* Number of usable sm_100 devices (0 when none). */
+int32_t fh_device_count(void);
+
+/* ---- host model (no device use) --------------------------------------- */
+
+/* Discretize a geometry into filaments.  Replaces discretize_geometry
+ * (fasterhenry/src/solve.rs:947-978) over discretize (filament.rs:320) /
+ * discretize_graded_per_axis (filament.rs:478).  Call with filaments == NULL
+ * to get *n_filaments; per_segment (optional, nseg entries) gets the bundle
+ * sizes. */
+fh_status fh_discretize(const fh_node *nodes, size_t n_nodes, const fh_segment_def *segments,
+                        size_t n_segments, const fh_discretization *disc, fh_filament *filaments,
+                        size_t capacity, size_t *n_filaments, int64_t *per_segment,
+                        fh_error_info *err);
+
+/* Loop basis as CSR rows of (branch, sign).  Replaces MeshMatrix::build
+ * (fasterhenry/src/mesh.rs:170-263).  Call with row_ptr == NULL to size. */
+fh_status fh_mesh_build(const fh_segment_def *segments, size_t n_segments, size_t n_nodes,
+                        const int64_t *per_segment, const fh_port *ports, size_t n_ports,
+                        int64_t *row_ptr, int64_t *branch, double *sign, size_t cap_rows,
+                        size_t cap_nnz, size_t *n_rows, size_t *nnz, size_t *n_internal,
+                        fh_error_info *err);
+
+/* SolverChoice::resolve (solve.rs:181-190): 0 dense, 1 iterative. */
+int32_t fh_solver_resolve(fh_solver_choice choice, size_t filaments);
+
+/* ---- GPU kernels exposed as library calls ----------------------------- */
+
+/* Symmetric n x n partial-inductance matrix, column-major, on cuda:0.
+ * Replaces partial_inductance_matrix (fasterhenry/src/inductance/batch.rs:246).
+ * `methods` (optional, n*n int8) receives the inductance::Method per entry
+ * (0 Orthogonal, 1 BarClosedForm, 2 AlignedQuadrature, 3 PointQuadrature,
+ * 4 SampledFilaments). */
+fh_status fh_partial_inductance_matrix(const fh_filament *filaments, size_t n, double *L,
+                                       int8_t *methods, fh_error_info *err);
+
+/* Solve a x = b for complex a (n x n, column-major) and b (n x nrhs,
+ * column-major) with the device FP64 blocked LU (partial pivoting).
+ * Replaces dense::lu_solve (fasterhenry/src/dense.rs:43).  x may alias b. */
+fh_status fh_lu_solve_c64(const double *a, size_t n, const double *b, size_t nrhs, double *x,
+                          fh_error_info *err);
+
+/* ---- the dense system (MeshSystem) ------------------------------------ */
+
+/* Assemble: discretize, loop basis, fill L on the device, congruence
+ * R_m = M R M^T, L_m = M L M^T kept resident in HBM.  Replaces
+ * MeshSystem::assemble (fasterhenry/src/solve.rs:680-766).  `choice` is
+ * resolved with fh_solver_resolve; FH_SOLVER_ITERATIVE returns
+ * FH_ERR_UNSUPPORTED in this build. */
+fh_status fh_system_create(const fh_node *nodes, size_t n_nodes, const fh_segment_def *segments,
+                           size_t n_segments, const fh_port *ports, size_t n_ports,
+                           const fh_discretization *disc, fh_solver_choice choice,
+                           fh_system **out, fh_error_info *err);
+
+void fh_system_destroy(fh_system *sys);
+
+fh_status fh_system_counts(const fh_system *sys, fh_counts *counts);
+fh_status fh_system_timing(const fh_system *sys, fh_timing *timing);
+
+/* Host copies of the assembled data (MeshSystem::filaments, ::filament_resistances). */
+fh_status fh_system_filaments(const fh_system *sys, fh_filament *out, size_t capacity);
+fh_status fh_system_resistances(const fh_system *sys, double *out, size_t capacity);
+/* R_m and L_m as full (meshes x meshes) column-major host matrices. */
+fh_status fh_system_mesh_matrices(const fh_system *sys, double *r_mesh, double *l_mesh);
+/* Device pointer of L_m (meshes x meshes, column-major, FP64); valid until destroy. */
+fh_status fh_system_device_l_mesh(const fh_system *sys, const double **l_mesh, const double **r_mesh);
+
+/* Z(w) at every frequency: z_out is nf x p x p complex (interleaved), row-major
+ * per frequency like SweepResult.impedance_ohm[k][i][j] (result.rs:47-66).
+ * Replaces MeshSystem::sweep (solve.rs:881-893) / sweep_impedances
+ * (solve.rs:1039-1079): frequencies are validated first (InvalidFrequency
+ * names the first bad index), and the first failing frequency in list order
+ * is reported.  All frequencies are factorized in batched launches. */
+fh_status fh_sweep(fh_system *sys, const double *frequencies_hz, size_t nf, fh_precision precision,
+                   double *z_out, fh_sweep_report *report, fh_error_info *err);
+
+/* One frequency (MeshSystem::impedance, solve.rs:806-830). */
+fh_status fh_impedance(fh_system *sys, double frequency_hz, fh_precision precision, double *z_out,
+                       fh_error_info *err);
+
+/* ---- outputs (host) ---------------------------------------------------- */
+
+/* SweepResult JSON (result.rs:1-40, schema_version 1).  port_names may be NULL.
+ * Writes at most `capacity` bytes (NUL-terminated) and sets *length to the
+ * full length; call with buf == NULL to size. */
+fh_status fh_sweep_json(const fh_port *ports, const char *const *port_names, size_t n_ports,
+                        const double *frequencies_hz, size_t nf, const double *z,
+                        const fh_counts *counts, const fh_timing *timing, char *buf,
+                        size_t capacity, size_t *length);
+
+/* MAT v4 Zc.mat (fasterhenry-cli/src/mat.rs:31-100) written to `path`. */
+fh_status fh_write_zc_mat(const char *path, size_t n_ports, const double *frequencies_hz, size_t nf,
+                          const double *z);
+
+/* SPICE subcircuit at frequency index k (fasterhenry-cli/src/spice.rs:64-135). */
+fh_status fh_spice_subckt(size_t n_ports, const double *frequencies_hz, size_t nf, const double *z,
+                          size_t k, const char *name, char *buf, size_t capacity, size_t *length);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FASTERHENRY_B200_H */

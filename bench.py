@@ -1,0 +1,345 @@
+"""Benchmark of the Z(w) sweep at 10,020 filaments x 32 frequencies.
+
+Workload (the metric's configuration): the 167-leg meander — 1 mm legs at
+40 um pitch, 20 um x 5 um copper, 10 x 3 filaments per segment — giving
+10,020 filaments and 9,686 internal loops; 32 log-spaced frequencies from
+1e5 to 1e10 Hz.  Synthetic geometry built in code (no dataset).
+
+A step is one Z(w) sweep of the assembled system (MeshSystem.sweep: all 32
+complex factorizations, solves, refinement and Schur complements) in the
+mixed form (FP32 factors with split-BF16 x3 tensor-core trailing updates and
+FP64-residual iterative refinement).  The FP64 form of the same sweep is
+timed alongside it, and the error of every mixed Z entry against the FP64
+form is reported.  Inputs (R_m, L_m: 1.5 GB) are resident in HBM and every
+factorization streams 24 GB, far larger than the 126 MB L2, so no flush is
+needed between steps.
+
+``e2e`` is ``solve()`` through the C ABI from host geometry to host Z:
+discretization, fill, congruence, sweep and the device-to-host copy.
+
+``--impl reference`` times the CPU oracle (a C++ restatement of the
+reference's Rust path; the Rust reference cannot be built here) on a bounded
+sample: one frequency's FP64 LU + Schur of a leading block of the same
+system, extrapolated to the full sweep by (m / m_sample)^3 x 32.
+
+Multi-GPU (torchrun, N ranks): replicas only — every rank sweeps its own
+copy of the workload (frequencies and geometries are independent; nothing is
+exchanged), timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Z(ω) sweep s at 10k filaments×32 freqs: mixed+IR vs FP64 LU at ≤1e-9 rel"
+UNIT = "s"
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return p, "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def init_dist(world: int, local: int):
+    if world <= 1:
+        return
+    import datetime
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+
+def run_ours(args):
+    import ctypes
+    rank, world, local = dist_env()
+    init_dist(world, local)
+    import torch
+    torch.cuda.set_device(local)
+    import fasterhenry_b200 as fh
+    from fasterhenry_b200 import fixtures as F
+    from fasterhenry_b200 import _native as N
+
+    deck, freqs = F.metric_meander()
+    geometry = fh.Geometry.from_deck(deck)
+    system = fh.MeshSystem.assemble(geometry, deck.ports, deck.discretization)
+    counts = system.counts()
+    fill = fh.fill_stats(system)
+    assembly = system.timing()
+    # FP64 form (the plain form) once for the error reference and its time.
+    torch.cuda.synchronize()
+    r64 = system.sweep(freqs, fh.Precision.FP64)
+    r64 = system.sweep(freqs, fh.Precision.FP64)
+    lib = N.load()
+
+    def sweep_device_s(precision):
+        f = np.ascontiguousarray(freqs, dtype=np.float64)
+        p = counts["ports"]
+        z = np.zeros((len(f), p, p), dtype=np.complex128)
+        it = np.zeros(len(f), dtype=np.int32)
+        rs = np.zeros(len(f))
+        rep = N.SweepReport(it.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), rs.ctypes.data_as(N.c_double_p))
+        info = N.ErrorInfo()
+        st = lib.fh_sweep(system._h, f.ctypes.data_as(N.c_double_p), len(f), int(precision),
+                          z.ctypes.data_as(N.c_double_p), ctypes.byref(rep), ctypes.byref(info))
+        if st:
+            raise RuntimeError("sweep failed: %s" % N.last_error())
+        return rep.solve_s, z, it, rs
+
+    fp64_s = [sweep_device_s(fh.Precision.FP64)[0] for _ in range(2)]
+    fp64_time = min(fp64_s)
+    for _ in range(args.warmup):
+        sweep_device_s(fh.Precision.MIXED_BF16X3)
+    torch.cuda.synchronize()
+    barrier(world)
+    times = []
+    zs = None
+    with ClockSampler(local) as clocks, fh.Profiler() as prof:
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            t, zs, iters, resid = sweep_device_s(fh.Precision.MIXED_BF16X3)
+            times.append(t)
+        torch.cuda.synchronize()
+        profile = prof.read()
+    barrier(world)
+    step_s = sum(times) / len(times)
+    step_max = max_over_ranks(step_s, world)
+    z64 = r64.impedance_ohm
+    rel = [float(np.max(np.abs(zs[k] - z64[k])) / np.max(np.abs(z64[k]))) for k in range(len(freqs))]
+
+    # e2e: solve() through the C ABI from host geometry to host Z.
+    e2e_times = []
+    for _ in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = fh.solve(geometry, deck.ports, deck.discretization, freqs, fh.Precision.MIXED_BF16X3)
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(statistics.median(e2e_times), world)
+    h2d = counts["filaments"] * 256 + counts["filaments"] * 8 + len(freqs) * 8 + (2 * counts["filaments"]) * 12
+    d2h = len(freqs) * counts["ports"] ** 2 * 16
+
+    peaks, peak_kind = _peaks()
+    # Roofline of the dominant kernel: the trailing-update GEMM.
+    gemm_cls = "gemm_tc" if profile["gemm_tc"]["launches"] else "gemm_fp32"
+    g = profile[gemm_cls]
+    gemm_launches = max(1, g["launches"])
+    per_launch_ms = g["ms"] / gemm_launches
+    if gemm_cls == "gemm_tc":
+        # bf16 tensor flops actually required: three split products per real product
+        achieved = 3.0 * g["work"] / (g["ms"] * 1e-3) / 1e12
+        peak = peaks.get("bf16_tflops", 1590.0)
+        unit = "TFLOP/s"
+        bound = "tensor"
+    else:
+        achieved = g["work"] / (g["ms"] * 1e-3) / 1e12 if g["ms"] else 0.0
+        peak = 80.0  # FP32 SIMT nominal (no measured figure)
+        unit = "TFLOP/s"
+        bound = "fp32-simt"
+    roofline = {"kernel": gemm_cls, "bound": bound, "achieved": round(achieved, 2), "peak": peak,
+                "unit": unit, "frac": round(achieved / peak, 4) if peak else None,
+                "peak_source": peak_kind if gemm_cls == "gemm_tc" else "nominal",
+                "traffic": None, "per_launch_ms": round(per_launch_ms, 4), "launches": g["launches"]}
+    launches = sum(v["launches"] for v in profile.values())
+
+    out = {
+        "metric": METRIC, "value": round(step_max, 6), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(step_max * 1e3, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64+bf16x3 (FP64 residual)", "data": "synthetic",
+        "config": {"workload": "meander 167 legs, 10,020 filaments, m = 9,686, 32 freqs 1e5-1e10 Hz",
+                   "filaments": counts["filaments"], "internal_meshes": counts["internal_meshes"],
+                   "frequencies": len(freqs), "precision": "mixed_bf16x3_ir", "l2": "inputs 24 GB >> L2 (no flush)",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "fp64_sweep_s": round(fp64_time, 6), "speedup_vs_fp64": round(fp64_time / step_max, 3),
+        "max_rel_err_vs_fp64": max(rel), "rel_err_per_freq": rel,
+        "refinement_iterations": [int(x) for x in iters], "fill": fill, "assembly": assembly,
+        "e2e": {"value": round(e2e_s, 6), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "what": "solve(): discretize + fill + congruence + mixed sweep + D2H of Z, via the C ABI"},
+        "roofline": roofline, "profile": profile, "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(args, budget_s=args.cpu_budget)
+    if rank == 0:
+        print(json.dumps(out))
+    system.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline(args, budget_s: float = 20.0):
+    """The oracle on a bounded sample (see the module docstring)."""
+    from oracle import oracle as O
+    from fasterhenry_b200 import fixtures as F
+    threads = os.cpu_count() or 1
+    deck, freqs = F.metric_meander()
+    t0 = time.perf_counter()
+    # Assemble a reduced leading system: the first legs of the same meander.
+    sample_legs = 40
+    sub = F.meander_legs(sample_legs)
+    s = O.System(sub, threads=threads)
+    assemble_s = time.perf_counter() - t0
+    m_sub = s.counts["internal_meshes"]
+    t1 = time.perf_counter()
+    s.impedance(freqs[len(freqs) // 2])
+    one = time.perf_counter() - t1
+    m_full = 9686
+    estimate = one * (m_full / m_sub) ** 3 * len(freqs)
+    return {"value": round(estimate, 3), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "oracle FP64 LU+Schur at one frequency of the 40-leg meander (m = %d), %.2f s, "
+                      "scaled by (9686/%d)^3 x 32 frequencies" % (m_sub, one, m_sub),
+            "sample_assemble_s": round(assemble_s, 3)}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from fasterhenry_b200 import fixtures as F
+    threads = os.cpu_count() or 1
+    deck, freqs = F.metric_meander()
+    # Leading block of the metric system sized for a bounded step.
+    sub = F.meander_legs(args.ref_legs)
+    s = O.System(sub, threads=threads)
+    m_sub = s.counts["internal_meshes"]
+    m_full = 9686
+    f_mid = freqs[len(freqs) // 2]
+    for _ in range(args.warmup):
+        s.impedance(f_mid)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        s.impedance(f_mid)
+        times.append(time.perf_counter() - t0)
+    one = statistics.median(times)
+    value = one * (m_full / m_sub) ** 3 * len(freqs)
+    sample = ("oracle (C++ restatement of the reference's Rust dense path) FP64 LU+Schur at one frequency of the "
+              "%d-leg meander (m = %d) per step, %.3f s, scaled by (9686/%d)^3 x 32 frequencies" %
+              (args.ref_legs, m_sub, one, m_sub))
+    out = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(one * 1e3, 3),
+           "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+           "config": {"workload": "meander 167 legs, 10,020 filaments, m = 9,686, 32 freqs 1e5-1e10 Hz",
+                      "precision": "fp64"},
+           "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "port",
+                            "sample": sample},
+           "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--ref-legs", type=int, default=40, help="meander legs of the reference arm's sample")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -11,5 +11,6 @@ from .api import (DENSE_PATH_MAX_FILAMENTS, MU0, CoincidentSamples, DiscretizeEr
                   SegmentDef, Singular, SolverChoice, SweepResult, Unsupported, build_info, device_count, discretize,
                   lu_solve, mesh_matrix, mutual_inductance, partial_inductance_matrix, self_inductance, skin_depth,
                   solve)
+from .api import Profiler, fill_stats
 
 __version__ = "0.1.0"

@@ -93,8 +93,18 @@ EXPORTS = [
     "fh_solver_resolve", "fh_partial_inductance_matrix", "fh_lu_solve_c64", "fh_system_create", "fh_system_destroy",
     "fh_system_counts", "fh_system_timing", "fh_system_filaments", "fh_system_resistances",
     "fh_system_mesh_matrices", "fh_system_device_l_mesh", "fh_sweep", "fh_impedance", "fh_sweep_json",
-    "fh_write_zc_mat", "fh_spice_subckt",
+    "fh_write_zc_mat", "fh_spice_subckt", "fh_system_fill_stats", "fh_profile_enable", "fh_profile_reset",
+    "fh_profile_read",
 ]
+
+PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual"]
+
+
+class FillStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in ("pairs", "orthogonal", "point_quadrature", "closed_form",
+                                              "aligned_quadrature", "sampled", "distinct_aligned_keys")] + \
+               [(k, ctypes.c_double) for k in ("point_evaluations", "ms_classify", "ms_point", "ms_closed_form",
+                                               "ms_aligned_quadrature", "ms_sampled", "ms_congruence")]
 
 _lib = None
 
@@ -138,10 +148,13 @@ def load():
                                 ctypes.c_char_p, sz, P(sz)]
     L.fh_write_zc_mat.argtypes = [ctypes.c_char_p, sz, c_double_p, sz, c_double_p]
     L.fh_spice_subckt.argtypes = [sz, c_double_p, sz, c_double_p, sz, ctypes.c_char_p, ctypes.c_char_p, sz, P(sz)]
-    for name in EXPORTS:
-        fn = getattr(L, name)
-        if fn.restype is ctypes.c_int:  # default
-            fn.restype = ctypes.c_int
+    L.fh_test_trailing_update.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_int64, ctypes.c_int32,
+                                          ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ei]
+    L.fh_system_fill_stats.argtypes = [ctypes.c_void_p, P(FillStats)]
+    L.fh_profile_enable.argtypes = [ctypes.c_int32]
+    L.fh_profile_enable.restype = None
+    L.fh_profile_reset.restype = None
+    L.fh_profile_read.argtypes = [ctypes.c_int32, c_int64_p, c_double_p, c_double_p]
     _lib = L
     return L
 

@@ -304,6 +304,7 @@ class Precision(enum.IntEnum):
     split-BF16 x3 tensor-core trailing updates and FP64-residual refinement."""
     FP64 = 0
     MIXED_BF16X3 = 1
+    MIXED_FP32 = 2
 
 
 # ---------------------------------------------------------------------------
@@ -375,9 +376,9 @@ def lu_solve(a: np.ndarray, b: np.ndarray) -> np.ndarray:
         raise InvalidArgument("lu_solve: the matrix must be square")
     bb = np.asarray(b, dtype=np.complex128)
     vec = bb.ndim == 1
-    bb = bb.reshape(a.shape[0], -1)
-    if bb.shape[0] != a.shape[0]:
+    if bb.ndim == 0 or bb.shape[0] != a.shape[0]:
         raise InvalidArgument("lu_solve: right-hand side has the wrong number of rows")
+    bb = bb.reshape(a.shape[0], -1)
     af = np.asfortranarray(a)
     bf = np.asfortranarray(bb)
     x = np.zeros_like(bf, order="F")
@@ -583,3 +584,34 @@ def device_count() -> int:
 
 def build_info() -> str:
     return N.load().fh_build_info().decode()
+
+
+def fill_stats(system: "MeshSystem") -> Dict[str, float]:
+    """Pairs per method and device time per fill kernel of an assembled system."""
+    s = N.FillStats()
+    _check(N.load().fh_system_fill_stats(system._h, ctypes.byref(s)))
+    return {k: (int(getattr(s, k)) if t is ctypes.c_int64 else float(getattr(s, k))) for k, t in N.FillStats._fields_}
+
+
+class Profiler:
+    """Device-event profile of the extraction kernels (per kernel class:
+    launches, milliseconds, algorithmic flops)."""
+
+    def __enter__(self):
+        L = N.load()
+        L.fh_profile_reset()
+        L.fh_profile_enable(1)
+        return self
+
+    def __exit__(self, *exc):
+        N.load().fh_profile_enable(0)
+
+    @staticmethod
+    def read() -> Dict[str, Dict[str, float]]:
+        L = N.load()
+        out = {}
+        for i, name in enumerate(N.PROFILE_CLASSES):
+            launches, ms, work = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+            _check(L.fh_profile_read(i, ctypes.byref(launches), ctypes.byref(ms), ctypes.byref(work)))
+            out[name] = {"launches": int(launches.value), "ms": float(ms.value), "work": float(work.value)}
+        return out

@@ -48,6 +48,13 @@ void host_quad_tables(QuadTables &t);
 
 fh_status ensure_device(fh_error_info *err);
 
+// Device-event profiler of kernel classes (enabled through fh_profile_enable).
+// prof_begin/prof_end bracket one launch on `s`; `work` is its algorithmic
+// flop (or byte) count.
+bool prof_on();
+void prof_begin(cudaStream_t s, int cls);
+void prof_end(cudaStream_t s, int cls, double work);
+
 // Fill the n x n column-major L on the device (d_L must be zero-filled by the
 // caller).  `d_methods` optional (n*n int8).  `stream` orders the work.
 struct FillStats {

@@ -1,12 +1,379 @@
-// Tensor-core trailing update for the FP32 LU (placeholder until the
-// tcgen05 kernel lands): reports FH_ERR_UNSUPPORTED so that no caller can
-// mistake the SIMT path for it.
+// Trailing update of the FP32 complex LU on the 5th-generation tensor cores:
+//
+//     A22 -= L21 * U12        (complex, FP32 storage, FP32 accumulation)
+//
+// with every FP32 operand split into two BF16 terms, x = x_hi + x_lo
+// (x_hi = bf16(x), x_lo = bf16(x - x_hi)), and each real product formed from
+// three BF16 products (hi*hi + hi*lo + lo*hi; the lo*lo term is below the
+// FP32 rounding of the sum).  The complex product is four real products:
+//
+//     Re += Ar Br - Ai Bi        Im += Ar Bi + Ai Br
+//
+// so one 16-wide complex k-chunk is 12 tcgen05.mma (kind::f16, BF16 inputs,
+// FP32 accumulators in TMEM); the minus sign of Ai Bi is the instruction
+// descriptor's A-negate bit.
+//
+// CTA tile: 128 rows x 128 columns of complex C; two accumulators of 128 TMEM
+// columns (Re at column 0, Im at column 128).  All 256 threads load the
+// chunk's FP32 operands from global memory, split them, and store them to
+// shared memory in the canonical K-major no-swizzle layout (8 x 16-byte core
+// matrices); thread 0 issues the MMAs and commits them to an mbarrier; chunks
+// are double-buffered so the loads of chunk c+1 overlap the MMAs of chunk c.
+// The epilogue reads the accumulators with tcgen05.ld (warp w owns TMEM lanes
+// 32 (w % 4) .. +31 = rows of the tile, and half w / 4 of the columns) and
+// applies C -= acc with coalesced loads and stores, 16 independent loads in
+// flight per thread.  The update is bound by the read + write of C (16 bytes
+// per complex entry per panel); two CTAs per SM keep enough bytes in flight.
+// Every mbarrier wait is bounded; a wait that runs out sets the error flag,
+// skips the epilogue and still frees the TMEM.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
 #include "fh_lu.cuh"
 
 namespace fhb {
 
-fh_status gemm_tc_update(float *, int64_t, int, int64_t, int, cudaStream_t, fh_error_info *err) {
-    return fail(err, FH_ERR_UNSUPPORTED, "tensor-core trailing update not built");
+namespace {
+
+constexpr int kTileM = 128;
+constexpr int kTileN = 128;
+constexpr int kChunk = 16;                                  // complex k per chunk = one MMA K-step
+constexpr int kTileBytes = kTileM * kChunk * 2;             // one bf16 operand tile: 4 KB
+constexpr int kTilesPerChunk = 8;                           // Ar/Ai hi/lo, Br/Bi hi/lo
+constexpr int kBufBytes = kTileBytes * kTilesPerChunk;      // 32 KB
+// Two 32 KB buffers + alignment + barriers, padded to 100 KB so that at most
+// two CTAs (2 x 256 TMEM columns = all 512) are resident per SM.  The padding
+// also keeps every address a descriptor could form inside the allocation.
+constexpr int kSmemBytes = 100 * 1024;
+constexpr int kTmemCols = 256;
+constexpr long long kSpinLimit = 1LL << 22;
+
+// Operand tile order inside a buffer.
+enum { ArH = 0, ArL, AiH, AiL, BrH, BrL, BiH, BiL };
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// SM100 shared-memory matrix descriptor, K-major, no swizzle.
+// start>>4 at [0,14), LBO>>4 at [16,30), SBO>>4 at [32,46), version 1 at [46,48).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// Instruction descriptor: kind::f16, BF16 x BF16 -> F32, K-major A and B,
+// M = 128, N = 128, optional A negate.
+__host__ __device__ constexpr uint32_t instr_desc(bool negate_a) {
+    return (1u << 4)                     // D format F32
+           | (1u << 7)                   // A format BF16
+           | (1u << 10)                  // B format BF16
+           | ((negate_a ? 1u : 0u) << 13)
+           | ((uint32_t)(kTileN >> 3) << 17)
+           | ((uint32_t)(kTileM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+// Bounded wait for the given phase parity; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long long i = 0; i < kSpinLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t"
+            ".reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t"
+            "}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void fence_async_shared() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Split one FP32 value into its BF16 hi and lo terms (bit patterns).
+__device__ __forceinline__ void split(float x, uint16_t &hi, uint16_t &lo) {
+    __nv_bfloat16 h = __float2bfloat16_rn(x);
+    __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
+    hi = __bfloat16_as_ushort(h);
+    lo = __bfloat16_as_ushort(l);
+}
+
+// Byte offset of (row r, k-group j) inside a tile: [j][r/8][r%8][8 bf16].
+__device__ __forceinline__ uint32_t tile_off(int r, int j) {
+    return (uint32_t)(j * (kTileM / 8) * 128 + (r >> 3) * 128 + (r & 7) * 16);
+}
+
+constexpr int kThreads = 256;
+
+// 16 consecutive TMEM columns of this warp's 32 lanes (one row per thread).
+// Asynchronous: the registers may be read only after tcgen05.wait::ld.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ uint32_t pack2(uint16_t a, uint16_t b) { return (uint32_t)a | ((uint32_t)b << 16); }
+
+// Splits 8 complex values into the four 16-byte core-matrix rows (re hi, re
+// lo, im hi, im lo) of tiles t_re_hi, t_re_hi+1, t_im_hi, t_im_hi+1.
+__device__ __forceinline__ void split_store8(const float2 *v, uint8_t *buf, int t_re_hi, int t_im_hi, uint32_t off) {
+    uint16_t rh[8], rl[8], ih[8], il[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        split(v[k].x, rh[k], rl[k]);
+        split(v[k].y, ih[k], il[k]);
+    }
+    *reinterpret_cast<uint4 *>(buf + t_re_hi * kTileBytes + off) =
+        make_uint4(pack2(rh[0], rh[1]), pack2(rh[2], rh[3]), pack2(rh[4], rh[5]), pack2(rh[6], rh[7]));
+    *reinterpret_cast<uint4 *>(buf + (t_re_hi + 1) * kTileBytes + off) =
+        make_uint4(pack2(rl[0], rl[1]), pack2(rl[2], rl[3]), pack2(rl[4], rl[5]), pack2(rl[6], rl[7]));
+    *reinterpret_cast<uint4 *>(buf + t_im_hi * kTileBytes + off) =
+        make_uint4(pack2(ih[0], ih[1]), pack2(ih[2], ih[3]), pack2(ih[4], ih[5]), pack2(ih[6], ih[7]));
+    *reinterpret_cast<uint4 *>(buf + (t_im_hi + 1) * kTileBytes + off) =
+        make_uint4(pack2(il[0], il[1]), pack2(il[2], il[3]), pack2(il[4], il[5]), pack2(il[6], il[7]));
+}
+
+// Loads complex chunk `c` (16 columns of L21 for the tile's 128 rows and 16
+// rows of U12 for its 128 columns), splits it and stores the 8 operand tiles
+// of `buf`.  Thread t handles (row or column t % 128, k-half t / 128): the
+// L21 loads are coalesced across rows, each U12 column half is one 64-byte
+// run read with 16-byte vector loads.
+__device__ __forceinline__ void load_chunk(const float2 *__restrict__ A, int64_t m, int64_t row0, int64_t col0,
+                                           int64_t k0, int c, uint8_t *buf) {
+    const int t = threadIdx.x & 127, j = threadIdx.x >> 7;
+    const int64_t kk = k0 + (int64_t)c * kChunk + 8 * j;
+    float2 va[8], vb[8];
+    const int64_t row = row0 + t;
+    const int64_t col = col0 + t;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) va[k] = row < m ? __ldg(A + row + (kk + k) * m) : make_float2(0.f, 0.f);
+    if (col < m) {
+        const float4 *src = reinterpret_cast<const float4 *>(A + kk + col * m);
+        if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float4 w = __ldg(src + q);
+                vb[2 * q] = make_float2(w.x, w.y);
+                vb[2 * q + 1] = make_float2(w.z, w.w);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) vb[k] = __ldg(A + kk + k + col * m);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) vb[k] = make_float2(0.f, 0.f);
+    }
+    const uint32_t off = tile_off(t, j);
+    split_store8(va, buf, ArH, AiH, off);
+    split_store8(vb, buf, BrH, BiH, off);
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+    gemm_bf16x3_kernel(float2 *__restrict__ a, int64_t m, int64_t base, int nb, int *__restrict__ err_flag) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    uint8_t *bufs[2] = {smem, smem + kBufBytes};
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * kBufBytes);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2);
+
+    const int f = blockIdx.z;
+    float2 *A = a + (int64_t)f * m * m;
+    const int64_t k0 = base - nb;  // panel columns [k0, base)
+    const int64_t row0 = base + (int64_t)blockIdx.y * kTileM;
+    const int64_t col0 = base + (int64_t)blockIdx.x * kTileN;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nchunks = nb / kChunk;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(smem_u32(&bars[0]), 1);
+        mbar_init(smem_u32(&bars[1]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    load_chunk(A, m, row0, col0, k0, 0, bufs[0]);
+    fence_async_shared();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t tmem_re = tmem, tmem_im = tmem + kTileN;
+
+    bool ok = true;
+    uint32_t uses[2] = {0u, 0u};  // commits made on each barrier
+    for (int c = 0; c < nchunks && ok; ++c) {
+        const int b = c & 1;
+        if (threadIdx.x == 0) {
+            tc_fence_after();
+            const uint32_t s = smem_u32(bufs[b]);
+            auto d = [&](int tile) { return smem_desc(s + tile * kTileBytes, (kTileM / 8) * 128, 128); };
+            const uint32_t acc = c > 0 ? 1u : 0u;
+            const uint32_t pos = instr_desc(false), neg = instr_desc(true);
+            // Re += Ar Br - Ai Bi
+            mma_bf16(tmem_re, d(ArH), d(BrH), pos, acc);
+            mma_bf16(tmem_re, d(ArH), d(BrL), pos, 1u);
+            mma_bf16(tmem_re, d(ArL), d(BrH), pos, 1u);
+            mma_bf16(tmem_re, d(AiH), d(BiH), neg, 1u);
+            mma_bf16(tmem_re, d(AiH), d(BiL), neg, 1u);
+            mma_bf16(tmem_re, d(AiL), d(BiH), neg, 1u);
+            // Im += Ar Bi + Ai Br
+            mma_bf16(tmem_im, d(ArH), d(BiH), pos, acc);
+            mma_bf16(tmem_im, d(ArH), d(BiL), pos, 1u);
+            mma_bf16(tmem_im, d(ArL), d(BiH), pos, 1u);
+            mma_bf16(tmem_im, d(AiH), d(BrH), pos, 1u);
+            mma_bf16(tmem_im, d(AiH), d(BrL), pos, 1u);
+            mma_bf16(tmem_im, d(AiL), d(BrH), pos, 1u);
+            mma_commit(smem_u32(&bars[b]));
+        }
+        uses[b] += 1;
+        if (c + 1 < nchunks) {
+            const int nbuf = (c + 1) & 1;
+            if (uses[nbuf] > 0) {
+                // The MMAs of chunk c-1 read buffer nbuf; wait for them.
+                if (!mbar_wait(smem_u32(&bars[nbuf]), (uses[nbuf] - 1) & 1)) ok = false;
+            }
+            if (ok) {
+                load_chunk(A, m, row0, col0, k0, c + 1, bufs[nbuf]);
+                fence_async_shared();
+            }
+            tc_fence_before();
+            ok = __syncthreads_and(ok);
+        }
+    }
+    // Completion of the last commit implies completion of every earlier MMA.
+    if (ok && nchunks > 0) {
+        const int b = (nchunks - 1) & 1;
+        if (!mbar_wait(smem_u32(&bars[b]), (uses[b] - 1) & 1)) ok = false;
+    }
+    ok = __syncthreads_and(ok);
+    tc_fence_after();
+    if (ok) {
+        // Warp w reads TMEM lanes 32 (w % 4) .. +31 (its rows) and the
+        // column half w / 4, 16 columns at a time; the 16 C loads of a step are
+        // issued together before any store.
+        const int quarter = warp & 3, half = warp >> 2;
+        const int64_t row = row0 + quarter * 32 + lane;
+        const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
+        for (int cc = half * (kTileN / 2); cc < (half + 1) * (kTileN / 2); cc += 16) {
+            uint32_t re[16], im[16];
+            tmem_ld16(tmem_re + lane_off + cc, re);
+            tmem_ld16(tmem_im + lane_off + cc, im);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < m) {
+                float2 *p = A + row + (col0 + cc) * m;
+                const int ncol = (int)min((int64_t)16, m - (col0 + cc));
+                float2 v[16];
+#pragma unroll
+                for (int jj = 0; jj < 16; ++jj) v[jj] = jj < ncol ? p[jj * m] : make_float2(0.f, 0.f);
+#pragma unroll
+                for (int jj = 0; jj < 16; ++jj)
+                    if (jj < ncol)
+                        p[jj * m] = make_float2(v[jj].x - __uint_as_float(re[jj]), v[jj].y - __uint_as_float(im[jj]));
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        atomicExch(err_flag, 1);
+        // Give MMAs still in flight a second bounded chance to drain before
+        // the TMEM and shared memory they use are released.
+        if (nchunks > 0) {
+            const int b = (nchunks - 1) & 1;
+            mbar_wait(smem_u32(&bars[b]), (uses[b] - 1) & 1);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+}
+
+int *g_err_flag[64] = {nullptr};
+
+}  // namespace
+
+fh_status gemm_tc_update(float *a, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err) {
+    if (nb % kChunk) return fail(err, FH_ERR_INVALID_ARGUMENT, "tensor-core update needs a panel width multiple of 16");
+    const int64_t base = k0 + nb;
+    const int64_t rem = m - base;
+    if (rem <= 0) return FH_OK;
+    int dev = 0;
+    FHB_CUDA(cudaGetDevice(&dev));
+    if (!g_err_flag[dev]) {
+        FHB_CUDA(cudaMalloc(&g_err_flag[dev], sizeof(int)));
+        FHB_CUDA(cudaMemset(g_err_flag[dev], 0, sizeof(int)));
+        FHB_CUDA(cudaFuncSetAttribute(gemm_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+    }
+    dim3 grid((unsigned)((rem + kTileN - 1) / kTileN), (unsigned)((rem + kTileM - 1) / kTileM), (unsigned)count);
+    gemm_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(reinterpret_cast<float2 *>(a), m, base, nb, g_err_flag[dev]);
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+fh_status gemm_tc_check(fh_error_info *err) {
+    int dev = 0;
+    FHB_CUDA(cudaGetDevice(&dev));
+    if (!g_err_flag[dev]) return FH_OK;
+    int flag = 0;
+    FHB_CUDA(cudaMemcpy(&flag, g_err_flag[dev], sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        cudaMemset(g_err_flag[dev], 0, sizeof(int));
+        return fail(err, FH_ERR_DEVICE_TIMEOUT, "a tensor-core wait ran out of its iteration limit");
+    }
+    return FH_OK;
 }
 
 }  // namespace fhb

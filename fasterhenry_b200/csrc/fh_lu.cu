@@ -25,8 +25,6 @@
 
 namespace fhb {
 
-fh_status gemm_tc_update(float *a, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err);
-
 namespace {
 
 template <class T>
@@ -519,6 +517,7 @@ fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaS
     FHB_CUDA(cudaFuncSetAttribute(gemm_update_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem));
     for (int64_t k0 = 0; k0 < m; k0 += nb) {
         const int w_nb = (int)std::min<int64_t>(nb, m - k0);
+        prof_begin(s, FH_PROF_PANEL);
         for (int c = 0; c < w_nb; ++c) {
             const int j = (int)(k0 + c);
             const int chunks = std::min(w.max_chunks, (int)((m - j + 1023) / 1024));
@@ -530,22 +529,47 @@ fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaS
             }
         }
         const int64_t c0 = k0 + w_nb;
+        prof_end(s, FH_PROF_PANEL, 0.0);
         if (c0 >= m) break;
         const int64_t ncols = m - c0;
+        prof_begin(s, FH_PROF_TRSM);
         swap_kernel<T><<<dim3(grid_for(ncols, 256, 1024), b.count), 256, 0, s>>>(a, m, (int)k0, w_nb, c0, b.pivots);
         trsm_kernel<T><<<dim3((unsigned)((ncols + 63) / 64), b.count), 64, trsm_smem, s>>>(a, m, (int)k0, w_nb);
+        prof_end(s, FH_PROF_TRSM, 4.0 * (double)w_nb * w_nb * ncols * b.count);
+        // complex GEMM: 8 real flops per complex multiply-add
+        const double flops = 8.0 * (double)ncols * (double)ncols * (double)w_nb * (double)b.count;
         if (mode == TrailingUpdate::TensorBf16x3 && sizeof(T) == 4 && w_nb == nb) {
+            prof_begin(s, FH_PROF_GEMM_TC);
             fh_status st = gemm_tc_update(reinterpret_cast<float *>(b.a), m, b.count, k0, nb, s, err);
+            prof_end(s, FH_PROF_GEMM_TC, flops);
             if (st) return st;
         } else {
+            const int cls = sizeof(T) == 8 ? FH_PROF_GEMM_FP64 : FH_PROF_GEMM_FP32;
+            prof_begin(s, cls);
             const unsigned tiles = (unsigned)((ncols + 63) / 64);
             gemm_update_kernel<T><<<dim3(tiles, tiles, b.count), 256, gemm_smem, s>>>(a, m, (int)k0, w_nb);
+            prof_end(s, cls, flops);
         }
         FHB_CUDA(cudaGetLastError());
     }
     FHB_CUDA(cudaGetLastError());
     return FH_OK;
 }
+
+template <class T>
+fh_status gemm_simt_update(T *av, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err) {
+    const int64_t ncols = m - k0 - nb;
+    if (ncols <= 0) return FH_OK;
+    const size_t gemm_smem = sizeof(Cx<T>) * (size_t)nb * 128;
+    FHB_CUDA(cudaFuncSetAttribute(gemm_update_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem));
+    const unsigned tiles = (unsigned)((ncols + 63) / 64);
+    gemm_update_kernel<T><<<dim3(tiles, tiles, count), 256, gemm_smem, s>>>(reinterpret_cast<Cx<T> *>(av), m, (int)k0,
+                                                                             nb);
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+template fh_status gemm_simt_update<float>(float *, int64_t, int, int64_t, int, cudaStream_t, fh_error_info *);
+template fh_status gemm_simt_update<double>(double *, int64_t, int, int64_t, int, cudaStream_t, fh_error_info *);
 
 template <class T>
 fh_status lu_solve(const LuBatch<T> &b, T *xv, int nrhs, int nb, cudaStream_t s, fh_error_info *err) {
@@ -555,6 +579,7 @@ fh_status lu_solve(const LuBatch<T> &b, T *xv, int nrhs, int nb, cudaStream_t s,
     const int64_t m = b.m;
     if (m == 0) return FH_OK;
     const int groups = b.count * nrhs;
+    prof_begin(s, FH_PROF_SOLVE);
     for (int64_t k0 = 0; k0 < m; k0 += nb) {
         const int w_nb = (int)std::min<int64_t>(nb, m - k0);
         fwd_panel_kernel<T><<<groups, 64, 0, s>>>(a, m, nrhs, (int)k0, w_nb, b.pivots, x);
@@ -570,6 +595,7 @@ fh_status lu_solve(const LuBatch<T> &b, T *xv, int nrhs, int nb, cudaStream_t s,
             gemv_update_kernel<T><<<dim3(grid_for(k0, 256, 64), groups), 256, 0, s>>>(a, m, nrhs, (int)k0, w_nb, 0,
                                                                                       k0, x);
     }
+    prof_end(s, FH_PROF_SOLVE, 8.0 * (double)m * (double)m * nrhs * b.count);
     FHB_CUDA(cudaGetLastError());
     return FH_OK;
 }
@@ -598,8 +624,10 @@ fh_status residual_fp64(const double *Rm, const double *Lm, int64_t ld, int64_t 
                         int count, const double *x, double *r, double *rnorm, cudaStream_t s, fh_error_info *err) {
     if (m == 0) return FH_OK;
     const int fgroups = (count + kResF - 1) / kResF;
+    prof_begin(s, FH_PROF_RESIDUAL);
     residual_kernel<<<dim3((unsigned)((m + 127) / 128), (unsigned)(fgroups * p)), 128, 0, s>>>(
         Rm, Lm, ld, m, p, omega, count, reinterpret_cast<const Cx<double> *>(x), reinterpret_cast<Cx<double> *>(r));
+    prof_end(s, FH_PROF_RESIDUAL, 16.0 * (double)m * (double)m);  // bytes: R and L read once
     FHB_CUDA(cudaGetLastError());
     if (rnorm) {
         max_abs_kernel<double><<<count, 256, 0, s>>>(r, 2 * m * p, rnorm);

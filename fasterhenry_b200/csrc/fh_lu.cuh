@@ -34,6 +34,15 @@ enum class TrailingUpdate { Simt, TensorBf16x3 };
 template <class T>
 fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaStream_t s, fh_error_info *err);
 
+// One trailing update A22 -= L21 U12 of the panel [k0, k0+nb) on the tensor
+// cores (split-BF16 x3), for every matrix of an FP32 batch.
+fh_status gemm_tc_update(float *a, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err);
+// Reports (and clears) a bounded tensor-core wait that ran out.
+fh_status gemm_tc_check(fh_error_info *err);
+// One SIMT trailing update (FP32 or FP64), for tests.
+template <class T>
+fh_status gemm_simt_update(T *a, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err);
+
 // Solve with the factors in place: x (count x m x nrhs, column-major per
 // matrix, stride m*nrhs) is overwritten.
 template <class T>

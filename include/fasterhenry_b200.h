@@ -148,8 +148,10 @@ typedef enum fh_solver_choice {
  * the reference always runs the FP64 form). */
 typedef enum fh_precision {
     FH_PRECISION_FP64 = 0,          /* FP64 blocked LU, partial pivoting (dense.rs) */
-    FH_PRECISION_MIXED_BF16X3 = 1   /* FP32 panels, split-BF16 x3 tensor-core trailing
+    FH_PRECISION_MIXED_BF16X3 = 1,  /* FP32 panels, split-BF16 x3 tensor-core trailing
                                        updates, FP64-residual iterative refinement */
+    FH_PRECISION_MIXED_FP32 = 2     /* FP32 factors with FP32 SIMT trailing updates,
+                                       FP64-residual iterative refinement */
 } fh_precision;
 
 /* Counts, result.rs:110-126. */
@@ -262,6 +264,45 @@ fh_status fh_sweep(fh_system *sys, const double *frequencies_hz, size_t nf, fh_p
 /* One frequency (MeshSystem::impedance, solve.rs:806-830). */
 fh_status fh_impedance(fh_system *sys, double frequency_hz, fh_precision precision, double *z_out,
                        fh_error_info *err);
+
+/* Fill statistics of an assembled system: pairs per method and device time
+ * per fill kernel (no reference counterpart; diagnostics). */
+typedef struct fh_fill_stats {
+    int64_t pairs, orthogonal, point_quadrature, closed_form, aligned_quadrature, sampled;
+    int64_t distinct_aligned_keys;
+    double point_evaluations;
+    double ms_classify, ms_point, ms_closed_form, ms_aligned_quadrature, ms_sampled, ms_congruence;
+} fh_fill_stats;
+fh_status fh_system_fill_stats(const fh_system *sys, fh_fill_stats *stats);
+
+/* ---- test hooks (no reference counterpart) ----------------------------- */
+
+/* One trailing update A22 -= L21 U12 of an LU panel [k0, k0+nb) applied to
+ * `count` complex FP32 matrices of order m (interleaved, column-major, back
+ * to back), in place on a host copy.  mode 0: FP32 SIMT; mode 1: split-BF16
+ * x3 on the tensor cores (nb a multiple of 16). */
+fh_status fh_test_trailing_update(float *a, int64_t m, int32_t count, int64_t k0, int32_t nb, int32_t mode,
+                                  fh_error_info *err);
+
+/* ---- device-event profiler (no reference counterpart) ------------------ */
+
+/* Kernel classes timed when profiling is on. */
+typedef enum fh_profile_class {
+    FH_PROF_GEMM_FP64 = 0,      /* trailing update A22 -= L21 U12, FP64 SIMT */
+    FH_PROF_GEMM_FP32 = 1,      /* trailing update, FP32 SIMT */
+    FH_PROF_GEMM_TC = 2,        /* trailing update, split-BF16 x3 tcgen05 */
+    FH_PROF_PANEL = 3,          /* panel factorization (pivot search + rank-1 updates) */
+    FH_PROF_TRSM = 4,           /* row interchanges + U12 triangular solve */
+    FH_PROF_SOLVE = 5,          /* forward/backward substitution */
+    FH_PROF_RESIDUAL = 6,       /* FP64 residual of R + jwL */
+    FH_PROF_CLASSES = 7
+} fh_profile_class;
+
+void fh_profile_enable(int32_t on);
+void fh_profile_reset(void);
+/* Totals since the last reset: launches, device milliseconds (sum of
+ * per-launch event durations) and algorithmic work (flops). */
+fh_status fh_profile_read(int32_t cls, int64_t *launches, double *ms, double *work);
 
 /* ---- outputs (host) ---------------------------------------------------- */
 

@@ -54,6 +54,12 @@ fh_status ensure_device(fh_error_info *err);
 bool prof_on();
 void prof_begin(cudaStream_t s, int cls);
 void prof_end(cudaStream_t s, int cls, double work);
+// While alive, the profiler records nothing on this thread (it would create
+// CUDA events); used by entry points that promise to acquire no resources.
+struct ProfSuppress {
+    ProfSuppress();
+    ~ProfSuppress();
+};
 
 // Fill the n x n column-major L on the device (d_L must be zero-filled by the
 // caller).  `d_methods` optional (n*n int8).  `stream` orders the work.

@@ -55,17 +55,22 @@ void fold() {
 
 }  // namespace
 
-bool prof_on() { return g_on; }
+thread_local int t_suppress = 0;
+
+ProfSuppress::ProfSuppress() { ++t_suppress; }
+ProfSuppress::~ProfSuppress() { --t_suppress; }
+
+bool prof_on() { return g_on && !t_suppress; }
 
 void prof_begin(cudaStream_t s, int cls) {
-    if (!g_on || cls < 0 || cls >= FH_PROF_CLASSES) return;
+    if (!g_on || t_suppress || cls < 0 || cls >= FH_PROF_CLASSES) return;
     std::lock_guard<std::mutex> lk(g_mu);
     t_open[cls] = take();
     cudaEventRecord(t_open[cls], s);
 }
 
 void prof_end(cudaStream_t s, int cls, double work) {
-    if (!g_on || cls < 0 || cls >= FH_PROF_CLASSES) return;
+    if (!g_on || t_suppress || cls < 0 || cls >= FH_PROF_CLASSES) return;
     std::lock_guard<std::mutex> lk(g_mu);
     cudaEvent_t b = take();
     cudaEventRecord(b, s);

@@ -227,6 +227,24 @@ fh_status fh_partial_inductance_matrix(const fh_filament *filaments, size_t n, d
 fh_status fh_lu_solve_c64(const double *a, size_t n, const double *b, size_t nrhs, double *x,
                           fh_error_info *err);
 
+/* The same FP64 LU solve for callers that cannot allocate device memory while
+ * they solve (for example an application that hands all device memory to its
+ * own pool, whose accounting a cudaMalloc would bypass, or a latency-critical
+ * loop that must not cudaMalloc/cudaFree).  No counterpart in the reference.
+ *   a: DEVICE pointer, n x n complex column-major; consumed as workspace
+ *      (overwritten with the LU factors), like the reference's lu_solve.
+ *   b: DEVICE pointer, n x nrhs complex column-major; overwritten with x.
+ *   stream: a cudaStream_t (NULL = the legacy default stream).
+ * Allocates nothing: its scratch (pivots, pivot-search partials, flags) is a
+ * file-scope device array sized for n <= FH_NOALLOC_MAX_ORDER; larger n is
+ * rejected with FH_ERR_INVALID_ARGUMENT.  The first call on a device looks up
+ * the array's address (make it before any stream capture).  All calls share
+ * the array: calls that overlap on the GPU race and must be serialised by the
+ * caller.  Returns after the solve has completed on `stream`. */
+#define FH_NOALLOC_MAX_ORDER 65536
+fh_status fh_lu_solve_c64_noalloc(double *a, size_t n, double *b, size_t nrhs, void *stream,
+                                  fh_error_info *err);
+
 /* ---- the dense system (MeshSystem) ------------------------------------ */
 
 /* Assemble: discretize, loop basis, fill L on the device, congruence

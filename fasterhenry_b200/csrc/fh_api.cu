@@ -95,6 +95,11 @@ std::string fstr(double v) {
 }
 
 constexpr double kTau = 6.283185307179586;
+// Outer panel widths: FP64 stays at 64 (shared-memory budget of its TRSM and
+// SIMT update); the FP32 form uses 128, which halves the trailing update's
+// C traffic per flop.
+constexpr int kNbFp64 = 64;
+constexpr int kNbFp32 = 128;
 
 // Factor + solve + Schur for `count` frequencies in FP64.  x_out (count x m x
 // p complex) receives the FP64 solutions; z (count x p x p) the impedances.
@@ -125,6 +130,18 @@ fh_status sweep_chunk_fp64(fh_system *s, const double *d_omega, int count, doubl
         w.partial_val = pv.p;
         w.partial_idx = pi.p;
         w.tickets = tk.p;
+        CoopScratch cs;
+        DBuf<unsigned char> coop_mem;
+        int per_matrix = 0;
+        size_t coop_bytes = 0;
+        e = coop_plan<double>(count, m, &per_matrix, &coop_bytes, err);
+        if (e) return e;
+        FHB_ALLOC(coop_mem, coop_bytes);
+        coop_bind<double>(coop_mem.p, count, per_matrix, cs);
+        w.coop = &cs;
+        DBuf<double> linv_mem;
+        FHB_ALLOC(linv_mem, (size_t)count * kNbFp64 * kNbFp64 * 2);
+        w.linv = linv_mem.p;
         LuBatch<double> b;
         b.a = a.p;
         b.pivots = piv.p;
@@ -135,9 +152,9 @@ fh_status sweep_chunk_fp64(fh_system *s, const double *d_omega, int count, doubl
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         cudaEventRecord(e0, st);
-        e = lu_factor<double>(b, w, 64, TrailingUpdate::Simt, st, err);
+        e = lu_factor<double>(b, w, kNbFp64, TrailingUpdate::Simt, st, err);
         cudaEventRecord(e1, st);
-        if (!e) e = lu_solve<double>(b, d_x, (int)p, 64, st, err);
+        if (!e) e = lu_solve<double>(b, d_x, (int)p, kNbFp64, st, err);
         if (e) {
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
@@ -202,6 +219,18 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     w.partial_val = pv.p;
     w.partial_idx = pi.p;
     w.tickets = tk.p;
+    CoopScratch cs;
+    DBuf<unsigned char> coop_mem;
+    int per_matrix = 0;
+    size_t coop_bytes = 0;
+    e = coop_plan<float>(count, m, &per_matrix, &coop_bytes, err);
+    if (e) return e;
+    FHB_ALLOC(coop_mem, coop_bytes);
+    coop_bind<float>(coop_mem.p, count, per_matrix, cs);
+    w.coop = &cs;
+    DBuf<float> linv_mem;
+    FHB_ALLOC(linv_mem, (size_t)count * kNbFp32 * kNbFp32 * 2);
+    w.linv = linv_mem.p;
     LuBatch<float> b;
     b.a = a.p;
     b.pivots = piv.p;
@@ -213,7 +242,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     cudaEventCreate(&e1);
     cudaEventCreate(&e2);
     cudaEventRecord(e0, st);
-    e = lu_factor<float>(b, w, 64, mode, st, err);
+    e = lu_factor<float>(b, w, kNbFp32, mode, st, err);
     cudaEventRecord(e1, st);
     if (e) return e;
     if (mode == TrailingUpdate::TensorBf16x3) {
@@ -228,7 +257,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     int it = 0;
     for (; it < kMaxIter; ++it) {
         e = convert_c64_to_c32(r.p, d32.p, count * vec, st, err);
-        if (!e) e = lu_solve<float>(b, d32.p, (int)p, 64, st, err);
+        if (!e) e = lu_solve<float>(b, d32.p, (int)p, kNbFp32, st, err);
         if (!e) e = add_c32_to_c64(d_x, d32.p, count * vec, st, err);
         if (!e) e = residual_fp64(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, r.p, rnorm.p, st, err);
         if (e) return e;

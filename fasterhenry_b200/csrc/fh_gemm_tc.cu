@@ -153,6 +153,18 @@ __device__ __forceinline__ uint32_t tile_off(int r, int j) {
 
 constexpr int kThreads = 256;
 
+struct GemmArgs {
+    const float2 *A;  // A operand: (row r, k) at A[f sA + r + k lda]
+    int64_t lda, sA;
+    const float2 *B;  // B operand: (k, column n) at B[f sB + k + n ldb]
+    int64_t ldb, sB;
+    float2 *C;        // C: (r, n) at C[f sC + r + n ldc]
+    int64_t ldc, sC;
+    int64_t M, N;
+    int K;
+    int assign;
+};
+
 // 16 consecutive TMEM columns of this warp's 32 lanes (one row per thread).
 // Asynchronous: the registers may be read only after tcgen05.wait::ld.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
@@ -190,17 +202,19 @@ __device__ __forceinline__ void split_store8(const float2 *v, uint8_t *buf, int 
 // of `buf`.  Thread t handles (row or column t % 128, k-half t / 128): the
 // L21 loads are coalesced across rows, each U12 column half is one 64-byte
 // run read with 16-byte vector loads.
-__device__ __forceinline__ void load_chunk(const float2 *__restrict__ A, int64_t m, int64_t row0, int64_t col0,
-                                           int64_t k0, int c, uint8_t *buf) {
+__device__ __forceinline__ void load_chunk(const GemmArgs &g, int f, int64_t row0, int64_t col0, int c,
+                                           uint8_t *buf) {
     const int t = threadIdx.x & 127, j = threadIdx.x >> 7;
-    const int64_t kk = k0 + (int64_t)c * kChunk + 8 * j;
+    const int64_t kk = (int64_t)c * kChunk + 8 * j;
     float2 va[8], vb[8];
     const int64_t row = row0 + t;
     const int64_t col = col0 + t;
+    const float2 *Aop = g.A + (int64_t)f * g.sA;
+    const float2 *Bop = g.B + (int64_t)f * g.sB;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) va[k] = row < m ? __ldg(A + row + (kk + k) * m) : make_float2(0.f, 0.f);
-    if (col < m) {
-        const float4 *src = reinterpret_cast<const float4 *>(A + kk + col * m);
+    for (int k = 0; k < 8; ++k) va[k] = row < g.M ? __ldg(Aop + row + (kk + k) * g.lda) : make_float2(0.f, 0.f);
+    if (col < g.N) {
+        const float4 *src = reinterpret_cast<const float4 *>(Bop + kk + col * g.ldb);
         if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
@@ -210,7 +224,7 @@ __device__ __forceinline__ void load_chunk(const float2 *__restrict__ A, int64_t
             }
         } else {
 #pragma unroll
-            for (int k = 0; k < 8; ++k) vb[k] = __ldg(A + kk + k + col * m);
+            for (int k = 0; k < 8; ++k) vb[k] = __ldg(Bop + kk + k + col * g.ldb);
         }
     } else {
 #pragma unroll
@@ -221,8 +235,11 @@ __device__ __forceinline__ void load_chunk(const float2 *__restrict__ A, int64_t
     split_store8(vb, buf, BrH, BiH, off);
 }
 
-__global__ void __launch_bounds__(kThreads, 2)
-    gemm_bf16x3_kernel(float2 *__restrict__ a, int64_t m, int64_t base, int nb, int *__restrict__ err_flag) {
+// C (M x N) = C - A B  (assign == 0)  or  C = A B  (assign == 1), batched over
+// blockIdx.z; K a multiple of 16.  In the assign form C may be B itself when
+// M <= 128 (one tile row): a CTA reads all of its B columns before it writes
+// them, and no other CTA reads them.
+__global__ void __launch_bounds__(kThreads, 2) gemm_bf16x3_kernel(GemmArgs g, int *__restrict__ err_flag) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     uint8_t *bufs[2] = {smem, smem + kBufBytes};
@@ -230,12 +247,11 @@ __global__ void __launch_bounds__(kThreads, 2)
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2);
 
     const int f = blockIdx.z;
-    float2 *A = a + (int64_t)f * m * m;
-    const int64_t k0 = base - nb;  // panel columns [k0, base)
-    const int64_t row0 = base + (int64_t)blockIdx.y * kTileM;
-    const int64_t col0 = base + (int64_t)blockIdx.x * kTileN;
+    float2 *C = g.C + (int64_t)f * g.sC;
+    const int64_t row0 = (int64_t)blockIdx.y * kTileM;
+    const int64_t col0 = (int64_t)blockIdx.x * kTileN;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nchunks = nb / kChunk;
+    const int nchunks = g.K / kChunk;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -247,7 +263,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         mbar_init(smem_u32(&bars[1]), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    load_chunk(A, m, row0, col0, k0, 0, bufs[0]);
+    load_chunk(g, f, row0, col0, 0, bufs[0]);
     fence_async_shared();
     tc_fence_before();
     __syncthreads();
@@ -289,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                 if (!mbar_wait(smem_u32(&bars[nbuf]), (uses[nbuf] - 1) & 1)) ok = false;
             }
             if (ok) {
-                load_chunk(A, m, row0, col0, k0, c + 1, bufs[nbuf]);
+                load_chunk(g, f, row0, col0, c + 1, bufs[nbuf]);
                 fence_async_shared();
             }
             tc_fence_before();
@@ -315,16 +331,23 @@ __global__ void __launch_bounds__(kThreads, 2)
             tmem_ld16(tmem_re + lane_off + cc, re);
             tmem_ld16(tmem_im + lane_off + cc, im);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < m) {
-                float2 *p = A + row + (col0 + cc) * m;
-                const int ncol = (int)min((int64_t)16, m - (col0 + cc));
-                float2 v[16];
+            if (row < g.M) {
+                float2 *p = C + row + (col0 + cc) * g.ldc;
+                const int ncol = (int)min((int64_t)16, g.N - (col0 + cc));
+                if (g.assign) {
 #pragma unroll
-                for (int jj = 0; jj < 16; ++jj) v[jj] = jj < ncol ? p[jj * m] : make_float2(0.f, 0.f);
+                    for (int jj = 0; jj < 16; ++jj)
+                        if (jj < ncol) p[jj * g.ldc] = make_float2(__uint_as_float(re[jj]), __uint_as_float(im[jj]));
+                } else {
+                    float2 v[16];
 #pragma unroll
-                for (int jj = 0; jj < 16; ++jj)
-                    if (jj < ncol)
-                        p[jj * m] = make_float2(v[jj].x - __uint_as_float(re[jj]), v[jj].y - __uint_as_float(im[jj]));
+                    for (int jj = 0; jj < 16; ++jj) v[jj] = jj < ncol ? p[jj * g.ldc] : make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj)
+                        if (jj < ncol)
+                            p[jj * g.ldc] =
+                                make_float2(v[jj].x - __uint_as_float(re[jj]), v[jj].y - __uint_as_float(im[jj]));
+                }
             }
         }
     } else if (threadIdx.x == 0) {
@@ -345,11 +368,10 @@ int *g_err_flag[64] = {nullptr};
 
 }  // namespace
 
-fh_status gemm_tc_update(float *a, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err) {
-    if (nb % kChunk) return fail(err, FH_ERR_INVALID_ARGUMENT, "tensor-core update needs a panel width multiple of 16");
-    const int64_t base = k0 + nb;
-    const int64_t rem = m - base;
-    if (rem <= 0) return FH_OK;
+fh_status gemm_tc_launch(const GemmArgs &g, int count, cudaStream_t s, fh_error_info *err) {
+    if (g.K % kChunk) return fail(err, FH_ERR_INVALID_ARGUMENT, "tensor-core GEMM needs K a multiple of 16");
+    if (g.M <= 0 || g.N <= 0 || g.K <= 0) return FH_OK;
+    if (g.assign && g.M > kTileM) return fail(err, FH_ERR_INVALID_ARGUMENT, "in-place assign GEMM needs M <= 128");
     int dev = 0;
     FHB_CUDA(cudaGetDevice(&dev));
     if (!g_err_flag[dev]) {
@@ -357,10 +379,55 @@ fh_status gemm_tc_update(float *a, int64_t m, int count, int64_t k0, int nb, cud
         FHB_CUDA(cudaMemset(g_err_flag[dev], 0, sizeof(int)));
         FHB_CUDA(cudaFuncSetAttribute(gemm_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
     }
-    dim3 grid((unsigned)((rem + kTileN - 1) / kTileN), (unsigned)((rem + kTileM - 1) / kTileM), (unsigned)count);
-    gemm_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(reinterpret_cast<float2 *>(a), m, base, nb, g_err_flag[dev]);
+    dim3 grid((unsigned)((g.N + kTileN - 1) / kTileN), (unsigned)((g.M + kTileM - 1) / kTileM), (unsigned)count);
+    gemm_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(g, g_err_flag[dev]);
     FHB_CUDA(cudaGetLastError());
     return FH_OK;
+}
+
+fh_status gemm_tc_update(float *a, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err) {
+    if (nb % kChunk) return fail(err, FH_ERR_INVALID_ARGUMENT, "tensor-core update needs a panel width multiple of 16");
+    const int64_t base = k0 + nb;
+    const int64_t rem = m - base;
+    if (rem <= 0) return FH_OK;
+    float2 *A = reinterpret_cast<float2 *>(a);
+    GemmArgs g;
+    g.A = A + base + k0 * m;  // L21: rows base.., panel columns
+    g.lda = m;
+    g.sA = m * m;
+    g.B = A + k0 + base * m;  // U12: panel rows, columns base..
+    g.ldb = m;
+    g.sB = m * m;
+    g.C = A + base + base * m;
+    g.ldc = m;
+    g.sC = m * m;
+    g.M = rem;
+    g.N = rem;
+    g.K = nb;
+    g.assign = 0;
+    return gemm_tc_launch(g, count, s, err);
+}
+
+fh_status gemm_tc_tri_apply(const float *linv, int nb, float *a, int64_t m, int count, int64_t k0, cudaStream_t s,
+                            fh_error_info *err) {
+    const int64_t c0 = k0 + nb;
+    if (c0 >= m) return FH_OK;
+    float2 *A = reinterpret_cast<float2 *>(a);
+    GemmArgs g;
+    g.A = reinterpret_cast<const float2 *>(linv);
+    g.lda = nb;
+    g.sA = (int64_t)nb * nb;
+    g.B = A + k0 + c0 * m;
+    g.ldb = m;
+    g.sB = m * m;
+    g.C = A + k0 + c0 * m;
+    g.ldc = m;
+    g.sC = m * m;
+    g.M = nb;
+    g.N = m - c0;
+    g.K = nb;
+    g.assign = 1;
+    return gemm_tc_launch(g, count, s, err);
 }
 
 fh_status gemm_tc_check(fh_error_info *err) {

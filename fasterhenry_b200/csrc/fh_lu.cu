@@ -21,38 +21,12 @@
 #include <climits>
 #include <cstdio>
 
+#include "fh_cx.cuh"
 #include "fh_lu.cuh"
 
 namespace fhb {
 
 namespace {
-
-template <class T>
-struct __align__(2 * sizeof(T)) Cx {
-    T re, im;
-};
-
-template <class T>
-__device__ __forceinline__ Cx<T> cmul(Cx<T> a, Cx<T> b) {
-    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
-}
-template <class T>
-__device__ __forceinline__ Cx<T> csub(Cx<T> a, Cx<T> b) {
-    return {a.re - b.re, a.im - b.im};
-}
-template <class T>
-__device__ __forceinline__ Cx<T> cdiv(Cx<T> a, Cx<T> b) {
-    T ns = b.re * b.re + b.im * b.im;
-    T re = a.re * b.re + a.im * b.im;
-    T im = a.im * b.re - a.re * b.im;
-    return {re / ns, im / ns};
-}
-// y -= f * x
-template <class T>
-__device__ __forceinline__ void csubmul(Cx<T> &y, Cx<T> f, Cx<T> x) {
-    y.re -= f.re * x.re - f.im * x.im;
-    y.im -= f.re * x.im + f.im * x.re;
-}
 
 // ---------------------------------------------------------------------------
 // Pivot search for column j (rows j..m-1) of every matrix.  The last block of
@@ -283,32 +257,96 @@ __global__ void __launch_bounds__(256) gemm_update_kernel(Cx<T> *__restrict__ a,
 // x + (f*nrhs + q)*m).
 // ---------------------------------------------------------------------------
 // Forward, one panel: apply the panel's interchanges, then L11 (unit).
+// L11 and the touched entries of x are staged in shared memory; the
+// interchanges run in order on one thread but only touch shared memory (an
+// interchange with a row below the panel uses the value of that row
+// preloaded in parallel, indexed by its first occurrence in the pivot list).
+// Dynamic shared memory: nb*nb complex + 3*nb complex + 2*nb ints.
 template <class T>
-__global__ void fwd_panel_kernel(const Cx<T> *__restrict__ a, int64_t m, int nrhs, int k0, int nb,
-                                 const int *__restrict__ pivots, Cx<T> *__restrict__ x) {
+__global__ void __launch_bounds__(128) fwd_panel_kernel(const Cx<T> *__restrict__ a, int64_t m, int nrhs, int k0,
+                                                        int nb, const int *__restrict__ pivots,
+                                                        Cx<T> *__restrict__ x) {
+    extern __shared__ unsigned char smem_raw[];
+    Cx<T> *Ls = reinterpret_cast<Cx<T> *>(smem_raw);  // Ls[r * nb + k]
+    Cx<T> *xs = Ls + nb * nb;
+    Cx<T> *ext = xs + nb;
+    int *piv = reinterpret_cast<int *>(ext + nb);
+    int *first = piv + nb;
     const int f = blockIdx.x / nrhs;
     const Cx<T> *A = a + (int64_t)f * m * m;
     Cx<T> *X = x + (int64_t)blockIdx.x * m;
-    __shared__ Cx<T> xs[128];
-    if (threadIdx.x == 0) {
-        const int *piv = pivots + (int64_t)f * m;
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+        const int r = idx % nb, k = idx / nb;
+        Ls[r * nb + k] = A[(k0 + r) + (int64_t)(k0 + k) * m];
+    }
+    for (int t = tid; t < nb; t += blockDim.x) {
+        xs[t] = X[k0 + t];
+        piv[t] = pivots[(int64_t)f * m + k0 + t];
+    }
+    __syncthreads();
+    for (int t = tid; t < nb; t += blockDim.x) {
+        const int p = piv[t];
+        int fst = t;
+        if (p >= k0 + nb) {
+            for (int q = 0; q < t; ++q)
+                if (piv[q] == p) {
+                    fst = q;
+                    break;
+                }
+            if (fst == t) ext[t] = X[p];
+        }
+        first[t] = fst;
+    }
+    __syncthreads();
+    if (tid == 0) {
         for (int jj = 0; jj < nb; ++jj) {
-            int p = piv[k0 + jj];
-            if (p != k0 + jj) {
-                Cx<T> t = X[k0 + jj];
-                X[k0 + jj] = X[p];
-                X[p] = t;
-            }
+            const int p = piv[jj];
+            if (p == k0 + jj) continue;
+            Cx<T> &other = p < k0 + nb ? xs[p - k0] : ext[first[jj]];
+            const Cx<T> tmp = xs[jj];
+            xs[jj] = other;
+            other = tmp;
         }
     }
     __syncthreads();
+    for (int t = tid; t < nb; t += blockDim.x)
+        if (piv[t] >= k0 + nb && first[t] == t) X[piv[t]] = ext[t];
+    for (int k = 0; k < nb; ++k) {
+        const Cx<T> xk = xs[k];
+        for (int r = k + 1 + tid; r < nb; r += blockDim.x) {
+            Cx<T> y = xs[r];
+            csubmul(y, xk, Ls[r * nb + k]);
+            xs[r] = y;
+        }
+        __syncthreads();
+    }
+    for (int r = tid; r < nb; r += blockDim.x) X[k0 + r] = xs[r];
+}
+
+// Backward, one panel: U11 (non-unit upper), staged in shared memory.
+template <class T>
+__global__ void __launch_bounds__(128) bwd_panel_kernel2(const Cx<T> *__restrict__ a, int64_t m, int nrhs, int k0,
+                                                         int nb, Cx<T> *__restrict__ x) {
+    extern __shared__ unsigned char smem_raw[];
+    Cx<T> *Us = reinterpret_cast<Cx<T> *>(smem_raw);  // Us[r * nb + k]
+    Cx<T> *xs = Us + nb * nb;
+    const int f = blockIdx.x / nrhs;
+    const Cx<T> *A = a + (int64_t)f * m * m;
+    Cx<T> *X = x + (int64_t)blockIdx.x * m;
+    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+        const int r = idx % nb, k = idx / nb;
+        Us[r * nb + k] = A[(k0 + r) + (int64_t)(k0 + k) * m];
+    }
     for (int r = threadIdx.x; r < nb; r += blockDim.x) xs[r] = X[k0 + r];
     __syncthreads();
-    for (int k = 0; k < nb; ++k) {
-        Cx<T> xk = xs[k];
-        for (int r = k + 1 + threadIdx.x; r < nb; r += blockDim.x) {
+    for (int k = nb - 1; k >= 0; --k) {
+        if (threadIdx.x == 0) xs[k] = cdiv(xs[k], Us[k * nb + k]);
+        __syncthreads();
+        const Cx<T> xk = xs[k];
+        for (int r = threadIdx.x; r < k; r += blockDim.x) {
             Cx<T> y = xs[r];
-            csubmul(y, xk, A[(k0 + r) + (int64_t)(k0 + k) * m]);
+            csubmul(y, xk, Us[r * nb + k]);
             xs[r] = y;
         }
         __syncthreads();
@@ -316,28 +354,117 @@ __global__ void fwd_panel_kernel(const Cx<T> *__restrict__ a, int64_t m, int nrh
     for (int r = threadIdx.x; r < nb; r += blockDim.x) X[k0 + r] = xs[r];
 }
 
-// Backward, one panel: U11 (non-unit upper).
+// Linv = L11^{-1} for the unit lower triangle of panel [k0, k0+nb) of every
+// matrix (column-major nb x nb per matrix).  One CTA per matrix, thread j
+// forms column j by forward substitution against e_j; the columns being built
+// live in shared memory (nb*nb complex), L11 is read through the cache.
 template <class T>
-__global__ void bwd_panel_kernel2(const Cx<T> *__restrict__ a, int64_t m, int nrhs, int k0, int nb,
-                                  Cx<T> *__restrict__ x) {
-    const int f = blockIdx.x / nrhs;
+__global__ void tri_inverse_kernel(const Cx<T> *__restrict__ a, int64_t m, int k0, int nb, Cx<T> *__restrict__ linv) {
+    extern __shared__ unsigned char smem_raw[];
+    Cx<T> *X = reinterpret_cast<Cx<T> *>(smem_raw);  // X[r * nb + j]
+    const int f = blockIdx.x;
     const Cx<T> *A = a + (int64_t)f * m * m;
-    Cx<T> *X = x + (int64_t)blockIdx.x * m;
-    __shared__ Cx<T> xs[128];
-    for (int r = threadIdx.x; r < nb; r += blockDim.x) xs[r] = X[k0 + r];
-    __syncthreads();
-    for (int k = nb - 1; k >= 0; --k) {
-        if (threadIdx.x == 0) xs[k] = cdiv(xs[k], A[(k0 + k) + (int64_t)(k0 + k) * m]);
-        __syncthreads();
-        Cx<T> xk = xs[k];
-        for (int r = threadIdx.x; r < k; r += blockDim.x) {
-            Cx<T> y = xs[r];
-            csubmul(y, xk, A[(k0 + r) + (int64_t)(k0 + k) * m]);
-            xs[r] = y;
+    const int j = threadIdx.x;
+    if (j < nb) {
+        for (int r = 0; r < nb; ++r) {
+            Cx<T> v{(T)0, (T)0};
+            if (r == j) {
+                v.re = (T)1;
+            } else if (r > j) {
+                Cx<T> acc{(T)0, (T)0};
+                for (int k = j; k < r; ++k) {
+                    const Cx<T> l = A[(k0 + r) + (int64_t)(k0 + k) * m];
+                    const Cx<T> xv = X[k * nb + j];
+                    acc.re += l.re * xv.re - l.im * xv.im;
+                    acc.im += l.re * xv.im + l.im * xv.re;
+                }
+                v = Cx<T>{-acc.re, -acc.im};
+            }
+            X[r * nb + j] = v;
         }
-        __syncthreads();
     }
-    for (int r = threadIdx.x; r < nb; r += blockDim.x) X[k0 + r] = xs[r];
+    __syncthreads();
+    Cx<T> *out = linv + (int64_t)f * nb * nb;
+    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+        const int r = idx % nb, c = idx / nb;
+        out[r + c * nb] = X[r * nb + c];
+    }
+}
+
+// C = A B (assign) or C -= A B for general strided complex operands, SIMT.
+// Tile 64 x 64, K <= 64 staged whole in shared memory; 256 threads, 4 x 4
+// outputs each.  In the assign form C may alias B when M <= 64.
+template <class T>
+struct SimtArgs {
+    const Cx<T> *A;
+    int64_t lda, sA;
+    const Cx<T> *B;
+    int64_t ldb, sB;
+    Cx<T> *C;
+    int64_t ldc, sC;
+    int64_t M, N;
+    int K;
+    int assign;
+};
+
+template <class T>
+__global__ void __launch_bounds__(256) gemm_simt_kernel(SimtArgs<T> g) {
+    extern __shared__ unsigned char smem_raw[];
+    Cx<T> *Ls = reinterpret_cast<Cx<T> *>(smem_raw);  // [K][64]
+    Cx<T> *Us = Ls + g.K * 64;                         // [K][64]
+    const int f = blockIdx.z;
+    const Cx<T> *Aop = g.A + (int64_t)f * g.sA;
+    const Cx<T> *Bop = g.B + (int64_t)f * g.sB;
+    Cx<T> *C = g.C + (int64_t)f * g.sC;
+    const int64_t i0 = (int64_t)blockIdx.y * 64, j0 = (int64_t)blockIdx.x * 64;
+    const int tid = threadIdx.x, K = g.K;
+    for (int idx = tid; idx < K * 64; idx += 256) {
+        const int ii = idx % 64, k = idx / 64;
+        Ls[k * 64 + ii] = i0 + ii < g.M ? Aop[(i0 + ii) + (int64_t)k * g.lda] : Cx<T>{0, 0};
+        const int kk = idx % K, jj = idx / K;
+        Us[kk * 64 + jj] = j0 + jj < g.N ? Bop[kk + (j0 + jj) * g.ldb] : Cx<T>{0, 0};
+    }
+    __syncthreads();
+    const int tx = tid & 15, ty = tid >> 4;
+    T accr[4][4], acci[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) accr[r][c] = acci[r][c] = (T)0;
+    for (int k = 0; k < K; ++k) {
+        Cx<T> l[4], u[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) l[r] = Ls[k * 64 + tx + 16 * r];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) u[c] = Us[k * 64 + ty + 16 * c];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                accr[r][c] += l[r].re * u[c].re - l[r].im * u[c].im;
+                acci[r][c] += l[r].re * u[c].im + l[r].im * u[c].re;
+            }
+    }
+    if (g.assign) __syncthreads();  // every B load of this CTA precedes any C store
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int64_t col = j0 + ty + 16 * c;
+        if (col >= g.N) continue;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int64_t row = i0 + tx + 16 * r;
+            if (row >= g.M) continue;
+            Cx<T> *p = C + row + col * g.ldc;
+            if (g.assign) {
+                *p = Cx<T>{accr[r][c], acci[r][c]};
+            } else {
+                Cx<T> y = *p;
+                y.re -= accr[r][c];
+                y.im -= acci[r][c];
+                *p = y;
+            }
+        }
+    }
 }
 
 // x[r] -= sum_c A[r, k0 + c] x[k0 + c] for r in [r0, r1).
@@ -510,7 +637,11 @@ fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaS
     C *a = reinterpret_cast<C *>(b.a);
     const int64_t m = b.m;
     if (m == 0 || b.count == 0) return FH_OK;
-    if (nb > 64 || nb < 1) return fail(err, FH_ERR_INVALID_ARGUMENT, "panel width must be in 1..64");
+    // Shared-memory budget of the TRSM / SIMT update kernels: 64 columns in
+    // FP64, 128 in FP32.
+    const int nb_max = sizeof(T) == 8 ? 64 : 128;
+    if (nb > nb_max || nb < 1)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "panel width must be in 1.." + std::to_string(nb_max));
     const size_t trsm_smem = sizeof(C) * (size_t)nb * (nb + 64);
     const size_t gemm_smem = sizeof(C) * (size_t)nb * 128;
     FHB_CUDA(cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
@@ -518,7 +649,11 @@ fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaS
     for (int64_t k0 = 0; k0 < m; k0 += nb) {
         const int w_nb = (int)std::min<int64_t>(nb, m - k0);
         prof_begin(s, FH_PROF_PANEL);
-        for (int c = 0; c < w_nb; ++c) {
+        if (w.coop) {
+            fh_status st = panel_coop<T>(b, k0, w_nb, *w.coop, s, err);
+            if (st) return st;
+        }
+        for (int c = 0; c < w_nb && !w.coop; ++c) {
             const int j = (int)(k0 + c);
             const int chunks = std::min(w.max_chunks, (int)((m - j + 1023) / 1024));
             pivot_kernel<T><<<dim3(chunks, b.count), 256, 0, s>>>(a, m, j, (int)k0, w_nb, b.pivots, b.singular,
@@ -534,7 +669,27 @@ fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaS
         const int64_t ncols = m - c0;
         prof_begin(s, FH_PROF_TRSM);
         swap_kernel<T><<<dim3(grid_for(ncols, 256, 1024), b.count), 256, 0, s>>>(a, m, (int)k0, w_nb, c0, b.pivots);
-        trsm_kernel<T><<<dim3((unsigned)((ncols + 63) / 64), b.count), 64, trsm_smem, s>>>(a, m, (int)k0, w_nb);
+        const bool tc_apply = mode == TrailingUpdate::TensorBf16x3 && sizeof(T) == 4 && w_nb % 16 == 0;
+        if (w.linv && (tc_apply || w_nb <= 64)) {
+            // U12 = L11^{-1} A12 as an explicit triangular inverse times A12:
+            // the product runs as a GEMM (tensor cores in the mixed form).
+            C *linv = reinterpret_cast<C *>(w.linv);
+            const size_t inv_smem = sizeof(C) * (size_t)w_nb * w_nb;
+            FHB_CUDA(cudaFuncSetAttribute(tri_inverse_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)inv_smem));
+            tri_inverse_kernel<T><<<b.count, std::max(32, ((w_nb + 31) / 32) * 32), inv_smem, s>>>(a, m, (int)k0,
+                                                                                                  w_nb, linv);
+            if (tc_apply) {
+                fh_status st = gemm_tc_tri_apply(reinterpret_cast<const float *>(w.linv), w_nb,
+                                                 reinterpret_cast<float *>(b.a), m, b.count, k0, s, err);
+                if (st) return st;
+            } else {
+                fh_status st = gemm_simt_assign<T>(linv, w_nb, b.a, m, b.count, k0, w_nb, s, err);
+                if (st) return st;
+            }
+        } else {
+            trsm_kernel<T><<<dim3((unsigned)((ncols + 63) / 64), b.count), 64, trsm_smem, s>>>(a, m, (int)k0, w_nb);
+        }
         prof_end(s, FH_PROF_TRSM, 4.0 * (double)w_nb * w_nb * ncols * b.count);
         // complex GEMM: 8 real flops per complex multiply-add
         const double flops = 8.0 * (double)ncols * (double)ncols * (double)w_nb * (double)b.count;
@@ -553,6 +708,7 @@ fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaS
         FHB_CUDA(cudaGetLastError());
     }
     FHB_CUDA(cudaGetLastError());
+    if (w.coop) return coop_check(*w.coop, s, err);
     return FH_OK;
 }
 
@@ -568,6 +724,40 @@ fh_status gemm_simt_update(T *av, int64_t m, int count, int64_t k0, int nb, cuda
     FHB_CUDA(cudaGetLastError());
     return FH_OK;
 }
+// U12 = Linv A12 for the panel [k0, k0+nb): C aliases B (rows k0..k0+nb of
+// the columns right of the panel); nb <= 64 so that one CTA row covers M.
+template <class T>
+fh_status gemm_simt_assign(const void *linv, int nb, T *av, int64_t m, int count, int64_t k0, int K, cudaStream_t s,
+                           fh_error_info *err) {
+    const int64_t c0 = k0 + nb;
+    if (c0 >= m) return FH_OK;
+    if (nb > 64) return fail(err, FH_ERR_INVALID_ARGUMENT, "SIMT triangular apply needs nb <= 64");
+    Cx<T> *A = reinterpret_cast<Cx<T> *>(av);
+    SimtArgs<T> g;
+    g.A = reinterpret_cast<const Cx<T> *>(linv);
+    g.lda = nb;
+    g.sA = (int64_t)nb * nb;
+    g.B = A + k0 + c0 * m;
+    g.ldb = m;
+    g.sB = m * m;
+    g.C = A + k0 + c0 * m;
+    g.ldc = m;
+    g.sC = m * m;
+    g.M = nb;
+    g.N = m - c0;
+    g.K = K;
+    g.assign = 1;
+    const size_t smem = sizeof(Cx<T>) * (size_t)K * 128;
+    FHB_CUDA(cudaFuncSetAttribute(gemm_simt_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    gemm_simt_kernel<T><<<dim3((unsigned)((g.N + 63) / 64), 1, count), 256, smem, s>>>(g);
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+template fh_status gemm_simt_assign<float>(const void *, int, float *, int64_t, int, int64_t, int, cudaStream_t,
+                                           fh_error_info *);
+template fh_status gemm_simt_assign<double>(const void *, int, double *, int64_t, int, int64_t, int, cudaStream_t,
+                                            fh_error_info *);
+
 template fh_status gemm_simt_update<float>(float *, int64_t, int, int64_t, int, cudaStream_t, fh_error_info *);
 template fh_status gemm_simt_update<double>(double *, int64_t, int, int64_t, int, cudaStream_t, fh_error_info *);
 
@@ -579,10 +769,14 @@ fh_status lu_solve(const LuBatch<T> &b, T *xv, int nrhs, int nb, cudaStream_t s,
     const int64_t m = b.m;
     if (m == 0) return FH_OK;
     const int groups = b.count * nrhs;
+    const size_t fwd_smem = sizeof(C) * ((size_t)nb * nb + 3 * (size_t)nb) + 2 * sizeof(int) * (size_t)nb;
+    const size_t bwd_smem = sizeof(C) * ((size_t)nb * nb + (size_t)nb);
+    FHB_CUDA(cudaFuncSetAttribute(fwd_panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
+    FHB_CUDA(cudaFuncSetAttribute(bwd_panel_kernel2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem));
     prof_begin(s, FH_PROF_SOLVE);
     for (int64_t k0 = 0; k0 < m; k0 += nb) {
         const int w_nb = (int)std::min<int64_t>(nb, m - k0);
-        fwd_panel_kernel<T><<<groups, 64, 0, s>>>(a, m, nrhs, (int)k0, w_nb, b.pivots, x);
+        fwd_panel_kernel<T><<<groups, 128, fwd_smem, s>>>(a, m, nrhs, (int)k0, w_nb, b.pivots, x);
         if (k0 + w_nb < m)
             gemv_update_kernel<T><<<dim3(grid_for(m - k0 - w_nb, 256, 64), groups), 256, 0, s>>>(
                 a, m, nrhs, (int)k0, w_nb, k0 + w_nb, m, x);
@@ -590,7 +784,7 @@ fh_status lu_solve(const LuBatch<T> &b, T *xv, int nrhs, int nb, cudaStream_t s,
     const int64_t last = ((m - 1) / nb) * nb;
     for (int64_t k0 = last; k0 >= 0; k0 -= nb) {
         const int w_nb = (int)std::min<int64_t>(nb, m - k0);
-        bwd_panel_kernel2<T><<<groups, 64, 0, s>>>(a, m, nrhs, (int)k0, w_nb, x);
+        bwd_panel_kernel2<T><<<groups, 128, bwd_smem, s>>>(a, m, nrhs, (int)k0, w_nb, x);
         if (k0 > 0)
             gemv_update_kernel<T><<<dim3(grid_for(k0, 256, 64), groups), 256, 0, s>>>(a, m, nrhs, (int)k0, w_nb, 0,
                                                                                       k0, x);

@@ -20,13 +20,40 @@ struct LuBatch {
     int count = 0;
 };
 
-// Workspace for the factorization (pivot search partials).
+// Scratch of the cooperative panel factorization (fh_panel.cu).
+struct CoopScratch {
+    unsigned *barrier = nullptr;  // arrivals, generation
+    int *error = nullptr;         // set when a bounded grid barrier gives up
+    double *cand_val = nullptr;   // pivot candidates, count * per_matrix * 2
+    int *cand_row = nullptr;
+    void *cand_data = nullptr;    // candidate rows, count * per_matrix * 2 * 128 complex
+    void *rowj = nullptr;         // row j of each matrix, count * 2 * 128 complex
+    int per_matrix = 0;           // CTAs per matrix
+};
+
+// Workspace for the factorization (pivot search partials).  With `coop`
+// set, panels are factored by the cooperative kernel; without it, one column
+// at a time (pivot search + rank-1 update launches).
 struct LuWork {
     double *partial_val = nullptr;
     int *partial_idx = nullptr;
     unsigned *tickets = nullptr;
     int max_chunks = 0;
+    const CoopScratch *coop = nullptr;
+    // count * nb * nb complex T: with it, U12 = L11^{-1} A12 is formed from
+    // the explicit triangular inverse and a GEMM; without it, by the
+    // column-at-a-time TRSM kernel.
+    void *linv = nullptr;
 };
+
+// Cooperative panel: sizing, binding of a scratch block, launch, error check.
+template <class T>
+fh_status coop_plan(int count, int64_t m, int *per_matrix, size_t *bytes, fh_error_info *err);
+template <class T>
+void coop_bind(void *mem, int count, int per_matrix, CoopScratch &cs);
+template <class T>
+fh_status panel_coop(LuBatch<T> &b, int64_t K0, int nb, const CoopScratch &cs, cudaStream_t s, fh_error_info *err);
+fh_status coop_check(const CoopScratch &cs, cudaStream_t s, fh_error_info *err);
 
 // How the trailing update A22 -= L21 U12 is computed for the FP32 form.
 enum class TrailingUpdate { Simt, TensorBf16x3 };
@@ -42,6 +69,12 @@ fh_status gemm_tc_check(fh_error_info *err);
 // One SIMT trailing update (FP32 or FP64), for tests.
 template <class T>
 fh_status gemm_simt_update(T *a, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err);
+// U12 = Linv A12 of panel [k0, k0+nb) in place (tensor cores / SIMT).
+fh_status gemm_tc_tri_apply(const float *linv, int nb, float *a, int64_t m, int count, int64_t k0, cudaStream_t s,
+                            fh_error_info *err);
+template <class T>
+fh_status gemm_simt_assign(const void *linv, int nb, T *a, int64_t m, int count, int64_t k0, int K, cudaStream_t s,
+                           fh_error_info *err);
 
 // Solve with the factors in place: x (count x m x nrhs, column-major per
 // matrix, stride m*nrhs) is overwritten.

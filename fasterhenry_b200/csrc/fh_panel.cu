@@ -1,0 +1,343 @@
+// Cooperative panel factorization: one launch factors an outer panel of NB
+// (<= 128) columns of every matrix of the batch with partial pivoting.
+//
+// Each CTA owns a contiguous slice of the panel's rows of one matrix
+// (per_matrix CTAs per matrix, all CTAs co-resident: cooperative launch).
+// The panel is factored in sub-panels of 16 columns:
+//
+//   per column j:   local arg-max of |re| + |im| over the CTA's rows, published
+//                   with the candidate row's NB values (and row j's, by its
+//                   owner) into a buffer double-buffered by the parity of j;
+//                   one grid barrier; every CTA picks the pivot (largest, then
+//                   first row, as dense.rs:157-166), the owners of rows j and p
+//                   exchange them across all NB panel columns, and each CTA
+//                   scales and rank-1-updates its own rows inside the sub-panel.
+//   per sub-panel:  barrier; U12 of the sub-panel (L11^-1 A12 over the rest of
+//                   the outer panel) by slice 0 of each matrix; barrier; each
+//                   CTA updates its own rows of the rest of the outer panel
+//                   (a tall GEMM with K = 16).
+//
+// The rank-1 traffic therefore stays inside 16 columns, and one launch
+// replaces the 2 x NB launches of a column-at-a-time panel.  Row interchanges
+// cover every column of the outer panel, so the forward substitution can
+// apply one outer panel's interchanges at a time.  Grid barriers are bounded:
+// a barrier that gives up sets the error flag and every CTA returns.
+#include <climits>
+
+#include "fh_cx.cuh"
+#include "fh_lu.cuh"
+
+namespace fhb {
+namespace {
+
+constexpr int kW = 16;         // sub-panel width
+constexpr int kNbMax = 128;    // outer panel width limit
+constexpr int kThreads = 256;
+constexpr long long kBarrierSpin = 1LL << 22;
+
+struct CoopArgs {
+    unsigned *barrier;
+    int *error;
+    double *cand_val;
+    int *cand_row;
+    void *cand_data;
+    void *rowj;
+    int per_matrix;
+};
+
+// Sense-reversing grid barrier with a bounded wait.
+__device__ bool grid_barrier(unsigned *bar, int *error) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *vgen = bar + 1;
+        const unsigned gen = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(bar, 1u);
+        int ok = 1;
+        if (arrived == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long i = 0;
+            while (*vgen == gen) {
+                if (++i > kBarrierSpin || *(volatile int *)error) {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        if (!ok) atomicExch(error, 1);
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) panel_coop_kernel(Cx<T> *__restrict__ a, int64_t m, int64_t K0, int NB,
+                                                              int *__restrict__ pivots, int *__restrict__ singular,
+                                                              CoopArgs args) {
+    const int per_matrix = args.per_matrix;
+    const int f = blockIdx.x / per_matrix, slice = blockIdx.x % per_matrix;
+    Cx<T> *A = a + (int64_t)f * m * m;
+    const int64_t rows_total = m - K0;
+    const int64_t chunk = (rows_total + per_matrix - 1) / per_matrix;
+    const int64_t r_begin = K0 + (int64_t)slice * chunk;
+    const int64_t r_end = min(m, r_begin + chunk);
+    Cx<T> *cand_data = reinterpret_cast<Cx<T> *>(args.cand_data);
+    Cx<T> *rowj_buf = reinterpret_cast<Cx<T> *>(args.rowj);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    __shared__ Cx<T> P[kNbMax];
+    __shared__ Cx<T> Rj[kNbMax];
+    __shared__ Cx<T> U[kW][kNbMax];
+    __shared__ double s_val[kThreads / 32];
+    __shared__ int s_idx[kThreads / 32];
+    __shared__ int s_best_slot, s_piv;
+
+    auto better = [](double v2, int i2, double v1, int i1) { return v2 > v1 || (v2 == v1 && i2 < i1); };
+
+    for (int s0 = 0; s0 < NB; s0 += kW) {
+        const int w = min(kW, NB - s0);
+        const int64_t k0 = K0 + s0;
+        for (int c = 0; c < w; ++c) {
+            const int64_t j = k0 + c;
+            const int par = (int)(j & 1);
+            // 1. local arg-max over the CTA's rows i >= j
+            double best = -1.0;
+            int bi = INT_MAX;
+            for (int64_t i = max(r_begin, j) + tid; i < r_end; i += kThreads) {
+                const Cx<T> v = ldcg(A + i + j * m);
+                const double n1 = (double)(fabs(v.re) + fabs(v.im));
+                if (n1 > best || (n1 == best && (int)i < bi)) {
+                    best = n1;
+                    bi = (int)i;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double v2 = __shfl_down_sync(0xffffffffu, best, o);
+                const int i2 = __shfl_down_sync(0xffffffffu, bi, o);
+                if (better(v2, i2, best, bi)) {
+                    best = v2;
+                    bi = i2;
+                }
+            }
+            if (lane == 0) {
+                s_val[warp] = best;
+                s_idx[warp] = bi;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                for (int q = 1; q < kThreads / 32; ++q)
+                    if (better(s_val[q], s_idx[q], best, bi)) {
+                        best = s_val[q];
+                        bi = s_idx[q];
+                    }
+                const int slot = (f * per_matrix + slice) * 2 + par;
+                args.cand_val[slot] = best;
+                args.cand_row[slot] = bi == INT_MAX ? -1 : bi;
+                s_idx[0] = bi;
+            }
+            __syncthreads();
+            {
+                const int brow = s_idx[0];
+                const int slot = (f * per_matrix + slice) * 2 + par;
+                if (brow != INT_MAX)
+                    for (int t = tid; t < NB; t += kThreads)
+                        cand_data[(int64_t)slot * kNbMax + t] = ldcg(A + brow + (K0 + t) * m);
+                if (j >= r_begin && j < r_end)
+                    for (int t = tid; t < NB; t += kThreads)
+                        rowj_buf[(int64_t)(f * 2 + par) * kNbMax + t] = ldcg(A + j + (K0 + t) * m);
+            }
+            // 2. every CTA's candidate is published
+            if (!grid_barrier(args.barrier, args.error)) return;
+            // 3. the pivot (warp 0 reduces the candidates of this matrix), and
+            //    the interchange of rows j and p
+            double bv = -1.0;
+            int brow = INT_MAX, bslot = -1;
+            if (warp == 0) {
+                for (int q = lane; q < per_matrix; q += 32) {
+                    const int slot = (f * per_matrix + q) * 2 + par;
+                    const double v2 = __ldcg(args.cand_val + slot);
+                    const int r2 = __ldcg(args.cand_row + slot);
+                    if (r2 >= 0 && better(v2, r2, bv, brow)) {
+                        bv = v2;
+                        brow = r2;
+                        bslot = slot;
+                    }
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double v2 = __shfl_down_sync(0xffffffffu, bv, o);
+                    const int r2 = __shfl_down_sync(0xffffffffu, brow, o);
+                    const int s2 = __shfl_down_sync(0xffffffffu, bslot, o);
+                    if (s2 >= 0 && better(v2, r2, bv, brow)) {
+                        bv = v2;
+                        brow = r2;
+                        bslot = s2;
+                    }
+                }
+            }
+            if (tid == 0) {  // lane 0 of warp 0 holds the reduced candidate
+                int p = (int)j;
+                if (bv == 0.0) {
+                    if (slice == 0) singular[f] = 1;  // exactly zero pivot (dense.rs:166-168)
+                    bslot = -1;
+                } else if (bv > 0.0) {
+                    p = brow;
+                } else {
+                    bslot = -1;  // all-NaN column: keep the diagonal
+                }
+                if (p == (int)j) bslot = -1;
+                s_piv = p;
+                s_best_slot = bslot;
+                if (slice == 0) pivots[(int64_t)f * m + j] = p;
+            }
+            __syncthreads();
+            const int p = s_piv, pslot = s_best_slot;
+            for (int t = tid; t < NB; t += kThreads) {
+                const Cx<T> rj = ldcg(rowj_buf + (int64_t)(f * 2 + par) * kNbMax + t);
+                Rj[t] = rj;
+                P[t] = pslot >= 0 ? ldcg(cand_data + (int64_t)pslot * kNbMax + t) : rj;
+            }
+            __syncthreads();
+            if (p != (int)j) {
+                if (p >= r_begin && p < r_end)
+                    for (int t = tid; t < NB; t += kThreads) A[p + (K0 + t) * m] = Rj[t];
+                if (j >= r_begin && j < r_end)
+                    for (int t = tid; t < NB; t += kThreads) A[j + (K0 + t) * m] = P[t];
+            }
+            __syncthreads();
+            // 4. scale by the pivot's reciprocal and rank-1 update inside the sub-panel
+            const Cx<T> one{(T)1, (T)0};
+            const Cx<T> inv = cdiv(one, P[s0 + c]);
+            for (int64_t i = max(r_begin, j + 1) + tid; i < r_end; i += kThreads) {
+                Cx<T> l = cmul(ldcg(A + i + j * m), inv);
+                A[i + j * m] = l;
+                for (int cc = c + 1; cc < w; ++cc) {
+                    Cx<T> y = ldcg(A + i + (k0 + cc) * m);
+                    csubmul(y, P[s0 + cc], l);
+                    A[i + (k0 + cc) * m] = y;
+                }
+            }
+        }
+        const int rest = NB - s0 - w;  // outer-panel columns right of the sub-panel
+        if (rest <= 0) continue;
+        // 5. the sub-panel is final everywhere
+        if (!grid_barrier(args.barrier, args.error)) return;
+        // 6. U12 of the sub-panel: rows [k0, k0+w), columns [k0+w, K0+NB)
+        if (slice == 0) {
+            for (int t = tid; t < rest; t += kThreads) {
+                const int64_t col = k0 + w + t;
+                Cx<T> x[kW];
+#pragma unroll
+                for (int r = 0; r < kW; ++r)
+                    if (r < w) x[r] = ldcg(A + (k0 + r) + col * m);
+#pragma unroll
+                for (int k = 0; k < kW; ++k) {
+                    if (k >= w) break;
+#pragma unroll
+                    for (int r = k + 1; r < kW; ++r)
+                        if (r < w) csubmul(x[r], x[k], ldcg(A + (k0 + r) + (k0 + k) * m));
+                }
+#pragma unroll
+                for (int r = 0; r < kW; ++r)
+                    if (r < w) A[(k0 + r) + col * m] = x[r];
+            }
+        }
+        // 7. U12 is visible to every CTA
+        if (!grid_barrier(args.barrier, args.error)) return;
+        // 8. own rows i >= k0+w: A[i, k0+w ..] -= A[i, k0 .. k0+w) U12
+        for (int idx = tid; idx < w * rest; idx += kThreads) {
+            const int r = idx / rest, t = idx % rest;
+            U[r][t] = ldcg(A + (k0 + r) + (k0 + w + t) * m);
+        }
+        __syncthreads();
+        for (int64_t i = max(r_begin, k0 + w) + tid; i < r_end; i += kThreads) {
+            Cx<T> l[kW];
+#pragma unroll
+            for (int r = 0; r < kW; ++r) l[r] = r < w ? ldcg(A + i + (k0 + r) * m) : Cx<T>{0, 0};
+            for (int t = 0; t < rest; ++t) {
+                Cx<T> y = ldcg(A + i + (k0 + w + t) * m);
+#pragma unroll
+                for (int r = 0; r < kW; ++r)
+                    if (r < w) csubmul(y, l[r], U[r][t]);
+                A[i + (k0 + w + t) * m] = y;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+template <class T>
+fh_status coop_plan(int count, int64_t m, int *per_matrix, size_t *bytes, fh_error_info *err) {
+    int dev = 0, sms = 0, occ = 0, coop = 0;
+    FHB_CUDA(cudaGetDevice(&dev));
+    FHB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    FHB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    if (!coop) return fail(err, FH_ERR_NO_DEVICE, "the device does not support cooperative launches");
+    FHB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_coop_kernel<T>, kThreads, 0));
+    const int capacity = occ * sms;
+    int pm = std::max(1, capacity / std::max(1, count));
+    pm = (int)std::min<int64_t>(pm, std::max<int64_t>(1, (m + 63) / 64));
+    if ((int64_t)pm * count > capacity)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "batch too large for one cooperative panel launch");
+    *per_matrix = pm;
+    const size_t slots = (size_t)count * pm * 2;
+    *bytes = 64 + 16 + slots * 8 + slots * 4 + slots * kNbMax * sizeof(Cx<T>) + (size_t)count * 2 * kNbMax * sizeof(Cx<T>) +
+             256;
+    return FH_OK;
+}
+
+template <class T>
+void coop_bind(void *mem, int count, int per_matrix, CoopScratch &cs) {
+    unsigned char *p = static_cast<unsigned char *>(mem);
+    const size_t slots = (size_t)count * per_matrix * 2;
+    cs.barrier = reinterpret_cast<unsigned *>(p);
+    cs.error = reinterpret_cast<int *>(p + 16);
+    size_t off = 64;
+    cs.cand_val = reinterpret_cast<double *>(p + off);
+    off += slots * 8;
+    cs.cand_row = reinterpret_cast<int *>(p + off);
+    off += slots * 4;
+    off = (off + 15) & ~(size_t)15;
+    cs.cand_data = p + off;
+    off += slots * kNbMax * sizeof(Cx<T>);
+    cs.rowj = p + off;
+    cs.per_matrix = per_matrix;
+}
+
+template <class T>
+fh_status panel_coop(LuBatch<T> &b, int64_t K0, int nb, const CoopScratch &cs, cudaStream_t s, fh_error_info *err) {
+    if (nb > kNbMax) return fail(err, FH_ERR_INVALID_ARGUMENT, "cooperative panel wider than 128 columns");
+    FHB_CUDA(cudaMemsetAsync(cs.barrier, 0, 64, s));  // barrier counters and error flag
+    CoopArgs args{cs.barrier, cs.error, cs.cand_val, cs.cand_row, cs.cand_data, cs.rowj, cs.per_matrix};
+    Cx<T> *a = reinterpret_cast<Cx<T> *>(b.a);
+    int64_t m = b.m;
+    void *params[] = {&a, &m, &K0, &nb, &b.pivots, &b.singular, &args};
+    FHB_CUDA(cudaLaunchCooperativeKernel((const void *)panel_coop_kernel<T>, dim3(cs.per_matrix * b.count), dim3(kThreads),
+                                         params, 0, s));
+    return FH_OK;
+}
+
+fh_status coop_check(const CoopScratch &cs, cudaStream_t s, fh_error_info *err) {
+    int flag = 0;
+    FHB_CUDA(cudaMemcpyAsync(&flag, cs.error, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FHB_CUDA(cudaStreamSynchronize(s));
+    if (flag) return fail(err, FH_ERR_DEVICE_TIMEOUT, "a panel grid barrier ran out of its iteration limit");
+    return FH_OK;
+}
+
+template fh_status coop_plan<double>(int, int64_t, int *, size_t *, fh_error_info *);
+template fh_status coop_plan<float>(int, int64_t, int *, size_t *, fh_error_info *);
+template void coop_bind<double>(void *, int, int, CoopScratch &);
+template void coop_bind<float>(void *, int, int, CoopScratch &);
+template fh_status panel_coop<double>(LuBatch<double> &, int64_t, int, const CoopScratch &, cudaStream_t, fh_error_info *);
+template fh_status panel_coop<float>(LuBatch<float> &, int64_t, int, const CoopScratch &, cudaStream_t, fh_error_info *);
+
+}  // namespace fhb

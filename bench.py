@@ -47,6 +47,18 @@ METRIC = "Z(ω) sweep s at 10k filaments×32 freqs: mixed+IR vs FP64 LU at ≤1e
 UNIT = "s"
 
 
+def _workload(name):
+    from fasterhenry_b200 import fixtures as F
+    return {"metric": F.metric_meander, "c2": F.c2_meander, "c1": F.c1_spiral}[name]()
+
+
+WORKLOADS = {
+    "metric": ("meander 167 legs, 10,020 filaments, m = 9,686, 32 freqs 1e5-1e10 Hz", lambda: _workload("metric")),
+    "c2": ("meander 40 legs, 2,400 filaments, m = 2,320, 32 freqs 1e5-1e10 Hz", lambda: _workload("c2")),
+    "c1": ("4-turn spiral, 240 filaments, m = 224, 10 freqs 1e6-1e10 Hz", lambda: _workload("c1")),
+}
+
+
 def _peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -154,7 +166,7 @@ def run_ours(args):
     from fasterhenry_b200 import fixtures as F
     from fasterhenry_b200 import _native as N
 
-    deck, freqs = F.metric_meander()
+    deck, freqs = WORKLOADS[args.config][1]()
     geometry = fh.Geometry.from_deck(deck)
     system = fh.MeshSystem.assemble(geometry, deck.ports, deck.discretization)
     counts = system.counts()
@@ -240,7 +252,7 @@ def run_ours(args):
         "metric": METRIC, "value": round(step_max, 6), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(step_max * 1e3, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "c64+bf16x3 (FP64 residual)", "data": "synthetic",
-        "config": {"workload": "meander 167 legs, 10,020 filaments, m = 9,686, 32 freqs 1e5-1e10 Hz",
+        "config": {"workload": WORKLOADS[args.config][0],
                    "filaments": counts["filaments"], "internal_meshes": counts["internal_meshes"],
                    "frequencies": len(freqs), "precision": "mixed_bf16x3_ir", "l2": "inputs 24 GB >> L2 (no flush)",
                    "parallelism": "replicas" if world > 1 else "single"},
@@ -332,6 +344,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--ref-legs", type=int, default=40, help="meander legs of the reference arm's sample")
+    ap.add_argument("--config", default="metric", choices=sorted(WORKLOADS),
+                    help="workload: the metric's 10k-filament meander (default) or a smaller parity config "
+                         "(used for profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

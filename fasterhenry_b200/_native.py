@@ -97,7 +97,7 @@ EXPORTS = [
     "fh_profile_read",
 ]
 
-PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual"]
+PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner"]
 
 
 class FillStats(ctypes.Structure):

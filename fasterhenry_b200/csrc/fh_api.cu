@@ -100,6 +100,15 @@ constexpr double kTau = 6.283185307179586;
 // C traffic per flop.
 constexpr int kNbFp64 = 64;
 constexpr int kNbFp32 = 128;
+// Super-panel width of the two-level FP32 factorization on the tensor cores:
+// the deep trailing update runs with K = 512, four times the arithmetic per
+// byte of C of a one-panel update.
+constexpr int kOuterFp32 = 512;
+
+// Super-panel width used for an FP32 batch of order m (0: one-level).
+int outer_for(int64_t m, TrailingUpdate mode) {
+    return mode == TrailingUpdate::TensorBf16x3 && m > kOuterFp32 ? kOuterFp32 : 0;
+}
 
 // Factor + solve + Schur for `count` frequencies in FP64.  x_out (count x m x
 // p complex) receives the FP64 solutions; z (count x p x p) the impedances.
@@ -228,9 +237,19 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     FHB_ALLOC(coop_mem, coop_bytes);
     coop_bind<float>(coop_mem.p, count, per_matrix, cs);
     w.coop = &cs;
+    const int outer = outer_for(m, mode);
     DBuf<float> linv_mem;
-    FHB_ALLOC(linv_mem, (size_t)count * kNbFp32 * kNbFp32 * 2);
+    FHB_ALLOC(linv_mem, (size_t)count * kNbFp32 * kNbFp32 * 2 * (outer ? outer / kNbFp32 : 1));
     w.linv = linv_mem.p;
+    DBuf<unsigned char> pack_a, pack_b;
+    if (outer) {
+        const size_t pb = packed_operand_bytes(m - outer, outer, count);
+        FHB_ALLOC(pack_a, pb);
+        FHB_ALLOC(pack_b, pb);
+        w.outer = outer;
+        w.pack_a = pack_a.p;
+        w.pack_b = pack_b.p;
+    }
     LuBatch<float> b;
     b.a = a.p;
     b.pivots = piv.p;
@@ -248,6 +267,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     if (mode == TrailingUpdate::TensorBf16x3) {
         FHB_CUDA(cudaStreamSynchronize(st));
         e = gemm_tc_check(err);
+        if (!e) e = gemm_tc_packed_check(err);
         if (e) return e;
     }
     std::vector<double> hb(count), hd(count), hx(count), hr(count), prev(count, INFINITY);
@@ -257,7 +277,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     int it = 0;
     for (; it < kMaxIter; ++it) {
         e = convert_c64_to_c32(r.p, d32.p, count * vec, st, err);
-        if (!e) e = lu_solve<float>(b, d32.p, (int)p, kNbFp32, st, err);
+        if (!e) e = lu_solve<float>(b, d32.p, (int)p, kNbFp32, st, err, outer);
         if (!e) e = add_c32_to_c64(d_x, d32.p, count * vec, st, err);
         if (!e) e = residual_fp64(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, r.p, rnorm.p, st, err);
         if (e) return e;
@@ -381,11 +401,26 @@ fh_status fh_test_trailing_update(float *a, int64_t m, int32_t count, int64_t k0
     DBuf<float> d;
     FHB_ALLOC(d, bytes / 4);
     FHB_CUDA(cudaMemcpy(d.p, a, bytes, cudaMemcpyHostToDevice));
-    st = mode == 1 ? gemm_tc_update(d.p, m, count, k0, nb, nullptr, err)
-                   : gemm_simt_update<float>(d.p, m, count, k0, nb, nullptr, err);
+    DBuf<unsigned char> pa, pb;
+    if (mode == 2) {
+        if (nb % 16) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update needs nb a multiple of 16");
+        const int64_t base = k0 + nb, rem = m - base;
+        if (rem > 0) {
+            FHB_ALLOC(pa, packed_operand_bytes(rem, nb, count));
+            FHB_ALLOC(pb, packed_operand_bytes(rem, nb, count));
+            float *A = d.p;
+            auto at = [&](int64_t r, int64_t c) { return A + 2 * (r + c * m); };
+            st = gemm_tc_packed_update(at(base, k0), m, m * m, at(k0, base), m, m * m, at(base, base), m, m * m, rem,
+                                       rem, nb, count, pa.p, pb.p, nullptr, err);
+        }
+    } else {
+        st = mode == 1 ? gemm_tc_update(d.p, m, count, k0, nb, nullptr, err)
+                       : gemm_simt_update<float>(d.p, m, count, k0, nb, nullptr, err);
+    }
     if (st) return st;
     FHB_CUDA(cudaDeviceSynchronize());
     st = gemm_tc_check(err);
+    if (!st) st = gemm_tc_packed_check(err);
     if (st) return st;
     FHB_CUDA(cudaMemcpy(a, d.p, bytes, cudaMemcpyDeviceToHost));
     return FH_OK;
@@ -605,7 +640,10 @@ fh_status fh_sweep(fh_system *sys, const double *freqs, size_t nf, fh_precision 
     const bool mixed = precision != FH_PRECISION_FP64;
     const TrailingUpdate update =
         precision == FH_PRECISION_MIXED_BF16X3 ? TrailingUpdate::TensorBf16x3 : TrailingUpdate::Simt;
-    const double per = (mixed ? 8.0 : 16.0) * (double)m * (double)m + 64.0 * (double)(m * p + 64);
+    // Per frequency: the matrix, the vectors, and for the two-level FP32
+    // form its two packed operands (8 bytes per entry of an m x 512 block each).
+    const double per = (mixed ? 8.0 : 16.0) * (double)m * (double)m + 64.0 * (double)(m * p + 64) +
+                       (outer_for(m, update) ? 16.0 * (double)m * kOuterFp32 : 0.0);
     int chunk = (int)std::max(1.0, std::min<double>((double)nf, 0.8 * (double)free_b / std::max(per, 1.0)));
     DBuf<double> d_omega, d_x, d_z;
     FHB_ALLOC(d_omega, (size_t)chunk);

@@ -430,6 +430,26 @@ fh_status gemm_tc_tri_apply(const float *linv, int nb, float *a, int64_t m, int 
     return gemm_tc_launch(g, count, s, err);
 }
 
+fh_status gemm_tc_strided(const float *A, int64_t lda, int64_t sA, const float *B, int64_t ldb, int64_t sB, float *C,
+                          int64_t ldc, int64_t sC, int64_t M, int64_t N, int K, int assign, int count, cudaStream_t s,
+                          fh_error_info *err) {
+    GemmArgs g;
+    g.A = reinterpret_cast<const float2 *>(A);
+    g.lda = lda;
+    g.sA = sA;
+    g.B = reinterpret_cast<const float2 *>(B);
+    g.ldb = ldb;
+    g.sB = sB;
+    g.C = reinterpret_cast<float2 *>(C);
+    g.ldc = ldc;
+    g.sC = sC;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.assign = assign;
+    return gemm_tc_launch(g, count, s, err);
+}
+
 fh_status gemm_tc_check(fh_error_info *err) {
     int dev = 0;
     FHB_CUDA(cudaGetDevice(&dev));

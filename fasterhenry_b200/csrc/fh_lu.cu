@@ -136,14 +136,14 @@ __global__ void __launch_bounds__(256) panel_update_kernel(Cx<T> *__restrict__ a
     }
 }
 
-// Row interchanges of the panel applied to columns [c0, m).
+// Row interchanges of rows [k0, k0+nb), in order, applied to columns [c0, c1).
 template <class T>
 __global__ void __launch_bounds__(256) swap_kernel(Cx<T> *__restrict__ a, int64_t m, int k0, int nb, int64_t c0,
-                                                   const int *__restrict__ pivots) {
+                                                   int64_t c1, const int *__restrict__ pivots) {
     const int f = blockIdx.y;
     Cx<T> *A = a + (int64_t)f * m * m;
     const int *piv = pivots + (int64_t)f * m;
-    for (int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m; c += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += (int64_t)gridDim.x * blockDim.x) {
         Cx<T> *col = A + c * m;
         for (int jj = 0; jj < nb; ++jj) {
             int p = piv[k0 + jj];
@@ -261,6 +261,7 @@ __global__ void __launch_bounds__(256) gemm_update_kernel(Cx<T> *__restrict__ a,
 // interchanges run in order on one thread but only touch shared memory (an
 // interchange with a row below the panel uses the value of that row
 // preloaded in parallel, indexed by its first occurrence in the pivot list).
+// With pivots == nullptr the interchanges were applied by fwd_swap_kernel.
 // Dynamic shared memory: nb*nb complex + 3*nb complex + 2*nb ints.
 template <class T>
 __global__ void __launch_bounds__(128) fwd_panel_kernel(const Cx<T> *__restrict__ a, int64_t m, int nrhs, int k0,
@@ -282,13 +283,73 @@ __global__ void __launch_bounds__(128) fwd_panel_kernel(const Cx<T> *__restrict_
     }
     for (int t = tid; t < nb; t += blockDim.x) {
         xs[t] = X[k0 + t];
-        piv[t] = pivots[(int64_t)f * m + k0 + t];
+        if (pivots) piv[t] = pivots[(int64_t)f * m + k0 + t];
     }
     __syncthreads();
-    for (int t = tid; t < nb; t += blockDim.x) {
+    if (pivots) {
+        for (int t = tid; t < nb; t += blockDim.x) {
+            const int p = piv[t];
+            int fst = t;
+            if (p >= k0 + nb) {
+                for (int q = 0; q < t; ++q)
+                    if (piv[q] == p) {
+                        fst = q;
+                        break;
+                    }
+                if (fst == t) ext[t] = X[p];
+            }
+            first[t] = fst;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            for (int jj = 0; jj < nb; ++jj) {
+                const int p = piv[jj];
+                if (p == k0 + jj) continue;
+                Cx<T> &other = p < k0 + nb ? xs[p - k0] : ext[first[jj]];
+                const Cx<T> tmp = xs[jj];
+                xs[jj] = other;
+                other = tmp;
+            }
+        }
+        __syncthreads();
+        for (int t = tid; t < nb; t += blockDim.x)
+            if (piv[t] >= k0 + nb && first[t] == t) X[piv[t]] = ext[t];
+    }
+    for (int k = 0; k < nb; ++k) {
+        const Cx<T> xk = xs[k];
+        for (int r = k + 1 + tid; r < nb; r += blockDim.x) {
+            Cx<T> y = xs[r];
+            csubmul(y, xk, Ls[r * nb + k]);
+            xs[r] = y;
+        }
+        __syncthreads();
+    }
+    for (int r = tid; r < nb; r += blockDim.x) X[k0 + r] = xs[r];
+}
+
+// Forward, interchanges only: rows [g0, g0+wg) of a swap group, applied in
+// order to x, with the same shared-memory staging as fwd_panel_kernel.
+// Dynamic shared memory: 2*wg complex + 2*wg ints.
+template <class T>
+__global__ void __launch_bounds__(128) fwd_swap_kernel(int64_t m, int nrhs, int g0, int wg,
+                                                       const int *__restrict__ pivots, Cx<T> *__restrict__ x) {
+    extern __shared__ unsigned char smem_raw[];
+    Cx<T> *xs = reinterpret_cast<Cx<T> *>(smem_raw);
+    Cx<T> *ext = xs + wg;
+    int *piv = reinterpret_cast<int *>(ext + wg);
+    int *first = piv + wg;
+    const int f = blockIdx.x / nrhs;
+    Cx<T> *X = x + (int64_t)blockIdx.x * m;
+    const int tid = threadIdx.x;
+    for (int t = tid; t < wg; t += blockDim.x) {
+        xs[t] = X[g0 + t];
+        piv[t] = pivots[(int64_t)f * m + g0 + t];
+    }
+    __syncthreads();
+    for (int t = tid; t < wg; t += blockDim.x) {
         const int p = piv[t];
         int fst = t;
-        if (p >= k0 + nb) {
+        if (p >= g0 + wg) {
             for (int q = 0; q < t; ++q)
                 if (piv[q] == p) {
                     fst = q;
@@ -300,28 +361,20 @@ __global__ void __launch_bounds__(128) fwd_panel_kernel(const Cx<T> *__restrict_
     }
     __syncthreads();
     if (tid == 0) {
-        for (int jj = 0; jj < nb; ++jj) {
+        for (int jj = 0; jj < wg; ++jj) {
             const int p = piv[jj];
-            if (p == k0 + jj) continue;
-            Cx<T> &other = p < k0 + nb ? xs[p - k0] : ext[first[jj]];
+            if (p == g0 + jj) continue;
+            Cx<T> &other = p < g0 + wg ? xs[p - g0] : ext[first[jj]];
             const Cx<T> tmp = xs[jj];
             xs[jj] = other;
             other = tmp;
         }
     }
     __syncthreads();
-    for (int t = tid; t < nb; t += blockDim.x)
-        if (piv[t] >= k0 + nb && first[t] == t) X[piv[t]] = ext[t];
-    for (int k = 0; k < nb; ++k) {
-        const Cx<T> xk = xs[k];
-        for (int r = k + 1 + tid; r < nb; r += blockDim.x) {
-            Cx<T> y = xs[r];
-            csubmul(y, xk, Ls[r * nb + k]);
-            xs[r] = y;
-        }
-        __syncthreads();
+    for (int t = tid; t < wg; t += blockDim.x) {
+        if (piv[t] >= g0 + wg && first[t] == t) X[piv[t]] = ext[t];
+        X[g0 + t] = xs[t];
     }
-    for (int r = tid; r < nb; r += blockDim.x) X[k0 + r] = xs[r];
 }
 
 // Backward, one panel: U11 (non-unit upper), staged in shared memory.
@@ -629,6 +682,95 @@ inline int grid_for(int64_t work, int threads, int cap = 148 * 32) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(g, cap));
 }
 
+// Two-level blocked factorization of an FP32 batch on the tensor cores.
+//
+// For each super-panel [K0, E) of `outer` columns:
+//   for each nb-wide panel [j0, j0+nb) inside it
+//     cooperative panel factorization (rows j0.., its own columns);
+//     its interchanges on the super-panel's other columns;
+//     Linv_j = (unit L_jj)^{-1};  U = Linv_j A[j0 block, j0+nb..E);
+//     A[j0+nb.., j0+nb..E) -= L[j0+nb.., panel] U       (K = nb)
+//   all interchanges of the super-panel, in order, on columns [E, m);
+//   U12 = L11^{-1} A12 block by block (Linv_j, then the rows below it inside
+//   the super-panel);
+//   A22 -= L21 U12 with K = outer from packed operands.
+//
+// The deep update moves the same 16 bytes of C per entry as a one-panel
+// update but does outer/nb times the arithmetic on them, which lifts it off
+// the HBM roofline.  The interchange convention differs from the one-level
+// path only inside a super-panel (all of its L columns carry all of its
+// interchanges), hence lu_solve(group = outer).
+fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, fh_error_info *err) {
+    using C = Cx<float>;
+    C *a = reinterpret_cast<C *>(b.a);
+    const int64_t m = b.m, mm = m * m;
+    const int count = b.count;
+    const int outer = w.outer;
+    if (nb % 16 || nb > 128 || outer % nb || !w.coop || !w.linv || !w.pack_a || !w.pack_b)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "two-level factorization needs nb | outer, nb <= 128 and scratch");
+    const size_t inv_smem = sizeof(C) * (size_t)nb * nb;
+    FHB_CUDA(cudaFuncSetAttribute(tri_inverse_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)inv_smem));
+    auto at = [&](int64_t r, int64_t c) { return b.a + 2 * (r + c * m); };
+    auto swaps = [&](int64_t k0, int n, int64_t c0, int64_t c1) {
+        if (c1 > c0)
+            swap_kernel<float><<<dim3(grid_for(c1 - c0, 256, 1024), count), 256, 0, s>>>(a, m, (int)k0, n, c0, c1,
+                                                                                        b.pivots);
+    };
+    fh_status st = FH_OK;
+    for (int64_t K0 = 0; K0 < m; K0 += outer) {
+        const int W = (int)std::min<int64_t>(outer, m - K0);
+        const int64_t E = K0 + W;
+        for (int64_t j0 = K0; j0 < E; j0 += nb) {
+            const int wj = (int)std::min<int64_t>(nb, E - j0);
+            const int64_t r1 = j0 + wj;  // first row / column after the panel
+            C *linv = reinterpret_cast<C *>(w.linv) + (size_t)((j0 - K0) / nb) * count * nb * nb;
+            prof_begin(s, FH_PROF_PANEL);
+            st = panel_coop<float>(b, j0, wj, *w.coop, s, err);
+            prof_end(s, FH_PROF_PANEL, 0.0);
+            if (st) return st;
+            if (r1 >= m) break;
+            prof_begin(s, FH_PROF_TRSM);
+            swaps(j0, wj, K0, j0);
+            swaps(j0, wj, r1, E);
+            tri_inverse_kernel<float><<<count, std::max(32, ((wj + 31) / 32) * 32), inv_smem, s>>>(a, m, (int)j0, wj,
+                                                                                                 linv);
+            if (r1 < E)
+                st = gemm_tc_strided(reinterpret_cast<const float *>(linv), wj, (int64_t)wj * wj, at(j0, r1), m, mm,
+                                     at(j0, r1), m, mm, wj, E - r1, wj, 1, count, s, err);
+            prof_end(s, FH_PROF_TRSM, 4.0 * (double)wj * wj * (double)(E - r1) * count);
+            if (st) return st;
+            if (r1 < E) {
+                prof_begin(s, FH_PROF_GEMM_TC_INNER);
+                st = gemm_tc_strided(at(r1, j0), m, mm, at(j0, r1), m, mm, at(r1, r1), m, mm, m - r1, E - r1, wj, 0,
+                                     count, s, err);
+                prof_end(s, FH_PROF_GEMM_TC_INNER, 8.0 * (double)(m - r1) * (double)(E - r1) * wj * count);
+                if (st) return st;
+            }
+        }
+        if (E >= m) break;
+        const int64_t n2 = m - E;
+        prof_begin(s, FH_PROF_TRSM);
+        swaps(K0, W, E, m);
+        for (int64_t j0 = K0; j0 < E && !st; j0 += nb) {
+            const C *linv = reinterpret_cast<const C *>(w.linv) + (size_t)((j0 - K0) / nb) * count * nb * nb;
+            st = gemm_tc_strided(reinterpret_cast<const float *>(linv), nb, (int64_t)nb * nb, at(j0, E), m, mm,
+                                 at(j0, E), m, mm, nb, n2, nb, 1, count, s, err);
+            if (!st && j0 + nb < E)
+                st = gemm_tc_strided(at(j0 + nb, j0), m, mm, at(j0, E), m, mm, at(j0 + nb, E), m, mm, E - j0 - nb,
+                                     n2, nb, 0, count, s, err);
+        }
+        prof_end(s, FH_PROF_TRSM, 4.0 * (double)W * W * (double)n2 * count);
+        if (st) return st;
+        st = gemm_tc_packed_update(at(E, K0), m, mm, at(K0, E), m, mm, at(E, E), m, mm, n2, n2, W, count, w.pack_a,
+                                   w.pack_b, s, err);
+        if (st) return st;
+        FHB_CUDA(cudaGetLastError());
+    }
+    FHB_CUDA(cudaGetLastError());
+    return coop_check(*w.coop, s, err);
+}
+
 }  // namespace
 
 template <class T>
@@ -637,6 +779,9 @@ fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaS
     C *a = reinterpret_cast<C *>(b.a);
     const int64_t m = b.m;
     if (m == 0 || b.count == 0) return FH_OK;
+    if constexpr (sizeof(T) == 4) {
+        if (w.outer > nb && mode == TrailingUpdate::TensorBf16x3) return lu_factor_deep(b, w, nb, s, err);
+    }
     // Shared-memory budget of the TRSM / SIMT update kernels: 64 columns in
     // FP64, 128 in FP32.
     const int nb_max = sizeof(T) == 8 ? 64 : 128;
@@ -668,7 +813,8 @@ fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaS
         if (c0 >= m) break;
         const int64_t ncols = m - c0;
         prof_begin(s, FH_PROF_TRSM);
-        swap_kernel<T><<<dim3(grid_for(ncols, 256, 1024), b.count), 256, 0, s>>>(a, m, (int)k0, w_nb, c0, b.pivots);
+        swap_kernel<T><<<dim3(grid_for(ncols, 256, 1024), b.count), 256, 0, s>>>(a, m, (int)k0, w_nb, c0, m,
+                                                                                  b.pivots);
         const bool tc_apply = mode == TrailingUpdate::TensorBf16x3 && sizeof(T) == 4 && w_nb % 16 == 0;
         if (w.linv && (tc_apply || w_nb <= 64)) {
             // U12 = L11^{-1} A12 as an explicit triangular inverse times A12:
@@ -762,24 +908,34 @@ template fh_status gemm_simt_update<float>(float *, int64_t, int, int64_t, int, 
 template fh_status gemm_simt_update<double>(double *, int64_t, int, int64_t, int, cudaStream_t, fh_error_info *);
 
 template <class T>
-fh_status lu_solve(const LuBatch<T> &b, T *xv, int nrhs, int nb, cudaStream_t s, fh_error_info *err) {
+fh_status lu_solve(const LuBatch<T> &b, T *xv, int nrhs, int nb, cudaStream_t s, fh_error_info *err, int group) {
     using C = Cx<T>;
     const C *a = reinterpret_cast<const C *>(b.a);
     C *x = reinterpret_cast<C *>(xv);
     const int64_t m = b.m;
     if (m == 0) return FH_OK;
+    if (group <= nb) group = nb;
+    if (group % nb || group > 4096)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "interchange group must be a multiple of the panel width");
     const int groups = b.count * nrhs;
     const size_t fwd_smem = sizeof(C) * ((size_t)nb * nb + 3 * (size_t)nb) + 2 * sizeof(int) * (size_t)nb;
     const size_t bwd_smem = sizeof(C) * ((size_t)nb * nb + (size_t)nb);
+    const size_t swap_smem = (2 * sizeof(C) + 2 * sizeof(int)) * (size_t)group;
     FHB_CUDA(cudaFuncSetAttribute(fwd_panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
     FHB_CUDA(cudaFuncSetAttribute(bwd_panel_kernel2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem));
+    FHB_CUDA(cudaFuncSetAttribute(fwd_swap_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)swap_smem));
     prof_begin(s, FH_PROF_SOLVE);
-    for (int64_t k0 = 0; k0 < m; k0 += nb) {
-        const int w_nb = (int)std::min<int64_t>(nb, m - k0);
-        fwd_panel_kernel<T><<<groups, 128, fwd_smem, s>>>(a, m, nrhs, (int)k0, w_nb, b.pivots, x);
-        if (k0 + w_nb < m)
-            gemv_update_kernel<T><<<dim3(grid_for(m - k0 - w_nb, 256, 64), groups), 256, 0, s>>>(
-                a, m, nrhs, (int)k0, w_nb, k0 + w_nb, m, x);
+    for (int64_t g0 = 0; g0 < m; g0 += group) {
+        const int wg = (int)std::min<int64_t>(group, m - g0);
+        if (group > nb) fwd_swap_kernel<T><<<groups, 128, swap_smem, s>>>(m, nrhs, (int)g0, wg, b.pivots, x);
+        for (int64_t k0 = g0; k0 < g0 + wg; k0 += nb) {
+            const int w_nb = (int)std::min<int64_t>(nb, g0 + wg - k0);
+            fwd_panel_kernel<T><<<groups, 128, fwd_smem, s>>>(a, m, nrhs, (int)k0, w_nb,
+                                                              group > nb ? nullptr : b.pivots, x);
+            if (k0 + w_nb < m)
+                gemv_update_kernel<T><<<dim3(grid_for(m - k0 - w_nb, 256, 64), groups), 256, 0, s>>>(
+                    a, m, nrhs, (int)k0, w_nb, k0 + w_nb, m, x);
+        }
     }
     const int64_t last = ((m - 1) / nb) * nb;
     for (int64_t k0 = last; k0 >= 0; k0 -= nb) {
@@ -871,8 +1027,8 @@ fh_status max_abs_per_matrix_f32(const float *v, int64_t per, int count, double 
 
 template fh_status lu_factor<double>(LuBatch<double> &, LuWork &, int, TrailingUpdate, cudaStream_t, fh_error_info *);
 template fh_status lu_factor<float>(LuBatch<float> &, LuWork &, int, TrailingUpdate, cudaStream_t, fh_error_info *);
-template fh_status lu_solve<double>(const LuBatch<double> &, double *, int, int, cudaStream_t, fh_error_info *);
-template fh_status lu_solve<float>(const LuBatch<float> &, float *, int, int, cudaStream_t, fh_error_info *);
+template fh_status lu_solve<double>(const LuBatch<double> &, double *, int, int, cudaStream_t, fh_error_info *, int);
+template fh_status lu_solve<float>(const LuBatch<float> &, float *, int, int, cudaStream_t, fh_error_info *, int);
 template fh_status form_system<double>(const double *, const double *, int64_t, int64_t, const double *, int, double *,
                                        cudaStream_t, fh_error_info *);
 template fh_status form_system<float>(const double *, const double *, int64_t, int64_t, const double *, int, float *,

@@ -42,8 +42,19 @@ struct LuWork {
     const CoopScratch *coop = nullptr;
     // count * nb * nb complex T: with it, U12 = L11^{-1} A12 is formed from
     // the explicit triangular inverse and a GEMM; without it, by the
-    // column-at-a-time TRSM kernel.
+    // column-at-a-time TRSM kernel.  With `outer` set it holds outer / nb
+    // such slots (one per panel of a super-panel).
     void *linv = nullptr;
+    // Two-level blocking (FP32 form on the tensor cores): super-panels of
+    // `outer` columns are factored with nb-wide panels and updates confined
+    // to the super-panel; the rest of the matrix then takes one deep update
+    // with K = outer from the packed operands in pack_a / pack_b
+    // (packed_operand_bytes(m, outer, count) each).  Row interchanges of a
+    // panel are applied to every column of its super-panel, so lu_solve must
+    // be called with group = outer.
+    int outer = 0;
+    void *pack_a = nullptr;
+    void *pack_b = nullptr;
 };
 
 // Cooperative panel: sizing, binding of a scratch block, launch, error check.
@@ -66,6 +77,21 @@ fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaS
 fh_status gemm_tc_update(float *a, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err);
 // Reports (and clears) a bounded tensor-core wait that ran out.
 fh_status gemm_tc_check(fh_error_info *err);
+// General strided form of the same kernel: C (M x N) -= A (M x K) B (K x N)
+// (assign == 0) or C = A B (assign == 1; C may alias B when M <= 128).
+// Complex FP32 operands, element (r, k) of A at A[2 (f sA + r + k lda)].
+fh_status gemm_tc_strided(const float *A, int64_t lda, int64_t sA, const float *B, int64_t ldb, int64_t sB, float *C,
+                          int64_t ldc, int64_t sC, int64_t M, int64_t N, int K, int assign, int count, cudaStream_t s,
+                          fh_error_info *err);
+// Bytes of one packed operand (rows rounded up to 128, K a multiple of 16).
+size_t packed_operand_bytes(int64_t rows, int K, int count);
+// C (M x N) -= A (M x K) B (K x N), complex FP32, strided as above: both
+// operands split into BF16 hi/lo and packed into pack_a / pack_b, then the
+// persistent warp-specialized tensor-core kernel (fh_gemm_packed.cu).
+fh_status gemm_tc_packed_update(const float *A, int64_t lda, int64_t sA, const float *B, int64_t ldb, int64_t sB,
+                                float *C, int64_t ldc, int64_t sC, int64_t M, int64_t N, int K, int count,
+                                void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err);
+fh_status gemm_tc_packed_check(fh_error_info *err);
 // One SIMT trailing update (FP32 or FP64), for tests.
 template <class T>
 fh_status gemm_simt_update(T *a, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err);
@@ -77,9 +103,11 @@ fh_status gemm_simt_assign(const void *linv, int nb, T *a, int64_t m, int count,
                            fh_error_info *err);
 
 // Solve with the factors in place: x (count x m x nrhs, column-major per
-// matrix, stride m*nrhs) is overwritten.
+// matrix, stride m*nrhs) is overwritten.  `group` is the span of columns
+// whose L entries carry each other's row interchanges (nb for the one-level
+// factorization, LuWork::outer for the two-level one).
 template <class T>
-fh_status lu_solve(const LuBatch<T> &b, T *x, int nrhs, int nb, cudaStream_t s, fh_error_info *err);
+fh_status lu_solve(const LuBatch<T> &b, T *x, int nrhs, int nb, cudaStream_t s, fh_error_info *err, int group = 0);
 
 // A_f = R + j w_f L for the top-left m x m block of R_m, L_m (ld = loops),
 // written as T complex into a (count x m x m).

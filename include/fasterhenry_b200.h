@@ -298,7 +298,8 @@ fh_status fh_system_fill_stats(const fh_system *sys, fh_fill_stats *stats);
 /* One trailing update A22 -= L21 U12 of an LU panel [k0, k0+nb) applied to
  * `count` complex FP32 matrices of order m (interleaved, column-major, back
  * to back), in place on a host copy.  mode 0: FP32 SIMT; mode 1: split-BF16
- * x3 on the tensor cores (nb a multiple of 16). */
+ * x3 on the tensor cores (nb a multiple of 16); mode 2: split-BF16 x3 from
+ * packed operands on the persistent tensor-core kernel (nb a multiple of 16). */
 fh_status fh_test_trailing_update(float *a, int64_t m, int32_t count, int64_t k0, int32_t nb, int32_t mode,
                                   fh_error_info *err);
 
@@ -308,12 +309,14 @@ fh_status fh_test_trailing_update(float *a, int64_t m, int32_t count, int64_t k0
 typedef enum fh_profile_class {
     FH_PROF_GEMM_FP64 = 0,      /* trailing update A22 -= L21 U12, FP64 SIMT */
     FH_PROF_GEMM_FP32 = 1,      /* trailing update, FP32 SIMT */
-    FH_PROF_GEMM_TC = 2,        /* trailing update, split-BF16 x3 tcgen05 */
+    FH_PROF_GEMM_TC = 2,        /* trailing update, split-BF16 x3 tcgen05 (deep update of a super-panel) */
     FH_PROF_PANEL = 3,          /* panel factorization (pivot search + rank-1 updates) */
     FH_PROF_TRSM = 4,           /* row interchanges + U12 triangular solve */
     FH_PROF_SOLVE = 5,          /* forward/backward substitution */
     FH_PROF_RESIDUAL = 6,       /* FP64 residual of R + jwL */
-    FH_PROF_CLASSES = 7
+    FH_PROF_PACK = 7,           /* BF16 split + packing of the deep update's operands */
+    FH_PROF_GEMM_TC_INNER = 8,  /* tensor-core updates inside a super-panel and of its U12 rows */
+    FH_PROF_CLASSES = 9
 } fh_profile_class;
 
 void fh_profile_enable(int32_t on);

@@ -52,3 +52,20 @@ def test_trailing_update(fh, m, count, k0, nb, mode, tol):
     assert np.array_equal(got[:, :, :b], a[:, :, :b])
     err = np.abs(got[:, b:, b:] - ref[:, b:, b:]) / bound[:, b:, b:]
     assert err.max() < tol, err.max()
+
+
+@pytest.mark.parametrize("m,count,k0,nb", [(1200, 1, 64, 512), (900, 3, 0, 256), (300, 2, 16, 128), (130, 2, 0, 16),
+                                           (777, 2, 100, 512), (1500, 1, 0, 1024)])
+def test_packed_update(fh, m, count, k0, nb):
+    """Persistent tensor-core kernel from packed split-BF16 operands (mode 2),
+    including deep K (512, 1024), ragged tiles and a batch."""
+    rng = np.random.default_rng(7 * m + count + k0)
+    a = (rng.standard_normal((count, m, m)) + 1j * rng.standard_normal((count, m, m))).astype(np.complex64)
+    a[:, :, k0:k0 + nb] *= 0.3
+    ref, bound = reference(a, k0, nb)
+    got = run(fh, a, k0, nb, 2)
+    b = k0 + nb
+    assert np.array_equal(got[:, :b, :], a[:, :b, :])
+    assert np.array_equal(got[:, :, :b], a[:, :, :b])
+    err = np.abs(got[:, b:, b:] - ref[:, b:, b:]) / bound[:, b:, b:]
+    assert err.max() < 2e-5, err.max()

@@ -152,3 +152,18 @@ def test_sweep_json_roundtrip(fh, c1_system):
     z = np.array([[[e["re"] + 1j * e["im"] for e in row] for row in m] for m in doc["impedance_ohm"]])
     assert np.array_equal(z, r.impedance_ohm)
     assert doc["provenance"]["counts"]["filaments"] == 240
+
+
+@pytest.mark.parametrize("legs", [9, 18])
+def test_two_level_mixed_matches_fp64(fh, legs):
+    """Orders just above one and two 512-column super-panels (m = 522, 1,044):
+    the two-level FP32 factorization (deep tensor-core updates, grouped
+    interchanges in the forward solve) refines to the FP64 answer."""
+    deck = F.meander_legs(legs)
+    freqs = F.logspace(5, 10, 8)
+    with fh.MeshSystem.assemble(fh.Geometry.from_deck(deck), deck.ports, deck.discretization) as s:
+        assert s.counts()["internal_meshes"] == 58 * legs
+        z64 = s.sweep(freqs, fh.Precision.FP64).impedance_ohm
+        rm = s.sweep(freqs, fh.Precision.MIXED_BF16X3)
+    assert rel_err(rm.impedance_ohm, z64) < MIXED_RTOL
+    assert all(1 <= i <= 10 for i in rm.refinement_iterations), rm.refinement_iterations

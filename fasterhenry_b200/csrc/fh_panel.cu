@@ -8,24 +8,30 @@
 //   per column j:   local arg-max of |re| + |im| over the CTA's rows, published
 //                   with the candidate row's NB values (and row j's, by its
 //                   owner) into a buffer double-buffered by the parity of j;
-//                   one grid barrier; every CTA picks the pivot (largest, then
-//                   first row, as dense.rs:157-166), the owners of rows j and p
-//                   exchange them across all NB panel columns, and each CTA
-//                   scales and rank-1-updates its own rows inside the sub-panel.
+//                   one barrier of the matrix's CTAs; every CTA picks the pivot
+//                   (largest, then first row, as dense.rs:157-166), the owners
+//                   of rows j and p exchange them across all NB panel columns,
+//                   and each CTA scales and rank-1-updates its own rows inside
+//                   the sub-panel.  The rank-1 pass writes column j+1, so the
+//                   arg-max of column j+1 is taken in that pass, not reread.
 //   per sub-panel:  barrier; U12 of the sub-panel (L11^-1 A12 over the rest of
 //                   the outer panel) by slice 0 of each matrix; barrier; each
 //                   CTA updates its own rows of the rest of the outer panel
-//                   (a tall GEMM with K = 16).
+//                   (a tall GEMM with K = 16, which also yields the arg-max of
+//                   the next sub-panel's first column).
 //
 // The rank-1 traffic therefore stays inside 16 columns, and one launch
 // replaces the 2 x NB launches of a column-at-a-time panel.  Row interchanges
 // cover every column of the outer panel, so the forward substitution can
-// apply one outer panel's interchanges at a time.  Grid barriers are bounded:
-// a barrier that gives up sets the error flag and every CTA returns.
+// apply one outer panel's interchanges at a time.  Barriers synchronise only
+// the CTAs of one matrix (a counter per matrix) and are bounded: a barrier
+// that gives up sets the error flag, which stays set for the whole
+// factorization, and every CTA returns.
 #include <climits>
 
 #include "fh_cx.cuh"
 #include "fh_lu.cuh"
+#include "fh_sync.cuh"
 
 namespace fhb {
 namespace {
@@ -33,7 +39,7 @@ namespace {
 constexpr int kW = 16;         // sub-panel width
 constexpr int kNbMax = 128;    // outer panel width limit
 constexpr int kThreads = 256;
-constexpr long long kBarrierSpin = 1LL << 22;
+constexpr int kBarrierStride = kGroupBarrierStride;
 
 struct CoopArgs {
     unsigned *barrier;
@@ -45,40 +51,8 @@ struct CoopArgs {
     int per_matrix;
 };
 
-// Sense-reversing grid barrier with a bounded wait.
-__device__ bool grid_barrier(unsigned *bar, int *error) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned *vgen = bar + 1;
-        const unsigned gen = *vgen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(bar, 1u);
-        int ok = 1;
-        if (arrived == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            long long i = 0;
-            while (*vgen == gen) {
-                if (++i > kBarrierSpin || *(volatile int *)error) {
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        if (!ok) atomicExch(error, 1);
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
-
 template <class T>
-__global__ void __launch_bounds__(kThreads) panel_coop_kernel(Cx<T> *__restrict__ a, int64_t m, int64_t K0, int NB,
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_kernel(Cx<T> *__restrict__ a, int64_t m, int64_t K0, int NB,
                                                               int *__restrict__ pivots, int *__restrict__ singular,
                                                               CoopArgs args) {
     const int per_matrix = args.per_matrix;
@@ -91,6 +65,7 @@ __global__ void __launch_bounds__(kThreads) panel_coop_kernel(Cx<T> *__restrict_
     Cx<T> *cand_data = reinterpret_cast<Cx<T> *>(args.cand_data);
     Cx<T> *rowj_buf = reinterpret_cast<Cx<T> *>(args.rowj);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    unsigned *bar = args.barrier + (size_t)f * kBarrierStride;
 
     __shared__ Cx<T> P[kNbMax];
     __shared__ Cx<T> Rj[kNbMax];
@@ -101,6 +76,11 @@ __global__ void __launch_bounds__(kThreads) panel_coop_kernel(Cx<T> *__restrict_
 
     auto better = [](double v2, int i2, double v1, int i1) { return v2 > v1 || (v2 == v1 && i2 < i1); };
 
+    // This thread's arg-max candidate for the next column, gathered while the
+    // previous step wrote that column (rank-1 update or sub-panel GEMM).
+    double best = -1.0;
+    int bi = INT_MAX;
+    bool fused = false;
     for (int s0 = 0; s0 < NB; s0 += kW) {
         const int w = min(kW, NB - s0);
         const int64_t k0 = K0 + s0;
@@ -108,16 +88,19 @@ __global__ void __launch_bounds__(kThreads) panel_coop_kernel(Cx<T> *__restrict_
             const int64_t j = k0 + c;
             const int par = (int)(j & 1);
             // 1. local arg-max over the CTA's rows i >= j
-            double best = -1.0;
-            int bi = INT_MAX;
-            for (int64_t i = max(r_begin, j) + tid; i < r_end; i += kThreads) {
-                const Cx<T> v = ldcg(A + i + j * m);
-                const double n1 = (double)(fabs(v.re) + fabs(v.im));
-                if (n1 > best || (n1 == best && (int)i < bi)) {
-                    best = n1;
-                    bi = (int)i;
+            if (!fused) {
+                best = -1.0;
+                bi = INT_MAX;
+                for (int64_t i = max(r_begin, j) + tid; i < r_end; i += kThreads) {
+                    const Cx<T> v = ldcg(A + i + j * m);
+                    const double n1 = (double)(fabs(v.re) + fabs(v.im));
+                    if (n1 > best || (n1 == best && (int)i < bi)) {
+                        best = n1;
+                        bi = (int)i;
+                    }
                 }
             }
+            fused = false;
             for (int o = 16; o > 0; o >>= 1) {
                 const double v2 = __shfl_down_sync(0xffffffffu, best, o);
                 const int i2 = __shfl_down_sync(0xffffffffu, bi, o);
@@ -154,7 +137,7 @@ __global__ void __launch_bounds__(kThreads) panel_coop_kernel(Cx<T> *__restrict_
                         rowj_buf[(int64_t)(f * 2 + par) * kNbMax + t] = ldcg(A + j + (K0 + t) * m);
             }
             // 2. every CTA's candidate is published
-            if (!grid_barrier(args.barrier, args.error)) return;
+            if (!group_barrier(bar, (unsigned)per_matrix, args.error)) return;
             // 3. the pivot (warp 0 reduces the candidates of this matrix), and
             //    the interchange of rows j and p
             double bv = -1.0;
@@ -211,25 +194,56 @@ __global__ void __launch_bounds__(kThreads) panel_coop_kernel(Cx<T> *__restrict_
                     for (int t = tid; t < NB; t += kThreads) A[j + (K0 + t) * m] = P[t];
             }
             __syncthreads();
-            // 4. scale by the pivot's reciprocal and rank-1 update inside the sub-panel
+            // 4. scale by the pivot's reciprocal and rank-1 update inside the
+            //    sub-panel; column j+1's new values feed its arg-max.
             const Cx<T> one{(T)1, (T)0};
             const Cx<T> inv = cdiv(one, P[s0 + c]);
+            best = -1.0;
+            bi = INT_MAX;
+            // All loads of a row's sub-panel entries (kR at a time) are issued
+            // before any of them is used, so a row costs one or two memory
+            // latencies, not w - c.
+            constexpr int kR = sizeof(T) == 4 ? kW : kW / 2;
             for (int64_t i = max(r_begin, j + 1) + tid; i < r_end; i += kThreads) {
-                Cx<T> l = cmul(ldcg(A + i + j * m), inv);
+                const Cx<T> l = cmul(ldcg(A + i + j * m), inv);
                 A[i + j * m] = l;
-                for (int cc = c + 1; cc < w; ++cc) {
-                    Cx<T> y = ldcg(A + i + (k0 + cc) * m);
-                    csubmul(y, P[s0 + cc], l);
-                    A[i + (k0 + cc) * m] = y;
+#pragma unroll
+                for (int h = 0; h < kW; h += kR) {
+                    if (h + kR <= c + 1 || h >= w) continue;
+                    Cx<T> y[kR];
+#pragma unroll
+                    for (int q = 0; q < kR; ++q)
+                        if (h + q > c && h + q < w) y[q] = ldcg(A + i + (k0 + h + q) * m);
+#pragma unroll
+                    for (int q = 0; q < kR; ++q) {
+                        if (h + q > c && h + q < w) {
+                            csubmul(y[q], P[s0 + h + q], l);
+                            A[i + (k0 + h + q) * m] = y[q];
+                            if (h + q == c + 1) {
+                                const double n1 = (double)(fabs(y[q].re) + fabs(y[q].im));
+                                if (n1 > best) {  // rows ascend per thread: ties keep the first
+                                    best = n1;
+                                    bi = (int)i;
+                                }
+                            }
+                        }
+                    }
                 }
             }
+            fused = c + 1 < w;
         }
         const int rest = NB - s0 - w;  // outer-panel columns right of the sub-panel
         if (rest <= 0) continue;
         // 5. the sub-panel is final everywhere
-        if (!grid_barrier(args.barrier, args.error)) return;
+        if (!group_barrier(bar, (unsigned)per_matrix, args.error)) return;
         // 6. U12 of the sub-panel: rows [k0, k0+w), columns [k0+w, K0+NB)
         if (slice == 0) {
+            // the unit lower w x w block, staged once (U doubles as its buffer)
+            for (int idx = tid; idx < kW * kW; idx += kThreads) {
+                const int r = idx % kW, k = idx / kW;
+                U[r][k] = (r < w && k < w) ? ldcg(A + (k0 + r) + (k0 + k) * m) : Cx<T>{0, 0};
+            }
+            __syncthreads();
             for (int t = tid; t < rest; t += kThreads) {
                 const int64_t col = k0 + w + t;
                 Cx<T> x[kW];
@@ -241,33 +255,55 @@ __global__ void __launch_bounds__(kThreads) panel_coop_kernel(Cx<T> *__restrict_
                     if (k >= w) break;
 #pragma unroll
                     for (int r = k + 1; r < kW; ++r)
-                        if (r < w) csubmul(x[r], x[k], ldcg(A + (k0 + r) + (k0 + k) * m));
+                        if (r < w) csubmul(x[r], x[k], U[r][k]);
                 }
 #pragma unroll
                 for (int r = 0; r < kW; ++r)
                     if (r < w) A[(k0 + r) + col * m] = x[r];
             }
         }
-        // 7. U12 is visible to every CTA
-        if (!grid_barrier(args.barrier, args.error)) return;
+        // 7. U12 is visible to every CTA (and slice 0 is done with U)
+        if (!group_barrier(bar, (unsigned)per_matrix, args.error)) return;
         // 8. own rows i >= k0+w: A[i, k0+w ..] -= A[i, k0 .. k0+w) U12
         for (int idx = tid; idx < w * rest; idx += kThreads) {
             const int r = idx / rest, t = idx % rest;
             U[r][t] = ldcg(A + (k0 + r) + (k0 + w + t) * m);
         }
         __syncthreads();
+        // Column k0+w (t = 0) starts the next sub-panel: its arg-max is taken here.
+        best = -1.0;
+        bi = INT_MAX;
+        // Columns go 8 at a time with their loads issued together (the
+        // sub-panel width w is 16 here: only the last sub-panel is narrower,
+        // and it has no columns to its right).
+        constexpr int kT = sizeof(T) == 4 ? 8 : 4;
         for (int64_t i = max(r_begin, k0 + w) + tid; i < r_end; i += kThreads) {
             Cx<T> l[kW];
 #pragma unroll
-            for (int r = 0; r < kW; ++r) l[r] = r < w ? ldcg(A + i + (k0 + r) * m) : Cx<T>{0, 0};
-            for (int t = 0; t < rest; ++t) {
-                Cx<T> y = ldcg(A + i + (k0 + w + t) * m);
+            for (int r = 0; r < kW; ++r) l[r] = ldcg(A + i + (k0 + r) * m);
+            for (int t0 = 0; t0 < rest; t0 += kT) {
+                Cx<T> y[kT];
 #pragma unroll
-                for (int r = 0; r < kW; ++r)
-                    if (r < w) csubmul(y, l[r], U[r][t]);
-                A[i + (k0 + w + t) * m] = y;
+                for (int q = 0; q < kT; ++q)
+                    if (t0 + q < rest) y[q] = ldcg(A + i + (k0 + w + t0 + q) * m);
+#pragma unroll
+                for (int q = 0; q < kT; ++q) {
+                    if (t0 + q < rest) {
+#pragma unroll
+                        for (int r = 0; r < kW; ++r) csubmul(y[q], l[r], U[r][t0 + q]);
+                        A[i + (k0 + w + t0 + q) * m] = y[q];
+                    }
+                }
+                if (t0 == 0) {
+                    const double n1 = (double)(fabs(y[0].re) + fabs(y[0].im));
+                    if (n1 > best) {
+                        best = n1;
+                        bi = (int)i;
+                    }
+                }
             }
         }
+        fused = true;
         __syncthreads();
     }
 }
@@ -289,8 +325,8 @@ fh_status coop_plan(int count, int64_t m, int *per_matrix, size_t *bytes, fh_err
         return fail(err, FH_ERR_INVALID_ARGUMENT, "batch too large for one cooperative panel launch");
     *per_matrix = pm;
     const size_t slots = (size_t)count * pm * 2;
-    *bytes = 64 + 16 + slots * 8 + slots * 4 + slots * kNbMax * sizeof(Cx<T>) + (size_t)count * 2 * kNbMax * sizeof(Cx<T>) +
-             256;
+    *bytes = 128 + (size_t)count * kBarrierStride * 4 + slots * 8 + slots * 4 + slots * kNbMax * sizeof(Cx<T>) +
+             (size_t)count * 2 * kNbMax * sizeof(Cx<T>) + 256;
     return FH_OK;
 }
 
@@ -298,9 +334,10 @@ template <class T>
 void coop_bind(void *mem, int count, int per_matrix, CoopScratch &cs) {
     unsigned char *p = static_cast<unsigned char *>(mem);
     const size_t slots = (size_t)count * per_matrix * 2;
-    cs.barrier = reinterpret_cast<unsigned *>(p);
-    cs.error = reinterpret_cast<int *>(p + 16);
-    size_t off = 64;
+    // [error flag, 128 B] [one 128-byte barrier per matrix] [candidates] [rows j]
+    cs.error = reinterpret_cast<int *>(p);
+    cs.barrier = reinterpret_cast<unsigned *>(p + 128);
+    size_t off = 128 + (size_t)count * kBarrierStride * 4;
     cs.cand_val = reinterpret_cast<double *>(p + off);
     off += slots * 8;
     cs.cand_row = reinterpret_cast<int *>(p + off);
@@ -315,7 +352,11 @@ void coop_bind(void *mem, int count, int per_matrix, CoopScratch &cs) {
 template <class T>
 fh_status panel_coop(LuBatch<T> &b, int64_t K0, int nb, const CoopScratch &cs, cudaStream_t s, fh_error_info *err) {
     if (nb > kNbMax) return fail(err, FH_ERR_INVALID_ARGUMENT, "cooperative panel wider than 128 columns");
-    FHB_CUDA(cudaMemsetAsync(cs.barrier, 0, 64, s));  // barrier counters and error flag
+    // Barrier counters are reset for every launch (a barrier that gave up may
+    // leave arrivals behind); the error flag only at the start of a
+    // factorization, so that coop_check sees a failure of any panel.
+    FHB_CUDA(cudaMemsetAsync(cs.barrier, 0, (size_t)b.count * kBarrierStride * 4, s));
+    if (K0 == 0) FHB_CUDA(cudaMemsetAsync(cs.error, 0, sizeof(int), s));
     CoopArgs args{cs.barrier, cs.error, cs.cand_val, cs.cand_row, cs.cand_data, cs.rowj, cs.per_matrix};
     Cx<T> *a = reinterpret_cast<Cx<T> *>(b.a);
     int64_t m = b.m;

@@ -238,9 +238,27 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     coop_bind<float>(coop_mem.p, count, per_matrix, cs);
     w.coop = &cs;
     const int outer = outer_for(m, mode);
-    DBuf<float> linv_mem;
-    FHB_ALLOC(linv_mem, (size_t)count * kNbFp32 * kNbFp32 * 2 * (outer ? outer / kNbFp32 : 1));
+    // Two-level form: the inverses of every diagonal block of L and U are
+    // kept for the cooperative solve; one-level form: one panel's L inverse.
+    const int64_t nblk = (m + kNbFp32 - 1) / kNbFp32;
+    DBuf<float> linv_mem, uinv_mem;
+    FHB_ALLOC(linv_mem, (size_t)count * kNbFp32 * kNbFp32 * 2 * (outer ? nblk : 1));
     w.linv = linv_mem.p;
+    SolveScratch ss;
+    DBuf<unsigned char> solve_mem;
+    if (outer) {
+        FHB_ALLOC(uinv_mem, (size_t)count * kNbFp32 * kNbFp32 * 2 * nblk);
+        w.uinv = uinv_mem.p;
+        int per_group = 0;
+        size_t solve_bytes = 0;
+        e = trisolve_plan(count * (int)p, m, &per_group, &solve_bytes, err);
+        if (e) return e;
+        if (per_group > 0) {
+            FHB_ALLOC(solve_mem, solve_bytes);
+            FHB_CUDA(cudaMemsetAsync(solve_mem.p, 0, solve_bytes, st));
+            trisolve_bind(solve_mem.p, count * (int)p, per_group, ss);
+        }
+    }
     DBuf<unsigned char> pack_a, pack_b;
     if (outer) {
         const size_t pb = packed_operand_bytes(m - outer, outer, count);
@@ -277,7 +295,12 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     int it = 0;
     for (; it < kMaxIter; ++it) {
         e = convert_c64_to_c32(r.p, d32.p, count * vec, st, err);
-        if (!e) e = lu_solve<float>(b, d32.p, (int)p, kNbFp32, st, err, outer);
+        if (!e) {
+            if (ss.per_group > 0)
+                e = lu_solve_inv(b, w.linv, w.uinv, d32.p, (int)p, kNbFp32, outer, ss, st, err);
+            else
+                e = lu_solve<float>(b, d32.p, (int)p, kNbFp32, st, err, outer);
+        }
         if (!e) e = add_c32_to_c64(d_x, d32.p, count * vec, st, err);
         if (!e) e = residual_fp64(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, r.p, rnorm.p, st, err);
         if (e) return e;
@@ -292,12 +315,20 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
         bool all = true;
         for (int f = 0; f < count; ++f) {
             if (done[f]) continue;
-            // Stopping rule: the correction is negligible (1e-12 of x), or it
+            // Stopping rule: the correction is negligible (1e-12 of x); or the
+            // iteration contracts geometrically (rho = |d_k| / |d_k-1| < 0.1)
+            // and the error left after this correction, estimated as
+            // |d_k| rho / (1 - rho), is below 1e-12 of x; or the correction
             // has stopped shrinking at a level below 1e-10 of x, which is the
             // attainable accuracy of an FP64 residual (about kappa * u64).
             double rel = hx[f] > 0 ? hd[f] / hx[f] : 0.0;
             const bool stalled = hd[f] > 0.5 * prev[f];
-            if (rel <= 1e-12 || hd[f] == 0.0 || (stalled && rel <= 1e-10)) {
+            const double rho = std::isfinite(prev[f]) && prev[f] > 0 ? hd[f] / prev[f] : 1.0;
+            const bool contracted = rho < 0.1 && rel * rho / (1.0 - rho) <= 1e-12;
+            // A small correction is only trusted with a small FP64 residual:
+            // |b - A x| <= 1e-6 |b| holds for any accurate x up to kappa ~ 1e10.
+            const bool resid_ok = hr[f] <= 1e-6 * hb[f];
+            if (resid_ok && (rel <= 1e-12 || hd[f] == 0.0 || contracted || (stalled && rel <= 1e-10))) {
                 done[f] = 1;
                 if (iters_out) iters_out[f] = it + 1;
                 continue;
@@ -320,6 +351,10 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
             if (iters_out) iters_out[f] = it;
         }
         if (resid_out) resid_out[f] = hb[f] > 0 ? hr[f] / hb[f] : 0.0;
+    }
+    if (ss.per_group > 0) {
+        e = trisolve_check(ss, st, err);
+        if (e) return e;
     }
     cudaEventRecord(e2, st);
     FHB_CUDA(cudaMemcpyAsync(h_singular, sing.p, sizeof(int) * count, cudaMemcpyDeviceToHost, st));
@@ -641,9 +676,11 @@ fh_status fh_sweep(fh_system *sys, const double *freqs, size_t nf, fh_precision 
     const TrailingUpdate update =
         precision == FH_PRECISION_MIXED_BF16X3 ? TrailingUpdate::TensorBf16x3 : TrailingUpdate::Simt;
     // Per frequency: the matrix, the vectors, and for the two-level FP32
-    // form its two packed operands (8 bytes per entry of an m x 512 block each).
+    // form its two packed operands (8 bytes per entry of an m x 512 block
+    // each) and the inverses of the diagonal blocks of L and U.
     const double per = (mixed ? 8.0 : 16.0) * (double)m * (double)m + 64.0 * (double)(m * p + 64) +
-                       (outer_for(m, update) ? 16.0 * (double)m * kOuterFp32 : 0.0);
+                       (outer_for(m, update) ? 16.0 * (double)m * kOuterFp32 + 16.0 * (double)(m + kNbFp32) * kNbFp32
+                                             : 0.0);
     int chunk = (int)std::max(1.0, std::min<double>((double)nf, 0.8 * (double)free_b / std::max(per, 1.0)));
     DBuf<double> d_omega, d_x, d_z;
     FHB_ALLOC(d_omega, (size_t)chunk);

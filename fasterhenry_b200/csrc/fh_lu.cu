@@ -408,37 +408,85 @@ __global__ void __launch_bounds__(128) bwd_panel_kernel2(const Cx<T> *__restrict
 }
 
 // Linv = L11^{-1} for the unit lower triangle of panel [k0, k0+nb) of every
-// matrix (column-major nb x nb per matrix).  One CTA per matrix, thread j
-// forms column j by forward substitution against e_j; the columns being built
-// live in shared memory (nb*nb complex), L11 is read through the cache.
+// matrix (column-major nb x nb, leading dimension nb, matrix f at
+// linv + f * mstride).  One CTA per matrix.  X starts as
+// the identity and is reduced column by column of L11 (right-looking forward
+// substitution on all nb right-hand sides at once):
+//     for k: X[r][j] -= L[r][k] X[k][j]   for r > k, j <= k,
+// with X in shared memory, all threads spread over the (r, j) pairs, and
+// column k+1 of L11 (contiguous in memory) fetched while step k computes.
+// Dynamic shared memory: (nb*nb + 2*nb) complex.
 template <class T>
-__global__ void tri_inverse_kernel(const Cx<T> *__restrict__ a, int64_t m, int k0, int nb, Cx<T> *__restrict__ linv) {
+__global__ void __launch_bounds__(256) tri_inverse_kernel(const Cx<T> *__restrict__ a, int64_t m, int k0, int nb,
+                                                          Cx<T> *__restrict__ linv, int64_t mstride) {
     extern __shared__ unsigned char smem_raw[];
     Cx<T> *X = reinterpret_cast<Cx<T> *>(smem_raw);  // X[r * nb + j]
-    const int f = blockIdx.x;
-    const Cx<T> *A = a + (int64_t)f * m * m;
-    const int j = threadIdx.x;
-    if (j < nb) {
-        for (int r = 0; r < nb; ++r) {
-            Cx<T> v{(T)0, (T)0};
-            if (r == j) {
-                v.re = (T)1;
-            } else if (r > j) {
-                Cx<T> acc{(T)0, (T)0};
-                for (int k = j; k < r; ++k) {
-                    const Cx<T> l = A[(k0 + r) + (int64_t)(k0 + k) * m];
-                    const Cx<T> xv = X[k * nb + j];
-                    acc.re += l.re * xv.re - l.im * xv.im;
-                    acc.im += l.re * xv.im + l.im * xv.re;
-                }
-                v = Cx<T>{-acc.re, -acc.im};
-            }
-            X[r * nb + j] = v;
-        }
-    }
+    Cx<T> *col = X + nb * nb;                          // two staged columns of L11
+    const int f = blockIdx.x, tid = threadIdx.x;
+    const Cx<T> *A = a + (int64_t)f * m * m + k0 + (int64_t)k0 * m;  // L11(r, k) at A[r + k m]
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x)
+        X[idx] = Cx<T>{(idx / nb == idx % nb) ? (T)1 : (T)0, (T)0};
+    for (int r = tid; r < nb; r += blockDim.x) col[r] = A[r];
     __syncthreads();
-    Cx<T> *out = linv + (int64_t)f * nb * nb;
-    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+    for (int k = 0; k + 1 < nb; ++k) {
+        const Cx<T> *ck = col + (k & 1) * nb;
+        Cx<T> nxt{(T)0, (T)0};
+        const bool fetch = k + 2 < nb && tid < nb;
+        if (fetch) nxt = A[tid + (int64_t)(k + 1) * m];
+        const int width = k + 1, count = (nb - k - 1) * width;
+        for (int idx = tid; idx < count; idx += blockDim.x) {
+            const int r = k + 1 + idx / width, jj = idx % width;
+            Cx<T> x = X[r * nb + jj];
+            csubmul(x, ck[r], X[k * nb + jj]);
+            X[r * nb + jj] = x;
+        }
+        if (fetch) col[((k + 1) & 1) * nb + tid] = nxt;
+        __syncthreads();
+    }
+    Cx<T> *out = linv + (int64_t)f * mstride;
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+        const int r = idx % nb, c = idx / nb;
+        out[r + c * nb] = X[r * nb + c];
+    }
+}
+
+// Uinv = U11^{-1} for the upper triangle (non-unit) of panel [k0, k0+nb),
+// same layout.  Backward, column by column of U11 from the last:
+//     X[k][j] /= U[k][k]                     for j >= k,
+//     X[r][j] -= U[r][k] X[k][j]             for r < k, j >= k.
+template <class T>
+__global__ void __launch_bounds__(256) tri_inverse_upper_kernel(const Cx<T> *__restrict__ a, int64_t m, int k0,
+                                                                int nb, Cx<T> *__restrict__ uinv, int64_t mstride) {
+    extern __shared__ unsigned char smem_raw[];
+    Cx<T> *X = reinterpret_cast<Cx<T> *>(smem_raw);  // X[r * nb + j]
+    Cx<T> *col = X + nb * nb;
+    const int f = blockIdx.x, tid = threadIdx.x;
+    const Cx<T> *A = a + (int64_t)f * m * m + k0 + (int64_t)k0 * m;  // U11(r, k) at A[r + k m]
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x)
+        X[idx] = Cx<T>{(idx / nb == idx % nb) ? (T)1 : (T)0, (T)0};
+    for (int r = tid; r < nb; r += blockDim.x) col[((nb - 1) & 1) * nb + r] = A[r + (int64_t)(nb - 1) * m];
+    __syncthreads();
+    const Cx<T> one{(T)1, (T)0};
+    for (int k = nb - 1; k >= 0; --k) {
+        const Cx<T> *ck = col + (k & 1) * nb;
+        const Cx<T> d = cdiv(one, ck[k]);
+        for (int jj = k + tid; jj < nb; jj += blockDim.x) X[k * nb + jj] = cmul(X[k * nb + jj], d);
+        Cx<T> nxt{(T)0, (T)0};
+        const bool fetch = k > 0 && tid < k;
+        if (fetch) nxt = A[tid + (int64_t)(k - 1) * m];
+        __syncthreads();
+        const int width = nb - k, count = k * width;
+        for (int idx = tid; idx < count; idx += blockDim.x) {
+            const int r = idx / width, jj = k + idx % width;
+            Cx<T> x = X[r * nb + jj];
+            csubmul(x, ck[r], X[k * nb + jj]);
+            X[r * nb + jj] = x;
+        }
+        if (fetch) col[((k - 1) & 1) * nb + tid] = nxt;
+        __syncthreads();
+    }
+    Cx<T> *out = uinv + (int64_t)f * mstride;
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
         const int r = idx % nb, c = idx / nb;
         out[r + c * nb] = X[r * nb + c];
     }
@@ -708,10 +756,14 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
     const int outer = w.outer;
     if (nb % 16 || nb > 128 || outer % nb || !w.coop || !w.linv || !w.pack_a || !w.pack_b)
         return fail(err, FH_ERR_INVALID_ARGUMENT, "two-level factorization needs nb | outer, nb <= 128 and scratch");
-    const size_t inv_smem = sizeof(C) * (size_t)nb * nb;
+    const size_t inv_smem = sizeof(C) * ((size_t)nb * nb + 2 * (size_t)nb);
     FHB_CUDA(cudaFuncSetAttribute(tri_inverse_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)inv_smem));
+    FHB_CUDA(cudaFuncSetAttribute(tri_inverse_upper_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)inv_smem));
     auto at = [&](int64_t r, int64_t c) { return b.a + 2 * (r + c * m); };
+    // Inverses of the diagonal blocks, slot j0 / nb (count * nb * nb each).
+    auto slot = [&](void *base, int64_t j0) { return reinterpret_cast<C *>(base) + (size_t)(j0 / nb) * count * nb * nb; };
     auto swaps = [&](int64_t k0, int n, int64_t c0, int64_t c1) {
         if (c1 > c0)
             swap_kernel<float><<<dim3(grid_for(c1 - c0, 256, 1024), count), 256, 0, s>>>(a, m, (int)k0, n, c0, c1,
@@ -724,19 +776,25 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
         for (int64_t j0 = K0; j0 < E; j0 += nb) {
             const int wj = (int)std::min<int64_t>(nb, E - j0);
             const int64_t r1 = j0 + wj;  // first row / column after the panel
-            C *linv = reinterpret_cast<C *>(w.linv) + (size_t)((j0 - K0) / nb) * count * nb * nb;
+            C *linv = slot(w.linv, j0);
             prof_begin(s, FH_PROF_PANEL);
             st = panel_coop<float>(b, j0, wj, *w.coop, s, err);
             prof_end(s, FH_PROF_PANEL, 0.0);
             if (st) return st;
-            if (r1 >= m) break;
             prof_begin(s, FH_PROF_TRSM);
+            const int64_t mstride = (int64_t)nb * nb;  // a partial last block keeps the full slot stride
+            tri_inverse_kernel<float><<<count, 256, inv_smem, s>>>(a, m, (int)j0, wj, linv, mstride);
+            if (w.uinv)
+                tri_inverse_upper_kernel<float><<<count, 256, inv_smem, s>>>(a, m, (int)j0, wj, slot(w.uinv, j0),
+                                                                             mstride);
+            if (r1 >= m) {
+                prof_end(s, FH_PROF_TRSM, 0.0);
+                break;
+            }
             swaps(j0, wj, K0, j0);
             swaps(j0, wj, r1, E);
-            tri_inverse_kernel<float><<<count, std::max(32, ((wj + 31) / 32) * 32), inv_smem, s>>>(a, m, (int)j0, wj,
-                                                                                                 linv);
             if (r1 < E)
-                st = gemm_tc_strided(reinterpret_cast<const float *>(linv), wj, (int64_t)wj * wj, at(j0, r1), m, mm,
+                st = gemm_tc_strided(reinterpret_cast<const float *>(linv), wj, mstride, at(j0, r1), m, mm,
                                      at(j0, r1), m, mm, wj, E - r1, wj, 1, count, s, err);
             prof_end(s, FH_PROF_TRSM, 4.0 * (double)wj * wj * (double)(E - r1) * count);
             if (st) return st;
@@ -753,7 +811,7 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
         prof_begin(s, FH_PROF_TRSM);
         swaps(K0, W, E, m);
         for (int64_t j0 = K0; j0 < E && !st; j0 += nb) {
-            const C *linv = reinterpret_cast<const C *>(w.linv) + (size_t)((j0 - K0) / nb) * count * nb * nb;
+            const C *linv = slot(w.linv, j0);
             st = gemm_tc_strided(reinterpret_cast<const float *>(linv), nb, (int64_t)nb * nb, at(j0, E), m, mm,
                                  at(j0, E), m, mm, nb, n2, nb, 1, count, s, err);
             if (!st && j0 + nb < E)
@@ -820,11 +878,10 @@ fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaS
             // U12 = L11^{-1} A12 as an explicit triangular inverse times A12:
             // the product runs as a GEMM (tensor cores in the mixed form).
             C *linv = reinterpret_cast<C *>(w.linv);
-            const size_t inv_smem = sizeof(C) * (size_t)w_nb * w_nb;
+            const size_t inv_smem = sizeof(C) * ((size_t)w_nb * w_nb + 2 * (size_t)w_nb);
             FHB_CUDA(cudaFuncSetAttribute(tri_inverse_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)inv_smem));
-            tri_inverse_kernel<T><<<b.count, std::max(32, ((w_nb + 31) / 32) * 32), inv_smem, s>>>(a, m, (int)k0,
-                                                                                                  w_nb, linv);
+            tri_inverse_kernel<T><<<b.count, 256, inv_smem, s>>>(a, m, (int)k0, w_nb, linv, (int64_t)w_nb * w_nb);
             if (tc_apply) {
                 fh_status st = gemm_tc_tri_apply(reinterpret_cast<const float *>(w.linv), w_nb,
                                                  reinterpret_cast<float *>(b.a), m, b.count, k0, s, err);

@@ -42,9 +42,13 @@ struct LuWork {
     const CoopScratch *coop = nullptr;
     // count * nb * nb complex T: with it, U12 = L11^{-1} A12 is formed from
     // the explicit triangular inverse and a GEMM; without it, by the
-    // column-at-a-time TRSM kernel.  With `outer` set it holds outer / nb
-    // such slots (one per panel of a super-panel).
+    // column-at-a-time TRSM kernel.  With `outer` set it holds one slot per
+    // nb-block of the matrix (ceil(m / nb) slots, slot j0 / nb, matrices
+    // back to back within a slot), kept for lu_solve_inv.
     void *linv = nullptr;
+    // With `outer` set: the inverses of the diagonal nb x nb blocks of U,
+    // laid out like linv (optional; lu_solve_inv needs them).
+    void *uinv = nullptr;
     // Two-level blocking (FP32 form on the tensor cores): super-panels of
     // `outer` columns are factored with nb-wide panels and updates confined
     // to the super-panel; the rest of the matrix then takes one deep update
@@ -108,6 +112,22 @@ fh_status gemm_simt_assign(const void *linv, int nb, T *a, int64_t m, int count,
 // factorization, LuWork::outer for the two-level one).
 template <class T>
 fh_status lu_solve(const LuBatch<T> &b, T *x, int nrhs, int nb, cudaStream_t s, fh_error_info *err, int group = 0);
+
+// Cooperative forward + backward solve with the two-level FP32 factors
+// (fh_trisolve.cu): one launch, groups of CTAs per (matrix, right-hand side)
+// meeting at their own bounded barriers, diagonal blocks applied through the
+// inverses kept in LuWork::linv / uinv.
+struct SolveScratch {
+    unsigned *barrier = nullptr;
+    int *error = nullptr;  // must start at zero
+    int groups = 0;        // count * nrhs
+    int per_group = 0;     // CTAs per group; 0 = the batch does not fit one launch
+};
+fh_status trisolve_plan(int groups, int64_t m, int *per_group, size_t *bytes, fh_error_info *err);
+void trisolve_bind(void *mem, int groups, int per_group, SolveScratch &ss);
+fh_status lu_solve_inv(const LuBatch<float> &b, const void *linv, const void *uinv, float *x, int nrhs, int nb,
+                       int group, const SolveScratch &ss, cudaStream_t s, fh_error_info *err);
+fh_status trisolve_check(const SolveScratch &ss, cudaStream_t s, fh_error_info *err);
 
 // A_f = R + j w_f L for the top-left m x m block of R_m, L_m (ld = loops),
 // written as T complex into a (count x m x m).

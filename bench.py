@@ -264,6 +264,8 @@ def run_ours(args):
         "roofline": roofline, "profile": profile, "gpu_launches": int(launches),
         "clocks": clocks.summary(),
     }
+    if rank == 0 and world == 1:
+        out["fp64_library_lu"] = library_fp64_lu(system, freqs, counts)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(args, budget_s=args.cpu_budget)
     if rank == 0:
@@ -272,6 +274,34 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def library_fp64_lu(system, freqs, counts):
+    """A library FP64 GPU LU for context: cuSOLVER's complex128 getrf (through
+    torch.linalg.lu_factor) on one frequency's m x m matrix R_ee + j w L_ee,
+    timed with CUDA events and multiplied by the number of frequencies (each
+    frequency is an independent factorization).  Not on the product path."""
+    import torch
+    m = counts["internal_meshes"]
+    R, L = system.mesh_matrices()
+    w = 2.0 * np.pi * freqs[len(freqs) // 2]
+    a = torch.from_numpy(np.ascontiguousarray(R[:m, :m] + 1j * w * L[:m, :m])).to("cuda")
+    torch.linalg.lu_factor(a)  # warm-up (workspace, handles)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(2):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.linalg.lu_factor(a)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    one = min(ms) * 1e-3
+    del a
+    torch.cuda.empty_cache()
+    return {"one_matrix_s": round(one, 6), "sweep_s": round(one * len(freqs), 6),
+            "what": "torch.linalg.lu_factor complex128 (cuSOLVER getrf) of one m x m matrix x %d frequencies"
+                    % len(freqs)}
 
 
 def cpu_baseline(args, budget_s: float = 20.0):

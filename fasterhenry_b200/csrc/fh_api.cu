@@ -15,7 +15,43 @@
 
 using namespace fhb;
 
+// Device workspace of a system's sweeps, kept between calls: one buffer per
+// role (slot), grown when a sweep needs more.  Repeated sweeps then allocate
+// nothing, and no cudaFree (which synchronizes the device) runs inside a
+// sweep after the first.
+struct DevPool {
+    std::vector<std::pair<void *, size_t>> slot;
+    ~DevPool() { release(); }
+    void release() {
+        for (auto &b : slot)
+            if (b.first) cudaFree(b.first);
+        slot.clear();
+    }
+    size_t held() const {
+        size_t t = 0;
+        for (const auto &b : slot) t += b.second;
+        return t;
+    }
+    cudaError_t get(int id, size_t bytes, void **out) {
+        if ((int)slot.size() <= id) slot.resize((size_t)id + 1, {nullptr, 0});
+        auto &b = slot[(size_t)id];
+        if (b.second < bytes) {
+            if (b.first) cudaFree(b.first);
+            b = {nullptr, 0};
+            const cudaError_t e = cudaMalloc(&b.first, std::max<size_t>(bytes, 1));
+            if (e != cudaSuccess) {
+                b.first = nullptr;
+                return e;
+            }
+            b.second = bytes;
+        }
+        *out = b.first;
+        return cudaSuccess;
+    }
+};
+
 struct fh_system {
+    DevPool pool;
     std::vector<fh_node> nodes;
     std::vector<fh_segment_def> segments;
     std::vector<fh_port> ports;
@@ -31,6 +67,7 @@ struct fh_system {
     FillStats fill{};
     float ms_congruence = 0;
     ~fh_system() {
+        pool.release();
         if (d_Lm) cudaFree(d_Lm);
         if (d_Rm) cudaFree(d_Rm);
         if (stream) cudaStreamDestroy(stream);
@@ -73,6 +110,32 @@ struct DBuf {
         return cudaMalloc((void **)&p, std::max<size_t>(1, count) * sizeof(T));
     }
 };
+
+// A view of a pooled buffer (the pool owns the memory).
+template <class T>
+struct PBuf {
+    T *p = nullptr;
+};
+
+// Workspace slots of the sweep paths (FP64 and mixed share the roles they have
+// in common, so the larger of the two is kept).
+enum PoolSlot {
+    kSlotA, kSlotD32, kSlotR, kSlotRnorm, kSlotBnorm, kSlotDnorm, kSlotXnorm, kSlotPiv, kSlotSing, kSlotPv,
+    kSlotPi, kSlotTk, kSlotCoop, kSlotLinv, kSlotUinv, kSlotSolve, kSlotPackA, kSlotPackB, kSlotOmega, kSlotX,
+    kSlotZ
+};
+
+#define FHB_PALLOC(pool, buf, slot_id, count)                                                          \
+    do {                                                                                               \
+        void *pp_ = nullptr;                                                                           \
+        if ((pool).get((slot_id), (size_t)(count) * sizeof(*(buf).p), &pp_) != cudaSuccess) {         \
+            cudaGetLastError();                                                                        \
+            return fail(err, FH_ERR_OUT_OF_MEMORY,                                                     \
+                        "device allocation of " + std::to_string((size_t)(count) * sizeof(*(buf).p)) + \
+                            " bytes failed");                                                          \
+        }                                                                                              \
+        (buf).p = static_cast<decltype((buf).p)>(pp_);                                                 \
+    } while (0)
 
 #define FHB_ALLOC(buf, count)                                                                   \
     do {                                                                                        \
@@ -117,39 +180,39 @@ fh_status sweep_chunk_fp64(fh_system *s, const double *d_omega, int count, doubl
     const int64_t m = s->m, p = s->p, ld = s->nloops;
     cudaStream_t st = s->stream;
     if (m > 0) {
-        DBuf<double> a;
-        DBuf<int> piv, sing;
-        FHB_ALLOC(a, (size_t)count * m * m * 2);
-        FHB_ALLOC(piv, (size_t)count * m);
-        FHB_ALLOC(sing, (size_t)count);
+        PBuf<double> a;
+        PBuf<int> piv, sing;
+        FHB_PALLOC(s->pool, a, kSlotA, (size_t)count * m * m * 2);
+        FHB_PALLOC(s->pool, piv, kSlotPiv, (size_t)count * m);
+        FHB_PALLOC(s->pool, sing, kSlotSing, (size_t)count);
         FHB_CUDA(cudaMemsetAsync(sing.p, 0, sizeof(int) * count, st));
         fh_status e = form_system<double>(s->d_Rm, s->d_Lm, ld, m, d_omega, count, a.p, st, err);
         if (e) return e;
         e = form_rhs<double>(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, st, err);
         if (e) return e;
         LuWork w;
-        DBuf<double> pv;
-        DBuf<int> pi;
-        DBuf<unsigned> tk;
+        PBuf<double> pv;
+        PBuf<int> pi;
+        PBuf<unsigned> tk;
         w.max_chunks = 16;
-        FHB_ALLOC(pv, (size_t)count * w.max_chunks);
-        FHB_ALLOC(pi, (size_t)count * w.max_chunks);
-        FHB_ALLOC(tk, (size_t)count);
+        FHB_PALLOC(s->pool, pv, kSlotPv, (size_t)count * w.max_chunks);
+        FHB_PALLOC(s->pool, pi, kSlotPi, (size_t)count * w.max_chunks);
+        FHB_PALLOC(s->pool, tk, kSlotTk, (size_t)count);
         FHB_CUDA(cudaMemsetAsync(tk.p, 0, sizeof(unsigned) * count, st));
         w.partial_val = pv.p;
         w.partial_idx = pi.p;
         w.tickets = tk.p;
         CoopScratch cs;
-        DBuf<unsigned char> coop_mem;
+        PBuf<unsigned char> coop_mem;
         int per_matrix = 0;
         size_t coop_bytes = 0;
         e = coop_plan<double>(count, m, &per_matrix, &coop_bytes, err);
         if (e) return e;
-        FHB_ALLOC(coop_mem, coop_bytes);
+        FHB_PALLOC(s->pool, coop_mem, kSlotCoop, coop_bytes);
         coop_bind<double>(coop_mem.p, count, per_matrix, cs);
         w.coop = &cs;
-        DBuf<double> linv_mem;
-        FHB_ALLOC(linv_mem, (size_t)count * kNbFp64 * kNbFp64 * 2);
+        PBuf<double> linv_mem;
+        FHB_PALLOC(s->pool, linv_mem, kSlotLinv, (size_t)count * kNbFp64 * kNbFp64 * 2);
         w.linv = linv_mem.p;
         LuBatch<double> b;
         b.a = a.p;
@@ -195,19 +258,20 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
         std::fill(h_singular, h_singular + count, 0);
         return schur(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, d_z, st, err);
     }
-    DBuf<float> a, d32;
-    DBuf<double> r, rnorm, bnorm, dnorm, xnorm;
-    DBuf<int> piv, sing;
+    PBuf<float> a, d32;
+    PBuf<double> r, rnorm, bnorm, dnorm, xnorm;
+    PBuf<int> piv, sing;
     const int64_t vec = m * p;  // complex entries per frequency
-    FHB_ALLOC(a, (size_t)count * m * m * 2);
-    FHB_ALLOC(d32, (size_t)count * vec * 2);
-    FHB_ALLOC(r, (size_t)count * vec * 2);
-    FHB_ALLOC(rnorm, (size_t)count);
-    FHB_ALLOC(bnorm, (size_t)count);
-    FHB_ALLOC(dnorm, (size_t)count);
-    FHB_ALLOC(xnorm, (size_t)count);
-    FHB_ALLOC(piv, (size_t)count * m);
-    FHB_ALLOC(sing, (size_t)count);
+    DevPool &pool = s->pool;
+    FHB_PALLOC(pool, a, kSlotA, (size_t)count * m * m * 2);
+    FHB_PALLOC(pool, d32, kSlotD32, (size_t)count * vec * 2);
+    FHB_PALLOC(pool, r, kSlotR, (size_t)count * vec * 2);
+    FHB_PALLOC(pool, rnorm, kSlotRnorm, (size_t)count);
+    FHB_PALLOC(pool, bnorm, kSlotBnorm, (size_t)count);
+    FHB_PALLOC(pool, dnorm, kSlotDnorm, (size_t)count);
+    FHB_PALLOC(pool, xnorm, kSlotXnorm, (size_t)count);
+    FHB_PALLOC(pool, piv, kSlotPiv, (size_t)count * m);
+    FHB_PALLOC(pool, sing, kSlotSing, (size_t)count);
     FHB_CUDA(cudaMemsetAsync(sing.p, 0, sizeof(int) * count, st));
     fh_status e = form_system<float>(s->d_Rm, s->d_Lm, ld, m, d_omega, count, a.p, st, err);
     if (e) return e;
@@ -217,53 +281,53 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     if (e) return e;
     FHB_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * 2 * count * vec, st));
     LuWork w;
-    DBuf<double> pv;
-    DBuf<int> pi;
-    DBuf<unsigned> tk;
+    PBuf<double> pv;
+    PBuf<int> pi;
+    PBuf<unsigned> tk;
     w.max_chunks = 16;
-    FHB_ALLOC(pv, (size_t)count * w.max_chunks);
-    FHB_ALLOC(pi, (size_t)count * w.max_chunks);
-    FHB_ALLOC(tk, (size_t)count);
+    FHB_PALLOC(pool, pv, kSlotPv, (size_t)count * w.max_chunks);
+    FHB_PALLOC(pool, pi, kSlotPi, (size_t)count * w.max_chunks);
+    FHB_PALLOC(pool, tk, kSlotTk, (size_t)count);
     FHB_CUDA(cudaMemsetAsync(tk.p, 0, sizeof(unsigned) * count, st));
     w.partial_val = pv.p;
     w.partial_idx = pi.p;
     w.tickets = tk.p;
     CoopScratch cs;
-    DBuf<unsigned char> coop_mem;
+    PBuf<unsigned char> coop_mem;
     int per_matrix = 0;
     size_t coop_bytes = 0;
     e = coop_plan<float>(count, m, &per_matrix, &coop_bytes, err);
     if (e) return e;
-    FHB_ALLOC(coop_mem, coop_bytes);
+    FHB_PALLOC(pool, coop_mem, kSlotCoop, coop_bytes);
     coop_bind<float>(coop_mem.p, count, per_matrix, cs);
     w.coop = &cs;
     const int outer = outer_for(m, mode);
     // Two-level form: the inverses of every diagonal block of L and U are
     // kept for the cooperative solve; one-level form: one panel's L inverse.
     const int64_t nblk = (m + kNbFp32 - 1) / kNbFp32;
-    DBuf<float> linv_mem, uinv_mem;
-    FHB_ALLOC(linv_mem, (size_t)count * kNbFp32 * kNbFp32 * 2 * (outer ? nblk : 1));
+    PBuf<float> linv_mem, uinv_mem;
+    FHB_PALLOC(pool, linv_mem, kSlotLinv, (size_t)count * kNbFp32 * kNbFp32 * 2 * (outer ? nblk : 1));
     w.linv = linv_mem.p;
     SolveScratch ss;
-    DBuf<unsigned char> solve_mem;
+    PBuf<unsigned char> solve_mem;
     if (outer) {
-        FHB_ALLOC(uinv_mem, (size_t)count * kNbFp32 * kNbFp32 * 2 * nblk);
+        FHB_PALLOC(pool, uinv_mem, kSlotUinv, (size_t)count * kNbFp32 * kNbFp32 * 2 * nblk);
         w.uinv = uinv_mem.p;
         int per_group = 0;
         size_t solve_bytes = 0;
         e = trisolve_plan(count * (int)p, m, &per_group, &solve_bytes, err);
         if (e) return e;
         if (per_group > 0) {
-            FHB_ALLOC(solve_mem, solve_bytes);
+            FHB_PALLOC(pool, solve_mem, kSlotSolve, solve_bytes);
             FHB_CUDA(cudaMemsetAsync(solve_mem.p, 0, solve_bytes, st));
             trisolve_bind(solve_mem.p, count * (int)p, per_group, ss);
         }
     }
-    DBuf<unsigned char> pack_a, pack_b;
+    PBuf<unsigned char> pack_a, pack_b;
     if (outer) {
         const size_t pb = packed_operand_bytes(m - outer, outer, count);
-        FHB_ALLOC(pack_a, pb);
-        FHB_ALLOC(pack_b, pb);
+        FHB_PALLOC(pool, pack_a, kSlotPackA, pb);
+        FHB_PALLOC(pool, pack_b, kSlotPackB, pb);
         w.outer = outer;
         w.pack_a = pack_a.p;
         w.pack_b = pack_b.p;
@@ -670,6 +734,7 @@ fh_status fh_sweep(fh_system *sys, const double *freqs, size_t nf, fh_precision 
     // reference's 2 GiB sweep budget, solve.rs:91 and 884).
     size_t free_b = 0, total_b = 0;
     FHB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    free_b += sys->pool.held();  // the system's own workspace is reused
     if (precision < FH_PRECISION_FP64 || precision > FH_PRECISION_MIXED_FP32)
         return fail(err, FH_ERR_INVALID_ARGUMENT, "unknown precision");
     const bool mixed = precision != FH_PRECISION_FP64;
@@ -682,10 +747,10 @@ fh_status fh_sweep(fh_system *sys, const double *freqs, size_t nf, fh_precision 
                        (outer_for(m, update) ? 16.0 * (double)m * kOuterFp32 + 16.0 * (double)(m + kNbFp32) * kNbFp32
                                              : 0.0);
     int chunk = (int)std::max(1.0, std::min<double>((double)nf, 0.8 * (double)free_b / std::max(per, 1.0)));
-    DBuf<double> d_omega, d_x, d_z;
-    FHB_ALLOC(d_omega, (size_t)chunk);
-    FHB_ALLOC(d_x, (size_t)chunk * m * p * 2);
-    FHB_ALLOC(d_z, (size_t)chunk * p * p * 2);
+    PBuf<double> d_omega, d_x, d_z;
+    FHB_PALLOC(sys->pool, d_omega, kSlotOmega, (size_t)chunk);
+    FHB_PALLOC(sys->pool, d_x, kSlotX, (size_t)chunk * m * p * 2);
+    FHB_PALLOC(sys->pool, d_z, kSlotZ, (size_t)chunk * p * p * 2);
     float ms_factor = 0, ms_refine = 0;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);

@@ -409,86 +409,98 @@ __global__ void __launch_bounds__(128) bwd_panel_kernel2(const Cx<T> *__restrict
 
 // Linv = L11^{-1} for the unit lower triangle of panel [k0, k0+nb) of every
 // matrix (column-major nb x nb, leading dimension nb, matrix f at
-// linv + f * mstride).  One CTA per matrix.  X starts as
-// the identity and is reduced column by column of L11 (right-looking forward
-// substitution on all nb right-hand sides at once):
-//     for k: X[r][j] -= L[r][k] X[k][j]   for r > k, j <= k,
-// with X in shared memory, all threads spread over the (r, j) pairs, and
-// column k+1 of L11 (contiguous in memory) fetched while step k computes.
-// Dynamic shared memory: (nb*nb + 2*nb) complex.
+// linv + f * mstride).  The columns of the inverse are independent
+// triangular solves, so CTA (f, c) forms columns [32c, 32c + 32) of matrix f:
+// X starts as those columns of the identity and is reduced column by column
+// of L11 (right-looking forward substitution),
+//     for k: X[r][j] -= L[r][k] X[k][j]   for r > k,
+// lane = column, warps over rows, X in shared memory, column k+1 of L11
+// (contiguous in memory) fetched while step k computes.
+// Grid (count, ceil(nb / 32)), 256 threads; dynamic shared memory
+// (32 nb + 2 nb) complex.
 template <class T>
 __global__ void __launch_bounds__(256) tri_inverse_kernel(const Cx<T> *__restrict__ a, int64_t m, int k0, int nb,
                                                           Cx<T> *__restrict__ linv, int64_t mstride) {
     extern __shared__ unsigned char smem_raw[];
-    Cx<T> *X = reinterpret_cast<Cx<T> *>(smem_raw);  // X[r * nb + j]
-    Cx<T> *col = X + nb * nb;                          // two staged columns of L11
-    const int f = blockIdx.x, tid = threadIdx.x;
+    Cx<T> *X = reinterpret_cast<Cx<T> *>(smem_raw);  // X[r * 32 + lane]
+    Cx<T> *col = X + 32 * nb;                          // two staged columns of L11
+    const int f = blockIdx.x, j0 = blockIdx.y * 32, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int j = j0 + lane;
     const Cx<T> *A = a + (int64_t)f * m * m + k0 + (int64_t)k0 * m;  // L11(r, k) at A[r + k m]
-    for (int idx = tid; idx < nb * nb; idx += blockDim.x)
-        X[idx] = Cx<T>{(idx / nb == idx % nb) ? (T)1 : (T)0, (T)0};
-    for (int r = tid; r < nb; r += blockDim.x) col[r] = A[r];
+    for (int idx = tid; idx < 32 * nb; idx += blockDim.x)
+        X[idx] = Cx<T>{(idx / 32 == j0 + idx % 32) ? (T)1 : (T)0, (T)0};
+    if (j0 < nb)
+        for (int r = tid; r < nb; r += blockDim.x) col[(j0 & 1) * nb + r] = A[r + (int64_t)j0 * m];
     __syncthreads();
-    for (int k = 0; k + 1 < nb; ++k) {
+    // Columns k < j0 of L do not touch these columns of X (their rows k are zero).
+    for (int k = j0; k + 1 < nb; ++k) {
         const Cx<T> *ck = col + (k & 1) * nb;
         Cx<T> nxt{(T)0, (T)0};
         const bool fetch = k + 2 < nb && tid < nb;
         if (fetch) nxt = A[tid + (int64_t)(k + 1) * m];
-        const int width = k + 1, count = (nb - k - 1) * width;
-        for (int idx = tid; idx < count; idx += blockDim.x) {
-            const int r = k + 1 + idx / width, jj = idx % width;
-            Cx<T> x = X[r * nb + jj];
-            csubmul(x, ck[r], X[k * nb + jj]);
-            X[r * nb + jj] = x;
+        if (j <= k && j < nb) {
+            const Cx<T> xk = X[k * 32 + lane];
+            for (int r = k + 1 + warp; r < nb; r += 8) {
+                Cx<T> x = X[r * 32 + lane];
+                csubmul(x, ck[r], xk);
+                X[r * 32 + lane] = x;
+            }
         }
         if (fetch) col[((k + 1) & 1) * nb + tid] = nxt;
         __syncthreads();
     }
     Cx<T> *out = linv + (int64_t)f * mstride;
-    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+    for (int idx = tid; idx < 32 * nb; idx += blockDim.x) {
         const int r = idx % nb, c = idx / nb;
-        out[r + c * nb] = X[r * nb + c];
+        if (j0 + c < nb) out[r + (int64_t)(j0 + c) * nb] = X[r * 32 + c];
     }
 }
 
 // Uinv = U11^{-1} for the upper triangle (non-unit) of panel [k0, k0+nb),
-// same layout.  Backward, column by column of U11 from the last:
-//     X[k][j] /= U[k][k]                     for j >= k,
-//     X[r][j] -= U[r][k] X[k][j]             for r < k, j >= k.
+// same layout and grid.  Backward, column by column of U11 from the last
+// that reaches these columns:
+//     X[k][j] /= U[k][k];   X[r][j] -= U[r][k] X[k][j]   for r < k.
 template <class T>
 __global__ void __launch_bounds__(256) tri_inverse_upper_kernel(const Cx<T> *__restrict__ a, int64_t m, int k0,
                                                                 int nb, Cx<T> *__restrict__ uinv, int64_t mstride) {
     extern __shared__ unsigned char smem_raw[];
-    Cx<T> *X = reinterpret_cast<Cx<T> *>(smem_raw);  // X[r * nb + j]
-    Cx<T> *col = X + nb * nb;
-    const int f = blockIdx.x, tid = threadIdx.x;
+    Cx<T> *X = reinterpret_cast<Cx<T> *>(smem_raw);  // X[r * 32 + lane]
+    Cx<T> *col = X + 32 * nb;
+    const int f = blockIdx.x, j0 = blockIdx.y * 32, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int j = j0 + lane;
     const Cx<T> *A = a + (int64_t)f * m * m + k0 + (int64_t)k0 * m;  // U11(r, k) at A[r + k m]
-    for (int idx = tid; idx < nb * nb; idx += blockDim.x)
-        X[idx] = Cx<T>{(idx / nb == idx % nb) ? (T)1 : (T)0, (T)0};
-    for (int r = tid; r < nb; r += blockDim.x) col[((nb - 1) & 1) * nb + r] = A[r + (int64_t)(nb - 1) * m];
+    for (int idx = tid; idx < 32 * nb; idx += blockDim.x)
+        X[idx] = Cx<T>{(idx / 32 == j0 + idx % 32) ? (T)1 : (T)0, (T)0};
+    const int klast = min(nb - 1, j0 + 31);  // rows k > klast of these columns are zero
+    for (int r = tid; r <= klast; r += blockDim.x) col[(klast & 1) * nb + r] = A[r + (int64_t)klast * m];
     __syncthreads();
     const Cx<T> one{(T)1, (T)0};
-    for (int k = nb - 1; k >= 0; --k) {
+    for (int k = klast; k >= 0; --k) {
         const Cx<T> *ck = col + (k & 1) * nb;
-        const Cx<T> d = cdiv(one, ck[k]);
-        for (int jj = k + tid; jj < nb; jj += blockDim.x) X[k * nb + jj] = cmul(X[k * nb + jj], d);
         Cx<T> nxt{(T)0, (T)0};
         const bool fetch = k > 0 && tid < k;
         if (fetch) nxt = A[tid + (int64_t)(k - 1) * m];
-        __syncthreads();
-        const int width = nb - k, count = k * width;
-        for (int idx = tid; idx < count; idx += blockDim.x) {
-            const int r = idx / width, jj = k + idx % width;
-            Cx<T> x = X[r * nb + jj];
-            csubmul(x, ck[r], X[k * nb + jj]);
-            X[r * nb + jj] = x;
+        const bool active = j >= k && j < nb;
+        Cx<T> xk{(T)0, (T)0};
+        if (active) {
+            xk = cmul(X[k * 32 + lane], cdiv(one, ck[k]));
+            for (int r = warp; r < k; r += 8) {
+                Cx<T> x = X[r * 32 + lane];
+                csubmul(x, ck[r], xk);
+                X[r * 32 + lane] = x;
+            }
         }
         if (fetch) col[((k - 1) & 1) * nb + tid] = nxt;
         __syncthreads();
+        // Row k is read by every warp above; it is final once all have read it,
+        // and no later step reads it again.
+        if (active && warp == 0) X[k * 32 + lane] = xk;
     }
+    __syncthreads();
     Cx<T> *out = uinv + (int64_t)f * mstride;
-    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+    for (int idx = tid; idx < 32 * nb; idx += blockDim.x) {
         const int r = idx % nb, c = idx / nb;
-        out[r + c * nb] = X[r * nb + c];
+        if (j0 + c < nb) out[r + (int64_t)(j0 + c) * nb] = X[r * 32 + c];
     }
 }
 
@@ -756,7 +768,8 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
     const int outer = w.outer;
     if (nb % 16 || nb > 128 || outer % nb || !w.coop || !w.linv || !w.pack_a || !w.pack_b)
         return fail(err, FH_ERR_INVALID_ARGUMENT, "two-level factorization needs nb | outer, nb <= 128 and scratch");
-    const size_t inv_smem = sizeof(C) * ((size_t)nb * nb + 2 * (size_t)nb);
+    const size_t inv_smem = sizeof(C) * (34 * (size_t)nb);
+    const dim3 inv_grid((unsigned)count, (unsigned)((nb + 31) / 32));
     FHB_CUDA(cudaFuncSetAttribute(tri_inverse_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)inv_smem));
     FHB_CUDA(cudaFuncSetAttribute(tri_inverse_upper_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -783,10 +796,10 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             if (st) return st;
             prof_begin(s, FH_PROF_TRSM);
             const int64_t mstride = (int64_t)nb * nb;  // a partial last block keeps the full slot stride
-            tri_inverse_kernel<float><<<count, 256, inv_smem, s>>>(a, m, (int)j0, wj, linv, mstride);
+            tri_inverse_kernel<float><<<inv_grid, 256, inv_smem, s>>>(a, m, (int)j0, wj, linv, mstride);
             if (w.uinv)
-                tri_inverse_upper_kernel<float><<<count, 256, inv_smem, s>>>(a, m, (int)j0, wj, slot(w.uinv, j0),
-                                                                             mstride);
+                tri_inverse_upper_kernel<float><<<inv_grid, 256, inv_smem, s>>>(a, m, (int)j0, wj, slot(w.uinv, j0),
+                                                                                mstride);
             if (r1 >= m) {
                 prof_end(s, FH_PROF_TRSM, 0.0);
                 break;
@@ -878,10 +891,11 @@ fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaS
             // U12 = L11^{-1} A12 as an explicit triangular inverse times A12:
             // the product runs as a GEMM (tensor cores in the mixed form).
             C *linv = reinterpret_cast<C *>(w.linv);
-            const size_t inv_smem = sizeof(C) * ((size_t)w_nb * w_nb + 2 * (size_t)w_nb);
+            const size_t inv_smem = sizeof(C) * (34 * (size_t)w_nb);
             FHB_CUDA(cudaFuncSetAttribute(tri_inverse_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)inv_smem));
-            tri_inverse_kernel<T><<<b.count, 256, inv_smem, s>>>(a, m, (int)k0, w_nb, linv, (int64_t)w_nb * w_nb);
+            tri_inverse_kernel<T><<<dim3((unsigned)b.count, (unsigned)((w_nb + 31) / 32)), 256, inv_smem, s>>>(
+                a, m, (int)k0, w_nb, linv, (int64_t)w_nb * w_nb);
             if (tc_apply) {
                 fh_status st = gemm_tc_tri_apply(reinterpret_cast<const float *>(w.linv), w_nb,
                                                  reinterpret_cast<float *>(b.a), m, b.count, k0, s, err);

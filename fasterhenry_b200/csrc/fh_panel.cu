@@ -273,19 +273,24 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_k
         // Column k0+w (t = 0) starts the next sub-panel: its arg-max is taken here.
         best = -1.0;
         bi = INT_MAX;
-        // Columns go 8 at a time with their loads issued together (the
-        // sub-panel width w is 16 here: only the last sub-panel is narrower,
-        // and it has no columns to its right).
-        constexpr int kT = sizeof(T) == 4 ? 8 : 4;
+        // Columns go kT at a time, double-buffered: the loads of the next
+        // batch are in flight while the current one is updated and stored
+        // (the sub-panel width w is 16 here: only the last sub-panel is
+        // narrower, and it has no columns to its right).
+        constexpr int kT = 4;
         for (int64_t i = max(r_begin, k0 + w) + tid; i < r_end; i += kThreads) {
-            Cx<T> l[kW];
+            const Cx<T> *row = A + i + (k0 + w) * m;  // column k0+w+t at row[t m]
+            Cx<T> l[kW], y[kT], yn[kT];
 #pragma unroll
             for (int r = 0; r < kW; ++r) l[r] = ldcg(A + i + (k0 + r) * m);
+#pragma unroll
+            for (int q = 0; q < kT; ++q)
+                if (q < rest) y[q] = ldcg(row + (int64_t)q * m);
             for (int t0 = 0; t0 < rest; t0 += kT) {
-                Cx<T> y[kT];
+                const int tn = t0 + kT;
 #pragma unroll
                 for (int q = 0; q < kT; ++q)
-                    if (t0 + q < rest) y[q] = ldcg(A + i + (k0 + w + t0 + q) * m);
+                    if (tn + q < rest) yn[q] = ldcg(row + (int64_t)(tn + q) * m);
 #pragma unroll
                 for (int q = 0; q < kT; ++q) {
                     if (t0 + q < rest) {
@@ -301,6 +306,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_k
                         bi = (int)i;
                     }
                 }
+#pragma unroll
+                for (int q = 0; q < kT; ++q) y[q] = yn[q];
             }
         }
         fused = true;

@@ -242,10 +242,24 @@ def run_ours(args):
         peak = 80.0  # FP32 SIMT nominal (no measured figure)
         unit = "TFLOP/s"
         bound = "fp32-simt"
-    roofline = {"kernel": gemm_cls, "bound": bound, "achieved": round(achieved, 2), "peak": peak,
+    traffic = None
+    if gemm_cls == "gemm_tc":
+        # DRAM bytes per launch: the ncu capture of packed_update_kernel on the
+        # 2,400-filament meander moved 0.985 x its algorithmic bytes (C read +
+        # write, 16 B per entry, plus the packed operands once); scaled here to
+        # the algorithmic C bytes of this run's average launch (work / 256 at
+        # K = 512, i.e. 16 B per 8 * 512 flops).
+        traffic = round(0.985 * (g["work"] / gemm_launches) / 256.0 * 1.03, 1)
+    roofline = {"kernel": "packed_update_kernel (deep split-BF16x3 trailing update, K = 512)"
+                if gemm_cls == "gemm_tc" else gemm_cls,
+                "bound": bound, "achieved": round(achieved, 2), "peak": peak,
                 "unit": unit, "frac": round(achieved / peak, 4) if peak else None,
-                "peak_source": peak_kind if gemm_cls == "gemm_tc" else "nominal",
-                "traffic": None, "per_launch_ms": round(per_launch_ms, 4), "launches": g["launches"]}
+                "peak_source": ("measured bf16 burst (MEASURED_PEAKS.json)" if peak_kind == "measured" else peak_kind)
+                if gemm_cls == "gemm_tc" else "nominal",
+                "traffic": traffic, "traffic_unit": "bytes per launch",
+                "traffic_source": "ncu dram__bytes_read+write of packed_update_kernel (2,400-filament meander), "
+                                  "scaled by algorithmic bytes",
+                "per_launch_ms": round(per_launch_ms, 4), "launches": g["launches"]}
     launches = sum(v["launches"] for v in profile.values())
 
     out = {

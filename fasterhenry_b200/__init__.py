@@ -2,7 +2,8 @@
 
 Filament-pair partial-inductance fill, mesh assembly ``Zm = M(R + jwL)M^T``
 and a batched complex LU per frequency (FP64, or FP32 with split-BF16 tensor
-trailing updates and FP64 iterative refinement), exposed through a C ABI
+trailing updates and FP64 iterative refinement), and the matrix-free
+precorrected-FFT operator with GMRES, exposed through a C ABI
 (include/fasterhenry_b200.h) and this Python mirror of the reference's API.
 """
 from .api import (DENSE_PATH_MAX_FILAMENTS, MU0, CoincidentSamples, DiscretizeError, Discretization,
@@ -11,6 +12,6 @@ from .api import (DENSE_PATH_MAX_FILAMENTS, MU0, CoincidentSamples, DiscretizeEr
                   SegmentDef, Singular, SolverChoice, SweepResult, Unsupported, build_info, device_count, discretize,
                   lu_solve, mesh_matrix, mutual_inductance, partial_inductance_matrix, self_inductance, skin_depth,
                   solve)
-from .api import Profiler, fill_stats
+from .api import PfftError, PfftOperator, PfftParams, Profiler, fill_stats
 
 __version__ = "0.1.0"

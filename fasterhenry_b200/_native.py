@@ -68,6 +68,19 @@ class SweepReport(ctypes.Structure):
                 ("solve_s", ctypes.c_double), ("factor_s", ctypes.c_double), ("refine_s", ctypes.c_double)]
 
 
+class PfftParams(ctypes.Structure):
+    _fields_ = [("spacing_kind", ctypes.c_int32), ("interpolation_order", ctypes.c_int32),
+                ("cells_per_filament", ctypes.c_double), ("spacing", ctypes.c_double),
+                ("near_field_radius", ctypes.c_double)]
+
+
+class PfftStats(ctypes.Structure):
+    _fields_ = [("filaments", ctypes.c_int64), ("grid_spacing", ctypes.c_double), ("grid_dims", ctypes.c_int64 * 3),
+                ("fft_dims", ctypes.c_int64 * 3), ("projection_entries", ctypes.c_int64),
+                ("near_entries", ctypes.c_int64), ("memory_bytes", ctypes.c_int64), ("setup_host_s", ctypes.c_double),
+                ("setup_device_s", ctypes.c_double)]
+
+
 # Status codes (fh_status)
 OK = 0
 ERR_INVALID_ARGUMENT = 1
@@ -94,7 +107,8 @@ EXPORTS = [
     "fh_system_counts", "fh_system_timing", "fh_system_filaments", "fh_system_resistances",
     "fh_system_mesh_matrices", "fh_system_device_l_mesh", "fh_sweep", "fh_impedance", "fh_sweep_json",
     "fh_write_zc_mat", "fh_spice_subckt", "fh_system_fill_stats", "fh_profile_enable", "fh_profile_reset",
-    "fh_profile_read",
+    "fh_profile_read", "fh_pfft_default_params", "fh_pfft_create", "fh_pfft_apply", "fh_pfft_get_stats",
+    "fh_pfft_destroy",
 ]
 
 PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner"]
@@ -134,6 +148,13 @@ def load():
     L.fh_lu_solve_c64.argtypes = [c_double_p, sz, c_double_p, sz, c_double_p, ei]
     L.fh_system_create.argtypes = [P(Node), sz, P(SegmentDef), sz, P(Port), sz, P(Discretization), ctypes.c_int,
                                    P(ctypes.c_void_p), ei]
+    L.fh_pfft_default_params.argtypes = [P(PfftParams)]
+    L.fh_pfft_default_params.restype = None
+    L.fh_pfft_create.argtypes = [P(Filament), sz, P(PfftParams), P(ctypes.c_void_p), ei]
+    L.fh_pfft_apply.argtypes = [ctypes.c_void_p, c_double_p, c_double_p, sz, ei]
+    L.fh_pfft_get_stats.argtypes = [ctypes.c_void_p, P(PfftStats)]
+    L.fh_pfft_destroy.argtypes = [ctypes.c_void_p]
+    L.fh_pfft_destroy.restype = None
     L.fh_system_destroy.argtypes = [ctypes.c_void_p]
     L.fh_system_destroy.restype = None
     L.fh_system_counts.argtypes = [ctypes.c_void_p, P(Counts)]

@@ -111,13 +111,18 @@ class Unsupported(FasterHenryError):
     status = N.ERR_UNSUPPORTED
 
 
+class PfftError(FasterHenryError):
+    """PfftError::{InvalidParameter, GridTooLarge} (pfft/mod.rs:234-253)."""
+    status = N.ERR_PFFT
+
+
 class InvalidArgument(FasterHenryError, ValueError):
     status = N.ERR_INVALID_ARGUMENT
 
 
 _ERRORS = {c.status: c for c in (NoDevice, CudaError, OutOfMemory, GeometryError, DiscretizeError, CoincidentSamples,
                                  NotFinite, MeshError, InvalidGrading, InvalidFrequency, Singular, NotConverged,
-                                 Unsupported, InvalidArgument)}
+                                 Unsupported, InvalidArgument, PfftError)}
 
 
 def _check(status: int, info: Optional[N.ErrorInfo] = None) -> None:
@@ -572,6 +577,88 @@ def solve(geometry, ports: Sequence, discretization: dict, frequencies: Sequence
     """MeshSystem.assemble followed by MeshSystem.sweep (solve.rs:931-938)."""
     with MeshSystem.assemble(geometry, ports, discretization) as system:
         return system.sweep(frequencies, precision)
+
+
+# ---------------------------------------------------------------------------
+# Matrix-free path: the precorrected-FFT operator (pfft/mod.rs)
+# ---------------------------------------------------------------------------
+@dataclasses.dataclass(frozen=True)
+class PfftParams:
+    """PfftParams (pfft/mod.rs:183-232).  ``spacing`` None means
+    GridSpacing::Auto with ``cells_per_filament``; a float is
+    GridSpacing::Fixed in metres."""
+    cells_per_filament: float = 8.0
+    spacing: Optional[float] = None
+    near_field_radius: float = 8.0
+    interpolation_order: int = 5
+
+    def _native(self) -> N.PfftParams:
+        p = N.PfftParams()
+        p.spacing_kind = 0 if self.spacing is None else 1
+        p.interpolation_order = int(self.interpolation_order)
+        p.cells_per_filament = float(self.cells_per_filament)
+        p.spacing = float(self.spacing or 0.0)
+        p.near_field_radius = float(self.near_field_radius)
+        return p
+
+
+class PfftOperator:
+    """Matrix-free partial-inductance operator: ``apply(x)`` = L x without
+    forming L (PfftOperator::new / apply / stats, pfft/mod.rs:332-597).
+    Set-up on the host and the device; products on the device."""
+
+    def __init__(self, filaments: np.ndarray, params: Optional[PfftParams] = None):
+        f = np.ascontiguousarray(filaments, dtype=np.float64).reshape(-1, FILAMENT_FIELDS)
+        self._n = len(f)
+        arr = _fil_array(f)
+        p = (params or PfftParams())._native()
+        h = ctypes.c_void_p()
+        info = N.ErrorInfo()
+        _check(N.load().fh_pfft_create(arr, self._n, ctypes.byref(p), ctypes.byref(h), ctypes.byref(info)), info)
+        self._h = h
+
+    def __len__(self) -> int:
+        return self._n
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            N.load().fh_pfft_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def apply(self, x: np.ndarray) -> np.ndarray:
+        """L x for one vector (length n) or several (count x n)."""
+        x = np.asarray(x, dtype=np.float64)
+        one = x.ndim == 1
+        xs = np.ascontiguousarray(x.reshape(1, -1) if one else x)
+        if xs.shape[1] != self._n:
+            raise InvalidArgument("pFFT operator of dimension %d applied to a vector of length %d"
+                                  % (self._n, xs.shape[1]))
+        y = np.zeros_like(xs)
+        info = N.ErrorInfo()
+        _check(N.load().fh_pfft_apply(self._h, xs.ctypes.data_as(N.c_double_p), y.ctypes.data_as(N.c_double_p),
+                                      xs.shape[0], ctypes.byref(info)), info)
+        return y[0] if one else y
+
+    def stats(self) -> Dict[str, object]:
+        s = N.PfftStats()
+        _check(N.load().fh_pfft_get_stats(self._h, ctypes.byref(s)))
+        return {"filaments": int(s.filaments), "grid_spacing": float(s.grid_spacing),
+                "grid_dims": [int(v) for v in s.grid_dims], "fft_dims": [int(v) for v in s.fft_dims],
+                "projection_entries": int(s.projection_entries), "near_entries": int(s.near_entries),
+                "memory_bytes": int(s.memory_bytes), "setup_host_s": float(s.setup_host_s),
+                "setup_device_s": float(s.setup_device_s)}
 
 
 def skin_depth(frequency_hz: float, sigma: float) -> float:

@@ -71,6 +71,10 @@ struct FillStats {
 };
 fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_methods, cudaStream_t stream,
                       FillStats *stats, fh_error_info *err);
+// The same evaluation for an explicit list of filament pairs: d_out[k] =
+// L(pairs[k].x, pairs[k].y), zero for orthogonal pairs.
+fh_status device_fill_pairs(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t n_pairs, double *d_out,
+                            cudaStream_t stream, FillStats *stats, fh_error_info *err);
 
 // R_m = M diag(R) M^T and L_m = M L M^T (loops x loops, column-major), upper
 // triangle evaluated in the reference's order and mirrored.

@@ -226,10 +226,17 @@ __device__ void record_error(DevError *e, int i, int j, int code) {
 }
 
 // Writes L[i][j] = L[j][i] and the method, or records a non-finite value.
-__device__ __forceinline__ void store_pair(double *L, int8_t *methods, int64_t n, int i, int j, double v, int8_t m,
+// Pair-list mode (n == 0): L and methods are indexed by the item's slot.
+__device__ __forceinline__ void store_pair(double *L, int8_t *methods, int64_t n, const int4 &it, double v, int8_t m,
                                            DevError *e) {
+    const int i = it.x, j = it.y;
     if (!isfinite(v)) {
         record_error(e, i, j, FH_ERR_KERNEL_NOT_FINITE);
+        return;
+    }
+    if (n == 0) {
+        L[it.w] = v;
+        if (methods) methods[it.w] = m;
         return;
     }
     L[(int64_t)i + (int64_t)j * n] = v;
@@ -295,6 +302,44 @@ __global__ void __launch_bounds__(256) classify_kernel(const DevFil *__restrict_
     }
 }
 
+// Classification of an explicit list of pairs (pair-list mode): the same
+// passes, one thread per pair; items carry the pair's slot in .w.
+template <bool kWrite>
+__global__ void __launch_bounds__(256) classify_list_kernel(const DevFil *__restrict__ fil,
+                                                            const int2 *__restrict__ pairs, int64_t count,
+                                                            unsigned long long *__restrict__ counts,
+                                                            unsigned long long *__restrict__ cursor,
+                                                            int4 *__restrict__ items) {
+    __shared__ unsigned s_count[kCats];
+    __shared__ unsigned long long s_base[kCats];
+    if (threadIdx.x < kCats) s_count[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    Classified cls;
+    cls.cat = -1;
+    unsigned slot = 0;
+    int2 pr = make_int2(0, 0);
+    if (t < count) {
+        pr = pairs[t];
+        cls = classify(fil[pr.x], fil[pr.y]);
+        if (cls.cat >= 0) slot = atomicAdd(&s_count[cls.cat], 1u);
+    }
+    __syncthreads();
+    if (!kWrite) {
+        if (threadIdx.x < kCats && s_count[threadIdx.x])
+            atomicAdd(&counts[threadIdx.x], (unsigned long long)s_count[threadIdx.x]);
+        return;
+    }
+    if (threadIdx.x < kCats)
+        s_base[threadIdx.x] =
+            s_count[threadIdx.x] ? atomicAdd(&cursor[threadIdx.x], (unsigned long long)s_count[threadIdx.x]) : 0ull;
+    __syncthreads();
+    if (cls.cat >= 0) {
+        const int a = cls.swap ? pr.y : pr.x, b = cls.swap ? pr.x : pr.y;
+        items[s_base[cls.cat] + slot] = make_int4(a, b, cls.orders, (int)t);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Point quadrature (neumann.rs:196-266), thread per pair.
 // ---------------------------------------------------------------------------
@@ -351,7 +396,7 @@ __global__ void __launch_bounds__(128) point_kernel(const DevFil *__restrict__ f
             }
         }
         const double cosv = ndot(A.axes, B.axes);
-        store_pair(L, methods, n, it.x, it.y, kMu0Over4Pi * (total * cosv), kPoint, err);
+        store_pair(L, methods, n, it, kMu0Over4Pi * (total * cosv), kPoint, err);
     }
 }
 
@@ -426,7 +471,7 @@ __global__ void __launch_bounds__(128) closed_form_kernel(const DevFil *__restri
         if (rel <= kClosedFormMaxError) {
             const double cosv = ndot(A.axes, B.axes);
             const double scale = signum(cosv) / (A.area * B.area);
-            store_pair(L, methods, n, it.x, it.y, kMu0Over4Pi * (v * scale), kClosedForm, err);
+            store_pair(L, methods, n, it, kMu0Over4Pi * (v * scale), kClosedForm, err);
         } else {
             unsigned long long k = atomicAdd(quad_count, 1ull);
             quad_items[k] = it;
@@ -676,7 +721,7 @@ __global__ void aligned_scatter_kernel(const DevFil *__restrict__ fil, const int
         const DevFil &B = fil[it.y];
         const double cosv = ndot(A.axes, B.axes);
         const double scale = signum(cosv) / (A.area * B.area);
-        store_pair(L, methods, n, it.x, it.y, kMu0Over4Pi * (head_value[head_of[t]] * scale), kAlignedQuadrature,
+        store_pair(L, methods, n, it, kMu0Over4Pi * (head_value[head_of[t]] * scale), kAlignedQuadrature,
                    err);
     }
 }
@@ -847,7 +892,7 @@ __global__ void __launch_bounds__(128) sampled_kernel(const DevFil *__restrict__
                 record_error(err, it.x, it.y, FH_ERR_KERNEL_COINCIDENT);
             } else {
                 const double direction = parallel ? signum(cosv) : cosv;
-                store_pair(L, methods, n, it.x, it.y, kMu0Over4Pi * (acc * direction), kSampled, err);
+                store_pair(L, methods, n, it, kMu0Over4Pi * (acc * direction), kSampled, err);
             }
         }
     }
@@ -923,10 +968,19 @@ namespace {
 bool g_tables_uploaded[64] = {false};
 }
 
-fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_methods, cudaStream_t stream,
-                      FillStats *stats, fh_error_info *err) {
-    if (n == 0) return FH_OK;
+namespace {
+
+// The fill pipeline: classification, then the method kernels.  With
+// d_pairs == nullptr it evaluates the upper triangle of the n x n matrix
+// into d_L (mirrored); with a pair list it evaluates those pairs into
+// d_L[k] (pair-list mode: orthogonal pairs are zero).
+fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t n_pairs, double *d_L,
+                   int8_t *d_methods, cudaStream_t stream, FillStats *stats, fh_error_info *err) {
+    const bool list = d_pairs != nullptr;
+    if (list ? n_pairs == 0 : n == 0) return FH_OK;
     if (n > 2000000000LL / 32) return fail(err, FH_ERR_INVALID_ARGUMENT, "too many filaments for the fill");
+    if (list && n_pairs > INT32_MAX) return fail(err, FH_ERR_INVALID_ARGUMENT, "too many pairs for one list fill");
+    const int64_t n_arg = list ? 0 : n;  // the method kernels' store mode
     int dev = 0;
     FHB_CUDA(cudaGetDevice(&dev));
     if (dev < 64 && !g_tables_uploaded[dev]) {
@@ -938,7 +992,8 @@ fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_met
     FillStats local;
     FillStats &st = stats ? *stats : local;
     st = FillStats();
-    st.pairs = n * (n + 1) / 2;
+    st.pairs = list ? n_pairs : n * (n + 1) / 2;
+    if (list) FHB_CUDA(cudaMemsetAsync(d_L, 0, sizeof(double) * n_pairs, stream));
     cudaEvent_t ev[6];
     for (auto &e : ev) FHB_CUDA(cudaEventCreate(&e));
     struct Guard {
@@ -964,8 +1019,13 @@ fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_met
     FHB_CUDA(cudaMemsetAsync(&d_err->code, 0, sizeof(int), stream));
     const int T = (int)((n + 31) / 32);
     dim3 grid(T, T), block(32, 8);
+    const unsigned list_blocks = (unsigned)((n_pairs + 255) / 256);
     FHB_CUDA(cudaEventRecord(ev[0], stream));
-    classify_kernel<false><<<grid, block, 0, stream>>>(d_fil, (int)n, d_counts, nullptr, nullptr);
+    if (list)
+        classify_list_kernel<false><<<list_blocks, 256, 0, stream>>>(d_fil, d_pairs, n_pairs, d_counts, nullptr,
+                                                                      nullptr);
+    else
+        classify_kernel<false><<<grid, block, 0, stream>>>(d_fil, (int)n, d_counts, nullptr, nullptr);
     FHB_CUDA(cudaGetLastError());
     unsigned long long counts[kCats];
     FHB_CUDA(cudaMemcpyAsync(counts, d_counts, sizeof counts, cudaMemcpyDeviceToHost, stream));
@@ -977,7 +1037,11 @@ fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_met
     int4 *d_items = nullptr;
     FHB_CUDA(alloc((void **)&d_items, sizeof(int4) * total_items));
     FHB_CUDA(cudaMemcpyAsync(d_cursor, offsets, sizeof(unsigned long long) * kCats, cudaMemcpyHostToDevice, stream));
-    classify_kernel<true><<<grid, block, 0, stream>>>(d_fil, (int)n, nullptr, d_cursor, d_items);
+    if (list)
+        classify_list_kernel<true><<<list_blocks, 256, 0, stream>>>(d_fil, d_pairs, n_pairs, nullptr, d_cursor,
+                                                                     d_items);
+    else
+        classify_kernel<true><<<grid, block, 0, stream>>>(d_fil, (int)n, nullptr, d_cursor, d_items);
     FHB_CUDA(cudaGetLastError());
     FHB_CUDA(cudaEventRecord(ev[1], stream));
     const int sms = 148;
@@ -987,7 +1051,7 @@ fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_met
     for (int c = 0; c < kPointBuckets; ++c) st.point_evaluations += (double)counts[c] * (1.5 * (double)(1ull << c));
     if (n_point) {
         int blocks = (int)std::min<int64_t>((n_point + 127) / 128, (int64_t)sms * 64);
-        point_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_items, n_point, d_L, d_methods, n, d_err);
+        point_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_items, n_point, d_L, d_methods, n_arg, d_err);
         FHB_CUDA(cudaGetLastError());
     }
     FHB_CUDA(cudaEventRecord(ev[2], stream));
@@ -1001,7 +1065,7 @@ fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_met
     if (n_aligned) {
         FHB_CUDA(alloc((void **)&d_quad, sizeof(int4) * n_aligned));
         int blocks = (int)std::min<int64_t>((n_aligned + 127) / 128, (int64_t)sms * 32);
-        closed_form_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_aligned, n_aligned, d_L, d_methods, n, d_quad,
+        closed_form_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_aligned, n_aligned, d_L, d_methods, n_arg, d_quad,
                                                        d_qcount, d_err);
         FHB_CUDA(cudaGetLastError());
         unsigned long long q = 0;
@@ -1066,7 +1130,7 @@ fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_met
         aligned_quadrature_kernel<<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads, d_values);
         FHB_CUDA(cudaGetLastError());
         aligned_scatter_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_quad, d_item_head, d_values, n_quad, d_L,
-                                                           d_methods, n, d_err);
+                                                           d_methods, n_arg, d_err);
         FHB_CUDA(cudaGetLastError());
     }
     FHB_CUDA(cudaEventRecord(ev[4], stream));
@@ -1074,8 +1138,8 @@ fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_met
     st.sampled = n_sampled;
     if (n_sampled) {
         int blocks = (int)std::min<int64_t>((n_sampled * 32 + 127) / 128, (int64_t)sms * 32);
-        sampled_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_items + offsets[kCatSampled], n_sampled, d_L, d_methods, n,
-                                                   d_err);
+        sampled_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_items + offsets[kCatSampled], n_sampled, d_L, d_methods,
+                                                   n_arg, d_err);
         FHB_CUDA(cudaGetLastError());
     }
     FHB_CUDA(cudaEventRecord(ev[5], stream));
@@ -1101,6 +1165,18 @@ fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_met
                     i, j);
     }
     return FH_OK;
+}
+
+}  // namespace
+
+fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_methods, cudaStream_t stream,
+                      FillStats *stats, fh_error_info *err) {
+    return fill_run(d_fil, n, nullptr, 0, d_L, d_methods, stream, stats, err);
+}
+
+fh_status device_fill_pairs(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t n_pairs, double *d_out,
+                            cudaStream_t stream, FillStats *stats, fh_error_info *err) {
+    return fill_run(d_fil, n, d_pairs, n_pairs, d_out, nullptr, stream, stats, err);
 }
 
 fh_status device_congruence(const double *d_L, const double *d_R, int64_t n, const int64_t *d_row_ptr,

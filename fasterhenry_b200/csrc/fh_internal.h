@@ -31,6 +31,9 @@ fh_status discretize_geometry(const fh_node *nodes, size_t n_nodes, const fh_seg
                               size_t n_segs, const fh_discretization *disc, Discretized &out,
                               fh_error_info *err);
 
+// n-point Gauss-Legendre rule on [-1, 1] (gauss.rs:25-75), nodes ascending.
+void gauss_rule(int n, double *nodes, double *weights);
+
 // Loop basis, CSR.
 struct LoopBasis {
     std::vector<int64_t> row_ptr;

@@ -1,0 +1,121 @@
+// Internal declarations of the precorrected-FFT operator (pfft/mod.rs,
+// grid.rs, fft.rs, near.rs of the reference).  The set-up runs on the host
+// (fh_pfft_setup.cpp), except the exact partial inductance of the near pairs,
+// which the device fill evaluates; the products run on the device
+// (fh_pfft.cu).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "fh_internal.h"
+
+namespace fhb {
+
+// Uniform grid (grid.rs:44-95): point (i, j, k) at origin + h (i, j, k),
+// linear index (i dims[1] + j) dims[2] + k.
+struct PfftGrid {
+    double origin[3] = {0, 0, 0};
+    double spacing = 0;
+    int64_t dims[3] = {0, 0, 0};
+    int stencil = 0;  // interpolation points per axis, order + 1
+    int64_t len() const { return dims[0] * dims[1] * dims[2]; }
+};
+
+// Everything the device operator needs, built on the host.
+struct PfftSetup {
+    int64_t n = 0;
+    PfftGrid grid;
+    int64_t padded[3] = {0, 0, 0};
+    // Projection weights per filament (CSR) and per grid point (transpose).
+    std::vector<int64_t> proj_offsets;
+    std::vector<uint32_t> proj_index;
+    std::vector<double> proj_weight;
+    std::vector<int64_t> spread_offsets;
+    std::vector<uint32_t> spread_filament;
+    std::vector<double> spread_weight;
+    std::vector<double> directions;  // 3 n, unit length vectors
+    std::vector<int> components;     // Cartesian components some direction carries
+    // Near pairs i <= j that are not orthogonal, row-major by i, with the
+    // grid's approximation sum_g sum_h W_ig W_jh K(g - h) and cos(i, j).
+    std::vector<int32_t> pair_i, pair_j;
+    std::vector<double> pair_grid, pair_cos;
+};
+
+// Parameters (PfftParams, pfft/mod.rs:183-232), validated.
+struct PfftConfig {
+    bool fixed_spacing = false;
+    double cells_per_filament = 8.0;
+    double spacing = 0.0;
+    double near_field_radius = 8.0;
+    int order = 5;
+};
+
+// Largest padded FFT grid, in points (MAX_FFT_POINTS, pfft/mod.rs:168).
+constexpr int64_t kMaxFftPoints = int64_t(1) << 26;
+
+// Smallest 2^a 3^b 5^c >= n (fft.rs:66-80) and the padded size of an axis.
+int64_t smooth_size(int64_t n);
+inline int64_t padded_size(int64_t n) { return smooth_size(2 * n - 1); }
+
+// The spacing h for which prod_a max(extent_a / h, 1) = cells (auto_spacing,
+// pfft/mod.rs:614-631).
+double auto_spacing(const double extent[3], double cells);
+
+// Builds grid, projections, near pairs and their grid approximations.
+fh_status pfft_setup(const fh_filament *fil, int64_t n, const PfftConfig &cfg, PfftSetup &out, fh_error_info *err);
+
+// The grid kernel 1 / |r_g - r_h| for an integer offset, zero at the origin
+// (near.rs:114-123).
+inline double grid_kernel(int64_t dx, int64_t dy, int64_t dz, double spacing);
+
+// The operator on the device (fh_pfft.cu).  Owns its device memory and its
+// FFT plans; products run on `stream`.
+struct PfftDevice {
+    int64_t n = 0, G = 0, P = 0;  // filaments, grid points, padded points
+    PfftGrid grid;
+    int64_t padded[3] = {0, 0, 0};
+    std::vector<int> components;
+    double *d_dir = nullptr;
+    int64_t *d_proj_off = nullptr;
+    uint32_t *d_proj_idx = nullptr;
+    double *d_proj_w = nullptr;
+    int64_t *d_spread_off = nullptr;
+    uint32_t *d_spread_fil = nullptr;
+    double *d_spread_w = nullptr;
+    int64_t *d_near_off = nullptr;
+    uint32_t *d_near_col = nullptr;
+    double *d_near_val = nullptr;
+    double *d_spectrum = nullptr;  // real spectrum of the kernel with the 1 / P of the inverse transform
+    void *d_work = nullptr;        // complex padded grids, reused across products
+    size_t work_bytes = 0;
+    std::vector<std::pair<int, int>> plans;  // (batch, cufftHandle)
+    void *stream = nullptr;                  // cudaStream_t
+    bool own_stream = false;
+    int64_t projection_entries = 0, near_entries = 0;
+    double setup_host_s = 0, setup_device_s = 0;
+    PfftDevice() = default;
+    PfftDevice(const PfftDevice &) = delete;
+    PfftDevice &operator=(const PfftDevice &) = delete;
+    ~PfftDevice();
+    size_t memory_bytes() const;
+};
+
+// Builds the operator for `fil` (host set-up, exact near pairs on the device,
+// kernel spectrum).  `stream` may be null: the operator then owns one.
+fh_status pfft_build(const fh_filament *fil, int64_t n, const PfftConfig &cfg, void *stream, PfftDevice &op,
+                     fh_error_info *err);
+// y = L x for `count` vectors of length n (device pointers, vector v at
+// x + v n), on op.stream.
+fh_status pfft_apply(PfftDevice &op, const double *d_x, double *d_y, int count, fh_error_info *err);
+
+}  // namespace fhb
+
+#include <cmath>
+
+namespace fhb {
+inline double grid_kernel(int64_t dx, int64_t dy, int64_t dz, double spacing) {
+    const double r2 = (double)(dx * dx + dy * dy + dz * dz);
+    return r2 == 0.0 ? 0.0 : 1.0 / (spacing * std::sqrt(r2));
+}
+}  // namespace fhb

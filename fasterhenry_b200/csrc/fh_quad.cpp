@@ -55,6 +55,8 @@ void legendre_rule(int n, double *nodes, double *weights) {
 
 }  // namespace
 
+void gauss_rule(int n, double *nodes, double *weights) { legendre_rule(n, nodes, weights); }
+
 void host_quad_tables(QuadTables &t) {
     for (int n = 0; n <= kMaxRule; ++n)
         for (int k = 0; k < kMaxRule; ++k) t.nodes[n][k] = t.weights[n][k] = 0.0;

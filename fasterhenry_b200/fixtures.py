@@ -202,3 +202,65 @@ def random_spirals(count: int = 64, seed: int = 2026) -> List[Deck]:
         decks.append(square_spiral(turns, width, spacing, thickness, outer, uniform(nw, nh),
                                    name="spiral_%d" % len(decks)))
     return decks
+
+
+# ---------------------------------------------------------------------------
+# Random filament clouds (the pFFT accuracy fixtures)
+# ---------------------------------------------------------------------------
+
+def cloud_side(n: int) -> float:
+    """Side of the cube holding n filaments at 400 filaments per 1,000 mm^3."""
+    return 10e-3 * (n / 400.0) ** (1.0 / 3.0)
+
+
+def cloud_bars(n: int, side: float, manhattan: bool, seed: int):
+    """n bars of length 0.5-1.5 mm in a cube of side `side`, axis-aligned
+    (random axis and sense) or in general position, cross-sections
+    0.1-0.3 x 0.05-0.15 mm; drawn from SplitMix64(seed)."""
+    r = SplitMix64(seed)
+    nodes, segs = [], []
+    for _ in range(n):
+        a = [side * r.uniform(0.0, 1.0) for _ in range(3)]
+        length = 1e-3 * (0.5 + r.uniform(0.0, 1.0))
+        if manhattan:
+            d = [0.0, 0.0, 0.0]
+            d[min(2, int(r.uniform(0.0, 1.0) * 3.0))] = -1.0 if r.uniform(0.0, 1.0) < 0.5 else 1.0
+        else:
+            v = [r.uniform(-0.5, 0.5) for _ in range(3)]
+            norm = math.sqrt(sum(c * c for c in v))
+            d = [c / norm for c in v]
+        b = [a[k] + length * d[k] for k in range(3)]
+        width = 0.1e-3 + 0.2e-3 * r.uniform(0.0, 1.0)
+        height = 0.05e-3 + 0.1e-3 * r.uniform(0.0, 1.0)
+        nodes += [tuple(a), tuple(b)]
+        segs.append(segment(len(nodes) - 2, len(nodes) - 1, width, height))
+    return nodes, segs
+
+
+def cloud_deck(n: int, manhattan: bool, seed: int, side: Optional[float] = None) -> Deck:
+    """The cloud as a deck of unconnected one-filament segments (no ports)."""
+    nodes, segs = cloud_bars(n, cloud_side(n) if side is None else side, manhattan, seed)
+    return Deck(nodes, segs, [], uniform(1, 1), "cloud_%d" % n)
+
+
+def scaling_meander(bars: int, pitch: float = 100e-6, width: float = 20e-6, thickness: float = 10e-6,
+                    nw: int = 2, nh: int = 2) -> Deck:
+    """A square meander of `bars` runs along +-x, each cut into `bars`
+    collinear segments one pitch long, joined by one-pitch jogs along +y
+    (bars (bars + 1) segments; 4 bars (bars + 1) filaments at 2 x 2).  One
+    port spans the chain.  bars = 157 gives 99,224 filaments, bars = 49
+    gives 9,800."""
+    nodes = [(0.0, 0.0, 0.0)]
+    segs = []
+
+    def add(x, y):
+        nodes.append((x, y, 0.0))
+        segs.append(segment(len(nodes) - 2, len(nodes) - 1, width, thickness))
+
+    for bar in range(bars):
+        y = bar * pitch
+        for step in range(1, bars + 1):
+            along = step if bar % 2 == 0 else bars - step
+            add(along * pitch, y)
+        add((bars if bar % 2 == 0 else 0) * pitch, y + pitch)
+    return Deck(nodes, segs, [(0, len(nodes) - 1)], uniform(nw, nh), "scaling_meander_%d" % bars)

@@ -343,6 +343,49 @@ fh_status fh_write_zc_mat(const char *path, size_t n_ports, const double *freque
 fh_status fh_spice_subckt(size_t n_ports, const double *frequencies_hz, size_t nf, const double *z,
                           size_t k, const char *name, char *buf, size_t capacity, size_t *length);
 
+/* ---- matrix-free path: precorrected FFT operator and GMRES ------------- */
+
+/* PfftParams (pfft/mod.rs:183-232).  spacing_kind 0 = GridSpacing::Auto with
+ * cells_per_filament, 1 = GridSpacing::Fixed(spacing, metres);
+ * near_field_radius in grid spacings (>= interpolation_order + 1). */
+typedef struct fh_pfft_params {
+    int32_t spacing_kind;
+    int32_t interpolation_order;
+    double cells_per_filament;
+    double spacing;
+    double near_field_radius;
+} fh_pfft_params;
+
+/* PfftParams::default(): Auto 8 cells per filament, radius 8, order 5. */
+void fh_pfft_default_params(fh_pfft_params *params);
+
+/* PfftStats (pfft/mod.rs:255-272) plus the set-up time split. */
+typedef struct fh_pfft_stats {
+    int64_t filaments;
+    double grid_spacing;
+    int64_t grid_dims[3];
+    int64_t fft_dims[3];
+    int64_t projection_entries;
+    int64_t near_entries;
+    int64_t memory_bytes;
+    double setup_host_s;   /* grid, projections, near pairs, grid precorrection */
+    double setup_device_s; /* exact near pairs, kernel spectrum, uploads */
+} fh_pfft_stats;
+
+typedef struct fh_pfft fh_pfft;
+
+/* PfftOperator::new (pfft/mod.rs:332-478).  Errors: FH_ERR_PFFT
+ * (PfftError::InvalidParameter / GridTooLarge), FH_ERR_KERNEL_* for a near
+ * pair (PfftError::Kernel). */
+fh_status fh_pfft_create(const fh_filament *filaments, size_t n, const fh_pfft_params *params, fh_pfft **out,
+                         fh_error_info *err);
+/* PfftOperator::apply (pfft/mod.rs:482-529): y = L x for `count` vectors of
+ * length n (host arrays, vector v at x + v n). */
+fh_status fh_pfft_apply(fh_pfft *op, const double *x, double *y, size_t count, fh_error_info *err);
+/* PfftOperator::stats (pfft/mod.rs:563-597). */
+fh_status fh_pfft_get_stats(const fh_pfft *op, fh_pfft_stats *stats);
+void fh_pfft_destroy(fh_pfft *op);
+
 #ifdef __cplusplus
 }
 #endif

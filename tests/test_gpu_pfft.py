@@ -1,0 +1,133 @@
+"""The precorrected-FFT operator against the dense partial-inductance matrix
+it replaces (the reference's own acceptance test, fasterhenry/tests/pfft.rs:
+44-196: norm-wise and max-entry relative error of L x below 1e-6 at the
+default parameters).
+
+The dense reference is the oracle's fill (the reference's evaluation, on the
+CPU); fixtures are random filament clouds at constant density, axis-aligned
+and in general position, a 2-turn spiral and a planar set.
+"""
+import numpy as np
+import pytest
+
+from fasterhenry_b200 import fixtures as F
+
+pytestmark = pytest.mark.gpu
+
+TOLERANCE = 1e-6
+
+
+def filaments_of(fh, deck):
+    f, _ = fh.discretize(fh.Geometry.from_deck(deck), deck.discretization)
+    return f
+
+
+def probe_vector(n, seed):
+    return np.random.default_rng(seed).random(n) - 0.5
+
+
+def errors(fh, oracle, filaments, params, x):
+    dense = oracle.fill(filaments)
+    ref = dense @ x
+    with fh.PfftOperator(filaments, params) as op:
+        y = op.apply(x)
+        stats = op.stats()
+    d = y - ref
+    return np.linalg.norm(d) / np.linalg.norm(ref), np.max(np.abs(d)) / np.max(np.abs(ref)), stats
+
+
+@pytest.mark.parametrize("n,seed", [(60, 1), (200, 2), (500, 3)])
+@pytest.mark.parametrize("manhattan", [True, False])
+def test_random_sets_match_the_dense_product(fh, oracle, n, seed, manhattan):
+    fil = filaments_of(fh, F.cloud_deck(n, manhattan, seed))
+    assert len(fil) == n
+    norm, mx, _ = errors(fh, oracle, fil, fh.PfftParams(), probe_vector(n, 99))
+    assert norm < TOLERANCE, norm
+    assert mx < TOLERANCE, mx
+
+
+def test_most_pairs_of_a_large_random_set_take_the_fft_path(fh):
+    n = 500
+    fil = filaments_of(fh, F.cloud_deck(n, True, 3))
+    with fh.PfftOperator(fil) as op:
+        st = op.stats()
+    assert st["near_entries"] / float(n * n) < 0.5, st
+    assert st["filaments"] == n and all(d >= 1 for d in st["grid_dims"])
+    assert all(f >= 2 * d - 1 for f, d in zip(st["fft_dims"], st["grid_dims"]))
+
+
+def test_the_operator_is_symmetric(fh):
+    fil = filaments_of(fh, F.cloud_deck(300, False, 5, side=10e-3))
+    u, v = probe_vector(len(fil), 1), probe_vector(len(fil), 2)
+    with fh.PfftOperator(fil) as op:
+        left, right = u @ op.apply(v), op.apply(u) @ v
+    assert abs(left - right) <= 1e-12 * max(abs(left), abs(right))
+
+
+def test_application_is_linear_batched_and_repeatable(fh):
+    fil = filaments_of(fh, F.cloud_deck(150, True, 6, side=8e-3))
+    u, v = probe_vector(len(fil), 3), probe_vector(len(fil), 4)
+    with fh.PfftOperator(fil) as op:
+        lu, lv, lc = op.apply(u), op.apply(v), op.apply(2.0 * u - 3.0 * v)
+        both = op.apply(np.stack([u, v]))
+        again = op.apply(u)
+    scale = np.max(np.abs(lc))
+    assert np.max(np.abs(lc - (2.0 * lu - 3.0 * lv))) <= 1e-12 * scale
+    # Two vectors share one complex transform (real and imaginary part), so a
+    # batched product matches single products to rounding, not bit for bit.
+    assert np.max(np.abs(both[0] - lu)) <= 1e-12 * np.max(np.abs(lu))
+    assert np.max(np.abs(both[1] - lv)) <= 1e-12 * np.max(np.abs(lv))
+    assert np.array_equal(again, lu)
+
+
+def test_spiral_fixture_matches_the_dense_product(fh, oracle):
+    # 2-turn square spiral, 2 x 2 um copper, 4 x 4 filaments per segment.
+    deck = F.square_spiral(2, 2 * F.UM, 13 * F.UM, 2 * F.UM, 105 * F.UM, F.uniform(4, 4))
+    fil = filaments_of(fh, deck)
+    assert len(fil) == 16 * len(deck.segments)
+    x = probe_vector(len(fil), 99)
+    norm, mx, _ = errors(fh, oracle, fil, fh.PfftParams(), x)
+    assert norm < TOLERANCE and mx < TOLERANCE, (norm, mx)
+    # A finer grid pushes most of the spiral onto the FFT path.
+    norm, mx, st = errors(fh, oracle, fil, fh.PfftParams(spacing=2e-6), x)
+    assert norm < TOLERANCE and mx < TOLERANCE, (norm, mx)
+    assert st["grid_spacing"] == 2e-6
+
+
+def test_a_planar_set_uses_a_flat_grid(fh, oracle):
+    deck = F.cloud_deck(200, True, 8, side=10e-3)
+    # Flatten: every bar in the plane z = 0 (axis-aligned along x or y only).
+    nodes = [(x, y, 0.0) for (x, y, _) in deck.nodes]
+    segs = []
+    for k, s in enumerate(deck.segments):
+        a, b = nodes[s["a"]], nodes[s["b"]]
+        if abs(a[0] - b[0]) + abs(a[1] - b[1]) == 0.0:  # a z-directed bar: lay it along x
+            nodes[s["b"]] = (a[0] + 1e-3, a[1], 0.0)
+        segs.append(dict(s, height=35e-6))
+    flat = F.Deck(nodes, segs, [], F.uniform(1, 1), "flat")
+    fil = filaments_of(fh, flat)
+    norm, mx, st = errors(fh, oracle, fil, fh.PfftParams(), probe_vector(len(fil), 7))
+    assert norm < TOLERANCE and mx < TOLERANCE, (norm, mx)
+    # The thin axis holds one stencil (order + 1 planes, half a stencil of
+    # padding each side, one spare plane); the wide axes many cells.
+    assert st["grid_dims"][2] <= 5 + 4 and min(st["grid_dims"][:2]) > 4 * st["grid_dims"][2]
+
+
+def test_cheaper_parameters_meet_their_own_bound(fh, oracle):
+    # p = 2 (3 x 3 x 3 stencil), k = 4: the reference's table gives ~2e-4.
+    fil = filaments_of(fh, F.cloud_deck(300, True, 12))
+    norm, mx, _ = errors(fh, oracle, fil, fh.PfftParams(near_field_radius=4.0, interpolation_order=2),
+                         probe_vector(len(fil), 5))
+    assert norm < 1e-3, norm
+
+
+def test_invalid_parameters_are_pfft_errors(fh):
+    fil = filaments_of(fh, F.cloud_deck(20, True, 1))
+    with pytest.raises(fh.PfftError):
+        fh.PfftOperator(fil, fh.PfftParams(interpolation_order=0))
+    with pytest.raises(fh.PfftError):
+        fh.PfftOperator(fil, fh.PfftParams(near_field_radius=3.0, interpolation_order=5))
+    with pytest.raises(fh.PfftError):
+        fh.PfftOperator(fil, fh.PfftParams(spacing=-1.0))
+    with pytest.raises(fh.PfftError):
+        fh.PfftOperator(fil, fh.PfftParams(spacing=1e-9))  # grid far beyond the FFT point limit

@@ -12,6 +12,7 @@ from .api import (DENSE_PATH_MAX_FILAMENTS, MU0, CoincidentSamples, DiscretizeEr
                   SegmentDef, Singular, SolverChoice, SweepResult, Unsupported, build_info, device_count, discretize,
                   lu_solve, mesh_matrix, mutual_inductance, partial_inductance_matrix, self_inductance, skin_depth,
                   solve)
-from .api import PfftError, PfftOperator, PfftParams, Profiler, fill_stats
+from .api import (GmresOutcome, GmresParams, IterativeParams, IterativeSystem, PfftError, PfftOperator, PfftParams,
+                  Profiler, fill_stats, gmres_dense)
 
 __version__ = "0.1.0"

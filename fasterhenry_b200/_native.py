@@ -81,6 +81,14 @@ class PfftStats(ctypes.Structure):
                 ("setup_device_s", ctypes.c_double)]
 
 
+class GmresParams(ctypes.Structure):
+    _fields_ = [("tolerance", ctypes.c_double), ("restart", ctypes.c_int32), ("max_iterations", ctypes.c_int32)]
+
+
+class GmresOutcome(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int64), ("relative_residual", ctypes.c_double), ("converged", ctypes.c_int32)]
+
+
 # Status codes (fh_status)
 OK = 0
 ERR_INVALID_ARGUMENT = 1
@@ -108,7 +116,8 @@ EXPORTS = [
     "fh_system_mesh_matrices", "fh_system_device_l_mesh", "fh_sweep", "fh_impedance", "fh_sweep_json",
     "fh_write_zc_mat", "fh_spice_subckt", "fh_system_fill_stats", "fh_profile_enable", "fh_profile_reset",
     "fh_profile_read", "fh_pfft_default_params", "fh_pfft_create", "fh_pfft_apply", "fh_pfft_get_stats",
-    "fh_pfft_destroy",
+    "fh_pfft_destroy", "fh_gmres_default_params", "fh_iterative_create", "fh_iterative_counts", "fh_iterative_timing",
+    "fh_iterative_pfft_stats", "fh_iterative_sweep", "fh_iterative_destroy", "fh_test_gmres_dense",
 ]
 
 PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner"]
@@ -155,6 +164,18 @@ def load():
     L.fh_pfft_get_stats.argtypes = [ctypes.c_void_p, P(PfftStats)]
     L.fh_pfft_destroy.argtypes = [ctypes.c_void_p]
     L.fh_pfft_destroy.restype = None
+    L.fh_gmres_default_params.argtypes = [P(GmresParams)]
+    L.fh_gmres_default_params.restype = None
+    L.fh_iterative_create.argtypes = [P(Node), sz, P(SegmentDef), sz, P(Port), sz, P(Discretization), P(PfftParams),
+                                      P(GmresParams), P(ctypes.c_void_p), ei]
+    L.fh_iterative_counts.argtypes = [ctypes.c_void_p, P(Counts)]
+    L.fh_iterative_timing.argtypes = [ctypes.c_void_p, P(Timing)]
+    L.fh_iterative_pfft_stats.argtypes = [ctypes.c_void_p, P(PfftStats)]
+    L.fh_iterative_sweep.argtypes = [ctypes.c_void_p, c_double_p, sz, c_double_p, P(GmresOutcome), ei]
+    L.fh_iterative_destroy.argtypes = [ctypes.c_void_p]
+    L.fh_iterative_destroy.restype = None
+    L.fh_test_gmres_dense.argtypes = [c_double_p, sz, c_double_p, c_double_p, c_double_p, P(GmresParams),
+                                      P(GmresOutcome), ei]
     L.fh_system_destroy.argtypes = [ctypes.c_void_p]
     L.fh_system_destroy.restype = None
     L.fh_system_counts.argtypes = [ctypes.c_void_p, P(Counts)]

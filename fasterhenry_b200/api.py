@@ -573,8 +573,16 @@ class MeshSystem:
 
 
 def solve(geometry, ports: Sequence, discretization: dict, frequencies: Sequence[float],
-          precision: Precision = Precision.FP64) -> SweepResult:
-    """MeshSystem.assemble followed by MeshSystem.sweep (solve.rs:931-938)."""
+          precision: Precision = Precision.FP64, solver: SolverChoice = SolverChoice.DENSE,
+          iterative: Optional[IterativeParams] = None) -> SweepResult:
+    """MeshSystem.assemble followed by MeshSystem.sweep (solve.rs:931-938),
+    or IterativeSystem when ``solver`` resolves to the iterative path
+    (SolverChoice::resolve, solve.rs:169-193)."""
+    n = len(discretize(geometry, discretization)[0]) if solver == SolverChoice.AUTO else 0
+    path = solver.resolve(n) if solver != SolverChoice.DENSE else "dense"
+    if path == "iterative":
+        with IterativeSystem.assemble(geometry, ports, discretization, iterative) as system:
+            return system.sweep(frequencies)
     with MeshSystem.assemble(geometry, ports, discretization) as system:
         return system.sweep(frequencies, precision)
 
@@ -659,6 +667,135 @@ class PfftOperator:
                 "projection_entries": int(s.projection_entries), "near_entries": int(s.near_entries),
                 "memory_bytes": int(s.memory_bytes), "setup_host_s": float(s.setup_host_s),
                 "setup_device_s": float(s.setup_device_s)}
+
+
+@dataclasses.dataclass(frozen=True)
+class GmresParams:
+    """GmresParams (gmres.rs:32-58)."""
+    tolerance: float = 1e-10
+    restart: int = 100
+    max_iterations: int = 5000
+
+    def _native(self) -> N.GmresParams:
+        g = N.GmresParams()
+        g.tolerance, g.restart, g.max_iterations = float(self.tolerance), int(self.restart), int(self.max_iterations)
+        return g
+
+
+@dataclasses.dataclass(frozen=True)
+class IterativeParams:
+    """IterativeParams (iterative.rs:100-107)."""
+    pfft: PfftParams = PfftParams()
+    gmres: GmresParams = GmresParams()
+
+
+@dataclasses.dataclass(frozen=True)
+class GmresOutcome:
+    """GmresOutcome (gmres.rs:61-73)."""
+    iterations: int
+    relative_residual: float
+    converged: bool
+
+
+class IterativeSystem:
+    """Matrix-free port impedance: GMRES on the precorrected-FFT operator
+    (IterativeSystem, iterative.rs:109-409).  Same results as MeshSystem to
+    the pFFT far-field accuracy and the GMRES tolerance."""
+
+    def __init__(self, handle, ports):
+        self._h = handle
+        self.ports = [p if isinstance(p, Port) else Port(p[0], p[1]) for p in ports]
+        self.last_outcomes: List[List[GmresOutcome]] = []
+
+    @classmethod
+    def assemble(cls, geometry, ports: Sequence, discretization: dict,
+                 params: Optional[IterativeParams] = None) -> "IterativeSystem":
+        params = params or IterativeParams()
+        nodes, segs = _geom_arrays(geometry)
+        pts = _ports(ports)
+        disc, keep = _disc(discretization)
+        pp, gp = params.pfft._native(), params.gmres._native()
+        h = ctypes.c_void_p()
+        info = N.ErrorInfo()
+        _check(N.load().fh_iterative_create(nodes, len(geometry.nodes), segs, len(geometry.segments), pts, len(ports),
+                                            ctypes.byref(disc), ctypes.byref(pp), ctypes.byref(gp), ctypes.byref(h),
+                                            ctypes.byref(info)), info)
+        return cls(h, ports)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            N.load().fh_iterative_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def counts(self) -> Dict[str, int]:
+        c = N.Counts()
+        _check(N.load().fh_iterative_counts(self._h, ctypes.byref(c)))
+        return {k: int(getattr(c, k)) for k, _ in N.Counts._fields_}
+
+    def timing(self) -> Dict[str, float]:
+        t = N.Timing()
+        _check(N.load().fh_iterative_timing(self._h, ctypes.byref(t)))
+        return {k: float(getattr(t, k)) for k, _ in N.Timing._fields_}
+
+    def operator_stats(self) -> Dict[str, object]:
+        s = N.PfftStats()
+        _check(N.load().fh_iterative_pfft_stats(self._h, ctypes.byref(s)))
+        return {"filaments": int(s.filaments), "grid_spacing": float(s.grid_spacing),
+                "grid_dims": [int(v) for v in s.grid_dims], "fft_dims": [int(v) for v in s.fft_dims],
+                "projection_entries": int(s.projection_entries), "near_entries": int(s.near_entries),
+                "memory_bytes": int(s.memory_bytes), "setup_host_s": float(s.setup_host_s),
+                "setup_device_s": float(s.setup_device_s)}
+
+    def sweep(self, frequencies: Sequence[float]) -> SweepResult:
+        f = np.ascontiguousarray(frequencies, dtype=np.float64)
+        p = len(self.ports)
+        z = np.zeros((len(f), p, p), dtype=np.complex128)
+        oc = (N.GmresOutcome * max(1, len(f) * p))()
+        info = N.ErrorInfo()
+        _check(N.load().fh_iterative_sweep(self._h, f.ctypes.data_as(N.c_double_p), len(f),
+                                           z.ctypes.data_as(N.c_double_p), oc, ctypes.byref(info)), info)
+        self.last_outcomes = [[GmresOutcome(int(oc[k * p + q].iterations), float(oc[k * p + q].relative_residual),
+                                            bool(oc[k * p + q].converged)) for q in range(p)] for k in range(len(f))]
+        return SweepResult(self.ports, [float(x) for x in f], z, self.counts(), self.timing())
+
+    def impedance(self, frequency: float) -> np.ndarray:
+        return self.sweep([frequency]).impedance_ohm[0]
+
+    def solve(self, frequency: float) -> Tuple[np.ndarray, List[GmresOutcome]]:
+        """Z at one frequency with the GMRES outcome of every port."""
+        z = self.impedance(frequency)
+        return z, self.last_outcomes[0]
+
+
+def gmres_dense(a: np.ndarray, b: np.ndarray, x0: Optional[np.ndarray] = None,
+                precondition: Optional[np.ndarray] = None, params: Optional[GmresParams] = None):
+    """The device GMRES on a dense complex system (test hook of the solver
+    that IterativeSystem uses).  Returns (x, GmresOutcome)."""
+    a = np.asfortranarray(a, dtype=np.complex128)
+    n = a.shape[0]
+    b = np.ascontiguousarray(b, dtype=np.complex128)
+    x = np.ascontiguousarray(np.zeros(n, dtype=np.complex128) if x0 is None else x0, dtype=np.complex128)
+    m = None if precondition is None else np.asfortranarray(precondition, dtype=np.complex128)
+    g = (params or GmresParams())._native()
+    oc = N.GmresOutcome()
+    info = N.ErrorInfo()
+    _check(N.load().fh_test_gmres_dense(a.ctypes.data_as(N.c_double_p), n, b.ctypes.data_as(N.c_double_p),
+                                        x.ctypes.data_as(N.c_double_p),
+                                        None if m is None else m.ctypes.data_as(N.c_double_p), ctypes.byref(g),
+                                        ctypes.byref(oc), ctypes.byref(info)), info)
+    return x, GmresOutcome(int(oc.iterations), float(oc.relative_residual), bool(oc.converged))
 
 
 def skin_depth(frequency_hz: float, sigma: float) -> float:

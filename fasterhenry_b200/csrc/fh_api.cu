@@ -590,7 +590,8 @@ fh_status fh_system_create(const fh_node *nodes, size_t n_nodes, const fh_segmen
     s->n = (int64_t)s->disc.filaments.size();
     if (fh_solver_resolve(choice, (size_t)s->n) != 0)
         return fail(err, FH_ERR_UNSUPPORTED,
-                    "the matrix-free (pFFT + GMRES) path is not provided by this build; choose FH_SOLVER_DENSE");
+                    "this choice resolves to the matrix-free path, which is fh_iterative_create (IterativeSystem); "
+                    "fh_system_create builds the dense MeshSystem");
     st = ensure_device(err);
     if (st) return st;
     FHB_CUDA(cudaGetDevice(&s->device));

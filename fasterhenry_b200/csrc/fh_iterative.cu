@@ -1,0 +1,563 @@
+// Matrix-free port impedance (iterative.rs of the reference): GMRES on the
+// precorrected-FFT operator, never forming L or Z_ee.
+//
+//   Z(w) = Z_pp - Z_ep^T Z_ee^-1 Z_ep,   Z_ee x = M_e (R c + j w L c),  c = M_e^T x
+//
+// Assembly (IterativeSystem::assemble, iterative.rs:155-239): discretize, loop
+// basis, the pFFT operator, the port columns Z_ep / Z_pp from one operator
+// product per port (R and L are frequency independent), and the Jacobi
+// diagonal of M_e R M_e^T and M_e L M_e^T (exact sum_a sum_b s_a s_b L_ab for
+// loops of at most 32 branches, the self terms otherwise; the pair values
+// come from the device fill in pair-list mode).
+// Per frequency (iterative.rs:269-302, 454-485): one Jacobi-preconditioned
+// GMRES solve per port on the device, each Z_ee product being a scatter to
+// branch currents, one pFFT product of the real and imaginary parts
+// together, the branch drops and a gather back to loops; then the Schur
+// complement with a plain transpose and Z <- (Z + Z^T) / 2.  At f = 0 the
+// system is M_e R M_e^T and no pFFT product runs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "fh_cx.cuh"
+#include "fh_device.cuh"
+#include "fh_gmres.cuh"
+#include "fh_pfft.h"
+
+using namespace fhb;
+
+namespace {
+
+constexpr double kTauI = 6.283185307179586;
+constexpr size_t kExactDiagonalMaxLoop = 32;  // iterative.rs:97
+
+double wall_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// c_b = sum over the internal loops through branch b of sign x_loop, in loop
+// order (transposed loop basis; iterative.rs:403-411).
+__global__ void scatter_kernel(const double2 *__restrict__ x, const int64_t *__restrict__ off,
+                               const int32_t *__restrict__ loop, const double *__restrict__ sign,
+                               double2 *__restrict__ c, int64_t n) {
+    for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < n; b += (int64_t)gridDim.x * blockDim.x) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int64_t k = off[b]; k < off[b + 1]; ++k) {
+            const double2 v = x[loop[k]];
+            const double s = sign[k];
+            acc.x += v.x * s;
+            acc.y += v.y * s;
+        }
+        c[b] = acc;
+    }
+}
+
+// Real and imaginary parts as two real vectors (one pFFT product of both).
+__global__ void split_kernel(const double2 *__restrict__ c, double *__restrict__ parts, int64_t n) {
+    for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < n; b += (int64_t)gridDim.x * blockDim.x) {
+        parts[b] = c[b].x;
+        parts[n + b] = c[b].y;
+    }
+}
+
+// drop_b = r_b c_b + j w (L c)_b  (iterative.rs:432-451); w = 0 skips L.
+__global__ void drop_kernel(const double2 *__restrict__ c, const double *__restrict__ r,
+                            const double *__restrict__ flux, double omega, double2 *__restrict__ drop, int64_t n) {
+    for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < n; b += (int64_t)gridDim.x * blockDim.x) {
+        const double rb = r[b];
+        if (flux)
+            drop[b] = make_double2(rb * c[b].x - omega * flux[n + b], rb * c[b].y + omega * flux[b]);
+        else
+            drop[b] = make_double2(c[b].x * rb, c[b].y * rb);
+    }
+}
+
+// y_i = sum over loop i's branches of sign v_b, in row order (iterative.rs:488-505).
+__global__ void gather_kernel(const double2 *__restrict__ v, const int64_t *__restrict__ row_ptr,
+                              const int32_t *__restrict__ branch, const double *__restrict__ sign,
+                              double2 *__restrict__ y, int64_t loops) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < loops; i += (int64_t)gridDim.x * blockDim.x) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
+            const double2 t = v[branch[k]];
+            const double s = sign[k];
+            acc.x += t.x * s;
+            acc.y += t.y * s;
+        }
+        y[i] = acc;
+    }
+}
+
+// Jacobi: out = v / d (num-complex division).
+__global__ void jacobi_kernel(const double2 *__restrict__ v, const double2 *__restrict__ d, double2 *__restrict__ out,
+                              int64_t m) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        const Cx<double> q = cdiv(Cx<double>{v[i].x, v[i].y}, Cx<double>{d[i].x, d[i].y});
+        out[i] = make_double2(q.re, q.im);
+    }
+}
+
+// y = A x for a dense column-major complex matrix (GMRES tests).
+__global__ void dense_matvec_kernel(const double2 *__restrict__ a, const double2 *__restrict__ x,
+                                    double2 *__restrict__ y, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int64_t k = 0; k < n; ++k) {
+            const double2 m = a[i + k * n], v = x[k];
+            acc.x += m.x * v.x - m.y * v.y;
+            acc.y += m.x * v.y + m.y * v.x;
+        }
+        y[i] = acc;
+    }
+}
+
+inline unsigned grid_n(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)); }
+
+template <class T>
+cudaError_t put(T **d, const std::vector<T> &h, cudaStream_t s) {
+    cudaError_t e = cudaMalloc((void **)d, std::max<size_t>(1, h.size()) * sizeof(T));
+    if (e != cudaSuccess || h.empty()) return e;
+    return cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+using cplx = std::complex<double>;
+
+}  // namespace
+
+struct fh_iterative {
+    Discretized disc;
+    LoopBasis loops;
+    std::vector<double> resistances;
+    int64_t n = 0, m = 0, p = 0, nloops = 0;
+    fh_counts counts{};
+    fh_timing timing{};
+    GmresParams gp;
+    PfftDevice op;
+    cudaStream_t stream = nullptr;
+    // Host blocks of M R M^T and M L M^T (column-major (m x p), (p x p)).
+    std::vector<double> r_ep, l_ep, r_pp, l_pp, r_diag, l_diag;
+    // Device: loop basis rows and its transpose over the internal loops.
+    int64_t *d_row_ptr = nullptr, *d_t_off = nullptr;
+    int32_t *d_branch = nullptr, *d_t_loop = nullptr;
+    double *d_sign = nullptr, *d_t_sign = nullptr, *d_r = nullptr;
+    double2 *d_c = nullptr, *d_drop = nullptr, *d_diag = nullptr, *d_b = nullptr, *d_x = nullptr;
+    double *d_parts = nullptr, *d_flux = nullptr;
+    GmresWork work;
+    double operator_s = 0;
+    ~fh_iterative() {
+        void *ptrs[] = {d_row_ptr, d_t_off, d_branch, d_t_loop, d_sign, d_t_sign, d_r, d_c,
+                        d_drop, d_diag, d_b, d_x, d_parts, d_flux};
+        for (void *q : ptrs)
+            if (q) cudaFree(q);
+    }
+};
+
+namespace {
+
+// Z_ee x (f > 0: omega > 0) or M_e R M_e^T x (omega == 0).
+fh_status apply_ee(fh_iterative *s, double omega, const double2 *x, double2 *y, fh_error_info *err) {
+    const int64_t n = s->n;
+    scatter_kernel<<<grid_n(n), 256, 0, s->stream>>>(x, s->d_t_off, s->d_t_loop, s->d_t_sign, s->d_c, n);
+    FHB_CUDA(cudaGetLastError());
+    const double *flux = nullptr;
+    if (omega != 0.0) {
+        split_kernel<<<grid_n(n), 256, 0, s->stream>>>(s->d_c, s->d_parts, n);
+        FHB_CUDA(cudaGetLastError());
+        fh_status st = pfft_apply(s->op, s->d_parts, s->d_flux, 2, err);
+        if (st) return st;
+        flux = s->d_flux;
+    }
+    drop_kernel<<<grid_n(n), 256, 0, s->stream>>>(s->d_c, s->d_r, flux, omega, s->d_drop, n);
+    gather_kernel<<<grid_n(s->m), 256, 0, s->stream>>>(s->d_drop, s->d_row_ptr, s->d_branch, s->d_sign, y, s->m);
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+// sum_a sum_b s_a s_b L_ab over one loop, or the self terms alone for long
+// loops (iterative.rs:516-536).  `self` per branch, `mutual` the loop's
+// (k < l) pairs in row order.
+double loop_inductance(const int32_t *br, size_t len, const double *self_l, const double *mutual, const double *sg) {
+    double own = 0.0;
+    for (size_t k = 0; k < len; ++k) own += self_l[br[k]];
+    if (len > kExactDiagonalMaxLoop) return own;
+    double mut = 0.0;
+    size_t q = 0;
+    for (size_t k = 0; k < len; ++k)
+        for (size_t l = k + 1; l < len; ++l) mut += sg[k] * sg[l] * mutual[q++];
+    return own + 2.0 * mut;
+}
+
+}  // namespace
+
+extern "C" {
+
+void fh_gmres_default_params(fh_gmres_params *params) {
+    if (!params) return;
+    params->tolerance = 1e-10;
+    params->restart = 100;
+    params->max_iterations = 5000;
+}
+
+fh_status fh_iterative_create(const fh_node *nodes, size_t n_nodes, const fh_segment_def *segments, size_t n_segments,
+                              const fh_port *ports, size_t n_ports, const fh_discretization *disc,
+                              const fh_pfft_params *pfft, const fh_gmres_params *gmres, fh_iterative **out,
+                              fh_error_info *err) {
+    clear_error(err);
+    if (!out) return fail(err, FH_ERR_INVALID_ARGUMENT, "null output handle");
+    *out = nullptr;
+    if (n_ports && !ports) return fail(err, FH_ERR_INVALID_ARGUMENT, "null ports");
+    const double t0 = wall_s();
+    std::unique_ptr<fh_iterative> s(new fh_iterative);
+    fh_gmres_params g;
+    fh_gmres_default_params(&g);
+    if (gmres) g = *gmres;
+    if (!(g.tolerance > 0.0) || g.restart < 1 || g.max_iterations < 0)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "GMRES tolerance must be positive and restart at least 1");
+    s->gp.tolerance = g.tolerance;
+    s->gp.restart = g.restart;
+    s->gp.max_iterations = g.max_iterations;
+    fh_pfft_params pp;
+    fh_pfft_default_params(&pp);
+    if (pfft) pp = *pfft;
+    PfftConfig cfg;
+    cfg.fixed_spacing = pp.spacing_kind == 1;
+    cfg.cells_per_filament = pp.cells_per_filament;
+    cfg.spacing = pp.spacing;
+    cfg.near_field_radius = pp.near_field_radius;
+    cfg.order = pp.interpolation_order;
+    fh_status st = discretize_geometry(nodes, n_nodes, segments, n_segments, disc, s->disc, err);
+    if (st) return st;
+    st = build_loops(segments, n_segments, n_nodes, s->disc.per_segment.data(), ports, n_ports, s->loops, err);
+    if (st) return st;
+    st = ensure_device(err);
+    if (st) return st;
+    FHB_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    cudaStream_t cs = s->stream;
+    const int64_t n = (int64_t)s->disc.filaments.size();
+    s->n = n;
+    s->nloops = s->loops.rows();
+    s->m = s->loops.internal;
+    s->p = s->nloops - s->m;
+    const int64_t m = s->m, p = s->p, L = s->nloops;
+    for (const fh_filament &f : s->disc.filaments) s->resistances.push_back(f.length / (f.sigma * (f.width * f.height)));
+
+    const double t_op = wall_s();
+    st = pfft_build(s->disc.filaments.data(), n, cfg, cs, s->op, err);
+    if (st) return st;
+    s->operator_s = wall_s() - t_op;
+
+    // Port columns: one operator product per port.
+    const auto &rp = s->loops.row_ptr;
+    const auto &br = s->loops.branch;
+    const auto &sg = s->loops.sign;
+    s->r_ep.assign((size_t)m * p, 0.0);
+    s->l_ep.assign((size_t)m * p, 0.0);
+    s->r_pp.assign((size_t)p * p, 0.0);
+    s->l_pp.assign((size_t)p * p, 0.0);
+    if (p > 0 && n > 0) {
+        double *d_cur = nullptr, *d_fl = nullptr;
+        FHB_CUDA(cudaMalloc(&d_cur, sizeof(double) * n));
+        std::unique_ptr<void, decltype(&cudaFree)> g1(d_cur, &cudaFree);
+        FHB_CUDA(cudaMalloc(&d_fl, sizeof(double) * n));
+        std::unique_ptr<void, decltype(&cudaFree)> g2(d_fl, &cudaFree);
+        std::vector<double> current((size_t)n), flux((size_t)n), drop((size_t)n);
+        for (int64_t q = 0; q < p; ++q) {
+            std::fill(current.begin(), current.end(), 0.0);
+            for (int64_t k = rp[m + q]; k < rp[m + q + 1]; ++k) current[br[k]] += sg[k];
+            FHB_CUDA(cudaMemcpyAsync(d_cur, current.data(), sizeof(double) * n, cudaMemcpyHostToDevice, cs));
+            st = pfft_apply(s->op, d_cur, d_fl, 1, err);
+            if (st) return st;
+            FHB_CUDA(cudaMemcpyAsync(flux.data(), d_fl, sizeof(double) * n, cudaMemcpyDeviceToHost, cs));
+            FHB_CUDA(cudaStreamSynchronize(cs));
+            for (int64_t b = 0; b < n; ++b) drop[b] = current[b] * s->resistances[b];
+            for (int64_t i = 0; i < L; ++i) {
+                double rv = 0.0, lv = 0.0;
+                for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
+                    rv += drop[br[k]] * sg[k];
+                    lv += flux[br[k]] * sg[k];
+                }
+                if (i < m) {
+                    s->r_ep[i + q * m] = rv;
+                    s->l_ep[i + q * m] = lv;
+                } else {
+                    s->r_pp[(i - m) + q * p] = rv;
+                    s->l_pp[(i - m) + q * p] = lv;
+                }
+            }
+        }
+        // Symmetric in exact arithmetic; made so to the last bit (iterative.rs:199-200).
+        std::vector<double> r2 = s->r_pp, l2 = s->l_pp;
+        for (int64_t a = 0; a < p; ++a)
+            for (int64_t b = 0; b < p; ++b) {
+                s->r_pp[a + b * p] = (r2[a + b * p] + r2[b + a * p]) * 0.5;
+                s->l_pp[a + b * p] = (l2[a + b * p] + l2[b + a * p]) * 0.5;
+            }
+    }
+
+    // Jacobi diagonal: self terms of every branch and the pairs of short loops.
+    std::vector<int2> pairs;
+    for (int64_t b = 0; b < n; ++b) pairs.push_back(make_int2((int)b, (int)b));
+    for (int64_t i = 0; i < m; ++i) {
+        const size_t len = (size_t)(rp[i + 1] - rp[i]);
+        if (len > kExactDiagonalMaxLoop) continue;
+        for (int64_t k = rp[i]; k < rp[i + 1]; ++k)
+            for (int64_t l = k + 1; l < rp[i + 1]; ++l) pairs.push_back(make_int2(br[k], br[l]));
+    }
+    std::vector<double> values(pairs.size(), 0.0);
+    if (!pairs.empty()) {
+        std::vector<DevFil> hf((size_t)n);
+        for (int64_t i = 0; i < n; ++i) hf[i] = make_devfil(s->disc.filaments[i]);
+        DevFil *d_fil = nullptr;
+        int2 *d_pairs = nullptr;
+        double *d_vals = nullptr;
+        FHB_CUDA(put(&d_fil, hf, cs));
+        std::unique_ptr<void, decltype(&cudaFree)> g1(d_fil, &cudaFree);
+        FHB_CUDA(put(&d_pairs, pairs, cs));
+        std::unique_ptr<void, decltype(&cudaFree)> g2(d_pairs, &cudaFree);
+        FHB_CUDA(cudaMalloc(&d_vals, sizeof(double) * pairs.size()));
+        std::unique_ptr<void, decltype(&cudaFree)> g3(d_vals, &cudaFree);
+        st = device_fill_pairs(d_fil, n, d_pairs, (int64_t)pairs.size(), d_vals, cs, nullptr, err);
+        if (st) return st;
+        FHB_CUDA(cudaMemcpyAsync(values.data(), d_vals, sizeof(double) * pairs.size(), cudaMemcpyDeviceToHost, cs));
+        FHB_CUDA(cudaStreamSynchronize(cs));
+    }
+    s->r_diag.assign((size_t)m, 0.0);
+    s->l_diag.assign((size_t)m, 0.0);
+    size_t cursor = (size_t)n;
+    for (int64_t i = 0; i < m; ++i) {
+        const size_t len = (size_t)(rp[i + 1] - rp[i]);
+        double r = 0.0;
+        for (int64_t k = rp[i]; k < rp[i + 1]; ++k) r += s->resistances[br[k]];
+        s->r_diag[i] = r;
+        const double *mutual = values.data() + cursor;
+        s->l_diag[i] = loop_inductance(&br[rp[i]], len, values.data(), mutual, &sg[rp[i]]);
+        if (len <= kExactDiagonalMaxLoop) cursor += len * (len - 1) / 2;
+    }
+
+    // Device copies of the loop basis, its transpose over internal loops, R.
+    std::vector<int64_t> t_off((size_t)n + 1, 0);
+    for (int64_t i = 0; i < m; ++i)
+        for (int64_t k = rp[i]; k < rp[i + 1]; ++k) t_off[br[k] + 1] += 1;
+    for (int64_t b = 0; b < n; ++b) t_off[b + 1] += t_off[b];
+    std::vector<int32_t> t_loop((size_t)t_off[n]);
+    std::vector<double> t_sign((size_t)t_off[n]);
+    std::vector<int64_t> fillp(t_off.begin(), t_off.end() - 1);
+    for (int64_t i = 0; i < m; ++i)
+        for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
+            const int64_t slot = fillp[br[k]]++;
+            t_loop[slot] = (int32_t)i;
+            t_sign[slot] = sg[k];
+        }
+    FHB_CUDA(put(&s->d_row_ptr, rp, cs));
+    FHB_CUDA(put(&s->d_branch, br, cs));
+    FHB_CUDA(put(&s->d_sign, sg, cs));
+    FHB_CUDA(put(&s->d_t_off, t_off, cs));
+    FHB_CUDA(put(&s->d_t_loop, t_loop, cs));
+    FHB_CUDA(put(&s->d_t_sign, t_sign, cs));
+    FHB_CUDA(put(&s->d_r, s->resistances, cs));
+    auto alloc = [&](void **q, size_t bytes) { return cudaMalloc(q, std::max<size_t>(bytes, 16)); };
+    if (alloc((void **)&s->d_c, sizeof(double2) * n) || alloc((void **)&s->d_drop, sizeof(double2) * n) ||
+        alloc((void **)&s->d_diag, sizeof(double2) * m) || alloc((void **)&s->d_b, sizeof(double2) * m) ||
+        alloc((void **)&s->d_x, sizeof(double2) * m * std::max<int64_t>(p, 1)) ||
+        alloc((void **)&s->d_parts, sizeof(double) * 2 * n) || alloc((void **)&s->d_flux, sizeof(double) * 2 * n)) {
+        cudaGetLastError();
+        return fail(err, FH_ERR_OUT_OF_MEMORY, "device allocation of the iterative system failed");
+    }
+    FHB_CUDA(cudaStreamSynchronize(cs));
+    s->counts = fh_counts{(int64_t)n_nodes, (int64_t)n_segments, n, L, m, p};
+    s->timing.inductance_s = s->operator_s;
+    s->timing.assembly_s = wall_s() - t0;
+    s->timing.total_s = s->timing.assembly_s;
+    *out = s.release();
+    return FH_OK;
+}
+
+fh_status fh_iterative_counts(const fh_iterative *s, fh_counts *out) {
+    if (!s || !out) return FH_ERR_INVALID_ARGUMENT;
+    *out = s->counts;
+    return FH_OK;
+}
+
+fh_status fh_iterative_timing(const fh_iterative *s, fh_timing *out) {
+    if (!s || !out) return FH_ERR_INVALID_ARGUMENT;
+    *out = s->timing;
+    return FH_OK;
+}
+
+fh_status fh_iterative_pfft_stats(const fh_iterative *s, fh_pfft_stats *out) {
+    if (!s || !out) return FH_ERR_INVALID_ARGUMENT;
+    const PfftDevice &d = s->op;
+    out->filaments = d.n;
+    out->grid_spacing = d.grid.spacing;
+    for (int a = 0; a < 3; ++a) {
+        out->grid_dims[a] = d.grid.dims[a];
+        out->fft_dims[a] = d.padded[a];
+    }
+    out->projection_entries = d.projection_entries;
+    out->near_entries = d.near_entries;
+    out->memory_bytes = (int64_t)d.memory_bytes();
+    out->setup_host_s = d.setup_host_s;
+    out->setup_device_s = d.setup_device_s;
+    return FH_OK;
+}
+
+fh_status fh_iterative_sweep(fh_iterative *s, const double *freqs, size_t nf, double *z_out,
+                             fh_gmres_outcome *outcomes, fh_error_info *err) {
+    clear_error(err);
+    if (!s || (nf && (!freqs || !z_out))) return fail(err, FH_ERR_INVALID_ARGUMENT, "null argument");
+    for (size_t k = 0; k < nf; ++k)
+        if (!(std::isfinite(freqs[k]) && freqs[k] >= 0.0))
+            return fail(err, FH_ERR_INVALID_FREQUENCY,
+                        "frequency " + std::to_string(k) + " is " + std::to_string(freqs[k]) +
+                            " Hz; frequencies must be finite and non-negative",
+                        (int64_t)k, -1, freqs[k]);
+    const double t0 = wall_s();
+    const int64_t m = s->m, p = s->p;
+    cudaStream_t cs = s->stream;
+    for (size_t fi = 0; fi < nf; ++fi) {
+        const double f = freqs[fi];
+        const double omega = f == 0.0 ? 0.0 : kTauI * f;
+        std::vector<cplx> z((size_t)p * p);
+        for (int64_t a = 0; a < p; ++a)
+            for (int64_t b = 0; b < p; ++b)
+                z[a + b * p] = cplx(s->r_pp[a + b * p], omega * s->l_pp[a + b * p]);
+        if (m > 0) {
+            std::vector<double2> diag((size_t)m), rhs((size_t)m);
+            for (int64_t i = 0; i < m; ++i) diag[i] = make_double2(s->r_diag[i], omega * s->l_diag[i]);
+            FHB_CUDA(cudaMemcpyAsync(s->d_diag, diag.data(), sizeof(double2) * m, cudaMemcpyHostToDevice, cs));
+            DeviceOp apply = [&](const double2 *in, double2 *out, fh_error_info *e) {
+                return apply_ee(s, omega, in, out, e);
+            };
+            DeviceOp precondition = [&](const double2 *in, double2 *out, fh_error_info *e) {
+                jacobi_kernel<<<grid_n(m), 256, 0, cs>>>(in, s->d_diag, out, m);
+                cudaError_t ce = cudaGetLastError();
+                if (ce != cudaSuccess) return fail(e, FH_ERR_CUDA, std::string("jacobi: ") + cudaGetErrorString(ce));
+                return FH_OK;
+            };
+            std::vector<double2> xs((size_t)m * p);
+            for (int64_t q = 0; q < p; ++q) {
+                for (int64_t i = 0; i < m; ++i) rhs[i] = make_double2(s->r_ep[i + q * m], omega * s->l_ep[i + q * m]);
+                FHB_CUDA(cudaMemcpyAsync(s->d_b, rhs.data(), sizeof(double2) * m, cudaMemcpyHostToDevice, cs));
+                double2 *xq = s->d_x + q * m;
+                FHB_CUDA(cudaMemsetAsync(xq, 0, sizeof(double2) * m, cs));
+                GmresOutcome oc;
+                fh_status st = gmres_solve(m, apply, precondition, s->d_b, xq, s->gp, cs, s->work, &oc, err);
+                if (st) return st;
+                if (outcomes) {
+                    outcomes[fi * p + q].iterations = oc.iterations;
+                    outcomes[fi * p + q].relative_residual = oc.relative_residual;
+                    outcomes[fi * p + q].converged = oc.converged ? 1 : 0;
+                }
+                if (!oc.converged) {
+                    fh_status e2 = fail(err, FH_ERR_NOT_CONVERGED,
+                                        "GMRES did not converge at " + std::to_string(f) + " Hz for port " +
+                                            std::to_string(q) + " after " + std::to_string(oc.iterations) +
+                                            " iterations (relative residual " + std::to_string(oc.relative_residual) +
+                                            ")",
+                                        (int64_t)q, -1, f);
+                    if (err) {
+                        err->iterations = oc.iterations;
+                        err->residual = oc.relative_residual;
+                    }
+                    return e2;
+                }
+            }
+            FHB_CUDA(cudaMemcpyAsync(xs.data(), s->d_x, sizeof(double2) * m * p, cudaMemcpyDeviceToHost, cs));
+            FHB_CUDA(cudaStreamSynchronize(cs));
+            // Z = Z_pp - Z_ep^T X (plain transpose: Z is complex symmetric).
+            for (int64_t a = 0; a < p; ++a)
+                for (int64_t b = 0; b < p; ++b) {
+                    cplx acc(0.0, 0.0);
+                    for (int64_t i = 0; i < m; ++i) {
+                        const cplx ep(s->r_ep[i + a * m], omega * s->l_ep[i + a * m]);
+                        const cplx xv(xs[i + b * m].x, xs[i + b * m].y);
+                        acc += cplx(ep.real() * xv.real() - ep.imag() * xv.imag(),
+                                    ep.real() * xv.imag() + ep.imag() * xv.real());
+                    }
+                    z[a + b * p] -= acc;
+                }
+        }
+        // (Z + Z^T) / 2, then finiteness (iterative.rs:291-301).
+        bool finite = true;
+        for (int64_t a = 0; a < p; ++a)
+            for (int64_t b = 0; b < p; ++b) {
+                const cplx v = (z[a + b * p] + z[b + a * p]) * 0.5;
+                finite = finite && std::isfinite(v.real()) && std::isfinite(v.imag());
+                // Row-major output like impedance_ohm[k][a][b].
+                z_out[2 * ((fi * p + a) * p + b)] = v.real();
+                z_out[2 * ((fi * p + a) * p + b) + 1] = v.imag();
+            }
+        if (!finite)
+            return fail(err, FH_ERR_SINGULAR, "the impedance at " + std::to_string(f) + " Hz is not finite", -1, -1, f);
+    }
+    s->timing.solve_s = wall_s() - t0;
+    s->timing.total_s = s->timing.assembly_s + s->timing.solve_s;
+    return FH_OK;
+}
+
+void fh_iterative_destroy(fh_iterative *s) {
+    if (!s) return;
+    cudaStream_t cs = s->stream;
+    delete s;
+    if (cs) cudaStreamDestroy(cs);
+}
+
+fh_status fh_test_gmres_dense(const double *a, size_t n, const double *b, double *x, const double *precond,
+                              const fh_gmres_params *params, fh_gmres_outcome *outcome, fh_error_info *err) {
+    clear_error(err);
+    if (!a || !b || !x || !params) return fail(err, FH_ERR_INVALID_ARGUMENT, "null argument");
+    fh_status st = ensure_device(err);
+    if (st) return st;
+    cudaStream_t cs;
+    FHB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    std::unique_ptr<CUstream_st, decltype(&cudaStreamDestroy)> sg(cs, &cudaStreamDestroy);
+    double2 *d_a = nullptr, *d_m = nullptr, *d_b = nullptr, *d_x = nullptr;
+    FHB_CUDA(cudaMalloc(&d_a, sizeof(double2) * n * n));
+    std::unique_ptr<void, decltype(&cudaFree)> g1(d_a, &cudaFree);
+    FHB_CUDA(cudaMalloc(&d_m, sizeof(double2) * n * n));
+    std::unique_ptr<void, decltype(&cudaFree)> g2(d_m, &cudaFree);
+    FHB_CUDA(cudaMalloc(&d_b, sizeof(double2) * n));
+    std::unique_ptr<void, decltype(&cudaFree)> g3(d_b, &cudaFree);
+    FHB_CUDA(cudaMalloc(&d_x, sizeof(double2) * n));
+    std::unique_ptr<void, decltype(&cudaFree)> g4(d_x, &cudaFree);
+    FHB_CUDA(cudaMemcpyAsync(d_a, a, sizeof(double2) * n * n, cudaMemcpyHostToDevice, cs));
+    if (precond) FHB_CUDA(cudaMemcpyAsync(d_m, precond, sizeof(double2) * n * n, cudaMemcpyHostToDevice, cs));
+    FHB_CUDA(cudaMemcpyAsync(d_b, b, sizeof(double2) * n, cudaMemcpyHostToDevice, cs));
+    FHB_CUDA(cudaMemcpyAsync(d_x, x, sizeof(double2) * n, cudaMemcpyHostToDevice, cs));
+    const int64_t nn = (int64_t)n;
+    DeviceOp apply = [&](const double2 *in, double2 *out, fh_error_info *) {
+        dense_matvec_kernel<<<grid_n(nn), 256, 0, cs>>>(d_a, in, out, nn);
+        return FH_OK;
+    };
+    DeviceOp pre = [&](const double2 *in, double2 *out, fh_error_info *) {
+        if (precond)
+            dense_matvec_kernel<<<grid_n(nn), 256, 0, cs>>>(d_m, in, out, nn);
+        else
+            cudaMemcpyAsync(out, in, sizeof(double2) * nn, cudaMemcpyDeviceToDevice, cs);
+        return FH_OK;
+    };
+    GmresParams gp;
+    gp.tolerance = params->tolerance;
+    gp.restart = params->restart;
+    gp.max_iterations = params->max_iterations;
+    GmresWork work;
+    GmresOutcome oc;
+    st = gmres_solve(nn, apply, pre, d_b, d_x, gp, cs, work, &oc, err);
+    if (st) return st;
+    FHB_CUDA(cudaMemcpyAsync(x, d_x, sizeof(double2) * n, cudaMemcpyDeviceToHost, cs));
+    FHB_CUDA(cudaStreamSynchronize(cs));
+    if (outcome) {
+        outcome->iterations = oc.iterations;
+        outcome->relative_residual = oc.relative_residual;
+        outcome->converged = oc.converged ? 1 : 0;
+    }
+    return FH_OK;
+}
+
+}  // extern "C"

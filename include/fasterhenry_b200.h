@@ -250,8 +250,9 @@ fh_status fh_lu_solve_c64_noalloc(double *a, size_t n, double *b, size_t nrhs, v
 /* Assemble: discretize, loop basis, fill L on the device, congruence
  * R_m = M R M^T, L_m = M L M^T kept resident in HBM.  Replaces
  * MeshSystem::assemble (fasterhenry/src/solve.rs:680-766).  `choice` is
- * resolved with fh_solver_resolve; FH_SOLVER_ITERATIVE returns
- * FH_ERR_UNSUPPORTED in this build. */
+ * resolved with fh_solver_resolve; a choice that resolves to the iterative
+ * path returns FH_ERR_UNSUPPORTED here: the matrix-free path has its own
+ * handle, fh_iterative_create (the reference's IterativeSystem). */
 fh_status fh_system_create(const fh_node *nodes, size_t n_nodes, const fh_segment_def *segments,
                            size_t n_segments, const fh_port *ports, size_t n_ports,
                            const fh_discretization *disc, fh_solver_choice choice,
@@ -385,6 +386,51 @@ fh_status fh_pfft_apply(fh_pfft *op, const double *x, double *y, size_t count, f
 /* PfftOperator::stats (pfft/mod.rs:563-597). */
 fh_status fh_pfft_get_stats(const fh_pfft *op, fh_pfft_stats *stats);
 void fh_pfft_destroy(fh_pfft *op);
+
+/* GmresParams (gmres.rs:32-58). */
+typedef struct fh_gmres_params {
+    double tolerance;       /* ||b - A x|| <= tolerance ||b||; default 1e-10 */
+    int32_t restart;        /* Krylov dimension between restarts; default 100 */
+    int32_t max_iterations; /* cap on products with A over all restarts; default 5000 */
+} fh_gmres_params;
+void fh_gmres_default_params(fh_gmres_params *params);
+
+/* GmresOutcome (gmres.rs:61-73). */
+typedef struct fh_gmres_outcome {
+    int64_t iterations;
+    double relative_residual;
+    int32_t converged;
+} fh_gmres_outcome;
+
+typedef struct fh_iterative fh_iterative;
+
+/* IterativeSystem::assemble (iterative.rs:155-239): discretization, loop
+ * basis, pFFT operator, port columns and the Jacobi diagonal.  Null params
+ * mean the defaults.  Errors as fh_system_create plus FH_ERR_PFFT. */
+fh_status fh_iterative_create(const fh_node *nodes, size_t n_nodes, const fh_segment_def *segments,
+                              size_t n_segments, const fh_port *ports, size_t n_ports,
+                              const fh_discretization *disc, const fh_pfft_params *pfft,
+                              const fh_gmres_params *gmres, fh_iterative **out, fh_error_info *err);
+fh_status fh_iterative_counts(const fh_iterative *sys, fh_counts *out);
+/* inductance_s = operator set-up, assembly_s, solve_s of the last sweep. */
+fh_status fh_iterative_timing(const fh_iterative *sys, fh_timing *out);
+/* IterativeSystem::operator_stats (iterative.rs:259). */
+fh_status fh_iterative_pfft_stats(const fh_iterative *sys, fh_pfft_stats *out);
+/* IterativeSystem::sweep / solve (iterative.rs:269-302, 379-398): z_out is
+ * nf x p x p interleaved complex, row-major per frequency; `outcomes`
+ * (optional) nf x p GMRES outcomes.  FH_ERR_NOT_CONVERGED carries the
+ * frequency, port (index_a), iterations and relative residual of the first
+ * failing solve; FH_ERR_SINGULAR a non-finite Z. */
+fh_status fh_iterative_sweep(fh_iterative *sys, const double *frequencies_hz, size_t nf, double *z_out,
+                             fh_gmres_outcome *outcomes, fh_error_info *err);
+void fh_iterative_destroy(fh_iterative *sys);
+
+/* Test hook (no reference counterpart): the device GMRES on a dense complex
+ * system a (n x n column-major, interleaved), right preconditioner `precond`
+ * (n x n, or NULL for none); x holds the initial guess and receives the
+ * solution. */
+fh_status fh_test_gmres_dense(const double *a, size_t n, const double *b, double *x, const double *precond,
+                              const fh_gmres_params *params, fh_gmres_outcome *outcome, fh_error_info *err);
 
 #ifdef __cplusplus
 }

@@ -22,6 +22,12 @@ reference's Rust path; the Rust reference cannot be built here) on a bounded
 sample: one frequency's FP64 LU + Schur of a leading block of the same
 system, extrapolated to the full sweep by (m / m_sample)^3 x 32.
 
+``--config c5`` runs the matrix-free path instead (its own JSON line): the
+square meander of 157 runs (99,224 filaments at 2 x 2) with the
+precorrected-FFT operator (3 x 3 x 3 stencil, near-field radius 8 cells) and
+GMRES to 1e-8; a step is one Z(1 GHz) solve; the 9,800-filament subset of the
+same fixture is checked against the dense FP64 path.
+
 Multi-GPU (torchrun, N ranks): replicas only — every rank sweeps its own
 copy of the workload (frequencies and geometries are independent; nothing is
 exchanged), timing is the max over ranks.
@@ -53,6 +59,8 @@ def _workload(name):
 
 
 WORKLOADS = {
+    "c5": ("matrix-free: square meander of 157 runs (24,806 segments at 2 x 2: 99,224 filaments), Z at 1 GHz, "
+           "pFFT p = 2 (3 x 3 x 3 stencil), near-field radius 8 cells, GMRES to 1e-8", None),
     "metric": ("meander 167 legs, 10,020 filaments, m = 9,686, 32 freqs 1e5-1e10 Hz", lambda: _workload("metric")),
     "c2": ("meander 40 legs, 2,400 filaments, m = 2,320, 32 freqs 1e5-1e10 Hz", lambda: _workload("c2")),
     "c1": ("4-turn spiral, 240 filaments, m = 224, 10 freqs 1e6-1e10 Hz", lambda: _workload("c1")),
@@ -290,6 +298,75 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_c5(args):
+    """The matrix-free path at the 99,224-filament scale: IterativeSystem
+    assembly (pFFT set-up) and Z(1 GHz) by GMRES, each step one solve; the
+    9,800-filament subset of the same fixture is checked against the dense
+    FP64 path (bound 1e-4 on Z).  Rank 0 only (one GPU)."""
+    import torch
+    import fasterhenry_b200 as fh
+    from fasterhenry_b200 import fixtures as F
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    params = fh.IterativeParams(pfft=fh.PfftParams(near_field_radius=8.0, interpolation_order=2),
+                                gmres=fh.GmresParams(tolerance=1e-8))
+    sub = F.scaling_meander(49)
+    g = fh.Geometry.from_deck(sub)
+    with fh.IterativeSystem.assemble(g, sub.ports, sub.discretization, params) as s:
+        z_it = s.impedance(1e9)
+    with fh.MeshSystem.assemble(g, sub.ports, sub.discretization) as d:
+        z_d = d.impedance(1e9)
+    subset_rel = float(np.max(np.abs(z_it - z_d) / np.abs(z_d)))
+    deck = F.scaling_meander(157)
+    geometry = fh.Geometry.from_deck(deck)
+    t0 = time.perf_counter()
+    system = fh.IterativeSystem.assemble(geometry, deck.ports, deck.discretization, params)
+    assemble_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        system.impedance(1e9)
+    times = []
+    with ClockSampler(local) as clocks, fh.Profiler() as prof:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            z = system.impedance(1e9)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t1)
+        profile = prof.read()
+    step = statistics.median(times)
+    stats = system.operator_stats()
+    outcome = system.last_outcomes[0][0]
+    pa = profile["pfft_apply"]
+    peaks, peak_kind = _peaks()
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    achieved = pa["work"] / (pa["ms"] * 1e-3) / 1e9 if pa["ms"] else 0.0
+    out = {
+        "metric": "matrix-free Z(1 GHz) at 99,224 filaments: GMRES solve s (pFFT operator)",
+        "value": round(step, 6), "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(step * 1e3, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOADS["c5"][0], "filaments": stats["filaments"],
+                   "internal_meshes": system.counts()["internal_meshes"], "grid_dims": stats["grid_dims"],
+                   "fft_dims": stats["fft_dims"], "projection_entries": stats["projection_entries"],
+                   "near_entries": stats["near_entries"], "l2": "FFT grids of %.0f MB each >> L2 (no flush)"
+                   % (16 * np.prod(stats["fft_dims"]) / 1e6)},
+        "assemble_s": round(assemble_s, 3), "setup_host_s": round(stats["setup_host_s"], 3),
+        "setup_device_s": round(stats["setup_device_s"], 3),
+        "gmres": {"iterations": outcome.iterations, "relative_residual": outcome.relative_residual},
+        "z_ohm": [float(z[0, 0].real), float(z[0, 0].imag)],
+        "subset_9800_rel_err_vs_dense": subset_rel,
+        "roofline": {"kernel": "pfft apply (near SpMV, spread, FFTs, interpolation)", "bound": "hbm",
+                     "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4) if hbm else None, "peak_source": peak_kind, "traffic": None,
+                     "launches": pa["launches"], "per_launch_ms": round(pa["ms"] / max(1, pa["launches"]), 4)},
+        "profile": profile, "clocks": clocks.summary(),
+    }
+    print(json.dumps(out))
+    system.close()
+
+
 def library_fp64_lu(system, freqs, counts):
     """A library FP64 GPU LU for context: cuSOLVER's complex128 getrf (through
     torch.linalg.lu_factor) on one frequency's m x m matrix R_ee + j w L_ee,
@@ -396,6 +473,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "c5":
+        run_c5(args)
     else:
         run_ours(args)
 

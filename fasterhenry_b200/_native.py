@@ -120,7 +120,8 @@ EXPORTS = [
     "fh_iterative_pfft_stats", "fh_iterative_sweep", "fh_iterative_destroy", "fh_test_gmres_dense",
 ]
 
-PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner"]
+PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner",
+                   "pfft_apply"]
 
 
 class FillStats(ctypes.Structure):

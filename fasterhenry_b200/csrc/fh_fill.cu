@@ -402,36 +402,50 @@ __global__ void __launch_bounds__(128) point_kernel(const DevFil *__restrict__ f
 
 // ---------------------------------------------------------------------------
 // Hoer-Love closed form (bar.rs:30-106), thread per pair, terms in order.
+// Every operation is an explicit round-to-nearest intrinsic, so nothing is
+// contracted into an FMA: the 64 terms cancel down to a value up to ~1e8
+// times smaller than their magnitudes, which would amplify any departure
+// from the reference's operation-by-operation rounding (its own rounding
+// estimate accepts the result up to 1e-10).
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ double mul_(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double div_(double a, double b) { return __ddiv_rn(a, b); }
+
 __device__ __forceinline__ double log_term(double coefficient, double x, double r, double rest_sq) {
     if (coefficient == 0.0 || x == 0.0) return 0.0;
-    double argument = x >= 0.0 ? x + r : rest_sq / (r - x);
-    return coefficient * x * log(argument);
+    double argument = x >= 0.0 ? add_(x, r) : div_(rest_sq, sub_(r, x));
+    return mul_(mul_(coefficient, x), log(argument));
 }
 __device__ __forceinline__ double atan_term(double x, double y, double z, double r) {
-    double product = x * y * z;
+    double product = mul_(mul_(x, y), z);
     if (product == 0.0) return 0.0;
-    return -(product * z * z / 6.0) * atan(x * y / (z * r));
+    return -mul_(div_(mul_(mul_(product, z), z), 6.0), atan(div_(mul_(x, y), mul_(z, r))));
 }
 __device__ double primitive(double x, double y, double z) {
-    const double x2 = x * x, y2 = y * y, z2 = z * z;
-    const double x4 = x2 * x2, y4 = y2 * y2, z4 = z2 * z2;
-    const double r = sqrt(x2 + y2 + z2);
-    double s = log_term(y2 * z2 / 4.0 - y4 / 24.0 - z4 / 24.0, x, r, y2 + z2);
-    s += log_term(x2 * z2 / 4.0 - x4 / 24.0 - z4 / 24.0, y, r, x2 + z2);
-    s += log_term(x2 * y2 / 4.0 - x4 / 24.0 - y4 / 24.0, z, r, x2 + y2);
-    s += (x4 + y4 + z4 - 3.0 * (x2 * y2 + y2 * z2 + z2 * x2)) * r / 60.0;
-    s += atan_term(x, y, z, r);
-    s += atan_term(x, z, y, r);
-    s += atan_term(y, z, x, r);
+    const double x2 = mul_(x, x), y2 = mul_(y, y), z2 = mul_(z, z);
+    const double x4 = mul_(x2, x2), y4 = mul_(y2, y2), z4 = mul_(z2, z2);
+    const double r = __dsqrt_rn(add_(add_(x2, y2), z2));
+    auto coef = [](double a2, double b2, double a4, double b4) {
+        return sub_(sub_(div_(mul_(a2, b2), 4.0), div_(a4, 24.0)), div_(b4, 24.0));
+    };
+    double s = log_term(coef(y2, z2, y4, z4), x, r, add_(y2, z2));
+    s = add_(s, log_term(coef(x2, z2, x4, z4), y, r, add_(x2, z2)));
+    s = add_(s, log_term(coef(x2, y2, x4, y4), z, r, add_(x2, y2)));
+    const double cross = add_(add_(mul_(x2, y2), mul_(y2, z2)), mul_(z2, x2));
+    s = add_(s, div_(mul_(sub_(add_(add_(x4, y4), z4), mul_(3.0, cross)), r), 60.0));
+    s = add_(s, atan_term(x, y, z, r));
+    s = add_(s, atan_term(x, z, y, r));
+    s = add_(s, atan_term(y, z, x, r));
     return s;
 }
 __device__ __forceinline__ void corner_differences(double e1, double e2, double offset, double q[4]) {
-    double sum = 0.5 * (e1 + e2), diff = 0.5 * (e1 - e2);
-    q[0] = offset + sum;
-    q[1] = offset + diff;
-    q[2] = offset - diff;
-    q[3] = offset - sum;
+    double sum = mul_(0.5, add_(e1, e2)), diff = mul_(0.5, sub_(e1, e2));
+    q[0] = add_(offset, sum);
+    q[1] = add_(offset, diff);
+    q[2] = sub_(offset, diff);
+    q[3] = sub_(offset, sum);
 }
 __device__ void bar_integral(const Aligned &b, double *value, double *rel) {
     double qx[4], qy[4], qz[4];
@@ -443,12 +457,12 @@ __device__ void bar_integral(const Aligned &b, double *value, double *rel) {
     for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j)
             for (int k = 0; k < 4; ++k) {
-                double term = signs[i] * signs[j] * signs[k] * primitive(qx[i], qy[j], qz[k]);
-                v += term;
-                mag += fabs(term);
+                double term = mul_(mul_(mul_(signs[i], signs[j]), signs[k]), primitive(qx[i], qy[j], qz[k]));
+                v = add_(v, term);
+                mag = add_(mag, fabs(term));
             }
     *value = v;
-    *rel = v > 0.0 ? 8.0 * kEps * mag / v : INFINITY;
+    *rel = v > 0.0 ? div_(mul_(mul_(8.0, kEps), mag), v) : INFINITY;
 }
 
 // Aligned pairs: closed form when its error estimate allows, else queue the

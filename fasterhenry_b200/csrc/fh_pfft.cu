@@ -228,6 +228,8 @@ inline unsigned blocks_for(int64_t work, int threads, int64_t cap = 148 * 16) {
 
 }  // namespace
 
+fh_status pfft_apply_impl(PfftDevice &op, const double *d_x, double *d_y, int count, fh_error_info *err);
+
 PfftDevice::~PfftDevice() {
     for (auto &p : plans) cufftDestroy((cufftHandle)p.second);
     void *ptrs[] = {d_dir, d_proj_off, d_proj_idx, d_proj_w, d_spread_off, d_spread_fil,
@@ -353,8 +355,26 @@ fh_status pfft_build(const fh_filament *fil, int64_t n, const PfftConfig &cfg, v
     return FH_OK;
 }
 
+// Algorithmic bytes of one product of `count` vectors: the near-field CSR
+// (12 B per entry) and both passes over the projection (12 B per entry each),
+// the vectors, and per padded complex grid its zeroing, three axis passes of
+// each transform (read + write), the spectrum product (read, write, spectrum).
+double pfft_apply_bytes(const PfftDevice &op, int count) {
+    const int ncomp = (int)op.components.size();
+    const double grids = (double)((count * ncomp + 1) / 2);
+    return 12.0 * (double)op.near_entries + 24.0 * (double)op.projection_entries + 32.0 * (double)op.n * count +
+           grids * (double)op.P * (16.0 + 2.0 * 3.0 * 32.0 + 40.0);
+}
+
 fh_status pfft_apply(PfftDevice &op, const double *d_x, double *d_y, int count, fh_error_info *err) {
     if (op.n == 0 || count <= 0) return FH_OK;
+    prof_begin((cudaStream_t)op.stream, FH_PROF_PFFT_APPLY);
+    fh_status st = pfft_apply_impl(op, d_x, d_y, count, err);
+    prof_end((cudaStream_t)op.stream, FH_PROF_PFFT_APPLY, pfft_apply_bytes(op, count));
+    return st;
+}
+
+fh_status pfft_apply_impl(PfftDevice &op, const double *d_x, double *d_y, int count, fh_error_info *err) {
     cudaStream_t s = (cudaStream_t)op.stream;
     near_kernel<<<blocks_for(op.n * 32, 256), 256, 0, s>>>(op.d_near_off, op.d_near_col, op.d_near_val, d_x, d_y,
                                                              op.n, count);

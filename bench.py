@@ -22,6 +22,9 @@ reference's Rust path; the Rust reference cannot be built here) on a bounded
 sample: one frequency's FP64 LU + Schur of a leading block of the same
 system, extrapolated to the full sweep by (m / m_sample)^3 x 32.
 
+``--config c3`` sweeps 64 seeded spirals of uneven size (16 frequencies each,
+mixed form) through one batched call, four systems in flight.
+
 ``--config c5`` runs the matrix-free path instead (its own JSON line): the
 square meander of 157 runs (99,224 filaments at 2 x 2) with the
 precorrected-FFT operator (3 x 3 x 3 stencil, near-field radius 8 cells) and
@@ -59,6 +62,8 @@ def _workload(name):
 
 
 WORKLOADS = {
+    "c3": ("batched uneven geometries: 64 seeded square spirals (turns 2-8, width 5-20 um, spacing 3-10 um, "
+           "thickness 1-4 um, outer 150-600 um, nw 3-10 x nh 2-3), 16 freqs 1e7-1e10 Hz each", None),
     "c5": ("matrix-free: square meander of 157 runs (24,806 segments at 2 x 2: 99,224 filaments), Z at 1 GHz, "
            "pFFT p = 2 (3 x 3 x 3 stencil), near-field radius 8 cells, GMRES to 1e-8", None),
     "metric": ("meander 167 legs, 10,020 filaments, m = 9,686, 32 freqs 1e5-1e10 Hz", lambda: _workload("metric")),
@@ -298,6 +303,61 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_c3(args):
+    """64 independent spirals of uneven size, each swept over 16 frequencies
+    in the mixed form, all through one batched call (fh_batch_sweep, four
+    systems in flight); a step is the whole batch.  Every Z is checked
+    against the FP64 form of the same batch.  Rank 0 only (one GPU)."""
+    import torch
+    import fasterhenry_b200 as fh
+    from fasterhenry_b200 import fixtures as F
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    decks = F.random_spirals(64, seed=2026)
+    t0 = time.perf_counter()
+    systems = [fh.MeshSystem.assemble(fh.Geometry.from_deck(d), d.ports, d.discretization) for d in decks]
+    assemble_s = time.perf_counter() - t0
+    freqs = [F.logspace(7, 10, 16) for _ in systems]
+    ref = fh.batch_sweep(systems, freqs, fh.Precision.FP64, concurrency=4)
+    for _ in range(args.warmup):
+        fh.batch_sweep(systems, freqs, fh.Precision.MIXED_BF16X3, concurrency=4)
+    times = []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            res = fh.batch_sweep(systems, freqs, fh.Precision.MIXED_BF16X3, concurrency=4)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t1)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    fh.batch_sweep(systems, freqs, fh.Precision.MIXED_BF16X3, concurrency=1)
+    torch.cuda.synchronize()
+    one_at_a_time = time.perf_counter() - t2
+    step = statistics.median(times)
+    rel = max(float(np.max(np.abs(m.impedance_ohm - r.impedance_ohm) / np.abs(r.impedance_ohm)))
+              for m, r in zip(res, ref))
+    counts = [s.counts() for s in systems]
+    out = {
+        "metric": "batched Z(w) sweeps of 64 uneven spirals x 16 freqs: mixed+IR, s", "value": round(step, 6),
+        "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step * 1e3, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c64+bf16x3 (FP64 residual)",
+        "data": "synthetic",
+        "config": {"workload": WORKLOADS["c3"][0], "systems": len(systems),
+                   "filaments_min": min(c["filaments"] for c in counts),
+                   "filaments_max": max(c["filaments"] for c in counts),
+                   "internal_meshes_total": sum(c["internal_meshes"] for c in counts),
+                   "concurrency": 4, "l2": "working sets of up to 64 MB per system; no flush"},
+        "assemble_all_s": round(assemble_s, 3), "one_system_at_a_time_s": round(one_at_a_time, 4),
+        "max_rel_err_vs_fp64": rel, "clocks": clocks.summary(),
+    }
+    print(json.dumps(out))
+    for s in systems:
+        s.close()
+
+
 def run_c5(args):
     """The matrix-free path at the 99,224-filament scale: IterativeSystem
     assembly (pFFT set-up) and Z(1 GHz) by GMRES, each step one solve; the
@@ -475,6 +535,8 @@ def main():
         run_reference(args)
     elif args.config == "c5":
         run_c5(args)
+    elif args.config == "c3":
+        run_c3(args)
     else:
         run_ours(args)
 

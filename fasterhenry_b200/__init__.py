@@ -13,6 +13,6 @@ from .api import (DENSE_PATH_MAX_FILAMENTS, MU0, CoincidentSamples, DiscretizeEr
                   lu_solve, mesh_matrix, mutual_inductance, partial_inductance_matrix, self_inductance, skin_depth,
                   solve)
 from .api import (GmresOutcome, GmresParams, IterativeParams, IterativeSystem, PfftError, PfftOperator, PfftParams,
-                  Profiler, fill_stats, gmres_dense)
+                  Profiler, batch_sweep, fill_stats, gmres_dense)
 
 __version__ = "0.1.0"

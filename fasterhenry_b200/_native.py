@@ -118,6 +118,7 @@ EXPORTS = [
     "fh_profile_read", "fh_pfft_default_params", "fh_pfft_create", "fh_pfft_apply", "fh_pfft_get_stats",
     "fh_pfft_destroy", "fh_gmres_default_params", "fh_iterative_create", "fh_iterative_counts", "fh_iterative_timing",
     "fh_iterative_pfft_stats", "fh_iterative_sweep", "fh_iterative_destroy", "fh_test_gmres_dense",
+    "fh_batch_sweep",
 ]
 
 PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner",
@@ -177,6 +178,8 @@ def load():
     L.fh_iterative_destroy.restype = None
     L.fh_test_gmres_dense.argtypes = [c_double_p, sz, c_double_p, c_double_p, c_double_p, P(GmresParams),
                                       P(GmresOutcome), ei]
+    L.fh_batch_sweep.argtypes = [P(ctypes.c_void_p), sz, P(c_double_p), P(sz), ctypes.c_int, P(c_double_p),
+                                 ctypes.c_int32, ei]
     L.fh_system_destroy.argtypes = [ctypes.c_void_p]
     L.fh_system_destroy.restype = None
     L.fh_system_counts.argtypes = [ctypes.c_void_p, P(Counts)]

@@ -587,6 +587,28 @@ def solve(geometry, ports: Sequence, discretization: dict, frequencies: Sequence
         return system.sweep(frequencies, precision)
 
 
+def batch_sweep(systems: Sequence["MeshSystem"], frequencies: Sequence[Sequence[float]],
+                precision: Precision = Precision.MIXED_BF16X3, concurrency: int = 4) -> List[SweepResult]:
+    """Sweeps many independent systems (uneven sizes) at once: each over its
+    own frequencies, up to ``concurrency`` concurrently on the device
+    (fh_batch_sweep).  Results as MeshSystem.sweep, in input order."""
+    k = len(systems)
+    if len(frequencies) != k:
+        raise InvalidArgument("one frequency list per system")
+    f_arrays = [np.ascontiguousarray(f, dtype=np.float64) for f in frequencies]
+    z_arrays = [np.zeros((len(f), s.counts()["ports"], s.counts()["ports"]), dtype=np.complex128)
+                for s, f in zip(systems, f_arrays)]
+    handles = (ctypes.c_void_p * max(1, k))(*[s._h for s in systems])
+    fptr = (N.c_double_p * max(1, k))(*[f.ctypes.data_as(N.c_double_p) for f in f_arrays])
+    nfs = (ctypes.c_size_t * max(1, k))(*[len(f) for f in f_arrays])
+    zptr = (N.c_double_p * max(1, k))(*[z.ctypes.data_as(N.c_double_p) for z in z_arrays])
+    info = N.ErrorInfo()
+    _check(N.load().fh_batch_sweep(handles, k, fptr, nfs, int(precision), zptr, int(concurrency),
+                                   ctypes.byref(info)), info)
+    return [SweepResult(s.ports, [float(x) for x in f], z, s.counts(), s.timing(), None, None, precision)
+            for s, f, z in zip(systems, f_arrays, z_arrays)]
+
+
 # ---------------------------------------------------------------------------
 # Matrix-free path: the precorrected-FFT operator (pfft/mod.rs)
 # ---------------------------------------------------------------------------

@@ -9,6 +9,9 @@
 #include <memory>
 #include <string>
 #include <vector>
+#include <atomic>
+#include <mutex>
+#include <thread>
 
 #include "fh_device.cuh"
 #include "fh_lu.cuh"
@@ -52,6 +55,9 @@ struct DevPool {
 
 struct fh_system {
     DevPool pool;
+    // Sweeps of this many systems may run at once (fh_batch_sweep): the
+    // cooperative kernels and the batch sizing take 1 / share of the device.
+    int share = 1;
     std::vector<fh_node> nodes;
     std::vector<fh_segment_def> segments;
     std::vector<fh_port> ports;
@@ -206,7 +212,7 @@ fh_status sweep_chunk_fp64(fh_system *s, const double *d_omega, int count, doubl
         PBuf<unsigned char> coop_mem;
         int per_matrix = 0;
         size_t coop_bytes = 0;
-        e = coop_plan<double>(count, m, &per_matrix, &coop_bytes, err);
+        e = coop_plan<double>(count, m, &per_matrix, &coop_bytes, err, s->share);
         if (e) return e;
         FHB_PALLOC(s->pool, coop_mem, kSlotCoop, coop_bytes);
         coop_bind<double>(coop_mem.p, count, per_matrix, cs);
@@ -296,7 +302,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     PBuf<unsigned char> coop_mem;
     int per_matrix = 0;
     size_t coop_bytes = 0;
-    e = coop_plan<float>(count, m, &per_matrix, &coop_bytes, err);
+    e = coop_plan<float>(count, m, &per_matrix, &coop_bytes, err, s->share);
     if (e) return e;
     FHB_PALLOC(pool, coop_mem, kSlotCoop, coop_bytes);
     coop_bind<float>(coop_mem.p, count, per_matrix, cs);
@@ -315,7 +321,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
         w.uinv = uinv_mem.p;
         int per_group = 0;
         size_t solve_bytes = 0;
-        e = trisolve_plan(count * (int)p, m, &per_group, &solve_bytes, err);
+        e = trisolve_plan(count * (int)p, m, &per_group, &solve_bytes, err, s->share);
         if (e) return e;
         if (per_group > 0) {
             FHB_PALLOC(pool, solve_mem, kSlotSolve, solve_bytes);
@@ -735,7 +741,7 @@ fh_status fh_sweep(fh_system *sys, const double *freqs, size_t nf, fh_precision 
     // reference's 2 GiB sweep budget, solve.rs:91 and 884).
     size_t free_b = 0, total_b = 0;
     FHB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    free_b += sys->pool.held();  // the system's own workspace is reused
+    free_b = free_b / (size_t)std::max(1, sys->share) + sys->pool.held();  // own workspace is reused
     if (precision < FH_PRECISION_FP64 || precision > FH_PRECISION_MIXED_FP32)
         return fail(err, FH_ERR_INVALID_ARGUMENT, "unknown precision");
     const bool mixed = precision != FH_PRECISION_FP64;
@@ -824,6 +830,56 @@ fh_status fh_sweep(fh_system *sys, const double *freqs, size_t nf, fh_precision 
         report->solve_s = ms_total * 1e-3;
         report->factor_s = ms_factor * 1e-3;
         report->refine_s = ms_refine * 1e-3;
+    }
+    return FH_OK;
+}
+
+fh_status fh_batch_sweep(fh_system *const *systems, size_t k, const double *const *freqs, const size_t *nf,
+                         fh_precision precision, double *const *z_out, int32_t concurrency, fh_error_info *err) {
+    clear_error(err);
+    if (k && (!systems || !freqs || !nf || !z_out)) return fail(err, FH_ERR_INVALID_ARGUMENT, "null argument");
+    for (size_t i = 0; i < k; ++i)
+        if (!systems[i]) return fail(err, FH_ERR_INVALID_ARGUMENT, "null system " + std::to_string(i));
+    if (k == 0) return FH_OK;
+    const int workers = (int)std::min<size_t>(k, (size_t)(concurrency > 0 ? concurrency : 4));
+    for (size_t i = 0; i < k; ++i) systems[i]->share = workers;
+    std::atomic<size_t> next(0);
+    std::mutex mu;
+    size_t failed = k;
+    fh_status failed_status = FH_OK;
+    fh_error_info failed_info{};
+    std::string failed_msg;
+    auto worker = [&]() {
+        for (;;) {
+            const size_t i = next.fetch_add(1);
+            if (i >= k) return;
+            fh_error_info e{};
+            const fh_status st = fh_sweep(systems[i], freqs[i], nf[i], precision, z_out[i], nullptr, &e);
+            if (st) {
+                std::lock_guard<std::mutex> lk(mu);
+                if (i < failed) {
+                    failed = i;
+                    failed_status = st;
+                    failed_info = e;
+                    const char *m = fh_last_error();
+                    failed_msg = m ? m : "";
+                }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < workers; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto &t : pool) t.join();
+    for (size_t i = 0; i < k; ++i) systems[i]->share = 1;
+    if (failed < k) {
+        fh_status st = fail(err, failed_status, "system " + std::to_string(failed) + ": " + failed_msg,
+                            failed_info.index_a, failed_info.index_b, failed_info.frequency, (int32_t)failed);
+        if (err) {
+            err->iterations = failed_info.iterations;
+            err->residual = failed_info.residual;
+        }
+        return st;
     }
     return FH_OK;
 }

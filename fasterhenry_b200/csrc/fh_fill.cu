@@ -22,6 +22,7 @@
 #include <cub/cub.cuh>
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "fh_device.cuh"
@@ -997,12 +998,15 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
     const int64_t n_arg = list ? 0 : n;  // the method kernels' store mode
     int dev = 0;
     FHB_CUDA(cudaGetDevice(&dev));
+    static std::mutex init_mu;  // first use on a device may race between host threads
+    std::unique_lock<std::mutex> lk(init_mu);
     if (dev < 64 && !g_tables_uploaded[dev]) {
         QuadTables t;
         host_quad_tables(t);
         FHB_CUDA(cudaMemcpyToSymbol(c_quad, &t, sizeof t));
         g_tables_uploaded[dev] = true;
     }
+    lk.unlock();
     FillStats local;
     FillStats &st = stats ? *stats : local;
     st = FillStats();

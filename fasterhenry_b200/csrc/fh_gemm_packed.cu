@@ -38,6 +38,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "fh_lu.cuh"
 
 namespace fhb {
@@ -446,12 +448,15 @@ fh_status gemm_tc_packed_update(const float *A, int64_t lda, int64_t sA, const f
     if (!pack_a || !pack_b) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update needs operand scratch");
     int dev = 0;
     FHB_CUDA(cudaGetDevice(&dev));
+    static std::mutex init_mu;  // first use on a device may race between host threads
+    std::unique_lock<std::mutex> lk(init_mu);
     if (!g_flag[dev]) {
         FHB_CUDA(cudaMalloc(&g_flag[dev], sizeof(int)));
         FHB_CUDA(cudaMemset(g_flag[dev], 0, sizeof(int)));
         FHB_CUDA(cudaFuncSetAttribute(packed_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
         FHB_CUDA(cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev));
     }
+    lk.unlock();
     const int nchunks = K / kChunk;
     const int rblocks = (int)((M + kTile - 1) / kTile), cblocks = (int)((N + kTile - 1) / kTile);
     uint8_t *pa = reinterpret_cast<uint8_t *>(pack_a), *pb = reinterpret_cast<uint8_t *>(pack_b);

@@ -30,6 +30,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "fh_lu.cuh"
 
 namespace fhb {
@@ -374,6 +376,8 @@ fh_status gemm_tc_launch(const GemmArgs &g, int count, cudaStream_t s, fh_error_
     if (g.assign && g.M > kTileM) return fail(err, FH_ERR_INVALID_ARGUMENT, "in-place assign GEMM needs M <= 128");
     int dev = 0;
     FHB_CUDA(cudaGetDevice(&dev));
+    static std::mutex init_mu;  // first use on a device may race between host threads
+    std::lock_guard<std::mutex> lk(init_mu);
     if (!g_err_flag[dev]) {
         FHB_CUDA(cudaMalloc(&g_err_flag[dev], sizeof(int)));
         FHB_CUDA(cudaMemset(g_err_flag[dev], 0, sizeof(int)));

@@ -62,8 +62,11 @@ struct LuWork {
 };
 
 // Cooperative panel: sizing, binding of a scratch block, launch, error check.
+// `share`: the number of cooperative launches that may run at once on the
+// device (concurrent sweeps); each is sized to 1 / share of the resident
+// capacity so that all of them are co-resident together.
 template <class T>
-fh_status coop_plan(int count, int64_t m, int *per_matrix, size_t *bytes, fh_error_info *err);
+fh_status coop_plan(int count, int64_t m, int *per_matrix, size_t *bytes, fh_error_info *err, int share = 1);
 template <class T>
 void coop_bind(void *mem, int count, int per_matrix, CoopScratch &cs);
 template <class T>
@@ -123,7 +126,7 @@ struct SolveScratch {
     int groups = 0;        // count * nrhs
     int per_group = 0;     // CTAs per group; 0 = the batch does not fit one launch
 };
-fh_status trisolve_plan(int groups, int64_t m, int *per_group, size_t *bytes, fh_error_info *err);
+fh_status trisolve_plan(int groups, int64_t m, int *per_group, size_t *bytes, fh_error_info *err, int share = 1);
 void trisolve_bind(void *mem, int groups, int per_group, SolveScratch &ss);
 fh_status lu_solve_inv(const LuBatch<float> &b, const void *linv, const void *uinv, float *x, int nrhs, int nb,
                        int group, const SolveScratch &ss, cudaStream_t s, fh_error_info *err);

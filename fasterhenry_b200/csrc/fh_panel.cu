@@ -318,14 +318,14 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_k
 }  // namespace
 
 template <class T>
-fh_status coop_plan(int count, int64_t m, int *per_matrix, size_t *bytes, fh_error_info *err) {
+fh_status coop_plan(int count, int64_t m, int *per_matrix, size_t *bytes, fh_error_info *err, int share) {
     int dev = 0, sms = 0, occ = 0, coop = 0;
     FHB_CUDA(cudaGetDevice(&dev));
     FHB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     FHB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     if (!coop) return fail(err, FH_ERR_NO_DEVICE, "the device does not support cooperative launches");
     FHB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_coop_kernel<T>, kThreads, 0));
-    const int capacity = occ * sms;
+    const int capacity = occ * sms / std::max(1, share);
     int pm = std::max(1, capacity / std::max(1, count));
     pm = (int)std::min<int64_t>(pm, std::max<int64_t>(1, (m + 63) / 64));
     if ((int64_t)pm * count > capacity)
@@ -381,8 +381,8 @@ fh_status coop_check(const CoopScratch &cs, cudaStream_t s, fh_error_info *err) 
     return FH_OK;
 }
 
-template fh_status coop_plan<double>(int, int64_t, int *, size_t *, fh_error_info *);
-template fh_status coop_plan<float>(int, int64_t, int *, size_t *, fh_error_info *);
+template fh_status coop_plan<double>(int, int64_t, int *, size_t *, fh_error_info *, int);
+template fh_status coop_plan<float>(int, int64_t, int *, size_t *, fh_error_info *, int);
 template void coop_bind<double>(void *, int, int, CoopScratch &);
 template void coop_bind<float>(void *, int, int, CoopScratch &);
 template fh_status panel_coop<double>(LuBatch<double> &, int64_t, int, const CoopScratch &, cudaStream_t, fh_error_info *);

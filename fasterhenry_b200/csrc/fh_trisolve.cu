@@ -194,14 +194,14 @@ __global__ void __launch_bounds__(kThreads) trisolve_kernel(SolveArgs g) {
 
 }  // namespace
 
-fh_status trisolve_plan(int groups, int64_t m, int *per_group, size_t *bytes, fh_error_info *err) {
+fh_status trisolve_plan(int groups, int64_t m, int *per_group, size_t *bytes, fh_error_info *err, int share) {
     int dev = 0, sms = 0, occ = 0, coop = 0;
     FHB_CUDA(cudaGetDevice(&dev));
     FHB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     FHB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     if (!coop) return fail(err, FH_ERR_NO_DEVICE, "the device does not support cooperative launches");
     FHB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, trisolve_kernel, kThreads, 0));
-    const int capacity = occ * sms;
+    const int capacity = occ * sms / std::max(1, share);
     if (groups <= 0 || groups > capacity) {
         *per_group = 0;  // the caller falls back to the one-launch-per-block solve
         *bytes = 0;

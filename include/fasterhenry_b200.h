@@ -280,6 +280,16 @@ fh_status fh_system_device_l_mesh(const fh_system *sys, const double **l_mesh, c
 fh_status fh_sweep(fh_system *sys, const double *frequencies_hz, size_t nf, fh_precision precision,
                    double *z_out, fh_sweep_report *report, fh_error_info *err);
 
+/* Batched sweep of independent systems (no reference counterpart: the
+ * reference sweeps one MeshSystem at a time).  System i is swept over its own
+ * frequencies freqs[i][0..nf[i]) into z_out[i] (nf[i] x p_i x p_i), as
+ * fh_sweep would; up to `concurrency` systems (<= 0: 4) run at once, each on
+ * its own stream, with their cooperative kernels and batch sizes taking an
+ * equal share of the device.  On failure the first failing system (lowest
+ * index) is reported, its index in fh_error_info.detail. */
+fh_status fh_batch_sweep(fh_system *const *systems, size_t k, const double *const *freqs, const size_t *nf,
+                         fh_precision precision, double *const *z_out, int32_t concurrency, fh_error_info *err);
+
 /* One frequency (MeshSystem::impedance, solve.rs:806-830). */
 fh_status fh_impedance(fh_system *sys, double frequency_hz, fh_precision precision, double *z_out,
                        fh_error_info *err);

@@ -85,6 +85,15 @@ class GmresParams(ctypes.Structure):
     _fields_ = [("tolerance", ctypes.c_double), ("restart", ctypes.c_int32), ("max_iterations", ctypes.c_int32)]
 
 
+class ParamSpec(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("reserved", ctypes.c_int32), ("index", ctypes.c_int64)]
+
+
+class GradientReport(ctypes.Structure):
+    _fields_ = [("solve_s", ctypes.c_double), ("derivative_fill_s", ctypes.c_double), ("contract_s", ctypes.c_double),
+                ("total_s", ctypes.c_double), ("pairs", ctypes.c_int64)]
+
+
 class GmresOutcome(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int64), ("relative_residual", ctypes.c_double), ("converged", ctypes.c_int32)]
 
@@ -118,7 +127,7 @@ EXPORTS = [
     "fh_profile_read", "fh_pfft_default_params", "fh_pfft_create", "fh_pfft_apply", "fh_pfft_get_stats",
     "fh_pfft_destroy", "fh_gmres_default_params", "fh_iterative_create", "fh_iterative_counts", "fh_iterative_timing",
     "fh_iterative_pfft_stats", "fh_iterative_sweep", "fh_iterative_destroy", "fh_test_gmres_dense",
-    "fh_batch_sweep",
+    "fh_batch_sweep", "fh_gradient", "fh_test_inductance_gradient",
 ]
 
 PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner",
@@ -180,6 +189,9 @@ def load():
                                       P(GmresOutcome), ei]
     L.fh_batch_sweep.argtypes = [P(ctypes.c_void_p), sz, P(c_double_p), P(sz), ctypes.c_int, P(c_double_p),
                                  ctypes.c_int32, ei]
+    L.fh_gradient.argtypes = [ctypes.c_void_p, ctypes.c_double, P(ParamSpec), sz, c_double_p, c_double_p,
+                              P(GradientReport), ei]
+    L.fh_test_inductance_gradient.argtypes = [P(Filament), c_double_p, sz, c_double_p, c_double_p, ei]
     L.fh_system_destroy.argtypes = [ctypes.c_void_p]
     L.fh_system_destroy.restype = None
     L.fh_system_counts.argtypes = [ctypes.c_void_p, P(Counts)]

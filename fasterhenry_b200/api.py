@@ -571,6 +571,81 @@ class MeshSystem:
     def impedance(self, frequency: float, precision: Precision = Precision.FP64) -> np.ndarray:
         return self.sweep([frequency], precision).impedance_ohm[0]
 
+    def gradient(self, frequency: float, params: Optional[Sequence["Param"]] = None) -> "GradientResult":
+        """dZ/dp at one frequency by the stationary (adjoint) form
+        (fh_gradient): one FP64 solve for the loop currents, one derivative
+        fill, one product per derivative matrix.  ``params`` defaults to
+        every segment's width, then every segment's thickness."""
+        if params is None:
+            nseg = self._counts["segments"]
+            params = [Param("width", s) for s in range(nseg)] + [Param("thickness", s) for s in range(nseg)]
+        params = list(params)
+        spec = (N.ParamSpec * max(1, len(params)))()
+        for k, q in enumerate(params):
+            spec[k].kind = Param.KINDS[q.kind]
+            spec[k].index = int(q.index)
+        p = self._counts["ports"]
+        z = np.zeros((p, p), dtype=np.complex128)
+        dz = np.zeros((max(1, len(params)), p, p), dtype=np.complex128)
+        rep = N.GradientReport()
+        info = N.ErrorInfo()
+        _check(N.load().fh_gradient(self._h, float(frequency), spec, len(params), z.ctypes.data_as(N.c_double_p),
+                                    dz.ctypes.data_as(N.c_double_p), ctypes.byref(rep), ctypes.byref(info)), info)
+        return GradientResult(float(frequency), params, z, dz[:len(params)],
+                              {k: (int(getattr(rep, k)) if k == "pairs" else float(getattr(rep, k)))
+                               for k, _ in N.GradientReport._fields_})
+
+
+@dataclasses.dataclass(frozen=True)
+class Param:
+    """A geometric parameter of dZ/dp: the "width" or "thickness" of segment
+    ``index``, or the "x" / "y" / "z" coordinate of node ``index`` (node
+    coordinates are rejected with Unsupported: moving a node rotates the
+    segments that meet there)."""
+    kind: str
+    index: int
+
+    KINDS = {"width": 0, "thickness": 1, "x": 2, "y": 3, "z": 4}
+
+
+@dataclasses.dataclass
+class GradientResult:
+    """Z (p x p) and dZ/dp (one p x p matrix per parameter, ohm per metre) at
+    one frequency.  ``resistance_gradient`` and ``inductance_gradient`` are
+    d Re Z / dp and d (Im Z / omega) / dp (zero frequency: inductance
+    gradient undefined, reported as NaN)."""
+    frequency_hz: float
+    params: List[Param]
+    impedance_ohm: np.ndarray
+    gradient: np.ndarray
+    report: Dict[str, float]
+
+    @property
+    def resistance_gradient(self) -> np.ndarray:
+        return self.gradient.real
+
+    @property
+    def inductance_gradient(self) -> np.ndarray:
+        w = 2.0 * np.pi * self.frequency_hz
+        return self.gradient.imag / w if w > 0 else np.full(self.gradient.shape, np.nan)
+
+
+def inductance_gradient(filaments: np.ndarray, tangents: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    """The derivative fill on its own (fh_test_inductance_gradient): for
+    filaments (n x 19) and their tangents (n x 4: sw, sh, gw, gh), returns
+    (Dw, Dh) with D[a, b] = dL_ab / d(side a)."""
+    f = np.ascontiguousarray(filaments, dtype=np.float64).reshape(-1, FILAMENT_FIELDS)
+    fil = _fil_array(f)
+    n = len(f)
+    t = np.ascontiguousarray(tangents, dtype=np.float64).reshape(n, 4) if n else np.zeros((1, 4))
+    dw = np.zeros((n, n), order="F")
+    dh = np.zeros((n, n), order="F")
+    info = N.ErrorInfo()
+    _check(N.load().fh_test_inductance_gradient(fil, t.ctypes.data_as(N.c_double_p), n,
+                                                dw.ctypes.data_as(N.c_double_p), dh.ctypes.data_as(N.c_double_p),
+                                                ctypes.byref(info)), info)
+    return dw, dh
+
 
 def solve(geometry, ports: Sequence, discretization: dict, frequencies: Sequence[float],
           precision: Precision = Precision.FP64, solver: SolverChoice = SolverChoice.DENSE,

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -887,6 +888,223 @@ fh_status fh_batch_sweep(fh_system *const *systems, size_t k, const double *cons
 fh_status fh_impedance(fh_system *sys, double frequency_hz, fh_precision precision, double *z_out,
                        fh_error_info *err) {
     return fh_sweep(sys, &frequency_hz, 1, precision, z_out, nullptr, err);
+}
+
+// ---------------------------------------------------------------------------
+// Impedance gradient by the stationary form (no reference counterpart).
+// Z_ab = I_a^T Zm I_b with the loop currents I = [-Z_ee^-1 Z_ep; 1] of unit
+// port currents; Zm = M (R + j w L) M^T is complex symmetric and Zm I has no
+// internal-loop rows, so the first-order change of I drops out and
+// dZ_ab = (M^T I_a)^T (dR + j w dL) (M^T I_b).
+// ---------------------------------------------------------------------------
+fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *params, size_t np, double *z_out,
+                      double *dz_out, fh_gradient_report *report, fh_error_info *err) {
+    clear_error(err);
+    if (!sys || (np && (!params || !dz_out))) return fail(err, FH_ERR_INVALID_ARGUMENT, "null argument");
+    if (!(std::isfinite(frequency_hz) && frequency_hz >= 0.0))
+        return fail(err, FH_ERR_INVALID_FREQUENCY,
+                    "frequency 0 is " + fstr(frequency_hz) + " Hz; frequencies must be finite and non-negative", 0, -1,
+                    frequency_hz);
+    const int64_t nseg = (int64_t)sys->segments.size();
+    for (size_t k = 0; k < np; ++k) {
+        const fh_param_spec &q = params[k];
+        if (q.kind == FH_PARAM_NODE_X || q.kind == FH_PARAM_NODE_Y || q.kind == FH_PARAM_NODE_Z)
+            return fail(err, FH_ERR_UNSUPPORTED,
+                        "parameter " + std::to_string(k) +
+                            " is a node coordinate: moving a node rotates the segments that meet there, and the "
+                            "derivative of the partial inductances under a rotation is not provided",
+                        (int64_t)k);
+        if (q.kind != FH_PARAM_WIDTH && q.kind != FH_PARAM_THICKNESS)
+            return fail(err, FH_ERR_INVALID_ARGUMENT, "parameter " + std::to_string(k) + " has an unknown kind",
+                        (int64_t)k);
+        if (q.index < 0 || q.index >= nseg)
+            return fail(err, FH_ERR_INVALID_ARGUMENT,
+                        "parameter " + std::to_string(k) + " names segment " + std::to_string(q.index) +
+                            ", but the geometry has " + std::to_string(nseg),
+                        (int64_t)k, q.index);
+    }
+    FHB_CUDA(cudaSetDevice(sys->device));
+    const double t0 = wall();
+    const int64_t n = sys->n, m = sys->m, p = sys->p, loops = sys->nloops;
+    cudaStream_t st = sys->stream;
+    // 1. Loop currents X = Z_ee^-1 Z_ep and Z, in FP64.
+    PBuf<double> d_omega, d_x, d_z;
+    FHB_PALLOC(sys->pool, d_omega, kSlotOmega, 1);
+    FHB_PALLOC(sys->pool, d_x, kSlotX, (size_t)std::max<int64_t>(1, m * p * 2));
+    FHB_PALLOC(sys->pool, d_z, kSlotZ, (size_t)p * p * 2);
+    const double omega = kTau * frequency_hz;
+    FHB_CUDA(cudaMemcpyAsync(d_omega.p, &omega, 8, cudaMemcpyHostToDevice, st));
+    int singular = 0;
+    fh_status e = sweep_chunk_fp64(sys, d_omega.p, 1, d_x.p, d_z.p, &singular, nullptr, err);
+    if (e) return e;
+    std::vector<double> x((size_t)(m * p * 2)), z((size_t)(p * p * 2));
+    if (m) FHB_CUDA(cudaMemcpyAsync(x.data(), d_x.p, 8 * x.size(), cudaMemcpyDeviceToHost, st));
+    FHB_CUDA(cudaMemcpyAsync(z.data(), d_z.p, 8 * z.size(), cudaMemcpyDeviceToHost, st));
+    FHB_CUDA(cudaStreamSynchronize(st));
+    bool bad = singular != 0;
+    for (double v : z) bad = bad || !std::isfinite(v);
+    if (bad)
+        return fail(err, FH_ERR_SINGULAR,
+                    "the mesh system is singular or ill-conditioned at " + fstr(frequency_hz) + " Hz", 0, -1,
+                    frequency_hz);
+    const double t1 = wall();
+    // 2. Branch currents I_b = M^T [-X; 1], n x p complex (column q at 2 q n).
+    std::vector<double> ib((size_t)(2 * n * p), 0.0);
+    for (int64_t r = 0; r < loops; ++r)
+        for (int64_t q = 0; q < p; ++q) {
+            double re, im;
+            if (r < m) {
+                re = -x[2 * (q * m + r)];
+                im = -x[2 * (q * m + r) + 1];
+            } else {
+                re = r - m == q ? 1.0 : 0.0;
+                im = 0.0;
+            }
+            if (re == 0.0 && im == 0.0) continue;
+            for (int64_t k = sys->loops.row_ptr[r]; k < sys->loops.row_ptr[r + 1]; ++k) {
+                const int64_t b = sys->loops.branch[k];
+                const double sg = sys->loops.sign[k];
+                ib[2 * (q * n + b)] += sg * re;
+                ib[2 * (q * n + b) + 1] += sg * im;
+            }
+        }
+    // 3. How each filament moves with its segment's width and thickness:
+    // the discretization places it at a + W c_w w + H c_h h with its own
+    // width f_w w and height f_h h (counts and grading ratios fixed).
+    std::vector<FilTan> tan((size_t)n);
+    std::vector<int64_t> seg_of((size_t)n);
+    {
+        int64_t i = 0;
+        for (int64_t s = 0; s < nseg; ++s) {
+            const fh_segment_def &sd = sys->segments[(size_t)s];
+            const fh_node &a = sys->nodes[(size_t)sd.a];
+            for (int64_t k = 0; k < sys->disc.per_segment[(size_t)s]; ++k, ++i) {
+                const fh_filament &f = sys->disc.filaments[(size_t)i];
+                const double d[3] = {f.start[0] - a.x, f.start[1] - a.y, f.start[2] - a.z};
+                const double cw = d[0] * f.dir_width[0] + d[1] * f.dir_width[1] + d[2] * f.dir_width[2];
+                const double ch = d[0] * f.dir_height[0] + d[1] * f.dir_height[1] + d[2] * f.dir_height[2];
+                tan[(size_t)i] = FilTan{cw / sd.width, ch / sd.height, f.width / sd.width, f.height / sd.height};
+                seg_of[(size_t)i] = s;
+            }
+        }
+    }
+    // 4. Derivative fill and the products with the branch currents.
+    size_t free_b = 0, total_b = 0;
+    FHB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t part = gradient_part_elems(n, (int)p);
+    const double need = 16.0 * (double)n * (double)n + 8.0 * (double)(part + 6 * n * p) + 288.0 * (double)n;
+    if (need > 0.9 * (double)free_b)
+        return fail(err, FH_ERR_OUT_OF_MEMORY,
+                    "the derivative fill of " + std::to_string(n) + " filaments needs " + fstr(need) +
+                        " bytes of device memory; " + std::to_string(free_b) + " are free");
+    std::vector<DevFil> h((size_t)n);
+    for (int64_t i = 0; i < n; ++i) h[(size_t)i] = make_devfil(sys->disc.filaments[(size_t)i]);
+    DBuf<DevFil> d_fil;
+    DBuf<FilTan> d_tan;
+    DBuf<double> d_D, d_I, d_y, d_part;
+    FHB_ALLOC(d_fil, (size_t)n);
+    FHB_ALLOC(d_tan, (size_t)n);
+    FHB_ALLOC(d_D, (size_t)(2 * n * n));
+    FHB_ALLOC(d_I, (size_t)(2 * n * p));
+    FHB_ALLOC(d_y, (size_t)(4 * n * p));
+    FHB_ALLOC(d_part, part);
+    FHB_CUDA(cudaMemcpyAsync(d_fil.p, h.data(), sizeof(DevFil) * n, cudaMemcpyHostToDevice, st));
+    FHB_CUDA(cudaMemcpyAsync(d_tan.p, tan.data(), sizeof(FilTan) * n, cudaMemcpyHostToDevice, st));
+    FHB_CUDA(cudaMemcpyAsync(d_I.p, ib.data(), 8 * ib.size(), cudaMemcpyHostToDevice, st));
+    FHB_CUDA(cudaMemsetAsync(d_D.p, 0, 16 * (size_t)n * n, st));
+    cudaEvent_t ev[3];
+    for (auto &v : ev) FHB_CUDA(cudaEventCreate(&v));
+    struct EvGuard {
+        cudaEvent_t *ev;
+        ~EvGuard() {
+            for (int k = 0; k < 3; ++k) cudaEventDestroy(ev[k]);
+        }
+    } evg{ev};
+    FillStats fs;
+    FHB_CUDA(cudaEventRecord(ev[0], st));
+    e = device_fill_grad(d_fil.p, d_tan.p, n, GradOut{d_D.p, d_D.p + n * n}, st, &fs, err);
+    if (e) return e;
+    FHB_CUDA(cudaEventRecord(ev[1], st));
+    e = gradient_products(d_D.p, d_D.p + n * n, n, d_I.p, (int)p, d_y.p, d_part.p, st, err);
+    if (e) return e;
+    FHB_CUDA(cudaEventRecord(ev[2], st));
+    std::vector<double> y((size_t)(4 * n * p));
+    FHB_CUDA(cudaMemcpyAsync(y.data(), d_y.p, 8 * y.size(), cudaMemcpyDeviceToHost, st));
+    FHB_CUDA(cudaStreamSynchronize(st));
+    float ms_fill = 0, ms_prod = 0;
+    cudaEventElapsedTime(&ms_fill, ev[0], ev[1]);
+    cudaEventElapsedTime(&ms_prod, ev[1], ev[2]);
+    // 5. Per segment and kind: sum over its filaments of
+    //    I_a I_b dR_i + j w (I_a (D I_b)_i + I_b (D I_a)_i).
+    typedef std::complex<double> C;
+    const size_t pp = (size_t)(p * p);
+    std::vector<C> acc((size_t)(2 * nseg) * pp, C(0.0, 0.0));
+    auto I = [&](int64_t q, int64_t i) { return C(ib[2 * (q * n + i)], ib[2 * (q * n + i) + 1]); };
+    auto Y = [&](int which, int64_t q, int64_t i) {
+        const size_t o = (size_t)(2 * (((int64_t)which * p + q) * n + i));
+        return C(y[o], y[o + 1]);
+    };
+    const C jw(0.0, omega);
+    for (int64_t i = 0; i < n; ++i) {
+        const fh_filament &f = sys->disc.filaments[(size_t)i];
+        const double r = sys->resistances[(size_t)i];
+        const double dr[2] = {-r * tan[(size_t)i].gw / f.width, -r * tan[(size_t)i].gh / f.height};
+        for (int which = 0; which < 2; ++which) {
+            C *out = acc.data() + (size_t)(2 * seg_of[(size_t)i] + which) * pp;
+            for (int64_t a = 0; a < p; ++a)
+                for (int64_t b = 0; b < p; ++b)
+                    out[a * p + b] += I(a, i) * I(b, i) * dr[which] + jw * (I(a, i) * Y(which, b, i) + I(b, i) * Y(which, a, i));
+        }
+    }
+    for (size_t k = 0; k < np; ++k) {
+        const C *src = acc.data() + (size_t)(2 * params[k].index + (params[k].kind == FH_PARAM_THICKNESS)) * pp;
+        for (size_t q = 0; q < pp; ++q) {
+            dz_out[2 * (k * pp + q)] = src[q].real();
+            dz_out[2 * (k * pp + q) + 1] = src[q].imag();
+        }
+    }
+    if (z_out) std::memcpy(z_out, z.data(), 8 * z.size());
+    if (report) {
+        report->solve_s = t1 - t0;
+        report->derivative_fill_s = ms_fill * 1e-3;
+        report->contract_s = ms_prod * 1e-3;
+        report->total_s = wall() - t0;
+        report->pairs = fs.pairs;
+    }
+    return FH_OK;
+}
+
+fh_status fh_test_inductance_gradient(const fh_filament *filaments, const double *tangents, size_t n, double *Dw,
+                                      double *Dh, fh_error_info *err) {
+    clear_error(err);
+    if (n && (!filaments || !tangents || !Dw || !Dh)) return fail(err, FH_ERR_INVALID_ARGUMENT, "null argument");
+    fh_status st = ensure_device(err);
+    if (st) return st;
+    if (n == 0) return FH_OK;
+    std::vector<DevFil> h(n);
+    std::vector<FilTan> t(n);
+    for (size_t i = 0; i < n; ++i) {
+        h[i] = make_devfil(filaments[i]);
+        t[i] = FilTan{tangents[4 * i], tangents[4 * i + 1], tangents[4 * i + 2], tangents[4 * i + 3]};
+    }
+    DBuf<DevFil> d_fil;
+    DBuf<FilTan> d_tan;
+    DBuf<double> d_D;
+    FHB_ALLOC(d_fil, n);
+    FHB_ALLOC(d_tan, n);
+    FHB_ALLOC(d_D, 2 * n * n);
+    cudaStream_t s;
+    FHB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    std::unique_ptr<CUstream_st, decltype(&cudaStreamDestroy)> guard(s, &cudaStreamDestroy);
+    FHB_CUDA(cudaMemcpyAsync(d_fil.p, h.data(), n * sizeof(DevFil), cudaMemcpyHostToDevice, s));
+    FHB_CUDA(cudaMemcpyAsync(d_tan.p, t.data(), n * sizeof(FilTan), cudaMemcpyHostToDevice, s));
+    FHB_CUDA(cudaMemsetAsync(d_D.p, 0, 16 * n * n, s));
+    st = device_fill_grad(d_fil.p, d_tan.p, (int64_t)n, GradOut{d_D.p, d_D.p + n * n}, s, nullptr, err);
+    if (st) return st;
+    FHB_CUDA(cudaMemcpyAsync(Dw, d_D.p, 8 * n * n, cudaMemcpyDeviceToHost, s));
+    FHB_CUDA(cudaMemcpyAsync(Dh, d_D.p + n * n, 8 * n * n, cudaMemcpyDeviceToHost, s));
+    FHB_CUDA(cudaStreamSynchronize(s));
+    return FH_OK;
 }
 
 }  // extern "C"

@@ -76,6 +76,32 @@ fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_met
 fh_status device_fill_pairs(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t n_pairs, double *d_out,
                             cudaStream_t stream, FillStats *stats, fh_error_info *err);
 
+// How a filament moves with the cross-section of its segment: d centre /
+// d width = sw * width axis, d (own width) / d width = gw, and likewise sh,
+// gh for the segment's thickness (the discretization's counts and grading
+// ratios held fixed).
+struct FilTan {
+    double sw, sh, gw, gh;
+};
+// Outputs of the derivative fill: n x n column-major, D[a + b n] = the
+// derivative of L_ab with respect to the width (Dw) or thickness (Dh) of the
+// segment of filament a, filament b held fixed.
+struct GradOut {
+    double *Dw, *Dh;
+};
+// Both matrices must be zero-filled by the caller (orthogonal pairs stay 0).
+// Pairs evaluated by sampled filaments (non-aligned parallel or skew bars)
+// have no derivative here: FH_ERR_UNSUPPORTED.
+fh_status device_fill_grad(const DevFil *d_fil, const FilTan *d_tan, int64_t n, GradOut out, cudaStream_t stream,
+                           FillStats *stats, fh_error_info *err);
+
+// y = D_w I and D_h I for p complex vectors I (n x p, column q at 2 q n):
+// y holds 2 x p columns (D_w's products first).  d_part is scratch of
+// gradient_part_elems(n, p) doubles.
+fh_status gradient_products(const double *d_Dw, const double *d_Dh, int64_t n, const double *d_I, int p, double *d_y,
+                            double *d_part, cudaStream_t stream, fh_error_info *err);
+size_t gradient_part_elems(int64_t n, int p);
+
 // R_m = M diag(R) M^T and L_m = M L M^T (loops x loops, column-major), upper
 // triangle evaluated in the reference's order and mirrored.
 fh_status device_congruence(const double *d_L, const double *d_R, int64_t n, const int64_t *d_row_ptr,

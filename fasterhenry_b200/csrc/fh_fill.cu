@@ -576,6 +576,47 @@ __device__ int break_points(double e1, double e2, double offset, double *out) {
     return m;
 }
 
+// Partials of one overlap weight (overlap_weight) with respect to e1, e2 and
+// offset at a fixed abscissa u: piecewise constant, following the branch
+// that min/max take.
+__device__ __forceinline__ double overlap_weight_grad(double e1, double e2, double offset, double u, double d[3]) {
+    const double a = 0.5 * e1, b = offset + 0.5 * e2 - u;
+    const double c = -0.5 * e1, e = offset - 0.5 * e2 - u;
+    const bool hi_a = a < b, lo_c = c > e;
+    const double hi = hi_a ? a : b, lo = lo_c ? c : e;
+    if (!(hi - lo > 0.0)) {
+        d[0] = d[1] = d[2] = 0.0;
+        return 0.0;
+    }
+    d[0] = (hi_a ? 0.5 : 0.0) - (lo_c ? -0.5 : 0.0);
+    d[1] = (hi_a ? 0.0 : 0.5) - (lo_c ? 0.0 : -0.5);
+    d[2] = (hi_a ? 0.0 : 1.0) - (lo_c ? 0.0 : 1.0);
+    return hi - lo;
+}
+// The integrand and its partials with respect to the six cross-section
+// inputs (width[0], width[1], offset[1], height[0], height[1], offset[2]) at
+// fixed (u, v): the axial kernel does not depend on them.  g[0] is the value.
+__device__ __forceinline__ void integrand_grad(const QuadCtx &c, double u, double v, double g[7]) {
+    double dw[3], dh[3];
+    const double ww = overlap_weight_grad(c.b.width[0], c.b.width[1], c.b.offset[1], u, dw);
+    const double wh = overlap_weight_grad(c.b.height[0], c.b.height[1], c.b.offset[2], v, dh);
+    if (ww == 0.0 || wh == 0.0) {
+        for (int k = 0; k < 7; ++k) g[k] = 0.0;
+        return;
+    }
+    double k;
+    if (!lines_parallel(c.b.length[0], c.b.length[1], c.axial_start, hypot(u, v), &k)) k = 0.0;
+    g[0] = ww * wh * k;
+    for (int q = 0; q < 3; ++q) {
+        g[1 + q] = dw[q] * wh * k;
+        g[4 + q] = ww * dh[q] * k;
+    }
+}
+
+// kGrad: values[7 h + 0..6] = the integral and its partials with respect to
+// (width[0], width[1], offset[1], height[0], height[1], offset[2]), the rule
+// (panel tree, leaves, nodes) held at the pair's own geometry.
+template <bool kGrad>
 __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
     const DevFil *__restrict__ fil, const int4 *__restrict__ items, const int64_t *__restrict__ heads,
     int64_t n_heads, double *__restrict__ values) {
@@ -583,7 +624,7 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
     __shared__ Leaf leaves[kLeaves];
     __shared__ int s_nleaves, s_done;
     __shared__ QuadCtx ctx;
-    __shared__ double s_red[kQuadThreads / 32];
+    __shared__ double s_red[kGrad ? 7 : 1][kQuadThreads / 32];
     __shared__ double r10n[10], r10w[10], r16n[16], r16w[16];
     if (threadIdx.x < 10) {
         r10n[threadIdx.x] = c_quad.nodes[10][threadIdx.x];
@@ -617,7 +658,7 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
             for (int a = nu - 2; a >= 0; --a)
                 for (int c = nv - 2; c >= 0; --c) stack[sp++] = Panel{us[a], us[a + 1], vs[c], vs[c + 1], 0, 0};
         }
-        double acc = 0.0;
+        double acc = 0.0, gacc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         long long visited = 0;  // panels popped; bounded so that no input can loop without end
         bool overflow = false;
         for (;;) {
@@ -693,7 +734,14 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
                         int a = k / 10, c = k % 10;
                         double uu = mu + hu * r10n[a], wu = hu * r10w[a];
                         double vv = mv + hv * r10n[c], wv = hv * r10w[c];
-                        acc += wu * wv * integrand(ctx, uu, vv);
+                        if (kGrad) {
+                            double g[7];
+                            integrand_grad(ctx, uu, vv, g);
+                            acc += wu * wv * g[0];
+                            for (int q = 0; q < 6; ++q) gacc[q] += wu * wv * g[1 + q];
+                        } else {
+                            acc += wu * wv * integrand(ctx, uu, vv);
+                        }
                     }
                 } else {
                     const double A = lf.a0, B = lf.b0, ab = fabs(A * B);
@@ -703,8 +751,17 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
                         double s = tau * tau * tau;
                         double radial = w_tau * 3.0 * tau * tau * s;
                         double t = 0.5 + 0.5 * r16n[c], w_t = 0.5 * r16w[c];
-                        double value = integrand(ctx, A * s, B * s * t) + integrand(ctx, A * s * t, B * s);
-                        acc += radial * w_t * value * ab;
+                        if (kGrad) {
+                            double g1[7], g2[7];
+                            integrand_grad(ctx, A * s, B * s * t, g1);
+                            integrand_grad(ctx, A * s * t, B * s, g2);
+                            const double f = radial * w_t * ab;
+                            acc += f * (g1[0] + g2[0]);
+                            for (int q = 0; q < 6; ++q) gacc[q] += f * (g1[1 + q] + g2[1 + q]);
+                        } else {
+                            double value = integrand(ctx, A * s, B * s * t) + integrand(ctx, A * s * t, B * s);
+                            acc += radial * w_t * value * ab;
+                        }
                     }
                 }
             }
@@ -713,12 +770,21 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
         }
         // block reduction
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-        if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
+        if ((threadIdx.x & 31) == 0) s_red[0][threadIdx.x >> 5] = acc;
+        if (kGrad) {
+            for (int q = 0; q < 6; ++q) {
+                double x = gacc[q];
+                for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+                if ((threadIdx.x & 31) == 0) s_red[kGrad ? 1 + q : 0][threadIdx.x >> 5] = x;
+            }
+        }
         __syncthreads();
         if (threadIdx.x == 0) {
-            double s = 0.0;
-            for (int w = 0; w < kQuadThreads / 32; ++w) s += s_red[w];
-            values[h] = overflow ? NAN : s;  // reported as NotFinite by the scatter
+            for (int q = 0; q < (kGrad ? 7 : 1); ++q) {
+                double s = 0.0;
+                for (int w = 0; w < kQuadThreads / 32; ++w) s += s_red[q][w];
+                values[kGrad ? 7 * h + q : h] = overflow ? NAN : s;  // reported as NotFinite by the scatter
+            }
         }
         __syncthreads();
     }
@@ -913,6 +979,262 @@ __global__ void __launch_bounds__(128) sampled_kernel(const DevFil *__restrict__
     }
 }
 
+// ---------------------------------------------------------------------------
+// Derivative fill: for every pair (a, b) the partial derivatives of L_ab with
+// respect to the width and the thickness of the segment of a (b held fixed)
+// and of the segment of b (a held fixed), evaluated with the pair's own
+// dispatch (method, Gauss orders, closed-form acceptance, panel tree).
+// Written to Dw/Dh as D[a + b n] = dL_ab / d(side a), D[b + a n] = dL_ab /
+// d(side b); on the diagonal only the first side (the second is equal by the
+// symmetry of the integral).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void store_grad(const GradOut &g, int64_t n, int a, int b, const double d[4],
+                                           DevError *e) {
+    if (!(isfinite(d[0]) && isfinite(d[1]) && isfinite(d[2]) && isfinite(d[3]))) {
+        record_error(e, a, b, FH_ERR_KERNEL_NOT_FINITE);
+        return;
+    }
+    g.Dw[(int64_t)a + (int64_t)b * n] = d[0];
+    g.Dh[(int64_t)a + (int64_t)b * n] = d[1];
+    if (a != b) {
+        g.Dw[(int64_t)b + (int64_t)a * n] = d[2];
+        g.Dh[(int64_t)b + (int64_t)a * n] = d[3];
+    }
+}
+
+// Point quadrature: the Gauss points of a move with its centre (sw, sh along
+// its width / height axes) and with its cross-section (gw, gh times the
+// point's fraction of the width / height); the weights do not move.  With
+// S = sum wp wq / |p - q| and d = p - q, dS = -sum wp wq d . (dp - dq) / |d|^3.
+__global__ void __launch_bounds__(128) point_grad_kernel(const DevFil *__restrict__ fil, const FilTan *__restrict__ tan,
+                                                         const int4 *__restrict__ items, int64_t count, GradOut g,
+                                                         int64_t n, DevError *err) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int4 it = items[t];
+        const DevFil &A = fil[it.x];
+        const DevFil &B = fil[it.y];
+        const int oa0 = it.z & 31, oa1 = (it.z >> 5) & 31, oa2 = (it.z >> 10) & 31;
+        const int ob0 = (it.z >> 15) & 31, ob1 = (it.z >> 20) & 31, ob2 = (it.z >> 25) & 31;
+        double aa[9], ba[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            aa[k] = A.axes[k];
+            ba[k] = B.axes[k];
+        }
+        const double ah0 = A.half[0], ah1 = 2.0 * A.half[1], ah2 = 2.0 * A.half[2];
+        const double bh0 = B.half[0], bh1 = 2.0 * B.half[1], bh2 = 2.0 * B.half[2];
+        // Pair totals: G = sum wp wq d / r^3, and the same weighted by a's
+        // width / height fraction (Aw, Ah) or by b's (Kw, Kh).
+        double G[3] = {0, 0, 0}, Aw[3] = {0, 0, 0}, Ah[3] = {0, 0, 0}, Kw[3] = {0, 0, 0}, Kh[3] = {0, 0, 0};
+        for (int la = 0; la < oa0; ++la) {
+            const double xl = ah0 * c_quad.nodes[oa0][la], wl = ah0 * c_quad.weights[oa0][la];
+            for (int wa = 0; wa < oa1; ++wa) {
+                const double fw = 0.5 * c_quad.nodes[oa1][wa];
+                const double xw = ah1 * fw, ww = 0.5 * c_quad.weights[oa1][wa];
+                for (int ha = 0; ha < oa2; ++ha) {
+                    const double fh = 0.5 * c_quad.nodes[oa2][ha];
+                    const double xh = ah2 * fh, wh = 0.5 * c_quad.weights[oa2][ha];
+                    double p[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) p[d] = A.centre[d] + aa[d] * xl + aa[3 + d] * xw + aa[6 + d] * xh;
+                    const double wpa = wl * ww * wh;
+                    double gi[3] = {0, 0, 0}, kw[3] = {0, 0, 0}, kh[3] = {0, 0, 0};
+                    for (int lb = 0; lb < ob0; ++lb) {
+                        const double yl = bh0 * c_quad.nodes[ob0][lb], vl = bh0 * c_quad.weights[ob0][lb];
+                        for (int wb = 0; wb < ob1; ++wb) {
+                            const double gwb = 0.5 * c_quad.nodes[ob1][wb];
+                            const double yw = bh1 * gwb;
+                            const double vlw = vl * (0.5 * c_quad.weights[ob1][wb]);
+                            double q[3];
+#pragma unroll
+                            for (int d = 0; d < 3; ++d) q[d] = p[d] - (B.centre[d] + ba[d] * yl + ba[3 + d] * yw);
+                            double sw[3] = {0, 0, 0};
+                            for (int hb = 0; hb < ob2; ++hb) {
+                                const double ghb = 0.5 * c_quad.nodes[ob2][hb];
+                                const double yh = bh2 * ghb;
+                                const double vh = 0.5 * c_quad.weights[ob2][hb];
+                                const double dx = q[0] - ba[6] * yh, dy = q[1] - ba[7] * yh, dz = q[2] - ba[8] * yh;
+                                const double ir = rsqrt(dx * dx + dy * dy + dz * dz);
+                                const double e = (vlw * vh) * ir * ir * ir;
+                                sw[0] += e * dx;
+                                sw[1] += e * dy;
+                                sw[2] += e * dz;
+                                kh[0] += e * ghb * dx;
+                                kh[1] += e * ghb * dy;
+                                kh[2] += e * ghb * dz;
+                            }
+#pragma unroll
+                            for (int d = 0; d < 3; ++d) {
+                                gi[d] += sw[d];
+                                kw[d] += gwb * sw[d];
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        G[d] += wpa * gi[d];
+                        Aw[d] += wpa * fw * gi[d];
+                        Ah[d] += wpa * fh * gi[d];
+                        Kw[d] += wpa * kw[d];
+                        Kh[d] += wpa * kh[d];
+                    }
+                }
+            }
+        }
+        const FilTan ta = tan[it.x], tb = tan[it.y];
+        const double scale = kMu0Over4Pi * ndot(A.axes, B.axes);
+        double out[4];
+        out[0] = -scale * (ta.sw * ndot(aa + 3, G) + ta.gw * ndot(aa + 3, Aw));
+        out[1] = -scale * (ta.sh * ndot(aa + 6, G) + ta.gh * ndot(aa + 6, Ah));
+        out[2] = scale * (tb.sw * ndot(ba + 3, G) + tb.gw * ndot(ba + 3, Kw));
+        out[3] = scale * (tb.sh * ndot(ba + 6, G) + tb.gh * ndot(ba + 6, Kh));
+        store_grad(g, n, it.x, it.y, out, err);
+    }
+}
+
+// Forward-mode value of the Hoer-Love primitive with two tangents (along its
+// y and z arguments); x is held fixed.
+struct D2 {
+    double v, y, z;
+};
+__device__ __forceinline__ D2 operator+(D2 a, D2 b) { return {a.v + b.v, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D2 operator-(D2 a, D2 b) { return {a.v - b.v, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D2 operator-(D2 a) { return {-a.v, -a.y, -a.z}; }
+__device__ __forceinline__ D2 operator*(D2 a, D2 b) { return {a.v * b.v, a.y * b.v + a.v * b.y, a.z * b.v + a.v * b.z}; }
+__device__ __forceinline__ D2 operator*(double s, D2 a) { return {s * a.v, s * a.y, s * a.z}; }
+__device__ __forceinline__ D2 operator/(D2 a, D2 b) {
+    const double q = a.v / b.v;
+    return {q, (a.y - q * b.y) / b.v, (a.z - q * b.z) / b.v};
+}
+__device__ __forceinline__ D2 dlog(D2 a) { return {log(a.v), a.y / a.v, a.z / a.v}; }
+__device__ __forceinline__ D2 datan(D2 a) {
+    const double s = 1.0 / (1.0 + a.v * a.v);
+    return {atan(a.v), a.y * s, a.z * s};
+}
+__device__ __forceinline__ D2 dsqrt(D2 a) {
+    const double r = sqrt(a.v);
+    return {r, 0.5 * a.y / r, 0.5 * a.z / r};
+}
+__device__ __forceinline__ bool dzero(D2 a) { return a.v == 0.0 && a.y == 0.0 && a.z == 0.0; }
+
+__device__ __forceinline__ D2 log_term_d(D2 coefficient, D2 x, D2 r, D2 rest_sq) {
+    if (dzero(coefficient)) return {0.0, 0.0, 0.0};
+    const D2 argument = x.v >= 0.0 ? x + r : rest_sq / (r - x);
+    return coefficient * x * dlog(argument);
+}
+// x y z z^2 atan(x y / (z r)) / 6 vanishes with all its first derivatives
+// wherever one of x, y, z is zero.
+__device__ __forceinline__ D2 atan_term_d(D2 x, D2 y, D2 z, D2 r) {
+    if (x.v == 0.0 || y.v == 0.0 || z.v == 0.0) return {0.0, 0.0, 0.0};
+    const D2 product = x * y * z;
+    return -((1.0 / 6.0) * (product * z * z)) * datan((x * y) / (z * r));
+}
+// The primitive is O(rho^5 log rho) at the origin, so its gradient is zero
+// there.
+__device__ D2 primitive_d(double xv, double yv, double zv) {
+    const D2 x{xv, 0.0, 0.0}, y{yv, 1.0, 0.0}, z{zv, 0.0, 1.0};
+    const D2 x2 = x * x, y2 = y * y, z2 = z * z;
+    const D2 x4 = x2 * x2, y4 = y2 * y2, z4 = z2 * z2;
+    const double rr = xv * xv + yv * yv + zv * zv;
+    if (rr == 0.0) return {0.0, 0.0, 0.0};
+    const D2 r = dsqrt(x2 + y2 + z2);
+    auto coef = [](D2 a2, D2 b2, D2 a4, D2 b4) {
+        return 0.25 * (a2 * b2) - (1.0 / 24.0) * a4 - (1.0 / 24.0) * b4;
+    };
+    D2 s = log_term_d(coef(y2, z2, y4, z4), x, r, y2 + z2);
+    s = s + log_term_d(coef(x2, z2, x4, z4), y, r, x2 + z2);
+    s = s + log_term_d(coef(x2, y2, x4, y4), z, r, x2 + y2);
+    const D2 cross = x2 * y2 + y2 * z2 + z2 * x2;
+    s = s + (1.0 / 60.0) * ((x4 + y4 + z4 - 3.0 * cross) * r);
+    s = s + atan_term_d(x, y, z, r);
+    s = s + atan_term_d(x, z, y, r);
+    s = s + atan_term_d(y, z, x, r);
+    return s;
+}
+
+// Chain rule from the partials of the aligned-bar integral V with respect to
+// (width[0], width[1], offset[1], height[0], height[1], offset[2]) to the four
+// side derivatives of L_ab = mu0/4pi sign(cos) V / (area_a area_b).  The
+// cross-section inputs follow aligned_bars: b's width is width[1] when its
+// width axis is a's, else height[1].
+__device__ __forceinline__ void aligned_chain(const DevFil &A, const DevFil &B, const FilTan &ta, const FilTan &tb,
+                                              double V, const double dV[6], double out[4]) {
+    const double *wa = A.axes + 3, *ha = A.axes + 6, *wb = B.axes + 3, *hb = B.axes + 6;
+    const bool same = fabs(ndot(wa, wb)) > 1.0 - 1e-12;
+    const double dVwA = dV[0] * ta.gw - ta.sw * (dV[2] * ndot(wa, wa) + dV[5] * ndot(wa, ha));
+    const double dVhA = dV[3] * ta.gh - ta.sh * (dV[2] * ndot(ha, wa) + dV[5] * ndot(ha, ha));
+    const double dVwB = (same ? dV[1] : dV[4]) * tb.gw + tb.sw * (dV[2] * ndot(wb, wa) + dV[5] * ndot(wb, ha));
+    const double dVhB = (same ? dV[4] : dV[1]) * tb.gh + tb.sh * (dV[2] * ndot(hb, wa) + dV[5] * ndot(hb, ha));
+    const double scale = kMu0Over4Pi * signum(ndot(A.axes, B.axes)) / (A.area * B.area);
+    out[0] = scale * (dVwA - V * ta.gw / A.width);
+    out[1] = scale * (dVhA - V * ta.gh / A.height);
+    out[2] = scale * (dVwB - V * tb.gw / B.width);
+    out[3] = scale * (dVhB - V * tb.gh / B.height);
+}
+
+// Aligned pairs: the closed form where it is accepted (its derivative by
+// forward mode through the 64 corner primitives), else queued for the
+// quadrature.
+__global__ void __launch_bounds__(128) closed_form_grad_kernel(const DevFil *__restrict__ fil,
+                                                               const FilTan *__restrict__ tan,
+                                                               const int4 *__restrict__ items, int64_t count,
+                                                               GradOut g, int64_t n, int4 *__restrict__ quad_items,
+                                                               unsigned long long *__restrict__ quad_count,
+                                                               DevError *err) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int4 it = items[t];
+        const DevFil &A = fil[it.x];
+        const DevFil &B = fil[it.y];
+        Aligned ab;
+        aligned_bars(A, B, &ab);
+        double v, rel;
+        bar_integral(ab, &v, &rel);
+        if (!(rel <= kClosedFormMaxError)) {
+            unsigned long long k = atomicAdd(quad_count, 1ull);
+            quad_items[k] = it;
+            continue;
+        }
+        double qx[4], qy[4], qz[4];
+        corner_differences(ab.length[0], ab.length[1], ab.offset[0], qx);
+        corner_differences(ab.width[0], ab.width[1], ab.offset[1], qy);
+        corner_differences(ab.height[0], ab.height[1], ab.offset[2], qz);
+        const double signs[4] = {1.0, -1.0, -1.0, 1.0};
+        double py[4] = {0, 0, 0, 0}, pz[4] = {0, 0, 0, 0};
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j)
+                for (int k = 0; k < 4; ++k) {
+                    const D2 f = primitive_d(qx[i], qy[j], qz[k]);
+                    const double s = signs[i] * signs[j] * signs[k];
+                    py[j] += s * f.y;
+                    pz[k] += s * f.z;
+                }
+        // q[0] = o + (e1 + e2)/2, q[1] = o + (e1 - e2)/2, q[2] = o - (e1 - e2)/2, q[3] = o - (e1 + e2)/2
+        const double dV[6] = {0.5 * (py[0] + py[1] - py[2] - py[3]), 0.5 * (py[0] - py[1] + py[2] - py[3]),
+                              py[0] + py[1] + py[2] + py[3],         0.5 * (pz[0] + pz[1] - pz[2] - pz[3]),
+                              0.5 * (pz[0] - pz[1] + pz[2] - pz[3]), pz[0] + pz[1] + pz[2] + pz[3]};
+        double out[4];
+        aligned_chain(A, B, tan[it.x], tan[it.y], v, dV, out);
+        store_grad(g, n, it.x, it.y, out, err);
+    }
+}
+
+// Quadrature pairs: the key's integral and partials, then the chain rule.
+__global__ void aligned_grad_scatter_kernel(const DevFil *__restrict__ fil, const FilTan *__restrict__ tan,
+                                            const int4 *__restrict__ items, const int64_t *__restrict__ head_of,
+                                            const double *__restrict__ head_value, int64_t count, GradOut g,
+                                            int64_t n, DevError *err) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int4 it = items[t];
+        const double *hv = head_value + 7 * head_of[t];
+        double out[4];
+        aligned_chain(fil[it.x], fil[it.y], tan[it.x], tan[it.y], hv[0], hv + 1, out);
+        store_grad(g, n, it.x, it.y, out, err);
+    }
+}
+
 // Upper-triangle congruence tile with mirrored store (solve.rs:1172-1200).
 // Entry (i, j), i <= j:  sum over (b, s_b) in row j of s_b * sum over (a, s_a)
 // in row i of s_a * B[b, a].  B is symmetric so B[b, a] is read as B[a + b n]
@@ -990,8 +1312,10 @@ namespace {
 // into d_L (mirrored); with a pair list it evaluates those pairs into
 // d_L[k] (pair-list mode: orthogonal pairs are zero).
 fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t n_pairs, double *d_L,
-                   int8_t *d_methods, cudaStream_t stream, FillStats *stats, fh_error_info *err) {
+                   int8_t *d_methods, cudaStream_t stream, FillStats *stats, fh_error_info *err,
+                   const FilTan *d_tan = nullptr, const GradOut *grad = nullptr) {
     const bool list = d_pairs != nullptr;
+    if (grad && list) return fail(err, FH_ERR_INVALID_ARGUMENT, "the derivative fill has no pair-list mode");
     if (list ? n_pairs == 0 : n == 0) return FH_OK;
     if (n > 2000000000LL / 32) return fail(err, FH_ERR_INVALID_ARGUMENT, "too many filaments for the fill");
     if (list && n_pairs > INT32_MAX) return fail(err, FH_ERR_INVALID_ARGUMENT, "too many pairs for one list fill");
@@ -1069,7 +1393,10 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
     for (int c = 0; c < kPointBuckets; ++c) st.point_evaluations += (double)counts[c] * (1.5 * (double)(1ull << c));
     if (n_point) {
         int blocks = (int)std::min<int64_t>((n_point + 127) / 128, (int64_t)sms * 64);
-        point_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_items, n_point, d_L, d_methods, n_arg, d_err);
+        if (grad)
+            point_grad_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_tan, d_items, n_point, *grad, n, d_err);
+        else
+            point_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_items, n_point, d_L, d_methods, n_arg, d_err);
         FHB_CUDA(cudaGetLastError());
     }
     FHB_CUDA(cudaEventRecord(ev[2], stream));
@@ -1083,8 +1410,12 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
     if (n_aligned) {
         FHB_CUDA(alloc((void **)&d_quad, sizeof(int4) * n_aligned));
         int blocks = (int)std::min<int64_t>((n_aligned + 127) / 128, (int64_t)sms * 32);
-        closed_form_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_aligned, n_aligned, d_L, d_methods, n_arg, d_quad,
-                                                       d_qcount, d_err);
+        if (grad)
+            closed_form_grad_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_tan, d_aligned, n_aligned, *grad, n, d_quad,
+                                                                d_qcount, d_err);
+        else
+            closed_form_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_aligned, n_aligned, d_L, d_methods, n_arg, d_quad,
+                                                           d_qcount, d_err);
         FHB_CUDA(cudaGetLastError());
         unsigned long long q = 0;
         FHB_CUDA(cudaMemcpyAsync(&q, d_qcount, sizeof q, cudaMemcpyDeviceToHost, stream));
@@ -1141,19 +1472,33 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
         double *d_values;
         FHB_CUDA(alloc((void **)&d_heads, 8 * n_heads));
         FHB_CUDA(alloc((void **)&d_item_head, 8 * n_quad));
-        FHB_CUDA(alloc((void **)&d_values, 8 * n_heads));
+        FHB_CUDA(alloc((void **)&d_values, (grad ? 56 : 8) * n_heads));
         FHB_CUDA(cudaMemcpyAsync(d_heads, head_item.data(), 8 * n_heads, cudaMemcpyHostToDevice, stream));
         FHB_CUDA(cudaMemcpyAsync(d_item_head, item_head.data(), 8 * n_quad, cudaMemcpyHostToDevice, stream));
         int qblocks = (int)std::min<int64_t>(n_heads, (int64_t)sms * 16);
-        aligned_quadrature_kernel<<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads, d_values);
-        FHB_CUDA(cudaGetLastError());
-        aligned_scatter_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_quad, d_item_head, d_values, n_quad, d_L,
-                                                           d_methods, n_arg, d_err);
+        if (grad) {
+            aligned_quadrature_kernel<true><<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads,
+                                                                                 d_values);
+            FHB_CUDA(cudaGetLastError());
+            aligned_grad_scatter_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_tan, d_quad, d_item_head, d_values, n_quad,
+                                                                    *grad, n, d_err);
+        } else {
+            aligned_quadrature_kernel<false><<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads,
+                                                                                  d_values);
+            FHB_CUDA(cudaGetLastError());
+            aligned_scatter_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_quad, d_item_head, d_values, n_quad, d_L,
+                                                               d_methods, n_arg, d_err);
+        }
         FHB_CUDA(cudaGetLastError());
     }
     FHB_CUDA(cudaEventRecord(ev[4], stream));
     const int64_t n_sampled = (int64_t)counts[kCatSampled];
     st.sampled = n_sampled;
+    if (n_sampled && grad)
+        return fail(err, FH_ERR_UNSUPPORTED,
+                    std::to_string(n_sampled) +
+                        " filament pairs are evaluated by sampled filaments (parallel bars with rotated "
+                        "cross-sections, or skew bars); their derivatives are not provided");
     if (n_sampled) {
         int blocks = (int)std::min<int64_t>((n_sampled * 32 + 127) / 128, (int64_t)sms * 32);
         sampled_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_items + offsets[kCatSampled], n_sampled, d_L, d_methods,
@@ -1195,6 +1540,12 @@ fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_met
 fh_status device_fill_pairs(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t n_pairs, double *d_out,
                             cudaStream_t stream, FillStats *stats, fh_error_info *err) {
     return fill_run(d_fil, n, d_pairs, n_pairs, d_out, nullptr, stream, stats, err);
+}
+
+fh_status device_fill_grad(const DevFil *d_fil, const FilTan *d_tan, int64_t n, GradOut out, cudaStream_t stream,
+                           FillStats *stats, fh_error_info *err) {
+    if (!d_tan || !out.Dw || !out.Dh) return fail(err, FH_ERR_INVALID_ARGUMENT, "null derivative-fill argument");
+    return fill_run(d_fil, n, nullptr, 0, nullptr, nullptr, stream, stats, err, d_tan, &out);
 }
 
 fh_status device_congruence(const double *d_L, const double *d_R, int64_t n, const int64_t *d_row_ptr,

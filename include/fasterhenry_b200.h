@@ -294,6 +294,53 @@ fh_status fh_batch_sweep(fh_system *const *systems, size_t k, const double *cons
 fh_status fh_impedance(fh_system *sys, double frequency_hz, fh_precision precision, double *z_out,
                        fh_error_info *err);
 
+/* ---- impedance gradient (no reference counterpart) --------------------- */
+
+/* A geometric parameter: the width or the thickness of segment `index`, or a
+ * coordinate of node `index` (node coordinates are not provided: moving a
+ * node rotates the segments that meet there, and the derivative of the
+ * integrals under a rotation is not built; FH_ERR_UNSUPPORTED). */
+typedef enum fh_param_kind {
+    FH_PARAM_WIDTH = 0,
+    FH_PARAM_THICKNESS = 1,
+    FH_PARAM_NODE_X = 2,
+    FH_PARAM_NODE_Y = 3,
+    FH_PARAM_NODE_Z = 4
+} fh_param_kind;
+
+typedef struct fh_param_spec {
+    int32_t kind; /* fh_param_kind */
+    int32_t reserved;
+    int64_t index;
+} fh_param_spec;
+
+typedef struct fh_gradient_report {
+    double solve_s;           /* FP64 factorization and solve for the loop currents */
+    double derivative_fill_s; /* device time of the derivative fill */
+    double contract_s;        /* device time of the products with the branch currents */
+    double total_s;           /* wall time of the call */
+    int64_t pairs;            /* filament pairs differentiated (upper triangle) */
+} fh_gradient_report;
+
+/* dZ/dp at one frequency for np parameters, by the stationary (adjoint) form
+ * dZ_ab/dp = I_a^T (dR/dp + j w dL/dp) I_b with the branch currents I of unit
+ * port currents: one FP64 solve, one derivative fill of all filament pairs,
+ * one product per derivative matrix.  Derivatives are those of the
+ * evaluation as dispatched at the nominal geometry (method, Gauss orders,
+ * closed-form acceptance, quadrature panels, and the discretization's
+ * filament counts and grading held fixed).  z_out (optional): p x p Z;
+ * dz_out: np x p x p complex (interleaved), row-major per parameter, in ohm
+ * per metre.  report optional. */
+fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *params, size_t np, double *z_out,
+                      double *dz_out, fh_gradient_report *report, fh_error_info *err);
+
+/* Test hook: the derivative fill of a filament set.  tangents: n x 4 (sw, sh,
+ * gw, gh per filament: d centre / d w = sw * width axis, d width / d w = gw,
+ * and the same for the thickness); Dw, Dh: n x n column-major with
+ * D[a + b n] = dL_ab / d(side a). */
+fh_status fh_test_inductance_gradient(const fh_filament *filaments, const double *tangents, size_t n, double *Dw,
+                                      double *Dh, fh_error_info *err);
+
 /* Fill statistics of an assembled system: pairs per method and device time
  * per fill kernel (no reference counterpart; diagnostics). */
 typedef struct fh_fill_stats {

@@ -736,6 +736,207 @@ int evaluate(const Fil &a0, const Fil &b0, double *out, int *method_out, bool *r
 }
 
 // ---------------------------------------------------------------------------
+// Frozen-dispatch evaluation, for finite-difference checks of the impedance
+// gradient (no reference counterpart).  Every decision the reference's
+// evaluate() takes (inductance/mod.rs:303-369: orthogonality, alignment,
+// Gauss orders, point quadrature vs aligned path, closed-form acceptance,
+// and the aligned quadrature's break points and panel tree, aligned.rs:
+// 86-232) is taken on the nominal pair and replayed on the perturbed pair,
+// so that a central difference sees the evaluation as one smooth function.
+// ---------------------------------------------------------------------------
+// Break points with the formula that produced each (aligned.rs:86-120):
+// 0 offset-sum, 1 offset-diff, 2 offset+diff, 3 offset+sum, 4 zero.
+std::vector<int> break_tags(double e1, double e2, double offset) {
+    double sum = 0.5 * (e1 + e2), diff = 0.5 * std::fabs(e1 - e2);
+    auto snap = [&](double x) { return std::fabs(x) <= kSnap * sum ? 0.0 : x; };
+    double raw[4] = {offset - sum, offset - diff, offset + diff, offset + sum};
+    std::vector<std::pair<double, int>> p;
+    for (int k = 0; k < 4; ++k) {
+        double v = snap(raw[k]);
+        p.push_back({v, v == 0.0 ? 4 : k});
+    }
+    if (p[0].first < 0.0 && p[3].first > 0.0) p.push_back({0.0, 4});
+    std::stable_sort(p.begin(), p.end(), [](const std::pair<double, int> &a, const std::pair<double, int> &b) {
+        if (a.first == b.first) return std::signbit(a.first) && !std::signbit(b.first);
+        return a.first < b.first;
+    });
+    std::vector<int> out;
+    double last = 0.0;
+    for (size_t k = 0; k < p.size(); ++k)
+        if (out.empty() || !(last == p[k].first)) {
+            out.push_back(p[k].second);
+            last = p[k].first;
+        }
+    return out;
+}
+double break_value(int tag, double e1, double e2, double offset) {
+    double sum = 0.5 * (e1 + e2), diff = 0.5 * std::fabs(e1 - e2);
+    switch (tag) {
+        case 0: return offset - sum;
+        case 1: return offset - diff;
+        case 2: return offset + diff;
+        case 3: return offset + sum;
+        default: return 0.0;
+    }
+}
+
+// Panel decisions (aligned.rs:153-200) as codes: 0 empty, 1 direct, 2/3
+// split u/v at the midpoint, 16 + 8 axis + 4 negative + source for a split
+// toward zero at +-target (source 0 su, 1 sv, 2 axial scale), 32 + 2 fu + fv
+// for a corner (fu: the far u is u1, else u0).
+struct FrozenIntegrator {
+    Integrator in;
+    std::vector<unsigned char> *log;
+    size_t cursor = 0;
+
+    double panel(double u0, double u1, double v0, double v1, unsigned depth, bool record) {
+        double su = u1 - u0, sv = v1 - v0;
+        unsigned char code;
+        if (record) {
+            if (su <= 0.0 || sv <= 0.0) {
+                code = 0;
+            } else {
+                auto gap = [](double r0, double r1) { return r0 > 0.0 ? r0 : (r1 < 0.0 ? -r1 : 0.0); };
+                double distance = std::hypot(gap(u0, u1), gap(v0, v1));
+                double size = rmax(su, sv);
+                if (depth >= 200) {
+                    code = 1;
+                } else if (distance > 0.0) {
+                    code = size <= distance ? 1 : (su >= sv ? 2 : 3);
+                } else {
+                    int src = 0;
+                    double target = su;
+                    if (sv < target) target = sv, src = 1;
+                    if (in.axial_scale < target) target = in.axial_scale, src = 2;
+                    if (su > 2.0 * target)
+                        code = (unsigned char)(16 + (u0 == 0.0 ? 0 : 4) + src);
+                    else if (sv > 2.0 * target)
+                        code = (unsigned char)(24 + (v0 == 0.0 ? 0 : 4) + src);
+                    else
+                        code = (unsigned char)(32 + (u0 == 0.0 ? 2 : 0) + (v0 == 0.0 ? 1 : 0));
+                }
+            }
+            log->push_back(code);
+        } else {
+            code = (*log)[cursor++];
+        }
+        if (code == 0) return 0.0;
+        if (code == 1) return in.direct(u0, u1, v0, v1);
+        if (code == 2) {
+            double at = 0.5 * (u0 + u1);
+            double a = panel(u0, at, v0, v1, depth + 1, record);
+            return a + panel(at, u1, v0, v1, depth + 1, record);
+        }
+        if (code == 3) {
+            double at = 0.5 * (v0 + v1);
+            double a = panel(u0, u1, v0, at, depth + 1, record);
+            return a + panel(u0, u1, at, v1, depth + 1, record);
+        }
+        if (code >= 32) {
+            double fu = (code & 2) ? u1 : u0, fv = (code & 1) ? v1 : v0;
+            return in.corner(fu, fv);
+        }
+        const int src = code & 3;
+        const double target = src == 0 ? su : (src == 1 ? sv : in.axial_scale);
+        const double at_len = (code & 4) ? -target : target;
+        if (code < 24) {
+            double a = panel(u0, at_len, v0, v1, depth + 1, record);
+            return a + panel(at_len, u1, v0, v1, depth + 1, record);
+        }
+        double a = panel(u0, u1, v0, at_len, depth + 1, record);
+        return a + panel(u0, u1, at_len, v1, depth + 1, record);
+    }
+};
+
+double frozen_quadrature(const AlignedBars &nom, const AlignedBars &per) {
+    auto setup = [](const AlignedBars &b, Integrator &in) {
+        double axial_start = b.offset[0] + 0.5 * (b.length[0] - b.length[1]);
+        double l1 = b.length[0], l2 = b.length[1];
+        double separations[4] = {axial_start + l2, axial_start, axial_start + l2 - l1, axial_start - l1};
+        double largest = 0.0;
+        for (double q : separations) largest = rmax(largest, std::fabs(q));
+        double axial_scale = std::numeric_limits<double>::infinity();
+        for (double q : separations)
+            if (std::fabs(q) > 1e-9 * largest) axial_scale = rmin(axial_scale, std::fabs(q));
+        in = Integrator{&b, axial_start, axial_scale};
+    };
+    std::vector<unsigned char> log;
+    FrozenIntegrator rec, rep;
+    setup(nom, rec.in);
+    setup(per, rep.in);
+    rec.log = rep.log = &log;
+    std::vector<int> tu = break_tags(nom.width[0], nom.width[1], nom.offset[1]);
+    std::vector<int> tv = break_tags(nom.height[0], nom.height[1], nom.offset[2]);
+    double sum = 0.0;
+    for (size_t a = 0; a + 1 < tu.size(); ++a)
+        for (size_t b = 0; b + 1 < tv.size(); ++b) {
+            rec.panel(break_value(tu[a], nom.width[0], nom.width[1], nom.offset[1]),
+                      break_value(tu[a + 1], nom.width[0], nom.width[1], nom.offset[1]),
+                      break_value(tv[b], nom.height[0], nom.height[1], nom.offset[2]),
+                      break_value(tv[b + 1], nom.height[0], nom.height[1], nom.offset[2]), 0, true);
+            sum += rep.panel(break_value(tu[a], per.width[0], per.width[1], per.offset[1]),
+                             break_value(tu[a + 1], per.width[0], per.width[1], per.offset[1]),
+                             break_value(tv[b], per.height[0], per.height[1], per.offset[2]),
+                             break_value(tv[b + 1], per.height[0], per.height[1], per.offset[2]), 0, false);
+        }
+    return sum;
+}
+
+// evaluate() with its decisions taken on (na, nb) and its arithmetic on
+// (pa, pb).  Sampled-filament pairs are not covered (ORC_ERR_ARGUMENT).
+int evaluate_frozen(const Fil &na0, const Fil &nb0, const Fil &pa0, const Fil &pb0, double *out) {
+    const bool swap = canonical(na0, nb0) > 0;
+    const Fil &na = swap ? nb0 : na0, &nb = swap ? na0 : nb0;
+    const Fil &pa = swap ? pb0 : pa0, &pb = swap ? pa0 : pb0;
+    double cosv = dot(na.l, nb.l);
+    if (std::fabs(cosv) < kOrthogonalCos) {
+        *out = 0.0;
+        return ORC_OK;
+    }
+    Bar ba = make_bar(na), bb = make_bar(nb);
+    bool parallel = norm(cross(na.l, nb.l)) < kParallelSin;
+    AlignedBars ab;
+    bool aligned = parallel && aligned_bars(ba, bb, &ab);
+    double gap = separation(ba, bb);
+    int oa[3], ob[3];
+    bool have = point_orders(ba, gap, oa) && point_orders(bb, gap, ob);
+    if (have && aligned) {
+        size_t pairs = (size_t)(oa[0] * oa[1] * oa[2]) * (size_t)(ob[0] * ob[1] * ob[2]);
+        if (pairs > kCheapPointPairs) have = false;
+    }
+    Bar qa = make_bar(pa), qb = make_bar(pb);
+    double integral;
+    if (have) {
+        integral = point_sum(qa, oa, qb, ob) * dot(pa.l, pb.l);
+    } else if (aligned) {
+        AlignedBars pab;
+        if (!aligned_bars(qa, qb, &pab)) return ORC_ERR_ARGUMENT;
+        double qx[4], qy[4], qz[4], value, rel;
+        corner_differences(ab.length[0], ab.length[1], ab.offset[0], qx);
+        corner_differences(ab.width[0], ab.width[1], ab.offset[1], qy);
+        corner_differences(ab.height[0], ab.height[1], ab.offset[2], qz);
+        bar_integral(qx, qy, qz, &value, &rel);
+        double v;
+        if (rel <= kClosedFormMaxError) {
+            corner_differences(pab.length[0], pab.length[1], pab.offset[0], qx);
+            corner_differences(pab.width[0], pab.width[1], pab.offset[1], qy);
+            corner_differences(pab.height[0], pab.height[1], pab.offset[2], qz);
+            bar_integral(qx, qy, qz, &v, &rel);
+        } else {
+            v = frozen_quadrature(ab, pab);
+        }
+        double scale = signum(dot(pa.l, pb.l)) / (area_of(pa) * area_of(pb));
+        integral = v * scale;
+    } else {
+        return ORC_ERR_ARGUMENT;
+    }
+    double value = kMu0Over4Pi * integral;
+    if (!std::isfinite(value)) return ORC_ERR_NOT_FINITE;
+    *out = value;
+    return ORC_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Geometry, discretization, grading (geometry.rs:223-275, filament.rs:227-553,
 // filament/grading.rs, solve.rs:388-510)
 // ---------------------------------------------------------------------------
@@ -1353,6 +1554,51 @@ int orc_fill(const double *filaments, long long n, double *L, signed char *metho
     std::vector<Fil> f((size_t)n);
     for (long long i = 0; i < n; ++i) f[i] = load_fil(filaments + 19 * i);
     return fill_matrix(f, L, methods, threads, ei, ej);
+}
+
+int orc_fill_frozen(const double *nominal, const double *perturbed, long long n, double *L, int threads) {
+    std::vector<Fil> fn((size_t)n), fp((size_t)n);
+    for (long long i = 0; i < n; ++i) {
+        fn[i] = load_fil(nominal + 19 * i);
+        fp[i] = load_fil(perturbed + 19 * i);
+    }
+    int status = ORC_OK;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+    for (long long i = 0; i < n; ++i) {
+        for (long long j = i; j < n; ++j) {
+            double v = NAN;
+            int st = evaluate_frozen(fn[i], fn[j], fp[i], fp[j], &v);
+            if (st) {
+#pragma omp critical
+                status = st;
+            }
+            L[i + j * n] = v;
+            L[j + i * n] = v;
+        }
+    }
+    return status;
+}
+
+int orc_fill_frozen_rows(const double *nominal, const double *perturbed, long long n, const long long *rows,
+                         long long nrows, double *out, int threads) {
+    std::vector<Fil> fn((size_t)n), fp((size_t)n);
+    for (long long i = 0; i < n; ++i) {
+        fn[i] = load_fil(nominal + 19 * i);
+        fp[i] = load_fil(perturbed + 19 * i);
+    }
+    int status = ORC_OK;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads)
+    for (long long t = 0; t < nrows * n; ++t) {
+        const long long r = rows[t / n], j = t % n;
+        double v = NAN;
+        int st = evaluate_frozen(fn[r], fn[j], fp[r], fp[j], &v);
+        if (st) {
+#pragma omp critical
+            status = st;
+        }
+        out[t] = v;
+    }
+    return status;
 }
 
 int orc_lu_solve(double *a, long long n, double *b, long long nrhs, int threads) {

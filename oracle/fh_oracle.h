@@ -91,6 +91,16 @@ double orc_separation(const double *fa, const double *fb);
 int orc_fill(const double *filaments, long long n, double *L, signed char *methods, int threads,
              long long *err_i, long long *err_j);
 
+/* The fill with every dispatch decision (method, orders, closed-form
+ * acceptance, aligned-quadrature break points and panel tree) taken on
+ * `nominal` and the arithmetic done on `perturbed` (same count and order):
+ * the frozen-dispatch evaluation that finite-difference checks of the
+ * impedance gradient differentiate.  Sampled-filament pairs: ORC_ERR_ARGUMENT. */
+int orc_fill_frozen(const double *nominal, const double *perturbed, long long n, double *L, int threads);
+/* The same for rows[0..nrows) of the matrix: out[r * n + j] = L(rows[r], j). */
+int orc_fill_frozen_rows(const double *nominal, const double *perturbed, long long n, const long long *rows,
+                         long long nrows, double *out, int threads);
+
 /* Solve a (n x n, complex interleaved, column-major) x = b in place (b: n x nrhs).
  * Returns ORC_ERR_SINGULAR on an exactly zero pivot. */
 int orc_lu_solve(double *a, long long n, double *b, long long nrhs, int threads);

@@ -78,6 +78,8 @@ def lib():
         L.orc_separation.restype = ctypes.c_double
         L.orc_fill.argtypes = [dp, ctypes.c_longlong, dp, ctypes.POINTER(ctypes.c_byte), ctypes.c_int, lp, lp]
         L.orc_lu_solve.argtypes = [dp, ctypes.c_longlong, dp, ctypes.c_longlong, ctypes.c_int]
+        L.orc_fill_frozen.argtypes = [dp, dp, ctypes.c_longlong, dp, ctypes.c_int]
+        L.orc_fill_frozen_rows.argtypes = [dp, dp, ctypes.c_longlong, lp, ctypes.c_longlong, dp, ctypes.c_int]
         L.orc_system_assemble.argtypes = [dp, ctypes.c_longlong, ctypes.POINTER(Segment), ctypes.c_longlong,
                                           lp, ctypes.c_longlong, ctypes.POINTER(Discretization),
                                           ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), dp]
@@ -245,6 +247,32 @@ def fill(filaments: np.ndarray, threads: Optional[int] = None, methods: bool = F
                         threads or default_threads(), ctypes.byref(ei), ctypes.byref(ej))
     _check(st, "fill")
     return (Lm, meth) if methods else Lm
+
+
+def fill_frozen(nominal: np.ndarray, perturbed: np.ndarray, threads: Optional[int] = None) -> np.ndarray:
+    """L of ``perturbed`` with every dispatch decision taken on ``nominal``
+    (the evaluation that finite differences of the gradient differentiate)."""
+    a = np.ascontiguousarray(nominal, dtype=np.float64)
+    b = np.ascontiguousarray(perturbed, dtype=np.float64)
+    assert a.shape == b.shape
+    n = len(a)
+    Lm = np.zeros((n, n), order="F")
+    _check(lib().orc_fill_frozen(_dp(a), _dp(b), n, Lm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                 threads or default_threads()), "fill_frozen")
+    return Lm
+
+
+def fill_frozen_rows(nominal: np.ndarray, perturbed: np.ndarray, rows: Sequence[int],
+                     threads: Optional[int] = None) -> np.ndarray:
+    """Rows of fill_frozen: out[r, j] = L(rows[r], j)."""
+    a = np.ascontiguousarray(nominal, dtype=np.float64)
+    b = np.ascontiguousarray(perturbed, dtype=np.float64)
+    r = np.ascontiguousarray(rows, dtype=np.int64)
+    n = len(a)
+    out = np.zeros((len(r), n))
+    _check(lib().orc_fill_frozen_rows(_dp(a), _dp(b), n, _lp(r), len(r), _dp(out), threads or default_threads()),
+           "fill_frozen_rows")
+    return out
 
 
 def lu_solve(a: np.ndarray, b: np.ndarray, threads: Optional[int] = None) -> np.ndarray:

@@ -127,7 +127,7 @@ EXPORTS = [
     "fh_profile_read", "fh_pfft_default_params", "fh_pfft_create", "fh_pfft_apply", "fh_pfft_get_stats",
     "fh_pfft_destroy", "fh_gmres_default_params", "fh_iterative_create", "fh_iterative_counts", "fh_iterative_timing",
     "fh_iterative_pfft_stats", "fh_iterative_sweep", "fh_iterative_destroy", "fh_test_gmres_dense",
-    "fh_batch_sweep", "fh_gradient", "fh_test_inductance_gradient",
+    "fh_batch_sweep", "fh_gradient", "fh_test_inductance_gradient", "fh_release_cached_memory",
 ]
 
 PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner",

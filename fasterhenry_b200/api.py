@@ -907,6 +907,12 @@ def build_info() -> str:
     return N.load().fh_build_info().decode()
 
 
+def release_cached_memory() -> None:
+    """Hands the device memory that finished systems left in the library's
+    cache back to the driver (fh_release_cached_memory)."""
+    _check(N.load().fh_release_cached_memory())
+
+
 def fill_stats(system: "MeshSystem") -> Dict[str, float]:
     """Pairs per method and device time per fill kernel of an assembled system."""
     s = N.FillStats()

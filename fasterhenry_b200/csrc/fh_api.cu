@@ -25,10 +25,11 @@ using namespace fhb;
 // sweep after the first.
 struct DevPool {
     std::vector<std::pair<void *, size_t>> slot;
+    cudaStream_t stream = nullptr;  // the owner's stream: allocations and frees are ordered on it
     ~DevPool() { release(); }
     void release() {
         for (auto &b : slot)
-            if (b.first) cudaFree(b.first);
+            if (b.first) cache_free(b.first, stream);
         slot.clear();
     }
     size_t held() const {
@@ -40,9 +41,9 @@ struct DevPool {
         if ((int)slot.size() <= id) slot.resize((size_t)id + 1, {nullptr, 0});
         auto &b = slot[(size_t)id];
         if (b.second < bytes) {
-            if (b.first) cudaFree(b.first);
+            if (b.first) cache_free(b.first, stream);
             b = {nullptr, 0};
-            const cudaError_t e = cudaMalloc(&b.first, std::max<size_t>(bytes, 1));
+            const cudaError_t e = cache_alloc(&b.first, std::max<size_t>(bytes, 1), stream);
             if (e != cudaSuccess) {
                 b.first = nullptr;
                 return e;
@@ -75,8 +76,8 @@ struct fh_system {
     float ms_congruence = 0;
     ~fh_system() {
         pool.release();
-        if (d_Lm) cudaFree(d_Lm);
-        if (d_Rm) cudaFree(d_Rm);
+        cache_free(d_Lm, stream);
+        cache_free(d_Rm, stream);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -102,19 +103,26 @@ fh_status ensure_device(fh_error_info *err) {
 
 namespace {
 
-// RAII device buffer.
+// RAII device buffer.  With a stream, allocated from the memory cache and
+// freed in that stream's order; without, plain cudaMalloc / cudaFree.
 template <class T>
 struct DBuf {
     T *p = nullptr;
     size_t n = 0;
+    cudaStream_t s = nullptr;
+    bool cached = false;
     DBuf() = default;
+    explicit DBuf(cudaStream_t stream) : s(stream), cached(true) {}
     DBuf(const DBuf &) = delete;
     ~DBuf() {
-        if (p) cudaFree(p);
+        if (!p) return;
+        if (cached) cache_free(p, s);
+        else cudaFree(p);
     }
     cudaError_t alloc(size_t count) {
         n = count;
-        return cudaMalloc((void **)&p, std::max<size_t>(1, count) * sizeof(T));
+        const size_t bytes = std::max<size_t>(1, count) * sizeof(T);
+        return cached ? cache_alloc((void **)&p, bytes, s) : cudaMalloc((void **)&p, bytes);
     }
 };
 
@@ -604,6 +612,7 @@ fh_status fh_system_create(const fh_node *nodes, size_t n_nodes, const fh_segmen
     FHB_CUDA(cudaGetDevice(&s->device));
     FHB_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     cudaStream_t cs = s->stream;
+    s->pool.stream = cs;
     s->nloops = s->loops.rows();
     s->m = s->loops.internal;
     s->p = s->nloops - s->m;
@@ -612,18 +621,18 @@ fh_status fh_system_create(const fh_node *nodes, size_t n_nodes, const fh_segmen
     const int64_t n = s->n, loops = s->nloops;
     std::vector<DevFil> h(n);
     for (int64_t i = 0; i < n; ++i) h[i] = make_devfil(s->disc.filaments[i]);
-    DBuf<DevFil> d_fil;
-    DBuf<double> d_L, d_R, d_sign;
-    DBuf<int64_t> d_rp;
-    DBuf<int32_t> d_br;
+    DBuf<DevFil> d_fil(cs);
+    DBuf<double> d_L(cs), d_R(cs), d_sign(cs);
+    DBuf<int64_t> d_rp(cs);
+    DBuf<int32_t> d_br(cs);
     FHB_ALLOC(d_fil, (size_t)n);
     FHB_ALLOC(d_L, (size_t)n * n);
     FHB_ALLOC(d_R, (size_t)n);
     FHB_ALLOC(d_rp, s->loops.row_ptr.size());
     FHB_ALLOC(d_br, s->loops.branch.size());
     FHB_ALLOC(d_sign, s->loops.sign.size());
-    if (cudaMalloc(&s->d_Lm, std::max<size_t>(1, (size_t)loops * loops) * 8) != cudaSuccess ||
-        cudaMalloc(&s->d_Rm, std::max<size_t>(1, (size_t)loops * loops) * 8) != cudaSuccess) {
+    if (cache_alloc((void **)&s->d_Lm, std::max<size_t>(1, (size_t)loops * loops) * 8, cs) != cudaSuccess ||
+        cache_alloc((void **)&s->d_Rm, std::max<size_t>(1, (size_t)loops * loops) * 8, cs) != cudaSuccess) {
         cudaGetLastError();
         return fail(err, FH_ERR_OUT_OF_MEMORY, "device allocation of the mesh matrices failed");
     }
@@ -642,7 +651,8 @@ fh_status fh_system_create(const fh_node *nodes, size_t n_nodes, const fh_segmen
     cudaEventCreate(&c0);
     cudaEventCreate(&c1);
     cudaEventRecord(c0, cs);
-    st = device_congruence(d_L.p, d_R.p, n, d_rp.p, d_br.p, d_sign.p, loops, s->d_Lm, s->d_Rm, cs, err);
+    st = device_congruence(d_L.p, d_R.p, n, d_rp.p, d_br.p, d_sign.p, loops, s->loops.row_ptr.data(), s->d_Lm,
+                           s->d_Rm, cs, err);
     cudaEventRecord(c1, cs);
     if (st) return st;
     FHB_CUDA(cudaStreamSynchronize(cs));
@@ -742,7 +752,8 @@ fh_status fh_sweep(fh_system *sys, const double *freqs, size_t nf, fh_precision 
     // reference's 2 GiB sweep budget, solve.rs:91 and 884).
     size_t free_b = 0, total_b = 0;
     FHB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    free_b = free_b / (size_t)std::max(1, sys->share) + sys->pool.held();  // own workspace is reused
+    // Own workspace is reused; memory the cache holds idle is available too.
+    free_b = (free_b + cache_idle_bytes()) / (size_t)std::max(1, sys->share) + sys->pool.held();
     if (precision < FH_PRECISION_FP64 || precision > FH_PRECISION_MIXED_FP32)
         return fail(err, FH_ERR_INVALID_ARGUMENT, "unknown precision");
     const bool mixed = precision != FH_PRECISION_FP64;
@@ -999,9 +1010,9 @@ fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *
                         " bytes of device memory; " + std::to_string(free_b) + " are free");
     std::vector<DevFil> h((size_t)n);
     for (int64_t i = 0; i < n; ++i) h[(size_t)i] = make_devfil(sys->disc.filaments[(size_t)i]);
-    DBuf<DevFil> d_fil;
-    DBuf<FilTan> d_tan;
-    DBuf<double> d_D, d_I, d_y, d_part;
+    DBuf<DevFil> d_fil(st);
+    DBuf<FilTan> d_tan(st);
+    DBuf<double> d_D(st), d_I(st), d_y(st), d_part(st);
     FHB_ALLOC(d_fil, (size_t)n);
     FHB_ALLOC(d_tan, (size_t)n);
     FHB_ALLOC(d_D, (size_t)(2 * n * n));

@@ -48,6 +48,14 @@ void host_quad_tables(QuadTables &t);
 
 fh_status ensure_device(fh_error_info *err);
 
+// Process-wide cache of device memory (fh_mem.cu): stream-ordered
+// allocations from a per-device pool that keeps freed memory for reuse.
+cudaError_t cache_alloc(void **p, size_t bytes, cudaStream_t s);
+void cache_free(void *p, cudaStream_t s);
+// Memory held by the cache and not in use (counted as available when sizing
+// sweep batches).
+size_t cache_idle_bytes();
+
 // Device-event profiler of kernel classes (enabled through fh_profile_enable).
 // prof_begin/prof_end bracket one launch on `s`; `work` is its algorithmic
 // flop (or byte) count.
@@ -104,8 +112,9 @@ size_t gradient_part_elems(int64_t n, int p);
 
 // R_m = M diag(R) M^T and L_m = M L M^T (loops x loops, column-major), upper
 // triangle evaluated in the reference's order and mirrored.
+// h_row_ptr: the same row pointers on the host (long rows take their own kernel).
 fh_status device_congruence(const double *d_L, const double *d_R, int64_t n, const int64_t *d_row_ptr,
-                            const int32_t *d_branch, const double *d_sign, int64_t loops, double *d_Lm,
-                            double *d_Rm, cudaStream_t stream, fh_error_info *err);
+                            const int32_t *d_branch, const double *d_sign, int64_t loops, const int64_t *h_row_ptr,
+                            double *d_Lm, double *d_Rm, cudaStream_t stream, fh_error_info *err);
 
 }  // namespace fhb

@@ -855,6 +855,24 @@ __global__ void key_heads_kernel(const DevFil *__restrict__ fil, const int4 *__r
     }
 }
 
+// flag[t] = 1 where sorted item t heads its key's run.
+__global__ void head_flag_kernel(const int64_t *__restrict__ headof, int64_t count, int64_t *__restrict__ flag) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x)
+        flag[t] = headof[t] == t ? 1 : 0;
+}
+
+// heads[rank] = the item of each run head; item_head[item] = its head's rank.
+__global__ void head_compact_kernel(const int64_t *__restrict__ order, const int64_t *__restrict__ headof,
+                                    const int64_t *__restrict__ rank, const int64_t *__restrict__ flag, int64_t count,
+                                    int64_t *__restrict__ heads, int64_t *__restrict__ item_head) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        if (flag[t]) heads[rank[t]] = order[t];
+        item_head[order[t]] = rank[headof[t]];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Sampled filaments (neumann.rs:280-325 with lines.rs:72-170), warp per pair.
 // ---------------------------------------------------------------------------
@@ -1235,37 +1253,80 @@ __global__ void aligned_grad_scatter_kernel(const DevFil *__restrict__ fil, cons
     }
 }
 
-// Upper-triangle congruence tile with mirrored store (solve.rs:1172-1200).
-// Entry (i, j), i <= j:  sum over (b, s_b) in row j of s_b * sum over (a, s_a)
-// in row i of s_a * B[b, a].  B is symmetric so B[b, a] is read as B[a + b n]
-// (bit-identical), which keeps the loads coalesced across i.
-template <bool kDiag>
-__global__ void __launch_bounds__(256) congruence_kernel(const double *__restrict__ B, const double *__restrict__ Rdiag,
-                                                         int64_t n, const int64_t *__restrict__ row_ptr,
-                                                         const int32_t *__restrict__ branch,
-                                                         const double *__restrict__ sign, int64_t loops,
-                                                         double *__restrict__ out) {
+// Congruence M B M^T in the reference's two steps (solve.rs:1172-1200):
+// for loop row i, product_i = sum over (a, s_a) in row i of s_a B[a, :], then
+// entry (i, j), j >= i, = sum over (b, s_b) in row j of s_b product_i[b],
+// each sum in row order, mirrored.  Here product_i is materialized as row i
+// of U (loops x n, column-major), so that both steps are coalesced column
+// combinations and no (long row) x (long row) pair is evaluated term by term.
+constexpr int kRowsCols = 32;  // columns of B per block in loop_rows_kernel
+constexpr int kShortRow = 8;   // longer rows go to loop_rows_long_kernel
+
+// U[i + c loops] = sum_p s_p B[a_p + c n], p over row i in order.
+__global__ void __launch_bounds__(128) loop_rows_kernel(const double *__restrict__ B, int64_t n,
+                                                        const int64_t *__restrict__ row_ptr,
+                                                        const int32_t *__restrict__ branch,
+                                                        const double *__restrict__ sign, int64_t loops,
+                                                        double *__restrict__ U) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= loops) return;
+    const int64_t c0 = (int64_t)blockIdx.y * kRowsCols, c1 = min(n, c0 + kRowsCols);
+    const int64_t p0 = row_ptr[i], p1 = row_ptr[i + 1];
+    if (p1 - p0 > kShortRow) return;  // loop_rows_long_kernel
+    for (int64_t c = c0; c < c1; ++c) {
+        const double *col = B + c * n;
+        double inner = 0.0;
+        for (int64_t p = p0; p < p1; ++p) inner = __dadd_rn(inner, __dmul_rn(sign[p], col[branch[p]]));
+        U[i + c * loops] = inner;
+    }
+}
+
+// Rows longer than kShortRow (link and port loops along a path): one thread
+// per column, the row's entries in order.
+__global__ void __launch_bounds__(256) loop_rows_long_kernel(const double *__restrict__ B, int64_t n,
+                                                             const int64_t *__restrict__ row_ptr,
+                                                             const int32_t *__restrict__ branch,
+                                                             const double *__restrict__ sign, int64_t loops,
+                                                             const int64_t *__restrict__ long_rows,
+                                                             double *__restrict__ U) {
+    const int64_t i = long_rows[blockIdx.y];
+    const int64_t p0 = row_ptr[i], p1 = row_ptr[i + 1];
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const double *col = B + c * n;
+        double inner = 0.0;
+        for (int64_t p = p0; p < p1; ++p) inner = __dadd_rn(inner, __dmul_rn(sign[p], col[branch[p]]));
+        U[i + c * loops] = inner;
+    }
+}
+
+// The same for a diagonal B (resistances): row i of U is zero except
+// s_p R[a_p] at column a_p (the zero terms of the sum change no bit; loop
+// rows hold each branch once).  U must be zero-filled.
+__global__ void loop_rows_diag_kernel(const double *__restrict__ Rdiag, const int64_t *__restrict__ row_ptr,
+                                      const int32_t *__restrict__ branch, const double *__restrict__ sign,
+                                      int64_t loops, double *__restrict__ U) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < loops; i += (int64_t)gridDim.x * blockDim.x)
+        for (int64_t p = row_ptr[i]; p < row_ptr[i + 1]; ++p)
+            U[i + (int64_t)branch[p] * loops] = __dmul_rn(sign[p], Rdiag[branch[p]]);
+}
+
+// out[i + j loops] = sum_q s_q U[i + b_q loops], q over row j in order, for
+// i <= j, mirrored through a shared-memory tile.  Block (32, 8) covers a
+// 32 x 32 tile of the upper triangle.
+__global__ void __launch_bounds__(256) loop_cols_kernel(const double *__restrict__ U, const int64_t *__restrict__ row_ptr,
+                                                        const int32_t *__restrict__ branch,
+                                                        const double *__restrict__ sign, int64_t loops,
+                                                        double *__restrict__ out) {
     const int64_t I = blockIdx.y, J = blockIdx.x;
     if (I > J) return;
     __shared__ double tile[32][33];
-    const int tx = threadIdx.x, ty = threadIdx.y;  // (32, 8)
+    const int tx = threadIdx.x, ty = threadIdx.y;
     for (int r = ty; r < 32; r += 8) {
         const int64_t i = I * 32 + tx, j = J * 32 + r;
         double v = 0.0;
         if (i < loops && j < loops && i <= j) {
-            const int64_t pi0 = row_ptr[i], pi1 = row_ptr[i + 1], pj0 = row_ptr[j], pj1 = row_ptr[j + 1];
-            for (int64_t q = pj0; q < pj1; ++q) {
-                const int64_t b = branch[q];
-                double inner = 0.0;
-                for (int64_t p = pi0; p < pi1; ++p) {
-                    const int64_t a = branch[p];
-                    double bab;
-                    if (kDiag) bab = a == b ? Rdiag[a] : 0.0;
-                    else bab = B[a + b * n];
-                    inner = __dadd_rn(inner, __dmul_rn(sign[p], bab));
-                }
-                v = __dadd_rn(v, __dmul_rn(sign[q], inner));
-            }
+            for (int64_t q = row_ptr[j]; q < row_ptr[j + 1]; ++q)
+                v = __dadd_rn(v, __dmul_rn(sign[q], U[i + (int64_t)branch[q] * loops]));
             out[i + j * loops] = v;
         }
         tile[r][tx] = v;
@@ -1338,16 +1399,20 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
     if (list) FHB_CUDA(cudaMemsetAsync(d_L, 0, sizeof(double) * n_pairs, stream));
     cudaEvent_t ev[6];
     for (auto &e : ev) FHB_CUDA(cudaEventCreate(&e));
+    // Scratch comes from the stream-ordered memory cache: no device-wide
+    // synchronization per buffer, released after the last kernel that reads
+    // it.
     struct Guard {
         std::vector<void *> ptrs;
         cudaEvent_t *ev;
+        cudaStream_t s;
         ~Guard() {
-            for (void *p : ptrs) cudaFree(p);
+            for (void *p : ptrs) cache_free(p, s);
             for (int k = 0; k < 6; ++k) cudaEventDestroy(ev[k]);
         }
-    } guard{{}, ev};
+    } guard{{}, ev, stream};
     auto alloc = [&](void **p, size_t bytes) -> cudaError_t {
-        cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+        cudaError_t e = cache_alloc(p, bytes, stream);
         if (e == cudaSuccess) guard.ptrs.push_back(*p);
         return e;
     };
@@ -1451,30 +1516,33 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
         key_heads_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_quad, d_hash_sorted, d_order, n_quad, d_headpos);
         FHB_CUDA(cudaGetLastError());
         FHB_CUDA(cub::DeviceScan::InclusiveScan(d_tmp, tmp_bytes, d_headpos, d_headof, cub::Max(), (int)n_quad, stream));
-        // Compact the heads: head positions are where headof[t] == t.
-        std::vector<int64_t> h_headof((size_t)n_quad), h_order((size_t)n_quad);
-        FHB_CUDA(cudaMemcpyAsync(h_headof.data(), d_headof, 8 * n_quad, cudaMemcpyDeviceToHost, stream));
-        FHB_CUDA(cudaMemcpyAsync(h_order.data(), d_order, 8 * n_quad, cudaMemcpyDeviceToHost, stream));
-        FHB_CUDA(cudaStreamSynchronize(stream));
-        // Build, per original item, the index of its head among the distinct keys.
-        std::vector<int64_t> head_item, item_head((size_t)n_quad);
-        std::vector<int64_t> head_rank((size_t)n_quad, -1);
-        for (int64_t t = 0; t < n_quad; ++t) {
-            if (h_headof[t] == t) {
-                head_rank[t] = (int64_t)head_item.size();
-                head_item.push_back(h_order[t]);
-            }
-            item_head[h_order[t]] = head_rank[h_headof[t]];
+        // Compact the heads on the device: head positions are where
+        // headof[t] == t; their ranks (exclusive sum of the flags) number
+        // the distinct keys.
+        int64_t *d_flag = d_headpos, *d_rank = reinterpret_cast<int64_t *>(d_hash);
+        head_flag_kernel<<<blocks, 256, 0, stream>>>(d_headof, n_quad, d_flag);
+        FHB_CUDA(cudaGetLastError());
+        size_t tmp3 = 0;
+        FHB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp3, d_flag, d_rank, (int)n_quad, stream));
+        if (tmp3 > tmp_bytes) {
+            FHB_CUDA(alloc(&d_tmp, tmp3));
+            tmp_bytes = tmp3;
         }
-        const int64_t n_heads = (int64_t)head_item.size();
+        FHB_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_flag, d_rank, (int)n_quad, stream));
+        int64_t last[2];
+        FHB_CUDA(cudaMemcpyAsync(&last[0], d_rank + n_quad - 1, 8, cudaMemcpyDeviceToHost, stream));
+        FHB_CUDA(cudaMemcpyAsync(&last[1], d_flag + n_quad - 1, 8, cudaMemcpyDeviceToHost, stream));
+        FHB_CUDA(cudaStreamSynchronize(stream));
+        const int64_t n_heads = last[0] + last[1];
         st.unique_aligned = n_heads;
         int64_t *d_heads, *d_item_head;
         double *d_values;
         FHB_CUDA(alloc((void **)&d_heads, 8 * n_heads));
         FHB_CUDA(alloc((void **)&d_item_head, 8 * n_quad));
         FHB_CUDA(alloc((void **)&d_values, (grad ? 56 : 8) * n_heads));
-        FHB_CUDA(cudaMemcpyAsync(d_heads, head_item.data(), 8 * n_heads, cudaMemcpyHostToDevice, stream));
-        FHB_CUDA(cudaMemcpyAsync(d_item_head, item_head.data(), 8 * n_quad, cudaMemcpyHostToDevice, stream));
+        head_compact_kernel<<<blocks, 256, 0, stream>>>(d_order, d_headof, d_rank, d_flag, n_quad, d_heads,
+                                                        d_item_head);
+        FHB_CUDA(cudaGetLastError());
         int qblocks = (int)std::min<int64_t>(n_heads, (int64_t)sms * 16);
         if (grad) {
             aligned_quadrature_kernel<true><<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads,
@@ -1549,14 +1617,49 @@ fh_status device_fill_grad(const DevFil *d_fil, const FilTan *d_tan, int64_t n, 
 }
 
 fh_status device_congruence(const double *d_L, const double *d_R, int64_t n, const int64_t *d_row_ptr,
-                            const int32_t *d_branch, const double *d_sign, int64_t loops, double *d_Lm, double *d_Rm,
-                            cudaStream_t stream, fh_error_info *err) {
+                            const int32_t *d_branch, const double *d_sign, int64_t loops, const int64_t *h_row_ptr,
+                            double *d_Lm, double *d_Rm, cudaStream_t stream, fh_error_info *err) {
     if (loops == 0) return FH_OK;
+    std::vector<int64_t> long_rows;
+    for (int64_t i = 0; i < loops; ++i)
+        if (h_row_ptr[i + 1] - h_row_ptr[i] > kShortRow) long_rows.push_back(i);
+    double *d_U = nullptr;
+    const size_t ubytes = sizeof(double) * (size_t)loops * (size_t)n;
+    if (cache_alloc((void **)&d_U, ubytes, stream) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(err, FH_ERR_OUT_OF_MEMORY,
+                    "device allocation of " + std::to_string(ubytes) + " bytes for the congruence failed");
+    }
+    struct Free {
+        double *p;
+        cudaStream_t s;
+        ~Free() { cache_free(p, s); }
+    } free_u{d_U, stream};
     const int T = (int)((loops + 31) / 32);
-    dim3 grid(T, T), block(32, 8);
-    congruence_kernel<false><<<grid, block, 0, stream>>>(d_L, nullptr, n, d_row_ptr, d_branch, d_sign, loops, d_Lm);
+    const dim3 rows_grid((unsigned)((loops + 127) / 128), (unsigned)((n + kRowsCols - 1) / kRowsCols));
+    loop_rows_kernel<<<rows_grid, 128, 0, stream>>>(d_L, n, d_row_ptr, d_branch, d_sign, loops, d_U);
     FHB_CUDA(cudaGetLastError());
-    congruence_kernel<true><<<grid, block, 0, stream>>>(nullptr, d_R, n, d_row_ptr, d_branch, d_sign, loops, d_Rm);
+    int64_t *d_long = nullptr;
+    if (!long_rows.empty()) {
+        if (cache_alloc((void **)&d_long, 8 * long_rows.size(), stream) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(err, FH_ERR_OUT_OF_MEMORY, "device allocation for the congruence failed");
+        }
+        FHB_CUDA(cudaMemcpyAsync(d_long, long_rows.data(), 8 * long_rows.size(), cudaMemcpyHostToDevice, stream));
+        const unsigned bx = (unsigned)std::min<int64_t>((n + 255) / 256, 64);
+        loop_rows_long_kernel<<<dim3(bx, (unsigned)long_rows.size()), 256, 0, stream>>>(
+            d_L, n, d_row_ptr, d_branch, d_sign, loops, d_long, d_U);
+        cudaError_t le = cudaGetLastError();
+        cache_free(d_long, stream);
+        if (le != cudaSuccess) return fail(err, FH_ERR_CUDA, std::string("congruence: ") + cudaGetErrorString(le));
+    }
+    loop_cols_kernel<<<dim3(T, T), dim3(32, 8), 0, stream>>>(d_U, d_row_ptr, d_branch, d_sign, loops, d_Lm);
+    FHB_CUDA(cudaGetLastError());
+    FHB_CUDA(cudaMemsetAsync(d_U, 0, ubytes, stream));
+    loop_rows_diag_kernel<<<(unsigned)std::min<int64_t>((loops + 255) / 256, 148 * 8), 256, 0, stream>>>(
+        d_R, d_row_ptr, d_branch, d_sign, loops, d_U);
+    FHB_CUDA(cudaGetLastError());
+    loop_cols_kernel<<<dim3(T, T), dim3(32, 8), 0, stream>>>(d_U, d_row_ptr, d_branch, d_sign, loops, d_Rm);
     FHB_CUDA(cudaGetLastError());
     return FH_OK;
 }

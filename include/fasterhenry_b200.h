@@ -188,6 +188,12 @@ const char *fh_last_error(void);
 /* Number of usable sm_100 devices (0 when none). */
 int32_t fh_device_count(void);
 
+/* Device memory of finished systems is kept in a per-device cache (a
+ * stream-ordered pool) and reused by later systems; this hands the idle part
+ * back to the driver (the analogue of emptying a framework's allocator
+ * cache).  Waits for the devices to finish their work first. */
+fh_status fh_release_cached_memory(void);
+
 /* ---- host model (no device use) --------------------------------------- */
 
 /* Discretize a geometry into filaments.  Replaces discretize_geometry

@@ -89,6 +89,11 @@ class ParamSpec(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("reserved", ctypes.c_int32), ("index", ctypes.c_int64)]
 
 
+class PowerBalance(ctypes.Structure):
+    _fields_ = [("dissipated_w", ctypes.c_double), ("input_w", ctypes.c_double),
+                ("relative_residual", ctypes.c_double)]
+
+
 class GradientReport(ctypes.Structure):
     _fields_ = [("solve_s", ctypes.c_double), ("derivative_fill_s", ctypes.c_double), ("contract_s", ctypes.c_double),
                 ("total_s", ctypes.c_double), ("pairs", ctypes.c_int64)]
@@ -128,6 +133,7 @@ EXPORTS = [
     "fh_pfft_destroy", "fh_gmres_default_params", "fh_iterative_create", "fh_iterative_counts", "fh_iterative_timing",
     "fh_iterative_pfft_stats", "fh_iterative_sweep", "fh_iterative_destroy", "fh_test_gmres_dense",
     "fh_batch_sweep", "fh_gradient", "fh_test_inductance_gradient", "fh_release_cached_memory",
+    "fh_system_layout", "fh_currents",
 ]
 
 PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner",
@@ -192,6 +198,9 @@ def load():
     L.fh_gradient.argtypes = [ctypes.c_void_p, ctypes.c_double, P(ParamSpec), sz, c_double_p, c_double_p,
                               P(GradientReport), ei]
     L.fh_test_inductance_gradient.argtypes = [P(Filament), c_double_p, sz, c_double_p, c_double_p, ei]
+    L.fh_system_layout.argtypes = [ctypes.c_void_p, c_int64_p, c_int64_p, c_int64_p]
+    L.fh_currents.argtypes = [ctypes.c_void_p, c_double_p, sz, c_double_p, sz, ctypes.c_int, c_double_p, c_double_p,
+                              c_double_p, c_double_p, c_double_p, c_int64_p, c_double_p, P(PowerBalance), ei]
     L.fh_system_destroy.argtypes = [ctypes.c_void_p]
     L.fh_system_destroy.restype = None
     L.fh_system_counts.argtypes = [ctypes.c_void_p, P(Counts)]

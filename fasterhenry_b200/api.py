@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import ctypes
 import dataclasses
+import math
 import enum
 import json
 from typing import Dict, List, Optional, Sequence, Tuple
@@ -107,6 +108,19 @@ class NotConverged(FasterHenryError):
     status = N.ERR_NOT_CONVERGED
 
 
+class InvalidExcitation(FasterHenryError):
+    """SolveError::InvalidExcitation{expected, got} (solve.rs:592-599)."""
+    status = N.ERR_INVALID_EXCITATION
+
+    @property
+    def expected(self) -> int:
+        return int(self.info.index_a)
+
+    @property
+    def got(self) -> int:
+        return int(self.info.index_b)
+
+
 class Unsupported(FasterHenryError):
     status = N.ERR_UNSUPPORTED
 
@@ -122,7 +136,7 @@ class InvalidArgument(FasterHenryError, ValueError):
 
 _ERRORS = {c.status: c for c in (NoDevice, CudaError, OutOfMemory, GeometryError, DiscretizeError, CoincidentSamples,
                                  NotFinite, MeshError, InvalidGrading, InvalidFrequency, Singular, NotConverged,
-                                 Unsupported, InvalidArgument, PfftError)}
+                                 Unsupported, InvalidArgument, PfftError, InvalidExcitation)}
 
 
 def _check(status: int, info: Optional[N.ErrorInfo] = None) -> None:
@@ -571,6 +585,54 @@ class MeshSystem:
     def impedance(self, frequency: float, precision: Precision = Precision.FP64) -> np.ndarray:
         return self.sweep([frequency], precision).impedance_ohm[0]
 
+    def layout(self) -> Tuple[np.ndarray, np.ndarray, int]:
+        """(segment of every filament, conductor of every segment, conductor
+        count): the Layout of currents.rs:128-170."""
+        n, nseg = self._counts["filaments"], self._counts["segments"]
+        sof = np.zeros(max(1, n), dtype=np.int64)
+        cos = np.zeros(max(1, nseg), dtype=np.int64)
+        nc = ctypes.c_int64()
+        _check(N.load().fh_system_layout(self._h, sof.ctypes.data_as(N.c_int64_p), cos.ctypes.data_as(N.c_int64_p),
+                                         ctypes.byref(nc)))
+        return sof[:n], cos[:nseg], int(nc.value)
+
+    def currents(self, frequency, excitation: Optional[Sequence[complex]] = None,
+                 precision: Precision = Precision.FP64):
+        """Filament currents for the port-current phasors ``excitation``
+        (default: 1 A into port 1, the other ports open) at one frequency or a
+        list of them (MeshSystem::currents, solve.rs:845-868): one
+        CurrentSolution per frequency."""
+        single = np.ndim(frequency) == 0
+        f = np.ascontiguousarray(np.atleast_1d(frequency), dtype=np.float64)
+        p, n, nseg = self._counts["ports"], self._counts["filaments"], self._counts["segments"]
+        if excitation is None:
+            excitation = unit_excitation(p)
+        exc = np.ascontiguousarray(np.asarray(excitation, dtype=np.complex128).ravel())
+        sof, cos, ncond = self.layout()
+        nf = len(f)
+        cur = np.zeros((nf, n), dtype=np.complex128)
+        dens = np.zeros((nf, n))
+        pw = np.zeros((nf, n))
+        segc = np.zeros((nf, nseg), dtype=np.complex128)
+        segp = np.zeros((nf, nseg))
+        pk = np.zeros((nf, max(1, ncond)), dtype=np.int64)
+        pkd = np.zeros((nf, max(1, ncond)))
+        bal = (N.PowerBalance * max(1, nf))()
+        info = N.ErrorInfo()
+        dp = lambda a: a.ctypes.data_as(N.c_double_p)
+        _check(N.load().fh_currents(self._h, dp(f), nf, exc.ctypes.data_as(N.c_double_p) if len(exc) else None,
+                                    len(exc), int(precision), dp(cur), dp(dens), dp(pw), dp(segc), dp(segp),
+                                    pk.ctypes.data_as(N.c_int64_p), dp(pkd), bal, ctypes.byref(info)), info)
+        fil = self.filaments()
+        centres = 0.5 * (fil[:, 0:3] + fil[:, 3:6])
+        out = []
+        for k in range(nf):
+            out.append(CurrentSolution(float(f[k]), exc.copy(), cur[k], dens[k], pw[k], sof, cos, centres, segc[k],
+                                       segp[k], pk[k, :ncond], pkd[k, :ncond],
+                                       {"dissipated_w": bal[k].dissipated_w, "input_w": bal[k].input_w,
+                                        "relative_residual": bal[k].relative_residual}))
+        return out[0] if single else out
+
     def gradient(self, frequency: float, params: Optional[Sequence["Param"]] = None) -> "GradientResult":
         """dZ/dp at one frequency by the stationary (adjoint) form
         (fh_gradient): one FP64 solve for the loop currents, one derivative
@@ -594,6 +656,89 @@ class MeshSystem:
         return GradientResult(float(frequency), params, z, dz[:len(params)],
                               {k: (int(getattr(rep, k)) if k == "pairs" else float(getattr(rep, k)))
                                for k, _ in N.GradientReport._fields_})
+
+
+CURRENTS_CSV_HEADER = ("frequency_hz,filament,segment,conductor,x_m,y_m,z_m,"
+                       "current_re_a,current_im_a,current_abs_a,j_abs_a_per_m2,power_w")
+
+
+def unit_excitation(ports: int) -> List[complex]:
+    """1 A into port 1, every other port open (currents.rs:121-128)."""
+    return [1.0 + 0j if k == 0 else 0j for k in range(ports)]
+
+
+@dataclasses.dataclass
+class CurrentSolution:
+    """All currents of one frequency and excitation (CurrentSolution,
+    currents.rs:107-119), held as arrays: phasor currents (peak amperes),
+    |J| in A/m^2 and time-average power P = |I|^2 R / 2 per filament, sums
+    per segment, the filament of largest |J| per conductor, and the power
+    balance."""
+    frequency_hz: float
+    excitation: np.ndarray
+    current: np.ndarray
+    current_density: np.ndarray
+    power_w: np.ndarray
+    segment_of_filament: np.ndarray
+    conductor_of_segment: np.ndarray
+    location: np.ndarray
+    segment_current: np.ndarray
+    segment_power_w: np.ndarray
+    peak_filament: np.ndarray
+    peak_current_density: np.ndarray
+    power_balance: Dict[str, float]
+
+    @property
+    def segments(self) -> List[dict]:
+        return [{"segment": s, "conductor": int(self.conductor_of_segment[s]),
+                 "current": complex(self.segment_current[s]), "power_w": float(self.segment_power_w[s])}
+                for s in range(len(self.segment_current))]
+
+    @property
+    def conductors(self) -> List[dict]:
+        return [{"conductor": c, "peak_current_density": float(self.peak_current_density[c]),
+                 "filament": int(self.peak_filament[c]), "location": [float(x) for x in self.location[self.peak_filament[c]]]}
+                for c in range(len(self.peak_filament))]
+
+    def csv_rows(self) -> List[str]:
+        """Rows of the CLI's --currents CSV for this frequency (fasterhenry-cli/src/lib.rs:238-276)."""
+        rows = []
+        for k in range(len(self.current)):
+            s = int(self.segment_of_filament[k])
+            i = self.current[k]
+            x, y, z = self.location[k]
+            rows.append(",".join([_rust_e(self.frequency_hz), str(k), str(s), str(int(self.conductor_of_segment[s])),
+                                  _rust_e(x), _rust_e(y), _rust_e(z), _rust_e(i.real), _rust_e(i.imag), _rust_e(abs(i)),
+                                  _rust_e(self.current_density[k]), _rust_e(self.power_w[k])]))
+        return rows
+
+    def json_block(self) -> dict:
+        """One entry of the CLI's ``currents.by_frequency`` JSON block."""
+        seg = [{"segment": d["segment"], "conductor": d["conductor"],
+                "current": [d["current"].real, d["current"].imag], "power_w": d["power_w"]} for d in self.segments]
+        return {"frequency_hz": self.frequency_hz, "power_balance": dict(self.power_balance),
+                "conductors": self.conductors, "segments": seg}
+
+
+def _rust_e(x: float) -> str:
+    """Rust's ``{:e}`` formatting of an f64: the shortest mantissa that reads
+    back to the same value, exponent without padding or plus sign (1e6,
+    2.5e-3, 0e0)."""
+    x = float(x)
+    if x != x:
+        return "NaN"
+    if math.isinf(x):
+        return "inf" if x > 0 else "-inf"
+    if x == 0.0:
+        return "-0e0" if math.copysign(1.0, x) < 0 else "0e0"
+    for prec in range(17):
+        cand = "%.*e" % (prec, x)
+        if float(cand) == x:
+            break
+    m, e = cand.split("e")
+    if "." in m:
+        m = m.rstrip("0").rstrip(".")
+    return "%se%d" % (m, int(e))
 
 
 @dataclasses.dataclass(frozen=True)

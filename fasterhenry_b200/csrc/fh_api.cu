@@ -70,6 +70,13 @@ struct fh_system {
     int device = 0;
     cudaStream_t stream = nullptr;
     double *d_Lm = nullptr, *d_Rm = nullptr;
+    // Layout (currents.rs:128-170) and, once currents are asked for, the
+    // transposed loop basis and per-filament (w, h, R) on the device.
+    std::vector<int64_t> segment_of_filament, conductor_of_segment, segment_first;
+    int64_t conductors = 0;
+    int64_t *d_col_ptr = nullptr, *d_first = nullptr;
+    int32_t *d_col_loop = nullptr;
+    double *d_col_sign = nullptr, *d_whr = nullptr;
     fh_counts counts{};
     fh_timing timing{};
     FillStats fill{};
@@ -78,6 +85,11 @@ struct fh_system {
         pool.release();
         cache_free(d_Lm, stream);
         cache_free(d_Rm, stream);
+        cache_free(d_col_ptr, stream);
+        cache_free(d_first, stream);
+        cache_free(d_col_loop, stream);
+        cache_free(d_col_sign, stream);
+        cache_free(d_whr, stream);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -660,6 +672,40 @@ fh_status fh_system_create(const fh_node *nodes, size_t n_nodes, const fh_segmen
     cudaEventDestroy(c0);
     cudaEventDestroy(c1);
     const double t3 = wall();
+    // Conductors: connected components of the segment graph by union-find
+    // over nodes, numbered in order of their first segment (currents.rs:137-163).
+    {
+        std::vector<int64_t> parent(n_nodes);
+        for (size_t v = 0; v < n_nodes; ++v) parent[v] = (int64_t)v;
+        auto find = [&](int64_t x) {
+            while (parent[(size_t)x] != x) {
+                parent[(size_t)x] = parent[(size_t)parent[(size_t)x]];
+                x = parent[(size_t)x];
+            }
+            return x;
+        };
+        for (size_t g = 0; g < n_segments; ++g) {
+            const int64_t a = find(segments[g].a), b = find(segments[g].b);
+            if (a != b) parent[(size_t)a] = b;
+        }
+        std::vector<int64_t> roots;
+        for (size_t g = 0; g < n_segments; ++g) {
+            const int64_t root = find(segments[g].a);
+            auto it = std::find(roots.begin(), roots.end(), root);
+            if (it == roots.end()) {
+                roots.push_back(root);
+                s->conductor_of_segment.push_back((int64_t)roots.size() - 1);
+            } else {
+                s->conductor_of_segment.push_back((int64_t)(it - roots.begin()));
+            }
+        }
+        s->conductors = (int64_t)roots.size();
+        s->segment_first.assign(1, 0);
+        for (size_t g = 0; g < n_segments; ++g) {
+            for (int64_t k = 0; k < s->disc.per_segment[g]; ++k) s->segment_of_filament.push_back((int64_t)g);
+            s->segment_first.push_back(s->segment_first.back() + s->disc.per_segment[g]);
+        }
+    }
     s->counts = fh_counts{(int64_t)n_nodes, (int64_t)n_segments, n, loops, s->m, s->p};
     s->timing.inductance_s = t2 - t1;
     s->timing.assembly_s = t3 - t0;
@@ -899,6 +945,196 @@ fh_status fh_batch_sweep(fh_system *const *systems, size_t k, const double *cons
 fh_status fh_impedance(fh_system *sys, double frequency_hz, fh_precision precision, double *z_out,
                        fh_error_info *err) {
     return fh_sweep(sys, &frequency_hz, 1, precision, z_out, nullptr, err);
+}
+
+fh_status fh_system_layout(const fh_system *sys, int64_t *segment_of_filament, int64_t *conductor_of_segment,
+                           int64_t *conductor_count) {
+    if (!sys) return fail(nullptr, FH_ERR_INVALID_ARGUMENT, "null system");
+    if (segment_of_filament)
+        std::copy(sys->segment_of_filament.begin(), sys->segment_of_filament.end(), segment_of_filament);
+    if (conductor_of_segment)
+        std::copy(sys->conductor_of_segment.begin(), sys->conductor_of_segment.end(), conductor_of_segment);
+    if (conductor_count) *conductor_count = sys->conductors;
+    return FH_OK;
+}
+
+fh_status fh_currents(fh_system *sys, const double *freqs, size_t nf, const double *excitation, size_t n_excitation,
+                      fh_precision precision, double *filament_current, double *current_density, double *power_w,
+                      double *segment_current, double *segment_power_w, int64_t *conductor_peak_filament,
+                      double *conductor_peak_density, fh_power_balance *balance, fh_error_info *err) {
+    clear_error(err);
+    if (!sys || (nf && !freqs) || (n_excitation && !excitation))
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "null argument");
+    for (size_t k = 0; k < nf; ++k)
+        if (!(std::isfinite(freqs[k]) && freqs[k] >= 0.0))
+            return fail(err, FH_ERR_INVALID_FREQUENCY,
+                        "frequency " + std::to_string(k) + " is " + fstr(freqs[k]) +
+                            " Hz; frequencies must be finite and non-negative",
+                        (int64_t)k, -1, freqs[k]);
+    const int64_t n = sys->n, m = sys->m, p = sys->p, loops = sys->nloops;
+    const int64_t nseg = (int64_t)sys->segments.size(), ncond = sys->conductors;
+    bool finite = (int64_t)n_excitation == p;
+    for (size_t q = 0; q < 2 * n_excitation && finite; ++q) finite = std::isfinite(excitation[q]);
+    if (!finite)
+        return fail(err, FH_ERR_INVALID_EXCITATION,
+                    "excitation must have one finite entry per port (" + std::to_string(p) + "), got " +
+                        std::to_string(n_excitation) + " entries",
+                    p, (int64_t)n_excitation);
+    if (precision < FH_PRECISION_FP64 || precision > FH_PRECISION_MIXED_FP32)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "unknown precision");
+    if (nf == 0) return FH_OK;
+    FHB_CUDA(cudaSetDevice(sys->device));
+    cudaStream_t st = sys->stream;
+    // Device layout, once: per branch its (loop, sign) in increasing loop order.
+    if (!sys->d_col_ptr) {
+        std::vector<int64_t> col_ptr((size_t)n + 1, 0);
+        for (size_t e = 0; e < sys->loops.branch.size(); ++e) ++col_ptr[(size_t)sys->loops.branch[e] + 1];
+        for (int64_t k = 0; k < n; ++k) col_ptr[(size_t)k + 1] += col_ptr[(size_t)k];
+        std::vector<int32_t> col_loop(sys->loops.branch.size());
+        std::vector<double> col_sign(sys->loops.branch.size());
+        std::vector<int64_t> fillp(col_ptr.begin(), col_ptr.end() - 1);
+        for (int64_t r = 0; r < loops; ++r)
+            for (int64_t e = sys->loops.row_ptr[(size_t)r]; e < sys->loops.row_ptr[(size_t)r + 1]; ++e) {
+                const int64_t slot = fillp[(size_t)sys->loops.branch[(size_t)e]]++;
+                col_loop[(size_t)slot] = (int32_t)r;
+                col_sign[(size_t)slot] = sys->loops.sign[(size_t)e];
+            }
+        std::vector<double> whr((size_t)(3 * n));
+        for (int64_t k = 0; k < n; ++k) {
+            whr[(size_t)(3 * k)] = sys->disc.filaments[(size_t)k].width;
+            whr[(size_t)(3 * k + 1)] = sys->disc.filaments[(size_t)k].height;
+            whr[(size_t)(3 * k + 2)] = sys->resistances[(size_t)k];
+        }
+        auto up = [&](void **d, const void *h, size_t bytes) -> cudaError_t {
+            cudaError_t e = cache_alloc(d, bytes, st);
+            if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(*d, h, bytes, cudaMemcpyHostToDevice, st);
+            return e;
+        };
+        FHB_CUDA(up((void **)&sys->d_col_ptr, col_ptr.data(), 8 * col_ptr.size()));
+        FHB_CUDA(up((void **)&sys->d_col_loop, col_loop.data(), 4 * col_loop.size()));
+        FHB_CUDA(up((void **)&sys->d_col_sign, col_sign.data(), 8 * col_sign.size()));
+        FHB_CUDA(up((void **)&sys->d_whr, whr.data(), 8 * whr.size()));
+        FHB_CUDA(up((void **)&sys->d_first, sys->segment_first.data(), 8 * sys->segment_first.size()));
+        FHB_CUDA(cudaStreamSynchronize(st));
+    }
+    const bool mixed = precision != FH_PRECISION_FP64;
+    const TrailingUpdate update =
+        precision == FH_PRECISION_MIXED_BF16X3 ? TrailingUpdate::TensorBf16x3 : TrailingUpdate::Simt;
+    size_t free_b = 0, total_b = 0;
+    FHB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    free_b = (free_b + cache_idle_bytes()) / (size_t)std::max(1, sys->share) + sys->pool.held();
+    const double per = (mixed ? 8.0 : 16.0) * (double)m * (double)m + 64.0 * (double)(m * p + 64) + 48.0 * (double)n +
+                       32.0 * (double)nseg +
+                       (outer_for(m, update) ? 16.0 * (double)m * kOuterFp32 + 16.0 * (double)(m + kNbFp32) * kNbFp32
+                                             : 0.0);
+    const int chunk = (int)std::max(1.0, std::min<double>((double)nf, 0.8 * (double)free_b / std::max(per, 1.0)));
+    PBuf<double> d_omega, d_x, d_z;
+    FHB_PALLOC(sys->pool, d_omega, kSlotOmega, (size_t)chunk);
+    FHB_PALLOC(sys->pool, d_x, kSlotX, (size_t)std::max<int64_t>(1, chunk * m * p * 2));
+    FHB_PALLOC(sys->pool, d_z, kSlotZ, (size_t)chunk * p * p * 2);
+    DBuf<double> d_ip(st), d_ib(st), d_dens(st), d_pow(st), d_segc(st), d_segp(st), d_segpk(st);
+    DBuf<int64_t> d_segi(st);
+    FHB_ALLOC(d_ip, (size_t)(2 * p));
+    FHB_ALLOC(d_ib, (size_t)(chunk * n * 2));
+    FHB_ALLOC(d_dens, (size_t)(chunk * n));
+    FHB_ALLOC(d_pow, (size_t)(chunk * n));
+    FHB_ALLOC(d_segc, (size_t)(chunk * nseg * 2));
+    FHB_ALLOC(d_segp, (size_t)(chunk * nseg));
+    FHB_ALLOC(d_segpk, (size_t)(chunk * nseg));
+    FHB_ALLOC(d_segi, (size_t)(chunk * nseg));
+    FHB_CUDA(cudaMemcpyAsync(d_ip.p, excitation, 16 * (size_t)p, cudaMemcpyHostToDevice, st));
+    typedef std::complex<double> C;
+    std::vector<double> z((size_t)(chunk * p * p * 2)), segp((size_t)(chunk * nseg)), segpk((size_t)(chunk * nseg));
+    std::vector<int64_t> segi((size_t)(chunk * nseg));
+    float ms_factor = 0, ms_refine = 0;
+    for (size_t c0 = 0; c0 < nf; c0 += (size_t)chunk) {
+        const int count = (int)std::min<size_t>((size_t)chunk, nf - c0);
+        std::vector<double> omega((size_t)count);
+        for (int f = 0; f < count; ++f) omega[(size_t)f] = kTau * freqs[c0 + (size_t)f];
+        FHB_CUDA(cudaMemcpyAsync(d_omega.p, omega.data(), 8 * (size_t)count, cudaMemcpyHostToDevice, st));
+        std::vector<int> singular((size_t)count, 0), failed((size_t)count, 0);
+        fh_status e;
+        bool redo = false;
+        if (mixed) {
+            e = sweep_chunk_mixed(sys, d_omega.p, count, d_x.p, d_z.p, singular.data(), failed.data(), nullptr,
+                                  nullptr, &ms_factor, &ms_refine, update, err);
+            if (e) return e;
+            for (int f = 0; f < count; ++f) redo = redo || failed[(size_t)f];
+        }
+        if (!mixed || redo) {  // refinement that did not converge: the whole batch in FP64
+            e = sweep_chunk_fp64(sys, d_omega.p, count, d_x.p, d_z.p, singular.data(), &ms_factor, err);
+            if (e) return e;
+        }
+        e = launch_currents(d_x.p, d_ip.p, m, (int)p, n, count, sys->d_col_ptr, sys->d_col_loop, sys->d_col_sign,
+                            sys->d_whr, sys->d_first, nseg, d_ib.p, d_dens.p, d_pow.p, d_segc.p, d_segp.p, d_segpk.p,
+                            d_segi.p, st, err);
+        if (e) return e;
+        FHB_CUDA(cudaMemcpyAsync(z.data(), d_z.p, 16 * (size_t)(count * p * p), cudaMemcpyDeviceToHost, st));
+        FHB_CUDA(cudaMemcpyAsync(segp.data(), d_segp.p, 8 * (size_t)(count * nseg), cudaMemcpyDeviceToHost, st));
+        FHB_CUDA(cudaMemcpyAsync(segpk.data(), d_segpk.p, 8 * (size_t)(count * nseg), cudaMemcpyDeviceToHost, st));
+        FHB_CUDA(cudaMemcpyAsync(segi.data(), d_segi.p, 8 * (size_t)(count * nseg), cudaMemcpyDeviceToHost, st));
+        const size_t o = c0;
+        if (filament_current)
+            FHB_CUDA(cudaMemcpyAsync(filament_current + 2 * o * n, d_ib.p, 16 * (size_t)(count * n),
+                                     cudaMemcpyDeviceToHost, st));
+        if (current_density)
+            FHB_CUDA(cudaMemcpyAsync(current_density + o * n, d_dens.p, 8 * (size_t)(count * n),
+                                     cudaMemcpyDeviceToHost, st));
+        if (power_w)
+            FHB_CUDA(cudaMemcpyAsync(power_w + o * n, d_pow.p, 8 * (size_t)(count * n), cudaMemcpyDeviceToHost, st));
+        if (segment_current)
+            FHB_CUDA(cudaMemcpyAsync(segment_current + 2 * o * nseg, d_segc.p, 16 * (size_t)(count * nseg),
+                                     cudaMemcpyDeviceToHost, st));
+        FHB_CUDA(cudaStreamSynchronize(st));
+        // Singular or non-finite: the first such frequency in list order.
+        for (int f = 0; f < count; ++f) {
+            bool bad = singular[(size_t)f] != 0;
+            for (int64_t q = 0; q < 2 * p * p && !bad; ++q) bad = !std::isfinite(z[(size_t)(2 * f * p * p + q)]);
+            if (bad)
+                return fail(err, FH_ERR_SINGULAR,
+                            "the mesh system is singular or ill-conditioned at " + fstr(freqs[c0 + (size_t)f]) + " Hz",
+                            (int64_t)(c0 + (size_t)f), -1, freqs[c0 + (size_t)f]);
+        }
+        for (int f = 0; f < count; ++f) {
+            const size_t k = c0 + (size_t)f;
+            if (segment_power_w)
+                std::copy(segp.begin() + (size_t)f * nseg, segp.begin() + (size_t)(f + 1) * nseg,
+                          segment_power_w + k * nseg);
+            // Conductor peaks: segments are contiguous in filament order, so
+            // the first strictly larger segment peak is the reference's
+            // first filament of largest |J|.
+            std::vector<double> best((size_t)ncond, -1.0);
+            std::vector<int64_t> at((size_t)ncond, -1);
+            double dissipated = 0.0;
+            for (int64_t g = 0; g < nseg; ++g) {
+                const size_t t = (size_t)(f * nseg + g);
+                dissipated += segp[t];
+                const int64_t c = sys->conductor_of_segment[(size_t)g];
+                if (segi[t] >= 0 && (at[(size_t)c] < 0 || segpk[t] > best[(size_t)c])) {
+                    best[(size_t)c] = segpk[t];
+                    at[(size_t)c] = segi[t];
+                }
+            }
+            if (conductor_peak_filament) std::copy(at.begin(), at.end(), conductor_peak_filament + k * ncond);
+            if (conductor_peak_density) std::copy(best.begin(), best.end(), conductor_peak_density + k * ncond);
+            if (balance) {
+                // V_p = Z I_p; input = 1/2 Re(I_p^H V_p).
+                double input = 0.0;
+                for (int64_t a = 0; a < p; ++a) {
+                    C v(0.0, 0.0);
+                    for (int64_t b = 0; b < p; ++b) {
+                        const size_t zi = (size_t)(2 * (f * p * p + a * p + b));
+                        v += C(z[zi], z[zi + 1]) * C(excitation[2 * b], excitation[2 * b + 1]);
+                    }
+                    input += (std::conj(C(excitation[2 * a], excitation[2 * a + 1])) * v).real();
+                }
+                input *= 0.5;
+                const double scale = std::max(dissipated, input);
+                balance[k] = fh_power_balance{dissipated, input, scale > 0.0 ? std::fabs(dissipated - input) / scale : 0.0};
+            }
+        }
+    }
+    return FH_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -110,6 +110,18 @@ fh_status gradient_products(const double *d_Dw, const double *d_Dh, int64_t n, c
                             double *d_part, cudaStream_t stream, fh_error_info *err);
 size_t gradient_part_elems(int64_t n, int p);
 
+// Branch currents, |J|, power per filament and per-segment sums / peaks for
+// `count` frequencies from X = Z_ee^-1 Z_ep (count x p x m complex) and the
+// excitation d_ip (p complex).  The transposed loop basis lists, per branch,
+// (loop, sign) in increasing loop order; d_whr holds (w, h, R) per filament,
+// d_first the first filament of each segment (nseg + 1).  Outputs are count x
+// n (complex / real) and count x nseg.
+fh_status launch_currents(const double *d_x, const double *d_ip, int64_t m, int p, int64_t n, int count,
+                          const int64_t *d_col_ptr, const int32_t *d_col_loop, const double *d_col_sign,
+                          const double *d_whr, const int64_t *d_first, int64_t nseg, double *d_ib, double *d_dens,
+                          double *d_pow, double *d_seg_cur, double *d_seg_pow, double *d_seg_peak,
+                          int64_t *d_seg_idx, cudaStream_t s, fh_error_info *err);
+
 // R_m = M diag(R) M^T and L_m = M L M^T (loops x loops, column-major), upper
 // triangle evaluated in the reference's order and mirrored.
 // h_row_ptr: the same row pointers on the host (long rows take their own kernel).

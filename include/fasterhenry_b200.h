@@ -300,6 +300,45 @@ fh_status fh_batch_sweep(fh_system *const *systems, size_t k, const double *cons
 fh_status fh_impedance(fh_system *sys, double frequency_hz, fh_precision precision, double *z_out,
                        fh_error_info *err);
 
+/* ---- filament currents and power (currents.rs) -------------------------- */
+
+/* Layout, currents.rs:128-170: the segment of every filament (n), the
+ * conductor (connected component of the segment graph, numbered by first
+ * segment) of every segment (n_segments), and the conductor count. */
+fh_status fh_system_layout(const fh_system *sys, int64_t *segment_of_filament, int64_t *conductor_of_segment,
+                           int64_t *conductor_count);
+
+/* PowerBalance, currents.rs:97-106 (time-average power of peak phasors). */
+typedef struct fh_power_balance {
+    double dissipated_w;
+    double input_w;
+    double relative_residual;
+} fh_power_balance;
+
+/* MeshSystem::currents (solve.rs:845-868 with currents.rs:172-274) at nf
+ * frequencies for one port-current excitation (p complex phasors, peak
+ * amperes): internal loop currents -Z_ee^-1 Z_ep I_p, branch currents
+ * M^T [I_e; I_p], |J| = |I| / (w h) and P = |I|^2 R / 2 per filament, sums
+ * per segment, the filament of largest |J| per conductor (first in filament
+ * order on ties), and the power balance against 1/2 Re(I_p^H V_p).  The
+ * frequencies are factorized in batches as by fh_sweep (precision as there).
+ * Every output is optional (NULL):
+ *   filament_current   nf x n complex (interleaved)
+ *   current_density    nf x n (A/m^2)
+ *   power_w            nf x n
+ *   segment_current    nf x n_segments complex
+ *   segment_power_w    nf x n_segments
+ *   conductor_peak_filament, conductor_peak_density   nf x conductors
+ *   balance            nf
+ * Errors: FH_ERR_INVALID_FREQUENCY (first bad index), FH_ERR_INVALID_EXCITATION
+ * (a non-finite entry; index_a = the port count, index_b = the entries
+ * given), FH_ERR_SINGULAR. */
+fh_status fh_currents(fh_system *sys, const double *frequencies_hz, size_t nf, const double *excitation,
+                      size_t n_excitation, fh_precision precision, double *filament_current, double *current_density,
+                      double *power_w, double *segment_current, double *segment_power_w,
+                      int64_t *conductor_peak_filament, double *conductor_peak_density, fh_power_balance *balance,
+                      fh_error_info *err);
+
 /* ---- impedance gradient (no reference counterpart) --------------------- */
 
 /* A geometric parameter: the width or the thickness of segment `index`, or a

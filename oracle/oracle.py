@@ -341,3 +341,69 @@ class System:
 
     def sweep(self, frequencies: Sequence[float]) -> np.ndarray:
         return np.stack([self.impedance(f) for f in frequencies])
+
+
+def currents(deck, frequency: float, excitation, threads: Optional[int] = None) -> dict:
+    """Filament currents, densities, powers, segment sums, conductor peaks and
+    the power balance at one frequency (MeshSystem::currents, solve.rs:
+    1110-1149, with currents.rs:128-274), restated with numpy on the
+    oracle's own matrices and LU."""
+    system = System(deck, threads)
+    R, L = system.blocks()
+    fil = system.filaments()
+    m, p = system.counts["internal_meshes"], system.counts["ports"]
+    w = 2 * np.pi * frequency
+    Z = R + 1j * w * L
+    ee, ep, pp = Z[:m, :m], Z[:m, m:], Z[m:, m:]
+    current = np.asarray(excitation, dtype=np.complex128)
+    internal = -lu_solve(ee, ep @ current) if m else np.zeros(0, dtype=np.complex128)
+    voltage = pp @ current + ep.T @ internal
+    fil_all, per = discretize(deck)
+    row_ptr, cols, signs, _ = mesh(deck, per)
+    branch = np.zeros(len(fil), dtype=np.complex128)
+    loops = np.concatenate([internal, current])
+    for i, x in enumerate(loops):  # currents.rs:183-190: row by row
+        for k in range(row_ptr[i], row_ptr[i + 1]):
+            branch[cols[k]] += x * signs[k]
+    # Layout, currents.rs:137-170.
+    nodes = len(deck.nodes)
+    parent = list(range(nodes))
+
+    def find(x):
+        while parent[x] != x:
+            parent[x] = parent[parent[x]]
+            x = parent[x]
+        return x
+    for sd in deck.segments:
+        a, b = find(sd["a"]), find(sd["b"])
+        if a != b:
+            parent[a] = b
+    roots, cond_of_seg = [], []
+    for sd in deck.segments:
+        r = find(sd["a"])
+        if r not in roots:
+            roots.append(r)
+        cond_of_seg.append(roots.index(r))
+    seg_of_fil = np.repeat(np.arange(len(per)), per)
+    res = fil[:, 6] / (fil[:, 18] * (fil[:, 16] * fil[:, 17]))
+    density = np.abs(branch) / (fil[:, 16] * fil[:, 17])
+    power = 0.5 * (branch.real ** 2 + branch.imag ** 2) * res
+    seg_cur = np.zeros(len(per), dtype=np.complex128)
+    seg_pow = np.zeros(len(per))
+    peaks = [None] * len(roots)
+    dissipated = 0.0
+    for k in range(len(fil)):
+        s = seg_of_fil[k]
+        dissipated += power[k]
+        seg_cur[s] += branch[k]
+        seg_pow[s] += power[k]
+        c = cond_of_seg[s]
+        if peaks[c] is None or density[k] > peaks[c][0]:
+            peaks[c] = (density[k], k)
+    inp = 0.5 * float(np.sum((np.conj(current) * voltage).real))
+    scale = max(dissipated, inp)
+    return {"current": branch, "density": density, "power": power, "segment_current": seg_cur,
+            "segment_power": seg_pow, "peak_filament": np.array([pk[1] for pk in peaks]),
+            "peak_density": np.array([pk[0] for pk in peaks]), "conductor_of_segment": np.array(cond_of_seg),
+            "balance": {"dissipated_w": dissipated, "input_w": inp,
+                        "relative_residual": abs(dissipated - inp) / scale if scale > 0 else 0.0}}

@@ -16,5 +16,6 @@ from .api import (GmresOutcome, GmresParams, IterativeParams, IterativeSystem, P
                   Profiler, batch_sweep, fill_stats, gmres_dense)
 from .api import GradientResult, Param, inductance_gradient, release_cached_memory
 from .api import CURRENTS_CSV_HEADER, CurrentSolution, InvalidExcitation, unit_excitation
+from .api import DEFAULT_GROUP, Coupling, CouplingError, TruncationWarning
 
 __version__ = "0.1.0"

@@ -121,6 +121,7 @@ ERR_SINGULAR = 17
 ERR_NOT_CONVERGED = 18
 ERR_PFFT = 19
 ERR_INVALID_EXCITATION = 20
+ERR_COUPLING = 21
 ERR_UNSUPPORTED = 30
 
 EXPORTS = [
@@ -133,7 +134,7 @@ EXPORTS = [
     "fh_pfft_destroy", "fh_gmres_default_params", "fh_iterative_create", "fh_iterative_counts", "fh_iterative_timing",
     "fh_iterative_pfft_stats", "fh_iterative_sweep", "fh_iterative_destroy", "fh_test_gmres_dense",
     "fh_batch_sweep", "fh_gradient", "fh_test_inductance_gradient", "fh_release_cached_memory",
-    "fh_system_layout", "fh_currents",
+    "fh_system_layout", "fh_currents", "fh_system_create_coupled", "fh_system_coupling",
 ]
 
 PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner",
@@ -144,7 +145,19 @@ class FillStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int64) for k in ("pairs", "orthogonal", "point_quadrature", "closed_form",
                                               "aligned_quadrature", "sampled", "distinct_aligned_keys")] + \
                [(k, ctypes.c_double) for k in ("point_evaluations", "ms_classify", "ms_point", "ms_closed_form",
-                                               "ms_aligned_quadrature", "ms_sampled", "ms_congruence")]
+                                               "ms_aligned_quadrature", "ms_sampled", "ms_congruence")] + \
+               [("truncated", ctypes.c_int64)]
+
+
+class CouplingSpec(ctypes.Structure):
+    _fields_ = [("segment_groups", ctypes.POINTER(ctypes.c_char_p)), ("n_segment_groups", ctypes.c_size_t),
+                ("truncate", ctypes.c_int32), ("couples", ctypes.POINTER(ctypes.c_char_p)),
+                ("n_couples", ctypes.c_size_t)]
+
+
+class TruncationWarning(ctypes.Structure):
+    _fields_ = [("group_a", ctypes.c_int64), ("group_b", ctypes.c_int64), ("separation", ctypes.c_double),
+                ("extent", ctypes.c_double)]
 
 _lib = None
 
@@ -199,6 +212,9 @@ def load():
                               P(GradientReport), ei]
     L.fh_test_inductance_gradient.argtypes = [P(Filament), c_double_p, sz, c_double_p, c_double_p, ei]
     L.fh_system_layout.argtypes = [ctypes.c_void_p, c_int64_p, c_int64_p, c_int64_p]
+    L.fh_system_create_coupled.argtypes = [P(Node), sz, P(SegmentDef), sz, P(Port), sz, P(Discretization),
+                                           P(CouplingSpec), ctypes.c_int, P(ctypes.c_void_p), ei]
+    L.fh_system_coupling.argtypes = [ctypes.c_void_p, c_int64_p, c_int64_p, P(TruncationWarning), sz, P(sz)]
     L.fh_currents.argtypes = [ctypes.c_void_p, c_double_p, sz, c_double_p, sz, ctypes.c_int, c_double_p, c_double_p,
                               c_double_p, c_double_p, c_double_p, c_int64_p, c_double_p, P(PowerBalance), ei]
     L.fh_system_destroy.argtypes = [ctypes.c_void_p]

@@ -108,6 +108,17 @@ class NotConverged(FasterHenryError):
     status = N.ERR_NOT_CONVERGED
 
 
+class CouplingError(FasterHenryError):
+    """SolveError::Coupling(CouplingError) (coupling.rs:93-130): ``kind`` is
+    "unknown_group", "segment_count_mismatch" or "non_transitive"."""
+    status = N.ERR_COUPLING
+
+    @property
+    def kind(self) -> str:
+        return {1: "unknown_group", 2: "segment_count_mismatch", 3: "non_transitive"}.get(
+            int(self.info.detail) if self.info else 0, "")
+
+
 class InvalidExcitation(FasterHenryError):
     """SolveError::InvalidExcitation{expected, got} (solve.rs:592-599)."""
     status = N.ERR_INVALID_EXCITATION
@@ -136,7 +147,8 @@ class InvalidArgument(FasterHenryError, ValueError):
 
 _ERRORS = {c.status: c for c in (NoDevice, CudaError, OutOfMemory, GeometryError, DiscretizeError, CoincidentSamples,
                                  NotFinite, MeshError, InvalidGrading, InvalidFrequency, Singular, NotConverged,
-                                 Unsupported, InvalidArgument, PfftError, InvalidExcitation)}
+                                 Unsupported, InvalidArgument, PfftError, InvalidExcitation,
+                                 CouplingError)}
 
 
 def _check(status: int, info: Optional[N.ErrorInfo] = None) -> None:
@@ -513,15 +525,41 @@ class MeshSystem:
 
     @classmethod
     def assemble(cls, geometry, ports: Sequence, discretization: dict,
-                 solver: SolverChoice = SolverChoice.DENSE) -> "MeshSystem":
+                 solver: SolverChoice = SolverChoice.DENSE, coupling: Optional["Coupling"] = None) -> "MeshSystem":
+        """MeshSystem::assemble, or assemble_with_coupling (solve.rs:680-766)
+        when ``coupling`` is given."""
         nodes, segs = _geom_arrays(geometry)
         pts = _ports(ports)
         disc, keep = _disc(discretization)
         h = ctypes.c_void_p()
         info = N.ErrorInfo()
-        _check(N.load().fh_system_create(nodes, len(geometry.nodes), segs, len(geometry.segments), pts, len(ports),
-                                         ctypes.byref(disc), int(solver), ctypes.byref(h), ctypes.byref(info)), info)
-        return cls(h, geometry, ports)
+        spec, hold = (coupling._spec() if coupling is not None else (None, None))
+        _check(N.load().fh_system_create_coupled(nodes, len(geometry.nodes), segs, len(geometry.segments), pts,
+                                                 len(ports), ctypes.byref(disc),
+                                                 ctypes.byref(spec) if spec is not None else None, int(solver),
+                                                 ctypes.byref(h), ctypes.byref(info)), info)
+        out = cls(h, geometry, ports)
+        out.coupling = coupling if coupling is not None else Coupling.all_pairs()
+        return out
+
+    def kept_pairs(self) -> Tuple[int, int]:
+        """(kept, total) filament pairs of the fill: PairMask::kept_pairs and
+        total_pairs (inductance/batch.rs:88-117)."""
+        kept, total = ctypes.c_int64(), ctypes.c_int64()
+        _check(N.load().fh_system_coupling(self._h, ctypes.byref(kept), ctypes.byref(total), None, 0, None))
+        return int(kept.value), int(total.value)
+
+    def truncation_warnings(self) -> List["TruncationWarning"]:
+        """Truncated group pairs closer than their extent
+        (Coupling::truncation_warnings, coupling.rs:285-318)."""
+        count = ctypes.c_size_t()
+        L = N.load()
+        _check(L.fh_system_coupling(self._h, None, None, None, 0, ctypes.byref(count)))
+        buf = (N.TruncationWarning * max(1, count.value))()
+        _check(L.fh_system_coupling(self._h, None, None, buf, count.value, ctypes.byref(count)))
+        names = getattr(self, "coupling", Coupling.all_pairs()).group_names(self._counts["segments"])
+        return [TruncationWarning((names[buf[k].group_a], names[buf[k].group_b]), buf[k].separation, buf[k].extent)
+                for k in range(count.value)]
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -656,6 +694,100 @@ class MeshSystem:
         return GradientResult(float(frequency), params, z, dz[:len(params)],
                               {k: (int(getattr(rep, k)) if k == "pairs" else float(getattr(rep, k)))
                                for k, _ in N.GradientReport._fields_})
+
+
+DEFAULT_GROUP = ""
+
+
+class Coupling:
+    """Segment group names and the group pairs whose mutual inductance is
+    kept (Coupling, coupling.rs:150-283).  ``Coupling.all_pairs()`` keeps
+    everything; ``Coupling.truncated(groups)`` keeps each group with itself
+    and the pairs declared with ``coupled``, and the fill never evaluates the
+    rest (they are zero in L).  Validation (unknown groups, too many tags,
+    non-transitive declarations) happens at assembly (CouplingError)."""
+
+    def __init__(self, segment_groups: Optional[Sequence[str]] = None, couples: Optional[List[Tuple[str, str]]] = None):
+        self.segment_groups = list(segment_groups or [])
+        self._couples = None if couples is None else [tuple(c) for c in couples]
+
+    @classmethod
+    def all_pairs(cls) -> "Coupling":
+        return cls()
+
+    @classmethod
+    def truncated(cls, segment_groups: Sequence[str]) -> "Coupling":
+        return cls(segment_groups, [])
+
+    def coupled(self, a: str, b: str) -> "Coupling":
+        return Coupling(self.segment_groups, (self._couples or []) + [(a, b)])
+
+    def is_all_pairs(self) -> bool:
+        return self._couples is None
+
+    def is_trivial(self) -> bool:
+        return not self.segment_groups and self._couples is None
+
+    def group_of(self, index: int) -> str:
+        return self.segment_groups[index] if index < len(self.segment_groups) else DEFAULT_GROUP
+
+    def couples(self, a: str, b: str) -> bool:
+        if self._couples is None or a == b:
+            return True
+        return any((x == a and y == b) or (x == b and y == a) for x, y in self._couples)
+
+    def group_names(self, segment_count: int) -> List[str]:
+        """Group names in order of first appearance over the segments."""
+        names: List[str] = []
+        for k in range(segment_count):
+            g = self.group_of(k)
+            if g not in names:
+                names.append(g)
+        return names
+
+    def to_json(self) -> dict:
+        """The serde form of the reference (coupling.rs:166-175): absent
+        fields are the defaults, so all_pairs() is ``{}``."""
+        d: dict = {}
+        if self.segment_groups:
+            d["segment_groups"] = list(self.segment_groups)
+        if self._couples is not None:
+            d["couples"] = [list(c) for c in self._couples]
+        return d
+
+    @classmethod
+    def from_json(cls, d: dict) -> "Coupling":
+        unknown = set(d) - {"segment_groups", "couples"}
+        if unknown:
+            raise InvalidArgument("unknown coupling field(s): %s" % ", ".join(sorted(unknown)))
+        couples = d.get("couples")
+        return cls(d.get("segment_groups", []), None if couples is None else [tuple(c) for c in couples])
+
+    def __eq__(self, other) -> bool:
+        return isinstance(other, Coupling) and self.to_json() == other.to_json()
+
+    def _spec(self):
+        enc = [g.encode() for g in self.segment_groups]
+        groups = (ctypes.c_char_p * max(1, len(enc)))(*enc)
+        flat = [x.encode() for c in (self._couples or []) for x in c]
+        pairs = (ctypes.c_char_p * max(1, len(flat)))(*flat)
+        spec = N.CouplingSpec(groups, len(enc), 0 if self._couples is None else 1, pairs, len(self._couples or []))
+        return spec, (enc, groups, flat, pairs)
+
+
+@dataclasses.dataclass
+class TruncationWarning:
+    """A truncated group pair closer than one extent (coupling.rs:132-160)."""
+    groups: Tuple[str, str]
+    separation: float
+    extent: float
+
+    def __str__(self) -> str:
+        name = lambda g: "(default)" if g == "" else "'%s'" % g
+        ratio = self.separation / self.extent if self.extent > 0 else float("inf")
+        return ("mutual inductance between groups %s and %s is truncated, but they are only %.3e m apart — %.2fx "
+                "their %.3e m extent; truncation is justified from about 10x"
+                % (name(self.groups[0]), name(self.groups[1]), self.separation, ratio, self.extent))
 
 
 CURRENTS_CSV_HEADER = ("frequency_hz,filament,segment,conductor,x_m,y_m,z_m,"

@@ -74,6 +74,22 @@ struct fh_system {
     // transposed loop basis and per-filament (w, h, R) on the device.
     std::vector<int64_t> segment_of_filament, conductor_of_segment, segment_first;
     int64_t conductors = 0;
+    // Coupling (coupling.rs): resolved groups, warnings, kept pairs, and the
+    // device mask when it truncates.
+    CouplingResolved coupling;
+    std::vector<fh_truncation_warning> warnings;
+    int64_t kept_pairs = 0, total_pairs = 0;
+    int32_t *d_group = nullptr;
+    uint8_t *d_coupled = nullptr;
+    PairMaskDev mask() const {
+        PairMaskDev m;
+        if (coupling.all_pairs) return m;
+        m.group = d_group;
+        m.coupled = d_coupled;
+        m.groups = (int32_t)coupling.groups();
+        m.dropped = total_pairs - kept_pairs;
+        return m;
+    }
     int64_t *d_col_ptr = nullptr, *d_first = nullptr;
     int32_t *d_col_loop = nullptr;
     double *d_col_sign = nullptr, *d_whr = nullptr;
@@ -90,6 +106,8 @@ struct fh_system {
         cache_free(d_col_loop, stream);
         cache_free(d_col_sign, stream);
         cache_free(d_whr, stream);
+        cache_free(d_group, stream);
+        cache_free(d_coupled, stream);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -601,6 +619,25 @@ fh_status fh_lu_solve_c64(const double *a, size_t n, const double *b, size_t nrh
 fh_status fh_system_create(const fh_node *nodes, size_t n_nodes, const fh_segment_def *segments, size_t n_segments,
                            const fh_port *ports, size_t n_ports, const fh_discretization *disc,
                            fh_solver_choice choice, fh_system **out, fh_error_info *err) {
+    return fh_system_create_coupled(nodes, n_nodes, segments, n_segments, ports, n_ports, disc, nullptr, choice, out,
+                                    err);
+}
+
+fh_status fh_system_coupling(const fh_system *sys, int64_t *kept_pairs, int64_t *total_pairs,
+                             fh_truncation_warning *warnings, size_t capacity, size_t *count) {
+    if (!sys) return fail(nullptr, FH_ERR_INVALID_ARGUMENT, "null system");
+    if (kept_pairs) *kept_pairs = sys->kept_pairs;
+    if (total_pairs) *total_pairs = sys->total_pairs;
+    if (count) *count = sys->warnings.size();
+    if (warnings)
+        for (size_t k = 0; k < std::min(capacity, sys->warnings.size()); ++k) warnings[k] = sys->warnings[k];
+    return FH_OK;
+}
+
+fh_status fh_system_create_coupled(const fh_node *nodes, size_t n_nodes, const fh_segment_def *segments,
+                                   size_t n_segments, const fh_port *ports, size_t n_ports,
+                                   const fh_discretization *disc, const fh_coupling *coupling,
+                                   fh_solver_choice choice, fh_system **out, fh_error_info *err) {
     clear_error(err);
     if (!out) return fail(err, FH_ERR_INVALID_ARGUMENT, "null output handle");
     *out = nullptr;
@@ -610,7 +647,13 @@ fh_status fh_system_create(const fh_node *nodes, size_t n_nodes, const fh_segmen
     s->segments.assign(segments, segments + n_segments);
     if (n_ports && !ports) return fail(err, FH_ERR_INVALID_ARGUMENT, "null ports");
     s->ports.assign(ports, ports + n_ports);
-    fh_status st = discretize_geometry(nodes, n_nodes, segments, n_segments, disc, s->disc, err);
+    // The coupling is checked before anything is paid for (solve.rs:710-712).
+    fh_status st = validate_geometry(nodes, n_nodes, segments, n_segments, err);
+    if (st) return st;
+    st = resolve_coupling(coupling, n_segments, s->coupling, err);
+    if (st) return st;
+    s->warnings = coupling_warnings(s->coupling, nodes, segments, n_segments);
+    st = discretize_geometry(nodes, n_nodes, segments, n_segments, disc, s->disc, err);
     if (st) return st;
     st = build_loops(segments, n_segments, n_nodes, s->disc.per_segment.data(), ports, n_ports, s->loops, err);
     if (st) return st;
@@ -654,8 +697,25 @@ fh_status fh_system_create(const fh_node *nodes, size_t n_nodes, const fh_segmen
     FHB_CUDA(cudaMemcpyAsync(d_br.p, s->loops.branch.data(), s->loops.branch.size() * 4, cudaMemcpyHostToDevice, cs));
     FHB_CUDA(cudaMemcpyAsync(d_sign.p, s->loops.sign.data(), s->loops.sign.size() * 8, cudaMemcpyHostToDevice, cs));
     FHB_CUDA(cudaMemsetAsync(d_L.p, 0, (size_t)n * n * 8, cs));
+    s->total_pairs = n * (n + 1) / 2;
+    s->kept_pairs = coupling_kept_pairs(s->coupling, s->disc.per_segment.data(), n_segments);
+    if (!s->coupling.all_pairs) {
+        std::vector<int32_t> group;
+        group.reserve((size_t)n);
+        for (size_t g = 0; g < n_segments; ++g)
+            for (int64_t k = 0; k < s->disc.per_segment[g]; ++k) group.push_back(s->coupling.of_segment[g]);
+        const size_t tb = s->coupling.couples.size();
+        if (cache_alloc((void **)&s->d_group, 4 * group.size(), cs) != cudaSuccess ||
+            cache_alloc((void **)&s->d_coupled, std::max<size_t>(tb, 1), cs) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(err, FH_ERR_OUT_OF_MEMORY, "device allocation of the coupling mask failed");
+        }
+        FHB_CUDA(cudaMemcpyAsync(s->d_group, group.data(), 4 * group.size(), cudaMemcpyHostToDevice, cs));
+        FHB_CUDA(cudaMemcpyAsync(s->d_coupled, s->coupling.couples.data(), tb, cudaMemcpyHostToDevice, cs));
+    }
+    const PairMaskDev pm = s->mask();
     const double t1 = wall();
-    st = device_fill(d_fil.p, n, d_L.p, nullptr, cs, &s->fill, err);
+    st = device_fill(d_fil.p, n, d_L.p, nullptr, cs, &s->fill, err, &pm);
     if (st) return st;
     FHB_CUDA(cudaStreamSynchronize(cs));
     const double t2 = wall();
@@ -740,6 +800,7 @@ fh_status fh_system_fill_stats(const fh_system *sys, fh_fill_stats *o) {
     o->ms_aligned_quadrature = f.ms_quadrature;
     o->ms_sampled = f.ms_sampled;
     o->ms_congruence = sys->ms_congruence;
+    o->truncated = f.truncated;
     return FH_OK;
 }
 
@@ -1269,7 +1330,8 @@ fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *
     } evg{ev};
     FillStats fs;
     FHB_CUDA(cudaEventRecord(ev[0], st));
-    e = device_fill_grad(d_fil.p, d_tan.p, n, GradOut{d_D.p, d_D.p + n * n}, st, &fs, err);
+    const PairMaskDev pm = sys->mask();
+    e = device_fill_grad(d_fil.p, d_tan.p, n, GradOut{d_D.p, d_D.p + n * n}, st, &fs, err, &pm);
     if (e) return e;
     FHB_CUDA(cudaEventRecord(ev[1], st));
     e = gradient_products(d_D.p, d_D.p + n * n, n, d_I.p, (int)p, d_y.p, d_part.p, st, err);

@@ -73,12 +73,22 @@ struct ProfSuppress {
 // caller).  `d_methods` optional (n*n int8).  `stream` orders the work.
 struct FillStats {
     int64_t pairs = 0, orthogonal = 0, point = 0, closed_form = 0, aligned_quadrature = 0, sampled = 0;
+    int64_t truncated = 0;
     int64_t unique_aligned = 0;
     double point_evaluations = 0.0;
     float ms_classify = 0, ms_point = 0, ms_aligned = 0, ms_quadrature = 0, ms_sampled = 0;
 };
+// A coupling's pair mask on the device (PairMask, inductance/batch.rs:37-117):
+// the group of every filament and the groups x groups table of kept pairs.
+// Pairs of uncoupled groups are never evaluated and stay zero.
+struct PairMaskDev {
+    const int32_t *group = nullptr;
+    const uint8_t *coupled = nullptr;
+    int32_t groups = 0;
+    int64_t dropped = 0;  // pairs the mask drops (for the statistics)
+};
 fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_methods, cudaStream_t stream,
-                      FillStats *stats, fh_error_info *err);
+                      FillStats *stats, fh_error_info *err, const PairMaskDev *mask = nullptr);
 // The same evaluation for an explicit list of filament pairs: d_out[k] =
 // L(pairs[k].x, pairs[k].y), zero for orthogonal pairs.
 fh_status device_fill_pairs(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t n_pairs, double *d_out,
@@ -101,7 +111,7 @@ struct GradOut {
 // Pairs evaluated by sampled filaments (non-aligned parallel or skew bars)
 // have no derivative here: FH_ERR_UNSUPPORTED.
 fh_status device_fill_grad(const DevFil *d_fil, const FilTan *d_tan, int64_t n, GradOut out, cudaStream_t stream,
-                           FillStats *stats, fh_error_info *err);
+                           FillStats *stats, fh_error_info *err, const PairMaskDev *mask = nullptr);
 
 // y = D_w I and D_h I for p complex vectors I (n x p, column q at 2 q n):
 // y holds 2 x p columns (D_w's products first).  d_part is scratch of

@@ -256,7 +256,7 @@ template <bool kWrite>
 __global__ void __launch_bounds__(256) classify_kernel(const DevFil *__restrict__ fil, int n,
                                                        unsigned long long *__restrict__ counts,
                                                        unsigned long long *__restrict__ cursor,
-                                                       int4 *__restrict__ items) {
+                                                       int4 *__restrict__ items, PairMaskDev mask) {
     const int ti = blockIdx.y, tj = blockIdx.x;
     if (ti > tj) return;
     __shared__ DevFil s_i[32], s_j[32];
@@ -282,7 +282,8 @@ __global__ void __launch_bounds__(256) classify_kernel(const DevFil *__restrict_
     for (int r = 0; r < 4; ++r) {
         const int i = ti * 32 + threadIdx.y + 8 * r;
         cls[r].cat = -1;
-        if (i < n && j < n && i <= j) {
+        if (i < n && j < n && i <= j &&
+            (!mask.group || mask.coupled[(int64_t)mask.group[i] * mask.groups + mask.group[j]])) {
             cls[r] = classify(s_i[threadIdx.y + 8 * r], s_j[threadIdx.x]);
             if (cls[r].cat >= 0) slot[r] = atomicAdd(&s_count[cls[r].cat], 1u);
         }
@@ -1374,8 +1375,12 @@ namespace {
 // d_L[k] (pair-list mode: orthogonal pairs are zero).
 fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t n_pairs, double *d_L,
                    int8_t *d_methods, cudaStream_t stream, FillStats *stats, fh_error_info *err,
-                   const FilTan *d_tan = nullptr, const GradOut *grad = nullptr) {
+                   const FilTan *d_tan = nullptr, const GradOut *grad = nullptr,
+                   const PairMaskDev *mask = nullptr) {
     const bool list = d_pairs != nullptr;
+    if (mask && mask->group && list) return fail(err, FH_ERR_INVALID_ARGUMENT, "the pair-list fill takes no mask");
+    const PairMaskDev no_mask;
+    const PairMaskDev &pm = mask ? *mask : no_mask;
     if (grad && list) return fail(err, FH_ERR_INVALID_ARGUMENT, "the derivative fill has no pair-list mode");
     if (list ? n_pairs == 0 : n == 0) return FH_OK;
     if (n > 2000000000LL / 32) return fail(err, FH_ERR_INVALID_ARGUMENT, "too many filaments for the fill");
@@ -1432,7 +1437,7 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
         classify_list_kernel<false><<<list_blocks, 256, 0, stream>>>(d_fil, d_pairs, n_pairs, d_counts, nullptr,
                                                                       nullptr);
     else
-        classify_kernel<false><<<grid, block, 0, stream>>>(d_fil, (int)n, d_counts, nullptr, nullptr);
+        classify_kernel<false><<<grid, block, 0, stream>>>(d_fil, (int)n, d_counts, nullptr, nullptr, pm);
     FHB_CUDA(cudaGetLastError());
     unsigned long long counts[kCats];
     FHB_CUDA(cudaMemcpyAsync(counts, d_counts, sizeof counts, cudaMemcpyDeviceToHost, stream));
@@ -1448,7 +1453,7 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
         classify_list_kernel<true><<<list_blocks, 256, 0, stream>>>(d_fil, d_pairs, n_pairs, nullptr, d_cursor,
                                                                      d_items);
     else
-        classify_kernel<true><<<grid, block, 0, stream>>>(d_fil, (int)n, nullptr, d_cursor, d_items);
+        classify_kernel<true><<<grid, block, 0, stream>>>(d_fil, (int)n, nullptr, d_cursor, d_items, pm);
     FHB_CUDA(cudaGetLastError());
     FHB_CUDA(cudaEventRecord(ev[1], stream));
     const int sms = 148;
@@ -1577,7 +1582,8 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
     DevError h_err;
     FHB_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof h_err, cudaMemcpyDeviceToHost, stream));
     FHB_CUDA(cudaStreamSynchronize(stream));
-    st.orthogonal = st.pairs - (int64_t)total_items;
+    st.truncated = pm.group ? pm.dropped : 0;
+    st.orthogonal = st.pairs - (int64_t)total_items - st.truncated;
     cudaEventElapsedTime(&st.ms_classify, ev[0], ev[1]);
     cudaEventElapsedTime(&st.ms_point, ev[1], ev[2]);
     cudaEventElapsedTime(&st.ms_aligned, ev[2], ev[3]);
@@ -1601,8 +1607,8 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
 }  // namespace
 
 fh_status device_fill(const DevFil *d_fil, int64_t n, double *d_L, int8_t *d_methods, cudaStream_t stream,
-                      FillStats *stats, fh_error_info *err) {
-    return fill_run(d_fil, n, nullptr, 0, d_L, d_methods, stream, stats, err);
+                      FillStats *stats, fh_error_info *err, const PairMaskDev *mask) {
+    return fill_run(d_fil, n, nullptr, 0, d_L, d_methods, stream, stats, err, nullptr, nullptr, mask);
 }
 
 fh_status device_fill_pairs(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t n_pairs, double *d_out,
@@ -1611,9 +1617,9 @@ fh_status device_fill_pairs(const DevFil *d_fil, int64_t n, const int2 *d_pairs,
 }
 
 fh_status device_fill_grad(const DevFil *d_fil, const FilTan *d_tan, int64_t n, GradOut out, cudaStream_t stream,
-                           FillStats *stats, fh_error_info *err) {
+                           FillStats *stats, fh_error_info *err, const PairMaskDev *mask) {
     if (!d_tan || !out.Dw || !out.Dh) return fail(err, FH_ERR_INVALID_ARGUMENT, "null derivative-fill argument");
-    return fill_run(d_fil, n, nullptr, 0, nullptr, nullptr, stream, stats, err, d_tan, &out);
+    return fill_run(d_fil, n, nullptr, 0, nullptr, nullptr, stream, stats, err, d_tan, &out, mask);
 }
 
 fh_status device_congruence(const double *d_L, const double *d_R, int64_t n, const int64_t *d_row_ptr,

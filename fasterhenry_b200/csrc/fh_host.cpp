@@ -3,6 +3,8 @@
 // Nothing here touches the device.  Compiled with -ffp-contract=off so that
 // the filaments are the reference's bit for bit (same operations, same order).
 #include <algorithm>
+#include <array>
+#include <functional>
 #include <charconv>
 #include <cmath>
 #include <cstdarg>
@@ -581,6 +583,139 @@ fh_status emit(const std::string &s, char *buf, size_t capacity, size_t *length)
 }
 
 }  // namespace
+
+// Coupling::resolve (coupling.rs:323-380) with check_transitive (:382-430).
+fh_status resolve_coupling(const fh_coupling *c, size_t n_segs, CouplingResolved &out, fh_error_info *err) {
+    out = CouplingResolved();
+    const bool truncate = c && c->truncate;
+    const size_t tags = c ? c->n_segment_groups : 0;
+    if (tags && !c->segment_groups) return fail(err, FH_ERR_INVALID_ARGUMENT, "null coupling group list");
+    if (c && c->n_couples && !c->couples) return fail(err, FH_ERR_INVALID_ARGUMENT, "null coupling pair list");
+    if (tags > n_segs)
+        return fail(err, FH_ERR_COUPLING,
+                    fmt("coupling names %zu segment groups, but the geometry has %zu segments", tags, n_segs),
+                    (int64_t)n_segs, (int64_t)tags, 0.0, FH_COUPLING_SEGMENT_COUNT_MISMATCH);
+    auto group_of = [&](size_t s) -> std::string {
+        if (s >= tags || !c->segment_groups[s]) return std::string();
+        return std::string(c->segment_groups[s]);
+    };
+    for (size_t s = 0; s < n_segs; ++s) {
+        const std::string name = group_of(s);
+        auto it = std::find(out.names.begin(), out.names.end(), name);
+        if (it == out.names.end()) {
+            out.names.push_back(name);
+            out.of_segment.push_back((int32_t)out.names.size() - 1);
+        } else {
+            out.of_segment.push_back((int32_t)(it - out.names.begin()));
+        }
+    }
+    const size_t g = out.names.size();
+    out.couples.assign(g * g, 0);
+    for (size_t k = 0; k < g; ++k) out.couples[k * g + k] = 1;
+    out.all_pairs = !truncate;
+    if (truncate) {
+        for (size_t k = 0; k < c->n_couples; ++k) {
+            int64_t ab[2];
+            for (int e = 0; e < 2; ++e) {
+                const char *nm = c->couples[2 * k + e];
+                const std::string name = nm ? nm : "";
+                auto it = std::find(out.names.begin(), out.names.end(), name);
+                if (it == out.names.end())
+                    return fail(err, FH_ERR_COUPLING,
+                                "coupling declares group '" + name + "', which no segment belongs to", (int64_t)k,
+                                -1, 0.0, FH_COUPLING_UNKNOWN_GROUP);
+                ab[e] = it - out.names.begin();
+            }
+            out.couples[(size_t)(ab[0] * (int64_t)g + ab[1])] = 1;
+            out.couples[(size_t)(ab[1] * (int64_t)g + ab[0])] = 1;
+        }
+    } else {
+        std::fill(out.couples.begin(), out.couples.end(), 1);
+    }
+    if (g >= 3) {
+        std::vector<size_t> parent(g);
+        for (size_t k = 0; k < g; ++k) parent[k] = k;
+        std::function<size_t(size_t)> find = [&](size_t x) {
+            if (parent[x] != x) parent[x] = find(parent[x]);
+            return parent[x];
+        };
+        for (size_t a = 0; a < g; ++a)
+            for (size_t b = a + 1; b < g; ++b)
+                if (out.couples[a * g + b]) {
+                    const size_t ra = find(a), rb = find(b);
+                    if (ra != rb) parent[ra] = rb;
+                }
+        for (size_t a = 0; a < g; ++a)
+            for (size_t b = a + 1; b < g; ++b) {
+                if (out.couples[a * g + b]) continue;
+                if (find(a) == find(b))
+                    return fail(err, FH_ERR_COUPLING,
+                                "coupling is not transitive: groups '" + out.names[a] + "' and '" + out.names[b] +
+                                    "' are only reachable through a third group, but are not declared coupled "
+                                    "directly — declare the whole clique",
+                                (int64_t)a, (int64_t)b, 0.0, FH_COUPLING_NON_TRANSITIVE);
+            }
+    }
+    return FH_OK;
+}
+
+std::vector<fh_truncation_warning> coupling_warnings(const CouplingResolved &r, const fh_node *nodes,
+                                                     const fh_segment_def *segs, size_t n_segs) {
+    std::vector<fh_truncation_warning> out;
+    if (r.all_pairs) return out;
+    const size_t g = r.names.size();
+    const double inf = std::numeric_limits<double>::infinity();
+    std::vector<std::array<double, 6>> box(g, {inf, inf, inf, -inf, -inf, -inf});
+    for (size_t s = 0; s < n_segs; ++s)
+        for (int64_t node : {segs[s].a, segs[s].b}) {
+            const double pt[3] = {nodes[node].x, nodes[node].y, nodes[node].z};
+            auto &b = box[(size_t)r.of_segment[s]];
+            for (int k = 0; k < 3; ++k) {
+                b[k] = std::fmin(b[k], pt[k]);
+                b[3 + k] = std::fmax(b[3 + k], pt[k]);
+            }
+        }
+    auto empty = [](const std::array<double, 6> &b) { return b[0] > b[3] || b[1] > b[4] || b[2] > b[5]; };
+    auto diagonal = [&](const std::array<double, 6> &b) {
+        if (empty(b)) return 0.0;
+        double sum = 0.0;
+        for (int k = 0; k < 3; ++k) sum += (b[3 + k] - b[k]) * (b[3 + k] - b[k]);
+        return std::sqrt(sum);
+    };
+    auto gap = [&](const std::array<double, 6> &a, const std::array<double, 6> &b) {
+        if (empty(a) || empty(b)) return inf;
+        double sum = 0.0;
+        for (int k = 0; k < 3; ++k) {
+            const double apart = std::fmax(std::fmax(a[k] - b[3 + k], b[k] - a[3 + k]), 0.0);
+            sum += apart * apart;
+        }
+        return std::sqrt(sum);
+    };
+    for (size_t a = 0; a < g; ++a)
+        for (size_t b = a + 1; b < g; ++b) {
+            if (r.couples[a * g + b]) continue;
+            const double extent = std::fmax(diagonal(box[a]), diagonal(box[b]));
+            const double separation = gap(box[a], box[b]);
+            if (separation < extent) out.push_back(fh_truncation_warning{(int64_t)a, (int64_t)b, separation, extent});
+        }
+    return out;
+}
+
+int64_t coupling_kept_pairs(const CouplingResolved &r, const int64_t *per_segment, size_t n_segs) {
+    int64_t n = 0;
+    const size_t g = r.names.size();
+    std::vector<int64_t> sizes(g, 0);
+    for (size_t s = 0; s < n_segs; ++s) {
+        n += per_segment[s];
+        if (!r.of_segment.empty()) sizes[(size_t)r.of_segment[s]] += per_segment[s];
+    }
+    int64_t dropped = 0;
+    for (size_t a = 0; a < g; ++a)
+        for (size_t b = a + 1; b < g; ++b)
+            if (!r.couples[a * g + b]) dropped += sizes[a] * sizes[b];
+    return n * (n + 1) / 2 - dropped;
+}
+
 }  // namespace fhb
 
 using namespace fhb;

@@ -46,4 +46,21 @@ fh_status build_loops(const fh_segment_def *segs, size_t n_segs, size_t n_nodes,
                       const int64_t *per_segment, const fh_port *ports, size_t n_ports,
                       LoopBasis &out, fh_error_info *err);
 
+// Coupling resolved against a segment count (coupling.rs:323-380): group of
+// each segment (numbered by first appearance), names, and the symmetric
+// groups x groups table of kept pairs.
+struct CouplingResolved {
+    bool all_pairs = true;
+    std::vector<int32_t> of_segment;
+    std::vector<std::string> names;
+    std::vector<uint8_t> couples;
+    int64_t groups() const { return (int64_t)names.size(); }
+};
+fh_status resolve_coupling(const fh_coupling *c, size_t n_segs, CouplingResolved &out, fh_error_info *err);
+// Truncated group pairs closer than their extent (coupling.rs:285-318).
+std::vector<fh_truncation_warning> coupling_warnings(const CouplingResolved &r, const fh_node *nodes,
+                                                     const fh_segment_def *segs, size_t n_segs);
+// PairMask::kept_pairs (inductance/batch.rs:88-112) for per-segment filament counts.
+int64_t coupling_kept_pairs(const CouplingResolved &r, const int64_t *per_segment, size_t n_segs);
+
 }  // namespace fhb

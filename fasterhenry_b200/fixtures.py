@@ -156,6 +156,29 @@ def c4_spiral(target_skin_depths: float = 0.1, ratio: float = 1.4, max_per_axis:
                          skin_depth(1e9, target_skin_depths, ratio, max_per_axis), name="c4_spiral")
 
 
+ISLAND_SIDE = 10e-3
+ISLAND_EXTENT = math.sqrt(2.0) * ISLAND_SIDE
+
+
+def two_islands(separation: float) -> Tuple[Deck, List[str]]:
+    """Two nearly closed square loops (side 10 mm, trace 0.4 mm x 35 um, the
+    left side broken by a gap of side / 20 that holds the port), bounding
+    boxes ``separation`` apart along x; uniform 2 x 1.  Returns the deck and
+    the group tag of each segment ("a" x 4, "b" x 4).  The coupling fixture of
+    fasterhenry/tests/coupling.rs:33-75."""
+    nodes: List[Tuple[float, float, float]] = []
+    segs, ports = [], []
+    gap = ISLAND_SIDE / 20.0
+    for x0 in (0.0, ISLAND_SIDE + separation):
+        base = len(nodes)
+        for (x, y) in ((0.0, 0.0), (ISLAND_SIDE, 0.0), (ISLAND_SIDE, ISLAND_SIDE), (0.0, ISLAND_SIDE), (0.0, gap)):
+            nodes.append((x0 + x, y, 0.0))
+        for k in range(4):
+            segs.append(segment(base + k, base + k + 1, 0.4e-3, 35e-6))
+        ports.append((base, base + 4))
+    return Deck(nodes, segs, ports, uniform(2, 1), "two_islands"), ["a"] * 4 + ["b"] * 4
+
+
 def with_segment(deck: Deck, index: int, **changes) -> Deck:
     """A copy of ``deck`` with segment ``index``'s fields replaced."""
     segs = [dict(s) for s in deck.segments]

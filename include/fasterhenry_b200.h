@@ -60,6 +60,7 @@ typedef enum fh_status {
                                       also: mixed-precision refinement that did not reach its target */
     FH_ERR_PFFT = 19,              /* SolveError::Pfft(PfftError) */
     FH_ERR_INVALID_EXCITATION = 20,/* SolveError::InvalidExcitation */
+    FH_ERR_COUPLING = 21,          /* SolveError::Coupling(CouplingError), kind in detail (FH_COUPLING_*) */
     FH_ERR_UNSUPPORTED = 30        /* a path this build does not provide */
 } fh_status;
 
@@ -71,6 +72,16 @@ enum {
     FH_MESH_PORT_NOT_CONNECTED = 4,
     FH_MESH_SEGMENT_COUNT_MISMATCH = 5,
     FH_MESH_EMPTY_SEGMENT = 6
+};
+
+/* CouplingError kinds (coupling.rs:93-130) carried in fh_error_info.detail for
+ * FH_ERR_COUPLING: a declared group no segment belongs to; more group tags than
+ * segments (index_a = segments, index_b = tags); a non-transitive declaration
+ * (index_a, index_b = the two groups, in order of first appearance). */
+enum {
+    FH_COUPLING_UNKNOWN_GROUP = 1,
+    FH_COUPLING_SEGMENT_COUNT_MISMATCH = 2,
+    FH_COUPLING_NON_TRANSITIVE = 3
 };
 
 /* Payload of a failure (all fields optional / -1 when not applicable). */
@@ -266,6 +277,43 @@ fh_status fh_system_create(const fh_node *nodes, size_t n_nodes, const fh_segmen
 
 void fh_system_destroy(fh_system *sys);
 
+/* Coupling (coupling.rs:150-215): the group of each segment and the group
+ * pairs whose mutual inductance is kept.  truncate = 0 is Coupling::all_pairs
+ * (group names ignored, every pair kept); truncate = 1 keeps every group with
+ * itself and the declared pairs, and stores zero for every other filament
+ * pair without evaluating it.  A NULL or empty name is the default group;
+ * segments past n_segment_groups are in the default group. */
+typedef struct fh_coupling {
+    const char *const *segment_groups;
+    size_t n_segment_groups;
+    int32_t truncate;
+    const char *const *couples; /* 2 x n_couples group names */
+    size_t n_couples;
+} fh_coupling;
+
+/* MeshSystem::assemble_with_coupling (solve.rs:703-766): the coupling is
+ * checked against the geometry first (FH_ERR_COUPLING), then as
+ * fh_system_create with the truncated pairs left out of the fill.  A NULL
+ * coupling is Coupling::all_pairs. */
+fh_status fh_system_create_coupled(const fh_node *nodes, size_t n_nodes, const fh_segment_def *segments,
+                                   size_t n_segments, const fh_port *ports, size_t n_ports,
+                                   const fh_discretization *disc, const fh_coupling *coupling,
+                                   fh_solver_choice choice, fh_system **out, fh_error_info *err);
+
+/* TruncationWarning (coupling.rs:132-148): a truncated group pair whose
+ * bounding boxes lie closer than the larger box diagonal.  Groups are
+ * numbered in order of first appearance over the segments. */
+typedef struct fh_truncation_warning {
+    int64_t group_a, group_b;
+    double separation, extent;
+} fh_truncation_warning;
+
+/* The assembled system's coupling: PairMask::kept_pairs / total_pairs
+ * (inductance/batch.rs:88-117) and Coupling::truncation_warnings
+ * (coupling.rs:285-318), `count` of them written up to `capacity`. */
+fh_status fh_system_coupling(const fh_system *sys, int64_t *kept_pairs, int64_t *total_pairs,
+                             fh_truncation_warning *warnings, size_t capacity, size_t *count);
+
 fh_status fh_system_counts(const fh_system *sys, fh_counts *counts);
 fh_status fh_system_timing(const fh_system *sys, fh_timing *timing);
 
@@ -393,6 +441,7 @@ typedef struct fh_fill_stats {
     int64_t distinct_aligned_keys;
     double point_evaluations;
     double ms_classify, ms_point, ms_closed_form, ms_aligned_quadrature, ms_sampled, ms_congruence;
+    int64_t truncated;  /* pairs dropped by the coupling (never evaluated, zero in L) */
 } fh_fill_stats;
 fh_status fh_system_fill_stats(const fh_system *sys, fh_fill_stats *stats);
 

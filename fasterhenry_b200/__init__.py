@@ -17,5 +17,7 @@ from .api import (GmresOutcome, GmresParams, IterativeParams, IterativeSystem, P
 from .api import GradientResult, Param, inductance_gradient, release_cached_memory
 from .api import CURRENTS_CSV_HEADER, CurrentSolution, InvalidExcitation, unit_excitation
 from .api import DEFAULT_GROUP, Coupling, CouplingError, TruncationWarning
+from . import problem
+from .problem import DeckError, Problem, ProblemError, load, parse_deck, run
 
 __version__ = "0.1.0"

@@ -1,0 +1,526 @@
+"""The problem document and the FastHenry `.inp` deck reader: the front end
+that turns an input file into geometry, ports, discretization, coupling and
+frequencies for the C ABI (fasterhenry-cli/src/problem.rs:1-50; the deck
+dialect of fasterhenry-cli/src/inp.rs:1-600 and docs/input-format.md).
+
+* :class:`Problem` is the JSON problem document: ``geometry`` (``nodes`` of
+  ``x, y, z``; ``segments`` of ``a, b, width, height, sigma[, width_dir]``),
+  ``ports`` (``positive, negative[, name]``), ``discretization`` (one of
+  ``uniform``, ``per_segment``, ``graded``, ``skin_depth``,
+  ``per_segment_graded``), optional ``coupling`` and ``frequencies_hz``, in
+  SI units, unknown keys rejected at every level.
+* :func:`parse_deck` reads the deck subset: ``.title``, ``.units`` (required),
+  ``.default``, ``N`` nodes, ``E`` segments (``w h nwinc nhinc rw rh wx wy wz
+  sigma|rho group``), ``.external``, ``.freq``, ``.equiv``, ``.couples``,
+  ``.end``; ``*`` comments and ``+`` continuations; directives and node names
+  case-insensitive.  Ground planes (``G``, ``.hole``, ``.contact``) are not
+  read by this front end and are rejected with the line number.
+* :func:`load` picks the reader by file extension (``.inp``/``.fh`` decks,
+  anything else JSON), and :func:`run` assembles and sweeps a problem
+  (fasterhenry-cli/src/lib.rs:183-230).
+"""
+from __future__ import annotations
+
+import dataclasses
+import json
+import math
+import os
+import re
+from typing import Dict, List, Optional, Sequence, Tuple
+
+from . import api as A
+
+UNITS = {"km": 1e3, "m": 1.0, "cm": 1e-2, "mm": 1e-3, "um": 1e-6, "in": 0.0254, "mils": 2.54e-5, "mil": 2.54e-5}
+DISCRETIZATION_KINDS = ("uniform", "per_segment", "graded", "skin_depth", "per_segment_graded")
+
+
+class ProblemError(A.InvalidArgument):
+    """A malformed problem document."""
+
+
+class DeckError(A.InvalidArgument):
+    """A deck line the reader rejects; ``line`` is 1-based (0: the whole deck)."""
+
+    def __init__(self, line: int, message: str):
+        super().__init__("line %d: %s" % (line, message))
+        self.line = line
+
+
+# ---------------------------------------------------------------------------
+# The JSON problem document
+# ---------------------------------------------------------------------------
+def _keys(obj, allowed, required, where):
+    if not isinstance(obj, dict):
+        raise ProblemError("%s must be an object" % where)
+    for k in obj:
+        if k not in allowed:
+            raise ProblemError("unknown field `%s` in %s" % (k, where))
+    for k in required:
+        if k not in obj:
+            raise ProblemError("missing field `%s` in %s" % (k, where))
+
+
+def _num(v, where) -> float:
+    if isinstance(v, bool) or not isinstance(v, (int, float)):
+        raise ProblemError("%s must be a number" % where)
+    return float(v)
+
+
+def _count(v, where) -> int:
+    if isinstance(v, bool) or not isinstance(v, int) or v < 0:
+        raise ProblemError("%s must be a non-negative integer" % where)
+    return int(v)
+
+
+@dataclasses.dataclass
+class Problem:
+    """A complete input: geometry, ports, discretization, coupling and the
+    frequency sweep (fasterhenry-cli/src/problem.rs:13-36)."""
+    nodes: List[Tuple[float, float, float]]
+    segments: List[dict]
+    ports: List[Tuple[int, int, Optional[str]]]
+    discretization: dict
+    frequencies_hz: List[float]
+    coupling: "A.Coupling" = dataclasses.field(default_factory=lambda: A.Coupling.all_pairs())
+    title: Optional[str] = None
+
+    # -- JSON --------------------------------------------------------------
+    @classmethod
+    def from_json(cls, doc) -> "Problem":
+        if isinstance(doc, (str, bytes)):
+            doc = json.loads(doc)
+        _keys(doc, ("geometry", "ports", "discretization", "coupling", "frequencies_hz"),
+              ("geometry", "ports", "discretization", "frequencies_hz"), "the problem document")
+        g = doc["geometry"]
+        _keys(g, ("nodes", "segments"), (), "geometry")
+        nodes = []
+        for i, n in enumerate(g.get("nodes", [])):
+            _keys(n, ("x", "y", "z"), ("x", "y", "z"), "node %d" % i)
+            nodes.append(tuple(_num(n[k], "node %d %s" % (i, k)) for k in ("x", "y", "z")))
+        segs = []
+        for i, s in enumerate(g.get("segments", [])):
+            _keys(s, ("a", "b", "width", "height", "sigma", "width_dir"), ("a", "b", "width", "height", "sigma"),
+                  "segment %d" % i)
+            seg = {"a": _count(s["a"], "segment %d a" % i), "b": _count(s["b"], "segment %d b" % i),
+                   "width": _num(s["width"], "segment %d width" % i),
+                   "height": _num(s["height"], "segment %d height" % i),
+                   "sigma": _num(s["sigma"], "segment %d sigma" % i), "width_dir": None}
+            if "width_dir" in s:
+                wd = s["width_dir"]
+                if not (isinstance(wd, list) and len(wd) == 3):
+                    raise ProblemError("segment %d width_dir must be [x, y, z]" % i)
+                seg["width_dir"] = tuple(_num(x, "segment %d width_dir" % i) for x in wd)
+            segs.append(seg)
+        if not isinstance(doc["ports"], list):
+            raise ProblemError("ports must be an array")
+        ports = []
+        for i, p in enumerate(doc["ports"]):
+            _keys(p, ("positive", "negative", "name"), ("positive", "negative"), "port %d" % i)
+            name = p.get("name")
+            if name is not None and not isinstance(name, str):
+                raise ProblemError("port %d name must be a string" % i)
+            ports.append((_count(p["positive"], "port %d positive" % i), _count(p["negative"], "port %d negative" % i),
+                          name))
+        disc = _discretization_from_json(doc["discretization"])
+        freqs = doc["frequencies_hz"]
+        if not isinstance(freqs, list):
+            raise ProblemError("frequencies_hz must be an array")
+        coupling = A.Coupling.from_json(doc["coupling"]) if "coupling" in doc else A.Coupling.all_pairs()
+        return cls(nodes, segs, ports, disc, [_num(f, "frequencies_hz") for f in freqs], coupling)
+
+    def to_json(self) -> dict:
+        out = {
+            "geometry": {
+                "nodes": [{"x": x, "y": y, "z": z} for (x, y, z) in self.nodes],
+                "segments": [dict({k: s[k] for k in ("a", "b", "width", "height", "sigma")},
+                                  **({"width_dir": list(s["width_dir"])} if s.get("width_dir") is not None else {}))
+                             for s in self.segments]},
+            "ports": [dict({"positive": a, "negative": b}, **({"name": n} if n is not None else {}))
+                      for (a, b, n) in self.ports],
+            "discretization": _discretization_to_json(self.discretization),
+            "frequencies_hz": list(self.frequencies_hz),
+        }
+        if not self.coupling.is_trivial():
+            out["coupling"] = self.coupling.to_json()
+        return out
+
+    # -- to the library ------------------------------------------------------
+    def geometry(self) -> "A.Geometry":
+        return A.Geometry.from_parts(self.nodes, [A.SegmentDef(s["a"], s["b"], s["width"], s["height"], s["sigma"],
+                                                               s.get("width_dir")) for s in self.segments])
+
+    def port_list(self) -> List["A.Port"]:
+        return [A.Port(a, b, n) for (a, b, n) in self.ports]
+
+
+def _discretization_from_json(d) -> dict:
+    if not isinstance(d, dict) or len(d) != 1:
+        raise ProblemError("discretization must be an object with exactly one of %s" % ", ".join(DISCRETIZATION_KINDS))
+    (kind, v), = d.items()
+    if kind == "uniform":
+        _keys(v, ("nw", "nh"), ("nw", "nh"), "discretization.uniform")
+        return {"kind": "uniform", "nw": _count(v["nw"], "nw"), "nh": _count(v["nh"], "nh")}
+    if kind == "graded":
+        _keys(v, ("nw", "nh", "ratio"), ("nw", "nh", "ratio"), "discretization.graded")
+        return {"kind": "graded", "nw": _count(v["nw"], "nw"), "nh": _count(v["nh"], "nh"),
+                "ratio": _num(v["ratio"], "ratio")}
+    if kind == "skin_depth":
+        keys = ("frequency_hz", "target_skin_depths", "ratio", "max_per_axis")
+        _keys(v, keys, keys, "discretization.skin_depth")
+        return {"kind": "skin_depth", "frequency_hz": _num(v["frequency_hz"], "frequency_hz"),
+                "target_skin_depths": _num(v["target_skin_depths"], "target_skin_depths"),
+                "ratio": _num(v["ratio"], "ratio"), "max_per_axis": _count(v["max_per_axis"], "max_per_axis")}
+    if kind == "per_segment":
+        if not isinstance(v, list):
+            raise ProblemError("discretization.per_segment must be an array")
+        grids = []
+        for i, g in enumerate(v):
+            _keys(g, ("nw", "nh"), ("nw", "nh"), "discretization.per_segment[%d]" % i)
+            grids.append((_count(g["nw"], "nw"), _count(g["nh"], "nh")))
+        return {"kind": "per_segment", "grids": grids}
+    if kind == "per_segment_graded":
+        if not isinstance(v, list):
+            raise ProblemError("discretization.per_segment_graded must be an array")
+        grids = []
+        keys = ("nw", "nh", "width_ratio", "height_ratio")
+        for i, g in enumerate(v):
+            _keys(g, keys, keys, "discretization.per_segment_graded[%d]" % i)
+            grids.append((_count(g["nw"], "nw"), _count(g["nh"], "nh"), _num(g["width_ratio"], "width_ratio"),
+                          _num(g["height_ratio"], "height_ratio")))
+        return {"kind": "per_segment_graded", "grids": grids}
+    raise ProblemError("unknown discretization `%s`; expected one of %s" % (kind, ", ".join(DISCRETIZATION_KINDS)))
+
+
+def _discretization_to_json(d: dict) -> dict:
+    k = d["kind"]
+    if k == "uniform":
+        return {"uniform": {"nw": d["nw"], "nh": d["nh"]}}
+    if k == "graded":
+        return {"graded": {"nw": d["nw"], "nh": d["nh"], "ratio": d["ratio"]}}
+    if k == "skin_depth":
+        return {"skin_depth": {"frequency_hz": d["frequency_hz"], "target_skin_depths": d["target_skin_depths"],
+                               "ratio": d["ratio"], "max_per_axis": d.get("max_per_axis", 32)}}
+    if k == "per_segment":
+        return {"per_segment": [{"nw": a, "nh": b} for a, b in d["grids"]]}
+    return {"per_segment_graded": [{"nw": g[0], "nh": g[1], "width_ratio": g[2], "height_ratio": g[3]}
+                                   for g in d["grids"]]}
+
+
+# ---------------------------------------------------------------------------
+# The `.inp` deck
+# ---------------------------------------------------------------------------
+def frequency_sweep(fmin: float, fmax: float, ndec: float) -> List[float]:
+    """`.freq fmin fmax ndec`: n = floor(ndec log10(fmax/fmin)) + 1 points
+    f(k) = fmin 10^(k/ndec), the exact fmin 10^q where k/ndec is whole
+    (inp.rs:509-526)."""
+    if not (math.isfinite(fmin) and math.isfinite(fmax)) or fmin < 0 or fmax < 0:
+        raise ValueError("frequencies must be finite and >= 0")
+    if fmin == fmax:
+        return [fmin]
+    if fmin == 0.0:
+        raise ValueError("fmin = 0 is only allowed when fmin = fmax (the DC solve)")
+    if not (math.isfinite(ndec) and ndec > 0):
+        raise ValueError("ndec must be positive")
+    if fmin > fmax:
+        raise ValueError("fmin must not exceed fmax")
+    n = int(math.floor(ndec * math.log10(fmax / fmin))) + 1
+    out = []
+    for k in range(n):
+        q = k / ndec
+        out.append(fmin * 10.0 ** int(q) if float(q).is_integer() else fmin * 10.0 ** q)
+    return out
+
+
+_FIELDS = {"x", "y", "z", "w", "h", "nwinc", "nhinc", "rw", "rh", "wx", "wy", "wz", "sigma", "rho"}
+_LENGTHS = {"x", "y", "z", "w", "h"}
+
+
+def _split_statements(text: str) -> List[Tuple[int, str]]:
+    """Logical lines: comments dropped, '+' lines joined onto the previous
+    statement (keeping the first line's number)."""
+    out: List[Tuple[int, str]] = []
+    for no, raw in enumerate(text.splitlines(), 1):
+        line = raw.strip()
+        if not line or line.startswith("*"):
+            continue
+        if line.startswith("+"):
+            if not out:
+                raise DeckError(no, "a continuation line with nothing to continue")
+            out[-1] = (out[-1][0], out[-1][1] + " " + line[1:])
+            continue
+        out.append((no, line))
+    return out
+
+
+def _tokens(body: str) -> List[str]:
+    """Whitespace-separated tokens with whitespace around '=' removed."""
+    body = re.sub(r"\s*=\s*", "=", body.strip())
+    return body.split()
+
+
+def _number(tok: str, line: int) -> float:
+    try:
+        return float(tok)
+    except ValueError:
+        raise DeckError(line, "'%s' is not a number" % tok) from None
+
+
+def _assignments(tokens: Sequence[str], line: int, allowed) -> Dict[str, str]:
+    out: Dict[str, str] = {}
+    for t in tokens:
+        if "=" not in t:
+            raise DeckError(line, "expected <field>=<value>, got '%s'" % t)
+        k, v = t.split("=", 1)
+        k = k.lower()
+        if not v:
+            raise DeckError(line, "'%s=' has no value" % k)
+        if k not in allowed:
+            raise DeckError(line, "unknown field '%s'" % k)
+        out[k] = v
+    if "sigma" in out and "rho" in out:
+        raise DeckError(line, "give either sigma= or rho=, not both")
+    return out
+
+
+def parse_deck(text: str) -> Problem:
+    """Parses a FastHenry `.inp` deck in this front end's subset into a
+    :class:`Problem` (SI units)."""
+    statements = _split_statements(text)
+    unit: Optional[float] = None
+    defaults: Dict[str, str] = {}
+    defaults_unit: Dict[str, float] = {}
+    node_index: Dict[str, int] = {}        # canonical lowercase name -> node slot
+    alias: Dict[str, str] = {}             # name -> canonical name
+    positions: List[Tuple[float, float, float]] = []
+    segments: List[dict] = []
+    seg_lines: List[int] = []
+    grids: List[Tuple[int, int, float, float]] = []
+    groups: List[str] = []
+    ports: List[Tuple[str, str, Optional[str], int]] = []
+    freqs: Optional[List[float]] = None
+    couples: Optional[List[str]] = None
+    couples_all = False
+    title = None
+    ended = False
+
+    def resolve(name: str, line: int) -> str:
+        key = name.lower()
+        key = alias.get(key, key)
+        if key not in node_index:
+            raise DeckError(line, "node '%s' is not defined (nodes must be declared before they are used)" % name)
+        return key
+
+    def field(vals: Dict[str, str], key: str, line: int) -> Optional[float]:
+        """A field's value in metres / S/m from the line, else the default."""
+        if key in vals:
+            v, u = _number(vals[key], line), unit
+        elif key in defaults:
+            v, u = _number(defaults[key], line), defaults_unit[key]
+        else:
+            return None
+        return v * u if key in _LENGTHS else v
+
+    for line, stmt in statements:
+        if ended:
+            raise DeckError(line, "content after .end")
+        head, _, rest = stmt.partition(" ")
+        low = head.lower()
+        if low == ".end":
+            if rest.strip():
+                raise DeckError(line, ".end takes no arguments")
+            ended = True
+            continue
+        if low == ".title":
+            title = rest.strip()
+            continue
+        if low == ".units":
+            u = rest.strip().lower()
+            if u not in UNITS:
+                raise DeckError(line, "unknown unit '%s'; expected one of km, m, cm, mm, um, in, mils" % rest.strip())
+            if unit is not None:
+                raise DeckError(line, ".units may appear once")
+            unit = UNITS[u]
+            continue
+        if unit is None and low not in (".title",):
+            raise DeckError(line, "a .units line must come first (the deck unit is required)")
+        if low == ".default":
+            vals = _assignments(_tokens(rest), line, _FIELDS)
+            for k, v in vals.items():
+                if k in ("sigma", "rho"):
+                    defaults.pop("rho" if k == "sigma" else "sigma", None)
+                defaults[k] = v
+                defaults_unit[k] = unit
+            continue
+        if low.startswith("n") and not low.startswith("."):
+            name = low
+            if name in node_index or name in alias:
+                raise DeckError(line, "node '%s' is declared twice" % head)
+            vals = _assignments(_tokens(rest), line, {"x", "y", "z"})
+            xyz = []
+            for k in ("x", "y", "z"):
+                v = field(vals, k, line)
+                xyz.append(0.0 if v is None else v)
+            node_index[name] = len(positions)
+            positions.append(tuple(xyz))
+            continue
+        if low.startswith("e") and not low.startswith("."):
+            toks = _tokens(rest)
+            if len(toks) < 2:
+                raise DeckError(line, "a segment needs two node names")
+            a, b = resolve(toks[0], line), resolve(toks[1], line)
+            vals = _assignments(toks[2:], line, (_FIELDS - {"x", "y", "z"}) | {"group"})
+            w, h = field(vals, "w", line), field(vals, "h", line)
+            if w is None or h is None:
+                raise DeckError(line, "segment '%s' needs w= and h= (on the line or in .default)" % head)
+            if "sigma" in vals or ("rho" not in vals and "sigma" in defaults):
+                src, su = (vals, unit) if "sigma" in vals else (defaults, defaults_unit["sigma"])
+                sigma = _number(src["sigma"], line) / su
+            elif "rho" in vals or "rho" in defaults:
+                src, su = (vals, unit) if "rho" in vals else (defaults, defaults_unit["rho"])
+                r = _number(src["rho"], line)
+                if r <= 0:
+                    raise DeckError(line, "rho must be positive")
+                sigma = 1.0 / (r * su)
+            else:
+                raise DeckError(line, "segment '%s' has no conductivity (sigma= or rho=)" % head)
+            nw = int(field(vals, "nwinc", line) or 1)
+            nh = int(field(vals, "nhinc", line) or 1)
+            rw = field(vals, "rw", line) or 1.0
+            rh = field(vals, "rh", line) or 1.0
+            for key, r in (("rw", rw), ("rh", rh)):
+                if r < 1.0:
+                    raise DeckError(line, "'%s' must be >= 1, got %g" % (key, r))
+            wdir = None
+            if any(k in vals or k in defaults for k in ("wx", "wy", "wz")):
+                wdir = tuple((field(vals, k, line) or 0.0) for k in ("wx", "wy", "wz"))
+            segments.append({"a": a, "b": b, "width": w, "height": h, "sigma": sigma, "width_dir": wdir})
+            seg_lines.append(line)
+            grids.append((nw, nh, rw, rh))
+            groups.append(vals.get("group", ""))
+            continue
+        if low == ".external":
+            toks = rest.split()
+            if len(toks) not in (2, 3):
+                raise DeckError(line, ".external takes two node names and an optional label")
+            pos, neg = resolve(toks[0], line), resolve(toks[1], line)
+            label = toks[2] if len(toks) == 3 else "%s/%s" % (toks[0].lower(), toks[1].lower())
+            ports.append((pos, neg, label, line))
+            continue
+        if low == ".freq":
+            vals = _assignments(_tokens(rest), line, {"fmin", "fmax", "ndec"})
+            try:
+                fmin, fmax = _number(vals["fmin"], line), _number(vals["fmax"], line)
+                ndec = _number(vals.get("ndec", "1"), line)
+                freqs = frequency_sweep(fmin, fmax, ndec)
+            except KeyError as e:
+                raise DeckError(line, ".freq needs %s=" % e.args[0]) from None
+            except ValueError as e:
+                raise DeckError(line, str(e)) from None
+            continue
+        if low == ".equiv":
+            names = [t.lower() for t in rest.split()]
+            if len(names) < 2:
+                raise DeckError(line, ".equiv joins two or more nodes")
+            canon = None
+            for nm in names:
+                key = alias.get(nm, nm)
+                if key in node_index:
+                    canon = key
+                    break
+            if canon is None:
+                raise DeckError(line, ".equiv names no defined node")
+            for nm in names:
+                key = alias.get(nm, nm)
+                if key == canon:
+                    if nm != canon and nm not in alias:
+                        raise DeckError(line, ".equiv names node '%s' twice" % nm)
+                    continue
+                if key in node_index:
+                    # a defined node becomes an alias of the canonical one
+                    for k2, v2 in list(alias.items()):
+                        if v2 == key:
+                            alias[k2] = canon
+                    alias[key] = canon
+                else:
+                    alias[nm] = canon
+            continue
+        if low == ".couples":
+            toks = rest.split()
+            if len(toks) == 1 and toks[0].lower() == "all":
+                couples_all = True
+            else:
+                couples = (couples or []) + toks
+            continue
+        if low.startswith("g") or low in (".hole", ".contact"):
+            raise DeckError(line, "ground planes ('%s') are not read by this front end; describe the plane's "
+                                  "conductors as segments" % head)
+        raise DeckError(line, "'%s' is not in the deck subset" % head)
+    if not ended:
+        raise DeckError(0, "the deck has no .end")
+    if unit is None:
+        raise DeckError(0, "the deck has no .units line")
+    # Compact the nodes: aliased nodes disappear, references go to the canonical slot.
+    live = [nm for nm in sorted(node_index, key=lambda k: node_index[k]) if nm not in alias]
+    slot = {nm: i for i, nm in enumerate(live)}
+    nodes = [positions[node_index[nm]] for nm in live]
+
+    def idx(nm: str) -> int:
+        return slot[alias.get(nm, nm)]
+    segs = [dict(s, a=idx(s["a"]), b=idx(s["b"])) for s in segments]
+    port_list = [(idx(p), idx(n), label) for (p, n, label, _) in ports]
+    if any(g[2] != 1.0 or g[3] != 1.0 for g in grids):
+        disc = {"kind": "per_segment_graded", "grids": grids}
+    elif grids and all(g[:2] == grids[0][:2] for g in grids):
+        disc = {"kind": "uniform", "nw": grids[0][0], "nh": grids[0][1]}
+    elif grids:
+        disc = {"kind": "per_segment", "grids": [g[:2] for g in grids]}
+    else:
+        disc = {"kind": "uniform", "nw": 1, "nh": 1}
+    if couples is not None and not couples_all:
+        for g in couples:
+            if g not in groups:
+                raise DeckError(0, ".couples names group '%s', which no segment carries" % g)
+        coupling = A.Coupling.truncated(groups)
+        for i in range(len(couples)):
+            for j in range(i + 1, len(couples)):
+                coupling = coupling.coupled(couples[i], couples[j])
+    elif any(groups):
+        coupling = A.Coupling(groups, None)
+    else:
+        coupling = A.Coupling.all_pairs()
+    return Problem(nodes, segs, port_list, disc, freqs or [], coupling, title)
+
+
+def load(path: str) -> Problem:
+    """A problem from a file: `.inp` / `.fh` as a deck, anything else as the
+    JSON document (fasterhenry-cli/src/lib.rs read_inputs)."""
+    with open(path) as f:
+        text = f.read()
+    if os.path.splitext(path)[1].lower() in (".inp", ".fh"):
+        return parse_deck(text)
+    return Problem.from_json(text)
+
+
+def run(problem: Problem, precision: "A.Precision" = A.Precision.FP64,
+        solver: "A.SolverChoice" = A.SolverChoice.AUTO, frequencies: Optional[Sequence[float]] = None):
+    """Assemble and sweep a problem (fasterhenry-cli/src/lib.rs:183-230): the
+    dense path with its coupling, or the matrix-free path when the solver
+    choice resolves there (which couples every pair).  Returns the
+    SweepResult and the truncation warnings."""
+    freqs = list(problem.frequencies_hz if frequencies is None else frequencies)
+    if not problem.ports:
+        raise A.InvalidArgument("no ports: give .external in the deck or ports in the document")
+    if not freqs:
+        raise A.InvalidArgument("no frequencies: give .freq in the deck or frequencies_hz in the document")
+    geometry = problem.geometry()
+    ports = problem.port_list()
+    n = len(A.discretize(geometry, problem.discretization)[0]) if solver == A.SolverChoice.AUTO else 0
+    path = solver.resolve(n) if solver != A.SolverChoice.DENSE else "dense"
+    if path == "iterative":
+        if not problem.coupling.is_all_pairs():
+            raise A.Unsupported("a truncating coupling is a dense-path feature; choose the dense solver")
+        with A.IterativeSystem.assemble(geometry, ports, problem.discretization) as system:
+            return system.sweep(freqs), []
+    with A.MeshSystem.assemble(geometry, ports, problem.discretization, coupling=problem.coupling) as system:
+        warnings = [str(w) for w in system.truncation_warnings()]
+        return system.sweep(freqs, precision), warnings

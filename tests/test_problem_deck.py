@@ -1,0 +1,161 @@
+"""The problem front end (fasterhenry_b200/problem.py): the JSON problem
+document (docs/input-format.md of the reference) and the `.inp` deck subset
+(fasterhenry-cli/src/inp.rs:12-600): units, defaults, nodes, segments,
+ports, frequency sweeps, node equivalence, coupling groups and the errors
+the reader reports with line numbers.  Host-only."""
+import json
+import math
+
+import pytest
+
+from fasterhenry_b200 import problem as P
+
+DECK = """* a two-segment trace
+.units mm
+.default sigma=5.8e4 w=0.1 h=0.035
+N1 x=0 y=0 z=0
+N2 x = 1 y=0 z=0
+N3 x=1 y=1
+E1 N1 N2 nwinc=3 nhinc=2
+E2 N2 n3 nwinc=3
++ nhinc=2
+.external N1 N3
+.freq fmin=1e3 fmax=1e6 ndec=10
+.end
+"""
+
+
+def test_a_small_deck_reads_in_si_units():
+    p = P.parse_deck(DECK)
+    assert p.nodes == [(0.0, 0.0, 0.0), (1e-3, 0.0, 0.0), (1e-3, 1e-3, 0.0)]
+    s = p.segments[0]
+    assert s["a"] == 0 and s["b"] == 1
+    assert math.isclose(s["width"], 1e-4, rel_tol=1e-15) and math.isclose(s["height"], 3.5e-5, rel_tol=1e-15)
+    assert math.isclose(s["sigma"], 5.8e7, rel_tol=1e-15)
+    assert p.discretization == {"kind": "uniform", "nw": 3, "nh": 2}
+    assert p.ports == [(0, 2, "n1/n3")]
+    assert len(p.frequencies_hz) == 31 and p.frequencies_hz[0] == 1e3 and p.frequencies_hz[30] == 1e6
+    assert p.coupling.is_trivial()
+
+
+def test_frequency_sweeps():
+    assert P.frequency_sweep(1e3, 1e7, 0.5) == [1e3, 1e5, 1e7]
+    assert P.frequency_sweep(5.0, 5.0, 3) == [5.0]
+    assert P.frequency_sweep(0.0, 0.0, 1) == [0.0]
+    with pytest.raises(ValueError):
+        P.frequency_sweep(0.0, 1e3, 1)
+    with pytest.raises(ValueError):
+        P.frequency_sweep(1e3, 1e6, -1)
+    f = P.frequency_sweep(1e6, 1e9, 1)
+    assert f == [1e6, 1e7, 1e8, 1e9]
+
+
+def test_resistivity_grading_and_per_segment_counts():
+    deck = """.units um
+N1 x=0 y=0 z=0
+N2 x=100 y=0 z=0
+N3 x=100 y=100 z=0
+E1 N1 N2 w=10 h=2 rho=0.0172 nwinc=5 rw=2
+E2 N2 N3 w=10 h=2 rho=0.0172 nwinc=4 nhinc=1
+.external N1 N3 coil
+.freq fmin=1e9 fmax=1e9 ndec=1
+.end"""
+    p = P.parse_deck(deck)
+    # rho in ohm * um: sigma = 1 / (rho * 1e-6) S/m
+    assert math.isclose(p.segments[0]["sigma"], 1.0 / (0.0172e-6), rel_tol=1e-15)
+    assert p.discretization["kind"] == "per_segment_graded"
+    assert p.discretization["grids"] == [(5, 1, 2.0, 1.0), (4, 1, 1.0, 1.0)]
+    assert p.ports == [(0, 2, "coil")]
+    p2 = P.parse_deck(deck.replace(" rw=2", ""))
+    assert p2.discretization == {"kind": "per_segment", "grids": [(5, 1), (4, 1)]}
+
+
+def test_equiv_joins_nodes_and_drops_the_alias():
+    deck = """.units m
+N1 x=0 y=0 z=0
+N2 x=1 y=0 z=0
+N3 x=1 y=0 z=0
+N4 x=2 y=0 z=0
+E1 N1 N2 w=0.1 h=0.1 sigma=1
+E2 N3 N4 w=0.1 h=0.1 sigma=1
+.equiv N2 N3 mid
+.external N1 mid
+.freq fmin=0 fmax=0
+.end"""
+    p = P.parse_deck(deck)
+    assert len(p.nodes) == 3
+    assert p.segments[0]["b"] == p.segments[1]["a"] == 1
+    assert p.ports == [(0, 1, "n1/mid")]
+    assert p.frequencies_hz == [0.0]
+
+
+def test_width_direction_and_groups():
+    deck = """.units m
+.default w=0.1 h=0.05 sigma=1
+N1 x=0 y=0 z=0
+N2 x=0 y=0 z=1
+N3 x=5 y=0 z=0
+N4 x=5 y=0 z=1
+E1 N1 N2 wy=1 group=left
+E2 N3 N4 group=right
+.external N1 N2
+.external N3 N4
+.couples left right
+.freq fmin=1e6 fmax=1e6
+.end"""
+    p = P.parse_deck(deck)
+    assert p.segments[0]["width_dir"] == (0.0, 1.0, 0.0) and p.segments[1]["width_dir"] is None
+    assert p.coupling.segment_groups == ["left", "right"] and p.coupling.couples("left", "right")
+    assert not p.coupling.is_all_pairs()
+    p_all = P.parse_deck(deck.replace(".couples left right", ".couples all"))
+    assert p_all.coupling.is_all_pairs()
+
+
+@pytest.mark.parametrize("text,line,what", [
+    ("N1 x=0\n.end", 1, ".units"),
+    (".units mm\nN1 x=0\n", 0, ".end"),
+    (".units mm\nN1 x=0\n.bogus\n.end", 3, "not in the deck subset"),
+    (".units mm\nN1 x=0\nGplane x1=0\n.end", 3, "ground planes"),
+    (".units mm\nN1 x=0\nE1 N1 N9 w=1 h=1 sigma=1\n.end", 3, "not defined"),
+    (".units mm\nN1 x=0\nN2 x=1\nE1 N1 N2 w=1 h=1\n.end", 4, "conductivity"),
+    (".units mm\nN1 x=0\nN2 x=1\nE1 N1 N2 w=1 h=1 sigma=1 rho=1\n.end", 4, "either"),
+    (".units mm\nN1 x=0\nn1 x=1\n.end", 3, "twice"),
+    (".units mm\nN1 x=0\n.end\nN2 x=1", 4, "after .end"),
+    (".units furlong\n.end", 1, "unknown unit"),
+])
+def test_errors_carry_the_line(text, line, what):
+    with pytest.raises(P.DeckError) as e:
+        P.parse_deck(text)
+    assert e.value.line == line and what in str(e.value), str(e.value)
+
+
+def test_json_document_round_trips_and_rejects_unknown_keys():
+    p = P.parse_deck(DECK)
+    doc = p.to_json()
+    assert set(doc) == {"geometry", "ports", "discretization", "frequencies_hz"}
+    assert doc["discretization"] == {"uniform": {"nw": 3, "nh": 2}}
+    back = P.Problem.from_json(json.dumps(doc))
+    assert back.nodes == p.nodes and back.segments == p.segments and back.ports == p.ports
+    assert back.discretization == p.discretization and back.frequencies_hz == p.frequencies_hz
+    bad = dict(doc, typo=1)
+    with pytest.raises(P.ProblemError, match="typo"):
+        P.Problem.from_json(bad)
+    port_typo = dict(doc, ports=[{"positive": 0, "negative": 1, "nmae": "x"}])
+    with pytest.raises(P.ProblemError, match="nmae"):
+        P.Problem.from_json(port_typo)
+    with pytest.raises(P.ProblemError, match="unknown discretization"):
+        P.Problem.from_json(dict(doc, discretization={"fancy": {}}))
+    sk = dict(doc, discretization={"skin_depth": {"frequency_hz": 1e9, "target_skin_depths": 0.5, "ratio": 2.0,
+                                                  "max_per_axis": 32}})
+    assert P.Problem.from_json(sk).discretization["kind"] == "skin_depth"
+    coupled = dict(doc, coupling={"segment_groups": ["a", "b"], "couples": [["a", "b"]]})
+    assert P.Problem.from_json(coupled).to_json()["coupling"] == coupled["coupling"]
+
+
+def test_load_picks_the_reader_by_extension(tmp_path):
+    deck = tmp_path / "trace.inp"
+    deck.write_text(DECK)
+    doc = tmp_path / "trace.json"
+    doc.write_text(json.dumps(P.parse_deck(DECK).to_json()))
+    a, b = P.load(str(deck)), P.load(str(doc))
+    assert a.nodes == b.nodes and a.segments == b.segments

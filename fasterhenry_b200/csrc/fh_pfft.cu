@@ -268,72 +268,59 @@ fh_status pfft_build(const fh_filament *fil, int64_t n, const PfftConfig &cfg, v
     op.G = st.grid.len();
     op.P = op.padded[0] * op.padded[1] * op.padded[2];
     op.components = st.components;
-    op.projection_entries = (int64_t)st.proj_index.size();
 
-    // Exact partial inductance of every near pair (device fill, pair list).
+    // Projections, their transpose and the grid approximations of the near
+    // pairs on the device; then the exact near pairs (device fill, pair list)
+    // and the near-field matrix.
+    PfftDeviceSetup ds;
+    e = pfft_device_setup(st, fil, s, ds, err);
+    op.d_proj_off = ds.proj_off;
+    op.d_proj_idx = ds.proj_idx;
+    op.d_proj_w = ds.proj_w;
+    op.d_spread_off = ds.spread_off;
+    op.d_spread_fil = ds.spread_fil;
+    op.d_spread_w = ds.spread_w;
+    struct FreeGrid {
+        double *p;
+        ~FreeGrid() {
+            if (p) cudaFree(p);
+        }
+    } free_grid{ds.pair_grid};
+    if (e) return e;
+    op.projection_entries = ds.entries;
     const int64_t np = (int64_t)st.pair_i.size();
-    std::vector<double> exact((size_t)np, 0.0);
-    if (np) {
+    {
         std::vector<DevFil> hf((size_t)n);
         for (int64_t i = 0; i < n; ++i) hf[i] = make_devfil(fil[i]);
         std::vector<int2> pairs((size_t)np);
         for (int64_t k = 0; k < np; ++k) pairs[k] = make_int2(st.pair_i[k], st.pair_j[k]);
         DevFil *d_fil = nullptr;
         int2 *d_pairs = nullptr;
-        double *d_exact = nullptr;
+        double *d_exact = nullptr, *d_cos = nullptr;
         struct Free {
-            void *a, *b, *c;
+            void *a, *b, *c, *d;
             ~Free() {
-                if (a) cudaFree(a);
-                if (b) cudaFree(b);
-                if (c) cudaFree(c);
+                for (void *q : {a, b, c, d})
+                    if (q) cudaFree(q);
             }
-        } guard{nullptr, nullptr, nullptr};
+        } guard{nullptr, nullptr, nullptr, nullptr};
         FHB_CUDA(upload(&d_fil, hf, s));
         guard.a = d_fil;
         FHB_CUDA(upload(&d_pairs, pairs, s));
         guard.b = d_pairs;
-        FHB_CUDA(cudaMalloc(&d_exact, sizeof(double) * np));
+        FHB_CUDA(cudaMalloc(&d_exact, sizeof(double) * std::max<int64_t>(np, 1)));
         guard.c = d_exact;
-        e = device_fill_pairs(d_fil, n, d_pairs, np, d_exact, s, nullptr, err);
-        if (e) return e;
-        FHB_CUDA(cudaMemcpyAsync(exact.data(), d_exact, sizeof(double) * np, cudaMemcpyDeviceToHost, s));
-        FHB_CUDA(cudaStreamSynchronize(s));
-    }
-    // Corrections, mirrored into full rows: row j receives the entries of
-    // rows i < j first (in i order), then its own (near.rs:263-298).
-    std::vector<int64_t> counts((size_t)n, 0);
-    for (int64_t k = 0; k < np; ++k) {
-        counts[st.pair_i[k]] += 1;
-        if (st.pair_j[k] != st.pair_i[k]) counts[st.pair_j[k]] += 1;
-    }
-    std::vector<int64_t> near_off((size_t)n + 1, 0);
-    for (int64_t i = 0; i < n; ++i) near_off[i + 1] = near_off[i] + counts[i];
-    const int64_t total = near_off[n];
-    std::vector<uint32_t> near_col((size_t)total);
-    std::vector<double> near_val((size_t)total);
-    std::vector<int64_t> fillp(near_off.begin(), near_off.end() - 1);
-    for (int64_t k = 0; k < np; ++k) {
-        const int32_t i = st.pair_i[k], j = st.pair_j[k];
-        const double c = exact[k] - kMu0Over4PiP * st.pair_cos[k] * st.pair_grid[k];
-        near_col[fillp[i]] = (uint32_t)j;
-        near_val[fillp[i]++] = c;
-        if (j != i) {
-            near_col[fillp[j]] = (uint32_t)i;
-            near_val[fillp[j]++] = c;
+        FHB_CUDA(upload(&d_cos, st.pair_cos, s));
+        guard.d = d_cos;
+        if (np) {
+            e = device_fill_pairs(d_fil, n, d_pairs, np, d_exact, s, nullptr, err);
+            if (e) return e;
         }
+        e = pfft_near_csr(n, np, d_pairs, d_exact, ds.pair_grid, d_cos, s, &op.d_near_off, &op.d_near_col,
+                          &op.d_near_val, &op.near_entries, err);
+        if (e) return e;
     }
-    op.near_entries = total;
     FHB_CUDA(upload(&op.d_dir, st.directions, s));
-    FHB_CUDA(upload(&op.d_proj_off, st.proj_offsets, s));
-    FHB_CUDA(upload(&op.d_proj_idx, st.proj_index, s));
-    FHB_CUDA(upload(&op.d_proj_w, st.proj_weight, s));
-    FHB_CUDA(upload(&op.d_spread_off, st.spread_offsets, s));
-    FHB_CUDA(upload(&op.d_spread_fil, st.spread_filament, s));
-    FHB_CUDA(upload(&op.d_spread_w, st.spread_weight, s));
-    FHB_CUDA(upload(&op.d_near_off, near_off, s));
-    FHB_CUDA(upload(&op.d_near_col, near_col, s));
-    FHB_CUDA(upload(&op.d_near_val, near_val, s));
 
     // Kernel spectrum.
     FHB_CUDA(cudaMalloc(&op.d_spectrum, sizeof(double) * op.P));

@@ -5,6 +5,8 @@
 // (fh_pfft.cu).
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <vector>
 
@@ -22,24 +24,19 @@ struct PfftGrid {
     int64_t len() const { return dims[0] * dims[1] * dims[2]; }
 };
 
-// Everything the device operator needs, built on the host.
+// The host part of the set-up: the grid, the near-field radius, the
+// non-orthogonal near pairs i <= j (row-major by i, pair_off[i] the first
+// pair of row i) with cos(i, j), and the filament directions.
 struct PfftSetup {
     int64_t n = 0;
     PfftGrid grid;
     int64_t padded[3] = {0, 0, 0};
-    // Projection weights per filament (CSR) and per grid point (transpose).
-    std::vector<int64_t> proj_offsets;
-    std::vector<uint32_t> proj_index;
-    std::vector<double> proj_weight;
-    std::vector<int64_t> spread_offsets;
-    std::vector<uint32_t> spread_filament;
-    std::vector<double> spread_weight;
+    double radius = 0.0;
     std::vector<double> directions;  // 3 n, unit length vectors
     std::vector<int> components;     // Cartesian components some direction carries
-    // Near pairs i <= j that are not orthogonal, row-major by i, with the
-    // grid's approximation sum_g sum_h W_ig W_jh K(g - h) and cos(i, j).
+    std::vector<int64_t> pair_off;
     std::vector<int32_t> pair_i, pair_j;
-    std::vector<double> pair_grid, pair_cos;
+    std::vector<double> pair_cos;
 };
 
 // Parameters (PfftParams, pfft/mod.rs:183-232), validated.
@@ -62,8 +59,35 @@ inline int64_t padded_size(int64_t n) { return smooth_size(2 * n - 1); }
 // pfft/mod.rs:614-631).
 double auto_spacing(const double extent[3], double cells);
 
-// Builds grid, projections, near pairs and their grid approximations.
+// Validates the parameters and builds the grid and the near pairs.
 fh_status pfft_setup(const fh_filament *fil, int64_t n, const PfftConfig &cfg, PfftSetup &out, fh_error_info *err);
+
+// Projection quadrature (grid.rs:38-40): tolerance and largest order.
+constexpr double kProjectionTolerance = 1e-10;
+constexpr int kProjectionMaxOrder = 12;
+
+// Device part of the set-up (fh_pfft_setup.cu), on `stream`:
+//   projection of every filament onto its stencil (CSR by filament, ascending
+//   grid index) and its transpose (CSR by grid point, ascending filament);
+//   the grid approximation sum_g sum_h W_ig W_jh K(g - h) of every near pair.
+struct PfftDeviceSetup {
+    int64_t *proj_off = nullptr;   // n + 1
+    uint32_t *proj_idx = nullptr;  // entries
+    double *proj_w = nullptr;
+    int64_t *spread_off = nullptr;   // G + 1
+    uint32_t *spread_fil = nullptr;  // entries
+    double *spread_w = nullptr;
+    double *pair_grid = nullptr;  // one per near pair
+    int64_t entries = 0;
+};
+fh_status pfft_device_setup(const PfftSetup &st, const fh_filament *fil, cudaStream_t stream, PfftDeviceSetup &out,
+                            fh_error_info *err);
+// The near-field matrix: mirrored rows of exact - mu0/4pi cos grid for the
+// near pairs (d_exact, d_grid, d_cos per pair; pair lists on the device),
+// each row ascending in column (near.rs:263-298).
+fh_status pfft_near_csr(int64_t n, int64_t np, const int2 *d_pairs, const double *d_exact, const double *d_grid,
+                        const double *d_cos, cudaStream_t stream, int64_t **near_off, uint32_t **near_col,
+                        double **near_val, int64_t *near_entries, fh_error_info *err);
 
 // The grid kernel 1 / |r_g - r_h| for an integer offset, zero at the origin
 // (near.rs:114-123).

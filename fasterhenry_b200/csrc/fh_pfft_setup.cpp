@@ -1,24 +1,19 @@
-// Host set-up of the precorrected-FFT operator: grid, projection of every
-// filament onto it, near-pair search and the grid's approximation of every
-// near pair (to be replaced by the exact value).  The method is the
-// reference's (pfft/mod.rs:332-460, grid.rs:44-216, near.rs:41-401):
+// Host part of the precorrected-FFT set-up: parameters, the grid, and the
+// near-pair search.  The method is the reference's (pfft/mod.rs:332-460,
+// grid.rs:44-95, near.rs:41-106):
 //
 //   * grid of spacing h over the filaments' bounding box, padded by half a
 //     stencil, h from GridSpacing::Auto (about cells_per_filament cells per
 //     filament) or fixed;
-//   * projection: a composite Gauss-Legendre rule over each filament's
-//     length, width and height (pieces no longer than h, order from the
-//     1e-10 / 12 order table at the near-field distance), every node
-//     interpolated onto its (order+1)^3 Lagrange stencil, weights summed per
-//     grid point;
 //   * near pairs: uniform bins about the radius in size; a pair is near when
-//     the separating-axis gap of the two bars is below radius = k h;
-//   * grid approximation of a near pair, sum_g sum_h W_ig W_jh K(g - h), by
-//     the cheaper of the direct double sum and the potential of i's
-//     projection over the box spanned by its partners' projections.
+//     the separating-axis gap of the two bars is below radius = k h; the
+//     non-orthogonal ones (i <= j) are the pairs whose grid approximation the
+//     device replaces by the exact value.
 //
-// Rows are independent and run in parallel (host threads); every row's arithmetic
-// is in a fixed order, so the result does not depend on the thread count.
+// The projections and the grid approximations of the near pairs are built on
+// the device (fh_pfft_setup.cu).  Rows of the search are independent and run
+// on the host's cores; each row's result is in a fixed order, so it does not
+// depend on the thread count.
 #include <algorithm>
 #include <array>
 #include <atomic>
@@ -56,13 +51,7 @@ void parallel_for(int64_t n, int64_t chunk, F body) {
     for (auto &t : pool) t.join();
 }
 
-constexpr double kQuadratureTolerance = 1e-10;  // grid.rs:38
-constexpr int kQuadratureMaxOrder = 12;         // grid.rs:40
 constexpr double kOrthogonalCos = 1e-14;        // near.rs:25
-
-struct Rule {
-    std::vector<double> x, w;
-};
 
 struct Bar {  // neumann.rs Bar: centre, unit axes, half extents
     double c[3];
@@ -123,118 +112,6 @@ double separation(const Bar &a, const Bar &b) {
             }
         }
     return best;
-}
-
-// OrderTable(1e-10, 12).order_for (gauss.rs:123-136); 0 when none suffices.
-struct OrderTable {
-    double threshold[kQuadratureMaxOrder];
-    OrderTable() {
-        const double lg = std::log(1.0 / kQuadratureTolerance);
-        for (int k = 1; k <= kQuadratureMaxOrder; ++k) threshold[k - 1] = std::sinh(lg / (2.0 * k));
-    }
-    int order_for(double half, double distance) const {
-        if (half <= 0.0) return 1;
-        if (std::isnan(distance) || distance <= 0.0) return 0;
-        const double delta = distance / half;
-        for (int k = 0; k < kQuadratureMaxOrder; ++k)
-            if (delta >= threshold[k]) return k + 1;
-        return 0;
-    }
-};
-
-// First stencil plane along `axis` for coordinate x and the Lagrange weights
-// of the m planes from there (grid.rs:100-120).
-int64_t axis_stencil(const PfftGrid &g, int axis, double x, double *w) {
-    const int m = g.stencil;
-    const double u = (x - g.origin[axis]) / g.spacing;
-    double f = std::floor(u - 0.5 * m) + 1.0;
-    int64_t first = f > 0.0 ? (int64_t)f : 0;
-    first = std::min<int64_t>(first, g.dims[axis] - m);
-    const double t = u - (double)first;
-    for (int k = 0; k < m; ++k) {
-        double v = 1.0;
-        for (int l = 0; l < m; ++l)
-            if (l != k) v *= (t - (double)l) / ((double)k - (double)l);
-        w[k] = v;
-    }
-    return first;
-}
-
-struct Projection {
-    std::vector<std::pair<uint32_t, double>> entries;  // ascending grid index
-    int64_t lo[3], hi[3];                               // inclusive box, grid coordinates
-};
-
-void point_of(const PfftGrid &g, int64_t index, int64_t p[3]) {
-    p[2] = index % g.dims[2];
-    const int64_t rest = index / g.dims[2];
-    p[0] = rest / g.dims[1];
-    p[1] = rest % g.dims[1];
-}
-
-// grid.rs:145-216.
-void project(const PfftGrid &g, const fh_filament &f, double far_distance, const OrderTable &table,
-             const std::vector<Rule> &rules, Projection &out) {
-    const double *axes[3] = {f.dir_length, f.dir_width, f.dir_height};
-    const double extents[3] = {f.length, f.width, f.height};
-    double corner[3];
-    for (int k = 0; k < 3; ++k) corner[k] = f.start[k] - 0.5 * f.width * f.dir_width[k] - 0.5 * f.height * f.dir_height[k];
-    std::vector<std::pair<double, double>> nodes[3];
-    for (int d = 0; d < 3; ++d) {
-        const double extent = extents[d];
-        const int64_t pieces = std::max<int64_t>(1, (int64_t)std::ceil(extent / g.spacing));
-        const double piece = extent / (double)pieces;
-        int order = table.order_for(0.5 * piece, far_distance);
-        if (order == 0) order = kQuadratureMaxOrder;
-        const Rule &r = rules[order];
-        for (int64_t p = 0; p < pieces; ++p) {
-            const double a = (double)p * piece, b = (double)(p + 1) * piece;
-            const double mid = 0.5 * (a + b), half = 0.5 * (b - a);
-            for (int q = 0; q < order; ++q) nodes[d].push_back({mid + half * r.x[q], half * r.w[q]});
-        }
-    }
-    const double inverse_area = 1.0 / (f.width * f.height);
-    const int m = g.stencil;
-    std::vector<std::pair<int64_t, double>> raw;
-    raw.reserve(nodes[0].size() * nodes[1].size() * nodes[2].size() * m * m * m);
-    double wx[16], wy[16], wz[16];
-    for (const auto &sn : nodes[0])
-        for (const auto &an : nodes[1])
-            for (const auto &bn : nodes[2]) {
-                double r[3];
-                for (int k = 0; k < 3; ++k) r[k] = corner[k] + sn.first * axes[0][k] + an.first * axes[1][k] + bn.first * axes[2][k];
-                const double weight = sn.second * an.second * bn.second * inverse_area;
-                const int64_t fx = axis_stencil(g, 0, r[0], wx);
-                const int64_t fy = axis_stencil(g, 1, r[1], wy);
-                const int64_t fz = axis_stencil(g, 2, r[2], wz);
-                for (int i = 0; i < m; ++i)
-                    for (int j = 0; j < m; ++j) {
-                        const int64_t row = ((fx + i) * g.dims[1] + (fy + j)) * g.dims[2] + fz;
-                        const double lxy = weight * wx[i] * wy[j];
-                        for (int k = 0; k < m; ++k) raw.push_back({row + k, lxy * wz[k]});
-                    }
-            }
-    std::stable_sort(raw.begin(), raw.end(),
-                     [](const std::pair<int64_t, double> &a, const std::pair<int64_t, double> &b) { return a.first < b.first; });
-    out.entries.clear();
-    for (const auto &e : raw) {
-        if (!out.entries.empty() && (int64_t)out.entries.back().first == e.first)
-            out.entries.back().second += e.second;
-        else
-            out.entries.push_back({(uint32_t)e.first, e.second});
-    }
-    for (int a = 0; a < 3; ++a) {
-        out.lo[a] = std::numeric_limits<int64_t>::max();
-        out.hi[a] = 0;
-    }
-    for (const auto &e : out.entries) {
-        int64_t p[3];
-        point_of(g, e.first, p);
-        for (int a = 0; a < 3; ++a) {
-            out.lo[a] = std::min(out.lo[a], p[a]);
-            out.hi[a] = std::max(out.hi[a], p[a]);
-        }
-    }
 }
 
 // near.rs:41-106: for each i, the j >= i within `radius` (i included), ascending.
@@ -309,100 +186,6 @@ void near_pairs(const std::vector<Bar> &bars, double radius, std::vector<std::ve
             if ((int64_t)other == idx || separation(bars[idx], bars[other]) < radius) keep.push_back(other);
         out[idx].swap(keep);
     });
-}
-
-// grid_kernel tabulated over |d_a| <= reach_a, z fastest (near.rs:134-170).
-struct KernelTable {
-    int64_t reach[3], dims[3];
-    std::vector<double> values;
-    KernelTable(const int64_t r[3], double spacing) {
-        for (int a = 0; a < 3; ++a) {
-            reach[a] = r[a];
-            dims[a] = 2 * r[a] + 1;
-        }
-        values.assign((size_t)(dims[0] * dims[1] * dims[2]), 0.0);
-        parallel_for(dims[0], 1, [&](int64_t x) {
-            for (int64_t y = 0; y < dims[1]; ++y)
-                for (int64_t z = 0; z < dims[2]; ++z)
-                    values[(x * dims[1] + y) * dims[2] + z] =
-                        grid_kernel(x - reach[0], y - reach[1], z - reach[2], spacing);
-        });
-    }
-    size_t index(int64_t dx, int64_t dy, int64_t dz) const {
-        return (size_t)(((dx + reach[0]) * dims[1] + (dy + reach[1])) * dims[2] + (dz + reach[2]));
-    }
-};
-
-// sum_g sum_h W_ig W_jh K(g - h) for every partner j of row i (near.rs:323-401).
-void grid_interactions(const PfftGrid &g, const std::vector<Projection> &proj, int64_t i,
-                       const std::vector<uint32_t> &partners, const KernelTable &table, std::vector<double> &out) {
-    const Projection &own = proj[i];
-    std::vector<std::array<int64_t, 3>> src_pt(own.entries.size());
-    for (size_t s = 0; s < own.entries.size(); ++s) {
-        int64_t p[3];
-        point_of(g, own.entries[s].first, p);
-        src_pt[s] = {p[0], p[1], p[2]};
-    }
-    int64_t lo[3], hi[3];
-    for (int a = 0; a < 3; ++a) {
-        lo[a] = std::numeric_limits<int64_t>::max();
-        hi[a] = 0;
-    }
-    int64_t partner_entries = 0;
-    for (uint32_t j : partners) {
-        for (int a = 0; a < 3; ++a) {
-            lo[a] = std::min(lo[a], proj[j].lo[a]);
-            hi[a] = std::max(hi[a], proj[j].hi[a]);
-        }
-        partner_entries += (int64_t)proj[j].entries.size();
-    }
-    const int64_t bx = hi[0] - lo[0] + 1, by = hi[1] - lo[1] + 1, bz = hi[2] - lo[2] + 1;
-    const int64_t box_len = bx * by * bz;
-    const int64_t ns = (int64_t)src_pt.size();
-    const int64_t direct_cost = ns * partner_entries;
-    const int64_t box_cost = ns * box_len + partner_entries;
-    out.assign(partners.size(), 0.0);
-    if (direct_cost <= box_cost) {
-        for (size_t q = 0; q < partners.size(); ++q) {
-            double total = 0.0;
-            for (const auto &e : proj[partners[q]].entries) {
-                int64_t h[3];
-                point_of(g, e.first, h);
-                double potential = 0.0;
-                for (int64_t s = 0; s < ns; ++s)
-                    potential += own.entries[s].second *
-                                 table.values[table.index(h[0] - src_pt[s][0], h[1] - src_pt[s][1], h[2] - src_pt[s][2])];
-                total += e.second * potential;
-            }
-            out[q] = total;
-        }
-        return;
-    }
-    std::vector<double> psi((size_t)box_len, 0.0);
-    for (int64_t s = 0; s < ns; ++s) {
-        const double wg = own.entries[s].second;
-        const int64_t *gp = src_pt[s].data();
-        for (int64_t x = 0; x < bx; ++x) {
-            const int64_t at0 = lo[0] + x - gp[0] + table.reach[0];
-            size_t start = (size_t)((at0 * table.dims[1] + (lo[1] - gp[1] + table.reach[1])) * table.dims[2] +
-                                    (lo[2] - gp[2] + table.reach[2]));
-            for (int64_t y = 0; y < by; ++y) {
-                const double *k = &table.values[start];
-                double *row = &psi[(size_t)((x * by + y) * bz)];
-                for (int64_t z = 0; z < bz; ++z) row[z] += wg * k[z];
-                start += (size_t)table.dims[2];
-            }
-        }
-    }
-    for (size_t q = 0; q < partners.size(); ++q) {
-        double total = 0.0;
-        for (const auto &e : proj[partners[q]].entries) {
-            int64_t p[3];
-            point_of(g, e.first, p);
-            total += e.second * psi[(size_t)(((p[0] - lo[0]) * by + (p[1] - lo[1])) * bz + (p[2] - lo[2]))];
-        }
-        out[q] = total;
-    }
 }
 
 }  // namespace
@@ -483,86 +266,24 @@ fh_status pfft_setup(const fh_filament *fil, int64_t n, const PfftConfig &cfg, P
                         std::to_string((long long)kMaxFftPoints));
     const double radius = cfg.near_field_radius * h;
 
-    // Projections.
-    std::vector<Rule> rules(kQuadratureMaxOrder + 1);
-    for (int k = 1; k <= kQuadratureMaxOrder; ++k) {
-        rules[k].x.resize(k);
-        rules[k].w.resize(k);
-        gauss_rule(k, rules[k].x.data(), rules[k].w.data());
-    }
-    const OrderTable table;
-    std::vector<Projection> proj((size_t)n);
-    parallel_for(n, 16, [&](int64_t i) { project(g, fil[i], radius, table, rules, proj[i]); });
+    out.radius = radius;
 
-    // Near pairs and the non-orthogonal partners of each row.
+    // Near pairs and the non-orthogonal partners of each row, row-major.
     std::vector<Bar> bars((size_t)n);
     for (int64_t i = 0; i < n; ++i) bars[i] = bar_of(fil[i]);
     std::vector<std::vector<uint32_t>> near;
     near_pairs(bars, radius, near);
-    std::vector<std::vector<uint32_t>> partners((size_t)n);
-    parallel_for(n, 256, [&](int64_t i) {
-        for (uint32_t j : near[i])
-            if (std::fabs(dot3(fil[i].dir_length, fil[j].dir_length)) >= kOrthogonalCos) partners[i].push_back(j);
-    });
-
-    // Offsets the precorrection evaluates (near.rs:244-253).
-    int64_t reach[3] = {0, 0, 0};
+    out.pair_off.assign((size_t)n + 1, 0);
     for (int64_t i = 0; i < n; ++i) {
-        if (partners[i].empty()) continue;
-        int64_t plo[3], phi[3];
-        for (int a = 0; a < 3; ++a) {
-            plo[a] = std::numeric_limits<int64_t>::max();
-            phi[a] = 0;
-        }
-        for (uint32_t j : partners[i])
-            for (int a = 0; a < 3; ++a) {
-                plo[a] = std::min(plo[a], proj[j].lo[a]);
-                phi[a] = std::max(phi[a], proj[j].hi[a]);
-            }
-        const Projection &own = proj[i];
-        for (int a = 0; a < 3; ++a) {
-            const int64_t r = std::max(phi[a] - std::min(own.lo[a], phi[a]), own.hi[a] - std::min(plo[a], own.hi[a]));
-            reach[a] = std::max(reach[a], r);
-        }
-    }
-    const KernelTable ktable(reach, h);
-
-    std::vector<std::vector<double>> approx((size_t)n);
-    parallel_for(n, 4, [&](int64_t i) {
-        if (!partners[i].empty()) grid_interactions(g, proj, i, partners[i], ktable, approx[i]);
-    });
-
-    for (int64_t i = 0; i < n; ++i)
-        for (size_t q = 0; q < partners[i].size(); ++q) {
-            const uint32_t j = partners[i][q];
+        for (uint32_t j : near[i]) {
+            const double c = dot3(fil[i].dir_length, fil[j].dir_length);
+            if (std::fabs(c) < kOrthogonalCos) continue;
             out.pair_i.push_back((int32_t)i);
             out.pair_j.push_back((int32_t)j);
-            out.pair_grid.push_back(approx[i][q]);
-            out.pair_cos.push_back(dot3(fil[i].dir_length, fil[j].dir_length));
+            out.pair_cos.push_back(c);
         }
-
-    // Projection CSR and its transpose (pfft/mod.rs:405-431).
-    out.proj_offsets.assign((size_t)n + 1, 0);
-    std::vector<int64_t> counts((size_t)g.len(), 0);
-    for (int64_t i = 0; i < n; ++i) {
-        for (const auto &e : proj[i].entries) {
-            out.proj_index.push_back(e.first);
-            out.proj_weight.push_back(e.second);
-            counts[e.first] += 1;
-        }
-        out.proj_offsets[i + 1] = (int64_t)out.proj_index.size();
+        out.pair_off[(size_t)i + 1] = (int64_t)out.pair_i.size();
     }
-    out.spread_offsets.assign((size_t)g.len() + 1, 0);
-    for (int64_t p = 0; p < g.len(); ++p) out.spread_offsets[p + 1] = out.spread_offsets[p] + counts[p];
-    std::vector<int64_t> fill(out.spread_offsets.begin(), out.spread_offsets.end() - 1);
-    out.spread_filament.assign(out.proj_index.size(), 0);
-    out.spread_weight.assign(out.proj_index.size(), 0.0);
-    for (int64_t i = 0; i < n; ++i)
-        for (const auto &e : proj[i].entries) {
-            const int64_t slot = fill[e.first]++;
-            out.spread_filament[slot] = (uint32_t)i;
-            out.spread_weight[slot] = e.second;
-        }
     out.directions.resize((size_t)n * 3);
     for (int64_t i = 0; i < n; ++i)
         for (int a = 0; a < 3; ++a) out.directions[3 * i + a] = fil[i].dir_length[a];

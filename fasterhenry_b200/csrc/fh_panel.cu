@@ -200,34 +200,54 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_k
             const Cx<T> inv = cdiv(one, P[s0 + c]);
             best = -1.0;
             bi = INT_MAX;
-            // All loads of a row's sub-panel entries (kR at a time) are issued
-            // before any of them is used, so a row costs one or two memory
-            // latencies, not w - c.
-            constexpr int kR = sizeof(T) == 4 ? kW : kW / 2;
-            for (int64_t i = max(r_begin, j + 1) + tid; i < r_end; i += kThreads) {
-                const Cx<T> l = cmul(ldcg(A + i + j * m), inv);
-                A[i + j * m] = l;
+            // Rows go kG at a time (their column-j entries loaded together),
+            // then the sub-panel columns right of j kQ at a time for all kG
+            // rows, so a group of rows costs a few memory latencies instead of
+            // two per row.  Each row's arithmetic and the arg-max order (rows
+            // ascending per thread, ties keep the first) are unchanged.
+            constexpr int kG = 4;
+            constexpr int kQ = 4;
+            for (int64_t ib = max(r_begin, j + 1) + tid; ib < r_end; ib += (int64_t)kG * kThreads) {
+                Cx<T> l[kG];
 #pragma unroll
-                for (int h = 0; h < kW; h += kR) {
-                    if (h + kR <= c + 1 || h >= w) continue;
-                    Cx<T> y[kR];
+                for (int g = 0; g < kG; ++g) {
+                    const int64_t i = ib + (int64_t)g * kThreads;
+                    if (i < r_end) l[g] = ldcg(A + i + j * m);
+                }
 #pragma unroll
-                    for (int q = 0; q < kR; ++q)
-                        if (h + q > c && h + q < w) y[q] = ldcg(A + i + (k0 + h + q) * m);
+                for (int g = 0; g < kG; ++g) {
+                    const int64_t i = ib + (int64_t)g * kThreads;
+                    if (i < r_end) {
+                        l[g] = cmul(l[g], inv);
+                        A[i + j * m] = l[g];
+                    }
+                }
+                for (int q0 = c + 1; q0 < w; q0 += kQ) {
+                    Cx<T> y[kG][kQ];
 #pragma unroll
-                    for (int q = 0; q < kR; ++q) {
-                        if (h + q > c && h + q < w) {
-                            csubmul(y[q], P[s0 + h + q], l);
-                            A[i + (k0 + h + q) * m] = y[q];
-                            if (h + q == c + 1) {
-                                const double n1 = (double)(fabs(y[q].re) + fabs(y[q].im));
-                                if (n1 > best) {  // rows ascend per thread: ties keep the first
-                                    best = n1;
-                                    bi = (int)i;
+                    for (int g = 0; g < kG; ++g)
+#pragma unroll
+                        for (int qq = 0; qq < kQ; ++qq) {
+                            const int64_t i = ib + (int64_t)g * kThreads;
+                            if (i < r_end && q0 + qq < w) y[g][qq] = ldcg(A + i + (k0 + q0 + qq) * m);
+                        }
+#pragma unroll
+                    for (int g = 0; g < kG; ++g)
+#pragma unroll
+                        for (int qq = 0; qq < kQ; ++qq) {
+                            const int64_t i = ib + (int64_t)g * kThreads;
+                            if (i < r_end && q0 + qq < w) {
+                                csubmul(y[g][qq], P[s0 + q0 + qq], l[g]);
+                                A[i + (k0 + q0 + qq) * m] = y[g][qq];
+                                if (q0 + qq == c + 1) {
+                                    const double n1 = (double)(fabs(y[g][qq].re) + fabs(y[g][qq].im));
+                                    if (n1 > best) {  // rows ascend per thread: ties keep the first
+                                        best = n1;
+                                        bi = (int)i;
+                                    }
                                 }
                             }
                         }
-                    }
                 }
             }
             fused = c + 1 < w;

@@ -254,7 +254,7 @@ fh_status sweep_chunk_fp64(fh_system *s, const double *d_omega, int count, doubl
         e = coop_plan<double>(count, m, &per_matrix, &coop_bytes, err, s->share);
         if (e) return e;
         FHB_PALLOC(s->pool, coop_mem, kSlotCoop, coop_bytes);
-        coop_bind<double>(coop_mem.p, count, per_matrix, cs);
+        coop_bind<double>(coop_mem.p, count, per_matrix, cs, s->share);
         w.coop = &cs;
         PBuf<double> linv_mem;
         FHB_PALLOC(s->pool, linv_mem, kSlotLinv, (size_t)count * kNbFp64 * kNbFp64 * 2);
@@ -344,7 +344,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     e = coop_plan<float>(count, m, &per_matrix, &coop_bytes, err, s->share);
     if (e) return e;
     FHB_PALLOC(pool, coop_mem, kSlotCoop, coop_bytes);
-    coop_bind<float>(coop_mem.p, count, per_matrix, cs);
+    coop_bind<float>(coop_mem.p, count, per_matrix, cs, s->share);
     w.coop = &cs;
     const int outer = outer_for(m, mode);
     // Two-level form: the inverses of every diagonal block of L and U are

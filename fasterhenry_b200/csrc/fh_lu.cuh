@@ -29,6 +29,7 @@ struct CoopScratch {
     void *cand_data = nullptr;    // candidate rows, count * per_matrix * 2 * 128 complex
     void *rowj = nullptr;         // row j of each matrix, count * 2 * 128 complex
     int per_matrix = 0;           // CTAs per matrix
+    bool cluster = false;         // the CTAs of a matrix form one thread-block cluster
 };
 
 // Workspace for the factorization (pivot search partials).  With `coop`
@@ -68,7 +69,12 @@ struct LuWork {
 template <class T>
 fh_status coop_plan(int count, int64_t m, int *per_matrix, size_t *bytes, fh_error_info *err, int share = 1);
 template <class T>
-void coop_bind(void *mem, int count, int per_matrix, CoopScratch &cs);
+void coop_bind(void *mem, int count, int per_matrix, CoopScratch &cs, int share = 1);
+// Whether coop_plan's per_matrix CTAs of type T run as one cluster per
+// matrix: when every cluster of `count` matrices (times `share` concurrent
+// sweeps) is resident at once.
+template <class T>
+bool coop_cluster(int count, int per_matrix, int share = 1);
 template <class T>
 fh_status panel_coop(LuBatch<T> &b, int64_t K0, int nb, const CoopScratch &cs, cudaStream_t s, fh_error_info *err);
 fh_status coop_check(const CoopScratch &cs, cudaStream_t s, fh_error_info *err);

@@ -27,6 +27,8 @@
 // the CTAs of one matrix (a counter per matrix) and are bounded: a barrier
 // that gives up sets the error flag, which stays set for the whole
 // factorization, and every CTA returns.
+#include <cooperative_groups.h>
+
 #include <climits>
 
 #include "fh_cx.cuh"
@@ -51,7 +53,12 @@ struct CoopArgs {
     int per_matrix;
 };
 
-template <class T>
+// kCluster: the CTAs of one matrix form a thread-block cluster (one
+// cluster per matrix); the pivot candidates and the rows they carry are
+// exchanged through distributed shared memory, and the matrix's barriers are
+// the cluster's hardware barrier.  Otherwise the CTAs of a cooperative launch
+// exchange them through global memory and meet at a bounded counter barrier.
+template <class T, bool kCluster>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_kernel(Cx<T> *__restrict__ a, int64_t m, int64_t K0, int NB,
                                                               int *__restrict__ pivots, int *__restrict__ singular,
                                                               CoopArgs args) {
@@ -73,6 +80,13 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_k
     __shared__ double s_val[kThreads / 32];
     __shared__ int s_idx[kThreads / 32];
     __shared__ int s_best_slot, s_piv;
+    // Cluster form: this CTA's candidate (value, row, its panel row) and, on
+    // the owner of row j, row j, double-buffered by the parity of j.
+    __shared__ double c_val[kCluster ? 2 : 1];
+    __shared__ int c_row[kCluster ? 2 : 1];
+    __shared__ Cx<T> c_data[kCluster ? 2 : 1][kCluster ? kNbMax : 1];
+    __shared__ Cx<T> c_rowj[kCluster ? 2 : 1][kCluster ? kNbMax : 1];
+    const int64_t rows_chunk = chunk;
 
     auto better = [](double v2, int i2, double v1, int i1) { return v2 > v1 || (v2 == v1 && i2 < i1); };
 
@@ -120,9 +134,14 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_k
                         best = s_val[q];
                         bi = s_idx[q];
                     }
-                const int slot = (f * per_matrix + slice) * 2 + par;
-                args.cand_val[slot] = best;
-                args.cand_row[slot] = bi == INT_MAX ? -1 : bi;
+                if constexpr (kCluster) {
+                    c_val[par] = best;
+                    c_row[par] = bi == INT_MAX ? -1 : bi;
+                } else {
+                    const int slot = (f * per_matrix + slice) * 2 + par;
+                    args.cand_val[slot] = best;
+                    args.cand_row[slot] = bi == INT_MAX ? -1 : bi;
+                }
                 s_idx[0] = bi;
             }
             __syncthreads();
@@ -130,23 +149,46 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_k
                 const int brow = s_idx[0];
                 const int slot = (f * per_matrix + slice) * 2 + par;
                 if (brow != INT_MAX)
-                    for (int t = tid; t < NB; t += kThreads)
-                        cand_data[(int64_t)slot * kNbMax + t] = ldcg(A + brow + (K0 + t) * m);
+                    for (int t = tid; t < NB; t += kThreads) {
+                        const Cx<T> v = ldcg(A + brow + (K0 + t) * m);
+                        if constexpr (kCluster)
+                            c_data[par][t] = v;
+                        else
+                            cand_data[(int64_t)slot * kNbMax + t] = v;
+                    }
                 if (j >= r_begin && j < r_end)
-                    for (int t = tid; t < NB; t += kThreads)
-                        rowj_buf[(int64_t)(f * 2 + par) * kNbMax + t] = ldcg(A + j + (K0 + t) * m);
+                    for (int t = tid; t < NB; t += kThreads) {
+                        const Cx<T> v = ldcg(A + j + (K0 + t) * m);
+                        if constexpr (kCluster)
+                            c_rowj[par][t] = v;
+                        else
+                            rowj_buf[(int64_t)(f * 2 + par) * kNbMax + t] = v;
+                    }
             }
             // 2. every CTA's candidate is published
-            if (!group_barrier(bar, (unsigned)per_matrix, args.error)) return;
+            if constexpr (kCluster) {
+                cooperative_groups::this_cluster().sync();
+            } else {
+                if (!group_barrier(bar, (unsigned)per_matrix, args.error)) return;
+            }
             // 3. the pivot (warp 0 reduces the candidates of this matrix), and
             //    the interchange of rows j and p
             double bv = -1.0;
             int brow = INT_MAX, bslot = -1;
             if (warp == 0) {
                 for (int q = lane; q < per_matrix; q += 32) {
-                    const int slot = (f * per_matrix + q) * 2 + par;
-                    const double v2 = __ldcg(args.cand_val + slot);
-                    const int r2 = __ldcg(args.cand_row + slot);
+                    double v2;
+                    int r2, slot;
+                    if constexpr (kCluster) {
+                        auto cl = cooperative_groups::this_cluster();
+                        v2 = *cl.map_shared_rank(&c_val[par], (unsigned)q);
+                        r2 = *cl.map_shared_rank(&c_row[par], (unsigned)q);
+                        slot = q;
+                    } else {
+                        slot = (f * per_matrix + q) * 2 + par;
+                        v2 = __ldcg(args.cand_val + slot);
+                        r2 = __ldcg(args.cand_row + slot);
+                    }
                     if (r2 >= 0 && better(v2, r2, bv, brow)) {
                         bv = v2;
                         brow = r2;
@@ -181,10 +223,21 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_k
             }
             __syncthreads();
             const int p = s_piv, pslot = s_best_slot;
-            for (int t = tid; t < NB; t += kThreads) {
-                const Cx<T> rj = ldcg(rowj_buf + (int64_t)(f * 2 + par) * kNbMax + t);
-                Rj[t] = rj;
-                P[t] = pslot >= 0 ? ldcg(cand_data + (int64_t)pslot * kNbMax + t) : rj;
+            if constexpr (kCluster) {
+                auto cl = cooperative_groups::this_cluster();
+                const unsigned owner_j = (unsigned)((j - K0) / rows_chunk);
+                const Cx<T> *rj_src = cl.map_shared_rank(&c_rowj[par][0], owner_j);
+                const Cx<T> *p_src = pslot >= 0 ? cl.map_shared_rank(&c_data[par][0], (unsigned)pslot) : rj_src;
+                for (int t = tid; t < NB; t += kThreads) {
+                    Rj[t] = rj_src[t];
+                    P[t] = p_src[t];
+                }
+            } else {
+                for (int t = tid; t < NB; t += kThreads) {
+                    const Cx<T> rj = ldcg(rowj_buf + (int64_t)(f * 2 + par) * kNbMax + t);
+                    Rj[t] = rj;
+                    P[t] = pslot >= 0 ? ldcg(cand_data + (int64_t)pslot * kNbMax + t) : rj;
+                }
             }
             __syncthreads();
             if (p != (int)j) {
@@ -205,8 +258,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_k
             // rows, so a group of rows costs a few memory latencies instead of
             // two per row.  Each row's arithmetic and the arg-max order (rows
             // ascending per thread, ties keep the first) are unchanged.
-            constexpr int kG = 4;
-            constexpr int kQ = 4;
+            constexpr int kG = sizeof(T) == 4 ? 4 : 2;
+            constexpr int kQ = sizeof(T) == 4 ? 4 : 2;
             for (int64_t ib = max(r_begin, j + 1) + tid; ib < r_end; ib += (int64_t)kG * kThreads) {
                 Cx<T> l[kG];
 #pragma unroll
@@ -255,7 +308,11 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_k
         const int rest = NB - s0 - w;  // outer-panel columns right of the sub-panel
         if (rest <= 0) continue;
         // 5. the sub-panel is final everywhere
-        if (!group_barrier(bar, (unsigned)per_matrix, args.error)) return;
+        if constexpr (kCluster) {
+            cooperative_groups::this_cluster().sync();
+        } else {
+            if (!group_barrier(bar, (unsigned)per_matrix, args.error)) return;
+        }
         // 6. U12 of the sub-panel: rows [k0, k0+w), columns [k0+w, K0+NB)
         if (slice == 0) {
             // the unit lower w x w block, staged once (U doubles as its buffer)
@@ -283,7 +340,11 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_k
             }
         }
         // 7. U12 is visible to every CTA (and slice 0 is done with U)
-        if (!group_barrier(bar, (unsigned)per_matrix, args.error)) return;
+        if constexpr (kCluster) {
+            cooperative_groups::this_cluster().sync();
+        } else {
+            if (!group_barrier(bar, (unsigned)per_matrix, args.error)) return;
+        }
         // 8. own rows i >= k0+w: A[i, k0+w ..] -= A[i, k0 .. k0+w) U12
         for (int idx = tid; idx < w * rest; idx += kThreads) {
             const int r = idx / rest, t = idx % rest;
@@ -333,9 +394,41 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_k
         fused = true;
         __syncthreads();
     }
+    // No CTA leaves while another may still read its shared memory.
+    if constexpr (kCluster) cooperative_groups::this_cluster().sync();
 }
 
 }  // namespace
+
+// Largest cluster of CTAs of the cluster form that the device can schedule
+// (0: none), for sizes up to kMaxCluster.
+constexpr int kMaxCluster = 16;
+
+template <class T>
+int cluster_fits(int size) {
+    if (size < 2 || size > kMaxCluster) return 0;
+    auto kernel = panel_coop_kernel<T, true>;
+    if (size > 8 && cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)size);
+    cfg.blockDim = dim3(kThreads);
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = (unsigned)size;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, (void *)kernel, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return clusters;
+}
 
 template <class T>
 fh_status coop_plan(int count, int64_t m, int *per_matrix, size_t *bytes, fh_error_info *err, int share) {
@@ -344,10 +437,19 @@ fh_status coop_plan(int count, int64_t m, int *per_matrix, size_t *bytes, fh_err
     FHB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     FHB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     if (!coop) return fail(err, FH_ERR_NO_DEVICE, "the device does not support cooperative launches");
-    FHB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_coop_kernel<T>, kThreads, 0));
+    FHB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_coop_kernel<T, false>, kThreads, 0));
     const int capacity = occ * sms / std::max(1, share);
     int pm = std::max(1, capacity / std::max(1, count));
     pm = (int)std::min<int64_t>(pm, std::max<int64_t>(1, (m + 63) / 64));
+    // A batch whose matrices get at most kMaxCluster CTAs each runs them as
+    // one cluster per matrix, of the largest size at which every matrix's
+    // cluster (of every sweep sharing the device) is resident at once: a
+    // second wave of clusters would double the panel's time.
+    if (pm >= 2 && pm <= kMaxCluster) {
+        int size = pm;
+        while (size >= 2 && cluster_fits<T>(size) < count * std::max(1, share)) --size;
+        if (size >= 2) pm = size;
+    }
     if ((int64_t)pm * count > capacity)
         return fail(err, FH_ERR_INVALID_ARGUMENT, "batch too large for one cooperative panel launch");
     *per_matrix = pm;
@@ -358,7 +460,13 @@ fh_status coop_plan(int count, int64_t m, int *per_matrix, size_t *bytes, fh_err
 }
 
 template <class T>
-void coop_bind(void *mem, int count, int per_matrix, CoopScratch &cs) {
+bool coop_cluster(int count, int per_matrix, int share) {
+    return per_matrix >= 2 && per_matrix <= kMaxCluster &&
+           cluster_fits<T>(per_matrix) >= count * std::max(1, share);
+}
+
+template <class T>
+void coop_bind(void *mem, int count, int per_matrix, CoopScratch &cs, int share) {
     unsigned char *p = static_cast<unsigned char *>(mem);
     const size_t slots = (size_t)count * per_matrix * 2;
     // [error flag, 128 B] [one 128-byte barrier per matrix] [candidates] [rows j]
@@ -374,6 +482,7 @@ void coop_bind(void *mem, int count, int per_matrix, CoopScratch &cs) {
     off += slots * kNbMax * sizeof(Cx<T>);
     cs.rowj = p + off;
     cs.per_matrix = per_matrix;
+    cs.cluster = coop_cluster<T>(count, per_matrix, share);
 }
 
 template <class T>
@@ -387,9 +496,24 @@ fh_status panel_coop(LuBatch<T> &b, int64_t K0, int nb, const CoopScratch &cs, c
     CoopArgs args{cs.barrier, cs.error, cs.cand_val, cs.cand_row, cs.cand_data, cs.rowj, cs.per_matrix};
     Cx<T> *a = reinterpret_cast<Cx<T> *>(b.a);
     int64_t m = b.m;
+    if (cs.cluster) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(cs.per_matrix * b.count));
+        cfg.blockDim = dim3(kThreads);
+        cfg.stream = s;
+        cudaLaunchAttribute attr;
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = (unsigned)cs.per_matrix;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        FHB_CUDA(cudaLaunchKernelEx(&cfg, panel_coop_kernel<T, true>, a, m, K0, nb, b.pivots, b.singular, args));
+        return FH_OK;
+    }
     void *params[] = {&a, &m, &K0, &nb, &b.pivots, &b.singular, &args};
-    FHB_CUDA(cudaLaunchCooperativeKernel((const void *)panel_coop_kernel<T>, dim3(cs.per_matrix * b.count), dim3(kThreads),
-                                         params, 0, s));
+    FHB_CUDA(cudaLaunchCooperativeKernel((const void *)panel_coop_kernel<T, false>, dim3(cs.per_matrix * b.count),
+                                         dim3(kThreads), params, 0, s));
     return FH_OK;
 }
 
@@ -403,8 +527,10 @@ fh_status coop_check(const CoopScratch &cs, cudaStream_t s, fh_error_info *err) 
 
 template fh_status coop_plan<double>(int, int64_t, int *, size_t *, fh_error_info *, int);
 template fh_status coop_plan<float>(int, int64_t, int *, size_t *, fh_error_info *, int);
-template void coop_bind<double>(void *, int, int, CoopScratch &);
-template void coop_bind<float>(void *, int, int, CoopScratch &);
+template void coop_bind<double>(void *, int, int, CoopScratch &, int);
+template void coop_bind<float>(void *, int, int, CoopScratch &, int);
+template bool coop_cluster<double>(int, int, int);
+template bool coop_cluster<float>(int, int, int);
 template fh_status panel_coop<double>(LuBatch<double> &, int64_t, int, const CoopScratch &, cudaStream_t, fh_error_info *);
 template fh_status panel_coop<float>(LuBatch<float> &, int64_t, int, const CoopScratch &, cudaStream_t, fh_error_info *);
 

@@ -30,6 +30,7 @@
 #include <cooperative_groups.h>
 
 #include <climits>
+#include <mutex>
 
 #include "fh_cx.cuh"
 #include "fh_lu.cuh"
@@ -405,8 +406,31 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) panel_coop_k
 constexpr int kMaxCluster = 16;
 
 template <class T>
+int cluster_fits_query(int size);
+
+// cluster_fits_query, asked once per device and size (the occupancy query
+// costs milliseconds; sweeps ask on every batch).
+template <class T>
 int cluster_fits(int size) {
     if (size < 2 || size > kMaxCluster) return 0;
+    static std::mutex mu;
+    static int known[64][kMaxCluster + 1];
+    static bool asked[64][kMaxCluster + 1] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return 0;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    if (!asked[dev][size]) {
+        known[dev][size] = cluster_fits_query<T>(size);
+        asked[dev][size] = true;
+    }
+    return known[dev][size];
+}
+
+template <class T>
+int cluster_fits_query(int size) {
     auto kernel = panel_coop_kernel<T, true>;
     if (size > 8 && cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
         cudaGetLastError();

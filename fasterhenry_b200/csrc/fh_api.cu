@@ -376,6 +376,10 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
         w.outer = outer;
         w.pack_a = pack_a.p;
         w.pack_b = pack_b.p;
+        // Z_ee = R_ee + jw L_ee with R_ee, L_ee symmetric positive definite:
+        // the FP32 factors go without pivoting (stable for this class; the
+        // FP64 residual refinement and its FP64 fallback decide the result).
+        w.nopivot = true;
     }
     LuBatch<float> b;
     b.a = a.p;

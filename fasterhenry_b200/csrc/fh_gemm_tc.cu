@@ -239,8 +239,9 @@ __device__ __forceinline__ void load_chunk(const GemmArgs &g, int f, int64_t row
 
 // C (M x N) = C - A B  (assign == 0)  or  C = A B  (assign == 1), batched over
 // blockIdx.z; K a multiple of 16.  In the assign form C may be B itself when
-// M <= 128 (one tile row): a CTA reads all of its B columns before it writes
-// them, and no other CTA reads them.
+// M <= 128 (one tile row), or A itself when N <= 128 (one tile column): a CTA
+// reads all of the aliased operand's part it writes before the epilogue
+// writes it, and no other CTA reads that part.
 __global__ void __launch_bounds__(kThreads, 2) gemm_bf16x3_kernel(GemmArgs g, int *__restrict__ err_flag) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -373,7 +374,12 @@ int *g_err_flag[64] = {nullptr};
 fh_status gemm_tc_launch(const GemmArgs &g, int count, cudaStream_t s, fh_error_info *err) {
     if (g.K % kChunk) return fail(err, FH_ERR_INVALID_ARGUMENT, "tensor-core GEMM needs K a multiple of 16");
     if (g.M <= 0 || g.N <= 0 || g.K <= 0) return FH_OK;
-    if (g.assign && g.M > kTileM) return fail(err, FH_ERR_INVALID_ARGUMENT, "in-place assign GEMM needs M <= 128");
+    // In place (C aliasing B, or C aliasing A) is safe when each tile reads
+    // the part of the aliased operand it writes and nothing else reads it:
+    // one tile along M (C = B) or along N (C = A).  The caller aliases the
+    // operand that matches.
+    if (g.assign && g.M > kTileM && g.N > kTileN)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "in-place assign GEMM needs M <= 128 or N <= 128");
     int dev = 0;
     FHB_CUDA(cudaGetDevice(&dev));
     static std::mutex init_mu;  // first use on a device may race between host threads

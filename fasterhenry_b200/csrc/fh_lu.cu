@@ -418,6 +418,47 @@ __global__ void __launch_bounds__(128) bwd_panel_kernel2(const Cx<T> *__restrict
 // (contiguous in memory) fetched while step k computes.
 // Grid (count, ceil(nb / 32)), 256 threads; dynamic shared memory
 // (32 nb + 2 nb) complex.
+// LU without pivoting of the nb x nb diagonal block at (k0, k0) of every
+// matrix, in shared memory (CTA per matrix): L unit lower below the
+// diagonal, U on and above it.  For A = R + jwL with R and L symmetric
+// positive definite (a mesh impedance matrix) elimination without pivoting
+// is stable (the growth factor is bounded); a zero or non-finite pivot of
+// any other matrix shows as a non-finite refinement correction, and the
+// caller falls back to the pivoted FP64 factorization.
+__global__ void __launch_bounds__(512) diag_lu_kernel(Cx<float> *__restrict__ a, int64_t m, int64_t k0, int nb) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<float> *S = reinterpret_cast<Cx<float> *>(smem_raw);  // column-major, ld nb
+    Cx<float> *A = a + (int64_t)blockIdx.x * m * m;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int idx = tid; idx < nb * nb; idx += nt) {
+        const int r = idx % nb, c = idx / nb;
+        S[idx] = A[(k0 + r) + (k0 + c) * m];
+    }
+    for (int k = 0; k < nb; ++k) {
+        __syncthreads();
+        const Cx<float> one{1.0f, 0.0f};
+        const Cx<float> inv = cdiv(one, S[k + k * nb]);
+        for (int r = k + 1 + tid; r < nb; r += nt) S[r + k * nb] = cmul(S[r + k * nb], inv);
+        __syncthreads();
+        const int rest = nb - k - 1;
+        for (int idx = tid; idx < rest * rest; idx += nt) {
+            const int r = k + 1 + idx % rest, c = k + 1 + idx / rest;
+            csubmul(S[r + c * nb], S[r + k * nb], S[k + c * nb]);
+        }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < nb * nb; idx += nt) {
+        const int r = idx % nb, c = idx / nb;
+        A[(k0 + r) + (k0 + c) * m] = S[idx];
+    }
+}
+
+// pivots[f m + k] = k: the identity interchanges of a factorization without pivoting.
+__global__ void identity_pivots_kernel(int *__restrict__ pivots, int64_t total, int64_t m) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x)
+        pivots[t] = (int)(t % m);
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) tri_inverse_kernel(const Cx<T> *__restrict__ a, int64_t m, int k0, int nb,
                                                           Cx<T> *__restrict__ linv, int64_t mstride) {
@@ -783,6 +824,15 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
                                                                                         b.pivots);
     };
     fh_status st = FH_OK;
+    const bool nopivot = w.nopivot;
+    if (nopivot) {
+        if (!w.uinv) return fail(err, FH_ERR_INVALID_ARGUMENT, "the factorization without pivoting needs uinv");
+        const size_t diag_smem = sizeof(C) * (size_t)nb * nb;
+        FHB_CUDA(cudaFuncSetAttribute(diag_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem));
+        const int64_t total = (int64_t)count * m;
+        identity_pivots_kernel<<<grid_for(total, 256, 1024), 256, 0, s>>>(b.pivots, total, m);
+        FHB_CUDA(cudaGetLastError());
+    }
     for (int64_t K0 = 0; K0 < m; K0 += outer) {
         const int W = (int)std::min<int64_t>(outer, m - K0);
         const int64_t E = K0 + W;
@@ -790,12 +840,17 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             const int wj = (int)std::min<int64_t>(nb, E - j0);
             const int64_t r1 = j0 + wj;  // first row / column after the panel
             C *linv = slot(w.linv, j0);
+            const int64_t mstride = (int64_t)nb * nb;  // a partial last block keeps the full slot stride
             prof_begin(s, FH_PROF_PANEL);
-            st = panel_coop<float>(b, j0, wj, *w.coop, s, err);
+            if (nopivot) {
+                diag_lu_kernel<<<(unsigned)count, 512, sizeof(C) * (size_t)wj * wj, s>>>(a, m, j0, wj);
+                st = cudaGetLastError() == cudaSuccess ? FH_OK : fail(err, FH_ERR_CUDA, "diagonal block LU launch failed");
+            } else {
+                st = panel_coop<float>(b, j0, wj, *w.coop, s, err);
+            }
             prof_end(s, FH_PROF_PANEL, 0.0);
             if (st) return st;
             prof_begin(s, FH_PROF_TRSM);
-            const int64_t mstride = (int64_t)nb * nb;  // a partial last block keeps the full slot stride
             tri_inverse_kernel<float><<<inv_grid, 256, inv_smem, s>>>(a, m, (int)j0, wj, linv, mstride);
             if (w.uinv)
                 tri_inverse_upper_kernel<float><<<inv_grid, 256, inv_smem, s>>>(a, m, (int)j0, wj, slot(w.uinv, j0),
@@ -804,8 +859,16 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
                 prof_end(s, FH_PROF_TRSM, 0.0);
                 break;
             }
-            swaps(j0, wj, K0, j0);
-            swaps(j0, wj, r1, E);
+            if (nopivot) {
+                // L21 = A21 U11^-1 for the rows below the block (in place: each
+                // tile of L21 reads exactly its own rows of A21).
+                st = gemm_tc_strided(at(r1, j0), m, mm, reinterpret_cast<const float *>(slot(w.uinv, j0)), wj,
+                                     mstride, at(r1, j0), m, mm, m - r1, wj, wj, 1, count, s, err);
+                if (st) return st;
+            } else {
+                swaps(j0, wj, K0, j0);
+                swaps(j0, wj, r1, E);
+            }
             if (r1 < E)
                 st = gemm_tc_strided(reinterpret_cast<const float *>(linv), wj, mstride, at(j0, r1), m, mm,
                                      at(j0, r1), m, mm, wj, E - r1, wj, 1, count, s, err);
@@ -822,7 +885,7 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
         if (E >= m) break;
         const int64_t n2 = m - E;
         prof_begin(s, FH_PROF_TRSM);
-        swaps(K0, W, E, m);
+        if (!nopivot) swaps(K0, W, E, m);
         for (int64_t j0 = K0; j0 < E && !st; j0 += nb) {
             const C *linv = slot(w.linv, j0);
             st = gemm_tc_strided(reinterpret_cast<const float *>(linv), nb, (int64_t)nb * nb, at(j0, E), m, mm,

@@ -60,6 +60,11 @@ struct LuWork {
     int outer = 0;
     void *pack_a = nullptr;
     void *pack_b = nullptr;
+    // Two-level form without pivoting (for matrices with symmetric positive
+    // definite real and imaginary parts): each diagonal block is factored
+    // in shared memory and L21 = A21 U11^-1 formed on the tensor cores;
+    // pivots are the identity.
+    bool nopivot = false;
 };
 
 // Cooperative panel: sizing, binding of a scratch block, launch, error check.

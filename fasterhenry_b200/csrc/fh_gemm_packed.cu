@@ -39,6 +39,7 @@
 #include <stdint.h>
 
 #include <mutex>
+#include <vector>
 
 #include "fh_lu.cuh"
 
@@ -222,13 +223,24 @@ struct PackedArgs {
     int64_t ldc, sC;
     int64_t M, N;
     int rblocks, cblocks, nchunks;
-    long long tiles;  // count * rblocks * cblocks
+    long long tiles;  // count * tiles per matrix
+    // With a tile table: the (row block, column block) of each of a matrix's
+    // per_matrix tiles, packed rb | cb << 16, in schedule order.
+    const uint32_t *table;
+    long long per_matrix;
 };
 
 // Tile t -> (matrix, row block, column block).  Within a matrix, groups of
 // kGroupRows row blocks; inside a group the row block runs fastest, so the
 // CTAs of one wave share a few A blocks and a few B blocks.
 __device__ __forceinline__ void tile_coords(const PackedArgs &g, long long t, int &f, int &rb, int &cb) {
+    if (g.table) {
+        f = (int)(t / g.per_matrix);
+        const uint32_t e = g.table[t - (long long)f * g.per_matrix];
+        rb = (int)(e & 0xffffu);
+        cb = (int)(e >> 16);
+        return;
+    }
     const long long per = (long long)g.rblocks * g.cblocks;
     f = (int)(t / per);
     const long long r = t - (long long)f * per;
@@ -442,7 +454,7 @@ size_t packed_operand_bytes(int64_t rows, int K, int count) {
 
 fh_status gemm_tc_packed_update(const float *A, int64_t lda, int64_t sA, const float *B, int64_t ldb, int64_t sB,
                                 float *C, int64_t ldc, int64_t sC, int64_t M, int64_t N, int K, int count,
-                                void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err) {
+                                void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err, int lower_from) {
     if (K % kChunk || K <= 0) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update needs K a positive multiple of 16");
     if (M <= 0 || N <= 0 || count <= 0) return FH_OK;
     if (!pack_a || !pack_b) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update needs operand scratch");
@@ -479,12 +491,46 @@ fh_status gemm_tc_packed_update(const float *A, int64_t lda, int64_t sA, const f
     g.rblocks = rblocks;
     g.cblocks = cblocks;
     g.nchunks = nchunks;
-    g.tiles = (long long)count * rblocks * cblocks;
+    g.table = nullptr;
+    g.per_matrix = (long long)rblocks * cblocks;
+    double entries = (double)M * (double)N;  // complex C entries updated per matrix
+    uint32_t *d_table = nullptr;
+    if (lower_from >= 0 && lower_from < cblocks) {
+        // Lower-triangle form (symmetric trailing matrix, C rows and columns
+        // on the same blocks): column blocks below lower_from in full, the
+        // rest only on and below the diagonal block; the same grouped order
+        // as the full schedule (row blocks fastest inside groups of
+        // kGroupRows), invalid tiles left out.
+        std::vector<uint32_t> table;
+        table.reserve((size_t)rblocks * cblocks);
+        entries = 0.0;
+        for (int g0 = 0; g0 < rblocks; g0 += kGroupRows) {
+            const int rows = std::min(kGroupRows, rblocks - g0);
+            for (int cb = 0; cb < cblocks; ++cb)
+                for (int r = 0; r < rows; ++r) {
+                    const int rb = g0 + r;
+                    if (cb < lower_from || rb >= cb) {
+                        table.push_back((uint32_t)rb | ((uint32_t)cb << 16));
+                        entries += (double)std::min<int64_t>(kTile, M - (int64_t)rb * kTile) *
+                                   (double)std::min<int64_t>(kTile, N - (int64_t)cb * kTile);
+                    }
+                }
+        }
+        if (rblocks > 0xffff || cblocks > 0xffff)
+            return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update tile table overflow");
+        FHB_CUDA(cache_alloc((void **)&d_table, table.size() * 4, s));
+        FHB_CUDA(cudaMemcpyAsync(d_table, table.data(), table.size() * 4, cudaMemcpyHostToDevice, s));
+        g.table = d_table;
+        g.per_matrix = (long long)table.size();
+    }
+    g.tiles = (long long)count * g.per_matrix;
     const int grid = (int)std::min<long long>(g.tiles, (long long)std::max(1, g_sms[dev]));
     if (prof) prof_begin(s, FH_PROF_GEMM_TC);
     packed_update_kernel<<<grid, kThreads, kSmemBytes, s>>>(g, g_flag[dev]);
-    if (prof) prof_end(s, FH_PROF_GEMM_TC, 8.0 * (double)M * (double)N * (double)K * count);
-    FHB_CUDA(cudaGetLastError());
+    if (prof) prof_end(s, FH_PROF_GEMM_TC, 8.0 * entries * (double)K * count);
+    cudaError_t le = cudaGetLastError();
+    if (d_table) cache_free(d_table, s);  // stream-ordered: after the kernel
+    if (le != cudaSuccess) return fail(err, FH_ERR_CUDA, std::string("packed update launch failed: ") + cudaGetErrorString(le));
     return FH_OK;
 }
 

@@ -453,6 +453,26 @@ __global__ void __launch_bounds__(512) diag_lu_kernel(Cx<float> *__restrict__ a,
     }
 }
 
+// U[k, c] = U[k, k] L[c, k] for rows k in [K0, K0 + W) and columns c >= E:
+// the U12 block of a symmetric matrix factored without pivoting (U = D L^T).
+// 32 x 32 tiles through shared memory, so both the reads of L (down a column)
+// and the writes of U (along a row) are coalesced.
+__global__ void u12_from_l21_kernel(Cx<float> *__restrict__ a, int64_t m, int64_t K0, int W, int64_t E) {
+    __shared__ Cx<float> t[32][33];
+    Cx<float> *A = a + (int64_t)blockIdx.z * m * m;
+    const int64_t c0 = E + (int64_t)blockIdx.x * 32, k0 = K0 + (int64_t)blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int r = ty; r < 32; r += 8) {
+        const int64_t c = c0 + tx, k = k0 + r;
+        if (c < m && k < K0 + W) t[r][tx] = A[c + k * m];  // L[c, k]
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int64_t k = k0 + tx, c = c0 + r;
+        if (c < m && k < K0 + W) A[k + c * m] = cmul(A[k + k * m], t[tx][r]);
+    }
+}
+
 // pivots[f m + k] = k: the identity interchanges of a factorization without pivoting.
 __global__ void identity_pivots_kernel(int *__restrict__ pivots, int64_t total, int64_t m) {
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x)
@@ -885,7 +905,21 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
         if (E >= m) break;
         const int64_t n2 = m - E;
         prof_begin(s, FH_PROF_TRSM);
-        if (!nopivot) swaps(K0, W, E, m);
+        if (nopivot) {
+            // Symmetric trailing matrix: U12 = D L21^T (D the diagonal of U11).
+            const dim3 tg((unsigned)((n2 + 31) / 32), (unsigned)((W + 31) / 32), (unsigned)count);
+            u12_from_l21_kernel<<<tg, dim3(32, 8), 0, s>>>(a, m, K0, W, E);
+            FHB_CUDA(cudaGetLastError());
+            prof_end(s, FH_PROF_TRSM, 0.0);
+            // Only the lower triangle of the trailing matrix is read from here
+            // on, besides the next super-panel's columns, which are updated in full.
+            const int next = (int)((std::min<int64_t>(outer, n2) + 127) / 128);
+            st = gemm_tc_packed_update(at(E, K0), m, mm, at(K0, E), m, mm, at(E, E), m, mm, n2, n2, W, count,
+                                       w.pack_a, w.pack_b, s, err, next);
+            if (st) return st;
+            continue;
+        }
+        swaps(K0, W, E, m);
         for (int64_t j0 = K0; j0 < E && !st; j0 += nb) {
             const C *linv = slot(w.linv, j0);
             st = gemm_tc_strided(reinterpret_cast<const float *>(linv), nb, (int64_t)nb * nb, at(j0, E), m, mm,

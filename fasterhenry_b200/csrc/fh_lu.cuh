@@ -108,7 +108,7 @@ size_t packed_operand_bytes(int64_t rows, int K, int count);
 // persistent warp-specialized tensor-core kernel (fh_gemm_packed.cu).
 fh_status gemm_tc_packed_update(const float *A, int64_t lda, int64_t sA, const float *B, int64_t ldb, int64_t sB,
                                 float *C, int64_t ldc, int64_t sC, int64_t M, int64_t N, int K, int count,
-                                void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err);
+                                void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err, int lower_from = -1);
 fh_status gemm_tc_packed_check(fh_error_info *err);
 // One SIMT trailing update (FP32 or FP64), for tests.
 template <class T>

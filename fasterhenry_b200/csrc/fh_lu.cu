@@ -407,6 +407,208 @@ __global__ void __launch_bounds__(128) bwd_panel_kernel2(const Cx<T> *__restrict
     for (int r = threadIdx.x; r < nb; r += blockDim.x) X[k0 + r] = xs[r];
 }
 
+// The diagonal block of a factorization without pivoting, in one CTA per
+// matrix: the LU of the nb x nb block at (k0, k0) in place (L unit lower below
+// the diagonal, U on and above it), then L^{-1} into linv and U^{-1} into
+// uinv (matrix f at + f * mstride, column-major with leading dimension nb).
+// For A = R + jwL with R and L symmetric positive definite (a mesh impedance
+// matrix) elimination without pivoting is stable (the growth factor is
+// bounded); a zero or non-finite pivot of any other matrix shows as a
+// non-finite refinement correction, and the caller falls back to the pivoted
+// FP64 factorization.
+//
+// Each of the 512 threads keeps 32 entries in registers: rows lane + 32 i
+// (i < 4) of columns warp + 16 j (j < 8), so a column belongs to one warp and a
+// row to one lane of every warp.  Step k of the elimination reads column k
+// and row k of the block as step k - 1 left them; the owners write those
+// entries to a shared double buffer as soon as their own update of step k - 1
+// produces them (with the reciprocal of the next pivot), so a step costs one
+// barrier.  Row groups and columns a step does not touch are skipped with
+// warp-uniform tests.  The inverses run in the same registers with the
+// factors kept in shared memory: X = L^{-1} by forward elimination on the
+// rows of I (row k of X is final before step k), Y = U^{-1} backward (row k
+// scaled by 1 / U_kk at step k, every thread scaling the published row).
+// All register indices are compile-time constants, so the block never leaves
+// the register file.
+constexpr int kDiagThreads = 512;
+constexpr int kDiagSmemExtra = 2 * 128 + 2 * 128 + 128 + 2;  // complex entries besides the nb x nb factors
+__global__ void __launch_bounds__(kDiagThreads, 1)
+    diag_factor_kernel(Cx<float> *__restrict__ a, int64_t m, int64_t k0, int nb, Cx<float> *__restrict__ linv,
+                       Cx<float> *__restrict__ uinv, int64_t mstride) {
+    using C = Cx<float>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *S = reinterpret_cast<C *>(smem_raw);  // the factors, column-major, ld nb
+    C *colb = S + nb * nb;                   // [2][128]
+    C *rowb = colb + 256;                    // [2][128]
+    C *dinv = rowb + 256;                    // [128]: 1 / U_kk
+    C *pinv = dinv + 128;                    // [2]: 1 / pivot of the step
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    C *A = a + (int64_t)blockIdx.x * m * m + k0 + k0 * m;
+    const C zero{0.f, 0.f}, one{1.f, 0.f};
+    C v[4][8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int r = lane + 32 * i, c = warp + 16 * j;
+            v[i][j] = (r < nb && c < nb) ? A[r + (int64_t)c * m] : zero;
+        }
+
+    // ---- LU: l_r = a_rk / a_kk,  a_rc -= l_r a_kc  (r, c > k) ----
+    if (warp == 0)  // column 0
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (lane + 32 * i < nb) colb[lane + 32 * i] = v[i][0];
+    if (lane == 0) {  // row 0
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (warp + 16 * j < nb) rowb[warp + 16 * j] = v[0][j];
+        if (warp == 0) pinv[0] = cdiv(one, v[0][0]);
+    }
+    __syncthreads();
+    for (int k = 0; k < nb; ++k) {
+        const int b = k & 1, k1 = k + 1;
+        const C inv = pinv[b];
+        C *cn = colb + (b ^ 1) * 128, *rn = rowb + (b ^ 1) * 128;
+        C l[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int r = lane + 32 * i;
+            l[i] = zero;
+            if (32 * i + 31 > k && r > k && r < nb) l[i] = cmul(colb[b * 128 + r], inv);
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int c = warp + 16 * j;  // warp-uniform
+            if (c > k && c < nb) {
+                const C u = rowb[b * 128 + c];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    if (32 * i + 31 > k) {
+                        const int r = lane + 32 * i;
+                        csubmul(v[i][j], l[i], u);  // l = 0 on rows <= k
+                        // column k + 1 and row k + 1 as this step leaves them
+                        if (c == k1 && r >= k1 && r < nb) cn[r] = v[i][j];
+                        if (r == k1) {
+                            rn[c] = v[i][j];
+                            if (c == k1) pinv[b ^ 1] = cdiv(one, v[i][j]);
+                        }
+                    }
+                }
+            } else if (c == k) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (lane + 32 * i > k) v[i][j] = l[i];
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int r = lane + 32 * i, c = warp + 16 * j;
+            if (r < nb && c < nb) {
+                A[r + (int64_t)c * m] = v[i][j];
+                S[r + c * nb] = v[i][j];
+            }
+        }
+    __syncthreads();
+    if (threadIdx.x < nb) dinv[threadIdx.x] = cdiv(one, S[threadIdx.x + threadIdx.x * nb]);
+    // row 0 of X = I
+    if (threadIdx.x < nb) rowb[threadIdx.x] = threadIdx.x == 0 ? one : zero;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[i][j] = (lane + 32 * i == warp + 16 * j) ? one : zero;
+    __syncthreads();
+
+    // ---- X = L^{-1}:  X[r][:] -= L[r][k] X[k][:]  for r > k ----
+    for (int k = 0; k + 1 < nb; ++k) {
+        const int b = k & 1, k1 = k + 1;
+        C *rn = rowb + (b ^ 1) * 128;
+        C lk[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int r = lane + 32 * i;
+            lk[i] = zero;
+            if (32 * i + 31 > k && r > k && r < nb) lk[i] = S[r + k * nb];
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int c = warp + 16 * j;
+            if (c <= k) {  // X[k][c] = 0 for c > k
+                const C xk = rowb[b * 128 + c];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    if (32 * i + 31 > k) {
+                        csubmul(v[i][j], lk[i], xk);
+                        if (lane + 32 * i == k1) rn[c] = v[i][j];  // row k + 1, columns <= k
+                    }
+                }
+            }
+        }
+        if (threadIdx.x == 0) rn[k1] = one;  // X[k+1][k+1]; later columns of the row are 0
+        __syncthreads();
+    }
+    C *out = linv + (int64_t)blockIdx.x * mstride;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int r = lane + 32 * i, c = warp + 16 * j;
+            if (r < nb && c < nb) out[r + c * nb] = v[i][j];
+        }
+    __syncthreads();  // every read of the row buffers above precedes their reuse
+    // row nb - 1 of Y before scaling = that row of I
+    if (threadIdx.x < nb) rowb[threadIdx.x] = (int)threadIdx.x == nb - 1 ? one : zero;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[i][j] = (lane + 32 * i == warp + 16 * j) ? one : zero;
+    __syncthreads();
+
+    // ---- Y = U^{-1}:  Y[k][:] /= U[k][k];  Y[r][:] -= U[r][k] Y[k][:]  for r < k ----
+    for (int k = nb - 1, t = 0; k >= 0; --k, ++t) {
+        const int b = t & 1, km = k - 1;
+        C *rn = rowb + (b ^ 1) * 128;
+        const C inv = dinv[k];
+        C uk[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int r = lane + 32 * i;
+            uk[i] = zero;
+            if (32 * i < k && r < k) uk[i] = S[r + k * nb];
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int c = warp + 16 * j;
+            if (c >= k && c < nb) {  // Y[k][c] = 0 for c < k
+                const C yk = cmul(rowb[b * 128 + c], inv);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = lane + 32 * i;
+                    if (32 * i < k) {
+                        csubmul(v[i][j], uk[i], yk);  // uk = 0 on rows >= k
+                        if (r == km) rn[c] = v[i][j];  // row k - 1 before its scaling, columns >= k
+                    }
+                    if (r == k) v[i][j] = yk;
+                }
+            }
+        }
+        if (threadIdx.x == 0 && km >= 0) rn[km] = one;  // Y[k-1][k-1] before scaling
+        __syncthreads();
+    }
+    out = uinv + (int64_t)blockIdx.x * mstride;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int r = lane + 32 * i, c = warp + 16 * j;
+            if (r < nb && c < nb) out[r + c * nb] = v[i][j];
+        }
+}
+
 // Linv = L11^{-1} for the unit lower triangle of panel [k0, k0+nb) of every
 // matrix (column-major nb x nb, leading dimension nb, matrix f at
 // linv + f * mstride).  The columns of the inverse are independent
@@ -418,41 +620,6 @@ __global__ void __launch_bounds__(128) bwd_panel_kernel2(const Cx<T> *__restrict
 // (contiguous in memory) fetched while step k computes.
 // Grid (count, ceil(nb / 32)), 256 threads; dynamic shared memory
 // (32 nb + 2 nb) complex.
-// LU without pivoting of the nb x nb diagonal block at (k0, k0) of every
-// matrix, in shared memory (CTA per matrix): L unit lower below the
-// diagonal, U on and above it.  For A = R + jwL with R and L symmetric
-// positive definite (a mesh impedance matrix) elimination without pivoting
-// is stable (the growth factor is bounded); a zero or non-finite pivot of
-// any other matrix shows as a non-finite refinement correction, and the
-// caller falls back to the pivoted FP64 factorization.
-__global__ void __launch_bounds__(512) diag_lu_kernel(Cx<float> *__restrict__ a, int64_t m, int64_t k0, int nb) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Cx<float> *S = reinterpret_cast<Cx<float> *>(smem_raw);  // column-major, ld nb
-    Cx<float> *A = a + (int64_t)blockIdx.x * m * m;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int idx = tid; idx < nb * nb; idx += nt) {
-        const int r = idx % nb, c = idx / nb;
-        S[idx] = A[(k0 + r) + (k0 + c) * m];
-    }
-    for (int k = 0; k < nb; ++k) {
-        __syncthreads();
-        const Cx<float> one{1.0f, 0.0f};
-        const Cx<float> inv = cdiv(one, S[k + k * nb]);
-        for (int r = k + 1 + tid; r < nb; r += nt) S[r + k * nb] = cmul(S[r + k * nb], inv);
-        __syncthreads();
-        const int rest = nb - k - 1;
-        for (int idx = tid; idx < rest * rest; idx += nt) {
-            const int r = k + 1 + idx % rest, c = k + 1 + idx / rest;
-            csubmul(S[r + c * nb], S[r + k * nb], S[k + c * nb]);
-        }
-    }
-    __syncthreads();
-    for (int idx = tid; idx < nb * nb; idx += nt) {
-        const int r = idx % nb, c = idx / nb;
-        A[(k0 + r) + (k0 + c) * m] = S[idx];
-    }
-}
-
 // U[k, c] = U[k, k] L[c, k] for rows k in [K0, K0 + W) and columns c >= E:
 // the U12 block of a symmetric matrix factored without pivoting (U = D L^T).
 // 32 x 32 tiles through shared memory, so both the reads of L (down a column)
@@ -687,51 +854,101 @@ __global__ void rhs_kernel(const double *__restrict__ R, const double *__restric
     }
 }
 
-// r = b - (R + j w L) x for 8 frequencies per block row; b = Z_ep column q.
-constexpr int kResF = 8;
-__global__ void __launch_bounds__(128) residual_kernel(const double *__restrict__ R, const double *__restrict__ L,
-                                                       int64_t ld, int64_t m, int64_t p, const double *__restrict__ omega,
-                                                       int count, const Cx<double> *__restrict__ x,
-                                                       Cx<double> *__restrict__ r) {
-    __shared__ Cx<double> xs[64][kResF];
-    const int fg = blockIdx.y / (int)p, q = blockIdx.y % (int)p;
-    const int f0 = fg * kResF;
-    const int nf = min(kResF, count - f0);
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    double sr_re[kResF], sr_im[kResF], sl_re[kResF], sl_im[kResF];
+// r = b - (R + j w L) x for every (frequency f, port column q), b = Z_ep
+// column q; x and r hold column g = f p + q at g m.  R x and L x are real
+// matrices times complex columns: a register-tiled FP64 product, block tile
+// 32 rows x 32 columns g, k in stages of 16 staged in shared memory (double
+// buffered, the next stage's loads in flight during the current one), thread
+// tile 4 rows x 2 columns for both R and L.  Each accumulator sums over k in
+// increasing order.
+constexpr int kResRows = 32, kResCols = 32, kResK = 16, kResThreads = 128;
+__global__ void __launch_bounds__(kResThreads) residual_kernel(const double *__restrict__ R,
+                                                               const double *__restrict__ L, int64_t ld, int64_t m,
+                                                               int64_t p, const double *__restrict__ omega, int count,
+                                                               const Cx<double> *__restrict__ x,
+                                                               Cx<double> *__restrict__ r) {
+    __shared__ double Rs[2][kResK][kResRows], Ls[2][kResK][kResRows];
+    __shared__ Cx<double> Xs[2][kResK][kResCols + 1];  // padded: the stores run down k
+    const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
+    const int64_t i0 = (int64_t)blockIdx.x * kResRows;
+    const int64_t g0 = (int64_t)blockIdx.y * kResCols, G = (int64_t)count * p;
+    double rv[4], lv[4];
+    Cx<double> xv[4];
+    auto load = [&](int64_t k0) {
 #pragma unroll
-    for (int f = 0; f < kResF; ++f) sr_re[f] = sr_im[f] = sl_re[f] = sl_im[f] = 0.0;
-    for (int64_t c0 = 0; c0 < m; c0 += 64) {
-        __syncthreads();
-        for (int idx = threadIdx.x; idx < 64 * kResF; idx += blockDim.x) {
-            int cc = idx % 64, f = idx / 64;
-            int64_t c = c0 + cc;
-            xs[cc][f] = (c < m && f < nf) ? x[((int64_t)(f0 + f) * p + q) * m + c] : Cx<double>{0.0, 0.0};
+        for (int e = 0; e < 4; ++e) {
+            const int idx = tid + kResThreads * e;
+            const int row = idx & 31, k = idx >> 5;
+            const int64_t i = i0 + row, kk = k0 + k;
+            const bool in = i < m && kk < m;
+            rv[e] = in ? R[i + kk * ld] : 0.0;
+            lv[e] = in ? L[i + kk * ld] : 0.0;
+            const int kx = idx & 15, g = idx >> 4;
+            const int64_t kkx = k0 + kx;
+            xv[e] = (g0 + g < G && kkx < m) ? x[(g0 + g) * m + kkx] : Cx<double>{0.0, 0.0};
         }
-        __syncthreads();
-        if (i < m) {
-            const int cmax = (int)min((int64_t)64, m - c0);
-            for (int cc = 0; cc < cmax; ++cc) {
-                const double rv = R[i + (c0 + cc) * ld], lv = L[i + (c0 + cc) * ld];
+    };
+    auto store = [&](int b) {
 #pragma unroll
-                for (int f = 0; f < kResF; ++f) {
-                    const Cx<double> xv = xs[cc][f];
-                    sr_re[f] += rv * xv.re;
-                    sr_im[f] += rv * xv.im;
-                    sl_re[f] += lv * xv.re;
-                    sl_im[f] += lv * xv.im;
-                }
+        for (int e = 0; e < 4; ++e) {
+            const int idx = tid + kResThreads * e;
+            Rs[b][idx >> 5][idx & 31] = rv[e];
+            Ls[b][idx >> 5][idx & 31] = lv[e];
+            Xs[b][idx & 15][idx >> 4] = xv[e];
+        }
+    };
+    Cx<double> ar[4][2], al[4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) ar[i][j] = al[i][j] = Cx<double>{0.0, 0.0};
+    const int64_t stages = (m + kResK - 1) / kResK;
+    load(0);
+    store(0);
+    __syncthreads();
+    for (int64_t st = 0; st < stages; ++st) {
+        const int b = (int)(st & 1);
+        if (st + 1 < stages) load((st + 1) * kResK);
+#pragma unroll
+        for (int k = 0; k < kResK; ++k) {
+            double rk[4], lk[4];
+            Cx<double> xk[2];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                rk[i] = Rs[b][k][tx + 8 * i];
+                lk[i] = Ls[b][k][tx + 8 * i];
             }
+#pragma unroll
+            for (int j = 0; j < 2; ++j) xk[j] = Xs[b][k][ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    ar[i][j].re += rk[i] * xk[j].re;
+                    ar[i][j].im += rk[i] * xk[j].im;
+                    al[i][j].re += lk[i] * xk[j].re;
+                    al[i][j].im += lk[i] * xk[j].im;
+                }
         }
+        if (st + 1 < stages) store(b ^ 1);
+        __syncthreads();
     }
-    if (i < m) {
-        const double br = R[i + (m + q) * ld], bl = L[i + (m + q) * ld];
-        for (int f = 0; f < nf; ++f) {
-            const double w = omega[f0 + f];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const int64_t g = g0 + ty + 16 * j;
+        if (g >= G) continue;
+        const int f = (int)(g / p);
+        const int64_t q = g % p;
+        const double w = omega[f];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int64_t row = i0 + tx + 8 * i;
+            if (row >= m) continue;
+            const double br = R[row + (m + q) * ld], bl = L[row + (m + q) * ld];
             // (R + jwL) x = R x + j w (L x)
-            const double ax_re = sr_re[f] - w * sl_im[f];
-            const double ax_im = sr_im[f] + w * sl_re[f];
-            r[((int64_t)(f0 + f) * p + q) * m + i] = Cx<double>{br - ax_re, w * bl - ax_im};
+            const double ax_re = ar[i][j].re - w * al[i][j].im;
+            const double ax_im = ar[i][j].im + w * al[i][j].re;
+            r[g * m + row] = Cx<double>{br - ax_re, w * bl - ax_im};
         }
     }
 }
@@ -847,8 +1064,9 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
     const bool nopivot = w.nopivot;
     if (nopivot) {
         if (!w.uinv) return fail(err, FH_ERR_INVALID_ARGUMENT, "the factorization without pivoting needs uinv");
-        const size_t diag_smem = sizeof(C) * (size_t)nb * nb;
-        FHB_CUDA(cudaFuncSetAttribute(diag_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem));
+        const size_t diag_smem = sizeof(C) * ((size_t)nb * nb + kDiagSmemExtra);
+        FHB_CUDA(cudaFuncSetAttribute(diag_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)diag_smem));
         const int64_t total = (int64_t)count * m;
         identity_pivots_kernel<<<grid_for(total, 256, 1024), 256, 0, s>>>(b.pivots, total, m);
         FHB_CUDA(cudaGetLastError());
@@ -863,18 +1081,23 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             const int64_t mstride = (int64_t)nb * nb;  // a partial last block keeps the full slot stride
             prof_begin(s, FH_PROF_PANEL);
             if (nopivot) {
-                diag_lu_kernel<<<(unsigned)count, 512, sizeof(C) * (size_t)wj * wj, s>>>(a, m, j0, wj);
-                st = cudaGetLastError() == cudaSuccess ? FH_OK : fail(err, FH_ERR_CUDA, "diagonal block LU launch failed");
+                // LU of the diagonal block and the inverses of its L and U.
+                diag_factor_kernel<<<(unsigned)count, kDiagThreads, sizeof(C) * ((size_t)wj * wj + kDiagSmemExtra), s>>>(
+                    a, m, j0, wj, linv, slot(w.uinv, j0), mstride);
+                st = cudaGetLastError() == cudaSuccess ? FH_OK
+                                                       : fail(err, FH_ERR_CUDA, "diagonal block factorization launch failed");
             } else {
                 st = panel_coop<float>(b, j0, wj, *w.coop, s, err);
             }
             prof_end(s, FH_PROF_PANEL, 0.0);
             if (st) return st;
             prof_begin(s, FH_PROF_TRSM);
-            tri_inverse_kernel<float><<<inv_grid, 256, inv_smem, s>>>(a, m, (int)j0, wj, linv, mstride);
-            if (w.uinv)
-                tri_inverse_upper_kernel<float><<<inv_grid, 256, inv_smem, s>>>(a, m, (int)j0, wj, slot(w.uinv, j0),
-                                                                                mstride);
+            if (!nopivot) {
+                tri_inverse_kernel<float><<<inv_grid, 256, inv_smem, s>>>(a, m, (int)j0, wj, linv, mstride);
+                if (w.uinv)
+                    tri_inverse_upper_kernel<float><<<inv_grid, 256, inv_smem, s>>>(a, m, (int)j0, wj,
+                                                                                    slot(w.uinv, j0), mstride);
+            }
             if (r1 >= m) {
                 prof_end(s, FH_PROF_TRSM, 0.0);
                 break;
@@ -1141,10 +1364,11 @@ fh_status form_rhs(const double *Rm, const double *Lm, int64_t ld, int64_t m, in
 fh_status residual_fp64(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega,
                         int count, const double *x, double *r, double *rnorm, cudaStream_t s, fh_error_info *err) {
     if (m == 0) return FH_OK;
-    const int fgroups = (count + kResF - 1) / kResF;
+    const int64_t cols = (int64_t)count * p;
     prof_begin(s, FH_PROF_RESIDUAL);
-    residual_kernel<<<dim3((unsigned)((m + 127) / 128), (unsigned)(fgroups * p)), 128, 0, s>>>(
-        Rm, Lm, ld, m, p, omega, count, reinterpret_cast<const Cx<double> *>(x), reinterpret_cast<Cx<double> *>(r));
+    residual_kernel<<<dim3((unsigned)((m + kResRows - 1) / kResRows), (unsigned)((cols + kResCols - 1) / kResCols)),
+                      kResThreads, 0, s>>>(Rm, Lm, ld, m, p, omega, count, reinterpret_cast<const Cx<double> *>(x),
+                                           reinterpret_cast<Cx<double> *>(r));
     prof_end(s, FH_PROF_RESIDUAL, 16.0 * (double)m * (double)m);  // bytes: R and L read once
     FHB_CUDA(cudaGetLastError());
     if (rnorm) {

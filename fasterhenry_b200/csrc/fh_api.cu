@@ -167,7 +167,7 @@ struct PBuf {
 enum PoolSlot {
     kSlotA, kSlotD32, kSlotR, kSlotRnorm, kSlotBnorm, kSlotDnorm, kSlotXnorm, kSlotPiv, kSlotSing, kSlotPv,
     kSlotPi, kSlotTk, kSlotCoop, kSlotLinv, kSlotUinv, kSlotSolve, kSlotPackA, kSlotPackB, kSlotOmega, kSlotX,
-    kSlotZ
+    kSlotZ, kSlotXinv, kSlotXpack, kSlotTbuf, kSlotDvec
 };
 
 #define FHB_PALLOC(pool, buf, slot_id, count)                                                          \
@@ -308,7 +308,8 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     PBuf<int> piv, sing;
     const int64_t vec = m * p;  // complex entries per frequency
     DevPool &pool = s->pool;
-    FHB_PALLOC(pool, a, kSlotA, (size_t)count * m * m * 2);
+    // 4 floats of slack: the panel solve copies raw columns from 16-byte boundaries
+    FHB_PALLOC(pool, a, kSlotA, (size_t)count * m * m * 2 + 4);
     FHB_PALLOC(pool, d32, kSlotD32, (size_t)count * vec * 2);
     FHB_PALLOC(pool, r, kSlotR, (size_t)count * vec * 2);
     FHB_PALLOC(pool, rnorm, kSlotRnorm, (size_t)count);
@@ -368,7 +369,8 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
             trisolve_bind(solve_mem.p, count * (int)p, per_group, ss);
         }
     }
-    PBuf<unsigned char> pack_a, pack_b;
+    PBuf<unsigned char> pack_a, pack_b, xpack;
+    PBuf<float> xinv, tbuf, dvec;
     if (outer) {
         const size_t pb = packed_operand_bytes(m - outer, outer, count);
         FHB_PALLOC(pool, pack_a, kSlotPackA, pb);
@@ -380,6 +382,14 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
         // the FP32 factors go without pivoting (stable for this class; the
         // FP64 residual refinement and its FP64 fallback decide the result).
         w.nopivot = true;
+        FHB_PALLOC(pool, xinv, kSlotXinv, (size_t)count * outer * outer * 2);
+        FHB_PALLOC(pool, xpack, kSlotXpack, packed_operand_bytes(outer, outer, count));
+        FHB_PALLOC(pool, tbuf, kSlotTbuf, (size_t)count * kNbFp32 * kNbFp32 * 2);
+        FHB_PALLOC(pool, dvec, kSlotDvec, (size_t)count * outer * 2);
+        w.xinv = xinv.p;
+        w.xpack = xpack.p;
+        w.tbuf = tbuf.p;
+        w.dvec = dvec.p;
     }
     LuBatch<float> b;
     b.a = a.p;
@@ -872,9 +882,11 @@ fh_status fh_sweep(fh_system *sys, const double *freqs, size_t nf, fh_precision 
         precision == FH_PRECISION_MIXED_BF16X3 ? TrailingUpdate::TensorBf16x3 : TrailingUpdate::Simt;
     // Per frequency: the matrix, the vectors, and for the two-level FP32
     // form its two packed operands (8 bytes per entry of an m x 512 block
-    // each) and the inverses of the diagonal blocks of L and U.
+    // each), the inverses of the diagonal blocks of L and U, and a
+    // super-panel's U^-1 in FP32 and packed.
     const double per = (mixed ? 8.0 : 16.0) * (double)m * (double)m + 64.0 * (double)(m * p + 64) +
-                       (outer_for(m, update) ? 16.0 * (double)m * kOuterFp32 + 16.0 * (double)(m + kNbFp32) * kNbFp32
+                       (outer_for(m, update) ? 16.0 * (double)m * kOuterFp32 + 16.0 * (double)(m + kNbFp32) * kNbFp32 +
+                                                   16.0 * kOuterFp32 * kOuterFp32 + 8.0 * kNbFp32 * kNbFp32
                                              : 0.0);
     int chunk = (int)std::max(1.0, std::min<double>((double)nf, 0.8 * (double)free_b / std::max(per, 1.0)));
     PBuf<double> d_omega, d_x, d_z;
@@ -1090,7 +1102,8 @@ fh_status fh_currents(fh_system *sys, const double *freqs, size_t nf, const doub
     free_b = (free_b + cache_idle_bytes()) / (size_t)std::max(1, sys->share) + sys->pool.held();
     const double per = (mixed ? 8.0 : 16.0) * (double)m * (double)m + 64.0 * (double)(m * p + 64) + 48.0 * (double)n +
                        32.0 * (double)nseg +
-                       (outer_for(m, update) ? 16.0 * (double)m * kOuterFp32 + 16.0 * (double)(m + kNbFp32) * kNbFp32
+                       (outer_for(m, update) ? 16.0 * (double)m * kOuterFp32 + 16.0 * (double)(m + kNbFp32) * kNbFp32 +
+                                                   16.0 * kOuterFp32 * kOuterFp32 + 8.0 * kNbFp32 * kNbFp32
                                              : 0.0);
     const int chunk = (int)std::max(1.0, std::min<double>((double)nf, 0.8 * (double)free_b / std::max(per, 1.0)));
     PBuf<double> d_omega, d_x, d_z;

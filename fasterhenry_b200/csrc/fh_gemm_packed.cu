@@ -442,6 +442,316 @@ __global__ void __launch_bounds__(kThreads, 1) packed_update_kernel(PackedArgs g
     }
 }
 
+// ---------------------------------------------------------------------------
+// The rows below a super-panel of the factorization without pivoting.
+//
+// For a factored super-panel [K0, E) (W = E - K0 columns, D = L_D U_D) and
+// the rows [E, m) below it, in place:
+//
+//     L21 = A21 X,    X = U_D^{-1}  (W x W upper triangular, packed as a B operand)
+//
+// and with L21 everything else the super-panel step needs from it: the matrix
+// is complex symmetric and factored without interchanges, so U = diag(U) L^T
+// and U12 = diag(d) L21^T (d_k = U_kk) is written over the rows [K0, E) of the
+// trailing columns; and the operands of the deep update are written packed
+// (A = L21 by 128-row blocks, B = U12 by 128-column blocks -- the same tiles
+// as A's, each k scaled by d_k).
+//
+// A work item is one 128-row block of one matrix; its output column blocks
+// are formed from the last to the first, block j from the k chunks
+// [0, 8 (j + 1)) (X is upper triangular), so the FP32 write of a block never
+// reaches a column that a later block of the item reads, and items own
+// disjoint rows.  Roles:
+//   warp 13, one lane  loader: per chunk, one plain bulk copy per column of
+//                      the raw FP32 rows (from a 16-byte boundary; the column
+//                      slot has room for the one-element shift of an odd
+//                      start) and the bulk copy of the X chunk, all counted
+//                      on the stage's `full` barrier;
+//   warps 0..3         splitters: thread t takes row t of the chunk from the
+//                      raw slots, splits it into BF16 hi/lo and stores the
+//                      four A tiles of the stage, then a proxy fence and an
+//                      arrival on `afull`;
+//   warp 12, one lane  TMEM allocation and the MMA issuer: 12 tcgen05.mma per
+//                      chunk into one of two TMEM accumulators;
+//   warps 4..11        epilogue: tcgen05.ld, then L21 and U12 in FP32 and the
+//                      two packed tiles.
+// A stage is reused once the MMAs that read it have completed (`empty`):
+// by then the splitters have consumed its raw slots too.  No cluster launch
+// and no multicast.  Every wait is bounded; a wait that runs out sets the
+// error flag and stops the role, and the loader and the MMA issuer wait
+// (bounded) for their operations in flight before the TMEM is freed.
+constexpr int kPsRawCol = 1040;                                   // bytes: 128 rows + 16 of slack
+constexpr int kPsRawBytes = kChunk * kPsRawCol;                   // 16,640
+constexpr int kPsStageBytes = ((2 * kOpBytes + kPsRawBytes + 1023) / 1024) * 1024;  // packed A, X, raw
+constexpr int kPsStages = 4;
+constexpr int kPsThreads = 32 * 14;
+constexpr int kPsSmemBytes = kPsStages * kPsStageBytes + 1024 + kBarBytes;
+static_assert(kPsSmemBytes <= 227 * 1024, "panel-solve shared memory");
+
+struct PanelSolveArgs {
+    float2 *A;             // the batch: (r, c) of matrix f at A[f mm + r + c m]
+    int64_t m, mm, K0, E;
+    int W, nbw, nch;       // super-panel width, its 128-blocks and 16-chunks
+    const uint8_t *Xp;     // X packed: [f][column block][chunk] 16 KB
+    const float2 *dvec;    // d_k = U_kk of the super-panel: [f][W]
+    uint8_t *Pa, *Pb;      // packed outputs: [f][row block][chunk] 16 KB
+    int rblocks;           // 128-row blocks of [E, m)
+    long long items;       // count * rblocks
+};
+
+__global__ void __launch_bounds__(kPsThreads, 1) panel_solve_kernel(PanelSolveArgs g, int *__restrict__ err_flag) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kPsStages * kPsStageBytes);
+    uint64_t *full = bars;                            // [kPsStages] loader: raw A + X bytes
+    uint64_t *afull = bars + kPsStages;               // [kPsStages] splitters
+    uint64_t *empty = bars + 2 * kPsStages;           // [kPsStages] MMA commit
+    uint64_t *tfull = bars + 3 * kPsStages;           // [2]
+    uint64_t *tempty = bars + 3 * kPsStages + 2;      // [2]
+    uint64_t *drain = bars + 3 * kPsStages + 4;       // [1]
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 3 * kPsStages + 5);
+    // stage layout: packed A (4 tiles) | X chunk (4 tiles) | raw columns
+    auto stage_a = [&](int st) { return smem + st * kPsStageBytes; };
+    auto stage_b = [&](int st) { return smem + st * kPsStageBytes + kOpBytes; };
+    auto stage_raw = [&](int st) { return smem + st * kPsStageBytes + 2 * kOpBytes; };
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 12) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < kPsStages; ++st) {
+            mbar_init(smem_u32(&full[st]), 1);
+            mbar_init(smem_u32(&afull[st]), 128);
+            mbar_init(smem_u32(&empty[st]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&tfull[b]), 1);
+            mbar_init(smem_u32(&tempty[b]), kEpiWarps);
+        }
+        mbar_init(smem_u32(drain), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+    // Element index of (row0, column K0 + 16 c + kk) of matrix f.
+    auto col_elem = [&](int f, int64_t row0, int c, int kk) {
+        return (int64_t)f * g.mm + row0 + (g.K0 + (int64_t)c * kChunk + kk) * g.m;
+    };
+
+    if (warp == 13) {
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0, issued = 0, last_phase = 0;
+            for (long long t = blockIdx.x; t < g.items && ok; t += gridDim.x) {
+                const int f = (int)(t / g.rblocks), rb = (int)(t % g.rblocks);
+                const int64_t row0 = g.E + (int64_t)rb * kTile;
+                const int rows = (int)min((int64_t)kTile, g.m - row0);
+                for (int j = g.nbw - 1; j >= 0 && ok; --j)
+                    for (int c = 0; c < 8 * (j + 1); ++c) {
+                        if (!mbar_wait(smem_u32(&empty[stage]), phase ^ 1u)) {
+                            ok = false;
+                            break;
+                        }
+                        const uint32_t bar = smem_u32(&full[stage]);
+                        uint32_t bytes = kOpBytes;
+#pragma unroll 1
+                        for (int kk = 0; kk < kChunk; ++kk) {
+                            const int o = (int)(col_elem(f, row0, c, kk) & 1);
+                            bytes += (uint32_t)(((rows + o) * 8 + 15) & ~15);
+                        }
+                        mbar_expect_tx(bar, bytes);
+                        bulk_load(smem_u32(stage_b(stage)), g.Xp + (((int64_t)f * g.nbw + j) * g.nch + c) * kOpBytes,
+                                  kOpBytes, bar);
+                        const uint32_t raw = smem_u32(stage_raw(stage));
+#pragma unroll 1
+                        for (int kk = 0; kk < kChunk; ++kk) {
+                            const int64_t e = col_elem(f, row0, c, kk);
+                            const int o = (int)(e & 1);
+                            bulk_load(raw + kk * kPsRawCol, g.A + (e - o), (uint32_t)(((rows + o) * 8 + 15) & ~15), bar);
+                        }
+                        issued |= 1u << stage;
+                        last_phase = (last_phase & ~(1u << stage)) | (phase << stage);
+                        if (++stage == kPsStages) {
+                            stage = 0;
+                            phase ^= 1u;
+                        }
+                    }
+            }
+            if (!ok) {
+                atomicExch(err_flag, 1);
+                for (int st = 0; st < kPsStages; ++st)
+                    if (issued >> st & 1u) mbar_wait(smem_u32(&full[st]), last_phase >> st & 1u);
+            }
+        }
+    } else if (warp < 4) {
+        const int tr = threadIdx.x;  // row of the block
+        int stage = 0;
+        uint32_t phase = 0;
+        for (long long t = blockIdx.x; t < g.items && ok; t += gridDim.x) {
+            const int f = (int)(t / g.rblocks), rb = (int)(t % g.rblocks);
+            const int64_t row0 = g.E + (int64_t)rb * kTile;
+            const bool in = row0 + tr < g.m;
+            for (int j = g.nbw - 1; j >= 0 && ok; --j)
+                for (int c = 0; c < 8 * (j + 1); ++c) {
+                    if (!mbar_wait(smem_u32(&full[stage]), phase)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint8_t *raw = stage_raw(stage);
+                    float2 v[kChunk];
+#pragma unroll
+                    for (int kk = 0; kk < kChunk; ++kk) {
+                        const int o = (int)(col_elem(f, row0, c, kk) & 1);
+                        v[kk] = in ? reinterpret_cast<const float2 *>(raw + kk * kPsRawCol)[o + tr]
+                                   : make_float2(0.f, 0.f);
+                    }
+                    uint8_t *dst = stage_a(stage);
+                    split_store8(v, dst, tile_off(tr, 0));
+                    split_store8(v + 8, dst, tile_off(tr, 1));
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    mbar_arrive(smem_u32(&afull[stage]));
+                    if (++stage == kPsStages) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+        }
+        if (!ok) atomicExch(err_flag, 1);
+    } else if (warp == 12) {
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0, n_tile = 0;
+            bool issued = false;
+            const uint32_t pos = instr_desc(false), neg = instr_desc(true);
+            for (long long t = blockIdx.x; t < g.items && ok; t += gridDim.x)
+                for (int j = g.nbw - 1; j >= 0 && ok; --j, ++n_tile) {
+                    const uint32_t buf = n_tile & 1u, use = n_tile >> 1;
+                    if (!mbar_wait(smem_u32(&tempty[buf]), (use & 1u) ^ 1u)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t d_re = tmem + buf * kAccCols, d_im = d_re + kTile;
+                    for (int c = 0; c < 8 * (j + 1); ++c) {
+                        if (!mbar_wait(smem_u32(&full[stage]), phase) || !mbar_wait(smem_u32(&afull[stage]), phase)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t sa = smem_u32(stage_a(stage)), sb = smem_u32(stage_b(stage));
+                        auto da = [&](int tile) { return smem_desc(sa + tile * kOpTileBytes); };
+                        auto db = [&](int tile) { return smem_desc(sb + tile * kOpTileBytes); };
+                        const uint32_t acc = c > 0 ? 1u : 0u;
+                        mma_bf16(d_re, da(ReH), db(ReH), pos, acc);
+                        mma_bf16(d_re, da(ReH), db(ReL), pos, 1u);
+                        mma_bf16(d_re, da(ReL), db(ReH), pos, 1u);
+                        mma_bf16(d_re, da(ImH), db(ImH), neg, 1u);
+                        mma_bf16(d_re, da(ImH), db(ImL), neg, 1u);
+                        mma_bf16(d_re, da(ImL), db(ImH), neg, 1u);
+                        mma_bf16(d_im, da(ReH), db(ImH), pos, acc);
+                        mma_bf16(d_im, da(ReH), db(ImL), pos, 1u);
+                        mma_bf16(d_im, da(ReL), db(ImH), pos, 1u);
+                        mma_bf16(d_im, da(ImH), db(ReH), pos, 1u);
+                        mma_bf16(d_im, da(ImH), db(ReL), pos, 1u);
+                        mma_bf16(d_im, da(ImL), db(ReH), pos, 1u);
+                        issued = true;
+                        mma_commit(smem_u32(&empty[stage]));
+                        if (++stage == kPsStages) {
+                            stage = 0;
+                            phase ^= 1u;
+                        }
+                    }
+                    if (!ok) break;
+                    mma_commit(smem_u32(&tfull[buf]));
+                }
+            if (!ok) {
+                atomicExch(err_flag, 1);
+                if (issued) {
+                    mma_commit(smem_u32(drain));
+                    mbar_wait(smem_u32(drain), 0u);
+                }
+            }
+        }
+    } else {
+        const int quarter = warp & 3;       // TMEM lanes 32*quarter.. (hardware: warp id % 4)
+        const int half = (warp - 4) >> 2;   // column half of the output block
+        const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
+        const int tr = quarter * 32 + lane;  // row of the block
+        uint32_t n_tile = 0;
+        for (long long t = blockIdx.x; t < g.items && ok; t += gridDim.x) {
+            const int f = (int)(t / g.rblocks), rb = (int)(t % g.rblocks);
+            const int64_t row = g.E + (int64_t)rb * kTile + tr;
+            const bool valid = row < g.m;
+            float2 *Af = g.A + (int64_t)f * g.mm;
+            for (int j = g.nbw - 1; j >= 0; --j, ++n_tile) {
+                const uint32_t buf = n_tile & 1u, use = n_tile >> 1;
+                if (!mbar_wait(smem_u32(&tfull[buf]), use & 1u)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t t_re = tmem + buf * kAccCols + lane_off + half * (kTile / 2);
+                const uint32_t t_im = t_re + kTile;
+#pragma unroll 1
+                for (int step = 0; step < kTile / 2 / 16; ++step) {
+                    const int kc = j * kTile + half * (kTile / 2) + step * 16;  // column in the super-panel
+                    uint32_t re[16], im[16];
+                    tmem_ld16(t_re + step * 16, re);
+                    tmem_ld16(t_im + step * 16, im);
+                    float2 d[16];
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) d[jj] = __ldg(g.dvec + (int64_t)f * g.W + kc + jj);
+                    tmem_wait_ld();
+                    if (step + 1 == kTile / 2 / 16) {
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(smem_u32(&tempty[buf]));
+                    }
+                    float2 l[16], u[16];
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) {
+                        l[jj] = make_float2(__uint_as_float(re[jj]), __uint_as_float(im[jj]));
+                        u[jj] = make_float2(d[jj].x * l[jj].x - d[jj].y * l[jj].y, d[jj].x * l[jj].y + d[jj].y * l[jj].x);
+                    }
+                    if (valid) {
+                        float2 *pl = Af + row + (g.K0 + kc) * g.m;  // L21: down the columns, coalesced over lanes
+#pragma unroll
+                        for (int jj = 0; jj < 16; ++jj) pl[(int64_t)jj * g.m] = l[jj];
+                        float2 *pu = Af + (g.K0 + kc) + row * g.m;  // U12: 16 consecutive entries of column `row`
+                        if ((reinterpret_cast<uintptr_t>(pu) & 15) == 0) {
+#pragma unroll
+                            for (int q = 0; q < 8; ++q)
+                                reinterpret_cast<float4 *>(pu)[q] = make_float4(u[2 * q].x, u[2 * q].y, u[2 * q + 1].x,
+                                                                                u[2 * q + 1].y);
+                        } else {
+#pragma unroll
+                            for (int jj = 0; jj < 16; ++jj) pu[jj] = u[jj];
+                        }
+                    }
+                    const int64_t tile = ((int64_t)f * g.rblocks + rb) * g.nch + kc / kChunk;
+                    split_store8(l, g.Pa + tile * kOpBytes, tile_off(tr, 0));
+                    split_store8(l + 8, g.Pa + tile * kOpBytes, tile_off(tr, 1));
+                    split_store8(u, g.Pb + tile * kOpBytes, tile_off(tr, 0));
+                    split_store8(u + 8, g.Pb + tile * kOpBytes, tile_off(tr, 1));
+                }
+            }
+        }
+        if (!ok && lane == 0) atomicExch(err_flag, 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 12) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+    }
+}
+
 int *g_flag[64] = {nullptr};
 int g_sms[64] = {0};
 
@@ -452,37 +762,39 @@ size_t packed_operand_bytes(int64_t rows, int K, int count) {
     return (size_t)count * (size_t)blocks * (size_t)(K / kChunk) * kOpBytes;
 }
 
-fh_status gemm_tc_packed_update(const float *A, int64_t lda, int64_t sA, const float *B, int64_t ldb, int64_t sB,
-                                float *C, int64_t ldc, int64_t sC, int64_t M, int64_t N, int K, int count,
-                                void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err, int lower_from) {
-    if (K % kChunk || K <= 0) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update needs K a positive multiple of 16");
-    if (M <= 0 || N <= 0 || count <= 0) return FH_OK;
-    if (!pack_a || !pack_b) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update needs operand scratch");
+namespace {
+// First use on a device: the error flag, the kernels' shared-memory limits,
+// the SM count.
+fh_status packed_init(int *dev_out, fh_error_info *err) {
     int dev = 0;
     FHB_CUDA(cudaGetDevice(&dev));
     static std::mutex init_mu;  // first use on a device may race between host threads
-    std::unique_lock<std::mutex> lk(init_mu);
+    std::lock_guard<std::mutex> lk(init_mu);
     if (!g_flag[dev]) {
         FHB_CUDA(cudaMalloc(&g_flag[dev], sizeof(int)));
         FHB_CUDA(cudaMemset(g_flag[dev], 0, sizeof(int)));
         FHB_CUDA(cudaFuncSetAttribute(packed_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+        FHB_CUDA(cudaFuncSetAttribute(panel_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPsSmemBytes));
         FHB_CUDA(cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev));
     }
-    lk.unlock();
+    *dev_out = dev;
+    return FH_OK;
+}
+}  // namespace
+
+fh_status gemm_tc_packed_run(const void *pack_a, const void *pack_b, float *C, int64_t ldc, int64_t sC, int64_t M,
+                             int64_t N, int K, int count, cudaStream_t s, fh_error_info *err, int lower_from) {
+    if (K % kChunk || K <= 0) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update needs K a positive multiple of 16");
+    if (M <= 0 || N <= 0 || count <= 0) return FH_OK;
+    if (!pack_a || !pack_b) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update needs packed operands");
+    int dev = 0;
+    fh_status st = packed_init(&dev, err);
+    if (st) return st;
     const int nchunks = K / kChunk;
     const int rblocks = (int)((M + kTile - 1) / kTile), cblocks = (int)((N + kTile - 1) / kTile);
-    uint8_t *pa = reinterpret_cast<uint8_t *>(pack_a), *pb = reinterpret_cast<uint8_t *>(pack_b);
-    const bool prof = prof_on();
-    if (prof) prof_begin(s, FH_PROF_PACK);
-    pack_a_kernel<<<dim3((unsigned)(rblocks * nchunks), (unsigned)count), 256, 0, s>>>(
-        reinterpret_cast<const float2 *>(A), lda, sA, M, nchunks, rblocks, pa);
-    pack_b_kernel<<<dim3((unsigned)(cblocks * nchunks), (unsigned)count), 256, 0, s>>>(
-        reinterpret_cast<const float2 *>(B), ldb, sB, N, nchunks, cblocks, pb);
-    if (prof) prof_end(s, FH_PROF_PACK, 16.0 * (double)(M + N) * K * count);
-    FHB_CUDA(cudaGetLastError());
     PackedArgs g;
-    g.Ap = pa;
-    g.Bp = pb;
+    g.Ap = reinterpret_cast<const uint8_t *>(pack_a);
+    g.Bp = reinterpret_cast<const uint8_t *>(pack_b);
     g.C = reinterpret_cast<float2 *>(C);
     g.ldc = ldc;
     g.sC = sC;
@@ -525,12 +837,82 @@ fh_status gemm_tc_packed_update(const float *A, int64_t lda, int64_t sA, const f
     }
     g.tiles = (long long)count * g.per_matrix;
     const int grid = (int)std::min<long long>(g.tiles, (long long)std::max(1, g_sms[dev]));
+    const bool prof = prof_on();
     if (prof) prof_begin(s, FH_PROF_GEMM_TC);
     packed_update_kernel<<<grid, kThreads, kSmemBytes, s>>>(g, g_flag[dev]);
     if (prof) prof_end(s, FH_PROF_GEMM_TC, 8.0 * entries * (double)K * count);
     cudaError_t le = cudaGetLastError();
     if (d_table) cache_free(d_table, s);  // stream-ordered: after the kernel
     if (le != cudaSuccess) return fail(err, FH_ERR_CUDA, std::string("packed update launch failed: ") + cudaGetErrorString(le));
+    return FH_OK;
+}
+
+fh_status gemm_tc_packed_update(const float *A, int64_t lda, int64_t sA, const float *B, int64_t ldb, int64_t sB,
+                                float *C, int64_t ldc, int64_t sC, int64_t M, int64_t N, int K, int count,
+                                void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err, int lower_from) {
+    if (K % kChunk || K <= 0) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update needs K a positive multiple of 16");
+    if (M <= 0 || N <= 0 || count <= 0) return FH_OK;
+    if (!pack_a || !pack_b) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update needs operand scratch");
+    const int nchunks = K / kChunk;
+    const int rblocks = (int)((M + kTile - 1) / kTile), cblocks = (int)((N + kTile - 1) / kTile);
+    uint8_t *pa = reinterpret_cast<uint8_t *>(pack_a), *pb = reinterpret_cast<uint8_t *>(pack_b);
+    const bool prof = prof_on();
+    if (prof) prof_begin(s, FH_PROF_PACK);
+    pack_a_kernel<<<dim3((unsigned)(rblocks * nchunks), (unsigned)count), 256, 0, s>>>(
+        reinterpret_cast<const float2 *>(A), lda, sA, M, nchunks, rblocks, pa);
+    pack_b_kernel<<<dim3((unsigned)(cblocks * nchunks), (unsigned)count), 256, 0, s>>>(
+        reinterpret_cast<const float2 *>(B), ldb, sB, N, nchunks, cblocks, pb);
+    if (prof) prof_end(s, FH_PROF_PACK, 16.0 * (double)(M + N) * K * count);
+    FHB_CUDA(cudaGetLastError());
+    return gemm_tc_packed_run(pa, pb, C, ldc, sC, M, N, K, count, s, err, lower_from);
+}
+
+fh_status gemm_tc_pack_b(const float *B, int64_t ldb, int64_t sB, int64_t N, int K, int count, void *out,
+                         cudaStream_t s, fh_error_info *err) {
+    if (K % kChunk || K <= 0) return fail(err, FH_ERR_INVALID_ARGUMENT, "packing needs K a positive multiple of 16");
+    if (N <= 0 || count <= 0) return FH_OK;
+    const int nchunks = K / kChunk, cblocks = (int)((N + kTile - 1) / kTile);
+    pack_b_kernel<<<dim3((unsigned)(cblocks * nchunks), (unsigned)count), 256, 0, s>>>(
+        reinterpret_cast<const float2 *>(B), ldb, sB, N, nchunks, cblocks, reinterpret_cast<uint8_t *>(out));
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+fh_status gemm_tc_panel_solve(float *a, int64_t m, int count, int64_t K0, int W, const void *xpack, const float *dvec,
+                              void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err) {
+    const int64_t E = K0 + W;
+    if (W <= 0 || W % kTile || W > 4 * kTile || K0 < 0 || E > m)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "panel solve needs a super-panel of 128-column blocks (at most 4)");
+    if (E == m || count <= 0) return FH_OK;
+    if (!xpack || !dvec || !pack_a || !pack_b)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "panel solve needs the packed inverse, the diagonal and outputs");
+    int dev = 0;
+    fh_status st = packed_init(&dev, err);
+    if (st) return st;
+    PanelSolveArgs g;
+    g.A = reinterpret_cast<float2 *>(a);
+    g.m = m;
+    g.mm = m * m;
+    g.K0 = K0;
+    g.E = E;
+    g.W = W;
+    g.nbw = W / kTile;
+    g.nch = W / kChunk;
+    g.Xp = reinterpret_cast<const uint8_t *>(xpack);
+    g.dvec = reinterpret_cast<const float2 *>(dvec);
+    g.Pa = reinterpret_cast<uint8_t *>(pack_a);
+    g.Pb = reinterpret_cast<uint8_t *>(pack_b);
+    g.rblocks = (int)((m - E + kTile - 1) / kTile);
+    g.items = (long long)count * g.rblocks;
+    const int grid = (int)std::min<long long>(g.items, (long long)std::max(1, g_sms[dev]));
+    const bool prof = prof_on();
+    // complex MACs of the triangular product (block j of each 128 rows takes K = 128 (j + 1))
+    const double macs = (double)(m - E) * kTile * kTile * (g.nbw * (g.nbw + 1) / 2) * count;
+    if (prof) prof_begin(s, FH_PROF_PANEL_SOLVE);
+    panel_solve_kernel<<<grid, kPsThreads, kPsSmemBytes, s>>>(g, g_flag[dev]);
+    if (prof) prof_end(s, FH_PROF_PANEL_SOLVE, 24.0 * macs);  // BF16 tensor flops (3 products x 8)
+    cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) return fail(err, FH_ERR_CUDA, std::string("panel solve launch failed: ") + cudaGetErrorString(le));
     return FH_OK;
 }
 

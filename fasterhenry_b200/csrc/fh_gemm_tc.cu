@@ -237,7 +237,8 @@ __device__ __forceinline__ void load_chunk(const GemmArgs &g, int f, int64_t row
     split_store8(vb, buf, BrH, BiH, off);
 }
 
-// C (M x N) = C - A B  (assign == 0)  or  C = A B  (assign == 1), batched over
+// C (M x N) = C - A B  (assign == 0), C = A B  (assign == 1) or C = -A B
+// (assign == 2), batched over
 // blockIdx.z; K a multiple of 16.  In the assign form C may be B itself when
 // M <= 128 (one tile row), or A itself when N <= 128 (one tile column): a CTA
 // reads all of the aliased operand's part it writes before the epilogue
@@ -338,9 +339,11 @@ __global__ void __launch_bounds__(kThreads, 2) gemm_bf16x3_kernel(GemmArgs g, in
                 float2 *p = C + row + (col0 + cc) * g.ldc;
                 const int ncol = (int)min((int64_t)16, g.N - (col0 + cc));
                 if (g.assign) {
+                    const float sg = g.assign == 2 ? -1.f : 1.f;
 #pragma unroll
                     for (int jj = 0; jj < 16; ++jj)
-                        if (jj < ncol) p[jj * g.ldc] = make_float2(__uint_as_float(re[jj]), __uint_as_float(im[jj]));
+                        if (jj < ncol)
+                            p[jj * g.ldc] = make_float2(sg * __uint_as_float(re[jj]), sg * __uint_as_float(im[jj]));
                 } else {
                     float2 v[16];
 #pragma unroll

@@ -410,7 +410,9 @@ __global__ void __launch_bounds__(128) bwd_panel_kernel2(const Cx<T> *__restrict
 // The diagonal block of a factorization without pivoting, in one CTA per
 // matrix: the LU of the nb x nb block at (k0, k0) in place (L unit lower below
 // the diagonal, U on and above it), then L^{-1} into linv and U^{-1} into
-// uinv (matrix f at + f * mstride, column-major with leading dimension nb).
+// uinv (matrix f at + f * mstride, column-major with leading dimension nb);
+// optionally U^{-1} also into x2 (matrix f at + f * stride2, leading dimension
+// ld2) and the diagonal of U into dv (matrix f at + f * dstride).
 // For A = R + jwL with R and L symmetric positive definite (a mesh impedance
 // matrix) elimination without pivoting is stable (the growth factor is
 // bounded); a zero or non-finite pivot of any other matrix shows as a
@@ -434,7 +436,8 @@ constexpr int kDiagThreads = 512;
 constexpr int kDiagSmemExtra = 2 * 128 + 2 * 128 + 128 + 2;  // complex entries besides the nb x nb factors
 __global__ void __launch_bounds__(kDiagThreads, 1)
     diag_factor_kernel(Cx<float> *__restrict__ a, int64_t m, int64_t k0, int nb, Cx<float> *__restrict__ linv,
-                       Cx<float> *__restrict__ uinv, int64_t mstride) {
+                       Cx<float> *__restrict__ uinv, int64_t mstride, Cx<float> *__restrict__ x2, int64_t ld2,
+                       int64_t stride2, Cx<float> *__restrict__ dv, int64_t dstride) {
     using C = Cx<float>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *S = reinterpret_cast<C *>(smem_raw);  // the factors, column-major, ld nb
@@ -514,7 +517,10 @@ __global__ void __launch_bounds__(kDiagThreads, 1)
             }
         }
     __syncthreads();
-    if (threadIdx.x < nb) dinv[threadIdx.x] = cdiv(one, S[threadIdx.x + threadIdx.x * nb]);
+    if (threadIdx.x < nb) {
+        dinv[threadIdx.x] = cdiv(one, S[threadIdx.x + threadIdx.x * nb]);
+        if (dv) dv[(int64_t)blockIdx.x * dstride + threadIdx.x] = S[threadIdx.x + threadIdx.x * nb];
+    }
     // row 0 of X = I
     if (threadIdx.x < nb) rowb[threadIdx.x] = threadIdx.x == 0 ? one : zero;
 #pragma unroll
@@ -600,12 +606,16 @@ __global__ void __launch_bounds__(kDiagThreads, 1)
         __syncthreads();
     }
     out = uinv + (int64_t)blockIdx.x * mstride;
+    Cx<float> *out2 = x2 ? x2 + (int64_t)blockIdx.x * stride2 : nullptr;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             const int r = lane + 32 * i, c = warp + 16 * j;
-            if (r < nb && c < nb) out[r + c * nb] = v[i][j];
+            if (r < nb && c < nb) {
+                out[r + c * nb] = v[i][j];
+                if (out2) out2[r + (int64_t)c * ld2] = v[i][j];
+            }
         }
 }
 
@@ -1071,9 +1081,16 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
         identity_pivots_kernel<<<grid_for(total, 256, 1024), 256, 0, s>>>(b.pivots, total, m);
         FHB_CUDA(cudaGetLastError());
     }
+    // Without pivoting and with the scratch for it, the rows below each
+    // super-panel are left to one tensor-core pass (gemm_tc_panel_solve);
+    // the per-block steps then stop at the super-panel's last row.
+    const bool fused = nopivot && w.xinv && w.xpack && w.tbuf && w.dvec && nb == 128 && outer % nb == 0;
+    C *xinv = reinterpret_cast<C *>(w.xinv), *dvec = reinterpret_cast<C *>(w.dvec);
     for (int64_t K0 = 0; K0 < m; K0 += outer) {
         const int W = (int)std::min<int64_t>(outer, m - K0);
         const int64_t E = K0 + W;
+        const bool below = fused && E < m;  // rows below this super-panel go to the fused pass
+        const int64_t rend = below ? E : m;  // rows the per-block steps update
         for (int64_t j0 = K0; j0 < E; j0 += nb) {
             const int wj = (int)std::min<int64_t>(nb, E - j0);
             const int64_t r1 = j0 + wj;  // first row / column after the panel
@@ -1081,9 +1098,13 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             const int64_t mstride = (int64_t)nb * nb;  // a partial last block keeps the full slot stride
             prof_begin(s, FH_PROF_PANEL);
             if (nopivot) {
-                // LU of the diagonal block and the inverses of its L and U.
+                // LU of the diagonal block and the inverses of its L and U
+                // (with the fused pass: U^-1 also into X's diagonal block, and
+                // U's diagonal into dvec).
+                const int64_t o = j0 - K0;
                 diag_factor_kernel<<<(unsigned)count, kDiagThreads, sizeof(C) * ((size_t)wj * wj + kDiagSmemExtra), s>>>(
-                    a, m, j0, wj, linv, slot(w.uinv, j0), mstride);
+                    a, m, j0, wj, linv, slot(w.uinv, j0), mstride, below ? xinv + o + o * W : nullptr, W,
+                    (int64_t)W * W, below ? dvec + o : nullptr, W);
                 st = cudaGetLastError() == cudaSuccess ? FH_OK
                                                        : fail(err, FH_ERR_CUDA, "diagonal block factorization launch failed");
             } else {
@@ -1105,8 +1126,9 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             if (nopivot) {
                 // L21 = A21 U11^-1 for the rows below the block (in place: each
                 // tile of L21 reads exactly its own rows of A21).
-                st = gemm_tc_strided(at(r1, j0), m, mm, reinterpret_cast<const float *>(slot(w.uinv, j0)), wj,
-                                     mstride, at(r1, j0), m, mm, m - r1, wj, wj, 1, count, s, err);
+                if (rend > r1)
+                    st = gemm_tc_strided(at(r1, j0), m, mm, reinterpret_cast<const float *>(slot(w.uinv, j0)), wj,
+                                         mstride, at(r1, j0), m, mm, rend - r1, wj, wj, 1, count, s, err);
                 if (st) return st;
             } else {
                 swaps(j0, wj, K0, j0);
@@ -1119,14 +1141,45 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             if (st) return st;
             if (r1 < E) {
                 prof_begin(s, FH_PROF_GEMM_TC_INNER);
-                st = gemm_tc_strided(at(r1, j0), m, mm, at(j0, r1), m, mm, at(r1, r1), m, mm, m - r1, E - r1, wj, 0,
+                st = gemm_tc_strided(at(r1, j0), m, mm, at(j0, r1), m, mm, at(r1, r1), m, mm, rend - r1, E - r1, wj, 0,
                                      count, s, err);
-                prof_end(s, FH_PROF_GEMM_TC_INNER, 8.0 * (double)(m - r1) * (double)(E - r1) * wj * count);
+                prof_end(s, FH_PROF_GEMM_TC_INNER, 8.0 * (double)(rend - r1) * (double)(E - r1) * wj * count);
                 if (st) return st;
             }
         }
         if (E >= m) break;
         const int64_t n2 = m - E;
+        if (below) {
+            // X = U_D^{-1} from the block inverses on its diagonal, one block
+            // column at a time from the diagonal up:
+            //     X_ij = -X_ii (sum_{k = i+1..j} U_ik X_kj)
+            const int nbw = W / nb;
+            auto xat = [&](int bi, int bj) {
+                return reinterpret_cast<float *>(xinv + (int64_t)bi * nb + (int64_t)bj * nb * W);
+            };
+            float *t = reinterpret_cast<float *>(w.tbuf);
+            const int64_t ww = (int64_t)W * W, tt = (int64_t)nb * nb;
+            prof_begin(s, FH_PROF_TRSM);
+            for (int bj = 1; bj < nbw && !st; ++bj)
+                for (int bi = bj - 1; bi >= 0 && !st; --bi) {
+                    st = gemm_tc_strided(at(K0 + (int64_t)bi * nb, K0 + (int64_t)(bi + 1) * nb), m, mm, xat(bi + 1, bj),
+                                         W, ww, t, nb, tt, nb, nb, (bj - bi) * nb, 1, count, s, err);
+                    if (!st)
+                        st = gemm_tc_strided(xat(bi, bi), W, ww, t, nb, tt, xat(bi, bj), W, ww, nb, nb, nb, 2, count, s,
+                                             err);
+                }
+            if (!st) st = gemm_tc_pack_b(reinterpret_cast<float *>(xinv), W, ww, W, W, count, w.xpack, s, err);
+            prof_end(s, FH_PROF_TRSM, 0.0);
+            if (st) return st;
+            // L21 = A21 X for every row below, U12 = D L21^T, packed operands.
+            st = gemm_tc_panel_solve(b.a, m, count, K0, W, w.xpack, reinterpret_cast<const float *>(dvec), w.pack_a,
+                                     w.pack_b, s, err);
+            if (st) return st;
+            const int next = (int)((std::min<int64_t>(outer, n2) + 127) / 128);
+            st = gemm_tc_packed_run(w.pack_a, w.pack_b, at(E, E), m, mm, n2, n2, W, count, s, err, next);
+            if (st) return st;
+            continue;
+        }
         prof_begin(s, FH_PROF_TRSM);
         if (nopivot) {
             // Symmetric trailing matrix: U12 = D L21^T (D the diagonal of U11).

@@ -65,6 +65,19 @@ struct LuWork {
     // in shared memory and L21 = A21 U11^-1 formed on the tensor cores;
     // pivots are the identity.
     bool nopivot = false;
+    // Scratch of the factorization without pivoting, for the rows below each
+    // super-panel (one super-panel at a time; outer = W columns):
+    //   xinv  count * W * W complex FP32: X = U_D^{-1} of the super-panel's
+    //         diagonal block D (column-major, leading dimension W);
+    //   xpack packed_operand_bytes(W, W, count): X packed as a B operand;
+    //   tbuf  count * nb * nb complex FP32: one block product;
+    //   dvec  count * W complex FP32: the diagonal of U_D.
+    // With all four set, L21, U12 and the packed operands of the deep update
+    // come from one tensor-core pass over the rows below (gemm_tc_panel_solve).
+    void *xinv = nullptr;
+    void *xpack = nullptr;
+    void *tbuf = nullptr;
+    void *dvec = nullptr;
 };
 
 // Cooperative panel: sizing, binding of a scratch block, launch, error check.
@@ -96,7 +109,8 @@ fh_status gemm_tc_update(float *a, int64_t m, int count, int64_t k0, int nb, cud
 // Reports (and clears) a bounded tensor-core wait that ran out.
 fh_status gemm_tc_check(fh_error_info *err);
 // General strided form of the same kernel: C (M x N) -= A (M x K) B (K x N)
-// (assign == 0) or C = A B (assign == 1; C may alias B when M <= 128).
+// (assign == 0), C = A B (assign == 1; C may alias B when M <= 128, or A when
+// N <= 128) or C = -A B (assign == 2, same aliasing rule).
 // Complex FP32 operands, element (r, k) of A at A[2 (f sA + r + k lda)].
 fh_status gemm_tc_strided(const float *A, int64_t lda, int64_t sA, const float *B, int64_t ldb, int64_t sB, float *C,
                           int64_t ldc, int64_t sC, int64_t M, int64_t N, int K, int assign, int count, cudaStream_t s,
@@ -109,6 +123,20 @@ size_t packed_operand_bytes(int64_t rows, int K, int count);
 fh_status gemm_tc_packed_update(const float *A, int64_t lda, int64_t sA, const float *B, int64_t ldb, int64_t sB,
                                 float *C, int64_t ldc, int64_t sC, int64_t M, int64_t N, int K, int count,
                                 void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err, int lower_from = -1);
+// The deep update from operands already packed (layout of pack_a / pack_b above).
+fh_status gemm_tc_packed_run(const void *pack_a, const void *pack_b, float *C, int64_t ldc, int64_t sC, int64_t M,
+                             int64_t N, int K, int count, cudaStream_t s, fh_error_info *err, int lower_from = -1);
+// Packs B (K x N, element (k, n) at B[2 (f sB + k + n ldb)]) as a B operand.
+fh_status gemm_tc_pack_b(const float *B, int64_t ldb, int64_t sB, int64_t N, int K, int count, void *out,
+                         cudaStream_t s, fh_error_info *err);
+// For the factored super-panel [K0, K0 + W) of a complex symmetric batch
+// factored without interchanges and the rows below it: L21 = A21 X in place
+// (X = U_D^{-1}, xpack from gemm_tc_pack_b), U12 = diag(dvec) L21^T over the
+// super-panel's rows of the trailing columns, and both operands of the deep
+// update packed into pack_a / pack_b.  The batch buffer needs 16 bytes of
+// slack after its last matrix (raw column copies start on a 16-byte boundary).
+fh_status gemm_tc_panel_solve(float *a, int64_t m, int count, int64_t K0, int W, const void *xpack, const float *dvec,
+                              void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err);
 fh_status gemm_tc_packed_check(fh_error_info *err);
 // One SIMT trailing update (FP32 or FP64), for tests.
 template <class T>

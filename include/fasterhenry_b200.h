@@ -469,7 +469,8 @@ typedef enum fh_profile_class {
     FH_PROF_PACK = 7,           /* BF16 split + packing of the deep update's operands */
     FH_PROF_GEMM_TC_INNER = 8,  /* tensor-core updates inside a super-panel and of its U12 rows */
     FH_PROF_PFFT_APPLY = 9,     /* one precorrected-FFT product (near field, spread, FFTs, interpolation) */
-    FH_PROF_CLASSES = 10
+    FH_PROF_PANEL_SOLVE = 10,   /* rows below a super-panel: L21 = A21 U^-1, U12 and the packed operands */
+    FH_PROF_CLASSES = 11
 } fh_profile_class;
 
 void fh_profile_enable(int32_t on);

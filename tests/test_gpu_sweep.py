@@ -167,3 +167,22 @@ def test_two_level_mixed_matches_fp64(fh, legs):
         rm = s.sweep(freqs, fh.Precision.MIXED_BF16X3)
     assert rel_err(rm.impedance_ohm, z64) < MIXED_RTOL
     assert all(1 <= i <= 10 for i in rm.refinement_iterations), rm.refinement_iterations
+
+
+def test_two_level_mixed_odd_order(fh):
+    """An odd order (m = 1,043: one segment of the 18-leg meander on a 29 x 1
+    grid, 28 loops instead of 29) over three super-panels: the rows below a
+    super-panel start on both even and odd element offsets, so the fused
+    pass copies its raw columns from both alignments."""
+    base = F.meander_legs(18)
+    grids = [(10, 3)] * base.segment_count()
+    grids[5] = (29, 1)
+    deck = F.Deck(list(base.nodes), [dict(sg) for sg in base.segments], list(base.ports), F.per_segment(grids),
+                  "meander_18_odd")
+    freqs = F.logspace(5, 10, 6)
+    with fh.MeshSystem.assemble(fh.Geometry.from_deck(deck), deck.ports, deck.discretization) as s:
+        assert s.counts()["internal_meshes"] == 1043
+        z64 = s.sweep(freqs, fh.Precision.FP64).impedance_ohm
+        rm = s.sweep(freqs, fh.Precision.MIXED_BF16X3)
+    assert rel_err(rm.impedance_ohm, z64) < MIXED_RTOL
+    assert all(1 <= i <= 10 for i in rm.refinement_iterations), rm.refinement_iterations

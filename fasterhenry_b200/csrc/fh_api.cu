@@ -308,8 +308,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     PBuf<int> piv, sing;
     const int64_t vec = m * p;  // complex entries per frequency
     DevPool &pool = s->pool;
-    // 4 floats of slack: the panel solve copies raw columns from 16-byte boundaries
-    FHB_PALLOC(pool, a, kSlotA, (size_t)count * m * m * 2 + 4);
+    FHB_PALLOC(pool, a, kSlotA, (size_t)count * m * m * 2);
     FHB_PALLOC(pool, d32, kSlotD32, (size_t)count * vec * 2);
     FHB_PALLOC(pool, r, kSlotR, (size_t)count * vec * 2);
     FHB_PALLOC(pool, rnorm, kSlotRnorm, (size_t)count);

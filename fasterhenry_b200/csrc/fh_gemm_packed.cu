@@ -34,8 +34,10 @@
 // runs out sets the error flag, the role stops, the MMA issuer and the
 // producer wait (bounded) for their operations in flight, and the TMEM is
 // freed before the CTA exits.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <stdint.h>
 
 #include <mutex>
@@ -151,42 +153,37 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-__device__ __forceinline__ uint32_t pack2(uint16_t a, uint16_t b) { return (uint32_t)a | ((uint32_t)b << 16); }
 
-__device__ __forceinline__ void split(float x, uint16_t &hi, uint16_t &lo) {
-    __nv_bfloat16 h = __float2bfloat16_rn(x);
-    __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
-    hi = __bfloat16_as_ushort(h);
-    lo = __bfloat16_as_ushort(l);
+// Two FP32 values split into BF16 hi and lo terms (x = hi + lo to 16 bits),
+// each pair converted by one cvt.rn.bf16x2.f32: the 32-bit words of the hi
+// and lo terms, first value in the low half.
+__device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t &lo) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    const float2 back = __bfloat1622float2(h);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(a - back.x, b - back.y);
+    hi = *reinterpret_cast<const uint32_t *>(&h);
+    lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
-// Byte offset of (row r, k group j) inside a 4 KB tile: [j][r/8][r%8][8 bf16].
 __device__ __forceinline__ uint32_t tile_off(int r, int j) {
     return (uint32_t)(j * (kTile / 8) * 128 + (r >> 3) * 128 + (r & 7) * 16);
 }
 
-// Splits 8 complex values (consecutive k of one row) into the four tiles of
-// one operand chunk at `dst`.
+// Splits 8 complex values (k consecutive) into the four 16-byte core-matrix
+// rows (re hi, re lo, im hi, im lo) at offset `off` of the four tiles at dst.
 __device__ __forceinline__ void split_store8(const float2 *v, uint8_t *dst, uint32_t off) {
-    uint16_t rh[8], rl[8], ih[8], il[8];
+    uint32_t rh[4], rl[4], ih[4], il[4];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        split(v[k].x, rh[k], rl[k]);
-        split(v[k].y, ih[k], il[k]);
+    for (int q = 0; q < 4; ++q) {
+        split2(v[2 * q].x, v[2 * q + 1].x, rh[q], rl[q]);
+        split2(v[2 * q].y, v[2 * q + 1].y, ih[q], il[q]);
     }
-    *reinterpret_cast<uint4 *>(dst + ReH * kOpTileBytes + off) =
-        make_uint4(pack2(rh[0], rh[1]), pack2(rh[2], rh[3]), pack2(rh[4], rh[5]), pack2(rh[6], rh[7]));
-    *reinterpret_cast<uint4 *>(dst + ReL * kOpTileBytes + off) =
-        make_uint4(pack2(rl[0], rl[1]), pack2(rl[2], rl[3]), pack2(rl[4], rl[5]), pack2(rl[6], rl[7]));
-    *reinterpret_cast<uint4 *>(dst + ImH * kOpTileBytes + off) =
-        make_uint4(pack2(ih[0], ih[1]), pack2(ih[2], ih[3]), pack2(ih[4], ih[5]), pack2(ih[6], ih[7]));
-    *reinterpret_cast<uint4 *>(dst + ImL * kOpTileBytes + off) =
-        make_uint4(pack2(il[0], il[1]), pack2(il[2], il[3]), pack2(il[4], il[5]), pack2(il[6], il[7]));
+    *reinterpret_cast<uint4 *>(dst + ReH * kOpTileBytes + off) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+    *reinterpret_cast<uint4 *>(dst + ReL * kOpTileBytes + off) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+    *reinterpret_cast<uint4 *>(dst + ImH * kOpTileBytes + off) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+    *reinterpret_cast<uint4 *>(dst + ImL * kOpTileBytes + off) = make_uint4(il[0], il[1], il[2], il[3]);
 }
 
-// Packs the A operand: element (row r, k) at A[f sA + r + k lda], rows
-// [0, M), k in [0, K).  Block (rb * nchunks + c, f), 256 threads: thread t
-// takes row rb*128 + t%128 and k group t/128 of chunk c.  Rows >= M are zero.
 __global__ void __launch_bounds__(256) pack_a_kernel(const float2 *__restrict__ A, int64_t lda, int64_t sA,
                                                      int64_t M, int nchunks, int rblocks, uint8_t *__restrict__ out) {
     const int rb = blockIdx.x / nchunks, c = blockIdx.x % nchunks, f = blockIdx.y;
@@ -462,13 +459,15 @@ __global__ void __launch_bounds__(kThreads, 1) packed_update_kernel(PackedArgs g
 // [0, 8 (j + 1)) (X is upper triangular), so the FP32 write of a block never
 // reaches a column that a later block of the item reads, and items own
 // disjoint rows.  Roles:
-//   warp 13, one lane  loader: per chunk, one plain bulk copy per column of
-//                      the raw FP32 rows (from a 16-byte boundary; the column
-//                      slot has room for the one-element shift of an odd
-//                      start) and the bulk copy of the X chunk, all counted
-//                      on the stage's `full` barrier;
+//   warp 13, one lane  loader: per chunk, one 2D tensor copy (no multicast)
+//                      of the raw FP32 rows -- box 128 rows x 16 columns of
+//                      the batch seen as an m x (count m) array of 8-byte
+//                      elements, rows past m filled with zeros -- and one
+//                      plain bulk copy of the X chunk, both counted on the
+//                      stage's `full` barrier (a tensor map needs a column
+//                      stride that is a multiple of 16 bytes: m even);
 //   warps 0..3         splitters: thread t takes row t of the chunk from the
-//                      raw slots, splits it into BF16 hi/lo and stores the
+//                      raw tile, splits it into BF16 hi/lo and stores the
 //                      four A tiles of the stage, then a proxy fence and an
 //                      arrival on `afull`;
 //   warp 12, one lane  TMEM allocation and the MMA issuer: 12 tcgen05.mma per
@@ -476,13 +475,12 @@ __global__ void __launch_bounds__(kThreads, 1) packed_update_kernel(PackedArgs g
 //   warps 4..11        epilogue: tcgen05.ld, then L21 and U12 in FP32 and the
 //                      two packed tiles.
 // A stage is reused once the MMAs that read it have completed (`empty`):
-// by then the splitters have consumed its raw slots too.  No cluster launch
+// by then the splitters have consumed its raw tile too.  No cluster launch
 // and no multicast.  Every wait is bounded; a wait that runs out sets the
 // error flag and stops the role, and the loader and the MMA issuer wait
 // (bounded) for their operations in flight before the TMEM is freed.
-constexpr int kPsRawCol = 1040;                                   // bytes: 128 rows + 16 of slack
-constexpr int kPsRawBytes = kChunk * kPsRawCol;                   // 16,640
-constexpr int kPsStageBytes = ((2 * kOpBytes + kPsRawBytes + 1023) / 1024) * 1024;  // packed A, X, raw
+constexpr int kPsRawBytes = kChunk * kTile * 8;                   // 16 columns x 128 rows of complex FP32
+constexpr int kPsStageBytes = 2 * kOpBytes + kPsRawBytes;          // packed A, X, raw: 48 KB
 constexpr int kPsStages = 4;
 constexpr int kPsThreads = 32 * 14;
 constexpr int kPsSmemBytes = kPsStages * kPsStageBytes + 1024 + kBarBytes;
@@ -499,7 +497,15 @@ struct PanelSolveArgs {
     long long items;       // count * rblocks
 };
 
-__global__ void __launch_bounds__(kPsThreads, 1) panel_solve_kernel(PanelSolveArgs g, int *__restrict__ err_flag) {
+__device__ __forceinline__ void tensor_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(kPsThreads, 1)
+    panel_solve_kernel(PanelSolveArgs g, const __grid_constant__ CUtensorMap rows_map, int *__restrict__ err_flag) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kPsStages * kPsStageBytes);
@@ -539,10 +545,6 @@ __global__ void __launch_bounds__(kPsThreads, 1) panel_solve_kernel(PanelSolveAr
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     bool ok = true;
-    // Element index of (row0, column K0 + 16 c + kk) of matrix f.
-    auto col_elem = [&](int f, int64_t row0, int c, int kk) {
-        return (int64_t)f * g.mm + row0 + (g.K0 + (int64_t)c * kChunk + kk) * g.m;
-    };
 
     if (warp == 13) {
         if (lane == 0) {
@@ -550,8 +552,8 @@ __global__ void __launch_bounds__(kPsThreads, 1) panel_solve_kernel(PanelSolveAr
             uint32_t phase = 0, issued = 0, last_phase = 0;
             for (long long t = blockIdx.x; t < g.items && ok; t += gridDim.x) {
                 const int f = (int)(t / g.rblocks), rb = (int)(t % g.rblocks);
-                const int64_t row0 = g.E + (int64_t)rb * kTile;
-                const int rows = (int)min((int64_t)kTile, g.m - row0);
+                const int x = (int)(g.E + (int64_t)rb * kTile);  // first row (even: a 16-byte boundary)
+                const int y0 = (int)((int64_t)f * g.m + g.K0);  // column K0 of matrix f
                 for (int j = g.nbw - 1; j >= 0 && ok; --j)
                     for (int c = 0; c < 8 * (j + 1); ++c) {
                         if (!mbar_wait(smem_u32(&empty[stage]), phase ^ 1u)) {
@@ -559,22 +561,10 @@ __global__ void __launch_bounds__(kPsThreads, 1) panel_solve_kernel(PanelSolveAr
                             break;
                         }
                         const uint32_t bar = smem_u32(&full[stage]);
-                        uint32_t bytes = kOpBytes;
-#pragma unroll 1
-                        for (int kk = 0; kk < kChunk; ++kk) {
-                            const int o = (int)(col_elem(f, row0, c, kk) & 1);
-                            bytes += (uint32_t)(((rows + o) * 8 + 15) & ~15);
-                        }
-                        mbar_expect_tx(bar, bytes);
+                        mbar_expect_tx(bar, kOpBytes + kPsRawBytes);
                         bulk_load(smem_u32(stage_b(stage)), g.Xp + (((int64_t)f * g.nbw + j) * g.nch + c) * kOpBytes,
                                   kOpBytes, bar);
-                        const uint32_t raw = smem_u32(stage_raw(stage));
-#pragma unroll 1
-                        for (int kk = 0; kk < kChunk; ++kk) {
-                            const int64_t e = col_elem(f, row0, c, kk);
-                            const int o = (int)(e & 1);
-                            bulk_load(raw + kk * kPsRawCol, g.A + (e - o), (uint32_t)(((rows + o) * 8 + 15) & ~15), bar);
-                        }
+                        tensor_load_2d(smem_u32(stage_raw(stage)), &rows_map, x, y0 + c * kChunk, bar);
                         issued |= 1u << stage;
                         last_phase = (last_phase & ~(1u << stage)) | (phase << stage);
                         if (++stage == kPsStages) {
@@ -594,23 +584,17 @@ __global__ void __launch_bounds__(kPsThreads, 1) panel_solve_kernel(PanelSolveAr
         int stage = 0;
         uint32_t phase = 0;
         for (long long t = blockIdx.x; t < g.items && ok; t += gridDim.x) {
-            const int f = (int)(t / g.rblocks), rb = (int)(t % g.rblocks);
-            const int64_t row0 = g.E + (int64_t)rb * kTile;
-            const bool in = row0 + tr < g.m;
             for (int j = g.nbw - 1; j >= 0 && ok; --j)
                 for (int c = 0; c < 8 * (j + 1); ++c) {
                     if (!mbar_wait(smem_u32(&full[stage]), phase)) {
                         ok = false;
                         break;
                     }
-                    const uint8_t *raw = stage_raw(stage);
+                    // raw tile: column kk of the chunk at kk * 128, rows contiguous (zeros past m)
+                    const float2 *raw = reinterpret_cast<const float2 *>(stage_raw(stage));
                     float2 v[kChunk];
 #pragma unroll
-                    for (int kk = 0; kk < kChunk; ++kk) {
-                        const int o = (int)(col_elem(f, row0, c, kk) & 1);
-                        v[kk] = in ? reinterpret_cast<const float2 *>(raw + kk * kPsRawCol)[o + tr]
-                                   : make_float2(0.f, 0.f);
-                    }
+                    for (int kk = 0; kk < kChunk; ++kk) v[kk] = raw[kk * kTile + tr];
                     uint8_t *dst = stage_a(stage);
                     split_store8(v, dst, tile_off(tr, 0));
                     split_store8(v + 8, dst, tile_off(tr, 1));
@@ -878,17 +862,50 @@ fh_status gemm_tc_pack_b(const float *B, int64_t ldb, int64_t sB, int64_t N, int
     return FH_OK;
 }
 
+namespace {
+// The driver's tensor-map encoder, looked up once through the runtime.
+PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
+    }();
+    return fn;
+}
+}  // namespace
+
+bool panel_solve_supported(int64_t m) { return m % 2 == 0 && m * 8 < ((int64_t)1 << 40); }
+
 fh_status gemm_tc_panel_solve(float *a, int64_t m, int count, int64_t K0, int W, const void *xpack, const float *dvec,
                               void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err) {
     const int64_t E = K0 + W;
-    if (W <= 0 || W % kTile || W > 4 * kTile || K0 < 0 || E > m)
+    if (W <= 0 || W % kTile || W > 4 * kTile || K0 < 0 || K0 % 2 || E > m)
         return fail(err, FH_ERR_INVALID_ARGUMENT, "panel solve needs a super-panel of 128-column blocks (at most 4)");
+    if (!panel_solve_supported(m) || (int64_t)count * m > INT32_MAX)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "panel solve needs an even order (16-byte column stride)");
     if (E == m || count <= 0) return FH_OK;
     if (!xpack || !dvec || !pack_a || !pack_b)
         return fail(err, FH_ERR_INVALID_ARGUMENT, "panel solve needs the packed inverse, the diagonal and outputs");
     int dev = 0;
     fh_status st = packed_init(&dev, err);
     if (st) return st;
+    // The batch as an m x (count m) array of 8-byte elements (complex FP32),
+    // column stride 8 m bytes; a box is 128 rows x 16 columns.
+    PFN_cuTensorMapEncodeTiled encode = tensor_map_encoder();
+    if (!encode) return fail(err, FH_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    CUtensorMap rows_map;
+    const cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)count * (cuuint64_t)m};
+    const cuuint64_t strides[1] = {(cuuint64_t)m * 8};
+    const cuuint32_t box[2] = {(cuuint32_t)kTile, (cuuint32_t)kChunk};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult cr = encode(&rows_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, a, dims, strides, box, estr,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS)
+        return fail(err, FH_ERR_CUDA, "tensor map of the batch rejected (driver error " + std::to_string((int)cr) + ")");
     PanelSolveArgs g;
     g.A = reinterpret_cast<float2 *>(a);
     g.m = m;
@@ -909,7 +926,7 @@ fh_status gemm_tc_panel_solve(float *a, int64_t m, int count, int64_t K0, int W,
     // complex MACs of the triangular product (block j of each 128 rows takes K = 128 (j + 1))
     const double macs = (double)(m - E) * kTile * kTile * (g.nbw * (g.nbw + 1) / 2) * count;
     if (prof) prof_begin(s, FH_PROF_PANEL_SOLVE);
-    panel_solve_kernel<<<grid, kPsThreads, kPsSmemBytes, s>>>(g, g_flag[dev]);
+    panel_solve_kernel<<<grid, kPsThreads, kPsSmemBytes, s>>>(g, rows_map, g_flag[dev]);
     if (prof) prof_end(s, FH_PROF_PANEL_SOLVE, 24.0 * macs);  // BF16 tensor flops (3 products x 8)
     cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) return fail(err, FH_ERR_CUDA, std::string("panel solve launch failed: ") + cudaGetErrorString(le));

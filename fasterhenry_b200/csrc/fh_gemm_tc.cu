@@ -140,12 +140,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Split one FP32 value into its BF16 hi and lo terms (bit patterns).
-__device__ __forceinline__ void split(float x, uint16_t &hi, uint16_t &lo) {
-    __nv_bfloat16 h = __float2bfloat16_rn(x);
-    __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
-    hi = __bfloat16_as_ushort(h);
-    lo = __bfloat16_as_ushort(l);
+// Two FP32 values split into BF16 hi and lo terms (x = hi + lo to 16 bits),
+// each pair converted by one cvt.rn.bf16x2.f32: the 32-bit words of the hi
+// and lo terms, first value in the low half.
+__device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t &lo) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    const float2 back = __bfloat1622float2(h);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(a - back.x, b - back.y);
+    hi = *reinterpret_cast<const uint32_t *>(&h);
+    lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
 // Byte offset of (row r, k-group j) inside a tile: [j][r/8][r%8][8 bf16].
@@ -178,25 +181,19 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
         : "r"(taddr));
 }
 
-__device__ __forceinline__ uint32_t pack2(uint16_t a, uint16_t b) { return (uint32_t)a | ((uint32_t)b << 16); }
-
 // Splits 8 complex values into the four 16-byte core-matrix rows (re hi, re
 // lo, im hi, im lo) of tiles t_re_hi, t_re_hi+1, t_im_hi, t_im_hi+1.
 __device__ __forceinline__ void split_store8(const float2 *v, uint8_t *buf, int t_re_hi, int t_im_hi, uint32_t off) {
-    uint16_t rh[8], rl[8], ih[8], il[8];
+    uint32_t rh[4], rl[4], ih[4], il[4];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        split(v[k].x, rh[k], rl[k]);
-        split(v[k].y, ih[k], il[k]);
+    for (int q = 0; q < 4; ++q) {
+        split2(v[2 * q].x, v[2 * q + 1].x, rh[q], rl[q]);
+        split2(v[2 * q].y, v[2 * q + 1].y, ih[q], il[q]);
     }
-    *reinterpret_cast<uint4 *>(buf + t_re_hi * kTileBytes + off) =
-        make_uint4(pack2(rh[0], rh[1]), pack2(rh[2], rh[3]), pack2(rh[4], rh[5]), pack2(rh[6], rh[7]));
-    *reinterpret_cast<uint4 *>(buf + (t_re_hi + 1) * kTileBytes + off) =
-        make_uint4(pack2(rl[0], rl[1]), pack2(rl[2], rl[3]), pack2(rl[4], rl[5]), pack2(rl[6], rl[7]));
-    *reinterpret_cast<uint4 *>(buf + t_im_hi * kTileBytes + off) =
-        make_uint4(pack2(ih[0], ih[1]), pack2(ih[2], ih[3]), pack2(ih[4], ih[5]), pack2(ih[6], ih[7]));
-    *reinterpret_cast<uint4 *>(buf + (t_im_hi + 1) * kTileBytes + off) =
-        make_uint4(pack2(il[0], il[1]), pack2(il[2], il[3]), pack2(il[4], il[5]), pack2(il[6], il[7]));
+    *reinterpret_cast<uint4 *>(buf + t_re_hi * kTileBytes + off) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+    *reinterpret_cast<uint4 *>(buf + (t_re_hi + 1) * kTileBytes + off) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+    *reinterpret_cast<uint4 *>(buf + t_im_hi * kTileBytes + off) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+    *reinterpret_cast<uint4 *>(buf + (t_im_hi + 1) * kTileBytes + off) = make_uint4(il[0], il[1], il[2], il[3]);
 }
 
 // Loads complex chunk `c` (16 columns of L21 for the tile's 128 rows and 16

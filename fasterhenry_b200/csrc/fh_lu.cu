@@ -1072,6 +1072,9 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
     };
     fh_status st = FH_OK;
     const bool nopivot = w.nopivot;
+    // The closing coop_check reads this flag whether or not a cooperative
+    // panel ran (the factorization without pivoting runs none).
+    FHB_CUDA(cudaMemsetAsync(w.coop->error, 0, sizeof(int), s));
     if (nopivot) {
         if (!w.uinv) return fail(err, FH_ERR_INVALID_ARGUMENT, "the factorization without pivoting needs uinv");
         const size_t diag_smem = sizeof(C) * ((size_t)nb * nb + kDiagSmemExtra);
@@ -1084,7 +1087,8 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
     // Without pivoting and with the scratch for it, the rows below each
     // super-panel are left to one tensor-core pass (gemm_tc_panel_solve);
     // the per-block steps then stop at the super-panel's last row.
-    const bool fused = nopivot && w.xinv && w.xpack && w.tbuf && w.dvec && nb == 128 && outer % nb == 0;
+    const bool fused = nopivot && w.xinv && w.xpack && w.tbuf && w.dvec && nb == 128 && outer % nb == 0 &&
+                       panel_solve_supported(m) && (int64_t)count * m <= INT32_MAX;
     C *xinv = reinterpret_cast<C *>(w.xinv), *dvec = reinterpret_cast<C *>(w.dvec);
     for (int64_t K0 = 0; K0 < m; K0 += outer) {
         const int W = (int)std::min<int64_t>(outer, m - K0);

@@ -133,8 +133,9 @@ fh_status gemm_tc_pack_b(const float *B, int64_t ldb, int64_t sB, int64_t N, int
 // factored without interchanges and the rows below it: L21 = A21 X in place
 // (X = U_D^{-1}, xpack from gemm_tc_pack_b), U12 = diag(dvec) L21^T over the
 // super-panel's rows of the trailing columns, and both operands of the deep
-// update packed into pack_a / pack_b.  The batch buffer needs 16 bytes of
-// slack after its last matrix (raw column copies start on a 16-byte boundary).
+// update packed into pack_a / pack_b.  The rows are read by 2D tensor copies,
+// so the order m must be even (a column stride of 16-byte multiples).
+bool panel_solve_supported(int64_t m);
 fh_status gemm_tc_panel_solve(float *a, int64_t m, int count, int64_t K0, int W, const void *xpack, const float *dvec,
                               void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err);
 fh_status gemm_tc_packed_check(fh_error_info *err);

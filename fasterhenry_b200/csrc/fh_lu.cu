@@ -423,32 +423,216 @@ __global__ void __launch_bounds__(128) bwd_panel_kernel2(const Cx<T> *__restrict
 // (i < 4) of columns warp + 16 j (j < 8), so a column belongs to one warp and a
 // row to one lane of every warp.  Step k of the elimination reads column k
 // and row k of the block as step k - 1 left them; the owners write those
-// entries to a shared double buffer as soon as their own update of step k - 1
-// produces them (with the reciprocal of the next pivot), so a step costs one
-// barrier.  Row groups and columns a step does not touch are skipped with
-// warp-uniform tests.  The inverses run in the same registers with the
-// factors kept in shared memory: X = L^{-1} by forward elimination on the
+// entries to a shared double buffer right after their own update of step
+// k - 1 (with the reciprocal of the next pivot), so a step costs one barrier.
+// The steps run in eight segments of 16 (a template per segment): inside one,
+// the row group and the column slot of k are constants, so the row groups and
+// column slots a step does not touch are left out at compile time and every
+// register index is a constant.  The inverses run in the same registers with
+// the factors kept in shared memory: X = L^{-1} by forward elimination on the
 // rows of I (row k of X is final before step k), Y = U^{-1} backward (row k
 // scaled by 1 / U_kk at step k, every thread scaling the published row).
-// All register indices are compile-time constants, so the block never leaves
-// the register file.
 constexpr int kDiagThreads = 512;
 constexpr int kDiagSmemExtra = 2 * 128 + 2 * 128 + 128 + 2;  // complex entries besides the nb x nb factors
+using Cf = Cx<float>;
+
+struct DiagSmem {
+    Cf *S;     // the factors, column-major, ld nb
+    Cf *colb;  // [2][128]
+    Cf *rowb;  // [2][128]
+    Cf *dinv;  // [128]: 1 / U_kk
+    Cf *pinv;  // [2]: 1 / pivot of the step
+};
+
+// Column k1 (slot J, rows >= k1) and row k1 (group I, columns >= k1) of the
+// block into cn / rn, and 1 / a(k1, k1) into *pn.
+template <int J, int I>
+__device__ __forceinline__ void diag_publish(const Cf (&v)[4][8], int k1, int nb, int lane, int warp, Cf *cn, Cf *rn,
+                                             Cf *pn) {
+    if (warp == (k1 & 15)) {
+#pragma unroll
+        for (int i = I; i < 4; ++i) {
+            const int r = lane + 32 * i;
+            if (r >= k1 && r < nb) cn[r] = v[i][J];
+        }
+    }
+    if (lane == (k1 & 31)) {
+#pragma unroll
+        for (int j = J; j < 8; ++j) {
+            const int c = warp + 16 * j;
+            if (c >= k1 && c < nb) {
+                rn[c] = v[I][j];
+                if (c == k1) *pn = cdiv(Cf{1.f, 0.f}, v[I][j]);
+            }
+        }
+    }
+}
+
+// LU steps k in [16 JS, 16 JS + 16):  l_r = a_rk / a_kk,  a_rc -= l_r a_kc  (r, c > k).
+template <int JS>
+__device__ __forceinline__ void diag_lu_segment(Cf (&v)[4][8], int nb, int lane, int warp, const DiagSmem &sm) {
+    constexpr int IS = JS / 2;  // row group of k
+    const Cf zero{0.f, 0.f};
+#pragma unroll 1
+    for (int kk = 0; kk < 16; ++kk) {
+        const int k = 16 * JS + kk;
+        if (k >= nb) return;  // uniform
+        const int b = k & 1, k1 = k + 1;
+        const Cf inv = sm.pinv[b];
+        Cf l[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            l[i] = zero;
+            const int r = lane + 32 * i;
+            if (i >= IS && (i > IS || r > k) && r < nb) l[i] = cmul(sm.colb[b * 128 + r], inv);
+        }
+#pragma unroll
+        for (int j = JS; j < 8; ++j) {
+            const int c = warp + 16 * j;
+            if (j == JS && warp <= kk) {
+                if (warp == kk) {  // column k takes the multipliers
+#pragma unroll
+                    for (int i = IS; i < 4; ++i)
+                        if (i > IS || lane + 32 * i > k) v[i][j] = l[i];
+                }
+                continue;
+            }
+            if (c >= nb) continue;
+            const Cf u = sm.rowb[b * 128 + c];
+#pragma unroll
+            for (int i = IS; i < 4; ++i) csubmul(v[i][j], l[i], u);  // l = 0 on rows <= k
+        }
+        if (k1 < nb) {
+            Cf *cn = sm.colb + (b ^ 1) * 128, *rn = sm.rowb + (b ^ 1) * 128;
+            if (kk < 15) {
+                diag_publish<JS, IS>(v, k1, nb, lane, warp, cn, rn, sm.pinv + (b ^ 1));
+            } else if constexpr (JS < 7) {
+                diag_publish<JS + 1, (JS + 1) / 2>(v, k1, nb, lane, warp, cn, rn, sm.pinv + (b ^ 1));
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Row k + 1 (group I) of X, columns <= k (slots <= JMAX), into rn.
+template <int JMAX, int I>
+__device__ __forceinline__ void diag_publish_xrow(const Cf (&v)[4][8], int k, int lane, int warp, Cf *rn) {
+    if (lane == ((k + 1) & 31)) {
+#pragma unroll
+        for (int j = 0; j <= JMAX; ++j) {
+            const int c = warp + 16 * j;
+            if (c <= k) rn[c] = v[I][j];
+        }
+    }
+}
+
+// X = L^{-1} steps k in [16 JS, 16 JS + 16):  X[r][:] -= L[r][k] X[k][:]  (r > k; X[k][c] = 0 for c > k).
+template <int JS>
+__device__ __forceinline__ void diag_linv_segment(Cf (&v)[4][8], int nb, int lane, int warp, const DiagSmem &sm) {
+    constexpr int IS = JS / 2;
+    const Cf zero{0.f, 0.f}, one{1.f, 0.f};
+#pragma unroll 1
+    for (int kk = 0; kk < 16; ++kk) {
+        const int k = 16 * JS + kk;
+        if (k + 1 >= nb) return;  // uniform
+        const int b = k & 1;
+        Cf *rn = sm.rowb + (b ^ 1) * 128;
+        Cf lk[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            lk[i] = zero;
+            const int r = lane + 32 * i;
+            if (i >= IS && (i > IS || r > k) && r < nb) lk[i] = sm.S[r + k * nb];
+        }
+#pragma unroll
+        for (int j = 0; j <= JS; ++j) {
+            if (j == JS && warp > kk) continue;  // columns c <= k only
+            const Cf xk = sm.rowb[b * 128 + warp + 16 * j];
+#pragma unroll
+            for (int i = IS; i < 4; ++i) csubmul(v[i][j], lk[i], xk);
+        }
+        if (kk < 15) {
+            diag_publish_xrow<JS, IS>(v, k, lane, warp, rn);
+        } else if constexpr (JS < 7) {
+            diag_publish_xrow<JS, (JS + 1) / 2>(v, k, lane, warp, rn);
+        }
+        if (threadIdx.x == 0) rn[k + 1] = one;  // X[k+1][k+1]; later columns of the row are 0
+        __syncthreads();
+    }
+}
+
+// Row km (group I) of Y before its scaling, columns >= k (slots >= JMIN), into rn.
+template <int JMIN, int I>
+__device__ __forceinline__ void diag_publish_yrow(const Cf (&v)[4][8], int km, int k, int nb, int lane, int warp,
+                                                  Cf *rn) {
+    if (lane == (km & 31)) {
+#pragma unroll
+        for (int j = JMIN; j < 8; ++j) {
+            const int c = warp + 16 * j;
+            if (c >= k && c < nb) rn[c] = v[I][j];
+        }
+    }
+}
+
+// Y = U^{-1} steps k = 16 JS + 15 .. 16 JS:  Y[k][:] /= U_kk;  Y[r][:] -= U[r][k] Y[k][:]  (r < k;
+// Y[k][c] = 0 for c < k).  t counts the steps taken (buffer parity).
+template <int JS>
+__device__ __forceinline__ void diag_uinv_segment(Cf (&v)[4][8], int nb, int lane, int warp, const DiagSmem &sm,
+                                                  int &t) {
+    constexpr int IS = JS / 2;
+    const Cf zero{0.f, 0.f}, one{1.f, 0.f};
+#pragma unroll 1
+    for (int kk = 15; kk >= 0; --kk) {
+        const int k = 16 * JS + kk;
+        if (k >= nb) continue;  // uniform
+        const int b = t & 1, km = k - 1;
+        ++t;
+        Cf *rn = sm.rowb + (b ^ 1) * 128;
+        const Cf inv = sm.dinv[k];
+        Cf uk[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            uk[i] = zero;
+            const int r = lane + 32 * i;
+            if (i <= IS && (i < IS || r < k)) uk[i] = sm.S[r + k * nb];
+        }
+#pragma unroll
+        for (int j = JS; j < 8; ++j) {
+            const int c = warp + 16 * j;
+            if (j == JS && warp < kk) continue;  // columns c >= k only
+            if (c >= nb) continue;
+            const Cf yk = cmul(sm.rowb[b * 128 + c], inv);
+#pragma unroll
+            for (int i = 0; i <= IS; ++i) csubmul(v[i][j], uk[i], yk);  // uk = 0 on rows >= k
+            if (lane == (k & 31)) v[IS][j] = yk;                       // row k, scaled
+        }
+        if (km >= 0) {
+            if (kk > 0) {
+                diag_publish_yrow<JS, IS>(v, km, k, nb, lane, warp, rn);
+            } else if constexpr (JS > 0) {
+                diag_publish_yrow<JS, (16 * JS - 1) / 32>(v, km, k, nb, lane, warp, rn);
+            }
+            if (threadIdx.x == 0) rn[km] = one;  // Y[k-1][k-1] before its scaling
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void __launch_bounds__(kDiagThreads, 1)
     diag_factor_kernel(Cx<float> *__restrict__ a, int64_t m, int64_t k0, int nb, Cx<float> *__restrict__ linv,
                        Cx<float> *__restrict__ uinv, int64_t mstride, Cx<float> *__restrict__ x2, int64_t ld2,
                        int64_t stride2, Cx<float> *__restrict__ dv, int64_t dstride) {
-    using C = Cx<float>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *S = reinterpret_cast<C *>(smem_raw);  // the factors, column-major, ld nb
-    C *colb = S + nb * nb;                   // [2][128]
-    C *rowb = colb + 256;                    // [2][128]
-    C *dinv = rowb + 256;                    // [128]: 1 / U_kk
-    C *pinv = dinv + 128;                    // [2]: 1 / pivot of the step
+    DiagSmem sm;
+    sm.S = reinterpret_cast<Cf *>(smem_raw);
+    sm.colb = sm.S + nb * nb;
+    sm.rowb = sm.colb + 256;
+    sm.dinv = sm.rowb + 256;
+    sm.pinv = sm.dinv + 128;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    C *A = a + (int64_t)blockIdx.x * m * m + k0 + k0 * m;
-    const C zero{0.f, 0.f}, one{1.f, 0.f};
-    C v[4][8];
+    Cf *A = a + (int64_t)blockIdx.x * m * m + k0 + k0 * m;
+    const Cf zero{0.f, 0.f}, one{1.f, 0.f};
+    Cf v[4][8];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -457,55 +641,17 @@ __global__ void __launch_bounds__(kDiagThreads, 1)
             v[i][j] = (r < nb && c < nb) ? A[r + (int64_t)c * m] : zero;
         }
 
-    // ---- LU: l_r = a_rk / a_kk,  a_rc -= l_r a_kc  (r, c > k) ----
-    if (warp == 0)  // column 0
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-            if (lane + 32 * i < nb) colb[lane + 32 * i] = v[i][0];
-    if (lane == 0) {  // row 0
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-            if (warp + 16 * j < nb) rowb[warp + 16 * j] = v[0][j];
-        if (warp == 0) pinv[0] = cdiv(one, v[0][0]);
-    }
+    // ---- LU ----
+    diag_publish<0, 0>(v, 0, nb, lane, warp, sm.colb, sm.rowb, sm.pinv);  // column 0, row 0, 1 / a_00
     __syncthreads();
-    for (int k = 0; k < nb; ++k) {
-        const int b = k & 1, k1 = k + 1;
-        const C inv = pinv[b];
-        C *cn = colb + (b ^ 1) * 128, *rn = rowb + (b ^ 1) * 128;
-        C l[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int r = lane + 32 * i;
-            l[i] = zero;
-            if (32 * i + 31 > k && r > k && r < nb) l[i] = cmul(colb[b * 128 + r], inv);
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int c = warp + 16 * j;  // warp-uniform
-            if (c > k && c < nb) {
-                const C u = rowb[b * 128 + c];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    if (32 * i + 31 > k) {
-                        const int r = lane + 32 * i;
-                        csubmul(v[i][j], l[i], u);  // l = 0 on rows <= k
-                        // column k + 1 and row k + 1 as this step leaves them
-                        if (c == k1 && r >= k1 && r < nb) cn[r] = v[i][j];
-                        if (r == k1) {
-                            rn[c] = v[i][j];
-                            if (c == k1) pinv[b ^ 1] = cdiv(one, v[i][j]);
-                        }
-                    }
-                }
-            } else if (c == k) {
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    if (lane + 32 * i > k) v[i][j] = l[i];
-            }
-        }
-        __syncthreads();
-    }
+    diag_lu_segment<0>(v, nb, lane, warp, sm);
+    diag_lu_segment<1>(v, nb, lane, warp, sm);
+    diag_lu_segment<2>(v, nb, lane, warp, sm);
+    diag_lu_segment<3>(v, nb, lane, warp, sm);
+    diag_lu_segment<4>(v, nb, lane, warp, sm);
+    diag_lu_segment<5>(v, nb, lane, warp, sm);
+    diag_lu_segment<6>(v, nb, lane, warp, sm);
+    diag_lu_segment<7>(v, nb, lane, warp, sm);
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -513,51 +659,31 @@ __global__ void __launch_bounds__(kDiagThreads, 1)
             const int r = lane + 32 * i, c = warp + 16 * j;
             if (r < nb && c < nb) {
                 A[r + (int64_t)c * m] = v[i][j];
-                S[r + c * nb] = v[i][j];
+                sm.S[r + c * nb] = v[i][j];
             }
         }
     __syncthreads();
     if (threadIdx.x < nb) {
-        dinv[threadIdx.x] = cdiv(one, S[threadIdx.x + threadIdx.x * nb]);
-        if (dv) dv[(int64_t)blockIdx.x * dstride + threadIdx.x] = S[threadIdx.x + threadIdx.x * nb];
+        sm.dinv[threadIdx.x] = cdiv(one, sm.S[threadIdx.x + threadIdx.x * nb]);
+        if (dv) dv[(int64_t)blockIdx.x * dstride + threadIdx.x] = sm.S[threadIdx.x + threadIdx.x * nb];
+        sm.rowb[threadIdx.x] = threadIdx.x == 0 ? one : zero;  // row 0 of X = I
     }
-    // row 0 of X = I
-    if (threadIdx.x < nb) rowb[threadIdx.x] = threadIdx.x == 0 ? one : zero;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[i][j] = (lane + 32 * i == warp + 16 * j) ? one : zero;
     __syncthreads();
 
-    // ---- X = L^{-1}:  X[r][:] -= L[r][k] X[k][:]  for r > k ----
-    for (int k = 0; k + 1 < nb; ++k) {
-        const int b = k & 1, k1 = k + 1;
-        C *rn = rowb + (b ^ 1) * 128;
-        C lk[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int r = lane + 32 * i;
-            lk[i] = zero;
-            if (32 * i + 31 > k && r > k && r < nb) lk[i] = S[r + k * nb];
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int c = warp + 16 * j;
-            if (c <= k) {  // X[k][c] = 0 for c > k
-                const C xk = rowb[b * 128 + c];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    if (32 * i + 31 > k) {
-                        csubmul(v[i][j], lk[i], xk);
-                        if (lane + 32 * i == k1) rn[c] = v[i][j];  // row k + 1, columns <= k
-                    }
-                }
-            }
-        }
-        if (threadIdx.x == 0) rn[k1] = one;  // X[k+1][k+1]; later columns of the row are 0
-        __syncthreads();
-    }
-    C *out = linv + (int64_t)blockIdx.x * mstride;
+    // ---- X = L^{-1} ----
+    diag_linv_segment<0>(v, nb, lane, warp, sm);
+    diag_linv_segment<1>(v, nb, lane, warp, sm);
+    diag_linv_segment<2>(v, nb, lane, warp, sm);
+    diag_linv_segment<3>(v, nb, lane, warp, sm);
+    diag_linv_segment<4>(v, nb, lane, warp, sm);
+    diag_linv_segment<5>(v, nb, lane, warp, sm);
+    diag_linv_segment<6>(v, nb, lane, warp, sm);
+    diag_linv_segment<7>(v, nb, lane, warp, sm);
+    Cf *out = linv + (int64_t)blockIdx.x * mstride;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -567,46 +693,25 @@ __global__ void __launch_bounds__(kDiagThreads, 1)
         }
     __syncthreads();  // every read of the row buffers above precedes their reuse
     // row nb - 1 of Y before scaling = that row of I
-    if (threadIdx.x < nb) rowb[threadIdx.x] = (int)threadIdx.x == nb - 1 ? one : zero;
+    if (threadIdx.x < nb) sm.rowb[threadIdx.x] = (int)threadIdx.x == nb - 1 ? one : zero;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[i][j] = (lane + 32 * i == warp + 16 * j) ? one : zero;
     __syncthreads();
 
-    // ---- Y = U^{-1}:  Y[k][:] /= U[k][k];  Y[r][:] -= U[r][k] Y[k][:]  for r < k ----
-    for (int k = nb - 1, t = 0; k >= 0; --k, ++t) {
-        const int b = t & 1, km = k - 1;
-        C *rn = rowb + (b ^ 1) * 128;
-        const C inv = dinv[k];
-        C uk[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int r = lane + 32 * i;
-            uk[i] = zero;
-            if (32 * i < k && r < k) uk[i] = S[r + k * nb];
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int c = warp + 16 * j;
-            if (c >= k && c < nb) {  // Y[k][c] = 0 for c < k
-                const C yk = cmul(rowb[b * 128 + c], inv);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int r = lane + 32 * i;
-                    if (32 * i < k) {
-                        csubmul(v[i][j], uk[i], yk);  // uk = 0 on rows >= k
-                        if (r == km) rn[c] = v[i][j];  // row k - 1 before its scaling, columns >= k
-                    }
-                    if (r == k) v[i][j] = yk;
-                }
-            }
-        }
-        if (threadIdx.x == 0 && km >= 0) rn[km] = one;  // Y[k-1][k-1] before scaling
-        __syncthreads();
-    }
+    // ---- Y = U^{-1} ----
+    int t = 0;
+    diag_uinv_segment<7>(v, nb, lane, warp, sm, t);
+    diag_uinv_segment<6>(v, nb, lane, warp, sm, t);
+    diag_uinv_segment<5>(v, nb, lane, warp, sm, t);
+    diag_uinv_segment<4>(v, nb, lane, warp, sm, t);
+    diag_uinv_segment<3>(v, nb, lane, warp, sm, t);
+    diag_uinv_segment<2>(v, nb, lane, warp, sm, t);
+    diag_uinv_segment<1>(v, nb, lane, warp, sm, t);
+    diag_uinv_segment<0>(v, nb, lane, warp, sm, t);
     out = uinv + (int64_t)blockIdx.x * mstride;
-    Cx<float> *out2 = x2 ? x2 + (int64_t)blockIdx.x * stride2 : nullptr;
+    Cf *out2 = x2 ? x2 + (int64_t)blockIdx.x * stride2 : nullptr;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll

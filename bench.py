@@ -229,9 +229,11 @@ def run_ours(args):
     z64 = r64.impedance_ohm
     rel = [float(np.max(np.abs(zs[k] - z64[k])) / np.max(np.abs(z64[k]))) for k in range(len(freqs))]
 
-    # e2e: solve() through the C ABI from host geometry to host Z.
+    # e2e: solve() through the C ABI from host geometry to host Z, after one
+    # untimed call (the first system of a process grows the device memory cache).
+    fh.solve(geometry, deck.ports, deck.discretization, freqs, fh.Precision.MIXED_BF16X3)
     e2e_times = []
-    for _ in range(max(1, min(args.steps, 3))):
+    for _ in range(max(1, min(args.steps, 5))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         res = fh.solve(geometry, deck.ports, deck.discretization, freqs, fh.Precision.MIXED_BF16X3)
@@ -290,6 +292,7 @@ def run_ours(args):
         "max_rel_err_vs_fp64": max(rel), "rel_err_per_freq": rel,
         "refinement_iterations": [int(x) for x in iters], "fill": fill, "assembly": assembly,
         "e2e": {"value": round(e2e_s, 6), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "samples": [round(t, 4) for t in e2e_times],
                 "what": "solve(): discretize + fill + congruence + mixed sweep + D2H of Z, via the C ABI"},
         "roofline": roofline, "profile": profile, "gpu_launches": int(launches),
         "clocks": clocks.summary(),

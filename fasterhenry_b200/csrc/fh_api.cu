@@ -383,7 +383,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
         w.nopivot = true;
         FHB_PALLOC(pool, xinv, kSlotXinv, (size_t)count * outer * outer * 2);
         FHB_PALLOC(pool, xpack, kSlotXpack, packed_operand_bytes(outer, outer, count));
-        FHB_PALLOC(pool, tbuf, kSlotTbuf, (size_t)count * kNbFp32 * kNbFp32 * 2);
+        FHB_PALLOC(pool, tbuf, kSlotTbuf, (size_t)count * kNbFp32 * (outer - kNbFp32) * 2);
         FHB_PALLOC(pool, dvec, kSlotDvec, (size_t)count * outer * 2);
         w.xinv = xinv.p;
         w.xpack = xpack.p;
@@ -885,7 +885,7 @@ fh_status fh_sweep(fh_system *sys, const double *freqs, size_t nf, fh_precision 
     // super-panel's U^-1 in FP32 and packed.
     const double per = (mixed ? 8.0 : 16.0) * (double)m * (double)m + 64.0 * (double)(m * p + 64) +
                        (outer_for(m, update) ? 16.0 * (double)m * kOuterFp32 + 16.0 * (double)(m + kNbFp32) * kNbFp32 +
-                                                   16.0 * kOuterFp32 * kOuterFp32 + 8.0 * kNbFp32 * kNbFp32
+                                                   16.0 * kOuterFp32 * kOuterFp32 + 8.0 * kNbFp32 * kOuterFp32
                                              : 0.0);
     int chunk = (int)std::max(1.0, std::min<double>((double)nf, 0.8 * (double)free_b / std::max(per, 1.0)));
     PBuf<double> d_omega, d_x, d_z;
@@ -1102,7 +1102,7 @@ fh_status fh_currents(fh_system *sys, const double *freqs, size_t nf, const doub
     const double per = (mixed ? 8.0 : 16.0) * (double)m * (double)m + 64.0 * (double)(m * p + 64) + 48.0 * (double)n +
                        32.0 * (double)nseg +
                        (outer_for(m, update) ? 16.0 * (double)m * kOuterFp32 + 16.0 * (double)(m + kNbFp32) * kNbFp32 +
-                                                   16.0 * kOuterFp32 * kOuterFp32 + 8.0 * kNbFp32 * kNbFp32
+                                                   16.0 * kOuterFp32 * kOuterFp32 + 8.0 * kNbFp32 * kOuterFp32
                                              : 0.0);
     const int chunk = (int)std::max(1.0, std::min<double>((double)nf, 0.8 * (double)free_b / std::max(per, 1.0)));
     PBuf<double> d_omega, d_x, d_z;

@@ -18,7 +18,9 @@
 // chunk's FP32 operands from global memory, split them, and store them to
 // shared memory in the canonical K-major no-swizzle layout (8 x 16-byte core
 // matrices); thread 0 issues the MMAs and commits them to an mbarrier; chunks
-// are double-buffered so the loads of chunk c+1 overlap the MMAs of chunk c.
+// are double-buffered in shared memory, and the global loads of chunk c+2 are
+// issued into registers right after chunk c+1 is stored, so they are in
+// flight during the MMAs of chunk c+1.
 // The epilogue reads the accumulators with tcgen05.ld (warp w owns TMEM lanes
 // 32 (w % 4) .. +31 = rows of the tile, and half w / 4 of the columns) and
 // applies C -= acc with coalesced loads and stores, 16 independent loads in
@@ -196,42 +198,49 @@ __device__ __forceinline__ void split_store8(const float2 *v, uint8_t *buf, int 
     *reinterpret_cast<uint4 *>(buf + (t_im_hi + 1) * kTileBytes + off) = make_uint4(il[0], il[1], il[2], il[3]);
 }
 
-// Loads complex chunk `c` (16 columns of L21 for the tile's 128 rows and 16
-// rows of U12 for its 128 columns), splits it and stores the 8 operand tiles
-// of `buf`.  Thread t handles (row or column t % 128, k-half t / 128): the
-// L21 loads are coalesced across rows, each U12 column half is one 64-byte
-// run read with 16-byte vector loads.
-__device__ __forceinline__ void load_chunk(const GemmArgs &g, int f, int64_t row0, int64_t col0, int c,
-                                           uint8_t *buf) {
+// Chunk `c` of a thread: 8 values of A (row t % 128 of the tile, k-half
+// t / 128) and 8 of B (column t % 128, same k-half), held in registers
+// between their global loads and their split into shared memory.
+struct ChunkRegs {
+    float2 a[8], b[8];
+};
+
+// Issues the global loads of chunk `c` (16 columns of A for the tile's 128
+// rows and 16 rows of B for its 128 columns): the A loads are coalesced
+// across rows, each B column half is one 64-byte run read with 16-byte loads.
+__device__ __forceinline__ void load_chunk(const GemmArgs &g, int f, int64_t row0, int64_t col0, int c, ChunkRegs &v) {
     const int t = threadIdx.x & 127, j = threadIdx.x >> 7;
     const int64_t kk = (int64_t)c * kChunk + 8 * j;
-    float2 va[8], vb[8];
     const int64_t row = row0 + t;
     const int64_t col = col0 + t;
     const float2 *Aop = g.A + (int64_t)f * g.sA;
     const float2 *Bop = g.B + (int64_t)f * g.sB;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) va[k] = row < g.M ? __ldg(Aop + row + (kk + k) * g.lda) : make_float2(0.f, 0.f);
+    for (int k = 0; k < 8; ++k) v.a[k] = row < g.M ? __ldg(Aop + row + (kk + k) * g.lda) : make_float2(0.f, 0.f);
     if (col < g.N) {
         const float4 *src = reinterpret_cast<const float4 *>(Bop + kk + col * g.ldb);
         if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 float4 w = __ldg(src + q);
-                vb[2 * q] = make_float2(w.x, w.y);
-                vb[2 * q + 1] = make_float2(w.z, w.w);
+                v.b[2 * q] = make_float2(w.x, w.y);
+                v.b[2 * q + 1] = make_float2(w.z, w.w);
             }
         } else {
 #pragma unroll
-            for (int k = 0; k < 8; ++k) vb[k] = __ldg(Bop + kk + k + col * g.ldb);
+            for (int k = 0; k < 8; ++k) v.b[k] = __ldg(Bop + kk + k + col * g.ldb);
         }
     } else {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) vb[k] = make_float2(0.f, 0.f);
+        for (int k = 0; k < 8; ++k) v.b[k] = make_float2(0.f, 0.f);
     }
-    const uint32_t off = tile_off(t, j);
-    split_store8(va, buf, ArH, AiH, off);
-    split_store8(vb, buf, BrH, BiH, off);
+}
+
+// Splits a thread's chunk values and stores the 8 operand tiles of `buf`.
+__device__ __forceinline__ void store_chunk(const ChunkRegs &v, uint8_t *buf) {
+    const uint32_t off = tile_off(threadIdx.x & 127, threadIdx.x >> 7);
+    split_store8(v.a, buf, ArH, AiH, off);
+    split_store8(v.b, buf, BrH, BiH, off);
 }
 
 // C (M x N) = C - A B  (assign == 0), C = A B  (assign == 1) or C = -A B
@@ -264,7 +273,10 @@ __global__ void __launch_bounds__(kThreads, 2) gemm_bf16x3_kernel(GemmArgs g, in
         mbar_init(smem_u32(&bars[1]), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    load_chunk(g, f, row0, col0, 0, bufs[0]);
+    ChunkRegs regs;
+    load_chunk(g, f, row0, col0, 0, regs);
+    store_chunk(regs, bufs[0]);
+    if (nchunks > 1) load_chunk(g, f, row0, col0, 1, regs);  // in flight during chunk 0's MMAs
     fence_async_shared();
     tc_fence_before();
     __syncthreads();
@@ -306,7 +318,8 @@ __global__ void __launch_bounds__(kThreads, 2) gemm_bf16x3_kernel(GemmArgs g, in
                 if (!mbar_wait(smem_u32(&bars[nbuf]), (uses[nbuf] - 1) & 1)) ok = false;
             }
             if (ok) {
-                load_chunk(g, f, row0, col0, c + 1, bufs[nbuf]);
+                store_chunk(regs, bufs[nbuf]);  // chunk c + 1, loaded one step ahead
+                if (c + 2 < nchunks) load_chunk(g, f, row0, col0, c + 2, regs);
                 fence_async_shared();
             }
             tc_fence_before();

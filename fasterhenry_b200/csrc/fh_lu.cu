@@ -425,6 +425,8 @@ __global__ void __launch_bounds__(128) bwd_panel_kernel2(const Cx<T> *__restrict
 // and row k of the block as step k - 1 left them; the owners write those
 // entries to a shared double buffer right after their own update of step
 // k - 1 (with the reciprocal of the next pivot), so a step costs one barrier.
+// The LU is one kernel (diag_lu_kernel); the two inverses, which need only
+// the factors, run as two CTAs per matrix of a second (diag_inv_kernel).
 // The steps run in eight segments of 16 (a template per segment): inside one,
 // the row group and the column slot of k are constants, so the row groups and
 // column slots a step does not touch are left out at compile time and every
@@ -435,6 +437,19 @@ __global__ void __launch_bounds__(128) bwd_panel_kernel2(const Cx<T> *__restrict
 constexpr int kDiagThreads = 512;
 constexpr int kDiagSmemExtra = 2 * 128 + 2 * 128 + 128 + 2;  // complex entries besides the nb x nb factors
 using Cf = Cx<float>;
+
+// y -= f x as four fused multiply-adds.
+__device__ __forceinline__ void cfms(Cf &y, Cf f, Cf x) {
+    y.re = fmaf(-f.re, x.re, y.re);
+    y.re = fmaf(f.im, x.im, y.re);
+    y.im = fmaf(-f.re, x.im, y.im);
+    y.im = fmaf(-f.im, x.re, y.im);
+}
+// 1 / p = conj(p) / |p|^2 with one reciprocal.
+__device__ __forceinline__ Cf crcp(Cf p) {
+    const float s = __frcp_rn(p.re * p.re + p.im * p.im);
+    return Cf{p.re * s, -p.im * s};
+}
 
 struct DiagSmem {
     Cf *S;     // the factors, column-major, ld nb
@@ -462,7 +477,7 @@ __device__ __forceinline__ void diag_publish(const Cf (&v)[4][8], int k1, int nb
             const int c = warp + 16 * j;
             if (c >= k1 && c < nb) {
                 rn[c] = v[I][j];
-                if (c == k1) *pn = cdiv(Cf{1.f, 0.f}, v[I][j]);
+                if (c == k1) *pn = crcp(v[I][j]);
             }
         }
     }
@@ -500,7 +515,7 @@ __device__ __forceinline__ void diag_lu_segment(Cf (&v)[4][8], int nb, int lane,
             if (c >= nb) continue;
             const Cf u = sm.rowb[b * 128 + c];
 #pragma unroll
-            for (int i = IS; i < 4; ++i) csubmul(v[i][j], l[i], u);  // l = 0 on rows <= k
+            for (int i = IS; i < 4; ++i) cfms(v[i][j], l[i], u);  // l = 0 on rows <= k
         }
         if (k1 < nb) {
             Cf *cn = sm.colb + (b ^ 1) * 128, *rn = sm.rowb + (b ^ 1) * 128;
@@ -549,7 +564,7 @@ __device__ __forceinline__ void diag_linv_segment(Cf (&v)[4][8], int nb, int lan
             if (j == JS && warp > kk) continue;  // columns c <= k only
             const Cf xk = sm.rowb[b * 128 + warp + 16 * j];
 #pragma unroll
-            for (int i = IS; i < 4; ++i) csubmul(v[i][j], lk[i], xk);
+            for (int i = IS; i < 4; ++i) cfms(v[i][j], lk[i], xk);
         }
         if (kk < 15) {
             diag_publish_xrow<JS, IS>(v, k, lane, warp, rn);
@@ -603,7 +618,7 @@ __device__ __forceinline__ void diag_uinv_segment(Cf (&v)[4][8], int nb, int lan
             if (c >= nb) continue;
             const Cf yk = cmul(sm.rowb[b * 128 + c], inv);
 #pragma unroll
-            for (int i = 0; i <= IS; ++i) csubmul(v[i][j], uk[i], yk);  // uk = 0 on rows >= k
+            for (int i = 0; i <= IS; ++i) cfms(v[i][j], uk[i], yk);  // uk = 0 on rows >= k
             if (lane == (k & 31)) v[IS][j] = yk;                       // row k, scaled
         }
         if (km >= 0) {
@@ -618,20 +633,20 @@ __device__ __forceinline__ void diag_uinv_segment(Cf (&v)[4][8], int nb, int lan
     }
 }
 
+// LU of the block in place (and the diagonal of U into dv); one CTA per matrix.
 __global__ void __launch_bounds__(kDiagThreads, 1)
-    diag_factor_kernel(Cx<float> *__restrict__ a, int64_t m, int64_t k0, int nb, Cx<float> *__restrict__ linv,
-                       Cx<float> *__restrict__ uinv, int64_t mstride, Cx<float> *__restrict__ x2, int64_t ld2,
-                       int64_t stride2, Cx<float> *__restrict__ dv, int64_t dstride) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    diag_lu_kernel(Cx<float> *__restrict__ a, int64_t m, int64_t k0, int nb, Cx<float> *__restrict__ dv,
+                   int64_t dstride) {
+    __shared__ Cf bufs[2 * 128 + 2 * 128 + 2];
     DiagSmem sm;
-    sm.S = reinterpret_cast<Cf *>(smem_raw);
-    sm.colb = sm.S + nb * nb;
-    sm.rowb = sm.colb + 256;
-    sm.dinv = sm.rowb + 256;
-    sm.pinv = sm.dinv + 128;
+    sm.S = nullptr;
+    sm.colb = bufs;
+    sm.rowb = bufs + 256;
+    sm.dinv = nullptr;
+    sm.pinv = bufs + 512;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Cf *A = a + (int64_t)blockIdx.x * m * m + k0 + k0 * m;
-    const Cf zero{0.f, 0.f}, one{1.f, 0.f};
+    const Cf zero{0.f, 0.f};
     Cf v[4][8];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -640,8 +655,6 @@ __global__ void __launch_bounds__(kDiagThreads, 1)
             const int r = lane + 32 * i, c = warp + 16 * j;
             v[i][j] = (r < nb && c < nb) ? A[r + (int64_t)c * m] : zero;
         }
-
-    // ---- LU ----
     diag_publish<0, 0>(v, 0, nb, lane, warp, sm.colb, sm.rowb, sm.pinv);  // column 0, row 0, 1 / a_00
     __syncthreads();
     diag_lu_segment<0>(v, nb, lane, warp, sm);
@@ -659,59 +672,68 @@ __global__ void __launch_bounds__(kDiagThreads, 1)
             const int r = lane + 32 * i, c = warp + 16 * j;
             if (r < nb && c < nb) {
                 A[r + (int64_t)c * m] = v[i][j];
-                sm.S[r + c * nb] = v[i][j];
+                if (dv && r == c) dv[(int64_t)blockIdx.x * dstride + r] = v[i][j];
             }
         }
+}
+
+// The inverses of the factored block's L (blockIdx.y == 0, into linv) and U
+// (blockIdx.y == 1, into uinv and optionally x2), in parallel: CTA (f, y).
+__global__ void __launch_bounds__(kDiagThreads, 1)
+    diag_inv_kernel(const Cx<float> *__restrict__ a, int64_t m, int64_t k0, int nb, Cx<float> *__restrict__ linv,
+                    Cx<float> *__restrict__ uinv, int64_t mstride, Cx<float> *__restrict__ x2, int64_t ld2,
+                    int64_t stride2) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    DiagSmem sm;
+    sm.S = reinterpret_cast<Cf *>(smem_raw);
+    sm.colb = sm.S + nb * nb;
+    sm.rowb = sm.colb + 256;
+    sm.dinv = sm.rowb + 256;
+    sm.pinv = sm.dinv + 128;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool upper = blockIdx.y == 1;
+    const Cf *A = a + (int64_t)blockIdx.x * m * m + k0 + k0 * m;
+    const Cf zero{0.f, 0.f}, one{1.f, 0.f};
+    for (int idx = threadIdx.x; idx < nb * nb; idx += kDiagThreads) {
+        const int r = idx % nb, c = idx / nb;
+        sm.S[idx] = A[r + (int64_t)c * m];
+    }
     __syncthreads();
     if (threadIdx.x < nb) {
-        sm.dinv[threadIdx.x] = cdiv(one, sm.S[threadIdx.x + threadIdx.x * nb]);
-        if (dv) dv[(int64_t)blockIdx.x * dstride + threadIdx.x] = sm.S[threadIdx.x + threadIdx.x * nb];
-        sm.rowb[threadIdx.x] = threadIdx.x == 0 ? one : zero;  // row 0 of X = I
+        sm.dinv[threadIdx.x] = crcp(sm.S[threadIdx.x + threadIdx.x * nb]);
+        // the first row the elimination reads: row 0 of I (X) or row nb - 1 of I (Y, before scaling)
+        sm.rowb[threadIdx.x] = (int)threadIdx.x == (upper ? nb - 1 : 0) ? one : zero;
     }
+    Cf v[4][8];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[i][j] = (lane + 32 * i == warp + 16 * j) ? one : zero;
     __syncthreads();
-
-    // ---- X = L^{-1} ----
-    diag_linv_segment<0>(v, nb, lane, warp, sm);
-    diag_linv_segment<1>(v, nb, lane, warp, sm);
-    diag_linv_segment<2>(v, nb, lane, warp, sm);
-    diag_linv_segment<3>(v, nb, lane, warp, sm);
-    diag_linv_segment<4>(v, nb, lane, warp, sm);
-    diag_linv_segment<5>(v, nb, lane, warp, sm);
-    diag_linv_segment<6>(v, nb, lane, warp, sm);
-    diag_linv_segment<7>(v, nb, lane, warp, sm);
-    Cf *out = linv + (int64_t)blockIdx.x * mstride;
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int r = lane + 32 * i, c = warp + 16 * j;
-            if (r < nb && c < nb) out[r + c * nb] = v[i][j];
-        }
-    __syncthreads();  // every read of the row buffers above precedes their reuse
-    // row nb - 1 of Y before scaling = that row of I
-    if (threadIdx.x < nb) sm.rowb[threadIdx.x] = (int)threadIdx.x == nb - 1 ? one : zero;
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) v[i][j] = (lane + 32 * i == warp + 16 * j) ? one : zero;
-    __syncthreads();
-
-    // ---- Y = U^{-1} ----
-    int t = 0;
-    diag_uinv_segment<7>(v, nb, lane, warp, sm, t);
-    diag_uinv_segment<6>(v, nb, lane, warp, sm, t);
-    diag_uinv_segment<5>(v, nb, lane, warp, sm, t);
-    diag_uinv_segment<4>(v, nb, lane, warp, sm, t);
-    diag_uinv_segment<3>(v, nb, lane, warp, sm, t);
-    diag_uinv_segment<2>(v, nb, lane, warp, sm, t);
-    diag_uinv_segment<1>(v, nb, lane, warp, sm, t);
-    diag_uinv_segment<0>(v, nb, lane, warp, sm, t);
-    out = uinv + (int64_t)blockIdx.x * mstride;
-    Cf *out2 = x2 ? x2 + (int64_t)blockIdx.x * stride2 : nullptr;
+    Cf *out;
+    if (!upper) {
+        diag_linv_segment<0>(v, nb, lane, warp, sm);
+        diag_linv_segment<1>(v, nb, lane, warp, sm);
+        diag_linv_segment<2>(v, nb, lane, warp, sm);
+        diag_linv_segment<3>(v, nb, lane, warp, sm);
+        diag_linv_segment<4>(v, nb, lane, warp, sm);
+        diag_linv_segment<5>(v, nb, lane, warp, sm);
+        diag_linv_segment<6>(v, nb, lane, warp, sm);
+        diag_linv_segment<7>(v, nb, lane, warp, sm);
+        out = linv + (int64_t)blockIdx.x * mstride;
+    } else {
+        int t = 0;
+        diag_uinv_segment<7>(v, nb, lane, warp, sm, t);
+        diag_uinv_segment<6>(v, nb, lane, warp, sm, t);
+        diag_uinv_segment<5>(v, nb, lane, warp, sm, t);
+        diag_uinv_segment<4>(v, nb, lane, warp, sm, t);
+        diag_uinv_segment<3>(v, nb, lane, warp, sm, t);
+        diag_uinv_segment<2>(v, nb, lane, warp, sm, t);
+        diag_uinv_segment<1>(v, nb, lane, warp, sm, t);
+        diag_uinv_segment<0>(v, nb, lane, warp, sm, t);
+        out = uinv + (int64_t)blockIdx.x * mstride;
+    }
+    Cf *out2 = upper && x2 ? x2 + (int64_t)blockIdx.x * stride2 : nullptr;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -956,6 +978,24 @@ __global__ void __launch_bounds__(256) form_kernel(const double *__restrict__ R,
     }
 }
 
+// FP32 form, two consecutive entries per thread and one 16-byte store per
+// frequency (m * m even, batch 16-byte aligned).
+__global__ void __launch_bounds__(256) form_pair_kernel(const double *__restrict__ R, const double *__restrict__ L,
+                                                        int64_t ld, int64_t m, const double *__restrict__ omega,
+                                                        int count, float4 *__restrict__ a) {
+    const int64_t pairs = m * m / 2;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < pairs; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = 2 * t, i = e % m, j = e / m;
+        const int64_t e1 = e + 1, i1 = e1 % m, j1 = e1 / m;
+        const double r0 = R[i + j * ld], l0 = L[i + j * ld];
+        const double r1 = R[i1 + j1 * ld], l1 = L[i1 + j1 * ld];
+        for (int f = 0; f < count; ++f) {
+            const double w = __ldg(omega + f);
+            __stcs(a + (int64_t)f * pairs + t, make_float4((float)r0, (float)(w * l0), (float)r1, (float)(w * l1)));
+        }
+    }
+}
+
 template <class T>
 __global__ void rhs_kernel(const double *__restrict__ R, const double *__restrict__ L, int64_t ld, int64_t m, int64_t p,
                            const double *__restrict__ omega, int count, Cx<T> *__restrict__ b) {
@@ -1183,8 +1223,7 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
     if (nopivot) {
         if (!w.uinv) return fail(err, FH_ERR_INVALID_ARGUMENT, "the factorization without pivoting needs uinv");
         const size_t diag_smem = sizeof(C) * ((size_t)nb * nb + kDiagSmemExtra);
-        FHB_CUDA(cudaFuncSetAttribute(diag_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)diag_smem));
+        FHB_CUDA(cudaFuncSetAttribute(diag_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem));
         const int64_t total = (int64_t)count * m;
         identity_pivots_kernel<<<grid_for(total, 256, 1024), 256, 0, s>>>(b.pivots, total, m);
         FHB_CUDA(cudaGetLastError());
@@ -1195,6 +1234,8 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
     const bool fused = nopivot && w.xinv && w.xpack && w.tbuf && w.dvec && nb == 128 && outer % nb == 0 &&
                        panel_solve_supported(m) && (int64_t)count * m <= INT32_MAX;
     C *xinv = reinterpret_cast<C *>(w.xinv), *dvec = reinterpret_cast<C *>(w.dvec);
+    // X's blocks below its diagonal are read as zeros and never written.
+    if (fused) FHB_CUDA(cudaMemsetAsync(w.xinv, 0, sizeof(C) * (size_t)count * outer * outer, s));
     for (int64_t K0 = 0; K0 < m; K0 += outer) {
         const int W = (int)std::min<int64_t>(outer, m - K0);
         const int64_t E = K0 + W;
@@ -1211,9 +1252,10 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
                 // (with the fused pass: U^-1 also into X's diagonal block, and
                 // U's diagonal into dvec).
                 const int64_t o = j0 - K0;
-                diag_factor_kernel<<<(unsigned)count, kDiagThreads, sizeof(C) * ((size_t)wj * wj + kDiagSmemExtra), s>>>(
-                    a, m, j0, wj, linv, slot(w.uinv, j0), mstride, below ? xinv + o + o * W : nullptr, W,
-                    (int64_t)W * W, below ? dvec + o : nullptr, W);
+                diag_lu_kernel<<<(unsigned)count, kDiagThreads, 0, s>>>(a, m, j0, wj, below ? dvec + o : nullptr, W);
+                diag_inv_kernel<<<dim3((unsigned)count, 2), kDiagThreads, sizeof(C) * ((size_t)wj * wj + kDiagSmemExtra),
+                                  s>>>(a, m, j0, wj, linv, slot(w.uinv, j0), mstride, below ? xinv + o + o * W : nullptr,
+                                       W, (int64_t)W * W);
                 st = cudaGetLastError() == cudaSuccess ? FH_OK
                                                        : fail(err, FH_ERR_CUDA, "diagonal block factorization launch failed");
             } else {
@@ -1259,24 +1301,26 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
         if (E >= m) break;
         const int64_t n2 = m - E;
         if (below) {
-            // X = U_D^{-1} from the block inverses on its diagonal, one block
-            // column at a time from the diagonal up:
-            //     X_ij = -X_ii (sum_{k = i+1..j} U_ik X_kj)
+            // X = U_D^{-1} from the block inverses on its diagonal, by block
+            // rows from the bottom: row i right of its diagonal block is
+            //     X_i,(i+1..) = -X_ii (U_i,(i+1..) X_(i+1..),(i+1..))
+            // (X_(i+1..),(i+1..) upper triangular and already formed): two
+            // products per block row.
             const int nbw = W / nb;
             auto xat = [&](int bi, int bj) {
                 return reinterpret_cast<float *>(xinv + (int64_t)bi * nb + (int64_t)bj * nb * W);
             };
             float *t = reinterpret_cast<float *>(w.tbuf);
-            const int64_t ww = (int64_t)W * W, tt = (int64_t)nb * nb;
+            const int64_t ww = (int64_t)W * W, tt = (int64_t)nb * (W - nb);
             prof_begin(s, FH_PROF_TRSM);
-            for (int bj = 1; bj < nbw && !st; ++bj)
-                for (int bi = bj - 1; bi >= 0 && !st; --bi) {
-                    st = gemm_tc_strided(at(K0 + (int64_t)bi * nb, K0 + (int64_t)(bi + 1) * nb), m, mm, xat(bi + 1, bj),
-                                         W, ww, t, nb, tt, nb, nb, (bj - bi) * nb, 1, count, s, err);
-                    if (!st)
-                        st = gemm_tc_strided(xat(bi, bi), W, ww, t, nb, tt, xat(bi, bj), W, ww, nb, nb, nb, 2, count, s,
-                                             err);
-                }
+            for (int bi = nbw - 2; bi >= 0 && !st; --bi) {
+                const int rest = (nbw - 1 - bi) * nb;  // columns right of the diagonal block
+                st = gemm_tc_strided(at(K0 + (int64_t)bi * nb, K0 + (int64_t)(bi + 1) * nb), m, mm, xat(bi + 1, bi + 1),
+                                     W, ww, t, nb, tt, nb, rest, rest, 1, count, s, err);
+                if (!st)
+                    st = gemm_tc_strided(xat(bi, bi), W, ww, t, nb, tt, xat(bi, bi + 1), W, ww, nb, rest, nb, 2, count, s,
+                                         err);
+            }
             if (!st) st = gemm_tc_pack_b(reinterpret_cast<float *>(xinv), W, ww, W, W, count, w.xpack, s, err);
             prof_end(s, FH_PROF_TRSM, 0.0);
             if (st) return st;
@@ -1507,6 +1551,14 @@ template <class T>
 fh_status form_system(const double *Rm, const double *Lm, int64_t ld, int64_t m, const double *omega, int count, T *a,
                       cudaStream_t s, fh_error_info *err) {
     if (m == 0) return FH_OK;
+    if constexpr (sizeof(T) == 4) {
+        if ((m * m) % 2 == 0 && (reinterpret_cast<uintptr_t>(a) & 15) == 0) {
+            form_pair_kernel<<<grid_for(m * m / 2, 256, 148 * 16), 256, 0, s>>>(Rm, Lm, ld, m, omega, count,
+                                                                             reinterpret_cast<float4 *>(a));
+            FHB_CUDA(cudaGetLastError());
+            return FH_OK;
+        }
+    }
     form_kernel<T><<<grid_for(m * m, 256, 148 * 16), 256, 0, s>>>(Rm, Lm, ld, m, omega, count,
                                                                    reinterpret_cast<Cx<T> *>(a));
     FHB_CUDA(cudaGetLastError());

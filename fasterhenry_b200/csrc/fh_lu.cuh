@@ -70,7 +70,7 @@ struct LuWork {
     //   xinv  count * W * W complex FP32: X = U_D^{-1} of the super-panel's
     //         diagonal block D (column-major, leading dimension W);
     //   xpack packed_operand_bytes(W, W, count): X packed as a B operand;
-    //   tbuf  count * nb * nb complex FP32: one block product;
+    //   tbuf  count * nb * (W - nb) complex FP32: one block row product;
     //   dvec  count * W complex FP32: the diagonal of U_D.
     // With all four set, L21, U12 and the packed operands of the deep update
     // come from one tensor-core pass over the rows below (gemm_tc_panel_solve).

@@ -454,13 +454,27 @@ __device__ __forceinline__ Cf crcp(Cf p) {
 struct DiagSmem {
     Cf *S;     // the factors, column-major, ld nb
     Cf *colb;  // [2][128]
-    Cf *rowb;  // [2][128]
+    Cf *rowb;  // [2][128], column c of a row at (c % 16) * 8 + c / 16 (diag_row_slot)
     Cf *dinv;  // [128]: 1 / U_kk
     Cf *pinv;  // [2]: 1 / pivot of the step
 };
 
-// Column k1 (slot J, rows >= k1) and row k1 (group I, columns >= k1) of the
-// block into cn / rn, and 1 / a(k1, k1) into *pn.
+// Position of column c in a row buffer: the 8 columns a thread owns (warp +
+// 16 j) are adjacent, so a row's owner lane writes them with four 16-byte
+// stores and the readers of a column slot read one broadcast address.
+__device__ __forceinline__ int diag_row_slot(int c) { return (c & 15) * 8 + (c >> 4); }
+
+// Row group I of a lane's registers into its 8 slots of the row buffer rn.
+template <int I>
+__device__ __forceinline__ void diag_store_row(const Cf (&v)[4][8], int warp, Cf *rn) {
+    float4 *d = reinterpret_cast<float4 *>(rn + warp * 8);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) d[q] = make_float4(v[I][2 * q].re, v[I][2 * q].im, v[I][2 * q + 1].re, v[I][2 * q + 1].im);
+}
+
+// Column k1 (slot J, rows >= k1) and row k1 (group I) of the block into cn /
+// rn, and 1 / a(k1, k1) into *pn.  The row is written whole: its columns
+// < k1 are never read.
 template <int J, int I>
 __device__ __forceinline__ void diag_publish(const Cf (&v)[4][8], int k1, int nb, int lane, int warp, Cf *cn, Cf *rn,
                                              Cf *pn) {
@@ -472,14 +486,8 @@ __device__ __forceinline__ void diag_publish(const Cf (&v)[4][8], int k1, int nb
         }
     }
     if (lane == (k1 & 31)) {
-#pragma unroll
-        for (int j = J; j < 8; ++j) {
-            const int c = warp + 16 * j;
-            if (c >= k1 && c < nb) {
-                rn[c] = v[I][j];
-                if (c == k1) *pn = crcp(v[I][j]);
-            }
-        }
+        diag_store_row<I>(v, warp, rn);
+        if (warp == (k1 & 15)) *pn = crcp(v[I][J]);
     }
 }
 
@@ -513,7 +521,7 @@ __device__ __forceinline__ void diag_lu_segment(Cf (&v)[4][8], int nb, int lane,
                 continue;
             }
             if (c >= nb) continue;
-            const Cf u = sm.rowb[b * 128 + c];
+            const Cf u = sm.rowb[b * 128 + warp * 8 + j];
 #pragma unroll
             for (int i = IS; i < 4; ++i) cfms(v[i][j], l[i], u);  // l = 0 on rows <= k
         }
@@ -529,23 +537,18 @@ __device__ __forceinline__ void diag_lu_segment(Cf (&v)[4][8], int nb, int lane,
     }
 }
 
-// Row k + 1 (group I) of X, columns <= k (slots <= JMAX), into rn.
-template <int JMAX, int I>
+// Row k + 1 (group I) of X into rn: its owner's registers hold the whole
+// row (columns <= k as step k left them, 1 at k + 1, zeros after).
+template <int I>
 __device__ __forceinline__ void diag_publish_xrow(const Cf (&v)[4][8], int k, int lane, int warp, Cf *rn) {
-    if (lane == ((k + 1) & 31)) {
-#pragma unroll
-        for (int j = 0; j <= JMAX; ++j) {
-            const int c = warp + 16 * j;
-            if (c <= k) rn[c] = v[I][j];
-        }
-    }
+    if (lane == ((k + 1) & 31)) diag_store_row<I>(v, warp, rn);
 }
 
 // X = L^{-1} steps k in [16 JS, 16 JS + 16):  X[r][:] -= L[r][k] X[k][:]  (r > k; X[k][c] = 0 for c > k).
 template <int JS>
 __device__ __forceinline__ void diag_linv_segment(Cf (&v)[4][8], int nb, int lane, int warp, const DiagSmem &sm) {
     constexpr int IS = JS / 2;
-    const Cf zero{0.f, 0.f}, one{1.f, 0.f};
+    const Cf zero{0.f, 0.f};
 #pragma unroll 1
     for (int kk = 0; kk < 16; ++kk) {
         const int k = 16 * JS + kk;
@@ -562,31 +565,25 @@ __device__ __forceinline__ void diag_linv_segment(Cf (&v)[4][8], int nb, int lan
 #pragma unroll
         for (int j = 0; j <= JS; ++j) {
             if (j == JS && warp > kk) continue;  // columns c <= k only
-            const Cf xk = sm.rowb[b * 128 + warp + 16 * j];
+            const Cf xk = sm.rowb[b * 128 + warp * 8 + j];
 #pragma unroll
             for (int i = IS; i < 4; ++i) cfms(v[i][j], lk[i], xk);
         }
         if (kk < 15) {
-            diag_publish_xrow<JS, IS>(v, k, lane, warp, rn);
+            diag_publish_xrow<IS>(v, k, lane, warp, rn);
         } else if constexpr (JS < 7) {
-            diag_publish_xrow<JS, (JS + 1) / 2>(v, k, lane, warp, rn);
+            diag_publish_xrow<(JS + 1) / 2>(v, k, lane, warp, rn);
         }
-        if (threadIdx.x == 0) rn[k + 1] = one;  // X[k+1][k+1]; later columns of the row are 0
         __syncthreads();
     }
 }
 
-// Row km (group I) of Y before its scaling, columns >= k (slots >= JMIN), into rn.
-template <int JMIN, int I>
-__device__ __forceinline__ void diag_publish_yrow(const Cf (&v)[4][8], int km, int k, int nb, int lane, int warp,
-                                                  Cf *rn) {
-    if (lane == (km & 31)) {
-#pragma unroll
-        for (int j = JMIN; j < 8; ++j) {
-            const int c = warp + 16 * j;
-            if (c >= k && c < nb) rn[c] = v[I][j];
-        }
-    }
+// Row km (group I) of Y before its scaling into rn: its owner's registers
+// hold the whole row (zeros before km, 1 at km, columns >= k as step k left
+// them).
+template <int I>
+__device__ __forceinline__ void diag_publish_yrow(const Cf (&v)[4][8], int km, int lane, int warp, Cf *rn) {
+    if (lane == (km & 31)) diag_store_row<I>(v, warp, rn);
 }
 
 // Y = U^{-1} steps k = 16 JS + 15 .. 16 JS:  Y[k][:] /= U_kk;  Y[r][:] -= U[r][k] Y[k][:]  (r < k;
@@ -595,7 +592,7 @@ template <int JS>
 __device__ __forceinline__ void diag_uinv_segment(Cf (&v)[4][8], int nb, int lane, int warp, const DiagSmem &sm,
                                                   int &t) {
     constexpr int IS = JS / 2;
-    const Cf zero{0.f, 0.f}, one{1.f, 0.f};
+    const Cf zero{0.f, 0.f};
 #pragma unroll 1
     for (int kk = 15; kk >= 0; --kk) {
         const int k = 16 * JS + kk;
@@ -616,18 +613,17 @@ __device__ __forceinline__ void diag_uinv_segment(Cf (&v)[4][8], int nb, int lan
             const int c = warp + 16 * j;
             if (j == JS && warp < kk) continue;  // columns c >= k only
             if (c >= nb) continue;
-            const Cf yk = cmul(sm.rowb[b * 128 + c], inv);
+            const Cf yk = cmul(sm.rowb[b * 128 + warp * 8 + j], inv);
 #pragma unroll
             for (int i = 0; i <= IS; ++i) cfms(v[i][j], uk[i], yk);  // uk = 0 on rows >= k
             if (lane == (k & 31)) v[IS][j] = yk;                       // row k, scaled
         }
         if (km >= 0) {
             if (kk > 0) {
-                diag_publish_yrow<JS, IS>(v, km, k, nb, lane, warp, rn);
+                diag_publish_yrow<IS>(v, km, lane, warp, rn);
             } else if constexpr (JS > 0) {
-                diag_publish_yrow<JS, (16 * JS - 1) / 32>(v, km, k, nb, lane, warp, rn);
+                diag_publish_yrow<(16 * JS - 1) / 32>(v, km, lane, warp, rn);
             }
-            if (threadIdx.x == 0) rn[km] = one;  // Y[k-1][k-1] before its scaling
         }
         __syncthreads();
     }
@@ -637,7 +633,7 @@ __device__ __forceinline__ void diag_uinv_segment(Cf (&v)[4][8], int nb, int lan
 __global__ void __launch_bounds__(kDiagThreads, 1)
     diag_lu_kernel(Cx<float> *__restrict__ a, int64_t m, int64_t k0, int nb, Cx<float> *__restrict__ dv,
                    int64_t dstride) {
-    __shared__ Cf bufs[2 * 128 + 2 * 128 + 2];
+    __shared__ __align__(16) Cf bufs[2 * 128 + 2 * 128 + 2];
     DiagSmem sm;
     sm.S = nullptr;
     sm.colb = bufs;
@@ -685,11 +681,11 @@ __global__ void __launch_bounds__(kDiagThreads, 1)
                     int64_t stride2) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     DiagSmem sm;
-    sm.S = reinterpret_cast<Cf *>(smem_raw);
-    sm.colb = sm.S + nb * nb;
+    sm.colb = reinterpret_cast<Cf *>(smem_raw);  // the buffers first: 16-byte aligned for any nb
     sm.rowb = sm.colb + 256;
     sm.dinv = sm.rowb + 256;
     sm.pinv = sm.dinv + 128;
+    sm.S = sm.pinv + 2;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool upper = blockIdx.y == 1;
     const Cf *A = a + (int64_t)blockIdx.x * m * m + k0 + k0 * m;
@@ -699,11 +695,9 @@ __global__ void __launch_bounds__(kDiagThreads, 1)
         sm.S[idx] = A[r + (int64_t)c * m];
     }
     __syncthreads();
-    if (threadIdx.x < nb) {
-        sm.dinv[threadIdx.x] = crcp(sm.S[threadIdx.x + threadIdx.x * nb]);
-        // the first row the elimination reads: row 0 of I (X) or row nb - 1 of I (Y, before scaling)
-        sm.rowb[threadIdx.x] = (int)threadIdx.x == (upper ? nb - 1 : 0) ? one : zero;
-    }
+    if (threadIdx.x < nb) sm.dinv[threadIdx.x] = crcp(sm.S[threadIdx.x + threadIdx.x * nb]);
+    // the first row the elimination reads: row 0 of I (X) or row nb - 1 of I (Y, before scaling)
+    if (threadIdx.x < 128) sm.rowb[diag_row_slot(threadIdx.x)] = (int)threadIdx.x == (upper ? nb - 1 : 0) ? one : zero;
     Cf v[4][8];
 #pragma unroll
     for (int i = 0; i < 4; ++i)

@@ -161,12 +161,14 @@ __global__ void __launch_bounds__(kThreads) trisolve_kernel(SolveArgs g) {
         if (!group_barrier(bar, expected, g.error)) return;
         for (int64_t k0 = g0; k0 < g0 + wg; k0 += nb) {
             const int wk = (int)min((int64_t)nb, g0 + wg - k0);
-            for (int t = tid; t < wk; t += kThreads) xin[t] = ldcg(X + k0 + t);
-            __syncthreads();
-            diag_apply(g.linv + (size_t)(k0 / nb) * blk_stride + (size_t)f * nb * nb, wk, xin, xs, part);
             int64_t r0, r1;
             share(k0 + wk, m, g.per_group, slice, r0, r1);
-            block_update(A + k0 * m, m, wk, xs, X, r0, r1);
+            if (slice == 0 || r0 < r1) {  // a CTA without rows in this step only meets the barrier
+                for (int t = tid; t < wk; t += kThreads) xin[t] = ldcg(X + k0 + t);
+                __syncthreads();
+                diag_apply(g.linv + (size_t)(k0 / nb) * blk_stride + (size_t)f * nb * nb, wk, xin, xs, part);
+                block_update(A + k0 * m, m, wk, xs, X, r0, r1);
+            }
             if (!group_barrier(bar, expected, g.error)) return;
             if (slice == 0)
                 for (int t = tid; t < wk; t += kThreads) X[k0 + t] = xs[t];
@@ -180,12 +182,14 @@ __global__ void __launch_bounds__(kThreads) trisolve_kernel(SolveArgs g) {
     for (int64_t blk = nblk - 1; blk >= 0; --blk) {
         const int64_t k0 = blk * nb;
         const int wk = (int)min((int64_t)nb, m - k0);
-        for (int t = tid; t < wk; t += kThreads) xin[t] = ldcg(X + k0 + t);
-        __syncthreads();
-        diag_apply(g.uinv + (size_t)blk * blk_stride + (size_t)f * nb * nb, wk, xin, xs, part);
         int64_t r0, r1;
         share(0, k0, g.per_group, slice, r0, r1);
-        block_update(A + k0 * m, m, wk, xs, X, r0, r1);
+        if (slice == 0 || r0 < r1) {
+            for (int t = tid; t < wk; t += kThreads) xin[t] = ldcg(X + k0 + t);
+            __syncthreads();
+            diag_apply(g.uinv + (size_t)blk * blk_stride + (size_t)f * nb * nb, wk, xin, xs, part);
+            block_update(A + k0 * m, m, wk, xs, X, r0, r1);
+        }
         if (!group_barrier(bar, expected, g.error)) return;
         if (slice == 0)
             for (int t = tid; t < wk; t += kThreads) X[k0 + t] = xs[t];

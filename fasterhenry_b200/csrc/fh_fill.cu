@@ -250,13 +250,23 @@ __device__ __forceinline__ void store_pair(double *L, int8_t *methods, int64_t n
 
 // ---------------------------------------------------------------------------
 // Classification: pass 0 counts per category, pass 1 writes the work lists.
-// Block (32, 8) covers a 32 x 32 tile of the upper triangle.
+// Block (32, 8) covers a 32 x 32 tile of the upper triangle.  With `rec`, the
+// counting pass also keeps each pair's classification (8 bytes: category + 1,
+// canonical swap and cost; packed orders) per upper tile, and the writing
+// pass is classify_scatter_kernel, which reads them back instead of
+// classifying again.
 // ---------------------------------------------------------------------------
+// Linear index of upper tile (ti <= tj) of a T x T tile grid.
+__device__ __forceinline__ int64_t upper_tile(int ti, int tj, int T) {
+    return (int64_t)ti * T - (int64_t)ti * (ti - 1) / 2 + (tj - ti);
+}
+
 template <bool kWrite>
 __global__ void __launch_bounds__(256) classify_kernel(const DevFil *__restrict__ fil, int n,
                                                        unsigned long long *__restrict__ counts,
                                                        unsigned long long *__restrict__ cursor,
-                                                       int4 *__restrict__ items, PairMaskDev mask) {
+                                                       int4 *__restrict__ items, PairMaskDev mask,
+                                                       uint2 *__restrict__ rec) {
     const int ti = blockIdx.y, tj = blockIdx.x;
     if (ti > tj) return;
     __shared__ DevFil s_i[32], s_j[32];
@@ -288,6 +298,16 @@ __global__ void __launch_bounds__(256) classify_kernel(const DevFil *__restrict_
             if (cls[r].cat >= 0) slot[r] = atomicAdd(&s_count[cls[r].cat], 1u);
         }
     }
+    if (!kWrite && rec) {
+        uint2 *out = rec + upper_tile(ti, tj, gridDim.x) * 1024;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            out[(threadIdx.y + 8 * r) * 32 + threadIdx.x] =
+                cls[r].cat < 0 ? make_uint2(0u, 0u)
+                               : make_uint2((unsigned)(cls[r].cat + 1) | ((cls[r].swap ? 1u : 0u) << 6) |
+                                                ((unsigned)cls[r].cost << 7),
+                                            (unsigned)cls[r].orders);
+    }
     __syncthreads();
     if (!kWrite) {
         if (tid < kCats && s_count[tid]) atomicAdd(&counts[tid], (unsigned long long)s_count[tid]);
@@ -301,6 +321,42 @@ __global__ void __launch_bounds__(256) classify_kernel(const DevFil *__restrict_
         const int i = ti * 32 + threadIdx.y + 8 * r;
         int a = cls[r].swap ? j : i, b = cls[r].swap ? i : j;
         items[s_base[cls[r].cat] + slot[r]] = make_int4(a, b, cls[r].orders, cls[r].cost);
+    }
+}
+
+// The writing pass from kept classifications (see classify_kernel): the same
+// work lists, with the slots taken per tile in the same way.
+__global__ void __launch_bounds__(256) classify_scatter_kernel(const uint2 *__restrict__ rec,
+                                                               unsigned long long *__restrict__ cursor,
+                                                               int4 *__restrict__ items) {
+    const int ti = blockIdx.y, tj = blockIdx.x;
+    if (ti > tj) return;
+    __shared__ unsigned s_count[kCats];
+    __shared__ unsigned long long s_base[kCats];
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    if (tid < kCats) s_count[tid] = 0;
+    __syncthreads();
+    const uint2 *in = rec + upper_tile(ti, tj, gridDim.x) * 1024;
+    const int j = tj * 32 + threadIdx.x;
+    uint2 c[4];
+    unsigned slot[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        c[r] = in[(threadIdx.y + 8 * r) * 32 + threadIdx.x];
+        const int cat = (int)(c[r].x & 63u) - 1;
+        if (cat >= 0) slot[r] = atomicAdd(&s_count[cat], 1u);
+    }
+    __syncthreads();
+    if (tid < kCats) s_base[tid] = s_count[tid] ? atomicAdd(&cursor[tid], (unsigned long long)s_count[tid]) : 0ull;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int cat = (int)(c[r].x & 63u) - 1;
+        if (cat < 0) continue;
+        const int i = ti * 32 + threadIdx.y + 8 * r;
+        const bool swap = (c[r].x >> 6) & 1u;
+        const int a = swap ? j : i, b = swap ? i : j;
+        items[s_base[cat] + slot[r]] = make_int4(a, b, (int)c[r].y, (int)(c[r].x >> 7));
     }
 }
 
@@ -1431,13 +1487,24 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
     FHB_CUDA(cudaMemsetAsync(&d_err->code, 0, sizeof(int), stream));
     const int T = (int)((n + 31) / 32);
     dim3 grid(T, T), block(32, 8);
+    // The counting pass keeps every pair's classification for the writing
+    // pass (8 bytes per pair of the upper tiles) when the memory is there;
+    // otherwise the writing pass classifies again.
+    uint2 *d_rec = nullptr;
+    if (!list) {
+        const size_t rec_bytes = sizeof(uint2) * 1024 * ((size_t)T * (T + 1) / 2);
+        if (alloc((void **)&d_rec, rec_bytes) != cudaSuccess) {
+            cudaGetLastError();
+            d_rec = nullptr;
+        }
+    }
     const unsigned list_blocks = (unsigned)((n_pairs + 255) / 256);
     FHB_CUDA(cudaEventRecord(ev[0], stream));
     if (list)
         classify_list_kernel<false><<<list_blocks, 256, 0, stream>>>(d_fil, d_pairs, n_pairs, d_counts, nullptr,
                                                                       nullptr);
     else
-        classify_kernel<false><<<grid, block, 0, stream>>>(d_fil, (int)n, d_counts, nullptr, nullptr, pm);
+        classify_kernel<false><<<grid, block, 0, stream>>>(d_fil, (int)n, d_counts, nullptr, nullptr, pm, d_rec);
     FHB_CUDA(cudaGetLastError());
     unsigned long long counts[kCats];
     FHB_CUDA(cudaMemcpyAsync(counts, d_counts, sizeof counts, cudaMemcpyDeviceToHost, stream));
@@ -1452,8 +1519,10 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
     if (list)
         classify_list_kernel<true><<<list_blocks, 256, 0, stream>>>(d_fil, d_pairs, n_pairs, nullptr, d_cursor,
                                                                      d_items);
+    else if (d_rec)
+        classify_scatter_kernel<<<grid, block, 0, stream>>>(d_rec, d_cursor, d_items);
     else
-        classify_kernel<true><<<grid, block, 0, stream>>>(d_fil, (int)n, nullptr, d_cursor, d_items, pm);
+        classify_kernel<true><<<grid, block, 0, stream>>>(d_fil, (int)n, nullptr, d_cursor, d_items, pm, nullptr);
     FHB_CUDA(cudaGetLastError());
     FHB_CUDA(cudaEventRecord(ev[1], stream));
     const int sms = 148;

@@ -146,7 +146,7 @@ class FillStats(ctypes.Structure):
                                               "aligned_quadrature", "sampled", "distinct_aligned_keys")] + \
                [(k, ctypes.c_double) for k in ("point_evaluations", "ms_classify", "ms_point", "ms_closed_form",
                                                "ms_aligned_quadrature", "ms_sampled", "ms_congruence")] + \
-               [("truncated", ctypes.c_int64)]
+               [("truncated", ctypes.c_int64), ("distinct_point_keys", ctypes.c_int64)]
 
 
 class CouplingSpec(ctypes.Structure):

@@ -814,6 +814,7 @@ fh_status fh_system_fill_stats(const fh_system *sys, fh_fill_stats *o) {
     o->ms_sampled = f.ms_sampled;
     o->ms_congruence = sys->ms_congruence;
     o->truncated = f.truncated;
+    o->distinct_point_keys = f.unique_point;
     return FH_OK;
 }
 

@@ -75,6 +75,7 @@ struct FillStats {
     int64_t pairs = 0, orthogonal = 0, point = 0, closed_form = 0, aligned_quadrature = 0, sampled = 0;
     int64_t truncated = 0;
     int64_t unique_aligned = 0;
+    int64_t unique_point = 0;  // distinct point-quadrature keys (value fill)
     double point_evaluations = 0.0;
     float ms_classify = 0, ms_point = 0, ms_aligned = 0, ms_quadrature = 0, ms_sampled = 0;
 };

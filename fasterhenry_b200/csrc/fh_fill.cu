@@ -401,61 +401,102 @@ __global__ void __launch_bounds__(256) classify_list_kernel(const DevFil *__rest
 // ---------------------------------------------------------------------------
 // Point quadrature (neumann.rs:196-266), thread per pair.
 // ---------------------------------------------------------------------------
+// The offset B.centre - A.centre a point-quadrature pair is evaluated with:
+// quantized to a multiple of q = 2^-36 times the smallest cross-section half
+// size (exact when it does not fit; `exact` bit d then set), so pairs that
+// differ only by the rounding of their absolute coordinates have the same
+// offset, quantum `code` and value.
+__device__ __forceinline__ void point_offset(const DevFil &A, const DevFil &B, double delta[3], long long code[3],
+                                             unsigned &exact) {
+    const double mh = fmin(fmin(A.half[1], A.half[2]), fmin(B.half[1], B.half[2]));
+    const double inv_q = mh > 0.0 ? ldexp(1.0 / mh, 36) : 0.0;
+    exact = 0;
+    for (int d = 0; d < 3; ++d) {
+        const double dd = __dsub_rn(B.centre[d], A.centre[d]);
+        const double sc = dd * inv_q;
+        if (inv_q > 0.0 && isfinite(sc) && fabs(sc) < 4.0e18) {
+            code[d] = llrint(sc);
+            delta[d] = (double)code[d] / inv_q;
+        } else {
+            code[d] = __double_as_longlong(dd);
+            delta[d] = dd;
+            exact |= 1u << d;
+        }
+    }
+}
+
+// The point sum of one pair, scaled to L: mu0/4pi cos(a, b) sum w_a w_b / |p_a - p_b|.
+// The points are placed relative to the centre of A; `delta` is the offset
+// B.centre - A.centre (see point_offset).
+__device__ __forceinline__ double point_value(const DevFil &A, const DevFil &B, int orders, const double delta[3]) {
+    const int oa0 = orders & 31, oa1 = (orders >> 5) & 31, oa2 = (orders >> 10) & 31;
+    const int ob0 = (orders >> 15) & 31, ob1 = (orders >> 20) & 31, ob2 = (orders >> 25) & 31;
+    double bc[3] = {delta[0], delta[1], delta[2]};
+    double aa[9], ba[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        aa[k] = A.axes[k];
+        ba[k] = B.axes[k];
+    }
+    const double ah0 = A.half[0], ah1 = 2.0 * A.half[1], ah2 = 2.0 * A.half[2];
+    const double bh0 = B.half[0], bh1 = 2.0 * B.half[1], bh2 = 2.0 * B.half[2];
+    double total = 0.0;
+    for (int la = 0; la < oa0; ++la) {
+        const double xl = ah0 * c_quad.nodes[oa0][la], wl = ah0 * c_quad.weights[oa0][la];
+        for (int wa = 0; wa < oa1; ++wa) {
+            const double xw = ah1 * (0.5 * c_quad.nodes[oa1][wa]), ww = 0.5 * c_quad.weights[oa1][wa];
+            for (int ha = 0; ha < oa2; ++ha) {
+                const double xh = ah2 * (0.5 * c_quad.nodes[oa2][ha]), wh = 0.5 * c_quad.weights[oa2][ha];
+                double p[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) p[d] = aa[d] * xl + aa[3 + d] * xw + aa[6 + d] * xh;
+                const double wpa = wl * ww * wh;
+                double inner = 0.0;
+                for (int lb = 0; lb < ob0; ++lb) {
+                    const double yl = bh0 * c_quad.nodes[ob0][lb], vl = bh0 * c_quad.weights[ob0][lb];
+                    for (int wb = 0; wb < ob1; ++wb) {
+                        const double yw = bh1 * (0.5 * c_quad.nodes[ob1][wb]);
+                        const double vlw = vl * (0.5 * c_quad.weights[ob1][wb]);
+                        double q[3];
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) q[d] = p[d] - (bc[d] + ba[d] * yl + ba[3 + d] * yw);
+                        for (int hb = 0; hb < ob2; ++hb) {
+                            const double yh = bh2 * (0.5 * c_quad.nodes[ob2][hb]);
+                            const double vh = 0.5 * c_quad.weights[ob2][hb];
+                            const double dx = q[0] - ba[6] * yh, dy = q[1] - ba[7] * yh, dz = q[2] - ba[8] * yh;
+                            inner += (vlw * vh) * rsqrt(dx * dx + dy * dy + dz * dz);
+                        }
+                    }
+                }
+                total += wpa * inner;
+            }
+        }
+    }
+    const double cosv = ndot(A.axes, B.axes);
+    return kMu0Over4Pi * (total * cosv);
+}
+
 __global__ void __launch_bounds__(128) point_kernel(const DevFil *__restrict__ fil, const int4 *__restrict__ items,
                                                     int64_t count, double *__restrict__ L, int8_t *methods,
                                                     int64_t n, DevError *err) {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
          t += (int64_t)gridDim.x * blockDim.x) {
         const int4 it = items[t];
-        const DevFil &A = fil[it.x];
-        const DevFil &B = fil[it.y];
-        const int oa0 = it.z & 31, oa1 = (it.z >> 5) & 31, oa2 = (it.z >> 10) & 31;
-        const int ob0 = (it.z >> 15) & 31, ob1 = (it.z >> 20) & 31, ob2 = (it.z >> 25) & 31;
-        double ac[3] = {A.centre[0], A.centre[1], A.centre[2]};
-        double bc[3] = {B.centre[0], B.centre[1], B.centre[2]};
-        double aa[9], ba[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            aa[k] = A.axes[k];
-            ba[k] = B.axes[k];
-        }
-        const double ah0 = A.half[0], ah1 = 2.0 * A.half[1], ah2 = 2.0 * A.half[2];
-        const double bh0 = B.half[0], bh1 = 2.0 * B.half[1], bh2 = 2.0 * B.half[2];
-        double total = 0.0;
-        for (int la = 0; la < oa0; ++la) {
-            const double xl = ah0 * c_quad.nodes[oa0][la], wl = ah0 * c_quad.weights[oa0][la];
-            for (int wa = 0; wa < oa1; ++wa) {
-                const double xw = ah1 * (0.5 * c_quad.nodes[oa1][wa]), ww = 0.5 * c_quad.weights[oa1][wa];
-                for (int ha = 0; ha < oa2; ++ha) {
-                    const double xh = ah2 * (0.5 * c_quad.nodes[oa2][ha]), wh = 0.5 * c_quad.weights[oa2][ha];
-                    double p[3];
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) p[d] = ac[d] + aa[d] * xl + aa[3 + d] * xw + aa[6 + d] * xh;
-                    const double wpa = wl * ww * wh;
-                    double inner = 0.0;
-                    for (int lb = 0; lb < ob0; ++lb) {
-                        const double yl = bh0 * c_quad.nodes[ob0][lb], vl = bh0 * c_quad.weights[ob0][lb];
-                        for (int wb = 0; wb < ob1; ++wb) {
-                            const double yw = bh1 * (0.5 * c_quad.nodes[ob1][wb]);
-                            const double vlw = vl * (0.5 * c_quad.weights[ob1][wb]);
-                            double q[3];
-#pragma unroll
-                            for (int d = 0; d < 3; ++d) q[d] = p[d] - (bc[d] + ba[d] * yl + ba[3 + d] * yw);
-                            for (int hb = 0; hb < ob2; ++hb) {
-                                const double yh = bh2 * (0.5 * c_quad.nodes[ob2][hb]);
-                                const double vh = 0.5 * c_quad.weights[ob2][hb];
-                                const double dx = q[0] - ba[6] * yh, dy = q[1] - ba[7] * yh, dz = q[2] - ba[8] * yh;
-                                inner += (vlw * vh) * rsqrt(dx * dx + dy * dy + dz * dz);
-                            }
-                        }
-                    }
-                    total += wpa * inner;
-                }
-            }
-        }
-        const double cosv = ndot(A.axes, B.axes);
-        store_pair(L, methods, n, it, kMu0Over4Pi * (total * cosv), kPoint, err);
+        double delta[3];
+        long long code[3];
+        unsigned exact;
+        point_offset(fil[it.x], fil[it.y], delta, code, exact);
+        store_pair(L, methods, n, it, point_value(fil[it.x], fil[it.y], it.z, delta), kPoint, err);
     }
+}
+
+// Every point pair takes the value of its key's run head.
+__global__ void point_scatter_kernel(const int4 *__restrict__ items, const int64_t *__restrict__ item_head,
+                                     const double *__restrict__ values, int64_t count, double *__restrict__ L,
+                                     int8_t *methods, int64_t n, DevError *err) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x)
+        store_pair(L, methods, n, items[t], values[item_head[t]], kPoint, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -865,22 +906,55 @@ __global__ void aligned_scatter_kernel(const DevFil *__restrict__ fil, const int
 }
 
 // Key of an aligned pair: the nine numbers of AlignedBars (memo.rs:61-76).
-__device__ __forceinline__ void aligned_key(const DevFil *fil, int4 it, unsigned long long k[9]) {
-    Aligned b;
-    aligned_bars(fil[it.x], fil[it.y], &b);
-    const double v[9] = {b.length[0], b.length[1], b.width[0], b.width[1], b.height[0],
-                         b.height[1], b.offset[0], b.offset[1], b.offset[2]};
-    for (int i = 0; i < 9; ++i) k[i] = (unsigned long long)__double_as_longlong(v[i]);
-}
+struct AlignedKey {
+    static constexpr int kWords = 9;
+    __device__ static void get(const DevFil *fil, int4 it, unsigned long long k[kWords]) {
+        Aligned b;
+        aligned_bars(fil[it.x], fil[it.y], &b);
+        const double v[9] = {b.length[0], b.length[1], b.width[0], b.width[1], b.height[0],
+                             b.height[1], b.offset[0], b.offset[1], b.offset[2]};
+        for (int i = 0; i < 9; ++i) k[i] = (unsigned long long)__double_as_longlong(v[i]);
+    }
+};
 
+// Key of a point-quadrature pair: its geometry up to a translation -- the
+// half sizes and axes of both filaments and the orders exactly, the offset
+// of the centres as point_offset quantizes it.  The pair's value is a
+// function of the key alone (point_value with that offset), so it does not
+// depend on which pair of a run is evaluated; it differs from the sum at the
+// unquantized offset by about q / distance, below 1e-11 of it (the point
+// method is only chosen for pairs at least a cross-section apart).
+struct PointKey {
+    static constexpr int kWords = 29;
+    __device__ static void get(const DevFil *fil, int4 it, unsigned long long k[kWords]) {
+        const DevFil &A = fil[it.x], &B = fil[it.y];
+        double delta[3];
+        long long code[3];
+        unsigned exact;
+        point_offset(A, B, delta, code, exact);
+        for (int d = 0; d < 3; ++d) k[d] = (unsigned long long)code[d];
+        k[3] = exact;
+        for (int d = 0; d < 3; ++d) {
+            k[4 + d] = (unsigned long long)__double_as_longlong(A.half[d]);
+            k[7 + d] = (unsigned long long)__double_as_longlong(B.half[d]);
+        }
+        for (int d = 0; d < 9; ++d) {
+            k[10 + d] = (unsigned long long)__double_as_longlong(A.axes[d]);
+            k[19 + d] = (unsigned long long)__double_as_longlong(B.axes[d]);
+        }
+        k[28] = (unsigned)it.z;
+    }
+};
+
+template <class Key>
 __global__ void key_hash_kernel(const DevFil *__restrict__ fil, const int4 *__restrict__ items, int64_t count,
                                 unsigned long long *__restrict__ hash, int64_t *__restrict__ index) {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
          t += (int64_t)gridDim.x * blockDim.x) {
-        unsigned long long k[9];
-        aligned_key(fil, items[t], k);
+        unsigned long long k[Key::kWords];
+        Key::get(fil, items[t], k);
         unsigned long long h = 0x9e3779b97f4a7c15ull;
-        for (int i = 0; i < 9; ++i) {
+        for (int i = 0; i < Key::kWords; ++i) {
             h = (h ^ k[i]) * 0x9e3779b97f4a7c15ull;
             h = (h << 29) | (h >> 35);
         }
@@ -894,22 +968,59 @@ __global__ void key_hash_kernel(const DevFil *__restrict__ fil, const int4 *__re
     }
 }
 
-// After sorting by hash: flag[t] = 1 when item t starts a new key run.
-__global__ void key_heads_kernel(const DevFil *__restrict__ fil, const int4 *__restrict__ items,
-                                 const unsigned long long *__restrict__ hash_sorted,
-                                 const int64_t *__restrict__ order, int64_t count, int64_t *__restrict__ head_pos) {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        bool head = t == 0 || hash_sorted[t] != hash_sorted[t - 1];
-        if (!head) {
-            unsigned long long a[9], b[9];
-            aligned_key(fil, items[order[t]], a);
-            aligned_key(fil, items[order[t - 1]], b);
-            for (int i = 0; i < 9; ++i)
-                if (a[i] != b[i]) head = true;
+// After sorting by hash: head_pos[t] = t when sorted item t starts a new
+// key run (hash or full key differs from item t - 1), else 0.  A block takes
+// 255 consecutive items and computes each key once into shared memory (256
+// keys: its items and the one before them).
+constexpr int kHeadsBlock = 256;
+template <class Key>
+__global__ void __launch_bounds__(kHeadsBlock) key_heads_kernel(const DevFil *__restrict__ fil,
+                                                                const int4 *__restrict__ items,
+                                                                const unsigned long long *__restrict__ hash_sorted,
+                                                                const int64_t *__restrict__ order, int64_t count,
+                                                                int64_t *__restrict__ head_pos) {
+    extern __shared__ unsigned long long keys[];  // [kHeadsBlock][Key::kWords]
+    for (int64_t s0 = (int64_t)blockIdx.x * (kHeadsBlock - 1); s0 < count;
+         s0 += (int64_t)gridDim.x * (kHeadsBlock - 1)) {
+        const int64_t u = s0 - 1 + threadIdx.x;  // the item whose key this thread forms
+        if (u >= 0 && u < count) Key::get(fil, items[order[u]], keys + threadIdx.x * Key::kWords);
+        __syncthreads();
+        const int64_t t = u;
+        if (threadIdx.x > 0 && t < count) {
+            bool head = t == 0 || hash_sorted[t] != hash_sorted[t - 1];
+            if (!head) {
+                const unsigned long long *a = keys + threadIdx.x * Key::kWords, *b = a - Key::kWords;
+                for (int i = 0; i < Key::kWords; ++i)
+                    if (a[i] != b[i]) head = true;
+            }
+            head_pos[t] = head ? t : 0;
         }
-        head_pos[t] = head ? t : 0;
+        __syncthreads();
     }
+}
+
+// values[rank[h]] = the value of the pair items[heads[h]] (heads in work-list
+// order, which is cost order for the point pairs).
+__global__ void __launch_bounds__(128) point_heads_ordered_kernel(const DevFil *__restrict__ fil,
+                                                                  const int4 *__restrict__ items,
+                                                                  const int64_t *__restrict__ heads,
+                                                                  const int64_t *__restrict__ rank, int64_t n_heads,
+                                                                  double *__restrict__ values) {
+    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < n_heads;
+         h += (int64_t)gridDim.x * blockDim.x) {
+        const int4 it = items[heads[h]];
+        double delta[3];
+        long long code[3];
+        unsigned exact;
+        point_offset(fil[it.x], fil[it.y], delta, code, exact);
+        values[rank[h]] = point_value(fil[it.x], fil[it.y], it.z, delta);
+    }
+}
+
+// rank[h] = h (the identity permutation).
+__global__ void iota_kernel(int64_t *__restrict__ v, int64_t count) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x)
+        v[t] = t;
 }
 
 // flag[t] = 1 where sorted item t heads its key's run.
@@ -1526,16 +1637,114 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
     FHB_CUDA(cudaGetLastError());
     FHB_CUDA(cudaEventRecord(ev[1], stream));
     const int sms = 148;
+    // Distinct keys of a list of pairs: hash, sort by hash, flag the heads of
+    // runs of equal keys (full keys compared), max-scan to map every pair to
+    // its run head, compact the heads.  heads[r] = the list index of distinct
+    // key r; item_head[t] = the rank of pair t's key.
+    auto distinct = [&](auto key, const int4 *d_list, int64_t count, int64_t &n_heads, int64_t *&d_heads,
+                        int64_t *&d_item_head) -> fh_status {
+        using Key = decltype(key);
+        unsigned long long *d_hash, *d_hash_sorted;
+        int64_t *d_idx, *d_order, *d_headpos, *d_headof;
+        FHB_CUDA(alloc((void **)&d_hash, 8 * count));
+        FHB_CUDA(alloc((void **)&d_hash_sorted, 8 * count));
+        FHB_CUDA(alloc((void **)&d_idx, 8 * count));
+        FHB_CUDA(alloc((void **)&d_order, 8 * count));
+        FHB_CUDA(alloc((void **)&d_headpos, 8 * count));
+        FHB_CUDA(alloc((void **)&d_headof, 8 * count));
+        const int blocks = (int)std::min<int64_t>((count + 255) / 256, (int64_t)sms * 16);
+        key_hash_kernel<Key><<<blocks, 256, 0, stream>>>(d_fil, d_list, count, d_hash, d_idx);
+        FHB_CUDA(cudaGetLastError());
+        size_t tmp_bytes = 0, tmp2 = 0;
+        // 32 bits of the hash are enough to group the keys: a collision only
+        // splits a run, because the full keys are compared after the sort.
+        FHB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_hash, d_hash_sorted, d_idx, d_order,
+                                                 (int)count, 0, 32, stream));
+        FHB_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tmp2, d_headpos, d_headof, cub::Max(), (int)count, stream));
+        void *d_tmp = nullptr;
+        FHB_CUDA(alloc(&d_tmp, std::max(tmp_bytes, tmp2)));
+        tmp_bytes = std::max(tmp_bytes, tmp2);
+        FHB_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_hash, d_hash_sorted, d_idx, d_order, (int)count,
+                                                 0, 32, stream));
+        {
+            const size_t key_smem = sizeof(unsigned long long) * kHeadsBlock * Key::kWords;
+            FHB_CUDA(cudaFuncSetAttribute(key_heads_kernel<Key>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)key_smem));
+            const int hb = (int)std::min<int64_t>((count + kHeadsBlock - 2) / (kHeadsBlock - 1), (int64_t)sms * 8);
+            key_heads_kernel<Key><<<hb, kHeadsBlock, key_smem, stream>>>(d_fil, d_list, d_hash_sorted, d_order, count,
+                                                                        d_headpos);
+        }
+        FHB_CUDA(cudaGetLastError());
+        FHB_CUDA(cub::DeviceScan::InclusiveScan(d_tmp, tmp_bytes, d_headpos, d_headof, cub::Max(), (int)count, stream));
+        // Compact the heads on the device: head positions are where
+        // headof[t] == t; their ranks (exclusive sum of the flags) number
+        // the distinct keys.
+        int64_t *d_flag = d_headpos, *d_rank = reinterpret_cast<int64_t *>(d_hash);
+        head_flag_kernel<<<blocks, 256, 0, stream>>>(d_headof, count, d_flag);
+        FHB_CUDA(cudaGetLastError());
+        size_t tmp3 = 0;
+        FHB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp3, d_flag, d_rank, (int)count, stream));
+        if (tmp3 > tmp_bytes) {
+            FHB_CUDA(alloc(&d_tmp, tmp3));
+            tmp_bytes = tmp3;
+        }
+        FHB_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_flag, d_rank, (int)count, stream));
+        int64_t last[2];
+        FHB_CUDA(cudaMemcpyAsync(&last[0], d_rank + count - 1, 8, cudaMemcpyDeviceToHost, stream));
+        FHB_CUDA(cudaMemcpyAsync(&last[1], d_flag + count - 1, 8, cudaMemcpyDeviceToHost, stream));
+        FHB_CUDA(cudaStreamSynchronize(stream));
+        n_heads = last[0] + last[1];
+        FHB_CUDA(alloc((void **)&d_heads, 8 * n_heads));
+        FHB_CUDA(alloc((void **)&d_item_head, 8 * count));
+        head_compact_kernel<<<blocks, 256, 0, stream>>>(d_order, d_headof, d_rank, d_flag, count, d_heads,
+                                                        d_item_head);
+        FHB_CUDA(cudaGetLastError());
+        return FH_OK;
+    };
     // Point quadrature over all buckets (contiguous, cost ascending).
     const int64_t n_point = (int64_t)offsets[kPointBuckets];
     st.point = n_point;
     for (int c = 0; c < kPointBuckets; ++c) st.point_evaluations += (double)counts[c] * (1.5 * (double)(1ull << c));
     if (n_point) {
         int blocks = (int)std::min<int64_t>((n_point + 127) / 128, (int64_t)sms * 64);
-        if (grad)
+        if (grad) {
             point_grad_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_tan, d_items, n_point, *grad, n, d_err);
-        else
+        } else if (n_point > INT32_MAX) {  // beyond the sort's 32-bit counts: every pair evaluated
             point_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_items, n_point, d_L, d_methods, n_arg, d_err);
+        } else {
+            // Pairs that are the same geometry up to a translation share one
+            // evaluation (PointKey).
+            int64_t n_heads = 0, *d_heads = nullptr, *d_item_head = nullptr;
+            fh_status ds = distinct(PointKey{}, d_items, n_point, n_heads, d_heads, d_item_head);
+            if (ds) return ds;
+            st.unique_point = n_heads;
+            double *d_pvalues;
+            int64_t *d_rank_in, *d_heads_sorted, *d_rank_sorted;
+            FHB_CUDA(alloc((void **)&d_pvalues, 8 * n_heads));
+            FHB_CUDA(alloc((void **)&d_rank_in, 8 * n_heads));
+            FHB_CUDA(alloc((void **)&d_heads_sorted, 8 * n_heads));
+            FHB_CUDA(alloc((void **)&d_rank_sorted, 8 * n_heads));
+            // Heads in work-list order (cost ascending), so a warp's pairs
+            // have similar loop counts; each value goes to its key's rank.
+            const int iblocks = (int)std::min<int64_t>((n_heads + 255) / 256, (int64_t)sms * 16);
+            iota_kernel<<<iblocks, 256, 0, stream>>>(d_rank_in, n_heads);
+            FHB_CUDA(cudaGetLastError());
+            size_t sort_bytes = 0;
+            const int bits = 64 - __builtin_clzll((unsigned long long)std::max<int64_t>(1, n_point));
+            FHB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, d_heads, d_heads_sorted, d_rank_in,
+                                                     d_rank_sorted, (int)n_heads, 0, bits, stream));
+            void *d_sort_tmp = nullptr;
+            FHB_CUDA(alloc(&d_sort_tmp, std::max<size_t>(sort_bytes, 16)));
+            FHB_CUDA(cub::DeviceRadixSort::SortPairs(d_sort_tmp, sort_bytes, d_heads, d_heads_sorted, d_rank_in,
+                                                     d_rank_sorted, (int)n_heads, 0, bits, stream));
+            const int hblocks = (int)std::min<int64_t>((n_heads + 127) / 128, (int64_t)sms * 64);
+            point_heads_ordered_kernel<<<hblocks, 128, 0, stream>>>(d_fil, d_items, d_heads_sorted, d_rank_sorted,
+                                                                    n_heads, d_pvalues);
+            FHB_CUDA(cudaGetLastError());
+            const int sblocks = (int)std::min<int64_t>((n_point + 255) / 256, (int64_t)sms * 16);
+            point_scatter_kernel<<<sblocks, 256, 0, stream>>>(d_items, d_item_head, d_pvalues, n_point, d_L, d_methods,
+                                                             n_arg, d_err);
+        }
         FHB_CUDA(cudaGetLastError());
     }
     FHB_CUDA(cudaEventRecord(ev[2], stream));
@@ -1565,58 +1774,13 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
     st.closed_form = n_aligned - n_quad;
     st.aligned_quadrature = n_quad;
     if (n_quad) {
-        // Distinct keys: hash, sort, flag run heads, max-scan to map every
-        // pair to its run head, evaluate heads only.
-        unsigned long long *d_hash, *d_hash_sorted;
-        int64_t *d_idx, *d_order, *d_headpos, *d_headof;
-        FHB_CUDA(alloc((void **)&d_hash, 8 * n_quad));
-        FHB_CUDA(alloc((void **)&d_hash_sorted, 8 * n_quad));
-        FHB_CUDA(alloc((void **)&d_idx, 8 * n_quad));
-        FHB_CUDA(alloc((void **)&d_order, 8 * n_quad));
-        FHB_CUDA(alloc((void **)&d_headpos, 8 * n_quad));
-        FHB_CUDA(alloc((void **)&d_headof, 8 * n_quad));
-        int blocks = (int)std::min<int64_t>((n_quad + 255) / 256, (int64_t)sms * 16);
-        key_hash_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_quad, n_quad, d_hash, d_idx);
-        FHB_CUDA(cudaGetLastError());
-        size_t tmp_bytes = 0, tmp2 = 0;
-        FHB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_hash, d_hash_sorted, d_idx, d_order,
-                                                 (int)n_quad, 0, 64, stream));
-        FHB_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tmp2, d_headpos, d_headof, cub::Max(), (int)n_quad, stream));
-        void *d_tmp = nullptr;
-        FHB_CUDA(alloc(&d_tmp, std::max(tmp_bytes, tmp2)));
-        tmp_bytes = std::max(tmp_bytes, tmp2);
-        FHB_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_hash, d_hash_sorted, d_idx, d_order, (int)n_quad,
-                                                 0, 64, stream));
-        key_heads_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_quad, d_hash_sorted, d_order, n_quad, d_headpos);
-        FHB_CUDA(cudaGetLastError());
-        FHB_CUDA(cub::DeviceScan::InclusiveScan(d_tmp, tmp_bytes, d_headpos, d_headof, cub::Max(), (int)n_quad, stream));
-        // Compact the heads on the device: head positions are where
-        // headof[t] == t; their ranks (exclusive sum of the flags) number
-        // the distinct keys.
-        int64_t *d_flag = d_headpos, *d_rank = reinterpret_cast<int64_t *>(d_hash);
-        head_flag_kernel<<<blocks, 256, 0, stream>>>(d_headof, n_quad, d_flag);
-        FHB_CUDA(cudaGetLastError());
-        size_t tmp3 = 0;
-        FHB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp3, d_flag, d_rank, (int)n_quad, stream));
-        if (tmp3 > tmp_bytes) {
-            FHB_CUDA(alloc(&d_tmp, tmp3));
-            tmp_bytes = tmp3;
-        }
-        FHB_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_flag, d_rank, (int)n_quad, stream));
-        int64_t last[2];
-        FHB_CUDA(cudaMemcpyAsync(&last[0], d_rank + n_quad - 1, 8, cudaMemcpyDeviceToHost, stream));
-        FHB_CUDA(cudaMemcpyAsync(&last[1], d_flag + n_quad - 1, 8, cudaMemcpyDeviceToHost, stream));
-        FHB_CUDA(cudaStreamSynchronize(stream));
-        const int64_t n_heads = last[0] + last[1];
+        int64_t n_heads = 0, *d_heads = nullptr, *d_item_head = nullptr;
+        fh_status ds = distinct(AlignedKey{}, d_quad, n_quad, n_heads, d_heads, d_item_head);
+        if (ds) return ds;
         st.unique_aligned = n_heads;
-        int64_t *d_heads, *d_item_head;
         double *d_values;
-        FHB_CUDA(alloc((void **)&d_heads, 8 * n_heads));
-        FHB_CUDA(alloc((void **)&d_item_head, 8 * n_quad));
         FHB_CUDA(alloc((void **)&d_values, (grad ? 56 : 8) * n_heads));
-        head_compact_kernel<<<blocks, 256, 0, stream>>>(d_order, d_headof, d_rank, d_flag, n_quad, d_heads,
-                                                        d_item_head);
-        FHB_CUDA(cudaGetLastError());
+        const int blocks = (int)std::min<int64_t>((n_quad + 255) / 256, (int64_t)sms * 16);
         int qblocks = (int)std::min<int64_t>(n_heads, (int64_t)sms * 16);
         if (grad) {
             aligned_quadrature_kernel<true><<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads,

@@ -442,6 +442,7 @@ typedef struct fh_fill_stats {
     double point_evaluations;
     double ms_classify, ms_point, ms_closed_form, ms_aligned_quadrature, ms_sampled, ms_congruence;
     int64_t truncated;  /* pairs dropped by the coupling (never evaluated, zero in L) */
+    int64_t distinct_point_keys;  /* point-quadrature pairs evaluated (one per geometry up to translation) */
 } fh_fill_stats;
 fh_status fh_system_fill_stats(const fh_system *sys, fh_fill_stats *stats);
 

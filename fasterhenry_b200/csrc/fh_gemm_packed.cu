@@ -483,7 +483,9 @@ constexpr int kPsRawBytes = kChunk * kTile * 8;                   // 16 columns 
 constexpr int kPsStageBytes = 2 * kOpBytes + kPsRawBytes;          // packed A, X, raw: 48 KB
 constexpr int kPsStages = 4;
 constexpr int kPsThreads = 32 * 14;
-constexpr int kPsSmemBytes = kPsStages * kPsStageBytes + 1024 + kBarBytes;
+// A staging tile per epilogue warp for U12 (32 rows x 16 complex, XOR-swizzled).
+constexpr int kPsU12Bytes = kEpiWarps * 32 * 16 * 8;
+constexpr int kPsSmemBytes = kPsStages * kPsStageBytes + kPsU12Bytes + 1024 + kBarBytes;
 static_assert(kPsSmemBytes <= 227 * 1024, "panel-solve shared memory");
 
 struct PanelSolveArgs {
@@ -508,7 +510,8 @@ __global__ void __launch_bounds__(kPsThreads, 1)
     panel_solve_kernel(PanelSolveArgs g, const __grid_constant__ CUtensorMap rows_map, int *__restrict__ err_flag) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kPsStages * kPsStageBytes);
+    float2 *u12_stage = reinterpret_cast<float2 *>(smem + kPsStages * kPsStageBytes);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kPsStages * kPsStageBytes + kPsU12Bytes);
     uint64_t *full = bars;                            // [kPsStages] loader: raw A + X bytes
     uint64_t *afull = bars + kPsStages;               // [kPsStages] splitters
     uint64_t *empty = bars + 2 * kPsStages;           // [kPsStages] MMA commit
@@ -707,16 +710,25 @@ __global__ void __launch_bounds__(kPsThreads, 1)
                         float2 *pl = Af + row + (g.K0 + kc) * g.m;  // L21: down the columns, coalesced over lanes
 #pragma unroll
                         for (int jj = 0; jj < 16; ++jj) pl[(int64_t)jj * g.m] = l[jj];
-                        float2 *pu = Af + (g.K0 + kc) + row * g.m;  // U12: 16 consecutive entries of column `row`
-                        if ((reinterpret_cast<uintptr_t>(pu) & 15) == 0) {
+                    }
+                    {
+                        // U12: the thread's 16 entries lie down column `row`; the
+                        // warp's tile goes through shared memory (column jj of row
+                        // r at r * 16 + (jj ^ (r % 16))) so that each store covers
+                        // 16 consecutive entries of two columns.
+                        float2 *stg = u12_stage + (warp - 4) * 512;
 #pragma unroll
-                            for (int q = 0; q < 8; ++q)
-                                reinterpret_cast<float4 *>(pu)[q] = make_float4(u[2 * q].x, u[2 * q].y, u[2 * q + 1].x,
-                                                                                u[2 * q + 1].y);
-                        } else {
+                        for (int jj = 0; jj < 16; ++jj) stg[lane * 16 + (jj ^ (lane & 15))] = u[jj];
+                        __syncwarp();
+                        const int64_t row_base = g.E + (int64_t)rb * kTile + quarter * 32;
 #pragma unroll
-                            for (int jj = 0; jj < 16; ++jj) pu[jj] = u[jj];
+                        for (int q = 0; q < 16; ++q) {
+                            const int rr = 2 * q + (lane >> 4), kk = lane & 15;
+                            const int64_t r_abs = row_base + rr;
+                            const float2 v = stg[rr * 16 + (kk ^ (rr & 15))];
+                            if (r_abs < g.m) Af[(g.K0 + kc + kk) + r_abs * g.m] = v;
                         }
+                        __syncwarp();
                     }
                     const int64_t tile = ((int64_t)f * g.rblocks + rb) * g.nch + kc / kChunk;
                     split_store8(l, g.Pa + tile * kOpBytes, tile_off(tr, 0));

@@ -136,3 +136,20 @@ def test_coincident_samples_are_reported(fh, oracle):
         assert (e.value.first, e.value.second) == (0, 1)
     else:
         compare(fh, oracle, fil)
+
+
+def test_point_pairs_evaluated_once_per_geometry(fh, oracle):
+    """A regular meander repeats the same relative geometry many times: the
+    point-quadrature pairs share one evaluation per geometry up to a
+    translation, the values still match the oracle's per-pair sums within the
+    fill tolerance, and a second fill gives the same bits."""
+    deck = F.meander_legs(6)
+    geometry = fh.Geometry.from_deck(deck)
+    fil, _ = fh.discretize(geometry, deck.discretization)
+    L, _ = compare(fh, oracle, fil)
+    L2 = fh.partial_inductance_matrix(fil)
+    assert np.array_equal(L, L2)
+    with fh.MeshSystem.assemble(geometry, deck.ports, deck.discretization) as s:
+        st = fh.fill_stats(s)
+    assert st["point_quadrature"] > 0
+    assert 0 < st["distinct_point_keys"] < st["point_quadrature"] // 4, st

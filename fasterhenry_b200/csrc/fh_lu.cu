@@ -1335,7 +1335,8 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             FHB_CUDA(cudaGetLastError());
             prof_end(s, FH_PROF_TRSM, 0.0);
             // Only the lower triangle of the trailing matrix is read from here
-            // on, besides the next super-panel's columns, which are updated in full.
+            // on, besides the next super-panel's columns (updated in full) and
+            // the diagonal 512 x 512 blocks of the later super-panels.
             const int next = (int)((std::min<int64_t>(outer, n2) + 127) / 128);
             st = gemm_tc_packed_update(at(E, K0), m, mm, at(K0, E), m, mm, at(E, E), m, mm, n2, n2, W, count,
                                        w.pack_a, w.pack_b, s, err, next);

@@ -186,3 +186,23 @@ def test_two_level_mixed_odd_order(fh):
         rm = s.sweep(freqs, fh.Precision.MIXED_BF16X3)
     assert rel_err(rm.impedance_ohm, z64) < MIXED_RTOL
     assert all(1 <= i <= 10 for i in rm.refinement_iterations), rm.refinement_iterations
+
+
+def test_two_level_mixed_strongly_coupled_loops(fh):
+    """Two thick segments on a 40 x 30 grid (m = 2,398): every mesh loop of a
+    segment shares the segment's first filament, so loops far apart in the
+    ordering stay strongly coupled -- unlike a meander, where couplings decay
+    fast with the distance between loops.  Every entry the factorization reads
+    must carry all earlier updates for the refinement to converge without the
+    FP64 fallback (iterations -1); this mesh is ill-conditioned enough that
+    it takes 4 to 6 steps."""
+    nodes = [(0.0, 0.0, 0.0), (200 * F.UM, 0.0, 0.0), (200 * F.UM, 200 * F.UM, 0.0)]
+    segs = [F.segment(0, 1, 40 * F.UM, 30 * F.UM), F.segment(1, 2, 40 * F.UM, 30 * F.UM)]
+    deck = F.Deck(nodes, segs, [(0, 2)], F.uniform(40, 30), "thick_bend")
+    freqs = F.logspace(5, 10, 6)
+    with fh.MeshSystem.assemble(fh.Geometry.from_deck(deck), deck.ports, deck.discretization) as s:
+        assert s.counts()["internal_meshes"] > 2048  # at least four 512-column super-panels
+        z64 = s.sweep(freqs, fh.Precision.FP64).impedance_ohm
+        rm = s.sweep(freqs, fh.Precision.MIXED_BF16X3)
+    assert rel_err(rm.impedance_ohm, z64) < MIXED_RTOL
+    assert all(1 <= i <= 8 for i in rm.refinement_iterations), rm.refinement_iterations

@@ -805,12 +805,11 @@ fh_status gemm_tc_packed_run(const void *pack_a, const void *pack_b, float *C, i
     uint32_t *d_table = nullptr;
     if (lower_from >= 0 && lower_from < cblocks) {
         // Lower-triangle form (symmetric trailing matrix, C rows and columns
-        // on the same blocks): column blocks below lower_from (the next
-        // super-panel) in full, the rest on and below the diagonal block, and
-        // the upper tiles inside each later super-panel's diagonal block
-        // (lower_from blocks wide), which that super-panel's own steps read;
-        // the same grouped order as the full schedule (row blocks fastest
-        // inside groups of kGroupRows), the other tiles left out.
+        // on the same blocks): column blocks below lower_from in full, the
+        // rest only on and below the diagonal block; the same grouped order
+        // as the full schedule (row blocks fastest inside groups of
+        // kGroupRows), invalid tiles left out.  The caller forms every U
+        // entry it reads from L (U = D L^T), so no upper tile is read.
         std::vector<uint32_t> table;
         table.reserve((size_t)rblocks * cblocks);
         entries = 0.0;
@@ -819,7 +818,7 @@ fh_status gemm_tc_packed_run(const void *pack_a, const void *pack_b, float *C, i
             for (int cb = 0; cb < cblocks; ++cb)
                 for (int r = 0; r < rows; ++r) {
                     const int rb = g0 + r;
-                    if (cb < lower_from || rb >= cb || rb / lower_from == cb / lower_from) {
+                    if (cb < lower_from || rb >= cb) {
                         table.push_back((uint32_t)rb | ((uint32_t)cb << 16));
                         entries += (double)std::min<int64_t>(kTile, M - (int64_t)rb * kTile) *
                                    (double)std::min<int64_t>(kTile, N - (int64_t)cb * kTile);

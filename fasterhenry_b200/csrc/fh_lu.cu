@@ -751,23 +751,23 @@ __global__ void __launch_bounds__(kDiagThreads, 1)
 // (contiguous in memory) fetched while step k computes.
 // Grid (count, ceil(nb / 32)), 256 threads; dynamic shared memory
 // (32 nb + 2 nb) complex.
-// U[k, c] = U[k, k] L[c, k] for rows k in [K0, K0 + W) and columns c >= E:
-// the U12 block of a symmetric matrix factored without pivoting (U = D L^T).
+// U[k, c] = U[k, k] L[c, k] for rows k in [K0, K0 + W) and columns c in
+// [E, c1): U12 of a symmetric matrix factored without pivoting (U = D L^T).
 // 32 x 32 tiles through shared memory, so both the reads of L (down a column)
 // and the writes of U (along a row) are coalesced.
-__global__ void u12_from_l21_kernel(Cx<float> *__restrict__ a, int64_t m, int64_t K0, int W, int64_t E) {
+__global__ void u12_from_l21_kernel(Cx<float> *__restrict__ a, int64_t m, int64_t K0, int W, int64_t E, int64_t c1) {
     __shared__ Cx<float> t[32][33];
     Cx<float> *A = a + (int64_t)blockIdx.z * m * m;
     const int64_t c0 = E + (int64_t)blockIdx.x * 32, k0 = K0 + (int64_t)blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     for (int r = ty; r < 32; r += 8) {
         const int64_t c = c0 + tx, k = k0 + r;
-        if (c < m && k < K0 + W) t[r][tx] = A[c + k * m];  // L[c, k]
+        if (c < c1 && k < K0 + W) t[r][tx] = A[c + k * m];  // L[c, k]
     }
     __syncthreads();
     for (int r = ty; r < 32; r += 8) {
         const int64_t k = k0 + tx, c = c0 + r;
-        if (c < m && k < K0 + W) A[k + c * m] = cmul(A[k + k * m], t[tx][r]);
+        if (c < c1 && k < K0 + W) A[k + c * m] = cmul(A[k + k * m], t[tx][r]);
     }
 }
 
@@ -1279,9 +1279,17 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
                 swaps(j0, wj, K0, j0);
                 swaps(j0, wj, r1, E);
             }
-            if (r1 < E)
+            if (r1 < E && nopivot) {
+                // U12 inside the super-panel = D L21^T from the L21 just formed,
+                // so nothing reads the upper tiles of a diagonal region, which
+                // the symmetric deep updates leave out.
+                const dim3 tg((unsigned)((E - r1 + 31) / 32), (unsigned)((wj + 31) / 32), (unsigned)count);
+                u12_from_l21_kernel<<<tg, dim3(32, 8), 0, s>>>(a, m, j0, wj, r1, E);
+                st = cudaGetLastError() == cudaSuccess ? FH_OK : fail(err, FH_ERR_CUDA, "U12 transpose launch failed");
+            } else if (r1 < E) {
                 st = gemm_tc_strided(reinterpret_cast<const float *>(linv), wj, mstride, at(j0, r1), m, mm,
                                      at(j0, r1), m, mm, wj, E - r1, wj, 1, count, s, err);
+            }
             prof_end(s, FH_PROF_TRSM, 4.0 * (double)wj * wj * (double)(E - r1) * count);
             if (st) return st;
             if (r1 < E) {
@@ -1331,12 +1339,13 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
         if (nopivot) {
             // Symmetric trailing matrix: U12 = D L21^T (D the diagonal of U11).
             const dim3 tg((unsigned)((n2 + 31) / 32), (unsigned)((W + 31) / 32), (unsigned)count);
-            u12_from_l21_kernel<<<tg, dim3(32, 8), 0, s>>>(a, m, K0, W, E);
+            u12_from_l21_kernel<<<tg, dim3(32, 8), 0, s>>>(a, m, K0, W, E, m);
             FHB_CUDA(cudaGetLastError());
             prof_end(s, FH_PROF_TRSM, 0.0);
             // Only the lower triangle of the trailing matrix is read from here
-            // on, besides the next super-panel's columns (updated in full) and
-            // the diagonal 512 x 512 blocks of the later super-panels.
+            // on, besides the next super-panel's columns, which are updated in
+            // full (U12 of later super-panels, inside their diagonal blocks too,
+            // comes from L21).
             const int next = (int)((std::min<int64_t>(outer, n2) + 127) / 128);
             st = gemm_tc_packed_update(at(E, K0), m, mm, at(K0, E), m, mm, at(E, E), m, mm, n2, n2, W, count,
                                        w.pack_a, w.pack_b, s, err, next);

@@ -318,7 +318,9 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     FHB_PALLOC(pool, piv, kSlotPiv, (size_t)count * m);
     FHB_PALLOC(pool, sing, kSlotSing, (size_t)count);
     FHB_CUDA(cudaMemsetAsync(sing.p, 0, sizeof(int) * count, st));
-    fh_status e = form_system<float>(s->d_Rm, s->d_Lm, ld, m, d_omega, count, a.p, st, err);
+    // The two-level form factors without pivoting and forms every U entry it
+    // reads from L: the tiles above the diagonal are not needed.
+    fh_status e = form_system<float>(s->d_Rm, s->d_Lm, ld, m, d_omega, count, a.p, st, err, outer_for(m, mode) > 0);
     if (e) return e;
     e = form_rhs<double>(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, r.p, st, err);  // r0 = b
     if (e) return e;

@@ -973,14 +973,16 @@ __global__ void __launch_bounds__(256) form_kernel(const double *__restrict__ R,
 }
 
 // FP32 form, two consecutive entries per thread and one 16-byte store per
-// frequency (m * m even, batch 16-byte aligned).
+// frequency (m * m even, batch 16-byte aligned).  With lower_tiles, pairs
+// whose entries both lie in 128 x 128 tiles above the diagonal are skipped.
 __global__ void __launch_bounds__(256) form_pair_kernel(const double *__restrict__ R, const double *__restrict__ L,
                                                         int64_t ld, int64_t m, const double *__restrict__ omega,
-                                                        int count, float4 *__restrict__ a) {
+                                                        int count, float4 *__restrict__ a, int lower_tiles) {
     const int64_t pairs = m * m / 2;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < pairs; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t e = 2 * t, i = e % m, j = e / m;
         const int64_t e1 = e + 1, i1 = e1 % m, j1 = e1 / m;
+        if (lower_tiles && (i >> 7) < (j >> 7) && (i1 >> 7) < (j1 >> 7)) continue;
         const double r0 = R[i + j * ld], l0 = L[i + j * ld];
         const double r1 = R[i1 + j1 * ld], l1 = L[i1 + j1 * ld];
         for (int f = 0; f < count; ++f) {
@@ -1553,12 +1555,12 @@ fh_status lu_solve(const LuBatch<T> &b, T *xv, int nrhs, int nb, cudaStream_t s,
 
 template <class T>
 fh_status form_system(const double *Rm, const double *Lm, int64_t ld, int64_t m, const double *omega, int count, T *a,
-                      cudaStream_t s, fh_error_info *err) {
+                      cudaStream_t s, fh_error_info *err, bool lower_tiles) {
     if (m == 0) return FH_OK;
     if constexpr (sizeof(T) == 4) {
         if ((m * m) % 2 == 0 && (reinterpret_cast<uintptr_t>(a) & 15) == 0) {
-            form_pair_kernel<<<grid_for(m * m / 2, 256, 148 * 16), 256, 0, s>>>(Rm, Lm, ld, m, omega, count,
-                                                                             reinterpret_cast<float4 *>(a));
+            form_pair_kernel<<<grid_for(m * m / 2, 256, 148 * 16), 256, 0, s>>>(
+                Rm, Lm, ld, m, omega, count, reinterpret_cast<float4 *>(a), lower_tiles ? 1 : 0);
             FHB_CUDA(cudaGetLastError());
             return FH_OK;
         }
@@ -1640,9 +1642,9 @@ template fh_status lu_factor<float>(LuBatch<float> &, LuWork &, int, TrailingUpd
 template fh_status lu_solve<double>(const LuBatch<double> &, double *, int, int, cudaStream_t, fh_error_info *, int);
 template fh_status lu_solve<float>(const LuBatch<float> &, float *, int, int, cudaStream_t, fh_error_info *, int);
 template fh_status form_system<double>(const double *, const double *, int64_t, int64_t, const double *, int, double *,
-                                       cudaStream_t, fh_error_info *);
+                                       cudaStream_t, fh_error_info *, bool);
 template fh_status form_system<float>(const double *, const double *, int64_t, int64_t, const double *, int, float *,
-                                      cudaStream_t, fh_error_info *);
+                                      cudaStream_t, fh_error_info *, bool);
 template fh_status form_rhs<double>(const double *, const double *, int64_t, int64_t, int64_t, const double *, int,
                                     double *, cudaStream_t, fh_error_info *);
 template fh_status form_rhs<float>(const double *, const double *, int64_t, int64_t, int64_t, const double *, int,

@@ -173,10 +173,12 @@ fh_status lu_solve_inv(const LuBatch<float> &b, const void *linv, const void *ui
 fh_status trisolve_check(const SolveScratch &ss, cudaStream_t s, fh_error_info *err);
 
 // A_f = R + j w_f L for the top-left m x m block of R_m, L_m (ld = loops),
-// written as T complex into a (count x m x m).
+// written as T complex into a (count x m x m).  With lower_tiles (FP32, for
+// the two-level factorization without pivoting, which forms every U entry it
+// reads from L) the 128 x 128 tiles above the diagonal are not written.
 template <class T>
 fh_status form_system(const double *Rm, const double *Lm, int64_t ld, int64_t m, const double *omega, int count,
-                      T *a, cudaStream_t s, fh_error_info *err);
+                      T *a, cudaStream_t s, fh_error_info *err, bool lower_tiles = false);
 
 // Right-hand sides b_f = Z_ep (m x p) at each frequency, as T complex.
 template <class T>

@@ -806,10 +806,10 @@ fh_status gemm_tc_packed_run(const void *pack_a, const void *pack_b, float *C, i
     if (lower_from >= 0 && lower_from < cblocks) {
         // Lower-triangle form (symmetric trailing matrix, C rows and columns
         // on the same blocks): column blocks below lower_from in full, the
-        // rest only on and below the diagonal block; the same grouped order
-        // as the full schedule (row blocks fastest inside groups of
-        // kGroupRows), invalid tiles left out.  The caller forms every U
-        // entry it reads from L (U = D L^T), so no upper tile is read.
+        // rest only on and below the diagonal block (lower_from = 0: the
+        // lower triangle of tiles); the same grouped order as the full
+        // schedule (row blocks fastest inside groups of kGroupRows), the
+        // other tiles left out.
         std::vector<uint32_t> table;
         table.reserve((size_t)rblocks * cblocks);
         entries = 0.0;

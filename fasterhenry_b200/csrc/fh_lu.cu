@@ -1332,8 +1332,9 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             st = gemm_tc_panel_solve(b.a, m, count, K0, W, w.xpack, reinterpret_cast<const float *>(dvec), w.pack_a,
                                      w.pack_b, s, err);
             if (st) return st;
-            const int next = (int)((std::min<int64_t>(outer, n2) + 127) / 128);
-            st = gemm_tc_packed_run(w.pack_a, w.pack_b, at(E, E), m, mm, n2, n2, W, count, s, err, next);
+            // Only the tiles on and below the diagonal: every U entry is formed
+            // from L (steps inside each diagonal region, panel solve beyond).
+            st = gemm_tc_packed_run(w.pack_a, w.pack_b, at(E, E), m, mm, n2, n2, W, count, s, err, 0);
             if (st) return st;
             continue;
         }
@@ -1344,13 +1345,11 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             u12_from_l21_kernel<<<tg, dim3(32, 8), 0, s>>>(a, m, K0, W, E, m);
             FHB_CUDA(cudaGetLastError());
             prof_end(s, FH_PROF_TRSM, 0.0);
-            // Only the lower triangle of the trailing matrix is read from here
-            // on, besides the next super-panel's columns, which are updated in
-            // full (U12 of later super-panels, inside their diagonal blocks too,
-            // comes from L21).
-            const int next = (int)((std::min<int64_t>(outer, n2) + 127) / 128);
+            // Only the tiles on and below the diagonal of the trailing matrix
+            // are read from here on: every U entry of the later super-panels,
+            // inside their diagonal blocks too, is formed from L.
             st = gemm_tc_packed_update(at(E, K0), m, mm, at(K0, E), m, mm, at(E, E), m, mm, n2, n2, W, count,
-                                       w.pack_a, w.pack_b, s, err, next);
+                                       w.pack_a, w.pack_b, s, err, 0);
             if (st) return st;
             continue;
         }

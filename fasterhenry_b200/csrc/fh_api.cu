@@ -167,7 +167,7 @@ struct PBuf {
 enum PoolSlot {
     kSlotA, kSlotD32, kSlotR, kSlotRnorm, kSlotBnorm, kSlotDnorm, kSlotXnorm, kSlotPiv, kSlotSing, kSlotPv,
     kSlotPi, kSlotTk, kSlotCoop, kSlotLinv, kSlotUinv, kSlotSolve, kSlotPackA, kSlotPackB, kSlotOmega, kSlotX,
-    kSlotZ, kSlotXinv, kSlotXpack, kSlotTbuf, kSlotDvec
+    kSlotZ, kSlotXinv, kSlotXpack, kSlotTbuf, kSlotDvec, kSlotFlow
 };
 
 #define FHB_PALLOC(pool, buf, slot_id, count)                                                          \
@@ -356,13 +356,25 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     FHB_PALLOC(pool, linv_mem, kSlotLinv, (size_t)count * kNbFp32 * kNbFp32 * 2 * (outer ? nblk : 1));
     w.linv = linv_mem.p;
     SolveScratch ss;
-    PBuf<unsigned char> solve_mem;
+    FlowScratch fs;
+    PBuf<unsigned char> solve_mem, flow_mem;
     if (outer) {
         FHB_PALLOC(pool, uinv_mem, kSlotUinv, (size_t)count * kNbFp32 * kNbFp32 * 2 * nblk);
         w.uinv = uinv_mem.p;
+        // The two-level form has no interchanges: the dataflow solve (flags
+        // per 128-row block), or the barrier-based one when it does not fit.
+        int flow_group = 0;
+        size_t flow_bytes = 0;
+        e = flowsolve_plan(count * (int)p, m, &flow_group, &flow_bytes, err, s->share);
+        if (e) return e;
+        if (flow_group > 0) {
+            FHB_PALLOC(pool, flow_mem, kSlotFlow, flow_bytes);
+            FHB_CUDA(cudaMemsetAsync(flow_mem.p, 0, flow_bytes, st));
+            flowsolve_bind(flow_mem.p, count * (int)p, flow_group, m, fs);
+        }
         int per_group = 0;
         size_t solve_bytes = 0;
-        e = trisolve_plan(count * (int)p, m, &per_group, &solve_bytes, err, s->share);
+        if (flow_group == 0) e = trisolve_plan(count * (int)p, m, &per_group, &solve_bytes, err, s->share);
         if (e) return e;
         if (per_group > 0) {
             FHB_PALLOC(pool, solve_mem, kSlotSolve, solve_bytes);
@@ -420,7 +432,9 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     for (; it < kMaxIter; ++it) {
         e = convert_c64_to_c32(r.p, d32.p, count * vec, st, err);
         if (!e) {
-            if (ss.per_group > 0)
+            if (fs.per_group > 0)
+                e = lu_solve_flow(b, w.linv, w.uinv, d32.p, (int)p, fs, st, err);
+            else if (ss.per_group > 0)
                 e = lu_solve_inv(b, w.linv, w.uinv, d32.p, (int)p, kNbFp32, outer, ss, st, err);
             else
                 e = lu_solve<float>(b, d32.p, (int)p, kNbFp32, st, err, outer);
@@ -478,6 +492,10 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     }
     if (ss.per_group > 0) {
         e = trisolve_check(ss, st, err);
+        if (e) return e;
+    }
+    if (fs.per_group > 0) {
+        e = flowsolve_check(fs, st, err);
         if (e) return e;
     }
     cudaEventRecord(e2, st);

@@ -890,6 +890,25 @@ PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
 }
 }  // namespace
 
+fh_status encode_column_tiles(void *map, const float *a, int64_t m, int count, int box_rows, int box_cols,
+                              fh_error_info *err) {
+    // The batch as an m x (count m) array of 8-byte elements (complex FP32),
+    // column stride 8 m bytes; rows past m read as zeros.
+    PFN_cuTensorMapEncodeTiled encode = tensor_map_encoder();
+    if (!encode) return fail(err, FH_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)count * (cuuint64_t)m};
+    const cuuint64_t strides[1] = {(cuuint64_t)m * 8};
+    const cuuint32_t box[2] = {(cuuint32_t)box_rows, (cuuint32_t)box_cols};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult cr = encode(static_cast<CUtensorMap *>(map), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
+                               const_cast<float *>(a), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS)
+        return fail(err, FH_ERR_CUDA, "tensor map of the batch rejected (driver error " + std::to_string((int)cr) + ")");
+    return FH_OK;
+}
+
 bool panel_solve_supported(int64_t m) { return m % 2 == 0 && m * 8 < ((int64_t)1 << 40); }
 
 fh_status gemm_tc_panel_solve(float *a, int64_t m, int count, int64_t K0, int W, const void *xpack, const float *dvec,
@@ -905,20 +924,9 @@ fh_status gemm_tc_panel_solve(float *a, int64_t m, int count, int64_t K0, int W,
     int dev = 0;
     fh_status st = packed_init(&dev, err);
     if (st) return st;
-    // The batch as an m x (count m) array of 8-byte elements (complex FP32),
-    // column stride 8 m bytes; a box is 128 rows x 16 columns.
-    PFN_cuTensorMapEncodeTiled encode = tensor_map_encoder();
-    if (!encode) return fail(err, FH_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
     CUtensorMap rows_map;
-    const cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)count * (cuuint64_t)m};
-    const cuuint64_t strides[1] = {(cuuint64_t)m * 8};
-    const cuuint32_t box[2] = {(cuuint32_t)kTile, (cuuint32_t)kChunk};
-    const cuuint32_t estr[2] = {1, 1};
-    const CUresult cr = encode(&rows_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, a, dims, strides, box, estr,
-                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (cr != CUDA_SUCCESS)
-        return fail(err, FH_ERR_CUDA, "tensor map of the batch rejected (driver error " + std::to_string((int)cr) + ")");
+    st = encode_column_tiles(&rows_map, a, m, count, kTile, kChunk, err);
+    if (st) return st;
     PanelSolveArgs g;
     g.A = reinterpret_cast<float2 *>(a);
     g.m = m;

@@ -172,6 +172,29 @@ fh_status lu_solve_inv(const LuBatch<float> &b, const void *linv, const void *ui
                        int group, const SolveScratch &ss, cudaStream_t s, fh_error_info *err);
 fh_status trisolve_check(const SolveScratch &ss, cudaStream_t s, fh_error_info *err);
 
+// Tensor map (a CUtensorMap, 64-byte aligned, at map) of a batch of count
+// column-major m x m complex FP32 matrices seen as one m x (count m) array
+// of 8-byte elements, box box_rows x box_cols; m must be even.
+fh_status encode_column_tiles(void *map, const float *a, int64_t m, int count, int box_rows, int box_cols,
+                              fh_error_info *err);
+
+// Dataflow form of the same solves for factors without interchanges
+// (fh_flowsolve.cu): a flag per 128-row block instead of barriers, the
+// factor tiles loaded by TMA.  The scratch (flowsolve_plan's bytes) must be
+// zeroed once per batch; per_group = 0 means the batch does not fit one
+// launch or the order is odd (the barrier-based solve is used instead).
+struct FlowScratch {
+    unsigned *flags = nullptr;  // [group][2][nblk]
+    int *error = nullptr;
+    int groups = 0, per_group = 0, nblk = 0;
+    unsigned epoch = 0;  // the flag value of the last launch
+};
+fh_status flowsolve_plan(int groups, int64_t m, int *per_group, size_t *bytes, fh_error_info *err, int share = 1);
+void flowsolve_bind(void *mem, int groups, int per_group, int64_t m, FlowScratch &fs);
+fh_status lu_solve_flow(const LuBatch<float> &b, const void *linv, const void *uinv, float *x, int nrhs,
+                        FlowScratch &fs, cudaStream_t s, fh_error_info *err);
+fh_status flowsolve_check(const FlowScratch &fs, cudaStream_t s, fh_error_info *err);
+
 // A_f = R + j w_f L for the top-left m x m block of R_m, L_m (ld = loops),
 // written as T complex into a (count x m x m).  With lower_tiles (FP32, for
 // the two-level factorization without pivoting, which forms every U entry it

@@ -398,7 +398,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
         FHB_PALLOC(pool, xinv, kSlotXinv, (size_t)count * outer * outer * 2);
         FHB_PALLOC(pool, xpack, kSlotXpack, packed_operand_bytes(outer, outer, count));
         FHB_PALLOC(pool, tbuf, kSlotTbuf, (size_t)count * kNbFp32 * (outer - kNbFp32) * 2);
-        FHB_PALLOC(pool, dvec, kSlotDvec, (size_t)count * outer * 2);
+        FHB_PALLOC(pool, dvec, kSlotDvec, (size_t)count * outer * 4);
         w.xinv = xinv.p;
         w.xpack = xpack.p;
         w.tbuf = tbuf.p;

@@ -450,9 +450,10 @@ __global__ void __launch_bounds__(kThreads, 1) packed_update_kernel(PackedArgs g
 // and with L21 everything else the super-panel step needs from it: the matrix
 // is complex symmetric and factored without interchanges, so U = diag(U) L^T
 // and U12 = diag(d) L21^T (d_k = U_kk) is written over the rows [K0, E) of the
-// trailing columns; and the operands of the deep update are written packed
-// (A = L21 by 128-row blocks, B = U12 by 128-column blocks -- the same tiles
-// as A's, each k scaled by d_k).
+// trailing columns; and the one operand of the deep update is written
+// packed: P = L21 diag(s) by 128-row blocks, s_k a square root of d_k, so
+// that L21 U12 = P P^T and the update takes P's tiles for both A (row
+// blocks) and B (column blocks).
 //
 // A work item is one 128-row block of one matrix; its output column blocks
 // are formed from the last to the first, block j from the k chunks
@@ -473,7 +474,7 @@ __global__ void __launch_bounds__(kThreads, 1) packed_update_kernel(PackedArgs g
 //   warp 12, one lane  TMEM allocation and the MMA issuer: 12 tcgen05.mma per
 //                      chunk into one of two TMEM accumulators;
 //   warps 4..11        epilogue: tcgen05.ld, then L21 and U12 in FP32 and the
-//                      two packed tiles.
+//                      packed tile of P.
 // A stage is reused once the MMAs that read it have completed (`empty`):
 // by then the splitters have consumed its raw tile too.  No cluster launch
 // and no multicast.  Every wait is bounded; a wait that runs out sets the
@@ -494,7 +495,8 @@ struct PanelSolveArgs {
     int W, nbw, nch;       // super-panel width, its 128-blocks and 16-chunks
     const uint8_t *Xp;     // X packed: [f][column block][chunk] 16 KB
     const float2 *dvec;    // d_k = U_kk of the super-panel: [f][W]
-    uint8_t *Pa, *Pb;      // packed outputs: [f][row block][chunk] 16 KB
+    const float2 *svec;    // s_k, s_k^2 = d_k: [f][W]
+    uint8_t *P;            // packed output L21 diag(s): [f][row block][chunk] 16 KB
     int rblocks;           // 128-row blocks of [E, m)
     long long items;       // count * rblocks
 };
@@ -730,11 +732,15 @@ __global__ void __launch_bounds__(kPsThreads, 1)
                         }
                         __syncwarp();
                     }
+                    // P = L21 diag(s): one operand for both sides of C -= P P^T
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) {
+                        const float2 sq = __ldg(g.svec + (int64_t)f * g.W + kc + jj);
+                        u[jj] = make_float2(sq.x * l[jj].x - sq.y * l[jj].y, sq.x * l[jj].y + sq.y * l[jj].x);
+                    }
                     const int64_t tile = ((int64_t)f * g.rblocks + rb) * g.nch + kc / kChunk;
-                    split_store8(l, g.Pa + tile * kOpBytes, tile_off(tr, 0));
-                    split_store8(l + 8, g.Pa + tile * kOpBytes, tile_off(tr, 1));
-                    split_store8(u, g.Pb + tile * kOpBytes, tile_off(tr, 0));
-                    split_store8(u + 8, g.Pb + tile * kOpBytes, tile_off(tr, 1));
+                    split_store8(u, g.P + tile * kOpBytes, tile_off(tr, 0));
+                    split_store8(u + 8, g.P + tile * kOpBytes, tile_off(tr, 1));
                 }
             }
         }
@@ -912,14 +918,14 @@ fh_status encode_column_tiles(void *map, const float *a, int64_t m, int count, i
 bool panel_solve_supported(int64_t m) { return m % 2 == 0 && m * 8 < ((int64_t)1 << 40); }
 
 fh_status gemm_tc_panel_solve(float *a, int64_t m, int count, int64_t K0, int W, const void *xpack, const float *dvec,
-                              void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err) {
+                              const float *svec, void *pack, cudaStream_t s, fh_error_info *err) {
     const int64_t E = K0 + W;
     if (W <= 0 || W % kTile || W > 4 * kTile || K0 < 0 || K0 % 2 || E > m)
         return fail(err, FH_ERR_INVALID_ARGUMENT, "panel solve needs a super-panel of 128-column blocks (at most 4)");
     if (!panel_solve_supported(m) || (int64_t)count * m > INT32_MAX)
         return fail(err, FH_ERR_INVALID_ARGUMENT, "panel solve needs an even order (16-byte column stride)");
     if (E == m || count <= 0) return FH_OK;
-    if (!xpack || !dvec || !pack_a || !pack_b)
+    if (!xpack || !dvec || !svec || !pack)
         return fail(err, FH_ERR_INVALID_ARGUMENT, "panel solve needs the packed inverse, the diagonal and outputs");
     int dev = 0;
     fh_status st = packed_init(&dev, err);
@@ -938,8 +944,8 @@ fh_status gemm_tc_panel_solve(float *a, int64_t m, int count, int64_t K0, int W,
     g.nch = W / kChunk;
     g.Xp = reinterpret_cast<const uint8_t *>(xpack);
     g.dvec = reinterpret_cast<const float2 *>(dvec);
-    g.Pa = reinterpret_cast<uint8_t *>(pack_a);
-    g.Pb = reinterpret_cast<uint8_t *>(pack_b);
+    g.svec = reinterpret_cast<const float2 *>(svec);
+    g.P = reinterpret_cast<uint8_t *>(pack);
     g.rblocks = (int)((m - E + kTile - 1) / kTile);
     g.items = (long long)count * g.rblocks;
     const int grid = (int)std::min<long long>(g.items, (long long)std::max(1, g_sms[dev]));

@@ -629,10 +629,21 @@ __device__ __forceinline__ void diag_uinv_segment(Cf (&v)[4][8], int nb, int lan
     }
 }
 
-// LU of the block in place (and the diagonal of U into dv); one CTA per matrix.
+// Principal square root of z, by the cancellation-free pair of formulas
+// (t = sqrt((|z| + |Re z|) / 2), the other part Im z / 2t), in FP64.
+__device__ __forceinline__ Cf csqrt_principal(Cf z) {
+    const double a = z.re, b = z.im, r = hypot(a, b);
+    if (r == 0.0) return Cf{0.f, 0.f};
+    const double t = sqrt(0.5 * (r + fabs(a)));
+    if (a >= 0.0) return Cf{(float)t, (float)(b / (2.0 * t))};
+    return Cf{(float)(fabs(b) / (2.0 * t)), (float)copysign(t, b)};
+}
+
+// LU of the block in place (the diagonal of U into dv and its principal
+// square roots into sv, when given); one CTA per matrix.
 __global__ void __launch_bounds__(kDiagThreads, 1)
     diag_lu_kernel(Cx<float> *__restrict__ a, int64_t m, int64_t k0, int nb, Cx<float> *__restrict__ dv,
-                   int64_t dstride) {
+                   Cx<float> *__restrict__ sv, int64_t dstride) {
     __shared__ __align__(16) Cf bufs[2 * 128 + 2 * 128 + 2];
     DiagSmem sm;
     sm.S = nullptr;
@@ -668,7 +679,10 @@ __global__ void __launch_bounds__(kDiagThreads, 1)
             const int r = lane + 32 * i, c = warp + 16 * j;
             if (r < nb && c < nb) {
                 A[r + (int64_t)c * m] = v[i][j];
-                if (dv && r == c) dv[(int64_t)blockIdx.x * dstride + r] = v[i][j];
+                if (dv && r == c) {
+                    dv[(int64_t)blockIdx.x * dstride + r] = v[i][j];
+                    sv[(int64_t)blockIdx.x * dstride + r] = csqrt_principal(v[i][j]);
+                }
             }
         }
 }
@@ -1230,6 +1244,7 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
     const bool fused = nopivot && w.xinv && w.xpack && w.tbuf && w.dvec && nb == 128 && outer % nb == 0 &&
                        panel_solve_supported(m) && (int64_t)count * m <= INT32_MAX;
     C *xinv = reinterpret_cast<C *>(w.xinv), *dvec = reinterpret_cast<C *>(w.dvec);
+    C *svec = fused ? dvec + (int64_t)count * outer : nullptr;
     // X's blocks below its diagonal are read as zeros and never written.
     if (fused) FHB_CUDA(cudaMemsetAsync(w.xinv, 0, sizeof(C) * (size_t)count * outer * outer, s));
     for (int64_t K0 = 0; K0 < m; K0 += outer) {
@@ -1248,7 +1263,8 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
                 // (with the fused pass: U^-1 also into X's diagonal block, and
                 // U's diagonal into dvec).
                 const int64_t o = j0 - K0;
-                diag_lu_kernel<<<(unsigned)count, kDiagThreads, 0, s>>>(a, m, j0, wj, below ? dvec + o : nullptr, W);
+                diag_lu_kernel<<<(unsigned)count, kDiagThreads, 0, s>>>(a, m, j0, wj, below ? dvec + o : nullptr,
+                                                                       below ? svec + o : nullptr, W);
                 diag_inv_kernel<<<dim3((unsigned)count, 2), kDiagThreads, sizeof(C) * ((size_t)wj * wj + kDiagSmemExtra),
                                   s>>>(a, m, j0, wj, linv, slot(w.uinv, j0), mstride, below ? xinv + o + o * W : nullptr,
                                        W, (int64_t)W * W);
@@ -1328,13 +1344,14 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             if (!st) st = gemm_tc_pack_b(reinterpret_cast<float *>(xinv), W, ww, W, W, count, w.xpack, s, err);
             prof_end(s, FH_PROF_TRSM, 0.0);
             if (st) return st;
-            // L21 = A21 X for every row below, U12 = D L21^T, packed operands.
-            st = gemm_tc_panel_solve(b.a, m, count, K0, W, w.xpack, reinterpret_cast<const float *>(dvec), w.pack_a,
-                                     w.pack_b, s, err);
+            // L21 = A21 X for every row below, U12 = D L21^T, P = L21 S packed.
+            st = gemm_tc_panel_solve(b.a, m, count, K0, W, w.xpack, reinterpret_cast<const float *>(dvec),
+                                     reinterpret_cast<const float *>(svec), w.pack_a, s, err);
             if (st) return st;
-            // Only the tiles on and below the diagonal: every U entry is formed
-            // from L (steps inside each diagonal region, panel solve beyond).
-            st = gemm_tc_packed_run(w.pack_a, w.pack_b, at(E, E), m, mm, n2, n2, W, count, s, err, 0);
+            // C -= P P^T, only the tiles on and below the diagonal: every U
+            // entry is formed from L (steps inside each diagonal region, panel
+            // solve beyond).
+            st = gemm_tc_packed_run(w.pack_a, w.pack_a, at(E, E), m, mm, n2, n2, W, count, s, err, 0);
             if (st) return st;
             continue;
         }

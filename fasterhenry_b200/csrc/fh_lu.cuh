@@ -71,8 +71,9 @@ struct LuWork {
     //         diagonal block D (column-major, leading dimension W);
     //   xpack packed_operand_bytes(W, W, count): X packed as a B operand;
     //   tbuf  count * nb * (W - nb) complex FP32: one block row product;
-    //   dvec  count * W complex FP32: the diagonal of U_D.
-    // With all four set, L21, U12 and the packed operands of the deep update
+    //   dvec  2 * count * W complex FP32: the diagonal d of U_D, then its
+    //         principal square roots s (matrix f's at count * W + f * W).
+    // With all four set, L21, U12 and the packed operand of the deep update
     // come from one tensor-core pass over the rows below (gemm_tc_panel_solve).
     void *xinv = nullptr;
     void *xpack = nullptr;
@@ -131,13 +132,14 @@ fh_status gemm_tc_pack_b(const float *B, int64_t ldb, int64_t sB, int64_t N, int
                          cudaStream_t s, fh_error_info *err);
 // For the factored super-panel [K0, K0 + W) of a complex symmetric batch
 // factored without interchanges and the rows below it: L21 = A21 X in place
-// (X = U_D^{-1}, xpack from gemm_tc_pack_b), U12 = diag(dvec) L21^T over the
-// super-panel's rows of the trailing columns, and both operands of the deep
-// update packed into pack_a / pack_b.  The rows are read by 2D tensor copies,
-// so the order m must be even (a column stride of 16-byte multiples).
+// (X = U_D^{-1}, xpack from gemm_tc_pack_b), U12 = diag(d) L21^T over the
+// super-panel's rows of the trailing columns, and P = L21 diag(s) packed into
+// pack (s_k^2 = d_k): the deep update C -= L21 U12 = P P^T takes P as both
+// its A and its B operand.  The rows are read by 2D tensor copies, so the
+// order m must be even (a column stride of 16-byte multiples).
 bool panel_solve_supported(int64_t m);
 fh_status gemm_tc_panel_solve(float *a, int64_t m, int count, int64_t K0, int W, const void *xpack, const float *dvec,
-                              void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err);
+                              const float *svec, void *pack, cudaStream_t s, fh_error_info *err);
 fh_status gemm_tc_packed_check(fh_error_info *err);
 // One SIMT trailing update (FP32 or FP64), for tests.
 template <class T>

@@ -372,6 +372,9 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
             FHB_CUDA(cudaMemsetAsync(flow_mem.p, 0, flow_bytes, st));
             flowsolve_bind(flow_mem.p, count * (int)p, flow_group, m, fs);
         }
+        // the dataflow solve reads U_ij as D_i L_ji^T: no U12 beyond the
+        // diagonal regions is written for it
+        w.upper = flow_group == 0;
         int per_group = 0;
         size_t solve_bytes = 0;
         if (flow_group == 0) e = trisolve_plan(count * (int)p, m, &per_group, &solve_bytes, err, s->share);
@@ -387,10 +390,14 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     if (outer) {
         const size_t pb = packed_operand_bytes(m - outer, outer, count);
         FHB_PALLOC(pool, pack_a, kSlotPackA, pb);
-        FHB_PALLOC(pool, pack_b, kSlotPackB, pb);
         w.outer = outer;
         w.pack_a = pack_a.p;
-        w.pack_b = pack_b.p;
+        // the rows-below pass packs one operand for both sides of the update;
+        // the separate B operand is for orders it does not take
+        if (!(panel_solve_supported(m) && (int64_t)count * m <= INT32_MAX)) {
+            FHB_PALLOC(pool, pack_b, kSlotPackB, pb);
+            w.pack_b = pack_b.p;
+        }
         // Z_ee = R_ee + jw L_ee with R_ee, L_ee symmetric positive definite:
         // the FP32 factors go without pivoting (stable for this class; the
         // FP64 residual refinement and its FP64 fallback decide the result).

@@ -178,9 +178,12 @@ struct TileCursor {
 __device__ __forceinline__ void issue_tile(const FlowArgs &g, const CUtensorMap *map, int f, const TileCursor &t,
                                            uint32_t dst, uint32_t bar) {
     if (t.s < t.nsrc(g.nblk)) {
+        // forward: L_ij (rows of block i, columns of block j); backward:
+        // L_ji (rows of block j, columns of block i), read transposed
         const int j = t.pass == 0 ? t.s : g.nblk - 1 - t.s;
+        const int rb = t.pass == 0 ? t.i : j, cb = t.pass == 0 ? j : t.i;
         mbar_expect_tx(bar, kFlowTileBytes);
-        tensor_load_2d(dst, map, t.i * kNb, (int)((int64_t)f * g.m + (int64_t)j * kNb + t.q * kFlowTileCols), bar);
+        tensor_load_2d(dst, map, rb * kNb, (int)((int64_t)f * g.m + (int64_t)cb * kNb + t.q * kFlowTileCols), bar);
     } else {
         const int wi = (int)min((int64_t)kNb, g.m - (int64_t)t.i * kNb), c0 = t.q * kFlowTileCols;
         const uint32_t bytes = (uint32_t)max(0, min(kFlowTileCols, wi - c0)) * wi * 8;
@@ -202,8 +205,9 @@ __global__ void __launch_bounds__(kFlowThreads) flowsolve_kernel(FlowArgs g, con
     const int64_t m = g.m;
     Cx<float> *X = g.x + (int64_t)grp * m;
     unsigned *ff = g.flags + (size_t)grp * 2 * g.nblk, *fb = ff + g.nblk;
-    const int tid = threadIdx.x, r = tid % kNb, h = tid / kNb;
-    __shared__ Cx<float> vs[kNb], part[kNb];
+    const int tid = threadIdx.x, r = tid % kNb, h = tid / kNb, warp = tid >> 5, lane = tid & 31;
+    const Cx<float> *Af = g.a + (int64_t)f * m * m;
+    __shared__ __align__(16) Cx<float> vs[kNb], part[kNb];
 
     if (tid == 0) {
         for (int k = 0; k < kFlowStages; ++k) mbar_init(smem_addr(&full[k]), 1);
@@ -252,31 +256,107 @@ __global__ void __launch_bounds__(kFlowThreads) flowsolve_kernel(FlowArgs g, con
         return true;
     };
 
-    // One output block: b_i - sum_j F_ij x_j over its sources as their flags
-    // come, then the stored inverse of the diagonal block, then publication.
+    // Backward source tile q (L_ji, 128 rows of block j x 16 columns of block
+    // i): t[q][c] += sum_r L_ji(r, q 16 + 2 warp + c) x_j(r) over the lane's
+    // rows r = 4 lane .. 4 lane + 3, kept per lane until the block's sources
+    // are done (U_ij = D_i L_ji^T, so U is never read).
+    float bt[kFlowTilesPerBlock][2][2];
+    auto step_t = [&](int q, const Cx<float> (&xr)[4]) -> bool {
+        const int slot = (int)(t_comp % kFlowStages);
+        const bool ok = mbar_wait(smem_addr(&full[slot]), (uint32_t)((t_comp / kFlowStages) & 1));
+        if (ok) {
+            const Cx<float> *tile = ring + slot * kFlowTileElems;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const float4 *col = reinterpret_cast<const float4 *>(tile + (2 * warp + c) * kNb + 4 * lane);
+                const float4 p0 = col[0], p1 = col[1];  // rows 4 lane, +1 | +2, +3
+                bt[q][c][0] += p0.x * xr[0].re - p0.y * xr[0].im + p0.z * xr[1].re - p0.w * xr[1].im +
+                               p1.x * xr[2].re - p1.y * xr[2].im + p1.z * xr[3].re - p1.w * xr[3].im;
+                bt[q][c][1] += p0.x * xr[0].im + p0.y * xr[0].re + p0.z * xr[1].im + p0.w * xr[1].re +
+                               p1.x * xr[2].im + p1.y * xr[2].re + p1.z * xr[3].im + p1.w * xr[3].re;
+            }
+        } else {
+            atomicExch(g.error, 1);
+        }
+        if (!__syncthreads_and(ok)) return false;
+        ++t_comp;
+        issue_next();
+        return true;
+    };
+
+    // One output block: its sources as their flags come, then the stored
+    // inverse of the diagonal block, then publication.  Forward
+    // y_i = Linv_i (b_i - sum_j L_ij y_j); backward
+    // x_i = Uinv_i (y_i - D_i sum_j L_ji^T x_j), D_i the diagonal of U.
     auto block = [&](int pass, int i) -> bool {
         const int64_t i0 = (int64_t)i * kNb;
         const int wi = (int)min((int64_t)kNb, m - i0);
         unsigned *flags = pass == 0 ? ff : fb;
-        Cx<float> acc{0.f, 0.f};
-        if (h == 0 && r < wi) acc = ldcg(X + i0 + r);
+        Cx<float> acc{0.f, 0.f}, dii{0.f, 0.f};
+        if (h == 0 && r < wi) {
+            acc = ldcg(X + i0 + r);
+            if (pass == 1) dii = Af[(i0 + r) * (m + 1)];
+        }
         const int nsrc = pass == 0 ? i : g.nblk - 1 - i;
+        if (pass == 1) {
+#pragma unroll
+            for (int q = 0; q < kFlowTilesPerBlock; ++q)
+                bt[q][0][0] = bt[q][0][1] = bt[q][1][0] = bt[q][1][1] = 0.f;
+        }
         for (int s = 0; s < nsrc; ++s) {
             const int j = pass == 0 ? s : g.nblk - 1 - s;
             if (!flow_wait(flags + j, g.epoch, g.error)) return false;
             const int64_t j0 = (int64_t)j * kNb;
             const int wj = (int)min((int64_t)kNb, m - j0);
-            if (tid < kNb) {  // negated: the steps accumulate -F_ij x_j
+            if (tid < kNb) {  // forward: negated, the steps accumulate -L_ij y_j
                 const Cx<float> x = tid < wj ? ldcg(X + j0 + tid) : Cx<float>{0.f, 0.f};
-                vs[tid] = Cx<float>{-x.re, -x.im};
+                vs[tid] = pass == 0 ? Cx<float>{-x.re, -x.im} : x;
             }
             __syncthreads();
-            for (int q = 0; q < kFlowTilesPerBlock; ++q)
-                if (!step(vs + q * kFlowTileCols, kNb, wj - q * kFlowTileCols, acc)) return false;
+            if (pass == 0) {
+                for (int q = 0; q < kFlowTilesPerBlock; ++q)
+                    if (!step(vs + q * kFlowTileCols, kNb, wj - q * kFlowTileCols, acc)) return false;
+            } else {
+                Cx<float> xr[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) xr[k] = vs[4 * lane + k];
+#pragma unroll
+                for (int q = 0; q < kFlowTilesPerBlock; ++q)
+                    if (!step_t(q, xr)) return false;
+            }
         }
-        if (h == 1) part[r] = acc;
+        if (pass == 0) {
+            if (h == 1) part[r] = acc;
+        } else {
+            // Sum bt over the warp's lanes: each halving exchanges half of the
+            // remaining values, so lane l ends with the total of value l,
+            // which is part of column q 16 + 2 warp + c (l = 4 q + 2 c + re/im).
+            float v[32];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) v[k] = bt[k >> 2][(k >> 1) & 1][k & 1];
+#pragma unroll
+            for (int off = 16; off >= 1; off >>= 1) {
+                const bool hi = (lane & off) != 0;
+#pragma unroll
+                for (int k = 0; k < off; ++k) {
+                    const float send = hi ? v[k] : v[k + off], keep = hi ? v[k + off] : v[k];
+                    v[k] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+                }
+            }
+            const int q = lane >> 2, c = (lane >> 1) & 1;
+            reinterpret_cast<float *>(part)[(q * kFlowTileCols + 2 * warp + c) * 2 + (lane & 1)] = v[0];
+        }
         __syncthreads();
-        if (h == 0) vs[r] = r < wi ? Cx<float>{acc.re + part[r].re, acc.im + part[r].im} : Cx<float>{0.f, 0.f};
+        if (h == 0) {
+            Cx<float> y{0.f, 0.f};
+            if (r < wi) {
+                const Cx<float> t = part[r];
+                y = pass == 0 ? Cx<float>{acc.re + t.re, acc.im + t.im}
+                              : Cx<float>{acc.re - (dii.re * t.re - dii.im * t.im),
+                                          acc.im - (dii.re * t.im + dii.im * t.re)};
+            }
+            vs[r] = y;
+        }
         __syncthreads();
         Cx<float> out{0.f, 0.f};
         for (int q = 0; q < kFlowTilesPerBlock; ++q)

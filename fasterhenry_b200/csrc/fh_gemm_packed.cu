@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(kThreads, 1) packed_update_kernel(PackedArgs g
 // and with L21 everything else the super-panel step needs from it: the matrix
 // is complex symmetric and factored without interchanges, so U = diag(U) L^T
 // and U12 = diag(d) L21^T (d_k = U_kk) is written over the rows [K0, E) of the
-// trailing columns; and the one operand of the deep update is written
+// trailing columns (unless no solve reads it); and the one operand of the deep update is written
 // packed: P = L21 diag(s) by 128-row blocks, s_k a square root of d_k, so
 // that L21 U12 = P P^T and the update takes P's tiles for both A (row
 // blocks) and B (column blocks).
@@ -496,6 +496,7 @@ struct PanelSolveArgs {
     const uint8_t *Xp;     // X packed: [f][column block][chunk] 16 KB
     const float2 *dvec;    // d_k = U_kk of the super-panel: [f][W]
     const float2 *svec;    // s_k, s_k^2 = d_k: [f][W]
+    int write_u12;         // 0: U12 is not written (no solve reads it)
     uint8_t *P;            // packed output L21 diag(s): [f][row block][chunk] 16 KB
     int rblocks;           // 128-row blocks of [E, m)
     long long items;       // count * rblocks
@@ -713,7 +714,7 @@ __global__ void __launch_bounds__(kPsThreads, 1)
 #pragma unroll
                         for (int jj = 0; jj < 16; ++jj) pl[(int64_t)jj * g.m] = l[jj];
                     }
-                    {
+                    if (g.write_u12) {
                         // U12: the thread's 16 entries lie down column `row`; the
                         // warp's tile goes through shared memory (column jj of row
                         // r at r * 16 + (jj ^ (r % 16))) so that each store covers
@@ -918,7 +919,7 @@ fh_status encode_column_tiles(void *map, const float *a, int64_t m, int count, i
 bool panel_solve_supported(int64_t m) { return m % 2 == 0 && m * 8 < ((int64_t)1 << 40); }
 
 fh_status gemm_tc_panel_solve(float *a, int64_t m, int count, int64_t K0, int W, const void *xpack, const float *dvec,
-                              const float *svec, void *pack, cudaStream_t s, fh_error_info *err) {
+                              const float *svec, void *pack, bool write_u12, cudaStream_t s, fh_error_info *err) {
     const int64_t E = K0 + W;
     if (W <= 0 || W % kTile || W > 4 * kTile || K0 < 0 || K0 % 2 || E > m)
         return fail(err, FH_ERR_INVALID_ARGUMENT, "panel solve needs a super-panel of 128-column blocks (at most 4)");
@@ -945,6 +946,7 @@ fh_status gemm_tc_panel_solve(float *a, int64_t m, int count, int64_t K0, int W,
     g.Xp = reinterpret_cast<const uint8_t *>(xpack);
     g.dvec = reinterpret_cast<const float2 *>(dvec);
     g.svec = reinterpret_cast<const float2 *>(svec);
+    g.write_u12 = write_u12 ? 1 : 0;
     g.P = reinterpret_cast<uint8_t *>(pack);
     g.rblocks = (int)((m - E + kTile - 1) / kTile);
     g.items = (long long)count * g.rblocks;

@@ -1209,7 +1209,7 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
     const int64_t m = b.m, mm = m * m;
     const int count = b.count;
     const int outer = w.outer;
-    if (nb % 16 || nb > 128 || outer % nb || !w.coop || !w.linv || !w.pack_a || !w.pack_b)
+    if (nb % 16 || nb > 128 || outer % nb || !w.coop || !w.linv || !w.pack_a)
         return fail(err, FH_ERR_INVALID_ARGUMENT, "two-level factorization needs nb | outer, nb <= 128 and scratch");
     const size_t inv_smem = sizeof(C) * (34 * (size_t)nb);
     const dim3 inv_grid((unsigned)count, (unsigned)((nb + 31) / 32));
@@ -1243,6 +1243,9 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
     // the per-block steps then stop at the super-panel's last row.
     const bool fused = nopivot && w.xinv && w.xpack && w.tbuf && w.dvec && nb == 128 && outer % nb == 0 &&
                        panel_solve_supported(m) && (int64_t)count * m <= INT32_MAX;
+    // the fused pass packs one operand for both sides; otherwise B has its own
+    if (!fused && !w.pack_b)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "two-level factorization needs a packed B operand scratch");
     C *xinv = reinterpret_cast<C *>(w.xinv), *dvec = reinterpret_cast<C *>(w.dvec);
     C *svec = fused ? dvec + (int64_t)count * outer : nullptr;
     // X's blocks below its diagonal are read as zeros and never written.
@@ -1346,7 +1349,7 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             if (st) return st;
             // L21 = A21 X for every row below, U12 = D L21^T, P = L21 S packed.
             st = gemm_tc_panel_solve(b.a, m, count, K0, W, w.xpack, reinterpret_cast<const float *>(dvec),
-                                     reinterpret_cast<const float *>(svec), w.pack_a, s, err);
+                                     reinterpret_cast<const float *>(svec), w.pack_a, w.upper, s, err);
             if (st) return st;
             // C -= P P^T, only the tiles on and below the diagonal: every U
             // entry is formed from L (steps inside each diagonal region, panel

@@ -65,6 +65,10 @@ struct LuWork {
     // in shared memory and L21 = A21 U11^-1 formed on the tensor cores;
     // pivots are the identity.
     bool nopivot = false;
+    // With the no-pivot form: whether U12 beyond each super-panel's diagonal
+    // region is written in FP32.  A solve that takes U_ij = D_i L_ji^T
+    // (lu_solve_flow) reads no U entry outside the diagonal regions.
+    bool upper = true;
     // Scratch of the factorization without pivoting, for the rows below each
     // super-panel (one super-panel at a time; outer = W columns):
     //   xinv  count * W * W complex FP32: X = U_D^{-1} of the super-panel's
@@ -133,13 +137,13 @@ fh_status gemm_tc_pack_b(const float *B, int64_t ldb, int64_t sB, int64_t N, int
 // For the factored super-panel [K0, K0 + W) of a complex symmetric batch
 // factored without interchanges and the rows below it: L21 = A21 X in place
 // (X = U_D^{-1}, xpack from gemm_tc_pack_b), U12 = diag(d) L21^T over the
-// super-panel's rows of the trailing columns, and P = L21 diag(s) packed into
+// super-panel's rows of the trailing columns (if write_u12), and P = L21 diag(s) packed into
 // pack (s_k^2 = d_k): the deep update C -= L21 U12 = P P^T takes P as both
 // its A and its B operand.  The rows are read by 2D tensor copies, so the
 // order m must be even (a column stride of 16-byte multiples).
 bool panel_solve_supported(int64_t m);
 fh_status gemm_tc_panel_solve(float *a, int64_t m, int count, int64_t K0, int W, const void *xpack, const float *dvec,
-                              const float *svec, void *pack, cudaStream_t s, fh_error_info *err);
+                              const float *svec, void *pack, bool write_u12, cudaStream_t s, fh_error_info *err);
 fh_status gemm_tc_packed_check(fh_error_info *err);
 // One SIMT trailing update (FP32 or FP64), for tests.
 template <class T>

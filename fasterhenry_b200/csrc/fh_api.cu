@@ -167,7 +167,7 @@ struct PBuf {
 enum PoolSlot {
     kSlotA, kSlotD32, kSlotR, kSlotRnorm, kSlotBnorm, kSlotDnorm, kSlotXnorm, kSlotPiv, kSlotSing, kSlotPv,
     kSlotPi, kSlotTk, kSlotCoop, kSlotLinv, kSlotUinv, kSlotSolve, kSlotPackA, kSlotPackB, kSlotOmega, kSlotX,
-    kSlotZ, kSlotXinv, kSlotXpack, kSlotTbuf, kSlotDvec, kSlotFlow
+    kSlotZ, kSlotXinv, kSlotXpack, kSlotTbuf, kSlotDvec, kSlotFlow, kSlotResPart
 };
 
 #define FHB_PALLOC(pool, buf, slot_id, count)                                                          \
@@ -431,6 +431,8 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
         if (!e) e = gemm_tc_packed_check(err);
         if (e) return e;
     }
+    PBuf<unsigned char> res_part;
+    if (const size_t rb = residual_scratch_bytes(m, p, count)) FHB_PALLOC(pool, res_part, kSlotResPart, rb);
     std::vector<double> hb(count), hd(count), hx(count), hr(count), prev(count, INFINITY);
     std::vector<int> done(count, 0), grow(count, 0);
     FHB_CUDA(cudaMemcpyAsync(hb.data(), bnorm.p, 8 * count, cudaMemcpyDeviceToHost, st));
@@ -447,7 +449,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
                 e = lu_solve<float>(b, d32.p, (int)p, kNbFp32, st, err, outer);
         }
         if (!e) e = add_c32_to_c64(d_x, d32.p, count * vec, st, err);
-        if (!e) e = residual_fp64(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, r.p, rnorm.p, st, err);
+        if (!e) e = residual_fp64(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, r.p, rnorm.p, st, err, res_part.p);
         if (e) return e;
         // correction and solution norms (max-abs) for the stopping rule
         e = max_abs_per_matrix_f32(d32.p, 2 * vec, count, dnorm.p, st, err);

@@ -17,6 +17,7 @@
 //     forward substitution applies each panel's interchanges to the
 //     right-hand side just before that panel's L columns are used, which is
 //     the same elimination order.
+#include <algorithm>
 #include <cfloat>
 #include <climits>
 #include <cstdio>
@@ -1025,13 +1026,18 @@ __global__ void rhs_kernel(const double *__restrict__ R, const double *__restric
 // 32 rows x 32 columns g, k in stages of 16 staged in shared memory (double
 // buffered, the next stage's loads in flight during the current one), thread
 // tile 4 rows x 2 columns for both R and L.  Each accumulator sums over k in
-// increasing order.
-constexpr int kResRows = 32, kResCols = 32, kResK = 16, kResThreads = 128;
+// increasing order.  With `part`, the k stages are split into gridDim.z
+// contiguous ranges (CTA z takes range z) and each CTA writes its sums
+// (R x re, im, L x re, im) to part[(z G + g) m + row]; residual_finish_kernel
+// then adds the ranges in order, so the result does not depend on the
+// schedule.  The split keeps every SM busy when the row tiles alone are few
+// or uneven across the SMs.
+constexpr int kResRows = 32, kResCols = 32, kResK = 16, kResThreads = 128, kResMaxSplits = 16;
 __global__ void __launch_bounds__(kResThreads) residual_kernel(const double *__restrict__ R,
                                                                const double *__restrict__ L, int64_t ld, int64_t m,
                                                                int64_t p, const double *__restrict__ omega, int count,
                                                                const Cx<double> *__restrict__ x,
-                                                               Cx<double> *__restrict__ r) {
+                                                               Cx<double> *__restrict__ r, double4 *__restrict__ part) {
     __shared__ double Rs[2][kResK][kResRows], Ls[2][kResK][kResRows];
     __shared__ Cx<double> Xs[2][kResK][kResCols + 1];  // padded: the stores run down k
     const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
@@ -1067,13 +1073,14 @@ __global__ void __launch_bounds__(kResThreads) residual_kernel(const double *__r
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 2; ++j) ar[i][j] = al[i][j] = Cx<double>{0.0, 0.0};
-    const int64_t stages = (m + kResK - 1) / kResK;
-    load(0);
+    const int64_t all_stages = (m + kResK - 1) / kResK, per = (all_stages + gridDim.z - 1) / gridDim.z;
+    const int64_t s_begin = min(all_stages, (int64_t)blockIdx.z * per), s_end = min(all_stages, s_begin + per);
+    load(s_begin * kResK);
     store(0);
     __syncthreads();
-    for (int64_t st = 0; st < stages; ++st) {
-        const int b = (int)(st & 1);
-        if (st + 1 < stages) load((st + 1) * kResK);
+    for (int64_t st = s_begin; st < s_end; ++st) {
+        const int b = (int)((st - s_begin) & 1);
+        if (st + 1 < s_end) load((st + 1) * kResK);
 #pragma unroll
         for (int k = 0; k < kResK; ++k) {
             double rk[4], lk[4];
@@ -1095,8 +1102,23 @@ __global__ void __launch_bounds__(kResThreads) residual_kernel(const double *__r
                     al[i][j].im += lk[i] * xk[j].im;
                 }
         }
-        if (st + 1 < stages) store(b ^ 1);
+        if (st + 1 < s_end) store(b ^ 1);
         __syncthreads();
+    }
+    if (part) {
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int64_t g = g0 + ty + 16 * j;
+            if (g >= G) continue;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int64_t row = i0 + tx + 8 * i;
+                if (row < m)
+                    part[((int64_t)blockIdx.z * G + g) * m + row] =
+                        make_double4(ar[i][j].re, ar[i][j].im, al[i][j].re, al[i][j].im);
+            }
+        }
+        return;
     }
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
@@ -1115,6 +1137,31 @@ __global__ void __launch_bounds__(kResThreads) residual_kernel(const double *__r
             const double ax_im = ar[i][j].im + w * al[i][j].re;
             r[g * m + row] = Cx<double>{br - ax_re, w * bl - ax_im};
         }
+    }
+}
+
+// The split residual's second pass: the k ranges' sums added in range order,
+// then r as in residual_kernel.
+__global__ void residual_finish_kernel(const double *__restrict__ R, const double *__restrict__ L, int64_t ld,
+                                       int64_t m, int64_t p, const double *__restrict__ omega, int count, int splits,
+                                       const double4 *__restrict__ part, Cx<double> *__restrict__ r) {
+    const int64_t G = (int64_t)count * p, total = G * m;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t g = t / m, row = t % m;
+        double4 a = part[t];
+        for (int z = 1; z < splits; ++z) {
+            const double4 b = part[(int64_t)z * total + t];
+            a.x += b.x;
+            a.y += b.y;
+            a.z += b.z;
+            a.w += b.w;
+        }
+        const int f = (int)(g / p);
+        const int64_t q = g % p;
+        const double w = omega[f];
+        const double br = R[row + (m + q) * ld], bl = L[row + (m + q) * ld];
+        const double ax_re = a.x - w * a.w, ax_im = a.y + w * a.z;
+        r[t] = Cx<double>{br - ax_re, w * bl - ax_im};
     }
 }
 
@@ -1600,14 +1647,39 @@ fh_status form_rhs(const double *Rm, const double *Lm, int64_t ld, int64_t m, in
     return FH_OK;
 }
 
+int residual_splits(int64_t m, int64_t p, int count) {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    const int64_t tiles = ((m + kResRows - 1) / kResRows) * (((int64_t)count * p + kResCols - 1) / kResCols);
+    const int64_t stages = (m + kResK - 1) / kResK;
+    // about 16 CTAs per SM over the launch, each range at least 16 stages
+    const int64_t want = (16 * (int64_t)sms + tiles - 1) / std::max<int64_t>(1, tiles);
+    return (int)std::max<int64_t>(1, std::min<int64_t>({want, kResMaxSplits, stages / 16}));
+}
+
+size_t residual_scratch_bytes(int64_t m, int64_t p, int count) {
+    const int splits = residual_splits(m, p, count);
+    return splits > 1 ? (size_t)splits * (size_t)count * (size_t)p * (size_t)m * sizeof(double4) : 0;
+}
+
 fh_status residual_fp64(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega,
-                        int count, const double *x, double *r, double *rnorm, cudaStream_t s, fh_error_info *err) {
+                        int count, const double *x, double *r, double *rnorm, cudaStream_t s, fh_error_info *err,
+                        void *scratch) {
     if (m == 0) return FH_OK;
     const int64_t cols = (int64_t)count * p;
+    const int splits = scratch ? residual_splits(m, p, count) : 1;
+    double4 *part = splits > 1 ? static_cast<double4 *>(scratch) : nullptr;
     prof_begin(s, FH_PROF_RESIDUAL);
-    residual_kernel<<<dim3((unsigned)((m + kResRows - 1) / kResRows), (unsigned)((cols + kResCols - 1) / kResCols)),
+    residual_kernel<<<dim3((unsigned)((m + kResRows - 1) / kResRows), (unsigned)((cols + kResCols - 1) / kResCols),
+                           (unsigned)(part ? splits : 1)),
                       kResThreads, 0, s>>>(Rm, Lm, ld, m, p, omega, count, reinterpret_cast<const Cx<double> *>(x),
-                                           reinterpret_cast<Cx<double> *>(r));
+                                           reinterpret_cast<Cx<double> *>(r), part);
+    if (part)
+        residual_finish_kernel<<<grid_for(cols * m, 256), 256, 0, s>>>(Rm, Lm, ld, m, p, omega, count, splits, part,
+                                                                      reinterpret_cast<Cx<double> *>(r));
     prof_end(s, FH_PROF_RESIDUAL, 16.0 * (double)m * (double)m);  // bytes: R and L read once
     FHB_CUDA(cudaGetLastError());
     if (rnorm) {

@@ -217,8 +217,12 @@ fh_status form_rhs(const double *Rm, const double *Lm, int64_t ld, int64_t m, in
 // r_f = b_f - (R_ee + j w_f L_ee) x_f in FP64 for all f at once (one pass
 // over R_ee and L_ee).  x, b, r: count x m x p complex double.  Also returns
 // per-frequency max-norms of r and b through rnorm/bnorm (device, count each).
+// With scratch (residual_scratch_bytes; 0 means none is used) the k range is
+// split across CTAs and the ranges' sums are added in a fixed order.
+size_t residual_scratch_bytes(int64_t m, int64_t p, int count);
 fh_status residual_fp64(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega,
-                        int count, const double *x, double *r, double *rnorm, cudaStream_t s, fh_error_info *err);
+                        int count, const double *x, double *r, double *rnorm, cudaStream_t s, fh_error_info *err,
+                        void *scratch = nullptr);
 
 // Z_f = Z_pp - Z_ep^T X_f (p x p complex, row-major per frequency).
 fh_status schur(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega, int count,

@@ -216,14 +216,21 @@ def run_ours(args):
     barrier(world)
     times = []
     zs = None
-    with ClockSampler(local) as clocks, fh.Profiler() as prof:
+    with ClockSampler(local) as clocks:
         torch.cuda.synchronize()
         for _ in range(args.steps):
             t, zs, iters, resid = sweep_device_s(fh.Precision.MIXED_BF16X3)
             times.append(t)
         torch.cuda.synchronize()
-        profile = prof.read()
     barrier(world)
+    # Per-kernel-class breakdown (and the roofline's launch times) from the
+    # same number of sweeps run again with the event profiler on: its two
+    # event records per launch stay out of the timed sweeps.
+    with fh.Profiler() as prof:
+        for _ in range(args.steps):
+            sweep_device_s(fh.Precision.MIXED_BF16X3)
+        torch.cuda.synchronize()
+        profile = prof.read()
     step_s = sum(times) / len(times)
     step_max = max_over_ranks(step_s, world)
     z64 = r64.impedance_ohm

@@ -461,32 +461,38 @@ __global__ void __launch_bounds__(kThreads, 1) packed_update_kernel(PackedArgs g
 // reaches a column that a later block of the item reads, and items own
 // disjoint rows.  Roles:
 //   warp 13, one lane  loader: per chunk, one 2D tensor copy (no multicast)
-//                      of the raw FP32 rows -- box 128 rows x 16 columns of
-//                      the batch seen as an m x (count m) array of 8-byte
-//                      elements, rows past m filled with zeros -- and one
-//                      plain bulk copy of the X chunk, both counted on the
-//                      stage's `full` barrier (a tensor map needs a column
-//                      stride that is a multiple of 16 bytes: m even);
-//   warps 0..3         splitters: thread t takes row t of the chunk from the
-//                      raw tile, splits it into BF16 hi/lo and stores the
-//                      four A tiles of the stage, then a proxy fence and an
-//                      arrival on `afull`;
+//                      of the raw FP32 rows into a ring of raw slots -- box
+//                      128 rows x 16 columns of the batch seen as an m x
+//                      (count m) array of 8-byte elements, rows past m
+//                      filled with zeros (a tensor map needs a column stride
+//                      that is a multiple of 16 bytes: m even);
+//   warps 0..3         splitters: thread t reads row t of the chunk from the
+//                      raw slot into registers and releases the slot; once
+//                      the MMAs are done with the A/X stage, thread 0 starts
+//                      the plain bulk copy of the X chunk into it and every
+//                      thread stores its row as BF16 hi/lo into the four A
+//                      tiles, then a proxy fence and an arrival on `afull`.
+//                      The raw ring and the A/X ring are separate, so a raw
+//                      slot is reused after the split, not after the MMAs;
 //   warp 12, one lane  TMEM allocation and the MMA issuer: 12 tcgen05.mma per
 //                      chunk into one of two TMEM accumulators;
 //   warps 4..11        epilogue: tcgen05.ld, then L21 and U12 in FP32 and the
 //                      packed tile of P.
-// A stage is reused once the MMAs that read it have completed (`empty`):
-// by then the splitters have consumed its raw tile too.  No cluster launch
+// An A/X stage is reused once the MMAs that read it have completed
+// (`empty`), a raw slot once the splitters have read it.  No cluster launch
 // and no multicast.  Every wait is bounded; a wait that runs out sets the
-// error flag and stops the role, and the loader and the MMA issuer wait
-// (bounded) for their operations in flight before the TMEM is freed.
+// error flag and stops the role, and the loader, the splitters' copy thread
+// and the MMA issuer wait (bounded) for their operations in flight before
+// the TMEM is freed.
 constexpr int kPsRawBytes = kChunk * kTile * 8;                   // 16 columns x 128 rows of complex FP32
-constexpr int kPsStageBytes = 2 * kOpBytes + kPsRawBytes;          // packed A, X, raw: 48 KB
-constexpr int kPsStages = 4;
+constexpr int kPsStageBytes = 2 * kOpBytes;                        // packed A, X: 32 KB
+constexpr int kPsStages = 4;                                       // A/X ring
+constexpr int kPsRawSlots = 4;                                     // raw ring
 constexpr int kPsThreads = 32 * 14;
 // A staging tile per epilogue warp for U12 (32 rows x 16 complex, XOR-swizzled).
 constexpr int kPsU12Bytes = kEpiWarps * 32 * 16 * 8;
-constexpr int kPsSmemBytes = kPsStages * kPsStageBytes + kPsU12Bytes + 1024 + kBarBytes;
+constexpr int kPsSmemBytes =
+    kPsStages * kPsStageBytes + kPsRawSlots * kPsRawBytes + kPsU12Bytes + 1024 + kBarBytes;
 static_assert(kPsSmemBytes <= 227 * 1024, "panel-solve shared memory");
 
 struct PanelSolveArgs {
@@ -513,19 +519,23 @@ __global__ void __launch_bounds__(kPsThreads, 1)
     panel_solve_kernel(PanelSolveArgs g, const __grid_constant__ CUtensorMap rows_map, int *__restrict__ err_flag) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-    float2 *u12_stage = reinterpret_cast<float2 *>(smem + kPsStages * kPsStageBytes);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kPsStages * kPsStageBytes + kPsU12Bytes);
-    uint64_t *full = bars;                            // [kPsStages] loader: raw A + X bytes
-    uint64_t *afull = bars + kPsStages;               // [kPsStages] splitters
-    uint64_t *empty = bars + 2 * kPsStages;           // [kPsStages] MMA commit
-    uint64_t *tfull = bars + 3 * kPsStages;           // [2]
-    uint64_t *tempty = bars + 3 * kPsStages + 2;      // [2]
-    uint64_t *drain = bars + 3 * kPsStages + 4;       // [1]
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 3 * kPsStages + 5);
-    // stage layout: packed A (4 tiles) | X chunk (4 tiles) | raw columns
+    uint8_t *raw_base = smem + kPsStages * kPsStageBytes;
+    float2 *u12_stage = reinterpret_cast<float2 *>(raw_base + kPsRawSlots * kPsRawBytes);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(raw_base + kPsRawSlots * kPsRawBytes + kPsU12Bytes);
+    uint64_t *rfull = bars;                           // [kPsRawSlots] loader: raw rows landed
+    uint64_t *rempty = rfull + kPsRawSlots;           // [kPsRawSlots] splitters: raw rows read
+    uint64_t *xfull = rempty + kPsRawSlots;           // [kPsStages] X chunk landed
+    uint64_t *afull = xfull + kPsStages;              // [kPsStages] splitters: A tiles written
+    uint64_t *empty = afull + kPsStages;              // [kPsStages] MMA commit
+    uint64_t *tfull = empty + kPsStages;              // [2]
+    uint64_t *tempty = tfull + 2;                     // [2]
+    uint64_t *drain = tempty + 2;                     // [1]
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    // A/X stage: packed A (4 tiles) | X chunk (4 tiles); raw slots apart, so a
+    // raw slot is free again as soon as the splitters have read it
     auto stage_a = [&](int st) { return smem + st * kPsStageBytes; };
     auto stage_b = [&](int st) { return smem + st * kPsStageBytes + kOpBytes; };
-    auto stage_raw = [&](int st) { return smem + st * kPsStageBytes + 2 * kOpBytes; };
+    auto stage_raw = [&](int rs) { return raw_base + rs * kPsRawBytes; };
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp == 12) {
@@ -534,8 +544,12 @@ __global__ void __launch_bounds__(kPsThreads, 1)
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (threadIdx.x == 0) {
+        for (int rs = 0; rs < kPsRawSlots; ++rs) {
+            mbar_init(smem_u32(&rfull[rs]), 1);
+            mbar_init(smem_u32(&rempty[rs]), 128);
+        }
         for (int st = 0; st < kPsStages; ++st) {
-            mbar_init(smem_u32(&full[st]), 1);
+            mbar_init(smem_u32(&xfull[st]), 1);
             mbar_init(smem_u32(&afull[st]), 128);
             mbar_init(smem_u32(&empty[st]), 1);
         }
@@ -554,7 +568,8 @@ __global__ void __launch_bounds__(kPsThreads, 1)
 
     if (warp == 13) {
         if (lane == 0) {
-            int stage = 0;
+            // raw rows only: one 2D tensor copy per chunk into the raw ring
+            int rs = 0;
             uint32_t phase = 0, issued = 0, last_phase = 0;
             for (long long t = blockIdx.x; t < g.items && ok; t += gridDim.x) {
                 const int f = (int)(t / g.rblocks), rb = (int)(t % g.rblocks);
@@ -562,45 +577,64 @@ __global__ void __launch_bounds__(kPsThreads, 1)
                 const int y0 = (int)((int64_t)f * g.m + g.K0);  // column K0 of matrix f
                 for (int j = g.nbw - 1; j >= 0 && ok; --j)
                     for (int c = 0; c < 8 * (j + 1); ++c) {
-                        if (!mbar_wait(smem_u32(&empty[stage]), phase ^ 1u)) {
+                        if (!mbar_wait(smem_u32(&rempty[rs]), phase ^ 1u)) {
                             ok = false;
                             break;
                         }
-                        const uint32_t bar = smem_u32(&full[stage]);
-                        mbar_expect_tx(bar, kOpBytes + kPsRawBytes);
-                        bulk_load(smem_u32(stage_b(stage)), g.Xp + (((int64_t)f * g.nbw + j) * g.nch + c) * kOpBytes,
-                                  kOpBytes, bar);
-                        tensor_load_2d(smem_u32(stage_raw(stage)), &rows_map, x, y0 + c * kChunk, bar);
-                        issued |= 1u << stage;
-                        last_phase = (last_phase & ~(1u << stage)) | (phase << stage);
-                        if (++stage == kPsStages) {
-                            stage = 0;
+                        const uint32_t bar = smem_u32(&rfull[rs]);
+                        mbar_expect_tx(bar, kPsRawBytes);
+                        tensor_load_2d(smem_u32(stage_raw(rs)), &rows_map, x, y0 + c * kChunk, bar);
+                        issued |= 1u << rs;
+                        last_phase = (last_phase & ~(1u << rs)) | (phase << rs);
+                        if (++rs == kPsRawSlots) {
+                            rs = 0;
                             phase ^= 1u;
                         }
                     }
             }
             if (!ok) {
                 atomicExch(err_flag, 1);
-                for (int st = 0; st < kPsStages; ++st)
-                    if (issued >> st & 1u) mbar_wait(smem_u32(&full[st]), last_phase >> st & 1u);
+                for (int r = 0; r < kPsRawSlots; ++r)
+                    if (issued >> r & 1u) mbar_wait(smem_u32(&rfull[r]), last_phase >> r & 1u);
             }
         }
     } else if (warp < 4) {
+        // splitters: raw rows -> registers (the raw slot is released at once),
+        // then, once the MMAs are done with the A/X stage, the X chunk's bulk
+        // copy (thread 0) and the BF16 hi/lo A tiles
         const int tr = threadIdx.x;  // row of the block
-        int stage = 0;
-        uint32_t phase = 0;
+        int rs = 0, stage = 0;
+        uint32_t rphase = 0, phase = 0, xissued = 0, xlast = 0;
         for (long long t = blockIdx.x; t < g.items && ok; t += gridDim.x) {
+            const int f = (int)(t / g.rblocks);
             for (int j = g.nbw - 1; j >= 0 && ok; --j)
                 for (int c = 0; c < 8 * (j + 1); ++c) {
-                    if (!mbar_wait(smem_u32(&full[stage]), phase)) {
+                    if (!mbar_wait(smem_u32(&rfull[rs]), rphase)) {
                         ok = false;
                         break;
                     }
                     // raw tile: column kk of the chunk at kk * 128, rows contiguous (zeros past m)
-                    const float2 *raw = reinterpret_cast<const float2 *>(stage_raw(stage));
+                    const float2 *raw = reinterpret_cast<const float2 *>(stage_raw(rs));
                     float2 v[kChunk];
 #pragma unroll
                     for (int kk = 0; kk < kChunk; ++kk) v[kk] = raw[kk * kTile + tr];
+                    mbar_arrive(smem_u32(&rempty[rs]));
+                    if (++rs == kPsRawSlots) {
+                        rs = 0;
+                        rphase ^= 1u;
+                    }
+                    if (!mbar_wait(smem_u32(&empty[stage]), phase ^ 1u)) {
+                        ok = false;
+                        break;
+                    }
+                    if (tr == 0) {
+                        const uint32_t bar = smem_u32(&xfull[stage]);
+                        mbar_expect_tx(bar, kOpBytes);
+                        bulk_load(smem_u32(stage_b(stage)), g.Xp + (((int64_t)f * g.nbw + j) * g.nch + c) * kOpBytes,
+                                  kOpBytes, bar);
+                        xissued |= 1u << stage;
+                        xlast = (xlast & ~(1u << stage)) | (phase << stage);
+                    }
                     uint8_t *dst = stage_a(stage);
                     split_store8(v, dst, tile_off(tr, 0));
                     split_store8(v + 8, dst, tile_off(tr, 1));
@@ -612,7 +646,12 @@ __global__ void __launch_bounds__(kPsThreads, 1)
                     }
                 }
         }
-        if (!ok) atomicExch(err_flag, 1);
+        if (!ok) {
+            atomicExch(err_flag, 1);
+            if (tr == 0)
+                for (int st = 0; st < kPsStages; ++st)
+                    if (xissued >> st & 1u) mbar_wait(smem_u32(&xfull[st]), xlast >> st & 1u);
+        }
     } else if (warp == 12) {
         if (lane == 0) {
             int stage = 0;
@@ -629,7 +668,7 @@ __global__ void __launch_bounds__(kPsThreads, 1)
                     tc_fence_after();
                     const uint32_t d_re = tmem + buf * kAccCols, d_im = d_re + kTile;
                     for (int c = 0; c < 8 * (j + 1); ++c) {
-                        if (!mbar_wait(smem_u32(&full[stage]), phase) || !mbar_wait(smem_u32(&afull[stage]), phase)) {
+                        if (!mbar_wait(smem_u32(&xfull[stage]), phase) || !mbar_wait(smem_u32(&afull[stage]), phase)) {
                             ok = false;
                             break;
                         }

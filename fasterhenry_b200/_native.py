@@ -138,7 +138,7 @@ EXPORTS = [
 ]
 
 PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner",
-                   "pfft_apply", "panel_solve"]
+                   "pfft_apply", "panel_solve", "form"]
 
 
 class FillStats(ctypes.Structure):

@@ -987,22 +987,44 @@ __global__ void __launch_bounds__(256) form_kernel(const double *__restrict__ R,
     }
 }
 
-// FP32 form, two consecutive entries per thread and one 16-byte store per
-// frequency (m * m even, batch 16-byte aligned).  With lower_tiles, pairs
-// whose entries both lie in 128 x 128 tiles above the diagonal are skipped.
+// FP32 form, two consecutive entries per 16-byte store (m * m even, batch
+// 16-byte aligned).  A CTA takes kFormPer x 256 consecutive entry pairs,
+// reads their R and L once and writes them frequency by frequency, so each
+// frequency's plane receives one contiguous 16 KB run per CTA.  With
+// lower_tiles, pairs whose entries both lie in 128 x 128 tiles above the
+// diagonal are skipped.
+constexpr int kFormPer = 4;
 __global__ void __launch_bounds__(256) form_pair_kernel(const double *__restrict__ R, const double *__restrict__ L,
                                                         int64_t ld, int64_t m, const double *__restrict__ omega,
                                                         int count, float4 *__restrict__ a, int lower_tiles) {
-    const int64_t pairs = m * m / 2;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < pairs; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t e = 2 * t, i = e % m, j = e / m;
-        const int64_t e1 = e + 1, i1 = e1 % m, j1 = e1 / m;
-        if (lower_tiles && (i >> 7) < (j >> 7) && (i1 >> 7) < (j1 >> 7)) continue;
-        const double r0 = R[i + j * ld], l0 = L[i + j * ld];
-        const double r1 = R[i1 + j1 * ld], l1 = L[i1 + j1 * ld];
+    const int64_t pairs = m * m / 2, chunk = 256 * kFormPer;
+    for (int64_t base = (int64_t)blockIdx.x * chunk; base < pairs; base += (int64_t)gridDim.x * chunk) {
+        double r0[kFormPer], l0[kFormPer], r1[kFormPer], l1[kFormPer];
+        bool keep[kFormPer];
+#pragma unroll
+        for (int k = 0; k < kFormPer; ++k) {
+            const int64_t t = base + k * 256 + threadIdx.x;
+            keep[k] = t < pairs;
+            if (!keep[k]) continue;
+            const int64_t e = 2 * t, i = e % m, j = e / m;
+            const int64_t i1 = i + 1 == m ? 0 : i + 1, j1 = i + 1 == m ? j + 1 : j;  // entry e + 1
+            if (lower_tiles && (i >> 7) < (j >> 7) && (i1 >> 7) < (j1 >> 7)) {
+                keep[k] = false;
+                continue;
+            }
+            r0[k] = R[i + j * ld];
+            l0[k] = L[i + j * ld];
+            r1[k] = R[i1 + j1 * ld];
+            l1[k] = L[i1 + j1 * ld];
+        }
         for (int f = 0; f < count; ++f) {
             const double w = __ldg(omega + f);
-            __stcs(a + (int64_t)f * pairs + t, make_float4((float)r0, (float)(w * l0), (float)r1, (float)(w * l1)));
+            float4 *plane = a + (int64_t)f * pairs + base + threadIdx.x;
+#pragma unroll
+            for (int k = 0; k < kFormPer; ++k)
+                if (keep[k])
+                    __stcs(plane + k * 256,
+                           make_float4((float)r0[k], (float)(w * l0[k]), (float)r1[k], (float)(w * l1[k])));
         }
     }
 }
@@ -1623,16 +1645,17 @@ template <class T>
 fh_status form_system(const double *Rm, const double *Lm, int64_t ld, int64_t m, const double *omega, int count, T *a,
                       cudaStream_t s, fh_error_info *err, bool lower_tiles) {
     if (m == 0) return FH_OK;
-    if constexpr (sizeof(T) == 4) {
-        if ((m * m) % 2 == 0 && (reinterpret_cast<uintptr_t>(a) & 15) == 0) {
-            form_pair_kernel<<<grid_for(m * m / 2, 256, 148 * 16), 256, 0, s>>>(
-                Rm, Lm, ld, m, omega, count, reinterpret_cast<float4 *>(a), lower_tiles ? 1 : 0);
-            FHB_CUDA(cudaGetLastError());
-            return FH_OK;
-        }
-    }
-    form_kernel<T><<<grid_for(m * m, 256, 148 * 16), 256, 0, s>>>(Rm, Lm, ld, m, omega, count,
-                                                                   reinterpret_cast<Cx<T> *>(a));
+    prof_begin(s, FH_PROF_FORM);
+    bool pairs = false;
+    if constexpr (sizeof(T) == 4) pairs = (m * m) % 2 == 0 && (reinterpret_cast<uintptr_t>(a) & 15) == 0;
+    if (pairs)
+        form_pair_kernel<<<grid_for((m * m / 2 + kFormPer - 1) / kFormPer, 256, 148 * 16), 256, 0, s>>>(
+            Rm, Lm, ld, m, omega, count, reinterpret_cast<float4 *>(a), lower_tiles ? 1 : 0);
+    else
+        form_kernel<T><<<grid_for(m * m, 256, 148 * 16), 256, 0, s>>>(Rm, Lm, ld, m, omega, count,
+                                                                       reinterpret_cast<Cx<T> *>(a));
+    // bytes written: every entry of every frequency (about half with lower_tiles)
+    prof_end(s, FH_PROF_FORM, (double)m * (double)m * count * 2.0 * sizeof(T));
     FHB_CUDA(cudaGetLastError());
     return FH_OK;
 }

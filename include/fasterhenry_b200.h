@@ -471,7 +471,8 @@ typedef enum fh_profile_class {
     FH_PROF_GEMM_TC_INNER = 8,  /* tensor-core updates inside a super-panel and of its U12 rows */
     FH_PROF_PFFT_APPLY = 9,     /* one precorrected-FFT product (near field, spread, FFTs, interpolation) */
     FH_PROF_PANEL_SOLVE = 10,   /* rows below a super-panel: L21 = A21 U^-1, U12 and the packed operands */
-    FH_PROF_CLASSES = 11
+    FH_PROF_FORM = 11,          /* the sweep's systems R + jwL (and right-hand sides) formed from R_m, L_m */
+    FH_PROF_CLASSES = 12
 } fh_profile_class;
 
 void fh_profile_enable(int32_t on);

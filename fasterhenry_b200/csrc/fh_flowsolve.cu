@@ -90,16 +90,18 @@ __device__ __forceinline__ bool flow_wait(const unsigned *flag, unsigned epoch, 
 }
 
 // Factor tiles and the blocks' inverses stream through a ring of
-// kFlowStages shared-memory tiles of 128 rows x 16 columns (16 KB): a factor
+// kFlowStages shared-memory tiles of 128 rows x 32 columns (32 KB): a factor
 // tile by one 2D TMA load (rows past m read as zeros), an inverse tile by a
-// bulk copy of its 16 contiguous columns.  The loads run ahead along the
+// bulk copy of its kFlowTileCols contiguous columns.  The loads run ahead along the
 // CTA's own sequence of tiles, independent of the flags: the factors do not
 // change during the solve, so only the vector pieces wait.
-constexpr int kFlowTileCols = 16;
-constexpr int kFlowStages = 6;
+constexpr int kFlowTileCols = 32;
+constexpr int kFlowStages = 3;
 constexpr int kFlowTileElems = kNb * kFlowTileCols;
 constexpr int kFlowTileBytes = kFlowTileElems * 8;
 constexpr int kFlowTilesPerBlock = kNb / kFlowTileCols;
+constexpr int kFlowWarpCols = kFlowTileCols / (kFlowThreads / 32);  // backward: a warp's columns per tile
+static_assert(kFlowTilesPerBlock * kFlowWarpCols * 2 == 32, "backward sums: one value per lane");
 constexpr int kFlowSmemBytes = kFlowStages * kFlowTileBytes + kFlowStages * 8;
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -142,12 +144,12 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_
 // Position in a CTA's tile sequence: forward blocks i = slice, slice + P, ...
 // then backward blocks from the last down; per block its source blocks
 // (forward j = 0 .. i-1, backward j = nblk-1 .. i+1), then its inverse, each
-// as 8 tiles of 16 columns.
+// as kFlowTilesPerBlock tiles of kFlowTileCols columns.
 struct TileCursor {
     int pass;  // 0 forward, 1 backward, 2 done
     int i;     // output block
     int s;     // source index; s == nsrc() is the block's inverse
-    int q;     // 16-column tile
+    int q;     // tile of kFlowTileCols columns
     __device__ int nsrc(int nblk) const { return pass == 0 ? i : nblk - 1 - i; }
     __device__ void start(int slice) {
         pass = 0;
@@ -256,19 +258,20 @@ __global__ void __launch_bounds__(kFlowThreads) flowsolve_kernel(FlowArgs g, con
         return true;
     };
 
-    // Backward source tile q (L_ji, 128 rows of block j x 16 columns of block
-    // i): t[q][c] += sum_r L_ji(r, q 16 + 2 warp + c) x_j(r) over the lane's
-    // rows r = 4 lane .. 4 lane + 3, kept per lane until the block's sources
-    // are done (U_ij = D_i L_ji^T, so U is never read).
-    float bt[kFlowTilesPerBlock][2][2];
+    // Backward source tile q (L_ji, 128 rows of block j x kFlowTileCols
+    // columns of block i): t[q][c] += sum_r L_ji(r, q kFlowTileCols +
+    // kFlowWarpCols warp + c) x_j(r) over the lane's rows r = 4 lane ..
+    // 4 lane + 3, kept per lane until the block's sources are done
+    // (U_ij = D_i L_ji^T, so U is never read).
+    float bt[kFlowTilesPerBlock][kFlowWarpCols][2];
     auto step_t = [&](int q, const Cx<float> (&xr)[4]) -> bool {
         const int slot = (int)(t_comp % kFlowStages);
         const bool ok = mbar_wait(smem_addr(&full[slot]), (uint32_t)((t_comp / kFlowStages) & 1));
         if (ok) {
             const Cx<float> *tile = ring + slot * kFlowTileElems;
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const float4 *col = reinterpret_cast<const float4 *>(tile + (2 * warp + c) * kNb + 4 * lane);
+            for (int c = 0; c < kFlowWarpCols; ++c) {
+                const float4 *col = reinterpret_cast<const float4 *>(tile + (kFlowWarpCols * warp + c) * kNb + 4 * lane);
                 const float4 p0 = col[0], p1 = col[1];  // rows 4 lane, +1 | +2, +3
                 bt[q][c][0] += p0.x * xr[0].re - p0.y * xr[0].im + p0.z * xr[1].re - p0.w * xr[1].im +
                                p1.x * xr[2].re - p1.y * xr[2].im + p1.z * xr[3].re - p1.w * xr[3].im;
@@ -301,7 +304,8 @@ __global__ void __launch_bounds__(kFlowThreads) flowsolve_kernel(FlowArgs g, con
         if (pass == 1) {
 #pragma unroll
             for (int q = 0; q < kFlowTilesPerBlock; ++q)
-                bt[q][0][0] = bt[q][0][1] = bt[q][1][0] = bt[q][1][1] = 0.f;
+#pragma unroll
+                for (int c = 0; c < kFlowWarpCols; ++c) bt[q][c][0] = bt[q][c][1] = 0.f;
         }
         for (int s = 0; s < nsrc; ++s) {
             const int j = pass == 0 ? s : g.nblk - 1 - s;
@@ -330,10 +334,11 @@ __global__ void __launch_bounds__(kFlowThreads) flowsolve_kernel(FlowArgs g, con
         } else {
             // Sum bt over the warp's lanes: each halving exchanges half of the
             // remaining values, so lane l ends with the total of value l,
-            // which is part of column q 16 + 2 warp + c (l = 4 q + 2 c + re/im).
+            // which is part of column q kFlowTileCols + kFlowWarpCols warp + c
+            // (l = 2 (kFlowWarpCols q + c) + re/im).
             float v[32];
 #pragma unroll
-            for (int k = 0; k < 32; ++k) v[k] = bt[k >> 2][(k >> 1) & 1][k & 1];
+            for (int k = 0; k < 32; ++k) v[k] = bt[(k >> 1) / kFlowWarpCols][(k >> 1) % kFlowWarpCols][k & 1];
 #pragma unroll
             for (int off = 16; off >= 1; off >>= 1) {
                 const bool hi = (lane & off) != 0;
@@ -343,8 +348,8 @@ __global__ void __launch_bounds__(kFlowThreads) flowsolve_kernel(FlowArgs g, con
                     v[k] = keep + __shfl_xor_sync(0xffffffffu, send, off);
                 }
             }
-            const int q = lane >> 2, c = (lane >> 1) & 1;
-            reinterpret_cast<float *>(part)[(q * kFlowTileCols + 2 * warp + c) * 2 + (lane & 1)] = v[0];
+            const int q = (lane >> 1) / kFlowWarpCols, c = (lane >> 1) % kFlowWarpCols;
+            reinterpret_cast<float *>(part)[(q * kFlowTileCols + kFlowWarpCols * warp + c) * 2 + (lane & 1)] = v[0];
         }
         __syncthreads();
         if (h == 0) {

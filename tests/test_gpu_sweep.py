@@ -206,3 +206,26 @@ def test_two_level_mixed_strongly_coupled_loops(fh):
         rm = s.sweep(freqs, fh.Precision.MIXED_BF16X3)
     assert rel_err(rm.impedance_ohm, z64) < MIXED_RTOL
     assert all(1 <= i <= 8 for i in rm.refinement_iterations), rm.refinement_iterations
+
+
+def test_two_level_mixed_many_ports(fh):
+    """Ten ports x 32 frequencies = 320 (matrix, right-hand side) pairs, more
+    than one cooperative launch of the dataflow solve holds (two CTAs per SM
+    at most), so the refinement solves with the barrier-based form.  That
+    form reads U12, which the rows-below pass then writes (m = 1,044, even:
+    the fused pass runs over two super-panels), while the dataflow solve
+    takes U from L and leaves it unwritten."""
+    base = F.meander_legs(18)
+    a, b = base.ports[0]
+    inner = [k for k in range(len(base.nodes)) if k not in (a, b)]
+    ports = list(base.ports) + [(a, inner[i]) for i in np.linspace(2, len(inner) - 3, 9).astype(int)]
+    deck = F.Deck(list(base.nodes), [dict(sg) for sg in base.segments], ports, dict(base.discretization),
+                  "meander_18_ten_ports")
+    freqs = F.logspace(5, 10, 32)
+    with fh.MeshSystem.assemble(fh.Geometry.from_deck(deck), deck.ports, deck.discretization) as s:
+        c = s.counts()
+        assert c["internal_meshes"] == 1044 and c["ports"] == 10
+        z64 = s.sweep(freqs, fh.Precision.FP64).impedance_ohm
+        rm = s.sweep(freqs, fh.Precision.MIXED_BF16X3)
+    assert rel_err(rm.impedance_ohm, z64) < MIXED_RTOL
+    assert all(1 <= i <= 10 for i in rm.refinement_iterations), rm.refinement_iterations

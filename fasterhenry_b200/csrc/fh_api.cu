@@ -114,6 +114,23 @@ struct fh_system {
 
 namespace fhb {
 
+// CUDA events that are destroyed on every return path of the scope that
+// holds them (error returns and time-outs included).
+template <int N>
+struct ScopedEvents {
+    cudaEvent_t e[N] = {};
+    ScopedEvents() {
+        for (auto &x : e) cudaEventCreate(&x);
+    }
+    ~ScopedEvents() {
+        for (auto &x : e)
+            if (x) cudaEventDestroy(x);
+    }
+    ScopedEvents(const ScopedEvents &) = delete;
+    ScopedEvents &operator=(const ScopedEvents &) = delete;
+};
+
+
 fh_status ensure_device(fh_error_info *err) {
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
@@ -265,25 +282,17 @@ fh_status sweep_chunk_fp64(fh_system *s, const double *d_omega, int count, doubl
         b.singular = sing.p;
         b.m = m;
         b.count = count;
-        cudaEvent_t e0, e1;
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
-        cudaEventRecord(e0, st);
+        ScopedEvents<2> ev;
+        cudaEventRecord(ev.e[0], st);
         e = lu_factor<double>(b, w, kNbFp64, TrailingUpdate::Simt, st, err);
-        cudaEventRecord(e1, st);
+        cudaEventRecord(ev.e[1], st);
         if (!e) e = lu_solve<double>(b, d_x, (int)p, kNbFp64, st, err);
-        if (e) {
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            return e;
-        }
+        if (e) return e;
         FHB_CUDA(cudaMemcpyAsync(h_singular, sing.p, sizeof(int) * count, cudaMemcpyDeviceToHost, st));
         FHB_CUDA(cudaStreamSynchronize(st));
         float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventElapsedTime(&ms, ev.e[0], ev.e[1]);
         if (ms_factor) *ms_factor += ms;
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
     } else {
         std::fill(h_singular, h_singular + count, 0);
     }
@@ -417,10 +426,8 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     b.singular = sing.p;
     b.m = m;
     b.count = count;
-    cudaEvent_t e0, e1, e2;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventCreate(&e2);
+    ScopedEvents<3> ev;
+    cudaEvent_t e0 = ev.e[0], e1 = ev.e[1], e2 = ev.e[2];
     cudaEventRecord(e0, st);
     e = lu_factor<float>(b, w, kNbFp32, mode, st, err);
     cudaEventRecord(e1, st);
@@ -517,9 +524,6 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     cudaEventElapsedTime(&ms2, e1, e2);
     if (ms_factor) *ms_factor += ms1;
     if (ms_refine) *ms_refine += ms2;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaEventDestroy(e2);
     return FH_OK;
 }
 
@@ -761,9 +765,8 @@ fh_status fh_system_create_coupled(const fh_node *nodes, size_t n_nodes, const f
     if (st) return st;
     FHB_CUDA(cudaStreamSynchronize(cs));
     const double t2 = wall();
-    cudaEvent_t c0, c1;
-    cudaEventCreate(&c0);
-    cudaEventCreate(&c1);
+    ScopedEvents<2> cev;
+    cudaEvent_t c0 = cev.e[0], c1 = cev.e[1];
     cudaEventRecord(c0, cs);
     st = device_congruence(d_L.p, d_R.p, n, d_rp.p, d_br.p, d_sign.p, loops, s->loops.row_ptr.data(), s->d_Lm,
                            s->d_Rm, cs, err);
@@ -771,8 +774,6 @@ fh_status fh_system_create_coupled(const fh_node *nodes, size_t n_nodes, const f
     if (st) return st;
     FHB_CUDA(cudaStreamSynchronize(cs));
     cudaEventElapsedTime(&s->ms_congruence, c0, c1);
-    cudaEventDestroy(c0);
-    cudaEventDestroy(c1);
     const double t3 = wall();
     // Conductors: connected components of the segment graph by union-find
     // over nodes, numbered in order of their first segment (currents.rs:137-163).
@@ -923,9 +924,8 @@ fh_status fh_sweep(fh_system *sys, const double *freqs, size_t nf, fh_precision 
     FHB_PALLOC(sys->pool, d_x, kSlotX, (size_t)chunk * m * p * 2);
     FHB_PALLOC(sys->pool, d_z, kSlotZ, (size_t)chunk * p * p * 2);
     float ms_factor = 0, ms_refine = 0;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
+    ScopedEvents<2> ev;
+    cudaEvent_t e0 = ev.e[0], e1 = ev.e[1];
     cudaEventRecord(e0, st);
     std::vector<int> singular((size_t)nf, 0), failed((size_t)nf, 0);
     for (size_t c0 = 0; c0 < nf; c0 += (size_t)chunk) {
@@ -975,8 +975,6 @@ fh_status fh_sweep(fh_system *sys, const double *freqs, size_t nf, fh_precision 
     FHB_CUDA(cudaStreamSynchronize(st));
     float ms_total = 0;
     cudaEventElapsedTime(&ms_total, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     // First failing frequency in list order (solve.rs:877-879).
     for (size_t k = 0; k < nf; ++k) {
         bool bad = singular[k] != 0;

@@ -18,9 +18,12 @@
 //     FH_ERR_INVALID_ARGUMENT before anything is launched;
 //   * the scratch array (about 257 KB) lives in every device that loads the
 //     library, until the process exits;
-//   * the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (once per device, with that device current); make
-//     that first call before any stream capture begins;
+//   * the first call in each device context (a device's primary context, and
+//     again after cudaDeviceReset has replaced it) looks up the array's
+//     device address with cudaGetSymbolAddress, with that device current;
+//     make that first call before any stream capture begins;
+//   * the call waits on the host until the solve has finished on its stream
+//     (it reads the zero-pivot flag back);
 //   * all calls share the one array: calls whose work overlaps on the GPU
 //     (concurrent streams, or threads on the same device) race on it and must
 //     be serialised by the caller.  Each call clears the parts that must
@@ -48,23 +51,61 @@ constexpr size_t kScratchBytes = kIdxOffset + sizeof(int) * kMaxChunks;
 // address: host code reaches the array through the address looked up below.
 static __device__ __align__(256) unsigned char g_lu_scratch[kScratchBytes];
 
+// The address of the array belongs to the module loaded in one context: a
+// cudaDeviceReset ends the primary context, the module is loaded again in the
+// next one and the array may move.  So the looked-up address is kept per
+// device together with the id of the context it was looked up in, and looked
+// up again when the current context is another one.
+using CtxGetCurrentFn = int (*)(void **);
+using CtxGetIdFn = int (*)(void *, unsigned long long *);
+
+struct ScratchSlot {
+    unsigned long long ctx_id = 0;
+    void *ptr = nullptr;
+};
+
 std::mutex g_mu;
-void *g_scratch[64] = {nullptr};
+ScratchSlot g_scratch[64];
+
+fh_status current_context_id(unsigned long long *id, fh_error_info *err) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *f0 = nullptr, *f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0, q1;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0) != cudaSuccess ||
+            q0 != cudaDriverEntryPointSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess || !f0 || !f1)
+            return fail(err, FH_ERR_CUDA, "fh_lu_solve_c64_noalloc: the driver's context queries are unavailable");
+        get_current = reinterpret_cast<CtxGetCurrentFn>(f0);
+        get_id = reinterpret_cast<CtxGetIdFn>(f1);
+    }
+    void *ctx = nullptr;
+    if (get_current(&ctx) != 0 || !ctx || get_id(ctx, id) != 0)
+        return fail(err, FH_ERR_CUDA, "fh_lu_solve_c64_noalloc: no current device context");
+    return FH_OK;
+}
 
 fh_status scratch_for_current_device(unsigned char **out, fh_error_info *err) {
     int dev = 0;
     FHB_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return fail(err, FH_ERR_INVALID_ARGUMENT, "device index out of range");
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch[dev]) {
+    unsigned long long ctx_id = 0;
+    fh_status st = current_context_id(&ctx_id, err);
+    if (st) return st;
+    ScratchSlot &slot = g_scratch[dev];
+    if (!slot.ptr || slot.ctx_id != ctx_id) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_lu_scratch);
         if (e != cudaSuccess || !p)
             return fail(err, FH_ERR_CUDA, std::string("cudaGetSymbolAddress of the LU scratch failed: ") +
                                               cudaGetErrorString(e));
-        g_scratch[dev] = p;
+        slot.ptr = p;
+        slot.ctx_id = ctx_id;
     }
-    *out = static_cast<unsigned char *>(g_scratch[dev]);
+    *out = static_cast<unsigned char *>(slot.ptr);
     return FH_OK;
 }
 

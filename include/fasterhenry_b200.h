@@ -8,8 +8,8 @@
  *     -> per frequency: Z(w) = Z_pp - Z_ep^T (R_ee + jwL_ee)^-1 Z_ep  (LU + Schur)
  * plus the matrix-free pFFT + GMRES alternative.  Each entry point below
  * names the reference interface it replaces (paths relative to the reference
- * project root).  A Rust crate binds these with `extern "C"` declarations
- * (see INTEGRATION.md); the Python package binds them with ctypes.
+ * project root).  A Rust crate binds these with `extern "C"` declarations;
+ * the Python package binds them with ctypes.
  *
  * Conventions
  *   - Plain pointers and sizes; all buffers are caller-owned HOST memory
@@ -254,10 +254,12 @@ fh_status fh_lu_solve_c64(const double *a, size_t n, const double *b, size_t nrh
  *   stream: a cudaStream_t (NULL = the legacy default stream).
  * Allocates nothing: its scratch (pivots, pivot-search partials, flags) is a
  * file-scope device array sized for n <= FH_NOALLOC_MAX_ORDER; larger n is
- * rejected with FH_ERR_INVALID_ARGUMENT.  The first call on a device looks up
- * the array's address (make it before any stream capture).  All calls share
- * the array: calls that overlap on the GPU race and must be serialised by the
- * caller.  Returns after the solve has completed on `stream`. */
+ * rejected with FH_ERR_INVALID_ARGUMENT.  The first call in each device
+ * context looks up the array's address (make that first call before any
+ * stream capture begins).  All calls share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller.  The call blocks the
+ * host until the solve has finished on `stream` (it reads back the
+ * zero-pivot flag). */
 #define FH_NOALLOC_MAX_ORDER 65536
 fh_status fh_lu_solve_c64_noalloc(double *a, size_t n, double *b, size_t nrhs, void *stream,
                                   fh_error_info *err);

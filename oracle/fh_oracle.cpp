@@ -1364,12 +1364,198 @@ inline void subtract_scaled(C *y, C factor, const C *x, long long len) {
 
 constexpr long long kPanel = 32;
 
+// The loops below visit the entries of a column in another order than
+// dense.rs's column-at-a-time `subtract_scaled` sweeps, but every entry still
+// receives exactly the reference's operations in the reference's order:
+//   y -= h_c * l_c  for c = 0, 1, ... (each product rounded as in cmul, then
+//   the subtraction), with h_c = the column's entry in row start + c,
+// which is final before any row below it uses it.  So the factors are the
+// reference's bit for bit (checked against the plain column sweeps in
+// tests/test_oracle_known_answers.py), only the memory traffic changes: the
+// trailing update goes row block by row block, four columns at a time, so a
+// block of the panel is loaded once for many columns instead of once per
+// column and panel column.
+
+// Rows [r0, r1) of `ncols` columns (y_j = col[j]): y_j[r] -= sum over c in
+// [0, width) of h[j][c] * l_c[r], in increasing c, where l_c = panel + c*order.
+static void rows_update_scalar(C *const *col, int ncols, const C *const *h, const C *panel, long long order,
+                               long long width, long long r0, long long r1) {
+    for (int j = 0; j < ncols; ++j)
+        for (long long r = r0; r < r1; ++r) {
+            C y = col[j][r];
+            for (long long c = 0; c < width; ++c) y = csub(y, cmul(h[j][c], panel[c * order + r]));
+            col[j][r] = y;
+        }
+}
+
+#if defined(__x86_64__)
+#include <immintrin.h>
+// The same per-entry sequence with AVX2 lanes: (hr * [lr, li]) addsub
+// (hi * [li, lr]) = [hr lr - hi li, hr li + hi lr] is cmul's rounding of both
+// parts, then one subtraction; no fused multiply-add is used.
+__attribute__((target("avx2"))) static void rows_update_avx2(C *const *col, int ncols, const C *const *h,
+                                                             const C *panel, long long order, long long width,
+                                                             long long r0, long long r1) {
+    long long r = r0;
+    if (ncols == 4) {
+        for (; r + 4 <= r1; r += 4) {
+            __m256d y[4][2];
+            for (int j = 0; j < 4; ++j) {
+                y[j][0] = _mm256_loadu_pd(&col[j][r].re);
+                y[j][1] = _mm256_loadu_pd(&col[j][r + 2].re);
+            }
+            for (long long c = 0; c < width; ++c) {
+                const C *l = panel + c * order + r;
+                __m256d l0 = _mm256_loadu_pd(&l[0].re), l1 = _mm256_loadu_pd(&l[2].re);
+                __m256d s0 = _mm256_permute_pd(l0, 0x5), s1 = _mm256_permute_pd(l1, 0x5);
+                for (int j = 0; j < 4; ++j) {
+                    __m256d hr = _mm256_broadcast_sd(&h[j][c].re), hi = _mm256_broadcast_sd(&h[j][c].im);
+                    y[j][0] = _mm256_sub_pd(y[j][0], _mm256_addsub_pd(_mm256_mul_pd(hr, l0), _mm256_mul_pd(hi, s0)));
+                    y[j][1] = _mm256_sub_pd(y[j][1], _mm256_addsub_pd(_mm256_mul_pd(hr, l1), _mm256_mul_pd(hi, s1)));
+                }
+            }
+            for (int j = 0; j < 4; ++j) {
+                _mm256_storeu_pd(&col[j][r].re, y[j][0]);
+                _mm256_storeu_pd(&col[j][r + 2].re, y[j][1]);
+            }
+        }
+    } else {
+        for (int j = 0; j < ncols; ++j) {
+            long long rr = r;
+            for (; rr + 2 <= r1; rr += 2) {
+                __m256d y = _mm256_loadu_pd(&col[j][rr].re);
+                for (long long c = 0; c < width; ++c) {
+                    __m256d l = _mm256_loadu_pd(&panel[c * order + rr].re);
+                    __m256d s = _mm256_permute_pd(l, 0x5);
+                    __m256d hr = _mm256_broadcast_sd(&h[j][c].re), hi = _mm256_broadcast_sd(&h[j][c].im);
+                    y = _mm256_sub_pd(y, _mm256_addsub_pd(_mm256_mul_pd(hr, l), _mm256_mul_pd(hi, s)));
+                }
+                _mm256_storeu_pd(&col[j][rr].re, y);
+            }
+            rows_update_scalar(&col[j], 1, &h[j], panel, order, width, rr, r1);
+        }
+        return;
+    }
+    rows_update_scalar(col, ncols, h, panel, order, width, r, r1);
+}
+static const bool kHaveAvx2 = __builtin_cpu_supports("avx2");
+#else
+static const bool kHaveAvx2 = false;
+#endif
+
+static inline void rows_update(C *const *col, int ncols, const C *const *h, const C *panel, long long order,
+                               long long width, long long r0, long long r1) {
+#if defined(__x86_64__)
+    if (kHaveAvx2) return rows_update_avx2(col, ncols, h, panel, order, width, r0, r1);
+#endif
+    rows_update_scalar(col, ncols, h, panel, order, width, r0, r1);
+}
+
+// Trailing columns [c0, c1) after the panel [start, start + width): the
+// interchanges, the panel's unit-lower forward substitution on rows
+// [start, start + width), then the rows below (dense.rs:117-136).
+static void update_trailing(C *a, long long order, long long start, long long width, const long long *piv,
+                            long long c0, long long c1) {
+    const C *panel = a + start * order;
+    const long long below = start + width;
+    std::vector<C> heads((size_t)((c1 - c0) * width));
+    for (long long col = c0; col < c1; ++col) {
+        C *y = a + col * order;
+        for (long long off = 0; off < width; ++off) std::swap(y[start + off], y[piv[off]]);
+        for (long long k = 1; k < width; ++k) {
+            C v = y[start + k];
+            for (long long c = 0; c < k; ++c) v = csub(v, cmul(y[start + c], panel[c * order + start + k]));
+            y[start + k] = v;
+        }
+        for (long long c = 0; c < width; ++c) heads[(col - c0) * width + c] = y[start + c];
+    }
+    constexpr long long kRowBlock = 256;
+    for (long long r0 = below; r0 < order; r0 += kRowBlock) {
+        long long r1 = std::min(order, r0 + kRowBlock);
+        for (long long g = c0; g < c1; g += 4) {
+            int nc = (int)std::min<long long>(4, c1 - g);
+            C *cols[4];
+            const C *hs[4];
+            for (int j = 0; j < nc; ++j) {
+                cols[j] = a + (g + j) * order;
+                hs[j] = heads.data() + (g + j - c0) * width;
+            }
+            rows_update(cols, nc, hs, panel, order, width, r0, r1);
+        }
+    }
+}
+
+// factorize_panel, dense.rs:144-189, column by column (left-looking): column
+// o first takes the interchanges and the eliminations of panel columns
+// 0..o-1 in order, which hands every entry the same operations in the same
+// order as the reference's right-looking sweep (a later interchange only
+// swaps rows below every earlier pivot row, in all columns alike).
+static bool factorize_panel(C *panel, long long order, long long start, long long width, long long *piv) {
+    const C *heads[1];
+    for (long long o = 0; o < width; ++o) {
+        C *y = panel + o * order;
+        for (long long c = 0; c < o; ++c) std::swap(y[start + c], y[piv[c]]);
+        // Rows start+1 .. start+o-1: the triangular part, then everything below
+        // takes the o eliminations at once.
+        for (long long k = 1; k < o; ++k) {
+            C v = y[start + k];
+            for (long long c = 0; c < k; ++c) v = csub(v, cmul(y[start + c], panel[c * order + start + k]));
+            y[start + k] = v;
+        }
+        if (o > 0) {
+            std::vector<C> h(y + start, y + start + o);
+            heads[0] = h.data();
+            C *cols[1] = {y};
+            rows_update(cols, 1, heads, panel, order, o, start + o, order);
+        }
+        const long long diagonal = start + o;
+        long long pivot = diagonal;
+        double largest = norm1(y[diagonal]);
+        for (long long row = diagonal + 1; row < order; ++row) {
+            double m = norm1(y[row]);
+            if (m > largest) {
+                pivot = row;
+                largest = m;
+            }
+        }
+        if (largest == 0.0) return false;
+        piv[o] = pivot;
+        if (pivot != diagonal)
+            for (long long k = 0; k <= o; ++k) std::swap(panel[k * order + diagonal], panel[k * order + pivot]);
+        C inverse = cdiv(C{1.0, 0.0}, y[diagonal]);
+        for (long long r = diagonal + 1; r < order; ++r) y[r] = cmul(y[r], inverse);
+    }
+    return true;
+}
+
 bool factorize(C *a, long long order, std::vector<long long> &pivots, int threads) {
     pivots.assign(order, 0);
     for (long long start = 0; start < order; start += kPanel) {
         long long width = std::min(kPanel, order - start);
         C *panel = a + start * order;
-        // factorize_panel, dense.rs:144-189
+        if (!factorize_panel(panel, order, start, width, pivots.data() + start)) return false;
+        const long long *piv = pivots.data() + start;
+        for (long long col = 0; col < start; ++col)
+            for (long long off = 0; off < width; ++off) std::swap(a[col * order + start + off], a[col * order + piv[off]]);
+        const long long right_begin = start + width;
+        const long long chunk = 32;
+        const long long tasks = (order - right_begin + chunk - 1) / chunk;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads) if (tasks > 1)
+        for (long long t = 0; t < tasks; ++t) {
+            long long c0 = right_begin + t * chunk;
+            update_trailing(a, order, start, width, piv, c0, std::min(order, c0 + chunk));
+        }
+    }
+    return true;
+}
+
+// The reference's column-at-a-time form (dense.rs:98-190), kept to check
+// that the blocked loops above give the same bits.
+bool factorize_plain(C *a, long long order, std::vector<long long> &pivots) {
+    pivots.assign(order, 0);
+    for (long long start = 0; start < order; start += kPanel) {
+        long long width = std::min(kPanel, order - start);
+        C *panel = a + start * order;
         for (long long c = 0; c < width; ++c) {
             long long diagonal = start + c;
             C *column = panel + c * order;
@@ -1398,9 +1584,7 @@ bool factorize(C *a, long long order, std::vector<long long> &pivots, int thread
             for (long long off = 0; off < width; ++off) std::swap(column[start + off], column[piv[off]]);
         };
         for (long long col = 0; col < start; ++col) interchange(a + col * order);
-        long long right_begin = start + width;
-#pragma omp parallel for schedule(static) num_threads(threads) if (order - right_begin > 8)
-        for (long long col = right_begin; col < order; ++col) {
+        for (long long col = start + width; col < order; ++col) {
             C *column = a + col * order;
             interchange(column);
             for (long long c = 0; c < width; ++c) {
@@ -1412,10 +1596,10 @@ bool factorize(C *a, long long order, std::vector<long long> &pivots, int thread
     return true;
 }
 
-int lu_solve(C *a, long long order, C *x, long long nrhs, int threads) {
+int lu_solve(C *a, long long order, C *x, long long nrhs, int threads, bool plain = false) {
     if (order == 0) return ORC_OK;
     std::vector<long long> pivots;
-    if (!factorize(a, order, pivots, threads)) return ORC_ERR_SINGULAR;
+    if (!(plain ? factorize_plain(a, order, pivots) : factorize(a, order, pivots, threads))) return ORC_ERR_SINGULAR;
 #pragma omp parallel for schedule(static) num_threads(threads) if (nrhs > 1)
     for (long long r = 0; r < nrhs; ++r) {
         C *rhs = x + r * order;
@@ -1603,6 +1787,10 @@ int orc_fill_frozen_rows(const double *nominal, const double *perturbed, long lo
 
 int orc_lu_solve(double *a, long long n, double *b, long long nrhs, int threads) {
     return lu_solve(reinterpret_cast<C *>(a), n, reinterpret_cast<C *>(b), nrhs, threads);
+}
+
+int orc_lu_solve_plain(double *a, long long n, double *b, long long nrhs) {
+    return lu_solve(reinterpret_cast<C *>(a), n, reinterpret_cast<C *>(b), nrhs, 1, true);
 }
 
 int orc_system_assemble(const double *nodes, long long nnode, const orc_segment *segs, long long nseg,

@@ -78,6 +78,7 @@ def lib():
         L.orc_separation.restype = ctypes.c_double
         L.orc_fill.argtypes = [dp, ctypes.c_longlong, dp, ctypes.POINTER(ctypes.c_byte), ctypes.c_int, lp, lp]
         L.orc_lu_solve.argtypes = [dp, ctypes.c_longlong, dp, ctypes.c_longlong, ctypes.c_int]
+        L.orc_lu_solve_plain.argtypes = [dp, ctypes.c_longlong, dp, ctypes.c_longlong]
         L.orc_fill_frozen.argtypes = [dp, dp, ctypes.c_longlong, dp, ctypes.c_int]
         L.orc_fill_frozen_rows.argtypes = [dp, dp, ctypes.c_longlong, lp, ctypes.c_longlong, dp, ctypes.c_int]
         L.orc_system_assemble.argtypes = [dp, ctypes.c_longlong, ctypes.POINTER(Segment), ctypes.c_longlong,
@@ -275,16 +276,21 @@ def fill_frozen_rows(nominal: np.ndarray, perturbed: np.ndarray, rows: Sequence[
     return out
 
 
-def lu_solve(a: np.ndarray, b: np.ndarray, threads: Optional[int] = None) -> np.ndarray:
-    """Solve a x = b with the reference's blocked partial-pivoting LU (complex)."""
+def lu_solve(a: np.ndarray, b: np.ndarray, threads: Optional[int] = None, plain: bool = False) -> np.ndarray:
+    """Solve a x = b with the reference's blocked partial-pivoting LU (complex).
+
+    ``plain=True`` runs the reference's column-at-a-time sweeps (dense.rs:98-190)
+    on one thread; the default runs the same per-entry operations in cache
+    blocks on all threads, and both give the same bits."""
     a = np.array(a, dtype=np.complex128, order="F", copy=True)
     b2 = np.array(b, dtype=np.complex128, order="F", copy=True)
     if b2.ndim == 1:
         b2 = b2.reshape(-1, 1, order="F")
     n = a.shape[0]
-    st = lib().orc_lu_solve(a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n,
-                            b2.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), b2.shape[1],
-                            threads or default_threads())
+    if plain:
+        st = lib().orc_lu_solve_plain(_dp(a), n, _dp(b2), b2.shape[1])
+    else:
+        st = lib().orc_lu_solve(_dp(a), n, _dp(b2), b2.shape[1], threads or default_threads())
     _check(st, "lu_solve")
     return b2.reshape(b.shape) if np.ndim(b) == 1 else b2
 

@@ -4,9 +4,11 @@ all belongs to its own pool, or a loop that must not cudaMalloc/cudaFree).
 
 The caller owns the device buffers (here: torch tensors); the entry point
 itself allocates nothing and keeps its scratch in a fixed device array.  Its
-result must equal the allocating entry point's (fh_lu_solve_c64) within the
-LU tests' tolerance, on two calls in a row (the second call sees the array
-the first one left behind).  This file is collected last on purpose.
+result must equal the allocating entry point's (fh_lu_solve_c64) and
+numpy.linalg.solve within the LU tests' tolerance, on two calls in a row (the
+second call sees the array the first one left behind), and the device's free
+memory must not move across its calls.  This file is collected last on
+purpose.
 """
 import ctypes
 
@@ -42,14 +44,24 @@ def _from_device(t, rows, cols):
     return flat.reshape(cols, rows).T
 
 
-def test_noalloc_lu_matches_allocating_lu_twice(fh):
+def _system(n, nrhs, seed):
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    b = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
+    return a, b
+
+
+def _rel(got, want):
+    return np.max(np.abs(got - want)) / np.max(np.abs(want))
+
+
+def test_noalloc_lu_matches_allocating_lu_and_numpy_twice(fh):
     import torch
     N, fn = _lib()
     for call, (n, nrhs) in enumerate([(300, 2), (129, 1)]):
-        rng = np.random.default_rng(100 + call)
-        a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
-        b = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
-        want = fh.lu_solve(a, b)  # the allocating entry point
+        a, b = _system(n, nrhs, 100 + call)
+        want = np.linalg.solve(a, b)
+        alloc = fh.lu_solve(a, b)  # the allocating entry point
         da = _device_complex(torch, a)
         db = _device_complex(torch, b)
         torch.cuda.synchronize()
@@ -58,7 +70,34 @@ def test_noalloc_lu_matches_allocating_lu_twice(fh):
         assert st == N.OK, N.last_error()
         torch.cuda.synchronize()
         got = _from_device(db, n, nrhs)
-        assert np.max(np.abs(got - want)) / np.max(np.abs(want)) < RTOL
+        assert _rel(got, want) < RTOL
+        assert _rel(got, alloc) < RTOL
+
+
+def test_noalloc_lu_leaves_device_memory_untouched(fh):
+    """No cudaMalloc (the driver's free memory stays put) and nothing taken from
+    the library's own pool (its idle memory is released first, so a pool
+    allocation would have to map new memory)."""
+    import torch
+    N, fn = _lib()
+    n, nrhs = 2000, 3
+    a, b = _system(n, nrhs, 7)
+    want = np.linalg.solve(a, b)
+    # Set-up call: loads the kernels and looks up the scratch array's address.
+    da, db = _device_complex(torch, a), _device_complex(torch, b)
+    info = N.ErrorInfo()
+    assert fn(da.data_ptr(), n, db.data_ptr(), nrhs, None, ctypes.byref(info)) == N.OK, N.last_error()
+    inputs = [(_device_complex(torch, a), _device_complex(torch, b)) for _ in range(2)]
+    torch.cuda.synchronize()
+    fh.release_cached_memory()
+    free_before = torch.cuda.mem_get_info()[0]
+    for da, db in inputs:
+        assert fn(da.data_ptr(), n, db.data_ptr(), nrhs, None, ctypes.byref(info)) == N.OK, N.last_error()
+    torch.cuda.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    assert free_after == free_before
+    for _, db in inputs:
+        assert _rel(_from_device(db, n, nrhs), want) < RTOL
 
 
 def test_noalloc_rejects_orders_beyond_the_limit():

@@ -61,7 +61,8 @@ UNIT = "s"
 
 def _workload(name):
     from fasterhenry_b200 import fixtures as F
-    return {"metric": F.metric_meander, "c2": F.c2_meander, "c1": F.c1_spiral}[name]()
+    return {"metric": F.metric_meander, "metric_odd": F.metric_meander_odd, "c2": F.c2_meander,
+            "c1": F.c1_spiral}[name]()
 
 
 WORKLOADS = {
@@ -73,6 +74,8 @@ WORKLOADS = {
            "skin-depth graded at 1 GHz (cells <= 0.1 skin depth, ratio 1.4: 3,672 filaments), dZ/dp for the "
            "24 widths and 24 thicknesses at 1 GHz", None),
     "metric": ("meander 167 legs, 10,020 filaments, m = 9,686, 32 freqs 1e5-1e10 Hz", lambda: _workload("metric")),
+    "metric_odd": ("meander 167 legs with one segment at 29 x 1, 10,019 filaments, m = 9,685 (odd), "
+                   "32 freqs 1e5-1e10 Hz", lambda: _workload("metric_odd")),
     "c2": ("meander 40 legs, 2,400 filaments, m = 2,320, 32 freqs 1e5-1e10 Hz", lambda: _workload("c2")),
     "c1": ("4-turn spiral, 240 filaments, m = 224, 10 freqs 1e6-1e10 Hz", lambda: _workload("c1")),
 }
@@ -312,7 +315,7 @@ def run_ours(args):
     }
     if rank == 0 and world == 1:
         out["fp64_library_lu"] = library_fp64_lu(system, freqs, counts)
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and args.config == "metric":
         out["cpu_baseline"] = cpu_baseline(args, z64, zs)
         for key in ("max_rel_err_fp64_vs_oracle", "max_rel_err_mixed_vs_oracle"):
             if key in out["cpu_baseline"]:
@@ -493,7 +496,7 @@ def run_c5(args):
                    "near_entries": stats["near_entries"], "l2": "FFT grids of %.0f MB each >> L2 (no flush)"
                    % (16 * np.prod(stats["fft_dims"]) / 1e6)},
         "assemble_s": round(assemble_s, 3), "setup_host_s": round(stats["setup_host_s"], 3),
-        "setup_device_s": round(stats["setup_device_s"], 3),
+        "setup_device_s": round(stats["setup_device_s"], 3), "setup_near_s": round(stats["setup_near_s"], 3),
         "gmres": {"iterations": outcome.iterations, "relative_residual": outcome.relative_residual},
         "z_ohm": [float(z[0, 0].real), float(z[0, 0].imag)],
         "subset_9800_rel_err_vs_dense": subset_rel,

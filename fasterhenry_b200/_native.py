@@ -78,7 +78,7 @@ class PfftStats(ctypes.Structure):
     _fields_ = [("filaments", ctypes.c_int64), ("grid_spacing", ctypes.c_double), ("grid_dims", ctypes.c_int64 * 3),
                 ("fft_dims", ctypes.c_int64 * 3), ("projection_entries", ctypes.c_int64),
                 ("near_entries", ctypes.c_int64), ("memory_bytes", ctypes.c_int64), ("setup_host_s", ctypes.c_double),
-                ("setup_device_s", ctypes.c_double)]
+                ("setup_device_s", ctypes.c_double), ("setup_near_s", ctypes.c_double)]
 
 
 class GmresParams(ctypes.Structure):
@@ -133,12 +133,12 @@ EXPORTS = [
     "fh_profile_read", "fh_pfft_default_params", "fh_pfft_create", "fh_pfft_apply", "fh_pfft_get_stats",
     "fh_pfft_destroy", "fh_gmres_default_params", "fh_iterative_create", "fh_iterative_counts", "fh_iterative_timing",
     "fh_iterative_pfft_stats", "fh_iterative_sweep", "fh_iterative_destroy", "fh_test_gmres_dense",
-    "fh_batch_sweep", "fh_gradient", "fh_test_inductance_gradient", "fh_release_cached_memory",
+    "fh_batch_sweep", "fh_gradient", "fh_test_inductance_gradient", "fh_release_cached_memory", "fh_test_near_pairs",
     "fh_system_layout", "fh_currents", "fh_system_create_coupled", "fh_system_coupling",
 ]
 
 PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner",
-                   "pfft_apply", "panel_solve", "form"]
+                   "pfft_apply", "panel_solve", "form", "solve_flow", "solve_barrier"]
 
 
 class FillStats(ctypes.Structure):
@@ -211,6 +211,7 @@ def load():
     L.fh_gradient.argtypes = [ctypes.c_void_p, ctypes.c_double, P(ParamSpec), sz, c_double_p, c_double_p,
                               P(GradientReport), ei]
     L.fh_test_inductance_gradient.argtypes = [P(Filament), c_double_p, sz, c_double_p, c_double_p, ei]
+    L.fh_test_near_pairs.argtypes = [P(Filament), sz, ctypes.c_double, c_int64_p, c_int64_p, sz, P(sz), ei]
     L.fh_system_layout.argtypes = [ctypes.c_void_p, c_int64_p, c_int64_p, c_int64_p]
     L.fh_system_create_coupled.argtypes = [P(Node), sz, P(SegmentDef), sz, P(Port), sz, P(Discretization),
                                            P(CouplingSpec), ctypes.c_int, P(ctypes.c_void_p), ei]

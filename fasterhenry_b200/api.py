@@ -924,6 +924,29 @@ def inductance_gradient(filaments: np.ndarray, tangents: np.ndarray) -> Tuple[np
     return dw, dh
 
 
+def near_pairs(filaments: np.ndarray, radius: float) -> Tuple[np.ndarray, np.ndarray]:
+    """The device near-pair search of the pFFT set-up on its own
+    (fh_test_near_pairs, pfft/near.rs:41-106): for each filament i the
+    filaments j >= i within `radius` (separating-axis gap) whose directions
+    are not orthogonal, ascending.  Returns (off, cols) as CSR arrays."""
+    f = np.ascontiguousarray(filaments, dtype=np.float64).reshape(-1, FILAMENT_FIELDS)
+    fil = _fil_array(f)
+    n = len(f)
+    off = np.zeros(n + 1, dtype=np.int64)
+    total = ctypes.c_size_t(0)
+    cap = max(64 * n, 1)
+    for _ in range(2):
+        cols = np.zeros(cap, dtype=np.int64)
+        info = N.ErrorInfo()
+        _check(N.load().fh_test_near_pairs(fil, n, float(radius), off.ctypes.data_as(N.c_int64_p),
+                                           cols.ctypes.data_as(N.c_int64_p), cap, ctypes.byref(total),
+                                           ctypes.byref(info)), info)
+        if total.value <= cap:
+            return off, cols[:total.value]
+        cap = total.value
+    raise RuntimeError("near_pairs: capacity")
+
+
 def solve(geometry, ports: Sequence, discretization: dict, frequencies: Sequence[float],
           precision: Precision = Precision.FP64, solver: SolverChoice = SolverChoice.DENSE,
           iterative: Optional[IterativeParams] = None) -> SweepResult:
@@ -1040,7 +1063,7 @@ class PfftOperator:
                 "grid_dims": [int(v) for v in s.grid_dims], "fft_dims": [int(v) for v in s.fft_dims],
                 "projection_entries": int(s.projection_entries), "near_entries": int(s.near_entries),
                 "memory_bytes": int(s.memory_bytes), "setup_host_s": float(s.setup_host_s),
-                "setup_device_s": float(s.setup_device_s)}
+                "setup_device_s": float(s.setup_device_s), "setup_near_s": float(s.setup_near_s)}
 
 
 @dataclasses.dataclass(frozen=True)
@@ -1130,7 +1153,7 @@ class IterativeSystem:
                 "grid_dims": [int(v) for v in s.grid_dims], "fft_dims": [int(v) for v in s.fft_dims],
                 "projection_entries": int(s.projection_entries), "near_entries": int(s.near_entries),
                 "memory_bytes": int(s.memory_bytes), "setup_host_s": float(s.setup_host_s),
-                "setup_device_s": float(s.setup_device_s)}
+                "setup_device_s": float(s.setup_device_s), "setup_near_s": float(s.setup_near_s)}
 
     def sweep(self, frequencies: Sequence[float]) -> SweepResult:
         f = np.ascontiguousarray(frequencies, dtype=np.float64)

@@ -316,20 +316,28 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     PBuf<double> r, rnorm, bnorm, dnorm, xnorm;
     PBuf<int> piv, sing;
     const int64_t vec = m * p;  // complex entries per frequency
+    // The FP32 system is factored at an even order mo: an odd Z_ee is bordered
+    // by one row and column of the identity, [Z_ee 0; 0 1], whose factors are
+    // Z_ee's plus a unit pivot and whose solve leaves the extra entry at zero.
+    // The column stride is then a multiple of 16 bytes, which the tensor
+    // copies of the rows-below pass and of the dataflow solve need.
+    const int64_t mo = m + (m & 1);
+    const int64_t vec32 = mo * p;  // complex entries per frequency, FP32 corrections
     DevPool &pool = s->pool;
-    FHB_PALLOC(pool, a, kSlotA, (size_t)count * m * m * 2);
-    FHB_PALLOC(pool, d32, kSlotD32, (size_t)count * vec * 2);
+    FHB_PALLOC(pool, a, kSlotA, (size_t)count * mo * mo * 2);
+    FHB_PALLOC(pool, d32, kSlotD32, (size_t)count * vec32 * 2);
     FHB_PALLOC(pool, r, kSlotR, (size_t)count * vec * 2);
     FHB_PALLOC(pool, rnorm, kSlotRnorm, (size_t)count);
     FHB_PALLOC(pool, bnorm, kSlotBnorm, (size_t)count);
     FHB_PALLOC(pool, dnorm, kSlotDnorm, (size_t)count);
     FHB_PALLOC(pool, xnorm, kSlotXnorm, (size_t)count);
-    FHB_PALLOC(pool, piv, kSlotPiv, (size_t)count * m);
+    FHB_PALLOC(pool, piv, kSlotPiv, (size_t)count * mo);
     FHB_PALLOC(pool, sing, kSlotSing, (size_t)count);
     FHB_CUDA(cudaMemsetAsync(sing.p, 0, sizeof(int) * count, st));
     // The two-level form factors without pivoting and forms every U entry it
     // reads from L: the tiles above the diagonal are not needed.
-    fh_status e = form_system<float>(s->d_Rm, s->d_Lm, ld, m, d_omega, count, a.p, st, err, outer_for(m, mode) > 0);
+    fh_status e =
+        form_system<float>(s->d_Rm, s->d_Lm, ld, m, d_omega, count, a.p, st, err, outer_for(mo, mode) > 0, mo);
     if (e) return e;
     e = form_rhs<double>(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, r.p, st, err);  // r0 = b
     if (e) return e;
@@ -352,15 +360,15 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     PBuf<unsigned char> coop_mem;
     int per_matrix = 0;
     size_t coop_bytes = 0;
-    e = coop_plan<float>(count, m, &per_matrix, &coop_bytes, err, s->share);
+    e = coop_plan<float>(count, mo, &per_matrix, &coop_bytes, err, s->share);
     if (e) return e;
     FHB_PALLOC(pool, coop_mem, kSlotCoop, coop_bytes);
     coop_bind<float>(coop_mem.p, count, per_matrix, cs, s->share);
     w.coop = &cs;
-    const int outer = outer_for(m, mode);
+    const int outer = outer_for(mo, mode);
     // Two-level form: the inverses of every diagonal block of L and U are
     // kept for the cooperative solve; one-level form: one panel's L inverse.
-    const int64_t nblk = (m + kNbFp32 - 1) / kNbFp32;
+    const int64_t nblk = (mo + kNbFp32 - 1) / kNbFp32;
     PBuf<float> linv_mem, uinv_mem;
     FHB_PALLOC(pool, linv_mem, kSlotLinv, (size_t)count * kNbFp32 * kNbFp32 * 2 * (outer ? nblk : 1));
     w.linv = linv_mem.p;
@@ -374,19 +382,19 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
         // per 128-row block), or the barrier-based one when it does not fit.
         int flow_group = 0;
         size_t flow_bytes = 0;
-        e = flowsolve_plan(count * (int)p, m, &flow_group, &flow_bytes, err, s->share);
+        e = flowsolve_plan(count * (int)p, mo, &flow_group, &flow_bytes, err, s->share);
         if (e) return e;
         if (flow_group > 0) {
             FHB_PALLOC(pool, flow_mem, kSlotFlow, flow_bytes);
             FHB_CUDA(cudaMemsetAsync(flow_mem.p, 0, flow_bytes, st));
-            flowsolve_bind(flow_mem.p, count * (int)p, flow_group, m, fs);
+            flowsolve_bind(flow_mem.p, count * (int)p, flow_group, mo, fs);
         }
         // the dataflow solve reads U_ij as D_i L_ji^T: no U12 beyond the
         // diagonal regions is written for it
         w.upper = flow_group == 0;
         int per_group = 0;
         size_t solve_bytes = 0;
-        if (flow_group == 0) e = trisolve_plan(count * (int)p, m, &per_group, &solve_bytes, err, s->share);
+        if (flow_group == 0) e = trisolve_plan(count * (int)p, mo, &per_group, &solve_bytes, err, s->share);
         if (e) return e;
         if (per_group > 0) {
             FHB_PALLOC(pool, solve_mem, kSlotSolve, solve_bytes);
@@ -397,13 +405,13 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     PBuf<unsigned char> pack_a, pack_b, xpack;
     PBuf<float> xinv, tbuf, dvec;
     if (outer) {
-        const size_t pb = packed_operand_bytes(m - outer, outer, count);
+        const size_t pb = packed_operand_bytes(mo - outer, outer, count);
         FHB_PALLOC(pool, pack_a, kSlotPackA, pb);
         w.outer = outer;
         w.pack_a = pack_a.p;
         // the rows-below pass packs one operand for both sides of the update;
         // the separate B operand is for orders it does not take
-        if (!(panel_solve_supported(m) && (int64_t)count * m <= INT32_MAX)) {
+        if (!(panel_solve_supported(mo) && (int64_t)count * mo <= INT32_MAX)) {
             FHB_PALLOC(pool, pack_b, kSlotPackB, pb);
             w.pack_b = pack_b.p;
         }
@@ -424,7 +432,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     b.a = a.p;
     b.pivots = piv.p;
     b.singular = sing.p;
-    b.m = m;
+    b.m = mo;
     b.count = count;
     ScopedEvents<3> ev;
     cudaEvent_t e0 = ev.e[0], e1 = ev.e[1], e2 = ev.e[2];
@@ -446,7 +454,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     const int kMaxIter = 40;
     int it = 0;
     for (; it < kMaxIter; ++it) {
-        e = convert_c64_to_c32(r.p, d32.p, count * vec, st, err);
+        e = convert_c64_to_c32(r.p, d32.p, count * vec, st, err, m, mo);
         if (!e) {
             if (fs.per_group > 0)
                 e = lu_solve_flow(b, w.linv, w.uinv, d32.p, (int)p, fs, st, err);
@@ -455,11 +463,11 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
             else
                 e = lu_solve<float>(b, d32.p, (int)p, kNbFp32, st, err, outer);
         }
-        if (!e) e = add_c32_to_c64(d_x, d32.p, count * vec, st, err);
+        if (!e) e = add_c32_to_c64(d_x, d32.p, count * vec, st, err, m, mo);
         if (!e) e = residual_fp64(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, r.p, rnorm.p, st, err, res_part.p);
         if (e) return e;
         // correction and solution norms (max-abs) for the stopping rule
-        e = max_abs_per_matrix_f32(d32.p, 2 * vec, count, dnorm.p, st, err);
+        e = max_abs_per_matrix_f32(d32.p, 2 * vec32, count, dnorm.p, st, err);
         if (!e) e = max_abs_per_matrix(d_x, 2 * vec, count, xnorm.p, st, err);
         if (e) return e;
         FHB_CUDA(cudaMemcpyAsync(hd.data(), dnorm.p, 8 * count, cudaMemcpyDeviceToHost, st));

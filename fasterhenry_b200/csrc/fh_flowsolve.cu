@@ -443,10 +443,10 @@ fh_status lu_solve_flow(const LuBatch<float> &b, const void *linv, const void *u
     fh_status st = encode_column_tiles(&map, b.a, b.m, b.count, kNb, kFlowTileCols, err);
     if (st) return st;
     void *params[] = {&g, &map};
-    prof_begin(s, FH_PROF_SOLVE);
+    prof_begin(s, FH_PROF_SOLVE_FLOW);
     FHB_CUDA(cudaLaunchCooperativeKernel((const void *)flowsolve_kernel, dim3(fs.groups * fs.per_group),
                                          dim3(kFlowThreads), params, kFlowSmemBytes, s));
-    prof_end(s, FH_PROF_SOLVE, 8.0 * (double)b.m * (double)b.m * nrhs * b.count);
+    prof_end(s, FH_PROF_SOLVE_FLOW, 8.0 * (double)b.m * (double)b.m * nrhs * b.count);
     return FH_OK;
 }
 

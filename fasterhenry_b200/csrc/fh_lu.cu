@@ -987,17 +987,20 @@ __global__ void __launch_bounds__(256) form_kernel(const double *__restrict__ R,
     }
 }
 
-// FP32 form, two consecutive entries per 16-byte store (m * m even, batch
+// FP32 form, two consecutive entries per 16-byte store (mo * mo even, batch
 // 16-byte aligned).  A CTA takes kFormPer x 256 consecutive entry pairs,
 // reads their R and L once and writes them frequency by frequency, so each
 // frequency's plane receives one contiguous 16 KB run per CTA.  With
 // lower_tiles, pairs whose entries both lie in 128 x 128 tiles above the
-// diagonal are skipped.
+// diagonal are skipped.  The formed matrix has order mo >= m: entries outside
+// the leading m x m block are those of the identity (the border of an odd
+// order, see the mixed sweep).
 constexpr int kFormPer = 4;
 __global__ void __launch_bounds__(256) form_pair_kernel(const double *__restrict__ R, const double *__restrict__ L,
-                                                        int64_t ld, int64_t m, const double *__restrict__ omega,
-                                                        int count, float4 *__restrict__ a, int lower_tiles) {
-    const int64_t pairs = m * m / 2, chunk = 256 * kFormPer;
+                                                        int64_t ld, int64_t m, int64_t mo,
+                                                        const double *__restrict__ omega, int count,
+                                                        float4 *__restrict__ a, int lower_tiles) {
+    const int64_t pairs = mo * mo / 2, chunk = 256 * kFormPer;
     for (int64_t base = (int64_t)blockIdx.x * chunk; base < pairs; base += (int64_t)gridDim.x * chunk) {
         double r0[kFormPer], l0[kFormPer], r1[kFormPer], l1[kFormPer];
         bool keep[kFormPer];
@@ -1006,16 +1009,17 @@ __global__ void __launch_bounds__(256) form_pair_kernel(const double *__restrict
             const int64_t t = base + k * 256 + threadIdx.x;
             keep[k] = t < pairs;
             if (!keep[k]) continue;
-            const int64_t e = 2 * t, i = e % m, j = e / m;
-            const int64_t i1 = i + 1 == m ? 0 : i + 1, j1 = i + 1 == m ? j + 1 : j;  // entry e + 1
+            const int64_t e = 2 * t, i = e % mo, j = e / mo;
+            const int64_t i1 = i + 1 == mo ? 0 : i + 1, j1 = i + 1 == mo ? j + 1 : j;  // entry e + 1
             if (lower_tiles && (i >> 7) < (j >> 7) && (i1 >> 7) < (j1 >> 7)) {
                 keep[k] = false;
                 continue;
             }
-            r0[k] = R[i + j * ld];
-            l0[k] = L[i + j * ld];
-            r1[k] = R[i1 + j1 * ld];
-            l1[k] = L[i1 + j1 * ld];
+            const bool in0 = i < m && j < m, in1 = i1 < m && j1 < m;
+            r0[k] = in0 ? R[i + j * ld] : (i == j ? 1.0 : 0.0);
+            l0[k] = in0 ? L[i + j * ld] : 0.0;
+            r1[k] = in1 ? R[i1 + j1 * ld] : (i1 == j1 ? 1.0 : 0.0);
+            l1[k] = in1 ? L[i1 + j1 * ld] : 0.0;
         }
         for (int f = 0; f < count; ++f) {
             const double w = __ldg(omega + f);
@@ -1233,6 +1237,25 @@ __global__ void c64_to_c32_kernel(const double *__restrict__ s, float *__restric
 __global__ void add_c32_kernel(double *__restrict__ x, const float *__restrict__ d, int64_t n) {
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * n; t += (int64_t)gridDim.x * blockDim.x)
         x[t] += (double)d[t];
+}
+// The same between columns of m entries (FP64) and columns of mo > m entries
+// (FP32, the bordered system): the border entries are written as zero / not
+// read back.  t runs over the FP32 side's interleaved values.
+__global__ void c64_to_c32_border_kernel(const double *__restrict__ s, float *__restrict__ d, int64_t m, int64_t mo,
+                                         int64_t cols) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * mo * cols;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = t >> 1, col = e / mo, i = e - col * mo;
+        d[t] = i < m ? (float)s[2 * (col * m + i) + (t & 1)] : 0.0f;
+    }
+}
+__global__ void add_c32_border_kernel(double *__restrict__ x, const float *__restrict__ d, int64_t m, int64_t mo,
+                                      int64_t cols) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * m * cols;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = t >> 1, col = e / m, i = e - col * m;
+        x[t] += (double)d[2 * (col * mo + i) + (t & 1)];
+    }
 }
 template <class T>
 __global__ void max_abs_kernel(const T *__restrict__ v, int64_t per, double *__restrict__ out) {
@@ -1643,19 +1666,23 @@ fh_status lu_solve(const LuBatch<T> &b, T *xv, int nrhs, int nb, cudaStream_t s,
 
 template <class T>
 fh_status form_system(const double *Rm, const double *Lm, int64_t ld, int64_t m, const double *omega, int count, T *a,
-                      cudaStream_t s, fh_error_info *err, bool lower_tiles) {
+                      cudaStream_t s, fh_error_info *err, bool lower_tiles, int64_t mo) {
     if (m == 0) return FH_OK;
+    if (mo <= 0) mo = m;
+    if (mo < m) return fail(err, FH_ERR_INVALID_ARGUMENT, "form_system: the formed order is below the system's");
     prof_begin(s, FH_PROF_FORM);
     bool pairs = false;
-    if constexpr (sizeof(T) == 4) pairs = (m * m) % 2 == 0 && (reinterpret_cast<uintptr_t>(a) & 15) == 0;
+    if constexpr (sizeof(T) == 4) pairs = (mo * mo) % 2 == 0 && (reinterpret_cast<uintptr_t>(a) & 15) == 0;
     if (pairs)
-        form_pair_kernel<<<grid_for((m * m / 2 + kFormPer - 1) / kFormPer, 256, 148 * 16), 256, 0, s>>>(
-            Rm, Lm, ld, m, omega, count, reinterpret_cast<float4 *>(a), lower_tiles ? 1 : 0);
-    else
+        form_pair_kernel<<<grid_for((mo * mo / 2 + kFormPer - 1) / kFormPer, 256, 148 * 16), 256, 0, s>>>(
+            Rm, Lm, ld, m, mo, omega, count, reinterpret_cast<float4 *>(a), lower_tiles ? 1 : 0);
+    else if (mo == m)
         form_kernel<T><<<grid_for(m * m, 256, 148 * 16), 256, 0, s>>>(Rm, Lm, ld, m, omega, count,
                                                                        reinterpret_cast<Cx<T> *>(a));
+    else
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "form_system: a bordered system needs the paired FP32 form");
     // bytes written: every entry of every frequency (about half with lower_tiles)
-    prof_end(s, FH_PROF_FORM, (double)m * (double)m * count * 2.0 * sizeof(T));
+    prof_end(s, FH_PROF_FORM, (double)mo * (double)mo * count * 2.0 * sizeof(T));
     FHB_CUDA(cudaGetLastError());
     return FH_OK;
 }
@@ -1722,16 +1749,28 @@ fh_status schur(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64
     return FH_OK;
 }
 
-fh_status convert_c64_to_c32(const double *src, float *dst, int64_t n, cudaStream_t s, fh_error_info *err) {
+fh_status convert_c64_to_c32(const double *src, float *dst, int64_t n, cudaStream_t s, fh_error_info *err, int64_t m,
+                             int64_t mo) {
     if (!n) return FH_OK;
-    c64_to_c32_kernel<<<grid_for(2 * n, 256), 256, 0, s>>>(src, dst, n);
+    if (mo > m && m > 0) {
+        const int64_t cols = n / m;
+        c64_to_c32_border_kernel<<<grid_for(2 * mo * cols, 256), 256, 0, s>>>(src, dst, m, mo, cols);
+    } else {
+        c64_to_c32_kernel<<<grid_for(2 * n, 256), 256, 0, s>>>(src, dst, n);
+    }
     FHB_CUDA(cudaGetLastError());
     return FH_OK;
 }
 
-fh_status add_c32_to_c64(double *x, const float *d, int64_t n, cudaStream_t s, fh_error_info *err) {
+fh_status add_c32_to_c64(double *x, const float *d, int64_t n, cudaStream_t s, fh_error_info *err, int64_t m,
+                         int64_t mo) {
     if (!n) return FH_OK;
-    add_c32_kernel<<<grid_for(2 * n, 256), 256, 0, s>>>(x, d, n);
+    if (mo > m && m > 0) {
+        const int64_t cols = n / m;
+        add_c32_border_kernel<<<grid_for(2 * m * cols, 256), 256, 0, s>>>(x, d, m, mo, cols);
+    } else {
+        add_c32_kernel<<<grid_for(2 * n, 256), 256, 0, s>>>(x, d, n);
+    }
     FHB_CUDA(cudaGetLastError());
     return FH_OK;
 }
@@ -1756,9 +1795,9 @@ template fh_status lu_factor<float>(LuBatch<float> &, LuWork &, int, TrailingUpd
 template fh_status lu_solve<double>(const LuBatch<double> &, double *, int, int, cudaStream_t, fh_error_info *, int);
 template fh_status lu_solve<float>(const LuBatch<float> &, float *, int, int, cudaStream_t, fh_error_info *, int);
 template fh_status form_system<double>(const double *, const double *, int64_t, int64_t, const double *, int, double *,
-                                       cudaStream_t, fh_error_info *, bool);
+                                       cudaStream_t, fh_error_info *, bool, int64_t);
 template fh_status form_system<float>(const double *, const double *, int64_t, int64_t, const double *, int, float *,
-                                      cudaStream_t, fh_error_info *, bool);
+                                      cudaStream_t, fh_error_info *, bool, int64_t);
 template fh_status form_rhs<double>(const double *, const double *, int64_t, int64_t, int64_t, const double *, int,
                                     double *, cudaStream_t, fh_error_info *);
 template fh_status form_rhs<float>(const double *, const double *, int64_t, int64_t, int64_t, const double *, int,

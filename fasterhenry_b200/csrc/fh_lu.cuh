@@ -204,10 +204,12 @@ fh_status flowsolve_check(const FlowScratch &fs, cudaStream_t s, fh_error_info *
 // A_f = R + j w_f L for the top-left m x m block of R_m, L_m (ld = loops),
 // written as T complex into a (count x m x m).  With lower_tiles (FP32, for
 // the two-level factorization without pivoting, which forms every U entry it
-// reads from L) the 128 x 128 tiles above the diagonal are not written.
+// reads from L) the 128 x 128 tiles above the diagonal are not written.  With
+// mo > m (FP32 only) each matrix has order mo and is bordered by the identity:
+// [A_f 0; 0 I].
 template <class T>
 fh_status form_system(const double *Rm, const double *Lm, int64_t ld, int64_t m, const double *omega, int count,
-                      T *a, cudaStream_t s, fh_error_info *err, bool lower_tiles = false);
+                      T *a, cudaStream_t s, fh_error_info *err, bool lower_tiles = false, int64_t mo = 0);
 
 // Right-hand sides b_f = Z_ep (m x p) at each frequency, as T complex.
 template <class T>
@@ -228,9 +230,13 @@ fh_status residual_fp64(const double *Rm, const double *Lm, int64_t ld, int64_t 
 fh_status schur(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega, int count,
                 const double *x, double *z, cudaStream_t s, fh_error_info *err);
 
-// Elementwise helpers.
-fh_status convert_c64_to_c32(const double *src, float *dst, int64_t n_complex, cudaStream_t s, fh_error_info *err);
-fh_status add_c32_to_c64(double *x, const float *d, int64_t n_complex, cudaStream_t s, fh_error_info *err);
+// Elementwise helpers.  With mo > m, the FP64 side holds columns of m
+// entries and the FP32 side columns of mo entries (the bordered system):
+// conversion writes the border entries as zero, the addition skips them.
+fh_status convert_c64_to_c32(const double *src, float *dst, int64_t n_complex, cudaStream_t s, fh_error_info *err,
+                             int64_t m = 0, int64_t mo = 0);
+fh_status add_c32_to_c64(double *x, const float *d, int64_t n_complex, cudaStream_t s, fh_error_info *err,
+                         int64_t m = 0, int64_t mo = 0);
 fh_status max_abs_per_matrix(const double *v, int64_t per_matrix, int count, double *out, cudaStream_t s,
                              fh_error_info *err);
 fh_status max_abs_per_matrix_f32(const float *v, int64_t per_matrix, int count, double *out, cudaStream_t s,

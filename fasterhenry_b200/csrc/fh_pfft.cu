@@ -269,11 +269,32 @@ fh_status pfft_build(const fh_filament *fil, int64_t n, const PfftConfig &cfg, v
     op.P = op.padded[0] * op.padded[1] * op.padded[2];
     op.components = st.components;
 
-    // Projections, their transpose and the grid approximations of the near
-    // pairs on the device; then the exact near pairs (device fill, pair list)
-    // and the near-field matrix.
+    // Near pairs (device search), projections, their transpose and the grid
+    // approximations of the near pairs on the device; then the exact near
+    // pairs (device fill, pair list) and the near-field matrix.
+    std::vector<DevFil> hf((size_t)n);
+    for (int64_t i = 0; i < n; ++i) hf[i] = make_devfil(fil[i]);
+    DevFil *d_fil = nullptr;
+    double *d_exact = nullptr;
+    NearPairs near;
+    struct Release {
+        cudaStream_t s;
+        DevFil **fil;
+        double **exact;
+        NearPairs *near;
+        ~Release() {
+            if (*fil) cudaFree(*fil);
+            if (*exact) cudaFree(*exact);
+            near_pairs_free(*near, s);
+        }
+    } release{s, &d_fil, &d_exact, &near};
+    FHB_CUDA(upload(&d_fil, hf, s));
+    const double tn = now_s();
+    e = near_pairs_device(d_fil, n, st.radius, s, near, err);
+    if (e) return e;
+    op.setup_near_s = now_s() - tn;
     PfftDeviceSetup ds;
-    e = pfft_device_setup(st, fil, s, ds, err);
+    e = pfft_device_setup(st, fil, near, s, ds, err);
     op.d_proj_off = ds.proj_off;
     op.d_proj_idx = ds.proj_idx;
     op.d_proj_w = ds.proj_w;
@@ -288,38 +309,15 @@ fh_status pfft_build(const fh_filament *fil, int64_t n, const PfftConfig &cfg, v
     } free_grid{ds.pair_grid};
     if (e) return e;
     op.projection_entries = ds.entries;
-    const int64_t np = (int64_t)st.pair_i.size();
-    {
-        std::vector<DevFil> hf((size_t)n);
-        for (int64_t i = 0; i < n; ++i) hf[i] = make_devfil(fil[i]);
-        std::vector<int2> pairs((size_t)np);
-        for (int64_t k = 0; k < np; ++k) pairs[k] = make_int2(st.pair_i[k], st.pair_j[k]);
-        DevFil *d_fil = nullptr;
-        int2 *d_pairs = nullptr;
-        double *d_exact = nullptr, *d_cos = nullptr;
-        struct Free {
-            void *a, *b, *c, *d;
-            ~Free() {
-                for (void *q : {a, b, c, d})
-                    if (q) cudaFree(q);
-            }
-        } guard{nullptr, nullptr, nullptr, nullptr};
-        FHB_CUDA(upload(&d_fil, hf, s));
-        guard.a = d_fil;
-        FHB_CUDA(upload(&d_pairs, pairs, s));
-        guard.b = d_pairs;
-        FHB_CUDA(cudaMalloc(&d_exact, sizeof(double) * std::max<int64_t>(np, 1)));
-        guard.c = d_exact;
-        FHB_CUDA(upload(&d_cos, st.pair_cos, s));
-        guard.d = d_cos;
-        if (np) {
-            e = device_fill_pairs(d_fil, n, d_pairs, np, d_exact, s, nullptr, err);
-            if (e) return e;
-        }
-        e = pfft_near_csr(n, np, d_pairs, d_exact, ds.pair_grid, d_cos, s, &op.d_near_off, &op.d_near_col,
-                          &op.d_near_val, &op.near_entries, err);
+    const int64_t np = near.count;
+    FHB_CUDA(cudaMalloc(&d_exact, sizeof(double) * std::max<int64_t>(np, 1)));
+    if (np) {
+        e = device_fill_pairs(d_fil, n, near.pairs, np, d_exact, s, nullptr, err);
         if (e) return e;
     }
+    e = pfft_near_csr(n, np, near.pairs, d_exact, ds.pair_grid, near.cos, s, &op.d_near_off, &op.d_near_col,
+                      &op.d_near_val, &op.near_entries, err);
+    if (e) return e;
     FHB_CUDA(upload(&op.d_dir, st.directions, s));
 
     // Kernel spectrum.

@@ -1,8 +1,8 @@
 // Internal declarations of the precorrected-FFT operator (pfft/mod.rs,
-// grid.rs, fft.rs, near.rs of the reference).  The set-up runs on the host
-// (fh_pfft_setup.cpp), except the exact partial inductance of the near pairs,
-// which the device fill evaluates; the products run on the device
-// (fh_pfft.cu).
+// grid.rs, fft.rs, near.rs of the reference).  The host chooses the grid
+// (fh_pfft_setup.cpp); the near-pair search (fh_near.cu), the projections and
+// precorrection (fh_pfft_setup.cu), the exact near pairs (the device fill)
+// and the products (fh_pfft.cu) run on the device.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -14,6 +14,8 @@
 
 namespace fhb {
 
+struct DevFil;
+
 // Uniform grid (grid.rs:44-95): point (i, j, k) at origin + h (i, j, k),
 // linear index (i dims[1] + j) dims[2] + k.
 struct PfftGrid {
@@ -24,9 +26,8 @@ struct PfftGrid {
     int64_t len() const { return dims[0] * dims[1] * dims[2]; }
 };
 
-// The host part of the set-up: the grid, the near-field radius, the
-// non-orthogonal near pairs i <= j (row-major by i, pair_off[i] the first
-// pair of row i) with cos(i, j), and the filament directions.
+// The host part of the set-up: the grid, the near-field radius and the
+// filament directions.
 struct PfftSetup {
     int64_t n = 0;
     PfftGrid grid;
@@ -34,10 +35,22 @@ struct PfftSetup {
     double radius = 0.0;
     std::vector<double> directions;  // 3 n, unit length vectors
     std::vector<int> components;     // Cartesian components some direction carries
-    std::vector<int64_t> pair_off;
-    std::vector<int32_t> pair_i, pair_j;
-    std::vector<double> pair_cos;
 };
+
+// The near pairs on the device (fh_near.cu): for each filament i the
+// filaments j >= i (i included) whose separating-axis gap is below the radius
+// and whose directions are not orthogonal, as CSR rows ascending in j
+// (off[n + 1], pairs (i, j) and their direction cosines).  Memory from the
+// device cache; release with near_pairs_free.
+struct NearPairs {
+    int64_t n = 0, count = 0;
+    int64_t *off = nullptr;
+    int2 *pairs = nullptr;
+    double *cos = nullptr;
+};
+fh_status near_pairs_device(const DevFil *d_fil, int64_t n, double radius, cudaStream_t s, NearPairs &out,
+                            fh_error_info *err);
+void near_pairs_free(NearPairs &p, cudaStream_t s);
 
 // Parameters (PfftParams, pfft/mod.rs:183-232), validated.
 struct PfftConfig {
@@ -59,7 +72,8 @@ inline int64_t padded_size(int64_t n) { return smooth_size(2 * n - 1); }
 // pfft/mod.rs:614-631).
 double auto_spacing(const double extent[3], double cells);
 
-// Validates the parameters and builds the grid and the near pairs.
+// Validates the parameters and builds the grid (the near pairs are found on
+// the device, near_pairs_device).
 fh_status pfft_setup(const fh_filament *fil, int64_t n, const PfftConfig &cfg, PfftSetup &out, fh_error_info *err);
 
 // Projection quadrature (grid.rs:38-40): tolerance and largest order.
@@ -80,8 +94,8 @@ struct PfftDeviceSetup {
     double *pair_grid = nullptr;  // one per near pair
     int64_t entries = 0;
 };
-fh_status pfft_device_setup(const PfftSetup &st, const fh_filament *fil, cudaStream_t stream, PfftDeviceSetup &out,
-                            fh_error_info *err);
+fh_status pfft_device_setup(const PfftSetup &st, const fh_filament *fil, const NearPairs &near, cudaStream_t stream,
+                            PfftDeviceSetup &out, fh_error_info *err);
 // The near-field matrix: mirrored rows of exact - mu0/4pi cos grid for the
 // near pairs (d_exact, d_grid, d_cos per pair; pair lists on the device),
 // each row ascending in column (near.rs:263-298).
@@ -117,7 +131,7 @@ struct PfftDevice {
     void *stream = nullptr;                  // cudaStream_t
     bool own_stream = false;
     int64_t projection_entries = 0, near_entries = 0;
-    double setup_host_s = 0, setup_device_s = 0;
+    double setup_host_s = 0, setup_device_s = 0, setup_near_s = 0;  // setup_near_s: the near-pair search (part of the device time)
     PfftDevice() = default;
     PfftDevice(const PfftDevice &) = delete;
     PfftDevice &operator=(const PfftDevice &) = delete;

@@ -107,6 +107,7 @@ fh_status fh_pfft_get_stats(const fh_pfft *op, fh_pfft_stats *stats) {
     stats->memory_bytes = (int64_t)d.memory_bytes();
     stats->setup_host_s = d.setup_host_s;
     stats->setup_device_s = d.setup_device_s;
+    stats->setup_near_s = d.setup_near_s;
     return FH_OK;
 }
 

@@ -368,8 +368,8 @@ fh_status upload_constants(fh_error_info *err) {
 
 }  // namespace
 
-fh_status pfft_device_setup(const PfftSetup &st, const fh_filament *fil, cudaStream_t s, PfftDeviceSetup &out,
-                            fh_error_info *err) {
+fh_status pfft_device_setup(const PfftSetup &st, const fh_filament *fil, const NearPairs &near, cudaStream_t s,
+                            PfftDeviceSetup &out, fh_error_info *err) {
     out = PfftDeviceSetup();
     const int64_t n = st.n;
     if (n == 0) return FH_OK;
@@ -485,19 +485,13 @@ fh_status pfft_device_setup(const PfftSetup &st, const fh_filament *fil, cudaStr
     FHB_CUDA(cub::DeviceScan::ExclusiveSum(d_tg, tg, reinterpret_cast<int64_t *>(d_gcount), out.spread_off,
                                            (int)(G + 1), s));
     // Grid approximations of the near pairs.
-    const int64_t np = (int64_t)st.pair_i.size();
+    const int64_t np = near.count;
     FHB_CUDA(persist(&out.pair_grid, (size_t)np));
     if (np) {
-        std::vector<int2> pairs((size_t)np);
-        for (int64_t k = 0; k < np; ++k) pairs[(size_t)k] = make_int2(st.pair_i[(size_t)k], st.pair_j[(size_t)k]);
-        int2 *d_pairs;
-        int64_t *d_poff;
+        const int2 *d_pairs = near.pairs;
+        const int64_t *d_poff = near.off;
         int *d_reach;
-        FHB_CUDA(tmp.get(&d_pairs, (size_t)np));
-        FHB_CUDA(tmp.get(&d_poff, (size_t)n + 1));
         FHB_CUDA(tmp.get(&d_reach, 4));
-        FHB_CUDA(cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(int2) * np, cudaMemcpyHostToDevice, s));
-        FHB_CUDA(cudaMemcpyAsync(d_poff, st.pair_off.data(), 8 * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
         FHB_CUDA(cudaMemsetAsync(d_reach, 0, 16, s));
         reach_kernel<<<blocks(np, 256), 256, 0, s>>>(d_pairs, np, d_lohi, d_reach);
         FHB_CUDA(cudaGetLastError());

@@ -249,10 +249,10 @@ fh_status lu_solve_inv(const LuBatch<float> &b, const void *linv, const void *ui
     g.bar = ss.barrier;
     g.error = ss.error;
     void *params[] = {&g};
-    prof_begin(s, FH_PROF_SOLVE);
+    prof_begin(s, FH_PROF_SOLVE_BARRIER);
     FHB_CUDA(cudaLaunchCooperativeKernel((const void *)trisolve_kernel, dim3(ss.groups * ss.per_group), dim3(kThreads),
                                          params, 0, s));
-    prof_end(s, FH_PROF_SOLVE, 8.0 * (double)b.m * (double)b.m * nrhs * b.count);
+    prof_end(s, FH_PROF_SOLVE_BARRIER, 8.0 * (double)b.m * (double)b.m * nrhs * b.count);
     return FH_OK;
 }
 

@@ -436,6 +436,15 @@ fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *
 fh_status fh_test_inductance_gradient(const fh_filament *filaments, const double *tangents, size_t n, double *Dw,
                                       double *Dh, fh_error_info *err);
 
+/* Test hook: the device near-pair search of the precorrected-FFT set-up
+ * (pfft/near.rs:41-106) for a filament set and a radius in metres: for each
+ * filament i the filaments j >= i (i included) with a separating-axis gap
+ * below the radius and non-orthogonal directions, ascending.  off: n + 1
+ * row offsets; cols: capacity `cap` column indices; *total: the pair count
+ * (may exceed cap, then only off is complete). */
+fh_status fh_test_near_pairs(const fh_filament *filaments, size_t n, double radius, int64_t *off, int64_t *cols,
+                             size_t cap, size_t *total, fh_error_info *err);
+
 /* Fill statistics of an assembled system: pairs per method and device time
  * per fill kernel (no reference counterpart; diagnostics). */
 typedef struct fh_fill_stats {
@@ -474,7 +483,9 @@ typedef enum fh_profile_class {
     FH_PROF_PFFT_APPLY = 9,     /* one precorrected-FFT product (near field, spread, FFTs, interpolation) */
     FH_PROF_PANEL_SOLVE = 10,   /* rows below a super-panel: L21 = A21 U^-1, U12 and the packed operands */
     FH_PROF_FORM = 11,          /* the sweep's systems R + jwL (and right-hand sides) formed from R_m, L_m */
-    FH_PROF_CLASSES = 12
+    FH_PROF_SOLVE_FLOW = 12,    /* dataflow forward/backward solve of the two-level factors (flags per block) */
+    FH_PROF_SOLVE_BARRIER = 13, /* barrier-based forward/backward solve of the two-level factors */
+    FH_PROF_CLASSES = 14
 } fh_profile_class;
 
 void fh_profile_enable(int32_t on);
@@ -526,8 +537,9 @@ typedef struct fh_pfft_stats {
     int64_t projection_entries;
     int64_t near_entries;
     int64_t memory_bytes;
-    double setup_host_s;   /* grid, projections, near pairs, grid precorrection */
-    double setup_device_s; /* exact near pairs, kernel spectrum, uploads */
+    double setup_host_s;   /* parameters and the grid (host) */
+    double setup_device_s; /* near-pair search, projections, precorrection, exact near pairs, kernel spectrum */
+    double setup_near_s;   /* the near-pair search alone (part of setup_device_s) */
 } fh_pfft_stats;
 
 typedef struct fh_pfft fh_pfft;

@@ -1740,6 +1740,85 @@ int orc_fill(const double *filaments, long long n, double *L, signed char *metho
     return fill_matrix(f, L, methods, threads, ei, ej);
 }
 
+// near_pairs, pfft/near.rs:41-106: for each filament i the filaments j >= i
+// (i itself included) whose separating-axis gap is below `radius`, found
+// through uniform bins over the filaments' bounding boxes, ascending in j.
+// Output in CSR form: off[n + 1], cols (capacity `cap`; the total count is
+// returned through *total even when it exceeds cap).
+int orc_near_pairs(const double *filaments, long long n, double radius, long long *off, long long *cols,
+                   long long cap, long long *total) {
+    *total = 0;
+    off[0] = 0;
+    if (n == 0) return ORC_OK;
+    std::vector<Bar> bars((size_t)n);
+    std::vector<V3> blo((size_t)n), bhi((size_t)n);
+    for (long long i = 0; i < n; ++i) {
+        bars[i] = make_bar(load_fil(filaments + 19 * i));
+        V3 reach{0.0, 0.0, 0.0};
+        for (int k = 0; k < 3; ++k) {
+            V3 a = bars[i].axes[k];
+            reach = add(reach, V3{std::fabs(a.x) * bars[i].half[k], std::fabs(a.y) * bars[i].half[k],
+                                  std::fabs(a.z) * bars[i].half[k]});
+        }
+        blo[i] = sub(bars[i].centre, reach);
+        bhi[i] = add(bars[i].centre, reach);
+    }
+    double lo[3] = {blo[0].x, blo[0].y, blo[0].z}, hi[3] = {bhi[0].x, bhi[0].y, bhi[0].z};
+    for (long long i = 0; i < n; ++i) {
+        const double a[3] = {blo[i].x, blo[i].y, blo[i].z}, b[3] = {bhi[i].x, bhi[i].y, bhi[i].z};
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = std::min(lo[k], a[k]);
+            hi[k] = std::max(hi[k], b[k]);
+        }
+    }
+    const double ext[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+    double size = std::max(std::max(radius, std::max(ext[0], std::max(ext[1], ext[2])) * 1e-9),
+                           std::numeric_limits<double>::min());
+    long long dims[3];
+    auto set_dims = [&]() {
+        for (int k = 0; k < 3; ++k) dims[k] = (long long)std::floor(ext[k] / size) + 1;
+    };
+    set_dims();
+    while (dims[0] * dims[1] * dims[2] > 8 * n + 64) {
+        size *= 1.5;
+        set_dims();
+    }
+    auto cell = [&](double x, int k) {
+        double c = std::floor((x - lo[k]) / size);
+        long long v = c > 0.0 ? (long long)c : 0;
+        return std::min(v, dims[k] - 1);
+    };
+    std::vector<std::vector<long long>> bins((size_t)(dims[0] * dims[1] * dims[2]));
+    for (long long i = 0; i < n; ++i) {
+        const double a[3] = {blo[i].x, blo[i].y, blo[i].z}, b[3] = {bhi[i].x, bhi[i].y, bhi[i].z};
+        for (long long x = cell(a[0], 0); x <= cell(b[0], 0); ++x)
+            for (long long y = cell(a[1], 1); y <= cell(b[1], 1); ++y)
+                for (long long z = cell(a[2], 2); z <= cell(b[2], 2); ++z)
+                    bins[(size_t)((x * dims[1] + y) * dims[2] + z)].push_back(i);
+    }
+    long long count = 0;
+    for (long long i = 0; i < n; ++i) {
+        const double a[3] = {blo[i].x - radius, blo[i].y - radius, blo[i].z - radius};
+        const double b[3] = {bhi[i].x + radius, bhi[i].y + radius, bhi[i].z + radius};
+        std::vector<long long> found;
+        for (long long x = cell(a[0], 0); x <= cell(b[0], 0); ++x)
+            for (long long y = cell(a[1], 1); y <= cell(b[1], 1); ++y)
+                for (long long z = cell(a[2], 2); z <= cell(b[2], 2); ++z)
+                    for (long long j : bins[(size_t)((x * dims[1] + y) * dims[2] + z)])
+                        if (j >= i) found.push_back(j);
+        std::sort(found.begin(), found.end());
+        found.erase(std::unique(found.begin(), found.end()), found.end());
+        for (long long j : found)
+            if (j == i || separation(bars[i], bars[j]) < radius) {
+                if (count < cap) cols[count] = j;
+                ++count;
+            }
+        off[i + 1] = count;
+    }
+    *total = count;
+    return ORC_OK;
+}
+
 int orc_fill_frozen(const double *nominal, const double *perturbed, long long n, double *L, int threads) {
     std::vector<Fil> fn((size_t)n), fp((size_t)n);
     for (long long i = 0; i < n; ++i) {

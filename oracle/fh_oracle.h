@@ -104,6 +104,9 @@ int orc_fill_frozen_rows(const double *nominal, const double *perturbed, long lo
 /* Solve a (n x n, complex interleaved, column-major) x = b in place (b: n x nrhs).
  * Returns ORC_ERR_SINGULAR on an exactly zero pivot. */
 int orc_lu_solve(double *a, long long n, double *b, long long nrhs, int threads);
+// near_pairs (pfft/near.rs:41-106) in CSR form; *total may exceed cap.
+int orc_near_pairs(const double *filaments, long long n, double radius, long long *off, long long *cols,
+                   long long cap, long long *total);
 // The same solve through the reference's column-at-a-time sweeps on one thread
 // (dense.rs:98-190); equal bits to orc_lu_solve.
 int orc_lu_solve_plain(double *a, long long n, double *b, long long nrhs);

@@ -79,6 +79,7 @@ def lib():
         L.orc_fill.argtypes = [dp, ctypes.c_longlong, dp, ctypes.POINTER(ctypes.c_byte), ctypes.c_int, lp, lp]
         L.orc_lu_solve.argtypes = [dp, ctypes.c_longlong, dp, ctypes.c_longlong, ctypes.c_int]
         L.orc_lu_solve_plain.argtypes = [dp, ctypes.c_longlong, dp, ctypes.c_longlong]
+        L.orc_near_pairs.argtypes = [dp, ctypes.c_longlong, ctypes.c_double, lp, lp, ctypes.c_longlong, lp]
         L.orc_fill_frozen.argtypes = [dp, dp, ctypes.c_longlong, dp, ctypes.c_int]
         L.orc_fill_frozen_rows.argtypes = [dp, dp, ctypes.c_longlong, lp, ctypes.c_longlong, dp, ctypes.c_int]
         L.orc_system_assemble.argtypes = [dp, ctypes.c_longlong, ctypes.POINTER(Segment), ctypes.c_longlong,
@@ -293,6 +294,25 @@ def lu_solve(a: np.ndarray, b: np.ndarray, threads: Optional[int] = None, plain:
         st = lib().orc_lu_solve(_dp(a), n, _dp(b2), b2.shape[1], threads or default_threads())
     _check(st, "lu_solve")
     return b2.reshape(b.shape) if np.ndim(b) == 1 else b2
+
+
+def near_pairs(filaments: np.ndarray, radius: float):
+    """pfft/near.rs:41-106: for each filament i, the j >= i (i included) whose
+    separating-axis gap is below `radius`, ascending.  Returns (off, cols) as
+    CSR arrays."""
+    f = np.ascontiguousarray(filaments, dtype=np.float64)
+    n = len(f)
+    off = np.zeros(n + 1, dtype=np.int64)
+    total = ctypes.c_longlong(0)
+    cap = max(16 * n, 1)
+    for _ in range(2):
+        cols = np.zeros(cap, dtype=np.int64)
+        _check(lib().orc_near_pairs(_dp(f), n, float(radius), _lp(off), _lp(cols), cap, ctypes.byref(total)),
+               "near_pairs")
+        if total.value <= cap:
+            return off, cols[:total.value]
+        cap = total.value
+    raise RuntimeError("near_pairs: capacity")
 
 
 class System:

@@ -1,0 +1,61 @@
+"""The reference's deck fixtures (tests/golden/decks, copied from
+fasterhenry-cli/tests/data) solved on the GPU: the spiral read from the `.inp`
+deck and from the JSON document give bit-identical sweeps
+(fasterhenry-cli/tests/roundtrip.rs:18-40), both within 1e-10 of the oracle,
+with the physical checks of roundtrip.rs:42-62; the two-bar deck's 2 x 2 Z
+against the oracle."""
+import os
+
+import numpy as np
+import pytest
+
+from fasterhenry_b200 import fixtures as F
+from fasterhenry_b200 import problem as P
+
+pytestmark = pytest.mark.gpu
+
+DECKS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "decks")
+
+
+def load(name):
+    return P.load(os.path.join(DECKS, name))
+
+
+def oracle_sweep(oracle, prob, freqs):
+    deck = F.Deck(list(prob.nodes), [dict(s) for s in prob.segments], [(a, b) for a, b, _ in prob.ports],
+                  dict(prob.discretization))
+    s = oracle.System(deck)
+    return np.array([s.impedance(f) for f in freqs])
+
+
+def test_spiral_deck_and_document_solve_bit_identically(fh, oracle):
+    a, b = load("spiral.inp"), load("spiral.json")
+    za, _ = fh.run(a, fh.Precision.FP64, fh.SolverChoice.DENSE)
+    zb, _ = fh.run(b, fh.Precision.FP64, fh.SolverChoice.DENSE)
+    assert np.array_equal(za.impedance_ohm, zb.impedance_ohm)
+    assert za.ports[0].name == "spiral"
+    ref = oracle_sweep(oracle, a, a.frequencies_hz)
+    assert np.max(np.abs(za.impedance_ohm - ref) / np.abs(ref)) < 1e-10
+    # physical checks of the reference's round-trip test
+    dc, _ = fh.run(a, fh.Precision.FP64, fh.SolverChoice.DENSE, frequencies=[0.0])
+    z_dc = dc.impedance_ohm[0, 0, 0]
+    assert z_dc.imag == 0.0 and z_dc.real > 0.0
+    rf = za.impedance_ohm[3, 0, 0]
+    inductance = rf.imag / (2 * np.pi * a.frequencies_hz[3])
+    assert 5e-9 <= inductance <= 200e-9
+    assert rf.real > z_dc.real
+    # the mixed form agrees with the FP64 form
+    zm, _ = fh.run(a, fh.Precision.MIXED_BF16X3, fh.SolverChoice.DENSE)
+    assert np.max(np.abs(zm.impedance_ohm - za.impedance_ohm) / np.abs(za.impedance_ohm)) < 1e-9
+
+
+def test_twobar_deck_matches_the_oracle(fh, oracle):
+    p = load("twobar.inp")
+    res, _ = fh.run(p, fh.Precision.FP64, fh.SolverChoice.DENSE)
+    z = res.impedance_ohm
+    assert z.shape == (4, 2, 2)
+    assert [q.name for q in res.ports] == ["barA", "barB"]
+    ref = oracle_sweep(oracle, p, p.frequencies_hz)
+    assert np.max(np.abs(z - ref)) / np.max(np.abs(ref)) < 1e-10
+    assert np.max(np.abs(z[:, 0, 1] - z[:, 1, 0]) / np.abs(z[:, 0, 1])) < 1e-12
+    assert np.all(z[:, 0, 1].imag > 0)  # positive mutual inductance of parallel bars

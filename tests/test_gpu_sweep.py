@@ -169,11 +169,12 @@ def test_two_level_mixed_matches_fp64(fh, legs):
     assert all(1 <= i <= 10 for i in rm.refinement_iterations), rm.refinement_iterations
 
 
-def test_two_level_mixed_odd_order(fh):
+def test_two_level_mixed_odd_order(fh, oracle):
     """An odd order (m = 1,043: one segment of the 18-leg meander on a 29 x 1
-    grid, 28 loops instead of 29) over three super-panels: the rows below a
-    super-panel start on both even and odd element offsets, so the fused
-    pass copies its raw columns from both alignments."""
+    grid, 28 loops instead of 29) over three super-panels.  The FP32 system is
+    bordered to the even order 1,044, so the rows-below pass and the dataflow
+    solve (both need a 16-byte column stride) run as for even orders; the
+    border entry of every correction stays zero and Z matches the oracle."""
     base = F.meander_legs(18)
     grids = [(10, 3)] * base.segment_count()
     grids[5] = (29, 1)
@@ -183,9 +184,16 @@ def test_two_level_mixed_odd_order(fh):
     with fh.MeshSystem.assemble(fh.Geometry.from_deck(deck), deck.ports, deck.discretization) as s:
         assert s.counts()["internal_meshes"] == 1043
         z64 = s.sweep(freqs, fh.Precision.FP64).impedance_ohm
-        rm = s.sweep(freqs, fh.Precision.MIXED_BF16X3)
+        with fh.Profiler() as prof:
+            rm = s.sweep(freqs, fh.Precision.MIXED_BF16X3)
+            profile = prof.read()
     assert rel_err(rm.impedance_ohm, z64) < MIXED_RTOL
     assert all(1 <= i <= 10 for i in rm.refinement_iterations), rm.refinement_iterations
+    assert profile["panel_solve"]["launches"] > 0 and profile["solve_flow"]["launches"] > 0
+    assert profile["solve_barrier"]["launches"] == 0 and profile["solve"]["launches"] == 0
+    ref = oracle.System(deck)
+    for k in (0, len(freqs) - 1):
+        assert rel_err(rm.impedance_ohm[k], ref.impedance(freqs[k])) < MIXED_RTOL
 
 
 def test_two_level_mixed_strongly_coupled_loops(fh):
@@ -226,6 +234,10 @@ def test_two_level_mixed_many_ports(fh):
         c = s.counts()
         assert c["internal_meshes"] == 1044 and c["ports"] == 10
         z64 = s.sweep(freqs, fh.Precision.FP64).impedance_ohm
-        rm = s.sweep(freqs, fh.Precision.MIXED_BF16X3)
+        with fh.Profiler() as prof:
+            rm = s.sweep(freqs, fh.Precision.MIXED_BF16X3)
+            profile = prof.read()
     assert rel_err(rm.impedance_ohm, z64) < MIXED_RTOL
     assert all(1 <= i <= 10 for i in rm.refinement_iterations), rm.refinement_iterations
+    # the barrier-based solve ran (and so the rows-below pass wrote U12)
+    assert profile["solve_barrier"]["launches"] > 0 and profile["solve_flow"]["launches"] == 0

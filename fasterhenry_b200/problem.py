@@ -13,8 +13,17 @@ dialect of fasterhenry-cli/src/inp.rs:1-600 and docs/input-format.md).
   ``.default``, ``N`` nodes, ``E`` segments (``w h nwinc nhinc rw rh wx wy wz
   sigma|rho group``), ``.external``, ``.freq``, ``.equiv``, ``.couples``,
   ``.end``; ``*`` comments and ``+`` continuations; directives and node names
-  case-insensitive.  Ground planes (``G``, ``.hole``, ``.contact``) are not
-  read by this front end and are rejected with the line number.
+  case-insensitive.  Ground planes (fasterhenry-cli/src/inp.rs:53-200,
+  2410-2790, 3981-4050, 4329-4398, 4437-4650) in both ``G`` grammars: the
+  FastHenry corner-point form (``x1= .. z3= thick= seg1= seg2= sigma=|rho=
+  nhinc=``, in-plane nodes ``N<name> (x, y, z)``, ``hole rect|point|circle``,
+  ``contact rect`` in its six- and seven-value spellings, ``contact
+  decay_rect``) and the extension form (``G<name> x1 y1 z1 x2 y2 z2 t nx= ny=
+  nhinc= sigma=|rho=`` with ``.hole`` and ``.contact``); the plane meshes come
+  first in the geometry, segment and port endpoints inside a plane's slab
+  (or joined to an in-plane node) land on its nearest live cell centre, and
+  only declared nodes still referenced as themselves are kept.  Other plane
+  clauses are rejected by name with the line number.
 * :func:`load` picks the reader by file extension (``.inp``/``.fh`` decks,
   anything else JSON), and :func:`run` assembles and sweeps a problem
   (fasterhenry-cli/src/lib.rs:183-230).
@@ -29,6 +38,7 @@ import re
 from typing import Dict, List, Optional, Sequence, Tuple
 
 from . import api as A
+from . import plane as PL
 
 UNITS = {"km": 1e3, "m": 1.0, "cm": 1e-2, "mm": 1e-3, "um": 1e-6, "in": 0.0254, "mils": 2.54e-5, "mil": 2.54e-5}
 DISCRETIZATION_KINDS = ("uniform", "per_segment", "graded", "skin_depth", "per_segment_graded")
@@ -282,6 +292,240 @@ def _assignments(tokens: Sequence[str], line: int, allowed) -> Dict[str, str]:
     return out
 
 
+_PLANE_ITEM = re.compile(r"\s*(?:(?P<key>[A-Za-z_][A-Za-z0-9_]*)\s*=\s*(?P<val>[^\s(]+)|"
+                         r"(?P<group>\([^)]*\))|(?P<word>[^\s(]+))")
+
+
+def _plane_items(body: str, line: int) -> List[Tuple[str, str]]:
+    """A G statement's body as items: ("key", "k=v"), ("group", "a, b, c")
+    and ("word", w)."""
+    out: List[Tuple[str, str]] = []
+    pos = 0
+    body = body.strip()
+    while pos < len(body):
+        m = _PLANE_ITEM.match(body, pos)
+        if not m or m.end() == pos:
+            raise DeckError(line, "cannot read the ground plane statement near '%s'" % body[pos:pos + 20])
+        if m.group("key"):
+            out.append(("key", m.group("key").lower() + "=" + m.group("val")))
+        elif m.group("group"):
+            out.append(("group", m.group("group")[1:-1]))
+        else:
+            out.append(("word", m.group("word")))
+        pos = m.end()
+        while pos < len(body) and body[pos].isspace():
+            pos += 1
+    return out
+
+
+def _group_values(text: str, line: int, unit: float) -> List[float]:
+    vals = [v.strip() for v in text.split(",")]
+    if any(not v for v in vals):
+        raise DeckError(line, "an empty value in '(%s)'" % text)
+    return [_number(v, line) * unit for v in vals]
+
+
+@dataclasses.dataclass
+class _PlaneSpec:
+    name: str
+    plane: "PL.GroundPlane"
+    nhinc: int
+    line: int
+    mid_z: float
+    axis1: int = 0
+
+
+def _plane_extension(head: str, toks: List[str], line: int, unit: float, sigma_default) -> _PlaneSpec:
+    """G<name> x1 y1 z1 x2 y2 z2 t [nx=] [ny=] [nhinc=] [sigma=|rho=]
+    (inp.rs:4329-4398): footprint corners, TOP surface z, thickness down."""
+    if len(toks) < 7:
+        raise DeckError(line, "expected G<name> x1 y1 z1 x2 y2 z2 thickness [nx=..] [ny=..] [nhinc=..], or the "
+                              "FastHenry corner-point form G<name> x1=.. y1=.. z1=.. x2=.. ... thick=.. seg1=.. seg2=..")
+    x1, y1, z1, x2, y2, z2, t = [_number(v, line) * unit for v in toks[:7]]
+    vals = _assignments(toks[7:], line, {"nx", "ny", "nhinc", "sigma", "rho"})
+    nx = int(_number(vals.get("nx", "1"), line))
+    ny = int(_number(vals.get("ny", "1"), line))
+    nhinc = int(_number(vals.get("nhinc", "1"), line))
+    sigma = _plane_sigma(vals, line, unit, sigma_default, head)
+    if nx < 1 or ny < 1:
+        raise DeckError(line, "ground plane '%s' needs nx and ny >= 1 (got nx=%d, ny=%d)" % (head, nx, ny))
+    plane = PL.GroundPlane((min(x1, x2), min(y1, y2)), (max(x1, x2), max(y1, y2)), max(z1, z2), t, nx, ny, sigma)
+    return _PlaneSpec(head, plane, nhinc, line, max(z1, z2) - t / 2.0)
+
+
+def _plane_sigma(vals, line, unit, sigma_default, head):
+    if "sigma" in vals:
+        return _number(vals["sigma"], line) / unit
+    if "rho" in vals:
+        r = _number(vals["rho"], line)
+        if r <= 0:
+            raise DeckError(line, "rho must be positive")
+        return 1.0 / (r * unit)
+    if sigma_default is None:
+        raise DeckError(line, "ground plane '%s' has no conductivity: set sigma= or rho= here or in .default" % head)
+    return sigma_default
+
+
+def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_default):
+    """The FastHenry corner-point G statement (inp.rs:1686-2790) in this
+    reader's subset.  Returns the plane and its in-plane nodes
+    [(name, position)]."""
+    items = _plane_items(body, line)
+    keys: Dict[str, str] = {}
+    nodes: List[Tuple[str, Tuple[float, float, float]]] = []
+    hole_rects, hole_points, hole_circles, contact_rects, contact_decays = [], [], [], [], []
+    k = 0
+    while k < len(items):
+        kind, text = items[k]
+        if kind == "key":
+            key, val = text.split("=", 1)
+            if key in keys:
+                raise DeckError(line, "ground plane '%s' gives '%s' twice" % (head, key))
+            keys[key] = val
+            k += 1
+            continue
+        if kind == "group":
+            raise DeckError(line, "ground plane '%s': a value list '(%s)' belongs to no clause" % (head, text))
+        word = text.lower()
+        if word.startswith("n") and k + 1 < len(items) and items[k + 1][0] == "group":
+            xyz = _group_values(items[k + 1][1], line, unit)
+            if len(xyz) != 3:
+                raise DeckError(line, "in-plane node '%s' needs (x, y, z)" % text)
+            nodes.append((word, tuple(xyz)))
+            k += 2
+            continue
+        if word in ("hole", "contact"):
+            if k + 2 >= len(items) or items[k + 1][0] != "word" or items[k + 2][0] != "group":
+                raise DeckError(line, "ground plane '%s': '%s' needs a shape and its values, e.g. "
+                                      "'%s rect (x1, y1, z1, x2, y2, z2)'" % (head, word, word))
+            shape = items[k + 1][1].lower()
+            vals = _group_values(items[k + 2][1], line, 1.0)
+            k += 3
+            if word == "hole" and shape == "rect" and len(vals) == 6:
+                hole_rects.append([v * unit for v in vals])
+            elif word == "hole" and shape == "point" and len(vals) == 3:
+                hole_points.append([v * unit for v in vals])
+            elif word == "hole" and shape == "circle" and len(vals) == 4:
+                hole_circles.append([v * unit for v in vals])
+            elif word == "contact" and shape == "rect" and len(vals) == 6:
+                contact_rects.append([v * unit for v in vals])
+            elif word == "contact" and shape == "rect" and len(vals) == 7:
+                contact_decays.append(("'contact rect'", [v * unit for v in vals[:7]] + [-1.0, -1.0]))
+            elif word == "contact" and shape == "decay_rect" and len(vals) == 9:
+                v = [x * unit for x in vals[:7]] + [vals[7] * unit if vals[7] >= 0 else -1.0,
+                                                    vals[8] * unit if vals[8] >= 0 else -1.0]
+                contact_decays.append(("'contact decay_rect'", v))
+            elif word == "contact" and shape == "rect":
+                raise DeckError(line, "'contact rect' takes seven values (x, y, z, xwidth, ywidth, xcell, ycell) "
+                                      "or six (x1, y1, z1, x2, y2, z2), got %d" % len(vals))
+            else:
+                raise DeckError(line, "ground plane '%s': '%s %s' with %d values is not read by this front end "
+                                      "(supported: hole rect/point/circle, contact rect, contact decay_rect)"
+                                % (head, word, shape, len(vals)))
+            continue
+        raise DeckError(line, "ground plane '%s': '%s' is not read by this front end" % (head, text))
+    allowed = {"x1", "y1", "z1", "x2", "y2", "z2", "x3", "y3", "z3", "thick", "seg1", "seg2", "sigma", "rho",
+               "nhinc"}
+    for key in keys:
+        if key not in allowed:
+            raise DeckError(line, "ground plane '%s': '%s=' is not read by this front end" % (head, key))
+    if "sigma" in keys and "rho" in keys:
+        raise DeckError(line, "give either sigma= or rho=, not both")
+    pts = []
+    for i in (1, 2, 3):
+        p = []
+        for a in "xyz":
+            key = "%s%d" % (a, i)
+            if key not in keys:
+                raise DeckError(line, "ground plane '%s' is missing '%s' (the corner points are x1..z1, x2..z2, "
+                                      "x3..z3)" % (head, key))
+            p.append(_number(keys[key], line) * unit)
+        pts.append(p)
+    e1 = (pts[1][0] - pts[0][0], pts[1][1] - pts[0][1])
+    e2 = (pts[2][0] - pts[1][0], pts[2][1] - pts[1][1])
+    tol = 1e-9 * (abs(e1[0]) + abs(e1[1]) + abs(e2[0]) + abs(e2[1]))
+    if abs(pts[1][2] - pts[0][2]) > tol or abs(pts[2][2] - pts[0][2]) > tol:
+        raise DeckError(line, "ground plane '%s' is not parallel to the xy plane; tilted planes are not supported"
+                        % head)
+
+    def axis_of(e):
+        big = (abs(e[0]) > tol, abs(e[1]) > tol)
+        return 0 if big == (True, False) else (1 if big == (False, True) else None)
+
+    a1, a2 = axis_of(e1), axis_of(e2)
+    if a1 is None or a2 is None or a1 == a2:
+        raise DeckError(line, "ground plane '%s': the corner points do not form an axis-aligned rectangle" % head)
+    for key in ("seg1", "seg2", "thick"):
+        if key not in keys:
+            raise DeckError(line, "ground plane '%s' has no '%s'" % (head, key))
+    cells = [0, 0]
+    cells[a1] = int(_number(keys["seg1"], line))
+    cells[a2] = int(_number(keys["seg2"], line))
+    thick = _number(keys["thick"], line) * unit
+    if thick <= 0:
+        raise DeckError(line, "ground plane '%s' needs a thickness > 0" % head)
+    sigma = _plane_sigma(keys, line, unit, sigma_default, head)
+    nhinc = int(_number(keys.get("nhinc", "1"), line))
+    lo = (min(p[0] for p in pts), min(p[1] for p in pts))
+    hi = (max(p[0] for p in pts), max(p[1] for p in pts))
+    mid_z = pts[0][2]
+
+    def in_slab(what, z):
+        if abs(z - mid_z) > thick + 1e-15:
+            raise DeckError(line, "%s: z=%r is not in ground plane '%s'" % (what, z, head))
+
+    def plane_pair(pair):
+        return list(pair) if a1 == 0 else [pair[1], pair[0]]
+
+    def misses(rlo, rhi):
+        return rhi[0] < lo[0] or rlo[0] > hi[0] or rhi[1] < lo[1] or rlo[1] > hi[1]
+
+    holes = []
+    for v in hole_rects:
+        in_slab("'hole rect'", v[2])
+        in_slab("'hole rect'", v[5])
+        holes.append(PL.Hole.rect((min(v[0], v[3]), min(v[1], v[4])), (max(v[0], v[3]), max(v[1], v[4]))))
+    for v in hole_points:
+        in_slab("'hole point'", v[2])
+        holes.append(PL.Hole.point((v[0], v[1])))
+    for v in hole_circles:
+        in_slab("'hole circle'", v[2])
+        holes.append(PL.Hole.circle((v[0], v[1]), v[3]))
+    contacts = []
+    for v in contact_rects:
+        in_slab("'contact rect'", v[2])
+        in_slab("'contact rect'", v[5])
+        rlo, rhi = (min(v[0], v[3]), min(v[1], v[4])), (max(v[0], v[3]), max(v[1], v[4]))
+        if misses(rlo, rhi):
+            continue
+        contacts.append(PL.ContactRegion.new(rlo, rhi, (2, 2), 2.0))
+    for what, v in contact_decays:
+        in_slab(what, v[2])
+        widths, cell, limit = plane_pair(v[3:5]), plane_pair(v[5:7]), plane_pair(v[7:9])
+        rlo, rhi, rc, ratio = [0.0, 0.0], [0.0, 0.0], [0, 0], [0.0, 0.0]
+        for a in range(2):
+            if not cell[a] > 0:
+                raise DeckError(line, "%s: the cell sizes must be positive" % what)
+            if not cell[a] < widths[a]:
+                raise DeckError(line, "%s: a cell must be smaller than the rectangle's width" % what)
+            half = widths[a] / 2.0
+            rlo[a] = v[a] - half
+            rhi[a] = v[a] + half
+            rc[a] = PL.cells_no_coarser_than(widths[a], cell[a])
+            ratio[a] = 1.0 / (1.0 - cell[a] / widths[a])
+            background = (hi[a] - lo[a]) / cells[a]
+            if limit[a] >= 0 and limit[a] < background * (1.0 - 1e-9):
+                raise DeckError(line, "%s: a maxcell finer than ground plane '%s''s background cell (%r metres) "
+                                      "is not supported; raise seg1/seg2" % (what, head, background))
+        if misses(rlo, rhi):
+            continue
+        contacts.append(PL.ContactRegion.graded_per_axis(rlo, rhi, rc, ratio))
+    for name, pos in nodes:
+        in_slab("in-plane node '%s'" % name, pos[2])
+    plane = PL.GroundPlane(lo, hi, mid_z + thick / 2.0, thick, cells[0], cells[1], sigma, holes, contacts)
+    return _PlaneSpec(head, plane, nhinc, line, mid_z, a1), nodes
+
+
 def parse_deck(text: str) -> Problem:
     """Parses a FastHenry `.inp` deck in this front end's subset into a
     :class:`Problem` (SI units)."""
@@ -302,6 +546,8 @@ def parse_deck(text: str) -> Problem:
     couples_all = False
     title = None
     ended = False
+    planes: List[_PlaneSpec] = []
+    plane_node: Dict[str, int] = {}        # in-plane node name -> plane index
 
     def resolve(name: str, line: int) -> str:
         key = name.lower()
@@ -319,6 +565,17 @@ def parse_deck(text: str) -> Problem:
         else:
             return None
         return v * u if key in _LENGTHS else v
+
+    def default_sigma(line: int) -> Optional[float]:
+        """The .default conductivity in S/m, or None."""
+        if "sigma" in defaults:
+            return _number(defaults["sigma"], line) / defaults_unit["sigma"]
+        if "rho" in defaults:
+            r = _number(defaults["rho"], line)
+            if r <= 0:
+                raise DeckError(line, "rho must be positive")
+            return 1.0 / (r * defaults_unit["rho"])
+        return None
 
     for line, stmt in statements:
         if ended:
@@ -451,23 +708,119 @@ def parse_deck(text: str) -> Problem:
             else:
                 couples = (couples or []) + toks
             continue
-        if low.startswith("g") or low in (".hole", ".contact"):
-            raise DeckError(line, "ground planes ('%s') are not read by this front end; describe the plane's "
-                                  "conductors as segments" % head)
+        if low.startswith("g") and not low.startswith("."):
+            if any(pl.name.lower() == low for pl in planes):
+                raise DeckError(line, "ground plane '%s' is declared twice" % head)
+            first = rest.strip().split(None, 1)[0] if rest.strip() else ""
+            try:
+                float(first)
+                bare = True
+            except ValueError:
+                bare = False
+            if bare:
+                planes.append(_plane_extension(head, _tokens(rest), line, unit, default_sigma(line)))
+            else:
+                spec, pnodes = _plane_corner_form(head, rest, line, unit, default_sigma(line))
+                for name, pos in pnodes:
+                    if name in node_index or name in alias:
+                        raise DeckError(line, "node '%s' is declared twice" % name)
+                    node_index[name] = len(positions)
+                    positions.append(pos)
+                    plane_node[name] = len(planes)
+                planes.append(spec)
+            continue
+        if low in (".hole", ".contact"):
+            toks = _tokens(rest)
+            if len(toks) < 5:
+                raise DeckError(line, "expected %s G<name> x1 y1 x2 y2%s"
+                                % (low, " [nx=..] [ny=..] [ratio=..]" if low == ".contact" else ""))
+            target = [pl for pl in planes if pl.name.lower() == toks[0].lower()]
+            if not target:
+                raise DeckError(line, "'%s' names unknown ground plane '%s'" % (low, toks[0]))
+            pl = target[0]
+            b = [_number(t, line) * unit for t in toks[1:5]]
+            lo = (min(b[0], b[2]), min(b[1], b[3]))
+            hi = (max(b[0], b[2]), max(b[1], b[3]))
+            if low == ".hole":
+                if len(toks) != 5:
+                    raise DeckError(line, "expected .hole G<name> x1 y1 x2 y2")
+                pl.plane.holes.append(PL.Hole.rect(lo, hi))
+            else:
+                vals = _assignments(toks[5:], line, {"nx", "ny", "ratio"})
+                cells = (int(_number(vals.get("nx", "2"), line)), int(_number(vals.get("ny", "2"), line)))
+                ratio = _number(vals.get("ratio", "2"), line)
+                if ratio < 1.0:
+                    raise DeckError(line, "contact decay ratio must be >= 1 (got %s)" % vals["ratio"])
+                pl.plane.contacts.append(PL.ContactRegion.new(lo, hi, cells, ratio))
+            continue
         raise DeckError(line, "'%s' is not in the deck subset" % head)
     if not ended:
         raise DeckError(0, "the deck has no .end")
     if unit is None:
         raise DeckError(0, "the deck has no .units line")
-    # Compact the nodes: aliased nodes disappear, references go to the canonical slot.
-    live = [nm for nm in sorted(node_index, key=lambda k: node_index[k]) if nm not in alias]
-    slot = {nm: i for i, nm in enumerate(live)}
-    nodes = [positions[node_index[nm]] for nm in live]
+    # Assembly (inp.rs:4437-4620): the ground-plane meshes first, then the
+    # declared nodes still referenced as themselves (in declaration order),
+    # then the segments.  An endpoint whose .equiv class holds an in-plane
+    # node lands on that plane's nearest live cell centre, and so does one
+    # whose position lies in a plane's slab.
+    geometry = A.Geometry()
+    meshes = []
+    plane_grids: List[Tuple[int, int, float, float]] = []
+    for pl in planes:
+        try:
+            centres = pl.plane.build_into(geometry)
+        except PL.PlaneError as e:
+            raise DeckError(pl.line, str(e)) from None
+        meshes.append(centres)
+        plane_grids += [(1, pl.nhinc, 1.0, 1.0)] * (len(geometry.segments) - len(plane_grids))
+    owner: Dict[str, Tuple[int, Tuple[float, float, float]]] = {}
+    for nm, k in sorted(plane_node.items(), key=lambda kv: node_index[kv[0]]):
+        canon = alias.get(nm, nm)
+        if canon in owner and owner[canon][0] != k:
+            raise DeckError(0, ".equiv joins in-plane nodes of two different ground planes; connect the planes "
+                               "with a segment instead")
+        owner.setdefault(canon, (k, positions[node_index[nm]]))
 
-    def idx(nm: str) -> int:
-        return slot[alias.get(nm, nm)]
-    segs = [dict(s, a=idx(s["a"]), b=idx(s["b"])) for s in segments]
-    port_list = [(idx(p), idx(n), label) for (p, n, label, _) in ports]
+    def snapped(nm: str) -> Optional[int]:
+        canon = alias.get(nm, nm)
+        if canon in owner:
+            k, pos = owner[canon]
+            return planes[k].plane.attach(meshes[k], pos)
+        pos = positions[node_index[canon]]
+        for k, pl in enumerate(planes):
+            if pl.plane.contains(pos, 0.0):
+                return pl.plane.attach(meshes[k], pos)
+        return None
+
+    seg_ends = [(snapped(sg["a"]), snapped(sg["b"])) for sg in segments]
+    port_ends = [(snapped(p), snapped(n)) for (p, n, _, _) in ports]
+    used = set()
+    for (sa, sb), sg in zip(seg_ends, segments):
+        if sa is None:
+            used.add(alias.get(sg["a"], sg["a"]))
+        if sb is None:
+            used.add(alias.get(sg["b"], sg["b"]))
+    for (sp, sn), (p, n, _, _) in zip(port_ends, ports):
+        if sp is None:
+            used.add(alias.get(p, p))
+        if sn is None:
+            used.add(alias.get(n, n))
+    slot: Dict[str, int] = {}
+    for nm in sorted(node_index, key=lambda k: node_index[k]):
+        if nm in alias or nm not in used:
+            continue
+        slot[nm] = geometry.add_node(A.Node(*positions[node_index[nm]]))
+    nodes = [(nd.x, nd.y, nd.z) for nd in geometry.nodes]
+
+    def end(nm: str, snap: Optional[int]) -> int:
+        return snap if snap is not None else slot[alias.get(nm, nm)]
+    plane_segs = [{"a": sd.a, "b": sd.b, "width": sd.width, "height": sd.height, "sigma": sd.sigma,
+                   "width_dir": None} for sd in geometry.segments]
+    segs = plane_segs + [dict(sg, a=end(sg["a"], sa), b=end(sg["b"], sb))
+                         for sg, (sa, sb) in zip(segments, seg_ends)]
+    port_list = [(end(p, sp), end(n, sn), label) for (p, n, label, _), (sp, sn) in zip(ports, port_ends)]
+    grids = plane_grids + grids
+    groups = [""] * len(plane_grids) + groups
     if any(g[2] != 1.0 or g[3] != 1.0 for g in grids):
         disc = {"kind": "per_segment_graded", "grids": grids}
     elif grids and all(g[:2] == grids[0][:2] for g in grids):

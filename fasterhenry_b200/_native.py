@@ -71,7 +71,8 @@ class SweepReport(ctypes.Structure):
 class PfftParams(ctypes.Structure):
     _fields_ = [("spacing_kind", ctypes.c_int32), ("interpolation_order", ctypes.c_int32),
                 ("cells_per_filament", ctypes.c_double), ("spacing", ctypes.c_double),
-                ("near_field_radius", ctypes.c_double)]
+                ("near_field_radius", ctypes.c_double), ("fft_precision", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class PfftStats(ctypes.Structure):
@@ -134,6 +135,7 @@ EXPORTS = [
     "fh_pfft_destroy", "fh_gmres_default_params", "fh_iterative_create", "fh_iterative_counts", "fh_iterative_timing",
     "fh_iterative_pfft_stats", "fh_iterative_sweep", "fh_iterative_destroy", "fh_test_gmres_dense",
     "fh_batch_sweep", "fh_gradient", "fh_test_inductance_gradient", "fh_release_cached_memory", "fh_test_near_pairs",
+    "fh_test_grid_convolution",
     "fh_system_layout", "fh_currents", "fh_system_create_coupled", "fh_system_coupling",
 ]
 
@@ -212,6 +214,8 @@ def load():
                               P(GradientReport), ei]
     L.fh_test_inductance_gradient.argtypes = [P(Filament), c_double_p, sz, c_double_p, c_double_p, ei]
     L.fh_test_near_pairs.argtypes = [P(Filament), sz, ctypes.c_double, c_int64_p, c_int64_p, sz, P(sz), ei]
+    L.fh_test_grid_convolution.argtypes = [c_int64_p, c_int64_p, ctypes.c_double, ctypes.c_int32, c_double_p,
+                                           ctypes.c_int32, c_double_p, ei]
     L.fh_system_layout.argtypes = [ctypes.c_void_p, c_int64_p, c_int64_p, c_int64_p]
     L.fh_system_create_coupled.argtypes = [P(Node), sz, P(SegmentDef), sz, P(Port), sz, P(Discretization),
                                            P(CouplingSpec), ctypes.c_int, P(ctypes.c_void_p), ei]

@@ -947,6 +947,23 @@ def near_pairs(filaments: np.ndarray, radius: float) -> Tuple[np.ndarray, np.nda
     raise RuntimeError("near_pairs: capacity")
 
 
+def grid_convolution(sources: np.ndarray, padded: Sequence[int], spacing: float, fp32: bool = False) -> np.ndarray:
+    """The pFFT grid convolution on its own (fh_test_grid_convolution):
+    ``sources`` (fields x n0 x n1 x n2) convolved with 1 / (spacing |d|) on
+    the padded torus ``padded`` by the library's own transforms."""
+    q = np.ascontiguousarray(sources, dtype=np.float64)
+    if q.ndim == 3:
+        q = q[None]
+    n = np.array(q.shape[1:], dtype=np.int64)
+    m = np.ascontiguousarray(padded, dtype=np.int64)
+    out = np.zeros_like(q)
+    info = N.ErrorInfo()
+    _check(N.load().fh_test_grid_convolution(n.ctypes.data_as(N.c_int64_p), m.ctypes.data_as(N.c_int64_p),
+                                             float(spacing), 1 if fp32 else 0, q.ctypes.data_as(N.c_double_p),
+                                             q.shape[0], out.ctypes.data_as(N.c_double_p), ctypes.byref(info)), info)
+    return out
+
+
 def solve(geometry, ports: Sequence, discretization: dict, frequencies: Sequence[float],
           precision: Precision = Precision.FP64, solver: SolverChoice = SolverChoice.DENSE,
           iterative: Optional[IterativeParams] = None) -> SweepResult:
@@ -991,11 +1008,14 @@ def batch_sweep(systems: Sequence["MeshSystem"], frequencies: Sequence[Sequence[
 class PfftParams:
     """PfftParams (pfft/mod.rs:183-232).  ``spacing`` None means
     GridSpacing::Auto with ``cells_per_filament``; a float is
-    GridSpacing::Fixed in metres."""
+    GridSpacing::Fixed in metres.  ``fft_fp32`` runs the grid convolution in
+    FP32 instead of FP64 (projection, interpolation and the near-field
+    precorrection stay FP64)."""
     cells_per_filament: float = 8.0
     spacing: Optional[float] = None
     near_field_radius: float = 8.0
     interpolation_order: int = 5
+    fft_fp32: bool = False
 
     def _native(self) -> N.PfftParams:
         p = N.PfftParams()
@@ -1004,6 +1024,7 @@ class PfftParams:
         p.cells_per_filament = float(self.cells_per_filament)
         p.spacing = float(self.spacing or 0.0)
         p.near_field_radius = float(self.near_field_radius)
+        p.fft_precision = 1 if self.fft_fp32 else 0
         return p
 
 

@@ -72,7 +72,7 @@ def build(verbose: bool = False) -> str:
     with concurrent.futures.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), sources))
     if not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", HOST_CXX, "-o", LIB] + objs + ["-L" + os.path.join(CUDA_HOME, "lib64"), "-lcufft",
+        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", HOST_CXX, "-o", LIB] + objs + ["-L" + os.path.join(CUDA_HOME, "lib64"),
                                                                                   "-Xlinker", "-rpath=" + os.path.join(CUDA_HOME, "lib64"),
                                                                                   "-lcudart_static", "-lrt", "-ldl",
                                                                                   "-lpthread"]

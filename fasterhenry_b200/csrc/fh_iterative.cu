@@ -231,6 +231,9 @@ fh_status fh_iterative_create(const fh_node *nodes, size_t n_nodes, const fh_seg
     cfg.spacing = pp.spacing;
     cfg.near_field_radius = pp.near_field_radius;
     cfg.order = pp.interpolation_order;
+    if (pp.fft_precision != 0 && pp.fft_precision != 1)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "fft_precision must be 0 (FP64) or 1 (FP32)");
+    cfg.fft_fp32 = pp.fft_precision == 1;
     fh_status st = discretize_geometry(nodes, n_nodes, segments, n_segments, disc, s->disc, err);
     if (st) return st;
     st = build_loops(segments, n_segments, n_nodes, s->disc.per_segment.data(), ports, n_ports, s->loops, err);

@@ -10,6 +10,7 @@
 #include <cstdint>
 #include <vector>
 
+#include "fh_fftconv.h"
 #include "fh_internal.h"
 
 namespace fhb {
@@ -59,6 +60,7 @@ struct PfftConfig {
     double spacing = 0.0;
     double near_field_radius = 8.0;
     int order = 5;
+    bool fft_fp32 = false;  // grid convolution in FP32 (else FP64)
 };
 
 // Largest padded FFT grid, in points (MAX_FFT_POINTS, pfft/mod.rs:168).
@@ -108,7 +110,7 @@ fh_status pfft_near_csr(int64_t n, int64_t np, const int2 *d_pairs, const double
 inline double grid_kernel(int64_t dx, int64_t dy, int64_t dz, double spacing);
 
 // The operator on the device (fh_pfft.cu).  Owns its device memory and its
-// FFT plans; products run on `stream`.
+// convolution tables; products run on `stream`.
 struct PfftDevice {
     int64_t n = 0, G = 0, P = 0;  // filaments, grid points, padded points
     PfftGrid grid;
@@ -124,11 +126,11 @@ struct PfftDevice {
     int64_t *d_near_off = nullptr;
     uint32_t *d_near_col = nullptr;
     double *d_near_val = nullptr;
-    double *d_spectrum = nullptr;  // real spectrum of the kernel with the 1 / P of the inverse transform
-    void *d_work = nullptr;        // complex padded grids, reused across products
+    FftConvTables conv;            // twiddles and the kernel's spectrum (fh_fftconv.cu)
+    bool fft_fp32 = false;
+    void *d_work = nullptr;        // the convolution's grids, reused across products (device cache)
     size_t work_bytes = 0;
-    std::vector<std::pair<int, int>> plans;  // (batch, cufftHandle)
-    void *stream = nullptr;                  // cudaStream_t
+    void *stream = nullptr;        // cudaStream_t
     bool own_stream = false;
     int64_t projection_entries = 0, near_entries = 0;
     double setup_host_s = 0, setup_device_s = 0, setup_near_s = 0;  // setup_near_s: the near-pair search (part of the device time)

@@ -33,6 +33,9 @@ fh_status to_config(const fh_pfft_params *p, PfftConfig &cfg, fh_error_info *err
     cfg.spacing = p->spacing;
     cfg.near_field_radius = p->near_field_radius;
     cfg.order = p->interpolation_order;
+    if (p->fft_precision != 0 && p->fft_precision != 1)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "fft_precision must be 0 (FP64) or 1 (FP32)");
+    cfg.fft_fp32 = p->fft_precision == 1;
     return FH_OK;
 }
 
@@ -47,6 +50,8 @@ void fh_pfft_default_params(fh_pfft_params *params) {
     params->cells_per_filament = 8.0;
     params->spacing = 0.0;
     params->near_field_radius = 8.0;
+    params->fft_precision = 0;
+    params->reserved = 0;
 }
 
 fh_status fh_pfft_create(const fh_filament *filaments, size_t n, const fh_pfft_params *params, fh_pfft **out,

@@ -308,3 +308,37 @@ def scaling_meander(bars: int, pitch: float = 100e-6, width: float = 20e-6, thic
             add(along * pitch, y)
         add((bars if bar % 2 == 0 else 0) * pitch, y + pitch)
     return Deck(nodes, segs, [(0, len(nodes) - 1)], uniform(nw, nh), "scaling_meander_%d" % bars)
+
+
+def meander_over_plane(bars: int, plane_side: float = 4e-3, cells: int = 64, gap: float = 50e-6,
+                       plane_thickness: float = 10e-6, hole_side: float = 0.5e-3) -> Deck:
+    """The square meander of `bars` runs (scaling_meander, 2 x 2 per segment)
+    over a copper ground plane: a `plane_side` square centred under the
+    meander, top surface `gap` below the meander's bottom face,
+    `plane_thickness` thick, meshed `cells` x `cells` (one filament per bar)
+    with one square hole of side `hole_side` at its centre.  The plane is not
+    connected to the meander: it carries the induced (eddy) currents.
+    bars = 157 with the defaults is the matrix-free large case (99,224
+    meander filaments plus 8,060 plane bars); bars = 49 its dense-checkable
+    subset."""
+    from .api import Geometry, Node, SegmentDef
+    from .plane import GroundPlane, Hole
+    base = scaling_meander(bars)
+    thickness = base.segments[0]["height"]
+    centre = bars * 100e-6 / 2.0
+    half = plane_side / 2.0
+    g = Geometry()
+    plane = GroundPlane((centre - half, centre - half), (centre + half, centre + half),
+                        -thickness / 2.0 - gap, plane_thickness, cells, cells, COPPER,
+                        holes=[Hole.rect((centre - hole_side / 2.0, centre - hole_side / 2.0),
+                                         (centre + hole_side / 2.0, centre + hole_side / 2.0))])
+    plane.build_into(g)
+    offset = len(g.nodes)
+    nodes = [(nd.x, nd.y, nd.z) for nd in g.nodes] + list(base.nodes)
+    segs = [segment(sd.a, sd.b, sd.width, sd.height, sd.sigma) for sd in g.segments]
+    nplane = len(segs)
+    segs += [dict(sg, a=sg["a"] + offset, b=sg["b"] + offset) for sg in base.segments]
+    ports = [(a + offset, b + offset) for a, b in base.ports]
+    grids = [(1, 1)] * nplane + [(2, 2)] * len(base.segments)
+    return Deck(nodes, segs, ports, per_segment(grids), "meander_%d_over_plane" % bars)
+

@@ -445,6 +445,14 @@ fh_status fh_test_inductance_gradient(const fh_filament *filaments, const double
 fh_status fh_test_near_pairs(const fh_filament *filaments, size_t n, double radius, int64_t *off, int64_t *cols,
                              size_t cap, size_t *total, fh_error_info *err);
 
+/* Test hook: the pFFT grid convolution on its own.  `fields` real source
+ * grids n[0] x n[1] x n[2] (axis 2 fastest, field f at sources + f G) are
+ * convolved with the kernel 1 / (spacing |d|) (zero at d = 0) on the padded
+ * torus m[0] x m[1] x m[2] (m_a >= 2 n_a - 1, 2^a 3^b 5^c) by the library's
+ * own transforms, fp32 != 0 in FP32; potentials like sources. */
+fh_status fh_test_grid_convolution(const int64_t *n, const int64_t *m, double spacing, int32_t fp32,
+                                   const double *sources, int32_t fields, double *potentials, fh_error_info *err);
+
 /* Fill statistics of an assembled system: pairs per method and device time
  * per fill kernel (no reference counterpart; diagnostics). */
 typedef struct fh_fill_stats {
@@ -523,9 +531,15 @@ typedef struct fh_pfft_params {
     double cells_per_filament;
     double spacing;
     double near_field_radius;
+    /* Precision of the grid convolution (no reference counterpart; the
+     * reference convolves in FP64): 0 = FP64, 1 = FP32.  Projection,
+     * interpolation and the near-field precorrection stay FP64. */
+    int32_t fft_precision;
+    int32_t reserved;
 } fh_pfft_params;
 
-/* PfftParams::default(): Auto 8 cells per filament, radius 8, order 5. */
+/* PfftParams::default(): Auto 8 cells per filament, radius 8, order 5; FP64
+ * convolution. */
 void fh_pfft_default_params(fh_pfft_params *params);
 
 /* PfftStats (pfft/mod.rs:255-272) plus the set-up time split. */

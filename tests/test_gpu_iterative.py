@@ -143,3 +143,24 @@ def test_solve_dispatches_on_the_solver_choice(fh):
     assert np.max(np.abs(it.impedance_ohm - dense.impedance_ohm) / np.abs(dense.impedance_ohm)) < 1e-4
     assert fh.SolverChoice.AUTO.resolve(240) == "dense"
     assert fh.SolverChoice.AUTO.resolve(20000) == "iterative"
+
+
+def test_meander_over_a_ground_plane_matches_the_dense_path(fh):
+    """A meander over a holed ground plane (the plane carries only induced
+    currents): the matrix-free Z within the reference's 1e-4 of the dense FP64
+    Z, with the grid convolution in FP64 and in FP32."""
+    deck = F.meander_over_plane(12, plane_side=1.0e-3, cells=16, hole_side=0.2e-3)
+    g = fh.Geometry.from_deck(deck)
+    with fh.MeshSystem.assemble(g, deck.ports, deck.discretization) as d:
+        z_dense = d.impedance(1e9)
+    for fp32 in (False, True):
+        params = fh.IterativeParams(pfft=fh.PfftParams(near_field_radius=8.0, interpolation_order=2, fft_fp32=fp32),
+                                    gmres=fh.GmresParams(tolerance=1e-8))
+        with fh.IterativeSystem.assemble(g, deck.ports, deck.discretization, params) as s:
+            z_it = s.impedance(1e9)
+        assert np.max(np.abs(z_it - z_dense) / np.abs(z_dense)) < 1e-4
+    # the plane's eddy currents lower the meander's inductance
+    bare = F.scaling_meander(12)
+    with fh.MeshSystem.assemble(fh.Geometry.from_deck(bare), bare.ports, bare.discretization) as d:
+        z_bare = d.impedance(1e9)
+    assert z_dense[0, 0].imag < z_bare[0, 0].imag

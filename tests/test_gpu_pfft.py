@@ -46,6 +46,20 @@ def test_random_sets_match_the_dense_product(fh, oracle, n, seed, manhattan):
     assert mx < TOLERANCE, mx
 
 
+# The grid convolution in FP32 (the rest of the product in FP64): bound 5e-6,
+# stated for this form (the reference's 1e-6 is for its FP64 convolution).
+FP32_TOLERANCE = 5e-6
+
+
+@pytest.mark.parametrize("n,seed", [(200, 2), (500, 3)])
+@pytest.mark.parametrize("manhattan", [True, False])
+def test_fp32_convolution_matches_the_dense_product(fh, oracle, n, seed, manhattan):
+    fil = filaments_of(fh, F.cloud_deck(n, manhattan, seed))
+    norm, mx, _ = errors(fh, oracle, fil, fh.PfftParams(fft_fp32=True), probe_vector(n, 99))
+    assert norm < FP32_TOLERANCE, norm
+    assert mx < FP32_TOLERANCE, mx
+
+
 def test_most_pairs_of_a_large_random_set_take_the_fft_path(fh):
     n = 500
     fil = filaments_of(fh, F.cloud_deck(n, True, 3))

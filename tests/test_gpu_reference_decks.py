@@ -59,3 +59,20 @@ def test_twobar_deck_matches_the_oracle(fh, oracle):
     assert np.max(np.abs(z - ref)) / np.max(np.abs(ref)) < 1e-10
     assert np.max(np.abs(z[:, 0, 1] - z[:, 1, 0]) / np.abs(z[:, 0, 1])) < 1e-12
     assert np.all(z[:, 0, 1].imag > 0)  # positive mutual inductance of parallel bars
+
+
+@pytest.mark.parametrize("a,b", [("plane_fasthenry.inp", "plane_extension.inp"),
+                                 ("plane_decay_rect.inp", "plane_decay_extension.inp")])
+def test_plane_deck_pairs_solve_bit_identically_and_match_the_oracle(fh, oracle, a, b):
+    """fasterhenry-cli/tests/roundtrip.rs:384-480: the two G grammars of one
+    plane give identical sweeps; both within 1e-10 of the oracle's dense Z."""
+    pa, pb = load(a), load(b)
+    za, _ = fh.run(pa, fh.Precision.FP64, fh.SolverChoice.DENSE)
+    zb, _ = fh.run(pb, fh.Precision.FP64, fh.SolverChoice.DENSE)
+    assert np.array_equal(za.impedance_ohm, zb.impedance_ohm)
+    ref = oracle_sweep(oracle, pa, pa.frequencies_hz)
+    assert np.max(np.abs(za.impedance_ohm - ref) / np.abs(ref)) < 1e-10
+    # the via pair over the plane: resistive and inductive, inductance falling
+    # as the plane's eddy currents take over
+    z = za.impedance_ohm[:, 0, 0]
+    assert np.all(z.real > 0) and np.all(z.imag > 0)

@@ -26,7 +26,8 @@ and highest frequency and reports the error of the GPU's FP64 and mixed Z
 against those oracle values (``max_rel_err_*_vs_oracle``).
 
 ``--config c3`` sweeps 64 seeded spirals of uneven size (16 frequencies each,
-mixed form) through one batched call, four systems in flight.
+mixed form) through one batched call: one persistent launch for all 1,024
+(system, frequency) items, tile shapes from the autotuner.
 
 ``--config c5`` runs the matrix-free path instead (its own JSON line): the
 square meander of 157 runs (99,224 filaments at 2 x 2) over a 4 mm x 4 mm
@@ -334,8 +335,10 @@ def run_ours(args):
 
 def run_c3(args):
     """64 independent spirals of uneven size, each swept over 16 frequencies
-    in the mixed form, all through one batched call (fh_batch_sweep, four
-    systems in flight); a step is the whole batch.  Every Z is checked
+    in the mixed form, all through one batched call (fh_batch_sweep): the
+    1,024 (system, frequency) items in ONE persistent launch, tile shapes per
+    order bucket from the autotuner (measured on the first call, cached in a
+    JSON file).  A step is the whole batch, host in/out.  Every Z is checked
     against the FP64 form of the same batch.  Rank 0 only (one GPU)."""
     import torch
     import fasterhenry_b200 as fh
@@ -350,36 +353,59 @@ def run_c3(args):
     assemble_s = time.perf_counter() - t0
     freqs = [F.logspace(7, 10, 16) for _ in systems]
     ref = fh.batch_sweep(systems, freqs, fh.Precision.FP64, concurrency=4)
+    t1 = time.perf_counter()
+    fh.batch_sweep(systems, freqs, fh.Precision.MIXED_BF16X3)  # first call: autotunes new buckets
+    first_call_s = time.perf_counter() - t1
     for _ in range(args.warmup):
-        fh.batch_sweep(systems, freqs, fh.Precision.MIXED_BF16X3, concurrency=4)
+        fh.batch_sweep(systems, freqs, fh.Precision.MIXED_BF16X3)
     times = []
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
             torch.cuda.synchronize()
             t1 = time.perf_counter()
-            res = fh.batch_sweep(systems, freqs, fh.Precision.MIXED_BF16X3, concurrency=4)
+            res = fh.batch_sweep(systems, freqs, fh.Precision.MIXED_BF16X3)
             torch.cuda.synchronize()
             times.append(time.perf_counter() - t1)
+    with fh.Profiler() as prof:
+        fh.batch_sweep(systems, freqs, fh.Precision.MIXED_BF16X3)
+        profile = prof.read()
+    # the per-system path for comparison: each system's own mixed sweep in turn
     torch.cuda.synchronize()
     t2 = time.perf_counter()
-    fh.batch_sweep(systems, freqs, fh.Precision.MIXED_BF16X3, concurrency=1)
+    for s, f in zip(systems, freqs):
+        s.sweep(f, fh.Precision.MIXED_BF16X3)
     torch.cuda.synchronize()
-    one_at_a_time = time.perf_counter() - t2
+    per_system_s = time.perf_counter() - t2
     step = statistics.median(times)
     rel = max(float(np.max(np.abs(m.impedance_ohm - r.impedance_ohm) / np.abs(r.impedance_ohm)))
               for m, r in zip(res, ref))
     counts = [s.counts() for s in systems]
+    b = profile["batch"]
+    peaks, _ = _peaks()
+    cache = os.environ.get("FH_AUTOTUNE_CACHE") or os.path.join(
+        os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache"),
+        "fasterhenry_b200", "batch_tiles.json")
+    try:
+        with open(cache) as f:
+            table = json.load(f)
+    except Exception:
+        table = None
     out = {
         "metric": "batched Z(w) sweeps of 64 uneven spirals x 16 freqs: mixed+IR, s", "value": round(step, 6),
         "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step * 1e3, 3),
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c64+bf16x3 (FP64 residual)",
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (FP32 SIMT) + FP64 residual",
         "data": "synthetic",
         "config": {"workload": WORKLOADS["c3"][0], "systems": len(systems),
                    "filaments_min": min(c["filaments"] for c in counts),
                    "filaments_max": max(c["filaments"] for c in counts),
+                   "internal_meshes_min": min(c["internal_meshes"] for c in counts),
+                   "internal_meshes_max": max(c["internal_meshes"] for c in counts),
                    "internal_meshes_total": sum(c["internal_meshes"] for c in counts),
-                   "concurrency": 4, "l2": "working sets of up to 64 MB per system; no flush"},
-        "assemble_all_s": round(assemble_s, 3), "one_system_at_a_time_s": round(one_at_a_time, 4),
+                   "items": sum(len(f) for f in freqs), "l2": "working sets of up to 4.3 MB per item; no flush"},
+        "launches_per_step": b["launches"], "kernel_ms": round(b["ms"], 3),
+        "kernel_tflops": round(b["work"] / (b["ms"] * 1e-3) / 1e12, 2) if b["ms"] else None,
+        "autotune": {"first_call_s": round(first_call_s, 3), "table": table},
+        "assemble_all_s": round(assemble_s, 3), "per_system_sweeps_s": round(per_system_s, 4),
         "max_rel_err_vs_fp64": rel, "clocks": clocks.summary(),
     }
     print(json.dumps(out))

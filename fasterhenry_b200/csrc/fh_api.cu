@@ -14,6 +14,7 @@
 #include <mutex>
 #include <thread>
 
+#include "fh_batchsolve.h"
 #include "fh_device.cuh"
 #include "fh_lu.cuh"
 
@@ -184,7 +185,9 @@ struct PBuf {
 enum PoolSlot {
     kSlotA, kSlotD32, kSlotR, kSlotRnorm, kSlotBnorm, kSlotDnorm, kSlotXnorm, kSlotPiv, kSlotSing, kSlotPv,
     kSlotPi, kSlotTk, kSlotCoop, kSlotLinv, kSlotUinv, kSlotSolve, kSlotPackA, kSlotPackB, kSlotOmega, kSlotX,
-    kSlotZ, kSlotXinv, kSlotXpack, kSlotTbuf, kSlotDvec, kSlotFlow, kSlotResPart
+    kSlotZ, kSlotXinv, kSlotXpack, kSlotTbuf, kSlotDvec, kSlotFlow, kSlotResPart,
+    // the persistent batched solve (fh_batch_sweep, mixed), in the first system's pool
+    kSlotBatchSys, kSlotBatchOne, kSlotBatchItems, kSlotBatchZ, kSlotBatchStatus, kSlotBatchCounter, kSlotBatchWork
 };
 
 #define FHB_PALLOC(pool, buf, slot_id, count)                                                          \
@@ -532,6 +535,135 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     cudaEventElapsedTime(&ms2, e1, e2);
     if (ms_factor) *ms_factor += ms1;
     if (ms_refine) *ms_refine += ms2;
+    return FH_OK;
+}
+
+// fh_batch_sweep in a mixed precision: every (system, frequency) of the
+// systems with m <= FH_BATCH_MAX_ORDER in one persistent launch
+// (fh_batchsolve.cu), largest first; items whose refinement did not converge
+// are redone by the FP64 sweep.  Frequencies are checked per system first:
+// a system with an invalid frequency is left to the per-system path, which
+// reports it.  done[i] is set for the systems finished here.
+fh_status batch_sweep_persistent(fh_system *const *systems, size_t k, const double *const *freqs, const size_t *nf,
+                                 double *const *z_out, std::vector<char> &done, fh_error_info *err) {
+    std::vector<size_t> take;
+    int dev0 = systems[0]->device;
+    for (size_t i = 0; i < k; ++i) {
+        const fh_system *s = systems[i];
+        bool ok = s->m <= FH_BATCH_MAX_ORDER && s->device == dev0 && (nf[i] == 0 || freqs[i]);
+        for (size_t f = 0; ok && f < nf[i]; ++f) ok = std::isfinite(freqs[i][f]) && freqs[i][f] >= 0.0;
+        if (ok) take.push_back(i);
+    }
+    if (take.empty()) return FH_OK;
+    FHB_CUDA(cudaSetDevice(dev0));
+    cudaStream_t st = systems[take[0]]->stream;
+    for (size_t i : take) FHB_CUDA(cudaStreamSynchronize(systems[i]->stream));
+    const double t0 = wall();
+    std::vector<BatchSys> sys(take.size());
+    int64_t mmax = 1;
+    int pmax = 1;
+    for (size_t t = 0; t < take.size(); ++t) {
+        const fh_system *s = systems[take[t]];
+        sys[t].R = s->d_Rm;
+        sys[t].L = s->d_Lm;
+        sys[t].ld = s->nloops;
+        sys[t].m = s->m;
+        sys[t].p = s->p;
+        mmax = std::max<int64_t>(mmax, s->m);
+        pmax = std::max<int>(pmax, (int)s->p);
+    }
+    PBuf<unsigned char> d_sys, d_one;
+    DevPool &pool = systems[take[0]]->pool;
+    FHB_PALLOC(pool, d_sys, kSlotBatchSys, sizeof(BatchSys) * sys.size());
+    FHB_PALLOC(pool, d_one, kSlotBatchOne, sizeof(BatchSys));
+    FHB_CUDA(cudaMemcpyAsync(d_sys.p, sys.data(), sizeof(BatchSys) * sys.size(), cudaMemcpyHostToDevice, st));
+    // tile configurations per order bucket (measured on first use)
+    std::vector<int> cfg(sys.size(), 0);
+    for (size_t t = 0; t < sys.size(); ++t) {
+        FHB_CUDA(cudaMemcpyAsync(d_one.p, &sys[t], sizeof(BatchSys), cudaMemcpyHostToDevice, st));
+        fh_status e = batch_tuner().config_for(sys[t], reinterpret_cast<const BatchSys *>(d_one.p), st, &cfg[t], err);
+        if (e) return e;
+    }
+    // items, largest first
+    std::vector<BatchItem> items;
+    std::vector<int64_t> zoff(sys.size() + 1, 0);
+    for (size_t t = 0; t < sys.size(); ++t) zoff[t + 1] = zoff[t] + (int64_t)nf[take[t]] * sys[t].p * sys[t].p;
+    for (size_t t = 0; t < sys.size(); ++t)
+        for (size_t f = 0; f < nf[take[t]]; ++f) {
+            BatchItem it;
+            it.sys = (int32_t)t;
+            it.cfg = cfg[t];
+            it.omega = kTau * freqs[take[t]][f];
+            it.z_offset = zoff[t] + (int64_t)f * sys[t].p * sys[t].p;
+            it.index = (int32_t)items.size();
+            items.push_back(it);
+        }
+    std::stable_sort(items.begin(), items.end(), [&](const BatchItem &a, const BatchItem &b) {
+        return sys[a.sys].m > sys[b.sys].m;
+    });
+    const int nitems = (int)items.size();
+    std::vector<double> z((size_t)(2 * std::max<int64_t>(1, zoff.back())));
+    std::vector<int32_t> status((size_t)std::max(1, nitems), 0);
+    if (nitems > 0) {
+        const int ctas = std::min(batch_resident_ctas(), nitems);
+        const size_t slot = batch_slot_bytes(mmax, pmax);
+        PBuf<unsigned char> d_items, d_z, d_status, d_counter, d_work;
+        FHB_PALLOC(pool, d_items, kSlotBatchItems, sizeof(BatchItem) * items.size());
+        FHB_PALLOC(pool, d_z, kSlotBatchZ, 8 * z.size());
+        FHB_PALLOC(pool, d_status, kSlotBatchStatus, sizeof(int32_t) * status.size());
+        FHB_PALLOC(pool, d_counter, kSlotBatchCounter, 16);
+        FHB_PALLOC(pool, d_work, kSlotBatchWork, slot * (size_t)ctas);
+        FHB_CUDA(cudaMemcpyAsync(d_items.p, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice, st));
+        double work = 0.0;
+        for (const BatchItem &it : items) work += 8.0 / 3.0 * std::pow((double)sys[it.sys].m, 3.0);
+        prof_begin(st, FH_PROF_BATCH);
+        fh_status e = batch_launch(reinterpret_cast<const BatchSys *>(d_sys.p),
+                                   reinterpret_cast<const BatchItem *>(d_items.p), nitems,
+                                   reinterpret_cast<unsigned *>(d_counter.p), d_work.p, slot, mmax, pmax,
+                                   reinterpret_cast<double2 *>(d_z.p), reinterpret_cast<int32_t *>(d_status.p), ctas,
+                                   st, err);
+        prof_end(st, FH_PROF_BATCH, work);
+        if (e) return e;
+        FHB_CUDA(cudaMemcpyAsync(z.data(), d_z.p, 8 * z.size(), cudaMemcpyDeviceToHost, st));
+        FHB_CUDA(cudaMemcpyAsync(status.data(), d_status.p, sizeof(int32_t) * status.size(), cudaMemcpyDeviceToHost,
+                                 st));
+        FHB_CUDA(cudaStreamSynchronize(st));
+    }
+    // outputs; FP64 for the items that did not converge
+    std::vector<size_t> item_of(items.size());
+    for (size_t q = 0; q < items.size(); ++q) item_of[(size_t)items[q].index] = q;
+    size_t idx = 0;
+    for (size_t t = 0; t < sys.size(); ++t) {
+        const size_t i = take[t];
+        const int64_t pp = sys[t].p * sys[t].p;
+        for (size_t f = 0; f < nf[i]; ++f, ++idx) {
+            double *dst = z_out[i] + 2 * (int64_t)f * pp;
+            if (status[idx] < 0) {
+                fh_error_info e{};
+                const fh_status s2 = fh_sweep(systems[i], freqs[i] + f, 1, FH_PRECISION_FP64, dst, nullptr, &e);
+                if (s2) {
+                    const char *msg = fh_last_error();
+                    fh_status r = fail(err, s2, "system " + std::to_string(i) + ": " + (msg ? msg : ""), e.index_a,
+                                       e.index_b, e.frequency, (int32_t)i);
+                    return r;
+                }
+                continue;
+            }
+            const double *src = z.data() + 2 * (zoff[t] + (int64_t)f * pp);
+            bool bad = false;
+            for (int64_t q = 0; q < 2 * pp; ++q) bad = bad || !std::isfinite(src[q]);
+            if (bad)
+                return fail(err, FH_ERR_SINGULAR,
+                            "system " + std::to_string(i) + ": the mesh system is singular or ill-conditioned at " +
+                                fstr(freqs[i][f]) + " Hz",
+                            (int64_t)f, -1, freqs[i][f], (int32_t)i);
+            std::memcpy(dst, src, 16 * (size_t)pp);
+        }
+        fh_system *s = systems[i];
+        s->timing.solve_s = wall() - t0;
+        s->timing.total_s = s->timing.assembly_s + s->timing.solve_s;
+        done[i] = 1;
+    }
     return FH_OK;
 }
 
@@ -1011,7 +1143,20 @@ fh_status fh_batch_sweep(fh_system *const *systems, size_t k, const double *cons
     for (size_t i = 0; i < k; ++i)
         if (!systems[i]) return fail(err, FH_ERR_INVALID_ARGUMENT, "null system " + std::to_string(i));
     if (k == 0) return FH_OK;
-    const int workers = (int)std::min<size_t>(k, (size_t)(concurrency > 0 ? concurrency : 4));
+    if (precision < FH_PRECISION_FP64 || precision > FH_PRECISION_MIXED_FP32)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "unknown precision");
+    // Mixed precisions: the small systems in one persistent launch; the
+    // others (and every system in FP64) through the per-system sweeps below.
+    std::vector<char> done(k, 0);
+    if (precision != FH_PRECISION_FP64) {
+        fh_status st = batch_sweep_persistent(systems, k, freqs, nf, z_out, done, err);
+        if (st) return st;
+    }
+    std::vector<size_t> rest;
+    for (size_t i = 0; i < k; ++i)
+        if (!done[i]) rest.push_back(i);
+    if (rest.empty()) return FH_OK;
+    const int workers = (int)std::min<size_t>(rest.size(), (size_t)(concurrency > 0 ? concurrency : 4));
     for (size_t i = 0; i < k; ++i) systems[i]->share = workers;
     std::atomic<size_t> next(0);
     std::mutex mu;
@@ -1021,8 +1166,9 @@ fh_status fh_batch_sweep(fh_system *const *systems, size_t k, const double *cons
     std::string failed_msg;
     auto worker = [&]() {
         for (;;) {
-            const size_t i = next.fetch_add(1);
-            if (i >= k) return;
+            const size_t ri = next.fetch_add(1);
+            if (ri >= rest.size()) return;
+            const size_t i = rest[ri];
             fh_error_info e{};
             const fh_status st = fh_sweep(systems[i], freqs[i], nf[i], precision, z_out[i], nullptr, &e);
             if (st) {

@@ -148,11 +148,13 @@ struct fh_iterative {
     double *d_sign = nullptr, *d_t_sign = nullptr, *d_r = nullptr;
     double2 *d_c = nullptr, *d_drop = nullptr, *d_diag = nullptr, *d_b = nullptr, *d_x = nullptr;
     double *d_parts = nullptr, *d_flux = nullptr;
+    // refinement of the FP32-convolution solves: residual, correction, product
+    double2 *d_res = nullptr, *d_cor = nullptr, *d_ax = nullptr;
     GmresWork work;
     double operator_s = 0;
     ~fh_iterative() {
         void *ptrs[] = {d_row_ptr, d_t_off, d_branch, d_t_loop, d_sign, d_t_sign, d_r, d_c,
-                        d_drop, d_diag, d_b, d_x, d_parts, d_flux};
+                        d_drop, d_diag, d_b, d_x, d_parts, d_flux, d_res, d_cor, d_ax};
         for (void *q : ptrs)
             if (q) cudaFree(q);
     }
@@ -160,8 +162,21 @@ struct fh_iterative {
 
 namespace {
 
-// Z_ee x (f > 0: omega > 0) or M_e R M_e^T x (omega == 0).
-fh_status apply_ee(fh_iterative *s, double omega, const double2 *x, double2 *y, fh_error_info *err) {
+// r = b - y (refinement residual) and x += d (its correction).
+__global__ void sub_kernel(const double2 *__restrict__ b, const double2 *__restrict__ y, double2 *__restrict__ r,
+                           int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        r[i] = make_double2(b[i].x - y[i].x, b[i].y - y[i].y);
+}
+__global__ void axpy_kernel(double2 *__restrict__ x, const double2 *__restrict__ d, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = make_double2(x[i].x + d[i].x, x[i].y + d[i].y);
+}
+
+// Z_ee x (f > 0: omega > 0) or M_e R M_e^T x (omega == 0).  full_precision:
+// an operator with the FP32 grid convolution convolves in FP64.
+fh_status apply_ee(fh_iterative *s, double omega, const double2 *x, double2 *y, fh_error_info *err,
+                   bool full_precision = false) {
     const int64_t n = s->n;
     scatter_kernel<<<grid_n(n), 256, 0, s->stream>>>(x, s->d_t_off, s->d_t_loop, s->d_t_sign, s->d_c, n);
     FHB_CUDA(cudaGetLastError());
@@ -169,7 +184,7 @@ fh_status apply_ee(fh_iterative *s, double omega, const double2 *x, double2 *y, 
     if (omega != 0.0) {
         split_kernel<<<grid_n(n), 256, 0, s->stream>>>(s->d_c, s->d_parts, n);
         FHB_CUDA(cudaGetLastError());
-        fh_status st = pfft_apply(s->op, s->d_parts, s->d_flux, 2, err);
+        fh_status st = pfft_apply(s->op, s->d_parts, s->d_flux, 2, err, full_precision);
         if (st) return st;
         flux = s->d_flux;
     }
@@ -191,6 +206,67 @@ double loop_inductance(const int32_t *br, size_t len, const double *self_l, cons
     for (size_t k = 0; k < len; ++k)
         for (size_t l = k + 1; l < len; ++l) mut += sg[k] * sg[l] * mutual[q++];
     return own + 2.0 * mut;
+}
+
+// GMRES with the FP32 grid convolution, refined against the FP64 operator:
+// x = 0; repeat r = b - A x (FP64 convolution), stop when |r| <= tol |b|,
+// else solve A d = r by GMRES with the FP32 convolution to a relative
+// residual of max(tol, 1e-5) (about the FP32 product's own accuracy) and
+// x += d.  The outcome counts all inner iterations and reports the FP64
+// relative residual.
+constexpr int kMaxRefinements = 12;
+fh_status refined_solve(fh_iterative *s, double omega, const DeviceOp &apply, const DeviceOp &precondition,
+                        double2 *x, GmresOutcome *out, fh_error_info *err) {
+    const int64_t m = s->m;
+    cudaStream_t cs = s->stream;
+    if (!s->d_res) {
+        FHB_CUDA(cudaMalloc(&s->d_res, sizeof(double2) * m));
+        FHB_CUDA(cudaMalloc(&s->d_cor, sizeof(double2) * m));
+        FHB_CUDA(cudaMalloc(&s->d_ax, sizeof(double2) * m));
+    }
+    std::vector<double2> hb((size_t)m), hr((size_t)m);
+    FHB_CUDA(cudaMemcpyAsync(hb.data(), s->d_b, sizeof(double2) * m, cudaMemcpyDeviceToHost, cs));
+    FHB_CUDA(cudaStreamSynchronize(cs));
+    auto norm = [&](const std::vector<double2> &v) {
+        double t = 0.0;
+        for (const double2 &z : v) t += z.x * z.x + z.y * z.y;
+        return std::sqrt(t);
+    };
+    const double bnorm = norm(hb);
+    *out = GmresOutcome();
+    if (bnorm == 0.0) {
+        out->converged = true;
+        return FH_OK;
+    }
+    GmresParams inner = s->gp;
+    inner.tolerance = std::max(s->gp.tolerance, 1e-5);
+    int64_t used = 0;
+    for (int k = 0; k <= kMaxRefinements; ++k) {
+        fh_status st = apply_ee(s, omega, x, s->d_ax, err, true);
+        if (st) return st;
+        sub_kernel<<<grid_n(m), 256, 0, cs>>>(s->d_b, s->d_ax, s->d_res, m);
+        FHB_CUDA(cudaGetLastError());
+        FHB_CUDA(cudaMemcpyAsync(hr.data(), s->d_res, sizeof(double2) * m, cudaMemcpyDeviceToHost, cs));
+        FHB_CUDA(cudaStreamSynchronize(cs));
+        const double rel = norm(hr) / bnorm;
+        out->relative_residual = rel;
+        out->iterations = used;
+        if (rel <= s->gp.tolerance) {
+            out->converged = true;
+            return FH_OK;
+        }
+        if (k == kMaxRefinements || used >= s->gp.max_iterations) break;
+        inner.max_iterations = (int)std::max<int64_t>(1, s->gp.max_iterations - used);
+        FHB_CUDA(cudaMemsetAsync(s->d_cor, 0, sizeof(double2) * m, cs));
+        GmresOutcome oc;
+        st = gmres_solve(m, apply, precondition, s->d_res, s->d_cor, inner, cs, s->work, &oc, err);
+        if (st) return st;
+        used += oc.iterations;
+        axpy_kernel<<<grid_n(m), 256, 0, cs>>>(x, s->d_cor, m);
+        FHB_CUDA(cudaGetLastError());
+    }
+    out->converged = false;
+    return FH_OK;
 }
 
 }  // namespace
@@ -450,7 +526,9 @@ fh_status fh_iterative_sweep(fh_iterative *s, const double *freqs, size_t nf, do
                 double2 *xq = s->d_x + q * m;
                 FHB_CUDA(cudaMemsetAsync(xq, 0, sizeof(double2) * m, cs));
                 GmresOutcome oc;
-                fh_status st = gmres_solve(m, apply, precondition, s->d_b, xq, s->gp, cs, s->work, &oc, err);
+                fh_status st = s->op.fft_fp32 ? refined_solve(s, omega, apply, precondition, xq, &oc, err)
+                                              : gmres_solve(m, apply, precondition, s->d_b, xq, s->gp, cs, s->work,
+                                                            &oc, err);
                 if (st) return st;
                 if (outcomes) {
                     outcomes[fi * p + q].iterations = oc.iterations;

@@ -168,11 +168,13 @@ inline unsigned blocks_for(int64_t work, int threads, int64_t cap = 148 * 16) {
 
 }  // namespace
 
-fh_status pfft_apply_impl(PfftDevice &op, const double *d_x, double *d_y, int count, fh_error_info *err);
+fh_status pfft_apply_impl(PfftDevice &op, const double *d_x, double *d_y, int count, fh_error_info *err,
+                          bool full_precision);
 
 PfftDevice::~PfftDevice() {
     cudaStream_t s = (cudaStream_t)stream;
     fftconv_free(conv, s);
+    fftconv_free(conv64, s);
     if (d_work) cache_free(d_work, s);
     void *ptrs[] = {d_dir, d_proj_off, d_proj_idx, d_proj_w, d_spread_off, d_spread_fil,
                     d_spread_w, d_near_off, d_near_col, d_near_val};
@@ -275,6 +277,10 @@ fh_status pfft_build(const fh_filament *fil, int64_t n, const PfftConfig &cfg, v
     e = op.fft_fp32 ? fftconv_setup<float>(shape, op.grid.spacing, op.conv, s, err)
                     : fftconv_setup<double>(shape, op.grid.spacing, op.conv, s, err);
     if (e) return e;
+    if (op.fft_fp32) {
+        e = fftconv_setup<double>(shape, op.grid.spacing, op.conv64, s, err);
+        if (e) return e;
+    }
     FHB_CUDA(cudaStreamSynchronize(s));
     op.setup_device_s = now_s() - t1;
     return FH_OK;
@@ -286,10 +292,10 @@ fh_status pfft_build(const fh_filament *fil, int64_t n, const PfftConfig &cfg, v
 // in FP64) the pruned transform chain of fh_fftconv.cu: the sources A written
 // and read, B = n0 n1 m2 and C = n0 m1 m2 written and read twice each, the
 // spectrum (P reals), and the potentials A written and read.
-double pfft_apply_bytes(const PfftDevice &op, int count) {
+double pfft_apply_bytes(const PfftDevice &op, int count, bool full_precision) {
     const int ncomp = (int)op.components.size();
     const double grids = (double)((count * ncomp + 1) / 2);
-    const double E = op.fft_fp32 ? 8.0 : 16.0;
+    const double E = op.fft_fp32 && !full_precision ? 8.0 : 16.0;
     const FftConvShape &sh = op.conv.shape;
     const double A = (double)sh.n[0] * sh.n[1] * sh.n[2], B = (double)sh.n[0] * sh.n[1] * sh.m[2],
                  C = (double)sh.n[0] * sh.m[1] * sh.m[2], P = (double)op.P;
@@ -298,21 +304,23 @@ double pfft_apply_bytes(const PfftDevice &op, int count) {
            grids * conv;
 }
 
-fh_status pfft_apply(PfftDevice &op, const double *d_x, double *d_y, int count, fh_error_info *err) {
+fh_status pfft_apply(PfftDevice &op, const double *d_x, double *d_y, int count, fh_error_info *err,
+                     bool full_precision) {
     if (op.n == 0 || count <= 0) return FH_OK;
     prof_begin((cudaStream_t)op.stream, FH_PROF_PFFT_APPLY);
-    fh_status st = pfft_apply_impl(op, d_x, d_y, count, err);
-    prof_end((cudaStream_t)op.stream, FH_PROF_PFFT_APPLY, pfft_apply_bytes(op, count));
+    fh_status st = pfft_apply_impl(op, d_x, d_y, count, err, full_precision);
+    prof_end((cudaStream_t)op.stream, FH_PROF_PFFT_APPLY, pfft_apply_bytes(op, count, full_precision));
     return st;
 }
 
 namespace {
 template <class T>
-fh_status apply_far(PfftDevice &op, const double *d_x, double *d_y, int count, fh_error_info *err) {
+fh_status apply_far(PfftDevice &op, const FftConvTables &conv, const double *d_x, double *d_y, int count,
+                    fh_error_info *err) {
     cudaStream_t s = (cudaStream_t)op.stream;
     const int ncomp = (int)op.components.size();
     const int grids = (count * ncomp + 1) / 2;
-    fh_status e = ensure_work(op, sizeof(T) * 2 * fftconv_work_elems(op.conv.shape) * (size_t)grids, err);
+    fh_status e = ensure_work(op, sizeof(T) * 2 * fftconv_work_elems(conv.shape) * (size_t)grids, err);
     if (e) return e;
     ApplyArgs a;
     a.n = op.n;
@@ -329,7 +337,7 @@ fh_status apply_far(PfftDevice &op, const double *d_x, double *d_y, int count, f
     spread_kernel<T><<<blocks_for(op.G, 256), 256, 0, s>>>(op.d_spread_off, op.d_spread_fil, op.d_spread_w, op.d_dir,
                                                             d_x, work, a);
     FHB_CUDA(cudaGetLastError());
-    e = fftconv_run<T>(op.conv, work, grids, s, err);
+    e = fftconv_run<T>(conv, work, grids, s, err);
     if (e) return e;
     interp_kernel<T><<<blocks_for(op.n * 32, 256), 256, 0, s>>>(op.d_proj_off, op.d_proj_idx, op.d_proj_w, op.d_dir,
                                                                  work, d_y, a);
@@ -338,13 +346,15 @@ fh_status apply_far(PfftDevice &op, const double *d_x, double *d_y, int count, f
 }
 }  // namespace
 
-fh_status pfft_apply_impl(PfftDevice &op, const double *d_x, double *d_y, int count, fh_error_info *err) {
+fh_status pfft_apply_impl(PfftDevice &op, const double *d_x, double *d_y, int count, fh_error_info *err,
+                          bool full_precision) {
     cudaStream_t s = (cudaStream_t)op.stream;
     near_kernel<<<blocks_for(op.n * 32, 256), 256, 0, s>>>(op.d_near_off, op.d_near_col, op.d_near_val, d_x, d_y,
                                                              op.n, count);
     FHB_CUDA(cudaGetLastError());
     if (op.components.empty()) return FH_OK;
-    return op.fft_fp32 ? apply_far<float>(op, d_x, d_y, count, err) : apply_far<double>(op, d_x, d_y, count, err);
+    if (op.fft_fp32 && !full_precision) return apply_far<float>(op, op.conv, d_x, d_y, count, err);
+    return apply_far<double>(op, op.fft_fp32 ? op.conv64 : op.conv, d_x, d_y, count, err);
 }
 
 }  // namespace fhb

@@ -128,6 +128,7 @@ struct PfftDevice {
     double *d_near_val = nullptr;
     FftConvTables conv;            // twiddles and the kernel's spectrum (fh_fftconv.cu)
     bool fft_fp32 = false;
+    FftConvTables conv64;          // with fft_fp32: FP64 tables for full-precision products (residuals)
     void *d_work = nullptr;        // the convolution's grids, reused across products (device cache)
     size_t work_bytes = 0;
     void *stream = nullptr;        // cudaStream_t
@@ -146,8 +147,10 @@ struct PfftDevice {
 fh_status pfft_build(const fh_filament *fil, int64_t n, const PfftConfig &cfg, void *stream, PfftDevice &op,
                      fh_error_info *err);
 // y = L x for `count` vectors of length n (device pointers, vector v at
-// x + v n), on op.stream.
-fh_status pfft_apply(PfftDevice &op, const double *d_x, double *d_y, int count, fh_error_info *err);
+// x + v n), on op.stream.  With full_precision, an operator built with the
+// FP32 convolution convolves in FP64 (for refinement residuals).
+fh_status pfft_apply(PfftDevice &op, const double *d_x, double *d_y, int count, fh_error_info *err,
+                     bool full_precision = false);
 
 }  // namespace fhb
 

@@ -339,10 +339,17 @@ fh_status fh_sweep(fh_system *sys, const double *frequencies_hz, size_t nf, fh_p
 /* Batched sweep of independent systems (no reference counterpart: the
  * reference sweeps one MeshSystem at a time).  System i is swept over its own
  * frequencies freqs[i][0..nf[i]) into z_out[i] (nf[i] x p_i x p_i), as
- * fh_sweep would; up to `concurrency` systems (<= 0: 4) run at once, each on
- * its own stream, with their cooperative kernels and batch sizes taking an
- * equal share of the device.  On failure the first failing system (lowest
- * index) is reported, its index in fh_error_info.detail. */
+ * fh_sweep would.  In the mixed precisions every (system, frequency) of the
+ * systems with at most FH_BATCH_MAX_ORDER internal loops is solved in ONE
+ * persistent launch (FP32 factors without interchanges, FP64-residual
+ * refinement, work items largest first, tile shapes per order bucket from an
+ * autotuner whose table is kept in a JSON file: $FH_AUTOTUNE_CACHE, else the
+ * user's cache directory); an item whose refinement does not converge is
+ * redone in FP64.  Larger systems, and every system in FP64, are swept as by
+ * fh_sweep, up to `concurrency` (<= 0: 4) at once on their own streams.  On
+ * failure the first failing system (lowest index) is reported, its index in
+ * fh_error_info.detail. */
+#define FH_BATCH_MAX_ORDER 1024
 fh_status fh_batch_sweep(fh_system *const *systems, size_t k, const double *const *freqs, const size_t *nf,
                          fh_precision precision, double *const *z_out, int32_t concurrency, fh_error_info *err);
 
@@ -493,7 +500,8 @@ typedef enum fh_profile_class {
     FH_PROF_FORM = 11,          /* the sweep's systems R + jwL (and right-hand sides) formed from R_m, L_m */
     FH_PROF_SOLVE_FLOW = 12,    /* dataflow forward/backward solve of the two-level factors (flags per block) */
     FH_PROF_SOLVE_BARRIER = 13, /* barrier-based forward/backward solve of the two-level factors */
-    FH_PROF_CLASSES = 14
+    FH_PROF_BATCH = 14,         /* the persistent batched solve of many small systems (fh_batch_sweep, mixed) */
+    FH_PROF_CLASSES = 15
 } fh_profile_class;
 
 void fh_profile_enable(int32_t on);

@@ -49,6 +49,9 @@ def test_grid_convolution_matches_numpy(fh, n, fields, fp32):
     h = 2.5e-5
     got = fh.grid_convolution(q, m, h, fp32=fp32)
     want = reference(q, m, h)
+    if n == (1, 1, 1):  # a single point has no partner: the potential is zero
+        assert np.all(got == 0.0)
+        return
     err = np.max(np.abs(got - want)) / np.max(np.abs(want))
     assert err < (2e-6 if fp32 else 1e-12), err
 

@@ -239,5 +239,8 @@ def test_two_level_mixed_many_ports(fh):
             profile = prof.read()
     assert rel_err(rm.impedance_ohm, z64) < MIXED_RTOL
     assert all(1 <= i <= 10 for i in rm.refinement_iterations), rm.refinement_iterations
-    # the barrier-based solve ran (and so the rows-below pass wrote U12)
-    assert profile["solve_barrier"]["launches"] > 0 and profile["solve_flow"]["launches"] == 0
+    # the dataflow solve did not run: the refinement solved with a form that
+    # reads U12 (the barrier-based one, or the per-block one when that does not
+    # fit either), so the rows-below pass wrote U12
+    assert profile["solve_flow"]["launches"] == 0, profile
+    assert profile["solve_barrier"]["launches"] + profile["solve"]["launches"] > 0, profile

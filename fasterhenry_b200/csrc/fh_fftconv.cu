@@ -286,10 +286,13 @@ unsigned blocks_of(int64_t work, int threads, int64_t cap = 148 * 16) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>((work + threads - 1) / threads, cap));
 }
 
+// Lines per CTA: as many as two buffers of them fit the shared-memory budget,
+// up to about 4,096 points per tile (short lines come many to a tile).
 template <class T>
 int tile_for(int m) {
     const size_t per = 2 * sizeof(typename Cplx<T>::type) * (size_t)m;
-    return (int)std::max<size_t>(1, std::min<size_t>(16, kFftSmemBudget / per));
+    const size_t want = std::max<size_t>(16, 4096 / (size_t)m);
+    return (int)std::max<size_t>(1, std::min<size_t>(want, kFftSmemBudget / per));
 }
 
 // One axis step: outer x n_in x inner -> outer x keep x inner, `batch` arrays.

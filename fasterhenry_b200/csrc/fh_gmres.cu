@@ -17,7 +17,6 @@ constexpr int kRB = 256;  // reduction blocks (fixed: the combination order neve
 constexpr int kRT = 256;  // threads per block
 
 // Layout of GmresWork::red (doubles).
-constexpr int kDotPartial = 0;                  // 2 kRB
 constexpr int kMaxPartial = 2 * kRB;            // kRB
 constexpr int kSumPartial = 3 * kRB;            // kRB
 constexpr int kScale = 4 * kRB;                 // 1
@@ -27,39 +26,6 @@ constexpr int kRedLen = 4 * kRB + 8;
 using cplx = std::complex<double>;
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-
-__global__ void __launch_bounds__(kRT) dot_partial_kernel(const double2 *__restrict__ u, const double2 *__restrict__ v,
-                                                          int64_t n, double *__restrict__ partial) {
-    __shared__ double2 sh[kRT];
-    double2 acc = make_double2(0.0, 0.0);
-    for (int64_t i = (int64_t)blockIdx.x * kRT + threadIdx.x; i < n; i += (int64_t)kRB * kRT) {
-        const double2 a = u[i], b = v[i];
-        // conj(a) b
-        acc = cadd(acc, make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x));
-    }
-    sh[threadIdx.x] = acc;
-    __syncthreads();
-    for (int s = kRT / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sh[threadIdx.x] = cadd(sh[threadIdx.x], sh[threadIdx.x + s]);
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        partial[2 * blockIdx.x] = sh[0].x;
-        partial[2 * blockIdx.x + 1] = sh[0].y;
-    }
-}
-
-// out = sum of the kRB partial complex values, fixed tree.
-__global__ void __launch_bounds__(kRT) dot_final_kernel(const double *__restrict__ partial, double2 *__restrict__ out) {
-    __shared__ double2 sh[kRT];
-    sh[threadIdx.x] = make_double2(partial[2 * threadIdx.x], partial[2 * threadIdx.x + 1]);
-    __syncthreads();
-    for (int s = kRT / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sh[threadIdx.x] = cadd(sh[threadIdx.x], sh[threadIdx.x + s]);
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *out = sh[0];
-}
 
 __global__ void __launch_bounds__(kRT) maxabs_partial_kernel(const double2 *__restrict__ v, int64_t n,
                                                              double *__restrict__ partial) {
@@ -127,15 +93,65 @@ __global__ void __launch_bounds__(kRT) sum_final_kernel(const double *__restrict
     if (threadIdx.x == 0) *out = sh[0];
 }
 
-// w -= h v with h read from device memory (one MGS projection).
-__global__ void axpy_dev_kernel(double2 *__restrict__ w, const double2 *__restrict__ v, const double2 *__restrict__ h,
-                                int64_t n) {
-    const double2 a = *h;
+// The projections of w on the cnt basis vectors V_0 .. V_cnt-1 at once
+// (classical Gram-Schmidt): per block and vector k, the partial sum of
+// conj(V_k[i]) w[i] over the block's rows (warp shuffles, then the warps in
+// order) into partial[2 (k kRB + block)].
+__global__ void __launch_bounds__(kRT) multidot_partial_kernel(const double2 *__restrict__ V,
+                                                               const double2 *__restrict__ w, int64_t n, int cnt,
+                                                               double *__restrict__ partial) {
+    __shared__ double2 sh[kRT / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < cnt; ++k) {
+        const double2 *vk = V + (size_t)k * n;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int64_t i = (int64_t)blockIdx.x * kRT + threadIdx.x; i < n; i += (int64_t)kRB * kRT) {
+            const double2 a = vk[i], b = w[i];
+            acc = cadd(acc, make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x));
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+            acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+        }
+        if (lane == 0) sh[warp] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double2 t = sh[0];
+            for (int q = 1; q < kRT / 32; ++q) t = cadd(t, sh[q]);
+            partial[2 * ((size_t)k * kRB + blockIdx.x)] = t.x;
+            partial[2 * ((size_t)k * kRB + blockIdx.x) + 1] = t.y;
+        }
+        __syncthreads();
+    }
+}
+
+// h[k] = the sum of vector k's kRB partials (block k, fixed tree).
+__global__ void __launch_bounds__(kRT) multidot_final_kernel(const double *__restrict__ partial,
+                                                             double2 *__restrict__ h) {
+    __shared__ double2 sh[kRT];
+    const size_t base = (size_t)blockIdx.x * kRB;
+    sh[threadIdx.x] = make_double2(partial[2 * (base + threadIdx.x)], partial[2 * (base + threadIdx.x) + 1]);
+    __syncthreads();
+    for (int s = kRT / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] = cadd(sh[threadIdx.x], sh[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) h[blockIdx.x] = sh[0];
+}
+
+// w -= sum_k h[k] V_k, the terms taken in increasing k.
+__global__ void multi_axpy_kernel(double2 *__restrict__ w, const double2 *__restrict__ V,
+                                  const double2 *__restrict__ h, int cnt, int64_t n) {
+    extern __shared__ double2 hs[];
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) hs[k] = h[k];
+    __syncthreads();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double2 b = v[i];
         double2 y = w[i];
-        y.x += -a.x * b.x + a.y * b.y;  // y += (-a) b
-        y.y += -a.x * b.y - a.y * b.x;
+        for (int k = 0; k < cnt; ++k) {
+            const double2 a = hs[k], b = V[(size_t)k * n + i];
+            y.x += -a.x * b.x + a.y * b.y;
+            y.y += -a.x * b.y - a.y * b.x;
+        }
         w[i] = y;
     }
 }
@@ -208,18 +224,18 @@ struct Norm {
 }  // namespace
 
 GmresWork::~GmresWork() {
-    void *p[] = {V, w, r, t, u, h, red};
+    void *p[] = {V, w, r, t, u, h, red, part};
     for (void *q : p)
         if (q) cudaFree(q);
 }
 
 fh_status GmresWork::ensure(int64_t n_, int restart_, fh_error_info *err) {
     if (n_ <= n && restart_ <= restart && V) return FH_OK;
-    void *p[] = {V, w, r, t, u, h, red};
+    void *p[] = {V, w, r, t, u, h, red, part};
     for (void *q : p)
         if (q) cudaFree(q);
     V = w = r = t = u = h = nullptr;
-    red = nullptr;
+    red = part = nullptr;
     n = n_;
     restart = restart_;
     auto alloc = [&](void **q, size_t bytes) { return cudaMalloc(q, std::max<size_t>(bytes, 16)); };
@@ -227,7 +243,8 @@ fh_status GmresWork::ensure(int64_t n_, int restart_, fh_error_info *err) {
         alloc((void **)&w, sizeof(double2) * n) != cudaSuccess || alloc((void **)&r, sizeof(double2) * n) != cudaSuccess ||
         alloc((void **)&t, sizeof(double2) * n) != cudaSuccess || alloc((void **)&u, sizeof(double2) * n) != cudaSuccess ||
         alloc((void **)&h, sizeof(double2) * 2 * (restart + 1)) != cudaSuccess ||
-        alloc((void **)&red, sizeof(double) * kRedLen) != cudaSuccess) {
+        alloc((void **)&red, sizeof(double) * kRedLen) != cudaSuccess ||
+        alloc((void **)&part, sizeof(double) * 2 * kRB * (size_t)(restart + 1)) != cudaSuccess) {
         cudaGetLastError();
         return fail(err, FH_ERR_OUT_OF_MEMORY, "device allocation of the GMRES workspace failed");
     }
@@ -307,13 +324,17 @@ fh_status gmres_solve(int64_t n, const DeviceOp &apply, const DeviceOp &precondi
             st = apply(work.u, work.w, err);
             if (st) return st;
             iterations += 1;
-            for (int pass = 0; pass < 2; ++pass)
-                for (int k = 0; k <= j; ++k) {
-                    double2 *hk = work.h + pass * (restart + 1) + k;
-                    dot_partial_kernel<<<kRB, kRT, 0, s>>>(work.V + (size_t)k * n, work.w, n, work.red + kDotPartial);
-                    dot_final_kernel<<<1, kRT, 0, s>>>(work.red + kDotPartial, hk);
-                    axpy_dev_kernel<<<grid_of(n), 256, 0, s>>>(work.w, work.V + (size_t)k * n, hk, n);
-                }
+            // Classical Gram-Schmidt twice: each pass projects w on all of
+            // V_0 .. V_j in one product and removes them in one update (the
+            // reference's modified Gram-Schmidt applied twice reaches the same
+            // orthogonality; three launches per pass instead of three per
+            // basis vector).
+            for (int pass = 0; pass < 2; ++pass) {
+                double2 *hp = work.h + pass * (restart + 1);
+                multidot_partial_kernel<<<kRB, kRT, 0, s>>>(work.V, work.w, n, j + 1, work.part);
+                multidot_final_kernel<<<j + 1, kRT, 0, s>>>(work.part, hp);
+                multi_axpy_kernel<<<grid_of(n), 256, sizeof(double2) * (j + 1), s>>>(work.w, work.V, hp, j + 1, n);
+            }
             FHB_CUDA(cudaGetLastError());
             Norm wn;
             st = norm_of(work.w, wn);

@@ -1,5 +1,7 @@
 // Restarted, right-preconditioned GMRES on device vectors (gmres.rs:91-215
-// of the reference): modified Gram-Schmidt applied twice, complex Givens
+// of the reference): Gram-Schmidt applied twice (classical, each pass one
+// multi-vector product and one update; the reference applies modified
+// Gram-Schmidt twice), complex Givens
 // rotations, the true residual recomputed at every restart.  Vectors are
 // complex doubles on the device; the small Hessenberg problem lives on the
 // host.  Reductions (inner products, norms) use a fixed grid and a fixed
@@ -37,6 +39,7 @@ struct GmresWork {
     double2 *w = nullptr, *r = nullptr, *t = nullptr, *u = nullptr;
     double2 *h = nullptr;    // 2 x (restart + 1) projections of one Arnoldi step
     double *red = nullptr;   // reduction partials and results
+    double *part = nullptr;  // per-block partial projections, 2 x kRB x (restart + 1)
     ~GmresWork();
     fh_status ensure(int64_t n_, int restart_, fh_error_info *err);
 };

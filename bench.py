@@ -77,7 +77,7 @@ WORKLOADS = {
            "8 cells, GMRES to 1e-8", None),
     "c4": ("impedance gradient: 6-turn square spiral (15 um wide, 5 um spacing, 3 um thick, 500 um outer), "
            "skin-depth graded at 1 GHz (cells <= 0.1 skin depth, ratio 1.4: 3,672 filaments), dZ/dp for the "
-           "24 widths and 24 thicknesses at 1 GHz", None),
+           "24 widths, 24 thicknesses and the x, y of its 25 nodes (98 parameters) at 1 GHz", None),
     "metric": ("meander 167 legs, 10,020 filaments, m = 9,686, 32 freqs 1e5-1e10 Hz", lambda: _workload("metric")),
     "metric_odd": ("meander 167 legs with one segment at 29 x 1, 10,019 filaments, m = 9,685 (odd), "
                    "32 freqs 1e5-1e10 Hz", lambda: _workload("metric_odd")),
@@ -414,12 +414,13 @@ def run_c3(args):
 
 
 def run_c4(args):
-    """dZ/dp of the 6-turn skin-graded spiral at 1 GHz for its 48 width and
-    thickness parameters by the stationary form (fh_gradient: one FP64 solve,
-    one derivative fill, one product per derivative matrix); a step is one
+    """dZ/dp of the 6-turn skin-graded spiral at 1 GHz for its 98 parameters
+    (24 widths, 24 thicknesses, x and y of 25 nodes) by the stationary form
+    (fh_gradient: one FP64 solve, the width / thickness and the coordinate
+    derivative fills, one product per derivative matrix); a step is one
     gradient through the public API.  For comparison, the cost of the same
     gradient by central differences through the public API is estimated as
-    96 x (assembly + one FP64 solve) of the same spiral.  Rank 0 only."""
+    196 x (assembly + one FP64 solve) of the same spiral.  Rank 0 only."""
     import torch
     import fasterhenry_b200 as fh
     from fasterhenry_b200 import fixtures as F
@@ -430,14 +431,17 @@ def run_c4(args):
     deck = F.c4_spiral()
     geometry = fh.Geometry.from_deck(deck)
     system = fh.MeshSystem.assemble(geometry, deck.ports, deck.discretization)
+    nseg, nnodes = len(deck.segments), len(deck.nodes)
+    params = ([fh.Param(k, s) for k in ("width", "thickness") for s in range(nseg)] +
+              [fh.Param(k, v) for v in range(nnodes) for k in ("x", "y")])
     for _ in range(args.warmup):
-        system.gradient(1e9)
+        system.gradient(1e9, params)
     times, reports = [], []
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
             torch.cuda.synchronize()
             t1 = time.perf_counter()
-            g = system.gradient(1e9)
+            g = system.gradient(1e9, params)
             torch.cuda.synchronize()
             times.append(time.perf_counter() - t1)
             reports.append(g.report)
@@ -454,16 +458,20 @@ def run_c4(args):
     fs = fh.fill_stats(system)
     med = lambda k: statistics.median(r[k] for r in reports)
     out = {
-        "metric": "dZ/dp (48 width/thickness params) of a 3,672-filament spiral at 1 GHz, s", "value": round(step, 6),
+        "metric": "dZ/dp (98 params: widths, thicknesses, node x/y) of a 3,672-filament spiral at 1 GHz, s",
+        "value": round(step, 6),
         "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step * 1e3, 3),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOADS["c4"][0], "filaments": counts["filaments"],
                    "internal_meshes": counts["internal_meshes"], "params": len(g.params),
-                   "l2": "derivative matrices 216 MB (> L2); no flush"},
+                   "l2": "derivative matrices 647 MB (> L2); no flush"},
         "solve_s": round(med("solve_s"), 6), "derivative_fill_s": round(med("derivative_fill_s"), 6),
         "contract_s": round(med("contract_s"), 6), "pairs": int(reports[-1]["pairs"]),
         "fill_methods": {k: fs[k] for k in ("point_quadrature", "closed_form", "aligned_quadrature", "orthogonal")},
-        "fd_equivalent_s": round(96 * min(fd_samples), 3),
+        "fd_equivalent_s": round(2 * len(params) * min(fd_samples), 3),
+        "dz_dx_node0": [g.gradient[2 * nseg, 0, 0].real, g.gradient[2 * nseg, 0, 0].imag],
+        "translation_residual": float(np.max(np.abs(g.gradient[2 * nseg::2].sum(axis=0))) /
+                                      np.max(np.abs(g.gradient[2 * nseg:]))),
         "z_ohm": [g.impedance_ohm[0, 0].real, g.impedance_ohm[0, 0].imag],
         "clocks": clocks.summary(),
     }

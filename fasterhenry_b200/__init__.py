@@ -14,7 +14,8 @@ from .api import (DENSE_PATH_MAX_FILAMENTS, MU0, CoincidentSamples, DiscretizeEr
                   solve)
 from .api import (GmresOutcome, GmresParams, IterativeParams, IterativeSystem, PfftError, PfftOperator, PfftParams,
                   Profiler, batch_sweep, fill_stats, gmres_dense)
-from .api import GradientResult, Param, grid_convolution, inductance_gradient, near_pairs, release_cached_memory
+from .api import (GradientResult, Param, coordinate_gradient, grid_convolution, inductance_gradient, near_pairs,
+                  release_cached_memory)
 from .api import CURRENTS_CSV_HEADER, CurrentSolution, InvalidExcitation, unit_excitation
 from .api import DEFAULT_GROUP, Coupling, CouplingError, TruncationWarning
 from . import problem

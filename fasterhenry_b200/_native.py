@@ -136,7 +136,8 @@ EXPORTS = [
     "fh_iterative_pfft_stats", "fh_iterative_sweep", "fh_iterative_destroy", "fh_test_gmres_dense",
     "fh_batch_sweep", "fh_gradient", "fh_test_inductance_gradient", "fh_release_cached_memory", "fh_test_near_pairs",
     "fh_test_grid_convolution",
-    "fh_system_layout", "fh_currents", "fh_system_create_coupled", "fh_system_coupling",
+    "fh_system_layout", "fh_currents", "fh_system_create_coupled", "fh_system_coupling", "fh_iterative_filaments",
+    "fh_iterative_layout", "fh_iterative_currents", "fh_test_coordinate_gradient",
 ]
 
 PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner",
@@ -222,6 +223,13 @@ def load():
     L.fh_system_coupling.argtypes = [ctypes.c_void_p, c_int64_p, c_int64_p, P(TruncationWarning), sz, P(sz)]
     L.fh_currents.argtypes = [ctypes.c_void_p, c_double_p, sz, c_double_p, sz, ctypes.c_int, c_double_p, c_double_p,
                               c_double_p, c_double_p, c_double_p, c_int64_p, c_double_p, P(PowerBalance), ei]
+    L.fh_test_coordinate_gradient.argtypes = [P(Filament), ctypes.POINTER(ctypes.c_int32), sz, c_double_p, c_double_p,
+                                              c_double_p, c_double_p, ei]
+    L.fh_iterative_filaments.argtypes = [ctypes.c_void_p, P(Filament), sz]
+    L.fh_iterative_layout.argtypes = [ctypes.c_void_p, c_int64_p, c_int64_p, c_int64_p]
+    L.fh_iterative_currents.argtypes = [ctypes.c_void_p, c_double_p, sz, c_double_p, sz, c_double_p, c_double_p,
+                                        c_double_p, c_double_p, c_double_p, c_int64_p, c_double_p, P(PowerBalance),
+                                        P(GmresOutcome), ei]
     L.fh_system_destroy.argtypes = [ctypes.c_void_p]
     L.fh_system_destroy.restype = None
     L.fh_system_counts.argtypes = [ctypes.c_void_p, P(Counts)]

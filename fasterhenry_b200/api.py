@@ -640,36 +640,8 @@ class MeshSystem:
         (default: 1 A into port 1, the other ports open) at one frequency or a
         list of them (MeshSystem::currents, solve.rs:845-868): one
         CurrentSolution per frequency."""
-        single = np.ndim(frequency) == 0
-        f = np.ascontiguousarray(np.atleast_1d(frequency), dtype=np.float64)
-        p, n, nseg = self._counts["ports"], self._counts["filaments"], self._counts["segments"]
-        if excitation is None:
-            excitation = unit_excitation(p)
-        exc = np.ascontiguousarray(np.asarray(excitation, dtype=np.complex128).ravel())
-        sof, cos, ncond = self.layout()
-        nf = len(f)
-        cur = np.zeros((nf, n), dtype=np.complex128)
-        dens = np.zeros((nf, n))
-        pw = np.zeros((nf, n))
-        segc = np.zeros((nf, nseg), dtype=np.complex128)
-        segp = np.zeros((nf, nseg))
-        pk = np.zeros((nf, max(1, ncond)), dtype=np.int64)
-        pkd = np.zeros((nf, max(1, ncond)))
-        bal = (N.PowerBalance * max(1, nf))()
-        info = N.ErrorInfo()
-        dp = lambda a: a.ctypes.data_as(N.c_double_p)
-        _check(N.load().fh_currents(self._h, dp(f), nf, exc.ctypes.data_as(N.c_double_p) if len(exc) else None,
-                                    len(exc), int(precision), dp(cur), dp(dens), dp(pw), dp(segc), dp(segp),
-                                    pk.ctypes.data_as(N.c_int64_p), dp(pkd), bal, ctypes.byref(info)), info)
-        fil = self.filaments()
-        centres = 0.5 * (fil[:, 0:3] + fil[:, 3:6])
-        out = []
-        for k in range(nf):
-            out.append(CurrentSolution(float(f[k]), exc.copy(), cur[k], dens[k], pw[k], sof, cos, centres, segc[k],
-                                       segp[k], pk[k, :ncond], pkd[k, :ncond],
-                                       {"dissipated_w": bal[k].dissipated_w, "input_w": bal[k].input_w,
-                                        "relative_residual": bal[k].relative_residual}))
-        return out[0] if single else out
+        return _solve_currents(self, frequency, excitation,
+                               lambda *a: N.load().fh_currents(self._h, *a[:4], int(precision), *a[4:]))
 
     def gradient(self, frequency: float, params: Optional[Sequence["Param"]] = None) -> "GradientResult":
         """dZ/dp at one frequency by the stationary (adjoint) form
@@ -799,6 +771,43 @@ def unit_excitation(ports: int) -> List[complex]:
     return [1.0 + 0j if k == 0 else 0j for k in range(ports)]
 
 
+def _solve_currents(system, frequency, excitation, call):
+    """The shared envelope of MeshSystem.currents and IterativeSystem.currents:
+    output arrays, the C call (``call(freqs, nf, excitation, n_excitation,
+    outputs..., balance, [outcomes,] info)`` with the system's own extras
+    bound), and one CurrentSolution per frequency."""
+    single = np.ndim(frequency) == 0
+    f = np.ascontiguousarray(np.atleast_1d(frequency), dtype=np.float64)
+    c = system.counts()
+    p, n, nseg = c["ports"], c["filaments"], c["segments"]
+    if excitation is None:
+        excitation = unit_excitation(p)
+    exc = np.ascontiguousarray(np.asarray(excitation, dtype=np.complex128).ravel())
+    sof, cos, ncond = system.layout()
+    nf = len(f)
+    cur = np.zeros((nf, n), dtype=np.complex128)
+    dens = np.zeros((nf, n))
+    pw = np.zeros((nf, n))
+    segc = np.zeros((nf, nseg), dtype=np.complex128)
+    segp = np.zeros((nf, nseg))
+    pk = np.zeros((nf, max(1, ncond)), dtype=np.int64)
+    pkd = np.zeros((nf, max(1, ncond)))
+    bal = (N.PowerBalance * max(1, nf))()
+    info = N.ErrorInfo()
+    dp = lambda a: a.ctypes.data_as(N.c_double_p)
+    _check(call(dp(f), nf, exc.ctypes.data_as(N.c_double_p) if len(exc) else None, len(exc), dp(cur), dp(dens),
+                dp(pw), dp(segc), dp(segp), pk.ctypes.data_as(N.c_int64_p), dp(pkd), bal, ctypes.byref(info)), info)
+    fil = system.filaments()
+    centres = 0.5 * (fil[:, 0:3] + fil[:, 3:6])
+    out = []
+    for k in range(nf):
+        out.append(CurrentSolution(float(f[k]), exc.copy(), cur[k], dens[k], pw[k], sof, cos, centres, segc[k],
+                                   segp[k], pk[k, :ncond], pkd[k, :ncond],
+                                   {"dissipated_w": bal[k].dissipated_w, "input_w": bal[k].input_w,
+                                    "relative_residual": bal[k].relative_residual}))
+    return out[0] if single else out
+
+
 @dataclasses.dataclass
 class CurrentSolution:
     """All currents of one frequency and excitation (CurrentSolution,
@@ -876,9 +885,8 @@ def _rust_e(x: float) -> str:
 @dataclasses.dataclass(frozen=True)
 class Param:
     """A geometric parameter of dZ/dp: the "width" or "thickness" of segment
-    ``index``, or the "x" / "y" / "z" coordinate of node ``index`` (node
-    coordinates are rejected with Unsupported: moving a node rotates the
-    segments that meet there)."""
+    ``index``, or the "x" / "y" coordinate of node ``index`` (its segments in
+    a plane z = const; "z" is rejected with Unsupported)."""
     kind: str
     index: int
 
@@ -922,6 +930,24 @@ def inductance_gradient(filaments: np.ndarray, tangents: np.ndarray) -> Tuple[np
                                                 dw.ctypes.data_as(N.c_double_p), dh.ctypes.data_as(N.c_double_p),
                                                 ctypes.byref(info)), info)
     return dw, dh
+
+
+def coordinate_gradient(filaments: np.ndarray, segment: Sequence[int]) -> Tuple[np.ndarray, ...]:
+    """The coordinate derivative fill on its own
+    (fh_test_coordinate_gradient): for filaments (n x 19) and the segment of
+    each, returns (Dl, Dp, Ds, Dr) with D[a, b] = dL_ab / d(coordinate of a):
+    translation along a's length axis, along z x l, stretch of its length,
+    rotation about z through its centre."""
+    f = np.ascontiguousarray(filaments, dtype=np.float64).reshape(-1, FILAMENT_FIELDS)
+    fil = _fil_array(f)
+    n = len(f)
+    seg = np.ascontiguousarray(segment, dtype=np.int32).reshape(-1) if n else np.zeros(1, dtype=np.int32)
+    outs = [np.zeros((n, n), order="F") for _ in range(4)]
+    info = N.ErrorInfo()
+    _check(N.load().fh_test_coordinate_gradient(fil, seg.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), n,
+                                                *[o.ctypes.data_as(N.c_double_p) for o in outs],
+                                                ctypes.byref(info)), info)
+    return tuple(outs)
 
 
 def near_pairs(filaments: np.ndarray, radius: float) -> Tuple[np.ndarray, np.ndarray]:
@@ -1195,6 +1221,38 @@ class IterativeSystem:
         """Z at one frequency with the GMRES outcome of every port."""
         z = self.impedance(frequency)
         return z, self.last_outcomes[0]
+
+    def filaments(self) -> np.ndarray:
+        n = self.counts()["filaments"]
+        out = (N.Filament * max(1, n))()
+        _check(N.load().fh_iterative_filaments(self._h, out, n))
+        return np.frombuffer(out, dtype=np.float64, count=n * FILAMENT_FIELDS).reshape(-1, FILAMENT_FIELDS).copy()
+
+    def layout(self) -> Tuple[np.ndarray, np.ndarray, int]:
+        """(segment of every filament, conductor of every segment, conductor
+        count), as MeshSystem.layout."""
+        c = self.counts()
+        n, nseg = c["filaments"], c["segments"]
+        sof = np.zeros(max(1, n), dtype=np.int64)
+        cos = np.zeros(max(1, nseg), dtype=np.int64)
+        nc = ctypes.c_int64()
+        _check(N.load().fh_iterative_layout(self._h, sof.ctypes.data_as(N.c_int64_p),
+                                            cos.ctypes.data_as(N.c_int64_p), ctypes.byref(nc)))
+        return sof[:n], cos[:nseg], int(nc.value)
+
+    def currents(self, frequency, excitation: Optional[Sequence[complex]] = None):
+        """Filament currents for the port-current phasors ``excitation``
+        (default: 1 A into port 1) at one frequency or a list of them
+        (IterativeSystem::currents, iterative.rs:316-377): one GMRES solve
+        per frequency, one CurrentSolution per frequency; the GMRES outcomes
+        land in ``last_outcomes`` (one list of one outcome per frequency)."""
+        nf = len(np.atleast_1d(frequency))
+        oc = (N.GmresOutcome * max(1, nf))()
+        out = _solve_currents(self, frequency, excitation,
+                              lambda *a: N.load().fh_iterative_currents(self._h, *a[:-1], oc, a[-1]))
+        self.last_outcomes = [[GmresOutcome(int(oc[k].iterations), float(oc[k].relative_residual),
+                                            bool(oc[k].converged))] for k in range(nf)]
+        return out
 
 
 def gmres_dense(a: np.ndarray, b: np.ndarray, x0: Optional[np.ndarray] = None,

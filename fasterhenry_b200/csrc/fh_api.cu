@@ -455,6 +455,8 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     std::vector<int> done(count, 0), grow(count, 0);
     FHB_CUDA(cudaMemcpyAsync(hb.data(), bnorm.p, 8 * count, cudaMemcpyDeviceToHost, st));
     const int kMaxIter = 40;
+    // The error a converged frequency may keep, relative to x.
+    constexpr double kRefineLeft = 1e-12;
     int it = 0;
     for (; it < kMaxIter; ++it) {
         e = convert_c64_to_c32(r.p, d32.p, count * vec, st, err, m, mo);
@@ -483,13 +485,14 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
             // Stopping rule: the correction is negligible (1e-12 of x); or the
             // iteration contracts geometrically (rho = |d_k| / |d_k-1| < 0.1)
             // and the error left after this correction, estimated as
-            // |d_k| rho / (1 - rho), is below 1e-12 of x; or the correction
-            // has stopped shrinking at a level below 1e-10 of x, which is the
-            // attainable accuracy of an FP64 residual (about kappa * u64).
+            // |d_k| rho / (1 - rho), is below kRefineLeft of x; or the
+            // correction has stopped shrinking at a level below 1e-10 of x,
+            // which is the attainable accuracy of an FP64 residual (about
+            // kappa * u64).
             double rel = hx[f] > 0 ? hd[f] / hx[f] : 0.0;
             const bool stalled = hd[f] > 0.5 * prev[f];
             const double rho = std::isfinite(prev[f]) && prev[f] > 0 ? hd[f] / prev[f] : 1.0;
-            const bool contracted = rho < 0.1 && rel * rho / (1.0 - rho) <= 1e-12;
+            const bool contracted = rho < 0.1 && rel * rho / (1.0 - rho) <= kRefineLeft;
             // A small correction is only trusted with a small FP64 residual:
             // |b - A x| <= 1e-6 |b| holds for any accurate x up to kappa ~ 1e10.
             const bool resid_ok = hr[f] <= 1e-6 * hb[f];
@@ -915,39 +918,13 @@ fh_status fh_system_create_coupled(const fh_node *nodes, size_t n_nodes, const f
     FHB_CUDA(cudaStreamSynchronize(cs));
     cudaEventElapsedTime(&s->ms_congruence, c0, c1);
     const double t3 = wall();
-    // Conductors: connected components of the segment graph by union-find
-    // over nodes, numbered in order of their first segment (currents.rs:137-163).
     {
-        std::vector<int64_t> parent(n_nodes);
-        for (size_t v = 0; v < n_nodes; ++v) parent[v] = (int64_t)v;
-        auto find = [&](int64_t x) {
-            while (parent[(size_t)x] != x) {
-                parent[(size_t)x] = parent[(size_t)parent[(size_t)x]];
-                x = parent[(size_t)x];
-            }
-            return x;
-        };
-        for (size_t g = 0; g < n_segments; ++g) {
-            const int64_t a = find(segments[g].a), b = find(segments[g].b);
-            if (a != b) parent[(size_t)a] = b;
-        }
-        std::vector<int64_t> roots;
-        for (size_t g = 0; g < n_segments; ++g) {
-            const int64_t root = find(segments[g].a);
-            auto it = std::find(roots.begin(), roots.end(), root);
-            if (it == roots.end()) {
-                roots.push_back(root);
-                s->conductor_of_segment.push_back((int64_t)roots.size() - 1);
-            } else {
-                s->conductor_of_segment.push_back((int64_t)(it - roots.begin()));
-            }
-        }
-        s->conductors = (int64_t)roots.size();
-        s->segment_first.assign(1, 0);
-        for (size_t g = 0; g < n_segments; ++g) {
-            for (int64_t k = 0; k < s->disc.per_segment[g]; ++k) s->segment_of_filament.push_back((int64_t)g);
-            s->segment_first.push_back(s->segment_first.back() + s->disc.per_segment[g]);
-        }
+        ConductorLayout layout;
+        conductor_layout(segments, n_segments, n_nodes, s->disc.per_segment.data(), layout);
+        s->segment_of_filament = std::move(layout.segment_of_filament);
+        s->conductor_of_segment = std::move(layout.conductor_of_segment);
+        s->segment_first = std::move(layout.segment_first);
+        s->conductors = layout.conductors;
     }
     s->counts = fh_counts{(int64_t)n_nodes, (int64_t)n_segments, n, loops, s->m, s->p};
     s->timing.inductance_s = t2 - t1;
@@ -1245,18 +1222,11 @@ fh_status fh_currents(fh_system *sys, const double *freqs, size_t nf, const doub
     cudaStream_t st = sys->stream;
     // Device layout, once: per branch its (loop, sign) in increasing loop order.
     if (!sys->d_col_ptr) {
-        std::vector<int64_t> col_ptr((size_t)n + 1, 0);
-        for (size_t e = 0; e < sys->loops.branch.size(); ++e) ++col_ptr[(size_t)sys->loops.branch[e] + 1];
-        for (int64_t k = 0; k < n; ++k) col_ptr[(size_t)k + 1] += col_ptr[(size_t)k];
-        std::vector<int32_t> col_loop(sys->loops.branch.size());
-        std::vector<double> col_sign(sys->loops.branch.size());
-        std::vector<int64_t> fillp(col_ptr.begin(), col_ptr.end() - 1);
-        for (int64_t r = 0; r < loops; ++r)
-            for (int64_t e = sys->loops.row_ptr[(size_t)r]; e < sys->loops.row_ptr[(size_t)r + 1]; ++e) {
-                const int64_t slot = fillp[(size_t)sys->loops.branch[(size_t)e]]++;
-                col_loop[(size_t)slot] = (int32_t)r;
-                col_sign[(size_t)slot] = sys->loops.sign[(size_t)e];
-            }
+        TransposedLoops cols;
+        transpose_loops(sys->loops, n, loops, cols);
+        const std::vector<int64_t> &col_ptr = cols.offset;
+        const std::vector<int32_t> &col_loop = cols.loop;
+        const std::vector<double> &col_sign = cols.sign;
         std::vector<double> whr((size_t)(3 * n));
         for (int64_t k = 0; k < n; ++k) {
             whr[(size_t)(3 * k)] = sys->disc.filaments[(size_t)k].width;
@@ -1324,7 +1294,7 @@ fh_status fh_currents(fh_system *sys, const double *freqs, size_t nf, const doub
             e = sweep_chunk_fp64(sys, d_omega.p, count, d_x.p, d_z.p, singular.data(), &ms_factor, err);
             if (e) return e;
         }
-        e = launch_currents(d_x.p, d_ip.p, m, (int)p, n, count, sys->d_col_ptr, sys->d_col_loop, sys->d_col_sign,
+        e = launch_currents(d_x.p, d_ip.p, m, (int)p, false, n, count, sys->d_col_ptr, sys->d_col_loop, sys->d_col_sign,
                             sys->d_whr, sys->d_first, nseg, d_ib.p, d_dens.p, d_pow.p, d_segc.p, d_segp.p, d_segpk.p,
                             d_segi.p, st, err);
         if (e) return e;
@@ -1411,14 +1381,49 @@ fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *
         return fail(err, FH_ERR_INVALID_FREQUENCY,
                     "frequency 0 is " + fstr(frequency_hz) + " Hz; frequencies must be finite and non-negative", 0, -1,
                     frequency_hz);
-    const int64_t nseg = (int64_t)sys->segments.size();
+    const int64_t nseg = (int64_t)sys->segments.size(), nnodes = (int64_t)sys->nodes.size();
+    // Segments that meet at a node (for node-coordinate parameters).
+    std::vector<std::vector<int64_t>> at_node((size_t)nnodes);
+    for (int64_t g = 0; g < nseg; ++g) {
+        at_node[(size_t)sys->segments[(size_t)g].a].push_back(g);
+        at_node[(size_t)sys->segments[(size_t)g].b].push_back(g);
+    }
+    std::vector<int64_t> first_fil((size_t)nseg + 1, 0);
+    for (int64_t g = 0; g < nseg; ++g) first_fil[(size_t)g + 1] = first_fil[(size_t)g] + sys->disc.per_segment[(size_t)g];
+    bool want_dims = false, want_coords = false;
+    std::vector<uint8_t> seg_moves((size_t)nseg, 0);
     for (size_t k = 0; k < np; ++k) {
         const fh_param_spec &q = params[k];
-        if (q.kind == FH_PARAM_NODE_X || q.kind == FH_PARAM_NODE_Y || q.kind == FH_PARAM_NODE_Z)
+        if (q.kind == FH_PARAM_NODE_X || q.kind == FH_PARAM_NODE_Y) {
+            if (q.index < 0 || q.index >= nnodes)
+                return fail(err, FH_ERR_INVALID_ARGUMENT,
+                            "parameter " + std::to_string(k) + " names node " + std::to_string(q.index) +
+                                ", but the geometry has " + std::to_string(nnodes),
+                            (int64_t)k, q.index);
+            // A node moving in the xy plane turns its segments about z: every
+            // filament of them must lie in the plane with z along one of its
+            // cross-section axes, so that its frame turns with it.
+            for (int64_t g : at_node[(size_t)q.index]) {
+                const fh_filament &f = sys->disc.filaments[(size_t)first_fil[(size_t)g]];
+                const bool flat = std::fabs(f.dir_length[2]) <= 1e-12 &&
+                                  (std::fabs(std::fabs(f.dir_width[2]) - 1.0) <= 1e-12 ||
+                                   std::fabs(std::fabs(f.dir_height[2]) - 1.0) <= 1e-12);
+                if (!flat)
+                    return fail(err, FH_ERR_UNSUPPORTED,
+                                "parameter " + std::to_string(k) + " moves node " + std::to_string(q.index) +
+                                    ", which segment " + std::to_string(g) +
+                                    " joins; node-coordinate derivatives need segments in a plane z = const "
+                                    "with z along their width or height",
+                                (int64_t)k, g);
+                seg_moves[(size_t)g] = 1;
+            }
+            want_coords = true;
+            continue;
+        }
+        if (q.kind == FH_PARAM_NODE_Z)
             return fail(err, FH_ERR_UNSUPPORTED,
                         "parameter " + std::to_string(k) +
-                            " is a node coordinate: moving a node rotates the segments that meet there, and the "
-                            "derivative of the partial inductances under a rotation is not provided",
+                            " is a node's z coordinate; node-coordinate derivatives are provided for x and y",
                         (int64_t)k);
         if (q.kind != FH_PARAM_WIDTH && q.kind != FH_PARAM_THICKNESS)
             return fail(err, FH_ERR_INVALID_ARGUMENT, "parameter " + std::to_string(k) + " has an unknown kind",
@@ -1428,6 +1433,7 @@ fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *
                         "parameter " + std::to_string(k) + " names segment " + std::to_string(q.index) +
                             ", but the geometry has " + std::to_string(nseg),
                         (int64_t)k, q.index);
+        want_dims = true;
     }
     FHB_CUDA(cudaSetDevice(sys->device));
     const double t0 = wall();
@@ -1494,11 +1500,13 @@ fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *
             }
         }
     }
-    // 4. Derivative fill and the products with the branch currents.
+    // 4. Derivative fills and the products with the branch currents.
     size_t free_b = 0, total_b = 0;
     FHB_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t part = gradient_part_elems(n, (int)p);
-    const double need = 16.0 * (double)n * (double)n + 8.0 * (double)(part + 6 * n * p) + 288.0 * (double)n;
+    const double need = (want_dims ? 16.0 : 0.0) * (double)n * (double)n +
+                        (want_coords ? 32.0 * (double)n * (double)n + 64.0 * (double)(n * p) : 0.0) +
+                        8.0 * (double)(part + 6 * n * p) + 296.0 * (double)n;
     if (need > 0.9 * (double)free_b)
         return fail(err, FH_ERR_OUT_OF_MEMORY,
                     "the derivative fill of " + std::to_string(n) + " filaments needs " + fstr(need) +
@@ -1507,17 +1515,34 @@ fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *
     for (int64_t i = 0; i < n; ++i) h[(size_t)i] = make_devfil(sys->disc.filaments[(size_t)i]);
     DBuf<DevFil> d_fil(st);
     DBuf<FilTan> d_tan(st);
-    DBuf<double> d_D(st), d_I(st), d_y(st), d_part(st);
+    DBuf<double> d_D(st), d_I(st), d_y(st), d_part(st), d_C(st), d_yc(st);
+    DBuf<int32_t> d_seg(st);
+    DBuf<uint8_t> d_move(st);
     FHB_ALLOC(d_fil, (size_t)n);
     FHB_ALLOC(d_tan, (size_t)n);
-    FHB_ALLOC(d_D, (size_t)(2 * n * n));
+    FHB_ALLOC(d_D, (size_t)(want_dims ? 2 * n * n : 1));
     FHB_ALLOC(d_I, (size_t)(2 * n * p));
     FHB_ALLOC(d_y, (size_t)(4 * n * p));
     FHB_ALLOC(d_part, part);
     FHB_CUDA(cudaMemcpyAsync(d_fil.p, h.data(), sizeof(DevFil) * n, cudaMemcpyHostToDevice, st));
     FHB_CUDA(cudaMemcpyAsync(d_tan.p, tan.data(), sizeof(FilTan) * n, cudaMemcpyHostToDevice, st));
     FHB_CUDA(cudaMemcpyAsync(d_I.p, ib.data(), 8 * ib.size(), cudaMemcpyHostToDevice, st));
-    FHB_CUDA(cudaMemsetAsync(d_D.p, 0, 16 * (size_t)n * n, st));
+    if (want_dims) FHB_CUDA(cudaMemsetAsync(d_D.p, 0, 16 * (size_t)n * n, st));
+    std::vector<int32_t> seg32((size_t)n);
+    std::vector<uint8_t> move((size_t)n);
+    if (want_coords) {
+        for (int64_t i = 0; i < n; ++i) {
+            seg32[(size_t)i] = (int32_t)seg_of[(size_t)i];
+            move[(size_t)i] = seg_moves[(size_t)seg_of[(size_t)i]];
+        }
+        FHB_ALLOC(d_C, (size_t)(4 * n * n));
+        FHB_ALLOC(d_yc, (size_t)(8 * n * p));
+        FHB_ALLOC(d_seg, (size_t)n);
+        FHB_ALLOC(d_move, (size_t)n);
+        FHB_CUDA(cudaMemcpyAsync(d_seg.p, seg32.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, st));
+        FHB_CUDA(cudaMemcpyAsync(d_move.p, move.data(), (size_t)n, cudaMemcpyHostToDevice, st));
+        FHB_CUDA(cudaMemsetAsync(d_C.p, 0, 32 * (size_t)n * n, st));
+    }
     cudaEvent_t ev[3];
     for (auto &v : ev) FHB_CUDA(cudaEventCreate(&v));
     struct EvGuard {
@@ -1526,17 +1551,36 @@ fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *
             for (int k = 0; k < 3; ++k) cudaEventDestroy(ev[k]);
         }
     } evg{ev};
-    FillStats fs;
+    FillStats fs, fc;
     FHB_CUDA(cudaEventRecord(ev[0], st));
     const PairMaskDev pm = sys->mask();
-    e = device_fill_grad(d_fil.p, d_tan.p, n, GradOut{d_D.p, d_D.p + n * n}, st, &fs, err, &pm);
-    if (e) return e;
+    if (want_dims) {
+        e = device_fill_grad(d_fil.p, d_tan.p, n, GradOut{d_D.p, d_D.p + n * n}, st, &fs, err, &pm);
+        if (e) return e;
+    }
+    if (want_coords) {
+        const size_t nn = (size_t)(n * n);
+        e = device_fill_coord(d_fil.p, d_seg.p, d_move.p, n,
+                              CoordOut{d_C.p, d_C.p + nn, d_C.p + 2 * nn, d_C.p + 3 * nn}, st, &fc, err, &pm);
+        if (e) return e;
+    }
     FHB_CUDA(cudaEventRecord(ev[1], st));
-    e = gradient_products(d_D.p, d_D.p + n * n, n, d_I.p, (int)p, d_y.p, d_part.p, st, err);
-    if (e) return e;
+    if (want_dims) {
+        e = gradient_products(d_D.p, d_D.p + n * n, n, d_I.p, (int)p, d_y.p, d_part.p, st, err);
+        if (e) return e;
+    }
+    if (want_coords) {
+        const size_t nn = (size_t)(n * n);
+        e = gradient_products(d_C.p, d_C.p + nn, n, d_I.p, (int)p, d_yc.p, d_part.p, st, err);
+        if (e) return e;
+        e = gradient_products(d_C.p + 2 * nn, d_C.p + 3 * nn, n, d_I.p, (int)p, d_yc.p + 4 * n * p, d_part.p, st,
+                              err);
+        if (e) return e;
+    }
     FHB_CUDA(cudaEventRecord(ev[2], st));
-    std::vector<double> y((size_t)(4 * n * p));
-    FHB_CUDA(cudaMemcpyAsync(y.data(), d_y.p, 8 * y.size(), cudaMemcpyDeviceToHost, st));
+    std::vector<double> y((size_t)(4 * n * p)), yc(want_coords ? (size_t)(8 * n * p) : 0);
+    if (want_dims) FHB_CUDA(cudaMemcpyAsync(y.data(), d_y.p, 8 * y.size(), cudaMemcpyDeviceToHost, st));
+    if (want_coords) FHB_CUDA(cudaMemcpyAsync(yc.data(), d_yc.p, 8 * yc.size(), cudaMemcpyDeviceToHost, st));
     FHB_CUDA(cudaStreamSynchronize(st));
     float ms_fill = 0, ms_prod = 0;
     cudaEventElapsedTime(&ms_fill, ev[0], ev[1]);
@@ -1552,19 +1596,75 @@ fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *
         return C(y[o], y[o + 1]);
     };
     const C jw(0.0, omega);
-    for (int64_t i = 0; i < n; ++i) {
-        const fh_filament &f = sys->disc.filaments[(size_t)i];
-        const double r = sys->resistances[(size_t)i];
-        const double dr[2] = {-r * tan[(size_t)i].gw / f.width, -r * tan[(size_t)i].gh / f.height};
-        for (int which = 0; which < 2; ++which) {
-            C *out = acc.data() + (size_t)(2 * seg_of[(size_t)i] + which) * pp;
-            for (int64_t a = 0; a < p; ++a)
-                for (int64_t b = 0; b < p; ++b)
-                    out[a * p + b] += I(a, i) * I(b, i) * dr[which] + jw * (I(a, i) * Y(which, b, i) + I(b, i) * Y(which, a, i));
+    if (want_dims)
+        for (int64_t i = 0; i < n; ++i) {
+            const fh_filament &f = sys->disc.filaments[(size_t)i];
+            const double r = sys->resistances[(size_t)i];
+            const double dr[2] = {-r * tan[(size_t)i].gw / f.width, -r * tan[(size_t)i].gh / f.height};
+            for (int which = 0; which < 2; ++which) {
+                C *out = acc.data() + (size_t)(2 * seg_of[(size_t)i] + which) * pp;
+                for (int64_t a = 0; a < p; ++a)
+                    for (int64_t b = 0; b < p; ++b)
+                        out[a * p + b] += I(a, i) * I(b, i) * dr[which] +
+                                          jw * (I(a, i) * Y(which, b, i) + I(b, i) * Y(which, a, i));
+            }
         }
-    }
+    // Node coordinates: a node moving by e (x or y) moves the segment a -> b
+    // with da or db = e; every filament of it stretches by dl = l . (db - da),
+    // turns about z by dphi = (z x l) . (db - da) / length, and its centre
+    // moves by (da + db) / 2 + dphi z x (c - (a + b) / 2).  Its resistance
+    // changes by R dl / length.
+    auto YC = [&](int which, int64_t q, int64_t i) {
+        const size_t o = (size_t)(2 * (((int64_t)which * p + q) * n + i));
+        return C(yc[o], yc[o + 1]);
+    };
+    auto node_grad = [&](int64_t node, int axis, C *out) {
+        for (size_t q = 0; q < pp; ++q) out[q] = C(0.0, 0.0);
+        for (int64_t g : at_node[(size_t)node]) {
+            const fh_segment_def &sd = sys->segments[(size_t)g];
+            const fh_node &na = sys->nodes[(size_t)sd.a], &nb = sys->nodes[(size_t)sd.b];
+            double da[3] = {0, 0, 0}, db[3] = {0, 0, 0};
+            if (sd.a == node) da[axis] = 1.0;
+            if (sd.b == node) db[axis] = 1.0;
+            const double span[3] = {nb.x - na.x, nb.y - na.y, nb.z - na.z};
+            const double len = std::sqrt(span[0] * span[0] + span[1] * span[1] + span[2] * span[2]);
+            const double l[3] = {span[0] / len, span[1] / len, span[2] / len};
+            const double dd[3] = {db[0] - da[0], db[1] - da[1], db[2] - da[2]};
+            const double dl = l[0] * dd[0] + l[1] * dd[1] + l[2] * dd[2];
+            const double dphi = (-l[1] * dd[0] + l[0] * dd[1]) / len;
+            const double mid[3] = {0.5 * (na.x + nb.x), 0.5 * (na.y + nb.y), 0.5 * (na.z + nb.z)};
+            for (int64_t i = first_fil[(size_t)g]; i < first_fil[(size_t)g + 1]; ++i) {
+                const fh_filament &f = sys->disc.filaments[(size_t)i];
+                const double o[3] = {0.5 * (f.start[0] + f.end[0]) - mid[0], 0.5 * (f.start[1] + f.end[1]) - mid[1],
+                                     0.5 * (f.start[2] + f.end[2]) - mid[2]};
+                const double dc[3] = {0.5 * (da[0] + db[0]) - dphi * o[1], 0.5 * (da[1] + db[1]) + dphi * o[0],
+                                      0.5 * (da[2] + db[2])};
+                const double *fl = f.dir_length;
+                double pl[3] = {-fl[1], fl[0], 0.0};
+                const double pn = std::sqrt(pl[0] * pl[0] + pl[1] * pl[1]);
+                for (double &v : pl) v = pn > 0.0 ? v / pn : 0.0;
+                const double dq[4] = {dc[0] * fl[0] + dc[1] * fl[1] + dc[2] * fl[2], dc[0] * pl[0] + dc[1] * pl[1], dl,
+                                      dphi};
+                const double drl = sys->resistances[(size_t)i] * dl / f.length;
+                for (int64_t a = 0; a < p; ++a)
+                    for (int64_t b = 0; b < p; ++b) {
+                        C sum(0.0, 0.0);
+                        for (int w = 0; w < 4; ++w)
+                            if (dq[w] != 0.0) sum += dq[w] * (I(a, i) * YC(w, b, i) + I(b, i) * YC(w, a, i));
+                        out[a * p + b] += I(a, i) * I(b, i) * drl + jw * sum;
+                    }
+            }
+        }
+    };
+    std::vector<C> node_out(pp);
     for (size_t k = 0; k < np; ++k) {
-        const C *src = acc.data() + (size_t)(2 * params[k].index + (params[k].kind == FH_PARAM_THICKNESS)) * pp;
+        const C *src;
+        if (params[k].kind == FH_PARAM_NODE_X || params[k].kind == FH_PARAM_NODE_Y) {
+            node_grad(params[k].index, params[k].kind == FH_PARAM_NODE_X ? 0 : 1, node_out.data());
+            src = node_out.data();
+        } else {
+            src = acc.data() + (size_t)(2 * params[k].index + (params[k].kind == FH_PARAM_THICKNESS)) * pp;
+        }
         for (size_t q = 0; q < pp; ++q) {
             dz_out[2 * (k * pp + q)] = src[q].real();
             dz_out[2 * (k * pp + q) + 1] = src[q].imag();
@@ -1576,7 +1676,7 @@ fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *
         report->derivative_fill_s = ms_fill * 1e-3;
         report->contract_s = ms_prod * 1e-3;
         report->total_s = wall() - t0;
-        report->pairs = fs.pairs;
+        report->pairs = want_dims ? fs.pairs : fc.pairs;
     }
     return FH_OK;
 }
@@ -1610,6 +1710,43 @@ fh_status fh_test_inductance_gradient(const fh_filament *filaments, const double
     if (st) return st;
     FHB_CUDA(cudaMemcpyAsync(Dw, d_D.p, 8 * n * n, cudaMemcpyDeviceToHost, s));
     FHB_CUDA(cudaMemcpyAsync(Dh, d_D.p + n * n, 8 * n * n, cudaMemcpyDeviceToHost, s));
+    FHB_CUDA(cudaStreamSynchronize(s));
+    return FH_OK;
+}
+
+fh_status fh_test_coordinate_gradient(const fh_filament *filaments, const int32_t *segment, size_t n, double *Dl,
+                                      double *Dp, double *Ds, double *Dr, fh_error_info *err) {
+    clear_error(err);
+    if (n && (!filaments || !segment || !Dl || !Dp || !Ds || !Dr))
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "null argument");
+    fh_status st = ensure_device(err);
+    if (st) return st;
+    if (n == 0) return FH_OK;
+    std::vector<DevFil> h(n);
+    for (size_t i = 0; i < n; ++i) h[i] = make_devfil(filaments[i]);
+    const std::vector<uint8_t> move(n, 1);
+    DBuf<DevFil> d_fil;
+    DBuf<int32_t> d_seg;
+    DBuf<uint8_t> d_move;
+    DBuf<double> d_D;
+    FHB_ALLOC(d_fil, n);
+    FHB_ALLOC(d_seg, n);
+    FHB_ALLOC(d_move, n);
+    FHB_ALLOC(d_D, 4 * n * n);
+    cudaStream_t s;
+    FHB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    std::unique_ptr<CUstream_st, decltype(&cudaStreamDestroy)> guard(s, &cudaStreamDestroy);
+    FHB_CUDA(cudaMemcpyAsync(d_fil.p, h.data(), n * sizeof(DevFil), cudaMemcpyHostToDevice, s));
+    FHB_CUDA(cudaMemcpyAsync(d_seg.p, segment, n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    FHB_CUDA(cudaMemcpyAsync(d_move.p, move.data(), n, cudaMemcpyHostToDevice, s));
+    FHB_CUDA(cudaMemsetAsync(d_D.p, 0, 32 * n * n, s));
+    const size_t nn = n * n;
+    st = device_fill_coord(d_fil.p, d_seg.p, d_move.p, (int64_t)n,
+                           CoordOut{d_D.p, d_D.p + nn, d_D.p + 2 * nn, d_D.p + 3 * nn}, s, nullptr, err);
+    if (st) return st;
+    double *outs[4] = {Dl, Dp, Ds, Dr};
+    for (int k = 0; k < 4; ++k)
+        FHB_CUDA(cudaMemcpyAsync(outs[k], d_D.p + k * nn, 8 * nn, cudaMemcpyDeviceToHost, s));
     FHB_CUDA(cudaStreamSynchronize(s));
     return FH_OK;
 }

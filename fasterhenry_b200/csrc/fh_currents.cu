@@ -14,9 +14,10 @@ namespace fhb {
 namespace {
 
 // Thread per (frequency, filament).  X holds Z_ee^-1 Z_ep per frequency
-// (count x p x m complex); the internal loop currents are -X I_p.
+// (count x p x m complex) and the internal loop currents are -X I_p; or, with
+// `applied`, X holds Z_ee^-1 Z_ep I_p itself (count x m).
 __global__ void branch_currents_kernel(const double2 *__restrict__ X, const double2 *__restrict__ ip, int64_t m,
-                                       int p, int64_t n, int count, const int64_t *__restrict__ col_ptr,
+                                       int p, bool applied, int64_t n, int count, const int64_t *__restrict__ col_ptr,
                                        const int32_t *__restrict__ col_loop, const double *__restrict__ col_sign,
                                        const double *__restrict__ whr, double2 *__restrict__ ib,
                                        double *__restrict__ dens, double *__restrict__ pow) {
@@ -29,7 +30,11 @@ __global__ void branch_currents_kernel(const double2 *__restrict__ X, const doub
             const int64_t r = col_loop[e];
             const double s = col_sign[e];
             double xr, xi;
-            if (r < m) {
+            if (r < m && applied) {
+                const double2 x = X[(int64_t)f * m + r];
+                xr = -x.x;
+                xi = -x.y;
+            } else if (r < m) {
                 double ar = 0.0, ai = 0.0;
                 for (int q = 0; q < p; ++q) {
                     const double2 x = X[((int64_t)f * p + q) * m + r], c = ip[q];
@@ -81,7 +86,7 @@ __global__ void segment_sums_kernel(const double2 *__restrict__ ib, const double
 
 }  // namespace
 
-fh_status launch_currents(const double *d_x, const double *d_ip, int64_t m, int p, int64_t n, int count,
+fh_status launch_currents(const double *d_x, const double *d_ip, int64_t m, int p, bool applied, int64_t n, int count,
                           const int64_t *d_col_ptr, const int32_t *d_col_loop, const double *d_col_sign,
                           const double *d_whr, const int64_t *d_first, int64_t nseg, double *d_ib, double *d_dens,
                           double *d_pow, double *d_seg_cur, double *d_seg_pow, double *d_seg_peak,
@@ -90,7 +95,7 @@ fh_status launch_currents(const double *d_x, const double *d_ip, int64_t m, int 
     if (total) {
         const unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 32);
         branch_currents_kernel<<<blocks, 256, 0, s>>>(
-            reinterpret_cast<const double2 *>(d_x), reinterpret_cast<const double2 *>(d_ip), m, p, n, count,
+            reinterpret_cast<const double2 *>(d_x), reinterpret_cast<const double2 *>(d_ip), m, p, applied, n, count,
             d_col_ptr, d_col_loop, d_col_sign, d_whr, reinterpret_cast<double2 *>(d_ib), d_dens, d_pow);
         FHB_CUDA(cudaGetLastError());
     }

@@ -114,6 +114,24 @@ struct GradOut {
 fh_status device_fill_grad(const DevFil *d_fil, const FilTan *d_tan, int64_t n, GradOut out, cudaStream_t stream,
                            FillStats *stats, fh_error_info *err, const PairMaskDev *mask = nullptr);
 
+// Outputs of the coordinate derivative fill: n x n column-major,
+// D[a + b n] = the derivative of L_ab with respect to a coordinate of
+// filament a (b held fixed): translation of its centre along its length axis
+// (Dl) and along z x l normalized (Dp), stretch of its length about its
+// centre (Ds), rotation about the z axis through its centre (Dr).  Pairs of
+// one segment (equal d_seg) get Ds only; the diagonal of Ds holds half of
+// dL_aa / d length.
+struct CoordOut {
+    double *Dl, *Dp, *Ds, *Dr;
+};
+// Pairs with a moving filament (d_move[i] != 0); the four matrices must be
+// zero-filled by the caller.  Pairs evaluated by sampled filaments, and
+// parallel pairs of different segments whose cross-sections meet when
+// projected along their length: FH_ERR_UNSUPPORTED.
+fh_status device_fill_coord(const DevFil *d_fil, const int32_t *d_seg, const uint8_t *d_move, int64_t n,
+                            CoordOut out, cudaStream_t stream, FillStats *stats, fh_error_info *err,
+                            const PairMaskDev *mask = nullptr);
+
 // y = D_w I and D_h I for p complex vectors I (n x p, column q at 2 q n):
 // y holds 2 x p columns (D_w's products first).  d_part is scratch of
 // gradient_part_elems(n, p) doubles.
@@ -123,12 +141,13 @@ size_t gradient_part_elems(int64_t n, int p);
 
 // Branch currents, |J|, power per filament and per-segment sums / peaks for
 // `count` frequencies from X = Z_ee^-1 Z_ep (count x p x m complex) and the
-// excitation d_ip (p complex).  The transposed loop basis lists, per branch,
+// excitation d_ip (p complex); with `applied`, d_x holds Z_ee^-1 Z_ep I_p
+// (count x m complex) instead.  The transposed loop basis lists, per branch,
 // (loop, sign) in increasing loop order; d_whr holds (w, h, R) per filament,
 // d_first the first filament of each segment (nseg + 1).  Outputs are count x
 // n (complex / real) and count x nseg.
-fh_status launch_currents(const double *d_x, const double *d_ip, int64_t m, int p, int64_t n, int count,
-                          const int64_t *d_col_ptr, const int32_t *d_col_loop, const double *d_col_sign,
+fh_status launch_currents(const double *d_x, const double *d_ip, int64_t m, int p, bool applied, int64_t n,
+                          int count, const int64_t *d_col_ptr, const int32_t *d_col_loop, const double *d_col_sign,
                           const double *d_whr, const int64_t *d_first, int64_t nseg, double *d_ib, double *d_dens,
                           double *d_pow, double *d_seg_cur, double *d_seg_pow, double *d_seg_peak,
                           int64_t *d_seg_idx, cudaStream_t s, fh_error_info *err);

@@ -115,6 +115,48 @@ __device__ bool aligned_bars(const DevFil &a, const DevFil &b, Aligned *o) {
     return true;
 }
 
+// Work-item flags of the coordinate derivative fill (int4.w).
+constexpr int kCoordTauMask = 3;   // a's cross-section axis along z x l_a: 1 width, 2 height, 0 none
+constexpr int kCoordSigmaNeg = 4;  // z x l_a points along minus that axis
+constexpr int kCoordRot = 8;       // rotation derivatives wanted
+constexpr int kCoordOrtho = 16;    // orthogonal pair, as two boxes in a's frame (ortho_aligned)
+constexpr int kCoordSame = 32;     // both filaments in one segment: stretch derivatives only
+
+// z x l: how a unit vector l changes per unit rotation about the z axis.
+__device__ __forceinline__ void zcross(const double *l, double o[3]) {
+    o[0] = -l[1];
+    o[1] = l[0];
+    o[2] = 0.0;
+}
+
+// An orthogonal pair as two boxes in a's frame: b's extents along a's axes,
+// each of b's axes coinciding with one of a's up to sign (false otherwise).
+// Its bar integral is the scalar coupling  int int 1/|r - r'|  of the two
+// volumes, whose rate under a rotation gives an orthogonal pair's derivative.
+__device__ bool ortho_aligned(const DevFil &a, const DevFil &b, Aligned *o) {
+    double ext[3] = {0.0, 0.0, 0.0};
+    for (int m = 0; m < 3; ++m) {
+        int hit = -1;
+        for (int k = 0; k < 3; ++k)
+            if (fabs(ndot(b.axes + 3 * m, a.axes + 3 * k)) > 1.0 - 1e-12) hit = k;
+        if (hit < 0) return false;
+        ext[hit] += 2.0 * b.half[m];
+    }
+    if (o) {
+        const double delta[3] = {b.centre[0] - a.centre[0], b.centre[1] - a.centre[1], b.centre[2] - a.centre[2]};
+        o->length[0] = 2.0 * a.half[0];
+        o->length[1] = ext[0];
+        o->width[0] = 2.0 * a.half[1];
+        o->width[1] = ext[1];
+        o->height[0] = 2.0 * a.half[2];
+        o->height[1] = ext[2];
+        o->offset[0] = ndot(delta, a.axes);
+        o->offset[1] = ndot(delta, a.axes + 3);
+        o->offset[2] = ndot(delta, a.axes + 6);
+    }
+    return true;
+}
+
 struct Classified {
     int cat;          // -1 orthogonal
     int orders;       // packed 5-bit orders (point), 6 fields
@@ -569,6 +611,11 @@ __device__ __forceinline__ bool lines_parallel(double l1, double l2, double offs
 struct QuadCtx {
     Aligned b;
     double axial_start;
+    // coordinate derivatives: a's in-plane transverse axis (1 width, 2
+    // height), its sign, and whether the rotation integrals are wanted
+    int tau;
+    int rot;
+    double sigma;
 };
 __device__ __forceinline__ double integrand(const QuadCtx &c, double u, double v) {
     double weight = overlap_weight(c.b.width[0], c.b.width[1], c.b.offset[1], u) *
@@ -654,18 +701,120 @@ __device__ __forceinline__ void integrand_grad(const QuadCtx &c, double u, doubl
     }
 }
 
-// kGrad: values[7 h + 0..6] = the integral and its partials with respect to
-// (width[0], width[1], offset[1], height[0], height[1], offset[2]), the rule
-// (panel tree, leaves, nodes) held at the pair's own geometry.
-template <bool kGrad>
+// Axial terms of two parallel lines A = [0, l1] and B = [as, as + l2] at
+// transverse distance rho (the coordinates of lines_parallel): the kernel
+// k = int int 1/R, its partials with respect to as, l1 and l2, and with
+// `moments` the first moments j1 = int int (x - l1/2) / R^3 and
+// j1b = int int (x' - as - l2/2) / R^3 (x on A, x' on B) that a rotation of
+// either line about its midpoint weighs.  Every double integral of a
+// function of x' - x over the rectangle is F(as + l2) - F(as) - F(as + l2 -
+// l1) + F(as - l1) for a second antiderivative F: here R(t) / rho^2 for
+// 1/R^3, and t R(t) / (2 rho^2) - asinh(t / rho) / 2 for t / R^3 after one
+// integration by parts.  The partials of lines_parallel follow its own
+// split: d/dq of |q| log(|q| + R) - R is sign(q) log(|q| + R), and the
+// -2 overlap log(rho) term moves with the overlap (a tie of the min / max
+// it is made of takes the mean of the two one-sided rates, consistent with
+// sign(0) = 0 on the primitive).
+struct LineTerms {
+    double k, das, dl1, dl2, j1, j1b;
+};
+__device__ __forceinline__ double parallel_primitive_d(double q, double rho_sq) {
+    if (q == 0.0) return 0.0;
+    const double aq = fabs(q);
+    const double l = log(aq + sqrt(aq * aq + rho_sq));  // sign(q) times it; negative for lengths below 1 m
+    return q > 0.0 ? l : -l;
+}
+__device__ bool line_terms(double l1, double l2, double as, double rho, bool moments, LineTerms *t) {
+    if (!lines_parallel(l1, l2, as, rho, &t->k)) return false;
+    const double r2 = rho * rho;
+    const double e = as + l2;
+    const double pa = parallel_primitive_d(e, r2), pb = parallel_primitive_d(as, r2);
+    const double pc = parallel_primitive_d(e - l1, r2), pd = parallel_primitive_d(as - l1, r2);
+    t->das = pa - pb - pc + pd;
+    t->dl1 = pc - pd;
+    t->dl2 = pa - pc;
+    const double overlap = rmax(rmin(l1, e) - rmax(as, 0.0), 0.0);
+    if (overlap > 0.0) {
+        const double hi = l1 < e ? 1.0 : (l1 == e ? 0.5 : 0.0);    // d min(l1, e) / d l1
+        const double lo = as > 0.0 ? 1.0 : (as == 0.0 ? 0.5 : 0.0);  // d max(as, 0) / d as
+        const double lr = 2.0 * log(rho);
+        t->dl1 -= lr * hi;
+        t->dl2 -= lr * (1.0 - hi);
+        t->das -= lr * ((1.0 - hi) - lo);
+    }
+    t->j1 = t->j1b = 0.0;
+    if (moments && r2 > 0.0) {
+        auto R = [&](double x) { return sqrt(x * x + r2); };
+        auto psi = [&](double x) { return x * R(x) / (2.0 * r2) - 0.5 * asinh(x / rho); };
+        const double a = as, b = e;
+        const double i00 = (R(b) - R(b - l1) - R(a) + R(a - l1)) / r2;
+        const double i10 = (b * (R(b) - R(b - l1)) / r2 + psi(b - l1) - psi(b)) -
+                           (a * (R(a) - R(a - l1)) / r2 + psi(a - l1) - psi(a));
+        const double i01 = i10 - t->das;  // int int (x' - x) / R^3 = -dk/das
+        t->j1 = i10 - 0.5 * l1 * i00;
+        t->j1b = i01 - (as + 0.5 * l2) * i00;
+    }
+    return true;
+}
+
+// The integrand of the coordinate derivatives at relative cross-section
+// offset (u, v) (b minus a): g[0] the value, g[1] d/d offset[0], g[2]
+// d/d offset[1], g[3] d/d offset[2], g[4] d/d length[0], g[5] d/d length[1]
+// (each length stretched about its own centre: as = offset[0] + (length[0] -
+// length[1]) / 2), and with c.rot the rates g[6], g[7] of the integral under
+// a rotation of a, resp. b, about the z axis through its centre.  For a,
+// the rotation moves a point at axial s and transverse t (along
+// p = z x l = sigma e_tau) by s p - t l, so the rate is
+//   sigma [u_tau W j1 + m_tau w_other dk/das],
+// m_tau = int y_tau dy_tau over the overlap at this offset (a's first
+// moment); for b, with its own centred coordinates,
+//   -sigma [u_tau W j1b + (m_tau + (u_tau - offset_tau) w_tau) w_other dk/das].
+__device__ __forceinline__ void integrand_coord(const QuadCtx &c, double u, double v, double g[8]) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) g[k] = 0.0;
+    double dw[3], dh[3];
+    const double ww = overlap_weight_grad(c.b.width[0], c.b.width[1], c.b.offset[1], u, dw);
+    const double wh = overlap_weight_grad(c.b.height[0], c.b.height[1], c.b.offset[2], v, dh);
+    if (ww == 0.0 || wh == 0.0) return;
+    LineTerms t;
+    if (!line_terms(c.b.length[0], c.b.length[1], c.axial_start, hypot(u, v), c.rot != 0, &t)) return;
+    const double W = ww * wh;
+    g[0] = W * t.k;
+    g[1] = W * t.das;
+    g[2] = dw[2] * wh * t.k;
+    g[3] = ww * dh[2] * t.k;
+    g[4] = W * (t.dl1 + 0.5 * t.das);
+    g[5] = W * (t.dl2 - 0.5 * t.das);
+    if (c.rot) {
+        const bool ty = c.tau == 1;
+        const double ut = ty ? u : v;
+        const double e1 = ty ? c.b.width[0] : c.b.height[0], e2 = ty ? c.b.width[1] : c.b.height[1];
+        const double ot = ty ? c.b.offset[1] : c.b.offset[2];
+        const double hi = rmin(0.5 * e1, ot + 0.5 * e2 - ut), lo = rmax(-0.5 * e1, ot - 0.5 * e2 - ut);
+        const double wt = hi - lo;
+        const double m = 0.5 * (hi * hi - lo * lo);
+        const double wo = ty ? wh : ww;
+        g[6] = c.sigma * (ut * W * t.j1 + m * wo * t.das);
+        g[7] = -c.sigma * (ut * W * t.j1b + (m + (ut - ot) * wt) * wo * t.das);
+    }
+}
+
+// kMode 0: values[h] = the integral.  kMode 1: values[7 h + 0..6] = the
+// integral and its partials with respect to (width[0], width[1], offset[1],
+// height[0], height[1], offset[2]).  kMode 2: values[8 h + 0..7] = the
+// coordinate derivatives of integrand_coord (the work item's flags choose
+// the frame and the rotation axis).  The rule (panel tree, leaves, nodes) is
+// held at the pair's own geometry.
+template <int kMode>
 __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
     const DevFil *__restrict__ fil, const int4 *__restrict__ items, const int64_t *__restrict__ heads,
     int64_t n_heads, double *__restrict__ values) {
+    constexpr int kVals = kMode == 0 ? 1 : (kMode == 1 ? 7 : 8);
     __shared__ Panel stack[kStack];
     __shared__ Leaf leaves[kLeaves];
     __shared__ int s_nleaves, s_done;
     __shared__ QuadCtx ctx;
-    __shared__ double s_red[kGrad ? 7 : 1][kQuadThreads / 32];
+    __shared__ double s_red[kVals][kQuadThreads / 32];
     __shared__ double r10n[10], r10w[10], r16n[16], r16w[16];
     if (threadIdx.x < 10) {
         r10n[threadIdx.x] = c_quad.nodes[10][threadIdx.x];
@@ -682,7 +831,13 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
         if (threadIdx.x == 0) {
             const DevFil &A = fil[it.x];
             const DevFil &B = fil[it.y];
-            aligned_bars(A, B, &ctx.b);
+            if (kMode == 2 && (it.w & kCoordOrtho))
+                ortho_aligned(A, B, &ctx.b);
+            else
+                aligned_bars(A, B, &ctx.b);
+            ctx.tau = kMode == 2 ? (it.w & kCoordTauMask) : 0;
+            ctx.rot = kMode == 2 && (it.w & kCoordRot) && ctx.tau != 0;
+            ctx.sigma = (it.w & kCoordSigmaNeg) ? -1.0 : 1.0;
             const Aligned &b = ctx.b;
             ctx.axial_start = b.offset[0] + 0.5 * (b.length[0] - b.length[1]);
             double l1 = b.length[0], l2 = b.length[1], as = ctx.axial_start;
@@ -699,7 +854,7 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
             for (int a = nu - 2; a >= 0; --a)
                 for (int c = nv - 2; c >= 0; --c) stack[sp++] = Panel{us[a], us[a + 1], vs[c], vs[c + 1], 0, 0};
         }
-        double acc = 0.0, gacc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        double acc = 0.0, gacc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         long long visited = 0;  // panels popped; bounded so that no input can loop without end
         bool overflow = false;
         for (;;) {
@@ -775,7 +930,12 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
                         int a = k / 10, c = k % 10;
                         double uu = mu + hu * r10n[a], wu = hu * r10w[a];
                         double vv = mv + hv * r10n[c], wv = hv * r10w[c];
-                        if (kGrad) {
+                        if (kMode == 2) {
+                            double g[8];
+                            integrand_coord(ctx, uu, vv, g);
+                            acc += wu * wv * g[0];
+                            for (int q = 0; q < 7; ++q) gacc[q] += wu * wv * g[1 + q];
+                        } else if (kMode == 1) {
                             double g[7];
                             integrand_grad(ctx, uu, vv, g);
                             acc += wu * wv * g[0];
@@ -792,7 +952,14 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
                         double s = tau * tau * tau;
                         double radial = w_tau * 3.0 * tau * tau * s;
                         double t = 0.5 + 0.5 * r16n[c], w_t = 0.5 * r16w[c];
-                        if (kGrad) {
+                        if (kMode == 2) {
+                            double g1[8], g2[8];
+                            integrand_coord(ctx, A * s, B * s * t, g1);
+                            integrand_coord(ctx, A * s * t, B * s, g2);
+                            const double f = radial * w_t * ab;
+                            acc += f * (g1[0] + g2[0]);
+                            for (int q = 0; q < 7; ++q) gacc[q] += f * (g1[1 + q] + g2[1 + q]);
+                        } else if (kMode == 1) {
                             double g1[7], g2[7];
                             integrand_grad(ctx, A * s, B * s * t, g1);
                             integrand_grad(ctx, A * s * t, B * s, g2);
@@ -812,19 +979,17 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
         // block reduction
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
         if ((threadIdx.x & 31) == 0) s_red[0][threadIdx.x >> 5] = acc;
-        if (kGrad) {
-            for (int q = 0; q < 6; ++q) {
-                double x = gacc[q];
-                for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-                if ((threadIdx.x & 31) == 0) s_red[kGrad ? 1 + q : 0][threadIdx.x >> 5] = x;
-            }
+        for (int q = 0; q + 1 < kVals; ++q) {
+            double x = gacc[q];
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if ((threadIdx.x & 31) == 0) s_red[1 + q][threadIdx.x >> 5] = x;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            for (int q = 0; q < (kGrad ? 7 : 1); ++q) {
+            for (int q = 0; q < kVals; ++q) {
                 double s = 0.0;
                 for (int w = 0; w < kQuadThreads / 32; ++w) s += s_red[q][w];
-                values[kGrad ? 7 * h + q : h] = overflow ? NAN : s;  // reported as NotFinite by the scatter
+                values[kVals * h + q] = overflow ? NAN : s;  // reported as NotFinite by the scatter
             }
         }
         __syncthreads();
@@ -857,6 +1022,24 @@ struct AlignedKey {
         const double v[9] = {b.length[0], b.length[1], b.width[0], b.width[1], b.height[0],
                              b.height[1], b.offset[0], b.offset[1], b.offset[2]};
         for (int i = 0; i < 9; ++i) k[i] = (unsigned long long)__double_as_longlong(v[i]);
+    }
+};
+
+// Key of a coordinate-derivative quadrature pair: the nine numbers of its
+// frame (aligned_bars, or ortho_aligned for an orthogonal pair) and the
+// flags that choose the frame and the rotation axis.
+struct CoordKey {
+    static constexpr int kWords = 10;
+    __device__ static void get(const DevFil *fil, int4 it, unsigned long long k[kWords]) {
+        Aligned b;
+        if (it.w & kCoordOrtho)
+            ortho_aligned(fil[it.x], fil[it.y], &b);
+        else
+            aligned_bars(fil[it.x], fil[it.y], &b);
+        const double v[9] = {b.length[0], b.length[1], b.width[0], b.width[1], b.height[0],
+                             b.height[1], b.offset[0], b.offset[1], b.offset[2]};
+        for (int i = 0; i < 9; ++i) k[i] = (unsigned long long)__double_as_longlong(v[i]);
+        k[9] = (unsigned long long)(it.w & (kCoordTauMask | kCoordSigmaNeg | kCoordRot | kCoordOrtho));
     }
 };
 
@@ -1364,6 +1547,409 @@ __global__ void aligned_grad_scatter_kernel(const DevFil *__restrict__ fil, cons
     }
 }
 
+// ---------------------------------------------------------------------------
+// Coordinate derivative fill (no reference counterpart).  A node moving in
+// the xy plane moves every filament of the segments that meet there by a
+// translation of its centre, a stretch of its length about its centre and a
+// rotation about the z axis through its centre.  For every pair (a, b) this
+// writes the partial derivatives of L_ab with respect to these coordinates
+// of a (b held fixed) to D[a + b n] and of b to D[b + a n]:
+//   Dl  translation along l_a          Dp  translation along z x l_a
+//   Ds  stretch of the length          Dr  rotation about z
+// Two filaments of one segment move together rigidly except for the common
+// stretch, which leaves their L_ab unchanged but for the stretch, so such
+// pairs get Ds only.  An orthogonal pair has L = 0, and only a rotation
+// changes it to first order: dL = mu0/4pi d(cos) / (A_a A_b) int int 1/R.
+// On the diagonal Ds holds half of dL_aa / d length (the products add both
+// sides, as in the width / thickness fill).
+// Methods: point quadrature where the fill takes it (one more Gauss node
+// per axis: the derivative kernel d/R^3 is one order steeper); otherwise the
+// closed form for a segment's own pairs (forward mode through the 64 corner
+// primitives along the length) and for orthogonal pairs (the bar integral
+// in a's frame), and the aligned quadrature with the integrand_coord terms
+// for pairs of different segments and wherever the closed form's error
+// estimate rejects it.
+// ---------------------------------------------------------------------------
+constexpr int kCoordCatPoint = 0, kCoordCatSame = 1, kCoordCatDiff = 2, kCoordCatOrtho = 3, kCoordCats = 4;
+
+struct CoordClass {
+    int cat;  // -1 nothing to write
+    int orders;
+    int flags;
+    int fail;  // FH_ERR_UNSUPPORTED for a pair this fill has no derivative for
+    bool swap;
+};
+
+__device__ __forceinline__ int bump_order(int o) { return o < kMaxRule - 1 ? o + 1 : o; }
+
+__device__ CoordClass coord_classify(const DevFil &fi, const DevFil &fj, bool same) {
+    CoordClass c{-1, 0, 0, 0, false};
+    c.swap = canonical_greater(fi, fj);
+    const DevFil &a = c.swap ? fj : fi;
+    const DevFil &b = c.swap ? fi : fj;
+    const double cosv = ndot(a.axes, b.axes);
+    int oa[3], ob[3];
+    auto pack = [&]() {
+        return bump_order(oa[0]) | (bump_order(oa[1]) << 5) | (bump_order(oa[2]) << 10) | (bump_order(ob[0]) << 15) |
+               (bump_order(ob[1]) << 20) | (bump_order(ob[2]) << 25);
+    };
+    if (fabs(cosv) < 1e-14) {
+        if (same) return c;
+        double za[3], zb[3];
+        zcross(a.axes, za);
+        zcross(b.axes, zb);
+        if (ndot(za, b.axes) == 0.0 && ndot(zb, a.axes) == 0.0) return c;  // stays orthogonal
+        const double gap = separation(a, b);
+        if (point_orders(a, gap, oa) && point_orders(b, gap, ob)) {
+            c.cat = kCoordCatPoint;
+            c.orders = pack();
+        } else if (ortho_aligned(a, b, nullptr)) {
+            c.cat = kCoordCatOrtho;
+            c.flags = kCoordOrtho;
+        } else {
+            c.fail = FH_ERR_UNSUPPORTED;
+        }
+        return c;
+    }
+    double cr[3];
+    ncross(a.axes, b.axes, cr);
+    Aligned ab;
+    if (!(nnorm(cr) < 1e-6 && aligned_bars(a, b, &ab))) {
+        c.fail = FH_ERR_UNSUPPORTED;
+        return c;
+    }
+    const double gap = separation(a, b);
+    bool point = point_orders(a, gap, oa) && point_orders(b, gap, ob);
+    if (point && oa[0] * oa[1] * oa[2] * ob[0] * ob[1] * ob[2] > 4096) point = false;
+    if (point) {
+        c.cat = kCoordCatPoint;
+        c.orders = pack();
+        c.flags = same ? kCoordSame : 0;
+        return c;
+    }
+    if (same) {
+        c.cat = kCoordCatSame;
+        c.flags = kCoordSame;
+        return c;
+    }
+    c.cat = kCoordCatDiff;
+    double za[3];
+    zcross(a.axes, za);
+    const double zn = nnorm(za);
+    if (zn > 1e-12) {  // not vertical: rotations about z apply
+        const double dw = ndot(za, a.axes + 3) / zn, dh = ndot(za, a.axes + 6) / zn;
+        const bool tw = fabs(dw) >= fabs(dh);
+        const double d = tw ? dw : dh;
+        // z x l must be a cross-section axis, and the cross-sections must
+        // not meet when projected along the length (the moment integrals
+        // are singular there).
+        if (fabs(d) < 1.0 - 1e-12 || fabs(a.axes[2]) > 1e-12 ||
+            (fabs(ab.offset[1]) <= 0.5 * (ab.width[0] + ab.width[1]) &&
+             fabs(ab.offset[2]) <= 0.5 * (ab.height[0] + ab.height[1]))) {
+            c.cat = -1;
+            c.fail = FH_ERR_UNSUPPORTED;
+            return c;
+        }
+        c.flags = (tw ? 1 : 2) | (d < 0.0 ? kCoordSigmaNeg : 0) | kCoordRot;
+    }
+    return c;
+}
+
+// Classification over the upper triangle (tiles as classify_kernel): pairs
+// with at least one moving filament, outside the coupling mask's dropped
+// pairs.  Pass 0 counts per category and records unsupported pairs; pass 1
+// writes the work lists (a, b, packed orders, flags).
+template <bool kWrite>
+__global__ void __launch_bounds__(256) coord_classify_kernel(const DevFil *__restrict__ fil,
+                                                             const int32_t *__restrict__ seg,
+                                                             const uint8_t *__restrict__ move, int n,
+                                                             unsigned long long *__restrict__ counts,
+                                                             unsigned long long *__restrict__ cursor,
+                                                             int4 *__restrict__ items, PairMaskDev mask,
+                                                             DevError *err) {
+    const int ti = blockIdx.y, tj = blockIdx.x;
+    if (ti > tj) return;
+    __shared__ DevFil s_i[32], s_j[32];
+    __shared__ unsigned s_count[kCoordCats];
+    __shared__ unsigned long long s_base[kCoordCats];
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    {
+        const double *gi = reinterpret_cast<const double *>(fil + (int64_t)ti * 32);
+        const double *gj = reinterpret_cast<const double *>(fil + (int64_t)tj * 32);
+        double *si = reinterpret_cast<double *>(s_i), *sj = reinterpret_cast<double *>(s_j);
+        int rows_i = min(32, n - ti * 32), rows_j = min(32, n - tj * 32);
+        for (int k = tid; k < 32 * 32; k += 256) {
+            if (k < rows_i * 32) si[k] = gi[k];
+            if (k < rows_j * 32) sj[k] = gj[k];
+        }
+    }
+    if (tid < kCoordCats) s_count[tid] = 0;
+    __syncthreads();
+    const int j = tj * 32 + threadIdx.x;
+    CoordClass cls[4];
+    unsigned slot[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int i = ti * 32 + threadIdx.y + 8 * r;
+        cls[r].cat = -1;
+        if (i < n && j < n && i <= j && (move[i] || move[j]) &&
+            (!mask.group || mask.coupled[(int64_t)mask.group[i] * mask.groups + mask.group[j]])) {
+            cls[r] = coord_classify(s_i[threadIdx.y + 8 * r], s_j[threadIdx.x], seg[i] == seg[j]);
+            if (!kWrite && cls[r].fail) record_error(err, i, j, cls[r].fail);
+            if (cls[r].cat >= 0) slot[r] = atomicAdd(&s_count[cls[r].cat], 1u);
+        }
+    }
+    __syncthreads();
+    if (!kWrite) {
+        if (tid < kCoordCats && s_count[tid]) atomicAdd(&counts[tid], (unsigned long long)s_count[tid]);
+        return;
+    }
+    if (tid < kCoordCats)
+        s_base[tid] = s_count[tid] ? atomicAdd(&cursor[tid], (unsigned long long)s_count[tid]) : 0ull;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        if (cls[r].cat < 0) continue;
+        const int i = ti * 32 + threadIdx.y + 8 * r;
+        const int a = cls[r].swap ? j : i, b = cls[r].swap ? i : j;
+        items[s_base[cls[r].cat] + slot[r]] = make_int4(a, b, cls[r].orders, cls[r].flags);
+    }
+}
+
+__device__ __forceinline__ void store_coord(const CoordOut &o, int64_t n, int a, int b, const double da[4],
+                                            const double db[4], DevError *e) {
+    bool ok = true;
+    for (int k = 0; k < 4; ++k) ok = ok && isfinite(da[k]) && isfinite(db[k]);
+    if (!ok) {
+        record_error(e, a, b, FH_ERR_KERNEL_NOT_FINITE);
+        return;
+    }
+    const int64_t ab = (int64_t)a + (int64_t)b * n, ba = (int64_t)b + (int64_t)a * n;
+    o.Dl[ab] = da[0];
+    o.Dp[ab] = da[1];
+    o.Ds[ab] = da[2];
+    o.Dr[ab] = da[3];
+    if (a != b) {
+        o.Dl[ba] = db[0];
+        o.Dp[ba] = db[1];
+        o.Ds[ba] = db[2];
+        o.Dr[ba] = db[3];
+    }
+}
+
+// z x l normalized (zero for a vertical l).
+__device__ __forceinline__ void plane_normal(const double *l, double p[3]) {
+    zcross(l, p);
+    const double nrm = nnorm(p);
+    for (int k = 0; k < 3; ++k) p[k] = nrm > 0.0 ? p[k] / nrm : 0.0;
+}
+
+// Point quadrature: with d = p - q over the Gauss points of a and b,
+// V = sum w / |d| (L = mu0/4pi cos V), G = sum w d / |d|^3, and the moments
+// SA = sum w x_a (d . l_a) / |d|^3, SB likewise with b's axial coordinate,
+// RA = sum w d . (z x (p - c_a)) / |d|^3, RB likewise for b.  A translation
+// e of a changes V by -G . e, of b by G . e; a stretch of a moves its
+// points by x_a / length along l_a and scales its weights; a rotation moves
+// its points by z x (p - c) and turns l by z x l.
+__global__ void __launch_bounds__(128) point_coord_kernel(const DevFil *__restrict__ fil,
+                                                          const int4 *__restrict__ items, int64_t count, CoordOut out,
+                                                          int64_t n, DevError *err) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int4 it = items[t];
+        const DevFil &A = fil[it.x];
+        const DevFil &B = fil[it.y];
+        const int oa0 = it.z & 31, oa1 = (it.z >> 5) & 31, oa2 = (it.z >> 10) & 31;
+        const int ob0 = (it.z >> 15) & 31, ob1 = (it.z >> 20) & 31, ob2 = (it.z >> 25) & 31;
+        double aa[9], ba[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            aa[k] = A.axes[k];
+            ba[k] = B.axes[k];
+        }
+        const double ah0 = A.half[0], ah1 = 2.0 * A.half[1], ah2 = 2.0 * A.half[2];
+        const double bh0 = B.half[0], bh1 = 2.0 * B.half[1], bh2 = 2.0 * B.half[2];
+        double V = 0.0, G[3] = {0.0, 0.0, 0.0}, SA = 0.0, SB = 0.0, RA = 0.0, RB = 0.0;
+        for (int la = 0; la < oa0; ++la) {
+            const double xl = ah0 * c_quad.nodes[oa0][la], wl = ah0 * c_quad.weights[oa0][la];
+            for (int wa = 0; wa < oa1; ++wa) {
+                const double xw = ah1 * (0.5 * c_quad.nodes[oa1][wa]), ww = 0.5 * c_quad.weights[oa1][wa];
+                for (int ha = 0; ha < oa2; ++ha) {
+                    const double xh = ah2 * (0.5 * c_quad.nodes[oa2][ha]), wh = 0.5 * c_quad.weights[oa2][ha];
+                    double oA[3], p[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        oA[d] = aa[d] * xl + aa[3 + d] * xw + aa[6 + d] * xh;
+                        p[d] = A.centre[d] + oA[d];
+                    }
+                    const double wpa = wl * ww * wh;
+                    double vi = 0.0, gi[3] = {0.0, 0.0, 0.0}, sbi = 0.0, rbi = 0.0;
+                    for (int lb = 0; lb < ob0; ++lb) {
+                        const double yl = bh0 * c_quad.nodes[ob0][lb], vl = bh0 * c_quad.weights[ob0][lb];
+                        for (int wb = 0; wb < ob1; ++wb) {
+                            const double yw = bh1 * (0.5 * c_quad.nodes[ob1][wb]);
+                            const double vlw = vl * (0.5 * c_quad.weights[ob1][wb]);
+                            for (int hb = 0; hb < ob2; ++hb) {
+                                const double yh = bh2 * (0.5 * c_quad.nodes[ob2][hb]);
+                                const double vh = 0.5 * c_quad.weights[ob2][hb];
+                                double oB[3], d[3];
+#pragma unroll
+                                for (int k = 0; k < 3; ++k) {
+                                    oB[k] = ba[k] * yl + ba[3 + k] * yw + ba[6 + k] * yh;
+                                    d[k] = p[k] - (B.centre[k] + oB[k]);
+                                }
+                                const double ir = rsqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+                                const double w = vlw * vh;
+                                const double e = w * ir * ir * ir;
+                                vi += w * ir;
+                                gi[0] += e * d[0];
+                                gi[1] += e * d[1];
+                                gi[2] += e * d[2];
+                                sbi += e * yl * (d[0] * ba[0] + d[1] * ba[1] + d[2] * ba[2]);
+                                rbi += e * (d[1] * oB[0] - d[0] * oB[1]);
+                            }
+                        }
+                    }
+                    V += wpa * vi;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) G[k] += wpa * gi[k];
+                    SA += wpa * xl * (gi[0] * aa[0] + gi[1] * aa[1] + gi[2] * aa[2]);
+                    RA += wpa * (gi[1] * oA[0] - gi[0] * oA[1]);
+                    SB += wpa * sbi;
+                    RB += wpa * rbi;
+                }
+            }
+        }
+        const double cosv = ndot(aa, ba);
+        double za[3], zb[3], pa[3], pb[3];
+        zcross(aa, za);
+        zcross(ba, zb);
+        plane_normal(aa, pa);
+        plane_normal(ba, pb);
+        const double k = kMu0Over4Pi;
+        double da[4], db[4];
+        da[2] = k * cosv * (V - SA) / (2.0 * A.half[0]);
+        db[2] = k * cosv * (V + SB) / (2.0 * B.half[0]);
+        if (it.w & kCoordSame) {
+            da[0] = da[1] = da[3] = db[0] = db[1] = db[3] = 0.0;
+        } else {
+            da[0] = -k * cosv * ndot(G, aa);
+            da[1] = -k * cosv * ndot(G, pa);
+            da[3] = k * (ndot(za, ba) * V - cosv * RA);
+            db[0] = k * cosv * ndot(G, ba);
+            db[1] = k * cosv * ndot(G, pb);
+            db[3] = k * (ndot(zb, aa) * V + cosv * RB);
+        }
+        store_coord(out, n, it.x, it.y, da, db, err);
+    }
+}
+
+// A segment's own aligned pairs (kOrtho false: the stretch by forward mode
+// along the length through the 64 corner primitives, which are symmetric in
+// their three arguments) and near orthogonal pairs (kOrtho: the bar integral
+// in a's frame), each where the closed form's error estimate accepts it;
+// the rest go to the quadrature list.
+template <bool kOrtho>
+__global__ void __launch_bounds__(128) closed_form_coord_kernel(const DevFil *__restrict__ fil,
+                                                                const int4 *__restrict__ items, int64_t count,
+                                                                CoordOut out, int64_t n, int4 *__restrict__ quad_items,
+                                                                unsigned long long *__restrict__ quad_count,
+                                                                DevError *err) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int4 it = items[t];
+        const DevFil &A = fil[it.x];
+        const DevFil &B = fil[it.y];
+        Aligned ab;
+        if (kOrtho)
+            ortho_aligned(A, B, &ab);
+        else
+            aligned_bars(A, B, &ab);
+        double v, rel;
+        bar_integral(ab, &v, &rel);
+        if (!(rel <= kClosedFormMaxError)) {
+            unsigned long long k = atomicAdd(quad_count, 1ull);
+            quad_items[k] = it;
+            continue;
+        }
+        double da[4] = {0.0, 0.0, 0.0, 0.0}, db[4] = {0.0, 0.0, 0.0, 0.0};
+        if (kOrtho) {
+            double za[3], zb[3];
+            zcross(A.axes, za);
+            zcross(B.axes, zb);
+            const double scale = kMu0Over4Pi / (A.area * B.area);
+            da[3] = scale * ndot(za, B.axes) * v;
+            db[3] = scale * ndot(zb, A.axes) * v;
+        } else {
+            double qx[4], qy[4], qz[4];
+            corner_differences(ab.length[0], ab.length[1], ab.offset[0], qx);
+            corner_differences(ab.width[0], ab.width[1], ab.offset[1], qy);
+            corner_differences(ab.height[0], ab.height[1], ab.offset[2], qz);
+            const double signs[4] = {1.0, -1.0, -1.0, 1.0};
+            double px[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int i = 0; i < 4; ++i)
+                for (int j = 0; j < 4; ++j)
+                    for (int k = 0; k < 4; ++k) px[i] += signs[i] * signs[j] * signs[k] *
+                                                          primitive_d(qy[j], qx[i], qz[k]).y;
+            const double d0 = 0.5 * (px[0] + px[1] - px[2] - px[3]), d1 = 0.5 * (px[0] - px[1] + px[2] - px[3]);
+            const double scale = kMu0Over4Pi * signum(ndot(A.axes, B.axes)) / (A.area * B.area);
+            if (it.x == it.y) {
+                da[2] = 0.5 * scale * (d0 + d1);
+            } else {
+                da[2] = scale * d0;
+                db[2] = scale * d1;
+            }
+        }
+        store_coord(out, n, it.x, it.y, da, db, err);
+    }
+}
+
+// Quadrature pairs: the key's eight values (integrand_coord), then the chain
+// rule to the two filaments' coordinates.
+__global__ void coord_quad_scatter_kernel(const DevFil *__restrict__ fil, const int4 *__restrict__ items,
+                                          const int64_t *__restrict__ head_of, const double *__restrict__ head_value,
+                                          int64_t count, CoordOut out, int64_t n, DevError *err) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int4 it = items[t];
+        const double *hv = head_value + 8 * head_of[t];
+        const DevFil &A = fil[it.x];
+        const DevFil &B = fil[it.y];
+        double da[4] = {0.0, 0.0, 0.0, 0.0}, db[4] = {0.0, 0.0, 0.0, 0.0};
+        if (it.w & kCoordOrtho) {
+            double za[3], zb[3];
+            zcross(A.axes, za);
+            zcross(B.axes, zb);
+            const double scale = kMu0Over4Pi / (A.area * B.area);
+            da[3] = scale * ndot(za, B.axes) * hv[0];
+            db[3] = scale * ndot(zb, A.axes) * hv[0];
+        } else {
+            const double c = signum(ndot(A.axes, B.axes));
+            const double scale = kMu0Over4Pi * c / (A.area * B.area);
+            if (it.x == it.y) {
+                da[2] = 0.5 * scale * (hv[4] + hv[5]);
+            } else if (it.w & kCoordSame) {
+                da[2] = scale * hv[4];
+                db[2] = scale * hv[5];
+            } else {
+                const int tau = it.w & kCoordTauMask;
+                const double sigma = (it.w & kCoordSigmaNeg) ? -1.0 : 1.0;
+                const double dtau = tau == 1 ? hv[2] : (tau == 2 ? hv[3] : 0.0);
+                const bool rot = (it.w & kCoordRot) && tau != 0;
+                da[0] = -scale * hv[1];
+                da[1] = -scale * sigma * dtau;
+                da[2] = scale * hv[4];
+                da[3] = rot ? scale * hv[6] : 0.0;
+                db[0] = scale * c * hv[1];
+                db[1] = scale * c * sigma * dtau;
+                db[2] = scale * hv[5];
+                db[3] = rot ? scale * hv[7] : 0.0;
+            }
+        }
+        store_coord(out, n, it.x, it.y, da, db, err);
+    }
+}
+
 // Congruence M B M^T in the reference's two steps (solve.rs:1172-1200):
 // for loop row i, product_i = sum over (a, s_a) in row i of s_a B[a, :], then
 // entry (i, j), j >= i, = sum over (b, s_b) in row j of s_b product_i[b],
@@ -1483,6 +2069,89 @@ namespace {
 // d_pairs == nullptr it evaluates the upper triangle of the n x n matrix
 // into d_L (mirrored); with a pair list it evaluates those pairs into
 // d_L[k] (pair-list mode: orthogonal pairs are zero).
+// Distinct keys of a list of pairs: hash, sort by hash, flag the heads of
+// runs of equal keys (full keys compared), max-scan to map every pair to its
+// run head, compact the heads.  heads[r] = the list index of distinct key r;
+// item_head[t] = the rank of pair t's key.  `alloc(ptr, bytes)` takes
+// stream-ordered scratch that the caller releases.
+template <class Key, class Alloc>
+fh_status distinct_keys(Key, const DevFil *d_fil, const int4 *d_list, int64_t count, Alloc &alloc,
+                        cudaStream_t stream, int64_t &n_heads, int64_t *&d_heads, int64_t *&d_item_head,
+                        fh_error_info *err) {
+    const int sms = 148;
+    unsigned long long *d_hash, *d_hash_sorted;
+    int64_t *d_idx, *d_order, *d_headpos, *d_headof;
+    FHB_CUDA(alloc((void **)&d_hash, 8 * count));
+    FHB_CUDA(alloc((void **)&d_hash_sorted, 8 * count));
+    FHB_CUDA(alloc((void **)&d_idx, 8 * count));
+    FHB_CUDA(alloc((void **)&d_order, 8 * count));
+    FHB_CUDA(alloc((void **)&d_headpos, 8 * count));
+    FHB_CUDA(alloc((void **)&d_headof, 8 * count));
+    const int blocks = (int)std::min<int64_t>((count + 255) / 256, (int64_t)sms * 16);
+    key_hash_kernel<Key><<<blocks, 256, 0, stream>>>(d_fil, d_list, count, d_hash, d_idx);
+    FHB_CUDA(cudaGetLastError());
+    size_t tmp_bytes = 0, tmp2 = 0;
+    // 32 bits of the hash are enough to group the keys: a collision only
+    // splits a run, because the full keys are compared after the sort.
+    FHB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_hash, d_hash_sorted, d_idx, d_order,
+                                             (int)count, 0, 32, stream));
+    FHB_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tmp2, d_headpos, d_headof, cub::Max(), (int)count, stream));
+    void *d_tmp = nullptr;
+    FHB_CUDA(alloc(&d_tmp, std::max(tmp_bytes, tmp2)));
+    tmp_bytes = std::max(tmp_bytes, tmp2);
+    FHB_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_hash, d_hash_sorted, d_idx, d_order, (int)count,
+                                             0, 32, stream));
+    {
+        const size_t key_smem = sizeof(unsigned long long) * kHeadsBlock * Key::kWords;
+        FHB_CUDA(cudaFuncSetAttribute(key_heads_kernel<Key>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)key_smem));
+        const int hb = (int)std::min<int64_t>((count + kHeadsBlock - 2) / (kHeadsBlock - 1), (int64_t)sms * 8);
+        key_heads_kernel<Key><<<hb, kHeadsBlock, key_smem, stream>>>(d_fil, d_list, d_hash_sorted, d_order, count,
+                                                                    d_headpos);
+    }
+    FHB_CUDA(cudaGetLastError());
+    FHB_CUDA(cub::DeviceScan::InclusiveScan(d_tmp, tmp_bytes, d_headpos, d_headof, cub::Max(), (int)count, stream));
+    // Compact the heads on the device: head positions are where
+    // headof[t] == t; their ranks (exclusive sum of the flags) number
+    // the distinct keys.
+    int64_t *d_flag = d_headpos, *d_rank = reinterpret_cast<int64_t *>(d_hash);
+    head_flag_kernel<<<blocks, 256, 0, stream>>>(d_headof, count, d_flag);
+    FHB_CUDA(cudaGetLastError());
+    size_t tmp3 = 0;
+    FHB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp3, d_flag, d_rank, (int)count, stream));
+    if (tmp3 > tmp_bytes) {
+        FHB_CUDA(alloc(&d_tmp, tmp3));
+        tmp_bytes = tmp3;
+    }
+    FHB_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_flag, d_rank, (int)count, stream));
+    int64_t last[2];
+    FHB_CUDA(cudaMemcpyAsync(&last[0], d_rank + count - 1, 8, cudaMemcpyDeviceToHost, stream));
+    FHB_CUDA(cudaMemcpyAsync(&last[1], d_flag + count - 1, 8, cudaMemcpyDeviceToHost, stream));
+    FHB_CUDA(cudaStreamSynchronize(stream));
+    n_heads = last[0] + last[1];
+    FHB_CUDA(alloc((void **)&d_heads, 8 * n_heads));
+    FHB_CUDA(alloc((void **)&d_item_head, 8 * count));
+    head_compact_kernel<<<blocks, 256, 0, stream>>>(d_order, d_headof, d_rank, d_flag, count, d_heads,
+                                                    d_item_head);
+    FHB_CUDA(cudaGetLastError());
+    return FH_OK;
+}
+
+// The Gauss rules and order thresholds in constant memory, once per device.
+fh_status upload_quad_tables(fh_error_info *err) {
+    int dev = 0;
+    FHB_CUDA(cudaGetDevice(&dev));
+    static std::mutex init_mu;  // first use on a device may race between host threads
+    std::lock_guard<std::mutex> lk(init_mu);
+    if (dev < 64 && !g_tables_uploaded[dev]) {
+        QuadTables t;
+        host_quad_tables(t);
+        FHB_CUDA(cudaMemcpyToSymbol(c_quad, &t, sizeof t));
+        g_tables_uploaded[dev] = true;
+    }
+    return FH_OK;
+}
+
 fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t n_pairs, double *d_L,
                    int8_t *d_methods, cudaStream_t stream, FillStats *stats, fh_error_info *err,
                    const FilTan *d_tan = nullptr, const GradOut *grad = nullptr,
@@ -1496,17 +2165,8 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
     if (n > 2000000000LL / 32) return fail(err, FH_ERR_INVALID_ARGUMENT, "too many filaments for the fill");
     if (list && n_pairs > INT32_MAX) return fail(err, FH_ERR_INVALID_ARGUMENT, "too many pairs for one list fill");
     const int64_t n_arg = list ? 0 : n;  // the method kernels' store mode
-    int dev = 0;
-    FHB_CUDA(cudaGetDevice(&dev));
-    static std::mutex init_mu;  // first use on a device may race between host threads
-    std::unique_lock<std::mutex> lk(init_mu);
-    if (dev < 64 && !g_tables_uploaded[dev]) {
-        QuadTables t;
-        host_quad_tables(t);
-        FHB_CUDA(cudaMemcpyToSymbol(c_quad, &t, sizeof t));
-        g_tables_uploaded[dev] = true;
-    }
-    lk.unlock();
+    fh_status ts = upload_quad_tables(err);
+    if (ts) return ts;
     FillStats local;
     FillStats &st = stats ? *stats : local;
     st = FillStats();
@@ -1580,69 +2240,9 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
     FHB_CUDA(cudaGetLastError());
     FHB_CUDA(cudaEventRecord(ev[1], stream));
     const int sms = 148;
-    // Distinct keys of a list of pairs: hash, sort by hash, flag the heads of
-    // runs of equal keys (full keys compared), max-scan to map every pair to
-    // its run head, compact the heads.  heads[r] = the list index of distinct
-    // key r; item_head[t] = the rank of pair t's key.
     auto distinct = [&](auto key, const int4 *d_list, int64_t count, int64_t &n_heads, int64_t *&d_heads,
                         int64_t *&d_item_head) -> fh_status {
-        using Key = decltype(key);
-        unsigned long long *d_hash, *d_hash_sorted;
-        int64_t *d_idx, *d_order, *d_headpos, *d_headof;
-        FHB_CUDA(alloc((void **)&d_hash, 8 * count));
-        FHB_CUDA(alloc((void **)&d_hash_sorted, 8 * count));
-        FHB_CUDA(alloc((void **)&d_idx, 8 * count));
-        FHB_CUDA(alloc((void **)&d_order, 8 * count));
-        FHB_CUDA(alloc((void **)&d_headpos, 8 * count));
-        FHB_CUDA(alloc((void **)&d_headof, 8 * count));
-        const int blocks = (int)std::min<int64_t>((count + 255) / 256, (int64_t)sms * 16);
-        key_hash_kernel<Key><<<blocks, 256, 0, stream>>>(d_fil, d_list, count, d_hash, d_idx);
-        FHB_CUDA(cudaGetLastError());
-        size_t tmp_bytes = 0, tmp2 = 0;
-        // 32 bits of the hash are enough to group the keys: a collision only
-        // splits a run, because the full keys are compared after the sort.
-        FHB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_hash, d_hash_sorted, d_idx, d_order,
-                                                 (int)count, 0, 32, stream));
-        FHB_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tmp2, d_headpos, d_headof, cub::Max(), (int)count, stream));
-        void *d_tmp = nullptr;
-        FHB_CUDA(alloc(&d_tmp, std::max(tmp_bytes, tmp2)));
-        tmp_bytes = std::max(tmp_bytes, tmp2);
-        FHB_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_hash, d_hash_sorted, d_idx, d_order, (int)count,
-                                                 0, 32, stream));
-        {
-            const size_t key_smem = sizeof(unsigned long long) * kHeadsBlock * Key::kWords;
-            FHB_CUDA(cudaFuncSetAttribute(key_heads_kernel<Key>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)key_smem));
-            const int hb = (int)std::min<int64_t>((count + kHeadsBlock - 2) / (kHeadsBlock - 1), (int64_t)sms * 8);
-            key_heads_kernel<Key><<<hb, kHeadsBlock, key_smem, stream>>>(d_fil, d_list, d_hash_sorted, d_order, count,
-                                                                        d_headpos);
-        }
-        FHB_CUDA(cudaGetLastError());
-        FHB_CUDA(cub::DeviceScan::InclusiveScan(d_tmp, tmp_bytes, d_headpos, d_headof, cub::Max(), (int)count, stream));
-        // Compact the heads on the device: head positions are where
-        // headof[t] == t; their ranks (exclusive sum of the flags) number
-        // the distinct keys.
-        int64_t *d_flag = d_headpos, *d_rank = reinterpret_cast<int64_t *>(d_hash);
-        head_flag_kernel<<<blocks, 256, 0, stream>>>(d_headof, count, d_flag);
-        FHB_CUDA(cudaGetLastError());
-        size_t tmp3 = 0;
-        FHB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp3, d_flag, d_rank, (int)count, stream));
-        if (tmp3 > tmp_bytes) {
-            FHB_CUDA(alloc(&d_tmp, tmp3));
-            tmp_bytes = tmp3;
-        }
-        FHB_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_flag, d_rank, (int)count, stream));
-        int64_t last[2];
-        FHB_CUDA(cudaMemcpyAsync(&last[0], d_rank + count - 1, 8, cudaMemcpyDeviceToHost, stream));
-        FHB_CUDA(cudaMemcpyAsync(&last[1], d_flag + count - 1, 8, cudaMemcpyDeviceToHost, stream));
-        FHB_CUDA(cudaStreamSynchronize(stream));
-        n_heads = last[0] + last[1];
-        FHB_CUDA(alloc((void **)&d_heads, 8 * n_heads));
-        FHB_CUDA(alloc((void **)&d_item_head, 8 * count));
-        head_compact_kernel<<<blocks, 256, 0, stream>>>(d_order, d_headof, d_rank, d_flag, count, d_heads,
-                                                        d_item_head);
-        FHB_CUDA(cudaGetLastError());
-        return FH_OK;
+        return distinct_keys(key, d_fil, d_list, count, alloc, stream, n_heads, d_heads, d_item_head, err);
     };
     // Point quadrature over all buckets (contiguous, cost ascending).
     const int64_t n_point = (int64_t)offsets[kPointBuckets];
@@ -1726,13 +2326,13 @@ fh_status fill_run(const DevFil *d_fil, int64_t n, const int2 *d_pairs, int64_t 
         const int blocks = (int)std::min<int64_t>((n_quad + 255) / 256, (int64_t)sms * 16);
         int qblocks = (int)std::min<int64_t>(n_heads, (int64_t)sms * 16);
         if (grad) {
-            aligned_quadrature_kernel<true><<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads,
+            aligned_quadrature_kernel<1><<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads,
                                                                                  d_values);
             FHB_CUDA(cudaGetLastError());
             aligned_grad_scatter_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_tan, d_quad, d_item_head, d_values, n_quad,
                                                                     *grad, n, d_err);
         } else {
-            aligned_quadrature_kernel<false><<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads,
+            aligned_quadrature_kernel<0><<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads,
                                                                                   d_values);
             FHB_CUDA(cudaGetLastError());
             aligned_scatter_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_quad, d_item_head, d_values, n_quad, d_L,
@@ -1796,6 +2396,134 @@ fh_status device_fill_grad(const DevFil *d_fil, const FilTan *d_tan, int64_t n, 
                            FillStats *stats, fh_error_info *err, const PairMaskDev *mask) {
     if (!d_tan || !out.Dw || !out.Dh) return fail(err, FH_ERR_INVALID_ARGUMENT, "null derivative-fill argument");
     return fill_run(d_fil, n, nullptr, 0, nullptr, nullptr, stream, stats, err, d_tan, &out, mask);
+}
+
+fh_status device_fill_coord(const DevFil *d_fil, const int32_t *d_seg, const uint8_t *d_move, int64_t n,
+                            CoordOut out, cudaStream_t stream, FillStats *stats, fh_error_info *err,
+                            const PairMaskDev *mask) {
+    if (!d_seg || !d_move || !out.Dl || !out.Dp || !out.Ds || !out.Dr)
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "null coordinate-fill argument");
+    if (n == 0) return FH_OK;
+    if (n > 2000000000LL / 32) return fail(err, FH_ERR_INVALID_ARGUMENT, "too many filaments for the fill");
+    const PairMaskDev no_mask;
+    const PairMaskDev &pm = mask ? *mask : no_mask;
+    fh_status ts = upload_quad_tables(err);
+    if (ts) return ts;
+    FillStats local;
+    FillStats &st = stats ? *stats : local;
+    st = FillStats();
+    st.pairs = n * (n + 1) / 2;
+    struct Guard {
+        std::vector<void *> ptrs;
+        cudaStream_t s;
+        ~Guard() {
+            for (void *p : ptrs) cache_free(p, s);
+        }
+    } guard{{}, stream};
+    auto alloc = [&](void **p, size_t bytes) -> cudaError_t {
+        cudaError_t e = cache_alloc(p, std::max<size_t>(bytes, 16), stream);
+        if (e == cudaSuccess) guard.ptrs.push_back(*p);
+        return e;
+    };
+    unsigned long long *d_counts = nullptr;
+    FHB_CUDA(alloc((void **)&d_counts, sizeof(unsigned long long) * (2 * kCoordCats + 2) + sizeof(DevError) + 64));
+    unsigned long long *d_cursor = d_counts + kCoordCats, *d_qcount = d_counts + 2 * kCoordCats;
+    DevError *d_err = reinterpret_cast<DevError *>(d_counts + 2 * kCoordCats + 2);
+    FHB_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * (2 * kCoordCats + 2), stream));
+    FHB_CUDA(cudaMemsetAsync(d_err, 0xff, sizeof(unsigned long long), stream));
+    FHB_CUDA(cudaMemsetAsync(&d_err->code, 0, sizeof(int), stream));
+    const int T = (int)((n + 31) / 32);
+    const dim3 grid(T, T), block(32, 8);
+    coord_classify_kernel<false><<<grid, block, 0, stream>>>(d_fil, d_seg, d_move, (int)n, d_counts, nullptr, nullptr,
+                                                             pm, d_err);
+    FHB_CUDA(cudaGetLastError());
+    unsigned long long counts[kCoordCats];
+    DevError h_err;
+    FHB_CUDA(cudaMemcpyAsync(counts, d_counts, sizeof counts, cudaMemcpyDeviceToHost, stream));
+    FHB_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof h_err, cudaMemcpyDeviceToHost, stream));
+    FHB_CUDA(cudaStreamSynchronize(stream));
+    if (h_err.key != ~0ull) {
+        const int64_t i = (int64_t)(h_err.key >> 32), j = (int64_t)(h_err.key & 0xffffffffull);
+        return fail(err, FH_ERR_UNSUPPORTED,
+                    "filaments " + std::to_string(i) + " and " + std::to_string(j) +
+                        " have no coordinate derivative here: a pair evaluated by sampled filaments (skew bars "
+                        "or rotated cross-sections), a segment off the xy plane, or parallel filaments of two "
+                        "segments whose cross-sections meet when projected along their length",
+                    i, j);
+    }
+    unsigned long long offsets[kCoordCats + 1];
+    offsets[0] = 0;
+    for (int c = 0; c < kCoordCats; ++c) offsets[c + 1] = offsets[c] + counts[c];
+    int4 *d_items = nullptr, *d_quad = nullptr;
+    FHB_CUDA(alloc((void **)&d_items, sizeof(int4) * offsets[kCoordCats]));
+    FHB_CUDA(cudaMemcpyAsync(d_cursor, offsets, sizeof(unsigned long long) * kCoordCats, cudaMemcpyHostToDevice,
+                             stream));
+    coord_classify_kernel<true><<<grid, block, 0, stream>>>(d_fil, d_seg, d_move, (int)n, nullptr, d_cursor, d_items,
+                                                            pm, d_err);
+    FHB_CUDA(cudaGetLastError());
+    const int sms = 148;
+    const int64_t n_point = (int64_t)counts[kCoordCatPoint];
+    st.point = n_point;
+    if (n_point) {
+        const int blocks = (int)std::min<int64_t>((n_point + 127) / 128, (int64_t)sms * 64);
+        point_coord_kernel<<<blocks, 128, 0, stream>>>(d_fil, d_items + offsets[kCoordCatPoint], n_point, out, n,
+                                                       d_err);
+        FHB_CUDA(cudaGetLastError());
+    }
+    // Quadrature list: the pairs of different segments, then whatever the
+    // closed forms reject.
+    const int64_t n_same = (int64_t)counts[kCoordCatSame], n_diff = (int64_t)counts[kCoordCatDiff];
+    const int64_t n_ortho = (int64_t)counts[kCoordCatOrtho];
+    FHB_CUDA(alloc((void **)&d_quad, sizeof(int4) * (size_t)(n_same + n_diff + n_ortho)));
+    if (n_diff)
+        FHB_CUDA(cudaMemcpyAsync(d_quad, d_items + offsets[kCoordCatDiff], sizeof(int4) * n_diff,
+                                 cudaMemcpyDeviceToDevice, stream));
+    const unsigned long long start = (unsigned long long)n_diff;
+    FHB_CUDA(cudaMemcpyAsync(d_qcount, &start, sizeof start, cudaMemcpyHostToDevice, stream));
+    if (n_same) {
+        const int blocks = (int)std::min<int64_t>((n_same + 127) / 128, (int64_t)sms * 32);
+        closed_form_coord_kernel<false><<<blocks, 128, 0, stream>>>(d_fil, d_items + offsets[kCoordCatSame], n_same,
+                                                                    out, n, d_quad, d_qcount, d_err);
+        FHB_CUDA(cudaGetLastError());
+    }
+    if (n_ortho) {
+        const int blocks = (int)std::min<int64_t>((n_ortho + 127) / 128, (int64_t)sms * 32);
+        closed_form_coord_kernel<true><<<blocks, 128, 0, stream>>>(d_fil, d_items + offsets[kCoordCatOrtho], n_ortho,
+                                                                   out, n, d_quad, d_qcount, d_err);
+        FHB_CUDA(cudaGetLastError());
+    }
+    unsigned long long q = 0;
+    FHB_CUDA(cudaMemcpyAsync(&q, d_qcount, sizeof q, cudaMemcpyDeviceToHost, stream));
+    FHB_CUDA(cudaStreamSynchronize(stream));
+    const int64_t n_quad = (int64_t)q;
+    st.closed_form = n_same + n_ortho - (n_quad - n_diff);
+    st.aligned_quadrature = n_quad;
+    if (n_quad) {
+        int64_t n_heads = 0, *d_heads = nullptr, *d_item_head = nullptr;
+        fh_status ds = distinct_keys(CoordKey{}, d_fil, d_quad, n_quad, alloc, stream, n_heads, d_heads, d_item_head,
+                                     err);
+        if (ds) return ds;
+        st.unique_aligned = n_heads;
+        double *d_values = nullptr;
+        FHB_CUDA(alloc((void **)&d_values, 64 * (size_t)n_heads));
+        const int qblocks = (int)std::min<int64_t>(n_heads, (int64_t)sms * 16);
+        aligned_quadrature_kernel<2><<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads, d_values);
+        FHB_CUDA(cudaGetLastError());
+        const int blocks = (int)std::min<int64_t>((n_quad + 255) / 256, (int64_t)sms * 16);
+        coord_quad_scatter_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_quad, d_item_head, d_values, n_quad, out, n,
+                                                              d_err);
+        FHB_CUDA(cudaGetLastError());
+    }
+    FHB_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof h_err, cudaMemcpyDeviceToHost, stream));
+    FHB_CUDA(cudaStreamSynchronize(stream));
+    if (h_err.key != ~0ull) {
+        const int64_t i = (int64_t)(h_err.key >> 32), j = (int64_t)(h_err.key & 0xffffffffull);
+        return fail(err, FH_ERR_KERNEL_NOT_FINITE,
+                    "coordinate derivative of the partial inductance of filaments " + std::to_string(i) + " and " +
+                        std::to_string(j) + " is not finite",
+                    i, j);
+    }
+    return FH_OK;
 }
 
 fh_status device_congruence(const double *d_L, const double *d_R, int64_t n, const int64_t *d_row_ptr,

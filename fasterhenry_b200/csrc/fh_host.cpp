@@ -701,6 +701,58 @@ std::vector<fh_truncation_warning> coupling_warnings(const CouplingResolved &r, 
     return out;
 }
 
+void conductor_layout(const fh_segment_def *segs, size_t n_segs, size_t n_nodes, const int64_t *per_segment,
+                      ConductorLayout &out) {
+    std::vector<int64_t> parent(n_nodes);
+    for (size_t v = 0; v < n_nodes; ++v) parent[v] = (int64_t)v;
+    auto find = [&](int64_t x) {
+        while (parent[(size_t)x] != x) {
+            parent[(size_t)x] = parent[(size_t)parent[(size_t)x]];
+            x = parent[(size_t)x];
+        }
+        return x;
+    };
+    for (size_t g = 0; g < n_segs; ++g) {
+        const int64_t a = find(segs[g].a), b = find(segs[g].b);
+        if (a != b) parent[(size_t)a] = b;
+    }
+    out = ConductorLayout();
+    std::vector<int64_t> roots;
+    for (size_t g = 0; g < n_segs; ++g) {
+        const int64_t root = find(segs[g].a);
+        auto it = std::find(roots.begin(), roots.end(), root);
+        if (it == roots.end()) {
+            roots.push_back(root);
+            out.conductor_of_segment.push_back((int64_t)roots.size() - 1);
+        } else {
+            out.conductor_of_segment.push_back((int64_t)(it - roots.begin()));
+        }
+    }
+    out.conductors = (int64_t)roots.size();
+    out.segment_first.assign(1, 0);
+    for (size_t g = 0; g < n_segs; ++g) {
+        for (int64_t k = 0; k < per_segment[g]; ++k) out.segment_of_filament.push_back((int64_t)g);
+        out.segment_first.push_back(out.segment_first.back() + per_segment[g]);
+    }
+}
+
+void transpose_loops(const LoopBasis &basis, int64_t n, int64_t rows, TransposedLoops &out) {
+    out.offset.assign((size_t)n + 1, 0);
+    for (int64_t i = 0; i < rows; ++i)
+        for (int64_t k = basis.row_ptr[(size_t)i]; k < basis.row_ptr[(size_t)i + 1]; ++k)
+            ++out.offset[(size_t)basis.branch[(size_t)k] + 1];
+    for (int64_t b = 0; b < n; ++b) out.offset[(size_t)b + 1] += out.offset[(size_t)b];
+    out.loop.assign((size_t)out.offset[(size_t)n], 0);
+    out.sign.assign((size_t)out.offset[(size_t)n], 0.0);
+    std::vector<int64_t> cursor(out.offset.begin(), out.offset.end() - 1);
+    for (int64_t i = 0; i < rows; ++i)
+        for (int64_t k = basis.row_ptr[(size_t)i]; k < basis.row_ptr[(size_t)i + 1]; ++k) {
+            const int64_t slot = cursor[(size_t)basis.branch[(size_t)k]]++;
+            out.loop[(size_t)slot] = (int32_t)i;
+            out.sign[(size_t)slot] = basis.sign[(size_t)k];
+        }
+}
+
 int64_t coupling_kept_pairs(const CouplingResolved &r, const int64_t *per_segment, size_t n_segs) {
     int64_t n = 0;
     const size_t g = r.names.size();

@@ -46,6 +46,27 @@ fh_status build_loops(const fh_segment_def *segs, size_t n_segs, size_t n_nodes,
                       const int64_t *per_segment, const fh_port *ports, size_t n_ports,
                       LoopBasis &out, fh_error_info *err);
 
+// Conductor layout (currents.rs:128-170): the segment of every filament, the
+// first filament of every segment (n_segs + 1 entries), and the conductor of
+// every segment, conductors being the connected components of the segment
+// graph numbered in order of their first segment.
+struct ConductorLayout {
+    std::vector<int64_t> segment_of_filament, segment_first, conductor_of_segment;
+    int64_t conductors = 0;
+};
+void conductor_layout(const fh_segment_def *segs, size_t n_segs, size_t n_nodes, const int64_t *per_segment,
+                      ConductorLayout &out);
+
+// The loop basis transposed over its first `rows` loops: per branch (n + 1
+// offsets) the (loop, sign) entries in increasing loop order, which is the
+// order in which a row-by-row scatter of the basis adds them.
+struct TransposedLoops {
+    std::vector<int64_t> offset;
+    std::vector<int32_t> loop;
+    std::vector<double> sign;
+};
+void transpose_loops(const LoopBasis &basis, int64_t n, int64_t rows, TransposedLoops &out);
+
 // Coupling resolved against a segment count (coupling.rs:323-380): group of
 // each segment (numbered by first appearance), names, and the symmetric
 // groups x groups table of kept pairs.

@@ -152,9 +152,18 @@ struct fh_iterative {
     double2 *d_res = nullptr, *d_cor = nullptr, *d_ax = nullptr;
     GmresWork work;
     double operator_s = 0;
+    // Currents (built on first use): segment / conductor layout, the loop
+    // basis transposed over all loops, (w, h, R) per filament, outputs.
+    ConductorLayout layout;
+    int64_t *d_col_ptr = nullptr, *d_first = nullptr, *d_segi = nullptr;
+    int32_t *d_col_loop = nullptr;
+    double *d_col_sign = nullptr, *d_whr = nullptr, *d_ip = nullptr, *d_ib = nullptr, *d_dens = nullptr,
+           *d_pow = nullptr, *d_segc = nullptr, *d_segp = nullptr, *d_segpk = nullptr;
     ~fh_iterative() {
-        void *ptrs[] = {d_row_ptr, d_t_off, d_branch, d_t_loop, d_sign, d_t_sign, d_r, d_c,
-                        d_drop, d_diag, d_b, d_x, d_parts, d_flux, d_res, d_cor, d_ax};
+        void *ptrs[] = {d_row_ptr, d_t_off, d_branch, d_t_loop, d_sign,  d_t_sign, d_r,    d_c,    d_drop,
+                        d_diag,    d_b,     d_x,      d_parts,  d_flux,  d_res,    d_cor,  d_ax,   d_col_ptr,
+                        d_first,   d_segi,  d_col_loop, d_col_sign, d_whr, d_ip,   d_ib,   d_dens, d_pow,
+                        d_segc,    d_segp,  d_segpk};
         for (void *q : ptrs)
             if (q) cudaFree(q);
     }
@@ -266,6 +275,77 @@ fh_status refined_solve(fh_iterative *s, double omega, const DeviceOp &apply, co
         FHB_CUDA(cudaGetLastError());
     }
     out->converged = false;
+    return FH_OK;
+}
+
+// Z_ee x = b for the right-hand side in s->d_b, x starting from zero: one
+// Jacobi-preconditioned GMRES solve on the pFFT operator (iterative.rs:
+// 269-288, 347-367), refined against the FP64 convolution when the operator
+// convolves in FP32.
+fh_status solve_ee(fh_iterative *s, double omega, double2 *x, GmresOutcome *oc, fh_error_info *err) {
+    const int64_t m = s->m;
+    cudaStream_t cs = s->stream;
+    std::vector<double2> diag((size_t)m);
+    for (int64_t i = 0; i < m; ++i) diag[i] = make_double2(s->r_diag[i], omega * s->l_diag[i]);
+    FHB_CUDA(cudaMemcpyAsync(s->d_diag, diag.data(), sizeof(double2) * m, cudaMemcpyHostToDevice, cs));
+    DeviceOp apply = [&](const double2 *in, double2 *out, fh_error_info *e) { return apply_ee(s, omega, in, out, e); };
+    DeviceOp precondition = [&](const double2 *in, double2 *out, fh_error_info *e) {
+        jacobi_kernel<<<grid_n(m), 256, 0, cs>>>(in, s->d_diag, out, m);
+        cudaError_t ce = cudaGetLastError();
+        if (ce != cudaSuccess) return fail(e, FH_ERR_CUDA, std::string("jacobi: ") + cudaGetErrorString(ce));
+        return FH_OK;
+    };
+    FHB_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * m, cs));
+    fh_status st = s->op.fft_fp32 ? refined_solve(s, omega, apply, precondition, x, oc, err)
+                                  : gmres_solve(m, apply, precondition, s->d_b, x, s->gp, cs, s->work, oc, err);
+    // Also keeps `diag` alive until its copy has run.
+    cudaError_t ce = cudaStreamSynchronize(cs);
+    if (st) return st;
+    FHB_CUDA(ce);
+    return FH_OK;
+}
+
+// SolveError::NotConverged (iterative.rs:368-375) for the first failing solve.
+fh_status not_converged(fh_error_info *err, double f, int64_t port, const GmresOutcome &oc) {
+    fh_status e = fail(err, FH_ERR_NOT_CONVERGED,
+                       "GMRES did not converge at " + std::to_string(f) + " Hz for port " + std::to_string(port) +
+                           " after " + std::to_string(oc.iterations) + " iterations (relative residual " +
+                           std::to_string(oc.relative_residual) + ")",
+                       port, -1, f);
+    if (err) {
+        err->iterations = oc.iterations;
+        err->residual = oc.relative_residual;
+    }
+    return e;
+}
+
+// Device buffers of the currents for one frequency, built on first use.
+fh_status prepare_currents(fh_iterative *s, fh_error_info *err) {
+    if (s->d_col_ptr) return FH_OK;
+    cudaStream_t cs = s->stream;
+    const int64_t n = s->n, p = s->p, nseg = (int64_t)s->layout.conductor_of_segment.size();
+    TransposedLoops cols;
+    transpose_loops(s->loops, n, s->nloops, cols);
+    std::vector<double> whr((size_t)(3 * n));
+    for (int64_t k = 0; k < n; ++k) {
+        whr[(size_t)(3 * k)] = s->disc.filaments[(size_t)k].width;
+        whr[(size_t)(3 * k + 1)] = s->disc.filaments[(size_t)k].height;
+        whr[(size_t)(3 * k + 2)] = s->resistances[(size_t)k];
+    }
+    FHB_CUDA(put(&s->d_col_ptr, cols.offset, cs));
+    FHB_CUDA(put(&s->d_col_loop, cols.loop, cs));
+    FHB_CUDA(put(&s->d_col_sign, cols.sign, cs));
+    FHB_CUDA(put(&s->d_whr, whr, cs));
+    FHB_CUDA(put(&s->d_first, s->layout.segment_first, cs));
+    auto alloc = [&](void **q, size_t bytes) { return cudaMalloc(q, std::max<size_t>(bytes, 16)); };
+    if (alloc((void **)&s->d_ip, 16 * (size_t)p) || alloc((void **)&s->d_ib, 16 * (size_t)n) ||
+        alloc((void **)&s->d_dens, 8 * (size_t)n) || alloc((void **)&s->d_pow, 8 * (size_t)n) ||
+        alloc((void **)&s->d_segc, 16 * (size_t)nseg) || alloc((void **)&s->d_segp, 8 * (size_t)nseg) ||
+        alloc((void **)&s->d_segpk, 8 * (size_t)nseg) || alloc((void **)&s->d_segi, 8 * (size_t)nseg)) {
+        cudaGetLastError();
+        return fail(err, FH_ERR_OUT_OF_MEMORY, "device allocation of the currents buffers failed");
+    }
+    FHB_CUDA(cudaStreamSynchronize(cs));
     return FH_OK;
 }
 
@@ -420,25 +500,14 @@ fh_status fh_iterative_create(const fh_node *nodes, size_t n_nodes, const fh_seg
     }
 
     // Device copies of the loop basis, its transpose over internal loops, R.
-    std::vector<int64_t> t_off((size_t)n + 1, 0);
-    for (int64_t i = 0; i < m; ++i)
-        for (int64_t k = rp[i]; k < rp[i + 1]; ++k) t_off[br[k] + 1] += 1;
-    for (int64_t b = 0; b < n; ++b) t_off[b + 1] += t_off[b];
-    std::vector<int32_t> t_loop((size_t)t_off[n]);
-    std::vector<double> t_sign((size_t)t_off[n]);
-    std::vector<int64_t> fillp(t_off.begin(), t_off.end() - 1);
-    for (int64_t i = 0; i < m; ++i)
-        for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
-            const int64_t slot = fillp[br[k]]++;
-            t_loop[slot] = (int32_t)i;
-            t_sign[slot] = sg[k];
-        }
+    TransposedLoops internal;
+    transpose_loops(s->loops, n, m, internal);
     FHB_CUDA(put(&s->d_row_ptr, rp, cs));
     FHB_CUDA(put(&s->d_branch, br, cs));
     FHB_CUDA(put(&s->d_sign, sg, cs));
-    FHB_CUDA(put(&s->d_t_off, t_off, cs));
-    FHB_CUDA(put(&s->d_t_loop, t_loop, cs));
-    FHB_CUDA(put(&s->d_t_sign, t_sign, cs));
+    FHB_CUDA(put(&s->d_t_off, internal.offset, cs));
+    FHB_CUDA(put(&s->d_t_loop, internal.loop, cs));
+    FHB_CUDA(put(&s->d_t_sign, internal.sign, cs));
     FHB_CUDA(put(&s->d_r, s->resistances, cs));
     auto alloc = [&](void **q, size_t bytes) { return cudaMalloc(q, std::max<size_t>(bytes, 16)); };
     if (alloc((void **)&s->d_c, sizeof(double2) * n) || alloc((void **)&s->d_drop, sizeof(double2) * n) ||
@@ -449,6 +518,7 @@ fh_status fh_iterative_create(const fh_node *nodes, size_t n_nodes, const fh_seg
         return fail(err, FH_ERR_OUT_OF_MEMORY, "device allocation of the iterative system failed");
     }
     FHB_CUDA(cudaStreamSynchronize(cs));
+    conductor_layout(segments, n_segments, n_nodes, s->disc.per_segment.data(), s->layout);
     s->counts = fh_counts{(int64_t)n_nodes, (int64_t)n_segments, n, L, m, p};
     s->timing.inductance_s = s->operator_s;
     s->timing.assembly_s = wall_s() - t0;
@@ -507,47 +577,20 @@ fh_status fh_iterative_sweep(fh_iterative *s, const double *freqs, size_t nf, do
             for (int64_t b = 0; b < p; ++b)
                 z[a + b * p] = cplx(s->r_pp[a + b * p], omega * s->l_pp[a + b * p]);
         if (m > 0) {
-            std::vector<double2> diag((size_t)m), rhs((size_t)m);
-            for (int64_t i = 0; i < m; ++i) diag[i] = make_double2(s->r_diag[i], omega * s->l_diag[i]);
-            FHB_CUDA(cudaMemcpyAsync(s->d_diag, diag.data(), sizeof(double2) * m, cudaMemcpyHostToDevice, cs));
-            DeviceOp apply = [&](const double2 *in, double2 *out, fh_error_info *e) {
-                return apply_ee(s, omega, in, out, e);
-            };
-            DeviceOp precondition = [&](const double2 *in, double2 *out, fh_error_info *e) {
-                jacobi_kernel<<<grid_n(m), 256, 0, cs>>>(in, s->d_diag, out, m);
-                cudaError_t ce = cudaGetLastError();
-                if (ce != cudaSuccess) return fail(e, FH_ERR_CUDA, std::string("jacobi: ") + cudaGetErrorString(ce));
-                return FH_OK;
-            };
+            std::vector<double2> rhs((size_t)m);
             std::vector<double2> xs((size_t)m * p);
             for (int64_t q = 0; q < p; ++q) {
                 for (int64_t i = 0; i < m; ++i) rhs[i] = make_double2(s->r_ep[i + q * m], omega * s->l_ep[i + q * m]);
                 FHB_CUDA(cudaMemcpyAsync(s->d_b, rhs.data(), sizeof(double2) * m, cudaMemcpyHostToDevice, cs));
-                double2 *xq = s->d_x + q * m;
-                FHB_CUDA(cudaMemsetAsync(xq, 0, sizeof(double2) * m, cs));
                 GmresOutcome oc;
-                fh_status st = s->op.fft_fp32 ? refined_solve(s, omega, apply, precondition, xq, &oc, err)
-                                              : gmres_solve(m, apply, precondition, s->d_b, xq, s->gp, cs, s->work,
-                                                            &oc, err);
+                fh_status st = solve_ee(s, omega, s->d_x + q * m, &oc, err);
                 if (st) return st;
                 if (outcomes) {
                     outcomes[fi * p + q].iterations = oc.iterations;
                     outcomes[fi * p + q].relative_residual = oc.relative_residual;
                     outcomes[fi * p + q].converged = oc.converged ? 1 : 0;
                 }
-                if (!oc.converged) {
-                    fh_status e2 = fail(err, FH_ERR_NOT_CONVERGED,
-                                        "GMRES did not converge at " + std::to_string(f) + " Hz for port " +
-                                            std::to_string(q) + " after " + std::to_string(oc.iterations) +
-                                            " iterations (relative residual " + std::to_string(oc.relative_residual) +
-                                            ")",
-                                        (int64_t)q, -1, f);
-                    if (err) {
-                        err->iterations = oc.iterations;
-                        err->residual = oc.relative_residual;
-                    }
-                    return e2;
-                }
+                if (!oc.converged) return not_converged(err, f, q, oc);
             }
             FHB_CUDA(cudaMemcpyAsync(xs.data(), s->d_x, sizeof(double2) * m * p, cudaMemcpyDeviceToHost, cs));
             FHB_CUDA(cudaStreamSynchronize(cs));
@@ -579,6 +622,148 @@ fh_status fh_iterative_sweep(fh_iterative *s, const double *freqs, size_t nf, do
     }
     s->timing.solve_s = wall_s() - t0;
     s->timing.total_s = s->timing.assembly_s + s->timing.solve_s;
+    return FH_OK;
+}
+
+fh_status fh_iterative_filaments(const fh_iterative *s, fh_filament *out, size_t capacity) {
+    if (!s || !out) return fail(nullptr, FH_ERR_INVALID_ARGUMENT, "null argument");
+    if (capacity < s->disc.filaments.size()) return fail(nullptr, FH_ERR_INVALID_ARGUMENT, "buffer too small");
+    std::copy(s->disc.filaments.begin(), s->disc.filaments.end(), out);
+    return FH_OK;
+}
+
+fh_status fh_iterative_layout(const fh_iterative *s, int64_t *segment_of_filament, int64_t *conductor_of_segment,
+                              int64_t *conductor_count) {
+    if (!s) return fail(nullptr, FH_ERR_INVALID_ARGUMENT, "null system");
+    const ConductorLayout &l = s->layout;
+    if (segment_of_filament) std::copy(l.segment_of_filament.begin(), l.segment_of_filament.end(), segment_of_filament);
+    if (conductor_of_segment)
+        std::copy(l.conductor_of_segment.begin(), l.conductor_of_segment.end(), conductor_of_segment);
+    if (conductor_count) *conductor_count = l.conductors;
+    return FH_OK;
+}
+
+// IterativeSystem::currents (iterative.rs:316-377 with solve.rs:1110-1149):
+// per frequency one GMRES solve Z_ee x = Z_ep I_p, internal loop currents
+// -x, port voltages V_p = Z_pp I_p + Z_ep^T I_e, then the same branch
+// currents, densities, powers, segment sums and conductor peaks as the dense
+// path.
+fh_status fh_iterative_currents(fh_iterative *s, const double *freqs, size_t nf, const double *excitation,
+                                size_t n_excitation, double *filament_current, double *current_density,
+                                double *power_w, double *segment_current, double *segment_power_w,
+                                int64_t *conductor_peak_filament, double *conductor_peak_density,
+                                fh_power_balance *balance, fh_gmres_outcome *outcomes, fh_error_info *err) {
+    clear_error(err);
+    if (!s || (nf && !freqs) || (n_excitation && !excitation))
+        return fail(err, FH_ERR_INVALID_ARGUMENT, "null argument");
+    for (size_t k = 0; k < nf; ++k)
+        if (!(std::isfinite(freqs[k]) && freqs[k] >= 0.0))
+            return fail(err, FH_ERR_INVALID_FREQUENCY,
+                        "frequency " + std::to_string(k) + " is " + std::to_string(freqs[k]) +
+                            " Hz; frequencies must be finite and non-negative",
+                        (int64_t)k, -1, freqs[k]);
+    const int64_t n = s->n, m = s->m, p = s->p;
+    const int64_t nseg = (int64_t)s->layout.conductor_of_segment.size(), ncond = s->layout.conductors;
+    bool finite = (int64_t)n_excitation == p;
+    for (size_t q = 0; q < 2 * n_excitation && finite; ++q) finite = std::isfinite(excitation[q]);
+    if (!finite)
+        return fail(err, FH_ERR_INVALID_EXCITATION,
+                    "excitation must have one finite entry per port (" + std::to_string(p) + "), got " +
+                        std::to_string(n_excitation) + " entries",
+                    p, (int64_t)n_excitation);
+    if (nf == 0) return FH_OK;
+    fh_status st = prepare_currents(s, err);
+    if (st) return st;
+    cudaStream_t cs = s->stream;
+    std::vector<cplx> ip((size_t)p);
+    for (int64_t q = 0; q < p; ++q) ip[(size_t)q] = cplx(excitation[2 * q], excitation[2 * q + 1]);
+    FHB_CUDA(cudaMemcpyAsync(s->d_ip, excitation, 16 * (size_t)p, cudaMemcpyHostToDevice, cs));
+    std::vector<double2> rhs((size_t)m), x((size_t)m);
+    std::vector<double> segp((size_t)nseg), segpk((size_t)nseg);
+    std::vector<int64_t> segi((size_t)nseg);
+    const double t0 = wall_s();
+    for (size_t fi = 0; fi < nf; ++fi) {
+        const double f = freqs[fi];
+        const double omega = f == 0.0 ? 0.0 : kTauI * f;
+        auto ep = [&](int64_t i, int64_t q) { return cplx(s->r_ep[i + q * m], omega * s->l_ep[i + q * m]); };
+        GmresOutcome oc;
+        oc.converged = true;
+        if (m > 0) {
+            for (int64_t i = 0; i < m; ++i) {
+                cplx acc(0.0, 0.0);
+                for (int64_t q = 0; q < p; ++q) acc += ep(i, q) * ip[(size_t)q];
+                rhs[(size_t)i] = make_double2(acc.real(), acc.imag());
+            }
+            FHB_CUDA(cudaMemcpyAsync(s->d_b, rhs.data(), sizeof(double2) * m, cudaMemcpyHostToDevice, cs));
+            st = solve_ee(s, omega, s->d_x, &oc, err);
+            if (st) return st;
+            if (outcomes) {
+                outcomes[fi].iterations = oc.iterations;
+                outcomes[fi].relative_residual = oc.relative_residual;
+                outcomes[fi].converged = oc.converged ? 1 : 0;
+            }
+            if (!oc.converged) return not_converged(err, f, 0, oc);
+        } else if (outcomes) {
+            outcomes[fi] = fh_gmres_outcome{0, 0.0, 1};
+        }
+        st = launch_currents(reinterpret_cast<const double *>(s->d_x), s->d_ip, m, (int)p, true, n, 1, s->d_col_ptr,
+                             s->d_col_loop, s->d_col_sign, s->d_whr, s->d_first, nseg, s->d_ib, s->d_dens, s->d_pow,
+                             s->d_segc, s->d_segp, s->d_segpk, s->d_segi, cs, err);
+        if (st) return st;
+        if (m > 0) FHB_CUDA(cudaMemcpyAsync(x.data(), s->d_x, sizeof(double2) * m, cudaMemcpyDeviceToHost, cs));
+        FHB_CUDA(cudaMemcpyAsync(segp.data(), s->d_segp, 8 * (size_t)nseg, cudaMemcpyDeviceToHost, cs));
+        FHB_CUDA(cudaMemcpyAsync(segpk.data(), s->d_segpk, 8 * (size_t)nseg, cudaMemcpyDeviceToHost, cs));
+        FHB_CUDA(cudaMemcpyAsync(segi.data(), s->d_segi, 8 * (size_t)nseg, cudaMemcpyDeviceToHost, cs));
+        if (filament_current)
+            FHB_CUDA(cudaMemcpyAsync(filament_current + 2 * fi * n, s->d_ib, 16 * (size_t)n, cudaMemcpyDeviceToHost, cs));
+        if (current_density)
+            FHB_CUDA(cudaMemcpyAsync(current_density + fi * n, s->d_dens, 8 * (size_t)n, cudaMemcpyDeviceToHost, cs));
+        if (power_w) FHB_CUDA(cudaMemcpyAsync(power_w + fi * n, s->d_pow, 8 * (size_t)n, cudaMemcpyDeviceToHost, cs));
+        if (segment_current)
+            FHB_CUDA(cudaMemcpyAsync(segment_current + 2 * fi * nseg, s->d_segc, 16 * (size_t)nseg,
+                                     cudaMemcpyDeviceToHost, cs));
+        FHB_CUDA(cudaStreamSynchronize(cs));
+        // V_p = Z_pp I_p + Z_ep^T I_e with I_e = -x (solve.rs:1128).
+        bool ok = true;
+        std::vector<cplx> v((size_t)p);
+        for (int64_t a = 0; a < p; ++a) {
+            cplx acc(0.0, 0.0);
+            for (int64_t b = 0; b < p; ++b)
+                acc += cplx(s->r_pp[a + b * p], omega * s->l_pp[a + b * p]) * ip[(size_t)b];
+            for (int64_t i = 0; i < m; ++i) acc -= ep(i, a) * cplx(x[(size_t)i].x, x[(size_t)i].y);
+            v[(size_t)a] = acc;
+            ok = ok && std::isfinite(acc.real()) && std::isfinite(acc.imag());
+        }
+        for (int64_t i = 0; i < m && ok; ++i) ok = std::isfinite(x[(size_t)i].x) && std::isfinite(x[(size_t)i].y);
+        if (!ok)
+            return fail(err, FH_ERR_SINGULAR, "the currents at " + std::to_string(f) + " Hz are not finite",
+                        (int64_t)fi, -1, f);
+        if (segment_power_w) std::copy(segp.begin(), segp.end(), segment_power_w + fi * nseg);
+        // Conductor peaks: segments are contiguous in filament order, so the
+        // first strictly larger segment peak is the first filament of
+        // largest |J|.
+        std::vector<double> best((size_t)ncond, -1.0);
+        std::vector<int64_t> at((size_t)ncond, -1);
+        double dissipated = 0.0;
+        for (int64_t g = 0; g < nseg; ++g) {
+            dissipated += segp[(size_t)g];
+            const int64_t c = s->layout.conductor_of_segment[(size_t)g];
+            if (segi[(size_t)g] >= 0 && (at[(size_t)c] < 0 || segpk[(size_t)g] > best[(size_t)c])) {
+                best[(size_t)c] = segpk[(size_t)g];
+                at[(size_t)c] = segi[(size_t)g];
+            }
+        }
+        if (conductor_peak_filament) std::copy(at.begin(), at.end(), conductor_peak_filament + fi * ncond);
+        if (conductor_peak_density) std::copy(best.begin(), best.end(), conductor_peak_density + fi * ncond);
+        if (balance) {
+            double input = 0.0;
+            for (int64_t a = 0; a < p; ++a) input += (std::conj(ip[(size_t)a]) * v[(size_t)a]).real();
+            input *= 0.5;
+            const double scale = std::max(dissipated, input);
+            balance[fi] = fh_power_balance{dissipated, input, scale > 0.0 ? std::fabs(dissipated - input) / scale : 0.0};
+        }
+    }
+    s->timing.solve_s = wall_s() - t0;
     return FH_OK;
 }
 

@@ -430,9 +430,16 @@ typedef struct fh_gradient_report {
  * one product per derivative matrix.  Derivatives are those of the
  * evaluation as dispatched at the nominal geometry (method, Gauss orders,
  * closed-form acceptance, quadrature panels, and the discretization's
- * filament counts and grading held fixed).  z_out (optional): p x p Z;
- * dz_out: np x p x p complex (interleaved), row-major per parameter, in ohm
- * per metre.  report optional. */
+ * filament counts and grading held fixed).  Parameters: a segment's width
+ * or thickness, or a node's x or y.  A node moving in the xy plane turns the
+ * segments that meet there about z and changes their length; those segments
+ * must lie in a plane z = const with z along their width or height, else
+ * FH_ERR_UNSUPPORTED (so is FH_PARAM_NODE_Z, and a coordinate parameter
+ * whose moving filaments have a parallel partner of another segment with
+ * cross-sections meeting along the length, such as collinear segments end
+ * to end).  z_out (optional): p x p Z; dz_out: np x p x p complex
+ * (interleaved), row-major per parameter, in ohm per metre.  report
+ * optional. */
 fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *params, size_t np, double *z_out,
                       double *dz_out, fh_gradient_report *report, fh_error_info *err);
 
@@ -442,6 +449,16 @@ fh_status fh_gradient(fh_system *sys, double frequency_hz, const fh_param_spec *
  * D[a + b n] = dL_ab / d(side a). */
 fh_status fh_test_inductance_gradient(const fh_filament *filaments, const double *tangents, size_t n, double *Dw,
                                       double *Dh, fh_error_info *err);
+
+/* Test hook: the coordinate derivative fill of a filament set (every filament
+ * moving; segment[i] numbers the segment of filament i).  Dl, Dp, Ds, Dr:
+ * n x n column-major, D[a + b n] = dL_ab / d(coordinate of a): translation
+ * of its centre along its length axis (Dl) and along z x l normalized (Dp),
+ * stretch of its length about its centre (Ds), rotation about the z axis
+ * through its centre (Dr).  Pairs of one segment carry Ds only; the diagonal
+ * of Ds is half of dL_aa / d length. */
+fh_status fh_test_coordinate_gradient(const fh_filament *filaments, const int32_t *segment, size_t n, double *Dl,
+                                      double *Dp, double *Ds, double *Dr, fh_error_info *err);
 
 /* Test hook: the device near-pair search of the precorrected-FFT set-up
  * (pfft/near.rs:41-106) for a filament set and a radius in metres: for each
@@ -614,6 +631,22 @@ fh_status fh_iterative_pfft_stats(const fh_iterative *sys, fh_pfft_stats *out);
  * failing solve; FH_ERR_SINGULAR a non-finite Z. */
 fh_status fh_iterative_sweep(fh_iterative *sys, const double *frequencies_hz, size_t nf, double *z_out,
                              fh_gmres_outcome *outcomes, fh_error_info *err);
+/* The discretized filaments (n, as fh_system_filaments) and the segment /
+ * conductor layout (as fh_system_layout) of an iterative system. */
+fh_status fh_iterative_filaments(const fh_iterative *sys, fh_filament *out, size_t capacity);
+fh_status fh_iterative_layout(const fh_iterative *sys, int64_t *segment_of_filament, int64_t *conductor_of_segment,
+                              int64_t *conductor_count);
+/* IterativeSystem::currents (iterative.rs:316-377 with solve.rs:1110-1149):
+ * per frequency one Jacobi-preconditioned GMRES solve Z_ee x = Z_ep I_p on
+ * the pFFT operator, internal loop currents -x, port voltages
+ * V_p = Z_pp I_p + Z_ep^T I_e; outputs and errors as fh_currents, plus the
+ * GMRES outcome of every frequency (`outcomes`, optional, nf) and
+ * FH_ERR_NOT_CONVERGED (port index 0) as fh_iterative_sweep. */
+fh_status fh_iterative_currents(fh_iterative *sys, const double *frequencies_hz, size_t nf, const double *excitation,
+                                size_t n_excitation, double *filament_current, double *current_density,
+                                double *power_w, double *segment_current, double *segment_power_w,
+                                int64_t *conductor_peak_filament, double *conductor_peak_density,
+                                fh_power_balance *balance, fh_gmres_outcome *outcomes, fh_error_info *err);
 void fh_iterative_destroy(fh_iterative *sys);
 
 /* Test hook (no reference counterpart): the device GMRES on a dense complex

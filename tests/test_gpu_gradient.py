@@ -234,7 +234,7 @@ def test_gradient_argument_errors(fh):
     deck = F.square_spiral(2, 10e-6, 5e-6, 2e-6, 150e-6, F.uniform(2, 1))
     with fh.MeshSystem.assemble(fh.Geometry.from_deck(deck), deck.ports, deck.discretization) as system:
         with pytest.raises(fh.Unsupported):
-            system.gradient(1e9, [fh.Param("x", 1)])
+            system.gradient(1e9, [fh.Param("z", 1)])
         with pytest.raises(fh.InvalidArgument):
             system.gradient(1e9, [fh.Param("width", 99)])
         with pytest.raises(fh.InvalidFrequency):

@@ -494,13 +494,6 @@ def run_c5(args):
     torch.cuda.set_device(local)
     params = fh.IterativeParams(pfft=fh.PfftParams(near_field_radius=8.0, interpolation_order=2, fft_fp32=True),
                                 gmres=fh.GmresParams(tolerance=1e-8))
-    sub = F.meander_over_plane(49)
-    g = fh.Geometry.from_deck(sub)
-    with fh.IterativeSystem.assemble(g, sub.ports, sub.discretization, params) as s:
-        z_it = s.impedance(1e9)
-    with fh.MeshSystem.assemble(g, sub.ports, sub.discretization) as d:
-        z_d = d.impedance(1e9)
-    subset_rel = float(np.max(np.abs(z_it - z_d) / np.abs(z_d)))
     deck = F.meander_over_plane(157)
     geometry = fh.Geometry.from_deck(deck)
     t0 = time.perf_counter()
@@ -521,6 +514,15 @@ def run_c5(args):
     stats = system.operator_stats()
     outcome = system.last_outcomes[0][0]
     pa = profile["pfft_apply"]
+    # The parity check after the timed solves (so that a launch list of this
+    # command starts with the full-size system's kernels).
+    sub = F.meander_over_plane(49)
+    g = fh.Geometry.from_deck(sub)
+    with fh.IterativeSystem.assemble(g, sub.ports, sub.discretization, params) as s:
+        z_it = s.impedance(1e9)
+    with fh.MeshSystem.assemble(g, sub.ports, sub.discretization) as d:
+        z_d = d.impedance(1e9)
+    subset_rel = float(np.max(np.abs(z_it - z_d) / np.abs(z_d)))
     peaks, peak_kind = _peaks()
     hbm = peaks.get("hbm_gbs", 6650.0)
     achieved = pa["work"] / (pa["ms"] * 1e-3) / 1e9 if pa["ms"] else 0.0

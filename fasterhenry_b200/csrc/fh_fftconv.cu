@@ -37,7 +37,12 @@
 namespace fhb {
 namespace {
 
-constexpr int kFftThreads = 256;
+// Threads per CTA: 512 for FP32 (two CTAs, 32 warps per SM), 256 for FP64
+// (whose wider lines leave fewer butterflies per tile).
+template <class T>
+constexpr int fft_threads() {
+    return sizeof(T) == 4 ? 512 : 256;
+}
 constexpr size_t kFftSmemBudget = 100 * 1024;  // two CTAs per SM
 constexpr double kPi = 3.14159265358979323846;
 
@@ -112,7 +117,8 @@ __device__ __forceinline__ void small_dft(V (&v)[R], int sign) {
 }
 
 // One Stockham pass of radix R over `lines` interleaved lines of length m
-// (element t of line l at t * lines + l), src -> dst.
+// (element t of line l at t * lines + l), src -> dst; tw holds
+// exp(-2 pi i t / m) in shared memory.
 template <int R, class V, class T>
 __device__ void stockham_pass(const V *__restrict__ src, V *__restrict__ dst, int m, int lines, int Ns,
                               const V *__restrict__ tw, int sign) {
@@ -172,16 +178,18 @@ __device__ V *stockham(V *a, V *b, int m, int lines, const FftAxis &ax, const V 
 // axis-0 step): a CTA reads its whole tile before it writes, and tiles are
 // disjoint.
 template <class T>
-__global__ void __launch_bounds__(kFftThreads)
+__global__ void __launch_bounds__(fft_threads<T>())
     fft_lines_kernel(const typename Cplx<T>::type *in, typename Cplx<T>::type *out,
                      int64_t in_stride, int64_t out_stride, int64_t outer, int64_t inner, int n_in, int keep,
-                     FftAxis ax, const typename Cplx<T>::type *__restrict__ tw, int sign, int tile,
+                     FftAxis ax, const typename Cplx<T>::type *__restrict__ tw_global, int sign, int tile,
                      const T *__restrict__ spectrum) {
     using V = typename Cplx<T>::type;
     extern __shared__ __align__(16) unsigned char fft_smem[];
     V *bufa = reinterpret_cast<V *>(fft_smem);
     V *bufb = bufa + (size_t)tile * ax.m;
+    V *tw = bufb + (size_t)tile * ax.m;  // the twiddles, read by every pass
     const int m = ax.m;
+    for (int t = threadIdx.x; t < m; t += blockDim.x) tw[t] = tw_global[t];
     const V *src = in + (int64_t)blockIdx.y * in_stride;
     V *dst = out + (int64_t)blockIdx.y * out_stride;
     const bool contiguous = inner == 1;
@@ -286,13 +294,16 @@ unsigned blocks_of(int64_t work, int threads, int64_t cap = 148 * 16) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>((work + threads - 1) / threads, cap));
 }
 
-// Lines per CTA: as many as two buffers of them fit the shared-memory budget,
-// up to about 4,096 points per tile (short lines come many to a tile).
+// Lines per CTA: as many as two buffers of them and the twiddles fit the
+// shared-memory budget, up to about 8,192 points per tile (short lines come
+// many to a tile).
 template <class T>
 int tile_for(int m) {
-    const size_t per = 2 * sizeof(typename Cplx<T>::type) * (size_t)m;
-    const size_t want = std::max<size_t>(16, 4096 / (size_t)m);
-    return (int)std::max<size_t>(1, std::min<size_t>(want, kFftSmemBudget / per));
+    const size_t elem = sizeof(typename Cplx<T>::type);
+    const size_t per = 2 * elem * (size_t)m;
+    const size_t want = std::max<size_t>(16, 8192 / (size_t)m);
+    const size_t room = kFftSmemBudget > elem * (size_t)m ? kFftSmemBudget - elem * (size_t)m : 0;
+    return (int)std::max<size_t>(1, std::min<size_t>(want, room / per));
 }
 
 // One axis step: outer x n_in x inner -> outer x keep x inner, `batch` arrays.
@@ -302,11 +313,14 @@ fh_status axis_step(const void *in, void *out, int64_t in_stride, int64_t out_st
                     cudaStream_t s, fh_error_info *err) {
     using V = typename Cplx<T>::type;
     const int tile = tile_for<T>(ax.m);
-    const size_t smem = 2 * sizeof(V) * (size_t)tile * ax.m;
+    const size_t smem = sizeof(V) * ((2 * (size_t)tile + 1) * ax.m);
+    if (smem > 227 * 1024)
+        return fail(err, FH_ERR_PFFT, "pFFT convolution: axis length " + std::to_string(ax.m) +
+                                          " does not fit the transform kernel's shared memory");
     const int64_t tiles = inner == 1 ? (outer + tile - 1) / tile : outer * ((inner + tile - 1) / tile);
     FHB_CUDA(cudaFuncSetAttribute(fft_lines_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, 148 * 8));
-    fft_lines_kernel<T><<<dim3(gx, (unsigned)batch), kFftThreads, smem, s>>>(
+    fft_lines_kernel<T><<<dim3(gx, (unsigned)batch), fft_threads<T>(), smem, s>>>(
         static_cast<const V *>(in), static_cast<V *>(out), in_stride, out_stride, outer, inner, n_in, keep, ax,
         static_cast<const V *>(tw), sign, tile, spectrum);
     FHB_CUDA(cudaGetLastError());

@@ -11,7 +11,7 @@
 namespace fhb {
 
 constexpr int kFftMaxFactors = 24;
-constexpr int64_t kFftMaxLength = 6144;  // longest padded axis (two FP64 lines of it fit a CTA's shared memory)
+constexpr int64_t kFftMaxLength = 4800;  // longest padded axis: two FP64 lines of it and its twiddles fit a CTA
 
 // One axis: its length and its radices (4, then 2, 3, 5), passed by value to
 // the kernels.

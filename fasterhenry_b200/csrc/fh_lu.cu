@@ -1558,12 +1558,16 @@ fh_status lu_factor(LuBatch<T> &b, LuWork &w, int nb, TrailingUpdate mode, cudaS
             fh_status st = gemm_tc_update(reinterpret_cast<float *>(b.a), m, b.count, k0, nb, s, err);
             prof_end(s, FH_PROF_GEMM_TC, flops);
             if (st) return st;
+        } else if constexpr (sizeof(T) == 8) {
+            prof_begin(s, FH_PROF_GEMM_FP64);
+            fh_status st = dmma_update(b.a, m, b.count, k0, w_nb, s, err);
+            prof_end(s, FH_PROF_GEMM_FP64, flops);
+            if (st) return st;
         } else {
-            const int cls = sizeof(T) == 8 ? FH_PROF_GEMM_FP64 : FH_PROF_GEMM_FP32;
-            prof_begin(s, cls);
+            prof_begin(s, FH_PROF_GEMM_FP32);
             const unsigned tiles = (unsigned)((ncols + 63) / 64);
             gemm_update_kernel<T><<<dim3(tiles, tiles, b.count), 256, gemm_smem, s>>>(a, m, (int)k0, w_nb);
-            prof_end(s, cls, flops);
+            prof_end(s, FH_PROF_GEMM_FP32, flops);
         }
         FHB_CUDA(cudaGetLastError());
     }
@@ -1576,6 +1580,7 @@ template <class T>
 fh_status gemm_simt_update(T *av, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err) {
     const int64_t ncols = m - k0 - nb;
     if (ncols <= 0) return FH_OK;
+    if constexpr (sizeof(T) == 8) return dmma_update(av, m, count, k0, nb, s, err);
     const size_t gemm_smem = sizeof(Cx<T>) * (size_t)nb * 128;
     FHB_CUDA(cudaFuncSetAttribute(gemm_update_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem));
     const unsigned tiles = (unsigned)((ncols + 63) / 64);

@@ -148,6 +148,10 @@ fh_status gemm_tc_packed_check(fh_error_info *err);
 // One SIMT trailing update (FP32 or FP64), for tests.
 template <class T>
 fh_status gemm_simt_update(T *a, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err);
+// The FP64 form of the same update on the FP64 tensor cores (mma.sync m8n8k4
+// f64, fh_dmma.cu): A22 -= L21 U12 for panel [k0, k0 + nb) of `count`
+// complex column-major m x m matrices.
+fh_status dmma_update(double *a, int64_t m, int count, int64_t k0, int nb, cudaStream_t s, fh_error_info *err);
 // U12 = Linv A12 of panel [k0, k0+nb) in place (tensor cores / SIMT).
 fh_status gemm_tc_tri_apply(const float *linv, int nb, float *a, int64_t m, int count, int64_t k0, cudaStream_t s,
                             fh_error_info *err);

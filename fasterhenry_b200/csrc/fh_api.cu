@@ -94,6 +94,11 @@ struct fh_system {
     int64_t *d_col_ptr = nullptr, *d_first = nullptr;
     int32_t *d_col_loop = nullptr;
     double *d_col_sign = nullptr, *d_whr = nullptr;
+    // The loop basis, its transpose over the internal loops and the branch
+    // resistances on the device: R_ee x of the refinement residuals.
+    int64_t *d_rp = nullptr, *d_toff = nullptr;
+    int32_t *d_br = nullptr, *d_tloop = nullptr;
+    double *d_sign = nullptr, *d_tsign = nullptr, *d_R = nullptr;
     fh_counts counts{};
     fh_timing timing{};
     FillStats fill{};
@@ -102,6 +107,9 @@ struct fh_system {
         pool.release();
         cache_free(d_Lm, stream);
         cache_free(d_Rm, stream);
+        for (void *q : {(void *)d_rp, (void *)d_toff, (void *)d_br, (void *)d_tloop, (void *)d_sign, (void *)d_tsign,
+                        (void *)d_R})
+            cache_free(q, stream);
         cache_free(d_col_ptr, stream);
         cache_free(d_first, stream);
         cache_free(d_col_loop, stream);
@@ -185,7 +193,7 @@ struct PBuf {
 enum PoolSlot {
     kSlotA, kSlotD32, kSlotR, kSlotRnorm, kSlotBnorm, kSlotDnorm, kSlotXnorm, kSlotPiv, kSlotSing, kSlotPv,
     kSlotPi, kSlotTk, kSlotCoop, kSlotLinv, kSlotUinv, kSlotSolve, kSlotPackA, kSlotPackB, kSlotOmega, kSlotX,
-    kSlotZ, kSlotXinv, kSlotXpack, kSlotTbuf, kSlotDvec, kSlotFlow, kSlotResPart,
+    kSlotZ, kSlotXinv, kSlotXpack, kSlotTbuf, kSlotDvec, kSlotFlow, kSlotResPart, kSlotSparseT, kSlotSparseY,
     // the persistent batched solve (fh_batch_sweep, mixed), in the first system's pool
     kSlotBatchSys, kSlotBatchOne, kSlotBatchItems, kSlotBatchZ, kSlotBatchStatus, kSlotBatchCounter, kSlotBatchWork
 };
@@ -451,6 +459,20 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
     }
     PBuf<unsigned char> res_part;
     if (const size_t rb = residual_scratch_bytes(m, p, count)) FHB_PALLOC(pool, res_part, kSlotResPart, rb);
+    PBuf<double> sp_t, sp_y;
+    FHB_PALLOC(pool, sp_t, kSlotSparseT, (size_t)std::max<int64_t>(1, 2 * count * p * s->n));
+    FHB_PALLOC(pool, sp_y, kSlotSparseY, (size_t)std::max<int64_t>(1, 2 * count * p * m));
+    SparseR sparse_r;
+    sparse_r.row_ptr = s->d_rp;
+    sparse_r.branch = s->d_br;
+    sparse_r.sign = s->d_sign;
+    sparse_r.t_off = s->d_toff;
+    sparse_r.t_loop = s->d_tloop;
+    sparse_r.t_sign = s->d_tsign;
+    sparse_r.R = s->d_R;
+    sparse_r.n = s->n;
+    sparse_r.t = sp_t.p;
+    sparse_r.y = sp_y.p;
     std::vector<double> hb(count), hd(count), hx(count), hr(count), prev(count, INFINITY);
     std::vector<int> done(count, 0), grow(count, 0);
     FHB_CUDA(cudaMemcpyAsync(hb.data(), bnorm.p, 8 * count, cudaMemcpyDeviceToHost, st));
@@ -469,7 +491,9 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
                 e = lu_solve<float>(b, d32.p, (int)p, kNbFp32, st, err, outer);
         }
         if (!e) e = add_c32_to_c64(d_x, d32.p, count * vec, st, err, m, mo);
-        if (!e) e = residual_fp64(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, r.p, rnorm.p, st, err, res_part.p);
+        if (!e)
+            e = residual_fp64(s->d_Rm, s->d_Lm, ld, m, p, d_omega, count, d_x, r.p, rnorm.p, st, err, res_part.p,
+                              &sparse_r);
         if (e) return e;
         // correction and solution norms (max-abs) for the stopping rule
         e = max_abs_per_matrix_f32(d32.p, 2 * vec32, count, dnorm.p, st, err);
@@ -866,25 +890,36 @@ fh_status fh_system_create_coupled(const fh_node *nodes, size_t n_nodes, const f
     std::vector<DevFil> h(n);
     for (int64_t i = 0; i < n; ++i) h[i] = make_devfil(s->disc.filaments[i]);
     DBuf<DevFil> d_fil(cs);
-    DBuf<double> d_L(cs), d_R(cs), d_sign(cs);
-    DBuf<int64_t> d_rp(cs);
-    DBuf<int32_t> d_br(cs);
+    DBuf<double> d_L(cs);
     FHB_ALLOC(d_fil, (size_t)n);
     FHB_ALLOC(d_L, (size_t)n * n);
-    FHB_ALLOC(d_R, (size_t)n);
-    FHB_ALLOC(d_rp, s->loops.row_ptr.size());
-    FHB_ALLOC(d_br, s->loops.branch.size());
-    FHB_ALLOC(d_sign, s->loops.sign.size());
+    TransposedLoops internal;
+    transpose_loops(s->loops, n, s->m, internal);
+    {
+        auto keep = [&](void **d, size_t bytes) { return cache_alloc(d, std::max<size_t>(bytes, 16), cs); };
+        if (keep((void **)&s->d_R, 8 * (size_t)n) || keep((void **)&s->d_rp, 8 * s->loops.row_ptr.size()) ||
+            keep((void **)&s->d_br, 4 * s->loops.branch.size()) || keep((void **)&s->d_sign, 8 * s->loops.sign.size()) ||
+            keep((void **)&s->d_toff, 8 * internal.offset.size()) || keep((void **)&s->d_tloop, 4 * internal.loop.size()) ||
+            keep((void **)&s->d_tsign, 8 * internal.sign.size())) {
+            cudaGetLastError();
+            return fail(err, FH_ERR_OUT_OF_MEMORY, "device allocation of the loop basis failed");
+        }
+    }
     if (cache_alloc((void **)&s->d_Lm, std::max<size_t>(1, (size_t)loops * loops) * 8, cs) != cudaSuccess ||
         cache_alloc((void **)&s->d_Rm, std::max<size_t>(1, (size_t)loops * loops) * 8, cs) != cudaSuccess) {
         cudaGetLastError();
         return fail(err, FH_ERR_OUT_OF_MEMORY, "device allocation of the mesh matrices failed");
     }
     FHB_CUDA(cudaMemcpyAsync(d_fil.p, h.data(), n * sizeof(DevFil), cudaMemcpyHostToDevice, cs));
-    FHB_CUDA(cudaMemcpyAsync(d_R.p, s->resistances.data(), n * 8, cudaMemcpyHostToDevice, cs));
-    FHB_CUDA(cudaMemcpyAsync(d_rp.p, s->loops.row_ptr.data(), s->loops.row_ptr.size() * 8, cudaMemcpyHostToDevice, cs));
-    FHB_CUDA(cudaMemcpyAsync(d_br.p, s->loops.branch.data(), s->loops.branch.size() * 4, cudaMemcpyHostToDevice, cs));
-    FHB_CUDA(cudaMemcpyAsync(d_sign.p, s->loops.sign.data(), s->loops.sign.size() * 8, cudaMemcpyHostToDevice, cs));
+    FHB_CUDA(cudaMemcpyAsync(s->d_R, s->resistances.data(), n * 8, cudaMemcpyHostToDevice, cs));
+    FHB_CUDA(cudaMemcpyAsync(s->d_rp, s->loops.row_ptr.data(), s->loops.row_ptr.size() * 8, cudaMemcpyHostToDevice, cs));
+    FHB_CUDA(cudaMemcpyAsync(s->d_br, s->loops.branch.data(), s->loops.branch.size() * 4, cudaMemcpyHostToDevice, cs));
+    FHB_CUDA(cudaMemcpyAsync(s->d_sign, s->loops.sign.data(), s->loops.sign.size() * 8, cudaMemcpyHostToDevice, cs));
+    FHB_CUDA(cudaMemcpyAsync(s->d_toff, internal.offset.data(), internal.offset.size() * 8, cudaMemcpyHostToDevice, cs));
+    if (!internal.loop.empty()) {
+        FHB_CUDA(cudaMemcpyAsync(s->d_tloop, internal.loop.data(), internal.loop.size() * 4, cudaMemcpyHostToDevice, cs));
+        FHB_CUDA(cudaMemcpyAsync(s->d_tsign, internal.sign.data(), internal.sign.size() * 8, cudaMemcpyHostToDevice, cs));
+    }
     FHB_CUDA(cudaMemsetAsync(d_L.p, 0, (size_t)n * n * 8, cs));
     s->total_pairs = n * (n + 1) / 2;
     s->kept_pairs = coupling_kept_pairs(s->coupling, s->disc.per_segment.data(), n_segments);
@@ -911,7 +946,7 @@ fh_status fh_system_create_coupled(const fh_node *nodes, size_t n_nodes, const f
     ScopedEvents<2> cev;
     cudaEvent_t c0 = cev.e[0], c1 = cev.e[1];
     cudaEventRecord(c0, cs);
-    st = device_congruence(d_L.p, d_R.p, n, d_rp.p, d_br.p, d_sign.p, loops, s->loops.row_ptr.data(), s->d_Lm,
+    st = device_congruence(d_L.p, s->d_R, n, s->d_rp, s->d_br, s->d_sign, loops, s->loops.row_ptr.data(), s->d_Lm,
                            s->d_Rm, cs, err);
     cudaEventRecord(c1, cs);
     if (st) return st;

@@ -1058,12 +1058,16 @@ __global__ void rhs_kernel(const double *__restrict__ R, const double *__restric
 // then adds the ranges in order, so the result does not depend on the
 // schedule.  The split keeps every SM busy when the row tiles alone are few
 // or uneven across the SMs.
+// kDenseR false: R x comes precomputed in rx (the loop-basis product) and the
+// pass reads L alone.
 constexpr int kResRows = 32, kResCols = 32, kResK = 16, kResThreads = 128, kResMaxSplits = 16;
+template <bool kDenseR>
 __global__ void __launch_bounds__(kResThreads) residual_kernel(const double *__restrict__ R,
                                                                const double *__restrict__ L, int64_t ld, int64_t m,
                                                                int64_t p, const double *__restrict__ omega, int count,
                                                                const Cx<double> *__restrict__ x,
-                                                               Cx<double> *__restrict__ r, double4 *__restrict__ part) {
+                                                               Cx<double> *__restrict__ r, double4 *__restrict__ part,
+                                                               const Cx<double> *__restrict__ rx) {
     __shared__ double Rs[2][kResK][kResRows], Ls[2][kResK][kResRows];
     __shared__ Cx<double> Xs[2][kResK][kResCols + 1];  // padded: the stores run down k
     const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
@@ -1078,7 +1082,7 @@ __global__ void __launch_bounds__(kResThreads) residual_kernel(const double *__r
             const int row = idx & 31, k = idx >> 5;
             const int64_t i = i0 + row, kk = k0 + k;
             const bool in = i < m && kk < m;
-            rv[e] = in ? R[i + kk * ld] : 0.0;
+            if (kDenseR) rv[e] = in ? R[i + kk * ld] : 0.0;
             lv[e] = in ? L[i + kk * ld] : 0.0;
             const int kx = idx & 15, g = idx >> 4;
             const int64_t kkx = k0 + kx;
@@ -1089,7 +1093,7 @@ __global__ void __launch_bounds__(kResThreads) residual_kernel(const double *__r
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
             const int idx = tid + kResThreads * e;
-            Rs[b][idx >> 5][idx & 31] = rv[e];
+            if (kDenseR) Rs[b][idx >> 5][idx & 31] = rv[e];
             Ls[b][idx >> 5][idx & 31] = lv[e];
             Xs[b][idx & 15][idx >> 4] = xv[e];
         }
@@ -1113,7 +1117,7 @@ __global__ void __launch_bounds__(kResThreads) residual_kernel(const double *__r
             Cx<double> xk[2];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                rk[i] = Rs[b][k][tx + 8 * i];
+                rk[i] = kDenseR ? Rs[b][k][tx + 8 * i] : 0.0;
                 lk[i] = Ls[b][k][tx + 8 * i];
             }
 #pragma unroll
@@ -1122,8 +1126,10 @@ __global__ void __launch_bounds__(kResThreads) residual_kernel(const double *__r
             for (int i = 0; i < 4; ++i)
 #pragma unroll
                 for (int j = 0; j < 2; ++j) {
-                    ar[i][j].re += rk[i] * xk[j].re;
-                    ar[i][j].im += rk[i] * xk[j].im;
+                    if (kDenseR) {
+                        ar[i][j].re += rk[i] * xk[j].re;
+                        ar[i][j].im += rk[i] * xk[j].im;
+                    }
                     al[i][j].re += lk[i] * xk[j].re;
                     al[i][j].im += lk[i] * xk[j].im;
                 }
@@ -1159,8 +1165,9 @@ __global__ void __launch_bounds__(kResThreads) residual_kernel(const double *__r
             if (row >= m) continue;
             const double br = R[row + (m + q) * ld], bl = L[row + (m + q) * ld];
             // (R + jwL) x = R x + j w (L x)
-            const double ax_re = ar[i][j].re - w * al[i][j].im;
-            const double ax_im = ar[i][j].im + w * al[i][j].re;
+            const Cx<double> rxv = kDenseR ? ar[i][j] : rx[g * m + row];
+            const double ax_re = rxv.re - w * al[i][j].im;
+            const double ax_im = rxv.im + w * al[i][j].re;
             r[g * m + row] = Cx<double>{br - ax_re, w * bl - ax_im};
         }
     }
@@ -1170,7 +1177,8 @@ __global__ void __launch_bounds__(kResThreads) residual_kernel(const double *__r
 // then r as in residual_kernel.
 __global__ void residual_finish_kernel(const double *__restrict__ R, const double *__restrict__ L, int64_t ld,
                                        int64_t m, int64_t p, const double *__restrict__ omega, int count, int splits,
-                                       const double4 *__restrict__ part, Cx<double> *__restrict__ r) {
+                                       const double4 *__restrict__ part, Cx<double> *__restrict__ r,
+                                       const Cx<double> *__restrict__ rx) {
     const int64_t G = (int64_t)count * p, total = G * m;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t g = t / m, row = t % m;
@@ -1186,6 +1194,10 @@ __global__ void residual_finish_kernel(const double *__restrict__ R, const doubl
         const int64_t q = g % p;
         const double w = omega[f];
         const double br = R[row + (m + q) * ld], bl = L[row + (m + q) * ld];
+        if (rx) {  // R x from the loop basis (the split sums hold zeros there)
+            a.x = rx[t].re;
+            a.y = rx[t].im;
+        }
         const double ax_re = a.x - w * a.w, ax_im = a.y + w * a.z;
         r[t] = Cx<double>{br - ax_re, w * bl - ax_im};
     }
@@ -1702,6 +1714,40 @@ fh_status form_rhs(const double *Rm, const double *Lm, int64_t ld, int64_t m, in
     return FH_OK;
 }
 
+// t[g n + b] = R_b sum over the internal loops of branch b of s x[g m + loop].
+__global__ void sparse_rt_kernel(const Cx<double> *__restrict__ x, int64_t m, int64_t n, int64_t G,
+                                 const int64_t *__restrict__ t_off, const int32_t *__restrict__ t_loop,
+                                 const double *__restrict__ t_sign, const double *__restrict__ R,
+                                 Cx<double> *__restrict__ t) {
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < G * n;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t g = idx / n, b = idx % n;
+        double re = 0.0, im = 0.0;
+        for (int64_t e = t_off[b]; e < t_off[b + 1]; ++e) {
+            const Cx<double> v = x[g * m + t_loop[e]];
+            re += t_sign[e] * v.re;
+            im += t_sign[e] * v.im;
+        }
+        t[idx] = Cx<double>{R[b] * re, R[b] * im};
+    }
+}
+// y[g m + i] = sum over the branches of loop i of s t[g n + branch].
+__global__ void sparse_ry_kernel(const Cx<double> *__restrict__ t, int64_t m, int64_t n, int64_t G,
+                                 const int64_t *__restrict__ row_ptr, const int32_t *__restrict__ branch,
+                                 const double *__restrict__ sign, Cx<double> *__restrict__ y) {
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < G * m;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t g = idx / m, i = idx % m;
+        double re = 0.0, im = 0.0;
+        for (int64_t e = row_ptr[i]; e < row_ptr[i + 1]; ++e) {
+            const Cx<double> v = t[g * n + branch[e]];
+            re += sign[e] * v.re;
+            im += sign[e] * v.im;
+        }
+        y[idx] = Cx<double>{re, im};
+    }
+}
+
 int residual_splits(int64_t m, int64_t p, int count) {
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
@@ -1722,20 +1768,36 @@ size_t residual_scratch_bytes(int64_t m, int64_t p, int count) {
 
 fh_status residual_fp64(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega,
                         int count, const double *x, double *r, double *rnorm, cudaStream_t s, fh_error_info *err,
-                        void *scratch) {
+                        void *scratch, const SparseR *sr) {
     if (m == 0) return FH_OK;
     const int64_t cols = (int64_t)count * p;
     const int splits = scratch ? residual_splits(m, p, count) : 1;
     double4 *part = splits > 1 ? static_cast<double4 *>(scratch) : nullptr;
     prof_begin(s, FH_PROF_RESIDUAL);
-    residual_kernel<<<dim3((unsigned)((m + kResRows - 1) / kResRows), (unsigned)((cols + kResCols - 1) / kResCols),
-                           (unsigned)(part ? splits : 1)),
-                      kResThreads, 0, s>>>(Rm, Lm, ld, m, p, omega, count, reinterpret_cast<const Cx<double> *>(x),
-                                           reinterpret_cast<Cx<double> *>(r), part);
+    const Cx<double> *rx = nullptr;
+    if (sr) {
+        Cx<double> *t = reinterpret_cast<Cx<double> *>(sr->t), *y = reinterpret_cast<Cx<double> *>(sr->y);
+        sparse_rt_kernel<<<grid_for(cols * sr->n, 256), 256, 0, s>>>(reinterpret_cast<const Cx<double> *>(x), m,
+                                                                     sr->n, cols, sr->t_off, sr->t_loop, sr->t_sign,
+                                                                     sr->R, t);
+        sparse_ry_kernel<<<grid_for(cols * m, 256), 256, 0, s>>>(t, m, sr->n, cols, sr->row_ptr, sr->branch, sr->sign,
+                                                                 y);
+        rx = y;
+    }
+    const dim3 rgrid((unsigned)((m + kResRows - 1) / kResRows), (unsigned)((cols + kResCols - 1) / kResCols),
+                     (unsigned)(part ? splits : 1));
+    if (rx)
+        residual_kernel<false><<<rgrid, kResThreads, 0, s>>>(Rm, Lm, ld, m, p, omega, count,
+                                                             reinterpret_cast<const Cx<double> *>(x),
+                                                             reinterpret_cast<Cx<double> *>(r), part, rx);
+    else
+        residual_kernel<true><<<rgrid, kResThreads, 0, s>>>(Rm, Lm, ld, m, p, omega, count,
+                                                            reinterpret_cast<const Cx<double> *>(x),
+                                                            reinterpret_cast<Cx<double> *>(r), part, nullptr);
     if (part)
         residual_finish_kernel<<<grid_for(cols * m, 256), 256, 0, s>>>(Rm, Lm, ld, m, p, omega, count, splits, part,
-                                                                      reinterpret_cast<Cx<double> *>(r));
-    prof_end(s, FH_PROF_RESIDUAL, 16.0 * (double)m * (double)m);  // bytes: R and L read once
+                                                                      reinterpret_cast<Cx<double> *>(r), rx);
+    prof_end(s, FH_PROF_RESIDUAL, (sr ? 8.0 : 16.0) * (double)m * (double)m);  // bytes: L (and R) read once
     FHB_CUDA(cudaGetLastError());
     if (rnorm) {
         max_abs_kernel<double><<<count, 256, 0, s>>>(r, 2 * m * p, rnorm);

@@ -226,9 +226,28 @@ fh_status form_rhs(const double *Rm, const double *Lm, int64_t ld, int64_t m, in
 // With scratch (residual_scratch_bytes; 0 means none is used) the k range is
 // split across CTAs and the ranges' sums are added in a fixed order.
 size_t residual_scratch_bytes(int64_t m, int64_t p, int count);
+// R_ee through the loop basis, R_ee = M_e diag(R) M_e^T: y = M_e (R (M_e^T x))
+// costs O(loop entries) per column instead of the m^2 of the dense R_ee.
+// row_ptr / branch / sign: the basis rows (the first m used); t_off /
+// t_loop / t_sign: per branch (n + 1 offsets) its internal loops in
+// increasing order; R: branch resistances; t (G x n) and y (G x m complex)
+// scratch, G = count p.
+struct SparseR {
+    const int64_t *row_ptr = nullptr;
+    const int32_t *branch = nullptr;
+    const double *sign = nullptr;
+    const int64_t *t_off = nullptr;
+    const int32_t *t_loop = nullptr;
+    const double *t_sign = nullptr;
+    const double *R = nullptr;
+    int64_t n = 0;
+    double *t = nullptr;
+    double *y = nullptr;
+};
+// With sr, R_ee x comes from the loop basis and the dense pass reads L_ee only.
 fh_status residual_fp64(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega,
                         int count, const double *x, double *r, double *rnorm, cudaStream_t s, fh_error_info *err,
-                        void *scratch = nullptr);
+                        void *scratch = nullptr, const SparseR *sr = nullptr);
 
 // Z_f = Z_pp - Z_ep^T X_f (p x p complex, row-major per frequency).
 fh_status schur(const double *Rm, const double *Lm, int64_t ld, int64_t m, int64_t p, const double *omega, int count,

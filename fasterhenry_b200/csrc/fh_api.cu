@@ -70,6 +70,9 @@ struct fh_system {
     int64_t n = 0, nloops = 0, m = 0, p = 0;
     int device = 0;
     cudaStream_t stream = nullptr;
+    // The factorization's look-ahead stream, joined to `stream` before each
+    // factorization returns.
+    cudaStream_t side = nullptr;
     double *d_Lm = nullptr, *d_Rm = nullptr;
     // Layout (currents.rs:128-170) and, once currents are asked for, the
     // transposed loop basis and per-filament (w, h, R) on the device.
@@ -117,6 +120,10 @@ struct fh_system {
         cache_free(d_whr, stream);
         cache_free(d_group, stream);
         cache_free(d_coupled, stream);
+        if (side) {
+            cudaStreamSynchronize(side);
+            cudaStreamDestroy(side);
+        }
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -194,6 +201,7 @@ enum PoolSlot {
     kSlotA, kSlotD32, kSlotR, kSlotRnorm, kSlotBnorm, kSlotDnorm, kSlotXnorm, kSlotPiv, kSlotSing, kSlotPv,
     kSlotPi, kSlotTk, kSlotCoop, kSlotLinv, kSlotUinv, kSlotSolve, kSlotPackA, kSlotPackB, kSlotOmega, kSlotX,
     kSlotZ, kSlotXinv, kSlotXpack, kSlotTbuf, kSlotDvec, kSlotFlow, kSlotResPart, kSlotSparseT, kSlotSparseY,
+    kSlotTileCounter,
     // the persistent batched solve (fh_batch_sweep, mixed), in the first system's pool
     kSlotBatchSys, kSlotBatchOne, kSlotBatchItems, kSlotBatchZ, kSlotBatchStatus, kSlotBatchCounter, kSlotBatchWork
 };
@@ -414,6 +422,7 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
         }
     }
     PBuf<unsigned char> pack_a, pack_b, xpack;
+    PBuf<int> tile_counter;
     PBuf<float> xinv, tbuf, dvec;
     if (outer) {
         const size_t pb = packed_operand_bytes(mo - outer, outer, count);
@@ -425,6 +434,11 @@ fh_status sweep_chunk_mixed(fh_system *s, const double *d_omega, int count, doub
         if (!(panel_solve_supported(mo) && (int64_t)count * mo <= INT32_MAX)) {
             FHB_PALLOC(pool, pack_b, kSlotPackB, pb);
             w.pack_b = pack_b.p;
+        } else if (s->side) {
+            // look-ahead of the fused form: the deep update's shared tile counter
+            FHB_PALLOC(pool, tile_counter, kSlotTileCounter, 1);
+            w.side = s->side;
+            w.tile_counter = tile_counter.p;
         }
         // Z_ee = R_ee + jw L_ee with R_ee, L_ee symmetric positive definite:
         // the FP32 factors go without pivoting (stable for this class; the
@@ -879,6 +893,9 @@ fh_status fh_system_create_coupled(const fh_node *nodes, size_t n_nodes, const f
     if (st) return st;
     FHB_CUDA(cudaGetDevice(&s->device));
     FHB_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    // Default priority: the look-ahead gets its SMs by the update leaving
+    // them free, not by scheduling ahead of queued update CTAs.
+    FHB_CUDA(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
     cudaStream_t cs = s->stream;
     s->pool.stream = cs;
     s->nloops = s->loops.rows();

@@ -59,7 +59,8 @@ constexpr int kAccCols = 2 * kTile;  // Re (columns 0..127) + Im (128..255)
 constexpr int kTmemCols = 2 * kAccCols;
 constexpr int kEpiWarps = 8;
 constexpr int kThreads = 32 * (2 + kEpiWarps);
-constexpr int kBarBytes = 256;
+constexpr int kRing = 8;  // tile numbers in flight from the producer to the MMA and epilogue warps
+constexpr int kBarBytes = 512;
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 + kBarBytes;
 constexpr int kGroupRows = 16;  // row blocks per raster group (L2 working set)
 constexpr long long kSpinLimit = 1LL << 24;
@@ -225,6 +226,10 @@ struct PackedArgs {
     // per_matrix tiles, packed rb | cb << 16, in schedule order.
     const uint32_t *table;
     long long per_matrix;
+    // With a tile counter the CTAs draw tiles from it (atomicAdd) instead of
+    // taking every gridDim.x-th: two grids on different streams then share
+    // one update, each CTA running until the counter passes the last tile.
+    int *next;
 };
 
 // Tile t -> (matrix, row block, column block).  Within a matrix, groups of
@@ -258,7 +263,14 @@ __global__ void __launch_bounds__(kThreads, 1) packed_update_kernel(PackedArgs g
     uint64_t *tfull = bars + 2 * kStages;      // [2]
     uint64_t *tempty = bars + 2 * kStages + 2; // [2]
     uint64_t *drain = bars + 2 * kStages + 4;  // [1]
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 5);
+    // Drawn tiles (with a tile counter): ring slot n % kRing holds the CTA's
+    // n-th tile (-1: none left); idfull[slot] completes when the producer has
+    // written it, idempty[slot] when the MMA warp and every epilogue warp
+    // have read it.
+    uint64_t *idfull = bars + 2 * kStages + 5;           // [kRing]
+    uint64_t *idempty = bars + 2 * kStages + 5 + kRing;  // [kRing]
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 5 + 2 * kRing);
+    volatile int *ring = reinterpret_cast<volatile int *>(tmem_slot + 2);  // [kRing]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp == 1) {
@@ -276,6 +288,10 @@ __global__ void __launch_bounds__(kThreads, 1) packed_update_kernel(PackedArgs g
             mbar_init(smem_u32(&tempty[b]), kEpiWarps);
         }
         mbar_init(smem_u32(drain), 1);
+        for (int r = 0; r < kRing; ++r) {
+            mbar_init(smem_u32(&idfull[r]), 1);
+            mbar_init(smem_u32(&idempty[r]), 1 + kEpiWarps);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
@@ -283,6 +299,31 @@ __global__ void __launch_bounds__(kThreads, 1) packed_update_kernel(PackedArgs g
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     bool ok = true;
+    // The n-th tile of a consumer (the MMA thread, or a whole epilogue warp
+    // through its lane 0): -1 when none is left or a wait for the
+    // producer's draw ran out (ok cleared).
+    auto consumer_tile = [&](uint32_t n, bool warp_wide) -> long long {
+        if (!g.next) {
+            const long long t = blockIdx.x + (long long)n * gridDim.x;
+            return t < g.tiles ? t : -1;
+        }
+        long long t = -1;
+        int good = 1;
+        if (!warp_wide || lane == 0) {
+            const uint32_t slot = n % kRing, parity = (n / kRing) & 1u;
+            good = mbar_wait(smem_u32(&idfull[slot]), parity) ? 1 : 0;
+            if (good) {
+                t = ring[slot];
+                mbar_arrive(smem_u32(&idempty[slot]));
+            }
+        }
+        if (warp_wide) {
+            t = __shfl_sync(0xffffffffu, t, 0);
+            good = __shfl_sync(0xffffffffu, good, 0);
+        }
+        if (!good) ok = false;
+        return t;
+    };
 
     if (warp == 0) {
         if (lane == 0) {
@@ -290,7 +331,23 @@ __global__ void __launch_bounds__(kThreads, 1) packed_update_kernel(PackedArgs g
             int stage = 0;
             uint32_t phase = 0;
             uint32_t issued = 0, last_phase = 0;  // per-stage bits: ever issued, phase of the last issue
-            for (long long t = blockIdx.x; t < g.tiles && ok; t += gridDim.x) {
+            for (uint32_t n = 0; ok; ++n) {
+                long long t;
+                if (g.next) {
+                    const uint32_t slot = n % kRing, parity = (n / kRing) & 1u;
+                    if (!mbar_wait(smem_u32(&idempty[slot]), parity ^ 1u)) {
+                        ok = false;
+                        break;
+                    }
+                    const int d = atomicAdd(g.next, 1);
+                    t = d < g.tiles ? d : -1;
+                    ring[slot] = (int)t;
+                    mbar_arrive(smem_u32(&idfull[slot]));
+                } else {
+                    t = blockIdx.x + (long long)n * gridDim.x;
+                    if (t >= g.tiles) t = -1;
+                }
+                if (t < 0) break;
                 int f, rb, cb;
                 tile_coords(g, t, f, rb, cb);
                 const uint8_t *a_src = g.Ap + (((int64_t)f * g.rblocks + rb) * g.nchunks) * kOpBytes;
@@ -328,7 +385,8 @@ __global__ void __launch_bounds__(kThreads, 1) packed_update_kernel(PackedArgs g
             uint32_t n_tile = 0;
             bool issued = false;
             const uint32_t pos = instr_desc(false), neg = instr_desc(true);
-            for (long long t = blockIdx.x; t < g.tiles && ok; t += gridDim.x, ++n_tile) {
+            for (;; ++n_tile) {
+                if (consumer_tile(n_tile, false) < 0) break;
                 const uint32_t buf = n_tile & 1u, use = n_tile >> 1;
                 if (!mbar_wait(smem_u32(&tempty[buf]), (use & 1u) ^ 1u)) {
                     ok = false;
@@ -383,8 +441,9 @@ __global__ void __launch_bounds__(kThreads, 1) packed_update_kernel(PackedArgs g
         const int quarter = warp & 3;        // TMEM lanes 32*quarter.. (hardware: warp id % 4)
         const int half = (warp - 2) >> 2;    // column half of the tile
         const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
-        uint32_t n_tile = 0;
-        for (long long t = blockIdx.x; t < g.tiles; t += gridDim.x, ++n_tile) {
+        for (uint32_t n_tile = 0;; ++n_tile) {
+            const long long t = consumer_tile(n_tile, true);
+            if (t < 0) break;
             const uint32_t buf = n_tile & 1u, use = n_tile >> 1;
             int f, rb, cb;
             tile_coords(g, t, f, rb, cb);
@@ -824,70 +883,121 @@ fh_status packed_init(int *dev_out, fh_error_info *err) {
 }
 }  // namespace
 
-fh_status gemm_tc_packed_run(const void *pack_a, const void *pack_b, float *C, int64_t ldc, int64_t sC, int64_t M,
-                             int64_t N, int K, int count, cudaStream_t s, fh_error_info *err, int lower_from) {
+fh_status gemm_tc_packed_schedule(PackedSchedule &ps, const void *pack_a, const void *pack_b, float *C, int64_t ldc,
+                                  int64_t sC, int64_t M, int64_t N, int K, int count, int lower_from, int col_lo,
+                                  int col_hi, cudaStream_t s, fh_error_info *err) {
+    ps = PackedSchedule{};
     if (K % kChunk || K <= 0) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update needs K a positive multiple of 16");
     if (M <= 0 || N <= 0 || count <= 0) return FH_OK;
     if (!pack_a || !pack_b) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update needs packed operands");
     int dev = 0;
     fh_status st = packed_init(&dev, err);
     if (st) return st;
-    const int nchunks = K / kChunk;
     const int rblocks = (int)((M + kTile - 1) / kTile), cblocks = (int)((N + kTile - 1) / kTile);
-    PackedArgs g;
-    g.Ap = reinterpret_cast<const uint8_t *>(pack_a);
-    g.Bp = reinterpret_cast<const uint8_t *>(pack_b);
-    g.C = reinterpret_cast<float2 *>(C);
-    g.ldc = ldc;
-    g.sC = sC;
-    g.M = M;
-    g.N = N;
-    g.rblocks = rblocks;
-    g.cblocks = cblocks;
-    g.nchunks = nchunks;
-    g.table = nullptr;
-    g.per_matrix = (long long)rblocks * cblocks;
-    double entries = (double)M * (double)N;  // complex C entries updated per matrix
-    uint32_t *d_table = nullptr;
-    if (lower_from >= 0 && lower_from < cblocks) {
+    if (col_hi < 0 || col_hi > cblocks) col_hi = cblocks;
+    col_lo = std::max(0, col_lo);
+    if (col_lo >= col_hi) return FH_OK;
+    ps.pack_a = pack_a;
+    ps.pack_b = pack_b;
+    ps.C = C;
+    ps.ldc = ldc;
+    ps.sC = sC;
+    ps.M = M;
+    ps.N = N;
+    ps.K = K;
+    ps.count = count;
+    ps.per_matrix = (long long)rblocks * cblocks;
+    ps.entries = (double)M * (double)N;  // complex C entries updated per matrix
+    const bool ranged = col_lo > 0 || col_hi < cblocks;
+    if ((lower_from >= 0 && lower_from < cblocks) || ranged) {
+        if (lower_from < 0 || lower_from > cblocks) lower_from = cblocks;  // a range of full column blocks
         // Lower-triangle form (symmetric trailing matrix, C rows and columns
         // on the same blocks): column blocks below lower_from in full, the
         // rest only on and below the diagonal block (lower_from = 0: the
-        // lower triangle of tiles); the same grouped order as the full
-        // schedule (row blocks fastest inside groups of kGroupRows), the
-        // other tiles left out.
+        // lower triangle of tiles), over the column blocks [col_lo, col_hi);
+        // the same grouped order as the full schedule (row blocks fastest
+        // inside groups of kGroupRows), the other tiles left out.
+        if (rblocks > 0xffff || cblocks > 0xffff)
+            return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update tile table overflow");
         std::vector<uint32_t> table;
-        table.reserve((size_t)rblocks * cblocks);
-        entries = 0.0;
+        table.reserve((size_t)rblocks * (col_hi - col_lo));
+        ps.entries = 0.0;
         for (int g0 = 0; g0 < rblocks; g0 += kGroupRows) {
             const int rows = std::min(kGroupRows, rblocks - g0);
-            for (int cb = 0; cb < cblocks; ++cb)
+            for (int cb = col_lo; cb < col_hi; ++cb)
                 for (int r = 0; r < rows; ++r) {
                     const int rb = g0 + r;
                     if (cb < lower_from || rb >= cb) {
                         table.push_back((uint32_t)rb | ((uint32_t)cb << 16));
-                        entries += (double)std::min<int64_t>(kTile, M - (int64_t)rb * kTile) *
-                                   (double)std::min<int64_t>(kTile, N - (int64_t)cb * kTile);
+                        ps.entries += (double)std::min<int64_t>(kTile, M - (int64_t)rb * kTile) *
+                                      (double)std::min<int64_t>(kTile, N - (int64_t)cb * kTile);
                     }
                 }
         }
-        if (rblocks > 0xffff || cblocks > 0xffff)
-            return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update tile table overflow");
-        FHB_CUDA(cache_alloc((void **)&d_table, table.size() * 4, s));
-        FHB_CUDA(cudaMemcpyAsync(d_table, table.data(), table.size() * 4, cudaMemcpyHostToDevice, s));
-        g.table = d_table;
-        g.per_matrix = (long long)table.size();
+        ps.per_matrix = (long long)table.size();
+        if (table.empty()) return FH_OK;
+        FHB_CUDA(cache_alloc((void **)&ps.table, table.size() * 4, s));
+        FHB_CUDA(cudaMemcpyAsync(ps.table, table.data(), table.size() * 4, cudaMemcpyHostToDevice, s));
     }
-    g.tiles = (long long)count * g.per_matrix;
-    const int grid = (int)std::min<long long>(g.tiles, (long long)std::max(1, g_sms[dev]));
-    const bool prof = prof_on();
+    ps.tiles = (long long)count * ps.per_matrix;
+    return FH_OK;
+}
+
+fh_status gemm_tc_packed_launch(const PackedSchedule &ps, int grid, int *next, cudaStream_t s, fh_error_info *err,
+                                bool profiled) {
+    if (ps.tiles <= 0) return FH_OK;
+    if (next && ps.tiles > INT32_MAX) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update tile counter overflow");
+    int dev = 0;
+    fh_status st = packed_init(&dev, err);
+    if (st) return st;
+    const int rblocks = (int)((ps.M + kTile - 1) / kTile), cblocks = (int)((ps.N + kTile - 1) / kTile);
+    PackedArgs g;
+    g.Ap = reinterpret_cast<const uint8_t *>(ps.pack_a);
+    g.Bp = reinterpret_cast<const uint8_t *>(ps.pack_b);
+    g.C = reinterpret_cast<float2 *>(ps.C);
+    g.ldc = ps.ldc;
+    g.sC = ps.sC;
+    g.M = ps.M;
+    g.N = ps.N;
+    g.rblocks = rblocks;
+    g.cblocks = cblocks;
+    g.nchunks = ps.K / kChunk;
+    g.tiles = ps.tiles;
+    g.table = ps.table;
+    g.per_matrix = ps.per_matrix;
+    g.next = next;
+    if (grid <= 0) grid = std::max(1, g_sms[dev]);
+    grid = (int)std::min<long long>(ps.tiles, grid);
+    const bool prof = profiled && prof_on();
     if (prof) prof_begin(s, FH_PROF_GEMM_TC);
     packed_update_kernel<<<grid, kThreads, kSmemBytes, s>>>(g, g_flag[dev]);
-    if (prof) prof_end(s, FH_PROF_GEMM_TC, 8.0 * entries * (double)K * count);
-    cudaError_t le = cudaGetLastError();
-    if (d_table) cache_free(d_table, s);  // stream-ordered: after the kernel
+    if (prof) prof_end(s, FH_PROF_GEMM_TC, 8.0 * ps.entries * (double)ps.K * ps.count);
+    const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) return fail(err, FH_ERR_CUDA, std::string("packed update launch failed: ") + cudaGetErrorString(le));
     return FH_OK;
+}
+
+void gemm_tc_packed_release(PackedSchedule &ps, cudaStream_t s) {
+    if (ps.table) cache_free(ps.table, s);  // stream-ordered: after the launches before it on s
+    ps.table = nullptr;
+    ps.tiles = 0;
+}
+
+int gemm_tc_sm_count() {
+    int dev = 0;
+    if (packed_init(&dev, nullptr)) return 1;
+    return std::max(1, g_sms[dev]);
+}
+
+fh_status gemm_tc_packed_run(const void *pack_a, const void *pack_b, float *C, int64_t ldc, int64_t sC, int64_t M,
+                             int64_t N, int K, int count, cudaStream_t s, fh_error_info *err, int lower_from, int col_lo,
+                             int col_hi) {
+    PackedSchedule ps;
+    fh_status st = gemm_tc_packed_schedule(ps, pack_a, pack_b, C, ldc, sC, M, N, K, count, lower_from, col_lo, col_hi, s,
+                                           err);
+    if (!st) st = gemm_tc_packed_launch(ps, 0, nullptr, s, err);
+    gemm_tc_packed_release(ps, s);
+    return st;
 }
 
 fh_status gemm_tc_packed_update(const float *A, int64_t lda, int64_t sA, const float *B, int64_t ldb, int64_t sB,

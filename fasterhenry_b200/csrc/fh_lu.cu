@@ -1289,6 +1289,14 @@ inline int grid_for(int64_t work, int threads, int cap = 148 * 32) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(g, cap));
 }
 
+// Look-ahead sizing: SMs left to the front while the deep update runs (at
+// least one per matrix, for the one-CTA-per-matrix diagonal kernels, and at
+// most a quarter of the GPU), and the smallest second part of an update, in
+// tiles per SM, worth splitting the update for (a 128 x 128 tile at K = 512
+// takes about 19 us of an SM; a front, about 1 ms on the whole GPU).
+constexpr int kAheadMinSpare = 16;
+constexpr int kAheadMinWaves = 16;
+
 // Two-level blocked factorization of an FP32 batch on the tensor cores.
 //
 // For each super-panel [K0, E) of `outer` columns:
@@ -1354,7 +1362,52 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
     C *svec = fused ? dvec + (int64_t)count * outer : nullptr;
     // X's blocks below its diagonal are read as zeros and never written.
     if (fused) FHB_CUDA(cudaMemsetAsync(w.xinv, 0, sizeof(C) * (size_t)count * outer * outer, s));
+    // Look-ahead (fused form, with a second stream and a tile counter): the
+    // diagonal region of each super-panel, its X and the packing of X (the
+    // "front", a chain of small launches of one or two CTAs per matrix) run
+    // on `side`, overlapping the previous super-panel's deep update.  That
+    // update goes in two parts on s: first the next super-panel's column
+    // blocks on every SM (the front needs them), then the rest from the tile
+    // counter on all SMs but `spare`; when the front is done, a grid of
+    // `spare` CTAs on the side stream joins the rest from the same counter.
+    // The rows-below pass stays on s (it needs the whole GPU and the packed
+    // operand, which the update reads until it ends).  A deep update too
+    // short to hide a front runs whole, without the split.
+    const bool ahead = fused && w.side && w.tile_counter;
+    const int sms = ahead ? gemm_tc_sm_count() : 0;
+    const int spare = std::min(sms / 4, std::max(count, kAheadMinSpare));
+    cudaEvent_t ev_go = nullptr, ev_done = nullptr;  // s -> side: the front may start; side -> s: front (+ helper) done
+    PackedSchedule rest;                             // the deep update's second part, waiting for its helper grid
+    struct AheadRelease {
+        cudaEvent_t *a, *b;
+        PackedSchedule *ps;
+        cudaStream_t s;
+        ~AheadRelease() {
+            if (ps->table) gemm_tc_packed_release(*ps, s);
+            if (*a) cudaEventDestroy(*a);
+            if (*b) cudaEventDestroy(*b);
+        }
+    } ahead_release{&ev_go, &ev_done, &rest, s};
+    if (ahead) {
+        FHB_CUDA(cudaEventCreateWithFlags(&ev_go, cudaEventDisableTiming));
+        FHB_CUDA(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
+        FHB_CUDA(cudaEventRecord(ev_go, s));  // the set-up above, before the first front
+        FHB_CUDA(cudaStreamWaitEvent(w.side, ev_go, 0));
+    }
+    // After a front: the helper grid of the update it overlapped, then s waits
+    // for both.
+    auto join_front = [&]() -> fh_status {
+        if (rest.tiles > 0) {
+            const fh_status hs = gemm_tc_packed_launch(rest, spare, w.tile_counter, w.side, err, false);
+            if (hs) return hs;
+        }
+        FHB_CUDA(cudaEventRecord(ev_done, w.side));
+        FHB_CUDA(cudaStreamWaitEvent(s, ev_done, 0));
+        if (rest.tiles > 0 || rest.table) gemm_tc_packed_release(rest, s);
+        return FH_OK;
+    };
     for (int64_t K0 = 0; K0 < m; K0 += outer) {
+        const cudaStream_t sx = ahead ? w.side : s;  // the front's stream
         const int W = (int)std::min<int64_t>(outer, m - K0);
         const int64_t E = K0 + W;
         const bool below = fused && E < m;  // rows below this super-panel go to the fused pass
@@ -1364,33 +1417,33 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             const int64_t r1 = j0 + wj;  // first row / column after the panel
             C *linv = slot(w.linv, j0);
             const int64_t mstride = (int64_t)nb * nb;  // a partial last block keeps the full slot stride
-            prof_begin(s, FH_PROF_PANEL);
+            prof_begin(sx, FH_PROF_PANEL);
             if (nopivot) {
                 // LU of the diagonal block and the inverses of its L and U
                 // (with the fused pass: U^-1 also into X's diagonal block, and
                 // U's diagonal into dvec).
                 const int64_t o = j0 - K0;
-                diag_lu_kernel<<<(unsigned)count, kDiagThreads, 0, s>>>(a, m, j0, wj, below ? dvec + o : nullptr,
-                                                                       below ? svec + o : nullptr, W);
+                diag_lu_kernel<<<(unsigned)count, kDiagThreads, 0, sx>>>(a, m, j0, wj, below ? dvec + o : nullptr,
+                                                                        below ? svec + o : nullptr, W);
                 diag_inv_kernel<<<dim3((unsigned)count, 2), kDiagThreads, sizeof(C) * ((size_t)wj * wj + kDiagSmemExtra),
-                                  s>>>(a, m, j0, wj, linv, slot(w.uinv, j0), mstride, below ? xinv + o + o * W : nullptr,
+                                  sx>>>(a, m, j0, wj, linv, slot(w.uinv, j0), mstride, below ? xinv + o + o * W : nullptr,
                                        W, (int64_t)W * W);
                 st = cudaGetLastError() == cudaSuccess ? FH_OK
                                                        : fail(err, FH_ERR_CUDA, "diagonal block factorization launch failed");
             } else {
-                st = panel_coop<float>(b, j0, wj, *w.coop, s, err);
+                st = panel_coop<float>(b, j0, wj, *w.coop, sx, err);
             }
-            prof_end(s, FH_PROF_PANEL, 0.0);
+            prof_end(sx, FH_PROF_PANEL, 0.0);
             if (st) return st;
-            prof_begin(s, FH_PROF_TRSM);
+            prof_begin(sx, FH_PROF_TRSM);
             if (!nopivot) {
-                tri_inverse_kernel<float><<<inv_grid, 256, inv_smem, s>>>(a, m, (int)j0, wj, linv, mstride);
+                tri_inverse_kernel<float><<<inv_grid, 256, inv_smem, sx>>>(a, m, (int)j0, wj, linv, mstride);
                 if (w.uinv)
-                    tri_inverse_upper_kernel<float><<<inv_grid, 256, inv_smem, s>>>(a, m, (int)j0, wj,
+                    tri_inverse_upper_kernel<float><<<inv_grid, 256, inv_smem, sx>>>(a, m, (int)j0, wj,
                                                                                     slot(w.uinv, j0), mstride);
             }
             if (r1 >= m) {
-                prof_end(s, FH_PROF_TRSM, 0.0);
+                prof_end(sx, FH_PROF_TRSM, 0.0);
                 break;
             }
             if (nopivot) {
@@ -1398,7 +1451,7 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
                 // tile of L21 reads exactly its own rows of A21).
                 if (rend > r1)
                     st = gemm_tc_strided(at(r1, j0), m, mm, reinterpret_cast<const float *>(slot(w.uinv, j0)), wj,
-                                         mstride, at(r1, j0), m, mm, rend - r1, wj, wj, 1, count, s, err);
+                                         mstride, at(r1, j0), m, mm, rend - r1, wj, wj, 1, count, sx, err);
                 if (st) return st;
             } else {
                 swaps(j0, wj, K0, j0);
@@ -1409,19 +1462,19 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
                 // so nothing reads the upper tiles of a diagonal region, which
                 // the symmetric deep updates leave out.
                 const dim3 tg((unsigned)((E - r1 + 31) / 32), (unsigned)((wj + 31) / 32), (unsigned)count);
-                u12_from_l21_kernel<<<tg, dim3(32, 8), 0, s>>>(a, m, j0, wj, r1, E);
+                u12_from_l21_kernel<<<tg, dim3(32, 8), 0, sx>>>(a, m, j0, wj, r1, E);
                 st = cudaGetLastError() == cudaSuccess ? FH_OK : fail(err, FH_ERR_CUDA, "U12 transpose launch failed");
             } else if (r1 < E) {
                 st = gemm_tc_strided(reinterpret_cast<const float *>(linv), wj, mstride, at(j0, r1), m, mm,
-                                     at(j0, r1), m, mm, wj, E - r1, wj, 1, count, s, err);
+                                     at(j0, r1), m, mm, wj, E - r1, wj, 1, count, sx, err);
             }
-            prof_end(s, FH_PROF_TRSM, 4.0 * (double)wj * wj * (double)(E - r1) * count);
+            prof_end(sx, FH_PROF_TRSM, 4.0 * (double)wj * wj * (double)(E - r1) * count);
             if (st) return st;
             if (r1 < E) {
-                prof_begin(s, FH_PROF_GEMM_TC_INNER);
+                prof_begin(sx, FH_PROF_GEMM_TC_INNER);
                 st = gemm_tc_strided(at(r1, j0), m, mm, at(j0, r1), m, mm, at(r1, r1), m, mm, rend - r1, E - r1, wj, 0,
-                                     count, s, err);
-                prof_end(s, FH_PROF_GEMM_TC_INNER, 8.0 * (double)(rend - r1) * (double)(E - r1) * wj * count);
+                                     count, sx, err);
+                prof_end(sx, FH_PROF_GEMM_TC_INNER, 8.0 * (double)(rend - r1) * (double)(E - r1) * wj * count);
                 if (st) return st;
             }
         }
@@ -1439,18 +1492,22 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             };
             float *t = reinterpret_cast<float *>(w.tbuf);
             const int64_t ww = (int64_t)W * W, tt = (int64_t)nb * (W - nb);
-            prof_begin(s, FH_PROF_TRSM);
+            prof_begin(sx, FH_PROF_TRSM);
             for (int bi = nbw - 2; bi >= 0 && !st; --bi) {
-                const int rest = (nbw - 1 - bi) * nb;  // columns right of the diagonal block
+                const int rest_cols = (nbw - 1 - bi) * nb;  // columns right of the diagonal block
                 st = gemm_tc_strided(at(K0 + (int64_t)bi * nb, K0 + (int64_t)(bi + 1) * nb), m, mm, xat(bi + 1, bi + 1),
-                                     W, ww, t, nb, tt, nb, rest, rest, 1, count, s, err);
+                                     W, ww, t, nb, tt, nb, rest_cols, rest_cols, 1, count, sx, err);
                 if (!st)
-                    st = gemm_tc_strided(xat(bi, bi), W, ww, t, nb, tt, xat(bi, bi + 1), W, ww, nb, rest, nb, 2, count, s,
-                                         err);
+                    st = gemm_tc_strided(xat(bi, bi), W, ww, t, nb, tt, xat(bi, bi + 1), W, ww, nb, rest_cols, nb, 2,
+                                         count, sx, err);
             }
-            if (!st) st = gemm_tc_pack_b(reinterpret_cast<float *>(xinv), W, ww, W, W, count, w.xpack, s, err);
-            prof_end(s, FH_PROF_TRSM, 0.0);
+            if (!st) st = gemm_tc_pack_b(reinterpret_cast<float *>(xinv), W, ww, W, W, count, w.xpack, sx, err);
+            prof_end(sx, FH_PROF_TRSM, 0.0);
             if (st) return st;
+            if (ahead) {
+                st = join_front();
+                if (st) return st;
+            }
             // L21 = A21 X for every row below, U12 = D L21^T, P = L21 S packed.
             st = gemm_tc_panel_solve(b.a, m, count, K0, W, w.xpack, reinterpret_cast<const float *>(dvec),
                                      reinterpret_cast<const float *>(svec), w.pack_a, w.upper, s, err);
@@ -1458,7 +1515,31 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             // C -= P P^T, only the tiles on and below the diagonal: every U
             // entry is formed from L (steps inside each diagonal region, panel
             // solve beyond).
-            st = gemm_tc_packed_run(w.pack_a, w.pack_a, at(E, E), m, mm, n2, n2, W, count, s, err, 0);
+            // With the look-ahead: the next super-panel's column blocks first,
+            // then the front of that super-panel may start.
+            const int next_blocks = (int)((std::min<int64_t>(outer, n2) + 127) / 128);
+            const int64_t rest_blocks = (n2 + 127) / 128 - next_blocks;
+            const double rest_tiles = (double)count * (double)rest_blocks * (double)(rest_blocks + 1) / 2.0;
+            if (!ahead || rest_tiles < (double)kAheadMinWaves * sms) {
+                st = gemm_tc_packed_run(w.pack_a, w.pack_a, at(E, E), m, mm, n2, n2, W, count, s, err, 0);
+                if (st) return st;
+                if (ahead) {
+                    FHB_CUDA(cudaEventRecord(ev_go, s));
+                    FHB_CUDA(cudaStreamWaitEvent(w.side, ev_go, 0));
+                }
+                continue;
+            }
+            st = gemm_tc_packed_run(w.pack_a, w.pack_a, at(E, E), m, mm, n2, n2, W, count, s, err, 0, 0, next_blocks);
+            if (st) return st;
+            // The counter and the rest's tile table are in place (on s)
+            // before the side stream, whose helper grid reads both, goes on.
+            FHB_CUDA(cudaMemsetAsync(w.tile_counter, 0, sizeof(int), s));
+            st = gemm_tc_packed_schedule(rest, w.pack_a, w.pack_a, at(E, E), m, mm, n2, n2, W, count, 0, next_blocks, -1,
+                                         s, err);
+            if (st) return st;
+            FHB_CUDA(cudaEventRecord(ev_go, s));
+            FHB_CUDA(cudaStreamWaitEvent(w.side, ev_go, 0));
+            st = gemm_tc_packed_launch(rest, sms - spare, w.tile_counter, s, err);
             if (st) return st;
             continue;
         }
@@ -1492,6 +1573,10 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
                                    w.pack_b, s, err);
         if (st) return st;
         FHB_CUDA(cudaGetLastError());
+    }
+    if (ahead) {  // the last front (the final diagonal region) and any helper, before what follows on s
+        st = join_front();
+        if (st) return st;
     }
     FHB_CUDA(cudaGetLastError());
     return coop_check(*w.coop, s, err);

@@ -83,6 +83,13 @@ struct LuWork {
     void *xpack = nullptr;
     void *tbuf = nullptr;
     void *dvec = nullptr;
+    // Look-ahead of the fused form (both given): each super-panel's diagonal
+    // region, X and its packing run on `side` while the bulk of the previous
+    // deep update runs on the factorization's stream on all SMs but a few,
+    // drawing its tiles from tile_counter; when the side stream's work is
+    // done a second grid on it joins the update and takes those SMs back.
+    cudaStream_t side = nullptr;
+    int *tile_counter = nullptr;
 };
 
 // Cooperative panel: sizing, binding of a scratch block, launch, error check.
@@ -128,9 +135,39 @@ size_t packed_operand_bytes(int64_t rows, int K, int count);
 fh_status gemm_tc_packed_update(const float *A, int64_t lda, int64_t sA, const float *B, int64_t ldb, int64_t sB,
                                 float *C, int64_t ldc, int64_t sC, int64_t M, int64_t N, int K, int count,
                                 void *pack_a, void *pack_b, cudaStream_t s, fh_error_info *err, int lower_from = -1);
-// The deep update from operands already packed (layout of pack_a / pack_b above).
+// The deep update from operands already packed (layout of pack_a / pack_b
+// above), one CTA per SM.  lower_from >= 0: column blocks (of 128) below it
+// in full, the rest on and below the diagonal tile only; col_lo / col_hi
+// restrict it to the column blocks in [col_lo, col_hi) (col_hi < 0: to the
+// end).
 fh_status gemm_tc_packed_run(const void *pack_a, const void *pack_b, float *C, int64_t ldc, int64_t sC, int64_t M,
-                             int64_t N, int K, int count, cudaStream_t s, fh_error_info *err, int lower_from = -1);
+                             int64_t N, int K, int count, cudaStream_t s, fh_error_info *err, int lower_from = -1,
+                             int col_lo = 0, int col_hi = -1);
+// The same update as a schedule (its tile table on the device) launched as
+// one or more grids: with a tile counter (zeroed before the first launch,
+// in stream order) the grids draw tiles from it, so a grid on a second
+// stream can join an update already running on fewer SMs.  The release
+// frees the table in stream order on s, after every launch it follows.
+struct PackedSchedule {
+    const void *pack_a = nullptr, *pack_b = nullptr;
+    float *C = nullptr;
+    int64_t ldc = 0, sC = 0, M = 0, N = 0;
+    int K = 0, count = 0;
+    uint32_t *table = nullptr;
+    long long per_matrix = 0, tiles = 0;
+    double entries = 0.0;  // complex C entries per matrix
+};
+fh_status gemm_tc_packed_schedule(PackedSchedule &ps, const void *pack_a, const void *pack_b, float *C, int64_t ldc,
+                                  int64_t sC, int64_t M, int64_t N, int K, int count, int lower_from, int col_lo,
+                                  int col_hi, cudaStream_t s, fh_error_info *err);
+// grid <= 0: one CTA per SM; next: the tile counter or nullptr (every
+// grid-th tile per CTA).  profiled = false leaves the launch out of the event
+// profiler (a grid joining an update whose first grid is timed: its time lies
+// inside that grid's, its work is counted there).
+fh_status gemm_tc_packed_launch(const PackedSchedule &ps, int grid, int *next, cudaStream_t s, fh_error_info *err,
+                                bool profiled = true);
+void gemm_tc_packed_release(PackedSchedule &ps, cudaStream_t s);
+int gemm_tc_sm_count();
 // Packs B (K x N, element (k, n) at B[2 (f sB + k + n ldb)]) as a B operand.
 fh_status gemm_tc_pack_b(const float *B, int64_t ldb, int64_t sB, int64_t N, int K, int count, void *out,
                          cudaStream_t s, fh_error_info *err);

@@ -169,6 +169,28 @@ def test_two_level_mixed_matches_fp64(fh, legs):
     assert all(1 <= i <= 10 for i in rm.refinement_iterations), rm.refinement_iterations
 
 
+def test_two_level_mixed_look_ahead(fh):
+    """The 40-leg meander (m = 2,320, five super-panels) at 96 frequencies in
+    one batch: the deep updates of the first two super-panels are long enough
+    to be split (the next super-panel's columns first, the rest on all SMs but
+    a few while the next diagonal region runs on the second stream, then a
+    second grid joining from the same tile counter); the later ones run
+    whole.  Every frequency refines without the FP64 fallback and Z matches
+    the FP64 sweep."""
+    deck = F.meander_legs(40)
+    freqs = F.logspace(5, 10, 96)
+    with fh.MeshSystem.assemble(fh.Geometry.from_deck(deck), deck.ports, deck.discretization) as s:
+        assert s.counts()["internal_meshes"] == 2320
+        z64 = s.sweep(freqs, fh.Precision.FP64).impedance_ohm
+        with fh.Profiler() as prof:
+            rm = s.sweep(freqs, fh.Precision.MIXED_BF16X3)
+            profile = prof.read()
+    assert rel_err(rm.impedance_ohm, z64) < MIXED_RTOL
+    assert all(1 <= i <= 10 for i in rm.refinement_iterations), rm.refinement_iterations
+    # four deep updates (super-panels with rows below), two of them in two parts
+    assert profile["gemm_tc"]["launches"] == 6, profile["gemm_tc"]
+
+
 def test_two_level_mixed_odd_order(fh, oracle):
     """An odd order (m = 1,043: one segment of the 18-leg meander on a 29 x 1
     grid, 28 loops instead of 29) over three super-panels.  The FP32 system is

@@ -131,7 +131,7 @@ EXPORTS = [
     "fh_system_counts", "fh_system_timing", "fh_system_filaments", "fh_system_resistances",
     "fh_system_mesh_matrices", "fh_system_device_l_mesh", "fh_sweep", "fh_impedance", "fh_sweep_json",
     "fh_write_zc_mat", "fh_spice_subckt", "fh_system_fill_stats", "fh_profile_enable", "fh_profile_reset",
-    "fh_profile_read", "fh_pfft_default_params", "fh_pfft_create", "fh_pfft_apply", "fh_pfft_get_stats",
+    "fh_profile_read", "fh_profile_overlap", "fh_pfft_default_params", "fh_pfft_create", "fh_pfft_apply", "fh_pfft_get_stats",
     "fh_pfft_destroy", "fh_gmres_default_params", "fh_iterative_create", "fh_iterative_counts", "fh_iterative_timing",
     "fh_iterative_pfft_stats", "fh_iterative_sweep", "fh_iterative_destroy", "fh_test_gmres_dense",
     "fh_batch_sweep", "fh_gradient", "fh_test_inductance_gradient", "fh_release_cached_memory", "fh_test_near_pairs",
@@ -251,6 +251,7 @@ def load():
     L.fh_profile_enable.restype = None
     L.fh_profile_reset.restype = None
     L.fh_profile_read.argtypes = [ctypes.c_int32, c_int64_p, c_double_p, c_double_p]
+    L.fh_profile_overlap.argtypes = [ctypes.c_uint32, ctypes.c_uint32, c_double_p, c_double_p, c_double_p]
     _lib = L
     return L
 

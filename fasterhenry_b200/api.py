@@ -1321,3 +1321,16 @@ class Profiler:
             _check(L.fh_profile_read(i, ctypes.byref(launches), ctypes.byref(ms), ctypes.byref(work)))
             out[name] = {"launches": int(launches.value), "ms": float(ms.value), "work": float(work.value)}
         return out
+
+    @staticmethod
+    def overlap(a, b) -> Dict[str, float]:
+        """Milliseconds during which a launch of the classes named in `a` ran,
+        of those in `b`, and both at once (fh_profile_overlap): the
+        factorization's look-ahead runs the diagonal regions ("panel",
+        "trsm", "gemm_tc_inner") beside the deep update ("gemm_tc")."""
+        idx = {name: i for i, name in enumerate(N.PROFILE_CLASSES)}
+        ma = sum(1 << idx[n] for n in a)
+        mb = sum(1 << idx[n] for n in b)
+        x, y, both = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(N.load().fh_profile_overlap(ma, mb, ctypes.byref(x), ctypes.byref(y), ctypes.byref(both)))
+        return {"a_ms": float(x.value), "b_ms": float(y.value), "both_ms": float(both.value)}

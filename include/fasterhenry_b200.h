@@ -526,6 +526,12 @@ void fh_profile_reset(void);
 /* Totals since the last reset: launches, device milliseconds (sum of
  * per-launch event durations) and algorithmic work (flops). */
 fh_status fh_profile_read(int32_t cls, int64_t *launches, double *ms, double *work);
+/* Time (ms, from the launches recorded since fh_profile_enable) during which
+ * a launch of a class in mask_a (bit 1 << class) ran, a launch of a class in
+ * mask_b ran, and both ran at once (launches on different streams: the
+ * factorization's look-ahead).  Each launch counts from the event before it
+ * to the event after it on its stream. */
+fh_status fh_profile_overlap(uint32_t mask_a, uint32_t mask_b, double *ms_a, double *ms_b, double *ms_both);
 
 /* ---- outputs (host) ---------------------------------------------------- */
 

@@ -717,39 +717,85 @@ __device__ __forceinline__ void integrand_grad(const QuadCtx &c, double u, doubl
 // sign(0) = 0 on the primitive).
 struct LineTerms {
     double k, das, dl1, dl2, j1, j1b;
+    double drho;  // dk / d rho, when asked for
 };
-__device__ __forceinline__ double parallel_primitive_d(double q, double rho_sq) {
-    if (q == 0.0) return 0.0;
-    const double aq = fabs(q);
-    const double l = log(aq + sqrt(aq * aq + rho_sq));  // sign(q) times it; negative for lengths below 1 m
-    return q > 0.0 ? l : -l;
-}
-__device__ bool line_terms(double l1, double l2, double as, double rho, bool moments, LineTerms *t) {
-    if (!lines_parallel(l1, l2, as, rho, &t->k)) return false;
+// line_terms evaluates the four corner distances q of the rectangle once:
+// R = sqrt(q^2 + rho^2) and L = log(|q| + R) serve the kernel (|q| L - R,
+// the terms of lines_parallel in its own operation order, so k is the same
+// double), its partials (sign(q) L) and the moments (R).
+__device__ bool line_terms(double l1, double l2, double as, double rho, bool moments, LineTerms *t,
+                           bool radial = false) {
     const double r2 = rho * rho;
     const double e = as + l2;
-    const double pa = parallel_primitive_d(e, r2), pb = parallel_primitive_d(as, r2);
-    const double pc = parallel_primitive_d(e - l1, r2), pd = parallel_primitive_d(as - l1, r2);
-    t->das = pa - pb - pc + pd;
-    t->dl1 = pc - pd;
-    t->dl2 = pa - pc;
+    const double q[4] = {e, as, e - l1, as - l1};
+    double R[4], P[4], D[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const double aq = fabs(q[i]);
+        R[i] = sqrt(aq * aq + r2);
+        if (aq == 0.0) {
+            P[i] = -R[i];
+            D[i] = 0.0;
+        } else {
+            const double L = log(aq + R[i]);
+            P[i] = aq * L - R[i];
+            D[i] = q[i] > 0.0 ? L : -L;
+        }
+    }
+    const double smooth = P[0] - P[1] - P[2] + P[3];
     const double overlap = rmax(rmin(l1, e) - rmax(as, 0.0), 0.0);
+    double log_rho = 0.0;
+    if (overlap == 0.0) {
+        t->k = smooth;
+    } else if (rho > 0.0) {
+        log_rho = log(rho);
+        t->k = smooth - 2.0 * overlap * log_rho;
+    } else {
+        return false;
+    }
+    t->das = D[0] - D[1] - D[2] + D[3];
+    t->dl1 = D[2] - D[3];
+    t->dl2 = D[0] - D[2];
+    if (radial) {
+        // d/d rho of |q| log(|q| + R) - R is -rho / (|q| + R); of the
+        // overlap term, -2 overlap / rho
+        double g[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) g[i] = -rho / (fabs(q[i]) + R[i]);
+        t->drho = g[0] - g[1] - g[2] + g[3];
+        if (overlap > 0.0) t->drho -= 2.0 * overlap / rho;
+    }
     if (overlap > 0.0) {
         const double hi = l1 < e ? 1.0 : (l1 == e ? 0.5 : 0.0);    // d min(l1, e) / d l1
         const double lo = as > 0.0 ? 1.0 : (as == 0.0 ? 0.5 : 0.0);  // d max(as, 0) / d as
-        const double lr = 2.0 * log(rho);
+        const double lr = 2.0 * log_rho;
         t->dl1 -= lr * hi;
         t->dl2 -= lr * (1.0 - hi);
         t->das -= lr * ((1.0 - hi) - lo);
     }
     t->j1 = t->j1b = 0.0;
     if (moments && r2 > 0.0) {
-        auto R = [&](double x) { return sqrt(x * x + r2); };
-        auto psi = [&](double x) { return x * R(x) / (2.0 * r2) - 0.5 * asinh(x / rho); };
+        // psi(x) = x R(x) / (2 rho^2) - asinh(x / rho) / 2 at the four
+        // corners; asinh(|x| / rho) = log(|x| + R) - log(rho), taken from the
+        // log already formed where |x| >= rho / 2 (there the difference
+        // keeps all but a few ulps of a result of at least 0.48)
+        const double lr1 = log_rho != 0.0 ? log_rho : log(rho);
+        double psi[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const double aq = fabs(q[i]);
+            double ash;
+            if (aq >= 0.5 * rho) {
+                const double L = q[i] > 0.0 ? D[i] : -D[i];  // log(|x| + R)
+                ash = q[i] > 0.0 ? L - lr1 : lr1 - L;
+            } else {
+                ash = asinh(q[i] / rho);
+            }
+            psi[i] = q[i] * R[i] / (2.0 * r2) - 0.5 * ash;
+        }
         const double a = as, b = e;
-        const double i00 = (R(b) - R(b - l1) - R(a) + R(a - l1)) / r2;
-        const double i10 = (b * (R(b) - R(b - l1)) / r2 + psi(b - l1) - psi(b)) -
-                           (a * (R(a) - R(a - l1)) / r2 + psi(a - l1) - psi(a));
+        const double i00 = (R[0] - R[2] - R[1] + R[3]) / r2;
+        const double i10 = (b * (R[0] - R[2]) / r2 + psi[2] - psi[0]) - (a * (R[1] - R[3]) / r2 + psi[3] - psi[1]);
         const double i01 = i10 - t->das;  // int int (x' - x) / R^3 = -dk/das
         t->j1 = i10 - 0.5 * l1 * i00;
         t->j1b = i01 - (as + 0.5 * l2) * i00;
@@ -799,20 +845,69 @@ __device__ __forceinline__ void integrand_coord(const QuadCtx &c, double u, doub
     }
 }
 
+// The coordinate derivatives of a pair whose cross-sections lie far apart
+// against their size, by a product Gauss rule over both cross-sections
+// (m x m points each, no panel tree): with the integrand smooth there, its
+// error falls like r^(-2m) for r = 1 + 2 g / s + ... (g the gap between the
+// cross-sections, s their largest side; the Bernstein ellipse of the nearest
+// singularity, rho = 0): below 1e-10 with m = 4 for g >= 4 s and with m = 5
+// for g >= 2 s.  In these variables the transverse partials are those of
+// the integrand (dk/d rho times u / rho, v / rho), where the offset form
+// differentiates the overlap weights, and the rotation moments are the
+// points' own coordinates (a's for a, b's about its centre for b).
+__device__ __forceinline__ int far_rule_order(const Aligned &b) {
+    const double gu = rmax(fabs(b.offset[1]) - 0.5 * (b.width[0] + b.width[1]), 0.0);
+    const double gv = rmax(fabs(b.offset[2]) - 0.5 * (b.height[0] + b.height[1]), 0.0);
+    const double g = hypot(gu, gv);
+    const double side = rmax(rmax(b.width[0], b.width[1]), rmax(b.height[0], b.height[1]));
+    if (g >= 4.0 * side) return 4;
+    if (g >= 2.0 * side) return 5;
+    return 0;
+}
+__device__ __forceinline__ void far_point_coord(const QuadCtx &c, int m, int k, double *acc, double gacc[7]) {
+    const int ia = k % m, ja = (k / m) % m, ib = (k / (m * m)) % m, jb = k / (m * m * m);
+    const Aligned &b = c.b;
+    const double ya = 0.5 * b.width[0] * c_quad.nodes[m][ia], za = 0.5 * b.height[0] * c_quad.nodes[m][ja];
+    const double yb = 0.5 * b.width[1] * c_quad.nodes[m][ib], zb = 0.5 * b.height[1] * c_quad.nodes[m][jb];
+    const double w = (0.25 * b.width[0] * b.height[0]) * (0.25 * b.width[1] * b.height[1]) * c_quad.weights[m][ia] *
+                     c_quad.weights[m][ja] * c_quad.weights[m][ib] * c_quad.weights[m][jb];
+    const double u = b.offset[1] + yb - ya, v = b.offset[2] + zb - za;
+    const double rho = hypot(u, v);
+    LineTerms t;
+    if (!line_terms(b.length[0], b.length[1], c.axial_start, rho, c.rot != 0, &t, true)) return;
+    *acc += w * t.k;
+    gacc[0] += w * t.das;
+    gacc[1] += w * t.drho * (u / rho);
+    gacc[2] += w * t.drho * (v / rho);
+    gacc[3] += w * (t.dl1 + 0.5 * t.das);
+    gacc[4] += w * (t.dl2 - 0.5 * t.das);
+    if (c.rot) {
+        const bool ty = c.tau == 1;
+        const double ut = ty ? u : v, pa = ty ? ya : za, pb = ty ? yb : zb;
+        gacc[5] += w * c.sigma * (ut * t.j1 + pa * t.das);
+        gacc[6] -= w * c.sigma * (ut * t.j1b + pb * t.das);
+    }
+}
+
 // kMode 0: values[h] = the integral.  kMode 1: values[7 h + 0..6] = the
 // integral and its partials with respect to (width[0], width[1], offset[1],
 // height[0], height[1], offset[2]).  kMode 2: values[8 h + 0..7] = the
 // coordinate derivatives of integrand_coord (the work item's flags choose
 // the frame and the rotation axis).  The rule (panel tree, leaves, nodes) is
-// held at the pair's own geometry.
+// held at the pair's own geometry.  With key_counter the CTAs draw their keys
+// from it (keys differ widely in cost), else take every gridDim.x-th; in
+// kMode 2 the threads share the points of a batch of leaves evenly (a
+// direct leaf has 100, fewer than the CTA's threads).
 template <int kMode>
 __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
     const DevFil *__restrict__ fil, const int4 *__restrict__ items, const int64_t *__restrict__ heads,
-    int64_t n_heads, double *__restrict__ values) {
+    int64_t n_heads, double *__restrict__ values, unsigned long long *__restrict__ key_counter = nullptr) {
     constexpr int kVals = kMode == 0 ? 1 : (kMode == 1 ? 7 : 8);
     __shared__ Panel stack[kStack];
     __shared__ Leaf leaves[kLeaves];
-    __shared__ int s_nleaves, s_done;
+    __shared__ int s_leaf_off[kLeaves + 1];
+    __shared__ long long s_key;
+    __shared__ int s_nleaves, s_done, s_far;
     __shared__ QuadCtx ctx;
     __shared__ double s_red[kVals][kQuadThreads / 32];
     __shared__ double r10n[10], r10w[10], r16n[16], r16w[16];
@@ -824,7 +919,13 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
         r16n[threadIdx.x] = c_quad.nodes[16][threadIdx.x];
         r16w[threadIdx.x] = c_quad.weights[16][threadIdx.x];
     }
-    for (int64_t h = blockIdx.x; h < n_heads; h += gridDim.x) {
+    auto draw = [&](int64_t prev) -> int64_t {
+        if (!key_counter) return prev < 0 ? (int64_t)blockIdx.x : prev + gridDim.x;
+        if (threadIdx.x == 0) s_key = (long long)atomicAdd(key_counter, 1ull);
+        __syncthreads();
+        return s_key;
+    };
+    for (int64_t h = draw(-1); h < n_heads; h = draw(h)) {
         const int4 it = items[heads[h]];
         int sp = 0;
         double axial_scale = 0.0;
@@ -853,11 +954,21 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
             // Push panels in reverse so that they pop in the reference's order.
             for (int a = nu - 2; a >= 0; --a)
                 for (int c = nv - 2; c >= 0; --c) stack[sp++] = Panel{us[a], us[a + 1], vs[c], vs[c + 1], 0, 0};
+            s_far = kMode == 2 ? far_rule_order(b) : 0;
         }
         double acc = 0.0, gacc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         long long visited = 0;  // panels popped; bounded so that no input can loop without end
         bool overflow = false;
-        for (;;) {
+        int far_m = 0;
+        if (kMode == 2) {
+            __syncthreads();
+            far_m = s_far;
+            if (far_m) {
+                const int points = far_m * far_m * far_m * far_m;
+                for (int k = threadIdx.x; k < points; k += kQuadThreads) far_point_coord(ctx, far_m, k, &acc, gacc);
+            }
+        }
+        for (; !far_m;) {
             if (threadIdx.x == 0) {
                 // Walk the panel tree until the leaf buffer is full or the tree is done.
                 int nl = 0;
@@ -917,11 +1028,47 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
                 }
                 s_nleaves = nl;
                 s_done = sp == 0;
+                s_leaf_off[0] = 0;
+                for (int l = 0; l < nl; ++l) s_leaf_off[l + 1] = s_leaf_off[l] + (leaves[l].corner ? 256 : 100);
             }
             __syncthreads();
             const int nl = s_nleaves;
+            if (kMode == 2) {
+                // the batch's points in one sequence, every kQuadThreads-th per thread
+                const int total = s_leaf_off[nl];
+                int l = 0;
+                for (int k = threadIdx.x; k < total; k += kQuadThreads) {
+                    while (k >= s_leaf_off[l + 1]) ++l;
+                    const Leaf lf = leaves[l];
+                    const int kk = k - s_leaf_off[l];
+                    if (!lf.corner) {
+                        const double mu = 0.5 * (lf.a0 + lf.a1), hu = 0.5 * (lf.a1 - lf.a0);
+                        const double mv = 0.5 * (lf.b0 + lf.b1), hv = 0.5 * (lf.b1 - lf.b0);
+                        const int a = kk / 10, c = kk % 10;
+                        const double uu = mu + hu * r10n[a], wu = hu * r10w[a];
+                        const double vv = mv + hv * r10n[c], wv = hv * r10w[c];
+                        double g[8];
+                        integrand_coord(ctx, uu, vv, g);
+                        acc += wu * wv * g[0];
+                        for (int q = 0; q < 7; ++q) gacc[q] += wu * wv * g[1 + q];
+                    } else {
+                        const double A = lf.a0, B = lf.b0, ab = fabs(A * B);
+                        const int a = kk / 16, c = kk % 16;
+                        const double tau = 0.5 + 0.5 * r16n[a], w_tau = 0.5 * r16w[a];
+                        const double s3 = tau * tau * tau;
+                        const double radial = w_tau * 3.0 * tau * tau * s3;
+                        const double t = 0.5 + 0.5 * r16n[c], w_t = 0.5 * r16w[c];
+                        double g1[8], g2[8];
+                        integrand_coord(ctx, A * s3, B * s3 * t, g1);
+                        integrand_coord(ctx, A * s3 * t, B * s3, g2);
+                        const double f = radial * w_t * ab;
+                        acc += f * (g1[0] + g2[0]);
+                        for (int q = 0; q < 7; ++q) gacc[q] += f * (g1[1 + q] + g2[1 + q]);
+                    }
+                }
+            }
             // Evaluate the leaves: direct leaves have 100 points, corner leaves 256 (each two terms).
-            for (int l = 0; l < nl; ++l) {
+            for (int l = 0; l < nl && kMode != 2; ++l) {
                 const Leaf lf = leaves[l];
                 if (!lf.corner) {
                     double mu = 0.5 * (lf.a0 + lf.a1), hu = 0.5 * (lf.a1 - lf.a0);
@@ -930,12 +1077,7 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
                         int a = k / 10, c = k % 10;
                         double uu = mu + hu * r10n[a], wu = hu * r10w[a];
                         double vv = mv + hv * r10n[c], wv = hv * r10w[c];
-                        if (kMode == 2) {
-                            double g[8];
-                            integrand_coord(ctx, uu, vv, g);
-                            acc += wu * wv * g[0];
-                            for (int q = 0; q < 7; ++q) gacc[q] += wu * wv * g[1 + q];
-                        } else if (kMode == 1) {
+                        if (kMode == 1) {
                             double g[7];
                             integrand_grad(ctx, uu, vv, g);
                             acc += wu * wv * g[0];
@@ -952,14 +1094,7 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
                         double s = tau * tau * tau;
                         double radial = w_tau * 3.0 * tau * tau * s;
                         double t = 0.5 + 0.5 * r16n[c], w_t = 0.5 * r16w[c];
-                        if (kMode == 2) {
-                            double g1[8], g2[8];
-                            integrand_coord(ctx, A * s, B * s * t, g1);
-                            integrand_coord(ctx, A * s * t, B * s, g2);
-                            const double f = radial * w_t * ab;
-                            acc += f * (g1[0] + g2[0]);
-                            for (int q = 0; q < 7; ++q) gacc[q] += f * (g1[1 + q] + g2[1 + q]);
-                        } else if (kMode == 1) {
+                        if (kMode == 1) {
                             double g1[7], g2[7];
                             integrand_grad(ctx, A * s, B * s * t, g1);
                             integrand_grad(ctx, A * s * t, B * s, g2);
@@ -2506,8 +2641,12 @@ fh_status device_fill_coord(const DevFil *d_fil, const int32_t *d_seg, const uin
         st.unique_aligned = n_heads;
         double *d_values = nullptr;
         FHB_CUDA(alloc((void **)&d_values, 64 * (size_t)n_heads));
+        unsigned long long *d_keys = nullptr;
+        FHB_CUDA(alloc((void **)&d_keys, sizeof(unsigned long long)));
+        FHB_CUDA(cudaMemsetAsync(d_keys, 0, sizeof(unsigned long long), stream));
         const int qblocks = (int)std::min<int64_t>(n_heads, (int64_t)sms * 16);
-        aligned_quadrature_kernel<2><<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads, d_values);
+        aligned_quadrature_kernel<2><<<qblocks, kQuadThreads, 0, stream>>>(d_fil, d_quad, d_heads, n_heads, d_values,
+                                                                          d_keys);
         FHB_CUDA(cudaGetLastError());
         const int blocks = (int)std::min<int64_t>((n_quad + 255) / 256, (int64_t)sms * 16);
         coord_quad_scatter_kernel<<<blocks, 256, 0, stream>>>(d_fil, d_quad, d_item_head, d_values, n_quad, out, n,

@@ -21,9 +21,10 @@
 //   * the first call in each device context (a device's primary context, and
 //     again after cudaDeviceReset has replaced it) looks up the array's
 //     device address with cudaGetSymbolAddress, with that device current;
-//     make that first call before any stream capture begins;
 //   * the call waits on the host until the solve has finished on its stream
-//     (it reads the zero-pivot flag back);
+//     (it reads the zero-pivot flag back with a copy and a stream
+//     synchronize), so it cannot be recorded into a CUDA graph: no call may
+//     be made while its stream, or the legacy stream, is being captured;
 //   * all calls share the one array: calls whose work overlaps on the GPU
 //     (concurrent streams, or threads on the same device) race on it and must
 //     be serialised by the caller.  Each call clears the parts that must

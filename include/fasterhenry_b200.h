@@ -255,11 +255,12 @@ fh_status fh_lu_solve_c64(const double *a, size_t n, const double *b, size_t nrh
  * Allocates nothing: its scratch (pivots, pivot-search partials, flags) is a
  * file-scope device array sized for n <= FH_NOALLOC_MAX_ORDER; larger n is
  * rejected with FH_ERR_INVALID_ARGUMENT.  The first call in each device
- * context looks up the array's address (make that first call before any
- * stream capture begins).  All calls share the array: calls that overlap on
- * the GPU race and must be serialised by the caller.  The call blocks the
- * host until the solve has finished on `stream` (it reads back the
- * zero-pivot flag). */
+ * context looks up the array's address.  All calls share the array: calls
+ * that overlap on the GPU race and must be serialised by the caller.  The
+ * call blocks the host until the solve has finished on `stream` (it copies
+ * the zero-pivot flag back and synchronizes the stream), so it must not be
+ * made while `stream`, or the legacy stream, is being captured into a CUDA
+ * graph. */
 #define FH_NOALLOC_MAX_ORDER 65536
 fh_status fh_lu_solve_c64_noalloc(double *a, size_t n, double *b, size_t nrhs, void *stream,
                                   fh_error_info *err);

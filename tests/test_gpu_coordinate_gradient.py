@@ -175,6 +175,35 @@ def test_near_orthogonal_pair_matches_the_oracle_bar_integral(fh, oracle):
         assert D[k][0, 1] == 0.0 and D[k][1, 0] == 0.0
 
 
+@pytest.mark.parametrize("gap_um,on_side", [(5.0, False), (13.0, False), (5.0, True), (13.0, True)])
+def test_orthogonal_pairs_apart_match_the_oracle_quadrature(fh, oracle, gap_um, on_side):
+    """Long orthogonal boxes whose gap is 2.5 and 6.5 times their largest
+    cross-section side (2 um): too near for point quadrature and rejected by
+    the closed form, so the coordinate fill integrates them -- by the product
+    rule over both cross-sections of the perpendicular-segment integral.  A
+    lies flat (B's length then runs along A's width axis) or on its side
+    (width along z: B's length runs along A's height axis).  The rotation
+    rates against the oracle's restatement of the reference's aligned
+    quadrature of the two boxes in A's frame."""
+    la, lb = 300 * UM, 250 * UM
+    a = Box([0, 0, 0], [1, 0, 0], [la, 2 * UM, 1 * UM], [0, 0, 1] if on_side else None)
+    b = Box([0.5 * la + gap_um * UM + 1 * UM, 0.5 * lb + 2 * UM, 0.2 * UM], [0, 1, 0], [lb, 2 * UM, 1 * UM])
+    D = device_d(fh, [a, b], [0, 1])
+    # b's box in a's frame: its extents along a's axes, its centre's offset
+    axes_a = [a.l, a.w, a.h]
+    ext_b = [sum(abs(ax @ bx) * d for bx, d in zip([b.l, b.w, b.h], b.dims)) for ax in axes_a]
+    off = [ax @ (b.c - a.c) for ax in axes_a]
+    v = oracle.aligned_quadrature([a.dims[0], ext_b[0]], [a.dims[1], ext_b[1]], [a.dims[2], ext_b[2]], off)
+    k = MU0_4PI / (a.dims[1] * a.dims[2] * b.dims[1] * b.dims[2])
+    want_a = k * (np.cross([0, 0, 1], a.l) @ b.l) * v
+    want_b = k * (np.cross([0, 0, 1], b.l) @ a.l) * v
+    assert abs(want_a) > 0 and abs(want_b) > 0
+    assert abs(D[3][0, 1] - want_a) <= 1e-9 * abs(want_a), (D[3][0, 1], want_a)
+    assert abs(D[3][1, 0] - want_b) <= 1e-9 * abs(want_b), (D[3][1, 0], want_b)
+    for q in range(3):
+        assert D[q][0, 1] == 0.0 and D[q][1, 0] == 0.0
+
+
 def test_segment_pairs_carry_the_stretch_of_the_frozen_fill(fh, oracle):
     """A bundle of one segment: only Ds, equal to differences of the oracle's
     frozen fill with one filament stretched about its centre (the diagonal:

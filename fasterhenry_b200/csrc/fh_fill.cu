@@ -861,8 +861,10 @@ __device__ __forceinline__ void integrand_coord(const QuadCtx &c, double u, doub
 // (m x m points each, no panel tree): with the integrand smooth there, its
 // error falls like r^(-2m) for r = 1 + 2 g / s + ... (g the gap between the
 // cross-sections, s their largest side; the Bernstein ellipse of the nearest
-// singularity, rho = 0): below 1e-10 with m = 4 for g >= 4 s and with m = 5
-// for g >= 2 s.  In these variables the transverse partials are those of
+// singularity, rho = 0): m = 4 for g >= 4 s, 5 for g >= 2 s, 6 for g >= s.
+// Against the restated aligned quadrature of the reference the values agreed
+// to 1e-11, 3e-12 and 2e-11 in those bands (random pairs of 50-400 um
+// bars with 0.2-3 um sides).  In these variables the transverse partials are those of
 // the integrand (dk/d rho times u / rho, v / rho), where the offset form
 // differentiates the overlap weights, and the rotation moments are the
 // points' own coordinates (a's for a, b's about its centre for b).
@@ -873,6 +875,7 @@ __device__ __forceinline__ int far_rule_order(const Aligned &b) {
     const double side = rmax(rmax(b.width[0], b.width[1]), rmax(b.height[0], b.height[1]));
     if (g >= 4.0 * side) return 4;
     if (g >= 2.0 * side) return 5;
+    if (g >= side) return 6;
     return 0;
 }
 __device__ __forceinline__ void far_point_coord(const QuadCtx &c, int m, int k, double *acc, double gacc[7]) {
@@ -907,9 +910,10 @@ __device__ __forceinline__ void far_point_coord(const QuadCtx &c, int m, int k, 
 // d the distance between the segments' parallel planes).  log(a + R) is
 // taken as log((b^2 + d^2) / (R - a)) for negative a, which has no
 // cancellation.  Against the restated aligned quadrature of the reference
-// the rule agreed to below 2e-13 with m = 4 for gaps of at least four times
-// the largest cross-section side and with m = 5 for at least twice (random
-// pairs of 50-400 um segments with 0.2-3 um sides).
+// the rule agreed to below 6e-13 with m = 4 for gaps of at least four times
+// the largest cross-section side, 1.2e-13 with m = 5 for at least twice and
+// 3.5e-13 with m = 6 for at least once (random pairs of 50-400 um segments
+// with 0.2-3 um sides).
 __device__ __forceinline__ double perp_primitive(double X, double Y, double d) {
     const double d2 = d * d, R = sqrt(X * X + Y * Y + d2);
     auto lg = [&](double a, double b) { return a >= 0.0 ? log(a + R) : log((b * b + d2) / (R - a)); };
@@ -930,6 +934,7 @@ __device__ __forceinline__ int ortho_rule_order(const OrthoBoxes &o) {
     const double side = rmax(rmax(o.ea[1], o.ea[2]), rmax(o.eb[0], o.eb[kq]));
     if (g >= 4.0 * side) return 4;
     if (g >= 2.0 * side) return 5;
+    if (g >= side) return 6;
     return 0;
 }
 __device__ __forceinline__ double ortho_point(const OrthoBoxes &o, int m, int k) {

@@ -117,6 +117,10 @@ PAIRS = {
     # B near A (gap 7 um against a 40 um length): aligned quadrature with rotations
     "quad_parallel": (Box([0, 0, 0], [1, 0, 0], [40 * UM, 2 * UM, 1 * UM]),
                       Box([6 * UM, 9 * UM, 0.5 * UM], [1, 0, 0], [30 * UM, 2 * UM, 1 * UM]), (8, 1, 1), (6, 1, 1)),
+    # the gap (3 um) 1.5 times the largest side: the sixth-order product rule
+    "quad_parallel_near": (Box([0, 0, 0], [1, 0, 0], [40 * UM, 2 * UM, 1 * UM]),
+                           Box([6 * UM, 5 * UM, 0.5 * UM], [1, 0, 0], [30 * UM, 2 * UM, 1 * UM]), (8, 1, 1),
+                           (6, 1, 1)),
     "quad_antiparallel": (Box([0, 0, 0], [1, 0, 0], [40 * UM, 2 * UM, 1 * UM]),
                           Box([-4 * UM, -9 * UM, 0], [-1, 0, 0], [30 * UM, 2 * UM, 1 * UM]), (8, 1, 1), (6, 1, 1)),
     # orthogonal, far: point quadrature (the derivative is the rotation's alone)

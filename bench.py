@@ -243,7 +243,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         profile = prof.read()
         # the look-ahead: diagonal-region launches (second stream) beside the deep update
-        ov = prof.overlap(["panel", "trsm", "gemm_tc_inner"], ["gemm_tc"])
+        ov = prof.overlap(["panel", "trsm", "gemm_tc_inner"], ["gemm_tc", "gemm_tc_shared"])
     look_ahead = {"front_ms": round(ov["a_ms"] / args.steps, 3), "update_ms": round(ov["b_ms"] / args.steps, 3),
                   "overlap_ms": round(ov["both_ms"] / args.steps, 3),
                   "what": "per sweep, event-timed: time the diagonal-region launches ran, the deep update ran, "
@@ -304,6 +304,17 @@ def run_ours(args):
                 "traffic_source": "ncu dram__bytes_read+write of packed_update_kernel (2,400-filament meander), "
                                   "scaled by algorithmic bytes",
                 "per_launch_ms": round(per_launch_ms, 4), "launches": g["launches"]}
+    if gemm_cls == "gemm_tc":
+        roofline["launches_counted"] = ("the deep updates and the first parts of split updates, on every SM; "
+                                        "the second parts below")
+        sh = profile.get("gemm_tc_shared", {"launches": 0, "ms": 0.0, "work": 0.0})
+        if sh["launches"]:
+            sh_achieved = 3.0 * sh["work"] / (sh["ms"] * 1e-3) / 1e12
+            roofline["shared_part"] = {
+                "launches": sh["launches"], "per_launch_ms": round(sh["ms"] / sh["launches"], 4),
+                "achieved": round(sh_achieved, 2), "frac": round(sh_achieved / peak, 4) if peak else None,
+                "what": "second parts of split deep updates: 116 of 148 SMs while the next diagonal region runs "
+                        "on the others, then all of them (a joining grid, not timed apart)"}
     launches = sum(v["launches"] for v in profile.values())
 
     out = {

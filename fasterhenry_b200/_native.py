@@ -141,7 +141,7 @@ EXPORTS = [
 ]
 
 PROFILE_CLASSES = ["gemm_fp64", "gemm_fp32", "gemm_tc", "panel", "trsm", "solve", "residual", "pack", "gemm_tc_inner",
-                   "pfft_apply", "panel_solve", "form", "solve_flow", "solve_barrier", "batch"]
+                   "pfft_apply", "panel_solve", "form", "solve_flow", "solve_barrier", "batch", "gemm_tc_shared"]
 
 
 class FillStats(ctypes.Structure):

@@ -944,7 +944,7 @@ fh_status gemm_tc_packed_schedule(PackedSchedule &ps, const void *pack_a, const 
 }
 
 fh_status gemm_tc_packed_launch(const PackedSchedule &ps, int grid, int *next, cudaStream_t s, fh_error_info *err,
-                                bool profiled) {
+                                int prof_class) {
     if (ps.tiles <= 0) return FH_OK;
     if (next && ps.tiles > INT32_MAX) return fail(err, FH_ERR_INVALID_ARGUMENT, "packed update tile counter overflow");
     int dev = 0;
@@ -968,10 +968,10 @@ fh_status gemm_tc_packed_launch(const PackedSchedule &ps, int grid, int *next, c
     g.next = next;
     if (grid <= 0) grid = std::max(1, g_sms[dev]);
     grid = (int)std::min<long long>(ps.tiles, grid);
-    const bool prof = profiled && prof_on();
-    if (prof) prof_begin(s, FH_PROF_GEMM_TC);
+    const bool prof = prof_class >= 0 && prof_on();
+    if (prof) prof_begin(s, prof_class);
     packed_update_kernel<<<grid, kThreads, kSmemBytes, s>>>(g, g_flag[dev]);
-    if (prof) prof_end(s, FH_PROF_GEMM_TC, 8.0 * ps.entries * (double)ps.K * ps.count);
+    if (prof) prof_end(s, prof_class, 8.0 * ps.entries * (double)ps.K * ps.count);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) return fail(err, FH_ERR_CUDA, std::string("packed update launch failed: ") + cudaGetErrorString(le));
     return FH_OK;

@@ -1398,7 +1398,7 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
     // for both.
     auto join_front = [&]() -> fh_status {
         if (rest.tiles > 0) {
-            const fh_status hs = gemm_tc_packed_launch(rest, spare, w.tile_counter, w.side, err, false);
+            const fh_status hs = gemm_tc_packed_launch(rest, spare, w.tile_counter, w.side, err, -1);
             if (hs) return hs;
         }
         FHB_CUDA(cudaEventRecord(ev_done, w.side));
@@ -1539,7 +1539,7 @@ fh_status lu_factor_deep(LuBatch<float> &b, LuWork &w, int nb, cudaStream_t s, f
             if (st) return st;
             FHB_CUDA(cudaEventRecord(ev_go, s));
             FHB_CUDA(cudaStreamWaitEvent(w.side, ev_go, 0));
-            st = gemm_tc_packed_launch(rest, sms - spare, w.tile_counter, s, err);
+            st = gemm_tc_packed_launch(rest, sms - spare, w.tile_counter, s, err, FH_PROF_GEMM_TC_SHARED);
             if (st) return st;
             continue;
         }

@@ -161,11 +161,11 @@ fh_status gemm_tc_packed_schedule(PackedSchedule &ps, const void *pack_a, const 
                                   int64_t sC, int64_t M, int64_t N, int K, int count, int lower_from, int col_lo,
                                   int col_hi, cudaStream_t s, fh_error_info *err);
 // grid <= 0: one CTA per SM; next: the tile counter or nullptr (every
-// grid-th tile per CTA).  profiled = false leaves the launch out of the event
-// profiler (a grid joining an update whose first grid is timed: its time lies
-// inside that grid's, its work is counted there).
+// grid-th tile per CTA).  prof_class: the event profiler's class of the
+// launch, or -1 to leave it out (a grid joining an update whose first grid
+// is timed: its time lies inside that grid's, its work is counted there).
 fh_status gemm_tc_packed_launch(const PackedSchedule &ps, int grid, int *next, cudaStream_t s, fh_error_info *err,
-                                bool profiled = true);
+                                int prof_class = FH_PROF_GEMM_TC);
 void gemm_tc_packed_release(PackedSchedule &ps, cudaStream_t s);
 int gemm_tc_sm_count();
 // Packs B (K x N, element (k, n) at B[2 (f sB + k + n ldb)]) as a B operand.

@@ -519,7 +519,8 @@ typedef enum fh_profile_class {
     FH_PROF_SOLVE_FLOW = 12,    /* dataflow forward/backward solve of the two-level factors (flags per block) */
     FH_PROF_SOLVE_BARRIER = 13, /* barrier-based forward/backward solve of the two-level factors */
     FH_PROF_BATCH = 14,         /* the persistent batched solve of many small systems (fh_batch_sweep, mixed) */
-    FH_PROF_CLASSES = 15
+    FH_PROF_GEMM_TC_SHARED = 15, /* the second part of a split deep update, on the SMs the look-ahead leaves it */
+    FH_PROF_CLASSES = 16
 } fh_profile_class;
 
 void fh_profile_enable(int32_t on);

@@ -728,14 +728,12 @@ __device__ __forceinline__ void integrand_grad(const QuadCtx &c, double u, doubl
 // sign(0) = 0 on the primitive).
 struct LineTerms {
     double k, das, dl1, dl2, j1, j1b;
-    double drho;  // dk / d rho, when asked for
 };
 // line_terms evaluates the four corner distances q of the rectangle once:
 // R = sqrt(q^2 + rho^2) and L = log(|q| + R) serve the kernel (|q| L - R,
 // the terms of lines_parallel in its own operation order, so k is the same
 // double), its partials (sign(q) L) and the moments (R).
-__device__ bool line_terms(double l1, double l2, double as, double rho, bool moments, LineTerms *t,
-                           bool radial = false) {
+__device__ bool line_terms(double l1, double l2, double as, double rho, bool moments, LineTerms *t) {
     const double r2 = rho * rho;
     const double e = as + l2;
     const double q[4] = {e, as, e - l1, as - l1};
@@ -767,15 +765,6 @@ __device__ bool line_terms(double l1, double l2, double as, double rho, bool mom
     t->das = D[0] - D[1] - D[2] + D[3];
     t->dl1 = D[2] - D[3];
     t->dl2 = D[0] - D[2];
-    if (radial) {
-        // d/d rho of |q| log(|q| + R) - R is -rho / (|q| + R); of the
-        // overlap term, -2 overlap / rho
-        double g[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) g[i] = -rho / (fabs(q[i]) + R[i]);
-        t->drho = g[0] - g[1] - g[2] + g[3];
-        if (overlap > 0.0) t->drho -= 2.0 * overlap / rho;
-    }
     if (overlap > 0.0) {
         const double hi = l1 < e ? 1.0 : (l1 == e ? 0.5 : 0.0);    // d min(l1, e) / d l1
         const double lo = as > 0.0 ? 1.0 : (as == 0.0 ? 0.5 : 0.0);  // d max(as, 0) / d as
@@ -857,17 +846,14 @@ __device__ __forceinline__ void integrand_coord(const QuadCtx &c, double u, doub
 }
 
 // The coordinate derivatives of a pair whose cross-sections lie far apart
-// against their size, by a product Gauss rule over both cross-sections
-// (m x m points each, no panel tree): with the integrand smooth there, its
-// error falls like r^(-2m) for r = 1 + 2 g / s + ... (g the gap between the
-// cross-sections, s their largest side; the Bernstein ellipse of the nearest
-// singularity, rho = 0): m = 4 for g >= 4 s, 5 for g >= 2 s, 6 for g >= s.
-// Against the restated aligned quadrature of the reference the values agreed
-// to 1e-11, 3e-12 and 2e-11 in those bands (random pairs of 50-400 um
-// bars with 0.2-3 um sides).  In these variables the transverse partials are those of
-// the integrand (dk/d rho times u / rho, v / rho), where the offset form
-// differentiates the overlap weights, and the rotation moments are the
-// points' own coordinates (a's for a, b's about its centre for b).
+// against their size, without the panel tree: a p x p Gauss rule on each of
+// the overlap weights' break-point panels (the integrand is a product of
+// linear weights and a kernel smooth there), p = 4 for gaps g >= 4 s, 5 for
+// g >= 2 s, 6 for g >= s (s the largest cross-section side).  The error
+// falls like r^(-2p) with r = 1 + 2 g / s, the Bernstein ellipse of the
+// nearest singularity (rho = 0); against the restated aligned quadrature
+// of the reference the values agreed to 2e-11, 7e-13 and 8e-12 in those
+// bands (random pairs of 50-400 um bars with 0.2-3 um sides).
 __device__ __forceinline__ int far_rule_order(const Aligned &b) {
     const double gu = rmax(fabs(b.offset[1]) - 0.5 * (b.width[0] + b.width[1]), 0.0);
     const double gv = rmax(fabs(b.offset[2]) - 0.5 * (b.height[0] + b.height[1]), 0.0);
@@ -878,30 +864,12 @@ __device__ __forceinline__ int far_rule_order(const Aligned &b) {
     if (g >= side) return 6;
     return 0;
 }
-__device__ __forceinline__ void far_point_coord(const QuadCtx &c, int m, int k, double *acc, double gacc[7]) {
-    const int ia = k % m, ja = (k / m) % m, ib = (k / (m * m)) % m, jb = k / (m * m * m);
-    const Aligned &b = c.b;
-    const double ya = 0.5 * b.width[0] * c_quad.nodes[m][ia], za = 0.5 * b.height[0] * c_quad.nodes[m][ja];
-    const double yb = 0.5 * b.width[1] * c_quad.nodes[m][ib], zb = 0.5 * b.height[1] * c_quad.nodes[m][jb];
-    const double w = (0.25 * b.width[0] * b.height[0]) * (0.25 * b.width[1] * b.height[1]) * c_quad.weights[m][ia] *
-                     c_quad.weights[m][ja] * c_quad.weights[m][ib] * c_quad.weights[m][jb];
-    const double u = b.offset[1] + yb - ya, v = b.offset[2] + zb - za;
-    const double rho = hypot(u, v);
-    LineTerms t;
-    if (!line_terms(b.length[0], b.length[1], c.axial_start, rho, c.rot != 0, &t, true)) return;
-    *acc += w * t.k;
-    gacc[0] += w * t.das;
-    gacc[1] += w * t.drho * (u / rho);
-    gacc[2] += w * t.drho * (v / rho);
-    gacc[3] += w * (t.dl1 + 0.5 * t.das);
-    gacc[4] += w * (t.dl2 - 0.5 * t.das);
-    if (c.rot) {
-        const bool ty = c.tau == 1;
-        const double ut = ty ? u : v, pa = ty ? ya : za, pb = ty ? yb : zb;
-        gacc[5] += w * c.sigma * (ut * t.j1 + pa * t.das);
-        gacc[6] -= w * c.sigma * (ut * t.j1b + pb * t.das);
-    }
-}
+// Gauss-Legendre rules of orders 3 to 6 in shared memory (row m - 3): the
+// far rules' threads index them at different points, which constant memory
+// would serialize.
+struct FarRules {
+    double n[4][6], w[4][6];
+};
 
 // The scalar coupling int int 1/R of two orthogonal boxes far apart against
 // their cross-sections, as a product Gauss rule over both cross-sections of
@@ -910,10 +878,10 @@ __device__ __forceinline__ void far_point_coord(const QuadCtx &c, int m, int k, 
 // d the distance between the segments' parallel planes).  log(a + R) is
 // taken as log((b^2 + d^2) / (R - a)) for negative a, which has no
 // cancellation.  Against the restated aligned quadrature of the reference
-// the rule agreed to below 6e-13 with m = 4 for gaps of at least four times
-// the largest cross-section side, 1.2e-13 with m = 5 for at least twice and
-// 3.5e-13 with m = 6 for at least once (random pairs of 50-400 um segments
-// with 0.2-3 um sides).
+// the rule agreed to below 1.2e-11 with m = 3 for gaps of at least eight
+// times the largest cross-section side, 6e-13 with m = 4 for at least four
+// times, 1.2e-13 with m = 5 for at least twice and 3.5e-13 with m = 6 for at
+// least once (random pairs of 50-400 um segments with 0.2-3 um sides).
 __device__ __forceinline__ double perp_primitive(double X, double Y, double d) {
     const double d2 = d * d, R = sqrt(X * X + Y * Y + d2);
     auto lg = [&](double a, double b) { return a >= 0.0 ? log(a + R) : log((b * b + d2) / (R - a)); };
@@ -932,19 +900,20 @@ __device__ __forceinline__ int ortho_rule_order(const OrthoBoxes &o) {
     const double g = sqrt(g2);
     const int kq = 3 - o.kb;
     const double side = rmax(rmax(o.ea[1], o.ea[2]), rmax(o.eb[0], o.eb[kq]));
+    if (g >= 8.0 * side) return 3;
     if (g >= 4.0 * side) return 4;
     if (g >= 2.0 * side) return 5;
     if (g >= side) return 6;
     return 0;
 }
-__device__ __forceinline__ double ortho_point(const OrthoBoxes &o, int m, int k) {
+__device__ __forceinline__ double ortho_point(const OrthoBoxes &o, const FarRules &fr, int m, int k) {
     const int i = k % m, j = (k / m) % m, kx = (k / (m * m)) % m, l = k / (m * m * m);
     const int kb = o.kb, kq = 3 - kb;
-    const double ap = 0.5 * o.ea[kb] * c_quad.nodes[m][i], aq = 0.5 * o.ea[kq] * c_quad.nodes[m][j];
-    const double xb = o.off[0] + 0.5 * o.eb[0] * c_quad.nodes[m][kx];
-    const double bq = o.off[kq] + 0.5 * o.eb[kq] * c_quad.nodes[m][l];
-    const double w = (0.25 * o.ea[kb] * o.ea[kq]) * (0.25 * o.eb[0] * o.eb[kq]) * c_quad.weights[m][i] *
-                     c_quad.weights[m][j] * c_quad.weights[m][kx] * c_quad.weights[m][l];
+    const double *nd = fr.n[m - 3], *wt = fr.w[m - 3];
+    const double ap = 0.5 * o.ea[kb] * nd[i], aq = 0.5 * o.ea[kq] * nd[j];
+    const double xb = o.off[0] + 0.5 * o.eb[0] * nd[kx];
+    const double bq = o.off[kq] + 0.5 * o.eb[kq] * nd[l];
+    const double w = (0.25 * o.ea[kb] * o.ea[kq]) * (0.25 * o.eb[0] * o.eb[kq]) * wt[i] * wt[j] * wt[kx] * wt[l];
     const double x0 = -0.5 * o.ea[0] - xb, x1 = 0.5 * o.ea[0] - xb;
     const double y0 = o.off[kb] - 0.5 * o.eb[kb] - ap, y1 = o.off[kb] + 0.5 * o.eb[kb] - ap;
     const double d = bq - aq;
@@ -970,13 +939,23 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
     __shared__ Leaf leaves[kLeaves];
     __shared__ int s_leaf_off[kLeaves + 1];
     __shared__ long long s_key;
-    __shared__ int s_nleaves, s_done, s_far;
+    __shared__ int s_nleaves, s_done, s_far, s_npanels;
+    __shared__ FarRules far_rules;
     __shared__ QuadCtx ctx;
     __shared__ double s_red[kVals][kQuadThreads / 32];
-    __shared__ double r10n[10], r10w[10], r16n[16], r16w[16];
+    __shared__ double r10n[10], r10w[10], r16n[16], r16w[16], r7n[7], r7w[7];
     if (threadIdx.x < 10) {
         r10n[threadIdx.x] = c_quad.nodes[10][threadIdx.x];
         r10w[threadIdx.x] = c_quad.weights[10][threadIdx.x];
+        if (threadIdx.x < 7) {
+            r7n[threadIdx.x] = c_quad.nodes[7][threadIdx.x];
+            r7w[threadIdx.x] = c_quad.weights[7][threadIdx.x];
+        }
+        if (kMode == 2 && threadIdx.x < 6)
+            for (int m = 3; m <= 6; ++m) {
+                far_rules.n[m - 3][threadIdx.x] = threadIdx.x < m ? c_quad.nodes[m][threadIdx.x] : 0.0;
+                far_rules.w[m - 3][threadIdx.x] = threadIdx.x < m ? c_quad.weights[m][threadIdx.x] : 0.0;
+            }
     }
     if (threadIdx.x < 16) {
         r16n[threadIdx.x] = c_quad.nodes[16][threadIdx.x];
@@ -1031,6 +1010,7 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
             // product rules for pairs far apart: negative order for the
             // orthogonal form
             s_far = kMode != 2 ? 0 : (ortho ? -ortho_rule_order(ctx.o) : far_rule_order(b));
+            s_npanels = sp;  // the break-point panels, for the far rule
         }
         double acc = 0.0, gacc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         long long visited = 0;  // panels popped; bounded so that no input can loop without end
@@ -1040,11 +1020,24 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
             __syncthreads();
             far_m = s_far;
             if (far_m > 0) {
-                const int points = far_m * far_m * far_m * far_m;
-                for (int k = threadIdx.x; k < points; k += kQuadThreads) far_point_coord(ctx, far_m, k, &acc, gacc);
+                // p x p points on each break-point panel, the panels as pushed
+                const int pp = far_m * far_m, points = s_npanels * pp;
+                const double *nd = far_rules.n[far_m - 3], *wt = far_rules.w[far_m - 3];
+                for (int k = threadIdx.x; k < points; k += kQuadThreads) {
+                    const Panel pn = stack[k / pp];
+                    const int a = (k % pp) / far_m, c = k % far_m;
+                    const double hu = 0.5 * (pn.u1 - pn.u0), hv = 0.5 * (pn.v1 - pn.v0);
+                    if (!(hu > 0.0 && hv > 0.0)) continue;
+                    const double uu = 0.5 * (pn.u0 + pn.u1) + hu * nd[a], vv = 0.5 * (pn.v0 + pn.v1) + hv * nd[c];
+                    const double wuv = (hu * wt[a]) * (hv * wt[c]);
+                    double g[8];
+                    integrand_coord(ctx, uu, vv, g);
+                    acc += wuv * g[0];
+                    for (int q = 0; q < 7; ++q) gacc[q] += wuv * g[1 + q];
+                }
             } else if (far_m < 0) {
                 const int mo = -far_m, points = mo * mo * mo * mo;
-                for (int k = threadIdx.x; k < points; k += kQuadThreads) acc += ortho_point(ctx.o, mo, k);
+                for (int k = threadIdx.x; k < points; k += kQuadThreads) acc += ortho_point(ctx.o, far_rules, mo, k);
             }
         }
         for (; !far_m;) {
@@ -1108,7 +1101,8 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
                 s_nleaves = nl;
                 s_done = sp == 0;
                 s_leaf_off[0] = 0;
-                for (int l = 0; l < nl; ++l) s_leaf_off[l + 1] = s_leaf_off[l] + (leaves[l].corner ? 256 : 100);
+                for (int l = 0; l < nl; ++l)
+                    s_leaf_off[l + 1] = s_leaf_off[l] + (leaves[l].corner ? 256 : kMode == 2 ? 49 : 100);
             }
             __syncthreads();
             const int nl = s_nleaves;
@@ -1123,9 +1117,14 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
                     if (!lf.corner) {
                         const double mu = 0.5 * (lf.a0 + lf.a1), hu = 0.5 * (lf.a1 - lf.a0);
                         const double mv = 0.5 * (lf.b0 + lf.b1), hv = 0.5 * (lf.b1 - lf.b0);
-                        const int a = kk / 10, c = kk % 10;
-                        const double uu = mu + hu * r10n[a], wu = hu * r10w[a];
-                        const double vv = mv + hv * r10n[c], wv = hv * r10w[c];
+                        // a direct leaf is no larger than its distance from
+                        // rho = 0, so the nearest singularity lies outside
+                        // the Bernstein ellipse of parameter 3 + 2 sqrt 2 and
+                        // 7 x 7 points leave below 1e-10 of it (the
+                        // reference's 10 x 10 serve the values)
+                        const int a = kk / 7, c = kk % 7;
+                        const double uu = mu + hu * r7n[a], wu = hu * r7w[a];
+                        const double vv = mv + hv * r7n[c], wv = hv * r7w[c];
                         double g[8];
                         integrand_coord(ctx, uu, vv, g);
                         acc += wu * wv * g[0];

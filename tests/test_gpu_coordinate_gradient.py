@@ -179,9 +179,9 @@ def test_near_orthogonal_pair_matches_the_oracle_bar_integral(fh, oracle):
         assert D[k][0, 1] == 0.0 and D[k][1, 0] == 0.0
 
 
-@pytest.mark.parametrize("gap_um,on_side", [(5.0, False), (13.0, False), (5.0, True), (13.0, True)])
+@pytest.mark.parametrize("gap_um,on_side", [(g, side) for g in (5.0, 13.0, 20.0) for side in (False, True)])
 def test_orthogonal_pairs_apart_match_the_oracle_quadrature(fh, oracle, gap_um, on_side):
-    """Long orthogonal boxes whose gap is 2.5 and 6.5 times their largest
+    """Long orthogonal boxes whose gap is 2.5, 6.5 and 10 times their largest
     cross-section side (2 um): too near for point quadrature and rejected by
     the closed form, so the coordinate fill integrates them -- by the product
     rule over both cross-sections of the perpendicular-segment integral.  A

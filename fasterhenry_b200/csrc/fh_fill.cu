@@ -926,7 +926,9 @@ __device__ __forceinline__ double ortho_point(const OrthoBoxes &o, const FarRule
 // height[0], height[1], offset[2]).  kMode 2: values[8 h + 0..7] = the
 // coordinate derivatives of integrand_coord (the work item's flags choose
 // the frame and the rotation axis).  The rule (panel tree, leaves, nodes) is
-// held at the pair's own geometry.  With key_counter the CTAs draw their keys
+// held at the pair's own geometry, except in kMode 1 and 2 for pairs whose
+// cross-sections lie at least one largest side apart (far_rule_order,
+// ortho_rule_order), which take fixed rules.  With key_counter the CTAs draw their keys
 // from it (keys differ widely in cost), else take every gridDim.x-th; in
 // kMode 2 the threads share the points of a batch of leaves evenly (a
 // direct leaf has 100, fewer than the CTA's threads).
@@ -951,7 +953,7 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
             r7n[threadIdx.x] = c_quad.nodes[7][threadIdx.x];
             r7w[threadIdx.x] = c_quad.weights[7][threadIdx.x];
         }
-        if (kMode == 2 && threadIdx.x < 6)
+        if (kMode >= 1 && threadIdx.x < 6)
             for (int m = 3; m <= 6; ++m) {
                 far_rules.n[m - 3][threadIdx.x] = threadIdx.x < m ? c_quad.nodes[m][threadIdx.x] : 0.0;
                 far_rules.w[m - 3][threadIdx.x] = threadIdx.x < m ? c_quad.weights[m][threadIdx.x] : 0.0;
@@ -1009,14 +1011,14 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
                 for (int c = nv - 2; c >= 0; --c) stack[sp++] = Panel{us[a], us[a + 1], vs[c], vs[c + 1], 0, 0};
             // product rules for pairs far apart: negative order for the
             // orthogonal form
-            s_far = kMode != 2 ? 0 : (ortho ? -ortho_rule_order(ctx.o) : far_rule_order(b));
+            s_far = kMode == 0 ? 0 : (ortho ? -ortho_rule_order(ctx.o) : far_rule_order(b));
             s_npanels = sp;  // the break-point panels, for the far rule
         }
         double acc = 0.0, gacc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         long long visited = 0;  // panels popped; bounded so that no input can loop without end
         bool overflow = false;
         int far_m = 0;
-        if (kMode == 2) {
+        if (kMode >= 1) {
             __syncthreads();
             far_m = s_far;
             if (far_m > 0) {
@@ -1030,10 +1032,17 @@ __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
                     if (!(hu > 0.0 && hv > 0.0)) continue;
                     const double uu = 0.5 * (pn.u0 + pn.u1) + hu * nd[a], vv = 0.5 * (pn.v0 + pn.v1) + hv * nd[c];
                     const double wuv = (hu * wt[a]) * (hv * wt[c]);
-                    double g[8];
-                    integrand_coord(ctx, uu, vv, g);
-                    acc += wuv * g[0];
-                    for (int q = 0; q < 7; ++q) gacc[q] += wuv * g[1 + q];
+                    if (kMode == 2) {
+                        double g[8];
+                        integrand_coord(ctx, uu, vv, g);
+                        acc += wuv * g[0];
+                        for (int q = 0; q < 7; ++q) gacc[q] += wuv * g[1 + q];
+                    } else {
+                        double g[7];
+                        integrand_grad(ctx, uu, vv, g);
+                        acc += wuv * g[0];
+                        for (int q = 0; q < 6; ++q) gacc[q] += wuv * g[1 + q];
+                    }
                 }
             } else if (far_m < 0) {
                 const int mo = -far_m, points = mo * mo * mo * mo;

@@ -931,7 +931,7 @@ __device__ __forceinline__ double ortho_point(const OrthoBoxes &o, const FarRule
 // ortho_rule_order), which take fixed rules.  With key_counter the CTAs draw their keys
 // from it (keys differ widely in cost), else take every gridDim.x-th; in
 // kMode 2 the threads share the points of a batch of leaves evenly (a
-// direct leaf has 100, fewer than the CTA's threads).
+// direct leaf has 49 there, fewer than the CTA's threads).
 template <int kMode>
 __global__ void __launch_bounds__(kQuadThreads) aligned_quadrature_kernel(
     const DevFil *__restrict__ fil, const int4 *__restrict__ items, const int64_t *__restrict__ heads,

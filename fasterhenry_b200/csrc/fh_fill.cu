@@ -414,6 +414,62 @@ __device__ __forceinline__ void point_offset(const DevFil &A, const DevFil &B, d
 // The point sum of one pair, scaled to L: mu0/4pi cos(a, b) sum w_a w_b / |p_a - p_b|.
 // The points are placed relative to the centre of A; `delta` is the offset
 // B.centre - A.centre (see point_offset).
+// Two bars of the same half sizes whose frames coincide up to the sign of
+// each axis.
+__device__ __forceinline__ bool same_frame(const DevFil &A, const DevFil &B) {
+    for (int d = 0; d < 3; ++d) {
+        const double *a = A.axes + 3 * d, *b = B.axes + 3 * d;
+        const bool plus = a[0] == b[0] && a[1] == b[1] && a[2] == b[2];
+        const bool minus = a[0] == -b[0] && a[1] == -b[1] && a[2] == -b[2];
+        if (!(plus || minus) || A.half[d] != B.half[d]) return false;
+    }
+    return true;
+}
+
+// The point sum of two such bars with the same orders.  B's node set along
+// each axis is A's (a sign of the axis only relabels a symmetric Gauss set:
+// nodes[n - 1 - k] = -nodes[k], equal weights), so a node pair's separation
+// depends on the per-axis differences x_i - x_j alone, and the pairs (i, j)
+// and (n - 1 - j, n - 1 - i) have the same difference and weight: the sum
+// runs over the n (n + 1) / 2 classes i + j <= n - 1 of each axis, weight
+// doubled off the anti-diagonal, instead of all n^2 pairs (the same terms
+// grouped, in another order).
+__device__ double point_value_same(const DevFil &A, int n0, int n1, int n2, const double *aa, const double bc[3]) {
+    const double h0 = A.half[0], h1 = A.half[1], h2 = A.half[2];
+    double total = 0.0;
+    for (int i0 = 0; i0 < n0; ++i0)
+        for (int j0 = 0; i0 + j0 < n0; ++j0) {
+            const double d0 = h0 * c_quad.nodes[n0][i0] - h0 * c_quad.nodes[n0][j0];
+            const double w0 = (h0 * c_quad.weights[n0][i0]) * (h0 * c_quad.weights[n0][j0]) *
+                              (i0 + j0 == n0 - 1 ? 1.0 : 2.0);
+            double r0[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) r0[d] = aa[d] * d0 - bc[d];
+            double s0 = 0.0;
+            for (int i1 = 0; i1 < n1; ++i1)
+                for (int j1 = 0; i1 + j1 < n1; ++j1) {
+                    const double d1 = h1 * c_quad.nodes[n1][i1] - h1 * c_quad.nodes[n1][j1];
+                    const double w1 = (0.5 * c_quad.weights[n1][i1]) * (0.5 * c_quad.weights[n1][j1]) *
+                                      (i1 + j1 == n1 - 1 ? 1.0 : 2.0);
+                    double r1[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) r1[d] = r0[d] + aa[3 + d] * d1;
+                    double s1 = 0.0;
+                    for (int i2 = 0; i2 < n2; ++i2)
+                        for (int j2 = 0; i2 + j2 < n2; ++j2) {
+                            const double d2 = h2 * c_quad.nodes[n2][i2] - h2 * c_quad.nodes[n2][j2];
+                            const double w2 = (0.5 * c_quad.weights[n2][i2]) * (0.5 * c_quad.weights[n2][j2]) *
+                                              (i2 + j2 == n2 - 1 ? 1.0 : 2.0);
+                            const double dx = r1[0] + aa[6] * d2, dy = r1[1] + aa[7] * d2, dz = r1[2] + aa[8] * d2;
+                            s1 += w2 * rsqrt(dx * dx + dy * dy + dz * dz);
+                        }
+                    s0 += w1 * s1;
+                }
+            total += w0 * s0;
+        }
+    return total;
+}
+
 __device__ __forceinline__ double point_value(const DevFil &A, const DevFil &B, int orders, const double delta[3]) {
     const int oa0 = orders & 31, oa1 = (orders >> 5) & 31, oa2 = (orders >> 10) & 31;
     const int ob0 = (orders >> 15) & 31, ob1 = (orders >> 20) & 31, ob2 = (orders >> 25) & 31;
@@ -424,6 +480,8 @@ __device__ __forceinline__ double point_value(const DevFil &A, const DevFil &B, 
         aa[k] = A.axes[k];
         ba[k] = B.axes[k];
     }
+    if (oa0 == ob0 && oa1 == ob1 && oa2 == ob2 && same_frame(A, B))
+        return kMu0Over4Pi * (point_value_same(A, oa0, oa1, oa2, aa, bc) * ndot(A.axes, B.axes));
     const double ah0 = A.half[0], ah1 = 2.0 * A.half[1], ah2 = 2.0 * A.half[2];
     const double bh0 = B.half[0], bh1 = 2.0 * B.half[1], bh2 = 2.0 * B.half[2];
     double total = 0.0;

@@ -214,12 +214,21 @@ class Geometry:
         if isinstance(seg, dict):
             seg = SegmentDef(seg["a"], seg["b"], seg["width"], seg["height"], seg["sigma"], seg.get("width_dir"))
         idx = len(self.segments)
-        # Validate through the library's own rule (Segment::validate).
-        nodes, segs = _nodes(self.nodes), _segments([seg])
+        # Validate through the library's own rule (Segment::validate).  With
+        # both ends in range only the segment's own two nodes take part (the
+        # nodes are finite by add_node), so they alone are passed; adding a
+        # segment then costs O(1) instead of O(nodes).
+        n = len(self.nodes)
+        if 0 <= seg.a < n and 0 <= seg.b < n:
+            ends = [self.nodes[seg.a]] if seg.a == seg.b else [self.nodes[seg.a], self.nodes[seg.b]]
+            local = dataclasses.replace(seg, a=0, b=0 if seg.a == seg.b else 1)
+            nodes, segs, count = _nodes(ends), _segments([local]), len(ends)
+        else:
+            nodes, segs, count = _nodes(self.nodes), _segments([seg]), n
         disc = _disc({"kind": "uniform", "nw": 1, "nh": 1})[0]
         cnt = ctypes.c_size_t()
         info = N.ErrorInfo()
-        st = N.load().fh_discretize(nodes, len(self.nodes), segs, 1, ctypes.byref(disc), None, 0, ctypes.byref(cnt),
+        st = N.load().fh_discretize(nodes, count, segs, 1, ctypes.byref(disc), None, 0, ctypes.byref(cnt),
                                     None, ctypes.byref(info))
         if st == N.ERR_GEOMETRY:
             msg = N.last_error().replace("segment 0", "segment %d" % idx)

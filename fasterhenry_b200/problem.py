@@ -15,15 +15,21 @@ dialect of fasterhenry-cli/src/inp.rs:1-600 and docs/input-format.md).
   ``.end``; ``*`` comments and ``+`` continuations; directives and node names
   case-insensitive.  Ground planes (fasterhenry-cli/src/inp.rs:53-200,
   2410-2790, 3981-4050, 4329-4398, 4437-4650) in both ``G`` grammars: the
-  FastHenry corner-point form (``x1= .. z3= thick= seg1= seg2= sigma=|rho=
-  nhinc=``, in-plane nodes ``N<name> (x, y, z)``, ``hole rect|point|circle``,
-  ``contact rect`` in its six- and seven-value spellings, ``contact
-  decay_rect``) and the extension form (``G<name> x1 y1 z1 x2 y2 z2 t nx= ny=
-  nhinc= sigma=|rho=`` with ``.hole`` and ``.contact``); the plane meshes come
-  first in the geometry, segment and port endpoints inside a plane's slab
-  (or joined to an in-plane node) land on its nearest live cell centre, and
-  only declared nodes still referenced as themselves are kept.  Other plane
-  clauses are rejected by name with the line number.
+  FastHenry corner-point form (``x1= .. z3= thick= seg1= seg2= segwid1=
+  segwid2= sigma=|rho= nhinc= relx= rely= relz= file=NONE``, in-plane nodes
+  ``N<name> (x, y, z)``, ``hole rect|point|circle``, ``contact rect`` in its
+  six- and seven-value spellings, ``contact decay_rect``, ``contact point``,
+  ``contact line``, ``contact trace`` along x or y, the named contact areas
+  ``contact equiv_rect N<name>`` and ``contact connection N<name>``, and
+  ``contact initial_grid`` / ``initial_mesh_grid``) and the extension form
+  (``G<name> x1 y1 z1 x2 y2 z2 t nx= ny= nhinc= sigma=|rho=`` with ``.hole``
+  and ``.contact``); the plane meshes come first in the geometry, segment and
+  port endpoints inside a plane's slab (or joined to an in-plane node) land
+  on its nearest live cell centre, a named contact area's node on the one
+  node its cells are tied to, and only declared nodes still referenced as
+  themselves are kept.  Other plane clauses (a diagonal ``contact trace``,
+  user-defined hole shapes, hierarchy files, tilted planes) are rejected by
+  name with the statement's line number.
 * :func:`load` picks the reader by file extension (``.inp``/``.fh`` decks,
   anything else JSON), and :func:`run` assembles and sweeps a problem
   (fasterhenry-cli/src/lib.rs:183-230).
@@ -333,6 +339,7 @@ class _PlaneSpec:
     line: int
     mid_z: float
     axis1: int = 0
+    bar_width: Tuple[Optional[float], Optional[float]] = (None, None)
 
 
 def _plane_extension(head: str, toks: List[str], line: int, unit: float, sigma_default) -> _PlaneSpec:
@@ -366,69 +373,327 @@ def _plane_sigma(vals, line, unit, sigma_default, head):
     return sigma_default
 
 
+def _finite(tok: str, line: int) -> float:
+    v = _number(tok, line)
+    if not math.isfinite(v):
+        raise DeckError(line, "'%s' is not finite" % tok)
+    return v
+
+
+def _deck_count(text: str, what: str, line: int) -> int:
+    """A whole number >= 1 (inp.rs:956-967 parse_count)."""
+    if not re.fullmatch(r"\+?[0-9]+", text):
+        raise DeckError(line, "'%s' is not a valid %s (a whole number >= 1)" % (text, what))
+    v = int(text)
+    if v < 1:
+        raise DeckError(line, "%s must be >= 1, got %d" % (what, v))
+    return v
+
+
+def _shown(x: float) -> str:
+    """A length in a message: shortest round-trip digits, positional (the
+    reference prints its f64 values that way)."""
+    import numpy as np
+    return np.format_float_positional(x, unique=True, trim="-")
+
+
+def _clause_values(text: str) -> List[str]:
+    """A clause's value list: fields separated by commas, whitespace or
+    both, empty fields dropped (inp.rs:1073-1124 read_list)."""
+    return [v for v in re.split(r"[\s,]+", text.strip()) if v]
+
+
+def _node_fields(text: str) -> List[str]:
+    """An in-plane node's value list with its empty fields kept ("" for a
+    field between two commas, or after a trailing one)."""
+    parts = text.split(",")
+    out: List[str] = []
+    for part in parts:
+        words = part.split()
+        if words:
+            out.extend(words)
+        elif len(parts) > 1:
+            out.append("")
+    return out
+
+
+# The clauses of a corner-point G statement and what they carry, as the
+# reference's reader accepts them (inp.rs:2061-2168 apply_clause).
+_CONTACT_SHAPES = ("'contact rect (x, y, z, xwidth, ywidth, xcell, ycell)' or '(x1, y1, z1, x2, y2, z2)', "
+                   "'contact decay_rect (x, y, z, xwidth, ywidth, xcell, ycell, xmaxcell, ymaxcell)', "
+                   "'contact point (x, y, z, xcell, ycell)', 'contact line (x0, y0, z0, x1, y1, z1, xcell, ycell)', "
+                   "'contact trace (x0, y0, z0, x1, y1, z1, trace_width, scale_factor)' along x or y, "
+                   "'contact equiv_rect N<name> (x, y, z, xwidth, ywidth)', "
+                   "'contact connection N<name> (x, y, z, xwidth, ywidth, ratio)', "
+                   "'contact initial_grid (n1, n2)' and 'contact initial_mesh_grid (n1, n2)'")
+
+
+@dataclasses.dataclass
+class _Refine:
+    """A `contact point` / `line` (and each of a trace's five lines): the
+    locus's two ends (x, y, z) and the largest cell wanted, in the plane's
+    own (p1->p2, p2->p3) axes."""
+    ends: List[List[float]]
+    cell: List[float]
+
+
+def _trace_lines(ends, width: float, along: int, axis1: int) -> List[_Refine]:
+    """The documented expansion of an axis-aligned `contact trace` into five
+    `contact line`s (inp.rs:1552-1579): at offsets 0 and +-w/2 across the
+    trace with cells (length, w/2), and at +-3w/2 with cells (length, w)."""
+    across = 1 - along
+    length = abs(ends[1][along] - ends[0][along])
+    along_slot = 0 if along == axis1 else 1
+    out = []
+    for offset, across_cell in ((0.0, width / 2.0), (width / 2.0, width / 2.0), (-width / 2.0, width / 2.0),
+                                (1.5 * width, width), (-1.5 * width, width)):
+        moved = [list(e) for e in ends]
+        for e in moved:
+            e[across] += offset
+        cell = [0.0, 0.0]
+        cell[along_slot] = length
+        cell[1 - along_slot] = across_cell
+        out.append(_Refine(moved, cell))
+    return out
+
+
 def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_default):
-    """The FastHenry corner-point G statement (inp.rs:1686-2790) in this
-    reader's subset.  Returns the plane and its in-plane nodes
-    [(name, position)]."""
+    """The FastHenry corner-point G statement (inp.rs:1686-2790).  Returns the
+    plane and its in-plane nodes [(name, position, equipotential index or
+    None)]; a node that a `contact equiv_rect` / `contact connection`
+    declares names its contact area, the others attach to the nearest live
+    cell.  Corner points, `thick`, `seg1`/`seg2` (or `contact initial_grid`),
+    `segwid1`/`segwid2`, `sigma`/`rho`, `nhinc`, `relx`/`rely`/`relz` and
+    `file=NONE` are read; every other field or clause is rejected by name."""
     items = _plane_items(body, line)
+    # relx / rely / relz move every node, hole and contact coordinate of the
+    # statement (not its corner points), wherever they are written; the last
+    # value of a repeated key wins (inp.rs:1982-2001).
+    offset = [0.0, 0.0, 0.0]
+    for kind, text in items:
+        if kind == "key":
+            key, val = text.split("=", 1)
+            if key in ("relx", "rely", "relz"):
+                offset["xyz".index(key[3])] = _finite(val, line) * unit
+
+    def triple(vals, what):
+        return [_finite(v, line) * unit + offset[a] for a, v in enumerate(vals[:3])]
+
+    def widths_of(vals, what):
+        out = []
+        for a in range(2):
+            w = _finite(vals[3 + a], line) * unit
+            if w <= 0:
+                raise DeckError(line, "%s: %swidth=%s must be > 0 - it is the rectangle's full width about its "
+                                      "centre, not a corner" % (what, "xy"[a], _shown(w)))
+            out.append(w)
+        return out
+
+    def node_name(name, what):
+        if name is None:
+            raise DeckError(line, "%s names the node it ties: write it as '%s N<name> (...)'"
+                            % (what, what.strip("'")))
+        if not name.lower().startswith("n"):
+            raise DeckError(line, "%s: '%s' is not a node name (node names start with 'N', as in '%s Ncontact "
+                                  "(...)')" % (what, name, what.strip("'")))
+        return name.lower()
+
     keys: Dict[str, str] = {}
-    nodes: List[Tuple[str, Tuple[float, float, float]]] = []
-    hole_rects, hole_points, hole_circles, contact_rects, contact_decays = [], [], [], [], []
+    seg: List[Optional[int]] = [None, None]
+    initial_grid: Optional[str] = None
+    meshed_grid = False
+    segwid: List[Optional[float]] = [None, None]
+    file_none = False
+    nodes: List[Tuple[str, List[float], Optional[int]]] = []
+    hole_rects, hole_points, hole_circles = [], [], []
+    contact_rects, contact_decays, contact_lines, contact_traces, contact_equivs = [], [], [], [], []
+    corner_keys = {"%s%d" % (a, i) for a in "xyz" for i in (1, 2, 3)}
     k = 0
     while k < len(items):
         kind, text = items[k]
         if kind == "key":
             key, val = text.split("=", 1)
-            if key in keys:
-                raise DeckError(line, "ground plane '%s' gives '%s' twice" % (head, key))
-            keys[key] = val
+            if key in ("seg1", "seg2"):
+                if initial_grid is not None:
+                    raise DeckError(line, "ground plane '%s': '%s' and %s both set this plane's cell counts (%s's "
+                                          "values are seg1 and seg2), so give one or the other"
+                                    % (head, key, initial_grid, initial_grid))
+                seg[key == "seg2"] = _deck_count(val, key, line)
+            elif key in ("segwid1", "segwid2"):
+                w = _finite(val, line) * unit
+                if w <= 0:
+                    raise DeckError(line, "ground plane '%s': '%s' needs a width > 0 (got '%s=%s')"
+                                    % (head, key, key, val))
+                segwid[key == "segwid2"] = w
+            elif key == "file":
+                if val.upper() != "NONE":
+                    raise DeckError(line, "ground plane '%s': 'file=%s' names a nonuniform-discretization file, "
+                                          "which this reader does not read (only 'file=NONE' is accepted); give "
+                                          "the discretization on the statement with 'seg1'/'seg2' or 'contact "
+                                          "initial_grid (n1, n2)' and the contact clauses" % (head, val))
+                file_none = True
+            elif key == "rh":
+                raise DeckError(line, "ground plane '%s': 'rh' (filaments graded through the thickness) is not "
+                                      "supported; plane filaments are uniform, so use 'nhinc' alone" % head)
+            elif key in ("nx", "ny"):
+                raise DeckError(line, "ground plane '%s': the corner-point form counts cells with 'seg1'/'seg2' "
+                                      "('%s' belongs to the 'G<name> x1 y1 z1 x2 y2 z2 t' extension form)"
+                                % (head, key))
+            elif key in corner_keys or key in ("thick", "sigma", "rho", "nhinc", "relx", "rely", "relz"):
+                keys[key] = val
+            else:
+                raise DeckError(line, "unknown ground-plane parameter '%s' (supported: x1..z3, thick, seg1, seg2, "
+                                      "segwid1, segwid2, sigma, rho, nhinc, relx, rely, relz, file=NONE)" % key)
             k += 1
             continue
         if kind == "group":
             raise DeckError(line, "ground plane '%s': a value list '(%s)' belongs to no clause" % (head, text))
-        word = text.lower()
-        if word.startswith("n") and k + 1 < len(items) and items[k + 1][0] == "group":
-            xyz = _group_values(items[k + 1][1], line, unit)
-            if len(xyz) != 3:
-                raise DeckError(line, "in-plane node '%s' needs (x, y, z)" % text)
-            nodes.append((word, tuple(xyz)))
+        low = text.lower()
+        if low in ("hole", "contact"):
+            if k + 1 >= len(items) or items[k + 1][0] != "word":
+                raise DeckError(line, "'%s' needs a shape name, as in '%s rect (...)'" % (low, low))
+            shape = items[k + 1][1].lower()
+            what = "'%s %s'" % (low, shape)
+            name = None
+            j = k + 2
+            if j + 1 < len(items) and items[j][0] == "word" and items[j + 1][0] == "group":
+                name = items[j][1]
+                j += 1
+            if j >= len(items) or items[j][0] != "group":
+                raise DeckError(line, "%s needs a parenthesised value list, as in '(x, y, z)'" % what)
+            vals = _clause_values(items[j][1])
+            k = j + 1
+            if name is not None and (low, shape) not in (("contact", "equiv_rect"), ("contact", "connection")):
+                raise DeckError(line, "%s takes no node name, but '%s' stands before its value list; only "
+                                      "'contact equiv_rect' and 'contact connection' name a node" % (what, name))
+
+            def arity(n, form):
+                if len(vals) != n:
+                    raise DeckError(line, "%s takes %d values (%s), got %d" % (what, n, form, len(vals)))
+
+            if low == "hole" and shape == "rect":
+                arity(6, "x1, y1, z1, x2, y2, z2")
+                hole_rects.append((triple(vals[:3], what), triple(vals[3:6], what)))
+            elif low == "hole" and shape == "point":
+                arity(3, "x, y, z")
+                hole_points.append(triple(vals, what))
+            elif low == "hole" and shape == "circle":
+                arity(4, "x, y, z, r")
+                r = _finite(vals[3], line) * unit
+                if r < 0:
+                    raise DeckError(line, "%s: r=%s metres must be >= 0" % (what, _shown(r)))
+                hole_circles.append((triple(vals, what), r))
+            elif low == "contact" and shape == "rect" and len(vals) == 7:
+                contact_decays.append(("'contact rect'", triple(vals, what),
+                                       [_finite(v, line) * unit for v in vals[3:7]] + [-1.0, -1.0]))
+            elif low == "contact" and shape == "rect" and len(vals) == 6:
+                contact_rects.append((triple(vals[:3], what), triple(vals[3:6], what)))
+            elif low == "contact" and shape == "rect":
+                raise DeckError(line, "'contact rect' takes 7 values (x, y, z, xwidth, ywidth, xcell, ycell) or 6 "
+                                      "(x1, y1, z1, x2, y2, z2), got %d" % len(vals))
+            elif low == "contact" and shape == "decay_rect":
+                arity(9, "x, y, z, xwidth, ywidth, xcell, ycell, xmaxcell, ymaxcell")
+                v = [_finite(x, line) * unit for x in vals[3:9]]
+                contact_decays.append(("'contact decay_rect'", triple(vals, what),
+                                       v[:4] + [v[4] if v[4] >= 0 else -1.0, v[5] if v[5] >= 0 else -1.0]))
+            elif low == "contact" and shape in ("point", "line"):
+                n = 5 if shape == "point" else 8
+                arity(n, "x, y, z, xcell, ycell" if shape == "point" else "x0, y0, z0, x1, y1, z1, xcell, ycell")
+                first = triple(vals[:3], what)
+                ends = [first, list(first)] if shape == "point" else [first, triple(vals[3:6], what)]
+                cell = [_finite(x, line) * unit for x in vals[n - 2:n]]
+                for a in range(2):
+                    if cell[a] <= 0:
+                        raise DeckError(line, "%s: %scell=%s metres must be > 0 - it is the largest cell wanted "
+                                              "along the %s" % (what, "xy"[a], _shown(cell[a]), shape))
+                contact_lines.append((what, _Refine(ends, cell)))
+            elif low == "contact" and shape == "trace":
+                arity(8, "x0, y0, z0, x1, y1, z1, trace_width, scale_factor")
+                ends = [triple(vals[:3], what), triple(vals[3:6], what)]
+                width = _finite(vals[6], line) * unit
+                if width <= 0:
+                    raise DeckError(line, "%s: trace_width=%s metres must be > 0" % (what, _shown(width)))
+                scale = _finite(vals[7], line)
+                if scale <= 0:
+                    raise DeckError(line, "%s: scale_factor=%s must be > 0 - it magnifies the cells under the "
+                                          "trace" % (what, _shown(scale)))
+                dx, dy = abs(ends[1][0] - ends[0][0]), abs(ends[1][1] - ends[0][1])
+                if dx == 0.0 and dy == 0.0:
+                    raise DeckError(line, "%s has zero length, so it has no direction to refine across; use "
+                                          "'contact point (x, y, z, xcell, ycell)' for a point" % what)
+                if dy <= 1e-9 * dx:
+                    along = 0
+                elif dx <= 1e-9 * dy:
+                    along = 1
+                else:
+                    raise DeckError(line, "%s from (%s, %s) to (%s, %s) metres is not parallel to x or y; a "
+                                          "diagonal 'contact trace' is not supported, because its published "
+                                          "description does not fix the cell size under it. Refine under it with "
+                                          "'contact line (x0, y0, z0, x1, y1, z1, xcell, ycell)', which refines a "
+                                          "diagonal line's bounding box to the cell you choose"
+                                    % (what, _shown(ends[0][0]), _shown(ends[0][1]), _shown(ends[1][0]),
+                                       _shown(ends[1][1])))
+                contact_traces.append((ends, width, along))
+            elif low == "contact" and shape in ("equiv_rect", "connection"):
+                n = 5 if shape == "equiv_rect" else 6
+                arity(n, "x, y, z, xwidth, ywidth" + ("" if n == 5 else ", ratio"))
+                centre, widths = triple(vals, what), widths_of(vals, what)
+                if shape == "connection":
+                    ratio = _finite(vals[5], line)
+                    if ratio <= 1.0:
+                        raise DeckError(line, "%s: ratio=%s must be > 1 - it divides the rectangle's widths into "
+                                              "the contact's own cells (xwidth/ratio, ywidth/ratio)"
+                                        % (what, _shown(ratio)))
+                nm = node_name(name, what)
+                contact_equivs.append((what, nm, centre, widths))
+                if shape == "connection":
+                    # an equiv_rect plus a decay_rect over the same rectangle
+                    # with cells widths / ratio and no outward limit
+                    contact_decays.append(("'contact connection'", centre,
+                                           widths + [widths[0] / ratio, widths[1] / ratio, -1.0, -1.0]))
+            elif low == "contact" and shape in ("initial_grid", "initial_mesh_grid"):
+                arity(2, "cells along p1->p2, cells along p2->p3: what 'seg1' and 'seg2' set")
+                if initial_grid is not None:
+                    raise DeckError(line, "ground plane '%s': %s sets the initial discretization %s has already "
+                                          "set on this statement; give one of the two clauses"
+                                    % (head, what, initial_grid))
+                if seg[0] is not None or seg[1] is not None:
+                    raise DeckError(line, "ground plane '%s': %s and 'seg1'/'seg2' both set this plane's cell "
+                                          "counts (its values are seg1 and seg2), so give one or the other"
+                                    % (head, what))
+                seg = [_deck_count(vals[0], "cell count along p1->p2", line),
+                       _deck_count(vals[1], "cell count along p2->p3", line)]
+                initial_grid = what
+                meshed_grid = shape == "initial_mesh_grid"
+            elif low == "contact" and shape == "circle":
+                raise DeckError(line, "ground plane '%s': 'contact circle' is not supported, and no contact shape "
+                                      "of that name is documented ('circle' is a hole shape: 'hole circle (x, y, "
+                                      "z, r)'); refine the disc's bounding square instead with 'contact decay_rect "
+                                      "(x, y, z, 2r, 2r, xcell, ycell, xmaxcell, ymaxcell)', or use 'contact point "
+                                      "(x, y, z, xcell, ycell)' at its centre" % head)
+            elif low == "hole":
+                raise DeckError(line, "ground plane '%s': 'hole %s' is not supported; the holes are 'hole rect "
+                                      "(x1, y1, z1, x2, y2, z2)', 'hole point (x, y, z)' and 'hole circle (x, y, "
+                                      "z, r)'" % (head, shape))
+            else:
+                raise DeckError(line, "ground plane '%s': 'contact %s' is not supported; the contacts are %s"
+                                % (head, shape, _CONTACT_SHAPES))
+            continue
+        if k + 1 < len(items) and items[k + 1][0] == "group":
+            if not low.startswith("n"):
+                raise DeckError(line, "'%s (...)' is not an in-plane node declaration: node names start with 'N'"
+                                % text)
+            fields = _node_fields(items[k + 1][1])
+            if any(f == "" for f in fields):
+                raise DeckError(line, "in-plane node '%s' has an empty coordinate field; write every coordinate "
+                                      "(x, y, z)" % text)
+            if len(fields) != 3:
+                raise DeckError(line, "in-plane node '%s' needs (x, y, z), got %d values" % (text, len(fields)))
+            nodes.append((low, triple(fields, "in-plane node '%s'" % text), None))
             k += 2
             continue
-        if word in ("hole", "contact"):
-            if k + 2 >= len(items) or items[k + 1][0] != "word" or items[k + 2][0] != "group":
-                raise DeckError(line, "ground plane '%s': '%s' needs a shape and its values, e.g. "
-                                      "'%s rect (x1, y1, z1, x2, y2, z2)'" % (head, word, word))
-            shape = items[k + 1][1].lower()
-            vals = _group_values(items[k + 2][1], line, 1.0)
-            k += 3
-            if word == "hole" and shape == "rect" and len(vals) == 6:
-                hole_rects.append([v * unit for v in vals])
-            elif word == "hole" and shape == "point" and len(vals) == 3:
-                hole_points.append([v * unit for v in vals])
-            elif word == "hole" and shape == "circle" and len(vals) == 4:
-                hole_circles.append([v * unit for v in vals])
-            elif word == "contact" and shape == "rect" and len(vals) == 6:
-                contact_rects.append([v * unit for v in vals])
-            elif word == "contact" and shape == "rect" and len(vals) == 7:
-                contact_decays.append(("'contact rect'", [v * unit for v in vals[:7]] + [-1.0, -1.0]))
-            elif word == "contact" and shape == "decay_rect" and len(vals) == 9:
-                v = [x * unit for x in vals[:7]] + [vals[7] * unit if vals[7] >= 0 else -1.0,
-                                                    vals[8] * unit if vals[8] >= 0 else -1.0]
-                contact_decays.append(("'contact decay_rect'", v))
-            elif word == "contact" and shape == "rect":
-                raise DeckError(line, "'contact rect' takes seven values (x, y, z, xwidth, ywidth, xcell, ycell) "
-                                      "or six (x1, y1, z1, x2, y2, z2), got %d" % len(vals))
-            else:
-                raise DeckError(line, "ground plane '%s': '%s %s' with %d values is not read by this front end "
-                                      "(supported: hole rect/point/circle, contact rect, contact decay_rect)"
-                                % (head, word, shape, len(vals)))
-            continue
-        raise DeckError(line, "ground plane '%s': '%s' is not read by this front end" % (head, text))
-    allowed = {"x1", "y1", "z1", "x2", "y2", "z2", "x3", "y3", "z3", "thick", "seg1", "seg2", "sigma", "rho",
-               "nhinc"}
-    for key in keys:
-        if key not in allowed:
-            raise DeckError(line, "ground plane '%s': '%s=' is not read by this front end" % (head, key))
+        raise DeckError(line, "'%s' is not a ground-plane parameter (expected <field>=<value>, 'N<name> (x, y, z)', "
+                              "'hole <shape> (...)' or 'contact <shape> (...)')" % text)
     if "sigma" in keys and "rho" in keys:
         raise DeckError(line, "give either sigma= or rho=, not both")
     pts = []
@@ -455,53 +720,127 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
     a1, a2 = axis_of(e1), axis_of(e2)
     if a1 is None or a2 is None or a1 == a2:
         raise DeckError(line, "ground plane '%s': the corner points do not form an axis-aligned rectangle" % head)
-    for key in ("seg1", "seg2", "thick"):
-        if key not in keys:
-            raise DeckError(line, "ground plane '%s' has no '%s'" % (head, key))
+    for i in (0, 1):
+        if seg[i] is None:
+            raise DeckError(line, "ground plane '%s' has no 'seg%d' (cells along %s)"
+                            % (head, i + 1, ("p1->p2", "p2->p3")[i]))
     cells = [0, 0]
-    cells[a1] = int(_number(keys["seg1"], line))
-    cells[a2] = int(_number(keys["seg2"], line))
-    thick = _number(keys["thick"], line) * unit
+    cells[a1], cells[a2] = seg[0], seg[1]
+    if "thick" not in keys:
+        raise DeckError(line, "ground plane '%s' has no 'thick' (its thickness)" % head)
+    thick = abs(_finite(keys["thick"], line)) * unit
     if thick <= 0:
         raise DeckError(line, "ground plane '%s' needs a thickness > 0" % head)
     sigma = _plane_sigma(keys, line, unit, sigma_default, head)
-    nhinc = int(_number(keys.get("nhinc", "1"), line))
+    nhinc = _deck_count(keys["nhinc"], "nhinc", line) if "nhinc" in keys else 1
     lo = (min(p[0] for p in pts), min(p[1] for p in pts))
     hi = (max(p[0] for p in pts), max(p[1] for p in pts))
+    origin = (pts[0][0], pts[0][1])
     mid_z = pts[0][2]
 
     def in_slab(what, z):
         if abs(z - mid_z) > thick + 1e-15:
             raise DeckError(line, "%s: z=%r is not in ground plane '%s'" % (what, z, head))
 
+    def contains(p):
+        return lo[0] - tol <= p[0] <= hi[0] + tol and lo[1] - tol <= p[1] <= hi[1] + tol
+
+    def on_plane(what, p):
+        in_slab(what, p[2])
+        if not contains(p):
+            raise DeckError(line, "%s: (%s, %s) metres is outside ground plane '%s'"
+                            % (what, _shown(p[0]), _shown(p[1]), head))
+
     def plane_pair(pair):
         return list(pair) if a1 == 0 else [pair[1], pair[0]]
 
+    def background(a):
+        return (hi[a] - lo[a]) / cells[a]
+
+    def footprint(what, corners):
+        in_slab(what, corners[0][2])
+        in_slab(what, corners[1][2])
+        rlo = (min(corners[0][0], corners[1][0]), min(corners[0][1], corners[1][1]))
+        rhi = (max(corners[0][0], corners[1][0]), max(corners[0][1], corners[1][1]))
+        if not (rhi[0] > rlo[0] and rhi[1] > rlo[1]):
+            raise DeckError(line, "%s is degenerate: its two corners share an x or a y" % what)
+        return rlo, rhi
+
     def misses(rlo, rhi):
-        return rhi[0] < lo[0] or rlo[0] > hi[0] or rhi[1] < lo[1] or rlo[1] > hi[1]
+        return any(rhi[a] < lo[a] - tol or rlo[a] > hi[a] + tol for a in range(2))
+
+    def touches(rlo, rhi):
+        return any(min(rhi[a], hi[a]) - max(rlo[a], lo[a]) <= PL.contact_slack(lo[a], hi[a]) for a in range(2))
+
+    def refine_region(refine):
+        """The region a refinement locus asks for (inp.rs:3201-3246): its
+        bounding box padded by half a cell, cut into cells no coarser than
+        the cell, graded outward at ratio 2.  An axis the background already
+        meets spans the whole plane at its own cell count; None when both
+        axes are met or the region misses the plane."""
+        want = plane_pair(refine.cell)
+        rlo, rhi, count = [0.0, 0.0], [0.0, 0.0], [0, 0]
+        met = True
+        for a in range(2):
+            if want[a] >= background(a) * (1.0 - 1e-9):
+                rlo[a], rhi[a], count[a] = lo[a], hi[a], cells[a]
+                continue
+            met = False
+            p, q = refine.ends[0][a], refine.ends[1][a]
+            rlo[a] = min(p, q) - want[a] / 2.0
+            rhi[a] = max(p, q) + want[a] / 2.0
+            count[a] = PL.cells_no_coarser_than(rhi[a] - rlo[a], want[a])
+        if met or touches(rlo, rhi):
+            return None
+        return PL.ContactRegion.new(rlo, rhi, count, 2.0)
+
+    nonuniform = (file_none or initial_grid is not None or
+                  bool(contact_rects or contact_decays or contact_lines or contact_traces or contact_equivs))
+    bar_width: List[Optional[float]] = [None, None]
+    for i, width in enumerate(segwid):
+        if width is None:
+            continue
+        if nonuniform:
+            raise DeckError(line, "ground plane '%s': 'segwid%d' needs a uniform plane, but this plane's mesh is "
+                                  "nonuniform ('file=NONE', 'contact initial_grid' or a 'contact' clause); drop "
+                                  "'segwid%d'" % (head, i + 1, i + 1))
+        bar_width[a1 if i == 0 else 1 - a1] = width
 
     holes = []
-    for v in hole_rects:
-        in_slab("'hole rect'", v[2])
-        in_slab("'hole rect'", v[5])
-        holes.append(PL.Hole.rect((min(v[0], v[3]), min(v[1], v[4])), (max(v[0], v[3]), max(v[1], v[4]))))
-    for v in hole_points:
-        in_slab("'hole point'", v[2])
-        holes.append(PL.Hole.point((v[0], v[1])))
-    for v in hole_circles:
-        in_slab("'hole circle'", v[2])
-        holes.append(PL.Hole.circle((v[0], v[1]), v[3]))
+    if meshed_grid:
+        # the checkerboard of `contact initial_mesh_grid` (inp.rs:2876-2911):
+        # every cell whose two 1-based indices, counted from the p1 corner,
+        # are even; cut into the initial grid before any refinement
+        def holed(a):
+            ascending = abs(origin[a] - lo[a]) <= abs(hi[a] - origin[a])
+            out = []
+            for index in range(1, cells[a], 2):
+                from_lo = index if ascending else cells[a] - 1 - index
+                out.append((lo[a] + from_lo * background(a), lo[a] + (from_lo + 1) * background(a)))
+            return out
+        for x0, x1 in holed(0):
+            for y0, y1 in holed(1):
+                holes.append(PL.Hole.rect((x0, y0), (x1, y1)))
+    for corners in hole_rects:
+        rlo, rhi = footprint("'hole rect'", corners)
+        holes.append(PL.Hole.rect(rlo, rhi))
+    for p in hole_points:
+        in_slab("'hole point'", p[2])
+        holes.append(PL.Hole.point((p[0], p[1])))
+    for p, r in hole_circles:
+        in_slab("'hole circle'", p[2])
+        holes.append(PL.Hole.circle((p[0], p[1]), r))
+    # contacts wholly outside the footprint, or only touching its boundary,
+    # refine nothing and are dropped (inp.rs:2695-2760)
     contacts = []
-    for v in contact_rects:
-        in_slab("'contact rect'", v[2])
-        in_slab("'contact rect'", v[5])
-        rlo, rhi = (min(v[0], v[3]), min(v[1], v[4])), (max(v[0], v[3]), max(v[1], v[4]))
-        if misses(rlo, rhi):
+    for corners in contact_rects:
+        rlo, rhi = footprint("'contact rect'", corners)
+        if misses(rlo, rhi) or touches(rlo, rhi):
             continue
         contacts.append(PL.ContactRegion.new(rlo, rhi, (2, 2), 2.0))
-    for what, v in contact_decays:
-        in_slab(what, v[2])
-        widths, cell, limit = plane_pair(v[3:5]), plane_pair(v[5:7]), plane_pair(v[7:9])
+    for what, centre, v in contact_decays:
+        in_slab(what, centre[2])
+        widths, cell, limit = plane_pair(v[0:2]), plane_pair(v[2:4]), plane_pair(v[4:6])
         rlo, rhi, rc, ratio = [0.0, 0.0], [0.0, 0.0], [0, 0], [0.0, 0.0]
         for a in range(2):
             if not cell[a] > 0:
@@ -509,21 +848,44 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
             if not cell[a] < widths[a]:
                 raise DeckError(line, "%s: a cell must be smaller than the rectangle's width" % what)
             half = widths[a] / 2.0
-            rlo[a] = v[a] - half
-            rhi[a] = v[a] + half
+            rlo[a] = centre[a] - half
+            rhi[a] = centre[a] + half
             rc[a] = PL.cells_no_coarser_than(widths[a], cell[a])
             ratio[a] = 1.0 / (1.0 - cell[a] / widths[a])
-            background = (hi[a] - lo[a]) / cells[a]
-            if limit[a] >= 0 and limit[a] < background * (1.0 - 1e-9):
+            if limit[a] >= 0 and limit[a] < background(a) * (1.0 - 1e-9):
                 raise DeckError(line, "%s: a maxcell finer than ground plane '%s''s background cell (%r metres) "
-                                      "is not supported; raise seg1/seg2" % (what, head, background))
-        if misses(rlo, rhi):
+                                      "is not supported; raise seg1/seg2" % (what, head, background(a)))
+        if misses(rlo, rhi) or touches(rlo, rhi):
             continue
         contacts.append(PL.ContactRegion.graded_per_axis(rlo, rhi, rc, ratio))
-    for name, pos in nodes:
+    for what, refine in contact_lines:
+        for p in refine.ends:
+            on_plane(what, p)
+        region = refine_region(refine)
+        if region is not None:
+            contacts.append(region)
+    for ends, width, along in contact_traces:
+        for p in ends:
+            on_plane("'contact trace'", p)
+        for refine in _trace_lines(ends, width, along, a1):
+            region = refine_region(refine)
+            if region is not None:
+                contacts.append(region)
+    # a named contact area: one equipotential patch plus the in-plane node
+    # that names it, at the rectangle's centre (inp.rs:2762-2776)
+    equipotentials = []
+    for what, name, centre, widths in contact_equivs:
+        in_slab(what, centre[2])
+        equipotentials.append(PL.Equipotential.centred((centre[0], centre[1]), plane_pair(widths)))
+        nodes.append((name, centre, len(equipotentials) - 1))
+    for name, pos, _ in nodes:
+        if not contains(pos):
+            raise DeckError(line, "in-plane node '%s' at (%s, %s) metres is outside ground plane '%s'"
+                            % (name, _shown(pos[0]), _shown(pos[1]), head))
         in_slab("in-plane node '%s'" % name, pos[2])
-    plane = PL.GroundPlane(lo, hi, mid_z + thick / 2.0, thick, cells[0], cells[1], sigma, holes, contacts)
-    return _PlaneSpec(head, plane, nhinc, line, mid_z, a1), nodes
+    plane = PL.GroundPlane(lo, hi, mid_z + thick / 2.0, thick, cells[0], cells[1], sigma, holes, contacts,
+                           equipotentials)
+    return _PlaneSpec(head, plane, nhinc, line, mid_z, a1, (bar_width[0], bar_width[1])), nodes
 
 
 def parse_deck(text: str) -> Problem:
@@ -548,6 +910,7 @@ def parse_deck(text: str) -> Problem:
     ended = False
     planes: List[_PlaneSpec] = []
     plane_node: Dict[str, int] = {}        # in-plane node name -> plane index
+    contact_area: Dict[str, int] = {}      # contact-area node name -> its equipotential on that plane
 
     def resolve(name: str, line: int) -> str:
         key = name.lower()
@@ -721,12 +1084,14 @@ def parse_deck(text: str) -> Problem:
                 planes.append(_plane_extension(head, _tokens(rest), line, unit, default_sigma(line)))
             else:
                 spec, pnodes = _plane_corner_form(head, rest, line, unit, default_sigma(line))
-                for name, pos in pnodes:
+                for name, pos, area in pnodes:
                     if name in node_index or name in alias:
                         raise DeckError(line, "node '%s' is declared twice" % name)
                     node_index[name] = len(positions)
-                    positions.append(pos)
+                    positions.append(tuple(pos))
                     plane_node[name] = len(planes)
+                    if area is not None:
+                        contact_area[name] = area
                 planes.append(spec)
             continue
         if low in (".hole", ".contact"):
@@ -768,24 +1133,46 @@ def parse_deck(text: str) -> Problem:
     plane_grids: List[Tuple[int, int, float, float]] = []
     for pl in planes:
         try:
-            centres = pl.plane.build_into(geometry)
+            centres = pl.plane.build_into(geometry, pl.bar_width)
         except PL.PlaneError as e:
             raise DeckError(pl.line, str(e)) from None
         meshes.append(centres)
         plane_grids += [(1, pl.nhinc, 1.0, 1.0)] * (len(geometry.segments) - len(plane_grids))
-    owner: Dict[str, Tuple[int, Tuple[float, float, float]]] = {}
+
+    def area_node(nm: str) -> int:
+        """The tie node of a named contact area (inp.rs:4663-4693); an area
+        that holds no live cell centre is an error whether or not anything
+        references it."""
+        k = plane_node[nm]
+        node = planes[k].plane.equipotential_node(meshes[k], contact_area[nm])
+        if node is None:
+            raise DeckError(planes[k].line, "ground plane '%s': the contact area named here covers no live cell of "
+                                            "the plane's mesh, so it ties nothing; widen it, or refine the mesh so "
+                                            "a cell centre falls inside it" % planes[k].name)
+        return node
+
+    for nm in sorted(contact_area, key=lambda k: node_index[k]):
+        area_node(nm)
+    # the in-plane node each .equiv class attaches through (inp.rs:4695-4731):
+    # the first in declaration order, except that a named contact area wins
+    # over a plain in-plane node of the same plane
+    owner: Dict[str, str] = {}
     for nm, k in sorted(plane_node.items(), key=lambda kv: node_index[kv[0]]):
         canon = alias.get(nm, nm)
-        if canon in owner and owner[canon][0] != k:
+        if canon in owner and plane_node[owner[canon]] != k:
             raise DeckError(0, ".equiv joins in-plane nodes of two different ground planes; connect the planes "
                                "with a segment instead")
-        owner.setdefault(canon, (k, positions[node_index[nm]]))
+        if canon not in owner or (owner[canon] not in contact_area and nm in contact_area):
+            owner[canon] = nm
 
     def snapped(nm: str) -> Optional[int]:
         canon = alias.get(nm, nm)
         if canon in owner:
-            k, pos = owner[canon]
-            return planes[k].plane.attach(meshes[k], pos)
+            pnode = owner[canon]
+            if pnode in contact_area:
+                return area_node(pnode)
+            k = plane_node[pnode]
+            return planes[k].plane.attach(meshes[k], positions[node_index[pnode]])
         pos = positions[node_index[canon]]
         for k, pl in enumerate(planes):
             if pl.plane.contains(pos, 0.0):

@@ -117,7 +117,7 @@ E2 N3 N4 group=right
     (".units mm\nN1 x=0\n.bogus\n.end", 3, "not in the deck subset"),
     (".units mm\nN1 x=0\nGplane x1=0\n.end", 3, "is missing 'y1'"),
     (".units mm\nGp 0 0 0 1 1 0 0.1 nx=2 ny=2 sigma=1\n.hole Gq 0 0 1 1\n.end", 3, "unknown ground plane 'Gq'"),
-    (".units mm\nGp x1=0 y1=0 z1=0 x2=1 y2=0 z2=0 x3=1 y3=1 z3=0 thick=0.1 seg1=2 seg2=2 sigma=1 hole user1 (1, 2)\n.end", 2, "not read by this front end"),
+    (".units mm\nGp x1=0 y1=0 z1=0 x2=1 y2=0 z2=0 x3=1 y3=1 z3=0 thick=0.1 seg1=2 seg2=2 sigma=1 hole user1 (1, 2)\n.end", 2, "'hole user1' is not supported"),
     (".units mm\nN1 x=0\nE1 N1 N9 w=1 h=1 sigma=1\n.end", 3, "not defined"),
     (".units mm\nN1 x=0\nN2 x=1\nE1 N1 N2 w=1 h=1\n.end", 4, "conductivity"),
     (".units mm\nN1 x=0\nN2 x=1\nE1 N1 N2 w=1 h=1 sigma=1 rho=1\n.end", 4, "either"),

@@ -360,14 +360,21 @@ def _plane_extension(head: str, toks: List[str], line: int, unit: float, sigma_d
     return _PlaneSpec(head, plane, nhinc, line, max(z1, z2) - t / 2.0)
 
 
+def _rho_sigma(text: str, unit: float, line: int) -> float:
+    """A resistivity per deck unit as a conductivity in S/m: 1/rho first,
+    then the unit, as the reference's reader does (inp.rs:976-987), so that
+    sigma = 1/rho spellings give bit-identical conductivities."""
+    r = _number(text, line)
+    if r <= 0:
+        raise DeckError(line, "rho must be positive")
+    return 1.0 / r / unit
+
+
 def _plane_sigma(vals, line, unit, sigma_default, head):
     if "sigma" in vals:
         return _number(vals["sigma"], line) / unit
     if "rho" in vals:
-        r = _number(vals["rho"], line)
-        if r <= 0:
-            raise DeckError(line, "rho must be positive")
-        return 1.0 / (r * unit)
+        return _rho_sigma(vals["rho"], unit, line)
     if sigma_default is None:
         raise DeckError(line, "ground plane '%s' has no conductivity: set sigma= or rho= here or in .default" % head)
     return sigma_default
@@ -927,6 +934,10 @@ def parse_deck(text: str) -> Problem:
             v, u = _number(defaults[key], line), defaults_unit[key]
         else:
             return None
+        if key in ("nwinc", "nhinc"):
+            return float(_deck_count(vals[key] if key in vals else defaults[key], key, line))
+        if key in ("w", "h"):
+            return abs(v * u)     # widths and heights are magnitudes (inp.rs:4140-4141)
         return v * u if key in _LENGTHS else v
 
     def default_sigma(line: int) -> Optional[float]:
@@ -934,10 +945,7 @@ def parse_deck(text: str) -> Problem:
         if "sigma" in defaults:
             return _number(defaults["sigma"], line) / defaults_unit["sigma"]
         if "rho" in defaults:
-            r = _number(defaults["rho"], line)
-            if r <= 0:
-                raise DeckError(line, "rho must be positive")
-            return 1.0 / (r * defaults_unit["rho"])
+            return _rho_sigma(defaults["rho"], defaults_unit["rho"], line)
         return None
 
     for line, stmt in statements:
@@ -979,7 +987,10 @@ def parse_deck(text: str) -> Problem:
             xyz = []
             for k in ("x", "y", "z"):
                 v = field(vals, k, line)
-                xyz.append(0.0 if v is None else v)
+                if v is None:
+                    raise DeckError(line, "node '%s': a coordinate is unset and no .default covers it (set it, or "
+                                          ".default x=.. y=.. z=..)" % head)
+                xyz.append(v)
             node_index[name] = len(positions)
             positions.append(tuple(xyz))
             continue
@@ -990,17 +1001,15 @@ def parse_deck(text: str) -> Problem:
             a, b = resolve(toks[0], line), resolve(toks[1], line)
             vals = _assignments(toks[2:], line, (_FIELDS - {"x", "y", "z"}) | {"group"})
             w, h = field(vals, "w", line), field(vals, "h", line)
-            if w is None or h is None:
-                raise DeckError(line, "segment '%s' needs w= and h= (on the line or in .default)" % head)
+            for what, v, key in (("width", w, "w"), ("height", h, "h")):
+                if v is None:
+                    raise DeckError(line, "segment '%s' has no %s: set %s= here or in .default" % (head, what, key))
             if "sigma" in vals or ("rho" not in vals and "sigma" in defaults):
                 src, su = (vals, unit) if "sigma" in vals else (defaults, defaults_unit["sigma"])
                 sigma = _number(src["sigma"], line) / su
             elif "rho" in vals or "rho" in defaults:
                 src, su = (vals, unit) if "rho" in vals else (defaults, defaults_unit["rho"])
-                r = _number(src["rho"], line)
-                if r <= 0:
-                    raise DeckError(line, "rho must be positive")
-                sigma = 1.0 / (r * su)
+                sigma = _rho_sigma(src["rho"], su, line)
             else:
                 raise DeckError(line, "segment '%s' has no conductivity (sigma= or rho=)" % head)
             nw = int(field(vals, "nwinc", line) or 1)

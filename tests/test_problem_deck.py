@@ -15,7 +15,7 @@ DECK = """* a two-segment trace
 .default sigma=5.8e4 w=0.1 h=0.035
 N1 x=0 y=0 z=0
 N2 x = 1 y=0 z=0
-N3 x=1 y=1
+N3 x=1 y=1 z=0
 E1 N1 N2 nwinc=3 nhinc=2
 E2 N2 n3 nwinc=3
 + nhinc=2
@@ -113,17 +113,20 @@ E2 N3 N4 group=right
 
 @pytest.mark.parametrize("text,line,what", [
     ("N1 x=0\n.end", 1, ".units"),
-    (".units mm\nN1 x=0\n", 0, ".end"),
-    (".units mm\nN1 x=0\n.bogus\n.end", 3, "not in the deck subset"),
-    (".units mm\nN1 x=0\nGplane x1=0\n.end", 3, "is missing 'y1'"),
+    (".units mm\nN1 x=0 y=0 z=0\n", 0, ".end"),
+    (".units mm\nN1 x=0 y=0 z=0\n.bogus\n.end", 3, "not in the deck subset"),
+    (".units mm\nN1 x=0 y=0 z=0\nGplane x1=0\n.end", 3, "is missing 'y1'"),
     (".units mm\nGp 0 0 0 1 1 0 0.1 nx=2 ny=2 sigma=1\n.hole Gq 0 0 1 1\n.end", 3, "unknown ground plane 'Gq'"),
     (".units mm\nGp x1=0 y1=0 z1=0 x2=1 y2=0 z2=0 x3=1 y3=1 z3=0 thick=0.1 seg1=2 seg2=2 sigma=1 hole user1 (1, 2)\n.end", 2, "'hole user1' is not supported"),
-    (".units mm\nN1 x=0\nE1 N1 N9 w=1 h=1 sigma=1\n.end", 3, "not defined"),
-    (".units mm\nN1 x=0\nN2 x=1\nE1 N1 N2 w=1 h=1\n.end", 4, "conductivity"),
-    (".units mm\nN1 x=0\nN2 x=1\nE1 N1 N2 w=1 h=1 sigma=1 rho=1\n.end", 4, "either"),
-    (".units mm\nN1 x=0\nn1 x=1\n.end", 3, "twice"),
-    (".units mm\nN1 x=0\n.end\nN2 x=1", 4, "after .end"),
+    (".units mm\nN1 x=0 y=0 z=0\nE1 N1 N9 w=1 h=1 sigma=1\n.end", 3, "not defined"),
+    (".units mm\nN1 x=0 y=0 z=0\nN2 x=1 y=0 z=0\nE1 N1 N2 w=1 h=1\n.end", 4, "conductivity"),
+    (".units mm\nN1 x=0 y=0 z=0\nN2 x=1 y=0 z=0\nE1 N1 N2 w=1 h=1 sigma=1 rho=1\n.end", 4, "either"),
+    (".units mm\nN1 x=0 y=0 z=0\nn1 x=1 y=0 z=0\n.end", 3, "twice"),
+    (".units mm\nN1 x=0 y=0 z=0\n.end\nN2 x=1 y=0 z=0", 4, "after .end"),
     (".units furlong\n.end", 1, "unknown unit"),
+    (".units m\nn1 x=0\n.end", 2, ".default"),
+    (".units m\nn1 x=0 y=0 z=0\nn2 x=1 y=0 z=0\ne1 n1 n2 h=1 sigma=1\n.end", 4, "'e1' has no width"),
+    (".units m\nn1 x=0 y=0 z=0\nn2 x=1 y=0 z=0\ne1 n1 n2 w=1 h=1 sigma=1 nwinc=2.5\n.end", 4, "nwinc"),
 ])
 def test_errors_carry_the_line(text, line, what):
     with pytest.raises(P.DeckError) as e:
@@ -161,3 +164,22 @@ def test_load_picks_the_reader_by_extension(tmp_path):
     doc.write_text(json.dumps(P.parse_deck(DECK).to_json()))
     a, b = P.load(str(deck)), P.load(str(doc))
     assert a.nodes == b.nodes and a.segments == b.segments
+
+
+@pytest.mark.parametrize("unit", ["m", "mm", "um", "mils"])
+@pytest.mark.parametrize("rho", ["0.0172", "1.72e-8", "3", "0.7"])
+def test_rho_and_its_reciprocal_sigma_give_the_same_conductivity_bits(unit, rho):
+    """1/rho first, then the unit (inp.rs:976-987): a deck written with
+    sigma = the correctly rounded 1/rho reads to the very same conductivity,
+    on a segment, in .default and on a ground plane."""
+    sigma = repr(1.0 / float(rho))
+    base = (".units %s\n%%s\nN1 x=0 y=0 z=0\nN2 x=1 y=0 z=0\nE1 N1 N2 w=0.1 h=0.1 %%s\n"
+            "Gp x1=0 y1=-3 z1=-1 x2=2 y2=-3 z2=-1 x3=2 y3=-2 z3=-1 thick=0.1 seg1=2 seg2=1 %%s\n"
+            ".external N1 N2\n.freq fmin=1 fmax=1\n.end" % unit)
+    for default, line_field, plane_field in [("", "rho=%s" % rho, "rho=%s" % rho),
+                                             (".default rho=%s" % rho, "", "")]:
+        a = P.parse_deck(base % (default, line_field, plane_field))
+        b = P.parse_deck(base % (default.replace("rho=" + rho, "sigma=" + sigma),
+                                 line_field.replace("rho=" + rho, "sigma=" + sigma),
+                                 plane_field.replace("rho=" + rho, "sigma=" + sigma)))
+        assert [s["sigma"] for s in a.segments] == [s["sigma"] for s in b.segments]

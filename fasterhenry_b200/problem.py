@@ -231,20 +231,55 @@ def frequency_sweep(fmin: float, fmax: float, ndec: float) -> List[float]:
     (inp.rs:509-526)."""
     if not (math.isfinite(fmin) and math.isfinite(fmax)) or fmin < 0 or fmax < 0:
         raise ValueError("frequencies must be finite and >= 0")
+    if not (math.isfinite(ndec) and ndec > 0):
+        raise ValueError("ndec must be > 0, got %r" % ndec)
+    if fmax < fmin:
+        raise ValueError("fmax (%r) is below fmin (%r)" % (fmax, fmin))
     if fmin == fmax:
         return [fmin]
     if fmin == 0.0:
-        raise ValueError("fmin = 0 is only allowed when fmin = fmax (the DC solve)")
-    if not (math.isfinite(ndec) and ndec > 0):
-        raise ValueError("ndec must be positive")
-    if fmin > fmax:
-        raise ValueError("fmin must not exceed fmax")
-    n = int(math.floor(ndec * math.log10(fmax / fmin))) + 1
+        raise ValueError("fmin = 0 is only allowed as the single-frequency case (.freq fmin=0 fmax=0 runs the DC "
+                         "solve)")
+    # the last step the rule admits, with 1e-9 of slack for rounding, and
+    # each point's exponent snapped to a whole decade within 1e-9
+    # (inp.rs:4833-4896)
+    last = ndec * (math.log10(fmax) - math.log10(fmin))
+    if last + 1.0 > MAX_SWEEP_POINTS:
+        raise ValueError("the sweep would have about %.3e points (at most %g); lower ndec or narrow fmin..fmax"
+                         % (last + 1.0, MAX_SWEEP_POINTS))
     out = []
-    for k in range(n):
-        q = k / ndec
-        out.append(fmin * 10.0 ** int(q) if float(q).is_integer() else fmin * 10.0 ** q)
+    for k in range(int(math.floor(last + 1e-9)) + 1):
+        exponent = k / ndec
+        whole = _round_half_away(exponent)
+        if abs(exponent - whole) <= 1e-9 * max(abs(whole), 1.0):
+            out.append(fmin * _pow10i(int(whole)))
+        else:
+            out.append(fmin * 10.0 ** exponent)
     return out
+
+
+MAX_SWEEP_POINTS = 1e7
+
+
+def _round_half_away(x: float) -> float:
+    """f64::round: the nearest integer, halves away from zero."""
+    a = abs(x)
+    r = math.floor(a)
+    if a - r >= 0.5:    # a - floor(a) is exact
+        r += 1
+    return math.copysign(r, x)
+
+
+def _pow10i(k: int) -> float:
+    """10^k by repeated squaring in binary (f64::powi's scheme); exact for
+    the powers of ten a float holds exactly."""
+    base, result, e = 10.0, 1.0, abs(k)
+    while e:
+        if e & 1:
+            result *= base
+        base *= base
+        e >>= 1
+    return result if k >= 0 else 1.0 / result
 
 
 _FIELDS = {"x", "y", "z", "w", "h", "nwinc", "nhinc", "rw", "rh", "wx", "wy", "wz", "sigma", "rho"}
@@ -1037,12 +1072,19 @@ def parse_deck(text: str) -> Problem:
             continue
         if low == ".freq":
             vals = _assignments(_tokens(rest), line, {"fmin", "fmax", "ndec"})
+            # all three are required: FastHenry's own defaults for an omitted
+            # or zero ndec are not read (inp.rs:3787-3870)
+            if "fmin" not in vals or "fmax" not in vals or "ndec" not in vals:
+                raise DeckError(line, ".freq needs fmin=, fmax= and ndec=")
+            fmin, fmax = _finite(vals["fmin"], line), _finite(vals["fmax"], line)
+            ndec = _number(vals["ndec"], line)
+            if ndec < 0:
+                raise DeckError(line, "ndec must be > 0, got %s (a negative ndec steps away from fmax)"
+                                % _shown(ndec))
+            if ndec == 0:
+                raise DeckError(line, "ndec must be > 0, got 0")
             try:
-                fmin, fmax = _number(vals["fmin"], line), _number(vals["fmax"], line)
-                ndec = _number(vals.get("ndec", "1"), line)
                 freqs = frequency_sweep(fmin, fmax, ndec)
-            except KeyError as e:
-                raise DeckError(line, ".freq needs %s=" % e.args[0]) from None
             except ValueError as e:
                 raise DeckError(line, str(e)) from None
             continue

@@ -45,7 +45,7 @@ def test_deck_coupling_groups_truncate(fh):
         lines.append("E%d N%d N%d w=%r h=%r group=%s" % (k, s["a"], s["b"], s["width"], s["height"], groups[k]))
     for a, b in deck.ports:
         lines.append(".external N%d N%d" % (a, b))
-    lines += [".couples a", ".freq fmin=1e9 fmax=1e9", ".end"]
+    lines += [".couples a", ".freq fmin=1e9 fmax=1e9 ndec=1", ".end"]
     prob = fh.parse_deck("\n".join(lines))
     res, warnings = fh.run(prob, fh.Precision.FP64, fh.SolverChoice.DENSE)
     assert len(warnings) == 1 and "truncated" in warnings[0]

@@ -48,6 +48,36 @@ def test_frequency_sweeps():
         P.frequency_sweep(1e3, 1e6, -1)
     f = P.frequency_sweep(1e6, 1e9, 1)
     assert f == [1e6, 1e7, 1e8, 1e9]
+    # the reference reader's sweep answers (inp.rs tests 8779-8790): whole
+    # decades exact at any ndec, the last point the stepped value, never fmax
+    g = P.frequency_sweep(1e3, 1e7, 1.5)
+    assert (g[0], g[3], g[6]) == (1e3, 1e5, 1e7)
+    g = P.frequency_sweep(1e3, 9e3, 2.5)
+    assert len(g) == 3 and g[2] < 9e3
+    assert P.frequency_sweep(1.0, 9.995, 1) == [1.0]
+    # a decade step that lands within rounding of a whole exponent is that
+    # exact power of ten (3 / 0.1 is 30.000000000000004 in floating point)
+    h = P.frequency_sweep(1.0, 1e3, 10.0 / 3.0 * 0.3 * 10.0)
+    assert h[0] == 1.0 and h[-1] == 1e3
+    with pytest.raises(ValueError, match="below fmin"):
+        P.frequency_sweep(1e6, 1e3, 1)
+    with pytest.raises(ValueError, match="ndec"):
+        P.frequency_sweep(5.0, 5.0, -0.5)
+    with pytest.raises(ValueError, match="points"):
+        P.frequency_sweep(1.0, 1e300, 1e6)
+
+
+@pytest.mark.parametrize("sweep,what", [
+    ("fmin=1e3 fmax=1e6", "ndec="), ("fmin=1e3 fmax=1e6 ndec=0", "ndec must be > 0, got 0"),
+    ("fmin=1e3 fmax=1e7 ndec=-1", "ndec"), ("fmin=1e3 fmax=1e3 ndec=-0.5", "ndec"),
+    ("fmin=1e3 fmax=1e6 ndec=1 fstep=2", "unknown field"),
+])
+def test_freq_needs_all_three_fields_and_a_positive_ndec(sweep, what):
+    deck = (".units m\nn1 x=0 y=0 z=0\nn2 x=1 y=0 z=0\ne1 n1 n2 w=1 h=1 sigma=1\n.external n1 n2\n.freq %s\n.end"
+            % sweep)
+    with pytest.raises(P.DeckError) as e:
+        P.parse_deck(deck)
+    assert e.value.line == 6 and what in str(e.value), str(e.value)
 
 
 def test_resistivity_grading_and_per_segment_counts():
@@ -80,7 +110,7 @@ E1 N1 N2 w=0.1 h=0.1 sigma=1
 E2 N3 N4 w=0.1 h=0.1 sigma=1
 .equiv N2 N3 mid
 .external N1 mid
-.freq fmin=0 fmax=0
+.freq fmin=0 fmax=0 ndec=1
 .end"""
     p = P.parse_deck(deck)
     assert len(p.nodes) == 3
@@ -101,7 +131,7 @@ E2 N3 N4 group=right
 .external N1 N2
 .external N3 N4
 .couples left right
-.freq fmin=1e6 fmax=1e6
+.freq fmin=1e6 fmax=1e6 ndec=1
 .end"""
     p = P.parse_deck(deck)
     assert p.segments[0]["width_dir"] == (0.0, 1.0, 0.0) and p.segments[1]["width_dir"] is None
@@ -175,7 +205,7 @@ def test_rho_and_its_reciprocal_sigma_give_the_same_conductivity_bits(unit, rho)
     sigma = repr(1.0 / float(rho))
     base = (".units %s\n%%s\nN1 x=0 y=0 z=0\nN2 x=1 y=0 z=0\nE1 N1 N2 w=0.1 h=0.1 %%s\n"
             "Gp x1=0 y1=-3 z1=-1 x2=2 y2=-3 z2=-1 x3=2 y3=-2 z3=-1 thick=0.1 seg1=2 seg2=1 %%s\n"
-            ".external N1 N2\n.freq fmin=1 fmax=1\n.end" % unit)
+            ".external N1 N2\n.freq fmin=1 fmax=1 ndec=1\n.end" % unit)
     for default, line_field, plane_field in [("", "rho=%s" % rho, "rho=%s" % rho),
                                              (".default rho=%s" % rho, "", "")]:
         a = P.parse_deck(base % (default, line_field, plane_field))

@@ -946,7 +946,9 @@ def parse_deck(text: str) -> Problem:
     groups: List[str] = []
     ports: List[Tuple[str, str, Optional[str], int]] = []
     freqs: Optional[List[float]] = None
-    couples: Optional[List[str]] = None
+    couples: Optional[List[Tuple[str, str]]] = None   # the coupled group pairs of every .couples line
+    couple_names: List[Tuple[int, str]] = []           # (line, group) of every group a .couples line names
+    couples_first: Optional[int] = None
     couples_all = False
     title = None
     ended = False
@@ -1092,20 +1094,21 @@ def parse_deck(text: str) -> Problem:
             names = [t.lower() for t in rest.split()]
             if len(names) < 2:
                 raise DeckError(line, ".equiv joins two or more nodes")
-            canon = None
-            for nm in names:
-                key = alias.get(nm, nm)
-                if key in node_index:
-                    canon = key
-                    break
-            if canon is None:
-                raise DeckError(line, ".equiv names no defined node")
-            for nm in names:
+            first = next((i for i, nm in enumerate(names) if alias.get(nm, nm) in node_index), None)
+            if first is None:
+                raise DeckError(line, ".equiv names no defined node (a name not yet defined becomes a pseudonym "
+                                      "for a defined node in the same list)")
+            canon = alias.get(names[first], names[first])
+            for i, nm in enumerate(names):
+                if i == first:
+                    continue
                 key = alias.get(nm, nm)
                 if key == canon:
-                    if nm != canon and nm not in alias:
-                        raise DeckError(line, ".equiv names node '%s' twice" % nm)
-                    continue
+                    # one node named twice (inp.rs:3879-3930)
+                    if nm == names[first]:
+                        raise DeckError(line, ".equiv of node '%s' with itself" % nm)
+                    raise DeckError(line, ".equiv of node '%s' with itself: '%s' and '%s' already name one node"
+                                    % (nm, nm, names[first]))
                 if key in node_index:
                     # a defined node becomes an alias of the canonical one
                     for k2, v2 in list(alias.items()):
@@ -1116,11 +1119,32 @@ def parse_deck(text: str) -> Problem:
                     alias[nm] = canon
             continue
         if low == ".couples":
+            # `.couples all`, or the groups of one line coupled pairwise with
+            # each other (not with other lines' groups); the two forms do not
+            # mix (inp.rs:3933-3979)
             toks = rest.split()
-            if len(toks) == 1 and toks[0].lower() == "all":
+            if not toks:
+                raise DeckError(line, "expected .couples all | .couples <group> <group> ...")
+            if couples_first is None:
+                couples_first = line
+            conflict = ("conflicting .couples declarations (the first is on line %d): 'all' cannot be combined "
+                        "with named groups" % couples_first)
+            if toks[0].lower() == "all":
+                if len(toks) != 1:
+                    raise DeckError(line, "'.couples all' takes no group names (it couples everything)")
+                if couples is not None:
+                    raise DeckError(line, conflict)
                 couples_all = True
-            else:
-                couples = (couples or []) + toks
+                continue
+            if couples_all:
+                raise DeckError(line, conflict)
+            couples = couples or []
+            for i, a in enumerate(toks):
+                for b in toks[i + 1:]:
+                    if a == b:
+                        raise DeckError(line, "'.couples' lists group '%s' twice" % a)
+                    couples.append((a, b))
+                couple_names.append((line, a))
             continue
         if low.startswith("g") and not low.startswith("."):
             if any(pl.name.lower() == low for pl in planes):
@@ -1267,17 +1291,17 @@ def parse_deck(text: str) -> Problem:
         disc = {"kind": "per_segment", "grids": [g[:2] for g in grids]}
     else:
         disc = {"kind": "uniform", "nw": 1, "nh": 1}
-    if couples is not None and not couples_all:
-        for g in couples:
+    if couples is not None:
+        # groups named but carried by no segment are a typo (inp.rs:4767-4796)
+        for cline, g in couple_names:
             if g not in groups:
-                raise DeckError(0, ".couples names group '%s', which no segment carries" % g)
+                raise DeckError(cline, "'.couples' names group '%s', which no segment carries" % g)
         coupling = A.Coupling.truncated(groups)
-        for i in range(len(couples)):
-            for j in range(i + 1, len(couples)):
-                coupling = coupling.coupled(couples[i], couples[j])
-    elif any(groups):
-        coupling = A.Coupling(groups, None)
+        for a, b in couples:
+            coupling = coupling.coupled(a, b)
     else:
+        # without named .couples every pair couples, whatever groups the
+        # segments carry
         coupling = A.Coupling.all_pairs()
     return Problem(nodes, segs, port_list, disc, freqs or [], coupling, title)
 

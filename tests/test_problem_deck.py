@@ -213,3 +213,51 @@ def test_rho_and_its_reciprocal_sigma_give_the_same_conductivity_bits(unit, rho)
                                  line_field.replace("rho=" + rho, "sigma=" + sigma),
                                  plane_field.replace("rho=" + rho, "sigma=" + sigma)))
         assert [s["sigma"] for s in a.segments] == [s["sigma"] for s in b.segments]
+
+
+COUPLE_DECK = """.units m
+.default w=0.1 h=0.05 sigma=1
+N1 x=0 y=0 z=0
+N2 x=0 y=0 z=1
+N3 x=5 y=0 z=0
+N4 x=5 y=0 z=1
+N5 x=10 y=0 z=0
+N6 x=10 y=0 z=1
+N7 x=15 y=0 z=0
+N8 x=15 y=0 z=1
+E1 N1 N2 group=a
+E2 N3 N4 group=b
+E3 N5 N6 group=c
+E4 N7 N8 group=d
+.external N1 N2
+%s
+.freq fmin=1e6 fmax=1e6 ndec=1
+.end"""
+
+
+def test_couples_pairs_the_groups_of_each_line_only():
+    """inp.rs:3933-3979: a .couples line couples its own groups pairwise;
+    two lines do not couple across each other."""
+    p = P.parse_deck(COUPLE_DECK % ".couples a b\n.couples c d")
+    c = p.coupling
+    assert c.couples("a", "b") and c.couples("c", "d")
+    assert not c.couples("a", "c") and not c.couples("b", "d")
+    three = P.parse_deck(COUPLE_DECK % ".couples a b c").coupling
+    assert three.couples("a", "c") and three.couples("b", "c") and not three.couples("a", "d")
+    # groups without a named .couples line: every pair couples
+    assert P.parse_deck(COUPLE_DECK % "").coupling.is_all_pairs()
+
+
+@pytest.mark.parametrize("couples,line,what", [
+    (".couples a b\n.couples all", 17, "conflicting .couples declarations (the first is on line 16)"),
+    (".couples all\n.couples a b", 17, "conflicting"),
+    (".couples all a", 16, "takes no group names"),
+    (".couples a b a", 16, "lists group 'a' twice"),
+    (".couples a zz", 16, "group 'zz', which no segment carries"),
+    (".equiv N1 N1", 16, "with itself"),
+    (".equiv N3 x\n.equiv x N3", 17, "with itself: 'n3' and 'x' already name one node"),
+])
+def test_couples_and_equiv_errors(couples, line, what):
+    with pytest.raises(P.DeckError) as e:
+        P.parse_deck(COUPLE_DECK % couples)
+    assert e.value.line == line and what in str(e.value), str(e.value)

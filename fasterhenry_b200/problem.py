@@ -385,9 +385,9 @@ def _plane_extension(head: str, toks: List[str], line: int, unit: float, sigma_d
                               "FastHenry corner-point form G<name> x1=.. y1=.. z1=.. x2=.. ... thick=.. seg1=.. seg2=..")
     x1, y1, z1, x2, y2, z2, t = [_number(v, line) * unit for v in toks[:7]]
     vals = _assignments(toks[7:], line, {"nx", "ny", "nhinc", "sigma", "rho"})
-    nx = int(_number(vals.get("nx", "1"), line))
-    ny = int(_number(vals.get("ny", "1"), line))
-    nhinc = int(_number(vals.get("nhinc", "1"), line))
+    nx = _deck_count(vals.get("nx", "1"), "nx", line)
+    ny = _deck_count(vals.get("ny", "1"), "ny", line)
+    nhinc = _deck_count(vals.get("nhinc", "1"), "nhinc", line)
     sigma = _plane_sigma(vals, line, unit, sigma_default, head)
     if nx < 1 or ny < 1:
         raise DeckError(line, "ground plane '%s' needs nx and ny >= 1 (got nx=%d, ny=%d)" % (head, nx, ny))
@@ -1187,7 +1187,7 @@ def parse_deck(text: str) -> Problem:
                 pl.plane.holes.append(PL.Hole.rect(lo, hi))
             else:
                 vals = _assignments(toks[5:], line, {"nx", "ny", "ratio"})
-                cells = (int(_number(vals.get("nx", "2"), line)), int(_number(vals.get("ny", "2"), line)))
+                cells = (_deck_count(vals.get("nx", "2"), "nx", line), _deck_count(vals.get("ny", "2"), "ny", line))
                 ratio = _number(vals.get("ratio", "2"), line)
                 if ratio < 1.0:
                     raise DeckError(line, "contact decay ratio must be >= 1 (got %s)" % vals["ratio"])

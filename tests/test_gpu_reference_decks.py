@@ -76,3 +76,40 @@ def test_plane_deck_pairs_solve_bit_identically_and_match_the_oracle(fh, oracle,
     # as the plane's eddy currents take over
     z = za.impedance_ohm[:, 0, 0]
     assert np.all(z.real > 0) and np.all(z.imag > 0)
+
+
+CLAUSE_DECK = """.units mm
+.default sigma=5.8e4
+Gp x1=0 y1=0 z1=0 x2=10 y2=0 z2=0 x3=10 y3=6 z3=0
++ thick=0.035 %s
+Nt x=5 y=3 z=0.5
+Nb x=5 y=3 z=0.2
+Ev Nt Nb w=0.2 h=0.2
+.equiv Nb Npad
+.external Nt Nb
+.freq fmin=1e6 fmax=1e9 ndec=1
+.end
+"""
+
+
+def test_plane_contact_clauses_solve_like_their_spelled_out_forms_and_match_the_oracle(fh, oracle):
+    """A `contact connection` deck and the same deck with its equiv_rect and
+    decay_rect written out give bit-identical sweeps, within 1e-10 of the
+    oracle's dense Z; so does a meshed initial grid refined under a trace,
+    the via landing on a named contact area."""
+    short = P.parse_deck(CLAUSE_DECK % "seg1=5 seg2=3\n+ contact connection Npad (5, 3, 0, 2, 2, 4)")
+    spelled = P.parse_deck(CLAUSE_DECK % ("seg1=5 seg2=3\n+ contact equiv_rect Npad (5, 3, 0, 2, 2)\n"
+                                          "+ contact decay_rect (5, 3, 0, 2, 2, 0.5, 0.5, -1, -1)"))
+    za, _ = fh.run(short, fh.Precision.FP64, fh.SolverChoice.DENSE)
+    zb, _ = fh.run(spelled, fh.Precision.FP64, fh.SolverChoice.DENSE)
+    assert np.array_equal(za.impedance_ohm, zb.impedance_ohm)
+    ref = oracle_sweep(oracle, short, short.frequencies_hz)
+    assert np.max(np.abs(za.impedance_ohm - ref) / np.abs(ref)) < 1e-10
+    meshed = P.parse_deck(CLAUSE_DECK % ("contact initial_mesh_grid (5, 3)\n"
+                                         "+ contact trace (2, 1, 0, 8, 1, 0, 0.4, 1)\n"
+                                         "+ contact equiv_rect Npad (5, 3, 0, 1, 1)"))
+    zm, _ = fh.run(meshed, fh.Precision.FP64, fh.SolverChoice.DENSE)
+    ref = oracle_sweep(oracle, meshed, meshed.frequencies_hz)
+    assert np.max(np.abs(zm.impedance_ohm - ref) / np.abs(ref)) < 1e-10
+    z = zm.impedance_ohm[:, 0, 0]
+    assert np.all(z.real > 0) and np.all(z.imag > 0)

@@ -19,6 +19,6 @@ from .api import (GradientResult, Param, coordinate_gradient, grid_convolution, 
 from .api import CURRENTS_CSV_HEADER, CurrentSolution, InvalidExcitation, unit_excitation
 from .api import DEFAULT_GROUP, Coupling, CouplingError, TruncationWarning
 from . import problem
-from .problem import DeckError, Problem, ProblemError, load, parse_deck, run
+from .problem import DeckError, DeckWarning, Problem, ProblemError, load, parse_deck, parse_deck_reporting, run
 
 __version__ = "0.1.0"

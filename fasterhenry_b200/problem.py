@@ -30,6 +30,12 @@ dialect of fasterhenry-cli/src/inp.rs:1-600 and docs/input-format.md).
   themselves are kept.  Other plane clauses (a diagonal ``contact trace``,
   user-defined hole shapes, hierarchy files, tilted planes) are rejected by
   name with the statement's line number.
+* ``parse_deck(text, fasthenry_compat=True)`` (and
+  :func:`parse_deck_reporting`, which also returns the :class:`DeckWarning`
+  list) reads third-party decks the way FastHenry does, each default stated
+  in a warning on its line: the title line, metres without ``.units``, the
+  long unit spellings, copper, FastHenry's sweep rules and the plane
+  defaults.
 * :func:`load` picks the reader by file extension (``.inp``/``.fh`` decks,
   anything else JSON), and :func:`run` assembles and sweeps a problem
   (fasterhenry-cli/src/lib.rs:183-230).
@@ -60,6 +66,33 @@ class DeckError(A.InvalidArgument):
     def __init__(self, line: int, message: str):
         super().__init__("line %d: %s" % (line, message))
         self.line = line
+
+
+@dataclasses.dataclass(frozen=True)
+class DeckWarning:
+    """A deck line read under a stated assumption: the FastHenry defaults the
+    ``fasthenry_compat`` mode applies (inp.rs ParseWarning); ``line`` as in
+    :class:`DeckError`."""
+    line: int
+    message: str
+
+    def __str__(self) -> str:
+        return "line %d: %s" % (self.line, self.message)
+
+
+# FastHenry's defaults, applied only in the compat mode (inp.rs:816, 1408,
+# 4814-4822): copper where a conductor names no conductivity, a contact cell
+# as wide as its rectangle clamped to 0.99 of it, ndec=0 read as 0.01, and
+# points up to 0.1 % above fmax kept.
+COPPER_SIGMA = 5.8e7
+COMPAT_CELL_CLAMP = 0.99
+COMPAT_ZERO_NDEC = 0.01
+COMPAT_FMAX_SLACK = 1.001
+# Unit spellings FastHenry reads at the right scale (its prefix match), read
+# in the compat mode with a warning (inp.rs:757-792).
+_COMPAT_UNITS = {"meter": ("m", 1.0), "meters": ("m", 1.0), "metre": ("m", 1.0), "metres": ("m", 1.0),
+                 "kilometer": ("km", 1e3), "kilometers": ("km", 1e3), "kilometre": ("km", 1e3),
+                 "kilometres": ("km", 1e3), "inch": ("in", 0.0254), "inches": ("in", 0.0254)}
 
 
 # ---------------------------------------------------------------------------
@@ -225,37 +258,52 @@ def _discretization_to_json(d: dict) -> dict:
 # ---------------------------------------------------------------------------
 # The `.inp` deck
 # ---------------------------------------------------------------------------
-def frequency_sweep(fmin: float, fmax: float, ndec: float) -> List[float]:
+def frequency_sweep(fmin: float, fmax: float, ndec: float, compat: bool = False) -> List[float]:
     """`.freq fmin fmax ndec`: n = floor(ndec log10(fmax/fmin)) + 1 points
     f(k) = fmin 10^(k/ndec), the exact fmin 10^q where k/ndec is whole
-    (inp.rs:509-526)."""
+    (inp.rs:509-526, 4829-4896).  ``compat`` keeps the points up to 0.1 %
+    above fmax and an fmin above fmax gives no point (FastHenry's rule)."""
     if not (math.isfinite(fmin) and math.isfinite(fmax)) or fmin < 0 or fmax < 0:
         raise ValueError("frequencies must be finite and >= 0")
     if not (math.isfinite(ndec) and ndec > 0):
         raise ValueError("ndec must be > 0, got %r" % ndec)
-    if fmax < fmin:
+    if fmax < fmin and not compat:
         raise ValueError("fmax (%r) is below fmin (%r)" % (fmax, fmin))
     if fmin == fmax:
         return [fmin]
     if fmin == 0.0:
         raise ValueError("fmin = 0 is only allowed as the single-frequency case (.freq fmin=0 fmax=0 runs the DC "
                          "solve)")
+    # compat keeps points up to 0.1 % above fmax, as FastHenry does
+    ceiling = COMPAT_FMAX_SLACK * fmax if compat else fmax
+    if fmin > ceiling:
+        return []
     # the last step the rule admits, with 1e-9 of slack for rounding, and
     # each point's exponent snapped to a whole decade within 1e-9
     # (inp.rs:4833-4896)
-    last = ndec * (math.log10(fmax) - math.log10(fmin))
+    last = ndec * (math.log10(ceiling) - math.log10(fmin))
     if last + 1.0 > MAX_SWEEP_POINTS:
         raise ValueError("the sweep would have about %.3e points (at most %g); lower ndec or narrow fmin..fmax"
                          % (last + 1.0, MAX_SWEEP_POINTS))
-    out = []
-    for k in range(int(math.floor(last + 1e-9)) + 1):
+
+    def point(k):
         exponent = k / ndec
         whole = _round_half_away(exponent)
         if abs(exponent - whole) <= 1e-9 * max(abs(whole), 1.0):
-            out.append(fmin * _pow10i(int(whole)))
-        else:
-            out.append(fmin * 10.0 ** exponent)
-    return out
+            return fmin * _pow10i(int(whole))
+        return fmin * 10.0 ** exponent
+
+    if compat:
+        # one candidate past the rule's last step, each checked against the
+        # ceiling
+        out = []
+        for k in range(int(math.floor(last + 1e-9)) + 2):
+            f = point(k)
+            if f > ceiling:
+                break
+            out.append(f)
+        return out
+    return [point(k) for k in range(int(math.floor(last + 1e-9)) + 1)]
 
 
 MAX_SWEEP_POINTS = 1e7
@@ -286,11 +334,20 @@ _FIELDS = {"x", "y", "z", "w", "h", "nwinc", "nhinc", "rw", "rh", "wx", "wy", "w
 _LENGTHS = {"x", "y", "z", "w", "h"}
 
 
-def _split_statements(text: str) -> List[Tuple[int, str]]:
+def _split_statements(text: str, compat: bool = False):
     """Logical lines: comments dropped, '+' lines joined onto the previous
-    statement (keeping the first line's number)."""
+    statement (keeping the first line's number).  In the compat mode the
+    physical first line is the deck's title, whatever it holds, and is not
+    read as a statement (inp.rs:3504-3560).  Returns (title, statements,
+    number of the last line)."""
     out: List[Tuple[int, str]] = []
-    for no, raw in enumerate(text.splitlines(), 1):
+    lines = text.splitlines()
+    title = None
+    start = 0
+    if compat and lines:
+        title = " ".join(lines[0].split()) or None
+        start = 1
+    for no, raw in enumerate(lines[start:], start + 1):
         line = raw.strip()
         if not line or line.startswith("*"):
             continue
@@ -300,7 +357,7 @@ def _split_statements(text: str) -> List[Tuple[int, str]]:
             out[-1] = (out[-1][0], out[-1][1] + " " + line[1:])
             continue
         out.append((no, line))
-    return out
+    return title, out, len(lines)
 
 
 def _tokens(body: str) -> List[str]:
@@ -377,7 +434,8 @@ class _PlaneSpec:
     bar_width: Tuple[Optional[float], Optional[float]] = (None, None)
 
 
-def _plane_extension(head: str, toks: List[str], line: int, unit: float, sigma_default) -> _PlaneSpec:
+def _plane_extension(head: str, toks: List[str], line: int, unit: float, sigma_default, compat: bool = False,
+                     warn=None) -> _PlaneSpec:
     """G<name> x1 y1 z1 x2 y2 z2 t [nx=] [ny=] [nhinc=] [sigma=|rho=]
     (inp.rs:4329-4398): footprint corners, TOP surface z, thickness down."""
     if len(toks) < 7:
@@ -388,7 +446,7 @@ def _plane_extension(head: str, toks: List[str], line: int, unit: float, sigma_d
     nx = _deck_count(vals.get("nx", "1"), "nx", line)
     ny = _deck_count(vals.get("ny", "1"), "ny", line)
     nhinc = _deck_count(vals.get("nhinc", "1"), "nhinc", line)
-    sigma = _plane_sigma(vals, line, unit, sigma_default, head)
+    sigma = _plane_sigma(vals, line, unit, sigma_default, head, compat, warn)
     if nx < 1 or ny < 1:
         raise DeckError(line, "ground plane '%s' needs nx and ny >= 1 (got nx=%d, ny=%d)" % (head, nx, ny))
     plane = PL.GroundPlane((min(x1, x2), min(y1, y2)), (max(x1, x2), max(y1, y2)), max(z1, z2), t, nx, ny, sigma)
@@ -405,12 +463,15 @@ def _rho_sigma(text: str, unit: float, line: int) -> float:
     return 1.0 / r / unit
 
 
-def _plane_sigma(vals, line, unit, sigma_default, head):
+def _plane_sigma(vals, line, unit, sigma_default, head, compat=False, warn=None):
     if "sigma" in vals:
         return _number(vals["sigma"], line) / unit
     if "rho" in vals:
         return _rho_sigma(vals["rho"], unit, line)
     if sigma_default is None:
+        if compat:
+            warn(line, "ground plane '%s' has no conductivity; using copper (5.8e7 S/m, FastHenry default)" % head)
+            return COPPER_SIGMA
         raise DeckError(line, "ground plane '%s' has no conductivity: set sigma= or rho= here or in .default" % head)
     return sigma_default
 
@@ -499,7 +560,8 @@ def _trace_lines(ends, width: float, along: int, axis1: int) -> List[_Refine]:
     return out
 
 
-def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_default):
+def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_default, compat: bool = False,
+                       warn=None):
     """The FastHenry corner-point G statement (inp.rs:1686-2790).  Returns the
     plane and its in-plane nodes [(name, position, equipotential index or
     None)]; a node that a `contact equiv_rect` / `contact connection`
@@ -530,6 +592,22 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
                                       "centre, not a corner" % (what, "xy"[a], _shown(w)))
             out.append(w)
         return out
+
+    # the compat mode's notes about this statement's clauses, given after
+    # the statement's own copper note
+    pending: List[str] = []
+
+    def clamped(what, v):
+        """[xwidth, ywidth, xcell, ycell]: in the compat mode a cell as wide
+        as its rectangle is clamped to 0.99 of the width (inp.rs:1364-1406)."""
+        for a in range(2):
+            if compat and v[2 + a] > 0 and v[2 + a] >= v[a]:
+                written, v[2 + a] = v[2 + a], COMPAT_CELL_CLAMP * v[a]
+                pending.append("ground plane '%s': %s: %scell=%s metres is not smaller than %swidth=%s metres; "
+                               "clamped to %s x %swidth = %s metres, as FastHenry does (--fasthenry-compat)"
+                               % (head, what, "xy"[a], _shown(written), "xy"[a], _shown(v[a]), COMPAT_CELL_CLAMP,
+                                  "xy"[a], _shown(v[2 + a])))
+        return v
 
     def node_name(name, what):
         if name is None:
@@ -627,7 +705,7 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
                 hole_circles.append((triple(vals, what), r))
             elif low == "contact" and shape == "rect" and len(vals) == 7:
                 contact_decays.append(("'contact rect'", triple(vals, what),
-                                       [_finite(v, line) * unit for v in vals[3:7]] + [-1.0, -1.0]))
+                                       clamped(what, [_finite(v, line) * unit for v in vals[3:7]]) + [-1.0, -1.0]))
             elif low == "contact" and shape == "rect" and len(vals) == 6:
                 contact_rects.append((triple(vals[:3], what), triple(vals[3:6], what)))
             elif low == "contact" and shape == "rect":
@@ -635,9 +713,16 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
                                       "(x1, y1, z1, x2, y2, z2), got %d" % len(vals))
             elif low == "contact" and shape == "decay_rect":
                 arity(9, "x, y, z, xwidth, ywidth, xcell, ycell, xmaxcell, ymaxcell")
-                v = [_finite(x, line) * unit for x in vals[3:9]]
-                contact_decays.append(("'contact decay_rect'", triple(vals, what),
-                                       v[:4] + [v[4] if v[4] >= 0 else -1.0, v[5] if v[5] >= 0 else -1.0]))
+                v = clamped(what, [_finite(x, line) * unit for x in vals[3:7]])
+                limits = []
+                for a in range(2):
+                    raw = _finite(vals[7 + a], line)
+                    if raw == 0:
+                        raise DeckError(line, "%s: %smaxcell=0 is neither a cell size nor the 'no limit' sentinel; "
+                                              "give a positive cell size, or a negative value to decay all the way "
+                                              "to the plane's background cell" % (what, "xy"[a]))
+                    limits.append(raw * unit if raw > 0 else -1.0)
+                contact_decays.append(("'contact decay_rect'", triple(vals, what), v + limits))
             elif low == "contact" and shape in ("point", "line"):
                 n = 5 if shape == "point" else 8
                 arity(n, "x, y, z, xcell, ycell" if shape == "point" else "x0, y0, z0, x1, y1, z1, xcell, ycell")
@@ -667,6 +752,11 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
                     along = 0
                 elif dx <= 1e-9 * dy:
                     along = 1
+                elif compat:
+                    along = None    # refined as its padded bounding box
+                    pending.append("ground plane '%s': diagonal 'contact trace' approximated by refining its padded "
+                                   "bounding box (a tensor-product refinement), not FastHenry's staircase "
+                                   "refinement; cells (trace_width/2)*scale_factor^min(|tan t|, |cot t|)" % head)
                 else:
                     raise DeckError(line, "%s from (%s, %s) to (%s, %s) metres is not parallel to x or y; a "
                                           "diagonal 'contact trace' is not supported, because its published "
@@ -675,7 +765,7 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
                                           "diagonal line's bounding box to the cell you choose"
                                     % (what, _shown(ends[0][0]), _shown(ends[0][1]), _shown(ends[1][0]),
                                        _shown(ends[1][1])))
-                contact_traces.append((ends, width, along))
+                contact_traces.append((ends, width, along, scale))
             elif low == "contact" and shape in ("equiv_rect", "connection"):
                 n = 5 if shape == "equiv_rect" else 6
                 arity(n, "x, y, z, xwidth, ywidth" + ("" if n == 5 else ", ratio"))
@@ -726,9 +816,19 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
                 raise DeckError(line, "'%s (...)' is not an in-plane node declaration: node names start with 'N'"
                                 % text)
             fields = _node_fields(items[k + 1][1])
-            if any(f == "" for f in fields):
+            empty = [i for i, f in enumerate(fields) if f == ""]
+            if empty and not compat:
                 raise DeckError(line, "in-plane node '%s' has an empty coordinate field; write every coordinate "
-                                      "(x, y, z)" % text)
+                                      "(x, y, z) (an empty field reads as 0 only in the compat mode)" % text)
+            if empty:
+                # compat: one empty field reads as 0, before the offset
+                # (inp.rs:2008-2059)
+                if len(fields) != 3 or len(empty) > 1:
+                    raise DeckError(line, "in-plane node '%s' needs 3 coordinates (x, y, z) with at most one empty "
+                                          "field, got %d value(s) of which %d empty" % (text, len(fields), len(empty)))
+                fields[empty[0]] = "0"
+                pending.append("ground plane '%s': in-plane node '%s' has an empty %s coordinate, read as 0 (before "
+                               "the statement's relx/rely/relz offset)" % (head, text, "xyz"[empty[0]]))
             if len(fields) != 3:
                 raise DeckError(line, "in-plane node '%s' needs (x, y, z), got %d values" % (text, len(fields)))
             nodes.append((low, triple(fields, "in-plane node '%s'" % text), None))
@@ -762,6 +862,11 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
     a1, a2 = axis_of(e1), axis_of(e2)
     if a1 is None or a2 is None or a1 == a2:
         raise DeckError(line, "ground plane '%s': the corner points do not form an axis-aligned rectangle" % head)
+    root_cell = compat and file_none and seg == [None, None] and initial_grid is None
+    if root_cell:
+        # file=NONE and no grid at all: one root cell, refined only by the
+        # contact clauses (inp.rs:2399-2404, 2460-2463)
+        seg = [1, 1]
     for i in (0, 1):
         if seg[i] is None:
             raise DeckError(line, "ground plane '%s' has no 'seg%d' (cells along %s)"
@@ -773,7 +878,11 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
     thick = abs(_finite(keys["thick"], line)) * unit
     if thick <= 0:
         raise DeckError(line, "ground plane '%s' needs a thickness > 0" % head)
-    sigma = _plane_sigma(keys, line, unit, sigma_default, head)
+    sigma = _plane_sigma(keys, line, unit, sigma_default, head, compat, warn)
+    if root_cell:
+        warn(line, "ground plane '%s' has 'file=NONE' and no 'seg1'/'seg2' or 'contact initial_grid': its initial "
+                   "grid is a single cell (as 'contact initial_grid (1, 1)'), refined only by its 'contact' clauses"
+             % head)
     nhinc = _deck_count(keys["nhinc"], "nhinc", line) if "nhinc" in keys else 1
     lo = (min(p[0] for p in pts), min(p[1] for p in pts))
     hi = (max(p[0] for p in pts), max(p[1] for p in pts))
@@ -842,6 +951,10 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
     for i, width in enumerate(segwid):
         if width is None:
             continue
+        if nonuniform and compat:
+            pending.append("ground plane '%s': 'segwid%d' is ignored on a nonuniform plane (full-width bars are "
+                           "used)" % (head, i + 1))
+            continue
         if nonuniform:
             raise DeckError(line, "ground plane '%s': 'segwid%d' needs a uniform plane, but this plane's mesh is "
                                   "nonuniform ('file=NONE', 'contact initial_grid' or a 'contact' clause); drop "
@@ -880,9 +993,10 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
         if misses(rlo, rhi) or touches(rlo, rhi):
             continue
         contacts.append(PL.ContactRegion.new(rlo, rhi, (2, 2), 2.0))
-    for what, centre, v in contact_decays:
+    def decay_region(what, centre, widths, cell, limit):
+        """The graded region of a decay rectangle (inp.rs:3060-3110), its
+        widths, cells and limits given per global axis (-1: no limit)."""
         in_slab(what, centre[2])
-        widths, cell, limit = plane_pair(v[0:2]), plane_pair(v[2:4]), plane_pair(v[4:6])
         rlo, rhi, rc, ratio = [0.0, 0.0], [0.0, 0.0], [0, 0], [0.0, 0.0]
         for a in range(2):
             if not cell[a] > 0:
@@ -897,18 +1011,34 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
             if limit[a] >= 0 and limit[a] < background(a) * (1.0 - 1e-9):
                 raise DeckError(line, "%s: a maxcell finer than ground plane '%s''s background cell (%r metres) "
                                       "is not supported; raise seg1/seg2" % (what, head, background(a)))
-        if misses(rlo, rhi) or touches(rlo, rhi):
+        return PL.ContactRegion.graded_per_axis(rlo, rhi, rc, ratio)
+
+    for what, centre, v in contact_decays:
+        region = decay_region(what, centre, plane_pair(v[0:2]), plane_pair(v[2:4]), plane_pair(v[4:6]))
+        if misses(region.lo, region.hi) or touches(region.lo, region.hi):
             continue
-        contacts.append(PL.ContactRegion.graded_per_axis(rlo, rhi, rc, ratio))
+        contacts.append(region)
     for what, refine in contact_lines:
         for p in refine.ends:
             on_plane(what, p)
         region = refine_region(refine)
         if region is not None:
             contacts.append(region)
-    for ends, width, along in contact_traces:
+    for ends, width, along, scale in contact_traces:
         for p in ends:
             on_plane("'contact trace'", p)
+        if along is None:
+            # compat: a diagonal trace is its bounding box padded by 3w/2,
+            # cells (w/2) s^min(|tan|, |cot|), at most half the narrower
+            # width, no outward limit (inp.rs:3167-3199)
+            span = [abs(ends[1][0] - ends[0][0]), abs(ends[1][1] - ends[0][1])]
+            ratio = min(span) / max(span)
+            pad = 3.0 * width / 2.0
+            widths = [span[0] + 2.0 * pad, span[1] + 2.0 * pad]
+            c = min(width / 2.0 * scale ** ratio, min(widths) / 2.0)
+            centre = [(ends[0][0] + ends[1][0]) / 2.0, (ends[0][1] + ends[1][1]) / 2.0, ends[0][2]]
+            contacts.append(decay_region("'contact trace'", centre, widths, [c, c], [-1.0, -1.0]))
+            continue
         for refine in _trace_lines(ends, width, along, a1):
             region = refine_region(refine)
             if region is not None:
@@ -927,13 +1057,40 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
         in_slab("in-plane node '%s'" % name, pos[2])
     plane = PL.GroundPlane(lo, hi, mid_z + thick / 2.0, thick, cells[0], cells[1], sigma, holes, contacts,
                            equipotentials)
+    for note in pending:
+        warn(line, note)
     return _PlaneSpec(head, plane, nhinc, line, mid_z, a1, (bar_width[0], bar_width[1])), nodes
 
 
-def parse_deck(text: str) -> Problem:
+def parse_deck(text: str, fasthenry_compat: bool = False) -> Problem:
     """Parses a FastHenry `.inp` deck in this front end's subset into a
-    :class:`Problem` (SI units)."""
-    statements = _split_statements(text)
+    :class:`Problem` (SI units).  ``fasthenry_compat`` reads third-party
+    decks the way FastHenry does (inp.rs ParseOptions::fasthenry_compat):
+    see :func:`parse_deck_reporting`, which also returns the warnings."""
+    return parse_deck_reporting(text, fasthenry_compat)[0]
+
+
+def parse_deck_reporting(text: str, fasthenry_compat: bool = False) -> Tuple[Problem, List[DeckWarning]]:
+    """:func:`parse_deck` with the warnings of the compat mode's defaults, in
+    line order.  The compat mode (inp.rs, its `--fasthenry-compat` rows):
+    the physical first line is the title; a missing `.units` reads as
+    metres and each `.units` applies from its own line on, in the long
+    spellings FastHenry reads correctly too; a conductor without a
+    conductivity is copper (5.8e7 S/m); `.equiv` of a node with itself is
+    ignored; `.freq` reads an omitted ndec as 1 and ndec=0 as 0.01 and keeps
+    points up to 0.1 % above fmax; on a ground plane one empty node
+    coordinate reads as 0, a contact cell as wide as its rectangle is
+    clamped to 0.99 of it, `segwid` on a nonuniform plane is ignored,
+    `file=NONE` without a grid is one root cell, and a diagonal `contact
+    trace` refines its padded bounding box.  Natively each of these is a
+    line-numbered error."""
+    compat = bool(fasthenry_compat)
+    warnings: List[Tuple[int, int, DeckWarning]] = []   # (line, order, warning)
+
+    def warn(line: int, message: str) -> None:
+        warnings.append((line, len(warnings), DeckWarning(line, message)))
+
+    first_line_title, statements, last_line = _split_statements(text, compat)
     unit: Optional[float] = None
     defaults: Dict[str, str] = {}
     defaults_unit: Dict[str, float] = {}
@@ -950,7 +1107,7 @@ def parse_deck(text: str) -> Problem:
     couple_names: List[Tuple[int, str]] = []           # (line, group) of every group a .couples line names
     couples_first: Optional[int] = None
     couples_all = False
-    title = None
+    title = first_line_title     # the compat mode's first line; a later .title replaces it
     ended = False
     planes: List[_PlaneSpec] = []
     plane_node: Dict[str, int] = {}        # in-plane node name -> plane index
@@ -996,18 +1153,39 @@ def parse_deck(text: str) -> Problem:
             ended = True
             continue
         if low == ".title":
-            title = rest.strip()
+            title = " ".join(rest.split())
             continue
         if low == ".units":
-            u = rest.strip().lower()
+            toks = rest.split()
+            if len(toks) != 1:
+                raise DeckError(line, "expected .units <unit>")
+            u = toks[0].lower()
             if u not in UNITS:
-                raise DeckError(line, "unknown unit '%s'; expected one of km, m, cm, mm, um, in, mils" % rest.strip())
-            if unit is not None:
-                raise DeckError(line, ".units may appear once")
+                if not compat:
+                    raise DeckError(line, "unknown unit '%s'; expected one of km, m, cm, mm, um, in, mils" % toks[0])
+                if u.startswith("milli") or u.startswith("micron") or u.startswith("micromet"):
+                    reads, documented = ("mils (2.54e-5 m)", "mm") if u.startswith("milli") else ("metres", "um")
+                    raise DeckError(line, "'.units %s' is not a documented unit, and FastHenry misreads it as %s, "
+                                          "which would scale every length wrongly; write '.units %s'"
+                                    % (toks[0], reads, documented))
+                if u not in _COMPAT_UNITS:
+                    raise DeckError(line, "unknown unit '%s'; expected one of km, m, cm, mm, um, in, mils" % toks[0])
+                documented, factor = _COMPAT_UNITS[u]
+                warn(line, "'.units %s' is not one of the documented units (km, m, cm, mm, um, in, mils); reading "
+                           "it as '%s', as FastHenry does" % (toks[0], documented))
+                unit = factor
+                continue
+            if unit is not None and not compat:
+                raise DeckError(line, "duplicate .units directive (.units may appear once)")
+            # compat: each .units applies from its own line on; every value
+            # read so far is already in metres and S/m
             unit = UNITS[u]
             continue
-        if unit is None and low not in (".title",):
-            raise DeckError(line, "a .units line must come first (the deck unit is required)")
+        if unit is None and (low in (".default", ".hole", ".contact") or low[:1] in ("n", "e", "g")):
+            if not compat:
+                raise DeckError(line, "a .units line must come before this line (the deck unit is required)")
+            warn(line, "no .units directive before this line; reading lengths in metres, as FastHenry does")
+            unit = 1.0
         if low == ".default":
             vals = _assignments(_tokens(rest), line, _FIELDS)
             for k, v in vals.items():
@@ -1047,8 +1225,12 @@ def parse_deck(text: str) -> Problem:
             elif "rho" in vals or "rho" in defaults:
                 src, su = (vals, unit) if "rho" in vals else (defaults, defaults_unit["rho"])
                 sigma = _rho_sigma(src["rho"], su, line)
+            elif compat:
+                warn(line, "segment '%s' has no conductivity; using copper (5.8e7 S/m, FastHenry default)" % head)
+                sigma = COPPER_SIGMA
             else:
-                raise DeckError(line, "segment '%s' has no conductivity (sigma= or rho=)" % head)
+                raise DeckError(line, "segment '%s' has no conductivity: set sigma= or rho= here or in .default"
+                                % head)
             nw = int(field(vals, "nwinc", line) or 1)
             nh = int(field(vals, "nhinc", line) or 1)
             rw = field(vals, "rw", line) or 1.0
@@ -1074,19 +1256,31 @@ def parse_deck(text: str) -> Problem:
             continue
         if low == ".freq":
             vals = _assignments(_tokens(rest), line, {"fmin", "fmax", "ndec"})
-            # all three are required: FastHenry's own defaults for an omitted
-            # or zero ndec are not read (inp.rs:3787-3870)
-            if "fmin" not in vals or "fmax" not in vals or "ndec" not in vals:
+            # all three are required natively; compat reads FastHenry's
+            # defaults for an omitted or zero ndec (inp.rs:3787-3870)
+            if "fmin" not in vals or "fmax" not in vals or ("ndec" not in vals and not compat):
                 raise DeckError(line, ".freq needs fmin=, fmax= and ndec=")
             fmin, fmax = _finite(vals["fmin"], line), _finite(vals["fmax"], line)
-            ndec = _number(vals["ndec"], line)
+            if "ndec" not in vals:
+                warn(line, ".freq has no ndec; using ndec=1 (FastHenry behavior)")
+                ndec = 1.0
+            else:
+                ndec = _number(vals["ndec"], line)
             if ndec < 0:
                 raise DeckError(line, "ndec must be > 0, got %s (a negative ndec steps away from fmax)"
                                 % _shown(ndec))
             if ndec == 0:
-                raise DeckError(line, "ndec must be > 0, got 0")
+                if not compat:
+                    raise DeckError(line, "ndec must be > 0, got 0")
+                warn(line, ".freq ndec=0 has no points per decade; using ndec=0.01 (FastHenry behavior)")
+                ndec = COMPAT_ZERO_NDEC
+            if compat and fmin > fmax >= 0.0:
+                warn(line, (".freq fmin (%s) is above fmax (%s): the sweep is empty (FastHenry behavior)"
+                            if fmin > COMPAT_FMAX_SLACK * fmax else
+                            ".freq fmin (%s) is above fmax (%s) but within FastHenry's 0.1%% slack; solving fmin "
+                            "alone") % (_shown(fmin), _shown(fmax)))
             try:
-                freqs = frequency_sweep(fmin, fmax, ndec)
+                freqs = frequency_sweep(fmin, fmax, ndec, compat)
             except ValueError as e:
                 raise DeckError(line, str(e)) from None
             continue
@@ -1105,10 +1299,13 @@ def parse_deck(text: str) -> Problem:
                 key = alias.get(nm, nm)
                 if key == canon:
                     # one node named twice (inp.rs:3879-3930)
-                    if nm == names[first]:
-                        raise DeckError(line, ".equiv of node '%s' with itself" % nm)
-                    raise DeckError(line, ".equiv of node '%s' with itself: '%s' and '%s' already name one node"
-                                    % (nm, nm, names[first]))
+                    message = (".equiv of node '%s' with itself" % nm if nm == names[first] else
+                               ".equiv of node '%s' with itself: '%s' and '%s' already name one node"
+                               % (nm, nm, names[first]))
+                    if compat:
+                        warn(line, message + "; ignored (--fasthenry-compat)")
+                        continue
+                    raise DeckError(line, message)
                 if key in node_index:
                     # a defined node becomes an alias of the canonical one
                     for k2, v2 in list(alias.items()):
@@ -1156,9 +1353,9 @@ def parse_deck(text: str) -> Problem:
             except ValueError:
                 bare = False
             if bare:
-                planes.append(_plane_extension(head, _tokens(rest), line, unit, default_sigma(line)))
+                planes.append(_plane_extension(head, _tokens(rest), line, unit, default_sigma(line), compat, warn))
             else:
-                spec, pnodes = _plane_corner_form(head, rest, line, unit, default_sigma(line))
+                spec, pnodes = _plane_corner_form(head, rest, line, unit, default_sigma(line), compat, warn)
                 for name, pos, area in pnodes:
                     if name in node_index or name in alias:
                         raise DeckError(line, "node '%s' is declared twice" % name)
@@ -1194,10 +1391,18 @@ def parse_deck(text: str) -> Problem:
                 pl.plane.contacts.append(PL.ContactRegion.new(lo, hi, cells, ratio))
             continue
         raise DeckError(line, "'%s' is not in the deck subset" % head)
+    # the deck-level checks (inp.rs:4401-4435)
     if not ended:
-        raise DeckError(0, "the deck has no .end")
-    if unit is None:
-        raise DeckError(0, "the deck has no .units line")
+        raise DeckError(last_line, "the deck has no .end directive")
+    if unit is None and not compat:
+        raise DeckError(last_line, "the deck has no .units directive (units are mandatory: .units <unit>, one of "
+                                   "km, m, cm, mm, um, in, mils)")
+    if not ports:
+        raise DeckError(0, "the deck has no .external port")
+    if freqs is None:
+        raise DeckError(0, "the deck has no .freq sweep")
+    if not segments and not planes:
+        raise DeckError(0, "the deck has no conductor: no E segment and no G ground plane")
     # Assembly (inp.rs:4437-4620): the ground-plane meshes first, then the
     # declared nodes still referenced as themselves (in declaration order),
     # then the segments.  An endpoint whose .equiv class holds an in-plane
@@ -1303,16 +1508,18 @@ def parse_deck(text: str) -> Problem:
         # without named .couples every pair couples, whatever groups the
         # segments carry
         coupling = A.Coupling.all_pairs()
-    return Problem(nodes, segs, port_list, disc, freqs or [], coupling, title)
+    problem = Problem(nodes, segs, port_list, disc, freqs or [], coupling, title)
+    return problem, [w for _, _, w in sorted(warnings, key=lambda t: (t[0], t[1]))]
 
 
-def load(path: str) -> Problem:
-    """A problem from a file: `.inp` / `.fh` as a deck, anything else as the
-    JSON document (fasterhenry-cli/src/lib.rs read_inputs)."""
+def load(path: str, fasthenry_compat: bool = False) -> Problem:
+    """A problem from a file: `.inp` / `.fh` as a deck (``fasthenry_compat``
+    as in :func:`parse_deck_reporting`), anything else as the JSON document
+    (fasterhenry-cli/src/lib.rs read_inputs)."""
     with open(path) as f:
         text = f.read()
     if os.path.splitext(path)[1].lower() in (".inp", ".fh"):
-        return parse_deck(text)
+        return parse_deck(text, fasthenry_compat)
     return Problem.from_json(text)
 
 

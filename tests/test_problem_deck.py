@@ -143,7 +143,7 @@ E2 N3 N4 group=right
 
 @pytest.mark.parametrize("text,line,what", [
     ("N1 x=0\n.end", 1, ".units"),
-    (".units mm\nN1 x=0 y=0 z=0\n", 0, ".end"),
+    (".units mm\nN1 x=0 y=0 z=0\n", 2, ".end"),
     (".units mm\nN1 x=0 y=0 z=0\n.bogus\n.end", 3, "not in the deck subset"),
     (".units mm\nN1 x=0 y=0 z=0\nGplane x1=0\n.end", 3, "is missing 'y1'"),
     (".units mm\nGp 0 0 0 1 1 0 0.1 nx=2 ny=2 sigma=1\n.hole Gq 0 0 1 1\n.end", 3, "unknown ground plane 'Gq'"),

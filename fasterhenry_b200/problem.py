@@ -1485,6 +1485,15 @@ def parse_deck_reporting(text: str, fasthenry_compat: bool = False) -> Tuple[Pro
                    "width_dir": None} for sd in geometry.segments]
     segs = plane_segs + [dict(sg, a=end(sg["a"], sa), b=end(sg["b"], sb))
                          for sg, (sa, sb) in zip(segments, seg_ends)]
+    # every E segment through the library's own rule (a zero length, a
+    # width direction along the segment, ...), reported on its own line
+    # (inp.rs:4573-4581)
+    check = A.Geometry.from_parts(nodes, [])
+    for k, sg in enumerate(segs[len(plane_segs):]):
+        try:
+            check.add_segment(sg)
+        except A.GeometryError as e:
+            raise DeckError(seg_lines[k], str(e)) from None
     port_list = [(end(p, sp), end(n, sn), label) for (p, n, label, _), (sp, sn) in zip(ports, port_ends)]
     grids = plane_grids + grids
     groups = [""] * len(plane_grids) + groups

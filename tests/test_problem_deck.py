@@ -261,3 +261,15 @@ def test_couples_and_equiv_errors(couples, line, what):
     with pytest.raises(P.DeckError) as e:
         P.parse_deck(COUPLE_DECK % couples)
     assert e.value.line == line and what in str(e.value), str(e.value)
+
+
+@pytest.mark.parametrize("segment,what", [
+    ("e1 n1 n2 w=1 h=1 sigma=1 wx=1", "width"),   # width direction along the segment
+    ("e1 n1 n3 w=1 h=1 sigma=1", "zero length"),
+])
+def test_a_segment_the_geometry_rejects_is_reported_on_its_line(segment, what):
+    deck = (".units m\nn1 x=0 y=0 z=0\nn2 x=1 y=0 z=0\nn3 x=0 y=0 z=0\n%s\n.external n1 n2\n"
+            ".freq fmin=1 fmax=1 ndec=1\n.end" % segment)
+    with pytest.raises(P.DeckError) as e:
+        P.parse_deck(deck)
+    assert e.value.line == 5 and what in str(e.value), str(e.value)

@@ -8,7 +8,10 @@ the reference at REFERENCE (default /root/reference):
 The files are small self-authored decks of the reference project:
 spiral.inp / spiral.json (the round-trip pair of
 fasterhenry-cli/tests/roundtrip.rs:18-40), twobar.inp (the two-port SPICE
-fixture) and the ground-plane decks plane_*.inp.
+fixture) and the ground-plane decks plane_*.inp.  It also writes the two
+```json example documents of docs/input-format.md, in order, as
+input_format_example_0.json (the minimal one) and input_format_example_1.json
+(the documented pins of fasterhenry-cli/tests/input_format_doc.rs).
 """
 import os
 import shutil
@@ -25,6 +28,22 @@ def main():
     for name in NAMES:
         shutil.copyfile(os.path.join(src, name), os.path.join(here, name))
         print("copied", name)
+    with open(os.path.join(ref, "docs", "input-format.md")) as f:
+        lines = f.read().splitlines()
+    blocks, block = [], None
+    for line in lines:
+        if block is None and line.rstrip() == "```json":
+            block = []
+        elif block is not None and line.rstrip() == "```":
+            blocks.append("\n".join(block) + "\n")
+            block = None
+        elif block is not None:
+            block.append(line)
+    for k, text in enumerate(blocks):
+        name = "input_format_example_%d.json" % k
+        with open(os.path.join(here, name), "w") as f:
+            f.write(text)
+        print("wrote", name)
     return 0
 
 

@@ -6,6 +6,8 @@ document read to the same problem field by field
 its stated geometry.  Host-only."""
 import os
 
+import pytest
+
 from fasterhenry_b200 import problem as P
 
 DECKS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "decks")
@@ -42,3 +44,57 @@ def test_twobar_deck_reads_two_named_ports():
     assert [(s["a"], s["b"]) for s in p.segments] == [(0, 1), (2, 3)]
     assert p.ports == [(0, 1, "barA"), (2, 3, "barB")]
     assert p.frequencies_hz == [1e6, 1e7, 1e8, 1e9]
+
+
+# The two ```json example documents of the reference's docs/input-format.md
+# (extracted in order by tests/golden/decks/copy_reference_decks.py), held to
+# what fasterhenry-cli/tests/input_format_doc.rs asserts of them.
+EXAMPLES = ["input_format_example_0.json", "input_format_example_1.json"]
+
+
+def example_text(k):
+    with open(os.path.join(DECKS, EXAMPLES[k])) as f:
+        return f.read()
+
+
+def test_every_documented_example_parses_and_the_first_is_the_minimal_one(oracle):
+    import numpy as np
+    from fasterhenry_b200 import fixtures as F
+    for k in range(len(EXAMPLES)):
+        prob = P.Problem.from_json(example_text(k))
+        # the oracle (the reference's dense path, restated) solves it: one
+        # p x p impedance per listed frequency
+        deck = F.Deck(list(prob.nodes), [dict(s) for s in prob.segments], [(a, b) for a, b, _ in prob.ports],
+                      dict(prob.discretization))
+        system = oracle.System(deck)
+        z = np.array([system.impedance(f) for f in prob.frequencies_hz])
+        assert z.shape == (len(prob.frequencies_hz), len(prob.ports), len(prob.ports)), k
+        assert np.all(np.isfinite(z)) and np.all(z[:, range(len(prob.ports)), range(len(prob.ports))].real > 0)
+        # and the document round-trips
+        assert P.Problem.from_json(prob.to_json()).to_json() == prob.to_json()
+    minimal = P.Problem.from_json(example_text(0))
+    assert len(minimal.segments) == 1 and len(minimal.ports) == 1 and minimal.coupling.is_trivial()
+    second = P.Problem.from_json(example_text(1))
+    assert [p[2] for p in second.ports] == ["coil", "sense"] and second.discretization["kind"] == "skin_depth"
+    assert second.segments[3]["width_dir"] == (0.0, 0.0, 1.0)
+    assert not second.coupling.is_all_pairs() and not second.coupling.couples("coil", "sense")
+
+
+@pytest.mark.parametrize("level,anchor,insertion", [
+    ("the top level", '"ports":', '"typo": true, '),
+    ("geometry", '"nodes":', '"typo": true, '),
+    ("a node", '"x": 0.0,', '"typo": true, '),
+    ("a segment", '"a": 0,', '"typo": true, '),
+    ("a port", '"positive": 0,', '"typo": true, '),
+    ("coupling", '"frequencies_hz":', '"coupling": { "typo": true }, '),
+    ("a discretization payload", '"nw": 3,', '"typo": 1, '),
+])
+def test_an_unknown_key_is_rejected_by_name_at_every_level(level, anchor, insertion):
+    minimal = example_text(0)
+    assert minimal.count(anchor) == 1, level
+    with pytest.raises((P.ProblemError, ValueError)) as e:
+        P.Problem.from_json(minimal.replace(anchor, insertion + anchor))
+    assert "typo" in str(e.value), (level, str(e.value))
+    misspelled = minimal.replace('"positive": 0,', '"nmae": "sense", "positive": 0,')
+    with pytest.raises(P.ProblemError, match="nmae"):
+        P.Problem.from_json(misspelled)

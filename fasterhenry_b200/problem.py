@@ -1510,6 +1510,7 @@ def parse_deck_reporting(text: str, fasthenry_compat: bool = False) -> Tuple[Pro
         for cline, g in couple_names:
             if g not in groups:
                 raise DeckError(cline, "'.couples' names group '%s', which no segment carries" % g)
+        _check_transitive(groups, couples, couples_first)
         coupling = A.Coupling.truncated(groups)
         for a, b in couples:
             coupling = coupling.coupled(a, b)
@@ -1519,6 +1520,46 @@ def parse_deck_reporting(text: str, fasthenry_compat: bool = False) -> Tuple[Pro
         coupling = A.Coupling.all_pairs()
     problem = Problem(nodes, segs, port_list, disc, freqs or [], coupling, title)
     return problem, [w for _, _, w in sorted(warnings, key=lambda t: (t[0], t[1]))]
+
+
+def _check_transitive(groups: Sequence[str], pairs: Sequence[Tuple[str, str]], line: int) -> None:
+    """The declared couples must be an equivalence: two groups coupled
+    through others are coupled to each other too (coupling.rs:326-420
+    Coupling::resolve and check_transitive, which the reference's reader
+    applies to a deck's .couples lines).  Groups in order of first
+    appearance over the segments; the error names the first pair, in that
+    order, that is joined but not declared."""
+    names: List[str] = []
+    for g in groups:
+        if g not in names:
+            names.append(g)
+    n = len(names)
+    if n < 3:
+        return
+    index = {g: i for i, g in enumerate(names)}
+    couples = [[a == b for b in range(n)] for a in range(n)]
+    for a, b in pairs:
+        couples[index[a]][index[b]] = couples[index[b]][index[a]] = True
+    parent = list(range(n))
+
+    def find(x: int) -> int:
+        while parent[x] != x:
+            parent[x] = parent[parent[x]]
+            x = parent[x]
+        return x
+
+    for a in range(n):
+        for b in range(a + 1, n):
+            if couples[a][b]:
+                ra, rb = find(a), find(b)
+                if ra != rb:
+                    parent[ra] = rb
+    for a in range(n):
+        for b in range(a + 1, n):
+            if not couples[a][b] and find(a) == find(b):
+                raise DeckError(line, "the .couples declarations are not transitive: groups '%s' and '%s' are "
+                                      "coupled through other groups but not to each other; declare them together "
+                                      "on one .couples line" % (names[a], names[b]))
 
 
 def load(path: str, fasthenry_compat: bool = False) -> Problem:

@@ -273,3 +273,12 @@ def test_a_segment_the_geometry_rejects_is_reported_on_its_line(segment, what):
     with pytest.raises(P.DeckError) as e:
         P.parse_deck(deck)
     assert e.value.line == 5 and what in str(e.value), str(e.value)
+
+
+def test_non_transitive_couples_lines_are_rejected():
+    """fasterhenry-cli/tests/roundtrip.rs:645-674: a b and b c without a c."""
+    with pytest.raises(P.DeckError) as e:
+        P.parse_deck(COUPLE_DECK % ".couples a b\n.couples b c")
+    assert "'a'" in str(e.value) and "'c'" in str(e.value) and e.value.line == 16
+    # declared together, the three are one coupled set
+    assert P.parse_deck(COUPLE_DECK % ".couples a b c").coupling.couples("a", "c")

@@ -98,3 +98,46 @@ def test_an_unknown_key_is_rejected_by_name_at_every_level(level, anchor, insert
     misspelled = minimal.replace('"positive": 0,', '"nmae": "sense", "positive": 0,')
     with pytest.raises(P.ProblemError, match="nmae"):
         P.Problem.from_json(misspelled)
+
+
+def test_plane_deck_matches_the_api_built_geometry():
+    """fasterhenry-cli/tests/roundtrip.rs:187-265: a trace over an
+    extension-form plane reads to exactly the geometry built through the
+    plane library (the plane first, then the trace's top nodes, the trace
+    and its two vias landing on the snapped cell centres), so the two solve
+    to the same Z bit for bit; 20 x 6 cells give 20*6*2 - 20 - 6 bars plus
+    the 3 segments, and 122 nodes once the via feet snap away."""
+    from fasterhenry_b200 import api as A
+    from fasterhenry_b200 import plane as PL
+    deck = P.parse_deck(""".units mm
+.default sigma=5.8e4
+Gp 0 -3 0 10 3 0 0.035 nx=20 ny=6
+n1 x=1 y=0 z=0.5
+n2 x=9 y=0 z=0.5
+n3 x=1 y=0 z=0
+n4 x=9 y=0 z=0
+e1 n1 n2 w=0.2 h=0.035 nwinc=2
+e2 n1 n3 w=0.2 h=0.035
+e3 n2 n4 w=0.2 h=0.035
+.external n1 n2
+.freq fmin=1e9 fmax=1e9 ndec=1
+.end
+""")
+    w, t, sigma = 0.2 * 1e-3, 0.035 * 1e-3, 5.8e4 / 1e-3
+    api = A.Geometry()
+    plane = PL.GroundPlane((0.0, -3.0e-3), (10.0e-3, 3.0e-3), 0.0, t, 20, 6, sigma)
+    centres = plane.build_into(api)
+    xa, xb, zt = 1.0 * 1e-3, 9.0 * 1e-3, 0.5 * 1e-3
+    snap_a, snap_b = plane.attach(centres, (xa, 0.0, 0.0)), plane.attach(centres, (xb, 0.0, 0.0))
+    a, b = api.add_node(A.Node(xa, 0.0, zt)), api.add_node(A.Node(xb, 0.0, zt))
+    api.add_segment(A.SegmentDef(a, b, w, t, sigma))
+    for top, bottom in ((a, snap_a), (b, snap_b)):
+        api.add_segment(A.SegmentDef(top, bottom, w, t, sigma))
+    assert deck.nodes == [(n.x, n.y, n.z) for n in api.nodes]
+    assert [(s["a"], s["b"], s["width"], s["height"], s["sigma"]) for s in deck.segments] == \
+        [(s.a, s.b, s.width, s.height, s.sigma) for s in api.segments]
+    grids = [(1, 1)] * len(api.segments)
+    grids[len(api.segments) - 3] = (2, 1)
+    assert deck.discretization == {"kind": "per_segment", "grids": grids}
+    assert deck.ports[0][:2] == (a, b)
+    assert len(deck.segments) == 20 * 6 * 2 - 20 - 6 + 3 and len(deck.nodes) == 20 * 6 + 2

@@ -976,21 +976,45 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
         for x0, x1 in holed(0):
             for y0, y1 in holed(1):
                 holes.append(PL.Hole.rect((x0, y0), (x1, y1)))
+    def outside(what, shape, effect):
+        # a clause wholly off the footprint is kept (a hole) or dropped (a
+        # contact) with a warning, not an error (inp.rs:2640-2760)
+        pending.append("%s %s lies wholly outside ground plane '%s' (x %s to %s, y %s to %s metres), so it %s; "
+                       "check its coordinates and the deck's .units"
+                       % (what, shape, head, _shown(lo[0]), _shown(hi[0]), _shown(lo[1]), _shown(hi[1]), effect))
+
+    def spanning(rlo, rhi):
+        return "spanning (%s, %s) to (%s, %s) metres" % (_shown(rlo[0]), _shown(rlo[1]), _shown(rhi[0]),
+                                                         _shown(rhi[1]))
+
     for corners in hole_rects:
         rlo, rhi = footprint("'hole rect'", corners)
+        if misses(rlo, rhi):
+            outside("'hole rect'", spanning(rlo, rhi), "removes nothing")
         holes.append(PL.Hole.rect(rlo, rhi))
     for p in hole_points:
         in_slab("'hole point'", p[2])
+        if not contains(p):
+            outside("'hole point'", "at (%s, %s) metres" % (_shown(p[0]), _shown(p[1])), "removes nothing")
         holes.append(PL.Hole.point((p[0], p[1])))
     for p, r in hole_circles:
         in_slab("'hole circle'", p[2])
+        gap = math.hypot(max(lo[0] - p[0], p[0] - hi[0], 0.0), max(lo[1] - p[1], p[1] - hi[1], 0.0))
+        if gap > r + tol:
+            outside("'hole circle'", "centred at (%s, %s) metres with r=%s metres"
+                    % (_shown(p[0]), _shown(p[1]), _shown(r)), "removes nothing")
         holes.append(PL.Hole.circle((p[0], p[1]), r))
     # contacts wholly outside the footprint, or only touching its boundary,
     # refine nothing and are dropped (inp.rs:2695-2760)
     contacts = []
     for corners in contact_rects:
         rlo, rhi = footprint("'contact rect'", corners)
-        if misses(rlo, rhi) or touches(rlo, rhi):
+        if misses(rlo, rhi):
+            outside("'contact rect'", spanning(rlo, rhi), "refines nothing and is ignored")
+            continue
+        if touches(rlo, rhi):
+            pending.append("'contact rect' %s only touches the boundary of ground plane '%s', so it refines "
+                           "nothing and is ignored" % (spanning(rlo, rhi), head))
             continue
         contacts.append(PL.ContactRegion.new(rlo, rhi, (2, 2), 2.0))
     def decay_region(what, centre, widths, cell, limit):
@@ -1015,7 +1039,12 @@ def _plane_corner_form(head: str, body: str, line: int, unit: float, sigma_defau
 
     for what, centre, v in contact_decays:
         region = decay_region(what, centre, plane_pair(v[0:2]), plane_pair(v[2:4]), plane_pair(v[4:6]))
-        if misses(region.lo, region.hi) or touches(region.lo, region.hi):
+        if misses(region.lo, region.hi):
+            outside(what, spanning(region.lo, region.hi), "refines nothing and is ignored")
+            continue
+        if touches(region.lo, region.hi):
+            pending.append("%s %s only touches the boundary of ground plane '%s', so it refines nothing and is "
+                           "ignored" % (what, spanning(region.lo, region.hi), head))
             continue
         contacts.append(region)
     for what, refine in contact_lines:

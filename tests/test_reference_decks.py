@@ -141,3 +141,19 @@ e3 n2 n4 w=0.2 h=0.035
     assert deck.discretization == {"kind": "per_segment", "grids": grids}
     assert deck.ports[0][:2] == (a, b)
     assert len(deck.segments) == 20 * 6 * 2 - 20 - 6 + 3 and len(deck.nodes) == 20 * 6 + 2
+
+
+@pytest.mark.parametrize("replacement", ["+ contact rect (11, 3, 0, 2, 2, 1, 1)",
+                                         "+ contact rect (11.000000000000002, 3, 0, 2, 2, 1, 1)"])
+def test_a_contact_rect_touching_the_plane_edge_is_dropped_with_a_warning(replacement):
+    """fasterhenry-cli/tests/roundtrip.rs:774-805: the deck reads as if the
+    clause were absent, with one warning."""
+    with open(os.path.join(DECKS, "plane_fasthenry.inp")) as f:
+        text = f.read()
+    original = "+ contact rect (5, 3, 0, 2, 2, 1, 1)"
+    assert original in text.splitlines()
+    baseline, none = P.parse_deck_reporting(text.replace(original + "\n", ""))
+    assert none == []
+    deck, warnings = P.parse_deck_reporting(text.replace(original, replacement))
+    assert len(warnings) == 1 and "ignored" in warnings[0].message
+    assert deck.to_json() == baseline.to_json()
